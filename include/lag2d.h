@@ -1,0 +1,134 @@
+/*
+ * lag2d.h -- C-ABI of the B200 Lagrangian DG time step (Lag2D, curved P2).
+ *
+ * The reference has no FFI: its seam is the Fortran subroutine
+ *   getsolvdg_lag(intfac, inpoel, iptri, ipqua, bface, cooro, coord, coora,
+ *                 geofa, geoel, gesgt0, gesgq0, uchar, unkno, unold, unkaw,
+ *                 unkgd, unogd, strnq_devtp, ltelem, estri, esqua, itime,
+ *                 amatr, amagd, ustar, coold, esuv1, esuv2)
+ * (srccurv-lag/Getrhslag.f90:1553-1555), called once per time step from the
+ * driver loop (srccurv-lag/dgflo2d.f90:372-373), with the inner seams
+ * getrhsdg_lag_mcnew (Getrhslagmc.f90:6693), getcellvol_lag
+ * (Limiterlag.f90:1869) and getdelt_lag (Getrhslag.f90:20600).
+ *
+ * Every entry point is bind(C)-compatible: plain ints, doubles and pointers.
+ * Arrays use the Fortran layouts (column-major, 1-based ids):
+ *   unkno(ndegr, nq, nsize), coord(2, npoin), ustar(2, npoin),
+ *   geoel(24, nsize), amatr(nmatr, ncell), ipqua(9, nquad), iptri(6, ntria),
+ *   bface(5, nbfac), esqua(4, nquad), esuv1(npoin1), esuv2(npoin+1).
+ * The caller owns host buffers; the library owns device buffers.  One CUDA
+ * stream per handle; calls on one handle are not thread-safe.  Every call
+ * returns LAG2D_OK (0) or a status code; lag2d_last_error() gives text.
+ */
+#ifndef LAG2D_H
+#define LAG2D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LAG2D_OK 0
+#define LAG2D_EINVAL 1      /* bad argument or array size */
+#define LAG2D_ECUDA 2       /* CUDA runtime error (message in lag2d_last_error) */
+#define LAG2D_EUNSUP 3      /* configuration outside the built path */
+#define LAG2D_ENONPHYS 4    /* non-positive cell volume or NaN in the state */
+#define LAG2D_ESTENCIL 5    /* WENO vertex valence the reference rejects (WENO.f90:7699) */
+#define LAG2D_ENODEV 6      /* no usable CUDA device */
+
+typedef struct lag2d_handle lag2d_handle;
+
+/* Mesh arrays as preprocess1/preprocess2 leave them (Preprocess.f90:4-1009)
+ * and getesuel produces them (dgflo2d.f90:1220-1309). */
+typedef struct {
+  int ntria, nquad, npoin, nbfac;
+  const int *iptri;     /* iptri(6, ntria)   1-based node ids            */
+  const int *ipqua;     /* ipqua(9, nquad)   1-based node ids            */
+  const int *bface;     /* bface(5, nbfac)   n1, n2, code, sub-code, mid */
+  const int *esuv1;     /* esuv1(npoin1)     cells surrounding points    */
+  const int *esuv2;     /* esuv2(npoin+1)    CSR offsets, esuv2(1) = 0   */
+  const int *esqua;     /* esqua(4, nquad)   face neighbours / ghost ids */
+  const double *coold;  /* coold(2, npoin)   initial coordinates         */
+} lag2d_mesh;
+
+/* The module-constant knobs the step reads (dgflo2d.f90:4-56). */
+typedef struct {
+  int npoly, ndegr, mdegr, nq;
+  int nstag;            /* 2 or 3 (SSP-RK2/3)                            */
+  int ndt;              /* 1: CFL dt (getdelt_lag), 0: fixed dtfix       */
+  int ncase;            /* initial-condition / source case               */
+  int nlimi, ndens;
+  int ngausd, ngausd_geo;
+  int precision;        /* 0: FP64; 1: FP32-mixed (not built: EUNSUP)    */
+  int nsedov;           /* number of Sedov energy cells (<= 4)           */
+  int sedov_cell[4];    /* their 1-based ids                             */
+  double gamlg, cfl, cdrho, cimpd, tend, sedov_energy;
+} lag2d_config;
+
+/* Create a handle: validates the mesh, builds the device connectivity
+ * (node-to-corner gather lists, WENO stencils, boundary node masks) and
+ * allocates device state.  Replaces the array set-up the Fortran driver does
+ * before its time loop (dgflo2d.f90:61-350). */
+int lag2d_create(const lag2d_mesh *mesh, const lag2d_config *cfg, lag2d_handle **out);
+
+/* Initial geometry, mass matrix and DOFs computed on the device:
+ * getgeoel_initial_lag + getgeoelho_initial_lag (GetInitial.f90:1278,1704),
+ * inifield_mcnew (Getrhslagmc.f90:3293) and getunkno_initial_lag
+ * (GetInitial.f90:151).  Sets the device state to it (coord = coold,
+ * ustar = 0) and copies geoel, amatr, unkno to the host pointers that are
+ * not NULL. */
+int lag2d_init_fields(lag2d_handle *h, double *geoel, double *amatr, double *unkno);
+
+/* Upload a state: unkno(ndegr,nq,nsize), coord(2,npoin), ustar(2,npoin),
+ * geoel(24,nsize) (fields 1-4 and 19-21 are read), amatr(nmatr,ncell).
+ * geoel/amatr may be NULL to keep the device copies. */
+int lag2d_set_state(lag2d_handle *h, const double *unkno, const double *coord,
+                    const double *ustar, const double *geoel, const double *amatr);
+
+/* One time step: getsolvdg_lag (Getrhslag.f90:1553-2035) followed by the
+ * driver's copy of unold into unkno and cooro into coord
+ * (dgflo2d.f90:407-423).  dtfix and tacru are the driver's mutable module
+ * scalars (in/out).  Synchronises the handle's stream. */
+int lag2d_step(lag2d_handle *h, int itime, double *dtfix, double *tacru);
+
+/* nsteps steps of the driver loop (dgflo2d.f90:358-472) with no host
+ * synchronisation in between; stops early (on the device) once
+ * |tacru - tend| / tend <= 1e-11 as the driver does (dgflo2d.f90:459).
+ * *done receives the number of steps taken.  Captured in a CUDA graph. */
+int lag2d_run(lag2d_handle *h, int itime0, int nsteps, double *dtfix, double *tacru, int *done);
+
+/* Download the state; any pointer may be NULL. geoel(24,nsize) receives the
+ * device geometry (fields 1-4, 19-21 and the current volume centre 5-6). */
+int lag2d_get_state(lag2d_handle *h, double *unkno, double *coord, double *ustar, double *geoel);
+
+/* getrhsdg_lag_mcnew (Getrhslagmc.f90:6693-8732, curved branch 7556-7710)
+ * on the current device state with ustar as the previous nodal velocity:
+ * limits unkno in place on the device, updates ustar, writes
+ * rhsel(ndegr,nq,ncell) and the Persson marks flags(ncell) (either may be
+ * NULL).  For per-stage parity checks. */
+int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags);
+
+/* weno_char_quad_orthgl (WENO.f90:5927) on the cells with flags(ie) != 0,
+ * applied to the device state.  For limiter parity checks. */
+int lag2d_weno(lag2d_handle *h, const int *flags);
+
+/* getcellvol_lag (Limiterlag.f90:1869) on the device coordinates; returns
+ * geoel(24,nsize) with fields 3, 5, 6 refreshed if geoel is not NULL. */
+int lag2d_cellvol(lag2d_handle *h, double *geoel);
+
+/* Number of this library's kernel launches since the handle was created. */
+long long lag2d_kernel_launches(const lag2d_handle *h);
+
+/* Average device time (ms) per launch of the named kernel family over the
+ * launches timed since lag2d_timing(h, 1); families: "corner", "node",
+ * "rhs", "update", "persson", "weno", "nodes", "geom", "dt".  Returns -1
+ * when timing is off or the family is unknown. */
+int lag2d_timing(lag2d_handle *h, int enable);
+double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *launches);
+
+void lag2d_destroy(lag2d_handle *h);
+const char *lag2d_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,77 @@
+"""Run configuration of the Lag2D time step and the named benchmark workloads.
+
+:class:`StepConfig` carries the knobs of the reference's ``module constant``
+(dgflo2d.f90:4-56) that the curved-P2 time step reads.  The workloads mirror
+the benchmark table: synthetic structured meshes with the sizes, gases and
+initial conditions of the reference's test cases (the reference ships no
+input files).
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Tuple
+
+from .mesh import Mesh, quad_mesh
+
+__all__ = ["StepConfig", "workload", "WORKLOADS"]
+
+
+@dataclasses.dataclass
+class StepConfig:
+    npoly: int = 2
+    ndegr: int = 6
+    mdegr: int = 6
+    nq: int = 4
+    nstag: int = 3          # 2: SSP-RK2, 3: SSP-RK3 (rklag, dgflo2d.f90:320-321)
+    ndt: int = 1            # 1: CFL-controlled dt (getdelt_lag), 0: fixed dtfix
+    ncase: int = 1          # initial-condition / source case (getunkin)
+    nlimi: int = 6
+    ndens: int = 1          # first field is the specific volume tau
+    ngausd: int = 7         # triangle volume rule (ctrl)
+    ngausd_geo: int = 7     # triangle geometry rule (ctrl)
+    gamlg: float = 1.4
+    cfl: float = 0.3
+    cdrho: float = 1.0      # sub-cell density correction weight
+    cimpd: float = 1.0      # shock-impedance weight of the nodal solver
+    tend: float = 1.0
+    dtfix: float = 1.0e-4   # initial / fixed time step
+    sedov_cells: Tuple[int, ...] = ()      # 1-based cells receiving the Sedov energy
+    sedov_energy: float = 0.244816
+
+    @property
+    def nmatr(self) -> int:
+        return 16 if self.npoly == 2 else 4
+
+
+def _tgv(n: int) -> Tuple[Mesh, StepConfig]:
+    m = quad_mesh(n, n, 0.0, 1.0, 0.0, 1.0)
+    c = StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=3, cfl=0.1, tend=10.0)
+    return m, c
+
+
+def _sedov(n: int) -> Tuple[Mesh, StepConfig]:
+    """Full-box Sedov as the reference's active setup runs it
+    (Getrhslagmc.f90:5634: E = 0.244816 in each of the 4 central cells);
+    ``n`` x ``n`` cells on [-1.2, 1.2]^2."""
+    m = quad_mesh(n, n, -1.2, 1.2, -1.2, 1.2)
+    h = n // 2
+    cells = ((h - 1) * n + h, (h - 1) * n + h + 1, h * n + h, h * n + h + 1)
+    c = StepConfig(ncase=7, gamlg=1.4, nstag=3, cfl=0.1, tend=1.0, sedov_cells=cells)
+    return m, c
+
+
+WORKLOADS = {
+    # Taylor-Green vortex: [0,1]^2, gamma 5/3, P2, RK3, energy source on
+    "tgv1024": lambda: _tgv(1024),
+    "tgv256": lambda: _tgv(256),
+    "tgv64": lambda: _tgv(64),
+    "tgv16": lambda: _tgv(16),
+    # Sedov blast: [0,1.2]^2, gamma 1.4, energy in the corner cell
+    "sedov128": lambda: _sedov(128),
+    "sedov32": lambda: _sedov(32),
+    "sedov16": lambda: _sedov(16),
+}
+
+
+def workload(name: str) -> Tuple[Mesh, StepConfig]:
+    return WORKLOADS[name]()

@@ -1,0 +1,641 @@
+// Host side of the Lag2D C-ABI (include/lag2d.h): handle, device memory,
+// connectivity set-up and the per-step launch sequence of getsolvdg_lag.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "lag2d.h"
+#include "lag2d_device.cuh"
+
+namespace lag2d {
+void set_tables(const QuadTables &q, cudaStream_t st);
+void launch_geom(const Dev &d, cudaStream_t st, const double *X, const double *Y);
+void launch_center_geom(const Dev &d, cudaStream_t st);
+void launch_reset_count(const Dev &d, cudaStream_t st);
+void launch_persson(const Dev &d, cudaStream_t st);
+void launch_flags_from_host(const Dev &d, cudaStream_t st, const int *flags);
+void launch_weno(const Dev &d, cudaStream_t st);
+void launch_weno_commit(const Dev &d, cudaStream_t st);
+void launch_corner(const Dev &d, cudaStream_t st);
+void launch_node(const Dev &d, cudaStream_t st);
+void launch_rhs(const Dev &d, cudaStream_t st);
+int dt_blocks(const Dev &d);
+void launch_dt(const Dev &d, cudaStream_t st, int ndt);
+void launch_update(const Dev &d, cudaStream_t st, double alfa);
+void launch_nodes(const Dev &d, cudaStream_t st, double alfa);
+void launch_copyback(const Dev &d, cudaStream_t st);
+void launch_step_begin(const Dev &d, cudaStream_t st, int itime);
+void launch_step_end(const Dev &d, cudaStream_t st, int check);
+void launch_init(const Dev &d, cudaStream_t st);
+void launch_init_msub(const Dev &d, cudaStream_t st);
+}  // namespace lag2d
+
+using namespace lag2d;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(LAG2D_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+struct Family {
+  double ms = 0.0;
+  long long n = 0;
+};
+
+struct lag2d_handle {
+  Dev d{};
+  lag2d_config cfg{};
+  cudaStream_t st = nullptr;
+  std::vector<void *> allocs;
+  int *flags_dev = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  long long launches = 0;
+  bool timing = false;
+  std::map<std::string, Family> fam;
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+};
+
+template <typename T>
+static int dalloc(lag2d_handle *h, T **p, size_t n) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) return fail(LAG2D_ECUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
+  h->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return LAG2D_OK;
+}
+
+// Quadrature literals of ruqope / ruqope_lobatto (dgflo2d.f90:2497-2783),
+// points ordered as the reference's 2-D loops produce them.
+static void fill_rule(int n, bool lobatto, double (*pos)[2], double *w) {
+  double p[6], q[6];
+  if (lobatto) {
+    p[0] = -1.0; p[1] = -0.6546536707079771437983; p[2] = 0.0; p[3] = 0.6546536707079771437983; p[4] = 1.0;
+    q[0] = 0.1; q[1] = 0.544444444444444444444; q[2] = 0.7111111111111111111111; q[3] = 0.544444444444444444444;
+    q[4] = 0.1;
+  } else if (n == 5) {
+    p[2] = 0.0;
+    p[3] = 0.5384693101056830910363144; p[1] = -0.5384693101056830910363144;
+    p[4] = 0.9061798459386639927976269; p[0] = -0.9061798459386639927976269;
+    q[2] = 0.5688888888888888888888889;
+    q[3] = 0.4786286704993664680412915; q[1] = 0.4786286704993664680412915;
+    q[4] = 0.2369268850561890875142640; q[0] = 0.2369268850561890875142640;
+  } else {
+    p[0] = 0.2386191860831969086305017; p[1] = -0.2386191860831969086305017;
+    p[2] = 0.6612093864662645136613996; p[3] = -0.6612093864662645136613996;
+    p[4] = -0.9324695142031520278123016; p[5] = 0.9324695142031520278123016;
+    q[0] = 0.4679139345726910; q[1] = 0.4679139345726910;
+    q[2] = 0.3607615730481386; q[3] = 0.3607615730481386;
+    q[4] = 0.1713244923791704; q[5] = 0.1713244923791704;
+  }
+  int ig = 0;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) {
+      w[ig] = q[i] * q[j];
+      pos[ig][0] = p[i];
+      pos[ig][1] = p[j];
+      ig++;
+    }
+}
+
+static const int kIPQSG[4][4] = {{0, 4, 8, 7}, {4, 1, 5, 8}, {8, 5, 2, 6}, {7, 8, 6, 3}};
+
+// WENO stencil of every quad from esqua and the cells-surrounding-point
+// lists, ordered as weno_stncl_quad_orthol3 orders it (WENO.f90:7646-7704).
+static void build_stencils(const lag2d_mesh *m, std::vector<int> &sten) {
+  const int nquad = m->nquad, ntria = m->ntria;
+  sten.assign(9 * (size_t)nquad, -1);
+  for (int iq = 0; iq < nquad; iq++) {
+    const int ielem = iq + ntria;  // 0-based
+    int ielaj[9];
+    ielaj[0] = ielem + 1;
+    // the reference reads esqua at the global cell id here (WENO.f90:7648)
+    const bool inrange = ielem < nquad;
+    for (int k = 0; k < 4; k++) ielaj[1 + k] = inrange ? m->esqua[4 * (size_t)ielem + k] : 0;
+    for (int k = 5; k < 9; k++) ielaj[k] = 0;
+    bool bad = false;
+    for (int iv = 0; iv < 4 && !bad; iv++) {
+      const int ip = m->ipqua[9 * (size_t)iq + iv];
+      int jelaj[5] = {0, 0, 0, 0, 0}, nvaj = 0;
+      for (int s = m->esuv2[ip - 1]; s < m->esuv2[ip]; s++) {
+        int je = m->esuv1[s];
+        if (je != ielem + 1) {
+          if (nvaj < 5) jelaj[nvaj] = je;
+          nvaj++;
+        }
+      }
+      int idxod = 1, idxiv[3] = {0, 0, 0};
+      for (int a = 0; a < 3; a++)
+        for (int f = 0; f < 4; f++)
+          if (jelaj[a] == ielaj[f + 1]) { idxod *= (f + 1); idxiv[a] = 1; }
+      for (int a = 0; a < 3; a++)
+        if (idxiv[a] == 0) {
+          if (idxod == 2) ielaj[5] = jelaj[a];
+          else if (idxod == 6) ielaj[6] = jelaj[a];
+          else if (idxod == 12) ielaj[7] = jelaj[a];
+          else if (idxod == 4) ielaj[8] = jelaj[a];
+          else bad = true;
+        }
+    }
+    if (bad) { sten[iq] = -2; continue; }
+    bool complete = true;
+    for (int k = 0; k < 9; k++) complete &= ielaj[k] != 0;
+    if (!complete) continue;
+    for (int k = 0; k < 9; k++) sten[k * (size_t)nquad + iq] = ielaj[k] - 1;
+  }
+}
+
+static double now_ms_event(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Launch helper: counts launches and, when timing is on, brackets the
+// launch with events on the handle's stream.
+template <typename F>
+static void run(lag2d_handle *h, const char *family, F &&f, int nlaunch = 1) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (h->timing) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, h->st);
+  }
+  f();
+  h->launches += nlaunch;
+  if (h->timing) {
+    cudaEventRecord(b, h->st);
+    h->pending.push_back({family, {a, b}});
+  }
+}
+
+static void flush_timing(lag2d_handle *h) {
+  for (auto &p : h->pending) {
+    cudaEventSynchronize(p.second.second);
+    Family &f = h->fam[p.first];
+    f.ms += now_ms_event(p.second.first, p.second.second);
+    f.n += 1;
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  h->pending.clear();
+}
+
+static const double kRK[2][3] = {{0.0, 0.5, 0.0}, {0.0, 0.75, 0.3333333333333333}};
+
+// getrhsdg_lag_mcnew, curved P2 branch (Getrhslagmc.f90:7556-7710)
+static void enqueue_rhs(lag2d_handle *h) {
+  const Dev &d = h->d;
+  run(h, "persson", [&] { launch_reset_count(d, h->st); launch_persson(d, h->st); }, 2);
+  run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
+  run(h, "corner", [&] { launch_corner(d, h->st); });
+  run(h, "node", [&] { launch_node(d, h->st); });
+  run(h, "rhs", [&] { launch_rhs(d, h->st); });
+}
+
+// getsolvdg_lag (Getrhslag.f90:1553-2035) + the driver copy-back
+static void enqueue_step(lag2d_handle *h, int itime) {
+  const Dev &d = h->d;
+  const int nstag = h->cfg.nstag;
+  run(h, "geom", [&] { launch_step_begin(d, h->st, itime); launch_geom(d, h->st, d.xn, d.yn); }, 2);
+  for (int istag = 1; istag <= nstag; istag++) {
+    const double alfa = kRK[nstag - 2][istag - 1];
+    enqueue_rhs(h);
+    if (istag == 1) run(h, "dt", [&] { launch_dt(d, h->st, h->cfg.ndt); }, 2);
+    run(h, "update", [&] { launch_update(d, h->st, alfa); });
+    run(h, "nodes", [&] { launch_nodes(d, h->st, alfa); });
+    run(h, "geom", [&] { launch_center_geom(d, h->st); launch_geom(d, h->st, d.xs, d.ys); }, 2);
+  }
+  run(h, "copy", [&] { launch_copyback(d, h->st); launch_step_end(d, h->st, 1); }, 2);
+}
+
+static int read_status(lag2d_handle *h) {
+  Scalars s;
+  CK(cudaMemcpyAsync(&s, h->d.sc_dev, sizeof(Scalars), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  if (s.status & ST_STENCIL)
+    return fail(LAG2D_ESTENCIL, "WENO: a troubled quad has a vertex valence the reference rejects");
+  if (s.status & ST_NONPHYS) return fail(LAG2D_ENONPHYS, "non-positive cell volume");
+  return LAG2D_OK;
+}
+
+extern "C" {
+
+const char *lag2d_last_error(void) { return g_err.c_str(); }
+
+int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out) {
+  if (!m || !c || !out) return fail(LAG2D_EINVAL, "null argument");
+  *out = nullptr;
+  if (m->nquad <= 0 || m->npoin <= 0 || m->nbfac < 0 || m->ntria < 0)
+    return fail(LAG2D_EINVAL, "mesh sizes must be positive");
+  if (!m->ipqua || !m->bface || !m->esuv1 || !m->esuv2 || !m->esqua || !m->coold)
+    return fail(LAG2D_EINVAL, "missing mesh array");
+  if (m->ntria > 0) return fail(LAG2D_EUNSUP, "triangles are not built on this path yet");
+  if (c->npoly != 2 || c->ndegr != 6 || c->nq != 4 || c->ndens != 1)
+    return fail(LAG2D_EUNSUP, "only P2 (npoly=2, ndegr=6, nq=4, ndens=1) is built");
+  if (c->mdegr < 1 || c->mdegr > 6) return fail(LAG2D_EINVAL, "mdegr out of range");
+  if (c->nstag != 2 && c->nstag != 3) return fail(LAG2D_EINVAL, "nstag must be 2 or 3");
+  if (c->precision != 0) return fail(LAG2D_EUNSUP, "FP32-mixed precision is not built");
+  if (c->nsedov < 0 || c->nsedov > 4) return fail(LAG2D_EINVAL, "nsedov must be 0..4");
+  if (c->ncase != 1 && c->ncase != 2 && c->ncase != 3 && c->ncase != 6 && c->ncase != 7)
+    return fail(LAG2D_EUNSUP, "initial-condition case not built");
+  const int ncell = m->ntria + m->nquad;
+  for (size_t i = 0; i < 9 * (size_t)m->nquad; i++)
+    if (m->ipqua[i] < 1 || m->ipqua[i] > m->npoin) return fail(LAG2D_EINVAL, "ipqua node id out of range");
+  for (size_t i = 0; i < (size_t)m->nbfac; i++) {
+    const int *b = m->bface + 5 * i;
+    if (b[0] < 1 || b[0] > m->npoin || b[1] < 1 || b[1] > m->npoin || b[4] < 1 || b[4] > m->npoin)
+      return fail(LAG2D_EINVAL, "bface node id out of range");
+  }
+  if (m->esuv2[0] != 0) return fail(LAG2D_EINVAL, "esuv2(1) must be 0");
+  for (int p = 0; p < m->npoin; p++)
+    if (m->esuv2[p + 1] < m->esuv2[p]) return fail(LAG2D_EINVAL, "esuv2 not monotone");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LAG2D_ENODEV, "no CUDA device");
+
+  lag2d_handle *h = new lag2d_handle();
+  h->cfg = *c;
+  Dev &d = h->d;
+  d.ntria = m->ntria; d.nquad = m->nquad; d.npoin = m->npoin; d.nbfac = m->nbfac; d.ncell = ncell;
+  d.ndegr = c->ndegr; d.mdegr = c->mdegr; d.ncase = c->ncase; d.nlimi = c->nlimi;
+  d.gamlg = c->gamlg; d.cfl = c->cfl; d.cdrho = c->cdrho; d.cimpd = c->cimpd; d.tend = c->tend;
+  d.sedov_energy = c->sedov_energy; d.nsedov = c->nsedov;
+  for (int i = 0; i < 4; i++) d.sedov_cell[i] = c->sedov_cell[i];
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return fail(LAG2D_ECUDA, "cudaStreamCreate failed");
+  }
+  const int nq = m->nquad, np = m->npoin;
+  // ---- connectivity
+  std::vector<int> ipq(9 * (size_t)nq), esq(4 * (size_t)nq), sten;
+  for (int iq = 0; iq < nq; iq++)
+    for (int k = 0; k < 9; k++) ipq[k * (size_t)nq + iq] = m->ipqua[9 * (size_t)iq + k] - 1;
+  for (int iq = 0; iq < nq; iq++)
+    for (int k = 0; k < 4; k++) {
+      int v = m->esqua[4 * (size_t)iq + k];
+      esq[k * (size_t)nq + iq] = (v >= 1 && v <= ncell) ? v - 1 : -1;
+    }
+  build_stencils(m, sten);
+  // node -> corner-face lists in the order getriem_quadsubg2 scatters
+  std::vector<int> cnt(np + 1, 0), nodecf(32 * (size_t)nq);
+  for (int iq = 0; iq < nq; iq++)
+    for (int isg = 0; isg < 4; isg++)
+      for (int ivsg = 0; ivsg < 4; ivsg++) cnt[ipq[kIPQSG[isg][ivsg] * (size_t)nq + iq] + 1] += 2;
+  for (int p = 0; p < np; p++) cnt[p + 1] += cnt[p];
+  std::vector<int> fillp(cnt.begin(), cnt.end() - 1);
+  for (int iq = 0; iq < nq; iq++)
+    for (int isg = 0; isg < 4; isg++)
+      for (int ivsg = 0; ivsg < 4; ivsg++) {
+        int p = ipq[kIPQSG[isg][ivsg] * (size_t)nq + iq];
+        for (int f = 0; f < 2; f++) nodecf[fillp[p]++] = iq * 32 + (f + 2 * (ivsg + 4 * isg));
+      }
+  // wall masks (getndvelo_lagsubg, Getrhslaggauss.f90:4420-4545)
+  std::vector<unsigned char> mask(np, 0);
+  for (int f = 0; f < m->nbfac; f++) {
+    const int *b = m->bface + 5 * (size_t)f;
+    const int nodes[3] = {b[0] - 1, b[1] - 1, b[4] - 1};
+    for (int k = 0; k < 3; k++) {
+      if (c->ncase == 2 || b[2] == 25) mask[nodes[k]] |= 4;
+      if (b[2] == 22 && b[3] == 221) mask[nodes[k]] |= 2;
+      if (b[2] == 22 && b[3] == 222) mask[nodes[k]] |= 1;
+      if (b[2] == 25) mask[nodes[k]] |= 3;
+    }
+  }
+  int rc = LAG2D_OK;
+  auto A = [&](auto **p, size_t n) { if (rc == LAG2D_OK) rc = dalloc(h, p, n); };
+  int *ipq_d, *esq_d, *sten_d, *ptr_d, *ncf_d;
+  unsigned char *mask_d;
+  double *x0, *y0;
+  A(&ipq_d, ipq.size()); A(&esq_d, esq.size()); A(&sten_d, sten.size());
+  A(&ptr_d, cnt.size()); A(&ncf_d, nodecf.size()); A(&mask_d, mask.size());
+  A(&x0, np); A(&y0, np);
+  A(&d.rc, ncell); A(&d.sc, ncell); A(&d.mass, ncell); A(&d.g19, ncell); A(&d.g20, ncell); A(&d.g21, ncell);
+  A(&d.vol, ncell); A(&d.vcx, ncell); A(&d.vcy, ncell); A(&d.msub, 4 * (size_t)nq);
+  A(&d.Un, NU * (size_t)ncell); A(&d.Us, NU * (size_t)ncell);
+  A(&d.xn, np); A(&d.yn, np); A(&d.xs, np); A(&d.ys, np); A(&d.us, np); A(&d.vs, np);
+  A(&d.amatr, 16 * (size_t)ncell); A(&d.rhs, NU * (size_t)ncell); A(&d.cf, 5 * 32 * (size_t)nq);
+  A(&d.flag, ncell); A(&d.geoph, 2 * (size_t)ncell); A(&d.mapmt, 4 * (size_t)ncell);
+  A(&d.Uw, 20 * (size_t)nq); A(&d.wlist, nq); A(&d.wcount, 1);
+  A(&d.dtpart, 2 * (size_t)dt_blocks(d) + 2); A(&d.sc_dev, 1); A(&h->flags_dev, ncell);
+  if (rc != LAG2D_OK) { lag2d_destroy(h); return rc; }
+  d.ipq = ipq_d; d.esq = esq_d; d.stencil = sten_d; d.node_ptr = ptr_d; d.node_cf = ncf_d;
+  d.bcmask = mask_d; d.x0 = x0; d.y0 = y0;
+  std::vector<double> xx(np), yy(np);
+  for (int p = 0; p < np; p++) { xx[p] = m->coold[2 * (size_t)p]; yy[p] = m->coold[2 * (size_t)p + 1]; }
+#define UP(dst, src, n) cudaMemcpyAsync((void *)(dst), (src), (n) * sizeof(*(src)), cudaMemcpyHostToDevice, h->st)
+  UP(ipq_d, ipq.data(), ipq.size()); UP(esq_d, esq.data(), esq.size()); UP(sten_d, sten.data(), sten.size());
+  UP(ptr_d, cnt.data(), cnt.size()); UP(ncf_d, nodecf.data(), nodecf.size()); UP(mask_d, mask.data(), mask.size());
+  UP(x0, xx.data(), np); UP(y0, yy.data(), np);
+  UP(d.xn, xx.data(), np); UP(d.yn, yy.data(), np); UP(d.xs, xx.data(), np); UP(d.ys, yy.data(), np);
+#undef UP
+  QuadTables qt;
+  fill_rule(5, false, qt.g25, qt.w25);
+  fill_rule(6, false, qt.g36, qt.w36);
+  fill_rule(5, true, qt.l25, qt.wl25);
+  set_tables(qt, h->st);
+  Scalars s0{};
+  cudaMemcpyAsync(d.sc_dev, &s0, sizeof(Scalars), cudaMemcpyHostToDevice, h->st);
+  run(h, "init", [&] { launch_init_msub(d, h->st); });
+  if (cudaStreamSynchronize(h->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    lag2d_destroy(h);
+    return fail(LAG2D_ECUDA, "device set-up failed");
+  }
+  *out = h;
+  return LAG2D_OK;
+}
+
+static int download_geoel(lag2d_handle *h, double *geoel) {
+  const Dev &d = h->d;
+  const int ncell = d.ncell, nsize = ncell + d.nbfac;
+  std::vector<double> f(ncell);
+  std::fill(geoel, geoel + 24 * (size_t)nsize, 0.0);
+  double *src[9] = {d.rc, d.sc, d.vol, d.mass, d.vcx, d.vcy, d.g19, d.g20, d.g21};
+  const int slot[9] = {0, 1, 2, 3, 4, 5, 18, 19, 20};
+  for (int k = 0; k < 9; k++) {
+    CK(cudaMemcpyAsync(f.data(), src[k], ncell * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int e = 0; e < ncell; e++) geoel[24 * (size_t)e + slot[k]] = f[e];
+  }
+  return LAG2D_OK;
+}
+
+static int download_unkno(lag2d_handle *h, const double *U, double *unkno) {
+  const Dev &d = h->d;
+  const int ncell = d.ncell, nsize = ncell + d.nbfac;
+  std::vector<double> f(NU * (size_t)ncell);
+  CK(cudaMemcpyAsync(f.data(), U, f.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  std::fill(unkno, unkno + NU * (size_t)nsize, 0.0);
+  for (int e = 0; e < ncell; e++)
+    for (int q = 0; q < NQ; q++)
+      for (int k = 0; k < NDEG; k++) unkno[(size_t)e * NU + q * NDEG + k] = f[(q * NDEG + k) * (size_t)ncell + e];
+  return LAG2D_OK;
+}
+
+static int download_xy(lag2d_handle *h, const double *X, const double *Y, double *xy) {
+  const int np = h->d.npoin;
+  std::vector<double> a(np), b(np);
+  CK(cudaMemcpyAsync(a.data(), X, np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(b.data(), Y, np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  for (int p = 0; p < np; p++) { xy[2 * (size_t)p] = a[p]; xy[2 * (size_t)p + 1] = b[p]; }
+  return LAG2D_OK;
+}
+
+int lag2d_init_fields(lag2d_handle *h, double *geoel, double *amatr, double *unkno) {
+  if (!h) return fail(LAG2D_EINVAL, "null handle");
+  Dev &d = h->d;
+  const int ncell = d.ncell, np = d.npoin;
+  run(h, "init", [&] { launch_init(d, h->st); }, 2);
+  CK(cudaMemcpyAsync(d.Us, d.Un, NU * (size_t)ncell * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(d.xn, d.x0, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(d.yn, d.y0, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(d.xs, d.x0, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(d.ys, d.y0, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemsetAsync(d.us, 0, np * sizeof(double), h->st));
+  CK(cudaMemsetAsync(d.vs, 0, np * sizeof(double), h->st));
+  run(h, "geom", [&] { launch_geom(d, h->st, d.xn, d.yn); });
+  int st = read_status(h);
+  if (st != LAG2D_OK) return st;
+  if (geoel) { int r = download_geoel(h, geoel); if (r) return r; }
+  if (amatr) {
+    std::vector<double> f(16 * (size_t)ncell);
+    CK(cudaMemcpyAsync(f.data(), d.amatr, f.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int e = 0; e < ncell; e++)
+      for (int k = 0; k < 16; k++) amatr[16 * (size_t)e + k] = f[k * (size_t)ncell + e];
+  }
+  if (unkno) { int r = download_unkno(h, d.Un, unkno); if (r) return r; }
+  return LAG2D_OK;
+}
+
+int lag2d_set_state(lag2d_handle *h, const double *unkno, const double *coord, const double *ustar,
+                    const double *geoel, const double *amatr) {
+  if (!h || !unkno || !coord || !ustar) return fail(LAG2D_EINVAL, "null argument");
+  Dev &d = h->d;
+  const int ncell = d.ncell, np = d.npoin;
+  std::vector<double> f(NU * (size_t)ncell);
+  for (int e = 0; e < ncell; e++)
+    for (int q = 0; q < NQ; q++)
+      for (int k = 0; k < NDEG; k++) f[(q * NDEG + k) * (size_t)ncell + e] = unkno[(size_t)e * NU + q * NDEG + k];
+  CK(cudaMemcpyAsync(d.Un, f.data(), f.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(d.Us, f.data(), f.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  std::vector<double> a(np), b(np);
+  for (int p = 0; p < np; p++) { a[p] = coord[2 * (size_t)p]; b[p] = coord[2 * (size_t)p + 1]; }
+  CK(cudaMemcpyAsync(d.xn, a.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(d.yn, b.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(d.xs, a.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(d.ys, b.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  for (int p = 0; p < np; p++) { a[p] = ustar[2 * (size_t)p]; b[p] = ustar[2 * (size_t)p + 1]; }
+  CK(cudaMemcpyAsync(d.us, a.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(d.vs, b.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (geoel) {
+    std::vector<double> g(ncell);
+    double *dst[7] = {d.rc, d.sc, d.vol, d.mass, d.g19, d.g20, d.g21};
+    const int slot[7] = {0, 1, 2, 3, 18, 19, 20};
+    for (int k = 0; k < 7; k++) {
+      for (int e = 0; e < ncell; e++) g[e] = geoel[24 * (size_t)e + slot[k]];
+      CK(cudaMemcpyAsync(dst[k], g.data(), ncell * sizeof(double), cudaMemcpyHostToDevice, h->st));
+      CK(cudaStreamSynchronize(h->st));
+    }
+  }
+  if (amatr) {
+    std::vector<double> g(16 * (size_t)ncell);
+    for (int e = 0; e < ncell; e++)
+      for (int k = 0; k < 16; k++) g[k * (size_t)ncell + e] = amatr[16 * (size_t)e + k];
+    CK(cudaMemcpyAsync(d.amatr, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+  }
+  Scalars s0{};
+  CK(cudaMemcpyAsync(d.sc_dev, &s0, sizeof(Scalars), cudaMemcpyHostToDevice, h->st));
+  run(h, "geom", [&] { launch_geom(d, h->st, d.xs, d.ys); });
+  return read_status(h);
+}
+
+static int put_scalars(lag2d_handle *h, int itime, double dtfix, double tacru) {
+  Scalars s{};
+  CK(cudaMemcpyAsync(&s, h->d.sc_dev, sizeof(Scalars), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  s.dtfix = dtfix; s.tacru = tacru; s.itime = itime; s.done = 0; s.status = 0;
+  CK(cudaMemcpyAsync(h->d.sc_dev, &s, sizeof(Scalars), cudaMemcpyHostToDevice, h->st));
+  return LAG2D_OK;
+}
+
+static int get_scalars(lag2d_handle *h, Scalars *s) {
+  CK(cudaMemcpyAsync(s, h->d.sc_dev, sizeof(Scalars), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return LAG2D_OK;
+}
+
+int lag2d_step(lag2d_handle *h, int itime, double *dtfix, double *tacru) {
+  if (!h || !dtfix || !tacru) return fail(LAG2D_EINVAL, "null argument");
+  int r = put_scalars(h, itime, *dtfix, *tacru);
+  if (r) return r;
+  enqueue_step(h, itime);
+  Scalars s;
+  r = get_scalars(h, &s);
+  if (r) return r;
+  if (h->timing) flush_timing(h);
+  *dtfix = s.dtfix;
+  *tacru = s.tacru;
+  return read_status(h);
+}
+
+int lag2d_run(lag2d_handle *h, int itime0, int nsteps, double *dtfix, double *tacru, int *done) {
+  if (!h || !dtfix || !tacru || nsteps < 0) return fail(LAG2D_EINVAL, "bad argument");
+  int r = put_scalars(h, itime0 - 1, *dtfix, *tacru);
+  if (r) return r;
+  int steps = 0;
+  if (h->timing) {
+    // timed path: no graph, events around every kernel family
+    for (int i = 0; i < nsteps; i++) { enqueue_step(h, itime0 + i); steps++; }
+    flush_timing(h);
+  } else {
+    if (!h->graph) {
+      // one step with itime incremented on the device, captured once
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+      long long before = h->launches;
+      enqueue_step(h, -1);
+      CK(cudaStreamEndCapture(h->st, &g));
+      CK(cudaGraphInstantiate(&h->graph, g, 0));
+      cudaGraphDestroy(g);
+      h->launches = before;  // counted per replay below
+    }
+    long long per_step = 0;
+    {
+      // launches per step: 2 + nstag * (2+2+1+1+1 + 1+1+2) + 2 (dt) + 2
+      per_step = 2 + (long long)h->cfg.nstag * 11 + 2 + 2;
+    }
+    for (int i = 0; i < nsteps; i++) {
+      CK(cudaGraphLaunch(h->graph, h->st));
+      h->launches += per_step;
+      steps++;
+    }
+  }
+  Scalars s;
+  r = get_scalars(h, &s);
+  if (r) return r;
+  *dtfix = s.dtfix;
+  *tacru = s.tacru;
+  if (done) *done = s.done ? std::min(steps, std::max(0, s.itime - itime0 + 1)) : steps;
+  return read_status(h);
+}
+
+int lag2d_get_state(lag2d_handle *h, double *unkno, double *coord, double *ustar, double *geoel) {
+  if (!h) return fail(LAG2D_EINVAL, "null handle");
+  int r;
+  if (unkno && (r = download_unkno(h, h->d.Un, unkno))) return r;
+  if (coord && (r = download_xy(h, h->d.xn, h->d.yn, coord))) return r;
+  if (ustar && (r = download_xy(h, h->d.us, h->d.vs, ustar))) return r;
+  if (geoel && (r = download_geoel(h, geoel))) return r;
+  return LAG2D_OK;
+}
+
+int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
+  if (!h) return fail(LAG2D_EINVAL, "null handle");
+  Dev &d = h->d;
+  int r = put_scalars(h, itime, 0.0, 0.0);
+  if (r) return r;
+  run(h, "persson", [&] { launch_reset_count(d, h->st); launch_persson(d, h->st); }, 2);
+  if (flags) {
+    CK(cudaMemcpyAsync(h->flags_dev, d.flag, d.ncell * sizeof(int), cudaMemcpyDeviceToDevice, h->st));
+  }
+  run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
+  run(h, "corner", [&] { launch_corner(d, h->st); });
+  run(h, "node", [&] { launch_node(d, h->st); });
+  run(h, "rhs", [&] { launch_rhs(d, h->st); });
+  r = read_status(h);
+  if (h->timing) flush_timing(h);
+  if (r) return r;
+  // the stage state is the limited one after the RHS, as in the reference
+  CK(cudaMemcpyAsync(d.Un, d.Us, NU * (size_t)d.ncell * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  if (rhsel) {
+    std::vector<double> f(NU * (size_t)d.ncell);
+    CK(cudaMemcpyAsync(f.data(), d.rhs, f.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int e = 0; e < d.ncell; e++)
+      for (int q = 0; q < NQ; q++)
+        for (int k = 0; k < NDEG; k++) rhsel[(size_t)e * NU + q * NDEG + k] = f[(q * NDEG + k) * (size_t)d.ncell + e];
+  }
+  if (flags) {
+    std::vector<int> fl(d.ncell);
+    CK(cudaMemcpyAsync(fl.data(), h->flags_dev, d.ncell * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int e = 0; e < d.ncell; e++) flags[e] = fl[e] != 0;
+  }
+  return LAG2D_OK;
+}
+
+int lag2d_weno(lag2d_handle *h, const int *flags) {
+  if (!h || !flags) return fail(LAG2D_EINVAL, "null argument");
+  Dev &d = h->d;
+  int r = put_scalars(h, 1, 0.0, 0.0);
+  if (r) return r;
+  CK(cudaMemcpyAsync(h->flags_dev, flags, d.ncell * sizeof(int), cudaMemcpyHostToDevice, h->st));
+  run(h, "persson", [&] { launch_reset_count(d, h->st); launch_persson(d, h->st); }, 2);
+  run(h, "persson", [&] { launch_reset_count(d, h->st); launch_flags_from_host(d, h->st, h->flags_dev); }, 2);
+  run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
+  CK(cudaMemcpyAsync(d.Un, d.Us, NU * (size_t)d.ncell * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  r = read_status(h);
+  if (h->timing) flush_timing(h);
+  return r;
+}
+
+int lag2d_cellvol(lag2d_handle *h, double *geoel) {
+  if (!h) return fail(LAG2D_EINVAL, "null handle");
+  run(h, "geom", [&] { launch_geom(h->d, h->st, h->d.xs, h->d.ys); });
+  int r = read_status(h);
+  if (r) return r;
+  if (geoel) return download_geoel(h, geoel);
+  return LAG2D_OK;
+}
+
+long long lag2d_kernel_launches(const lag2d_handle *h) { return h ? h->launches : -1; }
+
+int lag2d_timing(lag2d_handle *h, int enable) {
+  if (!h) return fail(LAG2D_EINVAL, "null handle");
+  h->timing = enable != 0;
+  h->fam.clear();
+  return LAG2D_OK;
+}
+
+double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *launches) {
+  if (!h || !family) return -1.0;
+  auto it = h->fam.find(family);
+  if (it == h->fam.end() || it->second.n == 0) return -1.0;
+  if (launches) *launches = it->second.n;
+  return it->second.ms / it->second.n;
+}
+
+void lag2d_destroy(lag2d_handle *h) {
+  if (!h) return;
+  if (h->st) cudaStreamSynchronize(h->st);
+  for (auto &p : h->pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (void *p : h->allocs) cudaFree(p);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+}
+
+}  // extern "C"

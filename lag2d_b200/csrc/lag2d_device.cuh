@@ -1,0 +1,70 @@
+// Device-side building blocks of the Lag2D curved-P2 time step.
+//
+// Layout in HBM (structure of arrays, 0-based, one contiguous slab per field):
+//   U[(q*6 + k)*ncell + e]   DOF k of field q (tau, u, v, e) of cell e
+//   x[p], y[p]               node coordinates (separate arrays per config)
+//   ipq[k*nquad + iq]        node k (0..8) of quad iq
+//   cf[(v*32 + slot)*nquad + iq]  corner coefficient v (m, m*u, m*v, s_x, s_y)
+//                                  of corner-face slot = f + 2*(ivsg + 4*isg)
+// Quads are cells ntria..ncell-1 (the reference numbers triangles first).
+#pragma once
+#include <cstdint>
+
+namespace lag2d {
+
+constexpr int NDEG = 6;   // P2 Taylor basis
+constexpr int NQ = 4;     // tau, u, v, e
+constexpr int NU = NDEG * NQ;
+
+// Status bits written by kernels and returned by the C-ABI.
+constexpr int ST_NONPHYS = 1;   // non-positive volume or NaN
+constexpr int ST_STENCIL = 2;   // WENO valence the reference stops on
+
+struct Scalars {           // device-resident module scalars
+  double dtfix, tacru;
+  int itime, done, status, pad;
+};
+
+struct Dev {
+  int ntria, nquad, npoin, nbfac, ncell;
+  int ndegr, mdegr, ncase, nlimi;
+  double gamlg, cfl, cdrho, cimpd, tend, sedov_energy;
+  int nsedov, sedov_cell[4];
+  // connectivity
+  const int *ipq;          // [9][nquad]
+  const int *esq;          // [4][nquad], -1 on boundary faces
+  const int *stencil;      // [9][nquad] WENO stencil cells (0-based); row 0 = -1: none, -2: valence error
+  const int *node_ptr;     // [npoin+1]
+  const int *node_cf;      // corner-face ids iq*32 + slot, reference summation order
+  const unsigned char *bcmask;  // [npoin] bit0: u=0, bit1: v=0, bit2: keep (no solve)
+  const double *x0, *y0;   // initial coordinates
+  // geometry (time invariant except vol / vcx / vcy)
+  double *rc, *sc, *mass, *g19, *g20, *g21;
+  double *vol, *vcx, *vcy;
+  double *msub;            // [4][nquad] initial sub-cell masses (time invariant)
+  // state
+  double *Un, *Us;         // U^n and the stage state
+  double *xn, *yn, *xs, *ys;   // x^n and stage coordinates
+  double *us, *vs;         // nodal velocity ustar
+  double *amatr;           // [16][ncell]
+  // work
+  double *rhs;             // [24][ncell]
+  double *cf;              // [5][32][nquad]
+  int *flag;               // [ncell] Persson troubled-cell marks
+  double *geoph;           // [2][ncell] physical mass centre
+  double *mapmt;           // [4][ncell] velocity-aligned frame
+  double *Uw;              // [20][nquad] WENO output (high-order moments)
+  int *wlist;              // compacted troubled-quad list
+  int *wcount;
+  double *dtpart;          // [2][nblocks] partial minima for getdelt_lag
+  Scalars *sc_dev;
+};
+
+// Quadrature tables (filled from the host with the reference's literals).
+struct QuadTables {
+  double g25[25][2], w25[25];   // 5x5 Gauss (ruqope)
+  double g36[36][2], w36[36];   // 6x6 Gauss (ruqope)
+  double l25[25][2], wl25[25];  // 5x5 Gauss-Lobatto (ruqope_lobatto)
+};
+
+}  // namespace lag2d

@@ -1,0 +1,1588 @@
+// CUDA kernels of the Lag2D curved-P2 Lagrangian DG time step (sm_100a).
+//
+// One RK stage is the sequence
+//   persson   (all quads)  troubled-cell marks, physical mass centre, frame
+//   weno      (troubled)   WENO reconstruction into a side buffer, then commit
+//   corner    (all quads)  sub-cell normals/densities, corner impedances and
+//                          Riemann coefficients per corner face
+//   node      (all nodes)  fixed-order gather of the corner coefficients and
+//                          the 2x2 nodal solve for ustar (no atomics)
+//   rhs       (all quads)  corner forces, face + volume integrals, source
+//   dt        (stage 1)    deterministic min-reduction for getdelt_lag
+//   update    (all cells)  M^-1 apply and RK combine
+//   nodes     (all nodes)  node motion; centre-node re-interpolation and the
+//                          cell volumes follow in the geom kernel
+// Each kernel cites the reference routine it replaces (srccurv-lag/...).
+// Arithmetic keeps the reference's expression order so that a build with
+// --fmad=false reproduces the CPU restatement bit for bit.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "lag2d_device.cuh"
+
+namespace lag2d {
+
+// Constant tables: one copy in constant memory for the kernels and a host
+// mirror so that the same __host__ __device__ bodies can be checked on a CPU.
+struct Tables {
+  QuadTables q;
+  double wrie[4][4][2];   // corner-face weights of the Riemann solver
+  double wmas[4][4][2];   // mass-equation face weights of the face integral
+  double wmom[4][4];      // momentum/energy face weights of the face integral
+};
+__constant__ Tables cT;
+static Tables hT;
+
+__host__ __host__ __device__ __forceinline__ const Tables &TB() {
+#ifdef __CUDA_ARCH__
+  return cT;
+#else
+  return hT;
+#endif
+}
+#define cQ (TB().q)
+#define cPI 3.14159265358979311599796346854
+
+__host__ __host__ __device__ __forceinline__ int atomic_add(int *p, int v) {
+#ifdef __CUDA_ARCH__
+  return atomicAdd(p, v);
+#else
+  int o = *p;
+  *p = o + v;
+  return o;
+#endif
+}
+__host__ __host__ __device__ __forceinline__ void atomic_or(int *p, int v) {
+#ifdef __CUDA_ARCH__
+  atomicOr(p, v);
+#else
+  *p |= v;
+#endif
+}
+
+// ---------------------------------------------------------------------------
+// Shape functions of the 9-node quad (GetFE.f90:89-127)
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ void shp9v(double r, double s, double *shp) {
+  const double c10 = 1.0;
+  shp[0] = 0.25 * (c10 - r) * r * s * (c10 - s);
+  shp[1] = -0.25 * (c10 + r) * (c10 - s) * r * s;
+  shp[2] = 0.25 * (c10 + r) * (c10 + s) * r * s;
+  shp[3] = -0.25 * (c10 - r) * (c10 + s) * r * s;
+  shp[4] = -0.5 * (c10 - r * r) * (c10 - s) * s;
+  shp[5] = 0.5 * (c10 + r) * (c10 - s * s) * r;
+  shp[6] = 0.5 * (c10 - r * r) * (c10 + s) * s;
+  shp[7] = -0.5 * (c10 - r) * (c10 - s * s) * r;
+  shp[8] = (c10 - r * r) * (c10 - s * s);
+}
+
+__host__ __device__ __forceinline__ void shp9d(double r, double s, double *dr, double *ds) {
+  const double c10 = 1.0;
+  dr[0] = 0.25 * (2.0 * r - c10) * s * (s - 1.0);
+  dr[1] = 0.25 * (2.0 * r + c10) * s * (s - 1.0);
+  dr[2] = 0.25 * (2.0 * r + c10) * s * (s + 1.0);
+  dr[3] = 0.25 * (2.0 * r - c10) * s * (s + 1.0);
+  dr[4] = -r * s * (s - c10);
+  dr[5] = 0.5 * (2.0 * r + c10) * (c10 - s * s);
+  dr[6] = -r * s * (s + c10);
+  dr[7] = 0.5 * (2.0 * r - c10) * (1.0 - s * s);
+  dr[8] = -2.0 * r * (1.0 - s * s);
+  ds[0] = 0.25 * (2.0 * s - c10) * r * (r - 1.0);
+  ds[1] = 0.25 * (2.0 * s - c10) * r * (r + 1.0);
+  ds[2] = 0.25 * (2.0 * s + c10) * r * (r + 1.0);
+  ds[3] = 0.25 * (2.0 * s + c10) * r * (r - 1.0);
+  ds[4] = 0.5 * (1.0 - r * r) * (2.0 * s - c10);
+  ds[5] = -r * s * (r + c10);
+  ds[6] = 0.5 * (1.0 - r * r) * (2.0 * s + c10);
+  ds[7] = -r * s * (r - c10);
+  ds[8] = -2.0 * s * (1.0 - r * r);
+}
+
+struct Jac { double xr, xs, yr, ys; };
+
+__host__ __device__ __forceinline__ Jac jac9(const double (*xp)[2], const double *dr, const double *ds) {
+  Jac j = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    j.xr = j.xr + dr[k] * xp[k][0];
+    j.xs = j.xs + ds[k] * xp[k][0];
+    j.yr = j.yr + dr[k] * xp[k][1];
+    j.ys = j.ys + ds[k] * xp[k][1];
+  }
+  return j;
+}
+
+__host__ __device__ __forceinline__ void map9(const double (*xp)[2], const double *shp, double &x, double &y) {
+  double a = 0.0, b = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    a = a + shp[k] * xp[k][0];
+    b = b + shp[k] * xp[k][1];
+  }
+  x = a;
+  y = b;
+}
+
+__host__ __device__ __forceinline__ void load_quad(const Dev &d, const double *X, const double *Y, int iq,
+                                          double (*xp)[2]) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    int p = d.ipq[k * d.nquad + iq];
+    xp[k][0] = X[p];
+    xp[k][1] = Y[p];
+  }
+}
+
+__host__ __device__ __forceinline__ double Uget(const Dev &d, const double *U, int k, int q, int e) {
+  return U[(q * NDEG + k) * d.ncell + e];
+}
+
+__host__ __device__ __forceinline__ double rho_initial(const Dev &d, double xc, double yc) {
+  if (d.ncase == 6) return (sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125;
+  return 1.0;
+}
+
+__host__ __device__ __forceinline__ bool stopped(const Dev &d) { return d.sc_dev->done != 0; }
+
+// ---------------------------------------------------------------------------
+// getcellvol_lag (Limiterlag.f90:2038-2165): 6x6 Gauss volume and volume
+// centre in reference coordinates.
+// ---------------------------------------------------------------------------
+__host__ __device__ void b_geom(const Dev &d, int iq, const double *X, const double *Y) {
+  if (iq >= d.nquad || stopped(d)) return;
+  const int e = iq + d.ntria;
+  double xp[9][2], shp[9], dr[9], ds[9];
+  load_quad(d, X, Y, iq, xp);
+  const double alfrz = 0.0;
+  double rcv = 0.0, scv = 0.0, volel = 0.0;
+  for (int ig = 0; ig < 36; ig++) {
+    double r = cQ.g36[ig][0], s = cQ.g36[ig][1], wi = cQ.w36[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    double rcoef = 1.0 - alfrz + alfrz * yg;
+    double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    volel = volel + djaco * rcoef;
+    rcv = rcv + r * djaco * rcoef;
+    scv = scv + s * djaco * rcoef;
+  }
+  d.vol[e] = volel;
+  d.vcx[e] = rcv / volel;
+  d.vcy[e] = scv / volel;
+  if (!(volel > 0.0)) atomic_or(&d.sc_dev->status, ST_NONPHYS);
+}
+__global__ void k_geom(Dev d, const double *X, const double *Y) { b_geom(d, blockIdx.x * blockDim.x + threadIdx.x, X, Y); }
+
+// Step 9th-node re-interpolation (Getrhslag.f90:1963-1971) fused in front of
+// the volume computation: the centre node belongs to one quad only.
+__host__ __device__ void b_center_geom(const Dev &d, int iq) {
+  if (iq >= d.nquad || stopped(d)) return;
+  int p[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) p[k] = d.ipq[k * d.nquad + iq];
+  double *XY[2] = {d.xs, d.ys};
+  for (int c = 0; c < 2; c++) {
+    double *X = XY[c];
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = X[p[k]];
+    X[p[8]] = -0.25 * (x[0] + x[1] + x[2] + x[3]) + 0.5 * (x[4] + x[5] + x[6] + x[7]);
+  }
+}
+__global__ void k_center_geom(Dev d) { b_center_geom(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// ---------------------------------------------------------------------------
+// getSIHO_Persson (Limiterlag.f90:12042-12239) + Part I of
+// weno_char_quad_orthgl (WENO.f90:5990-6090): troubled-cell marks, physical
+// mass centre and the velocity-aligned frame for every quad.
+// ---------------------------------------------------------------------------
+__host__ __device__ void b_persson(const Dev &d, int iq) {
+  if (iq >= d.nquad || stopped(d)) return;
+  const int e = iq + d.ntria;
+  double xp[9][2], xpi[9][2], shp[9], dr[9], ds[9];
+  load_quad(d, d.xs, d.ys, iq, xp);
+  load_quad(d, d.x0, d.y0, iq, xpi);
+  const double rc = d.rc[e], sc = d.sc[e];
+  const double g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
+  double u[NDEG];
+#pragma unroll
+  for (int k = 0; k < NDEG; k++) u[k] = Uget(d, d.Us, k, 0, e);
+  double unvar2 = 0.0, unvar1 = 0.0;
+  double xcrho, ycrho;
+  shp9v(rc, sc, shp);
+  map9(xpi, shp, xcrho, ycrho);
+  double xmc = 0.0, ymc = 0.0;
+  for (int ig = 0; ig < 25; ig++) {
+    double r = cQ.g25[ig][0], s = cQ.g25[ig][1], wi = cQ.w25[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    double b[NDEG];
+    b[0] = 1.0; b[1] = (r - rc) / 1.0; b[2] = (s - sc) / 1.0;
+    b[3] = 0.5 * b[1] * b[1] - g19;
+    b[4] = 0.5 * b[2] * b[2] - g20;
+    b[5] = b[1] * b[2] - g21;
+    double un = 0.0, up1 = 0.0;
+#pragma unroll
+    for (int k = 0; k < NDEG; k++) un = un + u[k] * b[k];
+#pragma unroll
+    for (int k = 0; k < 3; k++) up1 = up1 + u[k] * b[k];
+    unvar2 = unvar2 + (up1 - un) * (up1 - un) * djaco;
+    unvar1 = unvar1 + (un) * (un)*djaco;
+    // physical mass centre (WENO.f90:6040-6082)
+    Jac ji = jac9(xpi, dr, ds);
+    double djacoi = wi * (ji.xr * ji.ys - ji.yr * ji.xs);
+    double xgi, ygi, xg, yg;
+    map9(xpi, shp, xgi, ygi);
+    map9(xp, shp, xg, yg);
+    double rhogi = rho_initial(d, xcrho, ycrho);
+    xmc = xmc + rhogi * djacoi * xg;
+    ymc = ymc + rhogi * djacoi * yg;
+  }
+  const double thr = -3.0 * log10(4.0) - 4.0;
+  int fl = (log10(unvar2 / unvar1) <= thr) ? 0 : 1;
+  d.flag[e] = fl;
+  const double masel = d.mass[e];
+  d.geoph[e] = xmc / masel;
+  d.geoph[d.ncell + e] = ymc / masel;
+  double ma = Uget(d, d.Us, 0, 1, e), mb = Uget(d, d.Us, 0, 2, e);
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+  if (sqrt(ma * ma + mb * mb) > 1.0e-10) {
+    m0 = ma / sqrt(ma * ma + mb * mb);
+    m2 = mb / sqrt(ma * ma + mb * mb);
+    m1 = -mb / sqrt(ma * ma + mb * mb);
+    m3 = ma / sqrt(ma * ma + mb * mb);
+  }
+  d.mapmt[0 * d.ncell + e] = m0;
+  d.mapmt[1 * d.ncell + e] = m1;
+  d.mapmt[2 * d.ncell + e] = m2;
+  d.mapmt[3 * d.ncell + e] = m3;
+  if (fl) {
+    int slot = atomic_add(d.wcount, 1);
+    d.wlist[slot] = iq;
+  }
+}
+__global__ void k_persson(Dev d) { b_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// Marks given by the caller instead of the Persson indicator (lag2d_weno).
+__host__ __device__ void b_flags_from_host(const Dev &d, int iq, const int *flags) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  int fl = flags[e] != 0;
+  d.flag[e] = fl;
+  if (fl) {
+    int slot = atomic_add(d.wcount, 1);
+    d.wlist[slot] = iq;
+  }
+}
+__global__ void k_flags_from_host(Dev d, const int *flags) { b_flags_from_host(d, blockIdx.x * blockDim.x + threadIdx.x, flags); }
+
+// ---------------------------------------------------------------------------
+// WENO reconstruction of one troubled quad (weno_stncl_quad_orthol3,
+// WENO.f90:7541-8101; weno_cell_Taylor :7219; getgeophy_local_Taylor :6750;
+// getunknp_local_Taylor :7005; basis_orthg :6683 with nbsis = 1).
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ void vec_local(const double *mp, double &dx, double &dy) {
+  double xl = dx * mp[0] + dy * mp[2];
+  double yl = dx * mp[1] + dy * mp[3];
+  dx = xl;
+  dy = yl;
+}
+__host__ __device__ __forceinline__ void vec_local_back(const double *mp, double &dx, double &dy) {
+  double xl = dx * mp[3] + dy * (-mp[2]);
+  double yl = dx * (-mp[1]) + dy * mp[0];
+  dx = xl;
+  dy = yl;
+}
+__host__ __device__ __forceinline__ void basis_orthg1(const double *bt, const double *cf, double *bo) {
+  bo[0] = bt[0]; bo[1] = bt[1]; bo[2] = bt[2];
+  bo[3] = 0.5 * bt[1] * bt[1] - cf[0];
+  bo[4] = 0.5 * bt[2] * bt[2] - cf[1];
+  bo[5] = bt[1] * bt[2] - cf[2];
+}
+
+// n x n inverse (n <= 5), column-major, Gauss-Jordan with partial pivoting
+// (stands in for Matinv225, LinearAlgebra.f90:130; same inverse up to rounding).
+__host__ __device__ void inv_small(int n, const double *a, double *b) {
+  double t[25];
+  for (int i = 0; i < n * n; i++) { t[i] = a[i]; b[i] = 0.0; }
+  for (int i = 0; i < n; i++) b[i + n * i] = 1.0;
+  for (int k = 0; k < n; k++) {
+    int piv = k;
+    double big = fabs(t[k + n * k]);
+    for (int i = k + 1; i < n; i++)
+      if (fabs(t[i + n * k]) > big) { big = fabs(t[i + n * k]); piv = i; }
+    if (piv != k)
+      for (int j = 0; j < n; j++) {
+        double s = t[k + n * j]; t[k + n * j] = t[piv + n * j]; t[piv + n * j] = s;
+        s = b[k + n * j]; b[k + n * j] = b[piv + n * j]; b[piv + n * j] = s;
+      }
+    double dd = 1.0 / t[k + n * k];
+    for (int j = 0; j < n; j++) { t[k + n * j] *= dd; b[k + n * j] *= dd; }
+    for (int i = 0; i < n; i++) {
+      if (i == k) continue;
+      double f = t[i + n * k];
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; j++) {
+        t[i + n * j] -= f * t[k + n * j];
+        b[i + n * j] -= f * b[k + n * j];
+      }
+    }
+  }
+}
+
+// getmatrix_prj2 (Limiterlag.f90:16455-16562), column-major 4x4 outputs
+__host__ __device__ void matrix_prj2(double g, double *qmat, double *qinvm, double dnx, double dny,
+                            const double *ul, const double *ur) {
+  const double eps = 1.0e-6;
+  double rhoc1 = 1.0 / ul[0], u1 = ul[1], v1 = ul[2], e1 = ul[3];
+  double rhoc2 = 1.0 / ur[0], u2 = ur[1], v2 = ur[2], e2 = ur[3];
+  double rhof = sqrt(rhoc1 * rhoc2);
+  double rhosq = sqrt(rhoc1) + sqrt(rhoc2);
+  double uf = (sqrt(rhoc1) * u1 + sqrt(rhoc2) * u2) / rhosq;
+  double vf = (sqrt(rhoc1) * v1 + sqrt(rhoc2) * v2) / rhosq;
+  double h1 = fmax(eps, g * e1 - (g - 1.0) * 0.5 * (u1 * u1 + v1 * v1));
+  double h2 = fmax(eps, g * e2 - (g - 1.0) * 0.5 * (u2 * u2 + v2 * v2));
+  double hf = (sqrt(rhoc1) * h1 + sqrt(rhoc2) * h2) / rhosq;
+  double sdf = sqrt(fmax(eps, (g - 1.0) * (hf - 0.5 * (uf * uf + vf * vf))));
+  double rhosd = rhof * sdf;
+  double pf = sdf * sdf * rhof / g;
+  double gam1 = (g - 1.0) / g;
+  double vnm = vf * dnx - uf * dny;
+#define Q(a, i, j) a[(i - 1) + 4 * (j - 1)]
+  Q(qinvm, 1, 1) = -.5 / g;
+  Q(qinvm, 1, 2) = .5 * dnx / rhosd - 0.5 * uf / pf * gam1;
+  Q(qinvm, 1, 3) = .5 * dny / rhosd - 0.5 * vf / pf * gam1;
+  Q(qinvm, 1, 4) = .5 / pf * gam1;
+  Q(qinvm, 2, 1) = 1.0 / g;
+  Q(qinvm, 2, 2) = -dny * vnm / pf - uf / pf / g;
+  Q(qinvm, 2, 3) = dnx * vnm / pf - vf / pf / g;
+  Q(qinvm, 2, 4) = 1.0 / pf / g;
+  Q(qinvm, 3, 1) = 0.0;
+  Q(qinvm, 3, 2) = dny / pf;
+  Q(qinvm, 3, 3) = -dnx / pf;
+  Q(qinvm, 3, 4) = 0.0;
+  Q(qinvm, 4, 1) = .5 / g;
+  Q(qinvm, 4, 2) = .5 * dnx / rhosd + 0.5 * uf / pf * gam1;
+  Q(qinvm, 4, 3) = .5 * dny / rhosd + 0.5 * vf / pf * gam1;
+  Q(qinvm, 4, 4) = -.5 / pf * gam1;
+  double vedn = uf * dnx + vf * dny;
+  Q(qmat, 1, 1) = -1.0;
+  Q(qmat, 1, 2) = g - 1.0;
+  Q(qmat, 1, 3) = (g - 1.0) * vnm;
+  Q(qmat, 1, 4) = 1.0;
+  Q(qmat, 2, 1) = rhosd * dnx;
+  Q(qmat, 2, 2) = 0.0;
+  Q(qmat, 2, 3) = pf * dny;
+  Q(qmat, 2, 4) = rhosd * dnx;
+  Q(qmat, 3, 1) = rhosd * dny;
+  Q(qmat, 3, 2) = 0.0;
+  Q(qmat, 3, 3) = -pf * dnx;
+  Q(qmat, 3, 4) = rhosd * dny;
+  Q(qmat, 4, 1) = pf + rhosd * vedn;
+  Q(qmat, 4, 2) = pf;
+  Q(qmat, 4, 3) = 0.0;
+  Q(qmat, 4, 4) = -pf + rhosd * vedn;
+#undef Q
+}
+
+// Initial-config density weights and rotated physical positions of the 25
+// Gauss points of stencil cell jelem (shared by the WENO sub-steps).
+__host__ __device__ void weno_points(const Dev &d, int jelem, const double *mp, double *rhodj, double *xl,
+                            double *yl) {
+  const int je = jelem - d.ntria;
+  double xpqi[9][2], xpql[9][2], shp[9], dr[9], ds[9];
+  load_quad(d, d.x0, d.y0, je, xpqi);
+  load_quad(d, d.xs, d.ys, je, xpql);
+  for (int k = 0; k < 9; k++) vec_local(mp, xpql[k][0], xpql[k][1]);
+  double xcrho, ycrho;
+  shp9v(d.rc[jelem], d.sc[jelem], shp);
+  map9(xpqi, shp, xcrho, ycrho);
+  const double rhogi = rho_initial(d, xcrho, ycrho);
+  for (int ig = 0; ig < 25; ig++) {
+    double r = cQ.g25[ig][0], s = cQ.g25[ig][1], wi = cQ.w25[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xpqi, dr, ds);
+    double djacoi = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(xpql, shp, xg, yg);
+    rhodj[ig] = rhogi * djacoi;
+    xl[ig] = xg;
+    yl[ig] = yg;
+  }
+}
+
+__host__ __device__ void b_weno(const Dev &d, int t) {
+  if (stopped(d) || t >= *d.wcount) return;
+  const int iq = d.wlist[t];
+  const int ielem = iq + d.ntria;
+  int ielaj[9];
+  for (int k = 0; k < 9; k++) ielaj[k] = d.stencil[k * d.nquad + iq];
+  if (ielaj[0] == -2) { atomic_or(&d.sc_dev->status, ST_STENCIL); }
+  if (ielaj[0] < 0) return;  // boundary cell: the reference leaves it (WENO.f90:7704)
+  const int ielst1[4][7] = {{1, 2, 5, 6, 9, 8, 3}, {1, 3, 2, 7, 6, 9, 5},
+                                   {1, 4, 3, 8, 7, 6, 5}, {1, 5, 4, 9, 8, 7, 3}};
+  const int ielst2[4][4] = {{1, 2, 6, 9}, {1, 3, 6, 7}, {1, 4, 8, 7}, {1, 5, 8, 9}};
+  double mp[4];
+  for (int k = 0; k < 4; k++) mp[k] = d.mapmt[k * d.ncell + ielem];
+  double xpq[9][2];
+  load_quad(d, d.xs, d.ys, iq, xpq);
+  const double dxcl = sqrt(d.vol[ielem]), dycl = dxcl;
+
+  double unkrl[9][4][6];
+  for (int s = 0; s < 9; s++)
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) unkrl[s][q][k] = Uget(d, d.Us, k, q, ielaj[s]);
+  for (int s = 0; s < 9; s++)
+    for (int k = 0; k < 6; k++) vec_local(mp, unkrl[s][1][k], unkrl[s][2][k]);
+
+  double rhodj[9][25], xl[9][25], yl[9][25];
+  for (int s = 0; s < 9; s++) weno_points(d, ielaj[s], mp, rhodj[s], xl[s], yl[s]);
+
+  // getgeophy_local_Taylor (nbsis = 1)
+  double geopl[9][5];
+  for (int s = 0; s < 9; s++) {
+    int jelem = ielaj[s];
+    double xclj = d.geoph[jelem], yclj = d.geoph[d.ncell + jelem];
+    vec_local(mp, xclj, yclj);
+    geopl[s][0] = xclj;
+    geopl[s][1] = yclj;
+    double dxclj = sqrt(d.vol[jelem]), dyclj = dxclj;
+    double masel = d.mass[jelem];
+    double v1 = 0.0, v2 = 0.0, v3 = 0.0;
+    for (int ig = 0; ig < 25; ig++) {
+      double b2 = (xl[s][ig] - xclj) / dxclj, b3 = (yl[s][ig] - yclj) / dyclj;
+      v1 = v1 + rhodj[s][ig] * b2 * b2;
+      v2 = v2 + rhodj[s][ig] * b3 * b3;
+      v3 = v3 + rhodj[s][ig] * b2 * b3;
+    }
+    v1 = v1 / masel; v2 = v2 / masel; v3 = v3 / masel;
+    geopl[s][2] = 0.5 * v1;
+    geopl[s][3] = 0.5 * v2;
+    geopl[s][4] = v3;
+  }
+
+  // getunknp_local_Taylor: local orthogonal-basis coefficients per stencil cell
+  double unkpl[9][4][6], mtbbq[25], mtbbi[25];
+  for (int s = 0; s < 9; s++) {
+    int jelem = ielaj[s];
+    double rcj = d.rc[jelem], scj = d.sc[jelem];
+    double xclj = geopl[s][0], yclj = geopl[s][1];
+    double dxclj = sqrt(d.vol[jelem]), dyclj = dxclj;
+    double bb[25], bbq[25], bbi[25], bbqi[25];
+    for (int i = 0; i < 25; i++) { bb[i] = 0.0; bbq[i] = 0.0; }
+    for (int ig = 0; ig < 25; ig++) {
+      double r = cQ.g25[ig][0], s_ = cQ.g25[ig][1];
+      double bq[6], bqpl[3], bqol[6];
+      bq[0] = 1.0; bq[1] = (r - rcj) / 1.0; bq[2] = (s_ - scj) / 1.0;
+      bq[3] = 0.5 * bq[1] * bq[1] - d.g19[jelem];
+      bq[4] = 0.5 * bq[2] * bq[2] - d.g20[jelem];
+      bq[5] = bq[1] * bq[2] - d.g21[jelem];
+      bqpl[0] = 1.0; bqpl[1] = (xl[s][ig] - xclj) / dxclj; bqpl[2] = (yl[s][ig] - yclj) / dyclj;
+      basis_orthg1(bqpl, &geopl[s][2], bqol);
+      for (int i = 1; i < 6; i++)
+        for (int j = 1; j < 6; j++) {
+          bb[(i - 1) + 5 * (j - 1)] = bb[(i - 1) + 5 * (j - 1)] + rhodj[s][ig] * bq[i] * bqol[j];
+          bbq[(i - 1) + 5 * (j - 1)] = bbq[(i - 1) + 5 * (j - 1)] + rhodj[s][ig] * bqol[i] * bqol[j];
+        }
+    }
+    double rhs[6][4];
+    for (int i = 0; i < 6; i++) for (int q = 0; q < 4; q++) rhs[i][q] = 0.0;
+    for (int i = 1; i < 6; i++)
+      for (int j = 1; j < 6; j++)
+        for (int q = 0; q < 4; q++) rhs[i][q] = rhs[i][q] + unkrl[s][q][j] * bb[(j - 1) + 5 * (i - 1)];
+    inv_small(5, bbq, bbqi);
+    inv_small(5, bb, bbi);
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) unkpl[s][q][k] = 0.0;
+    for (int i = 1; i < 6; i++)
+      for (int j = 1; j < 6; j++)
+        for (int q = 0; q < 4; q++) unkpl[s][q][i] = unkpl[s][q][i] + rhs[j][q] * bbqi[(j - 1) + 5 * (i - 1)];
+    if (s == 0)
+      for (int i = 0; i < 25; i++) { mtbbq[i] = bbq[i]; mtbbi[i] = bbi[i]; }
+    for (int q = 0; q < 4; q++) unkpl[s][q][0] = unkrl[s][q][0];
+  }
+
+  // candidate polynomials: 1 central + 4 Lagrangian + 4 Hermite stencils
+  double unksl[9][4][6];
+  for (int is = 0; is < 9; is++)
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) unksl[is][q][k] = 0.0;
+  for (int is = 0; is < 9; is++) for (int q = 0; q < 4; q++) unksl[is][q][0] = unkpl[0][q][0];
+  for (int k = 0; k < 6; k++) for (int q = 0; q < 4; q++) unksl[0][q][k] = unkpl[0][q][k];
+  int isten = 0;
+  const double xmcl = geopl[0][0], ymcl = geopl[0][1];
+  for (int is = 0; is < 4; is++) {
+    isten++;
+    double matlg[25], rhslg[20], matin[25];
+    for (int i = 0; i < 25; i++) matlg[i] = 0.0;
+    for (int i = 0; i < 20; i++) rhslg[i] = 0.0;
+    for (int ies = 0; ies < 5; ies++) {
+      int sl = ielst1[is][ies + 1] - 1;
+      double masej = d.mass[ielaj[sl]];
+      for (int ig = 0; ig < 25; ig++) {
+        double bqplj[3], bqolj[6];
+        bqplj[0] = 1.0; bqplj[1] = (xl[sl][ig] - xmcl) / dxcl; bqplj[2] = (yl[sl][ig] - ymcl) / dycl;
+        basis_orthg1(bqplj, &geopl[0][2], bqolj);
+        for (int k = 0; k < 5; k++) matlg[ies + 5 * k] = matlg[ies + 5 * k] + rhodj[sl][ig] * bqolj[k + 1] / masej;
+      }
+      for (int q = 0; q < 4; q++) rhslg[q + 4 * ies] = unkpl[sl][q][0] - unkpl[0][q][0];
+    }
+    inv_small(5, matlg, matin);
+    for (int k = 1; k < 6; k++)
+      for (int ies = 0; ies < 5; ies++)
+        for (int q = 0; q < 4; q++)
+          unksl[isten][q][k] = unksl[isten][q][k] + matin[(k - 1) + 5 * ies] * rhslg[q + 4 * ies];
+  }
+  for (int is = 0; is < 4; is++) {
+    isten++;
+    double mathm[45], rhshm[36], matls[25], rhsls[20], matin[25];
+    for (int i = 0; i < 45; i++) mathm[i] = 0.0;
+    for (int i = 0; i < 36; i++) rhshm[i] = 0.0;
+    for (int ies = 0; ies < 3; ies++) {
+      int sl = ielst2[is][ies + 1] - 1;
+      int jelem = ielaj[sl];
+      double masej = d.mass[jelem];
+      double dxclj = sqrt(d.vol[jelem]), dyclj = dxclj;
+      double xclj = geopl[sl][0], yclj = geopl[sl][1];
+      for (int ig = 0; ig < 25; ig++) {
+        double bqplj[3], bqol[6], bqolj[6];
+        bqplj[0] = 1.0; bqplj[1] = (xl[sl][ig] - xmcl) / dxcl; bqplj[2] = (yl[sl][ig] - ymcl) / dycl;
+        basis_orthg1(bqplj, &geopl[0][2], bqol);
+        for (int k = 0; k < 5; k++) mathm[ies + 9 * k] = mathm[ies + 9 * k] + rhodj[sl][ig] * bqol[k + 1] / masej;
+        bqplj[0] = 1.0; bqplj[1] = (xl[sl][ig] - xclj) / dxclj; bqplj[2] = (yl[sl][ig] - yclj) / dyclj;
+        basis_orthg1(bqplj, &geopl[sl][2], bqolj);
+        int ieshm = 3 + 2 * ies;
+        for (int k = 1; k < 6; k++) {
+          mathm[ieshm + 9 * (k - 1)] = mathm[ieshm + 9 * (k - 1)] + rhodj[sl][ig] * bqol[k] * bqolj[1] / masej;
+          mathm[ieshm + 1 + 9 * (k - 1)] = mathm[ieshm + 1 + 9 * (k - 1)] + rhodj[sl][ig] * bqol[k] * bqolj[2] / masej;
+        }
+        for (int k = 1; k < 6; k++)
+          for (int q = 0; q < 4; q++) {
+            rhshm[q + 4 * ieshm] = rhshm[q + 4 * ieshm] + rhodj[sl][ig] * bqolj[k] * bqolj[1] * unkpl[sl][q][k] / masej;
+            rhshm[q + 4 * (ieshm + 1)] =
+                rhshm[q + 4 * (ieshm + 1)] + rhodj[sl][ig] * bqolj[k] * bqolj[2] * unkpl[sl][q][k] / masej;
+          }
+      }
+      for (int q = 0; q < 4; q++) rhshm[q + 4 * ies] = unkpl[sl][q][0] - unkpl[0][q][0];
+    }
+    // matrix_sym (LinearAlgebra.f90:89): normal equations of the 9x5 system
+    for (int i = 0; i < 25; i++) matls[i] = 0.0;
+    for (int i = 0; i < 20; i++) rhsls[i] = 0.0;
+    for (int im = 0; im < 5; im++)
+      for (int jm = 0; jm < 5; jm++)
+        for (int km = 0; km < 9; km++) matls[im + 5 * jm] = matls[im + 5 * jm] + mathm[km + 9 * im] * mathm[km + 9 * jm];
+    for (int q = 0; q < 4; q++)
+      for (int im = 0; im < 5; im++)
+        for (int km = 0; km < 9; km++) rhsls[q + 4 * im] = rhsls[q + 4 * im] + mathm[km + 9 * im] * rhshm[q + 4 * km];
+    inv_small(5, matls, matin);
+    for (int k = 1; k < 6; k++)
+      for (int ies = 0; ies < 5; ies++)
+        for (int q = 0; q < 4; q++)
+          unksl[isten][q][k] = unksl[isten][q][k] + matin[(k - 1) + 5 * ies] * rhsls[q + 4 * ies];
+  }
+  isten++;  // 9 candidate polynomials
+
+  // weno_cell_Taylor: characteristic WENO per interior face, averaged
+  const double epsil = 1.0e-6;
+  const double dxc = sqrt(d.vol[ielem]), dyc = dxc;
+  const int mapfe[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
+  double unk_phy[4][6];
+  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) unk_phy[q][k] = 0.0;
+  double unkf_phy[4][4][6];
+  for (int a = 0; a < 4; a++) for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) unkf_phy[a][q][k] = 0.0;
+  int ifprj = 0;
+  for (int ies = 0; ies < 4; ies++) {
+    int jelem = d.esq[ies * d.nquad + iq];
+    if (jelem < 0) continue;
+    double dtx = xpq[mapfe[ies][1]][0] - xpq[mapfe[ies][0]][0];
+    double dty = xpq[mapfe[ies][1]][1] - xpq[mapfe[ies][0]][1];
+    double dlgt = sqrt(dtx * dtx + dty * dty);
+    double dnx = dty / dlgt, dny = -dtx / dlgt;
+    vec_local(mp, dnx, dny);
+    double ul[4], ur[4];
+    for (int q = 0; q < 4; q++) { ul[q] = Uget(d, d.Us, 0, q, ielem); ur[q] = Uget(d, d.Us, 0, q, jelem); }
+    vec_local(mp, ul[1], ul[2]);
+    vec_local(mp, ur[1], ur[2]);
+    double qmat[16], qinvm[16];
+    matrix_prj2(d.gamlg, qmat, qinvm, dnx, dny, ul, ur);
+    double weigh[9][4], weigt[4] = {0.0, 0.0, 0.0, 0.0}, os1[9];
+    for (int is = 0; is < isten; is++) {
+      double mx = 0.0;
+      for (int k = 0; k < 4; k++) {
+        // characteristic coefficient k of moments 2 and 3 (first derivatives)
+        double c1 = 0.0, c2 = 0.0;
+        for (int q = 0; q < 4; q++) {
+          c1 = c1 + qinvm[k + 4 * q] * unksl[is][q][1];
+          c2 = c2 + qinvm[k + 4 * q] * unksl[is][q][2];
+        }
+        double t1 = c1 / dxc, t2 = c2 / dyc;
+        double os = t1 * t1 + t2 * t2;
+        if (k == 0 || os > mx) mx = os;
+      }
+      os1[is] = mx;
+    }
+    double weigl0 = .2, weigl1 = 0.8 / (isten - 1.0);
+    for (int is = 0; is < isten; is++)
+      for (int q = 0; q < 4; q++) {
+        double tt = epsil + os1[is];
+        weigh[is][q] = (is == 0 ? weigl0 : weigl1) / (tt * tt);
+      }
+    for (int q = 0; q < 4; q++)
+      for (int is = 0; is < isten; is++) weigt[q] = weigt[q] + weigh[is][q];
+    for (int is = 0; is < isten; is++)
+      for (int q = 0; q < 4; q++) weigh[is][q] = weigh[is][q] / weigt[q];
+    double fch[4][6];
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) fch[q][k] = 0.0;
+    for (int is = 0; is < isten; is++)
+      for (int kq = 0; kq < 4; kq++)
+        for (int k = 0; k < 6; k++) {
+          double ch = 0.0;
+          for (int q = 0; q < 4; q++) ch = ch + qinvm[kq + 4 * q] * unksl[is][q][k];
+          fch[kq][k] = fch[kq][k] + weigh[is][kq] * ch;
+        }
+    for (int kq = 0; kq < 4; kq++)
+      for (int k = 1; k < 6; k++)
+        for (int q = 0; q < 4; q++) unkf_phy[ifprj][q][k] = unkf_phy[ifprj][q][k] + qmat[q + 4 * kq] * fch[kq][k];
+    ifprj++;
+  }
+  double weigf = 1.0 / ifprj;
+  for (int a = 0; a < ifprj; a++)
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < 6; k++) unk_phy[q][k] = unk_phy[q][k] + weigf * unkf_phy[a][q][k];
+
+  // inverse L2 projection back to the target's Taylor basis, un-rotate
+  double rhsuk[5][4], out[4][6];
+  for (int i = 0; i < 5; i++) for (int q = 0; q < 4; q++) rhsuk[i][q] = 0.0;
+  for (int i = 1; i < 6; i++)
+    for (int j = 1; j < 6; j++)
+      for (int q = 0; q < 4; q++) rhsuk[i - 1][q] = rhsuk[i - 1][q] + unk_phy[q][j] * mtbbq[(j - 1) + 5 * (i - 1)];
+  for (int q = 0; q < 4; q++) for (int k = 1; k < 6; k++) out[q][k] = 0.0;
+  for (int i = 1; i < 6; i++)
+    for (int j = 1; j < 6; j++)
+      for (int q = 0; q < 4; q++) out[q][i] = out[q][i] + rhsuk[j - 1][q] * mtbbi[(j - 1) + 5 * (i - 1)];
+  for (int k = 1; k < 6; k++) vec_local_back(mp, out[1][k], out[2][k]);
+  for (int q = 0; q < 4; q++)
+    for (int k = 1; k < 6; k++) d.Uw[(q * 5 + (k - 1)) * d.nquad + iq] = out[q][k];
+  d.flag[ielem] = 2;  // reconstructed
+}
+__global__ void __launch_bounds__(64) k_weno(Dev d) { b_weno(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// Copy the reconstructions into the stage state once every read of the
+// pre-limit state is done (the reference's unknr copy, WENO.f90:6096).
+__host__ __device__ void b_weno_commit(const Dev &d, int t) {
+  if (stopped(d) || t >= *d.wcount) return;
+  const int iq = d.wlist[t];
+  const int e = iq + d.ntria;
+  if (d.flag[e] != 2) return;
+  for (int q = 0; q < 4; q++)
+    for (int k = 1; k < 6; k++) d.Us[(q * NDEG + k) * d.ncell + e] = d.Uw[(q * 5 + (k - 1)) * d.nquad + iq];
+}
+__global__ void k_weno_commit(Dev d) { b_weno_commit(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// ---------------------------------------------------------------------------
+// Sub-cell normals of a quad (getfnds_lagsmsif_hybrid, Getrhslaggauss.f90:
+// 3537-3599; getfnds_lagsms_simpsonhybrid, :9908-10010): gq[16][3].
+// ---------------------------------------------------------------------------
+__host__ __device__ void normals_quad(const double (*xpq)[2], double (*gq)[3]) {
+  const double posqc[4][2] = {{0.0, -0.5}, {0.5, 0.0}, {0.0, 0.5}, {-0.5, 0.0}};
+  double shp[9];
+#pragma unroll
+  for (int ifa = 0; ifa < 4; ifa++) {
+    double xv, yv;
+    shp9v(posqc[ifa][0], posqc[ifa][1], shp);
+    map9(xpq, shp, xv, yv);
+    const double r = -1.0;
+    double d0 = -0.5 + r, d1 = 0.5 + r, d2 = -2.0 * r;
+    double dxdr = 0.0, dydr = 0.0;
+    dxdr = dxdr + d0 * xpq[4 + ifa][0];
+    dydr = dydr + d0 * xpq[4 + ifa][1];
+    dxdr = dxdr + d1 * xpq[8][0];
+    dydr = dydr + d1 * xpq[8][1];
+    dxdr = dxdr + d2 * xv;
+    dydr = dydr + d2 * yv;
+    double djaco = sqrt(dxdr * dxdr + dydr * dydr);
+    double anx = -dydr, any = dxdr;
+    gq[8 + ifa][0] = anx / sqrt(anx * anx + any * any);
+    gq[8 + ifa][1] = any / sqrt(anx * anx + any * any);
+    gq[8 + ifa][2] = djaco * 2.0;
+  }
+  const double posiq[12][2] = {{-1, -1}, {1, -1}, {1, -1}, {1, 1}, {1, 1}, {-1, 1},
+                               {-1, 1}, {-1, -1}, {0, -1}, {1, 0}, {0, 1}, {-1, 0}};
+  const double vnx[4] = {0.0, 1.0, 0.0, -1.0}, vny[4] = {-1.0, 0.0, 1.0, 0.0};
+  const int side[12] = {0, 0, 1, 1, 2, 2, 3, 3, 0, 1, 2, 3};
+#pragma unroll
+  for (int ig = 0; ig < 12; ig++) {
+    double dr[9], ds[9];
+    shp9d(posiq[ig][0], posiq[ig][1], dr, ds);
+    Jac j = jac9(xpq, dr, ds);
+    double vn0 = vnx[side[ig]], vn1 = vny[side[ig]], larea = 2.0;
+    double anx = j.ys * vn0 + (-j.yr) * vn1;
+    double any = (-j.xs) * vn0 + j.xr * vn1;
+    double v0 = anx * larea, v1 = any * larea;
+    double farea = sqrt(v0 * v0 + v1 * v1);
+    int slot = (ig < 8) ? ig : ig + 4;
+    gq[slot][0] = anx * larea / farea;
+    gq[slot][1] = any * larea / farea;
+    gq[slot][2] = farea;
+  }
+}
+
+// sub-cell vertices (getndvelo_lagsubg ipqsg, Getrhslaggauss.f90:4424-4427), 0-based
+// corner-face -> gesgq slot with orientation sign (fnqsg, Getrhslaggauss.f90:10486-10506)
+__host__ __host__ __device__ __forceinline__ int ipqsg_(int isg, int ivsg) {
+  const int t[16] = {0, 4, 8, 7, 4, 1, 5, 8, 8, 5, 2, 6, 7, 8, 6, 3};
+  return t[4 * isg + ivsg];
+}
+__host__ __host__ __device__ __forceinline__ int fnqsg_(int isg, int k) {
+  const int t[32] = {8, 1, 13, -9, -9, 12, 12, 16, 9, 13, 2, 3, 14, -10, -10, 9,
+                     -11, 10, 10, 14, 4, 5, 15, -11, 16, -12, -12, 11, 11, 15, 6, 7};
+  return t[8 * isg + k];
+}
+__host__ __host__ __device__ __forceinline__ double xvq_(int iv) {
+  const double t[9] = {-1, 1, 1, -1, 0, 1, 0, -1, 0};
+  return t[iv];
+}
+__host__ __host__ __device__ __forceinline__ double yvq_(int iv) {
+  const double t[9] = {-1, -1, 1, 1, -1, 0, 1, 0, 0};
+  return t[iv];
+}
+#define cWRIE (TB().wrie)
+#define cWMAS (TB().wmas)
+#define cWMOM (TB().wmom)
+
+__host__ __device__ __forceinline__ void corner_normal(const double (*gq)[3], int isg, int ivsg, int f, double &n0,
+                                              double &n1, double &a) {
+  int code = fnqsg_(isg, 2 * ivsg + f);
+  int slot = abs(code) - 1;
+  double sg = (code >= 0) ? 1.0 : -1.0;
+  n0 = sg * gq[slot][0];
+  n1 = sg * gq[slot][1];
+  a = gq[slot][2];
+}
+
+// Taylor basis at the 9 nodes (bq of getriem_quadsubg2 / rhsifacedg_lagsubgq2)
+__host__ __device__ __forceinline__ void node_basis(double rc, double sc, double g19, double g20, double g21, int iv,
+                                           double *b) {
+  b[0] = 1.0;
+  b[1] = (xvq_(iv) - rc) / 1.0;
+  b[2] = (yvq_(iv) - sc) / 1.0;
+  b[3] = 0.5 * b[1] * b[1] - g19;
+  b[4] = 0.5 * b[2] * b[2] - g20;
+  b[5] = b[1] * b[2] - g21;
+}
+
+// ---------------------------------------------------------------------------
+// Corner pass: getriem_quadsubg2 (Getrhslaggauss.f90:10409-10867) with
+// getrhosubg_averg (:7067, initial sub-cell masses hoisted to set-up) and
+// getrhosubg_daverg (:10949).  Writes, per corner face, the Riemann
+// coefficients of getriecoef_matrixnew (Limiterlag.f90:1037): m = mu*A,
+// m*u_c, m*v_c and sigma.n*A.
+// ---------------------------------------------------------------------------
+__host__ __device__ void b_corner(const Dev &d, int iq) {
+  if (iq >= d.nquad || stopped(d)) return;
+  const int e = iq + d.ntria;
+  const double eps = 1.0e-6, g = d.gamlg;
+  const double slpdu = (g + 1.0) / 2.0;
+  double xpq[9][2];
+  load_quad(d, d.xs, d.ys, iq, xpq);
+  double gq[16][3];
+  normals_quad(xpq, gq);
+  const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
+  double u[4][NDEG];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < NDEG; k++) u[q][k] = Uget(d, d.Us, k, q, e);
+  const double rhomc = u[0][0];
+  const double uctr = u[1][0], vctr = u[2][0], ectr = u[3][0];
+  const double rhoct = 1.0 / rhomc;
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+
+  // getrhosubg_averg: initial sub-cell mass / current sub-cell volume
+  double unksgq[4];
+  {
+    const double posqc[12][2] = {{-0.5, -1.0}, {0.5, -1.0}, {1.0, -0.5}, {1.0, 0.5}, {0.5, 1.0}, {-0.5, 1.0},
+                                 {-1.0, 0.5}, {-1.0, -0.5}, {0.0, -0.5}, {0.5, 0.0}, {0.0, 0.5}, {-0.5, 0.0}};
+    const int ipqsc[4][4] = {{0, 8, 11, 7}, {1, 2, 9, 8}, {9, 3, 4, 10}, {11, 10, 5, 6}};
+    double xpqc[12][2], shp[9];
+#pragma unroll
+    for (int isc = 0; isc < 12; isc++) {
+      shp9v(posqc[isc][0], posqc[isc][1], shp);
+      map9(xpq, shp, xpqc[isc][0], xpqc[isc][1]);
+    }
+    for (int isg = 0; isg < 4; isg++) {
+      double xs[9][2];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        xs[k][0] = xpq[ipqsg_(isg, k)][0]; xs[k][1] = xpq[ipqsg_(isg, k)][1];
+        xs[4 + k][0] = xpqc[ipqsc[isg][k]][0]; xs[4 + k][1] = xpqc[ipqsc[isg][k]][1];
+      }
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+        xs[8][c] = -0.25 * (xs[0][c] + xs[1][c] + xs[2][c] + xs[3][c]) + 0.5 * (xs[4][c] + xs[5][c] + xs[6][c] + xs[7][c]);
+      double f0 = 0.0;
+      for (int ig = 0; ig < 25; ig++) {
+        double dr[9], ds[9];
+        shp9d(cQ.g25[ig][0], cQ.g25[ig][1], dr, ds);
+        Jac j = jac9(xs, dr, ds);
+        f0 = f0 + cQ.w25[ig] * (j.xr * j.ys - j.yr * j.xs);
+      }
+      unksgq[isg] = 0.0 + (1.0 / f0) * d.msub[isg * d.nquad + iq];
+    }
+  }
+  // getrhosubg_daverg: sub-cell harmonic specific volume of the DG tau
+  double uqsgc[4];
+  for (int isg = 0; isg < 4; isg++) {
+    double masel = 0.0, volel = 0.0;
+    const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
+    const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
+    for (int ig = 0; ig < 25; ig++) {
+      double r = (cQ.g25[ig][0] + ofr) / 2.0;
+      double s = (cQ.g25[ig][1] + ofs) / 2.0;
+      double b[6];
+      b[0] = 1.0; b[1] = (r - rc) / 1.0; b[2] = (s - sc) / 1.0;
+      b[3] = 0.5 * b[1] * b[1] - g19;
+      b[4] = 0.5 * b[2] * b[2] - g20;
+      b[5] = b[1] * b[2] - g21;
+      double rhomsg = 0.0;
+#pragma unroll
+      for (int k = 0; k < NDEG; k++)
+        if (k < d.mdegr) rhomsg = rhomsg + u[0][k] * b[k];
+      if (d.nlimi == 6) rhomsg = rhomc + 1.0 * (rhomsg - rhomc);
+      double dr[9], ds[9];
+      shp9d(r, s, dr, ds);
+      Jac j = jac9(xpq, dr, ds);
+      double djaco = cQ.w25[ig] * (j.xr * j.ys - j.yr * j.xs) * 0.25;
+      masel = masel + 1.0 / rhomsg * djaco;
+      volel = volel + djaco;
+    }
+    uqsgc[isg] = volel / masel;
+  }
+  // states at the 9 nodes
+  double unknvq[9][4];
+#pragma unroll
+  for (int iv = 0; iv < 9; iv++) {
+    double b[6];
+    node_basis(rc, sc, g19, g20, g21, iv, b);
+#pragma unroll
+    for (int q = 0; q < 4; q++) unknvq[iv][q] = 0.0;
+#pragma unroll
+    for (int k = 0; k < NDEG; k++)
+      if (k < d.mdegr)
+#pragma unroll
+        for (int q = 0; q < 4; q++) unknvq[iv][q] = unknvq[iv][q] + u[q][k] * b[k];
+  }
+  for (int isg = 0; isg < 4; isg++) {
+    double uv[4][2], sig[4], aj3[4];
+#pragma unroll
+    for (int ivsg = 0; ivsg < 4; ivsg++) {
+      const int iv = ipqsg_(isg, ivsg);
+      double rhovt = 1.0 / unknvq[iv][0];
+      double rhovsg = rhovt + d.cdrho * (unksgq[isg] - 1.0 / uqsgc[isg]);
+      double uvtx = unknvq[iv][1], vvtx = unknvq[iv][2], evtx = unknvq[iv][3];
+      double pvtx = fmax(eps, (g - 1.0) * rhovsg * (evtx - 0.5 * (uvtx * uvtx + vvtx * vvtx)));
+      uv[ivsg][0] = uvtx;
+      uv[ivsg][1] = vvtx;
+      sig[ivsg] = -pvtx;
+      const int p = d.ipq[iv * d.nquad + iq];
+      double acnx = d.us[p] - uvtx, acny = d.vs[p] - vvtx;
+      aj3[ivsg] = sqrt(acnx * acnx + acny * acny) / sdctr;
+    }
+#pragma unroll
+    for (int ivsg = 0; ivsg < 4; ivsg++) {
+      const int iv = ipqsg_(isg, ivsg);
+      const int p = d.ipq[iv * d.nquad + iq];
+      double dux = d.us[p] - uv[ivsg][0];
+      double duy = d.vs[p] - uv[ivsg][1];
+#pragma unroll
+      for (int f = 0; f < 2; f++) {
+        double n0, n1, a;
+        corner_normal(gq, isg, ivsg, f, n0, n1, a);
+        a = a * cWRIE[isg][ivsg][f];
+        double deltu = fabs(dux * n0 + duy * n1);
+        double murie = rhoct * sdctr + d.cimpd * rhoct * slpdu * deltu;
+        double vnau;
+        if (aj3[ivsg] < 1.0e12) {
+          vnau = 1.0;
+        } else {
+          // unit jump direction (Getrhslaggauss.f90:10780-10786)
+          double acnx = dux, acny = duy;
+          double ax, ay;
+          if (sqrt(acnx * acnx + acny * acny) < (double)1.e-11f) { ax = (double)1.e-11f; ay = (double)1.e-11f; }
+          else { ax = acnx / sqrt(acnx * acnx + acny * acny); ay = acny / sqrt(acnx * acnx + acny * acny); }
+          vnau = n0 * ax + n1 * ay;
+        }
+        double m = murie * a * fabs(vnau);
+        double mu0 = m * uv[ivsg][0] + 0.0 * uv[ivsg][1];
+        double mu1 = 0.0 * uv[ivsg][0] + m * uv[ivsg][1];
+        double sn0 = sig[ivsg] * a * n0 + 0.0 * a * n1;
+        double sn1 = 0.0 * a * n0 + sig[ivsg] * a * n1;
+        const int slot = f + 2 * (ivsg + 4 * isg);
+        d.cf[(0 * 32 + slot) * d.nquad + iq] = m;
+        d.cf[(1 * 32 + slot) * d.nquad + iq] = mu0;
+        d.cf[(2 * 32 + slot) * d.nquad + iq] = mu1;
+        d.cf[(3 * 32 + slot) * d.nquad + iq] = sn0;
+        d.cf[(4 * 32 + slot) * d.nquad + iq] = sn1;
+      }
+    }
+  }
+}
+__global__ void __launch_bounds__(128) k_corner(Dev d) { b_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// ---------------------------------------------------------------------------
+// Node pass: node sums in the reference's scatter order, 2x2 solve and wall
+// conditions (getndvelo_lagsubg, Getrhslaggauss.f90:4465-4545).
+// ---------------------------------------------------------------------------
+__host__ __device__ void b_node(const Dev &d, int p) {
+  if (p >= d.npoin || stopped(d)) return;
+  double mn0 = 0.0, mn1 = 0.0, mn2 = 0.0, mn3 = 0.0, mu0 = 0.0, mu1 = 0.0, sn0 = 0.0, sn1 = 0.0;
+  const int b = d.node_ptr[p], en = d.node_ptr[p + 1];
+  for (int i = b; i < en; i++) {
+    const int id = d.node_cf[i];
+    const int iq = id >> 5, slot = id & 31;
+    const double m = d.cf[(0 * 32 + slot) * d.nquad + iq];
+    mn0 = mn0 + m;
+    mn1 = mn1 + 0.0;
+    mn2 = mn2 + 0.0;
+    mn3 = mn3 + m;
+    mu0 = mu0 + d.cf[(1 * 32 + slot) * d.nquad + iq];
+    mu1 = mu1 + d.cf[(2 * 32 + slot) * d.nquad + iq];
+    sn0 = sn0 + d.cf[(3 * 32 + slot) * d.nquad + iq];
+    sn1 = sn1 + d.cf[(4 * 32 + slot) * d.nquad + iq];
+  }
+  const unsigned char mask = d.bcmask[p];
+  double us = d.us[p], vs = d.vs[p];
+  if (!(mask & 4)) {
+    double detma = mn0 * mn3 - mn1 * mn2;
+    double i11 = mn3 / detma, i12 = -mn2 / detma, i21 = -mn1 / detma, i22 = mn0 / detma;
+    double r1 = mu0 - sn0, r2 = mu1 - sn1;
+    us = i11 * r1 + i12 * r2;
+    vs = i21 * r1 + i22 * r2;
+  }
+  if (mask & 1) us = 0.0;
+  if (mask & 2) vs = 0.0;
+  d.us[p] = us;
+  d.vs[p] = vs;
+}
+__global__ void k_node(Dev d) { b_node(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// ---------------------------------------------------------------------------
+// RHS pass: corner forces (getndvelo_lagsubg Part III, :4588-4610), face
+// integral (rhsifacedg_lagsubgq2, :8501-8748), volume integral
+// (rhsdomndg_lagmc_curvquad, Getrhslag.f90:4716-5016, 5x5 Gauss-Lobatto,
+// cofactor form) and the Taylor-Green source (rhsdomnsrcdg_lag_curvquad,
+// Getrhslag.f90:4070-4251).
+// ---------------------------------------------------------------------------
+__host__ __device__ void b_rhs(const Dev &d, int iq) {
+  if (iq >= d.nquad || stopped(d)) return;
+  const int e = iq + d.ntria;
+  const double eps = 1.0e-6, g = d.gamlg;
+  double xpq[9][2];
+  load_quad(d, d.xs, d.ys, iq, xpq);
+  double gq[16][3];
+  normals_quad(xpq, gq);
+  const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
+  double ul[6] = {0, 0, 0, 0, 0, 0}, p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0},
+         el[6] = {0, 0, 0, 0, 0, 0};
+  for (int isg = 0; isg < 4; isg++) {
+#pragma unroll
+    for (int ivsg = 0; ivsg < 4; ivsg++) {
+      const int iv = ipqsg_(isg, ivsg);
+      const int p = d.ipq[iv * d.nquad + iq];
+      const double us0 = d.us[p], us1 = d.vs[p];
+      double b[6];
+      node_basis(rc, sc, g19, g20, g21, iv, b);
+      double n[2][2], a[2], fs[2][2];
+#pragma unroll
+      for (int f = 0; f < 2; f++) {
+        corner_normal(gq, isg, ivsg, f, n[f][0], n[f][1], a[f]);
+        a[f] = a[f] * cWMAS[isg][ivsg][f];
+        const int slot = f + 2 * (ivsg + 4 * isg);
+        const double m = d.cf[(0 * 32 + slot) * d.nquad + iq];
+        const double mu0 = d.cf[(1 * 32 + slot) * d.nquad + iq];
+        const double mu1 = d.cf[(2 * 32 + slot) * d.nquad + iq];
+        const double sn0 = d.cf[(3 * 32 + slot) * d.nquad + iq];
+        const double sn1 = d.cf[(4 * 32 + slot) * d.nquad + iq];
+        fs[f][0] = sn0 + m * us0 + 0.0 * us1 - mu0;
+        fs[f][1] = sn1 + 0.0 * us0 + m * us1 - mu1;
+      }
+      const double w1 = cWMOM[isg][ivsg], w2 = cWMOM[isg][ivsg];
+#pragma unroll
+      for (int k = 0; k < NDEG; k++) {
+        const double bk = b[k];
+        ul[k] = ul[k] + us0 * n[0][0] * a[0] * bk + us1 * n[0][1] * a[0] * bk + us0 * n[1][0] * a[1] * bk +
+                us1 * n[1][1] * a[1] * bk;
+        p0[k] = p0[k] + fs[0][0] * bk * w1 + fs[1][0] * bk * w2;
+        p1[k] = p1[k] + fs[0][1] * bk * w1 + fs[1][1] * bk * w2;
+        el[k] = el[k] + us0 * fs[0][0] * bk * w1 + us1 * fs[0][1] * bk * w1 + us0 * fs[1][0] * bk * w2 +
+                us1 * fs[1][1] * bk * w2;
+      }
+    }
+  }
+  // volume integral
+  double u[4][NDEG];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < NDEG; k++) u[q][k] = Uget(d, d.Us, k, q, e);
+  double dbdr[6] = {0.0, 1.0 / 1.0, 0.0, 0.0, 0.0, 0.0}, dbds[6] = {0.0, 0.0, 1.0 / 1.0, 0.0, 0.0, 0.0};
+  for (int ig = 0; ig < 25; ig++) {
+    const double r = cQ.l25[ig][0], s = cQ.l25[ig][1], wi = cQ.wl25[ig];
+    double dr[9], ds[9];
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xpq, dr, ds);
+    const double djaco = wi;
+    dbdr[3] = (r - rc) / (1.0 * 1.0); dbdr[4] = 0.0; dbdr[5] = (s - sc) / 1.0 / 1.0;
+    dbds[3] = 0.0; dbds[4] = (s - sc) / (1.0 * 1.0); dbds[5] = (r - rc) / 1.0 / 1.0;
+    double b[6];
+    b[0] = 1.0; b[1] = (r - rc) / 1.0; b[2] = (s - sc) / 1.0;
+    b[3] = 0.5 * b[1] * b[1] - g19;
+    b[4] = 0.5 * b[2] * b[2] - g20;
+    b[5] = b[1] * b[2] - g21;
+    double un[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < NDEG; k++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) un[q] = un[q] + u[q][k] * b[k];
+    const double rhoad = 1.0 / un[0];
+    const double uadv = un[1], vadv = un[2], eadv = un[3];
+    const double pres = fmax(eps, (g - 1.0) * rhoad * (eadv - 0.5 * (uadv * uadv + vadv * vadv)));
+#pragma unroll
+    for (int k = 0; k < NDEG; k++) {
+      double gd0 = j.ys * dbdr[k] + (-j.yr) * dbds[k];
+      double gd1 = (-j.xs) * dbdr[k] + j.xr * dbds[k];
+      double f0 = gd0 * uadv + gd1 * vadv;
+      double f1 = gd0 * (-pres);
+      double f2 = gd1 * (-pres);
+      double f3 = (gd0 * uadv + gd1 * vadv) * (-pres);
+      ul[k] = ul[k] - f0 * djaco;
+      p0[k] = p0[k] - f1 * djaco;
+      p1[k] = p1[k] - f2 * djaco;
+      el[k] = el[k] - f3 * djaco;
+    }
+  }
+  if (d.ncase == 1) {
+    for (int ig = 0; ig < 25; ig++) {
+      const double r = cQ.g25[ig][0], s = cQ.g25[ig][1], wi = cQ.w25[ig];
+      double shp[9], dr[9], ds[9];
+      shp9v(r, s, shp);
+      shp9d(r, s, dr, ds);
+      Jac j = jac9(xpq, dr, ds);
+      double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+      double xg, yg;
+      map9(xpq, shp, xg, yg);
+      double b[6];
+      b[0] = 1.0; b[1] = (r - rc) / 1.0; b[2] = (s - sc) / 1.0;
+      b[3] = 0.5 * b[1] * b[1] - g19;
+      b[4] = 0.5 * b[2] * b[2] - g20;
+      b[5] = b[1] * b[2] - g21;
+      double src = 0.25 * cPI * (cos(3.0 * cPI * xg) * cos(cPI * yg) - cos(3.0 * cPI * yg) * cos(cPI * xg)) / (g - 1.0);
+#pragma unroll
+      for (int k = 0; k < NDEG; k++) el[k] = el[k] + src * b[k] * djaco;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NDEG; k++) {
+    d.rhs[(0 * NDEG + k) * d.ncell + e] = ul[k];
+    d.rhs[(1 * NDEG + k) * d.ncell + e] = p0[k];
+    d.rhs[(2 * NDEG + k) * d.ncell + e] = p1[k];
+    d.rhs[(3 * NDEG + k) * d.ncell + e] = el[k];
+  }
+}
+__global__ void __launch_bounds__(128) k_rhs(Dev d) { b_rhs(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// ---------------------------------------------------------------------------
+// getdelt_lag (Getrhslag.f90:20600-20716): per-block minima of the CFL and
+// volume-change limits; min is exact, so the reduction is order independent.
+// ---------------------------------------------------------------------------
+// per-quad limits of getdelt_lag: dlen / c (CFL) and V / |dV/dt|
+__host__ __device__ void b_dt_values(const Dev &d, int iq, double &dtcfl, double &dtvol) {
+  dtcfl = 1e10;
+  dtvol = 1e10;
+  if (iq >= d.nquad || stopped(d)) return;
+  const int e = iq + d.ntria;
+  const double eps = 1.0e-6, g = d.gamlg;
+  double xp[9][2];
+  load_quad(d, d.xn, d.yn, iq, xp);
+  const int ed[4][3] = {{0, 4, 1}, {1, 5, 2}, {2, 6, 3}, {3, 7, 0}};
+  double dlen = 0.0;
+  for (int k = 0; k < 4; k++) {
+    const double *a = xp[ed[k][0]], *b = xp[ed[k][1]], *c = xp[ed[k][2]];
+    double dl = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1])) +
+                sqrt((b[0] - c[0]) * (b[0] - c[0]) + (b[1] - c[1]) * (b[1] - c[1]));
+    if (k == 0 || dl < dlen) dlen = dl;
+  }
+  const double rhomc = Uget(d, d.Us, 0, 0, e);
+  const double uctr = Uget(d, d.Us, 0, 1, e), vctr = Uget(d, d.Us, 0, 2, e), ectr = Uget(d, d.Us, 0, 3, e);
+  const double rhoct = 1.0 / rhomc;
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  dtcfl = dlen / sdctr;
+  dtvol = d.vol[e] / fabs(d.rhs[(0 * NDEG + 0) * d.ncell + e]);
+}
+
+// dtfix from the global minima (getdelt_lag :20705-20709, getsolvdg_lag :1766-1773)
+__host__ __device__ void b_dt_apply(const Dev &d, double mcfl, double mvol, int ndt) {
+  Scalars *S = d.sc_dev;
+  double dt = S->dtfix;
+  if (ndt == 1) {
+    double dtcfl = fmin(1e10, mcfl), dtvol = fmin(1e10, mvol);
+    if (S->itime == 1) dt = fmin(d.cfl * dtcfl, 0.1 * dtvol);
+    else dt = fmin(fmin(d.cfl * dtcfl, 0.1 * dtvol), 1.01 * dt);
+    if ((S->tacru + dt) > d.tend) dt = d.tend - S->tacru;
+  }
+  S->dtfix = dt;
+  S->tacru = S->tacru + dt;
+}
+
+// per-block minima; min is exact, so the reduction is order independent
+__global__ void k_dt_partial(Dev d) {
+  __shared__ double sm_cfl[256], sm_vol[256];
+  double dtcfl, dtvol;
+  b_dt_values(d, blockIdx.x * blockDim.x + threadIdx.x, dtcfl, dtvol);
+  sm_cfl[threadIdx.x] = dtcfl;
+  sm_vol[threadIdx.x] = dtvol;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sm_cfl[threadIdx.x] = fmin(sm_cfl[threadIdx.x], sm_cfl[threadIdx.x + s]);
+      sm_vol[threadIdx.x] = fmin(sm_vol[threadIdx.x], sm_vol[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    d.dtpart[2 * blockIdx.x] = sm_cfl[0];
+    d.dtpart[2 * blockIdx.x + 1] = sm_vol[0];
+  }
+}
+
+__global__ void k_dt_final(Dev d, int nblk, int ndt) {
+  __shared__ double sm_cfl[256], sm_vol[256];
+  if (stopped(d)) return;
+  double a = 1e10, b = 1e10;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+    a = fmin(a, d.dtpart[2 * i]);
+    b = fmin(b, d.dtpart[2 * i + 1]);
+  }
+  sm_cfl[threadIdx.x] = a;
+  sm_vol[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sm_cfl[threadIdx.x] = fmin(sm_cfl[threadIdx.x], sm_cfl[threadIdx.x + s]);
+      sm_vol[threadIdx.x] = fmin(sm_vol[threadIdx.x], sm_vol[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) b_dt_apply(d, sm_cfl[0], sm_vol[0], ndt);
+}
+
+// ---------------------------------------------------------------------------
+// Stage update (Getrhslag.f90:1789-1904): rhs *= dtfix, M^-1 apply and
+// U^(s+1) = alfa U^n + (1 - alfa)(U^(s) + M^-1 rhs).
+// ---------------------------------------------------------------------------
+__host__ __device__ void b_update(const Dev &d, int e, double alfa) {
+  if (e >= d.ncell || stopped(d)) return;
+  const double dt = d.sc_dev->dtfix;
+  double rhs[NDEG][4];
+#pragma unroll
+  for (int k = 0; k < NDEG; k++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) rhs[k][q] = dt * d.rhs[(q * NDEG + k) * d.ncell + e];
+  double am[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * d.ncell + e];
+  double mm[NDEG][NDEG];
+#pragma unroll
+  for (int i = 0; i < NDEG; i++)
+#pragma unroll
+    for (int j = 0; j < NDEG; j++) mm[i][j] = 0.0;
+  mm[0][0] = am[15];
+  {
+    int k = 0;
+#pragma unroll
+    for (int im = 1; im < NDEG; im++)
+#pragma unroll
+      for (int jm = im; jm < NDEG; jm++) {
+        mm[im][jm] = am[k];
+        mm[jm][im] = am[k];
+        k++;
+      }
+  }
+  const double oma = 1.0 - alfa;
+#pragma unroll
+  for (int id = 0; id < NDEG; id++) {
+    double unint[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int iu = 0; iu < NDEG; iu++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) unint[q] = unint[q] + mm[id][iu] * rhs[iu][q];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int idx = (q * NDEG + id) * d.ncell + e;
+      d.Us[idx] = alfa * d.Un[idx] + oma * (d.Us[idx] + unint[q]);
+    }
+  }
+}
+__global__ void k_update(Dev d, double alfa) { b_update(d, blockIdx.x * blockDim.x + threadIdx.x, alfa); }
+
+// Node motion (Getrhslag.f90:1948-1957)
+__host__ __device__ void b_nodes(const Dev &d, int p, double alfa) {
+  if (p >= d.npoin || stopped(d)) return;
+  const double dt = d.sc_dev->dtfix;
+  const double oma = 1.0 - alfa;
+  d.xs[p] = alfa * d.xn[p] + oma * (d.xs[p] + dt * d.us[p]);
+  d.ys[p] = alfa * d.yn[p] + oma * (d.ys[p] + dt * d.vs[p]);
+}
+__global__ void k_nodes(Dev d, double alfa) { b_nodes(d, blockIdx.x * blockDim.x + threadIdx.x, alfa); }
+
+// Driver copy-back (dgflo2d.f90:407-423) and exit test (dgflo2d.f90:459)
+__host__ __device__ void b_copyback(const Dev &d, int i, int stride) {
+  if (stopped(d)) return;
+  const int nu = NU * d.ncell;
+  for (int t = i; t < nu; t += stride) d.Un[t] = d.Us[t];
+  for (int t = i; t < d.npoin; t += stride) {
+    d.xn[t] = d.xs[t];
+    d.yn[t] = d.ys[t];
+  }
+}
+__global__ void k_copyback(Dev d) { b_copyback(d, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x); }
+
+// itime < 0: advance the device-resident step counter (graph replays)
+__host__ __device__ void b_step_begin(const Dev &d, int itime) {
+  Scalars *S = d.sc_dev;
+  if (S->done) return;
+  S->itime = (itime < 0) ? S->itime + 1 : itime;
+}
+__global__ void k_step_begin(Dev d, int itime) { b_step_begin(d, itime); }
+
+__host__ __device__ void b_step_end(const Dev &d, int check_done) {
+  Scalars *S = d.sc_dev;
+  if (S->done) return;
+  if (check_done && fabs(S->tacru - d.tend) / d.tend <= 1e-11) S->done = 1;
+}
+__global__ void k_step_end(Dev d, int check_done) { b_step_end(d, check_done); }
+
+__global__ void k_reset_count(Dev d) {
+  *d.wcount = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Initial fields on the device: getgeoel_initial_lag (GetInitial.f90:
+// 1484-1694), getgeoelho_initial_lag (:1891-2094), inifield_mcnew
+// (Getrhslagmc.f90:3621-3917), getunkno_initial_lag (GetInitial.f90:412-690)
+// and the initial sub-cell masses of getrhosubg_averg (Getrhslaggauss.f90:
+// 7300-7392), which the corner pass reuses every stage.
+// ---------------------------------------------------------------------------
+__host__ __device__ void getunkin(const Dev &d, double *unkin, double xg, double yg, int ielem1, double volel,
+                         double xc, double yc) {
+  const double g = d.gamlg;
+  double rhoini = 1.0, uini = 0.0, vini = 0.0, pini = 1.0;
+  if (d.ncase == 1) {
+    rhoini = 1.0;
+    uini = sin(cPI * xg) * cos(cPI * yg);
+    vini = -cos(cPI * xg) * sin(cPI * yg);
+    pini = 0.25 * (cos(2.0 * cPI * xg) + cos(2.0 * cPI * yg)) + 1.0;
+  } else if (d.ncase == 2) {
+    uini = -xg; vini = -yg; pini = (g - 1.0);
+  } else if (d.ncase == 3) {
+    uini = -xg / sqrt(xg * xg + yg * yg);
+    vini = -yg / sqrt(xg * xg + yg * yg);
+    pini = 1.0e-6;
+  } else if (d.ncase == 6) {
+    double ieini;
+    if (sqrt(xc * xc + (yc - 0.0) * (yc - 0.0)) <= 0.5) { rhoini = 1.0; ieini = 2.5; }
+    else { rhoini = 0.125; ieini = 2.0; }
+    pini = ieini * (g - 1.0) * rhoini;
+  } else if (d.ncase == 7) {
+    bool hit = false;
+    for (int i = 0; i < d.nsedov; i++) hit |= (d.sedov_cell[i] == ielem1);
+    pini = hit ? (g - 1.0) * 1.0 * d.sedov_energy / (1.0 * volel) : 1.0e-6;
+  }
+  unkin[0] = 1.0;
+  unkin[1] = rhoini * uini;
+  unkin[2] = rhoini * vini;
+  unkin[3] = (pini / rhoini / (g - 1.0) + 0.5 * (uini * uini + vini * vini)) * rhoini;
+}
+
+__host__ __device__ void b_init_geo(const Dev &d, int iq) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  const double alfrz = 0.0;
+  double xp[9][2], shp[9], dr[9], ds[9];
+  load_quad(d, d.x0, d.y0, iq, xp);
+  double xc, yc;
+  shp9v(0.0, 0.0, shp);
+  map9(xp, shp, xc, yc);
+  double xcent = 0, ycent = 0, xcel = 0, ycel = 0, volel = 0, masel = 0;
+  for (int ig = 0; ig < 36; ig++) {
+    double r = cQ.g36[ig][0], s = cQ.g36[ig][1], wi = cQ.w36[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    double rhog = rho_initial(d, xc, yc);
+    double rcoef = 1.0 - alfrz + alfrz * yg;
+    masel = masel + rhog * djaco * rcoef;
+    volel = volel + djaco * rcoef;
+    xcent = xcent + rhog * r * djaco * rcoef;
+    ycent = ycent + rhog * s * djaco * rcoef;
+    xcel = xcel + djaco * r * rcoef;
+    ycel = ycel + djaco * s * rcoef;
+  }
+  const double rc = xcent / masel, sc = ycent / masel;
+  const double rci = xcel / volel, sci = ycel / volel;
+  d.rc[e] = rc;
+  d.sc[e] = sc;
+  d.vol[e] = volel;
+  d.mass[e] = masel;
+  // P2 basis offsets
+  shp9v(rc, sc, shp);
+  map9(xp, shp, xc, yc);
+  double bq[6] = {0, 0, 0, 0, 0, 0}, bqi[6] = {0, 0, 0, 0, 0, 0};
+  for (int ig = 0; ig < 36; ig++) {
+    double r = cQ.g36[ig][0], s = cQ.g36[ig][1], wi = cQ.w36[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    double rhog = rho_initial(d, xc, yc);
+    double rcoef = 1.0 - alfrz + alfrz * yg;
+    bq[1] = (r - rc) / 1.0;
+    bq[2] = (s - sc) / 1.0;
+    bq[3] = bq[3] + 0.5 * rhog * bq[1] * bq[1] * djaco * rcoef;
+    bq[4] = bq[4] + 0.5 * rhog * bq[2] * bq[2] * djaco * rcoef;
+    bq[5] = bq[5] + rhog * bq[1] * bq[2] * djaco * rcoef;
+    bqi[1] = (r - rci) / 1.0;
+    bqi[2] = (s - sci) / 1.0;
+    bqi[3] = bqi[3] + 0.5 * bqi[1] * bqi[1] * djaco * rcoef;
+    bqi[4] = bqi[4] + 0.5 * bqi[2] * bqi[2] * djaco * rcoef;
+    bqi[5] = bqi[5] + bqi[1] * bqi[2] * djaco * rcoef;
+  }
+  d.g19[e] = bq[3] / masel;
+  d.g20[e] = bq[4] / masel;
+  d.g21[e] = bq[5] / masel;
+}
+__global__ void k_init_geo(Dev d) { b_init_geo(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// Initial sub-cell masses (getrhosubg_averg, Getrhslaggauss.f90:7300-7392):
+// time invariant, computed once from the initial coordinates.
+__host__ __device__ void b_init_msub(const Dev &d, int iq) {
+  if (iq >= d.nquad) return;
+  double xp[9][2], shp[9], dr[9], ds[9];
+  load_quad(d, d.x0, d.y0, iq, xp);
+  {
+    const double posqc[12][2] = {{-0.5, -1.0}, {0.5, -1.0}, {1.0, -0.5}, {1.0, 0.5}, {0.5, 1.0}, {-0.5, 1.0},
+                                 {-1.0, 0.5}, {-1.0, -0.5}, {0.0, -0.5}, {0.5, 0.0}, {0.0, 0.5}, {-0.5, 0.0}};
+    const int ipqsc[4][4] = {{0, 8, 11, 7}, {1, 2, 9, 8}, {9, 3, 4, 10}, {11, 10, 5, 6}};
+    double xpqc[12][2];
+    for (int isc = 0; isc < 12; isc++) {
+      shp9v(posqc[isc][0], posqc[isc][1], shp);
+      map9(xp, shp, xpqc[isc][0], xpqc[isc][1]);
+    }
+    double xci, yci;
+    shp9v(0.0, 0.0, shp);
+    map9(xp, shp, xci, yci);
+    for (int isg = 0; isg < 4; isg++) {
+      double xs[9][2];
+      for (int k = 0; k < 4; k++) {
+        xs[k][0] = xp[ipqsg_(isg, k)][0]; xs[k][1] = xp[ipqsg_(isg, k)][1];
+        xs[4 + k][0] = xpqc[ipqsc[isg][k]][0]; xs[4 + k][1] = xpqc[ipqsc[isg][k]][1];
+      }
+      for (int c = 0; c < 2; c++)
+        xs[8][c] = -0.25 * (xs[0][c] + xs[1][c] + xs[2][c] + xs[3][c]) + 0.5 * (xs[4][c] + xs[5][c] + xs[6][c] + xs[7][c]);
+      double rhs = 0.0;
+      for (int ig = 0; ig < 25; ig++) {
+        shp9d(cQ.g25[ig][0], cQ.g25[ig][1], dr, ds);
+        Jac j = jac9(xs, dr, ds);
+        double djaco = cQ.w25[ig] * (j.xr * j.ys - j.yr * j.xs);
+        double rhoi = rho_initial(d, xci, yci);
+        rhs = rhs + rhoi * 1.0 * djaco;
+      }
+      d.msub[isg * d.nquad + iq] = rhs;
+    }
+  }
+}
+__global__ void k_init_msub(Dev d) { b_init_msub(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+
+__host__ __device__ void getinvmat5(double *a, double *x) {
+  const int n = 5;
+  for (int k = 0; k < n; k++) {
+    for (int m = 0; m < k; m++) a[k + n * k] = a[k + n * k] - a[k + n * m] * a[m + n * k];
+    double adicv = 1.0 / a[k + n * k];
+    for (int i = k + 1; i < n; i++) {
+      for (int m = 0; m < k; m++) {
+        a[k + n * i] = a[k + n * i] - a[k + n * m] * a[m + n * i];
+        a[i + n * k] = a[i + n * k] - a[i + n * m] * a[m + n * k];
+      }
+      a[i + n * k] = a[i + n * k] * adicv;
+    }
+  }
+  for (int col = 0; col < n; col++) {
+    double *xc = x + n * col;
+    for (int i = 0; i < n; i++) {
+      double c = 0.0;
+      for (int j = 0; j < i; j++) c = c + a[i + n * j] * xc[j];
+      xc[i] = (i == col ? 1.0 : 0.0) - c;
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double c = 0.0;
+      for (int j = i + 1; j < n; j++) c = c + a[i + n * j] * xc[j];
+      xc[i] = (xc[i] - c) / a[i + n * i];
+    }
+  }
+}
+
+__host__ __device__ void b_init_fields(const Dev &d, int iq) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  const double alfrz = 0.0;
+  double xp[9][2], shp[9], dr[9], ds[9];
+  load_quad(d, d.x0, d.y0, iq, xp);
+  const double volel = d.vol[e], masel = d.mass[e];
+  const double rc = d.rc[e], sc = d.sc[e];
+  double unkin[4], rv[4] = {0, 0, 0, 0};
+  const double xcel = xp[8][0], ycel = xp[8][1];
+  for (int ig = 0; ig < 25; ig++) {
+    double r = cQ.g25[ig][0], s = cQ.g25[ig][1], wi = cQ.w25[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    getunkin(d, unkin, xg, yg, e + 1, volel, xcel, ycel);
+    double rcoef = 1.0 - alfrz + alfrz * yg;
+    for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
+  }
+  double u0[4];
+  for (int q = 0; q < 4; q++) u0[q] = rv[q] / masel;
+  double xc, yc;
+  shp9v(rc, sc, shp);
+  map9(xp, shp, xc, yc);
+  double rhsini[6][4], mmatr[25], matri[25];
+  for (int k = 0; k < 6; k++) for (int q = 0; q < 4; q++) rhsini[k][q] = 0.0;
+  for (int i = 0; i < 25; i++) mmatr[i] = 0.0;
+  double f0 = 0.0;
+  for (int ig = 0; ig < 25; ig++) {
+    double r = cQ.g25[ig][0], s = cQ.g25[ig][1], wi = cQ.w25[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    getunkin(d, unkin, xg, yg, e + 1, volel, xc, yc);
+    double bq[6];
+    bq[0] = 1.0; bq[1] = (r - rc) / 1.0; bq[2] = (s - sc) / 1.0;
+    bq[3] = 0.5 * bq[1] * bq[1] - d.g19[e];
+    bq[4] = 0.5 * bq[2] * bq[2] - d.g20[e];
+    bq[5] = bq[1] * bq[2] - d.g21[e];
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bq[k] * djaco;
+    double rho0 = rho_initial(d, xc, yc);
+    double rcoef = 1.0 - alfrz + alfrz * yg;
+    f0 = f0 + rho0 * djaco * rcoef;
+    for (int ix = 0; ix < 5; ix++)
+      for (int iy = 0; iy < 5; iy++) mmatr[ix + 5 * iy] = mmatr[ix + 5 * iy] + rho0 * bq[ix + 1] * bq[iy + 1] * djaco * rcoef;
+  }
+  getinvmat5(mmatr, matri);
+  {
+    int k = 0;
+    for (int im = 0; im < 5; im++)
+      for (int jm = im; jm < 5; jm++) d.amatr[(k++) * d.ncell + e] = matri[im + 5 * jm];
+    d.amatr[15 * d.ncell + e] = 1.0 / f0;
+  }
+  for (int q = 0; q < 4; q++) {
+    d.Un[(q * NDEG + 0) * d.ncell + e] = u0[q];
+    for (int ix = 0; ix < 5; ix++) {
+      double acc = 0.0;
+      for (int iy = 0; iy < 5; iy++) acc = acc + matri[ix + 5 * iy] * rhsini[iy + 1][q];
+      d.Un[(q * NDEG + ix + 1) * d.ncell + e] = acc;
+    }
+  }
+}
+__global__ void k_init_fields(Dev d) { b_init_fields(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// ---------------------------------------------------------------------------
+// Host-side launchers
+// ---------------------------------------------------------------------------
+void set_tables(const QuadTables &q, cudaStream_t st) {
+  Tables t;
+  t.q = q;
+  const double t1[4][4][2] = {
+      {{4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}, {1.0, 1.0}, {8.0 / 3.0, 4.0 / 3.0}},
+      {{8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}, {1.0, 1.0}},
+      {{1.0, 1.0}, {8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}},
+      {{4.0 / 3.0, 8.0 / 3.0}, {1.0, 1.0}, {8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}}};
+  const double t2[4][4][2] = {
+      {{4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 0.0}, {0.0, 0.0}, {0.0, 4.0 / 3.0}},
+      {{0.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 0.0 / 3.0}, {0.0, 0.0}},
+      {{0.0, 0.0}, {0.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 0.0 / 3.0}},
+      {{4.0 / 3.0, 0.0 / 3.0}, {0.0, 0.0}, {0.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}}};
+  const double t3[4][4] = {{1, 1, 0, 1}, {1, 1, 1, 0}, {0, 1, 1, 1}, {1, 0, 1, 1}};
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) {
+      t.wmom[a][b] = t3[a][b];
+      for (int f = 0; f < 2; f++) {
+        t.wrie[a][b][f] = 0.25 * t1[a][b][f];
+        t.wmas[a][b][f] = 0.25 * t2[a][b][f];
+      }
+    }
+  hT = t;
+  if (st) cudaMemcpyToSymbolAsync(cT, &t, sizeof(Tables), 0, cudaMemcpyHostToDevice, st);
+}
+
+static inline int nblk(int n, int b) { return (n + b - 1) / b; }
+
+#define LAUNCH_FAMILY(name) (name)
+
+void launch_geom(const Dev &d, cudaStream_t st, const double *X, const double *Y) {
+  k_geom<<<nblk(d.nquad, 128), 128, 0, st>>>(d, X, Y);
+}
+void launch_center_geom(const Dev &d, cudaStream_t st) {
+  k_center_geom<<<nblk(d.nquad, 256), 256, 0, st>>>(d);
+}
+void launch_reset_count(const Dev &d, cudaStream_t st) { k_reset_count<<<1, 1, 0, st>>>(d); }
+void launch_persson(const Dev &d, cudaStream_t st) { k_persson<<<nblk(d.nquad, 128), 128, 0, st>>>(d); }
+void launch_flags_from_host(const Dev &d, cudaStream_t st, const int *flags) {
+  k_flags_from_host<<<nblk(d.nquad, 256), 256, 0, st>>>(d, flags);
+}
+void launch_weno(const Dev &d, cudaStream_t st) { k_weno<<<nblk(d.nquad, 64), 64, 0, st>>>(d); }
+void launch_weno_commit(const Dev &d, cudaStream_t st) { k_weno_commit<<<nblk(d.nquad, 256), 256, 0, st>>>(d); }
+void launch_corner(const Dev &d, cudaStream_t st) { k_corner<<<nblk(d.nquad, 128), 128, 0, st>>>(d); }
+void launch_node(const Dev &d, cudaStream_t st) { k_node<<<nblk(d.npoin, 256), 256, 0, st>>>(d); }
+void launch_rhs(const Dev &d, cudaStream_t st) { k_rhs<<<nblk(d.nquad, 128), 128, 0, st>>>(d); }
+int dt_blocks(const Dev &d) { return nblk(d.nquad, 256); }
+void launch_dt(const Dev &d, cudaStream_t st, int ndt) {
+  int nb = nblk(d.nquad, 256);
+  k_dt_partial<<<nb, 256, 0, st>>>(d);
+  k_dt_final<<<1, 256, 0, st>>>(d, nb, ndt);
+}
+void launch_update(const Dev &d, cudaStream_t st, double alfa) {
+  k_update<<<nblk(d.ncell, 128), 128, 0, st>>>(d, alfa);
+}
+void launch_nodes(const Dev &d, cudaStream_t st, double alfa) {
+  k_nodes<<<nblk(d.npoin, 256), 256, 0, st>>>(d, alfa);
+}
+void launch_copyback(const Dev &d, cudaStream_t st) { k_copyback<<<1184, 256, 0, st>>>(d); }
+void launch_step_begin(const Dev &d, cudaStream_t st, int itime) { k_step_begin<<<1, 1, 0, st>>>(d, itime); }
+void launch_step_end(const Dev &d, cudaStream_t st, int check) { k_step_end<<<1, 1, 0, st>>>(d, check); }
+void launch_init_msub(const Dev &d, cudaStream_t st) {
+  k_init_msub<<<nblk(d.nquad, 128), 128, 0, st>>>(d);
+}
+void launch_init(const Dev &d, cudaStream_t st) {
+  k_init_geo<<<nblk(d.nquad, 128), 128, 0, st>>>(d);
+  k_init_fields<<<nblk(d.nquad, 128), 128, 0, st>>>(d);
+}
+
+}  // namespace lag2d

@@ -1,0 +1,1724 @@
+/*
+ * Lag2D CPU oracle -- TEST INFRASTRUCTURE ONLY (see lag2d_oracle.h).
+ *
+ * Single-threaded FP64 restatement of the reference time step for the
+ * curved-quad P2 path.  Every routine keeps the reference's loop nests and
+ * left-to-right accumulation order so that, compiled with
+ * -O2 -ffp-contract=off (no FMA, like gfortran -O on x86-64), it reproduces
+ * the reference arithmetic.  Citations are to srccurv-lag/<file>:<line>.
+ *
+ * Deliberate differences (each is rounding-level or a documented knob):
+ *  - small dense inverses (Matinv225, LinearAlgebra.f90:130) are computed by
+ *    Gauss-Jordan elimination instead of the expanded cofactor formulas;
+ *  - the Sedov energy cells are a parameter instead of the hard-coded ids
+ *    of Getrhslagmc.f90:5634;
+ *  - barthlimit_lagcurv (Limiterlag.f90:5957) is not called: on the P2
+ *    branch its node bounds are never read (Getrhslagmc.f90:7598-7656);
+ *  - getbc_lagc_general (GetBClag.f90:628) is not called: its force is
+ *    computed but the ustar solve has it commented out
+ *    (Getrhslaggauss.f90:4502-4503).
+ */
+#include "lag2d_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdio.h>
+
+#define U_(U, c, id, iq, ie) (U)[(id) + (c)->ndegr * ((iq) + (c)->nq * (ie))]
+#define G_(G, k, ie) (G)[(k) + 24 * (ie)]
+#define X_(X, d, ip) (X)[(d) + 2 * (ip)]
+
+static const double PI_ = 3.14159265358979311599796346854;  /* 4*atan(1) */
+
+/* Set when a troubled quad has a vertex neighbourhood the reference's WENO
+ * stencil search rejects with `stop` (WENO.f90:7699); the cell is skipped. */
+static int g_status = 0;
+int o_status(void) { int s = g_status; g_status = 0; return s; }
+
+/* ---------------------------------------------------------------------- */
+/* Quadrature rules: dgflo2d.f90:2497-2783 (2-D tensor rules).            */
+/* ---------------------------------------------------------------------- */
+static void gauss_1d(int n, double *p, double *w) {
+  /* ruqope, dgflo2d.f90:2700-2753 (points listed in the reference order) */
+  if (n == 5) {
+    p[2] = 0.0;
+    p[3] = 0.5384693101056830910363144;  p[1] = -0.5384693101056830910363144;
+    p[4] = 0.9061798459386639927976269;  p[0] = -0.9061798459386639927976269;
+    w[2] = 0.5688888888888888888888889;
+    w[3] = 0.4786286704993664680412915;  w[1] = 0.4786286704993664680412915;
+    w[4] = 0.2369268850561890875142640;  w[0] = 0.2369268850561890875142640;
+  } else if (n == 6) {
+    p[0] = 0.2386191860831969086305017;  p[1] = -0.2386191860831969086305017;
+    p[2] = 0.6612093864662645136613996;  p[3] = -0.6612093864662645136613996;
+    p[4] = -0.9324695142031520278123016; p[5] = 0.9324695142031520278123016;
+    w[0] = 0.4679139345726910; w[1] = 0.4679139345726910;
+    w[2] = 0.3607615730481386; w[3] = 0.3607615730481386;
+    w[4] = 0.1713244923791704; w[5] = 0.1713244923791704;
+  } else if (n == 3) {
+    p[0] = -0.7745966692414833770358531; p[1] = 0.0; p[2] = 0.7745966692414833770358531;
+    w[0] = 0.5555555555555555555555556; w[1] = 0.8888888888888888888888889;
+    w[2] = 0.5555555555555555555555556;
+  } else if (n == 2) {
+    p[0] = -0.5773502691896257645091488; p[1] = 0.5773502691896257645091488;
+    w[0] = 1.0; w[1] = 1.0;
+  } else {
+    fprintf(stderr, "oracle: unsupported Gauss rule %d\n", n);
+    abort();
+  }
+}
+
+static void lobatto_1d(int n, double *p, double *w) {
+  /* ruqope_lobatto, dgflo2d.f90:2551-2605 */
+  if (n == 5) {
+    p[0] = -1.0; p[1] = -0.6546536707079771437983; p[2] = 0.0;
+    p[3] = 0.6546536707079771437983; p[4] = 1.0;
+    w[0] = 0.1; w[1] = 0.544444444444444444444; w[2] = 0.7111111111111111111111;
+    w[3] = 0.544444444444444444444; w[4] = 0.1;
+  } else {
+    fprintf(stderr, "oracle: unsupported Lobatto rule %d\n", n);
+    abort();
+  }
+}
+
+/* 2-D tensor rule: point (i,j) with i the outer loop (dgflo2d.f90:2618-2626). */
+static int quad_rule(int ngaus, int lobatto, double (*pos)[2], double *wt) {
+  int n = 0;
+  while (n * n < ngaus) n++;
+  double p[8], w[8];
+  if (lobatto) lobatto_1d(n, p, w); else gauss_1d(n, p, w);
+  int ig = 0;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) {
+      wt[ig] = w[i] * w[j];
+      pos[ig][0] = p[i];
+      pos[ig][1] = p[j];
+      ig++;
+    }
+  return ig;
+}
+
+/* ---------------------------------------------------------------------- */
+/* 9-node quad shape functions: GetFE.f90:89-127 (same literal forms).     */
+/* ---------------------------------------------------------------------- */
+static void shp9(double r, double s, double *shp, double *dr, double *ds) {
+  const double c10 = 1.0;
+  if (shp) {
+    shp[0] = 0.25 * (c10 - r) * r * s * (c10 - s);
+    shp[1] = -0.25 * (c10 + r) * (c10 - s) * r * s;
+    shp[2] = 0.25 * (c10 + r) * (c10 + s) * r * s;
+    shp[3] = -0.25 * (c10 - r) * (c10 + s) * r * s;
+    shp[4] = -0.5 * (c10 - r * r) * (c10 - s) * s;
+    shp[5] = 0.5 * (c10 + r) * (c10 - s * s) * r;
+    shp[6] = 0.5 * (c10 - r * r) * (c10 + s) * s;
+    shp[7] = -0.5 * (c10 - r) * (c10 - s * s) * r;
+    shp[8] = (c10 - r * r) * (c10 - s * s);
+  }
+  if (dr) {
+    dr[0] = 0.25 * (2.0 * r - c10) * s * (s - 1.0);
+    dr[1] = 0.25 * (2.0 * r + c10) * s * (s - 1.0);
+    dr[2] = 0.25 * (2.0 * r + c10) * s * (s + 1.0);
+    dr[3] = 0.25 * (2.0 * r - c10) * s * (s + 1.0);
+    dr[4] = -r * s * (s - c10);
+    dr[5] = 0.5 * (2.0 * r + c10) * (c10 - s * s);
+    dr[6] = -r * s * (s + c10);
+    dr[7] = 0.5 * (2.0 * r - c10) * (1.0 - s * s);
+    dr[8] = -2.0 * r * (1.0 - s * s);
+  }
+  if (ds) {
+    ds[0] = 0.25 * (2.0 * s - c10) * r * (r - 1.0);
+    ds[1] = 0.25 * (2.0 * s - c10) * r * (r + 1.0);
+    ds[2] = 0.25 * (2.0 * s + c10) * r * (r + 1.0);
+    ds[3] = 0.25 * (2.0 * s + c10) * r * (r - 1.0);
+    ds[4] = 0.5 * (1.0 - r * r) * (2.0 * s - c10);
+    ds[5] = -r * s * (r + c10);
+    ds[6] = 0.5 * (1.0 - r * r) * (2.0 * s + c10);
+    ds[7] = -r * s * (r - c10);
+    ds[8] = -2.0 * s * (1.0 - r * r);
+  }
+}
+
+static void jac9(const double (*xp)[2], const double *dr, const double *ds,
+                 double *dxdr, double *dxds, double *dydr, double *dyds) {
+  double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
+  for (int k = 0; k < 9; k++) {
+    a = a + dr[k] * xp[k][0];
+    b = b + ds[k] * xp[k][0];
+    c = c + dr[k] * xp[k][1];
+    d = d + ds[k] * xp[k][1];
+  }
+  *dxdr = a; *dxds = b; *dydr = c; *dyds = d;
+}
+
+static void map9(const double (*xp)[2], const double *shp, double *x, double *y) {
+  double a = 0.0, b = 0.0;
+  for (int k = 0; k < 9; k++) {
+    a = a + shp[k] * xp[k][0];
+    b = b + shp[k] * xp[k][1];
+  }
+  *x = a; *y = b;
+}
+
+static void load_quad(const o_mesh *m, const double *X, int ie, double (*xp)[2]) {
+  for (int k = 0; k < 9; k++) {
+    int ip = m->ipqua[9 * ie + k] - 1;
+    xp[k][0] = X_(X, 0, ip);
+    xp[k][1] = X_(X, 1, ip);
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Small dense linear algebra.                                            */
+/* ---------------------------------------------------------------------- */
+/* Inverse of an n x n matrix (n <= 5), column-major a(i,j) = a[i + n*j].
+ * Gauss-Jordan with partial pivoting; replaces Matinv225
+ * (LinearAlgebra.f90:130) whose expanded cofactor forms give the same
+ * inverse up to rounding. */
+static void inv_small(int n, const double *a, double *b) {
+  double t[25], e[25];
+  memcpy(t, a, sizeof(double) * n * n);
+  for (int i = 0; i < n * n; i++) e[i] = 0.0;
+  for (int i = 0; i < n; i++) e[i + n * i] = 1.0;
+  for (int k = 0; k < n; k++) {
+    int piv = k;
+    double big = fabs(t[k + n * k]);
+    for (int i = k + 1; i < n; i++)
+      if (fabs(t[i + n * k]) > big) { big = fabs(t[i + n * k]); piv = i; }
+    if (piv != k)
+      for (int j = 0; j < n; j++) {
+        double s = t[k + n * j]; t[k + n * j] = t[piv + n * j]; t[piv + n * j] = s;
+        s = e[k + n * j]; e[k + n * j] = e[piv + n * j]; e[piv + n * j] = s;
+      }
+    double d = 1.0 / t[k + n * k];
+    for (int j = 0; j < n; j++) { t[k + n * j] *= d; e[k + n * j] *= d; }
+    for (int i = 0; i < n; i++) {
+      if (i == k) continue;
+      double f = t[i + n * k];
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; j++) {
+        t[i + n * j] -= f * t[k + n * j];
+        e[i + n * j] -= f * e[k + n * j];
+      }
+    }
+  }
+  memcpy(b, e, sizeof(double) * n * n);
+}
+
+/* getinvmat / ludeco / lureso, dgflo2d.f90:2792-2908: in-place LU without
+ * pivoting followed by n triangular solves (column-major). */
+static void getinvmat(int n, double *a, double *x) {
+  for (int k = 0; k < n; k++) {
+    for (int mm = 0; mm < k; mm++) a[k + n * k] = a[k + n * k] - a[k + n * mm] * a[mm + n * k];
+    double adicv = 1.0 / a[k + n * k];
+    for (int i = k + 1; i < n; i++) {
+      for (int mm = 0; mm < k; mm++) {
+        a[k + n * i] = a[k + n * i] - a[k + n * mm] * a[mm + n * i];
+        a[i + n * k] = a[i + n * k] - a[i + n * mm] * a[mm + n * k];
+      }
+      a[i + n * k] = a[i + n * k] * adicv;
+    }
+  }
+  for (int col = 0; col < n; col++) {
+    double b[8], *xc = x + n * col;
+    for (int j = 0; j < n; j++) b[j] = 0.0;
+    b[col] = 1.0;
+    for (int i = 0; i < n; i++) {
+      double c = 0.0;
+      for (int j = 0; j < i; j++) c = c + a[i + n * j] * xc[j];
+      xc[i] = b[i] - c;
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double c = 0.0;
+      for (int j = i + 1; j < n; j++) c = c + a[i + n * j] * xc[j];
+      xc[i] = (xc[i] - c) / a[i + n * i];
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Initial condition tables: getrhog_initial (GetInitial.f90:4-147) and   */
+/* getunkin (Getrhslagmc.f90:5527-5844), ideal-gas cases used here.      */
+/* ---------------------------------------------------------------------- */
+static double rho_initial(const o_cfg *c, double xg, double yg, double xc, double yc) {
+  (void)xg; (void)yg;
+  if (c->ncase == 6) return (sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125;
+  return 1.0;  /* TGV (1), shockless Noh (2), Noh (3), Sedov (7) */
+}
+
+static int is_sedov_cell(const o_cfg *c, int ielem1) {
+  for (int i = 0; i < c->sedov_ncell; i++) if (c->sedov_cell[i] == ielem1) return 1;
+  return 0;
+}
+
+static void getunkin(const o_cfg *c, double *unkin, double xg, double yg,
+                     int ielem1, double volel, double xc, double yc) {
+  const double g = c->gamlg;
+  double rhoini = 1.0, uini = 0.0, vini = 0.0, pini = 1.0, ieini;
+  switch (c->ncase) {
+    case 1:
+      rhoini = 1.0;
+      uini = sin(PI_ * xg) * cos(PI_ * yg);
+      vini = -cos(PI_ * xg) * sin(PI_ * yg);
+      pini = 0.25 * (cos(2.0 * PI_ * xg) + cos(2.0 * PI_ * yg)) + 1.0;
+      break;
+    case 2:
+      rhoini = 1.0; uini = -xg; vini = -yg; pini = (g - 1.0);
+      break;
+    case 3:
+      rhoini = 1.0;
+      uini = -xg / sqrt(xg * xg + yg * yg);
+      vini = -yg / sqrt(xg * xg + yg * yg);
+      pini = 1.0e-6;
+      break;
+    case 6:
+      if (sqrt(xc * xc + (yc - 0.0) * (yc - 0.0)) <= 0.5) {
+        rhoini = 1.0; ieini = 2.5; pini = ieini * (g - 1.0) * rhoini;
+      } else {
+        rhoini = 0.125; ieini = 2.0; pini = ieini * (g - 1.0) * rhoini;
+      }
+      break;
+    case 7:
+      rhoini = 1.0;
+      if (is_sedov_cell(c, ielem1)) pini = (g - 1.0) * 1.0 * c->sedov_energy / (1.0 * volel);
+      else pini = 1.0e-6;
+      break;
+    default:
+      fprintf(stderr, "oracle: unsupported ncase %d\n", c->ncase);
+      abort();
+  }
+  unkin[0] = 1.0;
+  unkin[1] = rhoini * uini;
+  unkin[2] = rhoini * vini;
+  unkin[3] = (pini / rhoini / (g - 1.0) + 0.5 * (uini * uini + vini * vini)) * rhoini;
+}
+
+/* GetCellctr_quad_initial, GetInitial.f90:2100-2159 */
+static void cellctr_quad(const double (*xpqi)[2], double rc, double sc, double *x, double *y) {
+  double shp[9];
+  shp9(rc, sc, shp, NULL, NULL);
+  map9(xpqi, shp, x, y);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Initialisation                                                         */
+/* ---------------------------------------------------------------------- */
+void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
+            double *geoel, double *amatr, double *unkno) {
+  const int ntria = m->ntria, nquad = m->nquad;
+  const int ncell = ntria + nquad, nsize = ncell + m->nbfac;
+  const double alfrz = 0.0;
+  double pos36[36][2], w36[36], pos25[25][2], w25[25];
+  quad_rule(36, 0, pos36, w36);
+  quad_rule(25, 0, pos25, w25);
+  if (ntria > 0) { fprintf(stderr, "oracle: triangles not supported\n"); abort(); }
+  memset(geoel, 0, sizeof(double) * 24 * nsize);
+  memset(unkno, 0, sizeof(double) * c->ndegr * c->nq * nsize);
+
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + ntria;
+    double xp[9][2], shp[9], dr[9], ds[9];
+    load_quad(m, coord, ie, xp);
+
+    /* getgeoel_initial_lag, GetInitial.f90:1484-1694 */
+    double xc, yc;
+    shp9(0.0, 0.0, shp, NULL, NULL);
+    map9((const double(*)[2])xp, shp, &xc, &yc);
+    double xcent = 0, ycent = 0, xcel = 0, ycel = 0, volel = 0, masel = 0;
+    for (int ig = 0; ig < 36; ig++) {
+      double r = pos36[ig][0], s = pos36[ig][1], wi = w36[ig];
+      double a, b, cc, d, xg, yg;
+      shp9(r, s, shp, dr, ds);
+      jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+      double djaco = wi * (a * d - cc * b);
+      map9((const double(*)[2])xp, shp, &xg, &yg);
+      double rhog = rho_initial(c, xg, yg, xc, yc);
+      double rcoef = 1.0 - alfrz + alfrz * yg;
+      masel = masel + rhog * djaco * rcoef;
+      volel = volel + djaco * rcoef;
+      xcent = xcent + rhog * r * djaco * rcoef;
+      ycent = ycent + rhog * s * djaco * rcoef;
+      xcel = xcel + djaco * r * rcoef;
+      ycel = ycel + djaco * s * rcoef;
+    }
+    G_(geoel, 0, ielem) = xcent / masel;
+    G_(geoel, 1, ielem) = ycent / masel;
+    G_(geoel, 2, ielem) = volel;
+    G_(geoel, 3, ielem) = masel;
+    {
+      double mx = xp[0][1], mn = xp[0][1];
+      for (int k = 1; k < 4; k++) { if (xp[k][1] > mx) mx = xp[k][1]; if (xp[k][1] < mn) mn = xp[k][1]; }
+      G_(geoel, 4, ielem) = mx - mn;
+    }
+    G_(geoel, 6, ielem) = xcel / volel;
+    G_(geoel, 7, ielem) = ycel / volel;
+  }
+
+  if (c->npoly == 2) {
+    /* getgeoelho_initial_lag, GetInitial.f90:1891-2094 */
+    for (int ie = 0; ie < nquad; ie++) {
+      const int ielem = ie + ntria;
+      double xp[9][2], shp[9], dr[9], ds[9];
+      load_quad(m, coord, ie, xp);
+      double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+      double rci = G_(geoel, 6, ielem), sci = G_(geoel, 7, ielem);
+      double volel = G_(geoel, 2, ielem), masel = G_(geoel, 3, ielem);
+      double xc, yc;
+      shp9(rc, sc, shp, NULL, NULL);
+      map9((const double(*)[2])xp, shp, &xc, &yc);
+      double bq[6] = {0, 0, 0, 0, 0, 0}, bqi[6] = {0, 0, 0, 0, 0, 0};
+      for (int ig = 0; ig < 36; ig++) {
+        double r = pos36[ig][0], s = pos36[ig][1], wi = w36[ig];
+        double a, b, cc, d, xg, yg;
+        shp9(r, s, shp, dr, ds);
+        jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+        double djaco = wi * (a * d - cc * b);
+        map9((const double(*)[2])xp, shp, &xg, &yg);
+        double rhog = rho_initial(c, xg, yg, xc, yc);
+        double rcoef = 1.0 - alfrz + alfrz * yg;
+        bq[0] = 1.0;
+        bq[1] = (r - rc) / 1.0;
+        bq[2] = (s - sc) / 1.0;
+        bq[3] = bq[3] + 0.5 * rhog * bq[1] * bq[1] * djaco * rcoef;
+        bq[4] = bq[4] + 0.5 * rhog * bq[2] * bq[2] * djaco * rcoef;
+        bq[5] = bq[5] + rhog * bq[1] * bq[2] * djaco * rcoef;
+        bqi[0] = 1.0;
+        bqi[1] = (r - rci) / 1.0;
+        bqi[2] = (s - sci) / 1.0;
+        bqi[3] = bqi[3] + 0.5 * bqi[1] * bqi[1] * djaco * rcoef;
+        bqi[4] = bqi[4] + 0.5 * bqi[2] * bqi[2] * djaco * rcoef;
+        bqi[5] = bqi[5] + bqi[1] * bqi[2] * djaco * rcoef;
+      }
+      G_(geoel, 18, ielem) = bq[3] / masel;
+      G_(geoel, 19, ielem) = bq[4] / masel;
+      G_(geoel, 20, ielem) = bq[5] / masel;
+      G_(geoel, 21, ielem) = bqi[3] / volel;
+      G_(geoel, 22, ielem) = bqi[4] / volel;
+      G_(geoel, 23, ielem) = bqi[5] / volel;
+    }
+  }
+
+  /* inifield_mcnew, Getrhslagmc.f90:3621-3917: cell averages */
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + ntria;
+    double xp[9][2], shp[9], dr[9], ds[9], unkin[4];
+    load_quad(m, coord, ie, xp);
+    double volel = G_(geoel, 2, ielem), masel = G_(geoel, 3, ielem);
+    double xcel = xp[8][0], ycel = xp[8][1];
+    double rv[4] = {0, 0, 0, 0};
+    for (int ig = 0; ig < 25; ig++) {
+      double r = pos25[ig][0], s = pos25[ig][1], wi = w25[ig];
+      double a, b, cc, d, xg, yg;
+      shp9(r, s, shp, dr, ds);
+      jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+      double djaco = wi * (a * d - cc * b);
+      map9((const double(*)[2])xp, shp, &xg, &yg);
+      getunkin(c, unkin, xg, yg, ielem + 1, volel, xcel, ycel);
+      double rcoef = 1.0 - alfrz + alfrz * yg;
+      for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
+    }
+    for (int q = 0; q < 4; q++) U_(unkno, c, 0, q, ielem) = rv[q] / masel;
+  }
+
+  /* getunkno_initial_lag, GetInitial.f90:412-690: M^-1 and L2 projection */
+  const int nmatr = (c->npoly == 2) ? 16 : 4;
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + ntria;
+    const int nd = c->ndegr, nb = nd - 1;
+    double xp[9][2], shp[9], dr[9], ds[9], unkin[4];
+    load_quad(m, coord, ie, xp);
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double volel = G_(geoel, 2, ielem);
+    double xc, yc;
+    shp9(rc, sc, shp, NULL, NULL);
+    map9((const double(*)[2])xp, shp, &xc, &yc);
+    double rhsini[6][4];
+    double mmatr[25], matri[25];
+    memset(rhsini, 0, sizeof rhsini);
+    memset(mmatr, 0, sizeof mmatr);
+    double f0 = 0.0;
+    for (int ig = 0; ig < 25; ig++) {
+      double r = pos25[ig][0], s = pos25[ig][1], wi = w25[ig];
+      double a, b, cc, d, xg, yg, bq[6];
+      shp9(r, s, shp, dr, ds);
+      jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+      double djaco = wi * (a * d - cc * b);
+      map9((const double(*)[2])xp, shp, &xg, &yg);
+      getunkin(c, unkin, xg, yg, ielem + 1, volel, xc, yc);
+      bq[0] = 1.0;
+      bq[1] = (r - rc) / 1.0;
+      bq[2] = (s - sc) / 1.0;
+      if (c->npoly == 2) {
+        bq[3] = 0.5 * bq[1] * bq[1] - G_(geoel, 18, ielem);
+        bq[4] = 0.5 * bq[2] * bq[2] - G_(geoel, 19, ielem);
+        bq[5] = bq[1] * bq[2] - G_(geoel, 20, ielem);
+      }
+      for (int q = 0; q < 4; q++)
+        for (int k = 0; k < nd; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bq[k] * djaco;
+      double rho0 = rho_initial(c, xg, yg, xc, yc);
+      double rcoef = 1.0 - alfrz + alfrz * yg;
+      f0 = f0 + rho0 * djaco * rcoef;
+      for (int ix = 0; ix < nb; ix++)
+        for (int iy = 0; iy < nb; iy++)
+          mmatr[ix + nb * iy] = mmatr[ix + nb * iy] + rho0 * bq[ix + 1] * bq[iy + 1] * djaco * rcoef;
+    }
+    double *am = amatr + nmatr * ielem;
+    if (c->npoly == 1) {
+      double det = mmatr[0] * mmatr[3] - mmatr[2] * mmatr[2];
+      am[0] = mmatr[3] / det;
+      am[1] = -mmatr[2] / det;
+      am[2] = mmatr[0] / det;
+      am[3] = 1.0 / f0;
+      matri[0] = am[0]; matri[2] = am[1]; matri[1] = am[1]; matri[3] = am[2];
+    } else {
+      getinvmat(5, mmatr, matri);
+      int k = 0;
+      for (int im = 0; im < 5; im++)
+        for (int jm = im; jm < 5; jm++) am[k++] = matri[im + 5 * jm];
+      am[15] = 1.0 / f0;
+    }
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < nd; k++) U_(unkno, c, k, q, ielem) = 0.0;
+    for (int q = 0; q < 4; q++)
+      for (int ix = 0; ix < nb; ix++)
+        for (int iy = 0; iy < nb; iy++)
+          U_(unkno, c, ix + 1, q, ielem) = U_(unkno, c, ix + 1, q, ielem) + matri[ix + nb * iy] * rhsini[iy + 1][q];
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* getcellvol_lag, Limiterlag.f90:1869-2167 (quad loop :2038-2165)        */
+/* ---------------------------------------------------------------------- */
+void o_cellvol(const o_mesh *m, const o_cfg *c, double *geoel, const double *coord) {
+  (void)c;
+  double pos36[36][2], w36[36];
+  quad_rule(36, 0, pos36, w36);
+  const double alfrz = 0.0;
+  for (int ie = 0; ie < m->nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double xp[9][2], shp[9], dr[9], ds[9];
+    load_quad(m, coord, ie, xp);
+    double rcv = 0, scv = 0, volel = 0;
+    for (int ig = 0; ig < 36; ig++) {
+      double r = pos36[ig][0], s = pos36[ig][1], wi = w36[ig];
+      double a, b, cc, d, xg, yg;
+      shp9(r, s, shp, dr, ds);
+      jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+      map9((const double(*)[2])xp, shp, &xg, &yg);
+      double rcoef = 1.0 - alfrz + alfrz * yg;
+      double djaco = wi * (a * d - cc * b);
+      volel = volel + djaco * rcoef;
+      rcv = rcv + r * djaco * rcoef;
+      scv = scv + s * djaco * rcoef;
+    }
+    G_(geoel, 2, ielem) = volel;
+    G_(geoel, 4, ielem) = rcv / volel;
+    G_(geoel, 5, ielem) = scv / volel;
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Sub-cell normals for quads.                                            */
+/* gesgq(3,16,nquad): 1..8 corner points of the 4 outer faces,            */
+/* 9..12 inner sub-cell faces at the edge nodes, 13..16 outer faces at    */
+/* the edge nodes.                                                        */
+/* ---------------------------------------------------------------------- */
+static void normals_quad(const double (*xpq)[2], double (*gq)[3]) {
+  const double c10 = 1.0;
+  /* getfnds_lagsmsif_hybrid, Getrhslaggauss.f90:3537-3599 */
+  static const double posqc[4][2] = {{0.0, -0.5}, {0.5, 0.0}, {0.0, 0.5}, {-0.5, 0.0}};
+  static const int ipifq[4][3] = {{5, 9, 1}, {6, 9, 2}, {7, 9, 3}, {8, 9, 4}};
+  double xpqv[4][2], shp[9];
+  for (int isv = 0; isv < 4; isv++) {
+    shp9(posqc[isv][0], posqc[isv][1], shp, NULL, NULL);
+    map9(xpq, shp, &xpqv[isv][0], &xpqv[isv][1]);
+  }
+  for (int ifa = 0; ifa < 4; ifa++) {
+    double xpf[3][2];
+    for (int d = 0; d < 2; d++) {
+      xpf[0][d] = xpq[ipifq[ifa][0] - 1][d];
+      xpf[1][d] = xpq[ipifq[ifa][1] - 1][d];
+      xpf[2][d] = xpqv[ipifq[ifa][2] - 1][d];
+    }
+    double r = -1.0, dsh[3];
+    dsh[0] = -0.5 + r; dsh[1] = 0.5 + r; dsh[2] = -2.0 * r;
+    double dxdr = 0.0, dydr = 0.0;
+    for (int k = 0; k < 3; k++) { dxdr = dxdr + dsh[k] * xpf[k][0]; dydr = dydr + dsh[k] * xpf[k][1]; }
+    double djaco = sqrt(dxdr * dxdr + dydr * dydr);
+    double anx = -dydr, any = dxdr;
+    gq[8 + ifa][0] = anx / sqrt(anx * anx + any * any);
+    gq[8 + ifa][1] = any / sqrt(anx * anx + any * any);
+    gq[8 + ifa][2] = djaco * 2.0;
+  }
+  (void)c10;
+  /* getfnds_lagsms_simpsonhybrid, Getrhslaggauss.f90:9908-10010 */
+  static const double posiq[12][2] = {{-1, -1}, {1, -1}, {1, -1}, {1, 1}, {1, 1}, {-1, 1},
+                                      {-1, 1}, {-1, -1}, {0, -1}, {1, 0}, {0, 1}, {-1, 0}};
+  for (int ig = 0; ig < 12; ig++) {
+    double dr[9], ds[9], dxdr, dxds, dydr, dyds;
+    shp9(posiq[ig][0], posiq[ig][1], NULL, dr, ds);
+    jac9(xpq, dr, ds, &dxdr, &dxds, &dydr, &dyds);
+    double c11 = dyds, c12 = -dydr, c21 = -dxds, c22 = dxdr;
+    double vn0, vn1, larea = 2.0;
+    int g1 = ig + 1;
+    if (g1 == 1 || g1 == 2 || g1 == 9) { vn0 = 0.0; vn1 = -1.0; }
+    else if (g1 == 3 || g1 == 4 || g1 == 10) { vn0 = 1.0; vn1 = 0.0; }
+    else if (g1 == 5 || g1 == 6 || g1 == 11) { vn0 = 0.0; vn1 = 1.0; }
+    else { vn0 = -1.0; vn1 = 0.0; }
+    double anx = c11 * vn0 + c12 * vn1;
+    double any = c21 * vn0 + c22 * vn1;
+    double v0 = anx * larea, v1 = any * larea;
+    double farea = sqrt(v0 * v0 + v1 * v1);
+    int slot = (ig < 8) ? ig : ig + 4;  /* gelagq(9..12) -> gesgq(13..16) */
+    gq[slot][0] = anx * larea / farea;
+    gq[slot][1] = any * larea / farea;
+    gq[slot][2] = farea;
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Persson troubled-cell indicator: getSIHO_Persson,                      */
+/* Limiterlag.f90:12042-12239.                                            */
+/* ---------------------------------------------------------------------- */
+static void persson(const o_mesh *m, const o_cfg *c, const double *coord,
+                    double *geoel, const double *unkno) {
+  double pos[25][2], w[25];
+  quad_rule(25, 0, pos, w);
+  const double thr = -3.0 * log10(4.0) - 4.0;
+  for (int ie = 0; ie < m->nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double xp[9][2], dr[9], ds[9];
+    load_quad(m, coord, ie, xp);
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double unvar2[4] = {0, 0, 0, 0}, unvar1[4] = {0, 0, 0, 0};
+    for (int ig = 0; ig < 25; ig++) {
+      double r = pos[ig][0], s = pos[ig][1], wi = w[ig];
+      double a, b, cc, d, bq[6];
+      shp9(r, s, NULL, dr, ds);
+      jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+      double djaco = wi * (a * d - cc * b);
+      bq[0] = 1.0; bq[1] = (r - rc) / 1.0; bq[2] = (s - sc) / 1.0;
+      bq[3] = 0.5 * bq[1] * bq[1] - G_(geoel, 18, ielem);
+      bq[4] = 0.5 * bq[2] * bq[2] - G_(geoel, 19, ielem);
+      bq[5] = bq[1] * bq[2] - G_(geoel, 20, ielem);
+      double un[4] = {0, 0, 0, 0}, up1[4] = {0, 0, 0, 0};
+      for (int k = 0; k < c->ndegr; k++)
+        for (int q = 0; q < 4; q++) un[q] = un[q] + U_(unkno, c, k, q, ielem) * bq[k];
+      for (int k = 0; k < 3; k++)
+        for (int q = 0; q < 4; q++) up1[q] = up1[q] + U_(unkno, c, k, q, ielem) * bq[k];
+      for (int q = 0; q < 4; q++) {
+        unvar2[q] = unvar2[q] + (up1[q] - un[q]) * (up1[q] - un[q]) * djaco;
+        unvar1[q] = unvar1[q] + (un[q]) * (un[q]) * djaco;
+      }
+    }
+    G_(geoel, 9, ielem) = (log10(unvar2[0] / unvar1[0]) <= thr) ? 0.0 : 100.0;
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* WENO (WENO.f90:5927-8101)                                              */
+/* ---------------------------------------------------------------------- */
+typedef struct {
+  const o_mesh *m;
+  const o_cfg *c;
+  const double *coord, *coold, *geoel, *unknr;
+  double *geoph;  /* (2, nsize) */
+} weno_ctx;
+
+/* getvector_local, Limiterlag.f90:19009 */
+static void vec_local(const double *mp, double *dx, double *dy) {
+  double a11 = mp[0], a12 = mp[2], a21 = mp[1], a22 = mp[3];
+  double xl = *dx * a11 + *dy * a12;
+  double yl = *dx * a21 + *dy * a22;
+  *dx = xl; *dy = yl;
+}
+/* getvector_local2(1, ...), WENO.f90:5889 */
+static void vec_local_back(const double *mp, double *dx, double *dy) {
+  double a11 = mp[3], a12 = -mp[2], a21 = -mp[1], a22 = mp[0];
+  double xl = *dx * a11 + *dy * a12;
+  double yl = *dx * a21 + *dy * a22;
+  *dx = xl; *dy = yl;
+}
+
+/* basis_orthg with nbsis=1, WENO.f90:6683-6746 */
+static void basis_orthg1(const double *bt, const double *cf, double *bo) {
+  bo[0] = bt[0]; bo[1] = bt[1]; bo[2] = bt[2];
+  bo[3] = 0.5 * bt[1] * bt[1] - cf[0];
+  bo[4] = 0.5 * bt[2] * bt[2] - cf[1];
+  bo[5] = bt[1] * bt[2] - cf[2];
+}
+
+/* matrix_sym, LinearAlgebra.f90:89-127 (column-major a(ni,nj), rhs(nq,ni)) */
+static void matrix_sym(int ni, int nj, const double *a, const double *rhs,
+                       double *ms, double *rs) {
+  for (int i = 0; i < nj * nj; i++) ms[i] = 0.0;
+  for (int i = 0; i < 4 * nj; i++) rs[i] = 0.0;
+  for (int im = 0; im < nj; im++)
+    for (int jm = 0; jm < nj; jm++)
+      for (int km = 0; km < ni; km++)
+        ms[im + nj * jm] = ms[im + nj * jm] + a[km + ni * im] * a[km + ni * jm];
+  for (int iq = 0; iq < 4; iq++)
+    for (int im = 0; im < nj; im++)
+      for (int km = 0; km < ni; km++)
+        rs[iq + 4 * im] = rs[iq + 4 * im] + a[km + ni * im] * rhs[iq + 4 * km];
+}
+
+/* getmatrix_prj2, Limiterlag.f90:16455-16562 */
+static void matrix_prj2(double g, double *qmat, double *qinvm, double dnx, double dny,
+                        const double *ul, const double *ur) {
+  const double eps = 1.0e-6;
+  double rhom1 = ul[0], u1 = ul[1], v1 = ul[2], e1 = ul[3];
+  double rhoc1 = 1.0 / rhom1;
+  double rhom2 = ur[0], u2 = ur[1], v2 = ur[2], e2 = ur[3];
+  double rhoc2 = 1.0 / rhom2;
+  double rhof = sqrt(rhoc1 * rhoc2);
+  double rhosq = sqrt(rhoc1) + sqrt(rhoc2);
+  double uf = (sqrt(rhoc1) * u1 + sqrt(rhoc2) * u2) / rhosq;
+  double vf = (sqrt(rhoc1) * v1 + sqrt(rhoc2) * v2) / rhosq;
+  double h1 = fmax(eps, g * e1 - (g - 1.0) * 0.5 * (u1 * u1 + v1 * v1));
+  double h2 = fmax(eps, g * e2 - (g - 1.0) * 0.5 * (u2 * u2 + v2 * v2));
+  double hf = (sqrt(rhoc1) * h1 + sqrt(rhoc2) * h2) / rhosq;
+  double sdf = sqrt(fmax(eps, (g - 1.0) * (hf - 0.5 * (uf * uf + vf * vf))));
+  double rhosd = rhof * sdf;
+  double pf = sdf * sdf * rhof / g;
+  double gam1 = (g - 1.0) / g;
+  double vnm = vf * dnx - uf * dny;
+  /* column-major 4x4: q(i,j) = q[i + 4*j] */
+#define Q(a, i, j) a[(i - 1) + 4 * (j - 1)]
+  for (int i = 0; i < 16; i++) { qinvm[i] = 0.0; qmat[i] = 0.0; }
+  Q(qinvm, 1, 1) = -.5 / g;
+  Q(qinvm, 1, 2) = .5 * dnx / rhosd - 0.5 * uf / pf * gam1;
+  Q(qinvm, 1, 3) = .5 * dny / rhosd - 0.5 * vf / pf * gam1;
+  Q(qinvm, 1, 4) = .5 / pf * gam1;
+  Q(qinvm, 2, 1) = 1.0 / g;
+  Q(qinvm, 2, 2) = -dny * vnm / pf - uf / pf / g;
+  Q(qinvm, 2, 3) = dnx * vnm / pf - vf / pf / g;
+  Q(qinvm, 2, 4) = 1.0 / pf / g;
+  Q(qinvm, 3, 1) = 0.0;
+  Q(qinvm, 3, 2) = dny / pf;
+  Q(qinvm, 3, 3) = -dnx / pf;
+  Q(qinvm, 3, 4) = 0.0;
+  Q(qinvm, 4, 1) = .5 / g;
+  Q(qinvm, 4, 2) = .5 * dnx / rhosd + 0.5 * uf / pf * gam1;
+  Q(qinvm, 4, 3) = .5 * dny / rhosd + 0.5 * vf / pf * gam1;
+  Q(qinvm, 4, 4) = -.5 / pf * gam1;
+  double vedn = uf * dnx + vf * dny;
+  Q(qmat, 1, 1) = -1.0;
+  Q(qmat, 1, 2) = g - 1.0;
+  Q(qmat, 1, 3) = (g - 1.0) * vnm;
+  Q(qmat, 1, 4) = 1.0;
+  Q(qmat, 2, 1) = rhosd * dnx;
+  Q(qmat, 2, 2) = 0.0;
+  Q(qmat, 2, 3) = pf * dny;
+  Q(qmat, 2, 4) = rhosd * dnx;
+  Q(qmat, 3, 1) = rhosd * dny;
+  Q(qmat, 3, 2) = 0.0;
+  Q(qmat, 3, 3) = -pf * dnx;
+  Q(qmat, 3, 4) = rhosd * dny;
+  Q(qmat, 4, 1) = pf + rhosd * vedn;
+  Q(qmat, 4, 2) = pf;
+  Q(qmat, 4, 3) = 0.0;
+  Q(qmat, 4, 4) = -pf + rhosd * vedn;
+#undef Q
+}
+
+/* Per-point data of a stencil cell j: initial-config Jacobian weight,
+ * density and the local (rotated) physical position of the Gauss point. */
+static void weno_cell_points(const weno_ctx *w, int jelem, const double *mapmt,
+                             double *rhodj, double *xl, double *yl) {
+  const o_mesh *m = w->m;
+  double pos[25][2], wt[25];
+  quad_rule(25, 0, pos, wt);
+  int je = jelem - m->ntria;
+  double xpqi[9][2], xpql[9][2], shp[9], dr[9], ds[9];
+  load_quad(m, w->coold, je, xpqi);
+  load_quad(m, w->coord, je, xpql);
+  for (int k = 0; k < 9; k++) vec_local(mapmt, &xpql[k][0], &xpql[k][1]);
+  double rcj = G_(w->geoel, 0, jelem), scj = G_(w->geoel, 1, jelem);
+  double xcrho, ycrho;
+  cellctr_quad((const double(*)[2])xpqi, rcj, scj, &xcrho, &ycrho);
+  for (int ig = 0; ig < 25; ig++) {
+    double r = pos[ig][0], s = pos[ig][1], wi = wt[ig];
+    double a, b, cc, d, xgi, ygi, xg, yg;
+    shp9(r, s, shp, dr, ds);
+    jac9((const double(*)[2])xpqi, dr, ds, &a, &b, &cc, &d);
+    double djacoi = wi * (a * d - cc * b);
+    map9((const double(*)[2])xpqi, shp, &xgi, &ygi);
+    map9((const double(*)[2])xpql, shp, &xg, &yg);
+    double rhogi = rho_initial(w->c, xgi, ygi, xcrho, ycrho);
+    rhodj[ig] = rhogi * djacoi;
+    xl[ig] = xg; yl[ig] = yg;
+  }
+}
+
+/* weno_cell_Taylor (nbsis=1, npoly=2), WENO.f90:7219-7537 */
+static void weno_cell(const weno_ctx *w, int isten, int ielem, const double (*xpq)[2],
+                      const double *mapmt, const double *unksl /* (6,4,10) */,
+                      double *unk_phy /* (6,4) */) {
+  const o_mesh *m = w->m;
+  const int ncell = m->ntria + m->nquad;
+  const int ie = ielem - m->ntria;
+  const double epsil = 1.0e-6;
+  double volel = G_(w->geoel, 2, ielem);
+  double dxc = sqrt(volel), dyc = dxc;
+  static const int mapfe[4][2] = {{1, 2}, {2, 3}, {3, 4}, {4, 1}};
+  double unkf_phy[4][4][6];
+  memset(unkf_phy, 0, sizeof unkf_phy);
+  int ifprj = 0;
+#define SL(id, iq, is) unksl[(id) + 6 * ((iq) + 4 * (is))]
+  for (int ies = 0; ies < 4; ies++) {
+    int jelem = m->esqua[4 * ie + ies];
+    if (jelem > ncell) continue;
+    jelem -= 1;
+    double dtx = xpq[mapfe[ies][1] - 1][0] - xpq[mapfe[ies][0] - 1][0];
+    double dty = xpq[mapfe[ies][1] - 1][1] - xpq[mapfe[ies][0] - 1][1];
+    double dlgt = sqrt(dtx * dtx + dty * dty);
+    double dnx = dty / dlgt, dny = -dtx / dlgt;
+    vec_local(mapmt, &dnx, &dny);
+    double ul[4], ur[4];
+    for (int q = 0; q < 4; q++) { ul[q] = U_(w->unknr, w->c, 0, q, ielem); ur[q] = U_(w->unknr, w->c, 0, q, jelem); }
+    vec_local(mapmt, &ul[1], &ul[2]);
+    vec_local(mapmt, &ur[1], &ur[2]);
+    double qmat[16], qinvm[16];
+    matrix_prj2(w->c->gamlg, qmat, qinvm, dnx, dny, ul, ur);
+    double cha[10][4][6];
+    memset(cha, 0, sizeof cha);
+    for (int is = 0; is < isten; is++)
+      for (int iq = 0; iq < 4; iq++)
+        for (int id = 0; id < 6; id++)
+          for (int k = 0; k < 4; k++)
+            cha[is][k][id] = cha[is][k][id] + qinvm[k + 4 * iq] * SL(id, iq, is);
+    double os1[10];
+    for (int is = 0; is < isten; is++) {
+      double mx = 0.0;
+      for (int iq = 0; iq < 4; iq++) {
+        double t1 = cha[is][iq][1] / dxc, t2 = cha[is][iq][2] / dyc;
+        double os = t1 * t1 + t2 * t2;
+        if (iq == 0 || os > mx) mx = os;
+      }
+      os1[is] = mx;
+    }
+    double weigl[10];
+    weigl[0] = .2;
+    for (int is = 1; is < isten; is++) weigl[is] = 0.8 / (isten - 1.0);
+    double weigh[10][4], weigt[4] = {0, 0, 0, 0};
+    for (int is = 0; is < isten; is++)
+      for (int iq = 0; iq < 4; iq++) {
+        double t = epsil + os1[is];
+        weigh[is][iq] = weigl[is] / (t * t);
+      }
+    for (int iq = 0; iq < 4; iq++)
+      for (int is = 0; is < isten; is++) weigt[iq] = weigt[iq] + weigh[is][iq];
+    for (int is = 0; is < isten; is++)
+      for (int iq = 0; iq < 4; iq++) weigh[is][iq] = weigh[is][iq] / weigt[iq];
+    double fch[4][6];
+    memset(fch, 0, sizeof fch);
+    for (int is = 0; is < isten; is++)
+      for (int iq = 0; iq < 4; iq++)
+        for (int id = 0; id < 6; id++) fch[iq][id] = fch[iq][id] + weigh[is][iq] * cha[is][iq][id];
+    for (int iq = 0; iq < 4; iq++)
+      for (int id = 1; id < 6; id++)
+        for (int k = 0; k < 4; k++)
+          unkf_phy[ifprj][k][id] = unkf_phy[ifprj][k][id] + qmat[k + 4 * iq] * fch[iq][id];
+    ifprj++;
+  }
+#undef SL
+  double weigf = 1.0 / ifprj;
+  for (int i = 0; i < 24; i++) unk_phy[i] = 0.0;
+  for (int ifa = 0; ifa < ifprj; ifa++)
+    for (int iq = 0; iq < 4; iq++)
+      for (int id = 1; id < 6; id++)
+        unk_phy[id + 6 * iq] = unk_phy[id + 6 * iq] + weigf * unkf_phy[ifa][iq][id];
+}
+
+/* weno_stncl_quad_orthol3, WENO.f90:7541-8101 */
+static void weno_stencil(const weno_ctx *w, int ielem, const double *mapmt, double *unkno) {
+  const o_mesh *m = w->m;
+  const o_cfg *c = w->c;
+  const int ntria = m->ntria;
+  static const int ielst1[4][7] = {{1, 2, 5, 6, 9, 8, 3}, {1, 3, 2, 7, 6, 9, 5},
+                                   {1, 4, 3, 8, 7, 6, 5}, {1, 5, 4, 9, 8, 7, 3}};
+  static const int ielst2[4][5] = {{1, 2, 6, 9, 6}, {1, 3, 6, 7, 7},
+                                   {1, 4, 8, 7, 8}, {1, 5, 8, 9, 9}};
+  const int ie = ielem - ntria;
+  double xpq[9][2];
+  load_quad(m, w->coord, ie, xpq);
+  double dxcl = sqrt(G_(w->geoel, 2, ielem)), dycl = dxcl;
+  int ielaj[9];
+  ielaj[0] = ielem + 1;
+  /* the reference indexes esqua by the global id here (WENO.f90:7648) */
+  for (int k = 0; k < 4; k++) ielaj[1 + k] = m->esqua[4 * ielem + k];
+  for (int k = 5; k < 9; k++) ielaj[k] = 0;
+  int ipq[9];
+  for (int k = 0; k < 9; k++) ipq[k] = m->ipqua[9 * ie + k];
+  for (int iv = 0; iv < 4; iv++) {
+    int jelaj[5] = {0, 0, 0, 0, 0}, nvaj = 0;
+    int ip = ipq[iv];
+    for (int is = m->esuv2[ip - 1]; is < m->esuv2[ip]; is++) {
+      int je = m->esuv1[is];
+      if (je != ielem + 1) { if (nvaj < 5) jelaj[nvaj] = je; nvaj++; }
+    }
+    int idxod = 1, idxiv[3] = {0, 0, 0};
+    for (int a = 0; a < 3; a++)
+      for (int f = 0; f < 4; f++)
+        if (jelaj[a] == ielaj[f + 1]) { idxod *= (f + 1); idxiv[a] = 1; }
+    for (int a = 0; a < 3; a++)
+      if (idxiv[a] == 0) {
+        if (idxod == 2) ielaj[5] = jelaj[a];
+        else if (idxod == 6) ielaj[6] = jelaj[a];
+        else if (idxod == 12) ielaj[7] = jelaj[a];
+        else if (idxod == 4) ielaj[8] = jelaj[a];
+        else { g_status |= 2; return; } /* the reference stops here (WENO.f90:7699) */
+      }
+  }
+  for (int k = 0; k < 9; k++) if (ielaj[k] == 0) return;  /* boundary cell */
+  for (int k = 0; k < 9; k++) ielaj[k] -= 1;               /* 0-based */
+
+  /* local copies of the stencil DOFs in the rotated frame */
+  double unkrl[9][4][6];
+  for (int s = 0; s < 9; s++)
+    for (int q = 0; q < 4; q++)
+      for (int d = 0; d < 6; d++) unkrl[s][q][d] = U_(w->unknr, c, d, q, ielaj[s]);
+  for (int s = 0; s < 9; s++)
+    for (int d = 0; d < 6; d++) vec_local(mapmt, &unkrl[s][1][d], &unkrl[s][2][d]);
+
+  /* per-cell point data (initial-config weights, local positions) */
+  double rhodj[9][25], xl[9][25], yl[9][25];
+  for (int s = 0; s < 9; s++) weno_cell_points(w, ielaj[s], mapmt, rhodj[s], xl[s], yl[s]);
+
+  /* getgeophy_local_Taylor (nbsis=1), WENO.f90:6750-7001 */
+  double geopl[9][16];
+  memset(geopl, 0, sizeof geopl);
+  for (int s = 0; s < 9; s++) {
+    int jelem = ielaj[s];
+    double xclj = w->geoph[2 * jelem], yclj = w->geoph[2 * jelem + 1];
+    vec_local(mapmt, &xclj, &yclj);
+    geopl[s][0] = xclj; geopl[s][1] = yclj;
+    double dxclj = sqrt(G_(w->geoel, 2, jelem)), dyclj = dxclj;
+    double masel = G_(w->geoel, 3, jelem);
+    double v1 = 0, v2 = 0, v3 = 0;
+    for (int ig = 0; ig < 25; ig++) {
+      double b2 = (xl[s][ig] - xclj) / dxclj, b3 = (yl[s][ig] - yclj) / dyclj;
+      v1 = v1 + rhodj[s][ig] * b2 * b2;
+      v2 = v2 + rhodj[s][ig] * b3 * b3;
+      v3 = v3 + rhodj[s][ig] * b2 * b3;
+    }
+    v1 = v1 / masel; v2 = v2 / masel; v3 = v3 / masel;
+    geopl[s][2] = 0.5 * v1;
+    geopl[s][3] = 0.5 * v2;
+    geopl[s][4] = v3;
+  }
+
+  /* getunknp_local_Taylor, WENO.f90:7005-7215 */
+  double pos[25][2], wt[25];
+  quad_rule(25, 0, pos, wt);
+  double unkpl[9][4][6], mtbbq[25], mtbbi[25];
+  for (int s = 0; s < 9; s++) {
+    int jelem = ielaj[s];
+    double rcj = G_(w->geoel, 0, jelem), scj = G_(w->geoel, 1, jelem);
+    double xclj = geopl[s][0], yclj = geopl[s][1];
+    double dxclj = sqrt(G_(w->geoel, 2, jelem)), dyclj = dxclj;
+    double bb[25], bbq[25], bbi[25], bbqi[25];
+    for (int i = 0; i < 25; i++) { bb[i] = 0.0; bbq[i] = 0.0; }
+    for (int ig = 0; ig < 25; ig++) {
+      double r = pos[ig][0], s_ = pos[ig][1];
+      double bq[6], bqpl[3], bqol[6];
+      bq[0] = 1.0; bq[1] = (r - rcj) / 1.0; bq[2] = (s_ - scj) / 1.0;
+      bq[3] = 0.5 * bq[1] * bq[1] - G_(w->geoel, 18, jelem);
+      bq[4] = 0.5 * bq[2] * bq[2] - G_(w->geoel, 19, jelem);
+      bq[5] = bq[1] * bq[2] - G_(w->geoel, 20, jelem);
+      bqpl[0] = 1.0; bqpl[1] = (xl[s][ig] - xclj) / dxclj; bqpl[2] = (yl[s][ig] - yclj) / dyclj;
+      basis_orthg1(bqpl, &geopl[s][2], bqol);
+      for (int i = 1; i < 6; i++)
+        for (int j = 1; j < 6; j++) {
+          bb[(i - 1) + 5 * (j - 1)] = bb[(i - 1) + 5 * (j - 1)] + rhodj[s][ig] * bq[i] * bqol[j];
+          bbq[(i - 1) + 5 * (j - 1)] = bbq[(i - 1) + 5 * (j - 1)] + rhodj[s][ig] * bqol[i] * bqol[j];
+        }
+    }
+    double rhs[6][4];
+    memset(rhs, 0, sizeof rhs);
+    for (int i = 1; i < 6; i++)
+      for (int j = 1; j < 6; j++)
+        for (int q = 0; q < 4; q++) rhs[i][q] = rhs[i][q] + unkrl[s][q][j] * bb[(j - 1) + 5 * (i - 1)];
+    inv_small(5, bbq, bbqi);
+    inv_small(5, bb, bbi);
+    for (int q = 0; q < 4; q++) for (int d = 0; d < 6; d++) unkpl[s][q][d] = 0.0;
+    for (int i = 1; i < 6; i++)
+      for (int j = 1; j < 6; j++)
+        for (int q = 0; q < 4; q++) unkpl[s][q][i] = unkpl[s][q][i] + rhs[j][q] * bbqi[(j - 1) + 5 * (i - 1)];
+    if (s == 0) { memcpy(mtbbq, bbq, sizeof bbq); memcpy(mtbbi, bbi, sizeof bbi); }
+    for (int q = 0; q < 4; q++) unkpl[s][q][0] = unkrl[s][q][0];
+  }
+
+  /* candidate stencil polynomials unksl(6,4,10) */
+  double unksl[10 * 4 * 6];
+#define SL(id, iq, is) unksl[(id) + 6 * ((iq) + 4 * (is))]
+  memset(unksl, 0, sizeof unksl);
+  for (int is = 0; is < 10; is++) for (int q = 0; q < 4; q++) SL(0, q, is) = unkpl[0][q][0];
+  for (int d = 0; d < 6; d++) for (int q = 0; q < 4; q++) SL(d, q, 0) = unkpl[0][q][d];
+  int isten = 0;
+  const double xmcl = geopl[0][0], ymcl = geopl[0][1];
+  /* 4 Lagrangian stencils: 5 cell-average equations each (WENO.f90:7740-7838) */
+  for (int is = 0; is < 4; is++) {
+    isten++;
+    double matlg[25], rhslg[20], matin[25];
+    for (int i = 0; i < 25; i++) matlg[i] = 0.0;
+    for (int i = 0; i < 20; i++) rhslg[i] = 0.0;
+    for (int ies = 0; ies < 5; ies++) {
+      int sl = ielst1[is][ies + 1] - 1;
+      double masej = G_(w->geoel, 3, ielaj[sl]);
+      for (int ig = 0; ig < 25; ig++) {
+        double bqplj[3], bqolj[6];
+        bqplj[0] = 1.0; bqplj[1] = (xl[sl][ig] - xmcl) / dxcl; bqplj[2] = (yl[sl][ig] - ymcl) / dycl;
+        basis_orthg1(bqplj, &geopl[0][2], bqolj);
+        for (int k = 0; k < 5; k++)
+          matlg[ies + 5 * k] = matlg[ies + 5 * k] + rhodj[sl][ig] * bqolj[k + 1] / masej;
+      }
+      for (int q = 0; q < 4; q++) rhslg[q + 4 * ies] = unkpl[sl][q][0] - unkpl[0][q][0];
+    }
+    inv_small(5, matlg, matin);
+    for (int d = 1; d < 6; d++)
+      for (int ies = 0; ies < 5; ies++)
+        for (int q = 0; q < 4; q++) SL(d, q, isten) = SL(d, q, isten) + matin[(d - 1) + 5 * ies] * rhslg[q + 4 * ies];
+  }
+  /* 4 Hermite stencils: 3 averages + 6 derivative equations, least squares
+   * (WENO.f90:7843-7990) */
+  for (int is = 0; is < 4; is++) {
+    isten++;
+    double mathm[45], rhshm[36], matls[25], rhsls[20], matin[25];
+    for (int i = 0; i < 45; i++) mathm[i] = 0.0;
+    for (int i = 0; i < 36; i++) rhshm[i] = 0.0;
+    for (int ies = 0; ies < 3; ies++) {
+      int sl = ielst2[is][ies + 1] - 1;
+      int jelem = ielaj[sl];
+      double masej = G_(w->geoel, 3, jelem);
+      double dxclj = sqrt(G_(w->geoel, 2, jelem)), dyclj = dxclj;
+      double xclj = geopl[sl][0], yclj = geopl[sl][1];
+      for (int ig = 0; ig < 25; ig++) {
+        double bqplj[3], bqol[6], bqolj[6];
+        bqplj[0] = 1.0; bqplj[1] = (xl[sl][ig] - xmcl) / dxcl; bqplj[2] = (yl[sl][ig] - ymcl) / dycl;
+        basis_orthg1(bqplj, &geopl[0][2], bqol);
+        for (int k = 0; k < 5; k++)
+          mathm[ies + 9 * k] = mathm[ies + 9 * k] + rhodj[sl][ig] * bqol[k + 1] / masej;
+        bqplj[0] = 1.0; bqplj[1] = (xl[sl][ig] - xclj) / dxclj; bqplj[2] = (yl[sl][ig] - yclj) / dyclj;
+        basis_orthg1(bqplj, &geopl[sl][2], bqolj);
+        int ieshm = 3 + 2 * (ies + 1) - 1 - 1; /* 0-based row */
+        for (int d = 1; d < 6; d++) {
+          mathm[ieshm + 9 * (d - 1)] = mathm[ieshm + 9 * (d - 1)] + rhodj[sl][ig] * bqol[d] * bqolj[1] / masej;
+          mathm[ieshm + 1 + 9 * (d - 1)] = mathm[ieshm + 1 + 9 * (d - 1)] + rhodj[sl][ig] * bqol[d] * bqolj[2] / masej;
+        }
+        for (int d = 1; d < 6; d++)
+          for (int q = 0; q < 4; q++) {
+            rhshm[q + 4 * ieshm] = rhshm[q + 4 * ieshm] + rhodj[sl][ig] * bqolj[d] * bqolj[1] * unkpl[sl][q][d] / masej;
+            rhshm[q + 4 * (ieshm + 1)] = rhshm[q + 4 * (ieshm + 1)] + rhodj[sl][ig] * bqolj[d] * bqolj[2] * unkpl[sl][q][d] / masej;
+          }
+      }
+      for (int q = 0; q < 4; q++) rhshm[q + 4 * ies] = unkpl[sl][q][0] - unkpl[0][q][0];
+    }
+    matrix_sym(9, 5, mathm, rhshm, matls, rhsls);
+    inv_small(5, matls, matin);
+    for (int d = 1; d < 6; d++)
+      for (int ies = 0; ies < 5; ies++)
+        for (int q = 0; q < 4; q++) SL(d, q, isten) = SL(d, q, isten) + matin[(d - 1) + 5 * ies] * rhsls[q + 4 * ies];
+  }
+#undef SL
+  isten++;  /* number of stencils = 9 */
+  double unk_phy[24];
+  weno_cell(w, isten, ielem, (const double(*)[2])xpq, mapmt, unksl, unk_phy);
+
+  /* inverse L2 projection back to the Taylor basis of the target cell */
+  double rhsuk[5][4];
+  memset(rhsuk, 0, sizeof rhsuk);
+  for (int i = 1; i < 6; i++)
+    for (int j = 1; j < 6; j++)
+      for (int q = 0; q < 4; q++) rhsuk[i - 1][q] = rhsuk[i - 1][q] + unk_phy[j + 6 * q] * mtbbq[(j - 1) + 5 * (i - 1)];
+  double out[4][6];
+  for (int q = 0; q < 4; q++) for (int d = 1; d < 6; d++) out[q][d] = 0.0;
+  for (int i = 1; i < 6; i++)
+    for (int j = 1; j < 6; j++)
+      for (int q = 0; q < 4; q++) out[q][i] = out[q][i] + rhsuk[j - 1][q] * mtbbi[(j - 1) + 5 * (i - 1)];
+  for (int d = 1; d < 6; d++) vec_local_back(mapmt, &out[1][d], &out[2][d]);
+  for (int q = 0; q < 4; q++)
+    for (int d = 1; d < 6; d++) U_(unkno, c, d, q, ielem) = out[q][d];
+}
+
+/* weno_char_quad_orthgl, WENO.f90:5927-6123 */
+static void weno(const o_mesh *m, const o_cfg *c, double *unkno, const double *geoel,
+                 const double *coord, const double *coold) {
+  const int ncell = m->ntria + m->nquad, nsize = ncell + m->nbfac;
+  double pos[25][2], wt[25];
+  quad_rule(25, 0, pos, wt);
+  double *geoph = (double *)calloc(2 * (size_t)nsize, sizeof(double));
+  double *mapmt = (double *)calloc(4 * (size_t)nsize, sizeof(double));
+  for (int ie = 0; ie < m->nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double xp[9][2], xpi[9][2], shp[9], dr[9], ds[9];
+    load_quad(m, coord, ie, xp);
+    load_quad(m, coold, ie, xpi);
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double xcrho, ycrho;
+    cellctr_quad((const double(*)[2])xpi, rc, sc, &xcrho, &ycrho);
+    double masel = G_(geoel, 3, ielem);
+    double xmc = 0.0, ymc = 0.0;
+    for (int ig = 0; ig < 25; ig++) {
+      double r = pos[ig][0], s = pos[ig][1], wi = wt[ig];
+      double a, b, cc, d, xgi, ygi, xg, yg;
+      shp9(r, s, shp, dr, ds);
+      jac9((const double(*)[2])xpi, dr, ds, &a, &b, &cc, &d);
+      double djacoi = wi * (a * d - cc * b);
+      map9((const double(*)[2])xpi, shp, &xgi, &ygi);
+      map9((const double(*)[2])xp, shp, &xg, &yg);
+      double rhogi = rho_initial(c, xgi, ygi, xcrho, ycrho);
+      xmc = xmc + rhogi * djacoi * xg;
+      ymc = ymc + rhogi * djacoi * yg;
+    }
+    geoph[2 * ielem] = xmc / masel;
+    geoph[2 * ielem + 1] = ymc / masel;
+    double ma = U_(unkno, c, 0, 1, ielem), mb = U_(unkno, c, 0, 2, ielem);
+    double *mp = mapmt + 4 * ielem;  /* column-major 2x2 */
+    if (sqrt(ma * ma + mb * mb) > 1.0e-10) {
+      mp[0] = ma / sqrt(ma * ma + mb * mb);
+      mp[2] = mb / sqrt(ma * ma + mb * mb);
+      mp[1] = -mb / sqrt(ma * ma + mb * mb);
+      mp[3] = ma / sqrt(ma * ma + mb * mb);
+    } else {
+      mp[0] = mp[1] = mp[2] = mp[3] = 0.0;
+    }
+  }
+  size_t nu = (size_t)c->ndegr * c->nq * nsize;
+  double *unknr = (double *)malloc(nu * sizeof(double));
+  memcpy(unknr, unkno, nu * sizeof(double));
+  weno_ctx w = {m, c, coord, coold, geoel, unknr, geoph};
+  for (int ie = 0; ie < m->nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    if (G_(geoel, 9, ielem) < 10) continue;
+    weno_stencil(&w, ielem, mapmt + 4 * ielem, unkno);
+  }
+  free(unknr);
+  free(geoph);
+  free(mapmt);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Sub-cell densities for the quad corners.                               */
+/* ---------------------------------------------------------------------- */
+static const int IPQSG[4][4] = {{1, 5, 9, 8}, {5, 2, 6, 9}, {9, 6, 3, 7}, {8, 9, 7, 4}};
+
+/* getrhosubg_averg, Getrhslaggauss.f90:7067-7395: initial sub-cell mass
+ * over current sub-cell volume. */
+static void rhosubg_averg(const o_cfg *c, const double (*xpq)[2], const double (*xpqi)[2],
+                          double *unksgq) {
+  static const double posqc[12][2] = {{-0.5, -1.0}, {0.5, -1.0}, {1.0, -0.5}, {1.0, 0.5},
+                                      {0.5, 1.0}, {-0.5, 1.0}, {-1.0, 0.5}, {-1.0, -0.5},
+                                      {0.0, -0.5}, {0.5, 0.0}, {0.0, 0.5}, {-0.5, 0.0}};
+  static const int ipqsc[4][4] = {{1, 9, 12, 8}, {2, 3, 10, 9}, {10, 4, 5, 11}, {12, 11, 6, 7}};
+  double pos[25][2], wt[25];
+  quad_rule(25, 0, pos, wt);
+  double xpqc[12][2], xpqic[12][2], shp[9], dr[9], ds[9];
+  for (int isc = 0; isc < 12; isc++) {
+    shp9(posqc[isc][0], posqc[isc][1], shp, NULL, NULL);
+    map9(xpq, shp, &xpqc[isc][0], &xpqc[isc][1]);
+    map9(xpqi, shp, &xpqic[isc][0], &xpqic[isc][1]);
+  }
+  double matin[4];
+  for (int isg = 0; isg < 4; isg++) {
+    double xs[9][2];
+    for (int k = 0; k < 4; k++) {
+      xs[k][0] = xpq[IPQSG[isg][k] - 1][0]; xs[k][1] = xpq[IPQSG[isg][k] - 1][1];
+      xs[4 + k][0] = xpqc[ipqsc[isg][k] - 1][0]; xs[4 + k][1] = xpqc[ipqsc[isg][k] - 1][1];
+    }
+    for (int d = 0; d < 2; d++)
+      xs[8][d] = -0.25 * (xs[0][d] + xs[1][d] + xs[2][d] + xs[3][d]) + 0.5 * (xs[4][d] + xs[5][d] + xs[6][d] + xs[7][d]);
+    double f0 = 0.0;
+    for (int ig = 0; ig < 25; ig++) {
+      double a, b, cc, d;
+      shp9(pos[ig][0], pos[ig][1], NULL, dr, ds);
+      jac9((const double(*)[2])xs, dr, ds, &a, &b, &cc, &d);
+      f0 = f0 + wt[ig] * (a * d - cc * b);
+    }
+    matin[isg] = 1.0 / f0;
+  }
+  for (int isg = 0; isg < 4; isg++) {
+    double xs[9][2];
+    for (int k = 0; k < 4; k++) {
+      xs[k][0] = xpqi[IPQSG[isg][k] - 1][0]; xs[k][1] = xpqi[IPQSG[isg][k] - 1][1];
+      xs[4 + k][0] = xpqic[ipqsc[isg][k] - 1][0]; xs[4 + k][1] = xpqic[ipqsc[isg][k] - 1][1];
+    }
+    for (int d = 0; d < 2; d++)
+      xs[8][d] = -0.25 * (xs[0][d] + xs[1][d] + xs[2][d] + xs[3][d]) + 0.5 * (xs[4][d] + xs[5][d] + xs[6][d] + xs[7][d]);
+    double rhs = 0.0, xci, yci;
+    /* getrhoig_quadcurv2 (Getrhslag.f90:17761) evaluates the density at the
+     * parent's initial centre for the piecewise cases */
+    shp9(0.0, 0.0, shp, NULL, NULL);
+    map9(xpqi, shp, &xci, &yci);
+    for (int ig = 0; ig < 25; ig++) {
+      double a, b, cc, d;
+      shp9(pos[ig][0], pos[ig][1], NULL, dr, ds);
+      jac9((const double(*)[2])xs, dr, ds, &a, &b, &cc, &d);
+      double djaco = wt[ig] * (a * d - cc * b);
+      double rhoi = rho_initial(c, 0, 0, xci, yci);
+      rhs = rhs + rhoi * 1.0 * djaco;
+    }
+    unksgq[isg] = 0.0 + matin[isg] * rhs;
+  }
+}
+
+/* getrhosubg_daverg, Getrhslaggauss.f90:10949-11112: harmonic mean of the
+ * DG specific volume over each sub-cell (uqsgc = volume / integral of rho). */
+static void rhosubg_daverg(const o_cfg *c, double rc, double sc, const double *bqho,
+                           const double (*xpq)[2], const double *u1 /* unkno(:,1) */,
+                           double aflim1, double *uqsgc) {
+  double pos[25][2], wt[25], dr[9], ds[9];
+  quad_rule(25, 0, pos, wt);
+  double rhomc = u1[0];
+  for (int isg = 0; isg < 4; isg++) {
+    double masel = 0.0, volel = 0.0;
+    for (int ig = 0; ig < 25; ig++) {
+      double r, s;
+      if (isg == 0) { r = (pos[ig][0] - 1.0) / 2.0; s = (pos[ig][1] - 1.0) / 2.0; }
+      else if (isg == 1) { r = (pos[ig][0] + 1.0) / 2.0; s = (pos[ig][1] - 1.0) / 2.0; }
+      else if (isg == 2) { r = (pos[ig][0] + 1.0) / 2.0; s = (pos[ig][1] + 1.0) / 2.0; }
+      else { r = (pos[ig][0] - 1.0) / 2.0; s = (pos[ig][1] + 1.0) / 2.0; }
+      double b[6];
+      b[0] = 1.0; b[1] = (r - rc) / 1.0; b[2] = (s - sc) / 1.0;
+      b[3] = 0.5 * b[1] * b[1] - bqho[0];
+      b[4] = 0.5 * b[2] * b[2] - bqho[1];
+      b[5] = b[1] * b[2] - bqho[2];
+      double rhomsg = 0.0;
+      for (int k = 0; k < c->mdegr; k++) rhomsg = rhomsg + u1[k] * b[k];
+      if (c->nlimi == 6) rhomsg = rhomc + aflim1 * (rhomsg - rhomc);
+      double a, bb, cc, d;
+      shp9(r, s, NULL, dr, ds);
+      jac9(xpq, dr, ds, &a, &bb, &cc, &d);
+      double djaco = wt[ig] * (a * d - cc * bb) * 0.25;
+      masel = masel + 1.0 / rhomsg * djaco;
+      volel = volel + djaco;
+    }
+    uqsgc[isg] = volel / masel;
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Corner tables shared by the Riemann solver and the face integral.      */
+/* fnqsg: gesgq slot (sign = orientation) of face ifsg at sub-cell vertex */
+/* ivsg of sub-cell isg (Getrhslaggauss.f90:10486-10506).                 */
+/* ---------------------------------------------------------------------- */
+static const int FNQSG[4][8] = {{8, 1, 13, -9, -9, 12, 12, 16},
+                                {9, 13, 2, 3, 14, -10, -10, 9},
+                                {-11, 10, 10, 14, 4, 5, 15, -11},
+                                {16, -12, -12, 11, 11, 15, 6, 7}};
+
+static void corner_normals(const double (*gq)[3], int isg, double vn[4][2][3]) {
+  for (int ivsg = 0; ivsg < 4; ivsg++)
+    for (int f = 0; f < 2; f++) {
+      int code = FNQSG[isg][2 * ivsg + f];
+      int slot = abs(code) - 1;
+      double sg = (code >= 0) ? 1.0 : -1.0;
+      vn[ivsg][f][0] = sg * gq[slot][0];
+      vn[ivsg][f][1] = sg * gq[slot][1];
+      vn[ivsg][f][2] = gq[slot][2];
+    }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Riemann input per quad: getriem_quadsubg2, Getrhslaggauss.f90:10409.   */
+/* Accumulates node sums and records the per-corner coefficients.         */
+/* ---------------------------------------------------------------------- */
+typedef struct { double mn[2][2], mu[2], sn[2]; } corner_t;  /* per (ifa,ivsg,isg) */
+
+static void riem_quad(const o_mesh *m, const o_cfg *c, int ie, const double *geoel,
+                      const double (*gq)[3], const double *vlave, const double *unkno,
+                      const double *coord, const double *coold,
+                      double *munacn, double *munacu, double *snsigm, corner_t *cq) {
+  const int ielem = ie + m->ntria;
+  const double eps = 1.0e-6, g = c->gamlg;
+  const double slpdu = (g + 1.0) / 2.0;
+  static const double xvq[9] = {-1, 1, 1, -1, 0, 1, 0, -1, 0};
+  static const double yvq[9] = {-1, -1, 1, 1, -1, 0, 1, 0, 0};
+  double wfgsq[4][4][2];  /* [isg][ivsg][ifsg] */
+  {
+    /* second table of Getrhslaggauss.f90:10534-10552, then *0.25 */
+    const double t[4][4][2] = {
+        {{4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}, {1.0, 1.0}, {8.0 / 3.0, 4.0 / 3.0}},
+        {{8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}, {1.0, 1.0}},
+        {{1.0, 1.0}, {8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}},
+        {{4.0 / 3.0, 8.0 / 3.0}, {1.0, 1.0}, {8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}}};
+    for (int a = 0; a < 4; a++) for (int b = 0; b < 4; b++) for (int f = 0; f < 2; f++) wfgsq[a][b][f] = 0.25 * t[a][b][f];
+  }
+  int ipq[9];
+  for (int k = 0; k < 9; k++) ipq[k] = m->ipqua[9 * ie + k] - 1;
+  double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+  double bq[9][6];
+  for (int iv = 0; iv < 9; iv++) {
+    bq[iv][0] = 1.0;
+    bq[iv][1] = (xvq[iv] - rc) / 1.0;
+    bq[iv][2] = (yvq[iv] - sc) / 1.0;
+    bq[iv][3] = 0.5 * bq[iv][1] * bq[iv][1] - G_(geoel, 18, ielem);
+    bq[iv][4] = 0.5 * bq[iv][2] * bq[iv][2] - G_(geoel, 19, ielem);
+    bq[iv][5] = bq[iv][1] * bq[iv][2] - G_(geoel, 20, ielem);
+  }
+  double rhomc = U_(unkno, c, 0, 0, ielem);
+  double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+  double rhoct = 1.0 / rhomc;
+  double pctr = fmax(eps, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  double unknvq[9][4];
+  for (int iv = 0; iv < 9; iv++) {
+    for (int q = 0; q < 4; q++) unknvq[iv][q] = 0.0;
+    for (int k = 0; k < c->mdegr; k++)
+      for (int q = 0; q < 4; q++) unknvq[iv][q] = unknvq[iv][q] + U_(unkno, c, k, q, ielem) * bq[iv][k];
+  }
+  double xpq[9][2], xpqi[9][2];
+  load_quad(m, coord, ie, xpq);
+  load_quad(m, coold, ie, xpqi);
+  double unksgq[4], uqsgc[4];
+  rhosubg_averg(c, (const double(*)[2])xpq, (const double(*)[2])xpqi, unksgq);
+  double u1[6];
+  for (int k = 0; k < c->ndegr; k++) u1[k] = U_(unkno, c, k, 0, ielem);
+  rhosubg_daverg(c, rc, sc, &G_(geoel, 18, ielem), (const double(*)[2])xpq, u1, 1.0, uqsgc);
+
+  for (int isg = 0; isg < 4; isg++) {
+    double vn[4][2][3];
+    corner_normals(gq, isg, vn);
+    for (int ivsg = 0; ivsg < 4; ivsg++)
+      for (int f = 0; f < 2; f++) vn[ivsg][f][2] = vn[ivsg][f][2] * wfgsq[isg][ivsg][f];
+    double uv[4][2], sig[4], aujmp[4][3];
+    for (int ivsg = 0; ivsg < 4; ivsg++) {
+      int iv = IPQSG[isg][ivsg] - 1;
+      double rhovt = 1.0 / unknvq[iv][0];
+      double rhovsg = rhovt + c->cdrho * (unksgq[isg] - 1.0 / uqsgc[isg]);
+      double uvtx = unknvq[iv][1], vvtx = unknvq[iv][2], evtx = unknvq[iv][3];
+      double pvtx = fmax(eps, (g - 1.0) * rhovsg * (evtx - 0.5 * (uvtx * uvtx + vvtx * vvtx)));
+      uv[ivsg][0] = uvtx; uv[ivsg][1] = vvtx;
+      sig[ivsg] = -pvtx;
+      double ax = X_(vlave, 0, ipq[iv]) - uvtx;
+      double ay = X_(vlave, 1, ipq[iv]) - vvtx;
+      double acnx = ax, acny = ay;
+      if (sqrt(acnx * acnx + acny * acny) < (double)1.e-11f) {
+        ax = (double)1.e-11f; ay = (double)1.e-11f;
+      } else {
+        ax = ax / sqrt(acnx * acnx + acny * acny);
+        ay = ay / sqrt(acnx * acnx + acny * acny);
+      }
+      aujmp[ivsg][0] = ax; aujmp[ivsg][1] = ay;
+      aujmp[ivsg][2] = sqrt(acnx * acnx + acny * acny);
+    }
+    double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+    for (int ivsg = 0; ivsg < 4; ivsg++) aujmp[ivsg][2] = aujmp[ivsg][2] / sdctr;
+    double murie[4][2];
+    for (int ivsg = 0; ivsg < 4; ivsg++) {
+      int iv = IPQSG[isg][ivsg] - 1;
+      double dux = X_(vlave, 0, ipq[iv]) - uv[ivsg][0];
+      double duy = X_(vlave, 1, ipq[iv]) - uv[ivsg][1];
+      for (int f = 0; f < 2; f++) {
+        double deltu = fabs(dux * vn[ivsg][f][0] + duy * vn[ivsg][f][1]);
+        murie[ivsg][f] = rhoct * sdctr + c->cimpd * rhoct * slpdu * deltu;
+      }
+    }
+    for (int ivsg = 0; ivsg < 4; ivsg++) {
+      int iv = IPQSG[isg][ivsg] - 1, ip = ipq[iv];
+      for (int f = 0; f < 2; f++) {
+        /* getriecoef_matrixnew, Limiterlag.f90:1037-1076 */
+        double area = vn[ivsg][f][2], n0 = vn[ivsg][f][0], n1 = vn[ivsg][f][1];
+        double vnau = (aujmp[ivsg][2] < 1.0e12) ? 1.0 : n0 * aujmp[ivsg][0] + n1 * aujmp[ivsg][1];
+        corner_t k;
+        k.mn[0][0] = murie[ivsg][f] * area * fabs(vnau); k.mn[1][0] = 0.0;
+        k.mn[0][1] = 0.0; k.mn[1][1] = murie[ivsg][f] * area * fabs(vnau);
+        /* k.mn[i][j] holds munacn(i+1, j+1) */
+        k.mu[0] = k.mn[0][0] * uv[ivsg][0] + k.mn[1][0] * uv[ivsg][1];
+        k.mu[1] = k.mn[1][0] * uv[ivsg][0] + k.mn[1][1] * uv[ivsg][1];
+        k.sn[0] = sig[ivsg] * area * n0 + 0.0 * area * n1;
+        k.sn[1] = 0.0 * area * n0 + sig[ivsg] * area * n1;
+        munacn[0 + 4 * ip] = munacn[0 + 4 * ip] + k.mn[0][0];
+        munacn[1 + 4 * ip] = munacn[1 + 4 * ip] + k.mn[1][0];
+        munacn[2 + 4 * ip] = munacn[2 + 4 * ip] + k.mn[0][1];
+        munacn[3 + 4 * ip] = munacn[3 + 4 * ip] + k.mn[1][1];
+        munacu[0 + 2 * ip] = munacu[0 + 2 * ip] + k.mu[0];
+        munacu[1 + 2 * ip] = munacu[1 + 2 * ip] + k.mu[1];
+        snsigm[0 + 2 * ip] = snsigm[0 + 2 * ip] + k.sn[0];
+        snsigm[1 + 2 * ip] = snsigm[1 + 2 * ip] + k.sn[1];
+        cq[(f + 2 * (ivsg + 4 * isg))] = k;
+      }
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* getndvelo_lagsubg, Getrhslaggauss.f90:4348-4617                        */
+/* ---------------------------------------------------------------------- */
+static void ndvelo(const o_mesh *m, const o_cfg *c, const double *geoel, const double *gq,
+                   const double *coord, const double *coold, const double *unkno,
+                   double *ustar, double *fstarq /* (2,2,4,4,nquad) */) {
+  const int npoin = m->npoin;
+  char *indnd = (char *)calloc(npoin, 1);
+  for (int f = 0; f < m->nbfac; f++) {
+    const int *bf = m->bface + 5 * f;
+    if (c->ncase == 2 || bf[2] == 25) { indnd[bf[0] - 1] = 1; indnd[bf[1] - 1] = 1; indnd[bf[4] - 1] = 1; }
+  }
+  double *vlave = (double *)malloc(sizeof(double) * 2 * npoin);
+  memcpy(vlave, ustar, sizeof(double) * 2 * npoin);
+  double *munacn = (double *)calloc(4 * (size_t)npoin, sizeof(double));
+  double *munacu = (double *)calloc(2 * (size_t)npoin, sizeof(double));
+  double *snsigm = (double *)calloc(2 * (size_t)npoin, sizeof(double));
+  corner_t *cq = (corner_t *)malloc(sizeof(corner_t) * 32 * (size_t)m->nquad);
+  for (int ie = 0; ie < m->nquad; ie++)
+    riem_quad(m, c, ie, geoel, (const double(*)[3])(gq + 48 * (size_t)ie), vlave, unkno, coord, coold,
+              munacn, munacu, snsigm, cq + 32 * (size_t)ie);
+  for (int ip = 0; ip < npoin; ip++) {
+    if (indnd[ip]) continue;
+    const double *mn = munacn + 4 * ip;  /* (1,1),(2,1),(1,2),(2,2) */
+    double detma = mn[0] * mn[3] - mn[1] * mn[2];
+    double i11 = mn[3] / detma, i12 = -mn[2] / detma, i21 = -mn[1] / detma, i22 = mn[0] / detma;
+    double r1 = munacu[2 * ip] - snsigm[2 * ip];
+    double r2 = munacu[2 * ip + 1] - snsigm[2 * ip + 1];
+    ustar[2 * ip] = i11 * r1 + i12 * r2;
+    ustar[2 * ip + 1] = i21 * r1 + i22 * r2;
+  }
+  for (int f = 0; f < m->nbfac; f++) {
+    const int *bf = m->bface + 5 * f;
+    int nodes[3] = {bf[0] - 1, bf[1] - 1, bf[4] - 1};
+    if (bf[2] == 22) {
+      if (bf[3] == 221) for (int k = 0; k < 3; k++) ustar[2 * nodes[k] + 1] = 0.0;
+      else if (bf[3] == 222) for (int k = 0; k < 3; k++) ustar[2 * nodes[k]] = 0.0;
+    } else if (bf[2] == 25) {
+      for (int k = 0; k < 3; k++) { ustar[2 * nodes[k] + 1] = 0.0; ustar[2 * nodes[k]] = 0.0; }
+    }
+  }
+  for (int ie = 0; ie < m->nquad; ie++) {
+    for (int isg = 0; isg < 4; isg++)
+      for (int ivsg = 0; ivsg < 4; ivsg++) {
+        int ip = m->ipqua[9 * ie + IPQSG[isg][ivsg] - 1] - 1;
+        for (int f = 0; f < 2; f++) {
+          const corner_t *k = cq + 32 * (size_t)ie + (f + 2 * (ivsg + 4 * isg));
+          double *fs = fstarq + 2 * (f + 2 * (ivsg + 4 * (isg + 4 * (size_t)ie)));
+          fs[0] = k->sn[0] + k->mn[0][0] * ustar[2 * ip] + k->mn[1][0] * ustar[2 * ip + 1] - k->mu[0];
+          fs[1] = k->sn[1] + k->mn[0][1] * ustar[2 * ip] + k->mn[1][1] * ustar[2 * ip + 1] - k->mu[1];
+        }
+      }
+  }
+  free(indnd); free(vlave); free(munacn); free(munacu); free(snsigm); free(cq);
+}
+
+/* ---------------------------------------------------------------------- */
+/* rhsifacedg_lagsubgq2, Getrhslaggauss.f90:8501-8748                     */
+/* ---------------------------------------------------------------------- */
+static void iface_quad(const o_mesh *m, const o_cfg *c, int ie, const double *geoel,
+                       const double (*gq)[3], const double *ustar, const double *fstarq,
+                       double *rhsel) {
+  const int ielem = ie + m->ntria;
+  static const double xvq[9] = {-1, 1, 1, -1, 0, 1, 0, -1, 0};
+  static const double yvq[9] = {-1, -1, 1, 1, -1, 0, 1, 0, 0};
+  /* wfgsq (momentum, 0/1) and wfgsqm (mass) of Getrhslaggauss.f90:8580-8637 */
+  static const double wq[4][4] = {{1, 1, 0, 1}, {1, 1, 1, 0}, {0, 1, 1, 1}, {1, 0, 1, 1}};
+  double wm[4][4][2];
+  {
+    const double t[4][4][2] = {
+        {{4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 0.0}, {0.0, 0.0}, {0.0, 4.0 / 3.0}},
+        {{0.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 0.0 / 3.0}, {0.0, 0.0}},
+        {{0.0, 0.0}, {0.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 0.0 / 3.0}},
+        {{4.0 / 3.0, 0.0 / 3.0}, {0.0, 0.0}, {0.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}}};
+    for (int a = 0; a < 4; a++) for (int b = 0; b < 4; b++) for (int f = 0; f < 2; f++) wm[a][b][f] = 0.25 * t[a][b][f];
+  }
+  double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+  double bq[9][6];
+  const int nd = c->ndegr;
+  for (int iv = 0; iv < 9; iv++) {
+    bq[iv][0] = 1.0;
+    bq[iv][1] = (xvq[iv] - rc) / 1.0;
+    bq[iv][2] = (yvq[iv] - sc) / 1.0;
+    bq[iv][3] = 0.5 * bq[iv][1] * bq[iv][1] - G_(geoel, 18, ielem);
+    bq[iv][4] = 0.5 * bq[iv][2] * bq[iv][2] - G_(geoel, 19, ielem);
+    bq[iv][5] = bq[iv][1] * bq[iv][2] - G_(geoel, 20, ielem);
+  }
+  double ul[6] = {0}, p0[6] = {0}, p1[6] = {0}, el[6] = {0};
+  for (int isg = 0; isg < 4; isg++) {
+    double vn[4][2][3];
+    corner_normals(gq, isg, vn);
+    for (int ivsg = 0; ivsg < 4; ivsg++)
+      for (int f = 0; f < 2; f++) vn[ivsg][f][2] = vn[ivsg][f][2] * wm[isg][ivsg][f];
+    for (int ivsg = 0; ivsg < 4; ivsg++) {
+      int iv = IPQSG[isg][ivsg] - 1;
+      int ip = m->ipqua[9 * ie + iv] - 1;
+      double us0 = ustar[2 * ip], us1 = ustar[2 * ip + 1];
+      const double *fs = fstarq + 2 * (0 + 2 * (ivsg + 4 * (isg + 4 * (size_t)ie)));
+      /* fs[0..1] = fstarq(1:2, 1, ...), fs[2..3] = fstarq(1:2, 2, ...) */
+      double w1 = wq[isg][ivsg], w2 = wq[isg][ivsg];
+      for (int k = 0; k < nd; k++) {
+        double b = bq[iv][k];
+        ul[k] = ul[k] + us0 * vn[ivsg][0][0] * vn[ivsg][0][2] * b + us1 * vn[ivsg][0][1] * vn[ivsg][0][2] * b +
+                us0 * vn[ivsg][1][0] * vn[ivsg][1][2] * b + us1 * vn[ivsg][1][1] * vn[ivsg][1][2] * b;
+        p0[k] = p0[k] + fs[0] * b * w1 + fs[2] * b * w2;
+        p1[k] = p1[k] + fs[1] * b * w1 + fs[3] * b * w2;
+        el[k] = el[k] + us0 * fs[0] * b * w1 + us1 * fs[1] * b * w1 + us0 * fs[2] * b * w2 + us1 * fs[3] * b * w2;
+      }
+    }
+  }
+  for (int k = 0; k < nd; k++) {
+    U_(rhsel, c, k, 0, ielem) = ul[k];
+    U_(rhsel, c, k, 1, ielem) = p0[k];
+    U_(rhsel, c, k, 2, ielem) = p1[k];
+    U_(rhsel, c, k, 3, ielem) = el[k];
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* rhsdomndg_lagmc_curvquad, Getrhslag.f90:4716-5016 (5x5 Gauss-Lobatto,   */
+/* cofactor form, no Jacobian determinant).                               */
+/* ---------------------------------------------------------------------- */
+static void domn_quad(const o_mesh *m, const o_cfg *c, int ie, const double *geoel,
+                      const double *coord, const double *unkno, double *rhsel) {
+  const int ielem = ie + m->ntria;
+  const double eps = 1.0e-6, g = c->gamlg;
+  double pos[25][2], wt[25], dr[9], ds[9];
+  quad_rule(25, 1, pos, wt);
+  double xp[9][2];
+  load_quad(m, coord, ie, xp);
+  double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+  double dbdr[6] = {0.0, 1.0 / 1.0, 0.0, 0, 0, 0}, dbds[6] = {0.0, 0.0, 1.0 / 1.0, 0, 0, 0};
+  const int nd = c->ndegr;
+  for (int ig = 0; ig < 25; ig++) {
+    double r = pos[ig][0], s = pos[ig][1], wi = wt[ig];
+    double dxdr, dxds, dydr, dyds;
+    shp9(r, s, NULL, dr, ds);
+    jac9((const double(*)[2])xp, dr, ds, &dxdr, &dxds, &dydr, &dyds);
+    double djaco = wi;
+    if (c->npoly == 2) {
+      dbdr[3] = (r - rc) / (1.0 * 1.0); dbdr[4] = 0.0; dbdr[5] = (s - sc) / 1.0 / 1.0;
+      dbds[3] = 0.0; dbds[4] = (s - sc) / (1.0 * 1.0); dbds[5] = (r - rc) / 1.0 / 1.0;
+    }
+    double j11 = dyds, j12 = -dydr, j21 = -dxds, j22 = dxdr;
+    double gd[6][2];
+    for (int k = 0; k < nd; k++) {
+      gd[k][0] = j11 * dbdr[k] + j12 * dbds[k];
+      gd[k][1] = j21 * dbdr[k] + j22 * dbds[k];
+    }
+    double b[6];
+    b[0] = 1.0; b[1] = (r - rc) / 1.0; b[2] = (s - sc) / 1.0;
+    if (c->npoly == 2) {
+      b[3] = 0.5 * b[1] * b[1] - G_(geoel, 18, ielem);
+      b[4] = 0.5 * b[2] * b[2] - G_(geoel, 19, ielem);
+      b[5] = b[1] * b[2] - G_(geoel, 20, ielem);
+    }
+    double un[4] = {0, 0, 0, 0};
+    for (int k = 0; k < nd; k++)
+      for (int q = 0; q < 4; q++) un[q] = un[q] + U_(unkno, c, k, q, ielem) * b[k];
+    double rhoma = un[0], rhoad = 1.0 / rhoma;
+    double uadv = un[1], vadv = un[2], eadv = un[3];
+    double pres = fmax(eps, (g - 1.0) * rhoad * (eadv - 0.5 * (uadv * uadv + vadv * vadv)));
+    for (int k = 0; k < nd; k++) {
+      double f0 = gd[k][0] * uadv + gd[k][1] * vadv;
+      double f1 = gd[k][0] * (-pres);
+      double f2 = gd[k][1] * (-pres);
+      double f3 = (gd[k][0] * uadv + gd[k][1] * vadv) * (-pres);
+      U_(rhsel, c, k, 0, ielem) = U_(rhsel, c, k, 0, ielem) - f0 * djaco;
+      U_(rhsel, c, k, 1, ielem) = U_(rhsel, c, k, 1, ielem) - f1 * djaco;
+      U_(rhsel, c, k, 2, ielem) = U_(rhsel, c, k, 2, ielem) - f2 * djaco;
+      U_(rhsel, c, k, 3, ielem) = U_(rhsel, c, k, 3, ielem) - f3 * djaco;
+    }
+  }
+}
+
+/* rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:4070-4251 (TGV energy source) */
+static void src_quad(const o_mesh *m, const o_cfg *c, int ie, const double *geoel,
+                     const double *coord, double *rhsel) {
+  const int ielem = ie + m->ntria;
+  double pos[25][2], wt[25], shp[9], dr[9], ds[9];
+  quad_rule(25, 0, pos, wt);
+  double xp[9][2];
+  load_quad(m, coord, ie, xp);
+  double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+  for (int ig = 0; ig < 25; ig++) {
+    double r = pos[ig][0], s = pos[ig][1], wi = wt[ig];
+    double a, b_, cc, d, xg, yg;
+    shp9(r, s, shp, dr, ds);
+    jac9((const double(*)[2])xp, dr, ds, &a, &b_, &cc, &d);
+    double djaco = wi * (a * d - cc * b_);
+    map9((const double(*)[2])xp, shp, &xg, &yg);
+    double b[6];
+    b[0] = 1.0; b[1] = (r - rc) / 1.0; b[2] = (s - sc) / 1.0;
+    b[3] = 0.5 * b[1] * b[1] - G_(geoel, 18, ielem);
+    b[4] = 0.5 * b[2] * b[2] - G_(geoel, 19, ielem);
+    b[5] = b[1] * b[2] - G_(geoel, 20, ielem);
+    double src = 0.25 * PI_ * (cos(3.0 * PI_ * xg) * cos(PI_ * yg) - cos(3.0 * PI_ * yg) * cos(PI_ * xg)) / (c->gamlg - 1.0);
+    for (int k = 0; k < c->ndegr; k++) U_(rhsel, c, k, 3, ielem) = U_(rhsel, c, k, 3, ielem) + src * b[k] * djaco;
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* getrhsdg_lag_mcnew, curved branch (Getrhslagmc.f90:7556-7710)          */
+/* ---------------------------------------------------------------------- */
+void o_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
+           double *rhsel, double *geoel, const double *coord,
+           const double *coold, const double *amatr, int itime, int *flags) {
+  (void)amatr; (void)itime;
+  const int ncell = m->ntria + m->nquad, nsize = ncell + m->nbfac;
+  if (m->ntria > 0) { fprintf(stderr, "oracle: triangles not supported\n"); abort(); }
+  memset(rhsel, 0, sizeof(double) * c->ndegr * c->nq * ncell);
+  double *gq = (double *)malloc(sizeof(double) * 48 * (size_t)m->nquad);
+  for (int ie = 0; ie < m->nquad; ie++) {
+    double xp[9][2];
+    load_quad(m, coord, ie, xp);
+    normals_quad((const double(*)[2])xp, (double(*)[3])(gq + 48 * (size_t)ie));
+  }
+  if (c->npoly > 1) persson(m, c, coord, geoel, unkno);
+  if (flags) for (int ie = 0; ie < ncell; ie++) flags[ie] = G_(geoel, 9, ie) >= 10.0;
+  weno(m, c, unkno, geoel, coord, coold);
+  for (int ie = 0; ie < nsize; ie++) G_(geoel, 9, ie) = 0.0;
+  double *fstarq = (double *)malloc(sizeof(double) * 64 * (size_t)m->nquad);
+  ndvelo(m, c, geoel, gq, coord, coold, unkno, ustar, fstarq);
+  for (int ie = 0; ie < m->nquad; ie++)
+    iface_quad(m, c, ie, geoel, (const double(*)[3])(gq + 48 * (size_t)ie), ustar, fstarq, rhsel);
+  for (int ie = 0; ie < m->nquad; ie++) domn_quad(m, c, ie, geoel, coord, unkno, rhsel);
+  if (c->ncase == 1)
+    for (int ie = 0; ie < m->nquad; ie++) src_quad(m, c, ie, geoel, coord, rhsel);
+  if (c->nlimi == 6 && c->npoly >= 1) {
+    /* II.4.6 with aflim = 1 and afvec = I (Getrhslagmc.f90:7695-7708) */
+    for (int ie = 0; ie < ncell; ie++) {
+      U_(unkno, c, 1, 0, ie) = U_(unkno, c, 1, 0, ie) * 1.0;
+      U_(unkno, c, 2, 0, ie) = U_(unkno, c, 2, 0, ie) * 1.0;
+      double dudr = 1.0 * U_(unkno, c, 1, 1, ie) + 0.0 * U_(unkno, c, 1, 2, ie);
+      double duds = 1.0 * U_(unkno, c, 2, 1, ie) + 0.0 * U_(unkno, c, 2, 2, ie);
+      double dvdr = 0.0 * U_(unkno, c, 1, 1, ie) + 1.0 * U_(unkno, c, 1, 2, ie);
+      double dvds = 0.0 * U_(unkno, c, 2, 1, ie) + 1.0 * U_(unkno, c, 2, 2, ie);
+      U_(unkno, c, 1, 1, ie) = dudr; U_(unkno, c, 2, 1, ie) = duds;
+      U_(unkno, c, 1, 2, ie) = dvdr; U_(unkno, c, 2, 2, ie) = dvds;
+      U_(unkno, c, 1, 3, ie) = U_(unkno, c, 1, 3, ie) * 1.0;
+      U_(unkno, c, 2, 3, ie) = U_(unkno, c, 2, 3, ie) * 1.0;
+    }
+  }
+  free(gq);
+  free(fstarq);
+}
+
+/* ---------------------------------------------------------------------- */
+/* getdelt_lag, Getrhslag.f90:20600-20716                                 */
+/* ---------------------------------------------------------------------- */
+double o_delt(const o_mesh *m, const o_cfg *c, const double *unkno,
+              const double *geoel, const double *coord, const double *dvdt,
+              int itime, double dtfix) {
+  const double eps = 1.0e-6, g = c->gamlg;
+  double dtcfl = 1e10, dtvol = 1e10;
+  for (int ie = 0; ie < m->nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double xp[9][2];
+    load_quad(m, coord, ie, xp);
+    double dl[4];
+    static const int e[4][3] = {{0, 4, 1}, {1, 5, 2}, {2, 6, 3}, {3, 7, 0}};
+    for (int k = 0; k < 4; k++) {
+      const double *a = xp[e[k][0]], *b = xp[e[k][1]], *cc = xp[e[k][2]];
+      dl[k] = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1])) +
+              sqrt((b[0] - cc[0]) * (b[0] - cc[0]) + (b[1] - cc[1]) * (b[1] - cc[1]));
+    }
+    double rhomc = U_(unkno, c, 0, 0, ielem);
+    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+    double rhoct = 1.0 / rhomc;
+    double pctr = fmax(eps, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+    double dlen = dl[0];
+    for (int k = 1; k < 4; k++) if (dl[k] < dlen) dlen = dl[k];
+    dtcfl = fmin(dtcfl, dlen / sdctr);
+  }
+  for (int ie = 0; ie < m->nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    dtvol = fmin(dtvol, G_(geoel, 2, ielem) / fabs(dvdt[ielem]));
+  }
+  if (itime == 1) return fmin(c->cfl * dtcfl, 0.1 * dtvol);
+  return fmin(fmin(c->cfl * dtcfl, 0.1 * dtvol), 1.01 * dtfix);
+}
+
+/* ---------------------------------------------------------------------- */
+/* getsolvdg_lag, Getrhslag.f90:1553-2035                                 */
+/* ---------------------------------------------------------------------- */
+void o_step(const o_mesh *m, const o_cfg *c, const double *unkno, double *unold,
+            const double *coord, double *cooro, const double *coold,
+            double *geoel, const double *amatr, double *ustar, int itime,
+            double *dtfix, double *tacru) {
+  static const double rklag[2][3] = {{0.0, 0.5, 0.0}, {0.0, 0.75, 0.3333333333333333}};
+  const int ncell = m->ntria + m->nquad;
+  const int nd = c->ndegr, nq = c->nq;
+  const int nmatr = (c->npoly == 2) ? 16 : 4;
+  double *rhsel = (double *)malloc(sizeof(double) * nd * nq * (size_t)ncell);
+  double *dvdt = (double *)malloc(sizeof(double) * (size_t)ncell);
+  o_cellvol(m, c, geoel, coord);
+  for (int istag = 1; istag <= c->nstag; istag++) {
+    double alfa = rklag[c->nstag - 2][istag - 1];
+    o_rhs(m, c, ustar, unold, rhsel, geoel, cooro, coold, amatr, itime, NULL);
+    if (c->ndt == 1) {
+      if (istag == 1) {
+        for (int ie = 0; ie < ncell; ie++) dvdt[ie] = U_(rhsel, c, 0, 0, ie);
+        *dtfix = o_delt(m, c, unold, geoel, coord, dvdt, itime, *dtfix);
+        if ((*tacru + *dtfix) > c->tend) *dtfix = c->tend - *tacru;
+        *tacru = *tacru + *dtfix;
+      }
+    } else if (istag == 1) {
+      *tacru = *tacru + *dtfix;
+    }
+    for (size_t i = 0; i < (size_t)nd * nq * ncell; i++) rhsel[i] = *dtfix * rhsel[i];
+    for (int ie = 0; ie < ncell; ie++) {
+      double mm[6][6];
+      const double *am = amatr + nmatr * (size_t)ie;
+      memset(mm, 0, sizeof mm);
+      if (c->npoly == 2) {
+        mm[0][0] = am[15];
+        int k = 0;
+        for (int im = 1; im < nd; im++)
+          for (int jm = im; jm < nd; jm++) { mm[im][jm] = am[k]; mm[jm][im] = am[k]; k++; }
+      } else {
+        mm[0][0] = am[3];
+        mm[1][1] = am[0]; mm[1][2] = am[1]; mm[2][1] = am[1]; mm[2][2] = am[2];
+      }
+      for (int id = 0; id < nd; id++) {
+        double unint[4] = {0, 0, 0, 0};
+        for (int iu = 0; iu < nd; iu++)
+          for (int q = 0; q < nq; q++) unint[q] = unint[q] + mm[id][iu] * U_(rhsel, c, iu, q, ie);
+        for (int q = 0; q < nq; q++)
+          U_(unold, c, id, q, ie) = alfa * U_(unkno, c, id, q, ie) + (1.0 - alfa) * (U_(unold, c, id, q, ie) + unint[q]);
+      }
+    }
+    for (int ip = 0; ip < m->npoin; ip++)
+      for (int d = 0; d < 2; d++)
+        X_(cooro, d, ip) = alfa * X_(coord, d, ip) + (1.0 - alfa) * (X_(cooro, d, ip) + *dtfix * X_(ustar, d, ip));
+    for (int ie = 0; ie < m->nquad; ie++) {
+      const int *ipq = m->ipqua + 9 * ie;
+      for (int d = 0; d < 2; d++) {
+        double x[8];
+        for (int k = 0; k < 8; k++) x[k] = X_(cooro, d, ipq[k] - 1);
+        X_(cooro, d, ipq[8] - 1) = -0.25 * (x[0] + x[1] + x[2] + x[3]) + 0.5 * (x[4] + x[5] + x[6] + x[7]);
+      }
+    }
+    o_cellvol(m, c, geoel, cooro);
+  }
+  free(rhsel);
+  free(dvdt);
+}
+
+int o_run(const o_mesh *m, const o_cfg *c, double *unkno, double *coord,
+          const double *coold, double *geoel, const double *amatr,
+          double *ustar, int itime0, int nsteps, double *dtfix, double *tacru) {
+  const int ncell = m->ntria + m->nquad, nsize = ncell + m->nbfac;
+  size_t nu = (size_t)c->ndegr * c->nq * nsize;
+  double *unold = (double *)malloc(nu * sizeof(double));
+  double *cooro = (double *)malloc(sizeof(double) * 2 * (size_t)m->npoin);
+  memcpy(unold, unkno, nu * sizeof(double));
+  memcpy(cooro, coord, sizeof(double) * 2 * (size_t)m->npoin);
+  int done = 0;
+  for (int it = itime0; it < itime0 + nsteps; it++) {
+    o_step(m, c, unkno, unold, coord, cooro, coold, geoel, amatr, ustar, it, dtfix, tacru);
+    done++;
+    for (int ie = 0; ie < ncell; ie++)
+      for (int q = 0; q < c->nq; q++)
+        for (int k = 0; k < c->ndegr; k++) U_(unkno, c, k, q, ie) = U_(unold, c, k, q, ie);
+    memcpy(coord, cooro, sizeof(double) * 2 * (size_t)m->npoin);
+    if (fabs(*tacru - c->tend) / c->tend <= 1e-11) break;
+  }
+  free(unold);
+  free(cooro);
+  return done;
+}
+
+/* WENO on the cells whose flag is set (test entry point; the step derives
+ * the flags from the Persson indicator). */
+void o_weno(const o_mesh *m, const o_cfg *c, double *unkno, double *geoel,
+            const double *coord, const double *coold, const int *flags) {
+  const int ncell = m->ntria + m->nquad;
+  for (int ie = 0; ie < ncell; ie++) G_(geoel, 9, ie) = flags[ie] ? 100.0 : 0.0;
+  weno(m, c, unkno, geoel, coord, coold);
+  for (int ie = 0; ie < ncell; ie++) G_(geoel, 9, ie) = 0.0;
+}
