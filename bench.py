@@ -1,0 +1,283 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Lagrangian DG time step (Lag2D curved-P2 path).
+
+Metric: DOF-updates/s per RK stage, FP64 = N_cells * ndegr * nq * stages / time.
+Workload: Taylor-Green vortex on [0,1]^2, 1024 x 1024 curved-capable 9-node
+quads (1,048,576 cells, 4,198,401 nodes), P2 Taylor basis, gamma 5/3, RK3,
+Persson + WENO limiting, energy source on; synthetic initial state, no input
+files.  A "step" is one full time step (3 RK stages) on the device-resident
+state, replayed from a CUDA graph.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+For N > 1 launch under torch.distributed.run; every rank runs an independent
+replica (the path does not shard), timings are device events, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF-updates/s per RK stage, FP64 vs FP32-mixed; adjoint/forward time ratio"
+UNIT = "DOF-updates/s"
+WORKLOAD = "tgv1024"
+CPU_SAMPLE = "tgv64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def config_block(name, mesh, cfg, n):
+    return {"workload": name, "cells": mesh.ncell, "nodes": mesh.npoin, "basis": "P2 Taylor (ndegr=6, nq=4)",
+            "rk_stages": cfg.nstag, "limiter": "Persson + WENO", "gamma": cfg.gamlg, "cfl": cfg.cfl,
+            "parallelism": f"replicas x{n}", "l2": "working set > 126 MB L2 (no flush needed)"}
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the oracle (C restatement of the reference), single thread
+# --------------------------------------------------------------------------
+def _cpu_worker(args):
+    name, warm, nsteps = args
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from lag2d_b200.config import workload
+    from oracle.oracle import Oracle
+    m, c = workload(name)
+    o = Oracle(m, c)
+    geoel, amatr, unkno = o.init()
+    coord = m.coord.copy()
+    ustar = np.zeros_like(coord)
+    dt, ta = c.dtfix, 0.0
+    it = 1
+    if warm:
+        _, dt, ta = o.run(unkno, coord, m.coord, geoel, amatr, ustar, it, warm, dt, ta)
+        it += warm
+    times = []
+    for _ in range(nsteps):
+        t0 = time.perf_counter()
+        _, dt, ta = o.run(unkno, coord, m.coord, geoel, amatr, ustar, it, 1, dt, ta)
+        times.append(time.perf_counter() - t0)
+        it += 1
+    return m.ncell, c.nstag, times
+
+
+def cpu_baseline(seconds: float):
+    """Time the oracle on a bounded sample of the workload (single thread)."""
+    ncell, nstag, t = _cpu_worker((CPU_SAMPLE, 0, 1))
+    per_step = max(t[0], 1e-3)
+    nsteps = max(2, int(seconds / per_step))
+    ncell, nstag, times = _cpu_worker((CPU_SAMPLE, 0, nsteps))
+    total = sum(times)
+    value = ncell * 24 * nstag * nsteps / total
+    return {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{CPU_SAMPLE}: Taylor-Green 64x64 P2 quads (same step: Persson+WENO, RK3), "
+                      f"{nsteps} steps, {total:.1f} s, oracle C restatement -O2 single thread"}
+
+
+def run_reference(args):
+    rank, local_rank, world = dist_env()
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    from lag2d_b200.config import workload
+    m, c = workload(args.workload)
+    nproc = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_cpu_worker, [(CPU_SAMPLE, args.warmup, args.steps)] * nproc)
+    wall = time.perf_counter() - t0
+    ncell, nstag = res[0][0], res[0][1]
+    per_step_max = [max(ts) for ts in zip(*[r[2] for r in res])]
+    elapsed = sum(per_step_max)
+    value = nproc * ncell * 24 * nstag * args.steps / elapsed
+    sample = (f"{CPU_SAMPLE}: Taylor-Green 64x64 P2 quads per process, {nproc} processes x {args.steps} timed "
+              f"steps (after {args.warmup} warm-up), oracle C restatement of the reference step "
+              f"(the Fortran reference cannot be compiled here), wall {wall:.1f} s")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": config_block(args.workload, m, c, args.gpus),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = sorted(float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit())
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def run_ours(args):
+    rank, local_rank, world = dist_env()
+    import numpy as np
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from lag2d_b200.api import Lag2DSolver
+    from lag2d_b200.config import workload
+    from lag2d_b200.replicas import aggregate_rate, max_over_ranks
+    from lag2d_b200.roofline import kernel_bytes, stage_bytes
+
+    m, c = workload(args.workload)
+    s = Lag2DSolver(m, c)
+    s.init_fields()
+    st = torch.cuda.ExternalStream(s.stream_ptr)
+    dof_stage = m.ncell * c.ndegr * c.nq
+
+    s.run(args.warmup)
+    # ---- timed region: K steps from the captured graph, device events
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local_rank)
+    l0 = s.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    done = s.run(args.steps)
+    e1.record(st)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = s.kernel_launches - l0
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms_per_step = ms / max(done, 1)
+    value = aggregate_rate(dof_stage * c.nstag * done, ms / 1e3, world)
+
+    # ---- per-kernel device times (separate pass, events around each family)
+    s.timing(True)
+    s.run(2)
+    fams = {}
+    for f in ("persson", "weno", "corner", "node", "rhs", "dt", "update", "nodes", "geom", "copy"):
+        k_ms, n = s.kernel_ms(f)
+        if k_ms is not None:
+            fams[f] = {"ms_per_launch": k_ms, "launches": n}
+    s.timing(False)
+    per_step = {f: v["ms_per_launch"] * v["launches"] / 2 for f, v in fams.items()}
+    dom = max((f for f in per_step if f in ("corner", "node", "rhs", "update", "persson", "nodes", "geom")),
+              key=lambda f: per_step[f])
+    peak, peak_kind = peaks()
+    kb = kernel_bytes(dom, m.ncell, m.npoin)
+    achieved = kb / (fams[dom]["ms_per_launch"] / 1e3) / 1e9
+    sb = stage_bytes(m.ncell, m.npoin)
+    stage_gbs = sb / (ms_per_step / c.nstag / 1e3) / 1e9
+
+    # ---- end to end through the C-ABI with pinned host buffers
+    u_h = torch.empty((m.nsize, c.nq, c.ndegr), dtype=torch.float64, pin_memory=True)
+    x_h = torch.empty((m.npoin, 2), dtype=torch.float64, pin_memory=True)
+    us_h = torch.empty((m.npoin, 2), dtype=torch.float64, pin_memory=True)
+    s.get_state_ptrs(u_h.data_ptr(), x_h.data_ptr(), us_h.data_ptr())
+    h2d = 8 * (m.ncell * 24 + 4 * m.npoin)
+    d2h = h2d
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        s.set_state_ptrs(u_h.data_ptr(), x_h.data_ptr(), us_h.data_ptr())
+        s.step()
+        s.get_state_ptrs(u_h.data_ptr(), x_h.data_ptr(), us_h.data_ptr())
+    te = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": aggregate_rate(dof_stage * c.nstag * args.e2e_steps, te, world), "unit": UNIT,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "api": "lag2d_set_state + lag2d_step + lag2d_get_state (pinned host, Fortran layout)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seedless structured mesh, analytic IC)",
+                "config": config_block(args.workload, m, c, world), "clocks": clocks, "gpu_launches": launches,
+                "e2e": e2e,
+                "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                             "bytes_per_launch": kb},
+                "stage_roofline": {"bytes_per_stage": sb, "achieved_gbs": stage_gbs, "peak": peak,
+                                   "frac": stage_gbs / peak, "roofline_dof_updates_per_s": dof_stage / (sb / (peak * 1e9))},
+                "kernels_ms_per_step": per_step}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

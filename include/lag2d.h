@@ -115,6 +115,10 @@ int lag2d_weno(lag2d_handle *h, const int *flags);
  * geoel(24,nsize) with fields 3, 5, 6 refreshed if geoel is not NULL. */
 int lag2d_cellvol(lag2d_handle *h, double *geoel);
 
+/* The handle's CUDA stream (a cudaStream_t), for callers that time or
+ * order work against the library's launches. */
+void *lag2d_stream(const lag2d_handle *h);
+
 /* Number of this library's kernel launches since the handle was created. */
 long long lag2d_kernel_launches(const lag2d_handle *h);
 

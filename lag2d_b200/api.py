@@ -62,8 +62,8 @@ class _Cfg(ctypes.Structure):
 _libs = {}
 
 EXPORTS = ("lag2d_create", "lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run",
-           "lag2d_get_state", "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_kernel_launches",
-           "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error")
+           "lag2d_get_state", "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_stream",
+           "lag2d_kernel_launches", "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error")
 
 
 def library_path(exact: bool = False) -> str:
@@ -82,6 +82,8 @@ def load(exact: bool = False):
     lib.lag2d_last_error.restype = ctypes.c_char_p
     lib.lag2d_kernel_launches.restype = ctypes.c_longlong
     lib.lag2d_kernel_ms.restype = ctypes.c_double
+    lib.lag2d_stream.restype = ctypes.c_void_p
+    lib.lag2d_stream.argtypes = [ctypes.c_void_p]
     lib.lag2d_create.argtypes = [ctypes.POINTER(_Mesh), ctypes.POINTER(_Cfg), ctypes.POINTER(ctypes.c_void_p)]
     for name in ("lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run", "lag2d_get_state",
                  "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_timing"):
@@ -196,6 +198,20 @@ class Lag2DSolver:
         return geoel
 
     # -- instrumentation ---------------------------------------------------------
+    @property
+    def stream_ptr(self) -> int:
+        """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return int(self.lib.lag2d_stream(self.h))
+
+    def set_state_ptrs(self, unkno_ptr: int, coord_ptr: int, ustar_ptr: int):
+        """set_state from raw host pointers (e.g. pinned buffers); geoel/amatr kept."""
+        self._check(self.lib.lag2d_set_state(self.h, ctypes.c_void_p(unkno_ptr), ctypes.c_void_p(coord_ptr),
+                                             ctypes.c_void_p(ustar_ptr), None, None))
+
+    def get_state_ptrs(self, unkno_ptr: int, coord_ptr: int, ustar_ptr: int):
+        self._check(self.lib.lag2d_get_state(self.h, ctypes.c_void_p(unkno_ptr), ctypes.c_void_p(coord_ptr),
+                                             ctypes.c_void_p(ustar_ptr), None))
+
     @property
     def kernel_launches(self) -> int:
         return int(self.lib.lag2d_kernel_launches(self.h))

@@ -34,6 +34,10 @@ void launch_step_begin(const Dev &d, cudaStream_t st, int itime);
 void launch_step_end(const Dev &d, cudaStream_t st, int check);
 void launch_init(const Dev &d, cudaStream_t st);
 void launch_init_msub(const Dev &d, cudaStream_t st);
+void launch_unkno_in(const Dev &d, cudaStream_t st, const double *aos, int both);
+void launch_unkno_out(const Dev &d, cudaStream_t st, double *aos);
+void launch_xy_in(int n, cudaStream_t st, const double *xy, double *x, double *y, double *x2, double *y2);
+void launch_xy_out(int n, cudaStream_t st, double *xy, const double *x, const double *y);
 }  // namespace lag2d
 
 using namespace lag2d;
@@ -63,6 +67,8 @@ struct lag2d_handle {
   cudaStream_t st = nullptr;
   std::vector<void *> allocs;
   int *flags_dev = nullptr;
+  double *stage_u = nullptr;   // staging for unkno(ndegr,nq,ncell) in the caller's layout
+  double *stage_x = nullptr;   // staging for coord / ustar (2,npoin)
   cudaGraphExec_t graph = nullptr;
   long long launches = 0;
   bool timing = false;
@@ -334,6 +340,7 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   A(&d.flag, ncell); A(&d.geoph, 2 * (size_t)ncell); A(&d.mapmt, 4 * (size_t)ncell);
   A(&d.Uw, 20 * (size_t)nq); A(&d.wlist, nq); A(&d.wcount, 1);
   A(&d.dtpart, 2 * (size_t)dt_blocks(d) + 2); A(&d.sc_dev, 1); A(&h->flags_dev, ncell);
+  A(&h->stage_u, NU * (size_t)ncell); A(&h->stage_x, 2 * (size_t)np);
   if (rc != LAG2D_OK) { lag2d_destroy(h); return rc; }
   d.ipq = ipq_d; d.esq = esq_d; d.stencil = sten_d; d.node_ptr = ptr_d; d.node_cf = ncf_d;
   d.bcmask = mask_d; d.x0 = x0; d.y0 = y0;
@@ -376,26 +383,24 @@ static int download_geoel(lag2d_handle *h, double *geoel) {
   return LAG2D_OK;
 }
 
-static int download_unkno(lag2d_handle *h, const double *U, double *unkno) {
+// unkno(ndegr,nq,nsize): the ncell real cells are copied, ghosts are zeroed
+static int download_unkno(lag2d_handle *h, double *unkno) {
   const Dev &d = h->d;
-  const int ncell = d.ncell, nsize = ncell + d.nbfac;
-  std::vector<double> f(NU * (size_t)ncell);
-  CK(cudaMemcpyAsync(f.data(), U, f.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  const size_t nu = NU * (size_t)d.ncell;
+  launch_unkno_out(d, h->st, h->stage_u);
+  h->launches += 1;
+  CK(cudaMemcpyAsync(unkno, h->stage_u, nu * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
-  std::fill(unkno, unkno + NU * (size_t)nsize, 0.0);
-  for (int e = 0; e < ncell; e++)
-    for (int q = 0; q < NQ; q++)
-      for (int k = 0; k < NDEG; k++) unkno[(size_t)e * NU + q * NDEG + k] = f[(q * NDEG + k) * (size_t)ncell + e];
+  std::fill(unkno + nu, unkno + NU * (size_t)(d.ncell + d.nbfac), 0.0);
   return LAG2D_OK;
 }
 
 static int download_xy(lag2d_handle *h, const double *X, const double *Y, double *xy) {
   const int np = h->d.npoin;
-  std::vector<double> a(np), b(np);
-  CK(cudaMemcpyAsync(a.data(), X, np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
-  CK(cudaMemcpyAsync(b.data(), Y, np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  launch_xy_out(np, h->st, h->stage_x, X, Y);
+  h->launches += 1;
+  CK(cudaMemcpyAsync(xy, h->stage_x, 2 * (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
-  for (int p = 0; p < np; p++) { xy[2 * (size_t)p] = a[p]; xy[2 * (size_t)p + 1] = b[p]; }
   return LAG2D_OK;
 }
 
@@ -422,7 +427,7 @@ int lag2d_init_fields(lag2d_handle *h, double *geoel, double *amatr, double *unk
     for (int e = 0; e < ncell; e++)
       for (int k = 0; k < 16; k++) amatr[16 * (size_t)e + k] = f[k * (size_t)ncell + e];
   }
-  if (unkno) { int r = download_unkno(h, d.Un, unkno); if (r) return r; }
+  if (unkno) { int r = download_unkno(h, unkno); if (r) return r; }
   return LAG2D_OK;
 }
 
@@ -431,24 +436,16 @@ int lag2d_set_state(lag2d_handle *h, const double *unkno, const double *coord, c
   if (!h || !unkno || !coord || !ustar) return fail(LAG2D_EINVAL, "null argument");
   Dev &d = h->d;
   const int ncell = d.ncell, np = d.npoin;
-  std::vector<double> f(NU * (size_t)ncell);
-  for (int e = 0; e < ncell; e++)
-    for (int q = 0; q < NQ; q++)
-      for (int k = 0; k < NDEG; k++) f[(q * NDEG + k) * (size_t)ncell + e] = unkno[(size_t)e * NU + q * NDEG + k];
-  CK(cudaMemcpyAsync(d.Un, f.data(), f.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(d.Us, f.data(), f.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  // straight copies of the caller's buffers (pinned buffers go at full link
+  // speed), then layout conversion on the device
+  CK(cudaMemcpyAsync(h->stage_u, unkno, NU * (size_t)ncell * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  launch_unkno_in(d, h->st, h->stage_u, 1);
+  CK(cudaMemcpyAsync(h->stage_x, coord, 2 * (size_t)np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  launch_xy_in(np, h->st, h->stage_x, d.xn, d.yn, d.xs, d.ys);
   CK(cudaStreamSynchronize(h->st));
-  std::vector<double> a(np), b(np);
-  for (int p = 0; p < np; p++) { a[p] = coord[2 * (size_t)p]; b[p] = coord[2 * (size_t)p + 1]; }
-  CK(cudaMemcpyAsync(d.xn, a.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(d.yn, b.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(d.xs, a.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(d.ys, b.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  CK(cudaStreamSynchronize(h->st));
-  for (int p = 0; p < np; p++) { a[p] = ustar[2 * (size_t)p]; b[p] = ustar[2 * (size_t)p + 1]; }
-  CK(cudaMemcpyAsync(d.us, a.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(d.vs, b.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  CK(cudaStreamSynchronize(h->st));
+  CK(cudaMemcpyAsync(h->stage_x, ustar, 2 * (size_t)np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  launch_xy_in(np, h->st, h->stage_x, d.us, d.vs, nullptr, nullptr);
+  h->launches += 3;
   if (geoel) {
     std::vector<double> g(ncell);
     double *dst[7] = {d.rc, d.sc, d.vol, d.mass, d.g19, d.g20, d.g21};
@@ -545,7 +542,7 @@ int lag2d_run(lag2d_handle *h, int itime0, int nsteps, double *dtfix, double *ta
 int lag2d_get_state(lag2d_handle *h, double *unkno, double *coord, double *ustar, double *geoel) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
   int r;
-  if (unkno && (r = download_unkno(h, h->d.Un, unkno))) return r;
+  if (unkno && (r = download_unkno(h, unkno))) return r;
   if (coord && (r = download_xy(h, h->d.xn, h->d.yn, coord))) return r;
   if (ustar && (r = download_xy(h, h->d.us, h->d.vs, ustar))) return r;
   if (geoel && (r = download_geoel(h, geoel))) return r;
@@ -612,6 +609,8 @@ int lag2d_cellvol(lag2d_handle *h, double *geoel) {
 }
 
 long long lag2d_kernel_launches(const lag2d_handle *h) { return h ? h->launches : -1; }
+
+void *lag2d_stream(const lag2d_handle *h) { return h ? (void *)h->st : nullptr; }
 
 int lag2d_timing(lag2d_handle *h, int enable) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");

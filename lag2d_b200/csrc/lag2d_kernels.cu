@@ -1514,6 +1514,51 @@ __host__ __device__ void b_init_fields(const Dev &d, int iq) {
 __global__ void k_init_fields(Dev d) { b_init_fields(d, blockIdx.x * blockDim.x + threadIdx.x); }
 
 // ---------------------------------------------------------------------------
+// Boundary layout conversion: the caller's Fortran arrays unkno(ndegr,nq,nsize)
+// and coord/ustar(2,npoin) <-> the device structure of arrays.
+// ---------------------------------------------------------------------------
+__global__ void k_unkno_in(Dev d, const double *aos, int to_both) {
+  const size_t n = (size_t)NU * d.ncell;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = t / NU;
+    const int qk = (int)(t % NU);  // q*6 + k, coalesced read of the caller's layout
+    const double v = aos[t];
+    d.Un[qk * (size_t)d.ncell + e] = v;
+    if (to_both) d.Us[qk * (size_t)d.ncell + e] = v;
+  }
+}
+__global__ void k_unkno_out(Dev d, double *aos) {
+  const size_t n = (size_t)NU * d.ncell;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = t / NU;
+    const int qk = (int)(t % NU);
+    aos[t] = d.Un[qk * (size_t)d.ncell + e];
+  }
+}
+__global__ void k_xy_in(int n, const double *xy, double *x, double *y, double *x2, double *y2) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const double2 v = reinterpret_cast<const double2 *>(xy)[p];
+    x[p] = v.x;
+    y[p] = v.y;
+    if (x2) { x2[p] = v.x; y2[p] = v.y; }
+  }
+}
+__global__ void k_xy_out(int n, double *xy, const double *x, const double *y) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    reinterpret_cast<double2 *>(xy)[p] = make_double2(x[p], y[p]);
+}
+void launch_unkno_in(const Dev &d, cudaStream_t st, const double *aos, int both) {
+  k_unkno_in<<<2368, 256, 0, st>>>(d, aos, both);
+}
+void launch_unkno_out(const Dev &d, cudaStream_t st, double *aos) { k_unkno_out<<<2368, 256, 0, st>>>(d, aos); }
+void launch_xy_in(int n, cudaStream_t st, const double *xy, double *x, double *y, double *x2, double *y2) {
+  k_xy_in<<<1184, 256, 0, st>>>(n, xy, x, y, x2, y2);
+}
+void launch_xy_out(int n, cudaStream_t st, double *xy, const double *x, const double *y) {
+  k_xy_out<<<1184, 256, 0, st>>>(n, xy, x, y);
+}
+
+// ---------------------------------------------------------------------------
 // Host-side launchers
 // ---------------------------------------------------------------------------
 void set_tables(const QuadTables &q, cudaStream_t st) {

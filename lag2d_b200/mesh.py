@@ -194,7 +194,7 @@ def write_domn(m: Mesh, path: str) -> None:
             f.write(f"{i + 1} " + " ".join(str(int(v)) for v in row) + "\n")
         f.write(" coordinates\n")
         for i, (x, y) in enumerate(m.coord):
-            f.write(f"{i + 1} {x!r} {y!r}\n")
+            f.write(f"{i + 1} {float(x)!r} {float(y)!r}\n")
         f.write(" unknowns\n")
         for i in range(m.npoin):
             f.write(f"{i + 1} 0.0 0.0 0.0 0.0\n")
@@ -245,10 +245,9 @@ def build_esqua(ipqua: np.ndarray, iptri: np.ndarray, bface: np.ndarray) -> np.n
     sk = flat[order]
     esqua = np.zeros((nquad, 4), dtype=np.int32)
     same = np.nonzero(sk[1:] == sk[:-1])[0]
-    for i in same:
-        f1, f2 = order[i], order[i + 1]
-        esqua[f1 // 4, f1 % 4] = f2 // 4 + ntria + 1
-        esqua[f2 // 4, f2 % 4] = f1 // 4 + ntria + 1
+    f1, f2 = order[same], order[same + 1]
+    esqua[f1 // 4, f1 % 4] = f2 // 4 + ntria + 1
+    esqua[f2 // 4, f2 % 4] = f1 // 4 + ntria + 1
     if ntria:
         for q in range(nquad):
             for k in range(4):
@@ -260,7 +259,8 @@ def build_esqua(ipqua: np.ndarray, iptri: np.ndarray, bface: np.ndarray) -> np.n
     for i, row in enumerate(bface):
         x, y = int(row[0]), int(row[1])
         bkey[(min(x, y), max(x, y))] = i + 1
-    for q, k in zip(*np.nonzero(esqua == 0)):
+    qs, ks = np.nonzero(esqua == 0)
+    for q, k in zip(qs.tolist(), ks.tolist()):
         key = (int(lo[q, k]), int(hi[q, k]))
         esqua[q, k] = ncell + bkey[key] if key in bkey else 0
     return esqua

@@ -1,0 +1,48 @@
+"""Regenerates the oracle fixtures in this folder.
+
+The reference (Fortran) cannot be compiled in this environment and ships no
+golden outputs, so these fixtures pin the CPU oracle against regressions and
+give the GPU path fixed targets: small Taylor-Green and Sedov runs (8 x 8 and
+a 12 x 12 Sedov with troubled cells), 3 time steps each.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from lag2d_b200 import quad_mesh, StepConfig  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+
+CASES = {
+    "tgv8": (lambda: quad_mesh(8, 8, 0.0, 1.0, 0.0, 1.0),
+             StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=3, cfl=0.1, tend=10.0), 3),
+    "sedov12": (lambda: quad_mesh(12, 12, -1.2, 1.2, -1.2, 1.2),
+                StepConfig(ncase=7, gamlg=1.4, nstag=3, cfl=0.1, tend=1.0, sedov_cells=(66, 67, 78, 79)), 3),
+    "tgv6_curved": (lambda: quad_mesh(6, 6, 0.0, 1.0, 0.0, 1.0, jitter=0.1, curve=0.05, seed=7),
+                    StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=2, cfl=0.1, tend=10.0), 3),
+}
+
+
+def run_case(name):
+    mk, cfg, nsteps = CASES[name]
+    m = mk()
+    o = Oracle(m, cfg)
+    geoel, amatr, unkno = o.init()
+    u0, g0 = unkno.copy(), geoel.copy()
+    coord = m.coord.copy()
+    ustar = np.zeros_like(coord)
+    _, dt, ta = o.run(unkno, coord, m.coord, geoel, amatr, ustar, 1, nsteps, cfg.dtfix, 0.0)
+    return dict(unkno0=u0, geoel0=g0, geoel=geoel, amatr=amatr, unkno=unkno, coord=coord, ustar=ustar,
+                dtfix=np.float64(dt), tacru=np.float64(ta), nsteps=np.int64(nsteps))
+
+
+if __name__ == "__main__":
+    for name in CASES:
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **run_case(name))
+        print("wrote", name)

@@ -1,0 +1,62 @@
+"""CPU checks of the C-ABI library: it loads, exports every entry point that
+include/lag2d.h declares, and validates arguments before touching a device."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from lag2d_b200 import api, workload
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "lag2d.h")).read()
+    return sorted(set(re.findall(r"\b(lag2d_[a-z_]+)\s*\(", txt)))
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_library_exports_header_symbols(exact):
+    lib = ctypes.CDLL(api.library_path(exact))
+    names = _declared()
+    assert "lag2d_step" in names and "lag2d_create" in names
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(api.EXPORTS) <= set(names)
+
+
+def test_create_validates_arguments_without_device():
+    lib = api.load()
+    h = ctypes.c_void_p()
+    rc = lib.lag2d_create(None, None, ctypes.byref(h))
+    assert rc == 1 and b"null" in lib.lag2d_last_error()
+    m, c = workload("tgv16")
+    s = object.__new__(api.Lag2DSolver)
+    # a mesh with an out-of-range node id is rejected before any CUDA call
+    bad = m.ipqua.copy()
+    bad[0, 0] = m.npoin + 5
+    k = [np.ascontiguousarray(a, dtype=np.int32) for a in (m.iptri, bad, m.bface, m.esuv1, m.esuv2, m.esqua)]
+    coold = np.ascontiguousarray(m.coord)
+    mm = api._Mesh(m.ntria, m.nquad, m.npoin, m.nbfac, *[api._p(a, api._ip) for a in k], api._p(coold, api._dp))
+    cc = api._Cfg(c.npoly, c.ndegr, c.mdegr, c.nq, c.nstag, c.ndt, c.ncase, c.nlimi, c.ndens, c.ngausd,
+                  c.ngausd_geo, 0, 0, (ctypes.c_int * 4)(), c.gamlg, c.cfl, c.cdrho, c.cimpd, c.tend,
+                  c.sedov_energy)
+    assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
+    # unsupported configurations are reported as such
+    cc.precision = 1
+    k[1] = np.ascontiguousarray(m.ipqua, dtype=np.int32)
+    mm.ipqua = api._p(k[1], api._ip)
+    assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 3
+    cc.precision = 0
+    cc.nstag = 4
+    assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
+    del s
+
+
+def test_missing_library_fails_loudly(tmp_path, monkeypatch):
+    monkeypatch.setattr(api, "_LIBDIR", str(tmp_path))
+    monkeypatch.setattr(api, "_libs", {})
+    with pytest.raises(FileNotFoundError):
+        api.load()
