@@ -190,38 +190,51 @@ def run_ours(args):
     m, c = workload(args.workload)
     s = Lag2DSolver(m, c)
     s.init_fields()
-    st = torch.cuda.ExternalStream(s.stream_ptr)
+    sm = Lag2DSolver(m, c, precision=1)   # FP32-mixed form of the same step
+    sm.init_fields()
     dof_stage = m.ncell * c.ndegr * c.nq
 
-    s.run(args.warmup)
-    # ---- timed region: K steps from the captured graph, device events
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
+    def timed(solver):
+        """K graph-replayed steps after W warm-up steps: device ms, steps, launches."""
+        stream = torch.cuda.ExternalStream(solver.stream_ptr)
+        solver.run(args.warmup)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = solver.kernel_launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        n = solver.run(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1)), n, solver.kernel_launches - l0
+
+    def families(solver):
+        solver.timing(True)
+        solver.run(2)
+        out = {}
+        for f in ("persson", "weno", "corner", "node", "rhs", "dt", "update", "nodes", "geom", "copy"):
+            k_ms, n = solver.kernel_ms(f)
+            if k_ms is not None:
+                out[f] = {"ms_per_launch": k_ms, "launches": n}
+        solver.timing(False)
+        return out
+
+    # ---- timed regions (FP64, then FP32-mixed), clocks sampled across both
     clk = Clocks(local_rank)
-    l0 = s.kernel_launches
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    done = s.run(args.steps)
-    e1.record(st)
-    e1.synchronize()
-    torch.cuda.synchronize()
+    ms, done, launches = timed(s)
+    ms_mx, done_mx, launches_mx = timed(sm)
     clocks = clk.stop()
-    launches = s.kernel_launches - l0
-    ms = max_over_ranks(e0.elapsed_time(e1))
     ms_per_step = ms / max(done, 1)
     value = aggregate_rate(dof_stage * c.nstag * done, ms / 1e3, world)
+    value_mx = aggregate_rate(dof_stage * c.nstag * done_mx, ms_mx / 1e3, world)
 
     # ---- per-kernel device times (separate pass, events around each family)
-    s.timing(True)
-    s.run(2)
-    fams = {}
-    for f in ("persson", "weno", "corner", "node", "rhs", "dt", "update", "nodes", "geom", "copy"):
-        k_ms, n = s.kernel_ms(f)
-        if k_ms is not None:
-            fams[f] = {"ms_per_launch": k_ms, "launches": n}
-    s.timing(False)
+    fams = families(s)
+    fams_mx = families(sm)
     per_step = {f: v["ms_per_launch"] * v["launches"] / 2 for f, v in fams.items()}
+    per_step_mx = {f: v["ms_per_launch"] * v["launches"] / 2 for f, v in fams_mx.items()}
     dom = max((f for f in per_step if f in ("corner", "node", "rhs", "update", "persson", "nodes", "geom")),
               key=lambda f: per_step[f])
     peak, peak_kind = peaks()
@@ -229,6 +242,30 @@ def run_ours(args):
     achieved = kb / (fams[dom]["ms_per_launch"] / 1e3) / 1e9
     sb = stage_bytes(m.ncell, m.npoin)
     stage_gbs = sb / (ms_per_step / c.nstag / 1e3) / 1e9
+
+    # ---- error of the mixed form: both forms from the same initial state
+    n_err = 10
+    s.init_fields()
+    sm.init_fields()
+    s.run(n_err)
+    sm.run(n_err)
+    u64, x64 = s.get_state()[:2]
+    umx, xmx = sm.get_state()[:2]
+    nc = m.ncell
+    diff = np.abs(umx[:nc, :, 0] - u64[:nc, :, 0])
+    err_mx = np.minimum(diff / np.maximum(np.abs(u64[:nc, :, 0]), 1e-300),
+                        diff / np.abs(u64[:nc, :, 0]).max(axis=0)).max(axis=0)
+    mixed = {"value": value_mx, "unit": UNIT, "ms_per_step": ms_mx / max(done_mx, 1), "steps": done_mx,
+             "speedup_vs_fp64": value_mx / value, "gpu_launches": launches_mx,
+             "dtype": "f32 flux/quadrature arithmetic; f64 storage, nodal solve, nodes, volumes, cell averages",
+             "cell_avg_err_vs_fp64": {"tau": float(err_mx[0]), "u": float(err_mx[1]), "v": float(err_mx[2]),
+                                      "e": float(err_mx[3])},
+             "node_err_vs_fp64": float(np.abs(xmx - x64).max()),
+             "err_note": (f"max over cells after {n_err} steps from the same initial state, against the FP64 GPU "
+                          "step (itself within 1e-12 of the FP64 oracle); relative to the value, or to the field "
+                          "scale where the field crosses zero"),
+             "kernels_ms_per_step": per_step_mx}
+    sm.close()
 
     # ---- end to end through the C-ABI with pinned host buffers
     u_h = torch.empty((m.nsize, c.nq, c.ndegr), dtype=torch.float64, pin_memory=True)
@@ -261,7 +298,8 @@ def run_ours(args):
                              "bytes_per_launch": kb},
                 "stage_roofline": {"bytes_per_stage": sb, "achieved_gbs": stage_gbs, "peak": peak,
                                    "frac": stage_gbs / peak, "roofline_dof_updates_per_s": dof_stage / (sb / (peak * 1e9))},
-                "kernels_ms_per_step": per_step}
+                "kernels_ms_per_step": per_step, "fp32_mixed": mixed,
+                "adjoint_forward_ratio": None, "adjoint_note": "adjoint step not built"}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)

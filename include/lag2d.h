@@ -59,6 +59,9 @@ typedef struct {
   int nlimi, ndens;
   int ngausd, ngausd_geo;
   int precision;        /* 0: FP64; 1: FP32-mixed (not built: EUNSUP)    */
+  int order_exact;      /* 1: kernels that keep the reference's loop and
+                           summation order (bit-identical to the CPU
+                           restatement in the no-FMA build); 0: optimised */
   int nsedov;           /* number of Sedov energy cells (<= 4)           */
   int sedov_cell[4];    /* their 1-based ids                             */
   double gamlg, cfl, cdrho, cimpd, tend, sedov_energy;

@@ -54,6 +54,7 @@ class _Cfg(ctypes.Structure):
                 ("nq", ctypes.c_int), ("nstag", ctypes.c_int), ("ndt", ctypes.c_int),
                 ("ncase", ctypes.c_int), ("nlimi", ctypes.c_int), ("ndens", ctypes.c_int),
                 ("ngausd", ctypes.c_int), ("ngausd_geo", ctypes.c_int), ("precision", ctypes.c_int),
+                ("order_exact", ctypes.c_int),
                 ("nsedov", ctypes.c_int), ("sedov_cell", ctypes.c_int * 4),
                 ("gamlg", ctypes.c_double), ("cfl", ctypes.c_double), ("cdrho", ctypes.c_double),
                 ("cimpd", ctypes.c_double), ("tend", ctypes.c_double), ("sedov_energy", ctypes.c_double)]
@@ -100,7 +101,13 @@ def _p(a, t):
 class Lag2DSolver:
     """One mesh + configuration on the current CUDA device."""
 
-    def __init__(self, mesh: Mesh, cfg: StepConfig, exact: bool = False):
+    def __init__(self, mesh: Mesh, cfg: StepConfig, exact: bool = False, order_exact: bool = False,
+                 precision: int = 0):
+        """exact: load the no-FMA build; order_exact: use the kernels that keep
+        the reference's summation order (both together reproduce the CPU
+        restatement bit for bit); precision: 0 = FP64, 1 = FP32-mixed (bulk
+        flux and quadrature arithmetic in FP32; nodal solve, node positions,
+        volumes and cell-average/energy bookkeeping in FP64)."""
         self.lib = load(exact)
         self.mesh, self.cfg = mesh, cfg
         self._keep = [np.ascontiguousarray(a, dtype=np.int32) for a in
@@ -111,7 +118,9 @@ class Lag2DSolver:
                         _p(k[2], _ip), _p(k[3], _ip), _p(k[4], _ip), _p(k[5], _ip), _p(self._coold, _dp))
         sc = (ctypes.c_int * 4)(*(list(cfg.sedov_cells) + [0, 0, 0, 0])[:4])
         self._c = _Cfg(cfg.npoly, cfg.ndegr, cfg.mdegr, cfg.nq, cfg.nstag, cfg.ndt, cfg.ncase, cfg.nlimi,
-                       cfg.ndens, cfg.ngausd, cfg.ngausd_geo, 0, len(cfg.sedov_cells), sc, cfg.gamlg, cfg.cfl,
+                       cfg.ndens, cfg.ngausd, cfg.ngausd_geo, int(precision), 1 if order_exact else 0,
+                       len(cfg.sedov_cells),
+                       sc, cfg.gamlg, cfg.cfl,
                        cfg.cdrho, cfg.cimpd, cfg.tend, cfg.sedov_energy)
         h = ctypes.c_void_p()
         self._check(self.lib.lag2d_create(ctypes.byref(self._m), ctypes.byref(self._c), ctypes.byref(h)))

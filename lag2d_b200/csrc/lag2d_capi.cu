@@ -38,6 +38,16 @@ void launch_unkno_in(const Dev &d, cudaStream_t st, const double *aos, int both)
 void launch_unkno_out(const Dev &d, cudaStream_t st, double *aos);
 void launch_xy_in(int n, cudaStream_t st, const double *xy, double *x, double *y, double *x2, double *y2);
 void launch_xy_out(int n, cudaStream_t st, double *xy, const double *x, const double *y);
+void launch_fast_persson(const Dev &d, cudaStream_t st);
+void launch_fast_corner(const Dev &d, cudaStream_t st);
+void launch_fast_node(const Dev &d, cudaStream_t st);
+void launch_fast_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa);
+void launch_fast_update(const Dev &d, cudaStream_t st, double alfa);
+void launch_mixed_corner(const Dev &d, cudaStream_t st);
+void launch_mixed_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa);
+void launch_fast_nodes(const Dev &d, cudaStream_t st, double alfa);
+void launch_fast_geom(const Dev &d, cudaStream_t st, int fix);
+void launch_init_wmom(const Dev &d, cudaStream_t st);
 }  // namespace lag2d
 
 using namespace lag2d;
@@ -48,6 +58,11 @@ static int fail(int code, const std::string &msg) {
   g_err = msg;
   return code;
 }
+
+namespace lag2d {
+// error text for lag2d_last_error from entry points in other translation units
+int set_error(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace lag2d
 
 #define CK(call)                                                                      \
   do {                                                                                \
@@ -70,6 +85,7 @@ struct lag2d_handle {
   double *stage_u = nullptr;   // staging for unkno(ndegr,nq,ncell) in the caller's layout
   double *stage_x = nullptr;   // staging for coord / ustar (2,npoin)
   cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;
   long long launches = 0;
   bool timing = false;
   std::map<std::string, Family> fam;
@@ -205,7 +221,8 @@ static void flush_timing(lag2d_handle *h) {
 
 static const double kRK[2][3] = {{0.0, 0.5, 0.0}, {0.0, 0.75, 0.3333333333333333}};
 
-// getrhsdg_lag_mcnew, curved P2 branch (Getrhslagmc.f90:7556-7710)
+// getrhsdg_lag_mcnew, curved P2 branch (Getrhslagmc.f90:7556-7710),
+// reference-order kernels
 static void enqueue_rhs(lag2d_handle *h) {
   const Dev &d = h->d;
   run(h, "persson", [&] { launch_reset_count(d, h->st); launch_persson(d, h->st); }, 2);
@@ -216,7 +233,7 @@ static void enqueue_rhs(lag2d_handle *h) {
 }
 
 // getsolvdg_lag (Getrhslag.f90:1553-2035) + the driver copy-back
-static void enqueue_step(lag2d_handle *h, int itime) {
+static void enqueue_step_reference_order(lag2d_handle *h, int itime) {
   const Dev &d = h->d;
   const int nstag = h->cfg.nstag;
   run(h, "geom", [&] { launch_step_begin(d, h->st, itime); launch_geom(d, h->st, d.xn, d.yn); }, 2);
@@ -229,6 +246,48 @@ static void enqueue_step(lag2d_handle *h, int itime) {
     run(h, "geom", [&] { launch_center_geom(d, h->st); launch_geom(d, h->st, d.xs, d.ys); }, 2);
   }
   run(h, "copy", [&] { launch_copyback(d, h->st); launch_step_end(d, h->st, 1); }, 2);
+}
+
+// Corner and RHS passes of the optimised step: FP64, or the FP32-mixed form
+// (config precision = 1) with the same node pass, update and geometry.
+static void corner_pass(lag2d_handle *h) {
+  if (h->cfg.precision == 1) launch_mixed_corner(h->d, h->st);
+  else launch_fast_corner(h->d, h->st);
+}
+static void rhs_pass(lag2d_handle *h, int fuse, double alfa) {
+  if (h->cfg.precision == 1) launch_mixed_rhs(h->d, h->st, fuse, alfa);
+  else launch_fast_rhs(h->d, h->st, fuse, alfa);
+}
+
+// The same step with the optimised kernels: node partial sums, recomputed
+// corner data, closed-form volumes and the stage update fused into the RHS
+// pass in stages 2 and 3.
+static void enqueue_step_fast(lag2d_handle *h, int itime) {
+  const Dev &d = h->d;
+  const int nstag = h->cfg.nstag;
+  run(h, "begin", [&] { launch_step_begin(d, h->st, itime); });
+  for (int istag = 1; istag <= nstag; istag++) {
+    const double alfa = kRK[nstag - 2][istag - 1];
+    run(h, "persson", [&] { launch_reset_count(d, h->st); launch_fast_persson(d, h->st); }, 2);
+    run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
+    run(h, "corner", [&] { corner_pass(h); });
+    run(h, "node", [&] { launch_fast_node(d, h->st); });
+    if (istag == 1) {
+      run(h, "rhs", [&] { rhs_pass(h, 0, alfa); });
+      run(h, "dt", [&] { launch_dt(d, h->st, h->cfg.ndt); }, 2);
+      run(h, "update", [&] { launch_fast_update(d, h->st, alfa); });
+    } else {
+      run(h, "rhs", [&] { rhs_pass(h, 1, alfa); });
+    }
+    run(h, "nodes", [&] { launch_fast_nodes(d, h->st, alfa); });
+    run(h, "geom", [&] { launch_fast_geom(d, h->st, 1); });
+  }
+  run(h, "copy", [&] { launch_copyback(d, h->st); launch_step_end(d, h->st, 1); }, 2);
+}
+
+static void enqueue_step(lag2d_handle *h, int itime) {
+  if (h->cfg.order_exact) enqueue_step_reference_order(h, itime);
+  else enqueue_step_fast(h, itime);
 }
 
 static int read_status(lag2d_handle *h) {
@@ -258,7 +317,8 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
     return fail(LAG2D_EUNSUP, "only P2 (npoly=2, ndegr=6, nq=4, ndens=1) is built");
   if (c->mdegr < 1 || c->mdegr > 6) return fail(LAG2D_EINVAL, "mdegr out of range");
   if (c->nstag != 2 && c->nstag != 3) return fail(LAG2D_EINVAL, "nstag must be 2 or 3");
-  if (c->precision != 0) return fail(LAG2D_EUNSUP, "FP32-mixed precision is not built");
+  if (c->precision != 0 && c->precision != 1) return fail(LAG2D_EINVAL, "precision must be 0 (FP64) or 1 (FP32-mixed)");
+  if (c->precision == 1 && c->order_exact) return fail(LAG2D_EINVAL, "order_exact needs precision = 0");
   if (c->nsedov < 0 || c->nsedov > 4) return fail(LAG2D_EINVAL, "nsedov must be 0..4");
   if (c->ncase != 1 && c->ncase != 2 && c->ncase != 3 && c->ncase != 6 && c->ncase != 7)
     return fail(LAG2D_EUNSUP, "initial-condition case not built");
@@ -312,6 +372,16 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
         int p = ipq[kIPQSG[isg][ivsg] * (size_t)nq + iq];
         for (int f = 0; f < 2; f++) nodecf[fillp[p]++] = iq * 32 + (f + 2 * (ivsg + 4 * isg));
       }
+  // node -> (quad, local node) lists in cell order for the optimised gather
+  std::vector<int> cnt2(np + 1, 0), slots(9 * (size_t)nq);
+  for (int iq = 0; iq < nq; iq++)
+    for (int k = 0; k < 9; k++) cnt2[ipq[k * (size_t)nq + iq] + 1]++;
+  for (int p = 0; p < np; p++) cnt2[p + 1] += cnt2[p];
+  {
+    std::vector<int> fp(cnt2.begin(), cnt2.end() - 1);
+    for (int iq = 0; iq < nq; iq++)
+      for (int k = 0; k < 9; k++) slots[fp[ipq[k * (size_t)nq + iq]]++] = iq * 9 + k;
+  }
   // wall masks (getndvelo_lagsubg, Getrhslaggauss.f90:4420-4545)
   std::vector<unsigned char> mask(np, 0);
   for (int f = 0; f < m->nbfac; f++) {
@@ -341,15 +411,21 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   A(&d.Uw, 20 * (size_t)nq); A(&d.wlist, nq); A(&d.wcount, 1);
   A(&d.dtpart, 2 * (size_t)dt_blocks(d) + 2); A(&d.sc_dev, 1); A(&h->flags_dev, ncell);
   A(&h->stage_u, NU * (size_t)ncell); A(&h->stage_x, 2 * (size_t)np);
+  int *ptr2_d, *slot_d;
+  A(&ptr2_d, cnt2.size()); A(&slot_d, slots.size());
+  A(&d.npart, 45 * (size_t)nq); A(&d.corr, 4 * (size_t)nq); A(&d.us_new, np); A(&d.vs_new, np);
+  A(&d.wmom, 9 * (size_t)nq);
   if (rc != LAG2D_OK) { lag2d_destroy(h); return rc; }
   d.ipq = ipq_d; d.esq = esq_d; d.stencil = sten_d; d.node_ptr = ptr_d; d.node_cf = ncf_d;
   d.bcmask = mask_d; d.x0 = x0; d.y0 = y0;
+  d.node_ptr2 = ptr2_d; d.node_slot = slot_d;
   std::vector<double> xx(np), yy(np);
   for (int p = 0; p < np; p++) { xx[p] = m->coold[2 * (size_t)p]; yy[p] = m->coold[2 * (size_t)p + 1]; }
 #define UP(dst, src, n) cudaMemcpyAsync((void *)(dst), (src), (n) * sizeof(*(src)), cudaMemcpyHostToDevice, h->st)
   UP(ipq_d, ipq.data(), ipq.size()); UP(esq_d, esq.data(), esq.size()); UP(sten_d, sten.data(), sten.size());
   UP(ptr_d, cnt.data(), cnt.size()); UP(ncf_d, nodecf.data(), nodecf.size()); UP(mask_d, mask.data(), mask.size());
   UP(x0, xx.data(), np); UP(y0, yy.data(), np);
+  UP(ptr2_d, cnt2.data(), cnt2.size()); UP(slot_d, slots.data(), slots.size());
   UP(d.xn, xx.data(), np); UP(d.yn, yy.data(), np); UP(d.xs, xx.data(), np); UP(d.ys, yy.data(), np);
 #undef UP
   QuadTables qt;
@@ -359,7 +435,7 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   set_tables(qt, h->st);
   Scalars s0{};
   cudaMemcpyAsync(d.sc_dev, &s0, sizeof(Scalars), cudaMemcpyHostToDevice, h->st);
-  run(h, "init", [&] { launch_init_msub(d, h->st); });
+  run(h, "init", [&] { launch_init_msub(d, h->st); launch_init_wmom(d, h->st); }, 2);
   if (cudaStreamSynchronize(h->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     lag2d_destroy(h);
     return fail(LAG2D_ECUDA, "device set-up failed");
@@ -517,13 +593,10 @@ int lag2d_run(lag2d_handle *h, int itime0, int nsteps, double *dtfix, double *ta
       CK(cudaStreamEndCapture(h->st, &g));
       CK(cudaGraphInstantiate(&h->graph, g, 0));
       cudaGraphDestroy(g);
+      h->graph_launches = h->launches - before;
       h->launches = before;  // counted per replay below
     }
-    long long per_step = 0;
-    {
-      // launches per step: 2 + nstag * (2+2+1+1+1 + 1+1+2) + 2 (dt) + 2
-      per_step = 2 + (long long)h->cfg.nstag * 11 + 2 + 2;
-    }
+    const long long per_step = h->graph_launches;
     for (int i = 0; i < nsteps; i++) {
       CK(cudaGraphLaunch(h->graph, h->st));
       h->launches += per_step;
@@ -554,14 +627,27 @@ int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
   Dev &d = h->d;
   int r = put_scalars(h, itime, 0.0, 0.0);
   if (r) return r;
-  run(h, "persson", [&] { launch_reset_count(d, h->st); launch_persson(d, h->st); }, 2);
+  const bool ex = h->cfg.order_exact != 0;
+  run(h, "persson", [&] {
+    launch_reset_count(d, h->st);
+    if (ex) launch_persson(d, h->st); else launch_fast_persson(d, h->st);
+  }, 2);
   if (flags) {
     CK(cudaMemcpyAsync(h->flags_dev, d.flag, d.ncell * sizeof(int), cudaMemcpyDeviceToDevice, h->st));
   }
   run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
-  run(h, "corner", [&] { launch_corner(d, h->st); });
-  run(h, "node", [&] { launch_node(d, h->st); });
-  run(h, "rhs", [&] { launch_rhs(d, h->st); });
+  if (ex) {
+    run(h, "corner", [&] { launch_corner(d, h->st); });
+    run(h, "node", [&] { launch_node(d, h->st); });
+    run(h, "rhs", [&] { launch_rhs(d, h->st); });
+  } else {
+    run(h, "corner", [&] { corner_pass(h); });
+    run(h, "node", [&] { launch_fast_node(d, h->st); });
+    run(h, "rhs", [&] { rhs_pass(h, 0, 0.0); });
+    // the RHS keeps ustar of the previous stage for the impedances; expose the new one
+    CK(cudaMemcpyAsync(d.us, d.us_new, d.npoin * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemcpyAsync(d.vs, d.vs_new, d.npoin * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  }
   r = read_status(h);
   if (h->timing) flush_timing(h);
   if (r) return r;

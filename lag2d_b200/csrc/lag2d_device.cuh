@@ -58,6 +58,13 @@ struct Dev {
   int *wcount;
   double *dtpart;          // [2][nblocks] partial minima for getdelt_lag
   Scalars *sc_dev;
+  // optimised path
+  const int *node_ptr2;    // [npoin+1]
+  const int *node_slot;    // iq*9 + k: quad iq touches the node as its node k, cells ascending
+  double *npart;           // [5][9][nquad] per-cell node partial sums (m, m*u, m*v, s_x, s_y)
+  double *corr;            // [4][nquad] sub-cell density corrections
+  double *us_new, *vs_new; // ustar of the current stage (us, vs hold the previous one)
+  double *wmom;            // [9][nquad] time-invariant mass-weighted shape moments
 };
 
 // Quadrature tables (filled from the host with the reference's literals).

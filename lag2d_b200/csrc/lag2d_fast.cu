@@ -1,0 +1,931 @@
+// Optimised kernels of the curved-P2 Lagrangian DG stage (sm_100a, FP64).
+//
+// Same arithmetic as the reference-order kernels (lag2d_kernels.cu) up to
+// rounding, with far fewer FP64 instructions per cell:
+//  * every volume the reference integrates with Gauss rules of a 9-node map
+//    (cell: getcellvol_lag 6x6; sub-cells: getrhosubg_averg 5x5) is exact for
+//    those polynomial integrands, so it is evaluated in closed form from the
+//    36 node cross products x_i y_j - x_j y_i (lag2d_tables.inc);
+//  * det J at fixed points (Persson, sub-cell densities, source) comes from its
+//    16 bicubic coefficients, a fixed linear map of the same cross products;
+//  * Jacobians on the 5x5 Gauss-Lobatto grid are sum-factorised on the 3x3
+//    tensor of quad nodes;
+//  * the corner pass reduces its 32 corner faces to per-node partial sums
+//    (9 nodes x 5 values) that the node pass gathers in cell order, and the
+//    RHS pass recomputes the cheap corner data instead of reading it back;
+//  * in RK stages 2 and 3 the mass-matrix solve and RK combine are fused into
+//    the RHS pass.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "lag2d_device.cuh"
+#include "lag2d_fast_tables.h"
+
+namespace lag2d {
+
+namespace fast {
+
+#include "lag2d_tables.inc"
+
+// Small lookup tables indexed by warp-uniform loop counters: constant memory
+// for the kernels, a host mirror for CPU checks of the same bodies.
+struct FastTables {
+  int nc_start[10];   // node k owns corner entries [nc_start[k], nc_start[k+1])
+  int nc_entry[16];   // isg * 4 + ivsg, in the reference's (isg, ivsg) order per node
+  int fnqsg[32];      // gesgq slot (sign = orientation) of corner face (isg, ivsg, f)
+  double wrie[32];    // Riemann corner-face weights (Getrhslaggauss.f90:10534-10552) x 0.25
+  double wmas[32];    // mass-equation face weights (Getrhslaggauss.f90:8611-8634) x 0.25
+  double wmom[16];    // momentum/energy face weights (Getrhslaggauss.f90:8580-8603)
+  int pa[12], pb[12], side[12];  // Simpson points as tensor nodes and their face
+  double dl[9];       // L'_c at r = -1, 0, 1: dl[3a + c]
+  double xv[9], yv[9];  // reference coordinates of the 9 nodes
+};
+__constant__ FastTables cFT = LAG2D_FAST_TABLES;
+static const FastTables hFT = LAG2D_FAST_TABLES;
+__host__ __device__ __forceinline__ const FastTables &FT() {
+#ifdef __CUDA_ARCH__
+  return cFT;
+#else
+  return hFT;
+#endif
+}
+
+// 1-D quadratic Lagrange basis on {-1, 0, 1} and its derivative
+__host__ __device__ __forceinline__ void lag3(double r, double *l) {
+  l[0] = 0.5 * r * (r - 1.0);
+  l[1] = 1.0 - r * r;
+  l[2] = 0.5 * r * (r + 1.0);
+}
+__host__ __device__ __forceinline__ void dlag3(double r, double *l) {
+  l[0] = r - 0.5;
+  l[1] = -2.0 * r;
+  l[2] = r + 0.5;
+}
+
+// reference node k at tensor position (a, b): X[a][b]
+__host__ __device__ __forceinline__ void to_tensor(const double (*xp)[2], double X[3][3], double Y[3][3]) {
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    X[A[k]][B[k]] = xp[k][0];
+    Y[A[k]][B[k]] = xp[k][1];
+  }
+}
+
+__host__ __device__ __forceinline__ double deteval(const double *D, double r, double s) {
+  double e[4];
+#pragma unroll
+  for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+  return e[0] + s * (e[1] + s * (e[2] + s * e[3]));
+}
+
+// integral of det J over the sub-square [r0, r0+1] x [s0, s0+1]
+__host__ __device__ __forceinline__ double det_integral(const double *D, double r0, double s0) {
+  double mr[4], ms[4];
+  const double r1 = r0 + 1.0, s1 = s0 + 1.0;
+  double pr0 = r0, pr1 = r1, ps0 = s0, ps1 = s1;
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    mr[m] = (pr1 - pr0) / (m + 1);
+    ms[m] = (ps1 - ps0) / (m + 1);
+    pr0 *= r0; pr1 *= r1; ps0 *= s0; ps1 *= s1;
+  }
+  double v = 0.0;
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+#pragma unroll
+    for (int n = 0; n < 4; n++) v += D[4 * m + n] * mr[m] * ms[n];
+  return v;
+}
+
+// 1-D Gauss (ruqope) and Gauss-Lobatto (ruqope_lobatto) 5-point rules
+__host__ __device__ __forceinline__ double g5p(int i) {
+  const double p[5] = {-0.9061798459386639927976269, -0.5384693101056830910363144, 0.0,
+                       0.5384693101056830910363144, 0.9061798459386639927976269};
+  return p[i];
+}
+__host__ __device__ __forceinline__ double g5w(int i) {
+  const double w[5] = {0.2369268850561890875142640, 0.4786286704993664680412915, 0.5688888888888888888888889,
+                       0.4786286704993664680412915, 0.2369268850561890875142640};
+  return w[i];
+}
+__host__ __device__ __forceinline__ double l5p(int i) {
+  const double p[5] = {-1.0, -0.6546536707079771437983, 0.0, 0.6546536707079771437983, 1.0};
+  return p[i];
+}
+__host__ __device__ __forceinline__ double l5w(int i) {
+  const double w[5] = {0.1, 0.544444444444444444444, 0.7111111111111111111111, 0.544444444444444444444, 0.1};
+  return w[i];
+}
+
+struct CellGeo {
+  double rc, sc, g19, g20, g21;
+};
+
+__host__ __device__ __forceinline__ void node_basis2(const CellGeo &g, int iv, double *b) {
+  b[0] = 1.0;
+  b[1] = FT().xv[iv] - g.rc;
+  b[2] = FT().yv[iv] - g.sc;
+  b[3] = 0.5 * b[1] * b[1] - g.g19;
+  b[4] = 0.5 * b[2] * b[2] - g.g20;
+  b[5] = b[1] * b[2] - g.g21;
+}
+
+// DG state evaluated at (r, s): Taylor basis about (rc, sc)
+__host__ __device__ __forceinline__ double eval_taylor(const double *u, const CellGeo &g, double r, double s) {
+  const double dr = r - g.rc, ds = s - g.sc;
+  return u[0] + u[1] * dr + u[2] * ds + u[3] * (0.5 * dr * dr - g.g19) + u[4] * (0.5 * ds * ds - g.g20) +
+         u[5] * (dr * ds - g.g21);
+}
+
+// Sub-cell normals (16 entries, same slots as gesgq of the reference):
+// Simpson-point normals from node derivatives of the tensor map and the four
+// inner sub-cell faces at the edge nodes.
+__host__ __device__ __forceinline__ void normals16(const double X[3][3], const double Y[3][3], double (*gq)[3]) {
+  const double DL[3][3] = {{-1.5, 2.0, -0.5}, {-0.5, 0.0, 0.5}, {0.5, -2.0, 1.5}};  // L'_c(r_a): DL[a][c]
+  // the 12 outer points (getfnds_lagsms_simpsonhybrid posiq order) as tensor nodes
+  const int PA[12] = {0, 2, 2, 2, 2, 0, 0, 0, 1, 2, 1, 0};
+  const int PB[12] = {0, 0, 0, 2, 2, 2, 2, 0, 0, 1, 2, 1};
+  const double vnx[4] = {0.0, 1.0, 0.0, -1.0}, vny[4] = {-1.0, 0.0, 1.0, 0.0};
+  const int side[12] = {0, 0, 1, 1, 2, 2, 3, 3, 0, 1, 2, 3};
+#pragma unroll
+  for (int ig = 0; ig < 12; ig++) {
+    const int a = PA[ig], b = PB[ig];
+    double xr = DL[a][0] * X[0][b] + DL[a][1] * X[1][b] + DL[a][2] * X[2][b];
+    double yr = DL[a][0] * Y[0][b] + DL[a][1] * Y[1][b] + DL[a][2] * Y[2][b];
+    double xs = DL[b][0] * X[a][0] + DL[b][1] * X[a][1] + DL[b][2] * X[a][2];
+    double ys = DL[b][0] * Y[a][0] + DL[b][1] * Y[a][1] + DL[b][2] * Y[a][2];
+    const double vn0 = vnx[side[ig]], vn1 = vny[side[ig]];
+    double anx = ys * vn0 - yr * vn1;
+    double any = -xs * vn0 + xr * vn1;
+    double farea = 2.0 * sqrt(anx * anx + any * any);
+    double inv = 1.0 / sqrt(anx * anx + any * any);
+    const int slot = (ig < 8) ? ig : ig + 4;
+    gq[slot][0] = anx * inv;
+    gq[slot][1] = any * inv;
+    gq[slot][2] = farea;
+  }
+  // inner faces from edge node (5..8) towards the centre, derivative at the
+  // edge node of the quadratic through (edge node, centre, map(posqc))
+  // posqc = (0,-.5), (.5,0), (0,.5), (-.5,0); L(-.5) = (.375, .75, -.125), L(.5) = (-.125, .75, .375)
+  const double lm[3] = {0.375, 0.75, -0.125}, lp[3] = {-0.125, 0.75, 0.375};
+  double ex[4], ey[4], vx[4], vy[4];
+  ex[0] = X[1][0]; ey[0] = Y[1][0];
+  vx[0] = lm[0] * X[1][0] + lm[1] * X[1][1] + lm[2] * X[1][2];
+  vy[0] = lm[0] * Y[1][0] + lm[1] * Y[1][1] + lm[2] * Y[1][2];
+  ex[1] = X[2][1]; ey[1] = Y[2][1];
+  vx[1] = lp[0] * X[0][1] + lp[1] * X[1][1] + lp[2] * X[2][1];
+  vy[1] = lp[0] * Y[0][1] + lp[1] * Y[1][1] + lp[2] * Y[2][1];
+  ex[2] = X[1][2]; ey[2] = Y[1][2];
+  vx[2] = lp[0] * X[1][0] + lp[1] * X[1][1] + lp[2] * X[1][2];
+  vy[2] = lp[0] * Y[1][0] + lp[1] * Y[1][1] + lp[2] * Y[1][2];
+  ex[3] = X[0][1]; ey[3] = Y[0][1];
+  vx[3] = lm[0] * X[0][1] + lm[1] * X[1][1] + lm[2] * X[2][1];
+  vy[3] = lm[0] * Y[0][1] + lm[1] * Y[1][1] + lm[2] * Y[2][1];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    double dxdr = -1.5 * ex[f] - 0.5 * X[1][1] + 2.0 * vx[f];
+    double dydr = -1.5 * ey[f] - 0.5 * Y[1][1] + 2.0 * vy[f];
+    double n2 = dxdr * dxdr + dydr * dydr;
+    double inv = 1.0 / sqrt(n2);
+    gq[8 + f][0] = -dydr * inv;
+    gq[8 + f][1] = dxdr * inv;
+    gq[8 + f][2] = 2.0 * sqrt(n2);
+  }
+}
+
+__host__ __device__ __forceinline__ int ipqsg2(int isg, int ivsg) {
+  const int t[16] = {0, 4, 8, 7, 4, 1, 5, 8, 8, 5, 2, 6, 7, 8, 6, 3};
+  return t[4 * isg + ivsg];
+}
+__host__ __device__ __forceinline__ int fnqsg2(int isg, int k) { return FT().fnqsg[8 * isg + k]; }
+// corner-face weights (Getrhslaggauss.f90:10534-10552 x 0.25; :8580-8637)
+__host__ __device__ __forceinline__ double wrie(int isg, int ivsg, int f) { return FT().wrie[8 * isg + 2 * ivsg + f]; }
+__host__ __device__ __forceinline__ double wmas(int isg, int ivsg, int f) { return FT().wmas[8 * isg + 2 * ivsg + f]; }
+__host__ __device__ __forceinline__ double wmom(int isg, int ivsg) { return FT().wmom[4 * isg + ivsg]; }
+
+__host__ __device__ __forceinline__ void corner_n(const double (*gq)[3], int isg, int ivsg, int f, double &n0,
+                                                  double &n1, double &a) {
+  const int code = fnqsg2(isg, 2 * ivsg + f);
+  const int slot = (code >= 0 ? code : -code) - 1;
+  const double sg = (code >= 0) ? 1.0 : -1.0;
+  n0 = sg * gq[slot][0];
+  n1 = sg * gq[slot][1];
+  a = gq[slot][2];
+}
+
+// Per-corner state shared by the corner and RHS passes: vertex velocity and
+// pressure with the sub-cell density correction (getriem_quadsubg2,
+// Getrhslaggauss.f90:10662-10710) and the cell-centre sound speed.
+struct CornerState {
+  double u[4][2], p[4];
+};
+
+__host__ __device__ __forceinline__ void corner_states(const double unknvq[9][4], const double *corr, double g,
+                                                       int isg, CornerState &cs) {
+  const double eps = 1.0e-6;
+#pragma unroll
+  for (int ivsg = 0; ivsg < 4; ivsg++) {
+    const int iv = ipqsg2(isg, ivsg);
+    const double rhovsg = 1.0 / unknvq[iv][0] + corr[isg];
+    const double uvtx = unknvq[iv][1], vvtx = unknvq[iv][2], evtx = unknvq[iv][3];
+    cs.u[ivsg][0] = uvtx;
+    cs.u[ivsg][1] = vvtx;
+    cs.p[ivsg] = fmax(eps, (g - 1.0) * rhovsg * (evtx - 0.5 * (uvtx * uvtx + vvtx * vvtx)));
+  }
+}
+
+// impedance-weighted area m = mu * A of one corner face (getriecoef_matrixnew,
+// Limiterlag.f90:1037): the jump-direction branch is taken only when
+// |u* - u_c| / c >= 1e12, tested on squares
+__host__ __device__ __forceinline__ double corner_m(double rhoct, double sdctr, double cimpd, double slpdu,
+                                                   double dux, double duy, double n0, double n1, double a) {
+  const double deltu = fabs(dux * n0 + duy * n1);
+  const double murie = rhoct * sdctr + cimpd * rhoct * slpdu * deltu;
+  const double j2 = dux * dux + duy * duy;
+  const double lim = 1.0e12 * sdctr;
+  if (j2 < lim * lim) return murie * a;
+  const double nrm = sqrt(j2);
+  double ax, ay;
+  if (nrm < (double)1.e-11f) { ax = (double)1.e-11f; ay = (double)1.e-11f; }
+  else { ax = dux / nrm; ay = duy / nrm; }
+  return murie * a * fabs(n0 * ax + n1 * ay);
+}
+
+// Corner faces grouped by the node they belong to, in the reference's
+// (isg, ivsg) order: node k is vertex ivsg of sub-cell isg for the entries
+// NODE_CORNERS[NC_START[k] .. NC_START[k+1]) encoded as isg * 4 + ivsg.
+__host__ __device__ __forceinline__ int nc_start(int k) { return FT().nc_start[k]; }
+__host__ __device__ __forceinline__ int nc_entry(int i) { return FT().nc_entry[i]; }
+
+// outer/inner face normal (unit n, length a) of the gesgq slot `slot`
+__host__ __device__ __forceinline__ void slot_normal(const double X[3][3], const double Y[3][3], int slot, double &n0,
+                                                     double &n1, double &a) {
+  if (slot >= 8 && slot < 12) {
+    // inner sub-cell face at edge node (5..8) towards the centre
+    const int f = slot - 8;
+    const double lm0 = 0.375, lm1 = 0.75, lm2 = -0.125, lp0 = -0.125, lp1 = 0.75, lp2 = 0.375;
+    double ex, ey, vx, vy;
+    if (f == 0) {
+      ex = X[1][0]; ey = Y[1][0];
+      vx = lm0 * X[1][0] + lm1 * X[1][1] + lm2 * X[1][2];
+      vy = lm0 * Y[1][0] + lm1 * Y[1][1] + lm2 * Y[1][2];
+    } else if (f == 1) {
+      ex = X[2][1]; ey = Y[2][1];
+      vx = lp0 * X[0][1] + lp1 * X[1][1] + lp2 * X[2][1];
+      vy = lp0 * Y[0][1] + lp1 * Y[1][1] + lp2 * Y[2][1];
+    } else if (f == 2) {
+      ex = X[1][2]; ey = Y[1][2];
+      vx = lp0 * X[1][0] + lp1 * X[1][1] + lp2 * X[1][2];
+      vy = lp0 * Y[1][0] + lp1 * Y[1][1] + lp2 * Y[1][2];
+    } else {
+      ex = X[0][1]; ey = Y[0][1];
+      vx = lm0 * X[0][1] + lm1 * X[1][1] + lm2 * X[2][1];
+      vy = lm0 * Y[0][1] + lm1 * Y[1][1] + lm2 * Y[2][1];
+    }
+    const double dxdr = -1.5 * ex - 0.5 * X[1][1] + 2.0 * vx;
+    const double dydr = -1.5 * ey - 0.5 * Y[1][1] + 2.0 * vy;
+    const double nn = sqrt(dxdr * dxdr + dydr * dydr);
+    const double inv = 1.0 / nn;
+    n0 = -dydr * inv;
+    n1 = dxdr * inv;
+    a = 2.0 * nn;
+    return;
+  }
+  // Simpson points (getfnds_lagsms_simpsonhybrid order) on the 4 outer faces
+  const int ig = slot < 8 ? slot : slot - 4;
+  const FastTables &T = FT();
+  const int ia = T.pa[ig], ib = T.pb[ig];
+  const double *da = T.dl + 3 * ia, *db = T.dl + 3 * ib;
+  // the tensor rows/columns are selected with uniform branches to keep X, Y in registers
+  double xa0, xa1, xa2, ya0, ya1, ya2, xb0, xb1, xb2, yb0, yb1, yb2;
+  if (ib == 0) { xa0 = X[0][0]; xa1 = X[1][0]; xa2 = X[2][0]; ya0 = Y[0][0]; ya1 = Y[1][0]; ya2 = Y[2][0]; }
+  else if (ib == 1) { xa0 = X[0][1]; xa1 = X[1][1]; xa2 = X[2][1]; ya0 = Y[0][1]; ya1 = Y[1][1]; ya2 = Y[2][1]; }
+  else { xa0 = X[0][2]; xa1 = X[1][2]; xa2 = X[2][2]; ya0 = Y[0][2]; ya1 = Y[1][2]; ya2 = Y[2][2]; }
+  if (ia == 0) { xb0 = X[0][0]; xb1 = X[0][1]; xb2 = X[0][2]; yb0 = Y[0][0]; yb1 = Y[0][1]; yb2 = Y[0][2]; }
+  else if (ia == 1) { xb0 = X[1][0]; xb1 = X[1][1]; xb2 = X[1][2]; yb0 = Y[1][0]; yb1 = Y[1][1]; yb2 = Y[1][2]; }
+  else { xb0 = X[2][0]; xb1 = X[2][1]; xb2 = X[2][2]; yb0 = Y[2][0]; yb1 = Y[2][1]; yb2 = Y[2][2]; }
+  const double xr = da[0] * xa0 + da[1] * xa1 + da[2] * xa2;
+  const double yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
+  const double xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
+  const double ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
+  double anx, any;
+  switch (T.side[ig]) {
+    case 0: anx = yr; any = -xr; break;     // vnorm (0,-1)
+    case 1: anx = ys; any = -xs; break;     // vnorm (1, 0)
+    case 2: anx = -yr; any = xr; break;     // vnorm (0, 1)
+    default: anx = -ys; any = xs; break;    // vnorm (-1,0)
+  }
+  const double nn = sqrt(anx * anx + any * any);
+  const double inv = 1.0 / nn;
+  n0 = anx * inv;
+  n1 = any * inv;
+  a = 2.0 * nn;
+}
+
+__host__ __device__ __forceinline__ void corner_face(const double X[3][3], const double Y[3][3], int isg, int ivsg,
+                                                     int f, double &n0, double &n1, double &a) {
+  const int code = fnqsg2(isg, 2 * ivsg + f);
+  const int slot = (code >= 0 ? code : -code) - 1;
+  slot_normal(X, Y, slot, n0, n1, a);
+  if (code < 0) { n0 = -n0; n1 = -n1; }
+}
+
+struct Loaded {
+  double X[3][3], Y[3][3];  // node coordinates on the 3x3 tensor
+};
+
+__host__ __device__ __forceinline__ void load_cell(const Dev &d, const double *XS, const double *YS, int iq, Loaded &L) {
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const int p = d.ipq[k * d.nquad + iq];
+    L.X[A[k]][B[k]] = XS[p];
+    L.Y[A[k]][B[k]] = YS[p];
+  }
+}
+
+// node coordinates back in the reference node order
+__host__ __device__ __forceinline__ void node_xy(const Loaded &L, double (*xp)[2]) {
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    xp[k][0] = L.X[A[k]][B[k]];
+    xp[k][1] = L.Y[A[k]][B[k]];
+  }
+}
+
+__host__ __device__ __forceinline__ void load_u(const Dev &d, const double *U, int e, double u[4][6]) {
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < 6; k++) u[q][k] = U[(q * 6 + k) * (size_t)d.ncell + e];
+}
+
+__host__ __device__ __forceinline__ void vertex_states(const double u[4][6], const CellGeo &g, double unknvq[9][4],
+                                                       int mdegr) {
+#pragma unroll
+  for (int iv = 0; iv < 9; iv++) {
+    double b[6];
+    node_basis2(g, iv, b);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; k++)
+        if (k < mdegr) acc += u[q][k] * b[k];
+      unknvq[iv][q] = acc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persson indicator + physical mass centre + frame (all quads)
+// ---------------------------------------------------------------------------
+__host__ __device__ void f_persson(const Dev &d, int iq) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  double c[36], D[16];
+  {
+    double xp[9][2];
+    node_xy(L, xp);
+    cross36(xp, c);
+  }
+  detpoly(c, D);
+  const CellGeo g{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double t[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) t[k] = d.Us[k * (size_t)d.ncell + e];
+  double unvar2 = 0.0, unvar1 = 0.0;
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    const double r = g5p(i);
+    const double dr = r - g.rc;
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const double s = g5p(j);
+      const double ds = s - g.sc;
+      const double djaco = g5w(i) * g5w(j) * deteval(D, r, s);
+      const double p1 = t[0] + t[1] * dr + t[2] * ds;
+      const double hi = t[3] * (0.5 * dr * dr - g.g19) + t[4] * (0.5 * ds * ds - g.g20) + t[5] * (dr * ds - g.g21);
+      const double un = p1 + hi;
+      unvar2 += hi * hi * djaco;
+      unvar1 += un * un * djaco;
+    }
+  }
+  const double thr = -3.0 * log10(4.0) - 4.0;
+  const int fl = (log10(unvar2 / unvar1) <= thr) ? 0 : 1;
+  d.flag[e] = fl;
+  // physical mass centre from the time-invariant mass-weighted shape moments
+  double xmc = 0.0, ymc = 0.0;
+  {
+    double xp[9][2];
+    node_xy(L, xp);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const double w = d.wmom[k * (size_t)d.nquad + iq];
+      xmc += w * xp[k][0];
+      ymc += w * xp[k][1];
+    }
+  }
+  const double masel = d.mass[e];
+  d.geoph[e] = xmc / masel;
+  d.geoph[d.ncell + e] = ymc / masel;
+  const double ma = d.Us[(1 * 6) * (size_t)d.ncell + e], mb = d.Us[(2 * 6) * (size_t)d.ncell + e];
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+  const double nrm = sqrt(ma * ma + mb * mb);
+  if (nrm > 1.0e-10) {
+    m0 = ma / nrm;
+    m2 = mb / nrm;
+    m1 = -mb / nrm;
+    m3 = ma / nrm;
+  }
+  d.mapmt[0 * (size_t)d.ncell + e] = m0;
+  d.mapmt[1 * (size_t)d.ncell + e] = m1;
+  d.mapmt[2 * (size_t)d.ncell + e] = m2;
+  d.mapmt[3 * (size_t)d.ncell + e] = m3;
+  if (fl) {
+#ifdef __CUDA_ARCH__
+    const int slot = atomicAdd(d.wcount, 1);
+#else
+    const int slot = (*d.wcount)++;
+#endif
+    d.wlist[slot] = iq;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Corner pass: node partial sums of the Riemann coefficients + sub-cell
+// density corrections (getriem_quadsubg2 with getrhosubg_averg/_daverg)
+// ---------------------------------------------------------------------------
+__host__ __device__ void f_corner(const Dev &d, int iq) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  double c[36], D[16];
+  {
+    double xp[9][2];
+    node_xy(L, xp);
+    cross36(xp, c);
+  }
+  detpoly(c, D);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double u[4][6];
+  load_u(d, d.Us, e, u);
+  const double rhoct = 1.0 / u[0][0];
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  // sub-cell densities: initial mass / exact sub-cell area, and the DG-implied
+  // harmonic mean of tau over each sub-cell (5x5 Gauss per sub-cell)
+  double corr[4], vsub4[4];
+  subareas(c, vsub4);
+#pragma unroll
+  for (int isg = 0; isg < 4; isg++) {
+    const double unksgq = (1.0 / vsub4[isg]) * d.msub[isg * (size_t)d.nquad + iq];
+    const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
+    const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
+    double masel = 0.0;
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) {
+      const double r = (g5p(i) + ofr) / 2.0;
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const double s = (g5p(j) + ofs) / 2.0;
+        const double tau = eval_taylor(u[0], G, r, s);
+        masel += (g5w(i) * g5w(j) * 0.25) * deteval(D, r, s) / tau;
+      }
+    }
+    const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
+    const double uqsgc = volel / masel;
+    corr[isg] = d.cdrho * (unksgq - 1.0 / uqsgc);
+    d.corr[isg * (size_t)d.nquad + iq] = corr[isg];
+  }
+  // per node: vertex state, then its corner faces in the reference's order
+#pragma unroll 1
+  for (int k = 0; k < 9; k++) {
+    double b[6];
+    node_basis2(G, k, b);
+    double st[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int kk = 0; kk < 6; kk++)
+        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
+      st[q] = acc;
+    }
+    const double rhovt = 1.0 / st[0];
+    const double ke = st[3] - 0.5 * (st[1] * st[1] + st[2] * st[2]);
+    const int pn = d.ipq[k * d.nquad + iq];
+    const double dux = d.us[pn] - st[1];
+    const double duy = d.vs[pn] - st[2];
+    double P0 = 0.0, P1 = 0.0, P2 = 0.0, P3 = 0.0, P4 = 0.0;
+#pragma unroll 1
+    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
+      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
+      const double ci = isg == 0 ? corr[0] : isg == 1 ? corr[1] : isg == 2 ? corr[2] : corr[3];
+      const double pv = fmax(eps, (g - 1.0) * (rhovt + ci) * ke);
+#pragma unroll
+      for (int f = 0; f < 2; f++) {
+        double n0, n1, a;
+        corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
+        const double aw = a * wrie(isg, ivsg, f);
+        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, n0, n1, aw);
+        P0 += m;
+        P1 += m * st[1];
+        P2 += m * st[2];
+        P3 += -pv * aw * n0;
+        P4 += -pv * aw * n1;
+      }
+    }
+    d.npart[(0 * 9 + k) * (size_t)d.nquad + iq] = P0;
+    d.npart[(1 * 9 + k) * (size_t)d.nquad + iq] = P1;
+    d.npart[(2 * 9 + k) * (size_t)d.nquad + iq] = P2;
+    d.npart[(3 * 9 + k) * (size_t)d.nquad + iq] = P3;
+    d.npart[(4 * 9 + k) * (size_t)d.nquad + iq] = P4;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Node pass: gather the per-cell partial sums in cell order, 2x2 solve and
+// wall conditions (getndvelo_lagsubg, Getrhslaggauss.f90:4465-4545)
+// ---------------------------------------------------------------------------
+__host__ __device__ void f_node(const Dev &d, int p) {
+  if (p >= d.npoin || d.sc_dev->done) return;
+  double mn = 0.0, mu0 = 0.0, mu1 = 0.0, sn0 = 0.0, sn1 = 0.0;
+  const int b = d.node_ptr2[p], en = d.node_ptr2[p + 1];
+  for (int i = b; i < en; i++) {
+    const int id = d.node_slot[i];
+    const int iq = id / 9, k = id - 9 * iq;
+    mn += d.npart[(0 * 9 + k) * (size_t)d.nquad + iq];
+    mu0 += d.npart[(1 * 9 + k) * (size_t)d.nquad + iq];
+    mu1 += d.npart[(2 * 9 + k) * (size_t)d.nquad + iq];
+    sn0 += d.npart[(3 * 9 + k) * (size_t)d.nquad + iq];
+    sn1 += d.npart[(4 * 9 + k) * (size_t)d.nquad + iq];
+  }
+  const unsigned char mask = d.bcmask[p];
+  double us = d.us[p], vs = d.vs[p];
+  if (!(mask & 4)) {
+    us = (mu0 - sn0) / mn;
+    vs = (mu1 - sn1) / mn;
+  }
+  if (mask & 1) us = 0.0;
+  if (mask & 2) vs = 0.0;
+  d.us_new[p] = us;
+  d.vs_new[p] = vs;
+}
+
+// ---------------------------------------------------------------------------
+// RHS pass: corner forces + face integral + volume integral (+ source), and
+// in stages 2 and 3 the M^-1 solve and RK combine
+// ---------------------------------------------------------------------------
+__host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double u[4][6];
+  load_u(d, d.Us, e, u);
+  const double rhoct = 1.0 / u[0][0];
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  double ul[6] = {0, 0, 0, 0, 0, 0}, p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
+  // face integral: corner forces F* = sigma.n A + m (u* - u_c), node by node
+#pragma unroll 1
+  for (int k = 0; k < 9; k++) {
+    double b[6];
+    node_basis2(G, k, b);
+    double st[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int kk = 0; kk < 6; kk++)
+        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
+      st[q] = acc;
+    }
+    const double rhovt = 1.0 / st[0];
+    const double ke = st[3] - 0.5 * (st[1] * st[1] + st[2] * st[2]);
+    const int pn = d.ipq[k * d.nquad + iq];
+    const double dux = d.us[pn] - st[1], duy = d.vs[pn] - st[2];
+    const double un = d.us_new[pn], vn = d.vs_new[pn];
+    const double du0 = un - st[1], du1 = vn - st[2];
+    double tw = 0.0, f0 = 0.0, f1 = 0.0, fe = 0.0;
+#pragma unroll 1
+    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
+      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
+      const double pv = fmax(eps, (g - 1.0) * (rhovt + d.corr[isg * (size_t)d.nquad + iq]) * ke);
+      const double wq = wmom(isg, ivsg);
+#pragma unroll
+      for (int f = 0; f < 2; f++) {
+        double n0, n1, a;
+        corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
+        const double aw = a * wrie(isg, ivsg, f);
+        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, n0, n1, aw);
+        const double fs0 = -pv * aw * n0 + m * du0;
+        const double fs1 = -pv * aw * n1 + m * du1;
+        tw += (un * n0 + vn * n1) * (a * wmas(isg, ivsg, f));
+        f0 += fs0 * wq;
+        f1 += fs1 * wq;
+        fe += (un * fs0 + vn * fs1) * wq;
+      }
+    }
+#pragma unroll
+    for (int kk = 0; kk < 6; kk++) {
+      ul[kk] += tw * b[kk];
+      p0[kk] += f0 * b[kk];
+      p1[kk] += f1 * b[kk];
+      el[kk] += fe * b[kk];
+    }
+  }
+  // volume integral on the 5x5 Gauss-Lobatto grid (cofactor form), sum
+  // factorised row by row: for fixed r_i, Q_b = sum_a L'_a(r_i) X[a][b] and
+  // P_b = sum_a L_a(r_i) X[a][b] give dx/dr and dx/ds along the row
+#pragma unroll 1
+  for (int i = 0; i < 5; i++) {
+    const double r = l5p(i), dr = r - G.rc;
+    double lr[3], dlr[3];
+    lag3(r, lr);
+    dlag3(r, dlr);
+    double Qx[3], Qy[3], Px[3], Py[3];
+#pragma unroll
+    for (int bb = 0; bb < 3; bb++) {
+      Qx[bb] = dlr[0] * L.X[0][bb] + dlr[1] * L.X[1][bb] + dlr[2] * L.X[2][bb];
+      Qy[bb] = dlr[0] * L.Y[0][bb] + dlr[1] * L.Y[1][bb] + dlr[2] * L.Y[2][bb];
+      Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
+      Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
+    }
+    const double wi = l5w(i);
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const double s = l5p(j), ds = s - G.sc;
+      double ls[3], dls[3];
+      lag3(s, ls);
+      dlag3(s, dls);
+      const double w = wi * l5w(j);
+      const double xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
+      const double yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
+      const double xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
+      const double ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
+      const double b3 = 0.5 * dr * dr - G.g19, b4 = 0.5 * ds * ds - G.g20, b5 = dr * ds - G.g21;
+      double un[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) un[q] = u[q][0] + u[q][1] * dr + u[q][2] * ds + u[q][3] * b3 + u[q][4] * b4 + u[q][5] * b5;
+      const double rhoad = 1.0 / un[0];
+      const double pres = fmax(eps, (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2])));
+      // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
+      double gd0[5], gd1[5];
+      gd0[0] = ys;       gd1[0] = -xs;
+      gd0[1] = -yr;      gd1[1] = xr;
+      gd0[2] = ys * dr;  gd1[2] = -xs * dr;
+      gd0[3] = -yr * ds; gd1[3] = xr * ds;
+      gd0[4] = ys * ds - yr * dr;
+      gd1[4] = -xs * ds + xr * dr;
+      const double wp = w * pres;
+#pragma unroll
+      for (int kk = 0; kk < 5; kk++) {
+        const double fv = gd0[kk] * un[1] + gd1[kk] * un[2];
+        ul[kk + 1] -= fv * w;
+        p0[kk + 1] += gd0[kk] * wp;
+        p1[kk + 1] += gd1[kk] * wp;
+        el[kk + 1] += fv * wp;
+      }
+    }
+  }
+  if (d.ncase == 1) {
+    // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:
+    // 4070-4251), 5x5 Gauss; cos(pi x) by cospi and cos(3t) = cos t (4 cos^2 t - 3)
+    double c[36], D[16];
+    {
+      double xp[9][2];
+      node_xy(L, xp);
+      cross36(xp, c);
+    }
+    detpoly(c, D);
+    const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) {
+      const double r = g5p(i), dr = r - G.rc;
+      double lr[3];
+      lag3(r, lr);
+      double Px[3], Py[3];
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
+        Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
+      }
+      const double wi = g5w(i);
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const double s = g5p(j), ds = s - G.sc;
+        double ls[3];
+        lag3(s, ls);
+        const double xg = Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2];
+        const double yg = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
+        const double djaco = wi * g5w(j) * deteval(D, r, s);
+        const double cx = cospi(xg), cy = cospi(yg);
+        const double c3x = cx * (4.0 * cx * cx - 3.0), c3y = cy * (4.0 * cy * cy - 3.0);
+        const double src = coef * (c3x * cy - c3y * cx) * djaco;
+        el[0] += src;
+        el[1] += src * dr;
+        el[2] += src * ds;
+        el[3] += src * (0.5 * dr * dr - G.g19);
+        el[4] += src * (0.5 * ds * ds - G.g20);
+        el[5] += src * (dr * ds - G.g21);
+      }
+    }
+  }
+  if (!fuse_update) {
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      d.rhs[(0 * 6 + k) * (size_t)d.ncell + e] = ul[k];
+      d.rhs[(1 * 6 + k) * (size_t)d.ncell + e] = p0[k];
+      d.rhs[(2 * 6 + k) * (size_t)d.ncell + e] = p1[k];
+      d.rhs[(3 * 6 + k) * (size_t)d.ncell + e] = el[k];
+    }
+    return;
+  }
+  // fused stage update (Getrhslag.f90:1789-1904)
+  const double dt = d.sc_dev->dtfix;
+  double am[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * (size_t)d.ncell + e];
+  double R[4][6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    R[0][k] = dt * ul[k];
+    R[1][k] = dt * p0[k];
+    R[2][k] = dt * p1[k];
+    R[3][k] = dt * el[k];
+  }
+  const double oma = 1.0 - alfa;
+  // symmetric 5x5 block rows from the packed upper triangle, M(1,1) = amatr(16)
+  const int IDX[5][5] = {{0, 1, 2, 3, 4}, {1, 5, 6, 7, 8}, {2, 6, 9, 10, 11}, {3, 7, 10, 12, 13}, {4, 8, 11, 13, 14}};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const size_t base = (size_t)(q * 6) * d.ncell + e;
+    const double d0 = am[15] * R[q][0];
+    d.Us[base] = alfa * d.Un[base] + oma * (u[q][0] + d0);
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < 5; j++) acc += am[IDX[i][j]] * R[q][j + 1];
+      const size_t idx = base + (size_t)(i + 1) * d.ncell;
+      d.Us[idx] = alfa * d.Un[idx] + oma * (u[q][i + 1] + acc);
+    }
+  }
+}
+
+// Stage update for stage 1 (the dt reduction sits between RHS and update)
+__host__ __device__ void f_update(const Dev &d, int e, double alfa) {
+  if (e >= d.ncell || d.sc_dev->done) return;
+  const double dt = d.sc_dev->dtfix;
+  double am[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * (size_t)d.ncell + e];
+  const double oma = 1.0 - alfa;
+  const int IDX[5][5] = {{0, 1, 2, 3, 4}, {1, 5, 6, 7, 8}, {2, 6, 9, 10, 11}, {3, 7, 10, 12, 13}, {4, 8, 11, 13, 14}};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    double R[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) R[k] = dt * d.rhs[(q * 6 + k) * (size_t)d.ncell + e];
+    const size_t base = (size_t)(q * 6) * d.ncell + e;
+    const double d0 = am[15] * R[0];
+    d.Us[base] = alfa * d.Un[base] + oma * (d.Us[base] + d0);
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < 5; j++) acc += am[IDX[i][j]] * R[j + 1];
+      const size_t idx = base + (size_t)(i + 1) * d.ncell;
+      d.Us[idx] = alfa * d.Un[idx] + oma * (d.Us[idx] + acc);
+    }
+  }
+}
+
+// Node motion with the new ustar, which becomes the previous ustar of the next stage
+__host__ __device__ void f_nodes(const Dev &d, int p, double alfa) {
+  if (p >= d.npoin || d.sc_dev->done) return;
+  const double dt = d.sc_dev->dtfix;
+  const double oma = 1.0 - alfa;
+  const double un = d.us_new[p], vn = d.vs_new[p];
+  d.xs[p] = alfa * d.xn[p] + oma * (d.xs[p] + dt * un);
+  d.ys[p] = alfa * d.yn[p] + oma * (d.ys[p] + dt * vn);
+  d.us[p] = un;
+  d.vs[p] = vn;
+}
+
+// Centre-node re-interpolation and the exact cell volume
+__host__ __device__ void f_geom(const Dev &d, int iq, int fix_centre) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  if (fix_centre) {
+    // X[1][1] is node 9; corners X[0|2][0|2], edge nodes X[1][0], X[2][1], X[1][2], X[0][1]
+    L.X[1][1] = -0.25 * (L.X[0][0] + L.X[2][0] + L.X[2][2] + L.X[0][2]) + 0.5 * (L.X[1][0] + L.X[2][1] + L.X[1][2] + L.X[0][1]);
+    L.Y[1][1] = -0.25 * (L.Y[0][0] + L.Y[2][0] + L.Y[2][2] + L.Y[0][2]) + 0.5 * (L.Y[1][0] + L.Y[2][1] + L.Y[1][2] + L.Y[0][1]);
+    const int pc = d.ipq[8 * d.nquad + iq];
+    d.xs[pc] = L.X[1][1];
+    d.ys[pc] = L.Y[1][1];
+  }
+  double c[36], D[16];
+  {
+    double xp[9][2];
+    node_xy(L, xp);
+    cross36(xp, c);
+  }
+  detpoly(c, D);
+  const double vol = cell_area(D);
+  d.vol[e] = vol;
+  if (!(vol > 0.0)) {
+#ifdef __CUDA_ARCH__
+    atomicOr(&d.sc_dev->status, ST_NONPHYS);
+#else
+    d.sc_dev->status |= ST_NONPHYS;
+#endif
+  }
+}
+
+// Time-invariant mass-weighted shape moments W_k = sum_g rho0 J0_g N_k(g)
+// (5x5 Gauss on the initial map) for the physical mass centre
+__host__ __device__ void f_init_wmom(const Dev &d, int iq) {
+  if (iq >= d.nquad) return;
+  Loaded L;
+  load_cell(d, d.x0, d.y0, iq, L);
+  double c[36], D[16];
+  {
+    double xp[9][2];
+    node_xy(L, xp);
+    cross36(xp, c);
+  }
+  detpoly(c, D);
+  // initial density of the reference cases is uniform per cell
+  double rho0 = 1.0;
+  if (d.ncase == 6) {
+    const double xc = L.X[1][1], yc = L.Y[1][1];
+    rho0 = (sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125;
+  }
+  double W[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) W[a][b] = 0.0;
+  for (int i = 0; i < 5; i++) {
+    double lr[3];
+    lag3(g5p(i), lr);
+    for (int j = 0; j < 5; j++) {
+      double ls[3];
+      lag3(g5p(j), ls);
+      const double w = rho0 * g5w(i) * g5w(j) * deteval(D, g5p(i), g5p(j));
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) W[a][b] += w * lr[a] * ls[b];
+    }
+  }
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  for (int k = 0; k < 9; k++) d.wmom[k * (size_t)d.nquad + iq] = W[A[k]][B[k]];
+}
+
+__global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(128, 3) k_corner2(Dev d) { f_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void k_node2(Dev d) { f_node(d, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(128) k_rhs2(Dev d, int fuse, double alfa) {
+  f_rhs(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa);
+}
+__global__ void k_update2(Dev d, double alfa) { f_update(d, blockIdx.x * blockDim.x + threadIdx.x, alfa); }
+__global__ void k_nodes2(Dev d, double alfa) { f_nodes(d, blockIdx.x * blockDim.x + threadIdx.x, alfa); }
+__global__ void k_geom2(Dev d, int fix) { f_geom(d, blockIdx.x * blockDim.x + threadIdx.x, fix); }
+__global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+static inline int nb(int n, int b) { return (n + b - 1) / b; }
+
+}  // namespace fast
+
+void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
+void launch_fast_corner(const Dev &d, cudaStream_t st) { fast::k_corner2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
+void launch_fast_node(const Dev &d, cudaStream_t st) { fast::k_node2<<<fast::nb(d.npoin, 256), 256, 0, st>>>(d); }
+void launch_fast_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa) {
+  fast::k_rhs2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d, fuse, alfa);
+}
+void launch_fast_update(const Dev &d, cudaStream_t st, double alfa) {
+  fast::k_update2<<<fast::nb(d.ncell, 256), 256, 0, st>>>(d, alfa);
+}
+void launch_fast_nodes(const Dev &d, cudaStream_t st, double alfa) {
+  fast::k_nodes2<<<fast::nb(d.npoin, 256), 256, 0, st>>>(d, alfa);
+}
+void launch_fast_geom(const Dev &d, cudaStream_t st, int fix) { fast::k_geom2<<<fast::nb(d.nquad, 256), 256, 0, st>>>(d, fix); }
+void launch_init_wmom(const Dev &d, cudaStream_t st) { fast::k_init_wmom<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
+
+}  // namespace lag2d

@@ -1,0 +1,560 @@
+// FP32-mixed corner and RHS passes of the curved-P2 Lagrangian DG stage.
+//
+// The same scheme as the FP64 passes of lag2d_fast.cu, with the precision
+// split of the mixed form:
+//   FP32  the bulk flux and quadrature arithmetic: DOF evaluation at nodes and
+//         quadrature points, sub-cell face normals, impedances and corner
+//         coefficients, the 100-point harmonic tau mean of the sub-cell
+//         densities, the 5x5 Gauss-Lobatto volume integral and the source
+//         quadrature, all accumulated in FP32;
+//   FP64  everything that decides mesh validity and conservation: node
+//         positions (read in FP64; FP32 geometry works on offsets from the
+//         cell's centre node, so it keeps FP32 precision relative to the cell
+//         size), the det J polynomial, cell and sub-cell volumes, the sub-cell
+//         density correction, the node partial sums and the nodal 2x2 solve
+//         (node pass of lag2d_fast.cu), the corner forces
+//         F* = sigma.n A + m (u* - u_c) and every cell-average (moment 0)
+//         contribution, the mass-matrix solve and the RK combine.
+// Both passes compute each corner's FP32 coefficients m, sigma.n A and the
+// vertex state with the same inline code from the same inputs, and the
+// corner forces are formed from them in FP64, so at every interior node the
+// corner forces of the surrounding cells cancel to FP64 rounding: momentum
+// and total energy are conserved to FP64 round-off, as in the FP64 step.
+// Storage (DOFs, M^-1, geometry, nodes) stays FP64.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "lag2d_device.cuh"
+#include "lag2d_fast_tables.h"
+
+namespace lag2d {
+
+namespace mixed {
+
+#include "lag2d_tables.inc"
+
+struct MixTables {
+  int nc_start[10];
+  int nc_entry[16];
+  int fnqsg[32];
+  float wrie[32];
+  float wmas[32];
+  float wmom[16];
+  int pa[12], pb[12], side[12];
+  float dl[9];
+  float xv[9], yv[9];
+};
+__constant__ MixTables cMT = LAG2D_FAST_TABLES;
+
+__device__ __forceinline__ void lag3f(float r, float *l) {
+  l[0] = 0.5f * r * (r - 1.0f);
+  l[1] = 1.0f - r * r;
+  l[2] = 0.5f * r * (r + 1.0f);
+}
+__device__ __forceinline__ void dlag3f(float r, float *l) {
+  l[0] = r - 0.5f;
+  l[1] = -2.0f * r;
+  l[2] = r + 0.5f;
+}
+
+__device__ __forceinline__ float detevalf(const float *D, float r, float s) {
+  float e[4];
+#pragma unroll
+  for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+  return e[0] + s * (e[1] + s * (e[2] + s * e[3]));
+}
+
+// integral of det J over the sub-square [r0, r0+1] x [s0, s0+1] (FP64)
+__device__ __forceinline__ double det_integral(const double *D, double r0, double s0) {
+  double mr[4], ms[4];
+  const double r1 = r0 + 1.0, s1 = s0 + 1.0;
+  double pr0 = r0, pr1 = r1, ps0 = s0, ps1 = s1;
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    mr[m] = (pr1 - pr0) / (m + 1);
+    ms[m] = (ps1 - ps0) / (m + 1);
+    pr0 *= r0; pr1 *= r1; ps0 *= s0; ps1 *= s1;
+  }
+  double v = 0.0;
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+#pragma unroll
+    for (int n = 0; n < 4; n++) v += D[4 * m + n] * mr[m] * ms[n];
+  return v;
+}
+
+// 5-point Gauss (ruqope) and Gauss-Lobatto (ruqope_lobatto) rules in FP32
+__device__ __forceinline__ float g5p(int i) {
+  const float p[5] = {-0.9061798459386640f, -0.5384693101056831f, 0.0f, 0.5384693101056831f, 0.9061798459386640f};
+  return p[i];
+}
+__device__ __forceinline__ float g5w(int i) {
+  const float w[5] = {0.2369268850561891f, 0.4786286704993665f, 0.5688888888888889f, 0.4786286704993665f,
+                      0.2369268850561891f};
+  return w[i];
+}
+__device__ __forceinline__ float l5p(int i) {
+  const float p[5] = {-1.0f, -0.6546536707079771f, 0.0f, 0.6546536707079771f, 1.0f};
+  return p[i];
+}
+__device__ __forceinline__ float l5w(int i) {
+  const float w[5] = {0.1f, 0.5444444444444444f, 0.7111111111111111f, 0.5444444444444444f, 0.1f};
+  return w[i];
+}
+
+struct GeoF {
+  float rc, sc, g19, g20, g21;
+};
+
+__device__ __forceinline__ void node_basis(const GeoF &g, int iv, float *b) {
+  b[0] = 1.0f;
+  b[1] = cMT.xv[iv] - g.rc;
+  b[2] = cMT.yv[iv] - g.sc;
+  b[3] = 0.5f * b[1] * b[1] - g.g19;
+  b[4] = 0.5f * b[2] * b[2] - g.g20;
+  b[5] = b[1] * b[2] - g.g21;
+}
+
+__device__ __forceinline__ float eval_taylor(const float *u, const GeoF &g, float r, float s) {
+  const float dr = r - g.rc, ds = s - g.sc;
+  return u[0] + u[1] * dr + u[2] * ds + u[3] * (0.5f * dr * dr - g.g19) + u[4] * (0.5f * ds * ds - g.g20) +
+         u[5] * (dr * ds - g.g21);
+}
+
+// unit normal (n0, n1) and length a of gesgq slot `slot` (getfnds_lagsms_simpsonhybrid)
+__device__ __forceinline__ void slot_normal(const float X[3][3], const float Y[3][3], int slot, float &n0, float &n1,
+                                            float &a) {
+  float anx, any;
+  if (slot >= 8 && slot < 12) {
+    // inner sub-cell face from edge node (5..8) towards the centre
+    const int f = slot - 8;
+    const float lm0 = 0.375f, lm1 = 0.75f, lm2 = -0.125f, lp0 = -0.125f, lp1 = 0.75f, lp2 = 0.375f;
+    float ex, ey, vx, vy;
+    if (f == 0) {
+      ex = X[1][0]; ey = Y[1][0];
+      vx = lm0 * X[1][0] + lm1 * X[1][1] + lm2 * X[1][2];
+      vy = lm0 * Y[1][0] + lm1 * Y[1][1] + lm2 * Y[1][2];
+    } else if (f == 1) {
+      ex = X[2][1]; ey = Y[2][1];
+      vx = lp0 * X[0][1] + lp1 * X[1][1] + lp2 * X[2][1];
+      vy = lp0 * Y[0][1] + lp1 * Y[1][1] + lp2 * Y[2][1];
+    } else if (f == 2) {
+      ex = X[1][2]; ey = Y[1][2];
+      vx = lp0 * X[1][0] + lp1 * X[1][1] + lp2 * X[1][2];
+      vy = lp0 * Y[1][0] + lp1 * Y[1][1] + lp2 * Y[1][2];
+    } else {
+      ex = X[0][1]; ey = Y[0][1];
+      vx = lm0 * X[0][1] + lm1 * X[1][1] + lm2 * X[2][1];
+      vy = lm0 * Y[0][1] + lm1 * Y[1][1] + lm2 * Y[2][1];
+    }
+    const float dxdr = -1.5f * ex - 0.5f * X[1][1] + 2.0f * vx;
+    const float dydr = -1.5f * ey - 0.5f * Y[1][1] + 2.0f * vy;
+    anx = -dydr;
+    any = dxdr;
+  } else {
+    const int ig = slot < 8 ? slot : slot - 4;
+    const int ia = cMT.pa[ig], ib = cMT.pb[ig];
+    const float *da = cMT.dl + 3 * ia, *db = cMT.dl + 3 * ib;
+    float xa0, xa1, xa2, ya0, ya1, ya2, xb0, xb1, xb2, yb0, yb1, yb2;
+    if (ib == 0) { xa0 = X[0][0]; xa1 = X[1][0]; xa2 = X[2][0]; ya0 = Y[0][0]; ya1 = Y[1][0]; ya2 = Y[2][0]; }
+    else if (ib == 1) { xa0 = X[0][1]; xa1 = X[1][1]; xa2 = X[2][1]; ya0 = Y[0][1]; ya1 = Y[1][1]; ya2 = Y[2][1]; }
+    else { xa0 = X[0][2]; xa1 = X[1][2]; xa2 = X[2][2]; ya0 = Y[0][2]; ya1 = Y[1][2]; ya2 = Y[2][2]; }
+    if (ia == 0) { xb0 = X[0][0]; xb1 = X[0][1]; xb2 = X[0][2]; yb0 = Y[0][0]; yb1 = Y[0][1]; yb2 = Y[0][2]; }
+    else if (ia == 1) { xb0 = X[1][0]; xb1 = X[1][1]; xb2 = X[1][2]; yb0 = Y[1][0]; yb1 = Y[1][1]; yb2 = Y[1][2]; }
+    else { xb0 = X[2][0]; xb1 = X[2][1]; xb2 = X[2][2]; yb0 = Y[2][0]; yb1 = Y[2][1]; yb2 = Y[2][2]; }
+    const float xr = da[0] * xa0 + da[1] * xa1 + da[2] * xa2;
+    const float yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
+    const float xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
+    const float ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
+    switch (cMT.side[ig]) {
+      case 0: anx = yr; any = -xr; break;
+      case 1: anx = ys; any = -xs; break;
+      case 2: anx = -yr; any = xr; break;
+      default: anx = -ys; any = xs; break;
+    }
+  }
+  const float n2 = anx * anx + any * any;
+  const float inv = rsqrtf(n2);
+  n0 = anx * inv;
+  n1 = any * inv;
+  a = 2.0f * n2 * inv;
+}
+
+__device__ __forceinline__ void corner_face(const float X[3][3], const float Y[3][3], int isg, int ivsg, int f,
+                                            float &n0, float &n1, float &a) {
+  const int code = cMT.fnqsg[8 * isg + 2 * ivsg + f];
+  const int slot = (code >= 0 ? code : -code) - 1;
+  slot_normal(X, Y, slot, n0, n1, a);
+  if (code < 0) { n0 = -n0; n1 = -n1; }
+}
+
+// m = mu * A of one corner face (getriecoef_matrixnew, Limiterlag.f90:1037);
+// the jump-direction branch needs |u* - u_c| >= 1e12 c
+__device__ __forceinline__ float corner_m(float rhoct, float sdctr, float cimpd, float slpdu, float dux, float duy,
+                                          float n0, float n1, float a) {
+  const float deltu = fabsf(dux * n0 + duy * n1);
+  const float murie = rhoct * sdctr + cimpd * rhoct * slpdu * deltu;
+  const float j2 = dux * dux + duy * duy;
+  if (j2 * 1.0e-24f < sdctr * sdctr) return murie * a;
+  const float inv = rsqrtf(j2);
+  return murie * a * fabsf((n0 * dux + n1 * duy) * inv);
+}
+
+// node coordinates of quad iq: FP64 centre node, FP32 offsets from it on the 3x3 tensor
+struct CellXY {
+  double ox, oy;
+  float X[3][3], Y[3][3];
+  double c[36];  // cross products of the FP64 offsets (det J, volumes)
+};
+
+__device__ __forceinline__ void load_cell(const Dev &d, int iq, CellXY &L) {
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  double xp[9][2];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const int p = d.ipq[k * d.nquad + iq];
+    xp[k][0] = d.xs[p];
+    xp[k][1] = d.ys[p];
+  }
+  L.ox = xp[8][0];
+  L.oy = xp[8][1];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    xp[k][0] -= L.ox;
+    xp[k][1] -= L.oy;
+    L.X[A[k]][B[k]] = (float)xp[k][0];
+    L.Y[A[k]][B[k]] = (float)xp[k][1];
+  }
+  cross36(xp, L.c);
+}
+
+__device__ __forceinline__ void load_u(const Dev &d, int e, float u[4][6]) {
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < 6; k++) u[q][k] = (float)d.Us[(q * 6 + k) * (size_t)d.ncell + e];
+}
+
+// cell-centre sound speed and 1/tau (getriem_quadsubg2)
+__device__ __forceinline__ void centre_state(const float u[4][6], float g, float &rhoct, float &sdctr) {
+  const float eps = 1.0e-6f;
+  rhoct = 1.0f / u[0][0];
+  const float pctr = fmaxf(eps, (g - 1.0f) * rhoct * (u[3][0] - 0.5f * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
+  sdctr = sqrtf(fmaxf(eps, g * pctr / rhoct));
+}
+
+// vertex state of node k: (tau, u, v, e) from the first mdegr Taylor modes
+__device__ __forceinline__ void vertex_state(const float u[4][6], const float *b, int mdegr, float st[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int kk = 0; kk < 6; kk++)
+      if (kk < mdegr) acc += u[q][kk] * b[kk];
+    st[q] = acc;
+  }
+}
+
+// FP32 coefficients of one corner face: m and sigma.n A (sx, sy)
+__device__ __forceinline__ void corner_coeffs(const CellXY &L, int isg, int ivsg, int f, float pv, float rhoct,
+                                              float sdctr, float cimpd, float slpdu, float dux, float duy, float &m,
+                                              float &sx, float &sy, float &n0, float &n1, float &a) {
+  corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
+  const float aw = a * cMT.wrie[8 * isg + 2 * ivsg + f];
+  m = corner_m(rhoct, sdctr, cimpd, slpdu, dux, duy, n0, n1, aw);
+  sx = -pv * aw * n0;
+  sy = -pv * aw * n1;
+}
+
+// ---------------------------------------------------------------------------
+// Corner pass (getriem_quadsubg2 with getrhosubg_averg/_daverg)
+// ---------------------------------------------------------------------------
+__device__ void m_corner(const Dev &d, int iq) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  const float eps = 1.0e-6f, g = (float)d.gamlg, slpdu = (g + 1.0f) / 2.0f, cimpd = (float)d.cimpd;
+  CellXY L;
+  load_cell(d, iq, L);
+  double D[16];
+  detpoly(L.c, D);
+  float Df[16];
+#pragma unroll
+  for (int t = 0; t < 16; t++) Df[t] = (float)D[t];
+  const GeoF G{(float)d.rc[e], (float)d.sc[e], (float)d.g19[e], (float)d.g20[e], (float)d.g21[e]};
+  float u[4][6];
+  load_u(d, e, u);
+  float rhoct, sdctr;
+  centre_state(u, g, rhoct, sdctr);
+  // sub-cell densities: initial mass / exact sub-cell area (FP64) against the
+  // DG-implied harmonic tau mean (FP32 5x5 Gauss per sub-cell)
+  double vsub4[4];
+  subareas(L.c, vsub4);
+  float corr[4];
+#pragma unroll
+  for (int isg = 0; isg < 4; isg++) {
+    const double unksgq = d.msub[isg * (size_t)d.nquad + iq] / vsub4[isg];
+    const float ofr = (isg == 0 || isg == 3) ? -1.0f : 1.0f;
+    const float ofs = (isg == 0 || isg == 1) ? -1.0f : 1.0f;
+    float masel = 0.0f;
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) {
+      const float r = (g5p(i) + ofr) * 0.5f;
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const float s = (g5p(j) + ofs) * 0.5f;
+        const float tau = eval_taylor(u[0], G, r, s);
+        masel += (g5w(i) * g5w(j) * 0.25f) * __fdividef(detevalf(Df, r, s), tau);
+      }
+    }
+    const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
+    const double cr = d.cdrho * (unksgq - (double)masel / volel);
+    d.corr[isg * (size_t)d.nquad + iq] = cr;
+    corr[isg] = (float)cr;
+  }
+#pragma unroll 1
+  for (int k = 0; k < 9; k++) {
+    float b[6], st[4];
+    node_basis(G, k, b);
+    vertex_state(u, b, d.mdegr, st);
+    const float rhovt = 1.0f / st[0];
+    const float ke = st[3] - 0.5f * (st[1] * st[1] + st[2] * st[2]);
+    const int pn = d.ipq[k * d.nquad + iq];
+    const float dux = (float)d.us[pn] - st[1];
+    const float duy = (float)d.vs[pn] - st[2];
+    double P0 = 0.0, P1 = 0.0, P2 = 0.0, P3 = 0.0, P4 = 0.0;
+#pragma unroll 1
+    for (int i = cMT.nc_start[k]; i < cMT.nc_start[k + 1]; i++) {
+      const int isg = cMT.nc_entry[i] >> 2, ivsg = cMT.nc_entry[i] & 3;
+      const float ci = isg == 0 ? corr[0] : isg == 1 ? corr[1] : isg == 2 ? corr[2] : corr[3];
+      const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
+#pragma unroll
+      for (int f = 0; f < 2; f++) {
+        float m, sx, sy, n0, n1, a;
+        corner_coeffs(L, isg, ivsg, f, pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy, n0, n1, a);
+        P0 += (double)m;
+        P1 += (double)m * (double)st[1];
+        P2 += (double)m * (double)st[2];
+        P3 += (double)sx;
+        P4 += (double)sy;
+      }
+    }
+    d.npart[(0 * 9 + k) * (size_t)d.nquad + iq] = P0;
+    d.npart[(1 * 9 + k) * (size_t)d.nquad + iq] = P1;
+    d.npart[(2 * 9 + k) * (size_t)d.nquad + iq] = P2;
+    d.npart[(3 * 9 + k) * (size_t)d.nquad + iq] = P3;
+    d.npart[(4 * 9 + k) * (size_t)d.nquad + iq] = P4;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RHS pass: face integral with FP64 corner forces, FP32 volume integral and
+// source, FP64 moment 0; in stages 2 and 3 the FP64 M^-1 solve and RK combine
+// ---------------------------------------------------------------------------
+__device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  const float eps = 1.0e-6f, g = (float)d.gamlg, slpdu = (g + 1.0f) / 2.0f, cimpd = (float)d.cimpd;
+  CellXY L;
+  load_cell(d, iq, L);
+  const GeoF G{(float)d.rc[e], (float)d.sc[e], (float)d.g19[e], (float)d.g20[e], (float)d.g21[e]};
+  float u[4][6];
+  load_u(d, e, u);
+  float rhoct, sdctr;
+  centre_state(u, g, rhoct, sdctr);
+  double ul0 = 0.0, pa0 = 0.0, pb0 = 0.0, el0 = 0.0;  // cell-average contributions
+  float ul[6] = {0, 0, 0, 0, 0, 0}, p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+  for (int k = 0; k < 9; k++) {
+    float b[6], st[4];
+    node_basis(G, k, b);
+    vertex_state(u, b, d.mdegr, st);
+    const float rhovt = 1.0f / st[0];
+    const float ke = st[3] - 0.5f * (st[1] * st[1] + st[2] * st[2]);
+    const int pn = d.ipq[k * d.nquad + iq];
+    const float dux = (float)d.us[pn] - st[1];
+    const float duy = (float)d.vs[pn] - st[2];
+    const double un = d.us_new[pn], vn = d.vs_new[pn];
+    const double du0 = un - (double)st[1], du1 = vn - (double)st[2];
+    double tw = 0.0, f0 = 0.0, f1 = 0.0, fe = 0.0;
+#pragma unroll 1
+    for (int i = cMT.nc_start[k]; i < cMT.nc_start[k + 1]; i++) {
+      const int isg = cMT.nc_entry[i] >> 2, ivsg = cMT.nc_entry[i] & 3;
+      const float ci = (float)d.corr[isg * (size_t)d.nquad + iq];
+      const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
+      const double wq = (double)cMT.wmom[4 * isg + ivsg];
+#pragma unroll
+      for (int f = 0; f < 2; f++) {
+        float m, sx, sy, n0, n1, a;
+        corner_coeffs(L, isg, ivsg, f, pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy, n0, n1, a);
+        const double fs0 = (double)sx + (double)m * du0;
+        const double fs1 = (double)sy + (double)m * du1;
+        tw += (un * (double)n0 + vn * (double)n1) * (double)(a * cMT.wmas[8 * isg + 2 * ivsg + f]);
+        f0 += fs0 * wq;
+        f1 += fs1 * wq;
+        fe += (un * fs0 + vn * fs1) * wq;
+      }
+    }
+    ul0 += tw;
+    pa0 += f0;
+    pb0 += f1;
+    el0 += fe;
+    const float twf = (float)tw, f0f = (float)f0, f1f = (float)f1, fef = (float)fe;
+#pragma unroll
+    for (int kk = 1; kk < 6; kk++) {
+      ul[kk] += twf * b[kk];
+      p0[kk] += f0f * b[kk];
+      p1[kk] += f1f * b[kk];
+      el[kk] += fef * b[kk];
+    }
+  }
+  // volume integral, 5x5 Gauss-Lobatto, cofactor form, sum-factorised rows
+#pragma unroll 1
+  for (int i = 0; i < 5; i++) {
+    const float r = l5p(i), dr = r - G.rc;
+    float lr[3], dlr[3];
+    lag3f(r, lr);
+    dlag3f(r, dlr);
+    float Qx[3], Qy[3], Px[3], Py[3];
+#pragma unroll
+    for (int bb = 0; bb < 3; bb++) {
+      Qx[bb] = dlr[0] * L.X[0][bb] + dlr[1] * L.X[1][bb] + dlr[2] * L.X[2][bb];
+      Qy[bb] = dlr[0] * L.Y[0][bb] + dlr[1] * L.Y[1][bb] + dlr[2] * L.Y[2][bb];
+      Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
+      Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
+    }
+    const float wi = l5w(i);
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const float s = l5p(j), ds = s - G.sc;
+      float ls[3], dls[3];
+      lag3f(s, ls);
+      dlag3f(s, dls);
+      const float w = wi * l5w(j);
+      const float xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
+      const float yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
+      const float xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
+      const float ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
+      const float b3 = 0.5f * dr * dr - G.g19, b4 = 0.5f * ds * ds - G.g20, b5 = dr * ds - G.g21;
+      float un[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) un[q] = u[q][0] + u[q][1] * dr + u[q][2] * ds + u[q][3] * b3 + u[q][4] * b4 + u[q][5] * b5;
+      const float rhoad = 1.0f / un[0];
+      const float pres = fmaxf(eps, (g - 1.0f) * rhoad * (un[3] - 0.5f * (un[1] * un[1] + un[2] * un[2])));
+      float gd0[5], gd1[5];
+      gd0[0] = ys;       gd1[0] = -xs;
+      gd0[1] = -yr;      gd1[1] = xr;
+      gd0[2] = ys * dr;  gd1[2] = -xs * dr;
+      gd0[3] = -yr * ds; gd1[3] = xr * ds;
+      gd0[4] = ys * ds - yr * dr;
+      gd1[4] = -xs * ds + xr * dr;
+      const float wp = w * pres;
+#pragma unroll
+      for (int kk = 0; kk < 5; kk++) {
+        const float fv = gd0[kk] * un[1] + gd1[kk] * un[2];
+        ul[kk + 1] -= fv * w;
+        p0[kk + 1] += gd0[kk] * wp;
+        p1[kk + 1] += gd1[kk] * wp;
+        el[kk + 1] += fv * wp;
+      }
+    }
+  }
+  if (d.ncase == 1) {
+    // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:4070-4251)
+    double D[16];
+    detpoly(L.c, D);
+    float Df[16];
+#pragma unroll
+    for (int t = 0; t < 16; t++) Df[t] = (float)D[t];
+    const float coef = (float)(0.25 * 3.14159265358979311599796346854 / (d.gamlg - 1.0));
+    const float oxf = (float)L.ox, oyf = (float)L.oy;
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) {
+      const float r = g5p(i), dr = r - G.rc;
+      float lr[3];
+      lag3f(r, lr);
+      float Px[3], Py[3];
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
+        Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
+      }
+      const float wi = g5w(i);
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const float s = g5p(j), ds = s - G.sc;
+        float ls[3];
+        lag3f(s, ls);
+        const float xg = oxf + (Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2]);
+        const float yg = oyf + (Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2]);
+        const float djaco = wi * g5w(j) * detevalf(Df, r, s);
+        const float cx = cospif(xg), cy = cospif(yg);
+        const float c3x = cx * (4.0f * cx * cx - 3.0f), c3y = cy * (4.0f * cy * cy - 3.0f);
+        const float src = coef * (c3x * cy - c3y * cx) * djaco;
+        el0 += (double)src;
+        el[1] += src * dr;
+        el[2] += src * ds;
+        el[3] += src * (0.5f * dr * dr - G.g19);
+        el[4] += src * (0.5f * ds * ds - G.g20);
+        el[5] += src * (dr * ds - G.g21);
+      }
+    }
+  }
+  double R[4][6];
+  R[0][0] = ul0;
+  R[1][0] = pa0;
+  R[2][0] = pb0;
+  R[3][0] = el0;
+#pragma unroll
+  for (int k = 1; k < 6; k++) {
+    R[0][k] = (double)ul[k];
+    R[1][k] = (double)p0[k];
+    R[2][k] = (double)p1[k];
+    R[3][k] = (double)el[k];
+  }
+  if (!fuse_update) {
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int k = 0; k < 6; k++) d.rhs[(q * 6 + k) * (size_t)d.ncell + e] = R[q][k];
+    return;
+  }
+  // fused stage update in FP64 (Getrhslag.f90:1789-1904)
+  const double dt = d.sc_dev->dtfix;
+  double am[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * (size_t)d.ncell + e];
+  const double oma = 1.0 - alfa;
+  const int IDX[5][5] = {{0, 1, 2, 3, 4}, {1, 5, 6, 7, 8}, {2, 6, 9, 10, 11}, {3, 7, 10, 12, 13}, {4, 8, 11, 13, 14}};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const size_t base = (size_t)(q * 6) * d.ncell + e;
+    d.Us[base] = alfa * d.Un[base] + oma * (d.Us[base] + am[15] * (dt * R[q][0]));
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < 5; j++) acc += am[IDX[i][j]] * (dt * R[q][j + 1]);
+      const size_t idx = base + (size_t)(i + 1) * d.ncell;
+      d.Us[idx] = alfa * d.Un[idx] + oma * (d.Us[idx] + acc);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_corner_mx(Dev d) { m_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(128) k_rhs_mx(Dev d, int fuse, double alfa) {
+  m_rhs(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa);
+}
+
+static inline int nb(int n, int b) { return (n + b - 1) / b; }
+
+}  // namespace mixed
+
+void launch_mixed_corner(const Dev &d, cudaStream_t st) {
+  mixed::k_corner_mx<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d);
+}
+void launch_mixed_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa) {
+  mixed::k_rhs_mx<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d, fuse, alfa);
+}
+
+}  // namespace lag2d

@@ -1,0 +1,33 @@
+"""Run a few time steps of a named workload, for profilers (ncu) and quick checks.
+
+    python -m lag2d_b200.profile_step tgv256 2            # FP64 step
+    python -m lag2d_b200.profile_step tgv256 2 --mixed    # FP32-mixed step
+
+Each step is one lag2d_step call (no graph), so every kernel launch of the
+step is visible to a profiler in launch order.
+"""
+from __future__ import annotations
+
+import argparse
+
+from .api import Lag2DSolver
+from .config import workload
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("workload", nargs="?", default="tgv256")
+    ap.add_argument("steps", nargs="?", type=int, default=2)
+    ap.add_argument("--mixed", action="store_true", help="FP32-mixed form (precision = 1)")
+    a = ap.parse_args()
+    m, c = workload(a.workload)
+    s = Lag2DSolver(m, c, precision=1 if a.mixed else 0)
+    s.init_fields()
+    for _ in range(a.steps):
+        s.step()
+    print(f"ok {a.workload} steps={a.steps} mixed={a.mixed} dtfix={s.dtfix:.6e} tacru={s.tacru:.6e}")
+    s.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -41,15 +41,20 @@ def test_create_validates_arguments_without_device():
     coold = np.ascontiguousarray(m.coord)
     mm = api._Mesh(m.ntria, m.nquad, m.npoin, m.nbfac, *[api._p(a, api._ip) for a in k], api._p(coold, api._dp))
     cc = api._Cfg(c.npoly, c.ndegr, c.mdegr, c.nq, c.nstag, c.ndt, c.ncase, c.nlimi, c.ndens, c.ngausd,
-                  c.ngausd_geo, 0, 0, (ctypes.c_int * 4)(), c.gamlg, c.cfl, c.cdrho, c.cimpd, c.tend,
+                  c.ngausd_geo, 0, 0, 0, (ctypes.c_int * 4)(), c.gamlg, c.cfl, c.cdrho, c.cimpd, c.tend,
                   c.sedov_energy)
     assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
-    # unsupported configurations are reported as such
-    cc.precision = 1
+    # invalid and unsupported configurations are reported as such
     k[1] = np.ascontiguousarray(m.ipqua, dtype=np.int32)
     mm.ipqua = api._p(k[1], api._ip)
+    cc.precision = 2
+    assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
+    cc.precision, cc.order_exact = 1, 1      # the reference-order kernels are FP64 only
+    assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
+    cc.precision, cc.order_exact = 0, 0
+    cc.npoly, cc.ndegr = 1, 3                # the linear P1 chain is not on this path
     assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 3
-    cc.precision = 0
+    cc.npoly, cc.ndegr = c.npoly, c.ndegr
     cc.nstag = 4
     assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
     del s

@@ -1,9 +1,13 @@
 """Parity of the CUDA path (through the C-ABI) against the CPU oracle.
 
-Tolerances: the production build contracts multiply-adds into FMA, so it is
-compared to the oracle at 1e-12 relative (cell averages) / 1e-10 (all
-moments, scaled by the field's magnitude); the --fmad=false build must agree
-to 1e-14.
+Two GPU configurations are checked:
+  * the production path (optimised kernels, FMA contraction): cell averages
+    within 1e-12 relative of the oracle after every step; single-stage RHS
+    within 1e-8 of the field scale (the tau RHS is a near-cancelling sum, so
+    its relative error is the rounding of the terms amplified by ~1e4);
+  * the reference-order kernels in the --fmad=false build: bit-identical to
+    the oracle except where CUDA's cos and the host libm's cos round
+    differently (the Taylor-Green source), within 1e-14 of the field scale.
 """
 import numpy as np
 import pytest
@@ -63,23 +67,30 @@ def test_rhs_single(name, exact):
     ustar = np.zeros_like(coord)
     # a few oracle steps to get a non-trivial state with motion and ustar
     o.run(unkno, coord, m.coord, geoel, amatr, ustar, 1, 3, c.dtfix, 0.0)
-    s = Lag2DSolver(m, c, exact=exact)
+    s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
     s.set_state(unkno, coord, ustar, geoel, amatr)
     r2, f2 = s.rhs(itime=4)
     u_gpu, _, us_gpu, _ = s.get_state()
     u1, us1, g1 = unkno.copy(), ustar.copy(), geoel.copy()
     r1, f1 = o.rhs(us1, u1, g1, coord, m.coord, amatr, 4)
     assert (f1 == f2).all()
-    tol = 1e-14 if exact else 1e-11
-    assert _field_err(r2, r1).max() < tol * 10
-    assert np.abs(us_gpu - us1).max() / np.abs(us1).max() < tol * 10
-    assert _field_err(u_gpu[:m.ncell], u1[:m.ncell]).max() < tol * 10
+    if exact:
+        if c.ncase != 1:
+            assert np.array_equal(r2, r1) and np.array_equal(us_gpu, us1)
+            assert np.array_equal(u_gpu[:m.ncell], u1[:m.ncell])
+        assert _field_err(r2, r1).max() < 1e-14
+        assert np.abs(us_gpu - us1).max() / np.abs(us1).max() < 1e-14
+        return
+    tol = 1e-8
+    assert _field_err(r2, r1).max() < tol
+    assert np.abs(us_gpu - us1).max() / np.abs(us1).max() < 1e-12
+    assert _field_err(u_gpu[:m.ncell], u1[:m.ncell]).max() < 1e-12
 
 
-@pytest.mark.parametrize("name,nsteps", [("tgv16", 10), ("sedov16", 12)])
-def test_steps_parity(name, nsteps):
+@pytest.mark.parametrize("name,nsteps,ordex", [("tgv16", 10, False), ("sedov16", 12, False), ("sedov16", 6, True)])
+def test_steps_parity(name, nsteps, ordex):
     m, c, o, geoel, amatr, unkno = _setup(name)
-    s = Lag2DSolver(m, c)
+    s = Lag2DSolver(m, c, exact=ordex, order_exact=ordex)
     s.init_fields()
     s.set_state(unkno, m.coord, np.zeros_like(m.coord), geoel, amatr)
     coord = m.coord.copy()
@@ -96,6 +107,8 @@ def test_steps_parity(name, nsteps):
         err_avg_abs = np.abs(u2[:n, :, 0] - unkno[:n, :, 0]) / np.abs(unkno[:n, :, 0]).max(axis=0)
         assert np.minimum(err_avg, err_avg_abs).max() < AVG_TOL, (it, np.minimum(err_avg, err_avg_abs).max())
         assert np.abs(x2 - coord).max() < 1e-13
+        if ordex:
+            assert np.array_equal(u2[:n], unkno[:n]) and np.array_equal(x2, coord)
 
 
 def test_run_matches_step():
