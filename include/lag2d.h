@@ -132,6 +132,47 @@ long long lag2d_kernel_launches(const lag2d_handle *h);
 int lag2d_timing(lag2d_handle *h, int enable);
 double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *launches);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free time-step size.  No counterpart in the reference: it is an
+ * addition of this library, computing what getdelt_lag (Getrhslag.f90:
+ * 20600-20716) computes, for callers that cannot allocate device memory.
+ *
+ * Which callers need it: every other entry point works on a handle whose
+ * device buffers lag2d_create allocated.  A host code that owns a fixed
+ * device arena and forbids the CUDA allocator after start-up, a step loop
+ * that must not synchronise the device (cudaMalloc and cudaFree may), or a
+ * caller that keeps its state in device memory in the reference's layouts
+ * and has no handle, can call this one: it calls no cudaMalloc, cudaFree or
+ * other allocating routine.  Its only scratch (per-block minima of the
+ * reduction) is a fixed array in the library's own device memory, sized for
+ * LAG2D_DELT_NOALLOC_MAX_QUADS quads (256 KiB); larger meshes are rejected
+ * with LAG2D_EINVAL.  Nothing in that scratch has to start at zero.
+ *
+ * Arguments: ntria, nquad, npoin, ndegr, nq, ngeel are the reference's
+ * dimensions; every array is a DEVICE pointer in the reference's layout:
+ * ipqua(9,nquad) 1-based, unkno(ndegr,nq,nsize) (the stage-1 state after
+ * limiting), geoel(ngeel,nsize) (geoel(3,:) = cell volume), coord(2,npoin)
+ * (positions at the start of the step), dvdt(ncell) = rhsel(1,1,:) of stage
+ * 1.  itime == 1 gives dtfix = min(cfl dtcfl, 0.1 dtvol); otherwise the
+ * previous *dtfix also bounds it by 1.01 dtfix.  dtfix is a device pointer
+ * (in/out); it receives NaN if a node id lies outside 1..npoin.  ndens
+ * selects how unkno(1,1,:) is read (1: tau, 2/3: density).  The work is
+ * queued on `stream` (a cudaStream_t; NULL = the default stream) and the call
+ * returns without synchronising.
+ *
+ * Set-up: the first call on each device (with that device current) looks up
+ * the scratch address and loads the kernels; make one call per device before
+ * any stream capture begins.  Concurrency: the scratch is one array per
+ * device, so calls that may overlap on the same device (different streams or
+ * host threads with no order between them) race and give wrong results:
+ * serialise them.
+ * ------------------------------------------------------------------------- */
+#define LAG2D_DELT_NOALLOC_MAX_QUADS 4194304
+int lag2d_delt_noalloc(int ntria, int nquad, int npoin, int ndegr, int nq, int ngeel,
+                       const int *ipqua, const double *unkno, const double *geoel,
+                       const double *coord, const double *dvdt, int itime, int ndens,
+                       double gamlg, double cfl, double *dtfix, void *stream);
+
 void lag2d_destroy(lag2d_handle *h);
 const char *lag2d_last_error(void);
 

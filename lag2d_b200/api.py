@@ -64,7 +64,8 @@ _libs = {}
 
 EXPORTS = ("lag2d_create", "lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run",
            "lag2d_get_state", "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_stream",
-           "lag2d_kernel_launches", "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error")
+           "lag2d_kernel_launches", "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error",
+           "lag2d_delt_noalloc")
 
 
 def library_path(exact: bool = False) -> str:

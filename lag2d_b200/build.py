@@ -14,7 +14,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", f) for f in ("lag2d_kernels.cu", "lag2d_fast.cu", "lag2d_mixed.cu", "lag2d_capi.cu")]
+SRC = [os.path.join(HERE, "csrc", f) for f in ("lag2d_kernels.cu", "lag2d_fast.cu", "lag2d_mixed.cu", "lag2d_capi.cu", "lag2d_noalloc.cu")]
 OUT_DIR = os.path.join(HERE, "_lib")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
