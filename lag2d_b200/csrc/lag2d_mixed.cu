@@ -2,19 +2,22 @@
 //
 // The same scheme as the FP64 passes of lag2d_fast.cu, with the precision
 // split of the mixed form:
-//   FP32  the bulk flux and quadrature arithmetic: DOF evaluation at nodes and
-//         quadrature points, sub-cell face normals, impedances and corner
-//         coefficients, the 100-point harmonic tau mean of the sub-cell
-//         densities, the 5x5 Gauss-Lobatto volume integral and the source
-//         quadrature, all accumulated in FP32;
+//   FP32  the bulk flux and quadrature arithmetic of the momentum and energy
+//         equations: vertex states, impedances and corner coefficients, the
+//         100-point harmonic tau mean of the sub-cell densities, pressure and
+//         the momentum/energy terms of the 5x5 Gauss-Lobatto volume integral,
+//         the source quadrature, all accumulated in FP32;
 //   FP64  everything that decides mesh validity and conservation: node
-//         positions (read in FP64; FP32 geometry works on offsets from the
-//         cell's centre node, so it keeps FP32 precision relative to the cell
-//         size), the det J polynomial, cell and sub-cell volumes, the sub-cell
-//         density correction, the node partial sums and the nodal 2x2 solve
-//         (node pass of lag2d_fast.cu), the corner forces
-//         F* = sigma.n A + m (u* - u_c) and every cell-average (moment 0)
-//         contribution, the mass-matrix solve and the RK combine.
+//         positions (geometry works on FP64 offsets from the cell's centre
+//         node), sub-cell face normals and Jacobians, the det J polynomial,
+//         cell and sub-cell volumes, the sub-cell density correction, the node
+//         partial sums and the nodal 2x2 solve (node pass of lag2d_fast.cu),
+//         the corner forces F* = sigma.n A + m (u* - u_c), every cell-average
+//         (moment 0) contribution, the whole specific-volume (tau) equation,
+//         the mass-matrix solve and the RK combine.  The tau equation is the
+//         discrete volume change: its face and volume terms cancel to
+//         O(h^2) of each other, so FP32 there would be amplified by 1/h^2
+//         (and would trip the Persson indicator, which reads tau).
 // Both passes compute each corner's FP32 coefficients m, sigma.n A and the
 // vertex state with the same inline code from the same inputs, and the
 // corner forces are formed from them in FP64, so at every interior node the
@@ -83,7 +86,7 @@ __device__ __forceinline__ double det_integral(const double *D, double r0, doubl
   return v;
 }
 
-// 5-point Gauss (ruqope) and Gauss-Lobatto (ruqope_lobatto) rules in FP32
+// 5-point Gauss (ruqope, FP32) and Gauss-Lobatto (ruqope_lobatto, FP64) rules
 __device__ __forceinline__ float g5p(int i) {
   const float p[5] = {-0.9061798459386640f, -0.5384693101056831f, 0.0f, 0.5384693101056831f, 0.9061798459386640f};
   return p[i];
@@ -93,12 +96,12 @@ __device__ __forceinline__ float g5w(int i) {
                       0.2369268850561891f};
   return w[i];
 }
-__device__ __forceinline__ float l5p(int i) {
-  const float p[5] = {-1.0f, -0.6546536707079771f, 0.0f, 0.6546536707079771f, 1.0f};
+__device__ __forceinline__ double l5pd(int i) {
+  const double p[5] = {-1.0, -0.6546536707079771437983, 0.0, 0.6546536707079771437983, 1.0};
   return p[i];
 }
-__device__ __forceinline__ float l5w(int i) {
-  const float w[5] = {0.1f, 0.5444444444444444f, 0.7111111111111111f, 0.5444444444444444f, 0.1f};
+__device__ __forceinline__ double l5wd(int i) {
+  const double w[5] = {0.1, 0.544444444444444444444, 0.7111111111111111111111, 0.544444444444444444444, 0.1};
   return w[i];
 }
 
@@ -121,15 +124,29 @@ __device__ __forceinline__ float eval_taylor(const float *u, const GeoF &g, floa
          u[5] * (dr * ds - g.g21);
 }
 
-// unit normal (n0, n1) and length a of gesgq slot `slot` (getfnds_lagsms_simpsonhybrid)
-__device__ __forceinline__ void slot_normal(const float X[3][3], const float Y[3][3], int slot, float &n0, float &n1,
-                                            float &a) {
-  float anx, any;
+// FP64 copies of the weights and node tables (same initialiser)
+struct MixTablesD {
+  int nc_start[10];
+  int nc_entry[16];
+  int fnqsg[32];
+  double wrie[32];
+  double wmas[32];
+  double wmom[16];
+  int pa[12], pb[12], side[12];
+  double dl[9];
+  double xv[9], yv[9];
+};
+__constant__ MixTablesD cMD = LAG2D_FAST_TABLES;
+
+// unit normal (n0, n1) and length a of gesgq slot `slot` (getfnds_lagsms_simpsonhybrid), FP64
+__device__ __forceinline__ void slot_normal(const double X[3][3], const double Y[3][3], int slot, double &n0,
+                                            double &n1, double &a) {
+  double anx, any;
   if (slot >= 8 && slot < 12) {
     // inner sub-cell face from edge node (5..8) towards the centre
     const int f = slot - 8;
-    const float lm0 = 0.375f, lm1 = 0.75f, lm2 = -0.125f, lp0 = -0.125f, lp1 = 0.75f, lp2 = 0.375f;
-    float ex, ey, vx, vy;
+    const double lm0 = 0.375, lm1 = 0.75, lm2 = -0.125, lp0 = -0.125, lp1 = 0.75, lp2 = 0.375;
+    double ex, ey, vx, vy;
     if (f == 0) {
       ex = X[1][0]; ey = Y[1][0];
       vx = lm0 * X[1][0] + lm1 * X[1][1] + lm2 * X[1][2];
@@ -147,42 +164,42 @@ __device__ __forceinline__ void slot_normal(const float X[3][3], const float Y[3
       vx = lm0 * X[0][1] + lm1 * X[1][1] + lm2 * X[2][1];
       vy = lm0 * Y[0][1] + lm1 * Y[1][1] + lm2 * Y[2][1];
     }
-    const float dxdr = -1.5f * ex - 0.5f * X[1][1] + 2.0f * vx;
-    const float dydr = -1.5f * ey - 0.5f * Y[1][1] + 2.0f * vy;
+    const double dxdr = -1.5 * ex - 0.5 * X[1][1] + 2.0 * vx;
+    const double dydr = -1.5 * ey - 0.5 * Y[1][1] + 2.0 * vy;
     anx = -dydr;
     any = dxdr;
   } else {
     const int ig = slot < 8 ? slot : slot - 4;
-    const int ia = cMT.pa[ig], ib = cMT.pb[ig];
-    const float *da = cMT.dl + 3 * ia, *db = cMT.dl + 3 * ib;
-    float xa0, xa1, xa2, ya0, ya1, ya2, xb0, xb1, xb2, yb0, yb1, yb2;
+    const int ia = cMD.pa[ig], ib = cMD.pb[ig];
+    const double *da = cMD.dl + 3 * ia, *db = cMD.dl + 3 * ib;
+    double xa0, xa1, xa2, ya0, ya1, ya2, xb0, xb1, xb2, yb0, yb1, yb2;
     if (ib == 0) { xa0 = X[0][0]; xa1 = X[1][0]; xa2 = X[2][0]; ya0 = Y[0][0]; ya1 = Y[1][0]; ya2 = Y[2][0]; }
     else if (ib == 1) { xa0 = X[0][1]; xa1 = X[1][1]; xa2 = X[2][1]; ya0 = Y[0][1]; ya1 = Y[1][1]; ya2 = Y[2][1]; }
     else { xa0 = X[0][2]; xa1 = X[1][2]; xa2 = X[2][2]; ya0 = Y[0][2]; ya1 = Y[1][2]; ya2 = Y[2][2]; }
     if (ia == 0) { xb0 = X[0][0]; xb1 = X[0][1]; xb2 = X[0][2]; yb0 = Y[0][0]; yb1 = Y[0][1]; yb2 = Y[0][2]; }
     else if (ia == 1) { xb0 = X[1][0]; xb1 = X[1][1]; xb2 = X[1][2]; yb0 = Y[1][0]; yb1 = Y[1][1]; yb2 = Y[1][2]; }
     else { xb0 = X[2][0]; xb1 = X[2][1]; xb2 = X[2][2]; yb0 = Y[2][0]; yb1 = Y[2][1]; yb2 = Y[2][2]; }
-    const float xr = da[0] * xa0 + da[1] * xa1 + da[2] * xa2;
-    const float yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
-    const float xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
-    const float ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
-    switch (cMT.side[ig]) {
+    const double xr = da[0] * xa0 + da[1] * xa1 + da[2] * xa2;
+    const double yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
+    const double xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
+    const double ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
+    switch (cMD.side[ig]) {
       case 0: anx = yr; any = -xr; break;
       case 1: anx = ys; any = -xs; break;
       case 2: anx = -yr; any = xr; break;
       default: anx = -ys; any = xs; break;
     }
   }
-  const float n2 = anx * anx + any * any;
-  const float inv = rsqrtf(n2);
+  const double nn = sqrt(anx * anx + any * any);
+  const double inv = 1.0 / nn;
   n0 = anx * inv;
   n1 = any * inv;
-  a = 2.0f * n2 * inv;
+  a = 2.0 * nn;
 }
 
-__device__ __forceinline__ void corner_face(const float X[3][3], const float Y[3][3], int isg, int ivsg, int f,
-                                            float &n0, float &n1, float &a) {
-  const int code = cMT.fnqsg[8 * isg + 2 * ivsg + f];
+__device__ __forceinline__ void corner_face(const double X[3][3], const double Y[3][3], int isg, int ivsg, int f,
+                                            double &n0, double &n1, double &a) {
+  const int code = cMD.fnqsg[8 * isg + 2 * ivsg + f];
   const int slot = (code >= 0 ? code : -code) - 1;
   slot_normal(X, Y, slot, n0, n1, a);
   if (code < 0) { n0 = -n0; n1 = -n1; }
@@ -200,14 +217,13 @@ __device__ __forceinline__ float corner_m(float rhoct, float sdctr, float cimpd,
   return murie * a * fabsf((n0 * dux + n1 * duy) * inv);
 }
 
-// node coordinates of quad iq: FP64 centre node, FP32 offsets from it on the 3x3 tensor
+// node coordinates of quad iq as FP64 offsets from its centre node on the 3x3 tensor
 struct CellXY {
   double ox, oy;
-  float X[3][3], Y[3][3];
-  double c[36];  // cross products of the FP64 offsets (det J, volumes)
+  double X[3][3], Y[3][3];
 };
 
-__device__ __forceinline__ void load_cell(const Dev &d, int iq, CellXY &L) {
+__device__ __forceinline__ void load_cell(const Dev &d, int iq, CellXY &L, double *c) {
   const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
   const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
   double xp[9][2];
@@ -223,20 +239,13 @@ __device__ __forceinline__ void load_cell(const Dev &d, int iq, CellXY &L) {
   for (int k = 0; k < 9; k++) {
     xp[k][0] -= L.ox;
     xp[k][1] -= L.oy;
-    L.X[A[k]][B[k]] = (float)xp[k][0];
-    L.Y[A[k]][B[k]] = (float)xp[k][1];
+    L.X[A[k]][B[k]] = xp[k][0];
+    L.Y[A[k]][B[k]] = xp[k][1];
   }
-  cross36(xp, L.c);
+  if (c) cross36(xp, c);
 }
 
-__device__ __forceinline__ void load_u(const Dev &d, int e, float u[4][6]) {
-#pragma unroll
-  for (int q = 0; q < 4; q++)
-#pragma unroll
-    for (int k = 0; k < 6; k++) u[q][k] = (float)d.Us[(q * 6 + k) * (size_t)d.ncell + e];
-}
-
-// cell-centre sound speed and 1/tau (getriem_quadsubg2)
+// cell-centre sound speed and 1/tau (getriem_quadsubg2), FP32
 __device__ __forceinline__ void centre_state(const float u[4][6], float g, float &rhoct, float &sdctr) {
   const float eps = 1.0e-6f;
   rhoct = 1.0f / u[0][0];
@@ -256,12 +265,12 @@ __device__ __forceinline__ void vertex_state(const float u[4][6], const float *b
   }
 }
 
-// FP32 coefficients of one corner face: m and sigma.n A (sx, sy)
-__device__ __forceinline__ void corner_coeffs(const CellXY &L, int isg, int ivsg, int f, float pv, float rhoct,
+// FP32 coefficients of one corner face from its FP64 normal: m and sigma.n A (sx, sy)
+__device__ __forceinline__ void corner_coeffs(double n0d, double n1d, double ad, float wrie, float pv, float rhoct,
                                               float sdctr, float cimpd, float slpdu, float dux, float duy, float &m,
-                                              float &sx, float &sy, float &n0, float &n1, float &a) {
-  corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
-  const float aw = a * cMT.wrie[8 * isg + 2 * ivsg + f];
+                                              float &sx, float &sy) {
+  const float n0 = (float)n0d, n1 = (float)n1d;
+  const float aw = (float)ad * wrie;
   m = corner_m(rhoct, sdctr, cimpd, slpdu, dux, duy, n0, n1, aw);
   sx = -pv * aw * n0;
   sy = -pv * aw * n1;
@@ -275,21 +284,24 @@ __device__ void m_corner(const Dev &d, int iq) {
   const int e = iq + d.ntria;
   const float eps = 1.0e-6f, g = (float)d.gamlg, slpdu = (g + 1.0f) / 2.0f, cimpd = (float)d.cimpd;
   CellXY L;
-  load_cell(d, iq, L);
-  double D[16];
-  detpoly(L.c, D);
+  double c[36], D[16];
+  load_cell(d, iq, L, c);
+  detpoly(c, D);
   float Df[16];
 #pragma unroll
   for (int t = 0; t < 16; t++) Df[t] = (float)D[t];
   const GeoF G{(float)d.rc[e], (float)d.sc[e], (float)d.g19[e], (float)d.g20[e], (float)d.g21[e]};
   float u[4][6];
-  load_u(d, e, u);
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < 6; k++) u[q][k] = (float)d.Us[(q * 6 + k) * (size_t)d.ncell + e];
   float rhoct, sdctr;
   centre_state(u, g, rhoct, sdctr);
   // sub-cell densities: initial mass / exact sub-cell area (FP64) against the
   // DG-implied harmonic tau mean (FP32 5x5 Gauss per sub-cell)
   double vsub4[4];
-  subareas(L.c, vsub4);
+  subareas(c, vsub4);
   float corr[4];
 #pragma unroll
   for (int isg = 0; isg < 4; isg++) {
@@ -330,8 +342,11 @@ __device__ void m_corner(const Dev &d, int iq) {
       const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
 #pragma unroll
       for (int f = 0; f < 2; f++) {
-        float m, sx, sy, n0, n1, a;
-        corner_coeffs(L, isg, ivsg, f, pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy, n0, n1, a);
+        double n0, n1, a;
+        corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
+        float m, sx, sy;
+        corner_coeffs(n0, n1, a, cMT.wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx,
+                      sy);
         P0 += (double)m;
         P1 += (double)m * (double)st[1];
         P2 += (double)m * (double)st[2];
@@ -348,22 +363,33 @@ __device__ void m_corner(const Dev &d, int iq) {
 }
 
 // ---------------------------------------------------------------------------
-// RHS pass: face integral with FP64 corner forces, FP32 volume integral and
-// source, FP64 moment 0; in stages 2 and 3 the FP64 M^-1 solve and RK combine
+// RHS pass: face integral with FP64 corner forces, the tau equation in FP64,
+// FP32 momentum/energy volume terms and source, FP64 moment 0; in stages 2
+// and 3 the FP64 M^-1 solve and RK combine
 // ---------------------------------------------------------------------------
 __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
   if (iq >= d.nquad || d.sc_dev->done) return;
   const int e = iq + d.ntria;
   const float eps = 1.0e-6f, g = (float)d.gamlg, slpdu = (g + 1.0f) / 2.0f, cimpd = (float)d.cimpd;
   CellXY L;
-  load_cell(d, iq, L);
-  const GeoF G{(float)d.rc[e], (float)d.sc[e], (float)d.g19[e], (float)d.g20[e], (float)d.g21[e]};
+  load_cell(d, iq, L, nullptr);
+  const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
+  const GeoF G{(float)rc, (float)sc, (float)g19, (float)g20, (float)g21};
+  double ud[3][6];  // tau, u, v in FP64 (tau equation)
   float u[4][6];
-  load_u(d, e, u);
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      const double v = d.Us[(q * 6 + k) * (size_t)d.ncell + e];
+      if (q < 3) ud[q][k] = v;
+      u[q][k] = (float)v;
+    }
   float rhoct, sdctr;
   centre_state(u, g, rhoct, sdctr);
-  double ul0 = 0.0, pa0 = 0.0, pb0 = 0.0, el0 = 0.0;  // cell-average contributions
-  float ul[6] = {0, 0, 0, 0, 0, 0}, p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
+  double tr[6] = {0, 0, 0, 0, 0, 0};          // tau equation, all moments
+  double pa0 = 0.0, pb0 = 0.0, el0 = 0.0;     // cell averages of momentum and energy
+  float p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll 1
   for (int k = 0; k < 9; k++) {
     float b[6], st[4];
@@ -382,90 +408,126 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
       const int isg = cMT.nc_entry[i] >> 2, ivsg = cMT.nc_entry[i] & 3;
       const float ci = (float)d.corr[isg * (size_t)d.nquad + iq];
       const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
-      const double wq = (double)cMT.wmom[4 * isg + ivsg];
+      const double wq = cMD.wmom[4 * isg + ivsg];
 #pragma unroll
       for (int f = 0; f < 2; f++) {
-        float m, sx, sy, n0, n1, a;
-        corner_coeffs(L, isg, ivsg, f, pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy, n0, n1, a);
+        double n0, n1, a;
+        corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
+        float m, sx, sy;
+        corner_coeffs(n0, n1, a, cMT.wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx,
+                      sy);
         const double fs0 = (double)sx + (double)m * du0;
         const double fs1 = (double)sy + (double)m * du1;
-        tw += (un * (double)n0 + vn * (double)n1) * (double)(a * cMT.wmas[8 * isg + 2 * ivsg + f]);
+        tw += (un * n0 + vn * n1) * (a * cMD.wmas[8 * isg + 2 * ivsg + f]);
         f0 += fs0 * wq;
         f1 += fs1 * wq;
         fe += (un * fs0 + vn * fs1) * wq;
       }
     }
-    ul0 += tw;
+    // tau: all moments in FP64 with the FP64 node basis
+    {
+      const double b1 = cMD.xv[k] - rc, b2 = cMD.yv[k] - sc;
+      tr[0] += tw;
+      tr[1] += tw * b1;
+      tr[2] += tw * b2;
+      tr[3] += tw * (0.5 * b1 * b1 - g19);
+      tr[4] += tw * (0.5 * b2 * b2 - g20);
+      tr[5] += tw * (b1 * b2 - g21);
+    }
     pa0 += f0;
     pb0 += f1;
     el0 += fe;
-    const float twf = (float)tw, f0f = (float)f0, f1f = (float)f1, fef = (float)fe;
+    const float f0f = (float)f0, f1f = (float)f1, fef = (float)fe;
 #pragma unroll
     for (int kk = 1; kk < 6; kk++) {
-      ul[kk] += twf * b[kk];
       p0[kk] += f0f * b[kk];
       p1[kk] += f1f * b[kk];
       el[kk] += fef * b[kk];
     }
   }
-  // volume integral, 5x5 Gauss-Lobatto, cofactor form, sum-factorised rows
+  // volume integral, 5x5 Gauss-Lobatto, cofactor form, sum-factorised rows:
+  // Jacobian and velocity in FP64 (tau equation), pressure work in FP32
 #pragma unroll 1
   for (int i = 0; i < 5; i++) {
-    const float r = l5p(i), dr = r - G.rc;
-    float lr[3], dlr[3];
-    lag3f(r, lr);
-    dlag3f(r, dlr);
-    float Qx[3], Qy[3], Px[3], Py[3];
+    const double r = l5pd(i);
+    const double dr = r - rc;
+    const double lr0 = 0.5 * r * (r - 1.0), lr1 = 1.0 - r * r, lr2 = 0.5 * r * (r + 1.0);
+    const double dl0 = r - 0.5, dl1 = -2.0 * r, dl2 = r + 0.5;
+    double Qx[3], Qy[3], Px[3], Py[3];
 #pragma unroll
     for (int bb = 0; bb < 3; bb++) {
-      Qx[bb] = dlr[0] * L.X[0][bb] + dlr[1] * L.X[1][bb] + dlr[2] * L.X[2][bb];
-      Qy[bb] = dlr[0] * L.Y[0][bb] + dlr[1] * L.Y[1][bb] + dlr[2] * L.Y[2][bb];
-      Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
-      Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
+      Qx[bb] = dl0 * L.X[0][bb] + dl1 * L.X[1][bb] + dl2 * L.X[2][bb];
+      Qy[bb] = dl0 * L.Y[0][bb] + dl1 * L.Y[1][bb] + dl2 * L.Y[2][bb];
+      Px[bb] = lr0 * L.X[0][bb] + lr1 * L.X[1][bb] + lr2 * L.X[2][bb];
+      Py[bb] = lr0 * L.Y[0][bb] + lr1 * L.Y[1][bb] + lr2 * L.Y[2][bb];
     }
-    const float wi = l5w(i);
+    const float drf = (float)dr;
 #pragma unroll
     for (int j = 0; j < 5; j++) {
-      const float s = l5p(j), ds = s - G.sc;
-      float ls[3], dls[3];
-      lag3f(s, ls);
-      dlag3f(s, dls);
-      const float w = wi * l5w(j);
-      const float xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
-      const float yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
-      const float xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
-      const float ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
-      const float b3 = 0.5f * dr * dr - G.g19, b4 = 0.5f * ds * ds - G.g20, b5 = dr * ds - G.g21;
-      float un[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) un[q] = u[q][0] + u[q][1] * dr + u[q][2] * ds + u[q][3] * b3 + u[q][4] * b4 + u[q][5] * b5;
-      const float rhoad = 1.0f / un[0];
-      const float pres = fmaxf(eps, (g - 1.0f) * rhoad * (un[3] - 0.5f * (un[1] * un[1] + un[2] * un[2])));
-      float gd0[5], gd1[5];
+      const double s = l5pd(j);
+      const double ds = s - sc;
+      const double ls0 = 0.5 * s * (s - 1.0), ls1 = 1.0 - s * s, ls2 = 0.5 * s * (s + 1.0);
+      const double dls0 = s - 0.5, dls1 = -2.0 * s, dls2 = s + 0.5;
+      const double wd = l5wd(i) * l5wd(j);
+      const double xr = Qx[0] * ls0 + Qx[1] * ls1 + Qx[2] * ls2;
+      const double yr = Qy[0] * ls0 + Qy[1] * ls1 + Qy[2] * ls2;
+      const double xs = Px[0] * dls0 + Px[1] * dls1 + Px[2] * dls2;
+      const double ys = Py[0] * dls0 + Py[1] * dls1 + Py[2] * dls2;
+      const double b3 = 0.5 * dr * dr - g19, b4 = 0.5 * ds * ds - g20, b5 = dr * ds - g21;
+      const double uq = ud[1][0] + ud[1][1] * dr + ud[1][2] * ds + ud[1][3] * b3 + ud[1][4] * b4 + ud[1][5] * b5;
+      const double vq = ud[2][0] + ud[2][1] * dr + ud[2][2] * ds + ud[2][3] * b3 + ud[2][4] * b4 + ud[2][5] * b5;
+      // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
+      double gd0[5], gd1[5];
       gd0[0] = ys;       gd1[0] = -xs;
       gd0[1] = -yr;      gd1[1] = xr;
       gd0[2] = ys * dr;  gd1[2] = -xs * dr;
       gd0[3] = -yr * ds; gd1[3] = xr * ds;
       gd0[4] = ys * ds - yr * dr;
       gd1[4] = -xs * ds + xr * dr;
-      const float wp = w * pres;
+      // FP32 pressure work
+      const float dsf = (float)ds, b3f = (float)b3, b4f = (float)b4, b5f = (float)b5;
+      const float tq = u[0][0] + u[0][1] * drf + u[0][2] * dsf + u[0][3] * b3f + u[0][4] * b4f + u[0][5] * b5f;
+      const float eq = u[3][0] + u[3][1] * drf + u[3][2] * dsf + u[3][3] * b3f + u[3][4] * b4f + u[3][5] * b5f;
+      const float uqf = (float)uq, vqf = (float)vq;
+      const float pres = fmaxf(eps, (g - 1.0f) * (1.0f / tq) * (eq - 0.5f * (uqf * uqf + vqf * vqf)));
+      const float wp = (float)wd * pres;
 #pragma unroll
       for (int kk = 0; kk < 5; kk++) {
-        const float fv = gd0[kk] * un[1] + gd1[kk] * un[2];
-        ul[kk + 1] -= fv * w;
-        p0[kk + 1] += gd0[kk] * wp;
-        p1[kk + 1] += gd1[kk] * wp;
-        el[kk + 1] += fv * wp;
+        const double fv = gd0[kk] * uq + gd1[kk] * vq;
+        tr[kk + 1] -= fv * wd;
+        const float g0 = (float)gd0[kk], g1 = (float)gd1[kk];
+        p0[kk + 1] += g0 * wp;
+        p1[kk + 1] += g1 * wp;
+        el[kk + 1] += (float)fv * wp;
       }
     }
   }
   if (d.ncase == 1) {
     // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:4070-4251)
-    double D[16];
-    detpoly(L.c, D);
+    double c[36], D[16];
+    {
+      const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+      const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+      double xp[9][2];
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        xp[k][0] = L.X[A[k]][B[k]];
+        xp[k][1] = L.Y[A[k]][B[k]];
+      }
+      cross36(xp, c);
+    }
+    detpoly(c, D);
     float Df[16];
 #pragma unroll
     for (int t = 0; t < 16; t++) Df[t] = (float)D[t];
+    float Xf[3][3], Yf[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        Xf[a][bb] = (float)L.X[a][bb];
+        Yf[a][bb] = (float)L.Y[a][bb];
+      }
     const float coef = (float)(0.25 * 3.14159265358979311599796346854 / (d.gamlg - 1.0));
     const float oxf = (float)L.ox, oyf = (float)L.oy;
 #pragma unroll 1
@@ -476,8 +538,8 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
       float Px[3], Py[3];
 #pragma unroll
       for (int bb = 0; bb < 3; bb++) {
-        Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
-        Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
+        Px[bb] = lr[0] * Xf[0][bb] + lr[1] * Xf[1][bb] + lr[2] * Xf[2][bb];
+        Py[bb] = lr[0] * Yf[0][bb] + lr[1] * Yf[1][bb] + lr[2] * Yf[2][bb];
       }
       const float wi = g5w(i);
 #pragma unroll
@@ -501,13 +563,13 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
     }
   }
   double R[4][6];
-  R[0][0] = ul0;
   R[1][0] = pa0;
   R[2][0] = pb0;
   R[3][0] = el0;
 #pragma unroll
+  for (int k = 0; k < 6; k++) R[0][k] = tr[k];
+#pragma unroll
   for (int k = 1; k < 6; k++) {
-    R[0][k] = (double)ul[k];
     R[1][k] = (double)p0[k];
     R[2][k] = (double)p1[k];
     R[3][k] = (double)el[k];
