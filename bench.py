@@ -167,6 +167,18 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def measured_traffic(family, ncell):
+    """DRAM bytes per launch of a kernel family from the committed ncu summary
+    (profiles/traffic.json: bytes per cell of a capture larger than L2),
+    scaled to this workload's cells; None when no capture is recorded."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t[family]["dram_bytes_per_cell"] * ncell
+    except Exception:
+        return None
+
+
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
@@ -238,7 +250,8 @@ def run_ours(args):
     dom = max((f for f in per_step if f in ("corner", "node", "rhs", "update", "persson", "nodes", "geom")),
               key=lambda f: per_step[f])
     peak, peak_kind = peaks()
-    kb = kernel_bytes(dom, m.ncell, m.npoin)
+    kb = kernel_bytes(dom, m.ncell, m.npoin, c.nstag)
+    traffic = measured_traffic(dom, m.ncell)
     achieved = kb / (fams[dom]["ms_per_launch"] / 1e3) / 1e9
     sb = stage_bytes(m.ncell, m.npoin)
     stage_gbs = sb / (ms_per_step / c.nstag / 1e3) / 1e9
@@ -294,7 +307,7 @@ def run_ours(args):
                 "config": config_block(args.workload, m, c, world), "clocks": clocks, "gpu_launches": launches,
                 "e2e": e2e,
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                              "bytes_per_launch": kb},
                 "stage_roofline": {"bytes_per_stage": sb, "achieved_gbs": stage_gbs, "peak": peak,
                                    "frac": stage_gbs / peak, "roofline_dof_updates_per_s": dof_stage / (sb / (peak * 1e9))},

@@ -58,7 +58,7 @@ typedef struct {
   int ncase;            /* initial-condition / source case               */
   int nlimi, ndens;
   int ngausd, ngausd_geo;
-  int precision;        /* 0: FP64; 1: FP32-mixed (not built: EUNSUP)    */
+  int precision;        /* 0: FP64; 1: FP32-mixed corner/RHS arithmetic  */
   int order_exact;      /* 1: kernels that keep the reference's loop and
                            summation order (bit-identical to the CPU
                            restatement in the no-FMA build); 0: optimised */

@@ -44,8 +44,12 @@ class StepConfig:
 
 
 def _tgv(n: int) -> Tuple[Mesh, StepConfig]:
+    """Taylor-Green vortex at CFL 0.05: at CFL 0.1 the scheme amplifies
+    perturbations of the P2 velocity moments by about 1.6x per step on meshes
+    of 64x64 cells and finer (FP64, measured with the CPU restatement), at
+    0.05 it does not."""
     m = quad_mesh(n, n, 0.0, 1.0, 0.0, 1.0)
-    c = StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=3, cfl=0.1, tend=10.0)
+    c = StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=3, cfl=0.05, tend=10.0)
     return m, c
 
 
@@ -63,7 +67,9 @@ def _sedov(n: int) -> Tuple[Mesh, StepConfig]:
 WORKLOADS = {
     # Taylor-Green vortex: [0,1]^2, gamma 5/3, P2, RK3, energy source on
     "tgv1024": lambda: _tgv(1024),
+    "tgv512": lambda: _tgv(512),
     "tgv256": lambda: _tgv(256),
+    "tgv128": lambda: _tgv(128),
     "tgv64": lambda: _tgv(64),
     "tgv16": lambda: _tgv(16),
     # Sedov blast: [0,1.2]^2, gamma 1.4, energy in the corner cell

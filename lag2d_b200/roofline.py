@@ -16,9 +16,21 @@ written once, intermediates excluded), FP64:
   16*N_c*4      the node-to-corner gather list (16 corners per quad)
 
 Per kernel family the same rule is applied to that kernel's own interface
-(its inputs read once, its outputs written once), so the intermediate arrays
-the split into kernels introduces (corner coefficients, the RHS) are counted
-where they are written and where they are read.
+(its inputs read once, its outputs written once), for the optimised kernels
+the step runs (corner data are recomputed in the RHS pass, not stored):
+
+  corner   U^(s), rc/sc/g19..g21, sub-cell masses, connectivity, x^(s),
+           ustar_prev -> 4 sub-cell corrections, 45 node partial sums
+  node     45 partial sums and 9 gather ids per quad, CSR offset, mask,
+           ustar_prev -> ustar
+  rhs      U^(s), geometry, corrections, connectivity, x^(s), ustar_prev,
+           ustar -> RHS (stage 1), or in stages 2..nstag also U^n and M^-1
+           -> U^(s+1) (the M^-1 solve and RK combine are fused there)
+  update   RHS, U^n, U^(s), M^-1 -> U^(s+1) (stage 1)
+  persson  tau DOFs, mean velocity, geometry, mass, shape moments,
+           connectivity, x^(s) -> flag, physical centre, frame
+  nodes    x^n, x^(s), ustar -> x^(s+1), ustar_prev
+  geom     connectivity, x^(s) -> volume, centre node
 """
 from __future__ import annotations
 
@@ -29,25 +41,22 @@ def stage_bytes(ncell: int, npoin: int, ndegr: int = 6, nq: int = 4) -> int:
     return ncell * (3 * ndegr * nq * W + 16 * W + 5 * W + 8 + 9 * 4) + npoin * (4 * 16 + 2 * 16 + 4) + 16 * ncell * 4
 
 
-def kernel_bytes(family: str, ncell: int, npoin: int) -> int:
-    """Interface bytes of one launch of a kernel family on an all-quad mesh."""
+def kernel_bytes(family: str, ncell: int, npoin: int, nstag: int = 3) -> int:
+    """Interface bytes of one launch of a kernel family on an all-quad mesh,
+    averaged over the family's launches in one time step."""
     U = 24 * W            # 24 DOFs of one cell
     GEO = 5 * W           # rc, sc, g19..g21
     CONN = 9 * 4          # ipqua row
-    CF = 160 * W          # corner coefficients of one quad (5 values x 32 corner faces)
-    XY = 2 * W
+    XY = 2 * W            # one node pair (x, y) or (u, v)
+    rhs_plain = ncell * (U + GEO + 4 * W + CONN + U) + npoin * 3 * XY
+    rhs_fused = ncell * (U + U + 16 * W + GEO + 4 * W + CONN + U) + npoin * 3 * XY
     fam = {
-        # U, geometry, sub-cell masses, connectivity, nodes (x, ustar) -> corner coefficients
-        "corner": ncell * (U + GEO + 4 * W + CONN + CF) + npoin * (XY + XY),
-        # corner coefficients via the gather list + ustar in/out + masks -> ustar
-        "node": ncell * (CF + 32 * 4) + npoin * (4 + 1 + XY + XY),
-        # U, geometry, connectivity, corner coefficients, nodes (x, ustar) -> RHS
-        "rhs": ncell * (U + GEO + CONN + CF + U) + npoin * (XY + XY),
-        # RHS, U^n, U^(s) in/out, M^-1
+        "corner": ncell * (U + GEO + 4 * W + CONN + 4 * W + 45 * W) + npoin * (XY + XY),
+        "node": ncell * (45 * W + 9 * 4) + npoin * (4 + 1 + XY + XY),
+        "rhs": (rhs_plain + (nstag - 1) * rhs_fused) // nstag,
         "update": ncell * (U + U + 2 * U + 16 * W),
-        # U, geometry, mass, connectivity, x, X0 -> flag, physical centre, frame
-        "persson": ncell * (U + GEO + W + CONN + 4 + 2 * W + 4 * W) + npoin * (XY + XY),
-        "nodes": npoin * (XY + XY + XY + XY),
-        "geom": ncell * (CONN + 3 * W) + npoin * XY,
+        "persson": ncell * (6 * W + 2 * W + GEO + W + 9 * W + CONN + 4 + 2 * W + 4 * W) + npoin * XY,
+        "nodes": npoin * (3 * XY + 2 * XY),
+        "geom": ncell * (CONN + W + XY) + npoin * XY,
     }
     return fam[family]
