@@ -62,17 +62,6 @@ __host__ __device__ __forceinline__ void dlag3(double r, double *l) {
   l[2] = r + 0.5;
 }
 
-// reference node k at tensor position (a, b): X[a][b]
-__host__ __device__ __forceinline__ void to_tensor(const double (*xp)[2], double X[3][3], double Y[3][3]) {
-  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
-  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
-#pragma unroll
-  for (int k = 0; k < 9; k++) {
-    X[A[k]][B[k]] = xp[k][0];
-    Y[A[k]][B[k]] = xp[k][1];
-  }
-}
-
 __host__ __device__ __forceinline__ double deteval(const double *D, double r, double s) {
   double e[4];
 #pragma unroll
@@ -132,125 +121,32 @@ __host__ __device__ __forceinline__ void node_basis2(const CellGeo &g, int iv, d
   b[5] = b[1] * b[2] - g.g21;
 }
 
-// DG state evaluated at (r, s): Taylor basis about (rc, sc)
-__host__ __device__ __forceinline__ double eval_taylor(const double *u, const CellGeo &g, double r, double s) {
-  const double dr = r - g.rc, ds = s - g.sc;
-  return u[0] + u[1] * dr + u[2] * ds + u[3] * (0.5 * dr * dr - g.g19) + u[4] * (0.5 * ds * ds - g.g20) +
-         u[5] * (dr * ds - g.g21);
-}
 
-// Sub-cell normals (16 entries, same slots as gesgq of the reference):
-// Simpson-point normals from node derivatives of the tensor map and the four
-// inner sub-cell faces at the edge nodes.
-__host__ __device__ __forceinline__ void normals16(const double X[3][3], const double Y[3][3], double (*gq)[3]) {
-  const double DL[3][3] = {{-1.5, 2.0, -0.5}, {-0.5, 0.0, 0.5}, {0.5, -2.0, 1.5}};  // L'_c(r_a): DL[a][c]
-  // the 12 outer points (getfnds_lagsms_simpsonhybrid posiq order) as tensor nodes
-  const int PA[12] = {0, 2, 2, 2, 2, 0, 0, 0, 1, 2, 1, 0};
-  const int PB[12] = {0, 0, 0, 2, 2, 2, 2, 0, 0, 1, 2, 1};
-  const double vnx[4] = {0.0, 1.0, 0.0, -1.0}, vny[4] = {-1.0, 0.0, 1.0, 0.0};
-  const int side[12] = {0, 0, 1, 1, 2, 2, 3, 3, 0, 1, 2, 3};
-#pragma unroll
-  for (int ig = 0; ig < 12; ig++) {
-    const int a = PA[ig], b = PB[ig];
-    double xr = DL[a][0] * X[0][b] + DL[a][1] * X[1][b] + DL[a][2] * X[2][b];
-    double yr = DL[a][0] * Y[0][b] + DL[a][1] * Y[1][b] + DL[a][2] * Y[2][b];
-    double xs = DL[b][0] * X[a][0] + DL[b][1] * X[a][1] + DL[b][2] * X[a][2];
-    double ys = DL[b][0] * Y[a][0] + DL[b][1] * Y[a][1] + DL[b][2] * Y[a][2];
-    const double vn0 = vnx[side[ig]], vn1 = vny[side[ig]];
-    double anx = ys * vn0 - yr * vn1;
-    double any = -xs * vn0 + xr * vn1;
-    double farea = 2.0 * sqrt(anx * anx + any * any);
-    double inv = 1.0 / sqrt(anx * anx + any * any);
-    const int slot = (ig < 8) ? ig : ig + 4;
-    gq[slot][0] = anx * inv;
-    gq[slot][1] = any * inv;
-    gq[slot][2] = farea;
-  }
-  // inner faces from edge node (5..8) towards the centre, derivative at the
-  // edge node of the quadratic through (edge node, centre, map(posqc))
-  // posqc = (0,-.5), (.5,0), (0,.5), (-.5,0); L(-.5) = (.375, .75, -.125), L(.5) = (-.125, .75, .375)
-  const double lm[3] = {0.375, 0.75, -0.125}, lp[3] = {-0.125, 0.75, 0.375};
-  double ex[4], ey[4], vx[4], vy[4];
-  ex[0] = X[1][0]; ey[0] = Y[1][0];
-  vx[0] = lm[0] * X[1][0] + lm[1] * X[1][1] + lm[2] * X[1][2];
-  vy[0] = lm[0] * Y[1][0] + lm[1] * Y[1][1] + lm[2] * Y[1][2];
-  ex[1] = X[2][1]; ey[1] = Y[2][1];
-  vx[1] = lp[0] * X[0][1] + lp[1] * X[1][1] + lp[2] * X[2][1];
-  vy[1] = lp[0] * Y[0][1] + lp[1] * Y[1][1] + lp[2] * Y[2][1];
-  ex[2] = X[1][2]; ey[2] = Y[1][2];
-  vx[2] = lp[0] * X[1][0] + lp[1] * X[1][1] + lp[2] * X[1][2];
-  vy[2] = lp[0] * Y[1][0] + lp[1] * Y[1][1] + lp[2] * Y[1][2];
-  ex[3] = X[0][1]; ey[3] = Y[0][1];
-  vx[3] = lm[0] * X[0][1] + lm[1] * X[1][1] + lm[2] * X[2][1];
-  vy[3] = lm[0] * Y[0][1] + lm[1] * Y[1][1] + lm[2] * Y[2][1];
-#pragma unroll
-  for (int f = 0; f < 4; f++) {
-    double dxdr = -1.5 * ex[f] - 0.5 * X[1][1] + 2.0 * vx[f];
-    double dydr = -1.5 * ey[f] - 0.5 * Y[1][1] + 2.0 * vy[f];
-    double n2 = dxdr * dxdr + dydr * dydr;
-    double inv = 1.0 / sqrt(n2);
-    gq[8 + f][0] = -dydr * inv;
-    gq[8 + f][1] = dxdr * inv;
-    gq[8 + f][2] = 2.0 * sqrt(n2);
-  }
-}
-
-__host__ __device__ __forceinline__ int ipqsg2(int isg, int ivsg) {
-  const int t[16] = {0, 4, 8, 7, 4, 1, 5, 8, 8, 5, 2, 6, 7, 8, 6, 3};
-  return t[4 * isg + ivsg];
-}
 __host__ __device__ __forceinline__ int fnqsg2(int isg, int k) { return FT().fnqsg[8 * isg + k]; }
 // corner-face weights (Getrhslaggauss.f90:10534-10552 x 0.25; :8580-8637)
 __host__ __device__ __forceinline__ double wrie(int isg, int ivsg, int f) { return FT().wrie[8 * isg + 2 * ivsg + f]; }
 __host__ __device__ __forceinline__ double wmas(int isg, int ivsg, int f) { return FT().wmas[8 * isg + 2 * ivsg + f]; }
 __host__ __device__ __forceinline__ double wmom(int isg, int ivsg) { return FT().wmom[4 * isg + ivsg]; }
 
-__host__ __device__ __forceinline__ void corner_n(const double (*gq)[3], int isg, int ivsg, int f, double &n0,
-                                                  double &n1, double &a) {
-  const int code = fnqsg2(isg, 2 * ivsg + f);
-  const int slot = (code >= 0 ? code : -code) - 1;
-  const double sg = (code >= 0) ? 1.0 : -1.0;
-  n0 = sg * gq[slot][0];
-  n1 = sg * gq[slot][1];
-  a = gq[slot][2];
-}
-
-// Per-corner state shared by the corner and RHS passes: vertex velocity and
-// pressure with the sub-cell density correction (getriem_quadsubg2,
-// Getrhslaggauss.f90:10662-10710) and the cell-centre sound speed.
-struct CornerState {
-  double u[4][2], p[4];
-};
-
-__host__ __device__ __forceinline__ void corner_states(const double unknvq[9][4], const double *corr, double g,
-                                                       int isg, CornerState &cs) {
-  const double eps = 1.0e-6;
-#pragma unroll
-  for (int ivsg = 0; ivsg < 4; ivsg++) {
-    const int iv = ipqsg2(isg, ivsg);
-    const double rhovsg = 1.0 / unknvq[iv][0] + corr[isg];
-    const double uvtx = unknvq[iv][1], vvtx = unknvq[iv][2], evtx = unknvq[iv][3];
-    cs.u[ivsg][0] = uvtx;
-    cs.u[ivsg][1] = vvtx;
-    cs.p[ivsg] = fmax(eps, (g - 1.0) * rhovsg * (evtx - 0.5 * (uvtx * uvtx + vvtx * vvtx)));
-  }
-}
-
-// impedance-weighted area m = mu * A of one corner face (getriecoef_matrixnew,
-// Limiterlag.f90:1037): the jump-direction branch is taken only when
-// |u* - u_c| / c >= 1e12, tested on squares
+// Impedance-weighted area m = mu * A * w of one corner face
+// (getriecoef_matrixnew, Limiterlag.f90:1037) from the unnormalised face
+// vector an (unit normal n = an / |an|, face length A = 2 |an|) and the face
+// weight w:  m = 2 w (rho c |an| + cimpd rho slpdu |du . an|), which needs no
+// division.  The jump-direction branch is taken only when |u* - u_c| / c >=
+// 1e12, tested on squares.
 __host__ __device__ __forceinline__ double corner_m(double rhoct, double sdctr, double cimpd, double slpdu,
-                                                   double dux, double duy, double n0, double n1, double a) {
-  const double deltu = fabs(dux * n0 + duy * n1);
-  const double murie = rhoct * sdctr + cimpd * rhoct * slpdu * deltu;
+                                                   double dux, double duy, double ax, double ay, double w) {
+  const double nn = sqrt(ax * ax + ay * ay);
+  const double dun = fabs(dux * ax + duy * ay);
   const double j2 = dux * dux + duy * duy;
   const double lim = 1.0e12 * sdctr;
-  if (j2 < lim * lim) return murie * a;
+  if (j2 < lim * lim) return 2.0 * w * (rhoct * sdctr * nn + cimpd * rhoct * slpdu * dun);
+  const double murie = rhoct * sdctr + cimpd * rhoct * slpdu * (dun / nn);
   const double nrm = sqrt(j2);
-  double ax, ay;
-  if (nrm < (double)1.e-11f) { ax = (double)1.e-11f; ay = (double)1.e-11f; }
-  else { ax = dux / nrm; ay = duy / nrm; }
-  return murie * a * fabs(n0 * ax + n1 * ay);
+  double jx, jy;
+  if (nrm < (double)1.e-11f) { jx = (double)1.e-11f; jy = (double)1.e-11f; }
+  else { jx = dux / nrm; jy = duy / nrm; }
+  return murie * 2.0 * w * fabs(ax * jx + ay * jy);
 }
 
 // Corner faces grouped by the node they belong to, in the reference's
@@ -259,9 +155,11 @@ __host__ __device__ __forceinline__ double corner_m(double rhoct, double sdctr, 
 __host__ __device__ __forceinline__ int nc_start(int k) { return FT().nc_start[k]; }
 __host__ __device__ __forceinline__ int nc_entry(int i) { return FT().nc_entry[i]; }
 
-// outer/inner face normal (unit n, length a) of the gesgq slot `slot`
-__host__ __device__ __forceinline__ void slot_normal(const double X[3][3], const double Y[3][3], int slot, double &n0,
-                                                     double &n1, double &a) {
+// Unnormalised face vector an of the gesgq slot `slot`: the unit normal is
+// an / |an| and the face length 2 |an| (getfnds_lagsms_simpsonhybrid and
+// getfnds_lagsmsif_hybrid, Getrhslaggauss.f90:9660-10021, 3356-3602)
+__host__ __device__ __forceinline__ void slot_an(const double X[3][3], const double Y[3][3], int slot, double &ax,
+                                                 double &ay) {
   if (slot >= 8 && slot < 12) {
     // inner sub-cell face at edge node (5..8) towards the centre
     const int f = slot - 8;
@@ -286,11 +184,8 @@ __host__ __device__ __forceinline__ void slot_normal(const double X[3][3], const
     }
     const double dxdr = -1.5 * ex - 0.5 * X[1][1] + 2.0 * vx;
     const double dydr = -1.5 * ey - 0.5 * Y[1][1] + 2.0 * vy;
-    const double nn = sqrt(dxdr * dxdr + dydr * dydr);
-    const double inv = 1.0 / nn;
-    n0 = -dydr * inv;
-    n1 = dxdr * inv;
-    a = 2.0 * nn;
+    ax = -dydr;
+    ay = dxdr;
     return;
   }
   // Simpson points (getfnds_lagsms_simpsonhybrid order) on the 4 outer faces
@@ -310,26 +205,21 @@ __host__ __device__ __forceinline__ void slot_normal(const double X[3][3], const
   const double yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
   const double xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
   const double ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
-  double anx, any;
   switch (T.side[ig]) {
-    case 0: anx = yr; any = -xr; break;     // vnorm (0,-1)
-    case 1: anx = ys; any = -xs; break;     // vnorm (1, 0)
-    case 2: anx = -yr; any = xr; break;     // vnorm (0, 1)
-    default: anx = -ys; any = xs; break;    // vnorm (-1,0)
+    case 0: ax = yr; ay = -xr; break;     // vnorm (0,-1)
+    case 1: ax = ys; ay = -xs; break;     // vnorm (1, 0)
+    case 2: ax = -yr; ay = xr; break;     // vnorm (0, 1)
+    default: ax = -ys; ay = xs; break;    // vnorm (-1,0)
   }
-  const double nn = sqrt(anx * anx + any * any);
-  const double inv = 1.0 / nn;
-  n0 = anx * inv;
-  n1 = any * inv;
-  a = 2.0 * nn;
 }
 
-__host__ __device__ __forceinline__ void corner_face(const double X[3][3], const double Y[3][3], int isg, int ivsg,
-                                                     int f, double &n0, double &n1, double &a) {
+// face vector of corner face f of vertex ivsg of sub-cell isg, oriented outwards
+__host__ __device__ __forceinline__ void corner_an(const double X[3][3], const double Y[3][3], int isg, int ivsg,
+                                                   int f, double &ax, double &ay) {
   const int code = fnqsg2(isg, 2 * ivsg + f);
   const int slot = (code >= 0 ? code : -code) - 1;
-  slot_normal(X, Y, slot, n0, n1, a);
-  if (code < 0) { n0 = -n0; n1 = -n1; }
+  slot_an(X, Y, slot, ax, ay);
+  if (code < 0) { ax = -ax; ay = -ay; }
 }
 
 struct Loaded {
@@ -365,23 +255,6 @@ __host__ __device__ __forceinline__ void load_u(const Dev &d, const double *U, i
     for (int k = 0; k < 6; k++) u[q][k] = U[(q * 6 + k) * (size_t)d.ncell + e];
 }
 
-__host__ __device__ __forceinline__ void vertex_states(const double u[4][6], const CellGeo &g, double unknvq[9][4],
-                                                       int mdegr) {
-#pragma unroll
-  for (int iv = 0; iv < 9; iv++) {
-    double b[6];
-    node_basis2(g, iv, b);
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      double acc = 0.0;
-#pragma unroll
-      for (int k = 0; k < 6; k++)
-        if (k < mdegr) acc += u[q][k] * b[k];
-      unknvq[iv][q] = acc;
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Persson indicator + physical mass centre + frame (all quads)
 // ---------------------------------------------------------------------------
@@ -402,17 +275,25 @@ __host__ __device__ void f_persson(const Dev &d, int iq) {
 #pragma unroll
   for (int k = 0; k < 6; k++) t[k] = d.Us[k * (size_t)d.ncell + e];
   double unvar2 = 0.0, unvar1 = 0.0;
-#pragma unroll
+#pragma unroll 1
   for (int i = 0; i < 5; i++) {
     const double r = g5p(i);
     const double dr = r - g.rc;
+    // along the row r: det J cubic, P1 part linear and P2 part quadratic in s
+    double e[4];
+#pragma unroll
+    for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+    const double a0 = t[0] + t[1] * dr;
+    const double h0 = t[3] * (0.5 * dr * dr - g.g19) - t[4] * g.g20 - t[5] * g.g21;
+    const double h1 = t[5] * dr, h2 = 0.5 * t[4];
+    const double wi = g5w(i);
 #pragma unroll
     for (int j = 0; j < 5; j++) {
       const double s = g5p(j);
       const double ds = s - g.sc;
-      const double djaco = g5w(i) * g5w(j) * deteval(D, r, s);
-      const double p1 = t[0] + t[1] * dr + t[2] * ds;
-      const double hi = t[3] * (0.5 * dr * dr - g.g19) + t[4] * (0.5 * ds * ds - g.g20) + t[5] * (dr * ds - g.g21);
+      const double djaco = wi * g5w(j) * (e[0] + s * (e[1] + s * (e[2] + s * e[3])));
+      const double p1 = a0 + t[2] * ds;
+      const double hi = h0 + ds * (h1 + h2 * ds);
       const double un = p1 + hi;
       unvar2 += hi * hi * djaco;
       unvar1 += un * un * djaco;
@@ -495,11 +376,21 @@ __host__ __device__ void f_corner(const Dev &d, int iq) {
 #pragma unroll 1
     for (int i = 0; i < 5; i++) {
       const double r = (g5p(i) + ofr) / 2.0;
+      // along the row r, det J is a cubic and tau a quadratic in s
+      double e[4];
+#pragma unroll
+      for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+      const double dr = r - G.rc;
+      const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
+      const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
+      const double wi = 0.25 * g5w(i);
 #pragma unroll
       for (int j = 0; j < 5; j++) {
         const double s = (g5p(j) + ofs) / 2.0;
-        const double tau = eval_taylor(u[0], G, r, s);
-        masel += (g5w(i) * g5w(j) * 0.25) * deteval(D, r, s) / tau;
+        const double ds = s - G.sc;
+        const double tau = t0 + ds * (t1 + t2 * ds);
+        const double det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
+        masel += (wi * g5w(j)) * det / tau;
       }
     }
     const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
@@ -534,15 +425,16 @@ __host__ __device__ void f_corner(const Dev &d, int iq) {
       const double pv = fmax(eps, (g - 1.0) * (rhovt + ci) * ke);
 #pragma unroll
       for (int f = 0; f < 2; f++) {
-        double n0, n1, a;
-        corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
-        const double aw = a * wrie(isg, ivsg, f);
-        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, n0, n1, aw);
+        double ax, ay;
+        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
+        const double w = wrie(isg, ivsg, f);
+        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w);
+        const double pw = -2.0 * pv * w;  // sigma . n A w = -p 2 w an
         P0 += m;
         P1 += m * st[1];
         P2 += m * st[2];
-        P3 += -pv * aw * n0;
-        P4 += -pv * aw * n1;
+        P3 += pw * ax;
+        P4 += pw * ay;
       }
     }
     d.npart[(0 * 9 + k) * (size_t)d.nquad + iq] = P0;
@@ -627,13 +519,14 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
       const double wq = wmom(isg, ivsg);
 #pragma unroll
       for (int f = 0; f < 2; f++) {
-        double n0, n1, a;
-        corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
-        const double aw = a * wrie(isg, ivsg, f);
-        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, n0, n1, aw);
-        const double fs0 = -pv * aw * n0 + m * du0;
-        const double fs1 = -pv * aw * n1 + m * du1;
-        tw += (un * n0 + vn * n1) * (a * wmas(isg, ivsg, f));
+        double ax, ay;
+        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
+        const double w = wrie(isg, ivsg, f);
+        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w);
+        const double pw = -2.0 * pv * w;
+        const double fs0 = pw * ax + m * du0;
+        const double fs1 = pw * ay + m * du1;
+        tw += (un * ax + vn * ay) * (2.0 * wmas(isg, ivsg, f));
         f0 += fs0 * wq;
         f1 += fs1 * wq;
         fe += (un * fs0 + vn * fs1) * wq;
@@ -899,7 +792,10 @@ __host__ __device__ void f_init_wmom(const Dev &d, int iq) {
 }
 
 __global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128, 3) k_corner2(Dev d) { f_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
+#ifndef LAG2D_CORNER_MIN_BLOCKS
+#define LAG2D_CORNER_MIN_BLOCKS 3  // resident blocks of 128 per SM the corner pass is compiled for
+#endif
+__global__ void __launch_bounds__(128, LAG2D_CORNER_MIN_BLOCKS) k_corner2(Dev d) { f_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_node2(Dev d) { f_node(d, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void __launch_bounds__(128) k_rhs2(Dev d, int fuse, double alfa) {
   f_rhs(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa);

@@ -118,11 +118,6 @@ __device__ __forceinline__ void node_basis(const GeoF &g, int iv, float *b) {
   b[5] = b[1] * b[2] - g.g21;
 }
 
-__device__ __forceinline__ float eval_taylor(const float *u, const GeoF &g, float r, float s) {
-  const float dr = r - g.rc, ds = s - g.sc;
-  return u[0] + u[1] * dr + u[2] * ds + u[3] * (0.5f * dr * dr - g.g19) + u[4] * (0.5f * ds * ds - g.g20) +
-         u[5] * (dr * ds - g.g21);
-}
 
 // FP64 copies of the weights and node tables (same initialiser)
 struct MixTablesD {
@@ -138,10 +133,11 @@ struct MixTablesD {
 };
 __constant__ MixTablesD cMD = LAG2D_FAST_TABLES;
 
-// unit normal (n0, n1) and length a of gesgq slot `slot` (getfnds_lagsms_simpsonhybrid), FP64
-__device__ __forceinline__ void slot_normal(const double X[3][3], const double Y[3][3], int slot, double &n0,
-                                            double &n1, double &a) {
-  double anx, any;
+// Unnormalised face vector an of gesgq slot `slot` in FP64 (unit normal
+// an / |an|, face length 2 |an|; getfnds_lagsms_simpsonhybrid and
+// getfnds_lagsmsif_hybrid)
+__device__ __forceinline__ void slot_an(const double X[3][3], const double Y[3][3], int slot, double &ax,
+                                        double &ay) {
   if (slot >= 8 && slot < 12) {
     // inner sub-cell face from edge node (5..8) towards the centre
     const int f = slot - 8;
@@ -164,57 +160,51 @@ __device__ __forceinline__ void slot_normal(const double X[3][3], const double Y
       vx = lm0 * X[0][1] + lm1 * X[1][1] + lm2 * X[2][1];
       vy = lm0 * Y[0][1] + lm1 * Y[1][1] + lm2 * Y[2][1];
     }
-    const double dxdr = -1.5 * ex - 0.5 * X[1][1] + 2.0 * vx;
-    const double dydr = -1.5 * ey - 0.5 * Y[1][1] + 2.0 * vy;
-    anx = -dydr;
-    any = dxdr;
-  } else {
-    const int ig = slot < 8 ? slot : slot - 4;
-    const int ia = cMD.pa[ig], ib = cMD.pb[ig];
-    const double *da = cMD.dl + 3 * ia, *db = cMD.dl + 3 * ib;
-    double xa0, xa1, xa2, ya0, ya1, ya2, xb0, xb1, xb2, yb0, yb1, yb2;
-    if (ib == 0) { xa0 = X[0][0]; xa1 = X[1][0]; xa2 = X[2][0]; ya0 = Y[0][0]; ya1 = Y[1][0]; ya2 = Y[2][0]; }
-    else if (ib == 1) { xa0 = X[0][1]; xa1 = X[1][1]; xa2 = X[2][1]; ya0 = Y[0][1]; ya1 = Y[1][1]; ya2 = Y[2][1]; }
-    else { xa0 = X[0][2]; xa1 = X[1][2]; xa2 = X[2][2]; ya0 = Y[0][2]; ya1 = Y[1][2]; ya2 = Y[2][2]; }
-    if (ia == 0) { xb0 = X[0][0]; xb1 = X[0][1]; xb2 = X[0][2]; yb0 = Y[0][0]; yb1 = Y[0][1]; yb2 = Y[0][2]; }
-    else if (ia == 1) { xb0 = X[1][0]; xb1 = X[1][1]; xb2 = X[1][2]; yb0 = Y[1][0]; yb1 = Y[1][1]; yb2 = Y[1][2]; }
-    else { xb0 = X[2][0]; xb1 = X[2][1]; xb2 = X[2][2]; yb0 = Y[2][0]; yb1 = Y[2][1]; yb2 = Y[2][2]; }
-    const double xr = da[0] * xa0 + da[1] * xa1 + da[2] * xa2;
-    const double yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
-    const double xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
-    const double ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
-    switch (cMD.side[ig]) {
-      case 0: anx = yr; any = -xr; break;
-      case 1: anx = ys; any = -xs; break;
-      case 2: anx = -yr; any = xr; break;
-      default: anx = -ys; any = xs; break;
-    }
+    ax = -(-1.5 * ey - 0.5 * Y[1][1] + 2.0 * vy);
+    ay = -1.5 * ex - 0.5 * X[1][1] + 2.0 * vx;
+    return;
   }
-  const double nn = sqrt(anx * anx + any * any);
-  const double inv = 1.0 / nn;
-  n0 = anx * inv;
-  n1 = any * inv;
-  a = 2.0 * nn;
+  const int ig = slot < 8 ? slot : slot - 4;
+  const int ia = cMD.pa[ig], ib = cMD.pb[ig];
+  const double *da = cMD.dl + 3 * ia, *db = cMD.dl + 3 * ib;
+  double xa0, xa1, xa2, ya0, ya1, ya2, xb0, xb1, xb2, yb0, yb1, yb2;
+  if (ib == 0) { xa0 = X[0][0]; xa1 = X[1][0]; xa2 = X[2][0]; ya0 = Y[0][0]; ya1 = Y[1][0]; ya2 = Y[2][0]; }
+  else if (ib == 1) { xa0 = X[0][1]; xa1 = X[1][1]; xa2 = X[2][1]; ya0 = Y[0][1]; ya1 = Y[1][1]; ya2 = Y[2][1]; }
+  else { xa0 = X[0][2]; xa1 = X[1][2]; xa2 = X[2][2]; ya0 = Y[0][2]; ya1 = Y[1][2]; ya2 = Y[2][2]; }
+  if (ia == 0) { xb0 = X[0][0]; xb1 = X[0][1]; xb2 = X[0][2]; yb0 = Y[0][0]; yb1 = Y[0][1]; yb2 = Y[0][2]; }
+  else if (ia == 1) { xb0 = X[1][0]; xb1 = X[1][1]; xb2 = X[1][2]; yb0 = Y[1][0]; yb1 = Y[1][1]; yb2 = Y[1][2]; }
+  else { xb0 = X[2][0]; xb1 = X[2][1]; xb2 = X[2][2]; yb0 = Y[2][0]; yb1 = Y[2][1]; yb2 = Y[2][2]; }
+  const double xr = da[0] * xa0 + da[1] * xa1 + da[2] * xa2;
+  const double yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
+  const double xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
+  const double ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
+  switch (cMD.side[ig]) {
+    case 0: ax = yr; ay = -xr; break;
+    case 1: ax = ys; ay = -xs; break;
+    case 2: ax = -yr; ay = xr; break;
+    default: ax = -ys; ay = xs; break;
+  }
 }
 
-__device__ __forceinline__ void corner_face(const double X[3][3], const double Y[3][3], int isg, int ivsg, int f,
-                                            double &n0, double &n1, double &a) {
+__device__ __forceinline__ void corner_an(const double X[3][3], const double Y[3][3], int isg, int ivsg, int f,
+                                          double &ax, double &ay) {
   const int code = cMD.fnqsg[8 * isg + 2 * ivsg + f];
   const int slot = (code >= 0 ? code : -code) - 1;
-  slot_normal(X, Y, slot, n0, n1, a);
-  if (code < 0) { n0 = -n0; n1 = -n1; }
+  slot_an(X, Y, slot, ax, ay);
+  if (code < 0) { ax = -ax; ay = -ay; }
 }
 
-// m = mu * A of one corner face (getriecoef_matrixnew, Limiterlag.f90:1037);
+// m = mu * A * w of one corner face (getriecoef_matrixnew, Limiterlag.f90:1037)
+// from the face vector an: m = 2 w (rho c |an| + cimpd rho slpdu |du . an|);
 // the jump-direction branch needs |u* - u_c| >= 1e12 c
 __device__ __forceinline__ float corner_m(float rhoct, float sdctr, float cimpd, float slpdu, float dux, float duy,
-                                          float n0, float n1, float a) {
-  const float deltu = fabsf(dux * n0 + duy * n1);
-  const float murie = rhoct * sdctr + cimpd * rhoct * slpdu * deltu;
+                                          float ax, float ay, float w) {
+  const float nn = sqrtf(ax * ax + ay * ay);
+  const float dun = fabsf(dux * ax + duy * ay);
   const float j2 = dux * dux + duy * duy;
-  if (j2 * 1.0e-24f < sdctr * sdctr) return murie * a;
-  const float inv = rsqrtf(j2);
-  return murie * a * fabsf((n0 * dux + n1 * duy) * inv);
+  if (j2 * 1.0e-24f < sdctr * sdctr) return 2.0f * w * (rhoct * sdctr * nn + cimpd * rhoct * slpdu * dun);
+  const float murie = rhoct * sdctr + cimpd * rhoct * slpdu * (dun / nn);
+  return murie * 2.0f * w * fabsf((ax * dux + ay * duy) * rsqrtf(j2));
 }
 
 // node coordinates of quad iq as FP64 offsets from its centre node on the 3x3 tensor
@@ -265,15 +255,16 @@ __device__ __forceinline__ void vertex_state(const float u[4][6], const float *b
   }
 }
 
-// FP32 coefficients of one corner face from its FP64 normal: m and sigma.n A (sx, sy)
-__device__ __forceinline__ void corner_coeffs(double n0d, double n1d, double ad, float wrie, float pv, float rhoct,
-                                              float sdctr, float cimpd, float slpdu, float dux, float duy, float &m,
-                                              float &sx, float &sy) {
-  const float n0 = (float)n0d, n1 = (float)n1d;
-  const float aw = (float)ad * wrie;
-  m = corner_m(rhoct, sdctr, cimpd, slpdu, dux, duy, n0, n1, aw);
-  sx = -pv * aw * n0;
-  sy = -pv * aw * n1;
+// FP32 coefficients of one corner face from its FP64 face vector: m and
+// sigma.n A w = -p 2 w an (sx, sy)
+__device__ __forceinline__ void corner_coeffs(double axd, double ayd, float w, float pv, float rhoct, float sdctr,
+                                              float cimpd, float slpdu, float dux, float duy, float &m, float &sx,
+                                              float &sy) {
+  const float ax = (float)axd, ay = (float)ayd;
+  m = corner_m(rhoct, sdctr, cimpd, slpdu, dux, duy, ax, ay, w);
+  const float pw = -2.0f * pv * w;
+  sx = pw * ax;
+  sy = pw * ay;
 }
 
 // ---------------------------------------------------------------------------
@@ -312,11 +303,21 @@ __device__ void m_corner(const Dev &d, int iq) {
 #pragma unroll 1
     for (int i = 0; i < 5; i++) {
       const float r = (g5p(i) + ofr) * 0.5f;
+      // along the row r, det J is a cubic and tau a quadratic in s
+      float e[4];
+#pragma unroll
+      for (int n = 0; n < 4; n++) e[n] = Df[n] + r * (Df[4 + n] + r * (Df[8 + n] + r * Df[12 + n]));
+      const float dr = r - G.rc;
+      const float t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5f * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
+      const float t1 = u[0][2] + u[0][5] * dr, t2 = 0.5f * u[0][4];
+      const float wi = 0.25f * g5w(i);
 #pragma unroll
       for (int j = 0; j < 5; j++) {
         const float s = (g5p(j) + ofs) * 0.5f;
-        const float tau = eval_taylor(u[0], G, r, s);
-        masel += (g5w(i) * g5w(j) * 0.25f) * __fdividef(detevalf(Df, r, s), tau);
+        const float ds = s - G.sc;
+        const float tau = t0 + ds * (t1 + t2 * ds);
+        const float det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
+        masel += (wi * g5w(j)) * __fdividef(det, tau);
       }
     }
     const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
@@ -342,11 +343,10 @@ __device__ void m_corner(const Dev &d, int iq) {
       const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
 #pragma unroll
       for (int f = 0; f < 2; f++) {
-        double n0, n1, a;
-        corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
+        double ax, ay;
+        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
         float m, sx, sy;
-        corner_coeffs(n0, n1, a, cMT.wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx,
-                      sy);
+        corner_coeffs(ax, ay, cMT.wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy);
         P0 += (double)m;
         P1 += (double)m * (double)st[1];
         P2 += (double)m * (double)st[2];
@@ -411,14 +411,13 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
       const double wq = cMD.wmom[4 * isg + ivsg];
 #pragma unroll
       for (int f = 0; f < 2; f++) {
-        double n0, n1, a;
-        corner_face(L.X, L.Y, isg, ivsg, f, n0, n1, a);
+        double ax, ay;
+        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
         float m, sx, sy;
-        corner_coeffs(n0, n1, a, cMT.wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx,
-                      sy);
+        corner_coeffs(ax, ay, cMT.wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy);
         const double fs0 = (double)sx + (double)m * du0;
         const double fs1 = (double)sy + (double)m * du1;
-        tw += (un * n0 + vn * n1) * (a * cMD.wmas[8 * isg + 2 * ivsg + f]);
+        tw += (un * ax + vn * ay) * (2.0 * cMD.wmas[8 * isg + 2 * ivsg + f]);
         f0 += fs0 * wq;
         f1 += fs1 * wq;
         fe += (un * fs0 + vn * fs1) * wq;
