@@ -62,6 +62,16 @@ __host__ __device__ __forceinline__ void dlag3(double r, double *l) {
   l[2] = r + 0.5;
 }
 
+// cos(pi d) and sin(pi d) for |d| <= 0.15 from their Taylor series in
+// t = pi d, to degree 14 and 13 (the first omitted terms are below 1e-17)
+__host__ __device__ __forceinline__ void cossin_pi_small(double d, double &c, double &s) {
+  const double t = 3.14159265358979311599796346854 * d, t2 = t * t;
+  c = 1.0 + t2 * (-1.0 / 2.0 + t2 * (1.0 / 24.0 + t2 * (-1.0 / 720.0 + t2 * (1.0 / 40320.0 + t2 * (-1.0 / 3628800.0 +
+      t2 * (1.0 / 479001600.0 - t2 * (1.0 / 87178291200.0)))))));
+  s = t * (1.0 + t2 * (-1.0 / 6.0 + t2 * (1.0 / 120.0 + t2 * (-1.0 / 5040.0 + t2 * (1.0 / 362880.0 + t2 * (-1.0 /
+      39916800.0 + t2 * (1.0 / 6227020800.0)))))));
+}
+
 __host__ __device__ __forceinline__ double deteval(const double *D, double r, double s) {
   double e[4];
 #pragma unroll
@@ -557,6 +567,13 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
       Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
       Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
     }
+    // the DOFs along the row: u_q(s) = a_q + ds (b_q + c_q ds), ds = s - sc
+    double ra[4], rb[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      ra[q] = u[q][0] + u[q][1] * dr + u[q][3] * (0.5 * dr * dr - G.g19) - u[q][4] * G.g20 - u[q][5] * G.g21;
+      rb[q] = u[q][2] + u[q][5] * dr;
+    }
     const double wi = l5w(i);
 #pragma unroll
     for (int j = 0; j < 5; j++) {
@@ -569,10 +586,9 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
       const double yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
       const double xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
       const double ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
-      const double b3 = 0.5 * dr * dr - G.g19, b4 = 0.5 * ds * ds - G.g20, b5 = dr * ds - G.g21;
       double un[4];
 #pragma unroll
-      for (int q = 0; q < 4; q++) un[q] = u[q][0] + u[q][1] * dr + u[q][2] * ds + u[q][3] * b3 + u[q][4] * b4 + u[q][5] * b5;
+      for (int q = 0; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * u[q][4] * ds);
       const double rhoad = 1.0 / un[0];
       const double pres = fmax(eps, (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2])));
       // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
@@ -596,7 +612,9 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
   }
   if (d.ncase == 1) {
     // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:
-    // 4070-4251), 5x5 Gauss; cos(pi x) by cospi and cos(3t) = cos t (4 cos^2 t - 3)
+    // 4070-4251), 5x5 Gauss; cos(3t) = cos t (4 cos^2 t - 3).  cos(pi x) at
+    // the Gauss points by angle addition from the centre node x_c:
+    // cos(pi x) = cos(pi x_c) cos(pi d) - sin(pi x_c) sin(pi d), d = x - x_c.
     double c[36], D[16];
     {
       double xp[9][2];
@@ -605,6 +623,8 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
     }
     detpoly(c, D);
     const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
+    const double xc = L.X[1][1], yc = L.Y[1][1];
+    const double cxc = cospi(xc), sxc = sinpi(xc), cyc = cospi(yc), syc = sinpi(yc);
 #pragma unroll 1
     for (int i = 0; i < 5; i++) {
       const double r = g5p(i), dr = r - G.rc;
@@ -613,19 +633,32 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
       double Px[3], Py[3];
 #pragma unroll
       for (int bb = 0; bb < 3; bb++) {
-        Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
-        Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
+        Px[bb] = lr[0] * (L.X[0][bb] - xc) + lr[1] * (L.X[1][bb] - xc) + lr[2] * (L.X[2][bb] - xc);
+        Py[bb] = lr[0] * (L.Y[0][bb] - yc) + lr[1] * (L.Y[1][bb] - yc) + lr[2] * (L.Y[2][bb] - yc);
       }
+      double e[4];
+#pragma unroll
+      for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
       const double wi = g5w(i);
 #pragma unroll
       for (int j = 0; j < 5; j++) {
         const double s = g5p(j), ds = s - G.sc;
         double ls[3];
         lag3(s, ls);
-        const double xg = Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2];
-        const double yg = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
-        const double djaco = wi * g5w(j) * deteval(D, r, s);
-        const double cx = cospi(xg), cy = cospi(yg);
+        const double dx = Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2];
+        const double dy = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
+        const double djaco = wi * g5w(j) * (e[0] + s * (e[1] + s * (e[2] + s * e[3])));
+        double cx, cy;
+        if (fabs(dx) <= 0.15 && fabs(dy) <= 0.15) {
+          double cdx, sdx, cdy, sdy;
+          cossin_pi_small(dx, cdx, sdx);
+          cossin_pi_small(dy, cdy, sdy);
+          cx = cxc * cdx - sxc * sdx;
+          cy = cyc * cdy - syc * sdy;
+        } else {
+          cx = cospi(xc + dx);
+          cy = cospi(yc + dy);
+        }
         const double c3x = cx * (4.0 * cx * cx - 3.0), c3y = cy * (4.0 * cy * cy - 3.0);
         const double src = coef * (c3x * cy - c3y * cx) * djaco;
         el[0] += src;
