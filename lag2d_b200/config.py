@@ -11,7 +11,9 @@ from __future__ import annotations
 import dataclasses
 from typing import Tuple
 
-from .mesh import Mesh, quad_mesh
+import numpy as np
+
+from .mesh import Mesh, hybrid_mesh, quad_mesh
 
 __all__ = ["StepConfig", "workload", "WORKLOADS"]
 
@@ -64,6 +66,25 @@ def _sedov(n: int) -> Tuple[Mesh, StepConfig]:
     return m, c
 
 
+def _tgv_hybrid(n: int) -> Tuple[Mesh, StepConfig]:
+    """Taylor-Green on the tri/quad mesh of hybrid_mesh (alternate rows split)."""
+    m = hybrid_mesh(n, n, 0.0, 1.0, 0.0, 1.0)
+    c = StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=3, cfl=0.05, tend=10.0)
+    return m, c
+
+
+def _sedov_hybrid(n: int, jitter: float = 0.0) -> Tuple[Mesh, StepConfig]:
+    """Full-box Sedov on the tri/quad mesh (alternate rows split); the energy
+    goes to the first four cells (by id) that touch the centre node."""
+    m = hybrid_mesh(n, n, -1.2, 1.2, -1.2, 1.2, jitter=jitter, seed=1234)
+    d = np.abs(m.coord).sum(axis=1)
+    centre = int(np.argmin(d)) + 1
+    touch = [i + 1 for i in range(m.ntria) if centre in m.iptri[i]]
+    touch += [m.ntria + i + 1 for i in range(m.nquad) if centre in m.ipqua[i]]
+    c = StepConfig(ncase=7, gamlg=1.4, nstag=3, cfl=0.1, tend=1.0, sedov_cells=tuple(sorted(touch)[:4]))
+    return m, c
+
+
 WORKLOADS = {
     # Taylor-Green vortex: [0,1]^2, gamma 5/3, P2, RK3, energy source on
     "tgv1024": lambda: _tgv(1024),
@@ -76,6 +97,11 @@ WORKLOADS = {
     "sedov128": lambda: _sedov(128),
     "sedov32": lambda: _sedov(32),
     "sedov16": lambda: _sedov(16),
+    # the same cases on tri/quad meshes (alternate rows of quads split into triangles)
+    "tgv_hybrid16": lambda: _tgv_hybrid(16),
+    "tgv_hybrid64": lambda: _tgv_hybrid(64),
+    "sedov_hybrid16": lambda: _sedov_hybrid(16),
+    "sedov_hybrid_jitter16": lambda: _sedov_hybrid(16, jitter=0.1),
 }
 
 

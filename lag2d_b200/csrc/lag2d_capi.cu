@@ -48,6 +48,10 @@ void launch_mixed_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa);
 void launch_fast_nodes(const Dev &d, cudaStream_t st, double alfa);
 void launch_fast_geom(const Dev &d, cudaStream_t st, int fix);
 void launch_init_wmom(const Dev &d, cudaStream_t st);
+void launch_tri_init(const Dev &d, cudaStream_t st);
+void launch_tri_geom(const Dev &d, cudaStream_t st, const double *X, const double *Y);
+void launch_tri_corner(const Dev &d, cudaStream_t st);
+void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa);
 }  // namespace lag2d
 
 using namespace lag2d;
@@ -138,6 +142,17 @@ static void fill_rule(int n, bool lobatto, double (*pos)[2], double *w) {
 
 static const int kIPQSG[4][4] = {{0, 4, 8, 7}, {4, 1, 5, 8}, {8, 5, 2, 6}, {7, 8, 6, 3}};
 
+// 7-point triangle rule of rutope (dgflo2d.f90:2232-2254), the reference's literals
+static void fill_tri_rule7(double (*pos)[2], double *w) {
+  const double a = 0.333333333333333, b1 = 0.059715871789770, b2 = 0.470142064105115;
+  const double c1 = 0.797426985353087, c2 = 0.101286507323456;
+  const double p[7][2] = {{a, a}, {b1, b2}, {b2, b1}, {b2, b2}, {c1, c2}, {c2, c1}, {c2, c2}};
+  for (int i = 0; i < 7; i++) { pos[i][0] = p[i][0]; pos[i][1] = p[i][1]; }
+  w[0] = 0.225000000000000;
+  w[1] = w[2] = w[3] = 0.132394152788506;
+  w[4] = w[5] = w[6] = 0.125939180544827;
+}
+
 // WENO stencil of every quad from esqua and the cells-surrounding-point
 // lists, ordered as weno_stncl_quad_orthol3 orders it (WENO.f90:7646-7704).
 static void build_stencils(const lag2d_mesh *m, std::vector<int> &sten) {
@@ -147,9 +162,12 @@ static void build_stencils(const lag2d_mesh *m, std::vector<int> &sten) {
     const int ielem = iq + ntria;  // 0-based
     int ielaj[9];
     ielaj[0] = ielem + 1;
-    // the reference reads esqua at the global cell id here (WENO.f90:7648)
-    const bool inrange = ielem < nquad;
-    for (int k = 0; k < 4; k++) ielaj[1 + k] = inrange ? m->esqua[4 * (size_t)ielem + k] : 0;
+    // the reference reads esqua at the global cell id here (WENO.f90:7648);
+    // on a mesh with triangles that id leaves the quad range and the quad's
+    // own row is read instead
+    const int row = ntria > 0 ? iq : ielem;
+    const bool inrange = row < nquad;
+    for (int k = 0; k < 4; k++) ielaj[1 + k] = inrange ? m->esqua[4 * (size_t)row + k] : 0;
     for (int k = 5; k < 9; k++) ielaj[k] = 0;
     bool bad = false;
     for (int iv = 0; iv < 4 && !bad; iv++) {
@@ -175,9 +193,13 @@ static void build_stencils(const lag2d_mesh *m, std::vector<int> &sten) {
           else bad = true;
         }
     }
-    if (bad) { sten[iq] = -2; continue; }
+    // the reference stops on this valence (WENO.f90:7699); on a mesh with
+    // triangles it is the normal case next to them and the quad is skipped
+    if (bad) { sten[iq] = ntria > 0 ? -1 : -2; continue; }
     bool complete = true;
     for (int k = 0; k < 9; k++) complete &= ielaj[k] != 0;
+    // a stencil reaching a triangle is not a 3x3 quad block: left unlimited
+    for (int k = 0; k < 9; k++) complete &= ielaj[k] > ntria;
     if (!complete) continue;
     for (int k = 0; k < 9; k++) sten[k * (size_t)nquad + iq] = ielaj[k] - 1;
   }
@@ -227,34 +249,45 @@ static void enqueue_rhs(lag2d_handle *h) {
   const Dev &d = h->d;
   run(h, "persson", [&] { launch_reset_count(d, h->st); launch_persson(d, h->st); }, 2);
   run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
-  run(h, "corner", [&] { launch_corner(d, h->st); });
+  const int T = d.ntria > 0;
+  run(h, "corner", [&] { launch_tri_corner(d, h->st); launch_corner(d, h->st); }, 1 + T);
   run(h, "node", [&] { launch_node(d, h->st); });
-  run(h, "rhs", [&] { launch_rhs(d, h->st); });
+  run(h, "rhs", [&] { launch_tri_rhs(d, h->st, d.us, d.vs, 0, 0.0); launch_rhs(d, h->st); }, 1 + T);
+}
+
+// volumes of all cells at the coordinates (X, Y): triangles, then quads
+static void geom_all(lag2d_handle *h, const double *X, const double *Y) {
+  launch_tri_geom(h->d, h->st, X, Y);
+  launch_geom(h->d, h->st, X, Y);
 }
 
 // getsolvdg_lag (Getrhslag.f90:1553-2035) + the driver copy-back
 static void enqueue_step_reference_order(lag2d_handle *h, int itime) {
   const Dev &d = h->d;
   const int nstag = h->cfg.nstag;
-  run(h, "geom", [&] { launch_step_begin(d, h->st, itime); launch_geom(d, h->st, d.xn, d.yn); }, 2);
+  const int T = d.ntria > 0;
+  run(h, "geom", [&] { launch_step_begin(d, h->st, itime); geom_all(h, d.xn, d.yn); }, 2 + T);
   for (int istag = 1; istag <= nstag; istag++) {
     const double alfa = kRK[nstag - 2][istag - 1];
     enqueue_rhs(h);
     if (istag == 1) run(h, "dt", [&] { launch_dt(d, h->st, h->cfg.ndt); }, 2);
     run(h, "update", [&] { launch_update(d, h->st, alfa); });
     run(h, "nodes", [&] { launch_nodes(d, h->st, alfa); });
-    run(h, "geom", [&] { launch_center_geom(d, h->st); launch_geom(d, h->st, d.xs, d.ys); }, 2);
+    run(h, "geom", [&] { launch_center_geom(d, h->st); geom_all(h, d.xs, d.ys); }, 2 + T);
   }
   run(h, "copy", [&] { launch_copyback(d, h->st); launch_step_end(d, h->st, 1); }, 2);
 }
 
 // Corner and RHS passes of the optimised step: FP64, or the FP32-mixed form
 // (config precision = 1) with the same node pass, update and geometry.
+// Triangles run their FP64 kernels in both forms.
 static void corner_pass(lag2d_handle *h) {
+  launch_tri_corner(h->d, h->st);
   if (h->cfg.precision == 1) launch_mixed_corner(h->d, h->st);
   else launch_fast_corner(h->d, h->st);
 }
 static void rhs_pass(lag2d_handle *h, int fuse, double alfa) {
+  launch_tri_rhs(h->d, h->st, h->d.us_new, h->d.vs_new, fuse, alfa);
   if (h->cfg.precision == 1) launch_mixed_rhs(h->d, h->st, fuse, alfa);
   else launch_fast_rhs(h->d, h->st, fuse, alfa);
 }
@@ -265,22 +298,23 @@ static void rhs_pass(lag2d_handle *h, int fuse, double alfa) {
 static void enqueue_step_fast(lag2d_handle *h, int itime) {
   const Dev &d = h->d;
   const int nstag = h->cfg.nstag;
+  const int T = d.ntria > 0;
   run(h, "begin", [&] { launch_step_begin(d, h->st, itime); });
   for (int istag = 1; istag <= nstag; istag++) {
     const double alfa = kRK[nstag - 2][istag - 1];
     run(h, "persson", [&] { launch_reset_count(d, h->st); launch_fast_persson(d, h->st); }, 2);
     run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
-    run(h, "corner", [&] { corner_pass(h); });
+    run(h, "corner", [&] { corner_pass(h); }, 1 + T);
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
-      run(h, "rhs", [&] { rhs_pass(h, 0, alfa); });
+      run(h, "rhs", [&] { rhs_pass(h, 0, alfa); }, 1 + T);
       run(h, "dt", [&] { launch_dt(d, h->st, h->cfg.ndt); }, 2);
       run(h, "update", [&] { launch_fast_update(d, h->st, alfa); });
     } else {
-      run(h, "rhs", [&] { rhs_pass(h, 1, alfa); });
+      run(h, "rhs", [&] { rhs_pass(h, 1, alfa); }, 1 + T);
     }
     run(h, "nodes", [&] { launch_fast_nodes(d, h->st, alfa); });
-    run(h, "geom", [&] { launch_fast_geom(d, h->st, 1); });
+    run(h, "geom", [&] { launch_tri_geom(d, h->st, d.xs, d.ys); launch_fast_geom(d, h->st, 1); }, 1 + T);
   }
   run(h, "copy", [&] { launch_copyback(d, h->st); launch_step_end(d, h->st, 1); }, 2);
 }
@@ -312,7 +346,9 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
     return fail(LAG2D_EINVAL, "mesh sizes must be positive");
   if (!m->ipqua || !m->bface || !m->esuv1 || !m->esuv2 || !m->esqua || !m->coold)
     return fail(LAG2D_EINVAL, "missing mesh array");
-  if (m->ntria > 0) return fail(LAG2D_EUNSUP, "triangles are not built on this path yet");
+  if (m->ntria > 0 && !m->iptri) return fail(LAG2D_EINVAL, "missing iptri");
+  if (m->ntria > 0 && (c->ngausd != 7 || c->ngausd_geo != 7))
+    return fail(LAG2D_EUNSUP, "triangles need the 7-point rule (ngausd = ngausd_geo = 7)");
   if (c->npoly != 2 || c->ndegr != 6 || c->nq != 4 || c->ndens != 1)
     return fail(LAG2D_EUNSUP, "only P2 (npoly=2, ndegr=6, nq=4, ndens=1) is built");
   if (c->mdegr < 1 || c->mdegr > 6) return fail(LAG2D_EINVAL, "mdegr out of range");
@@ -325,6 +361,8 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   const int ncell = m->ntria + m->nquad;
   for (size_t i = 0; i < 9 * (size_t)m->nquad; i++)
     if (m->ipqua[i] < 1 || m->ipqua[i] > m->npoin) return fail(LAG2D_EINVAL, "ipqua node id out of range");
+  for (size_t i = 0; i < 6 * (size_t)m->ntria; i++)
+    if (m->iptri[i] < 1 || m->iptri[i] > m->npoin) return fail(LAG2D_EINVAL, "iptri node id out of range");
   for (size_t i = 0; i < (size_t)m->nbfac; i++) {
     const int *b = m->bface + 5 * i;
     if (b[0] < 1 || b[0] > m->npoin || b[1] < 1 || b[1] > m->npoin || b[4] < 1 || b[4] > m->npoin)
@@ -359,26 +397,47 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
       esq[k * (size_t)nq + iq] = (v >= 1 && v <= ncell) ? v - 1 : -1;
     }
   build_stencils(m, sten);
-  // node -> corner-face lists in the order getriem_quadsubg2 scatters
-  std::vector<int> cnt(np + 1, 0), nodecf(32 * (size_t)nq);
+  const int nt = m->ntria;
+  std::vector<int> ipt(6 * (size_t)nt);
+  for (int it = 0; it < nt; it++)
+    for (int k = 0; k < 6; k++) ipt[k * (size_t)nt + it] = m->iptri[6 * (size_t)it + k] - 1;
+  // node -> corner-face lists in the order getndvelo_lagsubg scatters them:
+  // getriem_triasubg3 (triangles, entries -1 - (it*24 + slot)), then
+  // getriem_quadsubg2 (quads, entries iq*32 + slot)
+  static const int kIPTSG[4][3] = {{0, 3, 5}, {3, 4, 5}, {3, 1, 4}, {5, 4, 2}};
+  std::vector<int> cnt(np + 1, 0), nodecf(24 * (size_t)nt + 32 * (size_t)nq);
+  for (int it = 0; it < nt; it++)
+    for (int isg = 0; isg < 4; isg++)
+      for (int ivsg = 0; ivsg < 3; ivsg++) cnt[ipt[kIPTSG[isg][ivsg] * (size_t)nt + it] + 1] += 2;
   for (int iq = 0; iq < nq; iq++)
     for (int isg = 0; isg < 4; isg++)
       for (int ivsg = 0; ivsg < 4; ivsg++) cnt[ipq[kIPQSG[isg][ivsg] * (size_t)nq + iq] + 1] += 2;
   for (int p = 0; p < np; p++) cnt[p + 1] += cnt[p];
   std::vector<int> fillp(cnt.begin(), cnt.end() - 1);
+  for (int it = 0; it < nt; it++)
+    for (int isg = 0; isg < 4; isg++)
+      for (int ivsg = 0; ivsg < 3; ivsg++) {
+        int p = ipt[kIPTSG[isg][ivsg] * (size_t)nt + it];
+        for (int f = 0; f < 2; f++) nodecf[fillp[p]++] = -1 - (it * 24 + (f + 2 * (ivsg + 3 * isg)));
+      }
   for (int iq = 0; iq < nq; iq++)
     for (int isg = 0; isg < 4; isg++)
       for (int ivsg = 0; ivsg < 4; ivsg++) {
         int p = ipq[kIPQSG[isg][ivsg] * (size_t)nq + iq];
         for (int f = 0; f < 2; f++) nodecf[fillp[p]++] = iq * 32 + (f + 2 * (ivsg + 4 * isg));
       }
-  // node -> (quad, local node) lists in cell order for the optimised gather
-  std::vector<int> cnt2(np + 1, 0), slots(9 * (size_t)nq);
+  // node -> (cell, local node) lists in cell order for the optimised gather:
+  // triangles -1 - (it*6 + k), then quads iq*9 + k
+  std::vector<int> cnt2(np + 1, 0), slots(6 * (size_t)nt + 9 * (size_t)nq);
+  for (int it = 0; it < nt; it++)
+    for (int k = 0; k < 6; k++) cnt2[ipt[k * (size_t)nt + it] + 1]++;
   for (int iq = 0; iq < nq; iq++)
     for (int k = 0; k < 9; k++) cnt2[ipq[k * (size_t)nq + iq] + 1]++;
   for (int p = 0; p < np; p++) cnt2[p + 1] += cnt2[p];
   {
     std::vector<int> fp(cnt2.begin(), cnt2.end() - 1);
+    for (int it = 0; it < nt; it++)
+      for (int k = 0; k < 6; k++) slots[fp[ipt[k * (size_t)nt + it]]++] = -1 - (it * 6 + k);
     for (int iq = 0; iq < nq; iq++)
       for (int k = 0; k < 9; k++) slots[fp[ipq[k * (size_t)nq + iq]]++] = iq * 9 + k;
   }
@@ -415,7 +474,10 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   A(&ptr2_d, cnt2.size()); A(&slot_d, slots.size());
   A(&d.npart, 45 * (size_t)nq); A(&d.corr, 4 * (size_t)nq); A(&d.us_new, np); A(&d.vs_new, np);
   A(&d.wmom, 9 * (size_t)nq);
+  int *ipt_d;
+  A(&ipt_d, ipt.size()); A(&d.tmsub, 4 * (size_t)nt); A(&d.tcf, 5 * 24 * (size_t)nt); A(&d.tpart, 5 * 6 * (size_t)nt);
   if (rc != LAG2D_OK) { lag2d_destroy(h); return rc; }
+  d.ipt = ipt_d;
   d.ipq = ipq_d; d.esq = esq_d; d.stencil = sten_d; d.node_ptr = ptr_d; d.node_cf = ncf_d;
   d.bcmask = mask_d; d.x0 = x0; d.y0 = y0;
   d.node_ptr2 = ptr2_d; d.node_slot = slot_d;
@@ -426,16 +488,19 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   UP(ptr_d, cnt.data(), cnt.size()); UP(ncf_d, nodecf.data(), nodecf.size()); UP(mask_d, mask.data(), mask.size());
   UP(x0, xx.data(), np); UP(y0, yy.data(), np);
   UP(ptr2_d, cnt2.data(), cnt2.size()); UP(slot_d, slots.data(), slots.size());
+  if (nt) UP(ipt_d, ipt.data(), ipt.size());
   UP(d.xn, xx.data(), np); UP(d.yn, yy.data(), np); UP(d.xs, xx.data(), np); UP(d.ys, yy.data(), np);
 #undef UP
   QuadTables qt;
   fill_rule(5, false, qt.g25, qt.w25);
   fill_rule(6, false, qt.g36, qt.w36);
   fill_rule(5, true, qt.l25, qt.wl25);
+  fill_tri_rule7(qt.t7, qt.tw7);
   set_tables(qt, h->st);
   Scalars s0{};
   cudaMemcpyAsync(d.sc_dev, &s0, sizeof(Scalars), cudaMemcpyHostToDevice, h->st);
-  run(h, "init", [&] { launch_init_msub(d, h->st); launch_init_wmom(d, h->st); }, 2);
+  run(h, "init", [&] { launch_init_msub(d, h->st); launch_init_wmom(d, h->st); launch_tri_init(d, h->st); },
+      2 + (nt > 0));
   if (cudaStreamSynchronize(h->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     lag2d_destroy(h);
     return fail(LAG2D_ECUDA, "device set-up failed");
@@ -484,7 +549,7 @@ int lag2d_init_fields(lag2d_handle *h, double *geoel, double *amatr, double *unk
   if (!h) return fail(LAG2D_EINVAL, "null handle");
   Dev &d = h->d;
   const int ncell = d.ncell, np = d.npoin;
-  run(h, "init", [&] { launch_init(d, h->st); }, 2);
+  run(h, "init", [&] { launch_tri_init(d, h->st); launch_init(d, h->st); }, 2 + (d.ntria > 0));
   CK(cudaMemcpyAsync(d.Us, d.Un, NU * (size_t)ncell * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
   CK(cudaMemcpyAsync(d.xn, d.x0, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
   CK(cudaMemcpyAsync(d.yn, d.y0, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
@@ -492,7 +557,7 @@ int lag2d_init_fields(lag2d_handle *h, double *geoel, double *amatr, double *unk
   CK(cudaMemcpyAsync(d.ys, d.y0, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
   CK(cudaMemsetAsync(d.us, 0, np * sizeof(double), h->st));
   CK(cudaMemsetAsync(d.vs, 0, np * sizeof(double), h->st));
-  run(h, "geom", [&] { launch_geom(d, h->st, d.xn, d.yn); });
+  run(h, "geom", [&] { geom_all(h, d.xn, d.yn); }, 1 + (d.ntria > 0));
   int st = read_status(h);
   if (st != LAG2D_OK) return st;
   if (geoel) { int r = download_geoel(h, geoel); if (r) return r; }
@@ -541,7 +606,7 @@ int lag2d_set_state(lag2d_handle *h, const double *unkno, const double *coord, c
   }
   Scalars s0{};
   CK(cudaMemcpyAsync(d.sc_dev, &s0, sizeof(Scalars), cudaMemcpyHostToDevice, h->st));
-  run(h, "geom", [&] { launch_geom(d, h->st, d.xs, d.ys); });
+  run(h, "geom", [&] { geom_all(h, d.xs, d.ys); }, 1 + (d.ntria > 0));
   return read_status(h);
 }
 
@@ -637,13 +702,13 @@ int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
   }
   run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
   if (ex) {
-    run(h, "corner", [&] { launch_corner(d, h->st); });
+    run(h, "corner", [&] { launch_tri_corner(d, h->st); launch_corner(d, h->st); }, 1 + (d.ntria > 0));
     run(h, "node", [&] { launch_node(d, h->st); });
-    run(h, "rhs", [&] { launch_rhs(d, h->st); });
+    run(h, "rhs", [&] { launch_tri_rhs(d, h->st, d.us, d.vs, 0, 0.0); launch_rhs(d, h->st); }, 1 + (d.ntria > 0));
   } else {
-    run(h, "corner", [&] { corner_pass(h); });
+    run(h, "corner", [&] { corner_pass(h); }, 1 + (d.ntria > 0));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
-    run(h, "rhs", [&] { rhs_pass(h, 0, 0.0); });
+    run(h, "rhs", [&] { rhs_pass(h, 0, 0.0); }, 1 + (d.ntria > 0));
     // the RHS keeps ustar of the previous stage for the impedances; expose the new one
     CK(cudaMemcpyAsync(d.us, d.us_new, d.npoin * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemcpyAsync(d.vs, d.vs_new, d.npoin * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
@@ -687,7 +752,7 @@ int lag2d_weno(lag2d_handle *h, const int *flags) {
 
 int lag2d_cellvol(lag2d_handle *h, double *geoel) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
-  run(h, "geom", [&] { launch_geom(h->d, h->st, h->d.xs, h->d.ys); });
+  run(h, "geom", [&] { geom_all(h, h->d.xs, h->d.ys); }, 1 + (h->d.ntria > 0));
   int r = read_status(h);
   if (r) return r;
   if (geoel) return download_geoel(h, geoel);

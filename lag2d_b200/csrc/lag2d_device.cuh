@@ -6,7 +6,9 @@
 //   ipq[k*nquad + iq]        node k (0..8) of quad iq
 //   cf[(v*32 + slot)*nquad + iq]  corner coefficient v (m, m*u, m*v, s_x, s_y)
 //                                  of corner-face slot = f + 2*(ivsg + 4*isg)
-// Quads are cells ntria..ncell-1 (the reference numbers triangles first).
+//   ipt[k*ntria + it], tcf[(v*24 + slot)*ntria + it]   the same for triangles
+//                                  (slot = f + 2*(ivsg + 3*isg))
+// Triangles are cells 0..ntria-1, quads ntria..ncell-1 (the reference's order).
 #pragma once
 #include <cstdint>
 
@@ -65,6 +67,11 @@ struct Dev {
   double *corr;            // [4][nquad] sub-cell density corrections
   double *us_new, *vs_new; // ustar of the current stage (us, vs hold the previous one)
   double *wmom;            // [9][nquad] time-invariant mass-weighted shape moments
+  // triangles (cells 0..ntria-1)
+  const int *ipt;          // [6][ntria] node k of triangle it
+  double *tmsub;           // [4][ntria] initial sub-cell masses
+  double *tcf;             // [5][24][ntria] corner coefficients (m, m u, m v, sigma.n A) per corner face
+  double *tpart;           // [5][6][ntria] their per-node sums
 };
 
 // Quadrature tables (filled from the host with the reference's literals).
@@ -72,6 +79,7 @@ struct QuadTables {
   double g25[25][2], w25[25];   // 5x5 Gauss (ruqope)
   double g36[36][2], w36[36];   // 6x6 Gauss (ruqope)
   double l25[25][2], wl25[25];  // 5x5 Gauss-Lobatto (ruqope_lobatto)
+  double t7[7][2], tw7[7];      // 7-point triangle rule (rutope)
 };
 
 }  // namespace lag2d

@@ -465,6 +465,16 @@ __host__ __device__ void f_node(const Dev &d, int p) {
   const int b = d.node_ptr2[p], en = d.node_ptr2[p + 1];
   for (int i = b; i < en; i++) {
     const int id = d.node_slot[i];
+    if (id < 0) {  // triangle: -1 - (it*6 + k), partials of its node k
+      const int t = -1 - id, it = t / 6, k = t - 6 * it;
+      const size_t nt = d.ntria;
+      mn += d.tpart[(0 * 6 + k) * nt + it];
+      mu0 += d.tpart[(1 * 6 + k) * nt + it];
+      mu1 += d.tpart[(2 * 6 + k) * nt + it];
+      sn0 += d.tpart[(3 * 6 + k) * nt + it];
+      sn1 += d.tpart[(4 * 6 + k) * nt + it];
+      continue;
+    }
     const int iq = id / 9, k = id - 9 * iq;
     mn += d.npart[(0 * 9 + k) * (size_t)d.nquad + iq];
     mu0 += d.npart[(1 * 9 + k) * (size_t)d.nquad + iq];

@@ -28,6 +28,7 @@ struct Tables {
   double wrie[4][4][2];   // corner-face weights of the Riemann solver
   double wmas[4][4][2];   // mass-equation face weights of the face integral
   double wmom[4][4];      // momentum/energy face weights of the face integral
+  double wtri[4][3][2];   // triangle corner-face weights (Getrhslaggauss.f90:12289-12302) x 0.25
 };
 __constant__ Tables cT;
 static Tables hT;
@@ -943,16 +944,31 @@ __host__ __device__ void b_node(const Dev &d, int p) {
   const int b = d.node_ptr[p], en = d.node_ptr[p + 1];
   for (int i = b; i < en; i++) {
     const int id = d.node_cf[i];
-    const int iq = id >> 5, slot = id & 31;
-    const double m = d.cf[(0 * 32 + slot) * d.nquad + iq];
+    double m, a1, a2, a3, a4;
+    if (id < 0) {  // triangle corner face: -1 - (it*24 + slot)
+      const int t = -1 - id, it = t / 24, slot = t - 24 * it;
+      const size_t nt = d.ntria;
+      m = d.tcf[(0 * 24 + slot) * nt + it];
+      a1 = d.tcf[(1 * 24 + slot) * nt + it];
+      a2 = d.tcf[(2 * 24 + slot) * nt + it];
+      a3 = d.tcf[(3 * 24 + slot) * nt + it];
+      a4 = d.tcf[(4 * 24 + slot) * nt + it];
+    } else {
+      const int iq = id >> 5, slot = id & 31;
+      m = d.cf[(0 * 32 + slot) * d.nquad + iq];
+      a1 = d.cf[(1 * 32 + slot) * d.nquad + iq];
+      a2 = d.cf[(2 * 32 + slot) * d.nquad + iq];
+      a3 = d.cf[(3 * 32 + slot) * d.nquad + iq];
+      a4 = d.cf[(4 * 32 + slot) * d.nquad + iq];
+    }
     mn0 = mn0 + m;
     mn1 = mn1 + 0.0;
     mn2 = mn2 + 0.0;
     mn3 = mn3 + m;
-    mu0 = mu0 + d.cf[(1 * 32 + slot) * d.nquad + iq];
-    mu1 = mu1 + d.cf[(2 * 32 + slot) * d.nquad + iq];
-    sn0 = sn0 + d.cf[(3 * 32 + slot) * d.nquad + iq];
-    sn1 = sn1 + d.cf[(4 * 32 + slot) * d.nquad + iq];
+    mu0 = mu0 + a1;
+    mu1 = mu1 + a2;
+    sn0 = sn0 + a3;
+    sn1 = sn1 + a4;
   }
   const unsigned char mask = d.bcmask[p];
   double us = d.us[p], vs = d.vs[p];
@@ -1561,6 +1577,593 @@ void launch_xy_out(int n, cudaStream_t st, double *xy, const double *x, const do
 // ---------------------------------------------------------------------------
 // Host-side launchers
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Triangles (6-node, P2 map on the reference triangle (0,0), (1,0), (0,1);
+// nodes 1-3 vertices, 4 on edge 1-2, 5 on edge 2-3, 6 on edge 3-1).  The
+// same stage as the quads: init (GetInitial.f90 triangle loops), volume
+// (getcellvol_lag :1908-2036), corner coefficients (getriem_triasubg3 with
+// getrhosubgt_average2, Getrhslaggauss.f90:12201-12945), face integral
+// (rhsifacedg_lagsubgt3 :8297-8496), volume integral
+// (rhsdomndg_lagmc_curvtria, Getrhslag.f90:4449-4711) and source
+// (rhsdomnsrcdg_lag_curvtria :3907-4066).  Triangles are cells 0..ntria-1.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ void shp6v(double r, double s, double *shp) {
+  const double c10 = 1.0;
+  shp[0] = -(c10 - r - s) * (c10 - 2.0 * (c10 - r - s));
+  shp[1] = -r * (c10 - 2.0 * r);
+  shp[2] = -s * (c10 - 2.0 * s);
+  shp[3] = 4.0 * r * (c10 - r - s);
+  shp[4] = 4.0 * r * s;
+  shp[5] = 4.0 * s * (c10 - r - s);
+}
+__host__ __device__ __forceinline__ void shp6d(double r, double s, double *dspr, double *dsps) {
+  const double c10 = 1.0;
+  dspr[0] = c10 - 4.0 * (c10 - r - s);
+  dspr[1] = -1.0 + 4.0 * r;
+  dspr[2] = 0.0;
+  dspr[3] = 4.0 * (1.0 - 2.0 * r - s);
+  dspr[4] = 4.0 * s;
+  dspr[5] = -4.0 * s;
+  dsps[0] = c10 - 4.0 * (c10 - r - s);
+  dsps[1] = 0.0;
+  dsps[2] = -1.0 + 4.0 * s;
+  dsps[3] = -4.0 * r;
+  dsps[4] = 4.0 * r;
+  dsps[5] = 4.0 * (1.0 - r - 2.0 * s);
+}
+__host__ __device__ __forceinline__ Jac jac6(const double (*xp)[2], const double *dspr, const double *dsps) {
+  Jac j = {0.0, 0.0, 0.0, 0.0};
+  for (int k = 0; k < 6; k++) {
+    j.xr = j.xr + dspr[k] * xp[k][0];
+    j.xs = j.xs + dsps[k] * xp[k][0];
+    j.yr = j.yr + dspr[k] * xp[k][1];
+    j.ys = j.ys + dsps[k] * xp[k][1];
+  }
+  return j;
+}
+__host__ __device__ __forceinline__ void map6(const double (*xp)[2], const double *shp, double &x, double &y) {
+  x = 0.0;
+  y = 0.0;
+  for (int k = 0; k < 6; k++) {
+    x = x + shp[k] * xp[k][0];
+    y = y + shp[k] * xp[k][1];
+  }
+}
+__host__ __device__ __forceinline__ void load_tria(const Dev &d, const double *X, const double *Y, int it,
+                                                   double (*xp)[2]) {
+  for (int k = 0; k < 6; k++) {
+    const int p = d.ipt[k * d.ntria + it];
+    xp[k][0] = X[p];
+    xp[k][1] = Y[p];
+  }
+}
+__host__ __device__ __forceinline__ double xvt(int k) {
+  const double v[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
+  return v[k];
+}
+__host__ __device__ __forceinline__ double yvt(int k) {
+  const double v[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
+  return v[k];
+}
+// sub-triangle vertices (1-based node ids) and face slots (getriem_triasubg3 :12264-12287)
+__host__ __device__ __forceinline__ int iptsg(int isg, int ivsg) {
+  const int t[12] = {1, 4, 6, 4, 5, 6, 4, 2, 5, 6, 5, 3};
+  return t[3 * isg + ivsg];
+}
+__host__ __device__ __forceinline__ int fntsg(int isg, int k) {
+  const int t[24] = {6, 1, 10, -7, -13, 12, 7, 14, 8, 15, 9, 13, -14, 10, 2, 3, 11, -8, 12, -9, -15, 11, 4, 5};
+  return t[6 * isg + k];
+}
+// Taylor basis of a triangle at (r, s), scale 1/2 in r and s
+__host__ __device__ __forceinline__ void tri_basis(double rc, double sc, double g19, double g20, double g21,
+                                                   double r, double s, double *b) {
+  b[0] = 1.0;
+  b[1] = (r - rc) / 0.5;
+  b[2] = (s - sc) / 0.5;
+  b[3] = 0.5 * b[1] * b[1] - g19;
+  b[4] = 0.5 * b[2] * b[2] - g20;
+  b[5] = b[1] * b[2] - g21;
+}
+
+// Initial geometry and DOFs of one triangle (getgeoel_initial_lag :1334-1478,
+// getgeoelho_initial_lag :1754-1905, inifield_mcnew Getrhslagmc.f90:3344-3480,
+// getunkno_initial_lag GetInitial.f90:190-411) and its initial sub-cell
+// masses (getrhosubgt_average2, Getrhslaggauss.f90:12860-12940).
+__host__ __device__ void b_tri_init(const Dev &d, int it) {
+  if (it >= d.ntria) return;
+  const int e = it;
+  const double alfrz = 0.0;
+  double xp[6][2], shp[6], dspr[6], dsps[6];
+  load_tria(d, d.x0, d.y0, it, xp);
+  double xc, yc;
+  shp6v(1.0 / 3.0, 1.0 / 3.0, shp);
+  map6(xp, shp, xc, yc);
+  double xcent = 0, ycent = 0, volel = 0, masel = 0;
+  for (int ig = 0; ig < 7; ig++) {
+    const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+    shp6v(r, s, shp);
+    shp6d(r, s, dspr, dsps);
+    Jac j = jac6(xp, dspr, dsps);
+    const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map6(xp, shp, xg, yg);
+    const double rhog = rho_initial(d, xc, yc);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    masel = masel + rhog * djaco * rcoef;
+    volel = volel + djaco * rcoef;
+    xcent = xcent + rhog * r * djaco * rcoef;
+    ycent = ycent + rhog * s * djaco * rcoef;
+  }
+  const double rc = xcent / masel, sc = ycent / masel;
+  d.rc[e] = rc;
+  d.sc[e] = sc;
+  d.vol[e] = volel;
+  d.mass[e] = masel;
+  shp6v(rc, sc, shp);
+  map6(xp, shp, xc, yc);
+  double bt[6] = {0, 0, 0, 0, 0, 0};
+  for (int ig = 0; ig < 7; ig++) {
+    const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+    shp6v(r, s, shp);
+    shp6d(r, s, dspr, dsps);
+    Jac j = jac6(xp, dspr, dsps);
+    const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map6(xp, shp, xg, yg);
+    const double rhog = rho_initial(d, xc, yc);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    bt[1] = (r - rc) / 0.5;
+    bt[2] = (s - sc) / 0.5;
+    bt[3] = bt[3] + 0.5 * rhog * bt[1] * bt[1] * djaco * rcoef;
+    bt[4] = bt[4] + 0.5 * rhog * bt[2] * bt[2] * djaco * rcoef;
+    bt[5] = bt[5] + rhog * bt[1] * bt[2] * djaco * rcoef;
+  }
+  const double g19 = bt[3] / masel, g20 = bt[4] / masel, g21 = bt[5] / masel;
+  d.g19[e] = g19;
+  d.g20[e] = g20;
+  d.g21[e] = g21;
+  // cell averages (the centroid of the P2 triangle is the reference's xcel)
+  const double xce = (-xp[0][0] - xp[1][0] - xp[2][0] + 4.0 * xp[3][0] + 4.0 * xp[4][0] + 4.0 * xp[5][0]) / 9.0;
+  const double yce = (-xp[0][1] - xp[1][1] - xp[2][1] + 4.0 * xp[3][1] + 4.0 * xp[4][1] + 4.0 * xp[5][1]) / 9.0;
+  double unkin[4], rv[4] = {0, 0, 0, 0};
+  for (int ig = 0; ig < 7; ig++) {
+    const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+    shp6v(r, s, shp);
+    shp6d(r, s, dspr, dsps);
+    Jac j = jac6(xp, dspr, dsps);
+    const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map6(xp, shp, xg, yg);
+    getunkin(d, unkin, xg, yg, e + 1, volel, xce, yce);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
+  }
+  double u0[4];
+  for (int q = 0; q < 4; q++) u0[q] = rv[q] / masel;
+  // M^-1 and the L2 projection of the higher moments
+  double rhsini[6][4], mmatr[25], matri[25];
+  for (int k = 0; k < 6; k++) for (int q = 0; q < 4; q++) rhsini[k][q] = 0.0;
+  for (int i = 0; i < 25; i++) mmatr[i] = 0.0;
+  double f0 = 0.0;
+  for (int ig = 0; ig < 7; ig++) {
+    const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+    shp6v(r, s, shp);
+    shp6d(r, s, dspr, dsps);
+    Jac j = jac6(xp, dspr, dsps);
+    const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map6(xp, shp, xg, yg);
+    double b[6];
+    tri_basis(rc, sc, g19, g20, g21, r, s, b);
+    getunkin(d, unkin, xg, yg, e + 1, volel, xc, yc);
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * b[k] * djaco;
+    const double rho0 = rho_initial(d, xc, yc);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    f0 = f0 + rho0 * djaco * rcoef;
+    for (int ix = 0; ix < 5; ix++)
+      for (int iy = 0; iy < 5; iy++) mmatr[ix + 5 * iy] = mmatr[ix + 5 * iy] + rho0 * b[ix + 1] * b[iy + 1] * djaco * rcoef;
+  }
+  getinvmat5(mmatr, matri);
+  {
+    int k = 0;
+    for (int im = 0; im < 5; im++)
+      for (int jm = im; jm < 5; jm++) d.amatr[(k++) * d.ncell + e] = matri[im + 5 * jm];
+    d.amatr[15 * d.ncell + e] = 1.0 / f0;
+  }
+  for (int q = 0; q < 4; q++) {
+    d.Un[(q * NDEG + 0) * d.ncell + e] = u0[q];
+    for (int ix = 0; ix < 5; ix++) {
+      double acc = 0.0;
+      for (int iy = 0; iy < 5; iy++) acc = acc + matri[ix + 5 * iy] * rhsini[iy + 1][q];
+      d.Un[(q * NDEG + ix + 1) * d.ncell + e] = acc;
+    }
+  }
+  // initial sub-cell masses: sub-triangles of the initial map, 6-node each
+  {
+    const double postc[9][2] = {{0.25, 0.0}, {0.75, 0.0}, {0.75, 0.25}, {0.25, 0.75}, {0.0, 0.75},
+                                {0.0, 0.25}, {0.25, 0.25}, {0.5, 0.25}, {0.25, 0.5}};
+    const int iptsc[4][3] = {{1, 7, 6}, {8, 9, 7}, {2, 3, 8}, {9, 4, 5}};
+    double xptic[9][2];
+    for (int isc = 0; isc < 9; isc++) {
+      shp6v(postc[isc][0], postc[isc][1], shp);
+      map6(xp, shp, xptic[isc][0], xptic[isc][1]);
+    }
+    double xci, yci;
+    shp6v(1.0 / 3.0, 1.0 / 3.0, shp);
+    map6(xp, shp, xci, yci);
+    for (int isg = 0; isg < 4; isg++) {
+      double xs[6][2];
+      for (int k = 0; k < 3; k++)
+        for (int c = 0; c < 2; c++) {
+          xs[k][c] = xp[iptsg(isg, k) - 1][c];
+          xs[3 + k][c] = xptic[iptsc[isg][k] - 1][c];
+        }
+      double rhs = 0.0;
+      for (int ig = 0; ig < 7; ig++) {
+        shp6d(cQ.t7[ig][0], cQ.t7[ig][1], dspr, dsps);
+        Jac j = jac6(xs, dspr, dsps);
+        const double djaco = 0.5 * cQ.tw7[ig] * (j.xr * j.ys - j.yr * j.xs);
+        rhs = rhs + rho_initial(d, xci, yci) * 1.0 * djaco;
+      }
+      d.tmsub[isg * d.ntria + it] = rhs;
+    }
+  }
+}
+__global__ void k_tri_init(Dev d) { b_tri_init(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// getcellvol_lag triangle loop (Limiterlag.f90:1908-2036): volume and its
+// centre in reference coordinates
+__host__ __device__ void b_tri_geom(const Dev &d, int it, const double *X, const double *Y) {
+  if (it >= d.ntria || stopped(d)) return;
+  const double alfrz = 0.0;
+  double xp[6][2], shp[6], dspr[6], dsps[6];
+  load_tria(d, X, Y, it, xp);
+  double rcv = 0, scv = 0, volel = 0;
+  for (int ig = 0; ig < 7; ig++) {
+    const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+    shp6v(r, s, shp);
+    shp6d(r, s, dspr, dsps);
+    Jac j = jac6(xp, dspr, dsps);
+    double xg, yg;
+    map6(xp, shp, xg, yg);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+    volel = volel + djaco * rcoef;
+    rcv = rcv + r * djaco * rcoef;
+    scv = scv + s * djaco * rcoef;
+  }
+  d.vol[it] = volel;
+  d.vcx[it] = rcv / volel;
+  d.vcy[it] = scv / volel;
+  if (!(volel > 0.0)) atomic_or(&d.sc_dev->status, ST_NONPHYS);
+}
+__global__ void k_tri_geom(Dev d, const double *X, const double *Y) {
+  b_tri_geom(d, blockIdx.x * blockDim.x + threadIdx.x, X, Y);
+}
+
+// Sub-cell face normals gesgt(3,15) of a triangle (getfnds_lagsms_simpsonhybrid
+// :9735-9853 for slots 1-6 and 10-12, getfnds_lagsmsif_hybrid :3432-3520
+// for slots 7-9 and 13-15)
+__host__ __device__ void normals_tria(const double (*xpt)[2], double (*gt)[3]) {
+  const double postc[3][2] = {{0.25, 0.25}, {0.5, 0.25}, {0.25, 0.5}};
+  const int ipift[3][3] = {{4, 6, 1}, {5, 4, 2}, {6, 5, 3}};
+  double xptv[3][2], shp[6];
+  for (int isv = 0; isv < 3; isv++) {
+    shp6v(postc[isv][0], postc[isv][1], shp);
+    map6(xpt, shp, xptv[isv][0], xptv[isv][1]);
+  }
+  for (int ifa = 0; ifa < 3; ifa++) {
+    double xpf[3][2];
+    for (int c = 0; c < 2; c++) {
+      xpf[0][c] = xpt[ipift[ifa][0] - 1][c];
+      xpf[1][c] = xpt[ipift[ifa][1] - 1][c];
+      xpf[2][c] = xptv[ipift[ifa][2] - 1][c];
+    }
+    for (int end = 0; end < 2; end++) {
+      const double r = end == 0 ? -1.0 : 1.0;
+      const double dshpr[3] = {-0.5 + r, 0.5 + r, -2.0 * r};
+      double dxdr = 0.0, dydr = 0.0;
+      for (int k = 0; k < 3; k++) {
+        dxdr = dxdr + dshpr[k] * xpf[k][0];
+        dydr = dydr + dshpr[k] * xpf[k][1];
+      }
+      const double djaco = sqrt(dxdr * dxdr + dydr * dydr);
+      const double anx = -dydr, any = dxdr;
+      const int slot = (end == 0 ? 6 : 12) + ifa;
+      gt[slot][0] = anx / sqrt(anx * anx + any * any);
+      gt[slot][1] = any / sqrt(anx * anx + any * any);
+      gt[slot][2] = djaco * 2.0;
+    }
+  }
+  const double posit[9][2] = {{0, 0}, {1, 0}, {1, 0}, {0, 1}, {0, 1}, {0, 0}, {0.5, 0}, {0.5, 0.5}, {0, 0.5}};
+  for (int ig = 0; ig < 9; ig++) {
+    double dspr[6], dsps[6];
+    shp6d(posit[ig][0], posit[ig][1], dspr, dsps);
+    Jac j = jac6(xpt, dspr, dsps);
+    const double c11 = j.ys, c12 = -j.yr, c21 = -j.xs, c22 = j.xr;
+    const int g1 = ig + 1;
+    double vn0, vn1, larea;
+    if (g1 == 1 || g1 == 2 || g1 == 7) { vn0 = 0.0; vn1 = -1.0; larea = 1.0; }
+    else if (g1 == 3 || g1 == 4 || g1 == 8) { vn0 = sqrt(2.0) * 0.5; vn1 = sqrt(2.0) * 0.5; larea = sqrt(2.0); }
+    else { vn0 = -1.0; vn1 = 0.0; larea = 1.0; }
+    const double anx = c11 * vn0 + c12 * vn1;
+    const double any = c21 * vn0 + c22 * vn1;
+    const double v0 = anx * larea, v1 = any * larea;
+    const double farea = sqrt(v0 * v0 + v1 * v1);
+    const int slot = ig < 6 ? ig : ig + 3;
+    gt[slot][0] = anx * larea / farea;
+    gt[slot][1] = any * larea / farea;
+    gt[slot][2] = farea;
+  }
+}
+
+// corner-face normal (unit n, weighted area) of face f of vertex ivsg of sub-triangle isg
+__host__ __device__ __forceinline__ void tri_corner_normal(const double (*gt)[3], int isg, int ivsg, int f,
+                                                           double &n0, double &n1, double &a) {
+  const int code = fntsg(isg, 2 * ivsg + f);
+  const int slot = (code >= 0 ? code : -code) - 1;
+  const double sg = code >= 0 ? 1.0 : -1.0;
+  n0 = sg * gt[slot][0];
+  n1 = sg * gt[slot][1];
+  a = gt[slot][2] * TB().wtri[isg][ivsg][f];
+}
+
+// Corner coefficients of one triangle (getriem_triasubg3): per corner face
+// (f + 2 (ivsg + 3 isg)) the values m, m u_c, m v_c, sigma.n A (2) into
+// tcf, and their per-node sums into tpart (node k of the triangle, in the
+// face order above).  Triangles carry no impedance jump term and no cdrho.
+__host__ __device__ void b_tri_corner(const Dev &d, int it) {
+  if (it >= d.ntria || stopped(d)) return;
+  const int e = it;
+  const double eps = 1.0e-15, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
+  const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
+  double xpt[6][2];
+  load_tria(d, d.xs, d.ys, it, xpt);
+  double gt[15][3];
+  normals_tria(xpt, gt);
+  double u[4][6];
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) u[q][k] = Uget(d, d.Us, k, q, e);
+  const double rhomc = u[0][0];
+  const double rhoct = 1.0 / rhomc;
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
+  double unknvt[6][4];
+  for (int iv = 0; iv < 6; iv++) {
+    double b[6];
+    tri_basis(rc, sc, g19, g20, g21, xvt(iv), yvt(iv), b);
+    for (int q = 0; q < 4; q++) {
+      unknvt[iv][q] = 0.0;
+      for (int k = 0; k < d.mdegr; k++) unknvt[iv][q] = unknvt[iv][q] + u[q][k] * b[k];
+    }
+  }
+  // sub-cell densities (getrhosubgt_average2): current sub-cell volumes and
+  // the harmonic tau mean over each sub-triangle
+  double unksgt[4], utsgc[4];
+  {
+    const double postc[9][2] = {{0.25, 0.0}, {0.75, 0.0}, {0.75, 0.25}, {0.25, 0.75}, {0.0, 0.75},
+                                {0.0, 0.25}, {0.25, 0.25}, {0.5, 0.25}, {0.25, 0.5}};
+    const int iptsc[4][3] = {{1, 7, 6}, {8, 9, 7}, {2, 3, 8}, {9, 4, 5}};
+    double xptc[9][2], shp[6], dspr[6], dsps[6];
+    for (int isc = 0; isc < 9; isc++) {
+      shp6v(postc[isc][0], postc[isc][1], shp);
+      map6(xpt, shp, xptc[isc][0], xptc[isc][1]);
+    }
+    for (int isg = 0; isg < 4; isg++) {
+      double xs[6][2];
+      for (int k = 0; k < 3; k++)
+        for (int c = 0; c < 2; c++) {
+          xs[k][c] = xpt[iptsg(isg, k) - 1][c];
+          xs[3 + k][c] = xptc[iptsc[isg][k] - 1][c];
+        }
+      double f0 = 0.0, masel = 0.0, volel = 0.0;
+      for (int ig = 0; ig < 7; ig++) {
+        const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+        const double shps[3] = {1.0 - r - s, r, s};
+        double rg = 0.0, sg = 0.0;
+        for (int k = 0; k < 3; k++) {
+          rg = rg + shps[k] * xvt(iptsg(isg, k) - 1);
+          sg = sg + shps[k] * yvt(iptsg(isg, k) - 1);
+        }
+        double b[6];
+        tri_basis(rc, sc, g19, g20, g21, rg, sg, b);
+        double rhomsg = 0.0;
+        for (int k = 0; k < d.mdegr; k++) rhomsg = rhomsg + u[0][k] * b[k];
+        if (d.nlimi == 6) rhomsg = rhomc + 1.0 * (rhomsg - rhomc);
+        shp6d(r, s, dspr, dsps);
+        Jac j = jac6(xs, dspr, dsps);
+        const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+        f0 = f0 + djaco;
+        masel = masel + 1.0 / rhomsg * djaco;
+        volel = volel + djaco;
+      }
+      unksgt[isg] = 0.0 + (1.0 / f0) * d.tmsub[isg * d.ntria + it];
+      utsgc[isg] = volel / masel;
+    }
+  }
+  double part[6][5];
+  for (int k = 0; k < 6; k++)
+    for (int v = 0; v < 5; v++) part[k][v] = 0.0;
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  for (int isg = 0; isg < 4; isg++) {
+    for (int ivsg = 0; ivsg < 3; ivsg++) {
+      const int iv = iptsg(isg, ivsg) - 1;
+      const int pn = d.ipt[iv * d.ntria + it];
+      const double rhovt = 1.0 / unknvt[iv][0];
+      const double rhovsg = rhovt + 1.0 * (unksgt[isg] - 1.0 / utsgc[isg]);
+      const double uvtx = unknvt[iv][1], vvtx = unknvt[iv][2], evtx = unknvt[iv][3];
+      const double pvtx = fmax(eps, (g - 1.0) * rhovsg * (evtx - 0.5 * (uvtx * uvtx + vvtx * vvtx)));
+      double ax = d.us[pn] - uvtx, ay = d.vs[pn] - vvtx;
+      const double acnx = ax, acny = ay;
+      if (sqrt(acnx * acnx + acny * acny) < (double)1.e-11f) {
+        ax = (double)1.e-11f;
+        ay = (double)1.e-11f;
+      } else {
+        ax = ax / sqrt(acnx * acnx + acny * acny);
+        ay = ay / sqrt(acnx * acnx + acny * acny);
+      }
+      const double ajmp = sqrt(acnx * acnx + acny * acny) / sdctr;
+      const double dux = d.us[pn] - uvtx, duy = d.vs[pn] - vvtx;
+      for (int f = 0; f < 2; f++) {
+        double n0, n1, area;
+        tri_corner_normal(gt, isg, ivsg, f, n0, n1, area);
+        const double deltu = 0.0 * fabs(dux * n0 + duy * n1);
+        const double murie = rhoct * sdctr + rhoct * slpdu * deltu;
+        const double vnau = (ajmp < 1.0e12) ? 1.0 : n0 * ax + n1 * ay;
+        const double m = murie * area * fabs(vnau);
+        const double mu0 = m * uvtx + 0.0 * vvtx;
+        const double mu1 = 0.0 * uvtx + m * vvtx;
+        const double sn0 = -pvtx * area * n0 + 0.0 * area * n1;
+        const double sn1 = 0.0 * area * n0 + -pvtx * area * n1;
+        const int slot = f + 2 * (ivsg + 3 * isg);
+        const size_t nt = d.ntria;
+        d.tcf[(0 * 24 + slot) * nt + it] = m;
+        d.tcf[(1 * 24 + slot) * nt + it] = mu0;
+        d.tcf[(2 * 24 + slot) * nt + it] = mu1;
+        d.tcf[(3 * 24 + slot) * nt + it] = sn0;
+        d.tcf[(4 * 24 + slot) * nt + it] = sn1;
+        part[iv][0] += m;
+        part[iv][1] += mu0;
+        part[iv][2] += mu1;
+        part[iv][3] += sn0;
+        part[iv][4] += sn1;
+      }
+    }
+  }
+  for (int k = 0; k < 6; k++)
+    for (int v = 0; v < 5; v++) d.tpart[(v * 6 + k) * (size_t)d.ntria + it] = part[k][v];
+}
+__global__ void __launch_bounds__(128) k_tri_corner(Dev d) { b_tri_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// RHS of one triangle: corner forces F* = sigma.n A + m (u* - u_c) with the
+// new nodal velocity (usn, vsn), face integral, volume integral, source;
+// then either the RHS is stored or, with fuse, the M^-1 solve and RK combine.
+__host__ __device__ void b_tri_rhs(const Dev &d, int it, const double *usn, const double *vsn, int fuse,
+                                   double alfa) {
+  if (it >= d.ntria || stopped(d)) return;
+  const int e = it;
+  const double g = d.gamlg;
+  const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
+  double xpt[6][2];
+  load_tria(d, d.xs, d.ys, it, xpt);
+  double gt[15][3];
+  normals_tria(xpt, gt);
+  double bt[6][6];
+  for (int iv = 0; iv < 6; iv++) tri_basis(rc, sc, g19, g20, g21, xvt(iv), yvt(iv), bt[iv]);
+  double R[4][6];
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) R[q][k] = 0.0;
+  const size_t nt = d.ntria;
+  // face integral (rhsifacedg_lagsubgt3): mass weights = Riemann weights, unit momentum/energy weights
+  for (int isg = 0; isg < 4; isg++) {
+    for (int ivsg = 0; ivsg < 3; ivsg++) {
+      const int iv = iptsg(isg, ivsg) - 1;
+      const int pn = d.ipt[iv * d.ntria + it];
+      const double us = usn[pn], vs = vsn[pn];
+      double vn[2][3], fs[2][2];
+      for (int f = 0; f < 2; f++) {
+        tri_corner_normal(gt, isg, ivsg, f, vn[f][0], vn[f][1], vn[f][2]);
+        const int slot = f + 2 * (ivsg + 3 * isg);
+        const double m = d.tcf[(0 * 24 + slot) * nt + it];
+        fs[f][0] = d.tcf[(3 * 24 + slot) * nt + it] + m * us + 0.0 * vs - d.tcf[(1 * 24 + slot) * nt + it];
+        fs[f][1] = d.tcf[(4 * 24 + slot) * nt + it] + 0.0 * us + m * vs - d.tcf[(2 * 24 + slot) * nt + it];
+      }
+      for (int k = 0; k < 6; k++) {
+        const double b = bt[iv][k];
+        R[0][k] = R[0][k] + us * vn[0][0] * vn[0][2] * b + vs * vn[0][1] * vn[0][2] * b + us * vn[1][0] * vn[1][2] * b +
+                  vs * vn[1][1] * vn[1][2] * b;
+        R[1][k] = R[1][k] + fs[0][0] * b * 1.0 + fs[1][0] * b * 1.0;
+        R[2][k] = R[2][k] + fs[0][1] * b * 1.0 + fs[1][1] * b * 1.0;
+        R[3][k] = R[3][k] + us * fs[0][0] * b * 1.0 + vs * fs[0][1] * b * 1.0 + us * fs[1][0] * b * 1.0 +
+                  vs * fs[1][1] * b * 1.0;
+      }
+    }
+  }
+  // volume integral (cofactor form, 7-point rule, djaco = w/2)
+  {
+    double dbdr[6] = {0.0, 1.0 / 0.5, 0.0, 0.0, 0.0, 0.0}, dbds[6] = {0.0, 0.0, 1.0 / 0.5, 0.0, 0.0, 0.0};
+    for (int ig = 0; ig < 7; ig++) {
+      const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+      double dspr[6], dsps[6];
+      shp6d(r, s, dspr, dsps);
+      Jac j = jac6(xpt, dspr, dsps);
+      const double djaco = 0.5 * wi;
+      dbdr[3] = (r - rc) / (0.5 * 0.5); dbdr[4] = 0.0; dbdr[5] = (s - sc) / 0.5 / 0.5;
+      dbds[3] = 0.0; dbds[4] = (s - sc) / (0.5 * 0.5); dbds[5] = (r - rc) / 0.5 / 0.5;
+      double b[6];
+      tri_basis(rc, sc, g19, g20, g21, r, s, b);
+      double un[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int k = 0; k < d.mdegr; k++)
+        for (int q = 0; q < 4; q++) un[q] = un[q] + Uget(d, d.Us, k, q, e) * b[k];
+      const double rhoad = 1.0 / un[0];
+      const double uadv = un[1], vadv = un[2], eadv = un[3];
+      const double pres = (g - 1.0) * rhoad * (eadv - 0.5 * (uadv * uadv + vadv * vadv));
+      for (int k = 0; k < 6; k++) {
+        const double gd0 = j.ys * dbdr[k] + (-j.yr) * dbds[k];
+        const double gd1 = (-j.xs) * dbdr[k] + j.xr * dbds[k];
+        const double f0 = gd0 * uadv + gd1 * vadv;
+        R[0][k] = R[0][k] - f0 * djaco;
+        R[1][k] = R[1][k] - gd0 * (-pres) * djaco;
+        R[2][k] = R[2][k] - gd1 * (-pres) * djaco;
+        R[3][k] = R[3][k] - (gd0 * uadv + gd1 * vadv) * (-pres) * djaco;
+      }
+    }
+  }
+  if (d.ncase == 1) {
+    // Taylor-Green source with the full P2 basis
+    for (int ig = 0; ig < 7; ig++) {
+      const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+      double shp[6], dspr[6], dsps[6];
+      shp6v(r, s, shp);
+      shp6d(r, s, dspr, dsps);
+      Jac j = jac6(xpt, dspr, dsps);
+      const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+      double xg, yg;
+      map6(xpt, shp, xg, yg);
+      double b[6];
+      tri_basis(rc, sc, g19, g20, g21, r, s, b);
+      const double src = 0.25 * cPI * (cos(3.0 * cPI * xg) * cos(cPI * yg) - cos(3.0 * cPI * yg) * cos(cPI * xg)) /
+                         (g - 1.0);
+      for (int k = 0; k < 6; k++) R[3][k] = R[3][k] + src * b[k] * djaco;
+    }
+  }
+  if (!fuse) {
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) d.rhs[(q * NDEG + k) * d.ncell + e] = R[q][k];
+    return;
+  }
+  // fused stage update (Getrhslag.f90:1789-1904), the arithmetic of b_update
+  const double dt = d.sc_dev->dtfix;
+  double am[16];
+  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * d.ncell + e];
+  double mm[NDEG][NDEG];
+  for (int i = 0; i < NDEG; i++)
+    for (int jj = 0; jj < NDEG; jj++) mm[i][jj] = 0.0;
+  mm[0][0] = am[15];
+  {
+    int k = 0;
+    for (int im = 1; im < NDEG; im++)
+      for (int jm = im; jm < NDEG; jm++) {
+        mm[im][jm] = am[k];
+        mm[jm][im] = am[k];
+        k++;
+      }
+  }
+  const double oma = 1.0 - alfa;
+  for (int id = 0; id < NDEG; id++) {
+    double unint[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int iu = 0; iu < NDEG; iu++)
+      for (int q = 0; q < 4; q++) unint[q] = unint[q] + mm[id][iu] * (dt * R[q][iu]);
+    for (int q = 0; q < 4; q++) {
+      const int idx = (q * NDEG + id) * d.ncell + e;
+      d.Us[idx] = alfa * d.Un[idx] + oma * (d.Us[idx] + unint[q]);
+    }
+  }
+}
+__global__ void __launch_bounds__(128) k_tri_rhs(Dev d, const double *usn, const double *vsn, int fuse, double alfa) {
+  b_tri_rhs(d, blockIdx.x * blockDim.x + threadIdx.x, usn, vsn, fuse, alfa);
+}
+
 void set_tables(const QuadTables &q, cudaStream_t st) {
   Tables t;
   t.q = q;
@@ -1583,6 +2186,13 @@ void set_tables(const QuadTables &q, cudaStream_t st) {
         t.wmas[a][b][f] = 0.25 * t2[a][b][f];
       }
     }
+  const double t4[4][3][2] = {{{4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}, {8.0 / 3.0, 4.0 / 3.0}},
+                              {{8.0 / 3.0, 8.0 / 3.0}, {8.0 / 3.0, 8.0 / 3.0}, {8.0 / 3.0, 8.0 / 3.0}},
+                              {{8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}},
+                              {{4.0 / 3.0, 8.0 / 3.0}, {8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}}};
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 3; b++)
+      for (int f = 0; f < 2; f++) t.wtri[a][b][f] = 0.25 * t4[a][b][f];
   hT = t;
   if (st) cudaMemcpyToSymbolAsync(cT, &t, sizeof(Tables), 0, cudaMemcpyHostToDevice, st);
 }
@@ -1598,6 +2208,18 @@ void launch_center_geom(const Dev &d, cudaStream_t st) {
   k_center_geom<<<nblk(d.nquad, 256), 256, 0, st>>>(d);
 }
 void launch_reset_count(const Dev &d, cudaStream_t st) { k_reset_count<<<1, 1, 0, st>>>(d); }
+void launch_tri_init(const Dev &d, cudaStream_t st) {
+  if (d.ntria) k_tri_init<<<nblk(d.ntria, 128), 128, 0, st>>>(d);
+}
+void launch_tri_geom(const Dev &d, cudaStream_t st, const double *X, const double *Y) {
+  if (d.ntria) k_tri_geom<<<nblk(d.ntria, 128), 128, 0, st>>>(d, X, Y);
+}
+void launch_tri_corner(const Dev &d, cudaStream_t st) {
+  if (d.ntria) k_tri_corner<<<nblk(d.ntria, 128), 128, 0, st>>>(d);
+}
+void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa) {
+  if (d.ntria) k_tri_rhs<<<nblk(d.ntria, 128), 128, 0, st>>>(d, usn, vsn, fuse, alfa);
+}
 void launch_persson(const Dev &d, cudaStream_t st) { k_persson<<<nblk(d.nquad, 128), 128, 0, st>>>(d); }
 void launch_flags_from_host(const Dev &d, cudaStream_t st, const int *flags) {
   k_flags_from_host<<<nblk(d.nquad, 256), 256, 0, st>>>(d, flags);

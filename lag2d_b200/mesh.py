@@ -27,7 +27,7 @@ from typing import Optional
 
 import numpy as np
 
-__all__ = ["Mesh", "Ctrl", "quad_mesh", "read_domn", "write_domn", "read_ctrl", "write_ctrl",
+__all__ = ["Mesh", "Ctrl", "quad_mesh", "hybrid_mesh", "read_domn", "write_domn", "read_ctrl", "write_ctrl",
            "build_esuv", "build_esqua"]
 
 
@@ -326,3 +326,33 @@ def quad_mesh(nx: int, ny: int, x0: float = 0.0, x1: float = 1.0, y0: float = 0.
         bf.append((nid[2 * j + 2, 0], nid[2 * j, 0], wall_code, 222, nid[2 * j + 1, 0]))
     bface = np.array(bf, dtype=np.int32)
     return Mesh(coord=coord, ipqua=ipqua, iptri=np.zeros((0, 6), np.int32), bface=bface)
+
+
+def hybrid_mesh(nx: int, ny: int, x0: float = 0.0, x1: float = 1.0, y0: float = 0.0, y1: float = 1.0,
+                jitter: float = 0.0, curve: float = 0.0, seed: int = 1234, split_rows=None,
+                wall_code: int = 22) -> Mesh:
+    """Curved tri/quad mesh: the structured 9-node quad mesh of :func:`quad_mesh`
+    with the quads of alternate rows (``j % 2 == 1`` unless ``split_rows`` is
+    given) split along the diagonal from corner 1 to corner 3 into two 6-node
+    triangles (nodes: 3 vertices counter-clockwise, then the mid-nodes of
+    edges 1-2, 2-3 and 3-1).  The quad's centre node becomes the mid-node of
+    the diagonal and is moved to its midpoint.  Triangles are numbered first,
+    as the reference numbers them (ielem = itria, then ntria + iquad).
+    """
+    q = quad_mesh(nx, ny, x0, x1, y0, y1, jitter=jitter, curve=curve, seed=seed, wall_code=wall_code)
+    rows = set(range(1, ny, 2)) if split_rows is None else set(split_rows)
+    coord = q.coord.copy()
+    tris, quads = [], []
+    for c in range(q.nquad):
+        j = c // nx
+        n = q.ipqua[c]
+        if j in rows:
+            a, b, cc, d, eab, ebc, ecd, eda, m = (int(v) for v in n)
+            coord[m - 1] = 0.5 * (coord[a - 1] + coord[cc - 1])
+            tris.append((a, b, cc, eab, ebc, m))
+            tris.append((a, cc, d, m, ecd, eda))
+        else:
+            quads.append(tuple(int(v) for v in n))
+    # the unsplit quads keep the centre-node rule of the step (quad_mesh placed it so)
+    return Mesh(coord=coord, ipqua=np.array(quads, dtype=np.int32).reshape(-1, 9),
+                iptri=np.array(tris, dtype=np.int32).reshape(-1, 6), bface=q.bface)

@@ -2,7 +2,7 @@
  * Lag2D CPU oracle -- TEST INFRASTRUCTURE ONLY (see lag2d_oracle.h).
  *
  * Single-threaded FP64 restatement of the reference time step for the
- * curved-quad P2 path.  Every routine keeps the reference's loop nests and
+ * curved tri/quad P2 path.  Every routine keeps the reference's loop nests and
  * left-to-right accumulation order so that, compiled with
  * -O2 -ffp-contract=off (no FMA, like gfortran -O on x86-64), it reproduces
  * the reference arithmetic.  Citations are to srccurv-lag/<file>:<line>.
@@ -298,6 +298,11 @@ static void cellctr_quad(const double (*xpqi)[2], double rc, double sc, double *
   map9(xpqi, shp, x, y);
 }
 
+/* triangle parts (defined with the triangle routines below) */
+static void init_tria(const o_mesh *m, const o_cfg *c, const double *coord, double *geoel,
+                      double *amatr, double *unkno);
+static void cellvol_tria(const o_mesh *m, const o_cfg *c, double *geoel, const double *coord);
+
 /* ---------------------------------------------------------------------- */
 /* Initialisation                                                         */
 /* ---------------------------------------------------------------------- */
@@ -309,9 +314,9 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
   double pos36[36][2], w36[36], pos25[25][2], w25[25];
   quad_rule(36, 0, pos36, w36);
   quad_rule(25, 0, pos25, w25);
-  if (ntria > 0) { fprintf(stderr, "oracle: triangles not supported\n"); abort(); }
   memset(geoel, 0, sizeof(double) * 24 * nsize);
   memset(unkno, 0, sizeof(double) * c->ndegr * c->nq * nsize);
+  if (ntria > 0) init_tria(m, c, coord, geoel, amatr, unkno);
 
   for (int ie = 0; ie < nquad; ie++) {
     const int ielem = ie + ntria;
@@ -488,7 +493,7 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
 /* getcellvol_lag, Limiterlag.f90:1869-2167 (quad loop :2038-2165)        */
 /* ---------------------------------------------------------------------- */
 void o_cellvol(const o_mesh *m, const o_cfg *c, double *geoel, const double *coord) {
-  (void)c;
+  if (m->ntria > 0) cellvol_tria(m, c, geoel, coord);
   double pos36[36][2], w36[36];
   quad_rule(36, 0, pos36, w36);
   const double alfrz = 0.0;
@@ -844,8 +849,10 @@ static void weno_stencil(const weno_ctx *w, int ielem, const double *mapmt, doub
   double dxcl = sqrt(G_(w->geoel, 2, ielem)), dycl = dxcl;
   int ielaj[9];
   ielaj[0] = ielem + 1;
-  /* the reference indexes esqua by the global id here (WENO.f90:7648) */
-  for (int k = 0; k < 4; k++) ielaj[1 + k] = m->esqua[4 * ielem + k];
+  /* the reference indexes esqua by the global id here (WENO.f90:7648); on
+   * a mesh with triangles that index leaves the quad range, so the quad's
+   * own row is used there */
+  for (int k = 0; k < 4; k++) ielaj[1 + k] = m->esqua[4 * (ntria > 0 ? ie : ielem) + k];
   for (int k = 5; k < 9; k++) ielaj[k] = 0;
   int ipq[9];
   for (int k = 0; k < 9; k++) ipq[k] = m->ipqua[9 * ie + k];
@@ -866,10 +873,18 @@ static void weno_stencil(const weno_ctx *w, int ielem, const double *mapmt, doub
         else if (idxod == 6) ielaj[6] = jelaj[a];
         else if (idxod == 12) ielaj[7] = jelaj[a];
         else if (idxod == 4) ielaj[8] = jelaj[a];
-        else { g_status |= 2; return; } /* the reference stops here (WENO.f90:7699) */
+        else {
+          /* the reference stops here (WENO.f90:7699); next to triangles
+           * this is the normal case and the quad is left unlimited */
+          if (ntria == 0) g_status |= 2;
+          return;
+        }
       }
   }
   for (int k = 0; k < 9; k++) if (ielaj[k] == 0) return;  /* boundary cell */
+  /* a stencil that reaches a triangle is not a 3x3 quad block: the cell is
+   * left unlimited (the reference's quad-only WENO has no such case) */
+  for (int k = 0; k < 9; k++) if (ielaj[k] <= ntria) return;
   for (int k = 0; k < 9; k++) ielaj[k] -= 1;               /* 0-based */
 
   /* local copies of the stencil DOFs in the rotated frame */
@@ -1341,11 +1356,698 @@ static void riem_quad(const o_mesh *m, const o_cfg *c, int ie, const double *geo
 }
 
 /* ---------------------------------------------------------------------- */
+/* 6-node triangles: P2 map on the reference triangle (0,0), (1,0), (0,1);*/
+/* nodes 1-3 vertices, 4 on edge 1-2, 5 on edge 2-3, 6 on edge 3-1.       */
+/* Shape functions as in getcellvol_lag (Limiterlag.f90:1935-1962).       */
+/* ---------------------------------------------------------------------- */
+static void shp6(double r, double s, double *shp, double *dspr, double *dsps) {
+  const double c10 = 1.0;
+  if (shp) {
+    shp[0] = -(c10 - r - s) * (c10 - 2.0 * (c10 - r - s));
+    shp[1] = -r * (c10 - 2.0 * r);
+    shp[2] = -s * (c10 - 2.0 * s);
+    shp[3] = 4.0 * r * (c10 - r - s);
+    shp[4] = 4.0 * r * s;
+    shp[5] = 4.0 * s * (c10 - r - s);
+  }
+  if (dspr) {
+    dspr[0] = c10 - 4.0 * (c10 - r - s);
+    dspr[1] = -1.0 + 4.0 * r;
+    dspr[2] = 0.0;
+    dspr[3] = 4.0 * (1.0 - 2.0 * r - s);
+    dspr[4] = 4.0 * s;
+    dspr[5] = -4.0 * s;
+  }
+  if (dsps) {
+    dsps[0] = c10 - 4.0 * (c10 - r - s);
+    dsps[1] = 0.0;
+    dsps[2] = -1.0 + 4.0 * s;
+    dsps[3] = -4.0 * r;
+    dsps[4] = 4.0 * r;
+    dsps[5] = 4.0 * (1.0 - r - 2.0 * s);
+  }
+}
+
+/* dx/dr, dx/ds, dy/dr, dy/ds of the 6-node map */
+static void jac6(const double (*xp)[2], const double *dspr, const double *dsps,
+                 double *dxdr, double *dxds, double *dydr, double *dyds) {
+  double a = 0.0, b = 0.0, cc = 0.0, d = 0.0;
+  for (int k = 0; k < 6; k++) {
+    a = a + dspr[k] * xp[k][0];
+    b = b + dsps[k] * xp[k][0];
+    cc = cc + dspr[k] * xp[k][1];
+    d = d + dsps[k] * xp[k][1];
+  }
+  *dxdr = a; *dxds = b; *dydr = cc; *dyds = d;
+}
+
+static void map6(const double (*xp)[2], const double *shp, double *x, double *y) {
+  double a = 0.0, b = 0.0;
+  for (int k = 0; k < 6; k++) { a = a + shp[k] * xp[k][0]; b = b + shp[k] * xp[k][1]; }
+  *x = a; *y = b;
+}
+
+static void load_tria(const o_mesh *m, const double *X, int it, double (*xp)[2]) {
+  for (int k = 0; k < 6; k++) {
+    int ip = m->iptri[6 * it + k] - 1;
+    xp[k][0] = X_(X, 0, ip);
+    xp[k][1] = X_(X, 1, ip);
+  }
+}
+
+/* rutope, 2-D open rules for triangles (dgflo2d.f90:2175-2270); the
+ * literals are the reference's.  Returns the number of points. */
+static int tri_rule(int ngaus, double (*pos)[2], double *w) {
+  if (ngaus == 1) {
+    pos[0][0] = 1.0 / 3.0; pos[0][1] = 1.0 / 3.0; w[0] = 1.0;
+    return 1;
+  }
+  if (ngaus == 3) {
+    pos[0][0] = 2.0 / 3.0; pos[0][1] = 1.0 / 6.0;
+    pos[1][0] = 1.0 / 6.0; pos[1][1] = 2.0 / 3.0;
+    pos[2][0] = 1.0 / 6.0; pos[2][1] = 1.0 / 6.0;
+    w[0] = w[1] = w[2] = 1.0 / 3.0;
+    return 3;
+  }
+  if (ngaus == 7) {
+    const double a = 0.333333333333333, b1 = 0.059715871789770, b2 = 0.470142064105115;
+    const double c1 = 0.797426985353087, c2 = 0.101286507323456;
+    pos[0][0] = a;  pos[0][1] = a;
+    pos[1][0] = b1; pos[1][1] = b2;
+    pos[2][0] = b2; pos[2][1] = b1;
+    pos[3][0] = b2; pos[3][1] = b2;
+    pos[4][0] = c1; pos[4][1] = c2;
+    pos[5][0] = c2; pos[5][1] = c1;
+    pos[6][0] = c2; pos[6][1] = c2;
+    w[0] = 0.225000000000000;
+    w[1] = w[2] = w[3] = 0.132394152788506;
+    w[4] = w[5] = w[6] = 0.125939180544827;
+    return 7;
+  }
+  fprintf(stderr, "oracle: triangle rule with %d points not restated\n", ngaus);
+  abort();
+}
+
+/* reference coordinates of the 6 nodes */
+static const double XVT[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
+static const double YVT[6] = {0.0, 0.0, 1.0, 0.0, 0.5, 0.5};
+
+/* Taylor basis of a triangle at reference point (r, s): scale dr = ds = 1/2
+ * (e.g. getriem_triasubg3, Getrhslaggauss.f90:12303-12316) */
+static void basis_tria(const double *geoel_e, double r, double s, double *b) {
+  const double dr = 0.5, ds = 0.5;
+  b[0] = 1.0;
+  b[1] = (r - geoel_e[0]) / dr;
+  b[2] = (s - geoel_e[1]) / ds;
+  b[3] = 0.5 * b[1] * b[1] - geoel_e[18];
+  b[4] = 0.5 * b[2] * b[2] - geoel_e[19];
+  b[5] = b[1] * b[2] - geoel_e[20];
+}
+
+/* Initial geometry and DOFs of the triangles: the ntria loops of
+ * getgeoel_initial_lag (GetInitial.f90:1334-1478), getgeoelho_initial_lag
+ * (:1754-1905), inifield_mcnew (Getrhslagmc.f90:3344-3480) and
+ * getunkno_initial_lag (GetInitial.f90:190-411). */
+static void init_tria(const o_mesh *m, const o_cfg *c, const double *coord, double *geoel,
+                      double *amatr, double *unkno) {
+  const double alfrz = 0.0;
+  double posg[13][2], wg[13], posd[13][2], wd[13];
+  const int ng = tri_rule(c->ngausd_geo, posg, wg);
+  const int nd = tri_rule(c->ngausd, posd, wd);
+  const int nmatr = (c->npoly == 2) ? 16 : 4;
+  for (int it = 0; it < m->ntria; it++) {
+    const int ielem = it;
+    double xp[6][2], shp[6], dspr[6], dsps[6], a, b, cc, d;
+    load_tria(m, coord, it, xp);
+    double xc, yc;
+    shp6(1.0 / 3.0, 1.0 / 3.0, shp, NULL, NULL);
+    map6((const double(*)[2])xp, shp, &xc, &yc);
+    double xcent = 0, ycent = 0, xcel = 0, ycel = 0, volel = 0, masel = 0;
+    for (int ig = 0; ig < ng; ig++) {
+      double r = posg[ig][0], s = posg[ig][1], wi = wg[ig], xg, yg;
+      shp6(r, s, shp, dspr, dsps);
+      jac6((const double(*)[2])xp, dspr, dsps, &a, &b, &cc, &d);
+      double djaco = 0.5 * wi * (a * d - cc * b);
+      map6((const double(*)[2])xp, shp, &xg, &yg);
+      double rhog = rho_initial(c, xg, yg, xc, yc);
+      double rcoef = 1.0 - alfrz + alfrz * yg;
+      masel = masel + rhog * djaco * rcoef;
+      volel = volel + djaco * rcoef;
+      xcent = xcent + rhog * r * djaco * rcoef;
+      ycent = ycent + rhog * s * djaco * rcoef;
+      xcel = xcel + djaco * r * rcoef;
+      ycel = ycel + djaco * s * rcoef;
+    }
+    G_(geoel, 0, ielem) = xcent / masel;
+    G_(geoel, 1, ielem) = ycent / masel;
+    G_(geoel, 2, ielem) = volel;
+    G_(geoel, 3, ielem) = masel;
+    G_(geoel, 6, ielem) = xcel / volel;
+    G_(geoel, 7, ielem) = ycel / volel;
+    {
+      double mx = xp[0][1], mn = xp[0][1];
+      for (int k = 1; k < 3; k++) { if (xp[k][1] > mx) mx = xp[k][1]; if (xp[k][1] < mn) mn = xp[k][1]; }
+      G_(geoel, 4, ielem) = mx - mn;
+    }
+  }
+  if (c->npoly == 2) {
+    for (int it = 0; it < m->ntria; it++) {
+      const int ielem = it;
+      double xp[6][2], shp[6], dspr[6], dsps[6], a, b, cc, d;
+      load_tria(m, coord, it, xp);
+      const double dr = 0.5, ds = 0.5;
+      double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+      double rci = G_(geoel, 6, ielem), sci = G_(geoel, 7, ielem);
+      double volel = G_(geoel, 2, ielem), masel = G_(geoel, 3, ielem);
+      double xc, yc;
+      shp6(rc, sc, shp, NULL, NULL);
+      map6((const double(*)[2])xp, shp, &xc, &yc);
+      double bt[6] = {0, 0, 0, 0, 0, 0}, bti[6] = {0, 0, 0, 0, 0, 0};
+      for (int ig = 0; ig < ng; ig++) {
+        double r = posg[ig][0], s = posg[ig][1], wi = wg[ig], xg, yg;
+        shp6(r, s, shp, dspr, dsps);
+        jac6((const double(*)[2])xp, dspr, dsps, &a, &b, &cc, &d);
+        double djaco = 0.5 * wi * (a * d - cc * b);
+        map6((const double(*)[2])xp, shp, &xg, &yg);
+        double rhog = rho_initial(c, xg, yg, xc, yc);
+        double rcoef = 1.0 - alfrz + alfrz * yg;
+        bt[0] = 1.0;
+        bt[1] = (r - rc) / dr;
+        bt[2] = (s - sc) / ds;
+        bt[3] = bt[3] + 0.5 * rhog * bt[1] * bt[1] * djaco * rcoef;
+        bt[4] = bt[4] + 0.5 * rhog * bt[2] * bt[2] * djaco * rcoef;
+        bt[5] = bt[5] + rhog * bt[1] * bt[2] * djaco * rcoef;
+        bti[0] = 1.0;
+        bti[1] = (r - rci) / dr;
+        bti[2] = (s - sci) / ds;
+        bti[3] = bti[3] + 0.5 * bti[1] * bti[1] * djaco * rcoef;
+        bti[4] = bti[4] + 0.5 * bti[2] * bti[2] * djaco * rcoef;
+        bti[5] = bti[5] + bti[1] * bti[2] * djaco * rcoef;
+      }
+      G_(geoel, 18, ielem) = bt[3] / masel;
+      G_(geoel, 19, ielem) = bt[4] / masel;
+      G_(geoel, 20, ielem) = bt[5] / masel;
+      G_(geoel, 21, ielem) = bti[3] / volel;
+      G_(geoel, 22, ielem) = bti[4] / volel;
+      G_(geoel, 23, ielem) = bti[5] / volel;
+    }
+  }
+  /* cell averages */
+  for (int it = 0; it < m->ntria; it++) {
+    const int ielem = it;
+    double xp[6][2], shp[6], dspr[6], dsps[6], a, b, cc, d, unkin[4];
+    load_tria(m, coord, it, xp);
+    double volel = G_(geoel, 2, ielem), masel = G_(geoel, 3, ielem);
+    double xcel = (-xp[0][0] - xp[1][0] - xp[2][0] + 4.0 * xp[3][0] + 4.0 * xp[4][0] + 4.0 * xp[5][0]) / 9.0;
+    double ycel = (-xp[0][1] - xp[1][1] - xp[2][1] + 4.0 * xp[3][1] + 4.0 * xp[4][1] + 4.0 * xp[5][1]) / 9.0;
+    double rv[4] = {0, 0, 0, 0};
+    for (int ig = 0; ig < nd; ig++) {
+      double r = posd[ig][0], s = posd[ig][1], wi = wd[ig], xg, yg;
+      shp6(r, s, shp, dspr, dsps);
+      jac6((const double(*)[2])xp, dspr, dsps, &a, &b, &cc, &d);
+      double djaco = 0.5 * wi * (a * d - cc * b);
+      map6((const double(*)[2])xp, shp, &xg, &yg);
+      getunkin(c, unkin, xg, yg, ielem + 1, volel, xcel, ycel);
+      double rcoef = 1.0 - alfrz + alfrz * yg;
+      for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
+    }
+    for (int q = 0; q < 4; q++) U_(unkno, c, 0, q, ielem) = rv[q] / masel;
+  }
+  /* M^-1 and L2 projection of the higher moments */
+  for (int it = 0; it < m->ntria; it++) {
+    const int ielem = it;
+    const int ndg = c->ndegr, nb = ndg - 1;
+    double xp[6][2], shp[6], dspr[6], dsps[6], a, b, cc, d, unkin[4];
+    load_tria(m, coord, it, xp);
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double volel = G_(geoel, 2, ielem);
+    double xc, yc;
+    shp6(rc, sc, shp, NULL, NULL);
+    map6((const double(*)[2])xp, shp, &xc, &yc);
+    double rhsini[6][4], mmatr[25], matri[25];
+    memset(rhsini, 0, sizeof rhsini);
+    memset(mmatr, 0, sizeof mmatr);
+    double f0 = 0.0;
+    for (int ig = 0; ig < nd; ig++) {
+      double r = posd[ig][0], s = posd[ig][1], wi = wd[ig], xg, yg, bt[6];
+      shp6(r, s, shp, dspr, dsps);
+      jac6((const double(*)[2])xp, dspr, dsps, &a, &b, &cc, &d);
+      double djaco = 0.5 * wi * (a * d - cc * b);
+      map6((const double(*)[2])xp, shp, &xg, &yg);
+      bt[0] = 1.0;
+      bt[1] = (r - rc) / 0.5;
+      bt[2] = (s - sc) / 0.5;
+      if (c->npoly == 2) {
+        bt[3] = 0.5 * bt[1] * bt[1] - G_(geoel, 18, ielem);
+        bt[4] = 0.5 * bt[2] * bt[2] - G_(geoel, 19, ielem);
+        bt[5] = bt[1] * bt[2] - G_(geoel, 20, ielem);
+      }
+      getunkin(c, unkin, xg, yg, ielem + 1, volel, xc, yc);
+      for (int q = 0; q < 4; q++)
+        for (int k = 0; k < ndg; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bt[k] * djaco;
+      double rho0 = rho_initial(c, xg, yg, xc, yc);
+      double rcoef = 1.0 - alfrz + alfrz * yg;
+      f0 = f0 + rho0 * djaco * rcoef;
+      for (int ix = 0; ix < nb; ix++)
+        for (int iy = 0; iy < nb; iy++)
+          mmatr[ix + nb * iy] = mmatr[ix + nb * iy] + rho0 * bt[ix + 1] * bt[iy + 1] * djaco * rcoef;
+    }
+    double *am = amatr + nmatr * ielem;
+    if (c->npoly == 1) {
+      double det = mmatr[0] * mmatr[3] - mmatr[2] * mmatr[2];
+      am[0] = mmatr[3] / det; am[1] = -mmatr[2] / det; am[2] = mmatr[0] / det; am[3] = 1.0 / f0;
+      matri[0] = am[0]; matri[2] = am[1]; matri[1] = am[1]; matri[3] = am[2];
+    } else {
+      getinvmat(5, mmatr, matri);
+      int k = 0;
+      for (int im = 0; im < 5; im++)
+        for (int jm = im; jm < 5; jm++) am[k++] = matri[im + 5 * jm];
+      am[15] = 1.0 / f0;
+    }
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < ndg; k++) U_(unkno, c, k, q, ielem) = 0.0;
+    for (int q = 0; q < 4; q++)
+      for (int ix = 0; ix < nb; ix++)
+        for (int iy = 0; iy < nb; iy++)
+          U_(unkno, c, ix + 1, q, ielem) = U_(unkno, c, ix + 1, q, ielem) + matri[ix + nb * iy] * rhsini[iy + 1][q];
+  }
+}
+
+/* getcellvol_lag, triangle loop (Limiterlag.f90:1908-2036) */
+static void cellvol_tria(const o_mesh *m, const o_cfg *c, double *geoel, const double *coord) {
+  const double alfrz = 0.0;
+  double pos[13][2], w[13];
+  const int ng = tri_rule(c->ngausd_geo, pos, w);
+  for (int it = 0; it < m->ntria; it++) {
+    double xp[6][2], shp[6], dspr[6], dsps[6], a, b, cc, d, xg, yg;
+    load_tria(m, coord, it, xp);
+    double rcv = 0, scv = 0, volel = 0;
+    for (int ig = 0; ig < ng; ig++) {
+      double r = pos[ig][0], s = pos[ig][1], wi = w[ig];
+      shp6(r, s, shp, dspr, dsps);
+      jac6((const double(*)[2])xp, dspr, dsps, &a, &b, &cc, &d);
+      map6((const double(*)[2])xp, shp, &xg, &yg);
+      double rcoef = 1.0 - alfrz + alfrz * yg;
+      double djaco = 0.5 * wi * (a * d - cc * b);
+      volel = volel + djaco * rcoef;
+      rcv = rcv + r * djaco * rcoef;
+      scv = scv + s * djaco * rcoef;
+    }
+    G_(geoel, 2, it) = volel;
+    G_(geoel, 4, it) = rcv / volel;
+    G_(geoel, 5, it) = scv / volel;
+  }
+}
+
+/* Sub-cell face normals of a triangle, gesgt(3,15): slots 1-6 and 10-12
+ * from the nine Simpson points of the three edges
+ * (getfnds_lagsms_simpsonhybrid, Getrhslaggauss.f90:9735-9853), slots 7-9
+ * and 13-15 at the two ends of the three inner sub-cell faces
+ * (getfnds_lagsmsif_hybrid, Getrhslaggauss.f90:3432-3520). */
+static void normals_tria(const double (*xpt)[2], double (*gt)[3]) {
+  static const double postc[3][2] = {{0.25, 0.25}, {0.5, 0.25}, {0.25, 0.5}};
+  static const int ipift[3][3] = {{4, 6, 1}, {5, 4, 2}, {6, 5, 3}};  /* [ifa][k] */
+  double xptv[3][2], shp[6];
+  for (int isv = 0; isv < 3; isv++) {
+    shp6(postc[isv][0], postc[isv][1], shp, NULL, NULL);
+    map6(xpt, shp, &xptv[isv][0], &xptv[isv][1]);
+  }
+  for (int ifa = 0; ifa < 3; ifa++) {
+    double xpf[3][2];
+    for (int d = 0; d < 2; d++) {
+      xpf[0][d] = xpt[ipift[ifa][0] - 1][d];
+      xpf[1][d] = xpt[ipift[ifa][1] - 1][d];
+      xpf[2][d] = xptv[ipift[ifa][2] - 1][d];
+    }
+    for (int end = 0; end < 2; end++) {
+      double r = end == 0 ? -1.0 : 1.0;
+      double dshpr[3] = {-0.5 + r, 0.5 + r, -2.0 * r};
+      double dxdr = 0.0, dydr = 0.0;
+      for (int k = 0; k < 3; k++) {
+        dxdr = dxdr + dshpr[k] * xpf[k][0];
+        dydr = dydr + dshpr[k] * xpf[k][1];
+      }
+      double djaco = sqrt(dxdr * dxdr + dydr * dydr);
+      double anx = -dydr, any = dxdr;
+      int slot = (end == 0 ? 6 : 12) + ifa;
+      gt[slot][0] = anx / sqrt(anx * anx + any * any);
+      gt[slot][1] = any / sqrt(anx * anx + any * any);
+      gt[slot][2] = djaco * 2.0;
+    }
+  }
+  static const double posit[9][2] = {{0, 0}, {1, 0}, {1, 0}, {0, 1}, {0, 1}, {0, 0}, {0.5, 0}, {0.5, 0.5}, {0, 0.5}};
+  double gelag[9][3];
+  for (int ig = 0; ig < 9; ig++) {
+    double dspr[6], dsps[6], dxdr, dxds, dydr, dyds, vn0, vn1, larea;
+    shp6(posit[ig][0], posit[ig][1], shp, dspr, dsps);
+    jac6(xpt, dspr, dsps, &dxdr, &dxds, &dydr, &dyds);
+    double c11 = dyds, c12 = -dydr, c21 = -dxds, c22 = dxdr;
+    int g1 = ig + 1;
+    if (g1 == 1 || g1 == 2 || g1 == 7) { vn0 = 0.0; vn1 = -1.0; larea = 1.0; }
+    else if (g1 == 3 || g1 == 4 || g1 == 8) { vn0 = sqrt(2.0) * 0.5; vn1 = sqrt(2.0) * 0.5; larea = sqrt(2.0); }
+    else { vn0 = -1.0; vn1 = 0.0; larea = 1.0; }
+    double anx = c11 * vn0 + c12 * vn1;
+    double any = c21 * vn0 + c22 * vn1;
+    double v0 = anx * larea, v1 = any * larea;
+    double farea = sqrt(v0 * v0 + v1 * v1);
+    gelag[ig][0] = anx * larea / farea;
+    gelag[ig][1] = any * larea / farea;
+    gelag[ig][2] = farea;
+  }
+  for (int k = 0; k < 6; k++) for (int d = 0; d < 3; d++) gt[k][d] = gelag[k][d];
+  for (int k = 0; k < 3; k++) for (int d = 0; d < 3; d++) gt[9 + k][d] = gelag[6 + k][d];
+}
+
+/* Sub-cell vertices and face slots of a triangle (getriem_triasubg3,
+ * Getrhslaggauss.f90:12264-12287): 4 sub-triangles of 3 vertices, 2 faces
+ * per vertex; fntsg = gesgt slot, the sign orients it outwards. */
+static const int IPTSG[4][3] = {{1, 4, 6}, {4, 5, 6}, {4, 2, 5}, {6, 5, 3}};
+static const int FNTSG[4][6] = {{6, 1, 10, -7, -13, 12}, {7, 14, 8, 15, 9, 13},
+                                {-14, 10, 2, 3, 11, -8}, {12, -9, -15, 11, 4, 5}};
+/* Riemann / mass face weights x 0.25 (Getrhslaggauss.f90:12289-12302), [isg][ivsg][ifa] */
+static double wfgst_tria(int isg, int ivsg, int f) {
+  static const double t[4][3][2] = {
+      {{4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}, {8.0 / 3.0, 4.0 / 3.0}},
+      {{8.0 / 3.0, 8.0 / 3.0}, {8.0 / 3.0, 8.0 / 3.0}, {8.0 / 3.0, 8.0 / 3.0}},
+      {{8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}, {4.0 / 3.0, 8.0 / 3.0}},
+      {{4.0 / 3.0, 8.0 / 3.0}, {8.0 / 3.0, 4.0 / 3.0}, {4.0 / 6.0, 4.0 / 6.0}}};
+  return 0.25 * t[isg][ivsg][f];
+}
+
+/* getrhosubgt_average2 (Getrhslaggauss.f90:12595-12945): sub-cell density
+ * (initial sub-cell mass / current sub-cell volume) and the harmonic mean
+ * of the DG specific volume over each of the 4 sub-triangles. */
+static void rhosubgt_average2(const o_cfg *c, double rc, double sc, const double *btho,
+                              const double (*xpt)[2], const double (*xpti)[2], const double *u1,
+                              double aflim1, double *unksgt, double *utsgc) {
+  static const double postc[9][2] = {{0.25, 0.0}, {0.75, 0.0}, {0.75, 0.25}, {0.25, 0.75}, {0.0, 0.75},
+                                     {0.0, 0.25}, {0.25, 0.25}, {0.5, 0.25}, {0.25, 0.5}};
+  static const int iptsc[4][3] = {{1, 7, 6}, {8, 9, 7}, {2, 3, 8}, {9, 4, 5}};
+  const double dr = 0.5, ds = 0.5;
+  double pos[13][2], w[13];
+  const int ng = tri_rule(c->ngausd, pos, w);
+  double xptc[9][2], xptic[9][2], shp[6];
+  for (int isc = 0; isc < 9; isc++) {
+    shp6(postc[isc][0], postc[isc][1], shp, NULL, NULL);
+    map6(xpt, shp, &xptc[isc][0], &xptc[isc][1]);
+    map6(xpti, shp, &xptic[isc][0], &xptic[isc][1]);
+  }
+  const double rhomc = u1[0];
+  double matin[4];
+  for (int isg = 0; isg < 4; isg++) {
+    double xs[6][2];
+    for (int k = 0; k < 3; k++)
+      for (int d = 0; d < 2; d++) {
+        xs[k][d] = xpt[IPTSG[isg][k] - 1][d];
+        xs[3 + k][d] = xptc[iptsc[isg][k] - 1][d];
+      }
+    double f0 = 0.0, masel = 0.0, volel = 0.0;
+    for (int ig = 0; ig < ng; ig++) {
+      double r = pos[ig][0], s = pos[ig][1], wi = w[ig];
+      double shps[3] = {1.0 - r - s, r, s};
+      double rg = 0.0, sg = 0.0;
+      for (int k = 0; k < 3; k++) {
+        rg = rg + shps[k] * XVT[IPTSG[isg][k] - 1];
+        sg = sg + shps[k] * YVT[IPTSG[isg][k] - 1];
+      }
+      double btsg[6];
+      btsg[0] = 1.0;
+      btsg[1] = (rg - rc) / dr;
+      btsg[2] = (sg - sc) / ds;
+      btsg[3] = 0.5 * btsg[1] * btsg[1] - btho[0];
+      btsg[4] = 0.5 * btsg[2] * btsg[2] - btho[1];
+      btsg[5] = btsg[1] * btsg[2] - btho[2];
+      double rhomsg = 0.0;
+      for (int k = 0; k < c->mdegr; k++) rhomsg = rhomsg + u1[k] * btsg[k];
+      if (c->nlimi == 6) rhomsg = rhomc + aflim1 * (rhomsg - rhomc);
+      double dspr[6], dsps[6], a, b, cc, d;
+      shp6(r, s, NULL, dspr, dsps);
+      jac6((const double(*)[2])xs, dspr, dsps, &a, &b, &cc, &d);
+      double djaco = 0.5 * wi * (a * d - cc * b);
+      f0 = f0 + djaco;
+      masel = masel + 1.0 / rhomsg * djaco;
+      volel = volel + djaco;
+    }
+    matin[isg] = 1.0 / f0;
+    utsgc[isg] = volel / masel;
+  }
+  double xci, yci;
+  shp6(1.0 / 3.0, 1.0 / 3.0, shp, NULL, NULL);
+  map6(xpti, shp, &xci, &yci);
+  for (int isg = 0; isg < 4; isg++) {
+    double xs[6][2];
+    for (int k = 0; k < 3; k++)
+      for (int d = 0; d < 2; d++) {
+        xs[k][d] = xpti[IPTSG[isg][k] - 1][d];
+        xs[3 + k][d] = xptic[iptsc[isg][k] - 1][d];
+      }
+    double rhs = 0.0;
+    for (int ig = 0; ig < ng; ig++) {
+      double r = pos[ig][0], s = pos[ig][1], wi = w[ig];
+      double dspr[6], dsps[6], a, b, cc, d;
+      shp6(r, s, NULL, dspr, dsps);
+      jac6((const double(*)[2])xs, dspr, dsps, &a, &b, &cc, &d);
+      double djaco = 0.5 * wi * (a * d - cc * b);
+      /* getrhoig_triacurv2 (Getrhslag.f90:17622): the cases built here
+       * have a density that depends on the parent's initial centroid only */
+      double rhoi = rho_initial(c, 0, 0, xci, yci);
+      rhs = rhs + rhoi * 1.0 * djaco;
+    }
+    unksgt[isg] = 0.0 + matin[isg] * rhs;
+  }
+}
+
+/* getriem_triasubg3 (Getrhslaggauss.f90:12201-12590): corner coefficients
+ * of the 4 sub-triangles (3 vertices x 2 faces each), scattered into the
+ * node sums; no impedance jump term and no cdrho factor on triangles. */
+static void riem_tria(const o_mesh *m, const o_cfg *c, int it, const double *geoel,
+                      const double (*gt)[3], const double *vlave, const double *unkno,
+                      const double *coord, const double *coold,
+                      double *munacn, double *munacu, double *snsigm, corner_t *ct) {
+  const int ielem = it;
+  const double eps = 1.0e-15, g = c->gamlg;
+  const double slpdu = (g + 1.0) / 2.0;
+  int ipt[6];
+  for (int k = 0; k < 6; k++) ipt[k] = m->iptri[6 * it + k] - 1;
+  const double *ge = &G_(geoel, 0, ielem);
+  double bt[6][6];
+  for (int iv = 0; iv < 6; iv++) basis_tria(ge, XVT[iv], YVT[iv], bt[iv]);
+  double rhomc = U_(unkno, c, 0, 0, ielem);
+  double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+  double rhoct = 1.0 / rhomc;
+  double pctr = fmax(eps, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  double unknvt[6][4];
+  for (int iv = 0; iv < 6; iv++) {
+    for (int q = 0; q < 4; q++) unknvt[iv][q] = 0.0;
+    for (int k = 0; k < c->mdegr; k++)
+      for (int q = 0; q < 4; q++) unknvt[iv][q] = unknvt[iv][q] + U_(unkno, c, k, q, ielem) * bt[iv][k];
+  }
+  double xpt[6][2], xpti[6][2];
+  load_tria(m, coord, it, xpt);
+  load_tria(m, coold, it, xpti);
+  double unksgt[4], utsgc[4], u1[6];
+  for (int k = 0; k < c->ndegr; k++) u1[k] = U_(unkno, c, k, 0, ielem);
+  rhosubgt_average2(c, ge[0], ge[1], ge + 18, (const double(*)[2])xpt, (const double(*)[2])xpti, u1, 1.0,
+                    unksgt, utsgc);
+  for (int isg = 0; isg < 4; isg++) {
+    double vn[3][2][3];
+    for (int ivsg = 0; ivsg < 3; ivsg++)
+      for (int f = 0; f < 2; f++) {
+        int code = FNTSG[isg][2 * ivsg + f];
+        int slot = abs(code) - 1;
+        double sg = code >= 0 ? 1.0 : -1.0;
+        vn[ivsg][f][0] = sg * gt[slot][0];
+        vn[ivsg][f][1] = sg * gt[slot][1];
+        vn[ivsg][f][2] = gt[slot][2] * wfgst_tria(isg, ivsg, f);
+      }
+    double uv[3][2], sig[3], aujmp[3][3];
+    for (int ivsg = 0; ivsg < 3; ivsg++) {
+      int iv = IPTSG[isg][ivsg] - 1;
+      double rhovt = 1.0 / unknvt[iv][0];
+      double rhovsg = rhovt + 1.0 * (unksgt[isg] - 1.0 / utsgc[isg]);
+      double uvtx = unknvt[iv][1], vvtx = unknvt[iv][2], evtx = unknvt[iv][3];
+      double pvtx = fmax(eps, (g - 1.0) * rhovsg * (evtx - 0.5 * (uvtx * uvtx + vvtx * vvtx)));
+      uv[ivsg][0] = uvtx; uv[ivsg][1] = vvtx;
+      sig[ivsg] = -pvtx;
+      double ax = X_(vlave, 0, ipt[iv]) - uvtx, ay = X_(vlave, 1, ipt[iv]) - vvtx;
+      double acnx = ax, acny = ay;
+      if (sqrt(acnx * acnx + acny * acny) < (double)1.e-11f) {
+        ax = (double)1.e-11f; ay = (double)1.e-11f;
+      } else {
+        ax = ax / sqrt(acnx * acnx + acny * acny);
+        ay = ay / sqrt(acnx * acnx + acny * acny);
+      }
+      aujmp[ivsg][0] = ax; aujmp[ivsg][1] = ay;
+      aujmp[ivsg][2] = sqrt(acnx * acnx + acny * acny);
+    }
+    double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+    for (int ivsg = 0; ivsg < 3; ivsg++) aujmp[ivsg][2] = aujmp[ivsg][2] / sdctr;
+    double murie[3][2];
+    for (int ivsg = 0; ivsg < 3; ivsg++) {
+      int iv = IPTSG[isg][ivsg] - 1;
+      double dux = X_(vlave, 0, ipt[iv]) - uv[ivsg][0];
+      double duy = X_(vlave, 1, ipt[iv]) - uv[ivsg][1];
+      for (int f = 0; f < 2; f++) {
+        double deltu = 0.0 * fabs(dux * vn[ivsg][f][0] + duy * vn[ivsg][f][1]);
+        murie[ivsg][f] = rhoct * sdctr + rhoct * slpdu * deltu;
+      }
+    }
+    for (int ivsg = 0; ivsg < 3; ivsg++) {
+      int iv = IPTSG[isg][ivsg] - 1, ip = ipt[iv];
+      for (int f = 0; f < 2; f++) {
+        double area = vn[ivsg][f][2], n0 = vn[ivsg][f][0], n1 = vn[ivsg][f][1];
+        double vnau = (aujmp[ivsg][2] < 1.0e12) ? 1.0 : n0 * aujmp[ivsg][0] + n1 * aujmp[ivsg][1];
+        corner_t k;
+        k.mn[0][0] = murie[ivsg][f] * area * fabs(vnau); k.mn[1][0] = 0.0;
+        k.mn[0][1] = 0.0; k.mn[1][1] = murie[ivsg][f] * area * fabs(vnau);
+        k.mu[0] = k.mn[0][0] * uv[ivsg][0] + k.mn[1][0] * uv[ivsg][1];
+        k.mu[1] = k.mn[1][0] * uv[ivsg][0] + k.mn[1][1] * uv[ivsg][1];
+        k.sn[0] = sig[ivsg] * area * n0 + 0.0 * area * n1;
+        k.sn[1] = 0.0 * area * n0 + sig[ivsg] * area * n1;
+        munacn[0 + 4 * ip] = munacn[0 + 4 * ip] + k.mn[0][0];
+        munacn[1 + 4 * ip] = munacn[1 + 4 * ip] + k.mn[1][0];
+        munacn[2 + 4 * ip] = munacn[2 + 4 * ip] + k.mn[0][1];
+        munacn[3 + 4 * ip] = munacn[3 + 4 * ip] + k.mn[1][1];
+        munacu[0 + 2 * ip] = munacu[0 + 2 * ip] + k.mu[0];
+        munacu[1 + 2 * ip] = munacu[1 + 2 * ip] + k.mu[1];
+        snsigm[0 + 2 * ip] = snsigm[0 + 2 * ip] + k.sn[0];
+        snsigm[1 + 2 * ip] = snsigm[1 + 2 * ip] + k.sn[1];
+        ct[f + 2 * (ivsg + 3 * isg)] = k;
+      }
+    }
+  }
+}
+
+/* rhsifacedg_lagsubgt3 (Getrhslaggauss.f90:8297-8496): face integral of a
+ * triangle; mass-equation weights wfgstm (= the Riemann weights), unit
+ * momentum/energy weights. */
+static void iface_tria(const o_mesh *m, const o_cfg *c, int it, const double *geoel,
+                       const double (*gt)[3], const double *ustar, const double *fstart,
+                       double *rhsel) {
+  const int ielem = it;
+  const double *ge = &G_(geoel, 0, ielem);
+  double bt[6][6];
+  for (int iv = 0; iv < 6; iv++) basis_tria(ge, XVT[iv], YVT[iv], bt[iv]);
+  const int nd = c->ndegr;
+  double ulnpn[6] = {0}, pln0[6] = {0}, pln1[6] = {0}, elnpn[6] = {0};
+  for (int isg = 0; isg < 4; isg++) {
+    double vn[3][2][3];
+    for (int ivsg = 0; ivsg < 3; ivsg++)
+      for (int f = 0; f < 2; f++) {
+        int code = FNTSG[isg][2 * ivsg + f];
+        int slot = abs(code) - 1;
+        double sg = code >= 0 ? 1.0 : -1.0;
+        vn[ivsg][f][0] = sg * gt[slot][0];
+        vn[ivsg][f][1] = sg * gt[slot][1];
+        vn[ivsg][f][2] = gt[slot][2] * wfgst_tria(isg, ivsg, f);
+      }
+    for (int ivsg = 0; ivsg < 3; ivsg++) {
+      int iv = IPTSG[isg][ivsg] - 1;
+      int ip = m->iptri[6 * it + iv] - 1;
+      double us = X_(ustar, 0, ip), vs = X_(ustar, 1, ip);
+      const double *f1 = fstart + 2 * (0 + 2 * (ivsg + 3 * (isg + 4 * (size_t)it)));
+      const double *f2 = fstart + 2 * (1 + 2 * (ivsg + 3 * (isg + 4 * (size_t)it)));
+      for (int k = 0; k < nd; k++) {
+        double b = bt[iv][k];
+        ulnpn[k] = ulnpn[k] + us * vn[ivsg][0][0] * vn[ivsg][0][2] * b + vs * vn[ivsg][0][1] * vn[ivsg][0][2] * b +
+                   us * vn[ivsg][1][0] * vn[ivsg][1][2] * b + vs * vn[ivsg][1][1] * vn[ivsg][1][2] * b;
+        pln0[k] = pln0[k] + f1[0] * b * 1.0 + f2[0] * b * 1.0;
+        pln1[k] = pln1[k] + f1[1] * b * 1.0 + f2[1] * b * 1.0;
+        elnpn[k] = elnpn[k] + us * f1[0] * b * 1.0 + vs * f1[1] * b * 1.0 + us * f2[0] * b * 1.0 +
+                   vs * f2[1] * b * 1.0;
+      }
+    }
+  }
+  for (int k = 0; k < nd; k++) {
+    U_(rhsel, c, k, 0, ielem) = ulnpn[k];
+    U_(rhsel, c, k, 1, ielem) = pln0[k];
+    U_(rhsel, c, k, 2, ielem) = pln1[k];
+    U_(rhsel, c, k, 3, ielem) = elnpn[k];
+  }
+}
+
+/* rhsdomndg_lagmc_curvtria (Getrhslag.f90:4449-4711): volume integral in
+ * cofactor form, rutope(ngausd). */
+static void domn_tria(const o_mesh *m, const o_cfg *c, int it, const double *geoel,
+                      const double *coord, const double *unkno, double *rhsel) {
+  const int ielem = it;
+  const double dr = 0.5, ds = 0.5, g = c->gamlg;
+  double pos[13][2], w[13];
+  const int ng = tri_rule(c->ngausd, pos, w);
+  double xp[6][2];
+  load_tria(m, coord, it, xp);
+  const double *ge = &G_(geoel, 0, ielem);
+  double rc = ge[0], sc = ge[1];
+  double dbdr[6] = {0.0, 1.0 / dr, 0.0, 0, 0, 0}, dbds[6] = {0.0, 0.0, 1.0 / ds, 0, 0, 0};
+  for (int ig = 0; ig < ng; ig++) {
+    double r = pos[ig][0], s = pos[ig][1], wi = w[ig];
+    double shp[6], dspr[6], dsps[6], dxdr, dxds, dydr, dyds;
+    shp6(r, s, shp, dspr, dsps);
+    jac6((const double(*)[2])xp, dspr, dsps, &dxdr, &dxds, &dydr, &dyds);
+    double djaco = 0.5 * wi;
+    if (c->npoly == 2) {
+      dbdr[3] = (r - rc) / (dr * dr); dbdr[4] = 0.0; dbdr[5] = (s - sc) / dr / ds;
+      dbds[3] = 0.0; dbds[4] = (s - sc) / (ds * ds); dbds[5] = (r - rc) / dr / ds;
+    }
+    double gd[2][6];
+    for (int k = 0; k < c->ndegr; k++) {
+      gd[0][k] = dyds * dbdr[k] + (-dydr) * dbds[k];
+      gd[1][k] = (-dxds) * dbdr[k] + dxdr * dbds[k];
+    }
+    double b[6];
+    basis_tria(ge, r, s, b);
+    double un[4] = {0, 0, 0, 0};
+    for (int k = 0; k < c->mdegr; k++)
+      for (int q = 0; q < 4; q++) un[q] = un[q] + U_(unkno, c, k, q, ielem) * b[k];
+    double rhoad = 1.0 / un[0];
+    double uadv = un[1], vadv = un[2], eadv = un[3];
+    double pres = (g - 1.0) * rhoad * (eadv - 0.5 * (uadv * uadv + vadv * vadv));
+    for (int k = 0; k < c->ndegr; k++) {
+      double f0 = gd[0][k] * uadv + gd[1][k] * vadv;
+      double f1 = gd[0][k] * (-pres);
+      double f2 = gd[1][k] * (-pres);
+      double f3 = (gd[0][k] * uadv + gd[1][k] * vadv) * (-pres);
+      U_(rhsel, c, k, 0, ielem) = U_(rhsel, c, k, 0, ielem) - f0 * djaco;
+      U_(rhsel, c, k, 1, ielem) = U_(rhsel, c, k, 1, ielem) - f1 * djaco;
+      U_(rhsel, c, k, 2, ielem) = U_(rhsel, c, k, 2, ielem) - f2 * djaco;
+      U_(rhsel, c, k, 3, ielem) = U_(rhsel, c, k, 3, ielem) - f3 * djaco;
+    }
+  }
+}
+
+/* rhsdomnsrcdg_lag_curvtria (Getrhslag.f90:3907-4066): Taylor-Green energy
+ * source.  The reference sets only b(1:3) there and leaves b(4:6) of its
+ * P2 basis undefined; the full P2 basis is used here (as in the quad
+ * routine). */
+static void src_tria(const o_mesh *m, const o_cfg *c, int it, const double *geoel,
+                     const double *coord, double *rhsel) {
+  const int ielem = it;
+  const double g = c->gamlg;
+  double pos[13][2], w[13];
+  const int ng = tri_rule(c->ngausd, pos, w);
+  double xp[6][2];
+  load_tria(m, coord, it, xp);
+  const double *ge = &G_(geoel, 0, ielem);
+  for (int ig = 0; ig < ng; ig++) {
+    double r = pos[ig][0], s = pos[ig][1], wi = w[ig];
+    double shp[6], dspr[6], dsps[6], a, b, cc, d, xg, yg;
+    shp6(r, s, shp, dspr, dsps);
+    jac6((const double(*)[2])xp, dspr, dsps, &a, &b, &cc, &d);
+    double djaco = 0.5 * wi * (a * d - cc * b);
+    map6((const double(*)[2])xp, shp, &xg, &yg);
+    double bb[6];
+    basis_tria(ge, r, s, bb);
+    double src = 0.25 * PI_ * (cos(3.0 * PI_ * xg) * cos(PI_ * yg) - cos(3.0 * PI_ * yg) * cos(PI_ * xg)) / (g - 1.0);
+    for (int k = 0; k < c->ndegr; k++) U_(rhsel, c, k, 3, ielem) = U_(rhsel, c, k, 3, ielem) + src * bb[k] * djaco;
+  }
+}
+
+/* ---------------------------------------------------------------------- */
 /* getndvelo_lagsubg, Getrhslaggauss.f90:4348-4617                        */
 /* ---------------------------------------------------------------------- */
 static void ndvelo(const o_mesh *m, const o_cfg *c, const double *geoel, const double *gq,
-                   const double *coord, const double *coold, const double *unkno,
-                   double *ustar, double *fstarq /* (2,2,4,4,nquad) */) {
+                   const double *gt, const double *coord, const double *coold, const double *unkno,
+                   double *ustar, double *fstarq /* (2,2,4,4,nquad) */, double *fstart /* (2,2,3,4,ntria) */) {
   const int npoin = m->npoin;
   char *indnd = (char *)calloc(npoin, 1);
   for (int f = 0; f < m->nbfac; f++) {
@@ -1358,6 +2060,10 @@ static void ndvelo(const o_mesh *m, const o_cfg *c, const double *geoel, const d
   double *munacu = (double *)calloc(2 * (size_t)npoin, sizeof(double));
   double *snsigm = (double *)calloc(2 * (size_t)npoin, sizeof(double));
   corner_t *cq = (corner_t *)malloc(sizeof(corner_t) * 32 * (size_t)m->nquad);
+  corner_t *ct = (corner_t *)malloc(sizeof(corner_t) * 24 * (size_t)(m->ntria > 0 ? m->ntria : 1));
+  for (int it = 0; it < m->ntria; it++)
+    riem_tria(m, c, it, geoel, (const double(*)[3])(gt + 45 * (size_t)it), vlave, unkno, coord, coold,
+              munacn, munacu, snsigm, ct + 24 * (size_t)it);
   for (int ie = 0; ie < m->nquad; ie++)
     riem_quad(m, c, ie, geoel, (const double(*)[3])(gq + 48 * (size_t)ie), vlave, unkno, coord, coold,
               munacn, munacu, snsigm, cq + 32 * (size_t)ie);
@@ -1381,6 +2087,17 @@ static void ndvelo(const o_mesh *m, const o_cfg *c, const double *geoel, const d
       for (int k = 0; k < 3; k++) { ustar[2 * nodes[k] + 1] = 0.0; ustar[2 * nodes[k]] = 0.0; }
     }
   }
+  for (int it = 0; it < m->ntria; it++)
+    for (int isg = 0; isg < 4; isg++)
+      for (int ivsg = 0; ivsg < 3; ivsg++) {
+        int ip = m->iptri[6 * it + IPTSG[isg][ivsg] - 1] - 1;
+        for (int f = 0; f < 2; f++) {
+          const corner_t *k = ct + 24 * (size_t)it + (f + 2 * (ivsg + 3 * isg));
+          double *fs = fstart + 2 * (f + 2 * (ivsg + 3 * (isg + 4 * (size_t)it)));
+          fs[0] = k->sn[0] + k->mn[0][0] * ustar[2 * ip] + k->mn[1][0] * ustar[2 * ip + 1] - k->mu[0];
+          fs[1] = k->sn[1] + k->mn[0][1] * ustar[2 * ip] + k->mn[1][1] * ustar[2 * ip + 1] - k->mu[1];
+        }
+      }
   for (int ie = 0; ie < m->nquad; ie++) {
     for (int isg = 0; isg < 4; isg++)
       for (int ivsg = 0; ivsg < 4; ivsg++) {
@@ -1393,7 +2110,7 @@ static void ndvelo(const o_mesh *m, const o_cfg *c, const double *geoel, const d
         }
       }
   }
-  free(indnd); free(vlave); free(munacn); free(munacu); free(snsigm); free(cq);
+  free(indnd); free(vlave); free(munacn); free(munacu); free(snsigm); free(cq); free(ct);
 }
 
 /* ---------------------------------------------------------------------- */
@@ -1549,8 +2266,13 @@ void o_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
            const double *coold, const double *amatr, int itime, int *flags) {
   (void)amatr; (void)itime;
   const int ncell = m->ntria + m->nquad, nsize = ncell + m->nbfac;
-  if (m->ntria > 0) { fprintf(stderr, "oracle: triangles not supported\n"); abort(); }
   memset(rhsel, 0, sizeof(double) * c->ndegr * c->nq * ncell);
+  double *gt = (double *)malloc(sizeof(double) * 45 * (size_t)(m->ntria > 0 ? m->ntria : 1));
+  for (int it = 0; it < m->ntria; it++) {
+    double xp[6][2];
+    load_tria(m, coord, it, xp);
+    normals_tria((const double(*)[2])xp, (double(*)[3])(gt + 45 * (size_t)it));
+  }
   double *gq = (double *)malloc(sizeof(double) * 48 * (size_t)m->nquad);
   for (int ie = 0; ie < m->nquad; ie++) {
     double xp[9][2];
@@ -1562,12 +2284,18 @@ void o_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
   weno(m, c, unkno, geoel, coord, coold);
   for (int ie = 0; ie < nsize; ie++) G_(geoel, 9, ie) = 0.0;
   double *fstarq = (double *)malloc(sizeof(double) * 64 * (size_t)m->nquad);
-  ndvelo(m, c, geoel, gq, coord, coold, unkno, ustar, fstarq);
+  double *fstart = (double *)malloc(sizeof(double) * 48 * (size_t)(m->ntria > 0 ? m->ntria : 1));
+  ndvelo(m, c, geoel, gq, gt, coord, coold, unkno, ustar, fstarq, fstart);
+  for (int it = 0; it < m->ntria; it++)
+    iface_tria(m, c, it, geoel, (const double(*)[3])(gt + 45 * (size_t)it), ustar, fstart, rhsel);
   for (int ie = 0; ie < m->nquad; ie++)
     iface_quad(m, c, ie, geoel, (const double(*)[3])(gq + 48 * (size_t)ie), ustar, fstarq, rhsel);
+  for (int it = 0; it < m->ntria; it++) domn_tria(m, c, it, geoel, coord, unkno, rhsel);
   for (int ie = 0; ie < m->nquad; ie++) domn_quad(m, c, ie, geoel, coord, unkno, rhsel);
-  if (c->ncase == 1)
+  if (c->ncase == 1) {
+    for (int it = 0; it < m->ntria; it++) src_tria(m, c, it, geoel, coord, rhsel);
     for (int ie = 0; ie < m->nquad; ie++) src_quad(m, c, ie, geoel, coord, rhsel);
+  }
   if (c->nlimi == 6 && c->npoly >= 1) {
     /* II.4.6 with aflim = 1 and afvec = I (Getrhslagmc.f90:7695-7708) */
     for (int ie = 0; ie < ncell; ie++) {
@@ -1584,7 +2312,9 @@ void o_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
     }
   }
   free(gq);
+  free(gt);
   free(fstarq);
+  free(fstart);
 }
 
 /* ---------------------------------------------------------------------- */

@@ -2,7 +2,7 @@
  * Lag2D CPU oracle -- TEST INFRASTRUCTURE ONLY.
  *
  * A single-threaded FP64 C restatement of the reference Fortran time step
- * (cell-centred Lagrangian DG, curved 9-node quads, P2 Taylor basis, the
+ * (cell-centred Lagrangian DG, curved 9-node quads and 6-node triangles, P2 Taylor basis, the
  * ncurv=1 / nriem=1 / nfint=4 branch).  It exists to check the CUDA product
  * path and to serve as the timed CPU baseline; nothing in the product
  * library links or calls it.

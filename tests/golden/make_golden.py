@@ -2,10 +2,12 @@
 
 The reference (Fortran) cannot be compiled in this environment and ships no
 golden outputs, so these fixtures pin the CPU oracle against regressions and
-give the GPU path fixed targets: small Taylor-Green and Sedov runs (8 x 8 and
-a 12 x 12 Sedov with troubled cells), 3 time steps each.
+give the GPU path fixed targets: small Taylor-Green and Sedov runs (8 x 8, a
+12 x 12 Sedov with troubled cells, a curved 6 x 6 quad mesh and a curved
+tri/quad mesh), 3 time steps each.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py tgv6_hybrid # one fixture
 """
 import os
 import sys
@@ -17,6 +19,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from lag2d_b200 import quad_mesh, StepConfig  # noqa: E402
+from lag2d_b200.mesh import hybrid_mesh  # noqa: E402
 from oracle.oracle import Oracle  # noqa: E402
 
 CASES = {
@@ -26,6 +29,9 @@ CASES = {
                 StepConfig(ncase=7, gamlg=1.4, nstag=3, cfl=0.1, tend=1.0, sedov_cells=(66, 67, 78, 79)), 3),
     "tgv6_curved": (lambda: quad_mesh(6, 6, 0.0, 1.0, 0.0, 1.0, jitter=0.1, curve=0.05, seed=7),
                     StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=2, cfl=0.1, tend=10.0), 3),
+    # curved tri/quad mesh (alternate rows split into 6-node triangles)
+    "tgv6_hybrid": (lambda: hybrid_mesh(6, 6, 0.0, 1.0, 0.0, 1.0, jitter=0.1, curve=0.05, seed=7),
+                    StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=3, cfl=0.05, tend=10.0), 3),
 }
 
 
@@ -43,6 +49,6 @@ def run_case(name):
 
 
 if __name__ == "__main__":
-    for name in CASES:
+    for name in (sys.argv[1:] or CASES):
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **run_case(name))
         print("wrote", name)

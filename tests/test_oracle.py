@@ -11,6 +11,7 @@ import os
 import numpy as np
 import pytest
 
+from lag2d_b200.mesh import hybrid_mesh
 from lag2d_b200 import quad_mesh, StepConfig, workload
 from oracle.oracle import Oracle
 
@@ -60,8 +61,10 @@ def test_mass_matrix_inverse():
         assert np.linalg.eigvalsh(M).min() > 0
 
 
-@pytest.mark.parametrize("name,nsteps", [("tgv16", 15), ("sedov16", 15)])
-def test_mass_and_energy_conservation(name, nsteps):
+# on the tri/quad mesh the Taylor-Green source integrates to zero over the box
+# only up to the error of the 7-point triangle rule (~1e-13 of the energy)
+@pytest.mark.parametrize("name,nsteps,tol", [("tgv16", 15, 1e-13), ("sedov16", 15, 1e-13), ("tgv_hybrid16", 10, 1e-12)])
+def test_mass_and_energy_conservation(name, nsteps, tol):
     m, c = workload(name)
     o, geoel, amatr, unkno, coord, ustar, dt, ta = _run(m, c, nsteps)
     n = m.ncell
@@ -75,7 +78,7 @@ def test_mass_and_energy_conservation(name, nsteps):
     geoel0, _, u0 = Oracle(m, c).init()
     e0 = (geoel0[:n, 3] * u0[:n, 3, 0]).sum()
     e1 = (geoel[:n, 3] * unkno[:n, 3, 0]).sum()
-    assert abs(e1 - e0) / abs(e0) < 1e-13
+    assert abs(e1 - e0) / abs(e0) < tol
     assert not np.isnan(unkno).any()
 
 
@@ -148,7 +151,7 @@ def test_tgv_symmetry():
     assert np.abs(tau - np.rot90(tau, -1)).max() < 1e-12
 
 
-@pytest.mark.parametrize("name", ["tgv8", "sedov12", "tgv6_curved"])
+@pytest.mark.parametrize("name", ["tgv8", "sedov12", "tgv6_curved", "tgv6_hybrid"])
 def test_golden_fixtures(name):
     from tests.golden.make_golden import run_case
     ref = np.load(os.path.join(GOLDEN, f"{name}.npz"))
@@ -157,3 +160,48 @@ def test_golden_fixtures(name):
         scale = max(np.abs(ref[k]).max(), 1e-300)
         assert np.abs(got[k] - ref[k]).max() / scale < 1e-14, k
     assert abs(float(got["dtfix"]) - float(ref["dtfix"])) <= 1e-15 * float(ref["dtfix"])
+
+
+def test_free_stream_preservation_hybrid():
+    """Uniform states stay uniform on a jittered, curved tri/quad mesh: the
+    triangle sub-cell normals and weights close like the quad ones."""
+    m = hybrid_mesh(6, 6, jitter=0.15, curve=0.1, seed=3)
+    c = StepConfig(ncase=7, gamlg=1.4, sedov_cells=())
+    o = Oracle(m, c)
+    geoel, amatr, unkno = o.init()
+    bnodes = set((m.bface[:, [0, 1, 4]].reshape(-1) - 1).tolist())
+    inner = np.array([i for i in range(m.npoin) if i not in bnodes])
+    conn = [m.iptri[i] for i in range(m.ntria)] + [m.ipqua[i] for i in range(m.nquad)]
+    cells = [e for e in range(m.ncell) if not any((n - 1) in bnodes for n in conn[e])]
+    assert any(e < m.ntria for e in cells) and any(e >= m.ntria for e in cells)
+    for U, V in [(0.0, 0.0), (0.3, -0.7)]:
+        u = np.zeros_like(unkno)
+        u[:, 0, 0] = 1.0
+        u[:, 1, 0], u[:, 2, 0] = U, V
+        u[:, 3, 0] = 1.0 / 0.4 + 0.5 * (U * U + V * V)
+        ustar = np.zeros_like(m.coord)
+        ustar[:, 0], ustar[:, 1] = U, V
+        r, flags = o.rhs(ustar, u, geoel.copy(), m.coord.copy(), m.coord, amatr)
+        assert np.abs(ustar[inner] - [U, V]).max() < 1e-14
+        assert np.abs(r[cells]).max() < 1e-14
+        assert flags.sum() == 0
+
+
+def test_hybrid_mesh_geometry():
+    """Triangle cells of the hybrid mesh: exact areas (straight sides), total
+    area of the box, mass matrix SPD."""
+    m = hybrid_mesh(4, 4, 0.0, 1.0, 0.0, 1.0)
+    assert m.ntria == 16 and m.nquad == 8
+    c = StepConfig(ncase=1, gamlg=5.0 / 3.0)
+    geoel, amatr, unkno = Oracle(m, c).init()
+    n = m.ncell
+    assert abs(geoel[:n, 2].sum() - 1.0) < 1e-14
+    assert np.allclose(geoel[:m.ntria, 2], 1.0 / 32.0, rtol=0, atol=1e-15)
+    for e in range(m.ntria):
+        M = np.zeros((5, 5))
+        k = 0
+        for i in range(5):
+            for j in range(i, 5):
+                M[i, j] = M[j, i] = amatr[e, k]
+                k += 1
+        assert np.linalg.eigvalsh(M).min() > 0
