@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=4)
+    ap.add_argument("--adjoint-checkpoint", type=int, default=2)
     return ap.parse_args()
 
 
@@ -182,6 +184,30 @@ def measured_traffic(family, ncell):
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
+def adjoint_block(s, args, fwd_ms_per_step):
+    """Time lag2d_adjoint over a short window from the solver's current state:
+    the reverse sweep per step (excluding the segment recompute) over the
+    forward step time of the main timing; the recompute is reported beside it."""
+    import numpy as np
+    from lag2d_b200.api import Lag2DError
+
+    nsteps, k = args.adjoint_steps, args.adjoint_checkpoint
+    if nsteps <= 0:
+        return {"ratio": None, "note": "not run (--adjoint-steps 0)"}
+    try:
+        s.adjoint(min(2, nsteps), 1)          # loads the reverse kernels
+        J, gu, gx, gs, ms = s.adjoint(nsteps, k)
+    except Lag2DError as e:
+        return {"ratio": None, "note": str(e)}
+    rev = ms[2] / nsteps
+    return {"ratio": rev / fwd_ms_per_step, "reverse_ms_per_step": rev,
+            "recompute_ms_per_step": ms[1] / nsteps, "forward_with_checkpoints_ms_per_step": ms[0] / nsteps,
+            "forward_ms_per_step": fwd_ms_per_step, "steps": nsteps, "checkpoint_every": k,
+            "functional": "J = 1/2 sum_c m_c (u_c^2 + v_c^2) at the window end",
+            "grad_finite": bool(np.isfinite(gu).all() and np.isfinite(gx).all()),
+            "precision": "FP64 (the FP32-mixed adjoint is not built)"}
+
+
 def run_ours(args):
     rank, local_rank, world = dist_env()
     import numpy as np
@@ -300,6 +326,9 @@ def run_ours(args):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "api": "lag2d_set_state + lag2d_step + lag2d_get_state (pinned host, Fortran layout)"}
 
+    # ---- adjoint: reverse sweep per step against the forward step time
+    adjoint = adjoint_block(s, args, ms_per_step)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -312,7 +341,7 @@ def run_ours(args):
                 "stage_roofline": {"bytes_per_stage": sb, "achieved_gbs": stage_gbs, "peak": peak,
                                    "frac": stage_gbs / peak, "roofline_dof_updates_per_s": dof_stage / (sb / (peak * 1e9))},
                 "kernels_ms_per_step": per_step, "fp32_mixed": mixed,
-                "adjoint_forward_ratio": None, "adjoint_note": "adjoint step not built"}
+                "adjoint_forward_ratio": adjoint.get("ratio"), "adjoint": adjoint}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)

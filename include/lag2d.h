@@ -133,6 +133,43 @@ int lag2d_timing(lag2d_handle *h, int enable);
 double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *launches);
 
 /* ---------------------------------------------------------------------------
+ * Adjoint of the time step.  No counterpart in the reference (it has no
+ * adjoint); both entry points differentiate exactly what lag2d_step computes
+ * on an all-quad mesh with precision 0 and order_exact 0 (others return
+ * LAG2D_EUNSUP), reverse mode per RK stage with these held fixed: the time
+ * step size of each step (ndt == 1 picks it on the forward pass; the gradient
+ * treats it as a constant), the Persson marks, and the reference-
+ * configuration quantities (geoel fields 1-4 and 19-21, amatr).  A window in
+ * which the Persson sensor marks a troubled cell returns LAG2D_EUNSUP (the
+ * adjoint of the WENO reconstruction is not built).  Gradients use the
+ * layouts of lag2d_set_state: unkno(ndegr,nq,ncell), coord(2,npoin),
+ * ustar(2,npoin).
+ * ------------------------------------------------------------------------- */
+
+/* One step with its adjoint: from the handle's state (the step's input) runs
+ * lag2d_step(h, itime, dtfix, tacru), leaving the handle at the step's output,
+ * and returns the gradients of <seed, output> with respect to the input
+ * state.  Any seed pointer may be NULL (zero seed); any grad pointer may be
+ * NULL (not returned). */
+int lag2d_adjoint_step(lag2d_handle *h, int itime, double *dtfix, double *tacru,
+                       const double *seed_unkno, const double *seed_coord,
+                       const double *seed_ustar, double *grad_unkno, double *grad_coord,
+                       double *grad_ustar);
+
+/* nsteps steps from the handle's state with the gradient of the final kinetic
+ * energy J = 1/2 sum_c m_c (u_c^2 + v_c^2) (m_c = geoel field 4, u_c and v_c
+ * the cell averages unkno(1,2,c), unkno(1,3,c)) with respect to the initial
+ * unkno, coord and ustar.  Checkpoints are taken every checkpoint_every steps;
+ * each segment is recomputed once on the reverse sweep, so device memory is
+ * (nsteps / checkpoint_every + 1) states plus checkpoint_every steps of RK
+ * stage inputs.  dtfix and tacru are in/out as in lag2d_step; the handle ends
+ * at the final state.  ms[3] (may be NULL) receives the device time of the
+ * forward pass, of the segment recomputes and of the reverse sweep. */
+int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every, double *dtfix,
+                  double *tacru, double *J, double *dJ_dunkno, double *dJ_dcoord,
+                  double *dJ_dustar, double *ms);
+
+/* ---------------------------------------------------------------------------
  * Allocation-free time-step size.  No counterpart in the reference: it is an
  * addition of this library, computing what getdelt_lag (Getrhslag.f90:
  * 20600-20716) computes, for callers that cannot allocate device memory.

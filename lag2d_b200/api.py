@@ -65,7 +65,7 @@ _libs = {}
 EXPORTS = ("lag2d_create", "lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run",
            "lag2d_get_state", "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_stream",
            "lag2d_kernel_launches", "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error",
-           "lag2d_delt_noalloc")
+           "lag2d_delt_noalloc", "lag2d_adjoint_step", "lag2d_adjoint")
 
 
 def library_path(exact: bool = False) -> str:
@@ -88,7 +88,8 @@ def load(exact: bool = False):
     lib.lag2d_stream.argtypes = [ctypes.c_void_p]
     lib.lag2d_create.argtypes = [ctypes.POINTER(_Mesh), ctypes.POINTER(_Cfg), ctypes.POINTER(ctypes.c_void_p)]
     for name in ("lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run", "lag2d_get_state",
-                 "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_timing"):
+                 "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_timing", "lag2d_adjoint_step",
+                 "lag2d_adjoint"):
         getattr(lib, name).restype = ctypes.c_int
     lib.lag2d_destroy.argtypes = [ctypes.c_void_p]
     _libs[key] = lib
@@ -206,6 +207,50 @@ class Lag2DSolver:
         geoel = np.zeros((self.mesh.nsize, 24))
         self._check(self.lib.lag2d_cellvol(self.h, _p(geoel, _dp)))
         return geoel
+
+    # -- adjoint ---------------------------------------------------------------
+    def adjoint_step(self, seed_unkno=None, seed_coord=None, seed_ustar=None, itime: Optional[int] = None):
+        """One step from the handle's state plus the gradients of
+        <seed, step output> w.r.t. the step input: (grad_unkno (ncell, nq,
+        ndegr), grad_coord (npoin, 2), grad_ustar (npoin, 2)).  The handle
+        ends at the step's output, as after step()."""
+        m, c = self.mesh, self.cfg
+        seeds = []
+        for a, n in ((seed_unkno, m.ncell), (seed_coord, m.npoin), (seed_ustar, m.npoin)):
+            seeds.append(None if a is None else np.ascontiguousarray(np.asarray(a, dtype=np.float64)[:n]))
+        gu = np.zeros((m.ncell, c.nq, c.ndegr))
+        gx = np.zeros((m.npoin, 2))
+        gs = np.zeros((m.npoin, 2))
+        it = self.itime if itime is None else itime
+        dt = ctypes.c_double(self.dtfix)
+        ta = ctypes.c_double(self.tacru)
+        self._check(self.lib.lag2d_adjoint_step(self.h, ctypes.c_int(it), ctypes.byref(dt), ctypes.byref(ta),
+                                                _p(seeds[0], _dp), _p(seeds[1], _dp), _p(seeds[2], _dp),
+                                                _p(gu, _dp), _p(gx, _dp), _p(gs, _dp)))
+        self.dtfix, self.tacru, self.itime = dt.value, ta.value, it + 1
+        return gu, gx, gs
+
+    def adjoint(self, nsteps: int, checkpoint_every: int):
+        """nsteps steps from the handle's state and the gradient of the final
+        kinetic energy J = 1/2 sum m_c (u_c^2 + v_c^2) w.r.t. the initial
+        state.  Returns (J, dJ_dunkno (ncell, nq, ndegr), dJ_dcoord (npoin, 2),
+        dJ_dustar (npoin, 2), ms) with ms = [forward, recompute, reverse]
+        device milliseconds."""
+        m, c = self.mesh, self.cfg
+        gu = np.zeros((m.ncell, c.nq, c.ndegr))
+        gx = np.zeros((m.npoin, 2))
+        gs = np.zeros((m.npoin, 2))
+        ms = np.zeros(3)
+        J = ctypes.c_double(0.0)
+        dt = ctypes.c_double(self.dtfix)
+        ta = ctypes.c_double(self.tacru)
+        self._check(self.lib.lag2d_adjoint(self.h, ctypes.c_int(self.itime), ctypes.c_int(nsteps),
+                                           ctypes.c_int(checkpoint_every), ctypes.byref(dt), ctypes.byref(ta),
+                                           ctypes.byref(J), _p(gu, _dp), _p(gx, _dp), _p(gs, _dp),
+                                           _p(ms, _dp)))
+        self.dtfix, self.tacru = dt.value, ta.value
+        self.itime += nsteps
+        return J.value, gu, gx, gs, ms
 
     # -- instrumentation ---------------------------------------------------------
     @property

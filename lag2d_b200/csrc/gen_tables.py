@@ -187,6 +187,21 @@ def main():
     for isg in range(4):
         out.append(f"  v[{isg}] = {lincomb([(ksub[isg][p], f'c[{p}]') for p in range(36)])};")
     out.append("}")
+    # transposed maps for the reverse (adjoint) pass: lc[p] += sum_t table[p][t] * l[t]
+    out.append("// transpose of detpoly: lc[p] += sum_t dD[t]/dc[p] * lD[t]")
+    out.append("__host__ __device__ __forceinline__ void detpoly_T(const double *lD, double *lc) {")
+    for p in range(36):
+        e = lincomb([(detp[p][t], f'lD[{t}]') for t in range(16)])
+        if e != "0.0":
+            out.append(f"  lc[{p}] += {e};")
+    out.append("}")
+    out.append("// transpose of subareas: lc[p] += sum_isg dv[isg]/dc[p] * lv[isg]")
+    out.append("__host__ __device__ __forceinline__ void subareas_T(const double *lv, double *lc) {")
+    for p in range(36):
+        e = lincomb([(ksub[isg][p], f'lv[{isg}]') for isg in range(4)])
+        if e != "0.0":
+            out.append(f"  lc[{p}] += {e};")
+    out.append("}")
     out.append("// exact area of the cell from det J coefficients")
     out.append("__host__ __device__ __forceinline__ double cell_area(const double *D) {")
     out.append(f"  return {lincomb([(area[t], f'D[{t}]') for t in range(16)])};")

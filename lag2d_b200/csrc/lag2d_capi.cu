@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -52,6 +53,9 @@ void launch_tri_init(const Dev &d, cudaStream_t st);
 void launch_tri_geom(const Dev &d, cudaStream_t st, const double *X, const double *Y);
 void launch_tri_corner(const Dev &d, cudaStream_t st);
 void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa);
+void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp);
+void launch_adjoint_fold(const Dev &d, const void *adj, cudaStream_t st);
+int adjoint_stage_launches();
 }  // namespace lag2d
 
 using namespace lag2d;
@@ -295,20 +299,46 @@ static void rhs_pass(lag2d_handle *h, int fuse, double alfa) {
 // The same step with the optimised kernels: node partial sums, recomputed
 // corner data, closed-form volumes and the stage update fused into the RHS
 // pass in stages 2 and 3.
-static void enqueue_step_fast(lag2d_handle *h, int itime) {
+// Stage-input recorder of the adjoint's recompute pass: before each stage the
+// stage state (U^(s), x^(s), u*_prev) is copied into slot (step, stage), the
+// step's time step size after stage 1, and the troubled-cell count of each
+// stage is accumulated (the adjoint needs it to stay zero).
+struct StageRec {
+  double *U, *x, *y, *us, *vs, *dt;
+  int *troubled;
+  int step, nstag;
+  size_t nu, np;
+};
+__global__ void k_add_count(const int *c, int *acc) { *acc += *c; }
+
+static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = nullptr) {
   const Dev &d = h->d;
   const int nstag = h->cfg.nstag;
   const int T = d.ntria > 0;
   run(h, "begin", [&] { launch_step_begin(d, h->st, itime); });
   for (int istag = 1; istag <= nstag; istag++) {
     const double alfa = kRK[nstag - 2][istag - 1];
+    if (rec) {
+      const size_t slot = (size_t)rec->step * rec->nstag + (istag - 1);
+      cudaMemcpyAsync(rec->U + slot * rec->nu, d.Us, rec->nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+      cudaMemcpyAsync(rec->x + slot * rec->np, d.xs, rec->np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+      cudaMemcpyAsync(rec->y + slot * rec->np, d.ys, rec->np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+      cudaMemcpyAsync(rec->us + slot * rec->np, d.us, rec->np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+      cudaMemcpyAsync(rec->vs + slot * rec->np, d.vs, rec->np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    }
     run(h, "persson", [&] { launch_reset_count(d, h->st); launch_fast_persson(d, h->st); }, 2);
+    if (rec) {
+      k_add_count<<<1, 1, 0, h->st>>>(d.wcount, rec->troubled);
+      h->launches += 1;
+    }
     run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
     run(h, "corner", [&] { corner_pass(h); }, 1 + T);
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
       run(h, "rhs", [&] { rhs_pass(h, 0, alfa); }, 1 + T);
       run(h, "dt", [&] { launch_dt(d, h->st, h->cfg.ndt); }, 2);
+      if (rec)
+        cudaMemcpyAsync(rec->dt + rec->step, &d.sc_dev->dtfix, sizeof(double), cudaMemcpyDeviceToDevice, h->st);
       run(h, "update", [&] { launch_fast_update(d, h->st, alfa); });
     } else {
       run(h, "rhs", [&] { rhs_pass(h, 1, alfa); }, 1 + T);
@@ -776,6 +806,330 @@ double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *lau
   if (it == h->fam.end() || it->second.n == 0) return -1.0;
   if (launches) *launches = it->second.n;
   return it->second.ms / it->second.n;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint of the optimised FP64 step (all-quad meshes).
+//
+// Reverse mode per RK stage with the time step size, the Persson marks and the
+// WENO active set frozen from the forward pass; the forward pass must mark no
+// troubled cell in the window (the WENO reconstruction's adjoint is not built,
+// so a window that limits returns LAG2D_EUNSUP).  Reference-configuration
+// quantities (cell masses, mass matrices, initial-mesh moments) are constants.
+// The stage inputs are recorded by recomputing each checkpoint segment, so the
+// device memory of a window is (segments + 1) checkpoints plus K steps of
+// stage records.
+struct AdjBufs {
+  double *lU, *lUn, *lx, *ly, *lxn, *lyn, *lus, *lvs, *luw, *lvw, *lR, *lS, *lcorr, *pbuf, *tx, *ty;
+};
+struct AdjWork {
+  lag2d_handle *h;
+  std::vector<void *> mem;
+  AdjBufs a{};
+  StageRec rec{};
+  int rc = LAG2D_OK;
+  explicit AdjWork(lag2d_handle *hh) : h(hh) {}
+  ~AdjWork() {
+    cudaStreamSynchronize(h->st);
+    for (void *q : mem) cudaFree(q);
+  }
+  template <typename T> void alloc(T **p, size_t n) {
+    if (rc != LAG2D_OK) return;
+    void *q = nullptr;
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(LAG2D_ECUDA, std::string("cudaMalloc (adjoint): ") + cudaGetErrorString(e));
+      return;
+    }
+    cudaMemsetAsync(q, 0, bytes, h->st);
+    mem.push_back(q);
+    *p = static_cast<T *>(q);
+  }
+  // adjoint buffers plus the stage records of K steps
+  void setup(int K) {
+    const Dev &d = h->d;
+    const size_t nu = (size_t)NU * d.ncell, np = d.npoin;
+    const int nstag = h->cfg.nstag;
+    alloc(&a.lU, nu); alloc(&a.lUn, nu); alloc(&a.lR, nu);
+    alloc(&a.lx, np); alloc(&a.ly, np); alloc(&a.lxn, np); alloc(&a.lyn, np); alloc(&a.lus, np); alloc(&a.lvs, np);
+    alloc(&a.luw, np); alloc(&a.lvw, np); alloc(&a.tx, np); alloc(&a.ty, np);
+    alloc(&a.lS, 5 * np); alloc(&a.lcorr, 4 * (size_t)d.nquad); alloc(&a.pbuf, 54 * (size_t)d.nquad);
+    const size_t ns = (size_t)K * nstag;
+    alloc(&rec.U, ns * nu); alloc(&rec.x, ns * np); alloc(&rec.y, ns * np);
+    alloc(&rec.us, ns * np); alloc(&rec.vs, ns * np); alloc(&rec.dt, K); alloc(&rec.troubled, 1);
+    rec.nstag = nstag; rec.nu = nu; rec.np = np;
+  }
+  // forward of nk steps from the handle's state, recording every stage input
+  int record(int itime, int nk) {
+    cudaMemsetAsync(rec.troubled, 0, sizeof(int), h->st);
+    for (int k = 0; k < nk; k++) {
+      rec.step = k;
+      enqueue_step_fast(h, itime + k, &rec);
+    }
+    return LAG2D_OK;
+  }
+  int check_troubled() {
+    int troubled = 0;
+    CK(cudaMemcpyAsync(&troubled, rec.troubled, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (troubled) return fail(LAG2D_EUNSUP, "troubled cells in the adjoint window: the WENO adjoint is not built");
+    return LAG2D_OK;
+  }
+  // reverse of the nk recorded steps; a.lU / a.lx / a.lus hold the adjoints of
+  // the last step's outputs on entry and of the first step's inputs on return
+  void reverse(int nk) {
+    Dev &d = h->d;
+    const int nstag = h->cfg.nstag;
+    const size_t nu = rec.nu, np = rec.np;
+    for (int k = nk - 1; k >= 0; k--) {
+      for (int istag = nstag; istag >= 1; istag--) {
+        const size_t slot = (size_t)k * nstag + (istag - 1);
+        cudaMemcpyAsync(d.Us, rec.U + slot * nu, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+        cudaMemcpyAsync(d.xs, rec.x + slot * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+        cudaMemcpyAsync(d.ys, rec.y + slot * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+        cudaMemcpyAsync(d.us, rec.us + slot * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+        cudaMemcpyAsync(d.vs, rec.vs + slot * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+        launch_adjoint_stage(d, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k);
+        h->launches += adjoint_stage_launches();
+      }
+      // stage 1 read U^n and x^n directly: fold their adjoints in
+      launch_adjoint_fold(d, &a, h->st);
+      h->launches += 1;
+    }
+  }
+};
+
+// whole-state snapshot of the handle (U^n, x^n, ustar, scalars)
+struct Snapshot {
+  double *U = nullptr, *x = nullptr, *y = nullptr, *us = nullptr, *vs = nullptr;
+  Scalars *sc = nullptr;
+  void alloc(AdjWork &w, int n) {
+    const size_t nu = (size_t)NU * w.h->d.ncell, np = w.h->d.npoin;
+    w.alloc(&U, n * nu); w.alloc(&x, n * np); w.alloc(&y, n * np); w.alloc(&us, n * np); w.alloc(&vs, n * np);
+    w.alloc(&sc, n);
+  }
+  void save(lag2d_handle *h, int c) const {
+    const Dev &d = h->d;
+    const size_t nu = (size_t)NU * d.ncell, np = d.npoin;
+    cudaMemcpyAsync(U + c * nu, d.Un, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(x + c * np, d.xn, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(y + c * np, d.yn, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(us + c * np, d.us, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(vs + c * np, d.vs, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(sc + c, d.sc_dev, sizeof(Scalars), cudaMemcpyDeviceToDevice, h->st);
+  }
+  void restore(lag2d_handle *h, int c) const {
+    const Dev &d = h->d;
+    const size_t nu = (size_t)NU * d.ncell, np = d.npoin;
+    cudaMemcpyAsync(d.Un, U + c * nu, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(d.Us, U + c * nu, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(d.xn, x + c * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(d.xs, x + c * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(d.yn, y + c * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(d.ys, y + c * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(d.us, us + c * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(d.vs, vs + c * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+    cudaMemcpyAsync(d.sc_dev, sc + c, sizeof(Scalars), cudaMemcpyDeviceToDevice, h->st);
+  }
+};
+
+static int adjoint_supported(lag2d_handle *h) {
+  if (h->d.ntria > 0) return fail(LAG2D_EUNSUP, "the adjoint is built for all-quad meshes");
+  if (h->cfg.precision != 0 || h->cfg.order_exact)
+    return fail(LAG2D_EUNSUP, "the adjoint follows the optimised FP64 step (precision 0, order_exact 0)");
+  return LAG2D_OK;
+}
+
+// caller layouts <-> device SoA for the adjoint fields
+static int put_adjoint(lag2d_handle *h, const AdjBufs &a, const double *unkno, const double *coord,
+                       const double *ustar) {
+  const Dev &d = h->d;
+  const size_t nc = d.ncell, np = d.npoin, nu = (size_t)NU * nc;
+  std::vector<double> g(nu, 0.0);
+  if (unkno)
+    for (size_t e = 0; e < nc; e++)
+      for (int t = 0; t < NU; t++) g[(size_t)t * nc + e] = unkno[e * NU + t];
+  CK(cudaMemcpyAsync(a.lU, g.data(), nu * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  const double *src[2] = {coord, ustar};
+  double *dst[2][2] = {{a.lx, a.ly}, {a.lus, a.lvs}};
+  std::vector<double> gx(np), gy(np);
+  for (int f = 0; f < 2; f++) {
+    for (size_t p = 0; p < np; p++) {
+      gx[p] = src[f] ? src[f][2 * p] : 0.0;
+      gy[p] = src[f] ? src[f][2 * p + 1] : 0.0;
+    }
+    CK(cudaMemcpyAsync(dst[f][0], gx.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(dst[f][1], gy.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+  }
+  return LAG2D_OK;
+}
+static int get_adjoint(lag2d_handle *h, const AdjBufs &a, double *unkno, double *coord, double *ustar) {
+  const Dev &d = h->d;
+  const size_t nc = d.ncell, np = d.npoin, nu = (size_t)NU * nc;
+  if (unkno) {
+    std::vector<double> g(nu);
+    CK(cudaMemcpyAsync(g.data(), a.lU, nu * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (size_t e = 0; e < nc; e++)
+      for (int t = 0; t < NU; t++) unkno[e * NU + t] = g[(size_t)t * nc + e];
+  }
+  const double *src[2][2] = {{a.lx, a.ly}, {a.lus, a.lvs}};
+  double *dst[2] = {coord, ustar};
+  std::vector<double> gx(np), gy(np);
+  for (int f = 0; f < 2; f++) {
+    if (!dst[f]) continue;
+    CK(cudaMemcpyAsync(gx.data(), src[f][0], np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(gy.data(), src[f][1], np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (size_t p = 0; p < np; p++) {
+      dst[f][2 * p] = gx[p];
+      dst[f][2 * p + 1] = gy[p];
+    }
+  }
+  return LAG2D_OK;
+}
+
+extern "C" {
+
+int lag2d_adjoint_step(lag2d_handle *h, int itime, double *dtfix, double *tacru, const double *seed_unkno,
+                       const double *seed_coord, const double *seed_ustar, double *grad_unkno, double *grad_coord,
+                       double *grad_ustar) {
+  if (!h || !dtfix || !tacru) return fail(LAG2D_EINVAL, "null argument");
+  int r = adjoint_supported(h);
+  if (r) return r;
+  AdjWork w(h);
+  w.setup(1);
+  if (w.rc) return w.rc;
+  r = put_scalars(h, itime, *dtfix, *tacru);
+  if (r) return r;
+  w.record(itime, 1);
+  Scalars fin;
+  r = get_scalars(h, &fin);
+  if (r) return r;
+  if (fin.status) return read_status(h);
+  r = w.check_troubled();
+  if (r) return r;
+  r = put_adjoint(h, w.a, seed_unkno, seed_coord, seed_ustar);
+  if (r) return r;
+  // keep the step's outputs: the reverse pass overwrites the stage buffers
+  Snapshot out;
+  out.alloc(w, 1);
+  if (w.rc) return w.rc;
+  out.save(h, 0);
+  w.reverse(1);
+  out.restore(h, 0);
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  r = get_adjoint(h, w.a, grad_unkno, grad_coord, grad_ustar);
+  if (r) return r;
+  *dtfix = fin.dtfix;
+  *tacru = fin.tacru;
+  return LAG2D_OK;
+}
+
+int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every, double *dtfix, double *tacru,
+                  double *J, double *dJ_dunkno, double *dJ_dcoord, double *dJ_dustar, double *ms) {
+  if (!h || !dtfix || !tacru || !J) return fail(LAG2D_EINVAL, "null argument");
+  if (nsteps < 1 || checkpoint_every < 1) return fail(LAG2D_EINVAL, "nsteps and checkpoint_every must be >= 1");
+  int r = adjoint_supported(h);
+  if (r) return r;
+  Dev &d = h->d;
+  const int K = std::min(checkpoint_every, nsteps);
+  const int nseg = (nsteps + K - 1) / K;
+  const size_t nc = d.ncell, nu = (size_t)NU * nc;
+  AdjWork w(h);
+  w.setup(K);
+  Snapshot ck;
+  ck.alloc(w, nseg + 1);
+  if (w.rc) return w.rc;
+  cudaEvent_t ev[2];
+  CK(cudaEventCreate(&ev[0]));
+  CK(cudaEventCreate(&ev[1]));
+  struct EvGuard {
+    cudaEvent_t *e;
+    ~EvGuard() { cudaEventDestroy(e[0]); cudaEventDestroy(e[1]); }
+  } evg{ev};
+  auto elapsed = [&] {
+    float t = 0.f;
+    cudaEventSynchronize(ev[1]);
+    cudaEventElapsedTime(&t, ev[0], ev[1]);
+    return (double)t;
+  };
+  double t_fwd = 0, t_rec = 0, t_rev = 0;
+  // forward with a checkpoint at every segment start and at the end
+  r = put_scalars(h, itime0, *dtfix, *tacru);
+  if (r) return r;
+  cudaEventRecord(ev[0], h->st);
+  for (int n = 0; n < nsteps; n++) {
+    if (n % K == 0) ck.save(h, n / K);
+    enqueue_step_fast(h, itime0 + n);
+  }
+  ck.save(h, nseg);
+  cudaEventRecord(ev[1], h->st);
+  t_fwd = elapsed();
+  Scalars fin;
+  r = get_scalars(h, &fin);
+  if (r) return r;
+  if (fin.status) return read_status(h);
+  if (fin.done && fin.itime != itime0 + nsteps - 1)
+    return fail(LAG2D_EINVAL, "the window runs past tend (the steps after it are skipped)");
+  // J and its seed dJ/dU = m (0, u, v, 0) in the cell-average modes
+  {
+    std::vector<double> u(nc), v(nc), m(nc);
+    CK(cudaMemcpyAsync(u.data(), d.Un + 6 * nc, nc * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(v.data(), d.Un + 12 * nc, nc * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(m.data(), d.mass, nc * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    double s = 0.0;
+    std::vector<double> seed(nu, 0.0);
+    for (size_t e = 0; e < nc; e++) {
+      s += 0.5 * m[e] * (u[e] * u[e] + v[e] * v[e]);
+      seed[6 * nc + e] = m[e] * u[e];
+      seed[12 * nc + e] = m[e] * v[e];
+    }
+    *J = s;
+    CK(cudaMemcpyAsync(w.a.lU, seed.data(), nu * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+  }
+  // reverse sweep, one segment at a time: recompute it from its checkpoint
+  // with the stage inputs recorded, then run its steps backwards
+  for (int sg = nseg - 1; sg >= 0; sg--) {
+    const int n0 = sg * K, nk = std::min(K, nsteps - n0);
+    ck.restore(h, sg);
+    cudaEventRecord(ev[0], h->st);
+    w.record(itime0 + n0, nk);
+    cudaEventRecord(ev[1], h->st);
+    t_rec += elapsed();
+    r = w.check_troubled();
+    if (r) {
+      ck.restore(h, nseg);
+      return r;
+    }
+    cudaEventRecord(ev[0], h->st);
+    w.reverse(nk);
+    cudaEventRecord(ev[1], h->st);
+    t_rev += elapsed();
+  }
+  // the handle returns to the final forward state
+  ck.restore(h, nseg);
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  r = get_adjoint(h, w.a, dJ_dunkno, dJ_dcoord, dJ_dustar);
+  if (r) return r;
+  *dtfix = fin.dtfix;
+  *tacru = fin.tacru;
+  if (ms) {
+    ms[0] = t_fwd;
+    ms[1] = t_rec;
+    ms[2] = t_rev;
+  }
+  return LAG2D_OK;
 }
 
 void lag2d_destroy(lag2d_handle *h) {

@@ -834,6 +834,695 @@ __host__ __device__ void f_init_wmom(const Dev &d, int iq) {
   for (int k = 0; k < 9; k++) d.wmom[k * (size_t)d.nquad + iq] = W[A[k]][B[k]];
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint (reverse mode) of the optimised FP64 stage on all-quad meshes.
+//
+// The stage maps (U^(s), x^(s), u*_prev) through the corner pass, the node
+// solve, the RHS pass, the RK update and the node motion to the next stage;
+// each kernel below is the transpose of one of those maps at a recorded
+// forward state (the stage inputs are restored into Dev before the launch).
+// The time step size, the Persson marks and the WENO active set are frozen
+// from the forward pass (the adjoint is only formed when no cell is troubled,
+// so WENO is the identity).  Derivatives of max(eps, .) are taken on the
+// active branch; the impedance's jump-direction branch (|u* - u_c| >= 1e12 c)
+// is taken as the regular one.
+// ---------------------------------------------------------------------------
+struct Adj {
+  double *lU, *lUn;        // [24][ncell] adjoints of U^(s) and U^n
+  double *lx, *ly;         // adjoint of the stage coordinates
+  double *lxn, *lyn;       // adjoint of x^n
+  double *lus, *lvs;       // adjoint of the stage's previous ustar
+  double *luw, *lvw;       // adjoint of the stage's new ustar
+  double *lR;              // [24][ncell] adjoint of the stage RHS
+  double *lS;              // [5][npoin] adjoint of the node sums (m, m u, m v, sigma.n A)
+  double *lcorr;           // [4][nquad] adjoint of the sub-cell density corrections
+  double *pbuf;            // [6][9][nquad] per (quad, node) adjoint contributions
+  double *tx, *ty;         // scratch of the centre-node transpose
+};
+
+// transpose of cross36: c[p] = x_i y_j - x_j y_i
+__host__ __device__ __forceinline__ void cross36_T(const double (*xp)[2], const double *lc, double (*lxp)[2]) {
+  int p = 0;
+  for (int i = 0; i < 9; i++)
+    for (int j = i + 1; j < 9; j++, p++) {
+      lxp[i][0] += lc[p] * xp[j][1];
+      lxp[j][1] += lc[p] * xp[i][0];
+      lxp[j][0] -= lc[p] * xp[i][1];
+      lxp[i][1] -= lc[p] * xp[j][0];
+    }
+}
+
+// transpose of slot_an (a linear map of the tensor coordinates)
+__host__ __device__ __forceinline__ void slot_an_T(int slot, double lax, double lay, double lX[3][3], double lY[3][3]) {
+  if (slot >= 8 && slot < 12) {
+    // ax = -dydr, ay = dxdr, d.dr = -1.5 e - 0.5 c + 2 v with v = l0 q0 + l1 q1 + l2 q2
+    const int f = slot - 8;
+    const double ldx = lay, ldy = -lax;
+    const double lm[3] = {0.375, 0.75, -0.125}, lp[3] = {-0.125, 0.75, 0.375};
+    lX[1][1] += -0.5 * ldx;
+    lY[1][1] += -0.5 * ldy;
+    if (f == 0) {
+      lX[1][0] += -1.5 * ldx; lY[1][0] += -1.5 * ldy;
+      for (int t = 0; t < 3; t++) { lX[1][t] += 2.0 * lm[t] * ldx; lY[1][t] += 2.0 * lm[t] * ldy; }
+    } else if (f == 1) {
+      lX[2][1] += -1.5 * ldx; lY[2][1] += -1.5 * ldy;
+      for (int t = 0; t < 3; t++) { lX[t][1] += 2.0 * lp[t] * ldx; lY[t][1] += 2.0 * lp[t] * ldy; }
+    } else if (f == 2) {
+      lX[1][2] += -1.5 * ldx; lY[1][2] += -1.5 * ldy;
+      for (int t = 0; t < 3; t++) { lX[1][t] += 2.0 * lp[t] * ldx; lY[1][t] += 2.0 * lp[t] * ldy; }
+    } else {
+      lX[0][1] += -1.5 * ldx; lY[0][1] += -1.5 * ldy;
+      for (int t = 0; t < 3; t++) { lX[t][1] += 2.0 * lm[t] * ldx; lY[t][1] += 2.0 * lm[t] * ldy; }
+    }
+    return;
+  }
+  const int ig = slot < 8 ? slot : slot - 4;
+  const FastTables &T = FT();
+  const int ia = T.pa[ig], ib = T.pb[ig];
+  const double *da = T.dl + 3 * ia, *db = T.dl + 3 * ib;
+  double lxr = 0, lyr = 0, lxs = 0, lys = 0;
+  switch (T.side[ig]) {
+    case 0: lyr += lax; lxr -= lay; break;   // ax = yr, ay = -xr
+    case 1: lys += lax; lxs -= lay; break;   // ax = ys, ay = -xs
+    case 2: lyr -= lax; lxr += lay; break;   // ax = -yr, ay = xr
+    default: lys -= lax; lxs += lay; break;  // ax = -ys, ay = xs
+  }
+  // xr = sum_t da[t] X[t][ib], xs = sum_t db[t] X[ia][t]
+  for (int t = 0; t < 3; t++) {
+    lX[t][ib] += da[t] * lxr;
+    lY[t][ib] += da[t] * lyr;
+    lX[ia][t] += db[t] * lxs;
+    lY[ia][t] += db[t] * lys;
+  }
+}
+
+__host__ __device__ __forceinline__ void corner_an_T(int isg, int ivsg, int f, double lax, double lay, double lX[3][3],
+                                                     double lY[3][3]) {
+  const int code = fnqsg2(isg, 2 * ivsg + f);
+  const int slot = (code >= 0 ? code : -code) - 1;
+  if (code < 0) { lax = -lax; lay = -lay; }
+  slot_an_T(slot, lax, lay, lX, lY);
+}
+
+// transpose of corner_m (regular branch): m = 2 w (rho c nn + cimpd rho slpdu |dn|)
+__host__ __device__ __forceinline__ void corner_m_T(double rhoct, double sdctr, double cimpd, double slpdu, double dux,
+                                                    double duy, double ax, double ay, double w, double lm,
+                                                    double &lrho, double &lsd, double &ldux, double &lduy,
+                                                    double &lax, double &lay) {
+  const double nn = sqrt(ax * ax + ay * ay);
+  const double dn = dux * ax + duy * ay;
+  const double adn = fabs(dn), sg = dn >= 0.0 ? 1.0 : -1.0;
+  lrho += lm * 2.0 * w * (sdctr * nn + cimpd * slpdu * adn);
+  lsd += lm * 2.0 * w * rhoct * nn;
+  const double lnn = lm * 2.0 * w * rhoct * sdctr;
+  lax += lnn * ax / nn;
+  lay += lnn * ay / nn;
+  const double ldn = lm * 2.0 * w * cimpd * rhoct * slpdu * sg;
+  ldux += ldn * ax;
+  lduy += ldn * ay;
+  lax += ldn * dux;
+  lay += ldn * duy;
+}
+
+// transpose of the cell-centre state: rhoct = 1/tau, pctr = max(eps, ...),
+// sdctr = sqrt(max(eps, g pctr / rhoct)); adds into lu
+__host__ __device__ __forceinline__ void centre_T(const double u[4][6], double g, double lrho_in, double lsd,
+                                                  double lu[4][6]) {
+  const double eps = 1.0e-6;
+  const double rhoct = 1.0 / u[0][0];
+  const double kin = u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0]);
+  const double pe = (g - 1.0) * rhoct * kin;
+  const double pctr = fmax(eps, pe);
+  const double se = g * pctr / rhoct;
+  const double sdctr = sqrt(fmax(eps, se));
+  double lrho = lrho_in, lp = 0.0;
+  if (se > eps) {
+    const double lse = lsd / (2.0 * sdctr);
+    lp += lse * g / rhoct;
+    lrho += -lse * g * pctr / (rhoct * rhoct);
+  }
+  if (pe > eps) {
+    lrho += lp * (g - 1.0) * kin;
+    lu[3][0] += lp * (g - 1.0) * rhoct;
+    lu[1][0] -= lp * (g - 1.0) * rhoct * u[1][0];
+    lu[2][0] -= lp * (g - 1.0) * rhoct * u[2][0];
+  }
+  lu[0][0] += -lrho * rhoct * rhoct;
+}
+
+// vertex state transpose: st[q] = sum_{k<mdegr} u[q][k] b[k], rhovt = 1/st0,
+// ke = st3 - (st1^2 + st2^2)/2
+__host__ __device__ __forceinline__ void vertex_T(const double *b, int mdegr, const double st[4], double lrhovt,
+                                                  double lke, double lst1, double lst2, double lu[4][6]) {
+  double lst[4];
+  lst[0] = -lrhovt / (st[0] * st[0]);
+  lst[1] = lst1 - lke * st[1];
+  lst[2] = lst2 - lke * st[2];
+  lst[3] = lke;
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++)
+      if (k < mdegr) lu[q][k] += lst[q] * b[k];
+}
+
+// Reverse of the corner pass of quad iq: reads the node-sum adjoints lS at
+// its nodes and lcorr; adds the cell DOF adjoint into lU and writes the node
+// contributions (x, y, u*_prev, v*_prev) into pbuf.
+__host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  const size_t nq = d.nquad;
+  const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  double xp[9][2], c[36], D[16];
+  node_xy(L, xp);
+  cross36(xp, c);
+  detpoly(c, D);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double u[4][6];
+  load_u(d, d.Us, e, u);
+  const double rhoct = 1.0 / u[0][0];
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  double vsub4[4], corr[4], masel4[4], volel4[4];
+  subareas(c, vsub4);
+  for (int isg = 0; isg < 4; isg++) {
+    const double unksgq = (1.0 / vsub4[isg]) * d.msub[isg * nq + iq];
+    const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
+    const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
+    double masel = 0.0;
+    for (int i = 0; i < 5; i++) {
+      const double r = (g5p(i) + ofr) / 2.0;
+      double ee[4];
+      for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+      const double dr = r - G.rc;
+      const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
+      const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
+      const double wi = 0.25 * g5w(i);
+      for (int j = 0; j < 5; j++) {
+        const double s = (g5p(j) + ofs) / 2.0, ds = s - G.sc;
+        const double tau = t0 + ds * (t1 + t2 * ds);
+        const double det = ee[0] + s * (ee[1] + s * (ee[2] + s * ee[3]));
+        masel += (wi * g5w(j)) * det / tau;
+      }
+    }
+    const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
+    masel4[isg] = masel;
+    volel4[isg] = volel;
+    corr[isg] = d.cdrho * (unksgq - 1.0 / (volel / masel));
+  }
+  double lu[4][6];
+  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
+  double lX[3][3], lY[3][3];
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
+  double lrho = 0.0, lsd = 0.0, lcr[4] = {0, 0, 0, 0};
+  for (int k = 0; k < 9; k++) {
+    double b[6];
+    node_basis2(G, k, b);
+    double st[4];
+    for (int q = 0; q < 4; q++) {
+      double acc = 0.0;
+      for (int kk = 0; kk < 6; kk++)
+        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
+      st[q] = acc;
+    }
+    const double rhovt = 1.0 / st[0];
+    const double ke = st[3] - 0.5 * (st[1] * st[1] + st[2] * st[2]);
+    const int pn = d.ipq[k * d.nquad + iq];
+    const double dux = d.us[pn] - st[1], duy = d.vs[pn] - st[2];
+    const double lP0 = a.lS[0 * (size_t)d.npoin + pn], lP1 = a.lS[1 * (size_t)d.npoin + pn];
+    const double lP2 = a.lS[2 * (size_t)d.npoin + pn], lP3 = a.lS[3 * (size_t)d.npoin + pn];
+    const double lP4 = a.lS[4 * (size_t)d.npoin + pn];
+    double lst1 = 0, lst2 = 0, lrhovt = 0, lke = 0, ldux = 0, lduy = 0;
+    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
+      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
+      const double ci = corr[isg];
+      const double pe = (g - 1.0) * (rhovt + ci) * ke;
+      const double pv = fmax(eps, pe);
+      double lpv = 0.0;
+      for (int f = 0; f < 2; f++) {
+        double ax, ay;
+        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
+        const double w = wrie(isg, ivsg, f);
+        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w);
+        const double pw = -2.0 * pv * w;
+        const double lm = lP0 + lP1 * st[1] + lP2 * st[2];
+        lst1 += lP1 * m;
+        lst2 += lP2 * m;
+        const double lpw = lP3 * ax + lP4 * ay;
+        double lax = lP3 * pw, lay = lP4 * pw;
+        lpv += -2.0 * w * lpw;
+        corner_m_T(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w, lm, lrho, lsd, ldux, lduy, lax, lay);
+        corner_an_T(isg, ivsg, f, lax, lay, lX, lY);
+      }
+      if (pe > eps) {
+        lrhovt += lpv * (g - 1.0) * ke;
+        lcr[isg] += lpv * (g - 1.0) * ke;
+        lke += lpv * (g - 1.0) * (rhovt + ci);
+      }
+    }
+    // dux = us - st1, duy = vs - st2
+    double *pb = a.pbuf;
+    pb[(2 * 9 + k) * nq + iq] = ldux;
+    pb[(3 * 9 + k) * nq + iq] = lduy;
+    lst1 -= ldux;
+    lst2 -= lduy;
+    vertex_T(b, d.mdegr, st, lrhovt, lke, lst1, lst2, lu);
+  }
+  // sub-cell density corrections: corr = cdrho (msub / vsub - masel / volel)
+  double lD[16], lv4[4] = {0, 0, 0, 0};
+  for (int t = 0; t < 16; t++) lD[t] = 0.0;
+  for (int isg = 0; isg < 4; isg++) {
+    const double lc = lcr[isg] + a.lcorr[isg * nq + iq];
+    const double msub = d.msub[isg * nq + iq];
+    lv4[isg] += -d.cdrho * lc * msub / (vsub4[isg] * vsub4[isg]);
+    const double lmasel = -d.cdrho * lc / volel4[isg];
+    const double lvolel = d.cdrho * lc * masel4[isg] / (volel4[isg] * volel4[isg]);
+    // volel = sum_mn D[mn] mr[m] ms[n]
+    {
+      const double r0 = (isg == 0 || isg == 3) ? -1.0 : 0.0, s0 = (isg == 0 || isg == 1) ? -1.0 : 0.0;
+      double mr[4], ms[4];
+      const double r1 = r0 + 1.0, s1 = s0 + 1.0;
+      double pr0 = r0, pr1 = r1, ps0 = s0, ps1 = s1;
+      for (int mm = 0; mm < 4; mm++) {
+        mr[mm] = (pr1 - pr0) / (mm + 1);
+        ms[mm] = (ps1 - ps0) / (mm + 1);
+        pr0 *= r0; pr1 *= r1; ps0 *= s0; ps1 *= s1;
+      }
+      for (int mm = 0; mm < 4; mm++)
+        for (int n = 0; n < 4; n++) lD[4 * mm + n] += lvolel * mr[mm] * ms[n];
+    }
+    // masel = sum w det / tau
+    const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
+    const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
+    for (int i = 0; i < 5; i++) {
+      const double r = (g5p(i) + ofr) / 2.0, dr = r - G.rc;
+      for (int j = 0; j < 5; j++) {
+        const double s = (g5p(j) + ofs) / 2.0, ds = s - G.sc;
+        const double wij = 0.25 * g5w(i) * g5w(j);
+        double bb[6];
+        bb[0] = 1.0; bb[1] = dr; bb[2] = ds;
+        bb[3] = 0.5 * dr * dr - G.g19; bb[4] = 0.5 * ds * ds - G.g20; bb[5] = dr * ds - G.g21;
+        double tau = 0.0;
+        for (int k = 0; k < 6; k++) tau += u[0][k] * bb[k];
+        const double det = deteval(D, r, s);
+        const double ldet = lmasel * wij / tau;
+        const double ltau = -lmasel * wij * det / (tau * tau);
+        for (int k = 0; k < 6; k++) lu[0][k] += ltau * bb[k];
+        double rp = 1.0;
+        for (int mm = 0; mm < 4; mm++) {
+          double sp = 1.0;
+          for (int n = 0; n < 4; n++) {
+            lD[4 * mm + n] += ldet * rp * sp;
+            sp *= s;
+          }
+          rp *= r;
+        }
+      }
+    }
+  }
+  centre_T(u, g, lrho, lsd, lu);
+  double lc36[36];
+  for (int p = 0; p < 36; p++) lc36[p] = 0.0;
+  detpoly_T(lD, lc36);
+  subareas_T(lv4, lc36);
+  double lxp[9][2];
+  for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
+  cross36_T(xp, lc36, lxp);
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  for (int k = 0; k < 9; k++) {
+    a.pbuf[(0 * 9 + k) * nq + iq] = lxp[k][0] + lX[A[k]][B[k]];
+    a.pbuf[(1 * 9 + k) * nq + iq] = lxp[k][1] + lY[A[k]][B[k]];
+    a.pbuf[(4 * 9 + k) * nq + iq] = 0.0;
+    a.pbuf[(5 * 9 + k) * nq + iq] = 0.0;
+  }
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * (size_t)d.ncell + e] += lu[q][k];
+}
+
+// Reverse of the RHS pass of quad iq (the RHS written, no fused update):
+// from lR adds into lU, writes pbuf (x, y, u*_prev, v*_prev, u*_new, v*_new)
+// and lcorr.
+__host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  const size_t nq = d.nquad, nc = d.ncell;
+  const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double u[4][6];
+  load_u(d, d.Us, e, u);
+  const double rhoct = 1.0 / u[0][0];
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  double lR[4][6];
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) lR[q][k] = a.lR[(q * 6 + k) * nc + e];
+  double lu[4][6];
+  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
+  double lX[3][3], lY[3][3];
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
+  double lrho = 0.0, lsd = 0.0, lcr[4] = {0, 0, 0, 0};
+  // ---- face integral
+  for (int k = 0; k < 9; k++) {
+    double b[6];
+    node_basis2(G, k, b);
+    double st[4];
+    for (int q = 0; q < 4; q++) {
+      double acc = 0.0;
+      for (int kk = 0; kk < 6; kk++)
+        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
+      st[q] = acc;
+    }
+    const double rhovt = 1.0 / st[0];
+    const double ke = st[3] - 0.5 * (st[1] * st[1] + st[2] * st[2]);
+    const int pn = d.ipq[k * d.nquad + iq];
+    const double dux = d.us[pn] - st[1], duy = d.vs[pn] - st[2];
+    const double un = d.us_new[pn], vn = d.vs_new[pn];
+    const double du0 = un - st[1], du1 = vn - st[2];
+    double ltw = 0, lf0 = 0, lf1 = 0, lfe = 0;
+    for (int kk = 0; kk < 6; kk++) {
+      ltw += lR[0][kk] * b[kk];
+      lf0 += lR[1][kk] * b[kk];
+      lf1 += lR[2][kk] * b[kk];
+      lfe += lR[3][kk] * b[kk];
+    }
+    double lun = 0, lvn = 0, ldu0 = 0, ldu1 = 0, ldux = 0, lduy = 0, lst1 = 0, lst2 = 0, lrhovt = 0, lke = 0;
+    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
+      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
+      const double ci = d.corr[isg * nq + iq];
+      const double pe = (g - 1.0) * (rhovt + ci) * ke;
+      const double pv = fmax(eps, pe);
+      const double wq = wmom(isg, ivsg);
+      double lpv = 0.0;
+      for (int f = 0; f < 2; f++) {
+        double ax, ay;
+        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
+        const double w = wrie(isg, ivsg, f), wm2 = 2.0 * wmas(isg, ivsg, f);
+        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w);
+        const double pw = -2.0 * pv * w;
+        const double fs0 = pw * ax + m * du0, fs1 = pw * ay + m * du1;
+        double lfs0 = lf0 * wq + lfe * wq * un, lfs1 = lf1 * wq + lfe * wq * vn;
+        lun += lfe * wq * fs0 + ltw * wm2 * ax;
+        lvn += lfe * wq * fs1 + ltw * wm2 * ay;
+        double lax = ltw * wm2 * un + lfs0 * pw, lay = ltw * wm2 * vn + lfs1 * pw;
+        const double lpw = lfs0 * ax + lfs1 * ay;
+        const double lm = lfs0 * du0 + lfs1 * du1;
+        ldu0 += lfs0 * m;
+        ldu1 += lfs1 * m;
+        lpv += -2.0 * w * lpw;
+        corner_m_T(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w, lm, lrho, lsd, ldux, lduy, lax, lay);
+        corner_an_T(isg, ivsg, f, lax, lay, lX, lY);
+      }
+      if (pe > eps) {
+        lrhovt += lpv * (g - 1.0) * ke;
+        lcr[isg] += lpv * (g - 1.0) * ke;
+        lke += lpv * (g - 1.0) * (rhovt + ci);
+      }
+    }
+    lun += ldu0;
+    lvn += ldu1;
+    lst1 -= ldu0 + ldux;
+    lst2 -= ldu1 + lduy;
+    a.pbuf[(2 * 9 + k) * nq + iq] = ldux;
+    a.pbuf[(3 * 9 + k) * nq + iq] = lduy;
+    a.pbuf[(4 * 9 + k) * nq + iq] = lun;
+    a.pbuf[(5 * 9 + k) * nq + iq] = lvn;
+    vertex_T(b, d.mdegr, st, lrhovt, lke, lst1, lst2, lu);
+  }
+  // ---- volume integral (5x5 Gauss-Lobatto, cofactor form)
+  for (int i = 0; i < 5; i++) {
+    const double r = l5p(i), dr = r - G.rc;
+    double lr[3], dlr[3];
+    lag3(r, lr);
+    dlag3(r, dlr);
+    double Qx[3], Qy[3], Px[3], Py[3];
+    for (int bb = 0; bb < 3; bb++) {
+      Qx[bb] = dlr[0] * L.X[0][bb] + dlr[1] * L.X[1][bb] + dlr[2] * L.X[2][bb];
+      Qy[bb] = dlr[0] * L.Y[0][bb] + dlr[1] * L.Y[1][bb] + dlr[2] * L.Y[2][bb];
+      Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
+      Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
+    }
+    for (int j = 0; j < 5; j++) {
+      const double s = l5p(j), ds = s - G.sc;
+      double ls[3], dls[3];
+      lag3(s, ls);
+      dlag3(s, dls);
+      const double w = l5w(i) * l5w(j);
+      const double xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
+      const double yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
+      const double xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
+      const double ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
+      double bb[6];
+      bb[0] = 1.0; bb[1] = dr; bb[2] = ds;
+      bb[3] = 0.5 * dr * dr - G.g19; bb[4] = 0.5 * ds * ds - G.g20; bb[5] = dr * ds - G.g21;
+      double un[4];
+      for (int q = 0; q < 4; q++) {
+        un[q] = 0.0;
+        for (int k = 0; k < 6; k++) un[q] += u[q][k] * bb[k];
+      }
+      const double rhoad = 1.0 / un[0];
+      const double kin = un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]);
+      const double pe = (g - 1.0) * rhoad * kin;
+      const double pres = fmax(eps, pe);
+      double gd0[5], gd1[5];
+      gd0[0] = ys;       gd1[0] = -xs;
+      gd0[1] = -yr;      gd1[1] = xr;
+      gd0[2] = ys * dr;  gd1[2] = -xs * dr;
+      gd0[3] = -yr * ds; gd1[3] = xr * ds;
+      gd0[4] = ys * ds - yr * dr;
+      gd1[4] = -xs * ds + xr * dr;
+      const double wp = w * pres;
+      double lgd0[5], lgd1[5], lwp = 0.0, lun1 = 0.0, lun2 = 0.0;
+      for (int kk = 0; kk < 5; kk++) {
+        const double fv = gd0[kk] * un[1] + gd1[kk] * un[2];
+        const double lfv = -lR[0][kk + 1] * w + lR[3][kk + 1] * wp;
+        lwp += lR[3][kk + 1] * fv + lR[1][kk + 1] * gd0[kk] + lR[2][kk + 1] * gd1[kk];
+        lgd0[kk] = lR[1][kk + 1] * wp + lfv * un[1];
+        lgd1[kk] = lR[2][kk + 1] * wp + lfv * un[2];
+        lun1 += lfv * gd0[kk];
+        lun2 += lfv * gd1[kk];
+      }
+      const double lpres = lwp * w;
+      double lun0 = 0.0, lun3 = 0.0;
+      if (pe > eps) {
+        const double lrhoad = lpres * (g - 1.0) * kin;
+        lun3 += lpres * (g - 1.0) * rhoad;
+        lun1 -= lpres * (g - 1.0) * rhoad * un[1];
+        lun2 -= lpres * (g - 1.0) * rhoad * un[2];
+        lun0 += -lrhoad * rhoad * rhoad;
+      }
+      const double lunq[4] = {lun0, lun1, lun2, lun3};
+      for (int q = 0; q < 4; q++)
+        for (int k = 0; k < 6; k++) lu[q][k] += lunq[q] * bb[k];
+      const double lys = lgd0[0] + lgd0[2] * dr + lgd0[4] * ds;
+      const double lyr = -lgd0[1] - lgd0[3] * ds - lgd0[4] * dr;
+      const double lxs = -lgd1[0] - lgd1[2] * dr - lgd1[4] * ds;
+      const double lxr = lgd1[1] + lgd1[3] * ds + lgd1[4] * dr;
+      for (int aa = 0; aa < 3; aa++)
+        for (int b2 = 0; b2 < 3; b2++) {
+          lX[aa][b2] += lxr * dlr[aa] * ls[b2] + lxs * lr[aa] * dls[b2];
+          lY[aa][b2] += lyr * dlr[aa] * ls[b2] + lys * lr[aa] * dls[b2];
+        }
+    }
+  }
+  // ---- Taylor-Green source
+  double lxp[9][2];
+  for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
+  if (d.ncase == 1) {
+    double xp[9][2], c[36], D[16];
+    node_xy(L, xp);
+    cross36(xp, c);
+    detpoly(c, D);
+    const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
+    const double PI = 3.14159265358979311599796346854;
+    double lD[16];
+    for (int t = 0; t < 16; t++) lD[t] = 0.0;
+    for (int i = 0; i < 5; i++) {
+      const double r = g5p(i), dr = r - G.rc;
+      double lr[3];
+      lag3(r, lr);
+      for (int j = 0; j < 5; j++) {
+        const double s = g5p(j), ds = s - G.sc;
+        double ls[3];
+        lag3(s, ls);
+        double xg = 0.0, yg = 0.0;
+        for (int aa = 0; aa < 3; aa++)
+          for (int b2 = 0; b2 < 3; b2++) {
+            xg += lr[aa] * ls[b2] * L.X[aa][b2];
+            yg += lr[aa] * ls[b2] * L.Y[aa][b2];
+          }
+        const double wij = g5w(i) * g5w(j);
+        const double djaco = wij * deteval(D, r, s);
+        const double cx = cospi(xg), cy = cospi(yg), sx = sinpi(xg), sy = sinpi(yg);
+        const double c3x = cx * (4.0 * cx * cx - 3.0), c3y = cy * (4.0 * cy * cy - 3.0);
+        double bb[6];
+        bb[0] = 1.0; bb[1] = dr; bb[2] = ds;
+        bb[3] = 0.5 * dr * dr - G.g19; bb[4] = 0.5 * ds * ds - G.g20; bb[5] = dr * ds - G.g21;
+        double lsrc = 0.0;
+        for (int k = 0; k < 6; k++) lsrc += lR[3][k] * bb[k];
+        const double ldj = lsrc * coef * (c3x * cy - c3y * cx);
+        const double lc3x = lsrc * coef * djaco * cy, lc3y = -lsrc * coef * djaco * cx;
+        const double lcx = -lsrc * coef * djaco * c3y + lc3x * (12.0 * cx * cx - 3.0);
+        const double lcy = lsrc * coef * djaco * c3x + lc3y * (12.0 * cy * cy - 3.0);
+        const double lxg = -lcx * PI * sx, lyg = -lcy * PI * sy;
+        for (int aa = 0; aa < 3; aa++)
+          for (int b2 = 0; b2 < 3; b2++) {
+            lX[aa][b2] += lxg * lr[aa] * ls[b2];
+            lY[aa][b2] += lyg * lr[aa] * ls[b2];
+          }
+        double rp = 1.0;
+        for (int mm = 0; mm < 4; mm++) {
+          double sp = 1.0;
+          for (int n = 0; n < 4; n++) {
+            lD[4 * mm + n] += ldj * wij * rp * sp;
+            sp *= s;
+          }
+          rp *= r;
+        }
+      }
+    }
+    double lc36[36];
+    for (int p = 0; p < 36; p++) lc36[p] = 0.0;
+    detpoly_T(lD, lc36);
+    cross36_T(xp, lc36, lxp);
+  }
+  centre_T(u, g, lrho, lsd, lu);
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  for (int k = 0; k < 9; k++) {
+    a.pbuf[(0 * 9 + k) * nq + iq] = lxp[k][0] + lX[A[k]][B[k]];
+    a.pbuf[(1 * 9 + k) * nq + iq] = lxp[k][1] + lY[A[k]][B[k]];
+  }
+  for (int isg = 0; isg < 4; isg++) a.lcorr[isg * nq + iq] = lcr[isg];
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu[q][k];
+}
+
+// Gather of the per-(quad, node) contributions into the node adjoints:
+// nv = 4 (x, y, u*_prev, v*_prev) after the corner pass, 6 after the RHS
+// pass (also u*_new, v*_new); quads in cell order.
+__host__ __device__ void a_gather(const Dev &d, const Adj &a, int p, int nv) {
+  if (p >= d.npoin) return;
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  const int b = d.node_ptr2[p], en = d.node_slot ? d.node_ptr2[p + 1] : b;
+  for (int i = b; i < en; i++) {
+    const int id = d.node_slot[i];
+    if (id < 0) continue;
+    const int iq = id / 9, k = id - 9 * iq;
+    for (int v = 0; v < nv; v++) s[v] += a.pbuf[(v * 9 + k) * (size_t)d.nquad + iq];
+  }
+  a.lx[p] += s[0];
+  a.ly[p] += s[1];
+  a.lus[p] += s[2];
+  a.lvs[p] += s[3];
+  if (nv > 4) {
+    a.luw[p] += s[4];
+    a.lvw[p] += s[5];
+  }
+}
+
+// Reverse of the node solve: u* = (S1 - S3) / S0, v* = (S2 - S4) / S0 with the
+// wall masks; kept nodes take u*_prev.
+__host__ __device__ void a_nodesolve(const Dev &d, const Adj &a, int p) {
+  if (p >= d.npoin) return;
+  const unsigned char mask = d.bcmask[p];
+  const double lu = (mask & 1) ? 0.0 : a.luw[p];
+  const double lv = (mask & 2) ? 0.0 : a.lvw[p];
+  const size_t np = d.npoin;
+  for (int v = 0; v < 5; v++) a.lS[v * np + p] = 0.0;
+  if (mask & 4) {
+    a.lus[p] += lu;
+    a.lvs[p] += lv;
+    return;
+  }
+  double S[5] = {0, 0, 0, 0, 0};
+  for (int i = d.node_ptr2[p]; i < d.node_ptr2[p + 1]; i++) {
+    const int id = d.node_slot[i];
+    if (id < 0) continue;
+    const int iq = id / 9, k = id - 9 * iq;
+    for (int v = 0; v < 5; v++) S[v] += d.npart[(v * 9 + k) * (size_t)d.nquad + iq];
+  }
+  const double us = (S[1] - S[3]) / S[0], vs = (S[2] - S[4]) / S[0];
+  a.lS[0 * np + p] = -(lu * us + lv * vs) / S[0];
+  a.lS[1 * np + p] = lu / S[0];
+  a.lS[3 * np + p] = -lu / S[0];
+  a.lS[2 * np + p] = lv / S[0];
+  a.lS[4 * np + p] = -lv / S[0];
+}
+
+// Reverse of the RK update U = alfa U^n + (1 - alfa)(U^(s) + dt M^-1 R)
+__host__ __device__ void a_update(const Dev &d, const Adj &a, int e, double alfa, double dt) {
+  if (e >= d.ncell) return;
+  const size_t nc = d.ncell;
+  double am[16];
+  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * nc + e];
+  const int IDX[5][5] = {{0, 1, 2, 3, 4}, {1, 5, 6, 7, 8}, {2, 6, 9, 10, 11}, {3, 7, 10, 12, 13}, {4, 8, 11, 13, 14}};
+  const double oma = 1.0 - alfa;
+  for (int q = 0; q < 4; q++) {
+    double l[6];
+    for (int k = 0; k < 6; k++) l[k] = a.lU[(q * 6 + k) * nc + e];
+    for (int k = 0; k < 6; k++) {
+      a.lUn[(q * 6 + k) * nc + e] += alfa * l[k];
+      a.lU[(q * 6 + k) * nc + e] = oma * l[k];
+    }
+    a.lR[(q * 6) * nc + e] = oma * dt * am[15] * l[0];
+    for (int i = 0; i < 5; i++) {
+      double acc = 0.0;
+      for (int j = 0; j < 5; j++) acc += am[IDX[i][j]] * l[j + 1];
+      a.lR[(q * 6 + i + 1) * nc + e] = oma * dt * acc;
+    }
+  }
+}
+
+// Reverse of the node motion x = alfa x^n + (1 - alfa)(x + dt u*_new), with
+// u*_new becoming the next stage's u*_prev
+__host__ __device__ void a_nodes(const Dev &d, const Adj &a, int p, double alfa, double dt) {
+  if (p >= d.npoin) return;
+  const double oma = 1.0 - alfa;
+  a.lxn[p] += alfa * a.lx[p];
+  a.lyn[p] += alfa * a.ly[p];
+  a.luw[p] = oma * dt * a.lx[p] + a.lus[p];
+  a.lvw[p] = oma * dt * a.ly[p] + a.lvs[p];
+  a.lx[p] = oma * a.lx[p];
+  a.ly[p] = oma * a.ly[p];
+  a.lus[p] = 0.0;
+  a.lvs[p] = 0.0;
+}
+
+// Reverse of the centre-node re-interpolation x9 = -(x1+..+x4)/4 + (x5+..+x8)/2
+// (per node: its own adjoint plus the contributions of the quads whose
+// centre it feeds; a centre node's own coordinate is overwritten).
+__host__ __device__ void a_centre(const Dev &d, const Adj &a, int p) {
+  if (p >= d.npoin) return;
+  double sx = a.lx[p], sy = a.ly[p];
+  for (int i = d.node_ptr2[p]; i < d.node_ptr2[p + 1]; i++) {
+    const int id = d.node_slot[i];
+    if (id < 0) continue;
+    const int iq = id / 9, k = id - 9 * iq;
+    if (k == 8) { sx = 0.0; sy = 0.0; break; }
+  }
+  for (int i = d.node_ptr2[p]; i < d.node_ptr2[p + 1]; i++) {
+    const int id = d.node_slot[i];
+    if (id < 0) continue;
+    const int iq = id / 9, k = id - 9 * iq;
+    if (k == 8) continue;
+    const int pc = d.ipq[8 * d.nquad + iq];
+    const double cw = k < 4 ? -0.25 : 0.5;
+    sx += cw * a.lx[pc];
+    sy += cw * a.ly[pc];
+  }
+  a.tx[p] = sx;
+  a.ty[p] = sy;
+}
+__host__ __device__ void a_copy_centre(const Dev &d, const Adj &a, int p) {
+  if (p >= d.npoin) return;
+  a.lx[p] = a.tx[p];
+  a.ly[p] = a.ty[p];
+}
+
 __global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
 #ifndef LAG2D_CORNER_MIN_BLOCKS
 #define LAG2D_CORNER_MIN_BLOCKS 3  // resident blocks of 128 per SM the corner pass is compiled for
@@ -848,9 +1537,64 @@ __global__ void k_nodes2(Dev d, double alfa) { f_nodes(d, blockIdx.x * blockDim.
 __global__ void k_geom2(Dev d, int fix) { f_geom(d, blockIdx.x * blockDim.x + threadIdx.x, fix); }
 __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + threadIdx.x); }
 
+__global__ void __launch_bounds__(128) k_a_corner(Dev d, Adj a) { a_corner(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(128) k_a_rhs(Dev d, Adj a) { a_rhs(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void k_a_gather(Dev d, Adj a, int nv) { a_gather(d, a, blockIdx.x * blockDim.x + threadIdx.x, nv); }
+__global__ void k_a_nodesolve(Dev d, Adj a) { a_nodesolve(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void k_a_update(Dev d, Adj a, double alfa, const double *dtp) {
+  a_update(d, a, blockIdx.x * blockDim.x + threadIdx.x, alfa, *dtp);
+}
+__global__ void k_a_nodes(Dev d, Adj a, double alfa, const double *dtp) {
+  a_nodes(d, a, blockIdx.x * blockDim.x + threadIdx.x, alfa, *dtp);
+}
+__global__ void k_a_centre(Dev d, Adj a) { a_centre(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void k_a_copy_centre(Dev d, Adj a) { a_copy_centre(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+// end of a step's reverse: the stage-1 inputs are U^n and x^n themselves, and
+// the previous step's copy-back makes them its final stage state
+__global__ void k_a_fold(Dev d, Adj a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const size_t nu = (size_t)NU * d.ncell;
+  for (size_t t = i; t < nu; t += stride) {
+    a.lU[t] += a.lUn[t];
+    a.lUn[t] = 0.0;
+  }
+  for (int p = i; p < d.npoin; p += stride) {
+    a.lx[p] += a.lxn[p];
+    a.ly[p] += a.lyn[p];
+    a.lxn[p] = 0.0;
+    a.lyn[p] = 0.0;
+  }
+}
+
 static inline int nb(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace fast
+
+// Reverse of one RK stage of the optimised FP64 step (all-quad meshes).  The
+// stage inputs (U^(s), x^(s), u*_prev) must be in d.Us, d.xs/ys, d.us/vs; the
+// forward corner and node passes are recomputed first (node sums, sub-cell
+// corrections and u*_new), then the transposes run in reverse order.  dtp is
+// the device address of the step's time step size.
+void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp) {
+  const fast::Adj &a = *static_cast<const fast::Adj *>(adj);
+  const int bq = fast::nb(d.nquad, 128), bp = fast::nb(d.npoin, 256), bc = fast::nb(d.ncell, 256);
+  fast::k_corner2<<<bq, 128, 0, st>>>(d);
+  fast::k_node2<<<bp, 256, 0, st>>>(d);
+  fast::k_a_centre<<<bp, 256, 0, st>>>(d, a);
+  fast::k_a_copy_centre<<<bp, 256, 0, st>>>(d, a);
+  fast::k_a_nodes<<<bp, 256, 0, st>>>(d, a, alfa, dtp);
+  fast::k_a_update<<<bc, 256, 0, st>>>(d, a, alfa, dtp);
+  fast::k_a_rhs<<<bq, 128, 0, st>>>(d, a);
+  fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 6);
+  fast::k_a_nodesolve<<<bp, 256, 0, st>>>(d, a);
+  fast::k_a_corner<<<bq, 128, 0, st>>>(d, a);
+  fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
+}
+void launch_adjoint_fold(const Dev &d, const void *adj, cudaStream_t st) {
+  fast::k_a_fold<<<1184, 256, 0, st>>>(d, *static_cast<const fast::Adj *>(adj));
+}
+int adjoint_stage_launches() { return 11; }
+size_t adjoint_struct_size() { return sizeof(fast::Adj); }
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
 void launch_fast_corner(const Dev &d, cudaStream_t st) { fast::k_corner2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
