@@ -285,34 +285,57 @@ static void enqueue_step_reference_order(lag2d_handle *h, int itime) {
 // Corner and RHS passes of the optimised step: FP64, or the FP32-mixed form
 // (config precision = 1) with the same node pass, update and geometry.
 // Triangles run their FP64 kernels in both forms.
-static void corner_pass(lag2d_handle *h) {
-  launch_tri_corner(h->d, h->st);
-  if (h->cfg.precision == 1) launch_mixed_corner(h->d, h->st);
-  else launch_fast_corner(h->d, h->st);
+static void corner_pass(lag2d_handle *h, const Dev &d) {
+  launch_tri_corner(d, h->st);
+  if (h->cfg.precision == 1) launch_mixed_corner(d, h->st);
+  else launch_fast_corner(d, h->st);
 }
-static void rhs_pass(lag2d_handle *h, int fuse, double alfa) {
-  launch_tri_rhs(h->d, h->st, h->d.us_new, h->d.vs_new, fuse, alfa);
-  if (h->cfg.precision == 1) launch_mixed_rhs(h->d, h->st, fuse, alfa);
-  else launch_fast_rhs(h->d, h->st, fuse, alfa);
+static void rhs_pass(lag2d_handle *h, const Dev &d, int fuse, double alfa) {
+  launch_tri_rhs(d, h->st, d.us_new, d.vs_new, fuse, alfa);
+  if (h->cfg.precision == 1) launch_mixed_rhs(d, h->st, fuse, alfa);
+  else launch_fast_rhs(d, h->st, fuse, alfa);
 }
+
+// Stage recorder of the adjoint's recompute pass.  Before each stage the
+// stage state (U^(s), x^(s), u*_prev) is copied into slot (step, stage); the
+// stage's corner and node outputs (node partial sums, sub-cell density
+// corrections, u*_new) are written straight into the slot instead of the
+// handle's buffers; the step's time step size is kept after stage 1, and the
+// troubled-cell count of each stage is accumulated (the adjoint needs it to
+// stay zero).
+struct StageRec {
+  double *U, *x, *y, *us, *vs, *dt;
+  double *npart, *corr, *usn, *vsn;
+  int *troubled;
+  int step, nstag;
+  size_t nu, np, nq;
+  // the handle's device view with the corner/node outputs of a slot
+  Dev outputs(const Dev &d0, size_t slot) const {
+    Dev d = d0;
+    d.npart = npart + slot * 45 * nq;
+    d.corr = corr + slot * 4 * nq;
+    d.us_new = usn + slot * np;
+    d.vs_new = vsn + slot * np;
+    return d;
+  }
+  // ... and with the recorded stage inputs as well
+  Dev inputs(const Dev &d0, size_t slot) const {
+    Dev d = outputs(d0, slot);
+    d.Us = U + slot * nu;
+    d.xs = x + slot * np;
+    d.ys = y + slot * np;
+    d.us = us + slot * np;
+    d.vs = vs + slot * np;
+    return d;
+  }
+};
+__global__ void k_add_count(const int *c, int *acc) { *acc += *c; }
 
 // The same step with the optimised kernels: node partial sums, recomputed
 // corner data, closed-form volumes and the stage update fused into the RHS
 // pass in stages 2 and 3.
-// Stage-input recorder of the adjoint's recompute pass: before each stage the
-// stage state (U^(s), x^(s), u*_prev) is copied into slot (step, stage), the
-// step's time step size after stage 1, and the troubled-cell count of each
-// stage is accumulated (the adjoint needs it to stay zero).
-struct StageRec {
-  double *U, *x, *y, *us, *vs, *dt;
-  int *troubled;
-  int step, nstag;
-  size_t nu, np;
-};
-__global__ void k_add_count(const int *c, int *acc) { *acc += *c; }
-
 static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = nullptr) {
-  const Dev &d = h->d;
+  Dev d = h->d;
   const int nstag = h->cfg.nstag;
   const int T = d.ntria > 0;
   run(h, "begin", [&] { launch_step_begin(d, h->st, itime); });
@@ -320,6 +343,7 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
     const double alfa = kRK[nstag - 2][istag - 1];
     if (rec) {
       const size_t slot = (size_t)rec->step * rec->nstag + (istag - 1);
+      d = rec->outputs(h->d, slot);
       cudaMemcpyAsync(rec->U + slot * rec->nu, d.Us, rec->nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
       cudaMemcpyAsync(rec->x + slot * rec->np, d.xs, rec->np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
       cudaMemcpyAsync(rec->y + slot * rec->np, d.ys, rec->np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
@@ -332,16 +356,16 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
       h->launches += 1;
     }
     run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
-    run(h, "corner", [&] { corner_pass(h); }, 1 + T);
+    run(h, "corner", [&] { corner_pass(h, d); }, 1 + T);
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
-      run(h, "rhs", [&] { rhs_pass(h, 0, alfa); }, 1 + T);
+      run(h, "rhs", [&] { rhs_pass(h, d, 0, alfa); }, 1 + T);
       run(h, "dt", [&] { launch_dt(d, h->st, h->cfg.ndt); }, 2);
       if (rec)
         cudaMemcpyAsync(rec->dt + rec->step, &d.sc_dev->dtfix, sizeof(double), cudaMemcpyDeviceToDevice, h->st);
       run(h, "update", [&] { launch_fast_update(d, h->st, alfa); });
     } else {
-      run(h, "rhs", [&] { rhs_pass(h, 1, alfa); }, 1 + T);
+      run(h, "rhs", [&] { rhs_pass(h, d, 1, alfa); }, 1 + T);
     }
     run(h, "nodes", [&] { launch_fast_nodes(d, h->st, alfa); });
     run(h, "geom", [&] { launch_tri_geom(d, h->st, d.xs, d.ys); launch_fast_geom(d, h->st, 1); }, 1 + T);
@@ -736,9 +760,9 @@ int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
     run(h, "node", [&] { launch_node(d, h->st); });
     run(h, "rhs", [&] { launch_tri_rhs(d, h->st, d.us, d.vs, 0, 0.0); launch_rhs(d, h->st); }, 1 + (d.ntria > 0));
   } else {
-    run(h, "corner", [&] { corner_pass(h); }, 1 + (d.ntria > 0));
+    run(h, "corner", [&] { corner_pass(h, d); }, 1 + (d.ntria > 0));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
-    run(h, "rhs", [&] { rhs_pass(h, 0, 0.0); }, 1 + (d.ntria > 0));
+    run(h, "rhs", [&] { rhs_pass(h, d, 0, 0.0); }, 1 + (d.ntria > 0));
     // the RHS keeps ustar of the previous stage for the impedances; expose the new one
     CK(cudaMemcpyAsync(d.us, d.us_new, d.npoin * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemcpyAsync(d.vs, d.vs_new, d.npoin * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
@@ -861,7 +885,9 @@ struct AdjWork {
     const size_t ns = (size_t)K * nstag;
     alloc(&rec.U, ns * nu); alloc(&rec.x, ns * np); alloc(&rec.y, ns * np);
     alloc(&rec.us, ns * np); alloc(&rec.vs, ns * np); alloc(&rec.dt, K); alloc(&rec.troubled, 1);
-    rec.nstag = nstag; rec.nu = nu; rec.np = np;
+    alloc(&rec.npart, ns * 45 * (size_t)d.nquad); alloc(&rec.corr, ns * 4 * (size_t)d.nquad);
+    alloc(&rec.usn, ns * np); alloc(&rec.vsn, ns * np);
+    rec.nstag = nstag; rec.nu = nu; rec.np = np; rec.nq = d.nquad;
   }
   // forward of nk steps from the handle's state, recording every stage input
   int record(int itime, int nk) {
@@ -882,22 +908,15 @@ struct AdjWork {
   // reverse of the nk recorded steps; a.lU / a.lx / a.lus hold the adjoints of
   // the last step's outputs on entry and of the first step's inputs on return
   void reverse(int nk) {
-    Dev &d = h->d;
     const int nstag = h->cfg.nstag;
-    const size_t nu = rec.nu, np = rec.np;
     for (int k = nk - 1; k >= 0; k--) {
       for (int istag = nstag; istag >= 1; istag--) {
-        const size_t slot = (size_t)k * nstag + (istag - 1);
-        cudaMemcpyAsync(d.Us, rec.U + slot * nu, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
-        cudaMemcpyAsync(d.xs, rec.x + slot * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
-        cudaMemcpyAsync(d.ys, rec.y + slot * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
-        cudaMemcpyAsync(d.us, rec.us + slot * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
-        cudaMemcpyAsync(d.vs, rec.vs + slot * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
-        launch_adjoint_stage(d, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k);
+        const Dev ds = rec.inputs(h->d, (size_t)k * nstag + (istag - 1));
+        launch_adjoint_stage(ds, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k);
         h->launches += adjoint_stage_launches();
       }
       // stage 1 read U^n and x^n directly: fold their adjoints in
-      launch_adjoint_fold(d, &a, h->st);
+      launch_adjoint_fold(h->d, &a, h->st);
       h->launches += 1;
     }
   }

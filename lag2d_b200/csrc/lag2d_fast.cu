@@ -1112,32 +1112,47 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
       for (int mm = 0; mm < 4; mm++)
         for (int n = 0; n < 4; n++) lD[4 * mm + n] += lvolel * mr[mm] * ms[n];
     }
-    // masel = sum w det / tau
+    // masel = sum w det / tau, transposed row by row (per-row moments of the
+    // det and tau adjoints in s, as in the volume integral)
     const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
     const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
+#pragma unroll 1
     for (int i = 0; i < 5; i++) {
       const double r = (g5p(i) + ofr) / 2.0, dr = r - G.rc;
+      double ee[4];
+#pragma unroll
+      for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+      const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
+      const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
+      const double wi = 0.25 * g5w(i);
+      double m0 = 0.0, m1 = 0.0, m2 = 0.0, Ls[4] = {0, 0, 0, 0};
+#pragma unroll
       for (int j = 0; j < 5; j++) {
         const double s = (g5p(j) + ofs) / 2.0, ds = s - G.sc;
-        const double wij = 0.25 * g5w(i) * g5w(j);
-        double bb[6];
-        bb[0] = 1.0; bb[1] = dr; bb[2] = ds;
-        bb[3] = 0.5 * dr * dr - G.g19; bb[4] = 0.5 * ds * ds - G.g20; bb[5] = dr * ds - G.g21;
-        double tau = 0.0;
-        for (int k = 0; k < 6; k++) tau += u[0][k] * bb[k];
-        const double det = deteval(D, r, s);
-        const double ldet = lmasel * wij / tau;
-        const double ltau = -lmasel * wij * det / (tau * tau);
-        for (int k = 0; k < 6; k++) lu[0][k] += ltau * bb[k];
-        double rp = 1.0;
-        for (int mm = 0; mm < 4; mm++) {
-          double sp = 1.0;
-          for (int n = 0; n < 4; n++) {
-            lD[4 * mm + n] += ldet * rp * sp;
-            sp *= s;
-          }
-          rp *= r;
-        }
+        const double tau = t0 + ds * (t1 + t2 * ds);
+        const double det = ee[0] + s * (ee[1] + s * (ee[2] + s * ee[3]));
+        const double ldet = lmasel * (wi * g5w(j)) / tau;
+        const double ltau = -ldet * det / tau;
+        m0 += ltau;
+        m1 += ltau * ds;
+        m2 += ltau * ds * ds;
+        Ls[0] += ldet;
+        Ls[1] += ldet * s;
+        Ls[2] += ldet * s * s;
+        Ls[3] += ldet * s * s * s;
+      }
+      lu[0][0] += m0;
+      lu[0][1] += dr * m0;
+      lu[0][2] += m1;
+      lu[0][3] += (0.5 * dr * dr - G.g19) * m0;
+      lu[0][4] += 0.5 * m2 - G.g20 * m0;
+      lu[0][5] += dr * m1 - G.g21 * m0;
+      double rp = 1.0;
+#pragma unroll
+      for (int mm = 0; mm < 4; mm++) {
+#pragma unroll
+        for (int n = 0; n < 4; n++) lD[4 * mm + n] += rp * Ls[n];
+        rp *= r;
       }
     }
   }
@@ -1252,37 +1267,47 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     a.pbuf[(5 * 9 + k) * nq + iq] = lvn;
     vertex_T(b, d.mdegr, st, lrhovt, lke, lst1, lst2, lu);
   }
-  // ---- volume integral (5x5 Gauss-Lobatto, cofactor form)
+  // ---- volume integral (5x5 Gauss-Lobatto, cofactor form), row by row: the
+  // DOFs along a row are a_q + ds (b_q + c_q ds), and the transposed sums over
+  // a row collapse to per-row moments (sum l, sum l ds, sum l ds^2 for the
+  // DOF adjoints; sum l L_b(s), sum l L_b'(s) for the node adjoints)
+#pragma unroll 1
   for (int i = 0; i < 5; i++) {
     const double r = l5p(i), dr = r - G.rc;
     double lr[3], dlr[3];
     lag3(r, lr);
     dlag3(r, dlr);
     double Qx[3], Qy[3], Px[3], Py[3];
+#pragma unroll
     for (int bb = 0; bb < 3; bb++) {
       Qx[bb] = dlr[0] * L.X[0][bb] + dlr[1] * L.X[1][bb] + dlr[2] * L.X[2][bb];
       Qy[bb] = dlr[0] * L.Y[0][bb] + dlr[1] * L.Y[1][bb] + dlr[2] * L.Y[2][bb];
       Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
       Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
     }
+    double ra[4], rb[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      ra[q] = u[q][0] + u[q][1] * dr + u[q][3] * (0.5 * dr * dr - G.g19) - u[q][4] * G.g20 - u[q][5] * G.g21;
+      rb[q] = u[q][2] + u[q][5] * dr;
+    }
+    double m0[4] = {0, 0, 0, 0}, m1[4] = {0, 0, 0, 0}, m2[4] = {0, 0, 0, 0};
+    double Mxr[3] = {0, 0, 0}, Mxs[3] = {0, 0, 0}, Myr[3] = {0, 0, 0}, Mys[3] = {0, 0, 0};
+    const double wi = l5w(i);
+#pragma unroll 1
     for (int j = 0; j < 5; j++) {
       const double s = l5p(j), ds = s - G.sc;
       double ls[3], dls[3];
       lag3(s, ls);
       dlag3(s, dls);
-      const double w = l5w(i) * l5w(j);
+      const double w = wi * l5w(j);
       const double xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
       const double yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
       const double xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
       const double ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
-      double bb[6];
-      bb[0] = 1.0; bb[1] = dr; bb[2] = ds;
-      bb[3] = 0.5 * dr * dr - G.g19; bb[4] = 0.5 * ds * ds - G.g20; bb[5] = dr * ds - G.g21;
       double un[4];
-      for (int q = 0; q < 4; q++) {
-        un[q] = 0.0;
-        for (int k = 0; k < 6; k++) un[q] += u[q][k] * bb[k];
-      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * u[q][4] * ds);
       const double rhoad = 1.0 / un[0];
       const double kin = un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]);
       const double pe = (g - 1.0) * rhoad * kin;
@@ -1296,6 +1321,7 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
       gd1[4] = -xs * ds + xr * dr;
       const double wp = w * pres;
       double lgd0[5], lgd1[5], lwp = 0.0, lun1 = 0.0, lun2 = 0.0;
+#pragma unroll
       for (int kk = 0; kk < 5; kk++) {
         const double fv = gd0[kk] * un[1] + gd1[kk] * un[2];
         const double lfv = -lR[0][kk + 1] * w + lR[3][kk + 1] * wp;
@@ -1315,20 +1341,44 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
         lun0 += -lrhoad * rhoad * rhoad;
       }
       const double lunq[4] = {lun0, lun1, lun2, lun3};
-      for (int q = 0; q < 4; q++)
-        for (int k = 0; k < 6; k++) lu[q][k] += lunq[q] * bb[k];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        m0[q] += lunq[q];
+        m1[q] += lunq[q] * ds;
+        m2[q] += lunq[q] * ds * ds;
+      }
       const double lys = lgd0[0] + lgd0[2] * dr + lgd0[4] * ds;
       const double lyr = -lgd0[1] - lgd0[3] * ds - lgd0[4] * dr;
       const double lxs = -lgd1[0] - lgd1[2] * dr - lgd1[4] * ds;
       const double lxr = lgd1[1] + lgd1[3] * ds + lgd1[4] * dr;
-      for (int aa = 0; aa < 3; aa++)
-        for (int b2 = 0; b2 < 3; b2++) {
-          lX[aa][b2] += lxr * dlr[aa] * ls[b2] + lxs * lr[aa] * dls[b2];
-          lY[aa][b2] += lyr * dlr[aa] * ls[b2] + lys * lr[aa] * dls[b2];
-        }
+#pragma unroll
+      for (int b2 = 0; b2 < 3; b2++) {
+        Mxr[b2] += lxr * ls[b2];
+        Mxs[b2] += lxs * dls[b2];
+        Myr[b2] += lyr * ls[b2];
+        Mys[b2] += lys * dls[b2];
+      }
     }
+    // basis (1, dr, ds, dr^2/2 - g19, ds^2/2 - g20, dr ds - g21) along the row
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      lu[q][0] += m0[q];
+      lu[q][1] += dr * m0[q];
+      lu[q][2] += m1[q];
+      lu[q][3] += (0.5 * dr * dr - G.g19) * m0[q];
+      lu[q][4] += 0.5 * m2[q] - G.g20 * m0[q];
+      lu[q][5] += dr * m1[q] - G.g21 * m0[q];
+    }
+#pragma unroll
+    for (int aa = 0; aa < 3; aa++)
+#pragma unroll
+      for (int b2 = 0; b2 < 3; b2++) {
+        lX[aa][b2] += dlr[aa] * Mxr[b2] + lr[aa] * Mxs[b2];
+        lY[aa][b2] += dlr[aa] * Myr[b2] + lr[aa] * Mys[b2];
+      }
   }
-  // ---- Taylor-Green source
+  // ---- Taylor-Green source: cos and sin of pi x at the Gauss points by angle
+  // addition from the centre node, as in the forward pass
   double lxp[9][2];
   for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
   if (d.ncase == 1) {
@@ -1336,52 +1386,84 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     node_xy(L, xp);
     cross36(xp, c);
     detpoly(c, D);
-    const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
     const double PI = 3.14159265358979311599796346854;
+    const double coef = 0.25 * PI / (g - 1.0);
+    const double xc = L.X[1][1], yc = L.Y[1][1];
+    const double cxc = cospi(xc), sxc = sinpi(xc), cyc = cospi(yc), syc = sinpi(yc);
     double lD[16];
     for (int t = 0; t < 16; t++) lD[t] = 0.0;
+#pragma unroll 1
     for (int i = 0; i < 5; i++) {
       const double r = g5p(i), dr = r - G.rc;
       double lr[3];
       lag3(r, lr);
+      double Px[3], Py[3];
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        Px[bb] = lr[0] * (L.X[0][bb] - xc) + lr[1] * (L.X[1][bb] - xc) + lr[2] * (L.X[2][bb] - xc);
+        Py[bb] = lr[0] * (L.Y[0][bb] - yc) + lr[1] * (L.Y[1][bb] - yc) + lr[2] * (L.Y[2][bb] - yc);
+      }
+      double ee[4];
+#pragma unroll
+      for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+      // lsrc = sum_k lR[3][k] b_k(s) = sa + ds (sb + sc ds) along the row
+      const double sa = lR[3][0] + lR[3][1] * dr + lR[3][3] * (0.5 * dr * dr - G.g19) - lR[3][4] * G.g20 - lR[3][5] * G.g21;
+      const double sb = lR[3][2] + lR[3][5] * dr, sc = 0.5 * lR[3][4];
+      double Mx[3] = {0, 0, 0}, My[3] = {0, 0, 0}, Ls[4] = {0, 0, 0, 0};
+      const double wi = g5w(i);
+#pragma unroll 1
       for (int j = 0; j < 5; j++) {
         const double s = g5p(j), ds = s - G.sc;
         double ls[3];
         lag3(s, ls);
-        double xg = 0.0, yg = 0.0;
-        for (int aa = 0; aa < 3; aa++)
-          for (int b2 = 0; b2 < 3; b2++) {
-            xg += lr[aa] * ls[b2] * L.X[aa][b2];
-            yg += lr[aa] * ls[b2] * L.Y[aa][b2];
-          }
-        const double wij = g5w(i) * g5w(j);
-        const double djaco = wij * deteval(D, r, s);
-        const double cx = cospi(xg), cy = cospi(yg), sx = sinpi(xg), sy = sinpi(yg);
+        const double dx = Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2];
+        const double dy = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
+        const double wij = wi * g5w(j);
+        const double djaco = wij * (ee[0] + s * (ee[1] + s * (ee[2] + s * ee[3])));
+        double cx, sx, cy, sy;
+        if (fabs(dx) <= 0.15 && fabs(dy) <= 0.15) {
+          double cdx, sdx, cdy, sdy;
+          cossin_pi_small(dx, cdx, sdx);
+          cossin_pi_small(dy, cdy, sdy);
+          cx = cxc * cdx - sxc * sdx;
+          sx = sxc * cdx + cxc * sdx;
+          cy = cyc * cdy - syc * sdy;
+          sy = syc * cdy + cyc * sdy;
+        } else {
+          sincospi(xc + dx, &sx, &cx);
+          sincospi(yc + dy, &sy, &cy);
+        }
         const double c3x = cx * (4.0 * cx * cx - 3.0), c3y = cy * (4.0 * cy * cy - 3.0);
-        double bb[6];
-        bb[0] = 1.0; bb[1] = dr; bb[2] = ds;
-        bb[3] = 0.5 * dr * dr - G.g19; bb[4] = 0.5 * ds * ds - G.g20; bb[5] = dr * ds - G.g21;
-        double lsrc = 0.0;
-        for (int k = 0; k < 6; k++) lsrc += lR[3][k] * bb[k];
+        const double lsrc = sa + ds * (sb + sc * ds);
         const double ldj = lsrc * coef * (c3x * cy - c3y * cx);
         const double lc3x = lsrc * coef * djaco * cy, lc3y = -lsrc * coef * djaco * cx;
         const double lcx = -lsrc * coef * djaco * c3y + lc3x * (12.0 * cx * cx - 3.0);
         const double lcy = lsrc * coef * djaco * c3x + lc3y * (12.0 * cy * cy - 3.0);
         const double lxg = -lcx * PI * sx, lyg = -lcy * PI * sy;
-        for (int aa = 0; aa < 3; aa++)
-          for (int b2 = 0; b2 < 3; b2++) {
-            lX[aa][b2] += lxg * lr[aa] * ls[b2];
-            lY[aa][b2] += lyg * lr[aa] * ls[b2];
-          }
-        double rp = 1.0;
-        for (int mm = 0; mm < 4; mm++) {
-          double sp = 1.0;
-          for (int n = 0; n < 4; n++) {
-            lD[4 * mm + n] += ldj * wij * rp * sp;
-            sp *= s;
-          }
-          rp *= r;
+#pragma unroll
+        for (int b2 = 0; b2 < 3; b2++) {
+          Mx[b2] += lxg * ls[b2];
+          My[b2] += lyg * ls[b2];
         }
+        const double lw = ldj * wij;
+        Ls[0] += lw;
+        Ls[1] += lw * s;
+        Ls[2] += lw * s * s;
+        Ls[3] += lw * s * s * s;
+      }
+#pragma unroll
+      for (int aa = 0; aa < 3; aa++)
+#pragma unroll
+        for (int b2 = 0; b2 < 3; b2++) {
+          lX[aa][b2] += lr[aa] * Mx[b2];
+          lY[aa][b2] += lr[aa] * My[b2];
+        }
+      double rp = 1.0;
+#pragma unroll
+      for (int mm = 0; mm < 4; mm++) {
+#pragma unroll
+        for (int n = 0; n < 4; n++) lD[4 * mm + n] += rp * Ls[n];
+        rp *= r;
       }
     }
     double lc36[36];
@@ -1570,16 +1652,14 @@ static inline int nb(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace fast
 
-// Reverse of one RK stage of the optimised FP64 step (all-quad meshes).  The
-// stage inputs (U^(s), x^(s), u*_prev) must be in d.Us, d.xs/ys, d.us/vs; the
-// forward corner and node passes are recomputed first (node sums, sub-cell
-// corrections and u*_new), then the transposes run in reverse order.  dtp is
-// the device address of the step's time step size.
+// Reverse of one RK stage of the optimised FP64 step (all-quad meshes).  d
+// views the stage's inputs (U^(s) in d.Us, x^(s) in d.xs/ys, u*_prev in
+// d.us/vs) and the forward corner and node outputs of that stage (d.npart,
+// d.corr, d.us_new/vs_new); the transposes run in reverse order.  dtp is the
+// device address of the step's time step size.
 void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp) {
   const fast::Adj &a = *static_cast<const fast::Adj *>(adj);
   const int bq = fast::nb(d.nquad, 128), bp = fast::nb(d.npoin, 256), bc = fast::nb(d.ncell, 256);
-  fast::k_corner2<<<bq, 128, 0, st>>>(d);
-  fast::k_node2<<<bp, 256, 0, st>>>(d);
   fast::k_a_centre<<<bp, 256, 0, st>>>(d, a);
   fast::k_a_copy_centre<<<bp, 256, 0, st>>>(d, a);
   fast::k_a_nodes<<<bp, 256, 0, st>>>(d, a, alfa, dtp);
@@ -1593,7 +1673,7 @@ void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double
 void launch_adjoint_fold(const Dev &d, const void *adj, cudaStream_t st) {
   fast::k_a_fold<<<1184, 256, 0, st>>>(d, *static_cast<const fast::Adj *>(adj));
 }
-int adjoint_stage_launches() { return 11; }
+int adjoint_stage_launches() { return 9; }
 size_t adjoint_struct_size() { return sizeof(fast::Adj); }
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
