@@ -907,13 +907,29 @@ __host__ __device__ __forceinline__ void slot_an_T(int slot, double lax, double 
     case 2: lyr -= lax; lxr += lay; break;   // ax = -yr, ay = xr
     default: lys -= lax; lxs += lay; break;  // ax = -ys, ay = xs
   }
-  // xr = sum_t da[t] X[t][ib], xs = sum_t db[t] X[ia][t]
-  for (int t = 0; t < 3; t++) {
-    lX[t][ib] += da[t] * lxr;
-    lY[t][ib] += da[t] * lyr;
-    lX[ia][t] += db[t] * lxs;
-    lY[ia][t] += db[t] * lys;
-  }
+  // xr = sum_t da[t] X[t][ib], xs = sum_t db[t] X[ia][t]; column ib and row
+  // ia are selected with (warp-uniform) branches so that lX, lY stay in
+  // registers
+  const double cx0 = da[0] * lxr, cx1 = da[1] * lxr, cx2 = da[2] * lxr;
+  const double cy0 = da[0] * lyr, cy1 = da[1] * lyr, cy2 = da[2] * lyr;
+  if (ib == 0) { lX[0][0] += cx0; lX[1][0] += cx1; lX[2][0] += cx2; lY[0][0] += cy0; lY[1][0] += cy1; lY[2][0] += cy2; }
+  else if (ib == 1) { lX[0][1] += cx0; lX[1][1] += cx1; lX[2][1] += cx2; lY[0][1] += cy0; lY[1][1] += cy1; lY[2][1] += cy2; }
+  else { lX[0][2] += cx0; lX[1][2] += cx1; lX[2][2] += cx2; lY[0][2] += cy0; lY[1][2] += cy1; lY[2][2] += cy2; }
+  const double rx0 = db[0] * lxs, rx1 = db[1] * lxs, rx2 = db[2] * lxs;
+  const double ry0 = db[0] * lys, ry1 = db[1] * lys, ry2 = db[2] * lys;
+  if (ia == 0) { lX[0][0] += rx0; lX[0][1] += rx1; lX[0][2] += rx2; lY[0][0] += ry0; lY[0][1] += ry1; lY[0][2] += ry2; }
+  else if (ia == 1) { lX[1][0] += rx0; lX[1][1] += rx1; lX[1][2] += rx2; lY[1][0] += ry0; lY[1][1] += ry1; lY[1][2] += ry2; }
+  else { lX[2][0] += rx0; lX[2][1] += rx1; lX[2][2] += rx2; lY[2][0] += ry0; lY[2][1] += ry1; lY[2][2] += ry2; }
+}
+// entry isg of a 4-vector with a warp-uniform index, without local memory
+__host__ __device__ __forceinline__ double pick4(const double v[4], int i) {
+  return i == 0 ? v[0] : i == 1 ? v[1] : i == 2 ? v[2] : v[3];
+}
+__host__ __device__ __forceinline__ void add4(double v[4], int i, double x) {
+  if (i == 0) v[0] += x;
+  else if (i == 1) v[1] += x;
+  else if (i == 2) v[2] += x;
+  else v[3] += x;
 }
 
 __host__ __device__ __forceinline__ void corner_an_T(int isg, int ivsg, int f, double lax, double lay, double lX[3][3],
@@ -1056,7 +1072,7 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
     double lst1 = 0, lst2 = 0, lrhovt = 0, lke = 0, ldux = 0, lduy = 0;
     for (int i = nc_start(k); i < nc_start(k + 1); i++) {
       const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
-      const double ci = corr[isg];
+      const double ci = pick4(corr, isg);
       const double pe = (g - 1.0) * (rhovt + ci) * ke;
       const double pv = fmax(eps, pe);
       double lpv = 0.0;
@@ -1077,7 +1093,7 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
       }
       if (pe > eps) {
         lrhovt += lpv * (g - 1.0) * ke;
-        lcr[isg] += lpv * (g - 1.0) * ke;
+        add4(lcr, isg, lpv * (g - 1.0) * ke);
         lke += lpv * (g - 1.0) * (rhovt + ci);
       }
     }
@@ -1253,7 +1269,7 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
       }
       if (pe > eps) {
         lrhovt += lpv * (g - 1.0) * ke;
-        lcr[isg] += lpv * (g - 1.0) * ke;
+        add4(lcr, isg, lpv * (g - 1.0) * ke);
         lke += lpv * (g - 1.0) * (rhovt + ci);
       }
     }
