@@ -53,8 +53,7 @@ void launch_tri_init(const Dev &d, cudaStream_t st);
 void launch_tri_geom(const Dev &d, cudaStream_t st, const double *X, const double *Y);
 void launch_tri_corner(const Dev &d, cudaStream_t st);
 void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa);
-void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp);
-void launch_adjoint_fold(const Dev &d, const void *adj, cudaStream_t st);
+void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold);
 int adjoint_stage_launches();
 }  // namespace lag2d
 
@@ -912,12 +911,10 @@ struct AdjWork {
     for (int k = nk - 1; k >= 0; k--) {
       for (int istag = nstag; istag >= 1; istag--) {
         const Dev ds = rec.inputs(h->d, (size_t)k * nstag + (istag - 1));
-        launch_adjoint_stage(ds, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k);
+        // stage 1 reads U^n and x^n directly: its reverse folds their adjoints in
+        launch_adjoint_stage(ds, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k, istag == 1);
         h->launches += adjoint_stage_launches();
       }
-      // stage 1 read U^n and x^n directly: fold their adjoints in
-      launch_adjoint_fold(h->d, &a, h->st);
-      h->launches += 1;
     }
   }
 };

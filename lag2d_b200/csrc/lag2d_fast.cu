@@ -945,14 +945,15 @@ __host__ __device__ __forceinline__ void corner_m_T(double rhoct, double sdctr, 
                                                     double duy, double ax, double ay, double w, double lm,
                                                     double &lrho, double &lsd, double &ldux, double &lduy,
                                                     double &lax, double &lay) {
-  const double nn = sqrt(ax * ax + ay * ay);
+  const double nn2 = ax * ax + ay * ay;
+  const double rnn = rsqrt(nn2), nn = nn2 * rnn;
   const double dn = dux * ax + duy * ay;
   const double adn = fabs(dn), sg = dn >= 0.0 ? 1.0 : -1.0;
   lrho += lm * 2.0 * w * (sdctr * nn + cimpd * slpdu * adn);
   lsd += lm * 2.0 * w * rhoct * nn;
-  const double lnn = lm * 2.0 * w * rhoct * sdctr;
-  lax += lnn * ax / nn;
-  lay += lnn * ay / nn;
+  const double lnn = lm * 2.0 * w * rhoct * sdctr * rnn;
+  lax += lnn * ax;
+  lay += lnn * ay;
   const double ldn = lm * 2.0 * w * cimpd * rhoct * slpdu * sg;
   ldux += ldn * ax;
   lduy += ldn * ay;
@@ -1020,32 +1021,17 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   const double rhoct = 1.0 / u[0][0];
   const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
   const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  // the stage's sub-cell density corrections come from the forward pass;
+  // corr = cdrho (msub / vsub - masel / volel) gives the sub-cell masses
+  // masel back from the closed-form volumes volel
   double vsub4[4], corr[4], masel4[4], volel4[4];
   subareas(c, vsub4);
+#pragma unroll
   for (int isg = 0; isg < 4; isg++) {
-    const double unksgq = (1.0 / vsub4[isg]) * d.msub[isg * nq + iq];
-    const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
-    const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
-    double masel = 0.0;
-    for (int i = 0; i < 5; i++) {
-      const double r = (g5p(i) + ofr) / 2.0;
-      double ee[4];
-      for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
-      const double dr = r - G.rc;
-      const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
-      const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
-      const double wi = 0.25 * g5w(i);
-      for (int j = 0; j < 5; j++) {
-        const double s = (g5p(j) + ofs) / 2.0, ds = s - G.sc;
-        const double tau = t0 + ds * (t1 + t2 * ds);
-        const double det = ee[0] + s * (ee[1] + s * (ee[2] + s * ee[3]));
-        masel += (wi * g5w(j)) * det / tau;
-      }
-    }
-    const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
-    masel4[isg] = masel;
-    volel4[isg] = volel;
-    corr[isg] = d.cdrho * (unksgq - 1.0 / (volel / masel));
+    corr[isg] = d.corr[isg * nq + iq];
+    volel4[isg] = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
+    const double rho_sub = d.cdrho != 0.0 ? d.msub[isg * nq + iq] / vsub4[isg] - corr[isg] / d.cdrho : 0.0;
+    masel4[isg] = volel4[isg] * rho_sub;
   }
   double lu[4][6];
   for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
@@ -1147,8 +1133,9 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
         const double s = (g5p(j) + ofs) / 2.0, ds = s - G.sc;
         const double tau = t0 + ds * (t1 + t2 * ds);
         const double det = ee[0] + s * (ee[1] + s * (ee[2] + s * ee[3]));
-        const double ldet = lmasel * (wi * g5w(j)) / tau;
-        const double ltau = -ldet * det / tau;
+        const double itau = 1.0 / tau;
+        const double ldet = lmasel * (wi * g5w(j)) * itau;
+        const double ltau = -ldet * det * itau;
         m0 += ltau;
         m1 += ltau * ds;
         m2 += ltau * ds * ds;
@@ -1522,37 +1509,49 @@ __host__ __device__ void a_gather(const Dev &d, const Adj &a, int p, int nv) {
   }
 }
 
-// Reverse of the node solve: u* = (S1 - S3) / S0, v* = (S2 - S4) / S0 with the
-// wall masks; kept nodes take u*_prev.
-__host__ __device__ void a_nodesolve(const Dev &d, const Adj &a, int p) {
+// Gather of the RHS pass's per-(quad, node) contributions (x, y, u*_prev,
+// u*_new) fused with the reverse of the node solve u* = (S1 - S3) / S0,
+// v* = (S2 - S4) / S0 (wall masks; kept nodes take u*_prev).  Only S0 is
+// gathered again: u* itself is the forward pass's d.us_new / d.vs_new.
+__host__ __device__ void a_gather_solve(const Dev &d, const Adj &a, int p) {
   if (p >= d.npoin) return;
-  const unsigned char mask = d.bcmask[p];
-  const double lu = (mask & 1) ? 0.0 : a.luw[p];
-  const double lv = (mask & 2) ? 0.0 : a.lvw[p];
-  const size_t np = d.npoin;
-  for (int v = 0; v < 5; v++) a.lS[v * np + p] = 0.0;
-  if (mask & 4) {
-    a.lus[p] += lu;
-    a.lvs[p] += lv;
-    return;
-  }
-  double S[5] = {0, 0, 0, 0, 0};
+  double s[6] = {0, 0, 0, 0, 0, 0}, S0 = 0.0;
   for (int i = d.node_ptr2[p]; i < d.node_ptr2[p + 1]; i++) {
     const int id = d.node_slot[i];
     if (id < 0) continue;
     const int iq = id / 9, k = id - 9 * iq;
-    for (int v = 0; v < 5; v++) S[v] += d.npart[(v * 9 + k) * (size_t)d.nquad + iq];
+#pragma unroll
+    for (int v = 0; v < 6; v++) s[v] += a.pbuf[(v * 9 + k) * (size_t)d.nquad + iq];
+    S0 += d.npart[k * (size_t)d.nquad + iq];
   }
-  const double us = (S[1] - S[3]) / S[0], vs = (S[2] - S[4]) / S[0];
-  a.lS[0 * np + p] = -(lu * us + lv * vs) / S[0];
-  a.lS[1 * np + p] = lu / S[0];
-  a.lS[3 * np + p] = -lu / S[0];
-  a.lS[2 * np + p] = lv / S[0];
-  a.lS[4 * np + p] = -lv / S[0];
+  a.lx[p] += s[0];
+  a.ly[p] += s[1];
+  double lus = a.lus[p] + s[2], lvs = a.lvs[p] + s[3];
+  const double luw = a.luw[p] + s[4], lvw = a.lvw[p] + s[5];
+  const unsigned char mask = d.bcmask[p];
+  const double lu = (mask & 1) ? 0.0 : luw;
+  const double lv = (mask & 2) ? 0.0 : lvw;
+  const size_t np = d.npoin;
+  if (mask & 4) {
+    a.lus[p] = lus + lu;
+    a.lvs[p] = lvs + lv;
+#pragma unroll
+    for (int v = 0; v < 5; v++) a.lS[v * np + p] = 0.0;
+    return;
+  }
+  a.lus[p] = lus;
+  a.lvs[p] = lvs;
+  const double iS0 = 1.0 / S0;
+  a.lS[0 * np + p] = -(lu * d.us_new[p] + lv * d.vs_new[p]) * iS0;
+  a.lS[1 * np + p] = lu * iS0;
+  a.lS[3 * np + p] = -lu * iS0;
+  a.lS[2 * np + p] = lv * iS0;
+  a.lS[4 * np + p] = -lv * iS0;
 }
 
-// Reverse of the RK update U = alfa U^n + (1 - alfa)(U^(s) + dt M^-1 R)
-__host__ __device__ void a_update(const Dev &d, const Adj &a, int e, double alfa, double dt) {
+// fold (stage 1, the last one reversed): U^(1) is U^n itself, so the adjoint
+// of U^n gathered from the later stages joins the adjoint of U^(1).
+__host__ __device__ void a_update(const Dev &d, const Adj &a, int e, double alfa, double dt, int fold) {
   if (e >= d.ncell) return;
   const size_t nc = d.ncell;
   double am[16];
@@ -1563,8 +1562,14 @@ __host__ __device__ void a_update(const Dev &d, const Adj &a, int e, double alfa
     double l[6];
     for (int k = 0; k < 6; k++) l[k] = a.lU[(q * 6 + k) * nc + e];
     for (int k = 0; k < 6; k++) {
-      a.lUn[(q * 6 + k) * nc + e] += alfa * l[k];
-      a.lU[(q * 6 + k) * nc + e] = oma * l[k];
+      const double ln = a.lUn[(q * 6 + k) * nc + e] + alfa * l[k];
+      if (fold) {
+        a.lU[(q * 6 + k) * nc + e] = oma * l[k] + ln;
+        a.lUn[(q * 6 + k) * nc + e] = 0.0;
+      } else {
+        a.lU[(q * 6 + k) * nc + e] = oma * l[k];
+        a.lUn[(q * 6 + k) * nc + e] = ln;
+      }
     }
     a.lR[(q * 6) * nc + e] = oma * dt * am[15] * l[0];
     for (int i = 0; i < 5; i++) {
@@ -1576,16 +1581,27 @@ __host__ __device__ void a_update(const Dev &d, const Adj &a, int e, double alfa
 }
 
 // Reverse of the node motion x = alfa x^n + (1 - alfa)(x + dt u*_new), with
-// u*_new becoming the next stage's u*_prev
-__host__ __device__ void a_nodes(const Dev &d, const Adj &a, int p, double alfa, double dt) {
+// u*_new becoming the next stage's u*_prev.  The adjoint of the stage's
+// output coordinates is (tx, ty), after the centre-node transpose; fold as in
+// a_update.
+__host__ __device__ void a_nodes(const Dev &d, const Adj &a, int p, double alfa, double dt, int fold) {
   if (p >= d.npoin) return;
   const double oma = 1.0 - alfa;
-  a.lxn[p] += alfa * a.lx[p];
-  a.lyn[p] += alfa * a.ly[p];
-  a.luw[p] = oma * dt * a.lx[p] + a.lus[p];
-  a.lvw[p] = oma * dt * a.ly[p] + a.lvs[p];
-  a.lx[p] = oma * a.lx[p];
-  a.ly[p] = oma * a.ly[p];
+  const double lxo = a.tx[p], lyo = a.ty[p];
+  const double lxn = a.lxn[p] + alfa * lxo, lyn = a.lyn[p] + alfa * lyo;
+  a.luw[p] = oma * dt * lxo + a.lus[p];
+  a.lvw[p] = oma * dt * lyo + a.lvs[p];
+  if (fold) {
+    a.lx[p] = oma * lxo + lxn;
+    a.ly[p] = oma * lyo + lyn;
+    a.lxn[p] = 0.0;
+    a.lyn[p] = 0.0;
+  } else {
+    a.lx[p] = oma * lxo;
+    a.ly[p] = oma * lyo;
+    a.lxn[p] = lxn;
+    a.lyn[p] = lyn;
+  }
   a.lus[p] = 0.0;
   a.lvs[p] = 0.0;
 }
@@ -1615,11 +1631,6 @@ __host__ __device__ void a_centre(const Dev &d, const Adj &a, int p) {
   a.tx[p] = sx;
   a.ty[p] = sy;
 }
-__host__ __device__ void a_copy_centre(const Dev &d, const Adj &a, int p) {
-  if (p >= d.npoin) return;
-  a.lx[p] = a.tx[p];
-  a.ly[p] = a.ty[p];
-}
 
 __global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
 #ifndef LAG2D_CORNER_MIN_BLOCKS
@@ -1638,31 +1649,14 @@ __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + th
 __global__ void __launch_bounds__(128) k_a_corner(Dev d, Adj a) { a_corner(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void __launch_bounds__(128) k_a_rhs(Dev d, Adj a) { a_rhs(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_gather(Dev d, Adj a, int nv) { a_gather(d, a, blockIdx.x * blockDim.x + threadIdx.x, nv); }
-__global__ void k_a_nodesolve(Dev d, Adj a) { a_nodesolve(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void k_a_update(Dev d, Adj a, double alfa, const double *dtp) {
-  a_update(d, a, blockIdx.x * blockDim.x + threadIdx.x, alfa, *dtp);
+__global__ void k_a_gather_solve(Dev d, Adj a) { a_gather_solve(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void k_a_update(Dev d, Adj a, double alfa, const double *dtp, int fold) {
+  a_update(d, a, blockIdx.x * blockDim.x + threadIdx.x, alfa, *dtp, fold);
 }
-__global__ void k_a_nodes(Dev d, Adj a, double alfa, const double *dtp) {
-  a_nodes(d, a, blockIdx.x * blockDim.x + threadIdx.x, alfa, *dtp);
+__global__ void k_a_nodes(Dev d, Adj a, double alfa, const double *dtp, int fold) {
+  a_nodes(d, a, blockIdx.x * blockDim.x + threadIdx.x, alfa, *dtp, fold);
 }
 __global__ void k_a_centre(Dev d, Adj a) { a_centre(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void k_a_copy_centre(Dev d, Adj a) { a_copy_centre(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
-// end of a step's reverse: the stage-1 inputs are U^n and x^n themselves, and
-// the previous step's copy-back makes them its final stage state
-__global__ void k_a_fold(Dev d, Adj a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  const size_t nu = (size_t)NU * d.ncell;
-  for (size_t t = i; t < nu; t += stride) {
-    a.lU[t] += a.lUn[t];
-    a.lUn[t] = 0.0;
-  }
-  for (int p = i; p < d.npoin; p += stride) {
-    a.lx[p] += a.lxn[p];
-    a.ly[p] += a.lyn[p];
-    a.lxn[p] = 0.0;
-    a.lyn[p] = 0.0;
-  }
-}
 
 static inline int nb(int n, int b) { return (n + b - 1) / b; }
 
@@ -1672,24 +1666,20 @@ static inline int nb(int n, int b) { return (n + b - 1) / b; }
 // views the stage's inputs (U^(s) in d.Us, x^(s) in d.xs/ys, u*_prev in
 // d.us/vs) and the forward corner and node outputs of that stage (d.npart,
 // d.corr, d.us_new/vs_new); the transposes run in reverse order.  dtp is the
-// device address of the step's time step size.
-void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp) {
+// device address of the step's time step size; fold = 1 for stage 1, which
+// ends the step's reverse (U^(1) and x^(1) are U^n and x^n).
+void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold) {
   const fast::Adj &a = *static_cast<const fast::Adj *>(adj);
   const int bq = fast::nb(d.nquad, 128), bp = fast::nb(d.npoin, 256), bc = fast::nb(d.ncell, 256);
   fast::k_a_centre<<<bp, 256, 0, st>>>(d, a);
-  fast::k_a_copy_centre<<<bp, 256, 0, st>>>(d, a);
-  fast::k_a_nodes<<<bp, 256, 0, st>>>(d, a, alfa, dtp);
-  fast::k_a_update<<<bc, 256, 0, st>>>(d, a, alfa, dtp);
+  fast::k_a_nodes<<<bp, 256, 0, st>>>(d, a, alfa, dtp, fold);
+  fast::k_a_update<<<bc, 256, 0, st>>>(d, a, alfa, dtp, fold);
   fast::k_a_rhs<<<bq, 128, 0, st>>>(d, a);
-  fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 6);
-  fast::k_a_nodesolve<<<bp, 256, 0, st>>>(d, a);
+  fast::k_a_gather_solve<<<bp, 256, 0, st>>>(d, a);
   fast::k_a_corner<<<bq, 128, 0, st>>>(d, a);
   fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
 }
-void launch_adjoint_fold(const Dev &d, const void *adj, cudaStream_t st) {
-  fast::k_a_fold<<<1184, 256, 0, st>>>(d, *static_cast<const fast::Adj *>(adj));
-}
-int adjoint_stage_launches() { return 9; }
+int adjoint_stage_launches() { return 7; }
 size_t adjoint_struct_size() { return sizeof(fast::Adj); }
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
