@@ -13,9 +13,9 @@ from typing import Tuple
 
 import numpy as np
 
-from .mesh import Mesh, hybrid_mesh, quad_mesh
+from .mesh import Mesh, hybrid_mesh, polar_mesh, quad_mesh
 
-__all__ = ["StepConfig", "workload", "WORKLOADS"]
+__all__ = ["StepConfig", "workload", "WORKLOADS", "noh_parity_config"]
 
 
 @dataclasses.dataclass
@@ -85,6 +85,26 @@ def _sedov_hybrid(n: int, jitter: float = 0.0) -> Tuple[Mesh, StepConfig]:
     return m, c
 
 
+def _noh(n: int) -> Tuple[Mesh, StepConfig]:
+    """Cartesian Noh implosion (ncase 3: rho = 1, u = -r/|r|, p = 1e-6,
+    gamma 5/3) on the quarter disk of polar_mesh: ``n`` rings of curved P2
+    cells by ``n`` sectors, 6-node triangles on the axis ring, slip walls on
+    the two rays, a free outer arc."""
+    m = polar_mesh(n, n, 1.0)
+    c = StepConfig(ncase=3, gamlg=5.0 / 3.0, nstag=3, cfl=0.1, tend=0.6)
+    return m, c
+
+
+def noh_parity_config(c: StepConfig) -> StepConfig:
+    """The Noh workload with a fixed time step of 1e-4 (ndt 0).  On this
+    branch the triangles at the origin are never limited (Persson and WENO
+    are quad-only) and getdelt_lag bounds dt by the sound speed and volume
+    change only; from the CPU restatement, the implosion breaks down within
+    a few steps at the CFL time step and by t ~ 0.02-0.06 even at fixed small
+    steps, so parity runs cover the first 10 steps."""
+    return dataclasses.replace(c, ndt=0, dtfix=1.0e-4)
+
+
 WORKLOADS = {
     # Taylor-Green vortex: [0,1]^2, gamma 5/3, P2, RK3, energy source on
     "tgv1024": lambda: _tgv(1024),
@@ -102,6 +122,10 @@ WORKLOADS = {
     "tgv_hybrid64": lambda: _tgv_hybrid(64),
     "sedov_hybrid16": lambda: _sedov_hybrid(16),
     "sedov_hybrid_jitter16": lambda: _sedov_hybrid(16, jitter=0.1),
+    # Noh implosion on the quarter disk (triangles on the axis ring)
+    "noh100": lambda: _noh(100),
+    "noh16": lambda: _noh(16),
+    "noh8": lambda: _noh(8),
 }
 
 

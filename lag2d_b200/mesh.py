@@ -27,7 +27,7 @@ from typing import Optional
 
 import numpy as np
 
-__all__ = ["Mesh", "Ctrl", "quad_mesh", "hybrid_mesh", "read_domn", "write_domn", "read_ctrl", "write_ctrl",
+__all__ = ["Mesh", "Ctrl", "quad_mesh", "hybrid_mesh", "polar_mesh", "read_domn", "write_domn", "read_ctrl", "write_ctrl",
            "build_esuv", "build_esqua"]
 
 
@@ -356,3 +356,60 @@ def hybrid_mesh(nx: int, ny: int, x0: float = 0.0, x1: float = 1.0, y0: float = 
     # the unsplit quads keep the centre-node rule of the step (quad_mesh placed it so)
     return Mesh(coord=coord, ipqua=np.array(quads, dtype=np.int32).reshape(-1, 9),
                 iptri=np.array(tris, dtype=np.int32).reshape(-1, 6), bface=q.bface)
+
+
+def polar_mesh(nr: int, nt: int, radius: float = 1.0, wall_code: int = 22) -> Mesh:
+    """Quarter disk ``0 <= theta <= pi/2``, ``r <= radius`` of ``nr`` rings by
+    ``nt`` sectors with curved (P2) cells: the innermost ring is 6-node
+    triangles meeting at the origin, the others 9-node quads.  Nodes lie on
+    the exact circles and rays (edge mid-nodes at mid-radius or mid-angle);
+    the quad centre node is placed by the step's re-interpolation rule.
+    Boundary faces: the ray theta = 0 is a slip wall with v fixed
+    (``bface(3) = wall_code``, sub-code 221), the ray theta = pi/2 one with u
+    fixed (sub-code 222), the outer arc is free (sub-code 0).  Triangles are
+    numbered first, cells ring by ring.
+    """
+    dr, dt = radius / nr, 0.5 * np.pi / nt
+    ids = {}
+    xy = []
+
+    def node(a, b):
+        """Node at half-step lattice point (radius a dr/2, angle b dt/2); a = 0 is the origin."""
+        key = (0, 0) if a == 0 else (a, b)
+        if key not in ids:
+            ids[key] = len(xy) + 1
+            r, t = 0.5 * a * dr, 0.5 * b * dt
+            xy.append((r * np.cos(t), r * np.sin(t)))
+        return ids[key]
+
+    tris, quads = [], []
+    for j in range(nt):
+        b0, b1, b2 = 2 * j, 2 * j + 1, 2 * j + 2
+        tris.append((node(0, 0), node(2, b0), node(2, b2), node(1, b0), node(2, b1), node(1, b2)))
+    for i in range(1, nr):
+        a0, a1, a2 = 2 * i, 2 * i + 1, 2 * i + 2
+        for j in range(nt):
+            b0, b1, b2 = 2 * j, 2 * j + 1, 2 * j + 2
+            quads.append((node(a0, b0), node(a2, b0), node(a2, b2), node(a0, b2),
+                          node(a1, b0), node(a2, b1), node(a1, b2), node(a0, b1), node(a1, b1)))
+    coord = np.array(xy, dtype=np.float64)
+    ipqua = np.array(quads, dtype=np.int32).reshape(-1, 9)
+    c = ipqua - 1
+    for d in range(2):
+        v = coord[:, d]
+        v[c[:, 8]] = -0.25 * (v[c[:, 0]] + v[c[:, 1]] + v[c[:, 2]] + v[c[:, 3]]) + \
+            0.5 * (v[c[:, 4]] + v[c[:, 5]] + v[c[:, 6]] + v[c[:, 7]])
+    bf = []
+    # theta = 0: origin outwards (domain on the left)
+    bf.append((node(0, 0), node(2, 0), wall_code, 221, node(1, 0)))
+    for i in range(1, nr):
+        bf.append((node(2 * i, 0), node(2 * i + 2, 0), wall_code, 221, node(2 * i + 1, 0)))
+    # outer arc, counter-clockwise
+    for j in range(nt):
+        bf.append((node(2 * nr, 2 * j), node(2 * nr, 2 * j + 2), wall_code, 0, node(2 * nr, 2 * j + 1)))
+    # theta = pi/2: inwards to the origin
+    for i in range(nr - 1, 0, -1):
+        bf.append((node(2 * i + 2, 2 * nt), node(2 * i, 2 * nt), wall_code, 222, node(2 * i + 1, 2 * nt)))
+    bf.append((node(2, 2 * nt), node(0, 0), wall_code, 222, node(1, 2 * nt)))
+    return Mesh(coord=coord, ipqua=ipqua, iptri=np.array(tris, dtype=np.int32).reshape(-1, 6),
+                bface=np.array(bf, dtype=np.int32))

@@ -3,8 +3,9 @@
 The reference (Fortran) cannot be compiled in this environment and ships no
 golden outputs, so these fixtures pin the CPU oracle against regressions and
 give the GPU path fixed targets: small Taylor-Green and Sedov runs (8 x 8, a
-12 x 12 Sedov with troubled cells, a curved 6 x 6 quad mesh and a curved
-tri/quad mesh), 3 time steps each.
+12 x 12 Sedov with troubled cells, a curved 6 x 6 quad mesh, a curved
+tri/quad mesh and the Noh implosion on a 4 x 4 quarter-disk mesh with
+triangles at the origin), 3 time steps each.
 
     python tests/golden/make_golden.py            # all fixtures
     python tests/golden/make_golden.py tgv6_hybrid # one fixture
@@ -19,7 +20,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from lag2d_b200 import quad_mesh, StepConfig  # noqa: E402
-from lag2d_b200.mesh import hybrid_mesh  # noqa: E402
+from lag2d_b200.mesh import hybrid_mesh, polar_mesh  # noqa: E402
 from oracle.oracle import Oracle  # noqa: E402
 
 CASES = {
@@ -32,6 +33,9 @@ CASES = {
     # curved tri/quad mesh (alternate rows split into 6-node triangles)
     "tgv6_hybrid": (lambda: hybrid_mesh(6, 6, 0.0, 1.0, 0.0, 1.0, jitter=0.1, curve=0.05, seed=7),
                     StepConfig(ncase=1, gamlg=5.0 / 3.0, nstag=3, cfl=0.05, tend=10.0), 3),
+    # Noh on the curved quarter disk, fixed time step
+    "noh4_polar": (lambda: polar_mesh(4, 4),
+                   StepConfig(ncase=3, gamlg=5.0 / 3.0, nstag=3, ndt=0, dtfix=1.0e-4, tend=0.6), 3),
 }
 
 

@@ -8,16 +8,25 @@ for bit (Sedov; the Taylor-Green source differs by the device cos rounding,
 1e-12 relative after every step; single-stage RHS within 1e-8 of the field
 scale.  The Sedov run stops after 2 steps: triangles are never limited on
 this branch (Persson and WENO are quad-only), and the blast wave breaks the
-scheme on the triangles a few steps later in the oracle as well.
+scheme on the triangles a few steps later in the oracle as well.  The Noh
+implosion on the quarter disk (curved cells on exact arcs, 8 triangles meeting
+at the origin, a free outer boundary) runs with a fixed time step of 1e-4 for
+10 steps, for the same reason.
 """
 import numpy as np
 import pytest
 
-from lag2d_b200 import workload
+from lag2d_b200 import workload as _workload
 from lag2d_b200.api import Lag2DSolver
+from lag2d_b200.config import noh_parity_config
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
+
+
+def workload(name):
+    m, c = _workload(name)
+    return (m, noh_parity_config(c)) if name.startswith("noh") else (m, c)
 
 
 def _field_err(a, b):
@@ -28,9 +37,10 @@ def _field_err(a, b):
     return np.array(out)
 
 
+@pytest.mark.parametrize("name", ["tgv_hybrid16", "noh8"])
 @pytest.mark.parametrize("exact", [False, True])
-def test_hybrid_init_fields(exact):
-    m, c = workload("tgv_hybrid16")
+def test_hybrid_init_fields(name, exact):
+    m, c = workload(name)
     geoel, amatr, unkno = Oracle(m, c).init()
     s = Lag2DSolver(m, c, exact=exact)
     g2, a2, u2 = s.init_fields()
@@ -43,7 +53,7 @@ def test_hybrid_init_fields(exact):
     assert _field_err(u2[:n], unkno[:n]).max() < tol * 100
 
 
-@pytest.mark.parametrize("name", ["tgv_hybrid16", "sedov_hybrid16"])
+@pytest.mark.parametrize("name", ["tgv_hybrid16", "sedov_hybrid16", "noh8"])
 @pytest.mark.parametrize("exact", [False, True])
 def test_hybrid_rhs_single(name, exact):
     m, c = workload(name)
@@ -73,7 +83,8 @@ def test_hybrid_rhs_single(name, exact):
 
 
 @pytest.mark.parametrize("name,nsteps,ordex", [("tgv_hybrid16", 10, False), ("sedov_hybrid16", 2, False),
-                                               ("sedov_hybrid16", 2, True)])
+                                               ("sedov_hybrid16", 2, True), ("noh8", 10, False),
+                                               ("noh8", 10, True)])
 def test_hybrid_steps(name, nsteps, ordex):
     m, c = workload(name)
     o = Oracle(m, c)

@@ -11,7 +11,8 @@ import os
 import numpy as np
 import pytest
 
-from lag2d_b200.mesh import hybrid_mesh
+from lag2d_b200.config import noh_parity_config
+from lag2d_b200.mesh import hybrid_mesh, polar_mesh
 from lag2d_b200 import quad_mesh, StepConfig, workload
 from oracle.oracle import Oracle
 
@@ -63,9 +64,12 @@ def test_mass_matrix_inverse():
 
 # on the tri/quad mesh the Taylor-Green source integrates to zero over the box
 # only up to the error of the 7-point triangle rule (~1e-13 of the energy)
-@pytest.mark.parametrize("name,nsteps,tol", [("tgv16", 15, 1e-13), ("sedov16", 15, 1e-13), ("tgv_hybrid16", 10, 1e-12)])
+@pytest.mark.parametrize("name,nsteps,tol", [("tgv16", 15, 1e-13), ("sedov16", 15, 1e-13), ("tgv_hybrid16", 10, 1e-12),
+                                           ("noh8", 10, 1e-13)])
 def test_mass_and_energy_conservation(name, nsteps, tol):
     m, c = workload(name)
+    if name.startswith("noh"):
+        c = noh_parity_config(c)
     o, geoel, amatr, unkno, coord, ustar, dt, ta = _run(m, c, nsteps)
     n = m.ncell
     o.cellvol(geoel, coord)
@@ -151,7 +155,7 @@ def test_tgv_symmetry():
     assert np.abs(tau - np.rot90(tau, -1)).max() < 1e-12
 
 
-@pytest.mark.parametrize("name", ["tgv8", "sedov12", "tgv6_curved", "tgv6_hybrid"])
+@pytest.mark.parametrize("name", ["tgv8", "sedov12", "tgv6_curved", "tgv6_hybrid", "noh4_polar"])
 def test_golden_fixtures(name):
     from tests.golden.make_golden import run_case
     ref = np.load(os.path.join(GOLDEN, f"{name}.npz"))
@@ -205,3 +209,36 @@ def test_hybrid_mesh_geometry():
                 M[i, j] = M[j, i] = amatr[e, k]
                 k += 1
         assert np.linalg.eigvalsh(M).min() > 0
+
+
+def test_polar_mesh_geometry():
+    """Quarter-disk mesh of the Noh workload: every node used, curved cells
+    of positive volume whose total is the quarter disk up to the quadratic
+    arc interpolation (O(h^4)), SPD mass matrices, face neighbours paired."""
+    m = polar_mesh(8, 8)
+    assert m.ntria == 8 and m.nquad == 56
+    used = set(m.ipqua.reshape(-1).tolist()) | set(m.iptri.reshape(-1).tolist())
+    assert used == set(range(1, m.npoin + 1))
+    c = StepConfig(ncase=3, gamlg=5.0 / 3.0)
+    geoel, amatr, unkno = Oracle(m, c).init()
+    n = m.ncell
+    assert (geoel[:n, 2] > 0).all()
+    assert abs(geoel[:n, 2].sum() - np.pi / 4) < 1e-4
+    for e in range(n):
+        M = np.zeros((5, 5))
+        k = 0
+        for i in range(5):
+            for j in range(i, 5):
+                M[i, j] = M[j, i] = amatr[e, k]
+                k += 1
+        assert np.linalg.eigvalsh(M).min() > 0
+    # quad face neighbours: interior faces point back, boundary faces carry ghost ids
+    for q in range(m.nquad):
+        for k in range(4):
+            nb = m.esqua[q, k]
+            assert nb > 0
+            if m.ntria < nb <= n:
+                assert m.ntria + q + 1 in m.esqua[nb - m.ntria - 1]
+    # the Noh state: inward unit velocity, p = 1e-6
+    u, v = unkno[:n, 1, 0], unkno[:n, 2, 0]
+    assert np.abs(np.hypot(u, v) - 1.0).max() < 0.05
