@@ -87,11 +87,11 @@ def _sedov_hybrid(n: int, jitter: float = 0.0) -> Tuple[Mesh, StepConfig]:
 
 def _noh(n: int) -> Tuple[Mesh, StepConfig]:
     """Cartesian Noh implosion (ncase 3: rho = 1, u = -r/|r|, p = 1e-6,
-    gamma 5/3) on the quarter disk of polar_mesh: ``n`` rings of curved P2
+    gamma 5/3, SSP-RK2) on the quarter disk of polar_mesh: ``n`` rings of curved P2
     cells by ``n`` sectors, 6-node triangles on the axis ring, slip walls on
     the two rays, a free outer arc."""
     m = polar_mesh(n, n, 1.0)
-    c = StepConfig(ncase=3, gamlg=5.0 / 3.0, nstag=3, cfl=0.1, tend=0.6)
+    c = StepConfig(ncase=3, gamlg=5.0 / 3.0, nstag=2, cfl=0.1, tend=0.6)
     return m, c
 
 

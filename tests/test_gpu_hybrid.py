@@ -109,9 +109,11 @@ def test_hybrid_steps(name, nsteps, ordex):
             assert np.array_equal(u2[:n], unkno[:n]) and np.array_equal(x2, coord)
 
 
-def test_hybrid_mixed_steps():
-    """FP32-mixed quads next to FP64 triangles: cell averages within 1e-6."""
-    m, c = workload("tgv_hybrid16")
+@pytest.mark.parametrize("name", ["tgv_hybrid16", "noh8"])
+def test_hybrid_mixed_steps(name):
+    """FP32-mixed quads next to FP64 triangles: cell averages within 1e-6 of
+    the FP64 oracle, per field (tau, u, v, e)."""
+    m, c = workload(name)
     o = Oracle(m, c)
     geoel, amatr, unkno = o.init()
     s = Lag2DSolver(m, c, precision=1)
