@@ -184,28 +184,36 @@ def measured_traffic(family, ncell):
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
-def adjoint_block(s, args, fwd_ms_per_step):
-    """Time lag2d_adjoint over a short window from the solver's current state:
-    the reverse sweep per step (excluding the segment recompute) over the
-    forward step time of the main timing; the recompute is reported beside it."""
+def adjoint_block(s, args, fwd_ms_per_step, state, grads=None):
+    """Time lag2d_adjoint over a short window starting from ``state`` (unkno,
+    coord, ustar, itime, dtfix, tacru): the reverse sweep per step (excluding
+    the segment recompute) over the forward step time of the main timing; the
+    recompute is reported beside it.  The gradients are returned in
+    ``grads`` (a dict) when given."""
     import numpy as np
     from lag2d_b200.api import Lag2DError
 
     nsteps, k = args.adjoint_steps, args.adjoint_checkpoint
     if nsteps <= 0:
         return {"ratio": None, "note": "not run (--adjoint-steps 0)"}
+    u0, x0, us0, it0, dt0, ta0 = state
     try:
-        s.adjoint(min(2, nsteps), 1)          # loads the reverse kernels
-        J, gu, gx, gs, ms = s.adjoint(nsteps, k)
+        for K in (1, k):                      # the first call loads the reverse kernels
+            s.set_state(u0, x0, us0)
+            s.itime, s.dtfix, s.tacru = it0, dt0, ta0
+            J, gu, gx, gs, ms = s.adjoint(nsteps, K)
     except Lag2DError as e:
         return {"ratio": None, "note": str(e)}
+    if grads is not None:
+        grads.update(J=J, gu=gu, gx=gx, gs=gs)
     rev = ms[2] / nsteps
     return {"ratio": rev / fwd_ms_per_step, "reverse_ms_per_step": rev,
             "recompute_ms_per_step": ms[1] / nsteps, "forward_with_checkpoints_ms_per_step": ms[0] / nsteps,
             "forward_ms_per_step": fwd_ms_per_step, "steps": nsteps, "checkpoint_every": k,
             "functional": "J = 1/2 sum_c m_c (u_c^2 + v_c^2) at the window end",
             "grad_finite": bool(np.isfinite(gu).all() and np.isfinite(gx).all()),
-            "precision": "FP64 (the FP32-mixed adjoint is not built)"}
+            "precision": ("FP32-mixed (volume-integral and sub-cell-mass transposes in FP32)"
+                          if s._c.precision == 1 else "FP64")}
 
 
 def run_ours(args):
@@ -326,8 +334,24 @@ def run_ours(args):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "api": "lag2d_set_state + lag2d_step + lag2d_get_state (pinned host, Fortran layout)"}
 
-    # ---- adjoint: reverse sweep per step against the forward step time
-    adjoint = adjoint_block(s, args, ms_per_step)
+    # ---- adjoint: reverse sweep per step against the forward step time, FP64
+    # and FP32-mixed from the same state (the FP64 solver's current one)
+    u_a, x_a, us_a, _ = s.get_state()
+    state = (u_a, x_a, us_a, s.itime, s.dtfix, s.tacru)
+    g64, g32 = {}, {}
+    adjoint = adjoint_block(s, args, ms_per_step, state, g64)
+    sm2 = Lag2DSolver(m, c, precision=1)
+    sm2.init_fields()
+    adjoint["fp32_mixed"] = adjoint_block(sm2, args, mixed["ms_per_step"], state, g32)
+    sm2.close()
+    if g64 and g32:
+        import numpy as np
+        rel = {}
+        for key, name in (("gu", "dJ_dunkno"), ("gx", "dJ_dcoord"), ("gs", "dJ_dustar")):
+            a, b = g32[key], g64[key]
+            rel[name] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+        adjoint["fp32_mixed"]["grad_rel_l2_vs_fp64_adjoint"] = rel
+        adjoint["fp32_mixed"]["J_rel_vs_fp64"] = abs(g32["J"] - g64["J"]) / abs(g64["J"])
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done,

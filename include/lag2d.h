@@ -134,9 +134,12 @@ double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *lau
 
 /* ---------------------------------------------------------------------------
  * Adjoint of the time step.  No counterpart in the reference (it has no
- * adjoint); both entry points differentiate exactly what lag2d_step computes
- * on an all-quad mesh with precision 0 and order_exact 0 (others return
- * LAG2D_EUNSUP), reverse mode per RK stage with these held fixed: the time
+ * adjoint); both entry points differentiate what lag2d_step computes on an
+ * all-quad mesh with order_exact 0 (others return LAG2D_EUNSUP).  With
+ * precision 1 the forward passes are the FP32-mixed ones and the reverse runs
+ * its volume-integral and sub-cell-mass transposes in FP32 (the FP32-mixed
+ * adjoint); precision 0 is FP64 throughout.  Reverse mode per RK stage with
+ * these held fixed: the time
  * step size of each step (ndt == 1 picks it on the forward pass; the gradient
  * treats it as a constant), the Persson marks, and the reference-
  * configuration quantities (geoel fields 1-4 and 19-21, amatr).  A window in

@@ -233,7 +233,7 @@ class Lag2DSolver:
     def adjoint(self, nsteps: int, checkpoint_every: int):
         """nsteps steps from the handle's state and the gradient of the final
         kinetic energy J = 1/2 sum m_c (u_c^2 + v_c^2) w.r.t. the initial
-        state.  Returns (J, dJ_dunkno (ncell, nq, ndegr), dJ_dcoord (npoin, 2),
+        state (FP32-mixed adjoint when the solver has precision 1).  Returns (J, dJ_dunkno (ncell, nq, ndegr), dJ_dcoord (npoin, 2),
         dJ_dustar (npoin, 2), ms) with ms = [forward, recompute, reverse]
         device milliseconds."""
         m, c = self.mesh, self.cfg

@@ -53,7 +53,8 @@ void launch_tri_init(const Dev &d, cudaStream_t st);
 void launch_tri_geom(const Dev &d, cudaStream_t st, const double *X, const double *Y);
 void launch_tri_corner(const Dev &d, cudaStream_t st);
 void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa);
-void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold);
+void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold,
+                          int mixed);
 int adjoint_stage_launches();
 }  // namespace lag2d
 
@@ -834,7 +835,9 @@ double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *lau
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Adjoint of the optimised FP64 step (all-quad meshes).
+// Adjoint of the optimised step (all-quad meshes; FP64, or FP32-mixed when the
+// handle's precision is 1: the recompute runs the mixed forward passes and the
+// reverse the mixed transposes).
 //
 // Reverse mode per RK stage with the time step size, the Persson marks and the
 // WENO active set frozen from the forward pass; the forward pass must mark no
@@ -912,7 +915,8 @@ struct AdjWork {
       for (int istag = nstag; istag >= 1; istag--) {
         const Dev ds = rec.inputs(h->d, (size_t)k * nstag + (istag - 1));
         // stage 1 reads U^n and x^n directly: its reverse folds their adjoints in
-        launch_adjoint_stage(ds, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k, istag == 1);
+        launch_adjoint_stage(ds, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k, istag == 1,
+                             h->cfg.precision == 1);
         h->launches += adjoint_stage_launches();
       }
     }
@@ -955,8 +959,8 @@ struct Snapshot {
 
 static int adjoint_supported(lag2d_handle *h) {
   if (h->d.ntria > 0) return fail(LAG2D_EUNSUP, "the adjoint is built for all-quad meshes");
-  if (h->cfg.precision != 0 || h->cfg.order_exact)
-    return fail(LAG2D_EUNSUP, "the adjoint follows the optimised FP64 step (precision 0, order_exact 0)");
+  if (h->cfg.order_exact)
+    return fail(LAG2D_EUNSUP, "the adjoint follows the optimised step (order_exact 0)");
   return LAG2D_OK;
 }
 

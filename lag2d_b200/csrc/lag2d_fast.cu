@@ -1004,6 +1004,7 @@ __host__ __device__ __forceinline__ void vertex_T(const double *b, int mdegr, co
 // Reverse of the corner pass of quad iq: reads the node-sum adjoints lS at
 // its nodes and lcorr; adds the cell DOF adjoint into lU and writes the node
 // contributions (x, y, u*_prev, v*_prev) into pbuf.
+template <typename R>
 __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   if (iq >= d.nquad) return;
   const int e = iq + d.ntria;
@@ -1126,16 +1127,19 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
       for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
       const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
       const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
-      const double wi = 0.25 * g5w(i);
-      double m0 = 0.0, m1 = 0.0, m2 = 0.0, Ls[4] = {0, 0, 0, 0};
+      // point arithmetic in R (FP32 in the mixed adjoint), rows added in FP64
+      const R t0r = R(t0), t1r = R(t1), t2r = R(t2), lm = R(lmasel), wi = R(0.25 * g5w(i));
+      const R e0 = R(ee[0]), e1 = R(ee[1]), e2 = R(ee[2]), e3 = R(ee[3]);
+      R m0 = 0, m1 = 0, m2 = 0, Ls[4] = {0, 0, 0, 0};
 #pragma unroll
       for (int j = 0; j < 5; j++) {
-        const double s = (g5p(j) + ofs) / 2.0, ds = s - G.sc;
-        const double tau = t0 + ds * (t1 + t2 * ds);
-        const double det = ee[0] + s * (ee[1] + s * (ee[2] + s * ee[3]));
-        const double itau = 1.0 / tau;
-        const double ldet = lmasel * (wi * g5w(j)) * itau;
-        const double ltau = -ldet * det * itau;
+        const double sd = (g5p(j) + ofs) / 2.0;
+        const R s = R(sd), ds = R(sd - G.sc);
+        const R tau = t0r + ds * (t1r + t2r * ds);
+        const R det = e0 + s * (e1 + s * (e2 + s * e3));
+        const R itau = R(1) / tau;
+        const R ldet = lm * (wi * R(g5w(j))) * itau;
+        const R ltau = -ldet * det * itau;
         m0 += ltau;
         m1 += ltau * ds;
         m2 += ltau * ds * ds;
@@ -1144,17 +1148,18 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
         Ls[2] += ldet * s * s;
         Ls[3] += ldet * s * s * s;
       }
-      lu[0][0] += m0;
-      lu[0][1] += dr * m0;
-      lu[0][2] += m1;
-      lu[0][3] += (0.5 * dr * dr - G.g19) * m0;
-      lu[0][4] += 0.5 * m2 - G.g20 * m0;
-      lu[0][5] += dr * m1 - G.g21 * m0;
+      const double a0 = m0, a1 = m1, a2 = m2;
+      lu[0][0] += a0;
+      lu[0][1] += dr * a0;
+      lu[0][2] += a1;
+      lu[0][3] += (0.5 * dr * dr - G.g19) * a0;
+      lu[0][4] += 0.5 * a2 - G.g20 * a0;
+      lu[0][5] += dr * a1 - G.g21 * a0;
       double rp = 1.0;
 #pragma unroll
       for (int mm = 0; mm < 4; mm++) {
 #pragma unroll
-        for (int n = 0; n < 4; n++) lD[4 * mm + n] += rp * Ls[n];
+        for (int n = 0; n < 4; n++) lD[4 * mm + n] += rp * double(Ls[n]);
         rp *= r;
       }
     }
@@ -1179,9 +1184,137 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
     for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * (size_t)d.ncell + e] += lu[q][k];
 }
 
+// Reverse of the volume integral of the RHS pass (5x5 Gauss-Lobatto,
+// cofactor form), row by row: the DOFs along a row are a_q + ds (b_q + c_q ds),
+// and the transposed sums over a row collapse to per-row moments (sum l,
+// sum l ds, sum l ds^2 for the DOF adjoints; sum l L_b(s), sum l L_b'(s) for
+// the node adjoints).  R = double for the FP64 adjoint; R = float for the
+// FP32-mixed one, where the point arithmetic and the per-row moments are FP32
+// and the rows are added into the FP64 adjoints.
+template <typename R>
+__host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G, const double u[4][6],
+                                               const double lR[4][6], double g, double eps, double lu[4][6],
+                                               double lX[3][3], double lY[3][3]) {
+#pragma unroll 1
+  for (int i = 0; i < 5; i++) {
+    const double r = l5p(i), dr = r - G.rc;
+    double lr[3], dlr[3];
+    lag3(r, lr);
+    dlag3(r, dlr);
+    R Qx[3], Qy[3], Px[3], Py[3];
+#pragma unroll
+    for (int bb = 0; bb < 3; bb++) {
+      Qx[bb] = R(dlr[0] * L.X[0][bb] + dlr[1] * L.X[1][bb] + dlr[2] * L.X[2][bb]);
+      Qy[bb] = R(dlr[0] * L.Y[0][bb] + dlr[1] * L.Y[1][bb] + dlr[2] * L.Y[2][bb]);
+      Px[bb] = R(lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb]);
+      Py[bb] = R(lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb]);
+    }
+    R ra[4], rb[4], rc2[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      ra[q] = R(u[q][0] + u[q][1] * dr + u[q][3] * (0.5 * dr * dr - G.g19) - u[q][4] * G.g20 - u[q][5] * G.g21);
+      rb[q] = R(u[q][2] + u[q][5] * dr);
+      rc2[q] = R(0.5 * u[q][4]);
+    }
+    R lR1[4][5];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int kk = 0; kk < 5; kk++) lR1[q][kk] = R(lR[q][kk + 1]);
+    R m0[4] = {0, 0, 0, 0}, m1[4] = {0, 0, 0, 0}, m2[4] = {0, 0, 0, 0};
+    R Mxr[3] = {0, 0, 0}, Mxs[3] = {0, 0, 0}, Myr[3] = {0, 0, 0}, Mys[3] = {0, 0, 0};
+    const R wi = R(l5w(i)), drr = R(dr), gm1 = R(g - 1.0), epsr = R(eps), half = R(0.5), one = R(1);
+#pragma unroll 1
+    for (int j = 0; j < 5; j++) {
+      const R ds = R(l5p(j) - G.sc);
+      double lsd[3], dlsd[3];
+      lag3(l5p(j), lsd);
+      dlag3(l5p(j), dlsd);
+      const R ls[3] = {R(lsd[0]), R(lsd[1]), R(lsd[2])}, dls[3] = {R(dlsd[0]), R(dlsd[1]), R(dlsd[2])};
+      const R w = wi * R(l5w(j));
+      const R xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
+      const R yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
+      const R xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
+      const R ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
+      R un[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + rc2[q] * ds);
+      const R rhoad = one / un[0];
+      const R kin = un[3] - half * (un[1] * un[1] + un[2] * un[2]);
+      const R pe = gm1 * rhoad * kin;
+      const R pres = pe > epsr ? pe : epsr;
+      R gd0[5], gd1[5];
+      gd0[0] = ys;        gd1[0] = -xs;
+      gd0[1] = -yr;       gd1[1] = xr;
+      gd0[2] = ys * drr;  gd1[2] = -xs * drr;
+      gd0[3] = -yr * ds;  gd1[3] = xr * ds;
+      gd0[4] = ys * ds - yr * drr;
+      gd1[4] = -xs * ds + xr * drr;
+      const R wp = w * pres;
+      R lgd0[5], lgd1[5], lwp = 0, lun1 = 0, lun2 = 0;
+#pragma unroll
+      for (int kk = 0; kk < 5; kk++) {
+        const R fv = gd0[kk] * un[1] + gd1[kk] * un[2];
+        const R lfv = -lR1[0][kk] * w + lR1[3][kk] * wp;
+        lwp += lR1[3][kk] * fv + lR1[1][kk] * gd0[kk] + lR1[2][kk] * gd1[kk];
+        lgd0[kk] = lR1[1][kk] * wp + lfv * un[1];
+        lgd1[kk] = lR1[2][kk] * wp + lfv * un[2];
+        lun1 += lfv * gd0[kk];
+        lun2 += lfv * gd1[kk];
+      }
+      const R lpres = lwp * w;
+      R lun0 = 0, lun3 = 0;
+      if (pe > epsr) {
+        const R lrhoad = lpres * gm1 * kin;
+        lun3 += lpres * gm1 * rhoad;
+        lun1 -= lpres * gm1 * rhoad * un[1];
+        lun2 -= lpres * gm1 * rhoad * un[2];
+        lun0 += -lrhoad * rhoad * rhoad;
+      }
+      const R lunq[4] = {lun0, lun1, lun2, lun3};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        m0[q] += lunq[q];
+        m1[q] += lunq[q] * ds;
+        m2[q] += lunq[q] * ds * ds;
+      }
+      const R lys = lgd0[0] + lgd0[2] * drr + lgd0[4] * ds;
+      const R lyr = -lgd0[1] - lgd0[3] * ds - lgd0[4] * drr;
+      const R lxs = -lgd1[0] - lgd1[2] * drr - lgd1[4] * ds;
+      const R lxr = lgd1[1] + lgd1[3] * ds + lgd1[4] * drr;
+#pragma unroll
+      for (int b2 = 0; b2 < 3; b2++) {
+        Mxr[b2] += lxr * ls[b2];
+        Mxs[b2] += lxs * dls[b2];
+        Myr[b2] += lyr * ls[b2];
+        Mys[b2] += lys * dls[b2];
+      }
+    }
+    // basis (1, dr, ds, dr^2/2 - g19, ds^2/2 - g20, dr ds - g21) along the row
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const double a0 = m0[q], a1 = m1[q], a2 = m2[q];
+      lu[q][0] += a0;
+      lu[q][1] += dr * a0;
+      lu[q][2] += a1;
+      lu[q][3] += (0.5 * dr * dr - G.g19) * a0;
+      lu[q][4] += 0.5 * a2 - G.g20 * a0;
+      lu[q][5] += dr * a1 - G.g21 * a0;
+    }
+#pragma unroll
+    for (int aa = 0; aa < 3; aa++)
+#pragma unroll
+      for (int b2 = 0; b2 < 3; b2++) {
+        lX[aa][b2] += dlr[aa] * double(Mxr[b2]) + lr[aa] * double(Mxs[b2]);
+        lY[aa][b2] += dlr[aa] * double(Myr[b2]) + lr[aa] * double(Mys[b2]);
+      }
+  }
+}
+
 // Reverse of the RHS pass of quad iq (the RHS written, no fused update):
 // from lR adds into lU, writes pbuf (x, y, u*_prev, v*_prev, u*_new, v*_new)
 // and lcorr.
+template <typename R>
 __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
   if (iq >= d.nquad) return;
   const int e = iq + d.ntria;
@@ -1270,116 +1403,7 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     a.pbuf[(5 * 9 + k) * nq + iq] = lvn;
     vertex_T(b, d.mdegr, st, lrhovt, lke, lst1, lst2, lu);
   }
-  // ---- volume integral (5x5 Gauss-Lobatto, cofactor form), row by row: the
-  // DOFs along a row are a_q + ds (b_q + c_q ds), and the transposed sums over
-  // a row collapse to per-row moments (sum l, sum l ds, sum l ds^2 for the
-  // DOF adjoints; sum l L_b(s), sum l L_b'(s) for the node adjoints)
-#pragma unroll 1
-  for (int i = 0; i < 5; i++) {
-    const double r = l5p(i), dr = r - G.rc;
-    double lr[3], dlr[3];
-    lag3(r, lr);
-    dlag3(r, dlr);
-    double Qx[3], Qy[3], Px[3], Py[3];
-#pragma unroll
-    for (int bb = 0; bb < 3; bb++) {
-      Qx[bb] = dlr[0] * L.X[0][bb] + dlr[1] * L.X[1][bb] + dlr[2] * L.X[2][bb];
-      Qy[bb] = dlr[0] * L.Y[0][bb] + dlr[1] * L.Y[1][bb] + dlr[2] * L.Y[2][bb];
-      Px[bb] = lr[0] * L.X[0][bb] + lr[1] * L.X[1][bb] + lr[2] * L.X[2][bb];
-      Py[bb] = lr[0] * L.Y[0][bb] + lr[1] * L.Y[1][bb] + lr[2] * L.Y[2][bb];
-    }
-    double ra[4], rb[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      ra[q] = u[q][0] + u[q][1] * dr + u[q][3] * (0.5 * dr * dr - G.g19) - u[q][4] * G.g20 - u[q][5] * G.g21;
-      rb[q] = u[q][2] + u[q][5] * dr;
-    }
-    double m0[4] = {0, 0, 0, 0}, m1[4] = {0, 0, 0, 0}, m2[4] = {0, 0, 0, 0};
-    double Mxr[3] = {0, 0, 0}, Mxs[3] = {0, 0, 0}, Myr[3] = {0, 0, 0}, Mys[3] = {0, 0, 0};
-    const double wi = l5w(i);
-#pragma unroll 1
-    for (int j = 0; j < 5; j++) {
-      const double s = l5p(j), ds = s - G.sc;
-      double ls[3], dls[3];
-      lag3(s, ls);
-      dlag3(s, dls);
-      const double w = wi * l5w(j);
-      const double xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
-      const double yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
-      const double xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
-      const double ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
-      double un[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * u[q][4] * ds);
-      const double rhoad = 1.0 / un[0];
-      const double kin = un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]);
-      const double pe = (g - 1.0) * rhoad * kin;
-      const double pres = fmax(eps, pe);
-      double gd0[5], gd1[5];
-      gd0[0] = ys;       gd1[0] = -xs;
-      gd0[1] = -yr;      gd1[1] = xr;
-      gd0[2] = ys * dr;  gd1[2] = -xs * dr;
-      gd0[3] = -yr * ds; gd1[3] = xr * ds;
-      gd0[4] = ys * ds - yr * dr;
-      gd1[4] = -xs * ds + xr * dr;
-      const double wp = w * pres;
-      double lgd0[5], lgd1[5], lwp = 0.0, lun1 = 0.0, lun2 = 0.0;
-#pragma unroll
-      for (int kk = 0; kk < 5; kk++) {
-        const double fv = gd0[kk] * un[1] + gd1[kk] * un[2];
-        const double lfv = -lR[0][kk + 1] * w + lR[3][kk + 1] * wp;
-        lwp += lR[3][kk + 1] * fv + lR[1][kk + 1] * gd0[kk] + lR[2][kk + 1] * gd1[kk];
-        lgd0[kk] = lR[1][kk + 1] * wp + lfv * un[1];
-        lgd1[kk] = lR[2][kk + 1] * wp + lfv * un[2];
-        lun1 += lfv * gd0[kk];
-        lun2 += lfv * gd1[kk];
-      }
-      const double lpres = lwp * w;
-      double lun0 = 0.0, lun3 = 0.0;
-      if (pe > eps) {
-        const double lrhoad = lpres * (g - 1.0) * kin;
-        lun3 += lpres * (g - 1.0) * rhoad;
-        lun1 -= lpres * (g - 1.0) * rhoad * un[1];
-        lun2 -= lpres * (g - 1.0) * rhoad * un[2];
-        lun0 += -lrhoad * rhoad * rhoad;
-      }
-      const double lunq[4] = {lun0, lun1, lun2, lun3};
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        m0[q] += lunq[q];
-        m1[q] += lunq[q] * ds;
-        m2[q] += lunq[q] * ds * ds;
-      }
-      const double lys = lgd0[0] + lgd0[2] * dr + lgd0[4] * ds;
-      const double lyr = -lgd0[1] - lgd0[3] * ds - lgd0[4] * dr;
-      const double lxs = -lgd1[0] - lgd1[2] * dr - lgd1[4] * ds;
-      const double lxr = lgd1[1] + lgd1[3] * ds + lgd1[4] * dr;
-#pragma unroll
-      for (int b2 = 0; b2 < 3; b2++) {
-        Mxr[b2] += lxr * ls[b2];
-        Mxs[b2] += lxs * dls[b2];
-        Myr[b2] += lyr * ls[b2];
-        Mys[b2] += lys * dls[b2];
-      }
-    }
-    // basis (1, dr, ds, dr^2/2 - g19, ds^2/2 - g20, dr ds - g21) along the row
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      lu[q][0] += m0[q];
-      lu[q][1] += dr * m0[q];
-      lu[q][2] += m1[q];
-      lu[q][3] += (0.5 * dr * dr - G.g19) * m0[q];
-      lu[q][4] += 0.5 * m2[q] - G.g20 * m0[q];
-      lu[q][5] += dr * m1[q] - G.g21 * m0[q];
-    }
-#pragma unroll
-    for (int aa = 0; aa < 3; aa++)
-#pragma unroll
-      for (int b2 = 0; b2 < 3; b2++) {
-        lX[aa][b2] += dlr[aa] * Mxr[b2] + lr[aa] * Mxs[b2];
-        lY[aa][b2] += dlr[aa] * Myr[b2] + lr[aa] * Mys[b2];
-      }
-  }
+  vol_T<R>(L, G, u, lR, g, eps, lu, lX, lY);
   // ---- Taylor-Green source: cos and sin of pi x at the Gauss points by angle
   // addition from the centre node, as in the forward pass
   double lxp[9][2];
@@ -1646,8 +1670,10 @@ __global__ void k_nodes2(Dev d, double alfa) { f_nodes(d, blockIdx.x * blockDim.
 __global__ void k_geom2(Dev d, int fix) { f_geom(d, blockIdx.x * blockDim.x + threadIdx.x, fix); }
 __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + threadIdx.x); }
 
-__global__ void __launch_bounds__(128) k_a_corner(Dev d, Adj a) { a_corner(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128) k_a_rhs(Dev d, Adj a) { a_rhs(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+template <typename R>
+__global__ void __launch_bounds__(128) k_a_corner(Dev d, Adj a) { a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+template <typename R>
+__global__ void __launch_bounds__(128) k_a_rhs(Dev d, Adj a) { a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_gather(Dev d, Adj a, int nv) { a_gather(d, a, blockIdx.x * blockDim.x + threadIdx.x, nv); }
 __global__ void k_a_gather_solve(Dev d, Adj a) { a_gather_solve(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_update(Dev d, Adj a, double alfa, const double *dtp, int fold) {
@@ -1662,21 +1688,27 @@ static inline int nb(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace fast
 
-// Reverse of one RK stage of the optimised FP64 step (all-quad meshes).  d
-// views the stage's inputs (U^(s) in d.Us, x^(s) in d.xs/ys, u*_prev in
-// d.us/vs) and the forward corner and node outputs of that stage (d.npart,
-// d.corr, d.us_new/vs_new); the transposes run in reverse order.  dtp is the
-// device address of the step's time step size; fold = 1 for stage 1, which
-// ends the step's reverse (U^(1) and x^(1) are U^n and x^n).
-void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold) {
+// Reverse of one RK stage of the optimised step (all-quad meshes).  d views
+// the stage's inputs (U^(s) in d.Us, x^(s) in d.xs/ys, u*_prev in d.us/vs) and
+// the forward corner and node outputs of that stage (d.npart, d.corr,
+// d.us_new/vs_new); the transposes run in reverse order.  dtp is the device
+// address of the step's time step size; fold = 1 for stage 1, which ends the
+// step's reverse (U^(1) and x^(1) are U^n and x^n).  mixed = 1 selects the
+// FP32-mixed adjoint: the volume-integral and sub-cell-mass transposes run in
+// FP32 with per-row moments added into the FP64 adjoints; geometry, corner
+// coefficients, the node solve, the update and node motion stay FP64.
+void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold,
+                          int mixed) {
   const fast::Adj &a = *static_cast<const fast::Adj *>(adj);
   const int bq = fast::nb(d.nquad, 128), bp = fast::nb(d.npoin, 256), bc = fast::nb(d.ncell, 256);
   fast::k_a_centre<<<bp, 256, 0, st>>>(d, a);
   fast::k_a_nodes<<<bp, 256, 0, st>>>(d, a, alfa, dtp, fold);
   fast::k_a_update<<<bc, 256, 0, st>>>(d, a, alfa, dtp, fold);
-  fast::k_a_rhs<<<bq, 128, 0, st>>>(d, a);
+  if (mixed) fast::k_a_rhs<float><<<bq, 128, 0, st>>>(d, a);
+  else fast::k_a_rhs<double><<<bq, 128, 0, st>>>(d, a);
   fast::k_a_gather_solve<<<bp, 256, 0, st>>>(d, a);
-  fast::k_a_corner<<<bq, 128, 0, st>>>(d, a);
+  if (mixed) fast::k_a_corner<float><<<bq, 128, 0, st>>>(d, a);
+  else fast::k_a_corner<double><<<bq, 128, 0, st>>>(d, a);
   fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
 }
 int adjoint_stage_launches() { return 7; }

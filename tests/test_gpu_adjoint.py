@@ -15,6 +15,10 @@ Bounds:
     ends at the same state as plain steps;
   * a torch.autograd.Function around lag2d_step / lag2d_adjoint_step, chained
     over the 3 steps, gives the gradients of the checkpointed window to 1e-12;
+  * the FP32-mixed adjoint (precision 1: mixed forward passes, FP32
+    volume-integral and sub-cell-mass transposes) gives every directional
+    derivative of the FP64 adjoint to MIXED_TOL relative (or of the largest
+    one, for derivatives near zero);
   * configurations outside the differentiated path report LAG2D_EUNSUP.
 """
 import dataclasses
@@ -31,6 +35,7 @@ pytestmark = pytest.mark.gpu
 NSTEPS = 3
 EPS = 1e-5
 FD_TOL = 1e-5
+MIXED_TOL = 1e-4
 
 
 def _case():
@@ -196,12 +201,11 @@ def test_adjoint_unsupported_configurations():
         s.adjoint(1, 1)
     assert e.value.code == 3
     m, c = workload("tgv16")
-    for kw in (dict(precision=1), dict(order_exact=True)):
-        s = Lag2DSolver(m, c, **kw)
-        s.init_fields()
-        with pytest.raises(Lag2DError) as e:
-            s.adjoint_step()
-        assert e.value.code == 3
+    s = Lag2DSolver(m, c, order_exact=True)
+    s.init_fields()
+    with pytest.raises(Lag2DError) as e:
+        s.adjoint_step()
+    assert e.value.code == 3
     # Sedov: the Persson sensor marks cells from the second step on
     m, c = workload("sedov16")
     s = Lag2DSolver(m, dataclasses.replace(c, ndt=0))
@@ -209,3 +213,28 @@ def test_adjoint_unsupported_configurations():
     with pytest.raises(Lag2DError) as e:
         s.adjoint(3, 2)
     assert e.value.code == 3
+
+
+def test_mixed_adjoint_against_fp64_adjoint(case):
+    m, c, unkno = case["m"], case["c"], case["unkno"]
+    n = m.ncell
+    sm = Lag2DSolver(m, c, precision=1)
+    sm.init_fields()
+    _reset(sm, c, unkno, m.coord, np.zeros_like(m.coord), case["geoel"], case["amatr"])
+    J, gU, gX, gS, ms = sm.adjoint(NSTEPS, 2)
+    assert abs(J - case["J"]) <= 1e-6 * case["J"]
+    rng = np.random.default_rng(3)
+    dirs = []
+    for q in range(4):
+        for kk in ([0], [1, 2], [3, 4, 5]):
+            d = np.zeros((n, 4, 6))
+            for k in kk:
+                d[:, q, k] = rng.standard_normal(n)
+            dirs.append((float(np.sum(gU * d)), float(np.sum(case["gU"] * d)), f"U q={q} k={kk}"))
+    for _ in range(3):
+        d = rng.standard_normal(m.coord.shape)
+        dirs.append((float(np.sum(gX * d)), float(np.sum(case["gX"] * d)), "coord"))
+        dirs.append((float(np.sum(gS * d)), float(np.sum(case["gS"] * d)), "ustar"))
+    big = max(abs(r) for _, r, _ in dirs)
+    for got, ref, what in dirs:
+        assert abs(got - ref) <= MIXED_TOL * max(abs(ref), 1e-3 * big), (what, got, ref)
