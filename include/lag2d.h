@@ -134,17 +134,18 @@ double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *lau
 
 /* ---------------------------------------------------------------------------
  * Adjoint of the time step.  No counterpart in the reference (it has no
- * adjoint); both entry points differentiate what lag2d_step computes on an
- * all-quad mesh with order_exact 0 (others return LAG2D_EUNSUP).  With
- * precision 1 the forward passes are the FP32-mixed ones and the reverse runs
- * its volume-integral and sub-cell-mass transposes in FP32 (the FP32-mixed
- * adjoint); precision 0 is FP64 throughout.  Reverse mode per RK stage with
- * these held fixed: the time
- * step size of each step (ndt == 1 picks it on the forward pass; the gradient
- * treats it as a constant), the Persson marks, and the reference-
- * configuration quantities (geoel fields 1-4 and 19-21, amatr).  A window in
- * which the Persson sensor marks a troubled cell returns LAG2D_EUNSUP (the
- * adjoint of the WENO reconstruction is not built).  Gradients use the
+ * adjoint); both entry points differentiate what lag2d_step computes (quads
+ * and triangles) with order_exact 0 (order_exact 1 returns LAG2D_EUNSUP).
+ * With precision 1 the forward passes are the FP32-mixed ones and the reverse
+ * runs its volume-integral and sub-cell-mass transposes in FP32 (the
+ * FP32-mixed adjoint); precision 0 is FP64 throughout.  Reverse mode per RK
+ * stage with these held fixed: the time step size of each step (ndt == 1
+ * picks it on the forward pass; the gradient treats it as a constant), the
+ * Persson marks, and the reference-configuration quantities (geoel fields 1-4
+ * and 19-21, amatr, the initial sub-cell masses).  A window in which WENO
+ * replaces the DOFs of a cell returns LAG2D_EUNSUP (the adjoint of the WENO
+ * reconstruction is not built); marked cells whose stencil is rejected keep
+ * their DOFs and are differentiated as such.  Gradients use the
  * layouts of lag2d_set_state: unkno(ndegr,nq,ncell), coord(2,npoin),
  * ustar(2,npoin).
  * ------------------------------------------------------------------------- */

@@ -55,7 +55,7 @@ void launch_tri_corner(const Dev &d, cudaStream_t st);
 void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa);
 void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold,
                           int mixed);
-int adjoint_stage_launches();
+int adjoint_stage_launches(const Dev &d);
 }  // namespace lag2d
 
 using namespace lag2d;
@@ -301,14 +301,14 @@ static void rhs_pass(lag2d_handle *h, const Dev &d, int fuse, double alfa) {
 // stage's corner and node outputs (node partial sums, sub-cell density
 // corrections, u*_new) are written straight into the slot instead of the
 // handle's buffers; the step's time step size is kept after stage 1, and the
-// troubled-cell count of each stage is accumulated (the adjoint needs it to
-// stay zero).
+// number of cells WENO replaced in each stage is accumulated (the adjoint
+// needs it to stay zero).
 struct StageRec {
   double *U, *x, *y, *us, *vs, *dt;
-  double *npart, *corr, *usn, *vsn;
+  double *npart, *corr, *usn, *vsn, *tcf, *tpart;
   int *troubled;
   int step, nstag;
-  size_t nu, np, nq;
+  size_t nu, np, nq, nt;
   // the handle's device view with the corner/node outputs of a slot
   Dev outputs(const Dev &d0, size_t slot) const {
     Dev d = d0;
@@ -316,6 +316,10 @@ struct StageRec {
     d.corr = corr + slot * 4 * nq;
     d.us_new = usn + slot * np;
     d.vs_new = vsn + slot * np;
+    if (nt > 0) {
+      d.tcf = tcf + slot * 120 * nt;
+      d.tpart = tpart + slot * 30 * nt;
+    }
     return d;
   }
   // ... and with the recorded stage inputs as well
@@ -329,7 +333,13 @@ struct StageRec {
     return d;
   }
 };
-__global__ void k_add_count(const int *c, int *acc) { *acc += *c; }
+// cells the WENO pass actually replaced (flag 2): marked cells whose stencil
+// was rejected keep their DOFs, so the step stays differentiable there
+__global__ void k_count_limited(Dev d, int *acc) {
+  int n = 0;
+  for (int t = threadIdx.x; t < *d.wcount; t += blockDim.x) n += d.flag[d.wlist[t] + d.ntria] == 2;
+  if (n) atomicAdd(acc, n);
+}
 
 // The same step with the optimised kernels: node partial sums, recomputed
 // corner data, closed-form volumes and the stage update fused into the RHS
@@ -351,11 +361,11 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
       cudaMemcpyAsync(rec->vs + slot * rec->np, d.vs, rec->np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
     }
     run(h, "persson", [&] { launch_reset_count(d, h->st); launch_fast_persson(d, h->st); }, 2);
+    run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
     if (rec) {
-      k_add_count<<<1, 1, 0, h->st>>>(d.wcount, rec->troubled);
+      k_count_limited<<<1, 256, 0, h->st>>>(d, rec->troubled);
       h->launches += 1;
     }
-    run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
     run(h, "corner", [&] { corner_pass(h, d); }, 1 + T);
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
@@ -835,25 +845,23 @@ double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *lau
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Adjoint of the optimised step (all-quad meshes; FP64, or FP32-mixed when the
-// handle's precision is 1: the recompute runs the mixed forward passes and the
+// Adjoint of the optimised step (quads and triangles; FP64, or FP32-mixed when
+// the handle's precision is 1: the recompute runs the mixed forward passes and the
 // reverse the mixed transposes).
 //
-// Reverse mode per RK stage with the time step size, the Persson marks and the
-// WENO active set frozen from the forward pass; the forward pass must mark no
-// troubled cell in the window (the WENO reconstruction's adjoint is not built,
-// so a window that limits returns LAG2D_EUNSUP).  Reference-configuration
+// Reverse mode per RK stage with the time step size and the Persson marks
+// frozen from the forward pass; WENO must replace no cell in the window (its
+// reconstruction's adjoint is not built, so a window that limits returns
+// LAG2D_EUNSUP; marked cells whose stencil is rejected keep their DOFs and are
+// differentiated as unlimited cells).  Reference-configuration
 // quantities (cell masses, mass matrices, initial-mesh moments) are constants.
 // The stage inputs are recorded by recomputing each checkpoint segment, so the
 // device memory of a window is (segments + 1) checkpoints plus K steps of
 // stage records.
-struct AdjBufs {
-  double *lU, *lUn, *lx, *ly, *lxn, *lyn, *lus, *lvs, *luw, *lvw, *lR, *lS, *lcorr, *pbuf, *tx, *ty;
-};
 struct AdjWork {
   lag2d_handle *h;
   std::vector<void *> mem;
-  AdjBufs a{};
+  Adj a{};
   StageRec rec{};
   int rc = LAG2D_OK;
   explicit AdjWork(lag2d_handle *hh) : h(hh) {}
@@ -884,12 +892,14 @@ struct AdjWork {
     alloc(&a.lx, np); alloc(&a.ly, np); alloc(&a.lxn, np); alloc(&a.lyn, np); alloc(&a.lus, np); alloc(&a.lvs, np);
     alloc(&a.luw, np); alloc(&a.lvw, np); alloc(&a.tx, np); alloc(&a.ty, np);
     alloc(&a.lS, 5 * np); alloc(&a.lcorr, 4 * (size_t)d.nquad); alloc(&a.pbuf, 54 * (size_t)d.nquad);
+    alloc(&a.tbuf, 36 * (size_t)d.ntria); alloc(&a.ltcf, 120 * (size_t)d.ntria);
     const size_t ns = (size_t)K * nstag;
     alloc(&rec.U, ns * nu); alloc(&rec.x, ns * np); alloc(&rec.y, ns * np);
     alloc(&rec.us, ns * np); alloc(&rec.vs, ns * np); alloc(&rec.dt, K); alloc(&rec.troubled, 1);
     alloc(&rec.npart, ns * 45 * (size_t)d.nquad); alloc(&rec.corr, ns * 4 * (size_t)d.nquad);
     alloc(&rec.usn, ns * np); alloc(&rec.vsn, ns * np);
-    rec.nstag = nstag; rec.nu = nu; rec.np = np; rec.nq = d.nquad;
+    alloc(&rec.tcf, ns * 120 * (size_t)d.ntria); alloc(&rec.tpart, ns * 30 * (size_t)d.ntria);
+    rec.nstag = nstag; rec.nu = nu; rec.np = np; rec.nq = d.nquad; rec.nt = d.ntria;
   }
   // forward of nk steps from the handle's state, recording every stage input
   int record(int itime, int nk) {
@@ -904,7 +914,7 @@ struct AdjWork {
     int troubled = 0;
     CK(cudaMemcpyAsync(&troubled, rec.troubled, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    if (troubled) return fail(LAG2D_EUNSUP, "troubled cells in the adjoint window: the WENO adjoint is not built");
+    if (troubled) return fail(LAG2D_EUNSUP, "WENO limits cells in the adjoint window: its adjoint is not built");
     return LAG2D_OK;
   }
   // reverse of the nk recorded steps; a.lU / a.lx / a.lus hold the adjoints of
@@ -917,7 +927,7 @@ struct AdjWork {
         // stage 1 reads U^n and x^n directly: its reverse folds their adjoints in
         launch_adjoint_stage(ds, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k, istag == 1,
                              h->cfg.precision == 1);
-        h->launches += adjoint_stage_launches();
+        h->launches += adjoint_stage_launches(h->d);
       }
     }
   }
@@ -958,14 +968,13 @@ struct Snapshot {
 };
 
 static int adjoint_supported(lag2d_handle *h) {
-  if (h->d.ntria > 0) return fail(LAG2D_EUNSUP, "the adjoint is built for all-quad meshes");
   if (h->cfg.order_exact)
     return fail(LAG2D_EUNSUP, "the adjoint follows the optimised step (order_exact 0)");
   return LAG2D_OK;
 }
 
 // caller layouts <-> device SoA for the adjoint fields
-static int put_adjoint(lag2d_handle *h, const AdjBufs &a, const double *unkno, const double *coord,
+static int put_adjoint(lag2d_handle *h, const Adj &a, const double *unkno, const double *coord,
                        const double *ustar) {
   const Dev &d = h->d;
   const size_t nc = d.ncell, np = d.npoin, nu = (size_t)NU * nc;
@@ -989,7 +998,7 @@ static int put_adjoint(lag2d_handle *h, const AdjBufs &a, const double *unkno, c
   }
   return LAG2D_OK;
 }
-static int get_adjoint(lag2d_handle *h, const AdjBufs &a, double *unkno, double *coord, double *ustar) {
+static int get_adjoint(lag2d_handle *h, const Adj &a, double *unkno, double *coord, double *ustar) {
   const Dev &d = h->d;
   const size_t nc = d.ncell, np = d.npoin, nu = (size_t)NU * nc;
   if (unkno) {

@@ -82,4 +82,21 @@ struct QuadTables {
   double t7[7][2], tw7[7];      // 7-point triangle rule (rutope)
 };
 
+// Adjoint (reverse-mode) work arrays of one RK stage, shared by the quad and
+// triangle reverse kernels.
+struct Adj {
+  double *lU, *lUn;        // [24][ncell] adjoints of U^(s) and U^n
+  double *lx, *ly;         // adjoint of the stage coordinates
+  double *lxn, *lyn;       // adjoint of x^n
+  double *lus, *lvs;       // adjoint of the stage's previous ustar
+  double *luw, *lvw;       // adjoint of the stage's new ustar
+  double *lR;              // [24][ncell] adjoint of the stage RHS
+  double *lS;              // [5][npoin] adjoint of the node sums (m, m u, m v, sigma.n A)
+  double *lcorr;           // [4][nquad] adjoint of the sub-cell density corrections
+  double *pbuf;            // [6][9][nquad] per (quad, node) adjoint contributions
+  double *tx, *ty;         // scratch of the centre-node transpose
+  double *tbuf;            // [6][6][ntria] per (triangle, node) adjoint contributions
+  double *ltcf;            // [5][24][ntria] adjoint of the triangle corner coefficients (RHS pass)
+};
+
 }  // namespace lag2d

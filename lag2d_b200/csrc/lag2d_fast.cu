@@ -847,18 +847,6 @@ __host__ __device__ void f_init_wmom(const Dev &d, int iq) {
 // active branch; the impedance's jump-direction branch (|u* - u_c| >= 1e12 c)
 // is taken as the regular one.
 // ---------------------------------------------------------------------------
-struct Adj {
-  double *lU, *lUn;        // [24][ncell] adjoints of U^(s) and U^n
-  double *lx, *ly;         // adjoint of the stage coordinates
-  double *lxn, *lyn;       // adjoint of x^n
-  double *lus, *lvs;       // adjoint of the stage's previous ustar
-  double *luw, *lvw;       // adjoint of the stage's new ustar
-  double *lR;              // [24][ncell] adjoint of the stage RHS
-  double *lS;              // [5][npoin] adjoint of the node sums (m, m u, m v, sigma.n A)
-  double *lcorr;           // [4][nquad] adjoint of the sub-cell density corrections
-  double *pbuf;            // [6][9][nquad] per (quad, node) adjoint contributions
-  double *tx, *ty;         // scratch of the centre-node transpose
-};
 
 // transpose of cross36: c[p] = x_i y_j - x_j y_i
 __host__ __device__ __forceinline__ void cross36_T(const double (*xp)[2], const double *lc, double (*lxp)[2]) {
@@ -1519,7 +1507,11 @@ __host__ __device__ void a_gather(const Dev &d, const Adj &a, int p, int nv) {
   const int b = d.node_ptr2[p], en = d.node_slot ? d.node_ptr2[p + 1] : b;
   for (int i = b; i < en; i++) {
     const int id = d.node_slot[i];
-    if (id < 0) continue;
+    if (id < 0) {  // triangle: -1 - (it*6 + k)
+      const int t = -1 - id, it = t / 6, k = t - 6 * it;
+      for (int v = 0; v < nv; v++) s[v] += a.tbuf[(v * 6 + k) * (size_t)d.ntria + it];
+      continue;
+    }
     const int iq = id / 9, k = id - 9 * iq;
     for (int v = 0; v < nv; v++) s[v] += a.pbuf[(v * 9 + k) * (size_t)d.nquad + iq];
   }
@@ -1533,7 +1525,7 @@ __host__ __device__ void a_gather(const Dev &d, const Adj &a, int p, int nv) {
   }
 }
 
-// Gather of the RHS pass's per-(quad, node) contributions (x, y, u*_prev,
+// Gather of the RHS pass's per-(cell, node) contributions (x, y, u*_prev,
 // u*_new) fused with the reverse of the node solve u* = (S1 - S3) / S0,
 // v* = (S2 - S4) / S0 (wall masks; kept nodes take u*_prev).  Only S0 is
 // gathered again: u* itself is the forward pass's d.us_new / d.vs_new.
@@ -1542,7 +1534,13 @@ __host__ __device__ void a_gather_solve(const Dev &d, const Adj &a, int p) {
   double s[6] = {0, 0, 0, 0, 0, 0}, S0 = 0.0;
   for (int i = d.node_ptr2[p]; i < d.node_ptr2[p + 1]; i++) {
     const int id = d.node_slot[i];
-    if (id < 0) continue;
+    if (id < 0) {  // triangle: -1 - (it*6 + k)
+      const int t = -1 - id, it = t / 6, k = t - 6 * it;
+#pragma unroll
+      for (int v = 0; v < 6; v++) s[v] += a.tbuf[(v * 6 + k) * (size_t)d.ntria + it];
+      S0 += d.tpart[k * (size_t)d.ntria + it];
+      continue;
+    }
     const int iq = id / 9, k = id - 9 * iq;
 #pragma unroll
     for (int v = 0; v < 6; v++) s[v] += a.pbuf[(v * 9 + k) * (size_t)d.nquad + iq];
@@ -1688,7 +1686,11 @@ static inline int nb(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace fast
 
-// Reverse of one RK stage of the optimised step (all-quad meshes).  d views
+void launch_tri_adjoint_rhs(const Dev &d, const Adj &a, cudaStream_t st);
+void launch_tri_adjoint_corner(const Dev &d, const Adj &a, cudaStream_t st);
+
+// Reverse of one RK stage of the optimised step.  Triangles run their own
+// reverse corner and RHS kernels next to the quads' ones.  d views
 // the stage's inputs (U^(s) in d.Us, x^(s) in d.xs/ys, u*_prev in d.us/vs) and
 // the forward corner and node outputs of that stage (d.npart, d.corr,
 // d.us_new/vs_new); the transposes run in reverse order.  dtp is the device
@@ -1699,20 +1701,22 @@ static inline int nb(int n, int b) { return (n + b - 1) / b; }
 // coefficients, the node solve, the update and node motion stay FP64.
 void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold,
                           int mixed) {
-  const fast::Adj &a = *static_cast<const fast::Adj *>(adj);
+  const Adj &a = *static_cast<const Adj *>(adj);
   const int bq = fast::nb(d.nquad, 128), bp = fast::nb(d.npoin, 256), bc = fast::nb(d.ncell, 256);
   fast::k_a_centre<<<bp, 256, 0, st>>>(d, a);
   fast::k_a_nodes<<<bp, 256, 0, st>>>(d, a, alfa, dtp, fold);
   fast::k_a_update<<<bc, 256, 0, st>>>(d, a, alfa, dtp, fold);
   if (mixed) fast::k_a_rhs<float><<<bq, 128, 0, st>>>(d, a);
   else fast::k_a_rhs<double><<<bq, 128, 0, st>>>(d, a);
+  launch_tri_adjoint_rhs(d, a, st);
   fast::k_a_gather_solve<<<bp, 256, 0, st>>>(d, a);
   if (mixed) fast::k_a_corner<float><<<bq, 128, 0, st>>>(d, a);
   else fast::k_a_corner<double><<<bq, 128, 0, st>>>(d, a);
+  launch_tri_adjoint_corner(d, a, st);
   fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
 }
-int adjoint_stage_launches() { return 7; }
-size_t adjoint_struct_size() { return sizeof(fast::Adj); }
+int adjoint_stage_launches(const Dev &d) { return d.ntria > 0 ? 9 : 7; }
+
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
 void launch_fast_corner(const Dev &d, cudaStream_t st) { fast::k_corner2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }

@@ -2217,6 +2217,455 @@ void launch_tri_geom(const Dev &d, cudaStream_t st, const double *X, const doubl
 void launch_tri_corner(const Dev &d, cudaStream_t st) {
   if (d.ntria) k_tri_corner<<<nblk(d.ntria, 128), 128, 0, st>>>(d);
 }
+// ---------------------------------------------------------------------------
+// Adjoint of the triangle passes (reverse mode of b_tri_corner and b_tri_rhs;
+// the fused update, node motion and gathers are shared with the quads).
+// ---------------------------------------------------------------------------
+
+// transpose of normals_tria: lgt[slot] = (adjoint of n0, n1, A) -> lxpt
+__host__ __device__ void normals_tria_T(const double (*xpt)[2], const double (*lgt)[3], double (*lxpt)[2]) {
+  const double postc[3][2] = {{0.25, 0.25}, {0.5, 0.25}, {0.25, 0.5}};
+  const int ipift[3][3] = {{4, 6, 1}, {5, 4, 2}, {6, 5, 3}};
+  double xptv[3][2], shpv[3][6];
+  for (int isv = 0; isv < 3; isv++) {
+    shp6v(postc[isv][0], postc[isv][1], shpv[isv]);
+    map6(xpt, shpv[isv], xptv[isv][0], xptv[isv][1]);
+  }
+  double lxptv[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+  for (int ifa = 0; ifa < 3; ifa++) {
+    double xpf[3][2];
+    for (int c = 0; c < 2; c++) {
+      xpf[0][c] = xpt[ipift[ifa][0] - 1][c];
+      xpf[1][c] = xpt[ipift[ifa][1] - 1][c];
+      xpf[2][c] = xptv[ipift[ifa][2] - 1][c];
+    }
+    for (int end = 0; end < 2; end++) {
+      const double r = end == 0 ? -1.0 : 1.0;
+      const double dshpr[3] = {-0.5 + r, 0.5 + r, -2.0 * r};
+      double a = 0.0, b = 0.0;  // dx/dr, dy/dr
+      for (int k = 0; k < 3; k++) {
+        a += dshpr[k] * xpf[k][0];
+        b += dshpr[k] * xpf[k][1];
+      }
+      // n = (-b, a) / J, A = 2 J, J = |(a, b)|
+      const int slot = (end == 0 ? 6 : 12) + ifa;
+      const double J = sqrt(a * a + b * b), iJ = 1.0 / J, iJ3 = iJ * iJ * iJ;
+      const double t = lgt[slot][0] * a + lgt[slot][1] * b;
+      const double la = b * iJ3 * t + 2.0 * lgt[slot][2] * a * iJ;
+      const double lb = -a * iJ3 * t + 2.0 * lgt[slot][2] * b * iJ;
+      for (int k = 0; k < 3; k++) {
+        const double lx = la * dshpr[k], ly = lb * dshpr[k];
+        if (k < 2) {
+          lxpt[ipift[ifa][k] - 1][0] += lx;
+          lxpt[ipift[ifa][k] - 1][1] += ly;
+        } else {
+          lxptv[ipift[ifa][2] - 1][0] += lx;
+          lxptv[ipift[ifa][2] - 1][1] += ly;
+        }
+      }
+    }
+  }
+  for (int isv = 0; isv < 3; isv++)
+    for (int k = 0; k < 6; k++) {
+      lxpt[k][0] += lxptv[isv][0] * shpv[isv][k];
+      lxpt[k][1] += lxptv[isv][1] * shpv[isv][k];
+    }
+  const double posit[9][2] = {{0, 0}, {1, 0}, {1, 0}, {0, 1}, {0, 1}, {0, 0}, {0.5, 0}, {0.5, 0.5}, {0, 0.5}};
+  for (int ig = 0; ig < 9; ig++) {
+    double dspr[6], dsps[6];
+    shp6d(posit[ig][0], posit[ig][1], dspr, dsps);
+    Jac j = jac6(xpt, dspr, dsps);
+    const int g1 = ig + 1;
+    double vn0, vn1, larea;
+    if (g1 == 1 || g1 == 2 || g1 == 7) { vn0 = 0.0; vn1 = -1.0; larea = 1.0; }
+    else if (g1 == 3 || g1 == 4 || g1 == 8) { vn0 = sqrt(2.0) * 0.5; vn1 = sqrt(2.0) * 0.5; larea = sqrt(2.0); }
+    else { vn0 = -1.0; vn1 = 0.0; larea = 1.0; }
+    // v = larea (ys vn0 - yr vn1, -xs vn0 + xr vn1); n = v / |v|, A = |v|
+    const double v0 = larea * (j.ys * vn0 - j.yr * vn1), v1 = larea * (-j.xs * vn0 + j.xr * vn1);
+    const double A = sqrt(v0 * v0 + v1 * v1), iA = 1.0 / A;
+    const double n0 = v0 * iA, n1 = v1 * iA;
+    const int slot = ig < 6 ? ig : ig + 3;
+    const double ln0 = lgt[slot][0], ln1 = lgt[slot][1], lA = lgt[slot][2];
+    const double dot = ln0 * n0 + ln1 * n1;
+    const double lv0 = (ln0 - n0 * dot) * iA + lA * n0, lv1 = (ln1 - n1 * dot) * iA + lA * n1;
+    const double lys = larea * lv0 * vn0, lyr = -larea * lv0 * vn1;
+    const double lxs = -larea * lv1 * vn0, lxr = larea * lv1 * vn1;
+    for (int k = 0; k < 6; k++) {
+      lxpt[k][0] += lxr * dspr[k] + lxs * dsps[k];
+      lxpt[k][1] += lyr * dspr[k] + lys * dsps[k];
+    }
+  }
+}
+
+// transpose of the cell-average sound speed of the triangle passes (eps 1e-15)
+__host__ __device__ __forceinline__ void tri_centre_T(const double u[4][6], double g, double lrho_in, double lsd,
+                                                      double lu[4][6]) {
+  const double eps = 1.0e-15;
+  const double rhoct = 1.0 / u[0][0];
+  const double kin = u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0]);
+  const double pe = (g - 1.0) * rhoct * kin;
+  const double pctr = fmax(eps, pe);
+  const double se = g * pctr / rhoct;
+  const double sdctr = sqrt(fmax(eps, se));
+  double lrho = lrho_in, lp = 0.0;
+  if (se > eps) {
+    const double lse = lsd / (2.0 * sdctr);
+    lp += lse * g / rhoct;
+    lrho += -lse * g * pctr / (rhoct * rhoct);
+  }
+  if (pe > eps) {
+    lrho += lp * (g - 1.0) * kin;
+    lu[3][0] += lp * (g - 1.0) * rhoct;
+    lu[1][0] -= lp * (g - 1.0) * rhoct * u[1][0];
+    lu[2][0] -= lp * (g - 1.0) * rhoct * u[2][0];
+  }
+  lu[0][0] += -lrho * rhoct * rhoct;
+}
+
+// Reverse of b_tri_rhs: lR (RHS adjoint of the cell) -> adjoints of the cell
+// DOFs, the node coordinates, the new nodal velocity (tbuf v = 0, 1, 4, 5)
+// and the corner coefficients (ltcf).
+__host__ __device__ void a_tri_rhs(const Dev &d, const Adj &a, int it) {
+  if (it >= d.ntria) return;
+  const int e = it;
+  const double g = d.gamlg;
+  const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
+  const size_t nt = d.ntria;
+  double xpt[6][2];
+  load_tria(d, d.xs, d.ys, it, xpt);
+  double gt[15][3];
+  normals_tria(xpt, gt);
+  double u[4][6], lR[4][6], lu[4][6];
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) {
+      u[q][k] = Uget(d, d.Us, k, q, e);
+      lR[q][k] = a.lR[(q * NDEG + k) * d.ncell + e];
+      lu[q][k] = 0.0;
+    }
+  double lxpt[6][2], lun[6][2];
+  for (int k = 0; k < 6; k++) { lxpt[k][0] = lxpt[k][1] = 0.0; lun[k][0] = lun[k][1] = 0.0; }
+  double lgt[15][3];
+  for (int sl = 0; sl < 15; sl++) lgt[sl][0] = lgt[sl][1] = lgt[sl][2] = 0.0;
+  // face integral
+  for (int isg = 0; isg < 4; isg++)
+    for (int ivsg = 0; ivsg < 3; ivsg++) {
+      const int iv = iptsg(isg, ivsg) - 1;
+      const int pn = d.ipt[iv * d.ntria + it];
+      const double us = d.us_new[pn], vs = d.vs_new[pn];
+      double bt[6];
+      tri_basis(rc, sc, g19, g20, g21, xvt(iv), yvt(iv), bt);
+      double Lq[4];
+      for (int q = 0; q < 4; q++) {
+        Lq[q] = 0.0;
+        for (int k = 0; k < 6; k++) Lq[q] += lR[q][k] * bt[k];
+      }
+      for (int f = 0; f < 2; f++) {
+        const int code = fntsg(isg, 2 * ivsg + f);
+        const int slot = (code >= 0 ? code : -code) - 1;
+        const double sg = code >= 0 ? 1.0 : -1.0;
+        const double w = TB().wtri[isg][ivsg][f];
+        const double n0 = sg * gt[slot][0], n1 = sg * gt[slot][1], ar = gt[slot][2] * w;
+        const int cs = f + 2 * (ivsg + 3 * isg);
+        const double m = d.tcf[(0 * 24 + cs) * nt + it];
+        const double fs0 = d.tcf[(3 * 24 + cs) * nt + it] + m * us - d.tcf[(1 * 24 + cs) * nt + it];
+        const double fs1 = d.tcf[(4 * 24 + cs) * nt + it] + m * vs - d.tcf[(2 * 24 + cs) * nt + it];
+        const double lfs0 = Lq[1] + Lq[3] * us, lfs1 = Lq[2] + Lq[3] * vs;
+        lun[iv][0] += Lq[0] * n0 * ar + Lq[3] * fs0 + lfs0 * m;
+        lun[iv][1] += Lq[0] * n1 * ar + Lq[3] * fs1 + lfs1 * m;
+        a.ltcf[(0 * 24 + cs) * nt + it] = lfs0 * us + lfs1 * vs;
+        a.ltcf[(1 * 24 + cs) * nt + it] = -lfs0;
+        a.ltcf[(2 * 24 + cs) * nt + it] = -lfs1;
+        a.ltcf[(3 * 24 + cs) * nt + it] = lfs0;
+        a.ltcf[(4 * 24 + cs) * nt + it] = lfs1;
+        lgt[slot][0] += sg * Lq[0] * us * ar;
+        lgt[slot][1] += sg * Lq[0] * vs * ar;
+        lgt[slot][2] += w * Lq[0] * (us * n0 + vs * n1);
+      }
+    }
+  // volume integral (cofactor form, 7-point rule)
+  for (int ig = 0; ig < 7; ig++) {
+    const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+    double dspr[6], dsps[6];
+    shp6d(r, s, dspr, dsps);
+    Jac j = jac6(xpt, dspr, dsps);
+    const double djaco = 0.5 * wi;
+    double dbdr[6] = {0.0, 1.0 / 0.5, 0.0, 0.0, 0.0, 0.0}, dbds[6] = {0.0, 0.0, 1.0 / 0.5, 0.0, 0.0, 0.0};
+    dbdr[3] = (r - rc) / (0.5 * 0.5); dbdr[5] = (s - sc) / 0.5 / 0.5;
+    dbds[4] = (s - sc) / (0.5 * 0.5); dbds[5] = (r - rc) / 0.5 / 0.5;
+    double b[6];
+    tri_basis(rc, sc, g19, g20, g21, r, s, b);
+    double un[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < d.mdegr; k++)
+      for (int q = 0; q < 4; q++) un[q] += u[q][k] * b[k];
+    const double rhoad = 1.0 / un[0];
+    const double ke = un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]);
+    const double pres = (g - 1.0) * rhoad * ke;
+    double lp = 0.0, lua = 0.0, lva = 0.0, lxr = 0.0, lxs = 0.0, lyr = 0.0, lys = 0.0;
+    for (int k = 0; k < 6; k++) {
+      const double gd0 = j.ys * dbdr[k] - j.yr * dbds[k];
+      const double gd1 = -j.xs * dbdr[k] + j.xr * dbds[k];
+      const double f0 = gd0 * un[1] + gd1 * un[2];
+      const double lf0 = -lR[0][k] * djaco + lR[3][k] * pres * djaco;
+      lp += djaco * (lR[1][k] * gd0 + lR[2][k] * gd1 + lR[3][k] * f0);
+      const double lgd0 = lR[1][k] * pres * djaco + lf0 * un[1];
+      const double lgd1 = lR[2][k] * pres * djaco + lf0 * un[2];
+      lua += lf0 * gd0;
+      lva += lf0 * gd1;
+      lys += lgd0 * dbdr[k];
+      lyr -= lgd0 * dbds[k];
+      lxs -= lgd1 * dbdr[k];
+      lxr += lgd1 * dbds[k];
+    }
+    const double lrhoad = lp * (g - 1.0) * ke, lke = lp * (g - 1.0) * rhoad;
+    const double lq[4] = {-lrhoad * rhoad * rhoad, lua - lke * un[1], lva - lke * un[2], lke};
+    for (int k = 0; k < d.mdegr; k++)
+      for (int q = 0; q < 4; q++) lu[q][k] += lq[q] * b[k];
+    for (int k = 0; k < 6; k++) {
+      lxpt[k][0] += lxr * dspr[k] + lxs * dsps[k];
+      lxpt[k][1] += lyr * dspr[k] + lys * dsps[k];
+    }
+  }
+  if (d.ncase == 1) {
+    const double C = 0.25 * cPI / (g - 1.0);
+    for (int ig = 0; ig < 7; ig++) {
+      const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+      double shp[6], dspr[6], dsps[6];
+      shp6v(r, s, shp);
+      shp6d(r, s, dspr, dsps);
+      Jac j = jac6(xpt, dspr, dsps);
+      const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+      double xg, yg;
+      map6(xpt, shp, xg, yg);
+      double b[6];
+      tri_basis(rc, sc, g19, g20, g21, r, s, b);
+      double Ls = 0.0;
+      for (int k = 0; k < 6; k++) Ls += lR[3][k] * b[k];
+      const double c1x = cospi(xg), c1y = cospi(yg), s1x = sinpi(xg), s1y = sinpi(yg);
+      const double c3x = cospi(3.0 * xg), c3y = cospi(3.0 * yg), s3x = sinpi(3.0 * xg), s3y = sinpi(3.0 * yg);
+      const double src = C * (c3x * c1y - c3y * c1x);
+      const double dsx = C * cPI * (-3.0 * s3x * c1y + c3y * s1x);
+      const double dsy = C * cPI * (-c3x * s1y + 3.0 * s3y * c1x);
+      const double ldj = Ls * src * 0.5 * wi;
+      const double lxg = Ls * djaco * dsx, lyg = Ls * djaco * dsy;
+      const double lxr = ldj * j.ys, lys = ldj * j.xr, lyr = -ldj * j.xs, lxs = -ldj * j.yr;
+      for (int k = 0; k < 6; k++) {
+        lxpt[k][0] += lxr * dspr[k] + lxs * dsps[k] + lxg * shp[k];
+        lxpt[k][1] += lyr * dspr[k] + lys * dsps[k] + lyg * shp[k];
+      }
+    }
+  }
+  normals_tria_T(xpt, lgt, lxpt);
+  for (int k = 0; k < 6; k++) {
+    a.tbuf[(0 * 6 + k) * nt + it] = lxpt[k][0];
+    a.tbuf[(1 * 6 + k) * nt + it] = lxpt[k][1];
+    a.tbuf[(2 * 6 + k) * nt + it] = 0.0;
+    a.tbuf[(3 * 6 + k) * nt + it] = 0.0;
+    a.tbuf[(4 * 6 + k) * nt + it] = lun[k][0];
+    a.tbuf[(5 * 6 + k) * nt + it] = lun[k][1];
+  }
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) a.lU[(q * NDEG + k) * d.ncell + e] += lu[q][k];
+}
+__global__ void __launch_bounds__(128) k_a_tri_rhs(Dev d, Adj a) { a_tri_rhs(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+
+// Reverse of b_tri_corner (its normal branch: no impedance jump term, unit
+// jump factor): the adjoint of each corner coefficient is the RHS pass's
+// (ltcf) plus the node-sum adjoint lS of its node; -> adjoints of the cell
+// DOFs and node coordinates (tbuf v = 0, 1; the triangle corners do not read
+// the previous nodal velocity).
+__host__ __device__ void a_tri_corner(const Dev &d, const Adj &a, int it) {
+  if (it >= d.ntria) return;
+  const int e = it;
+  const double eps = 1.0e-15, g = d.gamlg;
+  const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
+  const size_t nt = d.ntria, np = d.npoin;
+  double xpt[6][2];
+  load_tria(d, d.xs, d.ys, it, xpt);
+  double gt[15][3];
+  normals_tria(xpt, gt);
+  double u[4][6], lu[4][6];
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) {
+      u[q][k] = Uget(d, d.Us, k, q, e);
+      lu[q][k] = 0.0;
+    }
+  const double rhomc = u[0][0], rhoct = 1.0 / rhomc;
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  double bt[6][6], unknvt[6][4];
+  for (int iv = 0; iv < 6; iv++) {
+    tri_basis(rc, sc, g19, g20, g21, xvt(iv), yvt(iv), bt[iv]);
+    for (int q = 0; q < 4; q++) {
+      unknvt[iv][q] = 0.0;
+      for (int k = 0; k < d.mdegr; k++) unknvt[iv][q] += u[q][k] * bt[iv][k];
+    }
+  }
+  // sub-cell areas f0 (= volel) and harmonic masses masel, as in the forward pass
+  const double postc[9][2] = {{0.25, 0.0}, {0.75, 0.0}, {0.75, 0.25}, {0.25, 0.75}, {0.0, 0.75},
+                              {0.0, 0.25}, {0.25, 0.25}, {0.5, 0.25}, {0.25, 0.5}};
+  const int iptsc[4][3] = {{1, 7, 6}, {8, 9, 7}, {2, 3, 8}, {9, 4, 5}};
+  double shpc[9][6], xptc[9][2];
+  for (int isc = 0; isc < 9; isc++) {
+    shp6v(postc[isc][0], postc[isc][1], shpc[isc]);
+    map6(xpt, shpc[isc], xptc[isc][0], xptc[isc][1]);
+  }
+  double f0v[4], masv[4];
+  for (int isg = 0; isg < 4; isg++) {
+    double xs[6][2];
+    for (int k = 0; k < 3; k++)
+      for (int c = 0; c < 2; c++) {
+        xs[k][c] = xpt[iptsg(isg, k) - 1][c];
+        xs[3 + k][c] = xptc[iptsc[isg][k] - 1][c];
+      }
+    double f0 = 0.0, masel = 0.0;
+    for (int ig = 0; ig < 7; ig++) {
+      const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+      const double shps[3] = {1.0 - r - s, r, s};
+      double rg = 0.0, sgp = 0.0;
+      for (int k = 0; k < 3; k++) {
+        rg += shps[k] * xvt(iptsg(isg, k) - 1);
+        sgp += shps[k] * yvt(iptsg(isg, k) - 1);
+      }
+      double b[6];
+      tri_basis(rc, sc, g19, g20, g21, rg, sgp, b);
+      double tau = 0.0;
+      for (int k = 0; k < d.mdegr; k++) tau += u[0][k] * b[k];
+      double dspr[6], dsps[6];
+      shp6d(r, s, dspr, dsps);
+      Jac j = jac6(xs, dspr, dsps);
+      const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+      f0 += djaco;
+      masel += djaco / tau;
+    }
+    f0v[isg] = f0;
+    masv[isg] = masel;
+  }
+  // corner coefficients, reversed
+  double lrho = 0.0, lsd = 0.0, lf0[4] = {0, 0, 0, 0}, lmas[4] = {0, 0, 0, 0};
+  double lunk[6][4];
+  for (int iv = 0; iv < 6; iv++)
+    for (int q = 0; q < 4; q++) lunk[iv][q] = 0.0;
+  double lgt[15][3];
+  for (int sl = 0; sl < 15; sl++) lgt[sl][0] = lgt[sl][1] = lgt[sl][2] = 0.0;
+  for (int isg = 0; isg < 4; isg++) {
+    const double tms = d.tmsub[isg * d.ntria + it];
+    for (int ivsg = 0; ivsg < 3; ivsg++) {
+      const int iv = iptsg(isg, ivsg) - 1;
+      const int pn = d.ipt[iv * d.ntria + it];
+      const double rhovt = 1.0 / unknvt[iv][0];
+      const double rhovsg = rhovt + (tms / f0v[isg] - masv[isg] / f0v[isg]);
+      const double uv = unknvt[iv][1], vv = unknvt[iv][2], ev = unknvt[iv][3];
+      const double kev = ev - 0.5 * (uv * uv + vv * vv);
+      const double pe = (g - 1.0) * rhovsg * kev;
+      const double pv = fmax(eps, pe);
+      double lpv = 0.0;
+      for (int f = 0; f < 2; f++) {
+        const int code = fntsg(isg, 2 * ivsg + f);
+        const int slot = (code >= 0 ? code : -code) - 1;
+        const double sg = code >= 0 ? 1.0 : -1.0;
+        const double w = TB().wtri[isg][ivsg][f];
+        const double n0 = sg * gt[slot][0], n1 = sg * gt[slot][1], ar = gt[slot][2] * w;
+        const int cs = f + 2 * (ivsg + 3 * isg);
+        double L[5];
+        for (int v = 0; v < 5; v++) L[v] = a.ltcf[(v * 24 + cs) * nt + it] + a.lS[v * np + pn];
+        const double m = rhoct * sdctr * ar;
+        // (m, m u, m v, -p A n0, -p A n1)
+        const double lm = L[0] + L[1] * uv + L[2] * vv;
+        lunk[iv][1] += L[1] * m;
+        lunk[iv][2] += L[2] * m;
+        lpv += -ar * (L[3] * n0 + L[4] * n1);
+        double lar = -pv * (L[3] * n0 + L[4] * n1) + lm * rhoct * sdctr;
+        lrho += lm * sdctr * ar;
+        lsd += lm * rhoct * ar;
+        lgt[slot][0] += sg * (-L[3] * pv * ar);
+        lgt[slot][1] += sg * (-L[4] * pv * ar);
+        lgt[slot][2] += w * lar;
+      }
+      if (pe > eps) {
+        const double lrs = lpv * (g - 1.0) * kev, lke = lpv * (g - 1.0) * rhovsg;
+        lunk[iv][3] += lke;
+        lunk[iv][1] -= lke * uv;
+        lunk[iv][2] -= lke * vv;
+        // rhovsg = 1/unknvt0 + (tmsub - masel) / f0
+        lunk[iv][0] += -lrs * rhovt * rhovt;
+        lf0[isg] += -lrs * (tms - masv[isg]) / (f0v[isg] * f0v[isg]);
+        lmas[isg] += -lrs / f0v[isg];
+      }
+    }
+  }
+  for (int iv = 0; iv < 6; iv++)
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < d.mdegr; k++) lu[q][k] += lunk[iv][q] * bt[iv][k];
+  tri_centre_T(u, g, lrho, lsd, lu);
+  // sub-cell quadratures, reversed
+  double lxpt[6][2], lxptc[9][2];
+  for (int k = 0; k < 6; k++) lxpt[k][0] = lxpt[k][1] = 0.0;
+  for (int k = 0; k < 9; k++) lxptc[k][0] = lxptc[k][1] = 0.0;
+  for (int isg = 0; isg < 4; isg++) {
+    double xs[6][2], lxs[6][2];
+    for (int k = 0; k < 3; k++)
+      for (int c = 0; c < 2; c++) {
+        xs[k][c] = xpt[iptsg(isg, k) - 1][c];
+        xs[3 + k][c] = xptc[iptsc[isg][k] - 1][c];
+      }
+    for (int k = 0; k < 6; k++) lxs[k][0] = lxs[k][1] = 0.0;
+    for (int ig = 0; ig < 7; ig++) {
+      const double r = cQ.t7[ig][0], s = cQ.t7[ig][1], wi = cQ.tw7[ig];
+      const double shps[3] = {1.0 - r - s, r, s};
+      double rg = 0.0, sgp = 0.0;
+      for (int k = 0; k < 3; k++) {
+        rg += shps[k] * xvt(iptsg(isg, k) - 1);
+        sgp += shps[k] * yvt(iptsg(isg, k) - 1);
+      }
+      double b[6];
+      tri_basis(rc, sc, g19, g20, g21, rg, sgp, b);
+      double tau = 0.0;
+      for (int k = 0; k < d.mdegr; k++) tau += u[0][k] * b[k];
+      double dspr[6], dsps[6];
+      shp6d(r, s, dspr, dsps);
+      Jac j = jac6(xs, dspr, dsps);
+      const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
+      const double ldj = lf0[isg] + lmas[isg] / tau;
+      const double ltau = -lmas[isg] * djaco / (tau * tau);
+      for (int k = 0; k < d.mdegr; k++) lu[0][k] += ltau * b[k];
+      const double h = 0.5 * wi * ldj;
+      const double lxr = h * j.ys, lys = h * j.xr, lyr = -h * j.xs, lxs_ = -h * j.yr;
+      for (int k = 0; k < 6; k++) {
+        lxs[k][0] += lxr * dspr[k] + lxs_ * dsps[k];
+        lxs[k][1] += lyr * dspr[k] + lys * dsps[k];
+      }
+    }
+    for (int k = 0; k < 3; k++)
+      for (int c = 0; c < 2; c++) {
+        lxpt[iptsg(isg, k) - 1][c] += lxs[k][c];
+        lxptc[iptsc[isg][k] - 1][c] += lxs[3 + k][c];
+      }
+  }
+  for (int isc = 0; isc < 9; isc++)
+    for (int k = 0; k < 6; k++) {
+      lxpt[k][0] += lxptc[isc][0] * shpc[isc][k];
+      lxpt[k][1] += lxptc[isc][1] * shpc[isc][k];
+    }
+  normals_tria_T(xpt, lgt, lxpt);
+  for (int k = 0; k < 6; k++) {
+    a.tbuf[(0 * 6 + k) * nt + it] = lxpt[k][0];
+    a.tbuf[(1 * 6 + k) * nt + it] = lxpt[k][1];
+    for (int v = 2; v < 6; v++) a.tbuf[(v * 6 + k) * nt + it] = 0.0;
+  }
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) a.lU[(q * NDEG + k) * d.ncell + e] += lu[q][k];
+}
+__global__ void __launch_bounds__(128) k_a_tri_corner(Dev d, Adj a) {
+  a_tri_corner(d, a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+void launch_tri_adjoint_rhs(const Dev &d, const Adj &a, cudaStream_t st) {
+  if (d.ntria > 0) k_a_tri_rhs<<<(d.ntria + 127) / 128, 128, 0, st>>>(d, a);
+}
+void launch_tri_adjoint_corner(const Dev &d, const Adj &a, cudaStream_t st) {
+  if (d.ntria > 0) k_a_tri_corner<<<(d.ntria + 127) / 128, 128, 0, st>>>(d, a);
+}
+
 void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa) {
   if (d.ntria) k_tri_rhs<<<nblk(d.ntria, 128), 128, 0, st>>>(d, usn, vsn, fuse, alfa);
 }
