@@ -81,6 +81,16 @@ int lag2d_create(const lag2d_mesh *mesh, const lag2d_config *cfg, lag2d_handle *
  * not NULL. */
 int lag2d_init_fields(lag2d_handle *h, double *geoel, double *amatr, double *unkno);
 
+/* Initial-condition hook: rho0(ncell) multiplies the initial density of each
+ * cell (getrhog_initial and the density of getunkin; pressure and velocity
+ * unchanged), so it enters the cell and sub-cell masses, the mass matrices
+ * and the initial DOFs that lag2d_init_fields computes, and the reference
+ * density of the physical mass centres.  Call before lag2d_init_fields;
+ * NULL restores the case's own density.  Values must be positive.  No
+ * counterpart in the reference, which reads the density from its case
+ * tables only. */
+int lag2d_set_rho0(lag2d_handle *h, const double *rho0);
+
 /* Upload a state: unkno(ndegr,nq,nsize), coord(2,npoin), ustar(2,npoin),
  * geoel(24,nsize) (fields 1-4 and 19-21 are read), amatr(nmatr,ncell).
  * geoel/amatr may be NULL to keep the device copies. */

@@ -65,7 +65,7 @@ _libs = {}
 EXPORTS = ("lag2d_create", "lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run",
            "lag2d_get_state", "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_stream",
            "lag2d_kernel_launches", "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error",
-           "lag2d_delt_noalloc", "lag2d_adjoint_step", "lag2d_adjoint")
+           "lag2d_delt_noalloc", "lag2d_adjoint_step", "lag2d_adjoint", "lag2d_set_rho0")
 
 
 def library_path(exact: bool = False) -> str:
@@ -89,7 +89,7 @@ def load(exact: bool = False):
     lib.lag2d_create.argtypes = [ctypes.POINTER(_Mesh), ctypes.POINTER(_Cfg), ctypes.POINTER(ctypes.c_void_p)]
     for name in ("lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run", "lag2d_get_state",
                  "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_timing", "lag2d_adjoint_step",
-                 "lag2d_adjoint"):
+                 "lag2d_adjoint", "lag2d_set_rho0"):
         getattr(lib, name).restype = ctypes.c_int
     lib.lag2d_destroy.argtypes = [ctypes.c_void_p]
     _libs[key] = lib
@@ -155,6 +155,15 @@ class Lag2DSolver:
         self._check(self.lib.lag2d_init_fields(self.h, _p(geoel, _dp), _p(amatr, _dp), _p(unkno, _dp)))
         self.dtfix, self.tacru, self.itime = self.cfg.dtfix, 0.0, 1
         return geoel, amatr, unkno
+
+    def set_rho0(self, rho0):
+        """Per-cell initial-density factors (ncell,) for init_fields; None
+        restores the case's density."""
+        a = None if rho0 is None else np.ascontiguousarray(rho0, dtype=np.float64).reshape(-1)
+        if a is not None and a.size != self.mesh.ncell:
+            raise ValueError("rho0 needs one value per cell")
+        self._rho0 = a
+        self._check(self.lib.lag2d_set_rho0(self.h, _p(a, _dp)))
 
     def set_state(self, unkno, coord, ustar, geoel=None, amatr=None):
         a = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None

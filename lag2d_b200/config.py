@@ -15,7 +15,7 @@ import numpy as np
 
 from .mesh import Mesh, hybrid_mesh, polar_mesh, quad_mesh
 
-__all__ = ["StepConfig", "workload", "WORKLOADS", "noh_parity_config"]
+__all__ = ["StepConfig", "workload", "WORKLOADS", "noh_parity_config", "initial_density_factors"]
 
 
 @dataclasses.dataclass
@@ -95,6 +95,13 @@ def _noh(n: int) -> Tuple[Mesh, StepConfig]:
     return m, c
 
 
+def initial_density_factors(mesh: Mesh, sigma: float = 0.01, seed: int = 5678) -> np.ndarray:
+    """Per-cell initial-density factors 1 + sigma N(0, 1) (seeded), in cell
+    order (triangles first), for lag2d_set_rho0 / Lag2DSolver.set_rho0: the
+    perturbed-density Sedov setup of the hybrid-mesh adjoint case."""
+    return 1.0 + sigma * np.random.default_rng(seed).standard_normal(mesh.ncell)
+
+
 def noh_parity_config(c: StepConfig) -> StepConfig:
     """The Noh workload with a fixed time step of 1e-4 (ndt 0).  On this
     branch the triangles at the origin are never limited (Persson and WENO
@@ -122,6 +129,8 @@ WORKLOADS = {
     "tgv_hybrid64": lambda: _tgv_hybrid(64),
     "sedov_hybrid16": lambda: _sedov_hybrid(16),
     "sedov_hybrid_jitter16": lambda: _sedov_hybrid(16, jitter=0.1),
+    # the adjoint case's mesh: 256x256, alternate rows split, nodes jittered by U(-0.1h, 0.1h)
+    "sedov_hybrid_jitter256": lambda: _sedov_hybrid(256, jitter=0.1),
     # Noh implosion on the quarter disk (triangles on the axis ring)
     "noh100": lambda: _noh(100),
     "noh16": lambda: _noh(16),

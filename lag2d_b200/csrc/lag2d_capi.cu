@@ -90,6 +90,7 @@ struct lag2d_handle {
   cudaStream_t st = nullptr;
   std::vector<void *> allocs;
   int *flags_dev = nullptr;
+  double *rho0_dev = nullptr;  // per-cell initial-density factors (lag2d_set_rho0)
   double *stage_u = nullptr;   // staging for unkno(ndegr,nq,ncell) in the caller's layout
   double *stage_x = nullptr;   // staging for coord / ustar (2,npoin)
   cudaGraphExec_t graph = nullptr;
@@ -606,6 +607,30 @@ static int download_xy(lag2d_handle *h, const double *X, const double *Y, double
   h->launches += 1;
   CK(cudaMemcpyAsync(xy, h->stage_x, 2 * (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
+  return LAG2D_OK;
+}
+
+int lag2d_set_rho0(lag2d_handle *h, const double *rho0) {
+  if (!h) return fail(LAG2D_EINVAL, "null handle");
+  Dev &d = h->d;
+  if (rho0) {
+    for (int e = 0; e < d.ncell; e++)
+      if (!(rho0[e] > 0.0)) return fail(LAG2D_EINVAL, "rho0 must be positive");
+    if (!h->rho0_dev) {
+      int r = dalloc(h, &h->rho0_dev, (size_t)d.ncell);
+      if (r) return r;
+    }
+    CK(cudaMemcpyAsync(h->rho0_dev, rho0, d.ncell * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    d.rho0 = h->rho0_dev;
+  } else {
+    d.rho0 = nullptr;
+  }
+  // the time-invariant reference-configuration masses lag2d_create computed
+  // (sub-cell masses, mass-weighted shape moments) follow the new density
+  run(h, "init", [&] { launch_init_msub(d, h->st); launch_init_wmom(d, h->st); launch_tri_init(d, h->st); },
+      2 + (d.ntria > 0));
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
   return LAG2D_OK;
 }
 

@@ -40,6 +40,7 @@ struct Dev {
   const int *node_cf;      // corner-face ids iq*32 + slot, reference summation order
   const unsigned char *bcmask;  // [npoin] bit0: u=0, bit1: v=0, bit2: keep (no solve)
   const double *x0, *y0;   // initial coordinates
+  const double *rho0;      // [ncell] caller's initial-density factor per cell, or null (1)
   // geometry (time invariant except vol / vcx / vcy)
   double *rc, *sc, *mass, *g19, *g20, *g21;
   double *vol, *vcx, *vcy;

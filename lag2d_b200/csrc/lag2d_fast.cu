@@ -808,10 +808,10 @@ __host__ __device__ void f_init_wmom(const Dev &d, int iq) {
   }
   detpoly(c, D);
   // initial density of the reference cases is uniform per cell
-  double rho0 = 1.0;
+  double rho0 = d.rho0 ? d.rho0[iq + d.ntria] : 1.0;
   if (d.ncase == 6) {
     const double xc = L.X[1][1], yc = L.Y[1][1];
-    rho0 = (sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125;
+    rho0 *= (sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125;
   }
   double W[3][3];
 #pragma unroll

@@ -137,9 +137,12 @@ __host__ __device__ __forceinline__ double Uget(const Dev &d, const double *U, i
   return U[(q * NDEG + k) * d.ncell + e];
 }
 
-__host__ __device__ __forceinline__ double rho_initial(const Dev &d, double xc, double yc) {
-  if (d.ncase == 6) return (sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125;
-  return 1.0;
+// initial density of cell e (getrhog_initial, GetInitial.f90:4-147: uniform per
+// cell in the cases built here), times the caller's per-cell factor if set
+__host__ __device__ __forceinline__ double rho_initial(const Dev &d, int e, double xc, double yc) {
+  const double f = d.rho0 ? d.rho0[e] : 1.0;
+  if (d.ncase == 6) return f * ((sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125);
+  return f;
 }
 
 __host__ __device__ __forceinline__ bool stopped(const Dev &d) { return d.sc_dev->done != 0; }
@@ -238,7 +241,7 @@ __host__ __device__ void b_persson(const Dev &d, int iq) {
     double xgi, ygi, xg, yg;
     map9(xpi, shp, xgi, ygi);
     map9(xp, shp, xg, yg);
-    double rhogi = rho_initial(d, xcrho, ycrho);
+    double rhogi = rho_initial(d, e, xcrho, ycrho);
     xmc = xmc + rhogi * djacoi * xg;
     ymc = ymc + rhogi * djacoi * yg;
   }
@@ -401,7 +404,7 @@ __host__ __device__ void weno_points(const Dev &d, int jelem, const double *mp, 
   double xcrho, ycrho;
   shp9v(d.rc[jelem], d.sc[jelem], shp);
   map9(xpqi, shp, xcrho, ycrho);
-  const double rhogi = rho_initial(d, xcrho, ycrho);
+  const double rhogi = rho_initial(d, jelem, xcrho, ycrho);
   for (int ig = 0; ig < 25; ig++) {
     double r = cQ.g25[ig][0], s = cQ.g25[ig][1], wi = cQ.w25[ig];
     shp9v(r, s, shp);
@@ -1319,6 +1322,7 @@ __host__ __device__ void getunkin(const Dev &d, double *unkin, double xg, double
     for (int i = 0; i < d.nsedov; i++) hit |= (d.sedov_cell[i] == ielem1);
     pini = hit ? (g - 1.0) * 1.0 * d.sedov_energy / (1.0 * volel) : 1.0e-6;
   }
+  if (d.rho0) rhoini *= d.rho0[ielem1 - 1];  // per-cell density factor at fixed p, u, v
   unkin[0] = 1.0;
   unkin[1] = rhoini * uini;
   unkin[2] = rhoini * vini;
@@ -1343,7 +1347,7 @@ __host__ __device__ void b_init_geo(const Dev &d, int iq) {
     double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
     double xg, yg;
     map9(xp, shp, xg, yg);
-    double rhog = rho_initial(d, xc, yc);
+    double rhog = rho_initial(d, e, xc, yc);
     double rcoef = 1.0 - alfrz + alfrz * yg;
     masel = masel + rhog * djaco * rcoef;
     volel = volel + djaco * rcoef;
@@ -1370,7 +1374,7 @@ __host__ __device__ void b_init_geo(const Dev &d, int iq) {
     double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
     double xg, yg;
     map9(xp, shp, xg, yg);
-    double rhog = rho_initial(d, xc, yc);
+    double rhog = rho_initial(d, e, xc, yc);
     double rcoef = 1.0 - alfrz + alfrz * yg;
     bq[1] = (r - rc) / 1.0;
     bq[2] = (s - sc) / 1.0;
@@ -1420,7 +1424,7 @@ __host__ __device__ void b_init_msub(const Dev &d, int iq) {
         shp9d(cQ.g25[ig][0], cQ.g25[ig][1], dr, ds);
         Jac j = jac9(xs, dr, ds);
         double djaco = cQ.w25[ig] * (j.xr * j.ys - j.yr * j.xs);
-        double rhoi = rho_initial(d, xci, yci);
+        double rhoi = rho_initial(d, iq + d.ntria, xci, yci);
         rhs = rhs + rhoi * 1.0 * djaco;
       }
       d.msub[isg * d.nquad + iq] = rhs;
@@ -1505,7 +1509,7 @@ __host__ __device__ void b_init_fields(const Dev &d, int iq) {
     bq[5] = bq[1] * bq[2] - d.g21[e];
     for (int q = 0; q < 4; q++)
       for (int k = 0; k < 6; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bq[k] * djaco;
-    double rho0 = rho_initial(d, xc, yc);
+    double rho0 = rho_initial(d, e, xc, yc);
     double rcoef = 1.0 - alfrz + alfrz * yg;
     f0 = f0 + rho0 * djaco * rcoef;
     for (int ix = 0; ix < 5; ix++)
@@ -1687,7 +1691,7 @@ __host__ __device__ void b_tri_init(const Dev &d, int it) {
     const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
     double xg, yg;
     map6(xp, shp, xg, yg);
-    const double rhog = rho_initial(d, xc, yc);
+    const double rhog = rho_initial(d, e, xc, yc);
     const double rcoef = 1.0 - alfrz + alfrz * yg;
     masel = masel + rhog * djaco * rcoef;
     volel = volel + djaco * rcoef;
@@ -1710,7 +1714,7 @@ __host__ __device__ void b_tri_init(const Dev &d, int it) {
     const double djaco = 0.5 * wi * (j.xr * j.ys - j.yr * j.xs);
     double xg, yg;
     map6(xp, shp, xg, yg);
-    const double rhog = rho_initial(d, xc, yc);
+    const double rhog = rho_initial(d, e, xc, yc);
     const double rcoef = 1.0 - alfrz + alfrz * yg;
     bt[1] = (r - rc) / 0.5;
     bt[2] = (s - sc) / 0.5;
@@ -1758,7 +1762,7 @@ __host__ __device__ void b_tri_init(const Dev &d, int it) {
     getunkin(d, unkin, xg, yg, e + 1, volel, xc, yc);
     for (int q = 0; q < 4; q++)
       for (int k = 0; k < 6; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * b[k] * djaco;
-    const double rho0 = rho_initial(d, xc, yc);
+    const double rho0 = rho_initial(d, e, xc, yc);
     const double rcoef = 1.0 - alfrz + alfrz * yg;
     f0 = f0 + rho0 * djaco * rcoef;
     for (int ix = 0; ix < 5; ix++)
@@ -1804,7 +1808,7 @@ __host__ __device__ void b_tri_init(const Dev &d, int it) {
         shp6d(cQ.t7[ig][0], cQ.t7[ig][1], dspr, dsps);
         Jac j = jac6(xs, dspr, dsps);
         const double djaco = 0.5 * cQ.tw7[ig] * (j.xr * j.ys - j.yr * j.xs);
-        rhs = rhs + rho_initial(d, xci, yci) * 1.0 * djaco;
+        rhs = rhs + rho_initial(d, e, xci, yci) * 1.0 * djaco;
       }
       d.tmsub[isg * d.ntria + it] = rhs;
     }

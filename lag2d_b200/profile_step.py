@@ -12,7 +12,7 @@ from __future__ import annotations
 import argparse
 
 from .api import Lag2DSolver
-from .config import workload
+from .config import initial_density_factors, workload
 
 
 def main():
@@ -20,11 +20,15 @@ def main():
     ap.add_argument("workload", nargs="?", default="tgv256")
     ap.add_argument("steps", nargs="?", type=int, default=2)
     ap.add_argument("--mixed", action="store_true", help="FP32-mixed form (precision = 1)")
+    ap.add_argument("--rho0", action="store_true",
+                    help="per-cell initial densities 1 + 0.01 N(0, 1) (seed 5678) before the initial fields")
     ap.add_argument("--adjoint", type=int, default=0, metavar="K",
                     help="run lag2d_adjoint over the steps with checkpoints every K steps")
     a = ap.parse_args()
     m, c = workload(a.workload)
     s = Lag2DSolver(m, c, precision=1 if a.mixed else 0)
+    if a.rho0:
+        s.set_rho0(initial_density_factors(m))
     s.init_fields()
     if a.adjoint > 0:
         J, _, _, _, ms = s.adjoint(a.steps, a.adjoint)

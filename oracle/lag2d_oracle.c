@@ -238,10 +238,11 @@ static void getinvmat(int n, double *a, double *x) {
 /* Initial condition tables: getrhog_initial (GetInitial.f90:4-147) and   */
 /* getunkin (Getrhslagmc.f90:5527-5844), ideal-gas cases used here.      */
 /* ---------------------------------------------------------------------- */
-static double rho_initial(const o_cfg *c, double xg, double yg, double xc, double yc) {
+static double rho_initial(const o_cfg *c, int ielem, double xg, double yg, double xc, double yc) {
   (void)xg; (void)yg;
-  if (c->ncase == 6) return (sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125;
-  return 1.0;  /* TGV (1), shockless Noh (2), Noh (3), Sedov (7) */
+  const double f = c->rho0 ? c->rho0[ielem] : 1.0;  /* caller's per-cell factor (0-based cell) */
+  if (c->ncase == 6) return f * ((sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125);
+  return f;  /* TGV (1), shockless Noh (2), Noh (3), Sedov (7) */
 }
 
 static int is_sedov_cell(const o_cfg *c, int ielem1) {
@@ -285,6 +286,7 @@ static void getunkin(const o_cfg *c, double *unkin, double xg, double yg,
       fprintf(stderr, "oracle: unsupported ncase %d\n", c->ncase);
       abort();
   }
+  if (c->rho0) rhoini *= c->rho0[ielem1 - 1];  /* per-cell density factor at fixed p, u, v */
   unkin[0] = 1.0;
   unkin[1] = rhoini * uini;
   unkin[2] = rhoini * vini;
@@ -335,7 +337,7 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
       jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
       double djaco = wi * (a * d - cc * b);
       map9((const double(*)[2])xp, shp, &xg, &yg);
-      double rhog = rho_initial(c, xg, yg, xc, yc);
+      double rhog = rho_initial(c, ielem, xg, yg, xc, yc);
       double rcoef = 1.0 - alfrz + alfrz * yg;
       masel = masel + rhog * djaco * rcoef;
       volel = volel + djaco * rcoef;
@@ -377,7 +379,7 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
         jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
         double djaco = wi * (a * d - cc * b);
         map9((const double(*)[2])xp, shp, &xg, &yg);
-        double rhog = rho_initial(c, xg, yg, xc, yc);
+        double rhog = rho_initial(c, ielem, xg, yg, xc, yc);
         double rcoef = 1.0 - alfrz + alfrz * yg;
         bq[0] = 1.0;
         bq[1] = (r - rc) / 1.0;
@@ -458,7 +460,7 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
       }
       for (int q = 0; q < 4; q++)
         for (int k = 0; k < nd; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bq[k] * djaco;
-      double rho0 = rho_initial(c, xg, yg, xc, yc);
+      double rho0 = rho_initial(c, ielem, xg, yg, xc, yc);
       double rcoef = 1.0 - alfrz + alfrz * yg;
       f0 = f0 + rho0 * djaco * rcoef;
       for (int ix = 0; ix < nb; ix++)
@@ -748,7 +750,7 @@ static void weno_cell_points(const weno_ctx *w, int jelem, const double *mapmt,
     double djacoi = wi * (a * d - cc * b);
     map9((const double(*)[2])xpqi, shp, &xgi, &ygi);
     map9((const double(*)[2])xpql, shp, &xg, &yg);
-    double rhogi = rho_initial(w->c, xgi, ygi, xcrho, ycrho);
+    double rhogi = rho_initial(w->c, jelem, xgi, ygi, xcrho, ycrho);
     rhodj[ig] = rhogi * djacoi;
     xl[ig] = xg; yl[ig] = yg;
   }
@@ -1081,7 +1083,7 @@ static void weno(const o_mesh *m, const o_cfg *c, double *unkno, const double *g
       double djacoi = wi * (a * d - cc * b);
       map9((const double(*)[2])xpi, shp, &xgi, &ygi);
       map9((const double(*)[2])xp, shp, &xg, &yg);
-      double rhogi = rho_initial(c, xgi, ygi, xcrho, ycrho);
+      double rhogi = rho_initial(c, ielem, xgi, ygi, xcrho, ycrho);
       xmc = xmc + rhogi * djacoi * xg;
       ymc = ymc + rhogi * djacoi * yg;
     }
@@ -1119,7 +1121,7 @@ static const int IPQSG[4][4] = {{1, 5, 9, 8}, {5, 2, 6, 9}, {9, 6, 3, 7}, {8, 9,
 
 /* getrhosubg_averg, Getrhslaggauss.f90:7067-7395: initial sub-cell mass
  * over current sub-cell volume. */
-static void rhosubg_averg(const o_cfg *c, const double (*xpq)[2], const double (*xpqi)[2],
+static void rhosubg_averg(const o_cfg *c, int ielem, const double (*xpq)[2], const double (*xpqi)[2],
                           double *unksgq) {
   static const double posqc[12][2] = {{-0.5, -1.0}, {0.5, -1.0}, {1.0, -0.5}, {1.0, 0.5},
                                       {0.5, 1.0}, {-0.5, 1.0}, {-1.0, 0.5}, {-1.0, -0.5},
@@ -1169,7 +1171,7 @@ static void rhosubg_averg(const o_cfg *c, const double (*xpq)[2], const double (
       shp9(pos[ig][0], pos[ig][1], NULL, dr, ds);
       jac9((const double(*)[2])xs, dr, ds, &a, &b, &cc, &d);
       double djaco = wt[ig] * (a * d - cc * b);
-      double rhoi = rho_initial(c, 0, 0, xci, yci);
+      double rhoi = rho_initial(c, ielem, 0, 0, xci, yci);
       rhs = rhs + rhoi * 1.0 * djaco;
     }
     unksgq[isg] = 0.0 + matin[isg] * rhs;
@@ -1284,7 +1286,7 @@ static void riem_quad(const o_mesh *m, const o_cfg *c, int ie, const double *geo
   load_quad(m, coord, ie, xpq);
   load_quad(m, coold, ie, xpqi);
   double unksgq[4], uqsgc[4];
-  rhosubg_averg(c, (const double(*)[2])xpq, (const double(*)[2])xpqi, unksgq);
+  rhosubg_averg(c, ielem, (const double(*)[2])xpq, (const double(*)[2])xpqi, unksgq);
   double u1[6];
   for (int k = 0; k < c->ndegr; k++) u1[k] = U_(unkno, c, k, 0, ielem);
   rhosubg_daverg(c, rc, sc, &G_(geoel, 18, ielem), (const double(*)[2])xpq, u1, 1.0, uqsgc);
@@ -1489,7 +1491,7 @@ static void init_tria(const o_mesh *m, const o_cfg *c, const double *coord, doub
       jac6((const double(*)[2])xp, dspr, dsps, &a, &b, &cc, &d);
       double djaco = 0.5 * wi * (a * d - cc * b);
       map6((const double(*)[2])xp, shp, &xg, &yg);
-      double rhog = rho_initial(c, xg, yg, xc, yc);
+      double rhog = rho_initial(c, ielem, xg, yg, xc, yc);
       double rcoef = 1.0 - alfrz + alfrz * yg;
       masel = masel + rhog * djaco * rcoef;
       volel = volel + djaco * rcoef;
@@ -1529,7 +1531,7 @@ static void init_tria(const o_mesh *m, const o_cfg *c, const double *coord, doub
         jac6((const double(*)[2])xp, dspr, dsps, &a, &b, &cc, &d);
         double djaco = 0.5 * wi * (a * d - cc * b);
         map6((const double(*)[2])xp, shp, &xg, &yg);
-        double rhog = rho_initial(c, xg, yg, xc, yc);
+        double rhog = rho_initial(c, ielem, xg, yg, xc, yc);
         double rcoef = 1.0 - alfrz + alfrz * yg;
         bt[0] = 1.0;
         bt[1] = (r - rc) / dr;
@@ -1605,7 +1607,7 @@ static void init_tria(const o_mesh *m, const o_cfg *c, const double *coord, doub
       getunkin(c, unkin, xg, yg, ielem + 1, volel, xc, yc);
       for (int q = 0; q < 4; q++)
         for (int k = 0; k < ndg; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bt[k] * djaco;
-      double rho0 = rho_initial(c, xg, yg, xc, yc);
+      double rho0 = rho_initial(c, ielem, xg, yg, xc, yc);
       double rcoef = 1.0 - alfrz + alfrz * yg;
       f0 = f0 + rho0 * djaco * rcoef;
       for (int ix = 0; ix < nb; ix++)
@@ -1737,7 +1739,7 @@ static double wfgst_tria(int isg, int ivsg, int f) {
 /* getrhosubgt_average2 (Getrhslaggauss.f90:12595-12945): sub-cell density
  * (initial sub-cell mass / current sub-cell volume) and the harmonic mean
  * of the DG specific volume over each of the 4 sub-triangles. */
-static void rhosubgt_average2(const o_cfg *c, double rc, double sc, const double *btho,
+static void rhosubgt_average2(const o_cfg *c, int ielem, double rc, double sc, const double *btho,
                               const double (*xpt)[2], const double (*xpti)[2], const double *u1,
                               double aflim1, double *unksgt, double *utsgc) {
   static const double postc[9][2] = {{0.25, 0.0}, {0.75, 0.0}, {0.75, 0.25}, {0.25, 0.75}, {0.0, 0.75},
@@ -1810,7 +1812,7 @@ static void rhosubgt_average2(const o_cfg *c, double rc, double sc, const double
       double djaco = 0.5 * wi * (a * d - cc * b);
       /* getrhoig_triacurv2 (Getrhslag.f90:17622): the cases built here
        * have a density that depends on the parent's initial centroid only */
-      double rhoi = rho_initial(c, 0, 0, xci, yci);
+      double rhoi = rho_initial(c, ielem, 0, 0, xci, yci);
       rhs = rhs + rhoi * 1.0 * djaco;
     }
     unksgt[isg] = 0.0 + matin[isg] * rhs;
@@ -1847,7 +1849,7 @@ static void riem_tria(const o_mesh *m, const o_cfg *c, int it, const double *geo
   load_tria(m, coold, it, xpti);
   double unksgt[4], utsgc[4], u1[6];
   for (int k = 0; k < c->ndegr; k++) u1[k] = U_(unkno, c, k, 0, ielem);
-  rhosubgt_average2(c, ge[0], ge[1], ge + 18, (const double(*)[2])xpt, (const double(*)[2])xpti, u1, 1.0,
+  rhosubgt_average2(c, ielem, ge[0], ge[1], ge + 18, (const double(*)[2])xpt, (const double(*)[2])xpti, u1, 1.0,
                     unksgt, utsgc);
   for (int isg = 0; isg < 4; isg++) {
     double vn[3][2][3];

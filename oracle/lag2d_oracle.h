@@ -49,6 +49,7 @@ typedef struct {
   int sedov_ncell, sedov_cell[4];  /* 1-based ids that receive the Sedov energy */
   double gamlg, cfl, cdrho, cimpd, tend;
   double sedov_energy;         /* 0.244816 in the reference */
+  const double *rho0;          /* (ncell) initial-density factor per cell, or NULL (1) */
 } o_cfg;
 
 /* Initial geometry, mass matrix and DOFs: getgeoel_initial_lag,

@@ -34,7 +34,7 @@ class _OCfg(ctypes.Structure):
                 ("sedov_ncell", ctypes.c_int), ("sedov_cell", ctypes.c_int * 4),
                 ("gamlg", ctypes.c_double), ("cfl", ctypes.c_double), ("cdrho", ctypes.c_double),
                 ("cimpd", ctypes.c_double), ("tend", ctypes.c_double),
-                ("sedov_energy", ctypes.c_double)]
+                ("sedov_energy", ctypes.c_double), ("rho0", ctypes.POINTER(ctypes.c_double))]
 
 
 def build() -> str:
@@ -54,14 +54,16 @@ def lib():
 
 
 def _p(a, t):
-    return a.ctypes.data_as(t)
+    return None if a is None else a.ctypes.data_as(t)
 
 
 class Oracle:
     """Holds a mesh and a configuration; methods mirror the reference routines."""
 
-    def __init__(self, mesh, cfg):
+    def __init__(self, mesh, cfg, rho0=None):
+        """rho0: optional per-cell initial-density factors (ncell,)."""
         self.mesh, self.cfg = mesh, cfg
+        self._rho0 = None if rho0 is None else np.ascontiguousarray(rho0, dtype=np.float64).reshape(-1)
         self._keep = [np.ascontiguousarray(a, dtype=np.int32) for a in
                       (mesh.iptri, mesh.ipqua, mesh.bface, mesh.esuv1, mesh.esuv2, mesh.esqua)]
         k = self._keep
@@ -71,7 +73,8 @@ class Oracle:
         sc = (ctypes.c_int * 4)(*(list(cfg.sedov_cells) + [0, 0, 0, 0])[:4])
         self.oc = _OCfg(cfg.npoly, cfg.ndegr, cfg.mdegr, cfg.nq, cfg.nstag, cfg.ndt, cfg.ncase,
                         cfg.nlimi, 1, cfg.ngausd, cfg.ngausd_geo, len(cfg.sedov_cells), sc,
-                        cfg.gamlg, cfg.cfl, cfg.cdrho, cfg.cimpd, cfg.tend, cfg.sedov_energy)
+                        cfg.gamlg, cfg.cfl, cfg.cdrho, cfg.cimpd, cfg.tend, cfg.sedov_energy,
+                        _p(self._rho0, _dp))
 
     # arrays are returned in C order with the Fortran memory layout:
     #   unkno (nsize, nq, ndegr), geoel (nsize, 24), amatr (ncell, nmatr), coord (npoin, 2)

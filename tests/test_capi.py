@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _declared():
     txt = open(os.path.join(ROOT, "include", "lag2d.h")).read()
-    return sorted(set(re.findall(r"\b(lag2d_[a-z_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(lag2d_[a-z0-9_]+)\s*\(", txt)))
 
 
 @pytest.mark.parametrize("exact", [False, True])

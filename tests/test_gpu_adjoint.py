@@ -200,12 +200,15 @@ def test_autograd_function_chain(case):
 
 
 def test_adjoint_hybrid_sedov_window():
-    """Sedov on the jittered tri/quad mesh: the Persson sensor marks quads,
+    """Sedov on the jittered tri/quad mesh with per-cell initial densities
+    1 + 0.01 N(0, 1): the Persson sensor marks quads,
     but WENO replaces none (every quad's 3x3 stencil reaches a triangle), so
     a 2-step window is differentiable; its gradients are finite and do not
     depend on the checkpoint interval."""
+    from lag2d_b200.config import initial_density_factors
     m, c = workload("sedov_hybrid_jitter16")
     s = Lag2DSolver(m, dataclasses.replace(c, ndt=0))
+    s.set_rho0(initial_density_factors(m))
     g, a, u = s.init_fields()
     out = []
     for K in (1, 2):

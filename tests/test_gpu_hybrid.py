@@ -129,3 +129,39 @@ def test_hybrid_mixed_steps(name):
         rel = np.abs(u2[:n, :, 0] - unkno[:n, :, 0]) / np.maximum(np.abs(unkno[:n, :, 0]), 1e-300)
         scl = np.abs(u2[:n, :, 0] - unkno[:n, :, 0]) / np.abs(unkno[:n, :, 0]).max(axis=0)
         assert np.minimum(rel, scl).max() < 1e-6, it
+
+
+@pytest.mark.parametrize("ordex", [False, True])
+def test_initial_density_factors_init_and_steps(ordex):
+    """Per-cell initial-density factors (lag2d_set_rho0) on the jittered
+    Sedov tri/quad mesh: initial fields and the first step against the oracle
+    with the same factors (bounds as above; bit for bit in the reference-order
+    build).  One step: at the second CFL step this case collapses (negative
+    cell volumes of order -1e8) in the oracle too, where the device path
+    reports LAG2D_ENONPHYS."""
+    from lag2d_b200.config import initial_density_factors
+    m, c = workload("sedov_hybrid_jitter16")
+    f = initial_density_factors(m)
+    o = Oracle(m, c, rho0=f)
+    geoel, amatr, unkno = o.init()
+    s = Lag2DSolver(m, c, exact=ordex, order_exact=ordex)
+    s.set_rho0(f)
+    g2, a2, u2 = s.init_fields()
+    n = m.ncell
+    tol = 1e-14 if ordex else 1e-12
+    assert np.abs(g2[:n, 3] - geoel[:n, 3]).max() / np.abs(geoel[:n, 3]).max() < tol * 10
+    assert np.abs(a2 - amatr).max() / np.abs(amatr).max() < tol * 100
+    assert _field_err(u2[:n], unkno[:n]).max() < tol * 100
+    s.set_state(unkno, m.coord, np.zeros_like(m.coord), geoel, amatr)
+    coord = m.coord.copy()
+    ustar = np.zeros_like(coord)
+    dt, ta = c.dtfix, 0.0
+    for it in range(1, 2):
+        _, dt, ta = o.run(unkno, coord, m.coord, geoel, amatr, ustar, it, 1, dt, ta)
+        s.step()
+        u3, x3, _, _ = s.get_state()
+        rel = np.abs(u3[:n, :, 0] - unkno[:n, :, 0]) / np.maximum(np.abs(unkno[:n, :, 0]), 1e-300)
+        scl = np.abs(u3[:n, :, 0] - unkno[:n, :, 0]) / np.abs(unkno[:n, :, 0]).max(axis=0)
+        assert np.minimum(rel, scl).max() < 1e-12, it
+        if ordex:
+            assert np.array_equal(u3[:n], unkno[:n]) and np.array_equal(x3, coord)

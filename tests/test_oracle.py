@@ -242,3 +242,21 @@ def test_polar_mesh_geometry():
     # the Noh state: inward unit velocity, p = 1e-6
     u, v = unkno[:n, 1, 0], unkno[:n, 2, 0]
     assert np.abs(np.hypot(u, v) - 1.0).max() < 0.05
+
+
+def test_initial_density_factors():
+    """The per-cell initial-density hook scales the cell mass (uniform base
+    density), keeps the volumes, and sets tau = 1/rho0 in the cell averages
+    while pressure and velocity stay those of the case."""
+    from lag2d_b200.config import initial_density_factors
+    m, c = workload("sedov_hybrid_jitter16")
+    f = initial_density_factors(m)
+    g0, a0, u0 = Oracle(m, c).init()
+    g1, a1, u1 = Oracle(m, c, rho0=f).init()
+    n = m.ncell
+    assert np.allclose(g1[:n, 2], g0[:n, 2], rtol=1e-14, atol=0)
+    assert np.allclose(g1[:n, 3], f * g0[:n, 3], rtol=1e-13, atol=0)
+    assert np.allclose(u1[:n, 0, 0], u0[:n, 0, 0] / f, rtol=1e-13, atol=0)
+    p0 = (c.gamlg - 1.0) / u0[:n, 0, 0] * (u0[:n, 3, 0] - 0.5 * (u0[:n, 1, 0] ** 2 + u0[:n, 2, 0] ** 2))
+    p1 = (c.gamlg - 1.0) / u1[:n, 0, 0] * (u1[:n, 3, 0] - 0.5 * (u1[:n, 1, 0] ** 2 + u1[:n, 2, 0] ** 2))
+    assert np.allclose(p1, p0, rtol=1e-11, atol=1e-17)
