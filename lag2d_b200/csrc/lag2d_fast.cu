@@ -40,14 +40,11 @@ struct FastTables {
   double dl[9];       // L'_c at r = -1, 0, 1: dl[3a + c]
   double xv[9], yv[9];  // reference coordinates of the 9 nodes
 };
-__constant__ FastTables cFT = LAG2D_FAST_TABLES;
-static const FastTables hFT = LAG2D_FAST_TABLES;
+// compile-time tables: lookups with indices known after unrolling fold to
+// constants (no constant-bank loads, no branches on the looked-up values)
 __host__ __device__ __forceinline__ const FastTables &FT() {
-#ifdef __CUDA_ARCH__
-  return cFT;
-#else
-  return hFT;
-#endif
+  static constexpr FastTables t = LAG2D_FAST_TABLES;
+  return t;
 }
 
 // 1-D quadratic Lagrange basis on {-1, 0, 1} and its derivative
@@ -409,7 +406,7 @@ __host__ __device__ void f_corner(const Dev &d, int iq) {
     d.corr[isg * (size_t)d.nquad + iq] = corr[isg];
   }
   // per node: vertex state, then its corner faces in the reference's order
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < 9; k++) {
     double b[6];
     node_basis2(G, k, b);
@@ -428,7 +425,7 @@ __host__ __device__ void f_corner(const Dev &d, int iq) {
     const double dux = d.us[pn] - st[1];
     const double duy = d.vs[pn] - st[2];
     double P0 = 0.0, P1 = 0.0, P2 = 0.0, P3 = 0.0, P4 = 0.0;
-#pragma unroll 1
+#pragma unroll
     for (int i = nc_start(k); i < nc_start(k + 1); i++) {
       const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
       const double ci = isg == 0 ? corr[0] : isg == 1 ? corr[1] : isg == 2 ? corr[2] : corr[3];
@@ -512,7 +509,7 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
   const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
   double ul[6] = {0, 0, 0, 0, 0, 0}, p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
   // face integral: corner forces F* = sigma.n A + m (u* - u_c), node by node
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < 9; k++) {
     double b[6];
     node_basis2(G, k, b);
@@ -532,7 +529,7 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
     const double un = d.us_new[pn], vn = d.vs_new[pn];
     const double du0 = un - st[1], du1 = vn - st[2];
     double tw = 0.0, f0 = 0.0, f1 = 0.0, fe = 0.0;
-#pragma unroll 1
+#pragma unroll
     for (int i = nc_start(k); i < nc_start(k + 1); i++) {
       const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
       const double pv = fmax(eps, (g - 1.0) * (rhovt + d.corr[isg * (size_t)d.nquad + iq]) * ke);

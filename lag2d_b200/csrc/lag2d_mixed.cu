@@ -47,7 +47,11 @@ struct MixTables {
   float dl[9];
   float xv[9], yv[9];
 };
-__constant__ MixTables cMT = LAG2D_FAST_TABLES;
+// compile-time tables (lookups fold to constants once the loops are unrolled)
+__device__ __forceinline__ const MixTables &MT() {
+  static constexpr MixTables t = LAG2D_FAST_TABLES;
+  return t;
+}
 
 __device__ __forceinline__ void lag3f(float r, float *l) {
   l[0] = 0.5f * r * (r - 1.0f);
@@ -111,8 +115,8 @@ struct GeoF {
 
 __device__ __forceinline__ void node_basis(const GeoF &g, int iv, float *b) {
   b[0] = 1.0f;
-  b[1] = cMT.xv[iv] - g.rc;
-  b[2] = cMT.yv[iv] - g.sc;
+  b[1] = MT().xv[iv] - g.rc;
+  b[2] = MT().yv[iv] - g.sc;
   b[3] = 0.5f * b[1] * b[1] - g.g19;
   b[4] = 0.5f * b[2] * b[2] - g.g20;
   b[5] = b[1] * b[2] - g.g21;
@@ -131,7 +135,10 @@ struct MixTablesD {
   double dl[9];
   double xv[9], yv[9];
 };
-__constant__ MixTablesD cMD = LAG2D_FAST_TABLES;
+__device__ __forceinline__ const MixTablesD &MD() {
+  static constexpr MixTablesD t = LAG2D_FAST_TABLES;
+  return t;
+}
 
 // Unnormalised face vector an of gesgq slot `slot` in FP64 (unit normal
 // an / |an|, face length 2 |an|; getfnds_lagsms_simpsonhybrid and
@@ -165,8 +172,8 @@ __device__ __forceinline__ void slot_an(const double X[3][3], const double Y[3][
     return;
   }
   const int ig = slot < 8 ? slot : slot - 4;
-  const int ia = cMD.pa[ig], ib = cMD.pb[ig];
-  const double *da = cMD.dl + 3 * ia, *db = cMD.dl + 3 * ib;
+  const int ia = MD().pa[ig], ib = MD().pb[ig];
+  const double *da = MD().dl + 3 * ia, *db = MD().dl + 3 * ib;
   double xa0, xa1, xa2, ya0, ya1, ya2, xb0, xb1, xb2, yb0, yb1, yb2;
   if (ib == 0) { xa0 = X[0][0]; xa1 = X[1][0]; xa2 = X[2][0]; ya0 = Y[0][0]; ya1 = Y[1][0]; ya2 = Y[2][0]; }
   else if (ib == 1) { xa0 = X[0][1]; xa1 = X[1][1]; xa2 = X[2][1]; ya0 = Y[0][1]; ya1 = Y[1][1]; ya2 = Y[2][1]; }
@@ -178,7 +185,7 @@ __device__ __forceinline__ void slot_an(const double X[3][3], const double Y[3][
   const double yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
   const double xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
   const double ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
-  switch (cMD.side[ig]) {
+  switch (MD().side[ig]) {
     case 0: ax = yr; ay = -xr; break;
     case 1: ax = ys; ay = -xs; break;
     case 2: ax = -yr; ay = xr; break;
@@ -188,7 +195,7 @@ __device__ __forceinline__ void slot_an(const double X[3][3], const double Y[3][
 
 __device__ __forceinline__ void corner_an(const double X[3][3], const double Y[3][3], int isg, int ivsg, int f,
                                           double &ax, double &ay) {
-  const int code = cMD.fnqsg[8 * isg + 2 * ivsg + f];
+  const int code = MD().fnqsg[8 * isg + 2 * ivsg + f];
   const int slot = (code >= 0 ? code : -code) - 1;
   slot_an(X, Y, slot, ax, ay);
   if (code < 0) { ax = -ax; ay = -ay; }
@@ -325,7 +332,7 @@ __device__ void m_corner(const Dev &d, int iq) {
     d.corr[isg * (size_t)d.nquad + iq] = cr;
     corr[isg] = (float)cr;
   }
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < 9; k++) {
     float b[6], st[4];
     node_basis(G, k, b);
@@ -336,9 +343,9 @@ __device__ void m_corner(const Dev &d, int iq) {
     const float dux = (float)d.us[pn] - st[1];
     const float duy = (float)d.vs[pn] - st[2];
     double P0 = 0.0, P1 = 0.0, P2 = 0.0, P3 = 0.0, P4 = 0.0;
-#pragma unroll 1
-    for (int i = cMT.nc_start[k]; i < cMT.nc_start[k + 1]; i++) {
-      const int isg = cMT.nc_entry[i] >> 2, ivsg = cMT.nc_entry[i] & 3;
+#pragma unroll
+    for (int i = MT().nc_start[k]; i < MT().nc_start[k + 1]; i++) {
+      const int isg = MT().nc_entry[i] >> 2, ivsg = MT().nc_entry[i] & 3;
       const float ci = isg == 0 ? corr[0] : isg == 1 ? corr[1] : isg == 2 ? corr[2] : corr[3];
       const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
 #pragma unroll
@@ -346,7 +353,7 @@ __device__ void m_corner(const Dev &d, int iq) {
         double ax, ay;
         corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
         float m, sx, sy;
-        corner_coeffs(ax, ay, cMT.wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy);
+        corner_coeffs(ax, ay, MT().wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy);
         P0 += (double)m;
         P1 += (double)m * (double)st[1];
         P2 += (double)m * (double)st[2];
@@ -390,7 +397,7 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
   double tr[6] = {0, 0, 0, 0, 0, 0};          // tau equation, all moments
   double pa0 = 0.0, pb0 = 0.0, el0 = 0.0;     // cell averages of momentum and energy
   float p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < 9; k++) {
     float b[6], st[4];
     node_basis(G, k, b);
@@ -403,21 +410,21 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
     const double un = d.us_new[pn], vn = d.vs_new[pn];
     const double du0 = un - (double)st[1], du1 = vn - (double)st[2];
     double tw = 0.0, f0 = 0.0, f1 = 0.0, fe = 0.0;
-#pragma unroll 1
-    for (int i = cMT.nc_start[k]; i < cMT.nc_start[k + 1]; i++) {
-      const int isg = cMT.nc_entry[i] >> 2, ivsg = cMT.nc_entry[i] & 3;
+#pragma unroll
+    for (int i = MT().nc_start[k]; i < MT().nc_start[k + 1]; i++) {
+      const int isg = MT().nc_entry[i] >> 2, ivsg = MT().nc_entry[i] & 3;
       const float ci = (float)d.corr[isg * (size_t)d.nquad + iq];
       const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
-      const double wq = cMD.wmom[4 * isg + ivsg];
+      const double wq = MD().wmom[4 * isg + ivsg];
 #pragma unroll
       for (int f = 0; f < 2; f++) {
         double ax, ay;
         corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
         float m, sx, sy;
-        corner_coeffs(ax, ay, cMT.wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy);
+        corner_coeffs(ax, ay, MT().wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy);
         const double fs0 = (double)sx + (double)m * du0;
         const double fs1 = (double)sy + (double)m * du1;
-        tw += (un * ax + vn * ay) * (2.0 * cMD.wmas[8 * isg + 2 * ivsg + f]);
+        tw += (un * ax + vn * ay) * (2.0 * MD().wmas[8 * isg + 2 * ivsg + f]);
         f0 += fs0 * wq;
         f1 += fs1 * wq;
         fe += (un * fs0 + vn * fs1) * wq;
@@ -425,7 +432,7 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
     }
     // tau: all moments in FP64 with the FP64 node basis
     {
-      const double b1 = cMD.xv[k] - rc, b2 = cMD.yv[k] - sc;
+      const double b1 = MD().xv[k] - rc, b2 = MD().yv[k] - sc;
       tr[0] += tw;
       tr[1] += tw * b1;
       tr[2] += tw * b2;
