@@ -282,7 +282,7 @@ __host__ __device__ void f_persson(const Dev &d, int iq) {
 #pragma unroll
   for (int k = 0; k < 6; k++) t[k] = d.Us[k * (size_t)d.ncell + e];
   double unvar2 = 0.0, unvar1 = 0.0;
-#pragma unroll 1
+#pragma unroll
   for (int i = 0; i < 5; i++) {
     const double r = g5p(i);
     const double dr = r - g.rc;

@@ -117,9 +117,9 @@ __device__ __forceinline__ void node_basis(const GeoF &g, int iv, float *b) {
   b[0] = 1.0f;
   b[1] = MT().xv[iv] - g.rc;
   b[2] = MT().yv[iv] - g.sc;
-  b[3] = 0.5f * b[1] * b[1] - g.g19;
-  b[4] = 0.5f * b[2] * b[2] - g.g20;
-  b[5] = b[1] * b[2] - g.g21;
+  b[3] = __fmaf_rn(__fmul_rn(0.5f, b[1]), b[1], -g.g19);
+  b[4] = __fmaf_rn(__fmul_rn(0.5f, b[2]), b[2], -g.g20);
+  b[5] = __fmaf_rn(b[1], b[2], -g.g21);
 }
 
 
@@ -143,6 +143,10 @@ __device__ __forceinline__ const MixTablesD &MD() {
 // Unnormalised face vector an of gesgq slot `slot` in FP64 (unit normal
 // an / |an|, face length 2 |an|; getfnds_lagsms_simpsonhybrid and
 // getfnds_lagsmsif_hybrid)
+// a0 x0 + a1 x1 + a2 x2 with a fixed rounding sequence (see vertex_state)
+__device__ __forceinline__ double dot3(double a0, double x0, double a1, double x1, double a2, double x2) {
+  return __fma_rn(a2, x2, __fma_rn(a1, x1, __dmul_rn(a0, x0)));
+}
 __device__ __forceinline__ void slot_an(const double X[3][3], const double Y[3][3], int slot, double &ax,
                                         double &ay) {
   if (slot >= 8 && slot < 12) {
@@ -152,23 +156,23 @@ __device__ __forceinline__ void slot_an(const double X[3][3], const double Y[3][
     double ex, ey, vx, vy;
     if (f == 0) {
       ex = X[1][0]; ey = Y[1][0];
-      vx = lm0 * X[1][0] + lm1 * X[1][1] + lm2 * X[1][2];
-      vy = lm0 * Y[1][0] + lm1 * Y[1][1] + lm2 * Y[1][2];
+      vx = dot3(lm0, X[1][0], lm1, X[1][1], lm2, X[1][2]);
+      vy = dot3(lm0, Y[1][0], lm1, Y[1][1], lm2, Y[1][2]);
     } else if (f == 1) {
       ex = X[2][1]; ey = Y[2][1];
-      vx = lp0 * X[0][1] + lp1 * X[1][1] + lp2 * X[2][1];
-      vy = lp0 * Y[0][1] + lp1 * Y[1][1] + lp2 * Y[2][1];
+      vx = dot3(lp0, X[0][1], lp1, X[1][1], lp2, X[2][1]);
+      vy = dot3(lp0, Y[0][1], lp1, Y[1][1], lp2, Y[2][1]);
     } else if (f == 2) {
       ex = X[1][2]; ey = Y[1][2];
-      vx = lp0 * X[1][0] + lp1 * X[1][1] + lp2 * X[1][2];
-      vy = lp0 * Y[1][0] + lp1 * Y[1][1] + lp2 * Y[1][2];
+      vx = dot3(lp0, X[1][0], lp1, X[1][1], lp2, X[1][2]);
+      vy = dot3(lp0, Y[1][0], lp1, Y[1][1], lp2, Y[1][2]);
     } else {
       ex = X[0][1]; ey = Y[0][1];
-      vx = lm0 * X[0][1] + lm1 * X[1][1] + lm2 * X[2][1];
-      vy = lm0 * Y[0][1] + lm1 * Y[1][1] + lm2 * Y[2][1];
+      vx = dot3(lm0, X[0][1], lm1, X[1][1], lm2, X[2][1]);
+      vy = dot3(lm0, Y[0][1], lm1, Y[1][1], lm2, Y[2][1]);
     }
-    ax = -(-1.5 * ey - 0.5 * Y[1][1] + 2.0 * vy);
-    ay = -1.5 * ex - 0.5 * X[1][1] + 2.0 * vx;
+    ax = -dot3(-1.5, ey, -0.5, Y[1][1], 2.0, vy);
+    ay = dot3(-1.5, ex, -0.5, X[1][1], 2.0, vx);
     return;
   }
   const int ig = slot < 8 ? slot : slot - 4;
@@ -181,10 +185,10 @@ __device__ __forceinline__ void slot_an(const double X[3][3], const double Y[3][
   if (ia == 0) { xb0 = X[0][0]; xb1 = X[0][1]; xb2 = X[0][2]; yb0 = Y[0][0]; yb1 = Y[0][1]; yb2 = Y[0][2]; }
   else if (ia == 1) { xb0 = X[1][0]; xb1 = X[1][1]; xb2 = X[1][2]; yb0 = Y[1][0]; yb1 = Y[1][1]; yb2 = Y[1][2]; }
   else { xb0 = X[2][0]; xb1 = X[2][1]; xb2 = X[2][2]; yb0 = Y[2][0]; yb1 = Y[2][1]; yb2 = Y[2][2]; }
-  const double xr = da[0] * xa0 + da[1] * xa1 + da[2] * xa2;
-  const double yr = da[0] * ya0 + da[1] * ya1 + da[2] * ya2;
-  const double xs = db[0] * xb0 + db[1] * xb1 + db[2] * xb2;
-  const double ys = db[0] * yb0 + db[1] * yb1 + db[2] * yb2;
+  const double xr = dot3(da[0], xa0, da[1], xa1, da[2], xa2);
+  const double yr = dot3(da[0], ya0, da[1], ya1, da[2], ya2);
+  const double xs = dot3(db[0], xb0, db[1], xb1, db[2], xb2);
+  const double ys = dot3(db[0], yb0, db[1], yb1, db[2], yb2);
   switch (MD().side[ig]) {
     case 0: ax = yr; ay = -xr; break;
     case 1: ax = ys; ay = -xs; break;
@@ -206,12 +210,15 @@ __device__ __forceinline__ void corner_an(const double X[3][3], const double Y[3
 // the jump-direction branch needs |u* - u_c| >= 1e12 c
 __device__ __forceinline__ float corner_m(float rhoct, float sdctr, float cimpd, float slpdu, float dux, float duy,
                                           float ax, float ay, float w) {
-  const float nn = sqrtf(ax * ax + ay * ay);
-  const float dun = fabsf(dux * ax + duy * ay);
-  const float j2 = dux * dux + duy * duy;
-  if (j2 * 1.0e-24f < sdctr * sdctr) return 2.0f * w * (rhoct * sdctr * nn + cimpd * rhoct * slpdu * dun);
-  const float murie = rhoct * sdctr + cimpd * rhoct * slpdu * (dun / nn);
-  return murie * 2.0f * w * fabsf((ax * dux + ay * duy) * rsqrtf(j2));
+  const float nn = __fsqrt_rn(__fmaf_rn(ax, ax, __fmul_rn(ay, ay)));
+  const float dn = __fmaf_rn(dux, ax, __fmul_rn(duy, ay));
+  const float dun = fabsf(dn);
+  const float j2 = __fmaf_rn(dux, dux, __fmul_rn(duy, duy));
+  const float rs = __fmul_rn(rhoct, sdctr), cr = __fmul_rn(__fmul_rn(cimpd, rhoct), slpdu);
+  const float w2 = __fmul_rn(2.0f, w);
+  if (__fmul_rn(j2, 1.0e-24f) < __fmul_rn(sdctr, sdctr)) return __fmul_rn(w2, __fmaf_rn(rs, nn, __fmul_rn(cr, dun)));
+  const float murie = __fmaf_rn(cr, __fdiv_rn(dun, nn), rs);
+  return __fmul_rn(__fmul_rn(murie, w2), fabsf(__fmul_rn(dn, rsqrtf(j2))));
 }
 
 // node coordinates of quad iq as FP64 offsets from its centre node on the 3x3 tensor
@@ -245,21 +252,30 @@ __device__ __forceinline__ void load_cell(const Dev &d, int iq, CellXY &L, doubl
 // cell-centre sound speed and 1/tau (getriem_quadsubg2), FP32
 __device__ __forceinline__ void centre_state(const float u[4][6], float g, float &rhoct, float &sdctr) {
   const float eps = 1.0e-6f;
-  rhoct = 1.0f / u[0][0];
-  const float pctr = fmaxf(eps, (g - 1.0f) * rhoct * (u[3][0] - 0.5f * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
-  sdctr = sqrtf(fmaxf(eps, g * pctr / rhoct));
+  rhoct = __fdiv_rn(1.0f, u[0][0]);
+  const float kc = __fmaf_rn(-0.5f, __fmaf_rn(u[1][0], u[1][0], __fmul_rn(u[2][0], u[2][0])), u[3][0]);
+  const float pctr = fmaxf(eps, __fmul_rn(__fmul_rn(g - 1.0f, rhoct), kc));
+  sdctr = __fsqrt_rn(fmaxf(eps, __fdiv_rn(__fmul_rn(g, pctr), rhoct)));
 }
 
 // vertex state of node k: (tau, u, v, e) from the first mdegr Taylor modes
+// The quantities that both the corner pass and the RHS pass compute (vertex
+// states, pressures, corner coefficients, face vectors) use explicitly rounded
+// operations: the two kernels must produce them bit for bit alike, or the
+// corner forces of the RHS no longer balance the node solve and total energy
+// drifts (the compiler may otherwise fuse multiply-adds differently in each).
 __device__ __forceinline__ void vertex_state(const float u[4][6], const float *b, int mdegr, float st[4]) {
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     float acc = 0.0f;
 #pragma unroll
     for (int kk = 0; kk < 6; kk++)
-      if (kk < mdegr) acc += u[q][kk] * b[kk];
+      if (kk < mdegr) acc = __fmaf_rn(u[q][kk], b[kk], acc);
     st[q] = acc;
   }
+}
+__device__ __forceinline__ float kinetic_f(const float st[4]) {
+  return __fmaf_rn(-0.5f, __fmaf_rn(st[1], st[1], __fmul_rn(st[2], st[2])), st[3]);
 }
 
 // FP32 coefficients of one corner face from its FP64 face vector: m and
@@ -269,9 +285,9 @@ __device__ __forceinline__ void corner_coeffs(double axd, double ayd, float w, f
                                               float &sy) {
   const float ax = (float)axd, ay = (float)ayd;
   m = corner_m(rhoct, sdctr, cimpd, slpdu, dux, duy, ax, ay, w);
-  const float pw = -2.0f * pv * w;
-  sx = pw * ax;
-  sy = pw * ay;
+  const float pw = __fmul_rn(__fmul_rn(-2.0f, pv), w);
+  sx = __fmul_rn(pw, ax);
+  sy = __fmul_rn(pw, ay);
 }
 
 // ---------------------------------------------------------------------------
@@ -337,8 +353,8 @@ __device__ void m_corner(const Dev &d, int iq) {
     float b[6], st[4];
     node_basis(G, k, b);
     vertex_state(u, b, d.mdegr, st);
-    const float rhovt = 1.0f / st[0];
-    const float ke = st[3] - 0.5f * (st[1] * st[1] + st[2] * st[2]);
+    const float rhovt = __fdiv_rn(1.0f, st[0]);
+    const float ke = kinetic_f(st);
     const int pn = d.ipq[k * d.nquad + iq];
     const float dux = (float)d.us[pn] - st[1];
     const float duy = (float)d.vs[pn] - st[2];
@@ -347,7 +363,7 @@ __device__ void m_corner(const Dev &d, int iq) {
     for (int i = MT().nc_start[k]; i < MT().nc_start[k + 1]; i++) {
       const int isg = MT().nc_entry[i] >> 2, ivsg = MT().nc_entry[i] & 3;
       const float ci = isg == 0 ? corr[0] : isg == 1 ? corr[1] : isg == 2 ? corr[2] : corr[3];
-      const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
+      const float pv = fmaxf(eps, __fmul_rn(__fmul_rn(g - 1.0f, __fadd_rn(rhovt, ci)), ke));
 #pragma unroll
       for (int f = 0; f < 2; f++) {
         double ax, ay;
@@ -402,8 +418,8 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
     float b[6], st[4];
     node_basis(G, k, b);
     vertex_state(u, b, d.mdegr, st);
-    const float rhovt = 1.0f / st[0];
-    const float ke = st[3] - 0.5f * (st[1] * st[1] + st[2] * st[2]);
+    const float rhovt = __fdiv_rn(1.0f, st[0]);
+    const float ke = kinetic_f(st);
     const int pn = d.ipq[k * d.nquad + iq];
     const float dux = (float)d.us[pn] - st[1];
     const float duy = (float)d.vs[pn] - st[2];
@@ -414,7 +430,7 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
     for (int i = MT().nc_start[k]; i < MT().nc_start[k + 1]; i++) {
       const int isg = MT().nc_entry[i] >> 2, ivsg = MT().nc_entry[i] & 3;
       const float ci = (float)d.corr[isg * (size_t)d.nquad + iq];
-      const float pv = fmaxf(eps, (g - 1.0f) * (rhovt + ci) * ke);
+      const float pv = fmaxf(eps, __fmul_rn(__fmul_rn(g - 1.0f, __fadd_rn(rhovt, ci)), ke));
       const double wq = MD().wmom[4 * isg + ivsg];
 #pragma unroll
       for (int f = 0; f < 2; f++) {
