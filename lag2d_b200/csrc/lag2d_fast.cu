@@ -495,6 +495,84 @@ __host__ __device__ void f_node(const Dev &d, int p) {
 // RHS pass: corner forces + face integral + volume integral (+ source), and
 // in stages 2 and 3 the M^-1 solve and RK combine
 // ---------------------------------------------------------------------------
+// Taylor-Green source moments el[k] += sum_g src(x_g) b_k(g) detJ_g w_g over
+// the 5x5 Gauss points.  cos(pi x) at the points by angle addition from the
+// centre node x_c: cos(pi x) = cos(pi x_c) cos(pi d) - sin(pi x_c) sin(pi d),
+// d = x - x_c, with the series of cossin_pi_small when every node of the cell
+// lies within 0.09 of the centre node in x and y (the quadratic map then keeps
+// |d| <= 1.5625 * 0.09 < 0.15 at the Gauss points), so the point loop has no
+// branch; otherwise cospi at each point.  The basis sums are taken per row:
+// b_k along a row is a polynomial in ds of degree <= 2.
+template <bool SMALL>
+__host__ __device__ __forceinline__ void tgv_source_rows(const Loaded &L, const CellGeo &G, const double D[16],
+                                                         double g, double el[6]) {
+  const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
+  const double xc = L.X[1][1], yc = L.Y[1][1];
+  const double cxc = cospi(xc), sxc = sinpi(xc), cyc = cospi(yc), syc = sinpi(yc);
+#pragma unroll 1
+  for (int i = 0; i < 5; i++) {
+    const double r = g5p(i), dr = r - G.rc;
+    double lr[3];
+    lag3(r, lr);
+    double Px[3], Py[3];
+#pragma unroll
+    for (int bb = 0; bb < 3; bb++) {
+      Px[bb] = lr[0] * (L.X[0][bb] - xc) + lr[1] * (L.X[1][bb] - xc) + lr[2] * (L.X[2][bb] - xc);
+      Py[bb] = lr[0] * (L.Y[0][bb] - yc) + lr[1] * (L.Y[1][bb] - yc) + lr[2] * (L.Y[2][bb] - yc);
+    }
+    double e[4];
+#pragma unroll
+    for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+    const double wi = coef * g5w(i);
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const double s = g5p(j), ds = s - G.sc;
+      double ls[3];
+      lag3(s, ls);
+      const double dx = Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2];
+      const double dy = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
+      const double djaco = wi * g5w(j) * (e[0] + s * (e[1] + s * (e[2] + s * e[3])));
+      double cx, cy;
+      if (SMALL) {
+        double cdx, sdx, cdy, sdy;
+        cossin_pi_small(dx, cdx, sdx);
+        cossin_pi_small(dy, cdy, sdy);
+        cx = cxc * cdx - sxc * sdx;
+        cy = cyc * cdy - syc * sdy;
+      } else {
+        cx = cospi(xc + dx);
+        cy = cospi(yc + dy);
+      }
+      const double c3x = cx * (4.0 * cx * cx - 3.0), c3y = cy * (4.0 * cy * cy - 3.0);
+      const double src = (c3x * cy - c3y * cx) * djaco;
+      m0 += src;
+      m1 += src * ds;
+      m2 += src * ds * ds;
+    }
+    // b = (1, dr, ds, dr^2/2 - g19, ds^2/2 - g20, dr ds - g21) along the row
+    el[0] += m0;
+    el[1] += m0 * dr;
+    el[2] += m1;
+    el[3] += m0 * (0.5 * dr * dr - G.g19);
+    el[4] += 0.5 * m2 - G.g20 * m0;
+    el[5] += m1 * dr - G.g21 * m0;
+  }
+}
+__host__ __device__ __forceinline__ void tgv_source(const Loaded &L, const CellGeo &G, const double D[16], double g,
+                                                    double el[6]) {
+  double mx = 0.0, my = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      mx = fmax(mx, fabs(L.X[a][b] - L.X[1][1]));
+      my = fmax(my, fabs(L.Y[a][b] - L.Y[1][1]));
+    }
+  if (mx <= 0.09 && my <= 0.09) tgv_source_rows<true>(L, G, D, g, el);
+  else tgv_source_rows<false>(L, G, D, g, el);
+}
+
 __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
   if (iq >= d.nquad || d.sc_dev->done) return;
   const int e = iq + d.ntria;
@@ -619,9 +697,7 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
   }
   if (d.ncase == 1) {
     // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:
-    // 4070-4251), 5x5 Gauss; cos(3t) = cos t (4 cos^2 t - 3).  cos(pi x) at
-    // the Gauss points by angle addition from the centre node x_c:
-    // cos(pi x) = cos(pi x_c) cos(pi d) - sin(pi x_c) sin(pi d), d = x - x_c.
+    // 4070-4251), 5x5 Gauss; cos(3t) = cos t (4 cos^2 t - 3).
     double c[36], D[16];
     {
       double xp[9][2];
@@ -629,53 +705,7 @@ __host__ __device__ void f_rhs(const Dev &d, int iq, int fuse_update, double alf
       cross36(xp, c);
     }
     detpoly(c, D);
-    const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
-    const double xc = L.X[1][1], yc = L.Y[1][1];
-    const double cxc = cospi(xc), sxc = sinpi(xc), cyc = cospi(yc), syc = sinpi(yc);
-#pragma unroll 1
-    for (int i = 0; i < 5; i++) {
-      const double r = g5p(i), dr = r - G.rc;
-      double lr[3];
-      lag3(r, lr);
-      double Px[3], Py[3];
-#pragma unroll
-      for (int bb = 0; bb < 3; bb++) {
-        Px[bb] = lr[0] * (L.X[0][bb] - xc) + lr[1] * (L.X[1][bb] - xc) + lr[2] * (L.X[2][bb] - xc);
-        Py[bb] = lr[0] * (L.Y[0][bb] - yc) + lr[1] * (L.Y[1][bb] - yc) + lr[2] * (L.Y[2][bb] - yc);
-      }
-      double e[4];
-#pragma unroll
-      for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
-      const double wi = g5w(i);
-#pragma unroll
-      for (int j = 0; j < 5; j++) {
-        const double s = g5p(j), ds = s - G.sc;
-        double ls[3];
-        lag3(s, ls);
-        const double dx = Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2];
-        const double dy = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
-        const double djaco = wi * g5w(j) * (e[0] + s * (e[1] + s * (e[2] + s * e[3])));
-        double cx, cy;
-        if (fabs(dx) <= 0.15 && fabs(dy) <= 0.15) {
-          double cdx, sdx, cdy, sdy;
-          cossin_pi_small(dx, cdx, sdx);
-          cossin_pi_small(dy, cdy, sdy);
-          cx = cxc * cdx - sxc * sdx;
-          cy = cyc * cdy - syc * sdy;
-        } else {
-          cx = cospi(xc + dx);
-          cy = cospi(yc + dy);
-        }
-        const double c3x = cx * (4.0 * cx * cx - 3.0), c3y = cy * (4.0 * cy * cy - 3.0);
-        const double src = coef * (c3x * cy - c3y * cx) * djaco;
-        el[0] += src;
-        el[1] += src * dr;
-        el[2] += src * ds;
-        el[3] += src * (0.5 * dr * dr - G.g19);
-        el[4] += src * (0.5 * ds * ds - G.g20);
-        el[5] += src * (dr * ds - G.g21);
-      }
-    }
+    tgv_source(L, G, D, g, el);
   }
   if (!fuse_update) {
 #pragma unroll
