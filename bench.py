@@ -41,6 +41,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dtfix", type=float, default=0.0,
+                    help="fixed time step (ndt = 0) instead of the CFL one, for the configurations whose "
+                         "CFL steps break the scheme (Noh, hybrid Sedov)")
+    ap.add_argument("--rho0", action="store_true", help="per-cell initial densities 1 + 0.01 N(0, 1)")
     ap.add_argument("--adjoint-steps", type=int, default=4)
     ap.add_argument("--adjoint-checkpoint", type=int, default=2)
     return ap.parse_args()
@@ -51,9 +55,34 @@ def dist_env():
 
 
 def config_block(name, mesh, cfg, n):
-    return {"workload": name, "cells": mesh.ncell, "nodes": mesh.npoin, "basis": "P2 Taylor (ndegr=6, nq=4)",
-            "rk_stages": cfg.nstag, "limiter": "Persson + WENO", "gamma": cfg.gamlg, "cfl": cfg.cfl,
-            "parallelism": f"replicas x{n}", "l2": "working set > 126 MB L2 (no flush needed)"}
+    out = {"workload": name, "cells": mesh.ncell, "triangles": mesh.ntria, "nodes": mesh.npoin,
+           "basis": "P2 Taylor (ndegr=6, nq=4)", "rk_stages": cfg.nstag, "limiter": "Persson + WENO",
+           "gamma": cfg.gamlg, "cfl": cfg.cfl, "parallelism": f"replicas x{n}",
+           "l2": ("working set > 126 MB L2 (no flush needed)" if mesh.ncell >= 262144
+                  else "working set within the 126 MB L2 (small configuration)")}
+    if cfg.ndt == 0:
+        out["dt"] = f"fixed {cfg.dtfix:g}"
+    return out
+
+
+def make_case(args):
+    """The workload of --workload, with the --dtfix and --rho0 options applied."""
+    import dataclasses
+    from lag2d_b200.config import initial_density_factors, workload
+    m, c = workload(args.workload)
+    if args.dtfix > 0:
+        c = dataclasses.replace(c, ndt=0, dtfix=args.dtfix)
+    rho0 = initial_density_factors(m) if args.rho0 else None
+    return m, c, rho0
+
+
+def new_solver(m, c, rho0, **kw):
+    from lag2d_b200.api import Lag2DSolver
+    s = Lag2DSolver(m, c, **kw)
+    if rho0 is not None:
+        s.set_rho0(rho0)
+    s.init_fields()
+    return s
 
 
 # --------------------------------------------------------------------------
@@ -228,16 +257,12 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from lag2d_b200.api import Lag2DSolver
-    from lag2d_b200.config import workload
     from lag2d_b200.replicas import aggregate_rate, max_over_ranks
     from lag2d_b200.roofline import kernel_bytes, stage_bytes
 
-    m, c = workload(args.workload)
-    s = Lag2DSolver(m, c)
-    s.init_fields()
-    sm = Lag2DSolver(m, c, precision=1)   # FP32-mixed form of the same step
-    sm.init_fields()
+    m, c, rho0 = make_case(args)
+    s = new_solver(m, c, rho0)
+    sm = new_solver(m, c, rho0, precision=1)   # FP32-mixed form of the same step
     dof_stage = m.ncell * c.ndegr * c.nq
 
     def timed(solver):
@@ -340,8 +365,7 @@ def run_ours(args):
     state = (u_a, x_a, us_a, s.itime, s.dtfix, s.tacru)
     g64, g32 = {}, {}
     adjoint = adjoint_block(s, args, ms_per_step, state, g64)
-    sm2 = Lag2DSolver(m, c, precision=1)
-    sm2.init_fields()
+    sm2 = new_solver(m, c, rho0, precision=1)
     adjoint["fp32_mixed"] = adjoint_block(sm2, args, mixed["ms_per_step"], state, g32)
     sm2.close()
     if g64 and g32:
