@@ -22,6 +22,7 @@ void launch_reset_count(const Dev &d, cudaStream_t st);
 void launch_persson(const Dev &d, cudaStream_t st);
 void launch_flags_from_host(const Dev &d, cudaStream_t st, const int *flags);
 void launch_weno(const Dev &d, cudaStream_t st);
+void launch_weno_warp(const Dev &d, cudaStream_t st);
 void launch_weno_commit(const Dev &d, cudaStream_t st);
 void launch_corner(const Dev &d, cudaStream_t st);
 void launch_node(const Dev &d, cudaStream_t st);
@@ -362,7 +363,7 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
       cudaMemcpyAsync(rec->vs + slot * rec->np, d.vs, rec->np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
     }
     run(h, "persson", [&] { launch_reset_count(d, h->st); launch_fast_persson(d, h->st); }, 2);
-    run(h, "weno", [&] { launch_weno(d, h->st); launch_weno_commit(d, h->st); }, 2);
+    run(h, "weno", [&] { launch_weno_warp(d, h->st); launch_weno_commit(d, h->st); }, 2);
     if (rec) {
       k_count_limited<<<1, 256, 0, h->st>>>(d, rec->troubled);
       h->launches += 1;

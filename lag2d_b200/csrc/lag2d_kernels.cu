@@ -687,6 +687,320 @@ __host__ __device__ void b_weno_commit(const Dev &d, int t) {
 __global__ void k_weno_commit(Dev d) { b_weno_commit(d, blockIdx.x * blockDim.x + threadIdx.x); }
 
 // ---------------------------------------------------------------------------
+// The same WENO reconstruction with one warp per troubled quad (the optimised
+// step's version).  The per-item arithmetic is b_weno's; the independent
+// items run on different lanes: the 216 stencil DOFs, the 81 stencil nodes,
+// the 225 stencil quadrature points, the 9 stencil cells' local geometry and
+// L2 projections, the 8 candidate stencils and the 4 faces, with the data
+// between phases in shared memory.  Lane 0 combines the faces in order and
+// writes the result.  Blocks of one warp loop over the troubled list.
+// ---------------------------------------------------------------------------
+struct WenoShared {
+  double unkrl[9][4][6];
+  double xpqi[9][9][2], xpql[9][9][2], rhogi[9];
+  double rhodj[9][25], xl[9][25], yl[9][25];
+  double geopl[9][5];
+  double unkpl[9][4][6];
+  double mtbbq[25], mtbbi[25];
+  double unksl[9][4][6];
+  double unkf[4][4][6];
+  int fvalid[4];
+};
+
+__device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
+  const int lane = threadIdx.x & 31;
+  const int iq = d.wlist[t];
+  const int ielem = iq + d.ntria;
+  int ielaj[9];
+  for (int k = 0; k < 9; k++) ielaj[k] = d.stencil[k * d.nquad + iq];
+  if (ielaj[0] == -2 && lane == 0) atomic_or(&d.sc_dev->status, ST_STENCIL);
+  if (ielaj[0] < 0) return;  // boundary cell: the reference leaves it (WENO.f90:7704)
+  const int ielst1[4][7] = {{1, 2, 5, 6, 9, 8, 3}, {1, 3, 2, 7, 6, 9, 5},
+                            {1, 4, 3, 8, 7, 6, 5}, {1, 5, 4, 9, 8, 7, 3}};
+  const int ielst2[4][4] = {{1, 2, 6, 9}, {1, 3, 6, 7}, {1, 4, 8, 7}, {1, 5, 8, 9}};
+  double mp[4];
+  for (int k = 0; k < 4; k++) mp[k] = d.mapmt[k * d.ncell + ielem];
+  const double dxcl = sqrt(d.vol[ielem]), dycl = dxcl;
+
+  // stencil DOFs (velocities rotated to the local frame) and stencil nodes
+  for (int e = lane; e < 216; e += 32) {
+    const int s = e / 24, q = (e / 6) % 4, k = e % 6;
+    S.unkrl[s][q][k] = Uget(d, d.Us, k, q, ielaj[s]);
+  }
+  for (int e = lane; e < 81; e += 32) {
+    const int s = e / 9, k = e % 9;
+    const int p = d.ipq[k * d.nquad + (ielaj[s] - d.ntria)];
+    S.xpqi[s][k][0] = d.x0[p];
+    S.xpqi[s][k][1] = d.y0[p];
+    double x = d.xs[p], y = d.ys[p];
+    vec_local(mp, x, y);
+    S.xpql[s][k][0] = x;
+    S.xpql[s][k][1] = y;
+  }
+  __syncwarp();
+  for (int e = lane; e < 54; e += 32) {
+    const int s = e / 6, k = e % 6;
+    vec_local(mp, S.unkrl[s][1][k], S.unkrl[s][2][k]);
+  }
+  if (lane < 9) {
+    const int jelem = ielaj[lane];
+    double shp[9], xcrho, ycrho;
+    shp9v(d.rc[jelem], d.sc[jelem], shp);
+    map9(S.xpqi[lane], shp, xcrho, ycrho);
+    S.rhogi[lane] = rho_initial(d, jelem, xcrho, ycrho);
+  }
+  __syncwarp();
+  // quadrature points of the stencil cells (weno_points)
+  for (int e = lane; e < 225; e += 32) {
+    const int s = e / 25, ig = e % 25;
+    const double r = cQ.g25[ig][0], sp = cQ.g25[ig][1], wi = cQ.w25[ig];
+    double shp[9], dr[9], ds[9];
+    shp9v(r, sp, shp);
+    shp9d(r, sp, dr, ds);
+    Jac j = jac9(S.xpqi[s], dr, ds);
+    const double djacoi = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(S.xpql[s], shp, xg, yg);
+    S.rhodj[s][ig] = S.rhogi[s] * djacoi;
+    S.xl[s][ig] = xg;
+    S.yl[s][ig] = yg;
+  }
+  __syncwarp();
+  // getgeophy_local_Taylor, then getunknp_local_Taylor, one stencil cell per lane
+  if (lane < 9) {
+    const int s = lane, jelem = ielaj[s];
+    double xclj = d.geoph[jelem], yclj = d.geoph[d.ncell + jelem];
+    vec_local(mp, xclj, yclj);
+    const double dxclj = sqrt(d.vol[jelem]), dyclj = dxclj;
+    const double masel = d.mass[jelem];
+    double v1 = 0.0, v2 = 0.0, v3 = 0.0;
+    for (int ig = 0; ig < 25; ig++) {
+      double b2 = (S.xl[s][ig] - xclj) / dxclj, b3 = (S.yl[s][ig] - yclj) / dyclj;
+      v1 = v1 + S.rhodj[s][ig] * b2 * b2;
+      v2 = v2 + S.rhodj[s][ig] * b3 * b3;
+      v3 = v3 + S.rhodj[s][ig] * b2 * b3;
+    }
+    v1 = v1 / masel; v2 = v2 / masel; v3 = v3 / masel;
+    double gp[5] = {xclj, yclj, 0.5 * v1, 0.5 * v2, v3};
+    for (int k = 0; k < 5; k++) S.geopl[s][k] = gp[k];
+    const double rcj = d.rc[jelem], scj = d.sc[jelem];
+    double bb[25], bbq[25], bbi[25], bbqi[25];
+    for (int i = 0; i < 25; i++) { bb[i] = 0.0; bbq[i] = 0.0; }
+    for (int ig = 0; ig < 25; ig++) {
+      double r = cQ.g25[ig][0], s_ = cQ.g25[ig][1];
+      double bq[6], bqpl[3], bqol[6];
+      bq[0] = 1.0; bq[1] = (r - rcj) / 1.0; bq[2] = (s_ - scj) / 1.0;
+      bq[3] = 0.5 * bq[1] * bq[1] - d.g19[jelem];
+      bq[4] = 0.5 * bq[2] * bq[2] - d.g20[jelem];
+      bq[5] = bq[1] * bq[2] - d.g21[jelem];
+      bqpl[0] = 1.0; bqpl[1] = (S.xl[s][ig] - xclj) / dxclj; bqpl[2] = (S.yl[s][ig] - yclj) / dyclj;
+      basis_orthg1(bqpl, &gp[2], bqol);
+      for (int i = 1; i < 6; i++)
+        for (int j = 1; j < 6; j++) {
+          bb[(i - 1) + 5 * (j - 1)] = bb[(i - 1) + 5 * (j - 1)] + S.rhodj[s][ig] * bq[i] * bqol[j];
+          bbq[(i - 1) + 5 * (j - 1)] = bbq[(i - 1) + 5 * (j - 1)] + S.rhodj[s][ig] * bqol[i] * bqol[j];
+        }
+    }
+    double rhs[6][4];
+    for (int i = 0; i < 6; i++) for (int q = 0; q < 4; q++) rhs[i][q] = 0.0;
+    for (int i = 1; i < 6; i++)
+      for (int j = 1; j < 6; j++)
+        for (int q = 0; q < 4; q++) rhs[i][q] = rhs[i][q] + S.unkrl[s][q][j] * bb[(j - 1) + 5 * (i - 1)];
+    inv_small(5, bbq, bbqi);
+    inv_small(5, bb, bbi);
+    double up[4][6];
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) up[q][k] = 0.0;
+    for (int i = 1; i < 6; i++)
+      for (int j = 1; j < 6; j++)
+        for (int q = 0; q < 4; q++) up[q][i] = up[q][i] + rhs[j][q] * bbqi[(j - 1) + 5 * (i - 1)];
+    for (int q = 0; q < 4; q++) up[q][0] = S.unkrl[s][q][0];
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) S.unkpl[s][q][k] = up[q][k];
+    if (s == 0)
+      for (int i = 0; i < 25; i++) { S.mtbbq[i] = bbq[i]; S.mtbbi[i] = bbi[i]; }
+  }
+  __syncwarp();
+  // candidate polynomials: 1 central (lane 8) + 4 Lagrangian (lanes 0-3) + 4 Hermite (lanes 4-7)
+  const double xmcl = S.geopl[0][0], ymcl = S.geopl[0][1];
+  if (lane < 9) {
+    const int isten = lane < 8 ? lane + 1 : 0;
+    double us[4][6];
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) us[q][k] = 0.0;
+    for (int q = 0; q < 4; q++) us[q][0] = S.unkpl[0][q][0];
+    if (isten == 0) {
+      for (int k = 0; k < 6; k++) for (int q = 0; q < 4; q++) us[q][k] = S.unkpl[0][q][k];
+    } else if (isten <= 4) {
+      const int is = isten - 1;
+      double matlg[25], rhslg[20], matin[25];
+      for (int i = 0; i < 25; i++) matlg[i] = 0.0;
+      for (int i = 0; i < 20; i++) rhslg[i] = 0.0;
+      for (int ies = 0; ies < 5; ies++) {
+        int sl = ielst1[is][ies + 1] - 1;
+        double masej = d.mass[ielaj[sl]];
+        for (int ig = 0; ig < 25; ig++) {
+          double bqplj[3], bqolj[6];
+          bqplj[0] = 1.0; bqplj[1] = (S.xl[sl][ig] - xmcl) / dxcl; bqplj[2] = (S.yl[sl][ig] - ymcl) / dycl;
+          basis_orthg1(bqplj, &S.geopl[0][2], bqolj);
+          for (int k = 0; k < 5; k++) matlg[ies + 5 * k] = matlg[ies + 5 * k] + S.rhodj[sl][ig] * bqolj[k + 1] / masej;
+        }
+        for (int q = 0; q < 4; q++) rhslg[q + 4 * ies] = S.unkpl[sl][q][0] - S.unkpl[0][q][0];
+      }
+      inv_small(5, matlg, matin);
+      for (int k = 1; k < 6; k++)
+        for (int ies = 0; ies < 5; ies++)
+          for (int q = 0; q < 4; q++) us[q][k] = us[q][k] + matin[(k - 1) + 5 * ies] * rhslg[q + 4 * ies];
+    } else {
+      const int is = isten - 5;
+      double mathm[45], rhshm[36], matls[25], rhsls[20], matin[25];
+      for (int i = 0; i < 45; i++) mathm[i] = 0.0;
+      for (int i = 0; i < 36; i++) rhshm[i] = 0.0;
+      for (int ies = 0; ies < 3; ies++) {
+        int sl = ielst2[is][ies + 1] - 1;
+        int jelem = ielaj[sl];
+        double masej = d.mass[jelem];
+        double dxclj = sqrt(d.vol[jelem]), dyclj = dxclj;
+        double xclj = S.geopl[sl][0], yclj = S.geopl[sl][1];
+        for (int ig = 0; ig < 25; ig++) {
+          double bqplj[3], bqol[6], bqolj[6];
+          bqplj[0] = 1.0; bqplj[1] = (S.xl[sl][ig] - xmcl) / dxcl; bqplj[2] = (S.yl[sl][ig] - ymcl) / dycl;
+          basis_orthg1(bqplj, &S.geopl[0][2], bqol);
+          for (int k = 0; k < 5; k++) mathm[ies + 9 * k] = mathm[ies + 9 * k] + S.rhodj[sl][ig] * bqol[k + 1] / masej;
+          bqplj[0] = 1.0; bqplj[1] = (S.xl[sl][ig] - xclj) / dxclj; bqplj[2] = (S.yl[sl][ig] - yclj) / dyclj;
+          basis_orthg1(bqplj, &S.geopl[sl][2], bqolj);
+          int ieshm = 3 + 2 * ies;
+          for (int k = 1; k < 6; k++) {
+            mathm[ieshm + 9 * (k - 1)] = mathm[ieshm + 9 * (k - 1)] + S.rhodj[sl][ig] * bqol[k] * bqolj[1] / masej;
+            mathm[ieshm + 1 + 9 * (k - 1)] =
+                mathm[ieshm + 1 + 9 * (k - 1)] + S.rhodj[sl][ig] * bqol[k] * bqolj[2] / masej;
+          }
+          for (int k = 1; k < 6; k++)
+            for (int q = 0; q < 4; q++) {
+              rhshm[q + 4 * ieshm] =
+                  rhshm[q + 4 * ieshm] + S.rhodj[sl][ig] * bqolj[k] * bqolj[1] * S.unkpl[sl][q][k] / masej;
+              rhshm[q + 4 * (ieshm + 1)] =
+                  rhshm[q + 4 * (ieshm + 1)] + S.rhodj[sl][ig] * bqolj[k] * bqolj[2] * S.unkpl[sl][q][k] / masej;
+            }
+        }
+        for (int q = 0; q < 4; q++) rhshm[q + 4 * ies] = S.unkpl[sl][q][0] - S.unkpl[0][q][0];
+      }
+      for (int i = 0; i < 25; i++) matls[i] = 0.0;
+      for (int i = 0; i < 20; i++) rhsls[i] = 0.0;
+      for (int im = 0; im < 5; im++)
+        for (int jm = 0; jm < 5; jm++)
+          for (int km = 0; km < 9; km++) matls[im + 5 * jm] = matls[im + 5 * jm] + mathm[km + 9 * im] * mathm[km + 9 * jm];
+      for (int q = 0; q < 4; q++)
+        for (int im = 0; im < 5; im++)
+          for (int km = 0; km < 9; km++) rhsls[q + 4 * im] = rhsls[q + 4 * im] + mathm[km + 9 * im] * rhshm[q + 4 * km];
+      inv_small(5, matls, matin);
+      for (int k = 1; k < 6; k++)
+        for (int ies = 0; ies < 5; ies++)
+          for (int q = 0; q < 4; q++) us[q][k] = us[q][k] + matin[(k - 1) + 5 * ies] * rhsls[q + 4 * ies];
+    }
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) S.unksl[isten][q][k] = us[q][k];
+  }
+  __syncwarp();
+  // weno_cell_Taylor: characteristic WENO per interior face (lanes 0-3)
+  const int isten = 9;
+  const double epsil = 1.0e-6;
+  const double dxc = sqrt(d.vol[ielem]), dyc = dxc;
+  if (lane < 4) {
+    const int ies = lane;
+    const int mapfe[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
+    const int jelem = d.esq[ies * d.nquad + iq];
+    S.fvalid[ies] = jelem >= 0;
+    if (jelem >= 0) {
+      const int pa = d.ipq[mapfe[ies][0] * d.nquad + iq], pb = d.ipq[mapfe[ies][1] * d.nquad + iq];
+      double dtx = d.xs[pb] - d.xs[pa];
+      double dty = d.ys[pb] - d.ys[pa];
+      double dlgt = sqrt(dtx * dtx + dty * dty);
+      double dnx = dty / dlgt, dny = -dtx / dlgt;
+      vec_local(mp, dnx, dny);
+      double ul[4], ur[4];
+      for (int q = 0; q < 4; q++) { ul[q] = Uget(d, d.Us, 0, q, ielem); ur[q] = Uget(d, d.Us, 0, q, jelem); }
+      vec_local(mp, ul[1], ul[2]);
+      vec_local(mp, ur[1], ur[2]);
+      double qmat[16], qinvm[16];
+      matrix_prj2(d.gamlg, qmat, qinvm, dnx, dny, ul, ur);
+      double weigh[9][4], weigt[4] = {0.0, 0.0, 0.0, 0.0}, os1[9];
+      for (int is = 0; is < isten; is++) {
+        double mx = 0.0;
+        for (int k = 0; k < 4; k++) {
+          double c1 = 0.0, c2 = 0.0;
+          for (int q = 0; q < 4; q++) {
+            c1 = c1 + qinvm[k + 4 * q] * S.unksl[is][q][1];
+            c2 = c2 + qinvm[k + 4 * q] * S.unksl[is][q][2];
+          }
+          double t1 = c1 / dxc, t2 = c2 / dyc;
+          double os = t1 * t1 + t2 * t2;
+          if (k == 0 || os > mx) mx = os;
+        }
+        os1[is] = mx;
+      }
+      double weigl0 = .2, weigl1 = 0.8 / (isten - 1.0);
+      for (int is = 0; is < isten; is++)
+        for (int q = 0; q < 4; q++) {
+          double tt = epsil + os1[is];
+          weigh[is][q] = (is == 0 ? weigl0 : weigl1) / (tt * tt);
+        }
+      for (int q = 0; q < 4; q++)
+        for (int is = 0; is < isten; is++) weigt[q] = weigt[q] + weigh[is][q];
+      for (int is = 0; is < isten; is++)
+        for (int q = 0; q < 4; q++) weigh[is][q] = weigh[is][q] / weigt[q];
+      double fch[4][6];
+      for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) fch[q][k] = 0.0;
+      for (int is = 0; is < isten; is++)
+        for (int kq = 0; kq < 4; kq++)
+          for (int k = 0; k < 6; k++) {
+            double ch = 0.0;
+            for (int q = 0; q < 4; q++) ch = ch + qinvm[kq + 4 * q] * S.unksl[is][q][k];
+            fch[kq][k] = fch[kq][k] + weigh[is][kq] * ch;
+          }
+      double uf[4][6];
+      for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) uf[q][k] = 0.0;
+      for (int kq = 0; kq < 4; kq++)
+        for (int k = 1; k < 6; k++)
+          for (int q = 0; q < 4; q++) uf[q][k] = uf[q][k] + qmat[q + 4 * kq] * fch[kq][k];
+      for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) S.unkf[ies][q][k] = uf[q][k];
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    int ifprj = 0;
+    for (int a = 0; a < 4; a++) ifprj += S.fvalid[a];
+    double unk_phy[4][6];
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) unk_phy[q][k] = 0.0;
+    const double weigf = 1.0 / ifprj;
+    for (int a = 0; a < 4; a++) {
+      if (!S.fvalid[a]) continue;
+      for (int q = 0; q < 4; q++)
+        for (int k = 1; k < 6; k++) unk_phy[q][k] = unk_phy[q][k] + weigf * S.unkf[a][q][k];
+    }
+    // inverse L2 projection back to the target's Taylor basis, un-rotate
+    double rhsuk[5][4], out[4][6];
+    for (int i = 0; i < 5; i++) for (int q = 0; q < 4; q++) rhsuk[i][q] = 0.0;
+    for (int i = 1; i < 6; i++)
+      for (int j = 1; j < 6; j++)
+        for (int q = 0; q < 4; q++) rhsuk[i - 1][q] = rhsuk[i - 1][q] + unk_phy[q][j] * S.mtbbq[(j - 1) + 5 * (i - 1)];
+    for (int q = 0; q < 4; q++) for (int k = 1; k < 6; k++) out[q][k] = 0.0;
+    for (int i = 1; i < 6; i++)
+      for (int j = 1; j < 6; j++)
+        for (int q = 0; q < 4; q++) out[q][i] = out[q][i] + rhsuk[j - 1][q] * S.mtbbi[(j - 1) + 5 * (i - 1)];
+    for (int k = 1; k < 6; k++) vec_local_back(mp, out[1][k], out[2][k]);
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < 6; k++) d.Uw[(q * 5 + (k - 1)) * d.nquad + iq] = out[q][k];
+    d.flag[ielem] = 2;  // reconstructed
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(32) k_weno_warp(Dev d) {
+  __shared__ WenoShared S;
+  if (stopped(d)) return;
+  const int n = *d.wcount;
+  for (int t = blockIdx.x; t < n; t += gridDim.x) weno_warp_cell(d, t, S);
+}
+
+
+// ---------------------------------------------------------------------------
 // Sub-cell normals of a quad (getfnds_lagsmsif_hybrid, Getrhslaggauss.f90:
 // 3537-3599; getfnds_lagsms_simpsonhybrid, :9908-10010): gq[16][3].
 // ---------------------------------------------------------------------------
@@ -2678,6 +2992,10 @@ void launch_flags_from_host(const Dev &d, cudaStream_t st, const int *flags) {
   k_flags_from_host<<<nblk(d.nquad, 256), 256, 0, st>>>(d, flags);
 }
 void launch_weno(const Dev &d, cudaStream_t st) { k_weno<<<nblk(d.nquad, 64), 64, 0, st>>>(d); }
+// one warp per troubled quad, a grid of at most 8 blocks per SM looping over the list
+void launch_weno_warp(const Dev &d, cudaStream_t st) {
+  k_weno_warp<<<d.nquad < 1184 ? (d.nquad > 0 ? d.nquad : 1) : 1184, 32, 0, st>>>(d);
+}
 void launch_weno_commit(const Dev &d, cudaStream_t st) { k_weno_commit<<<nblk(d.nquad, 256), 256, 0, st>>>(d); }
 void launch_corner(const Dev &d, cudaStream_t st) { k_corner<<<nblk(d.nquad, 128), 128, 0, st>>>(d); }
 void launch_node(const Dev &d, cudaStream_t st) { k_node<<<nblk(d.npoin, 256), 256, 0, st>>>(d); }
