@@ -65,3 +65,19 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
     monkeypatch.setattr(api, "_libs", {})
     with pytest.raises(FileNotFoundError):
         api.load()
+
+
+def test_entry_points_reject_null_handles_without_device():
+    """Every handle entry point returns LAG2D_EINVAL for a null handle before
+    any CUDA call (the adjoint and density-hook entries included)."""
+    lib = api.load()
+    d = ctypes.c_double(0.0)
+    buf = np.zeros(8)
+    p = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert lib.lag2d_step(None, 1, ctypes.byref(d), ctypes.byref(d)) == 1
+    assert lib.lag2d_set_rho0(None, p) == 1
+    assert lib.lag2d_adjoint(None, 1, 2, 1, ctypes.byref(d), ctypes.byref(d), ctypes.byref(d),
+                             None, None, None, None) == 1
+    assert lib.lag2d_adjoint_step(None, 1, ctypes.byref(d), ctypes.byref(d), None, None, None,
+                                  None, None, None) == 1
+    assert b"null" in lib.lag2d_last_error()
