@@ -14,7 +14,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", f) for f in ("lag2d_kernels.cu", "lag2d_fast.cu", "lag2d_mixed.cu", "lag2d_capi.cu", "lag2d_noalloc.cu")]
+SRC = [os.path.join(HERE, "csrc", f) for f in ("lag2d_kernels.cu", "lag2d_fast.cu", "lag2d_mixed.cu", "lag2d_capi.cu", "lag2d_noalloc.cu", "lag2d_p1.cu")]
 OUT_DIR = os.path.join(HERE, "_lib")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
@@ -35,7 +35,7 @@ def build(verbose: bool = False, force: bool = False) -> list:
     os.makedirs(OUT_DIR, exist_ok=True)
     built = []
     deps = SRC + [os.path.join(HERE, "csrc", "lag2d_device.cuh"), os.path.join(HERE, "csrc", "lag2d_tables.inc"),
-                  os.path.join(HERE, "csrc", "lag2d_fast_tables.h"),
+                  os.path.join(HERE, "csrc", "lag2d_fast_tables.h"), os.path.join(HERE, "csrc", "lag2d_shape9.cuh"), os.path.join(HERE, "csrc", "lag2d_p1.h"),
                   os.path.join(ROOT, "include", "lag2d.h")]
     newest = max(os.path.getmtime(p) for p in deps)
     for name, fmad in targets().items():

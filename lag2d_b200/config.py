@@ -13,7 +13,7 @@ from typing import Tuple
 
 import numpy as np
 
-from .mesh import Mesh, hybrid_mesh, polar_mesh, quad_mesh
+from .mesh import Mesh, hybrid_mesh, linear_quad_mesh, polar_mesh, quad_mesh
 
 __all__ = ["StepConfig", "workload", "WORKLOADS", "noh_parity_config", "initial_density_factors"]
 
@@ -95,6 +95,17 @@ def _noh(n: int) -> Tuple[Mesh, StepConfig]:
     return m, c
 
 
+def _sod(nx: int, ny: int, y1: float, jitter: float = 0.0) -> Tuple[Mesh, StepConfig]:
+    """Sod shock tube on the linear P1 path (``ncurv = 0, nfint = 1``): straight
+    4-node quads on [0,1] x [0,y1], gamma 1.4, SSP-RK2, CFL 0.3, t_end 0.2.
+    The initial state follows the reference's rule, which is radial: rho = 1,
+    e = 2.5 where the cell centre lies within 0.5 of the origin, rho = 0.125,
+    e = 2 elsewhere (getunkin, Getrhslagmc.f90:5599-5614); slip walls all round."""
+    m = linear_quad_mesh(nx, ny, 0.0, 1.0, 0.0, y1, jitter=jitter)
+    c = StepConfig(npoly=1, ndegr=3, mdegr=3, ncase=6, gamlg=1.4, nstag=2, cfl=0.3, tend=0.2)
+    return m, c
+
+
 def initial_density_factors(mesh: Mesh, sigma: float = 0.01, seed: int = 5678) -> np.ndarray:
     """Per-cell initial-density factors 1 + sigma N(0, 1) (seeded), in cell
     order (triangles first), for lag2d_set_rho0 / Lag2DSolver.set_rho0: the
@@ -135,6 +146,12 @@ WORKLOADS = {
     "noh100": lambda: _noh(100),
     "noh16": lambda: _noh(16),
     "noh8": lambda: _noh(8),
+    # Sod on straight 4-node quads, P1 (the linear branch): the reference's 200 x 10
+    # cells on [0,1] x [0,0.1], a small and a jittered case, and a 1024 x 512 one
+    "sod200": lambda: _sod(200, 10, 0.1),
+    "sod40": lambda: _sod(40, 4, 0.1),
+    "sod_jitter40": lambda: _sod(40, 8, 0.2, jitter=0.15),
+    "sod1024": lambda: _sod(1024, 512, 0.5),
 }
 
 

@@ -13,6 +13,7 @@
 
 #include "lag2d.h"
 #include "lag2d_device.cuh"
+#include "lag2d_p1.h"
 
 namespace lag2d {
 void set_tables(const QuadTables &q, cudaStream_t st);
@@ -100,6 +101,7 @@ struct lag2d_handle {
   bool timing = false;
   std::map<std::string, Family> fam;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  p1::Solver *p1 = nullptr;    // the linear P1 path (npoly = 1) when set; Dev d is then unused
 };
 
 template <typename T>
@@ -115,7 +117,8 @@ static int dalloc(lag2d_handle *h, T **p, size_t n) {
 
 // Quadrature literals of ruqope / ruqope_lobatto (dgflo2d.f90:2497-2783),
 // points ordered as the reference's 2-D loops produce them.
-static void fill_rule(int n, bool lobatto, double (*pos)[2], double *w) {
+namespace lag2d {
+void fill_rule(int n, bool lobatto, double (*pos)[2], double *w) {
   double p[6], q[6];
   if (lobatto) {
     p[0] = -1.0; p[1] = -0.6546536707079771437983; p[2] = 0.0; p[3] = 0.6546536707079771437983; p[4] = 1.0;
@@ -146,6 +149,7 @@ static void fill_rule(int n, bool lobatto, double (*pos)[2], double *w) {
     }
 }
 
+}  // namespace lag2d
 static const int kIPQSG[4][4] = {{0, 4, 8, 7}, {4, 1, 5, 8}, {8, 5, 2, 6}, {7, 8, 6, 3}};
 
 // 7-point triangle rule of rutope (dgflo2d.f90:2232-2254), the reference's literals
@@ -401,18 +405,64 @@ static int read_status(lag2d_handle *h) {
   return LAG2D_OK;
 }
 
+// npoly = 1: the linear branch on straight 4-node quads (ipqua(4, nquad)),
+// quads only, ndens = 1, the cases without a source term
+static int create_p1(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out) {
+  if (m->ntria > 0) return fail(LAG2D_EUNSUP, "the P1 path is built for quads only (ntria = 0)");
+  if (c->ndegr != 3 || c->nq != 4 || c->ndens != 1 || c->nlimi != 6)
+    return fail(LAG2D_EUNSUP, "the P1 path needs ndegr=3, nq=4, ndens=1, nlimi=6");
+  if (c->mdegr < 1 || c->mdegr > 3) return fail(LAG2D_EINVAL, "mdegr out of range");
+  if (c->nstag != 2 && c->nstag != 3) return fail(LAG2D_EINVAL, "nstag must be 2 or 3");
+  if (c->precision != 0) return fail(LAG2D_EUNSUP, "the P1 path is FP64 only (precision = 0)");
+  if (c->nsedov < 0 || c->nsedov > 4) return fail(LAG2D_EINVAL, "nsedov must be 0..4");
+  if (c->ncase != 3 && c->ncase != 6 && c->ncase != 7)
+    return fail(LAG2D_EUNSUP, "the P1 path is built for the cases 3, 6 and 7");
+  if (m->esuv2[0] != 0) return fail(LAG2D_EINVAL, "esuv2(1) must be 0");
+  for (int p = 0; p < m->npoin; p++)
+    if (m->esuv2[p + 1] < m->esuv2[p]) return fail(LAG2D_EINVAL, "esuv2 not monotone");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LAG2D_ENODEV, "no CUDA device");
+  lag2d_handle *h = new lag2d_handle();
+  h->cfg = *c;
+  h->d.nquad = m->nquad; h->d.npoin = m->npoin; h->d.ncell = m->nquad; h->d.nbfac = m->nbfac;
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return fail(LAG2D_ECUDA, "cudaStreamCreate failed");
+  }
+  std::string err;
+  int r = p1::create(m, c, h->st, &h->p1, err);
+  if (r) {
+    cudaStreamDestroy(h->st);
+    delete h;
+    return fail(r, err);
+  }
+  *out = h;
+  return LAG2D_OK;
+}
+
+// forwards a P1 call, turning its message into the thread's last error
+#define P1_CALL(expr)              \
+  do {                             \
+    std::string err_;              \
+    int r_ = (expr);               \
+    if (r_) return fail(r_, err_); \
+    return LAG2D_OK;               \
+  } while (0)
+
 extern "C" {
 
 const char *lag2d_last_error(void) { return g_err.c_str(); }
 
 int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out) {
   if (!m || !c || !out) return fail(LAG2D_EINVAL, "null argument");
+  (void)cudaGetLastError();  // an earlier call's launch error is not this handle's
   *out = nullptr;
   if (m->nquad <= 0 || m->npoin <= 0 || m->nbfac < 0 || m->ntria < 0)
     return fail(LAG2D_EINVAL, "mesh sizes must be positive");
   if (!m->ipqua || !m->bface || !m->esuv1 || !m->esuv2 || !m->esqua || !m->coold)
     return fail(LAG2D_EINVAL, "missing mesh array");
   if (m->ntria > 0 && !m->iptri) return fail(LAG2D_EINVAL, "missing iptri");
+  if (c->npoly == 1) return create_p1(m, c, out);
   if (m->ntria > 0 && (c->ngausd != 7 || c->ngausd_geo != 7))
     return fail(LAG2D_EUNSUP, "triangles need the 7-point rule (ngausd = ngausd_geo = 7)");
   if (c->npoly != 2 || c->ndegr != 6 || c->nq != 4 || c->ndens != 1)
@@ -613,6 +663,7 @@ static int download_xy(lag2d_handle *h, const double *X, const double *Y, double
 
 int lag2d_set_rho0(lag2d_handle *h, const double *rho0) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
+  if (h->p1) return fail(LAG2D_EUNSUP, "the initial-density hook is built for the P2 path");
   Dev &d = h->d;
   if (rho0) {
     for (int e = 0; e < d.ncell; e++)
@@ -637,6 +688,7 @@ int lag2d_set_rho0(lag2d_handle *h, const double *rho0) {
 
 int lag2d_init_fields(lag2d_handle *h, double *geoel, double *amatr, double *unkno) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
+  if (h->p1) P1_CALL(p1::init_fields(h->p1, geoel, amatr, unkno, err_));
   Dev &d = h->d;
   const int ncell = d.ncell, np = d.npoin;
   run(h, "init", [&] { launch_tri_init(d, h->st); launch_init(d, h->st); }, 2 + (d.ntria > 0));
@@ -665,6 +717,7 @@ int lag2d_init_fields(lag2d_handle *h, double *geoel, double *amatr, double *unk
 int lag2d_set_state(lag2d_handle *h, const double *unkno, const double *coord, const double *ustar,
                     const double *geoel, const double *amatr) {
   if (!h || !unkno || !coord || !ustar) return fail(LAG2D_EINVAL, "null argument");
+  if (h->p1) P1_CALL(p1::set_state(h->p1, unkno, coord, ustar, geoel, amatr, err_));
   Dev &d = h->d;
   const int ncell = d.ncell, np = d.npoin;
   // straight copies of the caller's buffers (pinned buffers go at full link
@@ -717,6 +770,7 @@ static int get_scalars(lag2d_handle *h, Scalars *s) {
 
 int lag2d_step(lag2d_handle *h, int itime, double *dtfix, double *tacru) {
   if (!h || !dtfix || !tacru) return fail(LAG2D_EINVAL, "null argument");
+  if (h->p1) P1_CALL(p1::step(h->p1, itime, dtfix, tacru, err_));
   int r = put_scalars(h, itime, *dtfix, *tacru);
   if (r) return r;
   enqueue_step(h, itime);
@@ -731,6 +785,7 @@ int lag2d_step(lag2d_handle *h, int itime, double *dtfix, double *tacru) {
 
 int lag2d_run(lag2d_handle *h, int itime0, int nsteps, double *dtfix, double *tacru, int *done) {
   if (!h || !dtfix || !tacru || nsteps < 0) return fail(LAG2D_EINVAL, "bad argument");
+  if (h->p1) P1_CALL(p1::run(h->p1, itime0, nsteps, dtfix, tacru, done, err_));
   int r = put_scalars(h, itime0 - 1, *dtfix, *tacru);
   if (r) return r;
   int steps = 0;
@@ -769,6 +824,7 @@ int lag2d_run(lag2d_handle *h, int itime0, int nsteps, double *dtfix, double *ta
 
 int lag2d_get_state(lag2d_handle *h, double *unkno, double *coord, double *ustar, double *geoel) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
+  if (h->p1) P1_CALL(p1::get_state(h->p1, unkno, coord, ustar, geoel, err_));
   int r;
   if (unkno && (r = download_unkno(h, unkno))) return r;
   if (coord && (r = download_xy(h, h->d.xn, h->d.yn, coord))) return r;
@@ -779,6 +835,11 @@ int lag2d_get_state(lag2d_handle *h, double *unkno, double *coord, double *ustar
 
 int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
+  if (h->p1) {
+    // no troubled-cell marking on the P1 branch
+    if (flags) std::fill(flags, flags + h->d.ncell, 0);
+    P1_CALL(p1::rhs(h->p1, rhsel, err_));
+  }
   Dev &d = h->d;
   int r = put_scalars(h, itime, 0.0, 0.0);
   if (r) return r;
@@ -827,6 +888,7 @@ int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
 
 int lag2d_weno(lag2d_handle *h, const int *flags) {
   if (!h || !flags) return fail(LAG2D_EINVAL, "null argument");
+  if (h->p1) return fail(LAG2D_EUNSUP, "WENO is not on the P1 branch");
   Dev &d = h->d;
   int r = put_scalars(h, 1, 0.0, 0.0);
   if (r) return r;
@@ -842,6 +904,7 @@ int lag2d_weno(lag2d_handle *h, const int *flags) {
 
 int lag2d_cellvol(lag2d_handle *h, double *geoel) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
+  if (h->p1) P1_CALL(p1::cellvol(h->p1, geoel, err_));
   run(h, "geom", [&] { geom_all(h, h->d.xs, h->d.ys); }, 1 + (h->d.ntria > 0));
   int r = read_status(h);
   if (r) return r;
@@ -849,12 +912,16 @@ int lag2d_cellvol(lag2d_handle *h, double *geoel) {
   return LAG2D_OK;
 }
 
-long long lag2d_kernel_launches(const lag2d_handle *h) { return h ? h->launches : -1; }
+long long lag2d_kernel_launches(const lag2d_handle *h) {
+  if (!h) return -1;
+  return h->p1 ? p1::launches(h->p1) : h->launches;
+}
 
 void *lag2d_stream(const lag2d_handle *h) { return h ? (void *)h->st : nullptr; }
 
 int lag2d_timing(lag2d_handle *h, int enable) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
+  if (h->p1) p1::set_timing(h->p1, enable != 0);
   h->timing = enable != 0;
   h->fam.clear();
   return LAG2D_OK;
@@ -862,6 +929,7 @@ int lag2d_timing(lag2d_handle *h, int enable) {
 
 double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *launches) {
   if (!h || !family) return -1.0;
+  if (h->p1) return p1::kernel_ms(h->p1, family, launches);
   auto it = h->fam.find(family);
   if (it == h->fam.end() || it->second.n == 0) return -1.0;
   if (launches) *launches = it->second.n;
@@ -994,6 +1062,7 @@ struct Snapshot {
 };
 
 static int adjoint_supported(lag2d_handle *h) {
+  if (h->p1) return fail(LAG2D_EUNSUP, "the adjoint is built for the P2 path");
   if (h->cfg.order_exact)
     return fail(LAG2D_EUNSUP, "the adjoint follows the optimised step (order_exact 0)");
   return LAG2D_OK;
@@ -1189,6 +1258,7 @@ int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every,
 
 void lag2d_destroy(lag2d_handle *h) {
   if (!h) return;
+  if (h->p1) p1::destroy(h->p1);
   if (h->st) cudaStreamSynchronize(h->st);
   for (auto &p : h->pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
   if (h->graph) cudaGraphExecDestroy(h->graph);

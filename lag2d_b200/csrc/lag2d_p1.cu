@@ -1,0 +1,1348 @@
+// The linear P1 time step of Lag2D on straight 4-node quads (sm_100a): the
+// branch ncurv = 0, nriem = 1, nfint = 1, nlimi = 6, nrz = 0 of
+// getrhsdg_lag_mcnew (srccurv-lag/Getrhslagmc.f90:6810-6980, slope
+// application :7283-7298) inside getsolvdg_lag (Getrhslag.f90:1553-2035),
+// the configuration of the reference's Sod shock tube.
+//
+// One RK stage is
+//   bounds  (nodes)  Barth node bounds of (tau, u, v, p, e) over the cells
+//                    around each node (barthlimit_lag_vtxunknew,
+//                    Getrhslagmctria.f90:2373-2643)
+//   cell    (quads)  the limiter (barthlimit_lagsym_quad, Limiterlag.f90:
+//                    4-404, with barthlimit_sympre_quadlb :8127-8692 and
+//                    barthfct, Getrhslagmc.f90:9171-9222) and the corner
+//                    Riemann coefficients (getriem_quad_matrixsym,
+//                    Limiterlag.f90:708-1033, getriecoef_matrixnew :1037)
+//   node    (nodes)  fixed-order gather of the corner coefficients, the 2x2
+//                    nodal solve and the wall conditions
+//                    (getndvelo_lag_mc_matrixsym, Limiterlag.f90:408-704)
+//   rhs     (quads)  corner forces, face integral (rhsifacedg_lag_mc_
+//                    hybridquad2, Getrhslagmc.f90:14468-14618), volume
+//                    integral (rhsdomndg_lag_mc_quadsym, Limiterlag.f90:
+//                    1108-1490), then (stages after the first) the limited
+//                    slopes and the M^-1 update fused in
+//   dt, update (stage 1), nodes, geom (getcellvol_lag on the 9-node image of
+//                    the straight quad, Limiterlag.f90:2038-2165)
+//
+// Calls of the reference branch that do not change its result are not
+// made: getbc_lagmaire2 (Getrhslag.f90:11269) forms a boundary force that the
+// nodal solve leaves unused, getAS_llnl (Limiterlag.f90:15476) ends by
+// zeroing its stress, and the divergence limiter of
+// barthlimit_sympre_quadlb writes only geoel(10), which this branch never
+// reads.  Arithmetic keeps the reference's expression order, so the build
+// with --fmad=false reproduces the CPU restatement bit for bit.
+//
+// Layout in HBM (0-based, structure of arrays):
+//   U[(q*3 + k)*ncell + e]        P1 DOF k of field q (tau, u, v, e)
+//   ipq[k*nquad + iq]             vertex k (0..3, counter-clockwise) of quad iq
+//   cf[(v*8 + f + 2*iv)*nquad+iq] corner-face coefficient v (m, m u, m v,
+//                                 sigma.n A x, y) of corner iv, face f
+//   lim[k*ncell + e]              aflim(1), aflim(4), aflim(5), afvec(1,1),
+//                                 afvec(1,2), afvec(2,1), afvec(2,2)
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "lag2d.h"
+#include "lag2d_device.cuh"
+#include "lag2d_p1.h"
+#include "lag2d_shape9.cuh"
+
+namespace lag2d {
+void fill_rule(int n, bool lobatto, double (*pos)[2], double *w);
+void launch_xy_in(int n, cudaStream_t st, const double *xy, double *x, double *y, double *x2, double *y2);
+void launch_xy_out(int n, cudaStream_t st, double *xy, const double *x, const double *y);
+
+namespace p1 {
+
+constexpr int ND = 3;            // P1 Taylor basis
+constexpr int NU1 = ND * NQ;     // 12 DOFs per cell
+
+// Literals the Fortran writes in single precision (`eps = 1.e-6`,
+// `1.e-11`), widened to double as gfortran does.
+#define EPS_S ((double)1.0e-6f)
+#define TINY_S ((double)1.0e-11f)
+
+// node flags
+constexpr unsigned char BC_V0 = 1;    // bface 22 / 221: v* = 0
+constexpr unsigned char BC_U0 = 2;    // bface 22 / 222: u* = 0
+constexpr unsigned char BC_UV0 = 4;   // bface 25: u* = v* = 0
+constexpr unsigned char BC_KEEP = 8;  // no nodal solve (indnd = 1)
+
+struct Dev1 {
+  int nquad, npoin, ncell, mdegr, ncase, nsedov, sedov_cell[4];
+  double gamlg, cfl, cimpd, tend, sedov_energy;
+  const int *ipq;                     // [4][nquad]
+  const int *esuv_ptr, *esuv;         // cells around each node (0-based)
+  const int *ncor_ptr, *ncor;         // corners (iq*4 + iv) at each node, cells ascending
+  const unsigned char *bc;            // [npoin] BC_* flags
+  const unsigned char *wall;          // [npoin] limiter wall class 0, 2, 3, 10
+  const double *x0, *y0;              // initial coordinates
+  double *rc, *sc, *vol, *vcx, *vcy, *mass, *amatr;  // amatr [4][ncell]
+  double *Un, *Us;                    // [12][ncell]
+  double *xn, *yn, *xs, *ys, *us, *vs;
+  double *bmax, *bmin;                // [5][npoin]
+  double *lim;                        // [7][ncell]
+  double *cf;                         // [5][8][nquad]
+  double *rhs;                        // [12][ncell]
+  double *dtpart;
+  Scalars *sc_dev;
+};
+
+struct Rules {
+  double g25[25][2], w25[25];
+  double g36[36][2], w36[36];
+};
+__constant__ Rules cR;
+
+__device__ __forceinline__ bool stopped(const Dev1 &d) { return d.sc_dev->done != 0; }
+__device__ __forceinline__ double U(const Dev1 &d, const double *A, int k, int q, int e) {
+  return A[(q * ND + k) * (size_t)d.ncell + e];
+}
+
+__device__ __forceinline__ void load4(const Dev1 &d, const double *X, const double *Y, int iq, double (*xp)[2]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int p = d.ipq[k * d.nquad + iq];
+    xp[k][0] = X[p];
+    xp[k][1] = Y[p];
+  }
+}
+
+// the straight quad's 9-node image (Limiterlag.f90:2040-2048)
+__device__ __forceinline__ void image9(const double (*x4)[2], double (*xp)[2]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) { xp[k][0] = x4[k][0]; xp[k][1] = x4[k][1]; }
+#pragma unroll
+  for (int c = 0; c < 2; c++) {
+    xp[4][c] = 0.5 * (xp[0][c] + xp[1][c]);
+    xp[5][c] = 0.5 * (xp[1][c] + xp[2][c]);
+    xp[6][c] = 0.5 * (xp[2][c] + xp[3][c]);
+    xp[7][c] = 0.5 * (xp[3][c] + xp[0][c]);
+    xp[8][c] = 0.5 * (xp[4][c] + xp[6][c]);
+  }
+}
+
+// bilinear Jacobian at (r, s) (Limiterlag.f90:8262-8282)
+__device__ __forceinline__ void jac4(const double (*x)[2], double r, double s, double &dxdr, double &dxds,
+                                     double &dydr, double &dyds) {
+  const double rp = 1.0 + r, rm = 1.0 - r, sp = 1.0 + s, sm = 1.0 - s;
+  const double dr[4] = {-0.25 * sm, 0.25 * sm, 0.25 * sp, -0.25 * sp};
+  const double ds[4] = {-0.25 * rm, -0.25 * rp, 0.25 * rp, 0.25 * rm};
+  double a = 0.0, b = 0.0, c = 0.0, e = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    a = a + dr[k] * x[k][0];
+    b = b + ds[k] * x[k][0];
+    c = c + dr[k] * x[k][1];
+    e = e + ds[k] * x[k][1];
+  }
+  dxdr = a; dxds = b; dydr = c; dyds = e;
+}
+
+__device__ __forceinline__ double barthfct(double umax, double umin, double uctr, double dunk) {
+  const double coef = 0.7;
+  double fiy;
+  if (dunk > 1.0e-8) {
+    fiy = coef * (umax - uctr) / dunk;
+    return fmin((fiy * fiy + 2.0 * fiy) / (fiy * fiy + fiy + 2.0), 1.0);
+  } else if (dunk < -1.0e-8) {
+    fiy = coef * (umin - uctr) / dunk;
+    return fmin((fiy * fiy + 2.0 * fiy) / (fiy * fiy + fiy + 2.0), 1.0);
+  }
+  return 1.0;
+}
+
+__device__ __forceinline__ double xv(int iv) { return (iv == 0 || iv == 3) ? -1.0 : 1.0; }
+__device__ __forceinline__ double yv(int iv) { return (iv < 2) ? -1.0 : 1.0; }
+
+// ---------------------------------------------------------------------------
+// Initial geometry and fields: getgeoel_initial_lag (GetInitial.f90:1484-
+// 1694), inifield_mcnew (Getrhslagmc.f90:3621-3917) and getunkno_initial_lag
+// (GetInitial.f90:412-690) on the 9-node image, npoly = 1
+// ---------------------------------------------------------------------------
+__device__ double rho_initial1(const Dev1 &d, double xc, double yc) {
+  if (d.ncase == 6) return (sqrt(xc * xc + yc * yc) <= 0.5) ? 1.0 : 0.125;
+  return 1.0;
+}
+
+__device__ void getunkin1(const Dev1 &d, double *unkin, double xg, double yg, int ielem1, double volel, double xc,
+                          double yc) {
+  const double g = d.gamlg;
+  double rhoini = 1.0, uini = 0.0, vini = 0.0, pini = 1.0;
+  if (d.ncase == 3) {
+    uini = -xg / sqrt(xg * xg + yg * yg);
+    vini = -yg / sqrt(xg * xg + yg * yg);
+    pini = 1.0e-6;
+  } else if (d.ncase == 6) {
+    double ieini;
+    if (sqrt(xc * xc + (yc - 0.0) * (yc - 0.0)) <= 0.5) { rhoini = 1.0; ieini = 2.5; }
+    else { rhoini = 0.125; ieini = 2.0; }
+    pini = ieini * (g - 1.0) * rhoini;
+  } else if (d.ncase == 7) {
+    bool hit = false;
+    for (int i = 0; i < d.nsedov; i++) hit |= (d.sedov_cell[i] == ielem1);
+    pini = hit ? (g - 1.0) * 1.0 * d.sedov_energy / (1.0 * volel) : 1.0e-6;
+  }
+  unkin[0] = 1.0;
+  unkin[1] = rhoini * uini;
+  unkin[2] = rhoini * vini;
+  unkin[3] = (pini / rhoini / (g - 1.0) + 0.5 * (uini * uini + vini * vini)) * rhoini;
+}
+
+__global__ void k1_init_geo(Dev1 d) {
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iq >= d.nquad) return;
+  const double alfrz = 0.0;
+  double x4[4][2], xp[9][2], shp[9], dr[9], ds[9];
+  load4(d, d.x0, d.y0, iq, x4);
+  image9(x4, xp);
+  double xc, yc;
+  shp9v(0.0, 0.0, shp);
+  map9(xp, shp, xc, yc);
+  double xcent = 0, ycent = 0, volel = 0, masel = 0;
+  for (int ig = 0; ig < 36; ig++) {
+    const double r = cR.g36[ig][0], s = cR.g36[ig][1], wi = cR.w36[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    const double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    const double rhog = rho_initial1(d, xc, yc);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    masel = masel + rhog * djaco * rcoef;
+    volel = volel + djaco * rcoef;
+    xcent = xcent + rhog * r * djaco * rcoef;
+    ycent = ycent + rhog * s * djaco * rcoef;
+  }
+  d.rc[iq] = xcent / masel;
+  d.sc[iq] = ycent / masel;
+  d.vol[iq] = volel;
+  d.mass[iq] = masel;
+}
+
+__global__ void k1_init_fields(Dev1 d) {
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iq >= d.nquad) return;
+  const int e = iq;
+  const double alfrz = 0.0;
+  double x4[4][2], xp[9][2], shp[9], dr[9], ds[9];
+  load4(d, d.x0, d.y0, iq, x4);
+  image9(x4, xp);
+  const double volel = d.vol[e], masel = d.mass[e], rc = d.rc[e], sc = d.sc[e];
+  double unkin[4], rv[4] = {0, 0, 0, 0};
+  const double xcel = xp[8][0], ycel = xp[8][1];
+  for (int ig = 0; ig < 25; ig++) {
+    const double r = cR.g25[ig][0], s = cR.g25[ig][1], wi = cR.w25[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    const double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    getunkin1(d, unkin, xg, yg, e + 1, volel, xcel, ycel);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
+  }
+  double xc, yc;
+  shp9v(rc, sc, shp);
+  map9(xp, shp, xc, yc);
+  double rhsini[ND][4], mm[4] = {0.0, 0.0, 0.0, 0.0}, f0 = 0.0;
+  for (int k = 0; k < ND; k++)
+    for (int q = 0; q < 4; q++) rhsini[k][q] = 0.0;
+  for (int ig = 0; ig < 25; ig++) {
+    const double r = cR.g25[ig][0], s = cR.g25[ig][1], wi = cR.w25[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    const double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    getunkin1(d, unkin, xg, yg, e + 1, volel, xc, yc);
+    const double bq[ND] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < ND; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bq[k] * djaco;
+    const double rho0 = rho_initial1(d, xc, yc);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    f0 = f0 + rho0 * djaco * rcoef;
+    // mmatr(1,1), (2,1), (1,2), (2,2) (GetInitial.f90:622-627); (2,1) is not used
+    mm[0] = mm[0] + rho0 * bq[1] * bq[1] * djaco * rcoef;
+    mm[2] = mm[2] + rho0 * bq[1] * bq[2] * djaco * rcoef;
+    mm[3] = mm[3] + rho0 * bq[2] * bq[2] * djaco * rcoef;
+  }
+  const double det = mm[0] * mm[3] - mm[2] * mm[2];
+  const double a1 = mm[3] / det, a2 = -mm[2] / det, a3 = mm[0] / det;
+  d.amatr[0 * (size_t)d.ncell + e] = a1;
+  d.amatr[1 * (size_t)d.ncell + e] = a2;
+  d.amatr[2 * (size_t)d.ncell + e] = a3;
+  d.amatr[3 * (size_t)d.ncell + e] = 1.0 / f0;
+  const double mi[2][2] = {{a1, a2}, {a2, a3}};
+  for (int q = 0; q < 4; q++) {
+    d.Un[(q * ND + 0) * (size_t)d.ncell + e] = rv[q] / masel;
+    for (int ix = 0; ix < 2; ix++) {
+      double acc = 0.0;
+      for (int iy = 0; iy < 2; iy++) acc = acc + mi[ix][iy] * rhsini[iy + 1][q];
+      d.Un[(q * ND + ix + 1) * (size_t)d.ncell + e] = acc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// getcellvol_lag on the 9-node image (Limiterlag.f90:2038-2165)
+// ---------------------------------------------------------------------------
+__global__ void k1_geom(Dev1 d, const double *X, const double *Y) {
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iq >= d.nquad || stopped(d)) return;
+  const double alfrz = 0.0;
+  double x4[4][2], xp[9][2], shp[9], dr[9], ds[9];
+  load4(d, X, Y, iq, x4);
+  image9(x4, xp);
+  double rcv = 0.0, scv = 0.0, volel = 0.0;
+  for (int ig = 0; ig < 36; ig++) {
+    const double r = cR.g36[ig][0], s = cR.g36[ig][1], wi = cR.w36[ig];
+    shp9v(r, s, shp);
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    double xg, yg;
+    map9(xp, shp, xg, yg);
+    const double rcoef = 1.0 - alfrz + alfrz * yg;
+    const double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    volel = volel + djaco * rcoef;
+    rcv = rcv + r * djaco * rcoef;
+    scv = scv + s * djaco * rcoef;
+  }
+  d.vol[iq] = volel;
+  d.vcx[iq] = rcv / volel;
+  d.vcy[iq] = scv / volel;
+  if (!(volel > 0.0)) atomicOr(&d.sc_dev->status, ST_NONPHYS);
+}
+
+// ---------------------------------------------------------------------------
+// Node bounds (barthlimit_lag_vtxunknew, Getrhslagmctria.f90:2548-2641):
+// max/min over the cells around the node, so the visiting order is free
+// ---------------------------------------------------------------------------
+__global__ void k1_bounds(Dev1 d) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= d.npoin || stopped(d)) return;
+  const double g = d.gamlg;
+  double mx[5], mn[5];
+#pragma unroll
+  for (int q = 0; q < 5; q++) { mx[q] = -1.0e10; mn[q] = 1.0e10; }
+  for (int i = d.esuv_ptr[p]; i < d.esuv_ptr[p + 1]; i++) {
+    const int e = d.esuv[i];
+    const double rhom = U(d, d.Us, 0, 0, e);
+    const double uctr = U(d, d.Us, 0, 1, e), vctr = U(d, d.Us, 0, 2, e), ectr = U(d, d.Us, 0, 3, e);
+    const double rhoct = 1.0 / rhom;
+    const double pctr = fmax(EPS_S, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    const double v[5] = {rhom, uctr, vctr, pctr, ectr};
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      if (v[q] > mx[q]) mx[q] = v[q];
+      if (v[q] < mn[q]) mn[q] = v[q];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 5; q++) {
+    d.bmax[q * (size_t)d.npoin + p] = mx[q];
+    d.bmin[q * (size_t)d.npoin + p] = mn[q];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Limiter and corner coefficients of one quad
+// ---------------------------------------------------------------------------
+__device__ void cell_pass(const Dev1 &d, int iq) {
+  const int e = iq;
+  const double g = d.gamlg, epsd = 1.0e-6, slpdu = (g + 1.0) / 2.0;
+  double x4[4][2];
+  load4(d, d.xs, d.ys, iq, x4);
+  int ip[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) ip[k] = d.ipq[k * d.nquad + iq];
+  const double rc = d.rc[e], sc = d.sc[e];
+  double u[4][ND];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < ND; k++) u[q][k] = U(d, d.Us, k, q, e);
+  double bq[4][ND];
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (xv(iv) - rc) / 1.0; bq[iv][2] = (yv(iv) - sc) / 1.0; }
+  // vertex values of the unlimited DOFs
+  double uvq[4][4];
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      double a = 0.0;
+      for (int k = 0; k < d.mdegr; k++) a = a + u[q][k] * bq[iv][k];
+      uvq[iv][q] = a;
+    }
+  const double rhom = u[0][0], uctr = u[1][0], vctr = u[2][0], ectr = u[3][0];
+  const double rhoct = 1.0 / rhom;
+  const double pctr_s = fmax(EPS_S, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+
+  // (1) aflim(1..4) against the node bounds (Limiterlag.f90:69-188)
+  double af[4];
+  {
+    const double unctr[4] = {1.0 / rhoct, uctr, vctr, pctr_s};
+#pragma unroll
+    for (int q = 0; q < 4; q++) af[q] = 0.0;
+#pragma unroll
+    for (int iv = 0; iv < 4; iv++) {
+      const double rhov = 1.0 / uvq[iv][0];
+      const double uv = uvq[iv][1], vv = uvq[iv][2], ev = uvq[iv][3];
+      const double pvtx = fmax(EPS_S, (g - 1.0) * rhov * (ev - 0.5 * (uv * uv + vv * vv)));
+      const double w[4] = {1.0 / rhov, uv, vv, pvtx};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const double dunk = w[q] - unctr[q];
+        const double a = barthfct(d.bmax[q * (size_t)d.npoin + ip[iv]], d.bmin[q * (size_t)d.npoin + ip[iv]],
+                                  unctr[q], dunk);
+        if (iv == 0 || a < af[q]) af[q] = a;
+      }
+    }
+  }
+
+  // (2) the velocity limited in the principal frame of the strain rate
+  // (barthlimit_sympre_quadlb, Limiterlag.f90:8242-8692)
+  double m11 = 0.0, m12 = 0.0, m21 = 0.0, m22 = 0.0;
+  {
+    const double dudr = u[1][1] / 1.0, duds = u[1][2] / 1.0, dvdr = u[2][1] / 1.0, dvds = u[2][2] / 1.0;
+    double dxdr, dxds, dydr, dyds;
+    jac4(x4, rc, sc, dxdr, dxds, dydr, dyds);
+    const double jacom = dxdr * dyds - dydr * dxds;
+    const double drdx = dyds / jacom, drdy = -dxds / jacom, dsdx = -dydr / jacom, dsdy = dxdr / jacom;
+    const double dudx = dudr * drdx + duds * dsdx, dudy = dudr * drdy + duds * dsdy;
+    const double dvdx = dvdr * drdx + dvds * dsdx, dvdy = dvdr * drdy + dvds * dsdy;
+    const double matra = dudx, matrb = 0.5 * (dudy + dvdx), matrc = matrb, matrd = dvdy;
+    const double mapt = matra + matrd, mapd = matra * matrd - matrb * matrc;
+    const double lamda1 = 0.5 * mapt + sqrt(0.25 * (mapt * mapt) - mapd);
+    const double lamda2 = 0.5 * mapt - sqrt(0.25 * (mapt * mapt) - mapd);
+    if (fabs(matrc) > 1.0e-8) {
+      const double lmat1 = sqrt((lamda1 - matrd) * (lamda1 - matrd) + matrc * matrc);
+      const double lmat2 = sqrt((lamda2 - matrd) * (lamda2 - matrd) + matrc * matrc);
+      const double a1 = (lamda1 - matrd) / lmat1, b1 = matrc / lmat1;
+      const double a2 = (lamda2 - matrd) / lmat2, b2 = matrc / lmat2;
+      if (matrc > 0.0) { m11 = a1; m12 = b1; m21 = a2; m22 = b2; }
+      else { m21 = a1; m22 = b1; m11 = a2; m12 = b2; }
+    }
+  }
+  double fl1 = 0.0, fl2 = 0.0;
+  {
+    const double uc = uctr * m11 + vctr * m12, vc = uctr * m21 + vctr * m22;
+#pragma unroll 1
+    for (int iv = 0; iv < 4; iv++) {
+      const double ur = uvq[iv][1] * m11 + uvq[iv][2] * m12;
+      const double vr = uvq[iv][1] * m21 + uvq[iv][2] * m22;
+      double mx1 = uc, mx2 = vc, mn1 = uc, mn2 = vc;
+      const int p = ip[iv];
+      const int cls = (d.ncase != 1) ? d.wall[p] : 0;
+      for (int i = d.esuv_ptr[p]; i < d.esuv_ptr[p + 1]; i++) {
+        const int je = d.esuv[i];
+        const double uj = U(d, d.Us, 0, 1, je), vj = U(d, d.Us, 0, 2, je);
+        // the cell's own average, then its images across the walls at the node
+        double iu[4], iv2[4];
+        int n = 0;
+        iu[n] = uj; iv2[n] = vj; n++;
+        if (cls == 3) { iu[n] = uj; iv2[n] = -vj; n++; }
+        else if (cls == 2) { iu[n] = -uj; iv2[n] = vj; n++; }
+        else if (cls == 10) {
+          iu[n] = uj; iv2[n] = -vj; n++;
+          iu[n] = -uj; iv2[n] = vj; n++;
+          iu[n] = -uj; iv2[n] = -vj; n++;
+        }
+        for (int k = 0; k < n; k++) {
+          const double ul = iu[k] * m11 + iv2[k] * m12;
+          const double vl = iu[k] * m21 + iv2[k] * m22;
+          mx1 = fmax(mx1, ul); mx2 = fmax(mx2, vl);
+          mn1 = fmin(mn1, ul); mn2 = fmin(mn2, vl);
+        }
+      }
+      const double a1 = barthfct(mx1, mn1, uc, ur - uc);
+      const double a2 = barthfct(mx2, mn2, vc, vr - vc);
+      if (iv == 0 || a1 < fl1) fl1 = a1;
+      if (iv == 0 || a2 < fl2) fl2 = a2;
+    }
+  }
+  // afvec = R^T diag(fixi, fiet) R, R = mapmt (Limiterlag.f90:8679-8691)
+  const double fi11 = (m11 * m11) * fl1 + (m21 * m21) * fl2;
+  const double fi12 = m11 * m12 * fl1 + m21 * m22 * fl2;
+  const double fi22 = (m12 * m12) * fl1 + (m22 * m22) * fl2;
+
+  // (3) aflim(5): the energy of the limited vertex state (Limiterlag.f90:290-380)
+  double af5 = 0.0;
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++) {
+    const double rhov = 1.0 / uvq[iv][0];
+    const double uv = uvq[iv][1], vv = uvq[iv][2], ev = uvq[iv][3];
+    const double pvtx = fmax(EPS_S, (g - 1.0) * rhov * (ev - 0.5 * (uv * uv + vv * vv)));
+    const double t = rhom + af[0] * (1.0 / rhov - rhom);
+    const double pv = pctr_s + af[3] * (pvtx - pctr_s);
+    const double e5 = pv / (g - 1.0) * t + 0.5 * (uv * uv + vv * vv);
+    const double a = barthfct(d.bmax[4 * (size_t)d.npoin + ip[iv]], d.bmin[4 * (size_t)d.npoin + ip[iv]], ectr,
+                              e5 - ectr);
+    if (iv == 0 || a < af5) af5 = a;
+  }
+  const size_t nc = d.ncell;
+  d.lim[0 * nc + e] = af[0];
+  d.lim[1 * nc + e] = af[3];
+  d.lim[2 * nc + e] = af5;
+  d.lim[3 * nc + e] = fi11;
+  d.lim[4 * nc + e] = fi12;
+  d.lim[5 * nc + e] = fi12;
+  d.lim[6 * nc + e] = fi22;
+
+  // (4) corner Riemann coefficients (getriem_quad_matrixsym, Limiterlag.f90:
+  // 708-1033): face f of quad iq joins vertices f and f+1, its normal is
+  // (dy, -dx)/|.| (getfnds_lag_mc_hybrid, Getrhslagmc.f90:2210-2262)
+  double fn[4][3];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int b = (f + 1) & 3;
+    const double anx = x4[b][1] - x4[f][1];
+    const double any = -(x4[b][0] - x4[f][0]);
+    fn[f][0] = anx / sqrt(anx * anx + any * any);
+    fn[f][1] = any / sqrt(anx * anx + any * any);
+    fn[f][2] = sqrt(anx * anx + any * any);
+  }
+  const double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  const double sdctr = sqrt(fmax(epsd, g * pctr / rhoct));
+  const double dudr = fi11 * u[1][1] + fi12 * u[2][1];
+  const double duds = fi11 * u[1][2] + fi12 * u[2][2];
+  const double dvdr = fi12 * u[1][1] + fi22 * u[2][1];
+  const double dvds = fi12 * u[1][2] + fi22 * u[2][2];
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++) {
+    const double rhovt = 1.0 / uvq[iv][0];
+    const double ev = uvq[iv][3];
+    double pvtx = fmax(epsd, (g - 1.0) * rhovt * (ev - 0.5 * (uvq[iv][1] * uvq[iv][1] + uvq[iv][2] * uvq[iv][2])));
+    const double uvl = uctr + dudr * bq[iv][1] + duds * bq[iv][2];
+    const double vvl = vctr + dvdr * bq[iv][1] + dvds * bq[iv][2];
+    pvtx = pctr + af[3] * (pvtx - pctr);
+    const double sig = -pvtx + 0.0;
+    const int p = ip[iv];
+    const double us0 = d.us[p], vs0 = d.vs[p];
+    const double acnx = us0 - uvl, acny = vs0 - vvl;
+    const double nrm = sqrt(acnx * acnx + acny * acny);
+    double aj0, aj1;
+    if (nrm < TINY_S) { aj0 = TINY_S; aj1 = TINY_S; }
+    else { aj0 = acnx / nrm; aj1 = acny / nrm; }
+    const double aj2 = nrm / sdctr;
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const int face = (f == 0) ? ((iv + 3) & 3) : iv;
+      const double n1 = fn[face][0], n2 = fn[face][1];
+      const double area = (2.0 * 1.0 + 1.0) / 3.0 * 0.5 * fn[face][2];
+      const double deltu = fabs(acnx * n1 + acny * n2);
+      const double murie = rhoct * sdctr + d.cimpd * rhoct * slpdu * deltu;
+      // getriecoef_matrixnew (Limiterlag.f90:1037-1076): a diagonal mu A
+      const double vnau = (aj2 < 1.0e12) ? 1.0 : n1 * aj0 + n2 * aj1;
+      const double m = murie * area * fabs(vnau);
+      const double mu1 = m * uvl + 0.0 * vvl;
+      const double mu2 = 0.0 * uvl + m * vvl;
+      const double s1 = sig * area * n1 + (0.0 + 0.0) * area * n2;
+      const double s2 = (0.0 + 0.0) * area * n1 + sig * area * n2;
+      const int slot = f + 2 * iv;
+      d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq] = m;
+      d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq] = mu1;
+      d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq] = mu2;
+      d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq] = s1;
+      d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq] = s2;
+    }
+  }
+}
+__global__ void __launch_bounds__(128) k1_cell(Dev1 d) {
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iq >= d.nquad || stopped(d)) return;
+  cell_pass(d, iq);
+}
+
+// ---------------------------------------------------------------------------
+// Nodal solve (getndvelo_lag_mc_matrixsym, Limiterlag.f90:478-642): the
+// corner sums in the order the reference scatters them (cells ascending,
+// corner faces 1, 2), the 2x2 solve and the wall conditions
+// ---------------------------------------------------------------------------
+__global__ void k1_node(Dev1 d) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= d.npoin || stopped(d)) return;
+  double n11 = 0.0, n21 = 0.0, n12 = 0.0, n22 = 0.0, a1 = 0.0, a2 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int i = d.ncor_ptr[p]; i < d.ncor_ptr[p + 1]; i++) {
+    const int c = d.ncor[i], iq = c >> 2, iv = c & 3;
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const int slot = f + 2 * iv;
+      const double m = d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq];
+      n11 = n11 + m;
+      n21 = n21 + 0.0;
+      n12 = n12 + 0.0;
+      n22 = n22 + m;
+      a1 = a1 + d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq];
+      a2 = a2 + d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq];
+      s1 = s1 + d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq];
+      s2 = s2 + d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq];
+    }
+  }
+  const unsigned char bc = d.bc[p];
+  double us = d.us[p], vs = d.vs[p];
+  if (!(bc & BC_KEEP)) {
+    const double detma = n11 * n22 - n21 * n12;
+    const double i11 = n22 / detma, i12 = -n12 / detma, i21 = -n21 / detma, i22 = n11 / detma;
+    const double r1 = a1 - s1, r2 = a2 - s2;
+    us = i11 * r1 + i12 * r2;
+    vs = i21 * r1 + i22 * r2;
+  }
+  if (bc & (BC_V0 | BC_UV0)) vs = 0.0;
+  if (bc & (BC_U0 | BC_UV0)) us = 0.0;
+  d.us[p] = us;
+  d.vs[p] = vs;
+}
+
+// ---------------------------------------------------------------------------
+// Limited slopes into the stage state (Getrhslagmc.f90:7283-7298) and the
+// stage update (Getrhslag.f90:1789-1904, npoly = 1)
+// ---------------------------------------------------------------------------
+__device__ void update_cell(const Dev1 &d, int e, double alfa, const double (*R)[4]) {
+  const size_t nc = d.ncell;
+  const double dt = d.sc_dev->dtfix;
+  const double af1 = d.lim[0 * nc + e], af5 = d.lim[2 * nc + e];
+  const double v11 = d.lim[3 * nc + e], v12 = d.lim[4 * nc + e], v21 = d.lim[5 * nc + e], v22 = d.lim[6 * nc + e];
+  double s[4][ND];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < ND; k++) s[q][k] = U(d, d.Us, k, q, e);
+  s[0][1] = s[0][1] * af1;
+  s[0][2] = s[0][2] * af1;
+  {
+    const double u22 = s[1][1], u32 = s[1][2], u23 = s[2][1], u33 = s[2][2];
+    s[1][1] = v11 * u22 + v12 * u23;
+    s[1][2] = v11 * u32 + v12 * u33;
+    s[2][1] = v21 * u22 + v22 * u23;
+    s[2][2] = v21 * u32 + v22 * u33;
+  }
+  s[3][1] = s[3][1] * af5;
+  s[3][2] = s[3][2] * af5;
+  double r[ND][4];
+#pragma unroll
+  for (int k = 0; k < ND; k++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) r[k][q] = dt * R[k][q];
+  const double a1 = d.amatr[0 * nc + e], a2 = d.amatr[1 * nc + e], a3 = d.amatr[2 * nc + e];
+  const double a4 = d.amatr[3 * nc + e];
+  const double mm[ND][ND] = {{a4, 0.0, 0.0}, {0.0, a1, a2}, {0.0, a2, a3}};
+  const double oma = 1.0 - alfa;
+#pragma unroll
+  for (int id = 0; id < ND; id++) {
+    double unint[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int iu = 0; iu < ND; iu++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) unint[q] = unint[q] + mm[id][iu] * r[iu][q];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const size_t idx = (q * ND + id) * nc + e;
+      d.Us[idx] = alfa * d.Un[idx] + oma * (s[q][id] + unint[q]);
+    }
+  }
+}
+
+__global__ void k1_update(Dev1 d, double alfa) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.ncell || stopped(d)) return;
+  double R[ND][4];
+#pragma unroll
+  for (int k = 0; k < ND; k++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) R[k][q] = d.rhs[(q * ND + k) * (size_t)d.ncell + e];
+  update_cell(d, e, alfa, R);
+}
+
+// ---------------------------------------------------------------------------
+// Corner forces, face and volume integrals of one quad
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iq >= d.nquad || stopped(d)) return;
+  const int e = iq;
+  const double g = d.gamlg, epsd = 1.0e-6;
+  const size_t nc = d.ncell;
+  double x4[4][2];
+  load4(d, d.xs, d.ys, iq, x4);
+  const double rc = d.rc[e], sc = d.sc[e];
+  double u[4][ND];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < ND; k++) u[q][k] = U(d, d.Us, k, q, e);
+  double fn[4][3];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int b = (f + 1) & 3;
+    const double anx = x4[b][1] - x4[f][1];
+    const double any = -(x4[b][0] - x4[f][0]);
+    fn[f][0] = anx / sqrt(anx * anx + any * any);
+    fn[f][1] = any / sqrt(anx * anx + any * any);
+    fn[f][2] = sqrt(anx * anx + any * any);
+  }
+  // face integral (rhsifacedg_lag_mc_hybridquad2)
+  const double c16 = 0.1666666666666666, c13 = 0.3333333333333333;
+  double R[ND][4];
+#pragma unroll
+  for (int k = 0; k < ND; k++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) R[k][q] = 0.0;
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++) {
+    const int p = d.ipq[iv * d.nquad + iq];
+    const double us = d.us[p], vs = d.vs[p];
+    // fstarq (Limiterlag.f90:686-698): sigma.n A + mu A (u* - u_v)
+    double F[2][2];
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const int slot = f + 2 * iv;
+      const double m = d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq];
+      const double mu1 = d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq];
+      const double mu2 = d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq];
+      const double s1 = d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq];
+      const double s2 = d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq];
+      F[f][0] = s1 + m * us + 0.0 * vs - mu1;
+      F[f][1] = s2 + 0.0 * us + m * vs - mu2;
+    }
+    const int fa = (iv + 3) & 3, fb = iv;
+    const double bqv[ND] = {1.0, (xv(iv) - rc) / 1.0, (yv(iv) - sc) / 1.0};
+#pragma unroll
+    for (int k = 0; k < ND; k++) {
+      const double b3 = 2.0 * bqv[k] + bqv[k];
+      const double l1x = c16 * b3 * fn[fa][0] * fn[fa][2], l1y = c16 * b3 * fn[fa][1] * fn[fa][2];
+      const double l2x = c16 * b3 * fn[fb][0] * fn[fb][2], l2y = c16 * b3 * fn[fb][1] * fn[fb][2];
+      R[k][0] = R[k][0] + us * l1x + vs * l1y + us * l2x + vs * l2y;
+      R[k][1] = R[k][1] + F[0][0] * c13 * b3 + F[1][0] * c13 * b3;
+      R[k][2] = R[k][2] + F[0][1] * c13 * b3 + F[1][1] * c13 * b3;
+      R[k][3] = R[k][3] + us * F[0][0] * c13 * b3 + vs * F[0][1] * c13 * b3 + us * F[1][0] * c13 * b3 +
+                vs * F[1][1] * c13 * b3;
+    }
+  }
+  // volume integral (rhsdomndg_lag_mc_quadsym, 5x5 Gauss)
+  const double af4 = d.lim[1 * nc + e];
+  const double v11 = d.lim[3 * nc + e], v12 = d.lim[4 * nc + e], v21 = d.lim[5 * nc + e], v22 = d.lim[6 * nc + e];
+  const double rhomc = u[0][0], uctr = u[1][0], vctr = u[2][0], ectr = u[3][0];
+  const double rhoct = 1.0 / rhomc;
+  const double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  const double dudr = v11 * u[1][1] + v12 * u[2][1];
+  const double duds = v11 * u[1][2] + v12 * u[2][2];
+  const double dvdr = v21 * u[1][1] + v22 * u[2][1];
+  const double dvds = v21 * u[1][2] + v22 * u[2][2];
+  for (int ig = 0; ig < 25; ig++) {
+    const double r = cR.g25[ig][0], s = cR.g25[ig][1], wi = cR.w25[ig];
+    double dxdr, dxds, dydr, dyds;
+    jac4(x4, r, s, dxdr, dxds, dydr, dyds);
+    const double djaco = wi, rcoef = 1.0;
+    // gdshp = adj(J) grad_xi b, b = (1, r - rc, s - sc): the rows for b2, b3
+    const double g1[ND] = {dyds * 0.0 + (-dydr) * 0.0, dyds * 1.0 + (-dydr) * 0.0, dyds * 0.0 + (-dydr) * 1.0};
+    const double g2[ND] = {(-dxds) * 0.0 + dxdr * 0.0, (-dxds) * 1.0 + dxdr * 0.0, (-dxds) * 0.0 + dxdr * 1.0};
+    const double b1 = (r - rc) / 1.0, b2 = (s - sc) / 1.0;
+    double un[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const double bb[ND] = {1.0, b1, b2};
+      double a = 0.0;
+      for (int k = 0; k < d.mdegr; k++) a = a + u[q][k] * bb[k];
+      un[q] = a;
+    }
+    const double rhoad = 1.0 / un[0];
+    double pres = (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]));
+    const double uadv = uctr + dudr * b1 + duds * b2;
+    const double vadv = vctr + dvdr * b1 + dvds * b2;
+    pres = pctr + af4 * (pres - pctr);
+    const double s11 = -pres + 0.0, s12 = 0.0 + 0.0, s21 = 0.0 + 0.0, s22 = -pres + 0.0;
+#pragma unroll
+    for (int k = 0; k < ND; k++) {
+      const double f1 = g1[k] * uadv + g2[k] * vadv;
+      const double f2 = g1[k] * s11 + g2[k] * s12;
+      const double f3 = g1[k] * s21 + g2[k] * s22;
+      const double f4 = g1[k] * (s11 * uadv + s12 * vadv) + g2[k] * (s21 * uadv + s22 * vadv);
+      R[k][0] = R[k][0] - f1 * djaco * rcoef;
+      R[k][1] = R[k][1] - f2 * djaco * rcoef;
+      R[k][2] = R[k][2] - f3 * djaco * rcoef;
+      R[k][3] = R[k][3] - f4 * djaco * rcoef;
+    }
+  }
+  if (!fuse) {
+#pragma unroll
+    for (int k = 0; k < ND; k++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) d.rhs[(q * ND + k) * nc + e] = R[k][q];
+    return;
+  }
+  update_cell(d, e, alfa, R);
+}
+
+// ---------------------------------------------------------------------------
+// getdelt_lag (Getrhslag.f90:20600-20716, straight edges :20649-20654)
+// ---------------------------------------------------------------------------
+__global__ void k1_dt_partial(Dev1 d) {
+  __shared__ double sm_cfl[256], sm_vol[256];
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  double dtcfl = 1e10, dtvol = 1e10;
+  if (iq < d.nquad && !stopped(d)) {
+    const double eps = 1.0e-6, g = d.gamlg;
+    double x4[4][2];
+    load4(d, d.xn, d.yn, iq, x4);
+    double dlen = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int b = (k + 1) & 3;
+      const double dl = sqrt((x4[k][0] - x4[b][0]) * (x4[k][0] - x4[b][0]) + (x4[k][1] - x4[b][1]) * (x4[k][1] - x4[b][1]));
+      if (k == 0 || dl < dlen) dlen = dl;
+    }
+    const double rhomc = U(d, d.Us, 0, 0, iq);
+    const double uctr = U(d, d.Us, 0, 1, iq), vctr = U(d, d.Us, 0, 2, iq), ectr = U(d, d.Us, 0, 3, iq);
+    const double rhoct = 1.0 / rhomc;
+    const double pctr = fmax(eps, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+    dtcfl = dlen / sdctr;
+    dtvol = d.vol[iq] / fabs(d.rhs[0 * (size_t)d.ncell + iq]);
+  }
+  sm_cfl[threadIdx.x] = dtcfl;
+  sm_vol[threadIdx.x] = dtvol;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sm_cfl[threadIdx.x] = fmin(sm_cfl[threadIdx.x], sm_cfl[threadIdx.x + s]);
+      sm_vol[threadIdx.x] = fmin(sm_vol[threadIdx.x], sm_vol[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    d.dtpart[2 * blockIdx.x] = sm_cfl[0];
+    d.dtpart[2 * blockIdx.x + 1] = sm_vol[0];
+  }
+}
+
+__global__ void k1_dt_final(Dev1 d, int nblk, int ndt) {
+  __shared__ double sm_cfl[256], sm_vol[256];
+  if (stopped(d)) return;
+  double a = 1e10, b = 1e10;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+    a = fmin(a, d.dtpart[2 * i]);
+    b = fmin(b, d.dtpart[2 * i + 1]);
+  }
+  sm_cfl[threadIdx.x] = a;
+  sm_vol[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sm_cfl[threadIdx.x] = fmin(sm_cfl[threadIdx.x], sm_cfl[threadIdx.x + s]);
+      sm_vol[threadIdx.x] = fmin(sm_vol[threadIdx.x], sm_vol[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    Scalars *S = d.sc_dev;
+    double dt = S->dtfix;
+    if (ndt == 1) {
+      const double dtcfl = fmin(1e10, sm_cfl[0]), dtvol = fmin(1e10, sm_vol[0]);
+      if (S->itime == 1) dt = fmin(d.cfl * dtcfl, 0.1 * dtvol);
+      else dt = fmin(fmin(d.cfl * dtcfl, 0.1 * dtvol), 1.01 * dt);
+      if ((S->tacru + dt) > d.tend) dt = d.tend - S->tacru;
+    }
+    S->dtfix = dt;
+    S->tacru = S->tacru + dt;
+  }
+}
+
+// node motion (Getrhslag.f90:1948-1957); no centre node on straight quads
+__global__ void k1_nodes(Dev1 d, double alfa) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= d.npoin || stopped(d)) return;
+  const double dt = d.sc_dev->dtfix, oma = 1.0 - alfa;
+  d.xs[p] = alfa * d.xn[p] + oma * (d.xs[p] + dt * d.us[p]);
+  d.ys[p] = alfa * d.yn[p] + oma * (d.ys[p] + dt * d.vs[p]);
+}
+
+// driver copy-back (dgflo2d.f90:407-423)
+__global__ void k1_copyback(Dev1 d) {
+  if (stopped(d)) return;
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < NU1 * d.ncell; t += stride) d.Un[t] = d.Us[t];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < d.npoin; t += stride) {
+    d.xn[t] = d.xs[t];
+    d.yn[t] = d.ys[t];
+  }
+}
+
+__global__ void k1_step_begin(Dev1 d, int itime) {
+  Scalars *S = d.sc_dev;
+  if (S->done) return;
+  S->itime = (itime < 0) ? S->itime + 1 : itime;
+}
+
+__global__ void k1_step_end(Dev1 d) {
+  Scalars *S = d.sc_dev;
+  if (S->done) return;
+  if (fabs(S->tacru - d.tend) / d.tend <= 1e-11) S->done = 1;
+}
+
+// caller layout unkno(3, 4, ncell) <-> device slabs
+__global__ void k1_unkno_in(Dev1 d, const double *aos) {
+  const int n = NU1 * d.ncell;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int e = t / NU1, qk = t % NU1;
+    d.Un[qk * (size_t)d.ncell + e] = aos[t];
+    d.Us[qk * (size_t)d.ncell + e] = aos[t];
+  }
+}
+__global__ void k1_unkno_out(Dev1 d, const double *src, double *aos) {
+  const int n = NU1 * d.ncell;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int e = t / NU1, qk = t % NU1;
+    aos[t] = src[qk * (size_t)d.ncell + e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct Family { double ms = 0.0; long long n = 0; };
+
+struct Solver {
+  Dev1 d{};
+  lag2d_config cfg{};
+  cudaStream_t st = nullptr;
+  std::vector<void *> allocs;
+  double *stage_u = nullptr, *stage_x = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0, launches = 0;
+  bool timing = false;
+  std::map<std::string, Family> fam;
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+};
+
+static int nb(int n, int t) { return std::max(1, (n + t - 1) / t); }
+
+template <typename T>
+static bool dalloc(Solver *s, T **p, size_t n) {
+  void *q = nullptr;
+  if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return false;
+  cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), s->st);
+  s->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return true;
+}
+
+template <typename F>
+static void launch(Solver *s, const char *family, F &&f, int n = 1) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (s->timing) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s->st);
+  }
+  f();
+  s->launches += n;
+  if (s->timing) {
+    cudaEventRecord(b, s->st);
+    s->pending.push_back({family, {a, b}});
+  }
+}
+
+static void flush_timing(Solver *s) {
+  for (auto &p : s->pending) {
+    cudaEventSynchronize(p.second.second);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+    Family &f = s->fam[p.first];
+    f.ms += ms;
+    f.n += 1;
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  s->pending.clear();
+}
+
+#define CK1(call)                                                          \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) {                                               \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+      return LAG2D_ECUDA;                                                  \
+    }                                                                      \
+  } while (0)
+
+static const double kRK[2][3] = {{0.0, 0.5, 0.0}, {0.0, 0.75, 0.3333333333333333}};
+
+static void geom(Solver *s, const double *X, const double *Y) {
+  const Dev1 &d = s->d;
+  launch(s, "geom", [&] { k1_geom<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, X, Y); });
+}
+
+// the stage sequence of getrhsdg_lag_mcnew's linear branch
+static void enqueue_rhs(Solver *s, int fuse, double alfa) {
+  const Dev1 &d = s->d;
+  launch(s, "bounds", [&] { k1_bounds<<<nb(d.npoin, 256), 256, 0, s->st>>>(d); });
+  launch(s, "cell", [&] { k1_cell<<<nb(d.nquad, 128), 128, 0, s->st>>>(d); });
+  launch(s, "node", [&] { k1_node<<<nb(d.npoin, 256), 256, 0, s->st>>>(d); });
+  launch(s, "rhs", [&] { k1_rhs<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, fuse, alfa); });
+}
+
+// getsolvdg_lag (Getrhslag.f90:1553-2035) and the driver copy-back
+static void enqueue_step(Solver *s, int itime) {
+  const Dev1 &d = s->d;
+  const int ns = s->cfg.nstag;
+  launch(s, "copy", [&] { k1_step_begin<<<1, 1, 0, s->st>>>(d, itime); });
+  geom(s, d.xn, d.yn);
+  for (int istag = 1; istag <= ns; istag++) {
+    const double alfa = kRK[ns - 2][istag - 1];
+    if (istag == 1) {
+      enqueue_rhs(s, 0, 0.0);
+      const int nblk = nb(d.nquad, 256);
+      launch(s, "dt", [&] {
+        k1_dt_partial<<<nblk, 256, 0, s->st>>>(d);
+        k1_dt_final<<<1, 256, 0, s->st>>>(d, nblk, s->cfg.ndt);
+      }, 2);
+      launch(s, "update", [&] { k1_update<<<nb(d.ncell, 128), 128, 0, s->st>>>(d, alfa); });
+    } else {
+      enqueue_rhs(s, 1, alfa);
+    }
+    launch(s, "nodes", [&] { k1_nodes<<<nb(d.npoin, 256), 256, 0, s->st>>>(d, alfa); });
+    geom(s, d.xs, d.ys);
+  }
+  launch(s, "copy", [&] {
+    k1_copyback<<<nb(std::max(NU1 * d.ncell, d.npoin), 256), 256, 0, s->st>>>(d);
+    k1_step_end<<<1, 1, 0, s->st>>>(d);
+  }, 2);
+}
+
+static int read_status(Solver *s, std::string &err) {
+  Scalars sc;
+  CK1(cudaMemcpyAsync(&sc, s->d.sc_dev, sizeof(Scalars), cudaMemcpyDeviceToHost, s->st));
+  CK1(cudaStreamSynchronize(s->st));
+  CK1(cudaGetLastError());
+  if (sc.status & ST_NONPHYS) { err = "non-positive cell volume"; return LAG2D_ENONPHYS; }
+  return LAG2D_OK;
+}
+
+static int put_scalars(Solver *s, int itime, double dtfix, double tacru, std::string &err) {
+  Scalars sc{};
+  sc.dtfix = dtfix; sc.tacru = tacru; sc.itime = itime;
+  CK1(cudaMemcpyAsync(s->d.sc_dev, &sc, sizeof(Scalars), cudaMemcpyHostToDevice, s->st));
+  CK1(cudaStreamSynchronize(s->st));
+  return LAG2D_OK;
+}
+
+int create(const lag2d_mesh *m, const lag2d_config *c, cudaStream_t st, Solver **out, std::string &err) {
+  *out = nullptr;
+  const int nq = m->nquad, np = m->npoin;
+  for (size_t i = 0; i < 4 * (size_t)nq; i++)
+    if (m->ipqua[i] < 1 || m->ipqua[i] > np) { err = "ipqua node id out of range"; return LAG2D_EINVAL; }
+  for (int i = 0; i < m->nbfac; i++) {
+    const int *b = m->bface + 5 * (size_t)i;
+    if (b[0] < 1 || b[0] > np || b[1] < 1 || b[1] > np) { err = "bface node id out of range"; return LAG2D_EINVAL; }
+  }
+  const int nsu = m->esuv2[np];
+  for (int i = 0; i < nsu; i++)
+    if (m->esuv1[i] < 1 || m->esuv1[i] > nq) { err = "esuv1 cell id out of range"; return LAG2D_EINVAL; }
+  Solver *s = new Solver();
+  s->cfg = *c;
+  s->st = st;
+  Dev1 &d = s->d;
+  d.nquad = nq; d.npoin = np; d.ncell = nq; d.mdegr = c->mdegr; d.ncase = c->ncase;
+  d.nsedov = c->nsedov;
+  for (int i = 0; i < 4; i++) d.sedov_cell[i] = c->sedov_cell[i];
+  d.gamlg = c->gamlg; d.cfl = c->cfl; d.cimpd = c->cimpd; d.tend = c->tend; d.sedov_energy = c->sedov_energy;
+  // connectivity
+  std::vector<int> ipq(4 * (size_t)nq), eptr(np + 1), esv(nsu), cptr(np + 1, 0), cor(4 * (size_t)nq);
+  for (int iq = 0; iq < nq; iq++)
+    for (int k = 0; k < 4; k++) ipq[k * (size_t)nq + iq] = m->ipqua[4 * (size_t)iq + k] - 1;
+  for (int p = 0; p <= np; p++) eptr[p] = m->esuv2[p];
+  for (int i = 0; i < nsu; i++) esv[i] = m->esuv1[i] - 1;
+  // corners at each node in the order getriem_quad_matrixsym scatters them
+  for (int iq = 0; iq < nq; iq++)
+    for (int k = 0; k < 4; k++) cptr[ipq[k * (size_t)nq + iq] + 1]++;
+  for (int p = 0; p < np; p++) cptr[p + 1] += cptr[p];
+  {
+    std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+    for (int iq = 0; iq < nq; iq++)
+      for (int k = 0; k < 4; k++) cor[fill[ipq[k * (size_t)nq + iq]]++] = iq * 4 + k;
+  }
+  // wall conditions of the nodal solve (Limiterlag.f90:462-476, 617-642) and
+  // the limiter's wall classes (Limiterlag.f90:8197-8234)
+  std::vector<unsigned char> bc(np, 0), wall(np, 0);
+  for (int i = 0; i < m->nbfac; i++) {
+    const int *b = m->bface + 5 * (size_t)i;
+    for (int k = 0; k < 2; k++) {
+      const int p = b[k] - 1;
+      if (b[2] == 22 && b[3] == 221) bc[p] |= BC_V0;
+      else if (b[2] == 22 && b[3] == 222) bc[p] |= BC_U0;
+      else if (b[2] == 25) bc[p] |= BC_UV0 | BC_KEEP;
+      if (c->ncase == 2) bc[p] |= BC_KEEP;
+    }
+  }
+  for (int i = 0; i < m->nbfac; i++) {
+    const int *b = m->bface + 5 * (size_t)i;
+    if (b[2] == 22 && b[3] == 221)
+      for (int k = 0; k < 2; k++) wall[b[k] - 1] = 3;
+  }
+  for (int i = 0; i < m->nbfac; i++) {
+    const int *b = m->bface + 5 * (size_t)i;
+    if (b[2] == 22 && b[3] == 222)
+      for (int k = 0; k < 2; k++) wall[b[k] - 1] = (wall[b[k] - 1] == 3) ? 10 : 2;
+  }
+  int *ipq_d, *eptr_d, *esv_d, *cptr_d, *cor_d;
+  unsigned char *bc_d, *wall_d;
+  double *x0, *y0;
+  bool ok = dalloc(s, &ipq_d, ipq.size()) && dalloc(s, &eptr_d, eptr.size()) && dalloc(s, &esv_d, esv.size()) &&
+            dalloc(s, &cptr_d, cptr.size()) && dalloc(s, &cor_d, cor.size()) && dalloc(s, &bc_d, bc.size()) &&
+            dalloc(s, &wall_d, wall.size()) && dalloc(s, &x0, np) && dalloc(s, &y0, np);
+  const size_t ncl = nq;
+  ok = ok && dalloc(s, &d.rc, ncl) && dalloc(s, &d.sc, ncl) && dalloc(s, &d.vol, ncl) && dalloc(s, &d.vcx, ncl) &&
+       dalloc(s, &d.vcy, ncl) && dalloc(s, &d.mass, ncl) && dalloc(s, &d.amatr, 4 * ncl) &&
+       dalloc(s, &d.Un, NU1 * ncl) && dalloc(s, &d.Us, NU1 * ncl) && dalloc(s, &d.xn, np) && dalloc(s, &d.yn, np) &&
+       dalloc(s, &d.xs, np) && dalloc(s, &d.ys, np) && dalloc(s, &d.us, np) && dalloc(s, &d.vs, np) &&
+       dalloc(s, &d.bmax, 5 * (size_t)np) && dalloc(s, &d.bmin, 5 * (size_t)np) && dalloc(s, &d.lim, 7 * ncl) &&
+       dalloc(s, &d.cf, 40 * ncl) && dalloc(s, &d.rhs, NU1 * ncl) &&
+       dalloc(s, &d.dtpart, 2 * (size_t)nb(nq, 256)) && dalloc(s, &d.sc_dev, 1) &&
+       dalloc(s, &s->stage_u, NU1 * ncl) && dalloc(s, &s->stage_x, 2 * (size_t)np);
+  if (!ok) {
+    destroy(s);
+    err = "cudaMalloc failed";
+    return LAG2D_ECUDA;
+  }
+  d.ipq = ipq_d; d.esuv_ptr = eptr_d; d.esuv = esv_d; d.ncor_ptr = cptr_d; d.ncor = cor_d; d.bc = bc_d;
+  d.wall = wall_d; d.x0 = x0; d.y0 = y0;
+  std::vector<double> xx(np), yy(np);
+  for (int p = 0; p < np; p++) { xx[p] = m->coold[2 * (size_t)p]; yy[p] = m->coold[2 * (size_t)p + 1]; }
+#define UP1(dst, src, n) cudaMemcpyAsync((void *)(dst), (src), (n) * sizeof(*(src)), cudaMemcpyHostToDevice, st)
+  UP1(ipq_d, ipq.data(), ipq.size()); UP1(eptr_d, eptr.data(), eptr.size()); UP1(esv_d, esv.data(), esv.size());
+  UP1(cptr_d, cptr.data(), cptr.size()); UP1(cor_d, cor.data(), cor.size()); UP1(bc_d, bc.data(), bc.size());
+  UP1(wall_d, wall.data(), wall.size()); UP1(x0, xx.data(), np); UP1(y0, yy.data(), np);
+  UP1(d.xn, xx.data(), np); UP1(d.yn, yy.data(), np); UP1(d.xs, xx.data(), np); UP1(d.ys, yy.data(), np);
+#undef UP1
+  Rules rl;
+  fill_rule(5, false, rl.g25, rl.w25);
+  fill_rule(6, false, rl.g36, rl.w36);
+  cudaMemcpyToSymbolAsync(cR, &rl, sizeof(Rules), 0, cudaMemcpyHostToDevice, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    destroy(s);
+    err = "device set-up failed";
+    return LAG2D_ECUDA;
+  }
+  *out = s;
+  return LAG2D_OK;
+}
+
+static int download_geoel(Solver *s, double *geoel, std::string &err) {
+  const Dev1 &d = s->d;
+  const int ncell = d.ncell;
+  std::vector<double> f(ncell);
+  double *src[6] = {d.rc, d.sc, d.vol, d.mass, d.vcx, d.vcy};
+  for (int k = 0; k < 6; k++) {
+    CK1(cudaMemcpyAsync(f.data(), src[k], ncell * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK1(cudaStreamSynchronize(s->st));
+    for (int e = 0; e < ncell; e++) geoel[24 * (size_t)e + k] = f[e];
+  }
+  return LAG2D_OK;
+}
+
+static int download_unkno(Solver *s, const double *src, double *unkno, std::string &err) {
+  const Dev1 &d = s->d;
+  launch(s, "copy", [&] { k1_unkno_out<<<nb(NU1 * d.ncell, 256), 256, 0, s->st>>>(d, src, s->stage_u); });
+  CK1(cudaMemcpyAsync(unkno, s->stage_u, NU1 * (size_t)d.ncell * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  CK1(cudaStreamSynchronize(s->st));
+  return LAG2D_OK;
+}
+
+static int download_xy(Solver *s, const double *X, const double *Y, double *xy, std::string &err) {
+  const int np = s->d.npoin;
+  launch_xy_out(np, s->st, s->stage_x, X, Y);
+  s->launches += 1;
+  CK1(cudaMemcpyAsync(xy, s->stage_x, 2 * (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  CK1(cudaStreamSynchronize(s->st));
+  return LAG2D_OK;
+}
+
+int init_fields(Solver *s, double *geoel, double *amatr, double *unkno, std::string &err) {
+  const Dev1 &d = s->d;
+  const int np = d.npoin, ncell = d.ncell;
+  launch(s, "init", [&] {
+    k1_init_geo<<<nb(d.nquad, 128), 128, 0, s->st>>>(d);
+    k1_init_fields<<<nb(d.nquad, 128), 128, 0, s->st>>>(d);
+  }, 2);
+  CK1(cudaMemcpyAsync(d.Us, d.Un, NU1 * (size_t)ncell * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+  CK1(cudaMemcpyAsync(d.xn, d.x0, np * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+  CK1(cudaMemcpyAsync(d.yn, d.y0, np * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+  CK1(cudaMemcpyAsync(d.xs, d.x0, np * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+  CK1(cudaMemcpyAsync(d.ys, d.y0, np * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+  CK1(cudaMemsetAsync(d.us, 0, np * sizeof(double), s->st));
+  CK1(cudaMemsetAsync(d.vs, 0, np * sizeof(double), s->st));
+  Scalars s0{};
+  CK1(cudaMemcpyAsync(d.sc_dev, &s0, sizeof(Scalars), cudaMemcpyHostToDevice, s->st));
+  geom(s, d.xn, d.yn);
+  int r = read_status(s, err);
+  if (r) return r;
+  if (geoel) {
+    std::fill(geoel, geoel + 24 * (size_t)ncell, 0.0);
+    if ((r = download_geoel(s, geoel, err))) return r;
+  }
+  if (amatr) {
+    std::vector<double> f(4 * (size_t)ncell);
+    CK1(cudaMemcpyAsync(f.data(), d.amatr, f.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK1(cudaStreamSynchronize(s->st));
+    for (int e = 0; e < ncell; e++)
+      for (int k = 0; k < 4; k++) amatr[4 * (size_t)e + k] = f[k * (size_t)ncell + e];
+  }
+  if (unkno && (r = download_unkno(s, d.Un, unkno, err))) return r;
+  return LAG2D_OK;
+}
+
+int set_state(Solver *s, const double *unkno, const double *coord, const double *ustar, const double *geoel,
+              const double *amatr, std::string &err) {
+  const Dev1 &d = s->d;
+  const int ncell = d.ncell, np = d.npoin;
+  CK1(cudaMemcpyAsync(s->stage_u, unkno, NU1 * (size_t)ncell * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  launch(s, "copy", [&] { k1_unkno_in<<<nb(NU1 * ncell, 256), 256, 0, s->st>>>(d, s->stage_u); });
+  CK1(cudaMemcpyAsync(s->stage_x, coord, 2 * (size_t)np * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  launch_xy_in(np, s->st, s->stage_x, d.xn, d.yn, d.xs, d.ys);
+  CK1(cudaStreamSynchronize(s->st));
+  CK1(cudaMemcpyAsync(s->stage_x, ustar, 2 * (size_t)np * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  launch_xy_in(np, s->st, s->stage_x, d.us, d.vs, nullptr, nullptr);
+  s->launches += 2;
+  if (geoel) {
+    std::vector<double> g(ncell);
+    double *dst[4] = {d.rc, d.sc, d.vol, d.mass};
+    for (int k = 0; k < 4; k++) {
+      for (int e = 0; e < ncell; e++) g[e] = geoel[24 * (size_t)e + k];
+      CK1(cudaMemcpyAsync(dst[k], g.data(), ncell * sizeof(double), cudaMemcpyHostToDevice, s->st));
+      CK1(cudaStreamSynchronize(s->st));
+    }
+  }
+  if (amatr) {
+    std::vector<double> g(4 * (size_t)ncell);
+    for (int e = 0; e < ncell; e++)
+      for (int k = 0; k < 4; k++) g[k * (size_t)ncell + e] = amatr[4 * (size_t)e + k];
+    CK1(cudaMemcpyAsync(d.amatr, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK1(cudaStreamSynchronize(s->st));
+  }
+  Scalars s0{};
+  CK1(cudaMemcpyAsync(d.sc_dev, &s0, sizeof(Scalars), cudaMemcpyHostToDevice, s->st));
+  geom(s, d.xs, d.ys);
+  return read_status(s, err);
+}
+
+int step(Solver *s, int itime, double *dtfix, double *tacru, std::string &err) {
+  int r = put_scalars(s, itime, *dtfix, *tacru, err);
+  if (r) return r;
+  enqueue_step(s, itime);
+  Scalars sc;
+  CK1(cudaMemcpyAsync(&sc, s->d.sc_dev, sizeof(Scalars), cudaMemcpyDeviceToHost, s->st));
+  CK1(cudaStreamSynchronize(s->st));
+  if (s->timing) flush_timing(s);
+  *dtfix = sc.dtfix;
+  *tacru = sc.tacru;
+  return read_status(s, err);
+}
+
+int run(Solver *s, int itime0, int nsteps, double *dtfix, double *tacru, int *done, std::string &err) {
+  int r = put_scalars(s, itime0 - 1, *dtfix, *tacru, err);
+  if (r) return r;
+  int steps = 0;
+  if (s->timing) {
+    for (int i = 0; i < nsteps; i++) { enqueue_step(s, itime0 + i); steps++; }
+    flush_timing(s);
+  } else {
+    if (!s->graph) {
+      cudaGraph_t g;
+      CK1(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+      const long long before = s->launches;
+      enqueue_step(s, -1);
+      CK1(cudaStreamEndCapture(s->st, &g));
+      CK1(cudaGraphInstantiate(&s->graph, g, 0));
+      cudaGraphDestroy(g);
+      s->graph_launches = s->launches - before;
+      s->launches = before;
+    }
+    for (int i = 0; i < nsteps; i++) {
+      CK1(cudaGraphLaunch(s->graph, s->st));
+      s->launches += s->graph_launches;
+      steps++;
+    }
+  }
+  Scalars sc;
+  CK1(cudaMemcpyAsync(&sc, s->d.sc_dev, sizeof(Scalars), cudaMemcpyDeviceToHost, s->st));
+  CK1(cudaStreamSynchronize(s->st));
+  *dtfix = sc.dtfix;
+  *tacru = sc.tacru;
+  if (done) *done = sc.done ? std::min(steps, std::max(0, sc.itime - itime0 + 1)) : steps;
+  return read_status(s, err);
+}
+
+int get_state(Solver *s, double *unkno, double *coord, double *ustar, double *geoel, std::string &err) {
+  int r;
+  if (unkno && (r = download_unkno(s, s->d.Un, unkno, err))) return r;
+  if (coord && (r = download_xy(s, s->d.xn, s->d.yn, coord, err))) return r;
+  if (ustar && (r = download_xy(s, s->d.us, s->d.vs, ustar, err))) return r;
+  if (geoel) {
+    std::fill(geoel, geoel + 24 * (size_t)s->d.ncell, 0.0);
+    if ((r = download_geoel(s, geoel, err))) return r;
+  }
+  return LAG2D_OK;
+}
+
+// the inner seam getrhsdg_lag_mcnew on the current state: limits the state,
+// updates ustar, returns rhsel(3, 4, ncell)
+int rhs(Solver *s, double *rhsel, std::string &err) {
+  const Dev1 &d = s->d;
+  int r = put_scalars(s, 1, 0.0, 0.0, err);
+  if (r) return r;
+  enqueue_rhs(s, 0, 0.0);
+  // the slope application of :7283-7298 alone: the update with alfa = 0 and dt = 0
+  launch(s, "update", [&] { k1_update<<<nb(d.ncell, 128), 128, 0, s->st>>>(d, 0.0); });
+  if ((r = read_status(s, err))) return r;
+  if (s->timing) flush_timing(s);
+  CK1(cudaMemcpyAsync(d.Un, d.Us, NU1 * (size_t)d.ncell * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+  if (rhsel) return download_unkno(s, d.rhs, rhsel, err);
+  return LAG2D_OK;
+}
+
+int cellvol(Solver *s, double *geoel, std::string &err) {
+  geom(s, s->d.xs, s->d.ys);
+  int r = read_status(s, err);
+  if (r) return r;
+  if (geoel) {
+    std::fill(geoel, geoel + 24 * (size_t)s->d.ncell, 0.0);
+    return download_geoel(s, geoel, err);
+  }
+  return LAG2D_OK;
+}
+
+long long launches(const Solver *s) { return s->launches; }
+
+void set_timing(Solver *s, bool on) {
+  s->timing = on;
+  s->fam.clear();
+}
+
+double kernel_ms(const Solver *s, const char *family, long long *n) {
+  auto it = s->fam.find(family);
+  if (it == s->fam.end() || it->second.n == 0) return -1.0;
+  if (n) *n = it->second.n;
+  return it->second.ms / it->second.n;
+}
+
+void destroy(Solver *s) {
+  if (!s) return;
+  if (s->st) cudaStreamSynchronize(s->st);
+  for (auto &p : s->pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  for (void *p : s->allocs) cudaFree(p);
+  delete s;
+}
+
+}  // namespace p1
+}  // namespace lag2d

@@ -41,10 +41,11 @@ class Mesh:
     esuv1: np.ndarray = None     # (npoin1,) int32
     esuv2: np.ndarray = None     # (npoin+1,) int32
     esqua: np.ndarray = None     # (nquad, 4) int32    == esqua(4, nquad)
+    nvqua: int = 9               # nodes per quad: 9 (curved, ncurv=1) or 4 (straight, ncurv=0)
 
     def __post_init__(self):
         self.coord = np.ascontiguousarray(self.coord, dtype=np.float64)
-        self.ipqua = np.ascontiguousarray(self.ipqua, dtype=np.int32).reshape(-1, 9)
+        self.ipqua = np.ascontiguousarray(self.ipqua, dtype=np.int32).reshape(-1, self.nvqua)
         self.iptri = np.ascontiguousarray(self.iptri, dtype=np.int32).reshape(-1, 6)
         self.bface = np.ascontiguousarray(self.bface, dtype=np.int32).reshape(-1, 5)
         if self.esuv1 is None or self.esuv2 is None:
@@ -210,8 +211,9 @@ def build_esuv(iptri: np.ndarray, ipqua: np.ndarray, npoin: int):
     point's list is in increasing cell order because cells are visited in order.
     """
     ntria = iptri.shape[0]
-    cells = np.concatenate([np.repeat(np.arange(1, ntria + 1, dtype=np.int64), 6),
-                            np.repeat(np.arange(ntria + 1, ntria + ipqua.shape[0] + 1, dtype=np.int64), 9)])
+    cells = np.concatenate([np.repeat(np.arange(1, ntria + 1, dtype=np.int64), iptri.shape[1]),
+                            np.repeat(np.arange(ntria + 1, ntria + ipqua.shape[0] + 1, dtype=np.int64),
+                                      ipqua.shape[1])])
     pts = np.concatenate([iptri.reshape(-1).astype(np.int64), ipqua.reshape(-1).astype(np.int64)])
     order = np.lexsort((cells, pts))
     counts = np.bincount(pts - 1, minlength=npoin)
@@ -413,3 +415,42 @@ def polar_mesh(nr: int, nt: int, radius: float = 1.0, wall_code: int = 22) -> Me
     bf.append((node(2, 2 * nt), node(0, 0), wall_code, 222, node(1, 2 * nt)))
     return Mesh(coord=coord, ipqua=ipqua, iptri=np.array(tris, dtype=np.int32).reshape(-1, 6),
                 bface=np.array(bf, dtype=np.int32))
+
+
+def linear_quad_mesh(nx: int, ny: int, x0: float = 0.0, x1: float = 1.0, y0: float = 0.0,
+                     y1: float = 1.0, jitter: float = 0.0, seed: int = 1234,
+                     wall_code: int = 22) -> Mesh:
+    """Structured ``nx`` x ``ny`` mesh of straight 4-node quads (``ncurv = 0``,
+    ``ipqua(4, nquad)``) on ``[x0,x1] x [y0,y1]``, counter-clockwise corners,
+    cells row by row.  ``jitter`` moves interior vertices by U(-jitter*h,
+    jitter*h) (seeded).  Boundary faces as in :func:`quad_mesh` (slip walls,
+    221 on the y-walls, 222 on the x-walls; the mid-node column is 0).
+    """
+    hx, hy = (x1 - x0) / nx, (y1 - y0) / ny
+    ii, jj = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1))
+    X = x0 + ii * hx
+    Y = y0 + jj * hy
+    X[:, nx] = x1
+    Y[ny, :] = y1
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        vi, vj = np.meshgrid(np.arange(1, nx), np.arange(1, ny))
+        X[vj, vi] += rng.uniform(-jitter * hx, jitter * hx, size=vi.shape)
+        Y[vj, vi] += rng.uniform(-jitter * hy, jitter * hy, size=vi.shape)
+    nid = (jj * (nx + 1) + ii + 1).astype(np.int64)
+    ci, cj = np.meshgrid(np.arange(nx), np.arange(ny))
+    ci, cj = ci.reshape(-1), cj.reshape(-1)
+    ipqua = np.stack([nid[cj, ci], nid[cj, ci + 1], nid[cj + 1, ci + 1], nid[cj + 1, ci]],
+                     axis=1).astype(np.int32)
+    coord = np.stack([X.reshape(-1), Y.reshape(-1)], axis=1)
+    bf = []
+    for i in range(nx):
+        bf.append((nid[0, i], nid[0, i + 1], wall_code, 221, 0))
+    for j in range(ny):
+        bf.append((nid[j, nx], nid[j + 1, nx], wall_code, 222, 0))
+    for i in range(nx - 1, -1, -1):
+        bf.append((nid[ny, i + 1], nid[ny, i], wall_code, 221, 0))
+    for j in range(ny - 1, -1, -1):
+        bf.append((nid[j + 1, 0], nid[j, 0], wall_code, 222, 0))
+    return Mesh(coord=coord, ipqua=ipqua, iptri=np.zeros((0, 3), np.int32),
+                bface=np.array(bf, dtype=np.int32), nvqua=4)

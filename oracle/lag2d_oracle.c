@@ -159,6 +159,24 @@ static void map9(const double (*xp)[2], const double *shp, double *x, double *y)
 }
 
 static void load_quad(const o_mesh *m, const double *X, int ie, double (*xp)[2]) {
+  if (m->nvqua == 4) {
+    /* ncurv = 0: the straight quad's 9-node image, built from its vertices
+     * as every geometry routine does (e.g. Limiterlag.f90:2040-2048,
+     * GetInitial.f90:1513-1521) */
+    for (int k = 0; k < 4; k++) {
+      int ip = m->ipqua[4 * ie + k] - 1;
+      xp[k][0] = X_(X, 0, ip);
+      xp[k][1] = X_(X, 1, ip);
+    }
+    for (int d = 0; d < 2; d++) {
+      xp[4][d] = 0.5 * (xp[0][d] + xp[1][d]);
+      xp[5][d] = 0.5 * (xp[1][d] + xp[2][d]);
+      xp[6][d] = 0.5 * (xp[2][d] + xp[3][d]);
+      xp[7][d] = 0.5 * (xp[3][d] + xp[0][d]);
+      xp[8][d] = 0.5 * (xp[4][d] + xp[6][d]);
+    }
+    return;
+  }
   for (int k = 0; k < 9; k++) {
     int ip = m->ipqua[9 * ie + k] - 1;
     xp[k][0] = X_(X, 0, ip);
@@ -2335,6 +2353,10 @@ double o_delt(const o_mesh *m, const o_cfg *c, const double *unkno,
     static const int e[4][3] = {{0, 4, 1}, {1, 5, 2}, {2, 6, 3}, {3, 7, 0}};
     for (int k = 0; k < 4; k++) {
       const double *a = xp[e[k][0]], *b = xp[e[k][1]], *cc = xp[e[k][2]];
+      if (m->nvqua == 4) {  /* ncurv = 0: straight edges (Getrhslag.f90:20649-20654) */
+        dl[k] = sqrt((a[0] - cc[0]) * (a[0] - cc[0]) + (a[1] - cc[1]) * (a[1] - cc[1]));
+        continue;
+      }
       dl[k] = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1])) +
               sqrt((b[0] - cc[0]) * (b[0] - cc[0]) + (b[1] - cc[1]) * (b[1] - cc[1]));
     }
@@ -2371,7 +2393,8 @@ void o_step(const o_mesh *m, const o_cfg *c, const double *unkno, double *unold,
   o_cellvol(m, c, geoel, coord);
   for (int istag = 1; istag <= c->nstag; istag++) {
     double alfa = rklag[c->nstag - 2][istag - 1];
-    o_rhs(m, c, ustar, unold, rhsel, geoel, cooro, coold, amatr, itime, NULL);
+    if (c->npoly == 1) o1_rhs(m, c, ustar, unold, rhsel, geoel, cooro, NULL, NULL);
+    else o_rhs(m, c, ustar, unold, rhsel, geoel, cooro, coold, amatr, itime, NULL);
     if (c->ndt == 1) {
       if (istag == 1) {
         for (int ie = 0; ie < ncell; ie++) dvdt[ie] = U_(rhsel, c, 0, 0, ie);
@@ -2407,7 +2430,7 @@ void o_step(const o_mesh *m, const o_cfg *c, const double *unkno, double *unold,
     for (int ip = 0; ip < m->npoin; ip++)
       for (int d = 0; d < 2; d++)
         X_(cooro, d, ip) = alfa * X_(coord, d, ip) + (1.0 - alfa) * (X_(cooro, d, ip) + *dtfix * X_(ustar, d, ip));
-    for (int ie = 0; ie < m->nquad; ie++) {
+    for (int ie = 0; ie < m->nquad && m->nvqua != 4; ie++) {  /* ncurv = 1 only (:1963-1971) */
       const int *ipq = m->ipqua + 9 * ie;
       for (int d = 0; d < 2; d++) {
         double x[8];
@@ -2453,4 +2476,541 @@ void o_weno(const o_mesh *m, const o_cfg *c, double *unkno, double *geoel,
   for (int ie = 0; ie < ncell; ie++) G_(geoel, 9, ie) = flags[ie] ? 100.0 : 0.0;
   weno(m, c, unkno, geoel, coord, coold);
   for (int ie = 0; ie < ncell; ie++) G_(geoel, 9, ie) = 0.0;
+}
+
+/* ====================================================================== */
+/* Linear P1 path: ncurv=0, nriem=1, nfint=1, nlimi=6, nrz=0 on 4-node    */
+/* quads (the Sod configuration).  getrhsdg_lag_mcnew's branch at         */
+/* Getrhslagmc.f90:6810-6980 and the slope application at :7283-7298.    */
+/* Calls that do not change the result are left out: getbc_lagmaire2      */
+/* (Getrhslag.f90:11269) only forms the unused boundary force `fpres`;    */
+/* getAS_llnl (Limiterlag.f90:15476) ends with `sgmas = 0`; the           */
+/* divergence limiter of barthlimit_sympre_quadlb (Limiterlag.f90:        */
+/* 8127-8692, the `afdu` loops) only writes geoel(10), which this branch  */
+/* never reads, and so does not need the divergence bound unmax(nq+2) of  */
+/* barthlimit_lag_vtxunknew either (computed there from `dr`, `ds` that   */
+/* are set only in its triangle loop).                                    */
+/* ====================================================================== */
+
+/* Literals the Fortran writes in single precision (`eps = 1.e-6`,
+ * `1.e-11`), widened to double as gfortran does. */
+#define EPS_S ((double)1.0e-6f)
+#define TINY_S ((double)1.0e-11f)
+
+/* barthfct, Getrhslagmc.f90:9171-9222 */
+static double barthfct(double umax, double umin, double uctr, double dunk) {
+  const double coef = 0.7;
+  double fiy;
+  if (dunk > 1.0e-8) {
+    fiy = coef * (umax - uctr) / dunk;
+    return fmin((fiy * fiy + 2.0 * fiy) / (fiy * fiy + fiy + 2.0), 1.0);
+  } else if (dunk < -1.0e-8) {
+    fiy = coef * (umin - uctr) / dunk;
+    return fmin((fiy * fiy + 2.0 * fiy) / (fiy * fiy + fiy + 2.0), 1.0);
+  }
+  return 1.0;
+}
+
+static const double XVQ[4] = {-1.0, 1.0, 1.0, -1.0}, YVQ[4] = {-1.0, -1.0, 1.0, 1.0};
+
+/* vertex values of the P1 DOFs: bq = (1, (xv-rc)/dr, (yv-sc)/ds), dr = ds = 1 */
+static void p1_vertex(const o_cfg *c, const double *unkno, int ielem, double rc, double sc,
+                      double unknvq[4][5]) {
+  for (int iv = 0; iv < 4; iv++) {
+    double bq[3] = {1.0, (XVQ[iv] - rc) / 1.0, (YVQ[iv] - sc) / 1.0};
+    for (int q = 0; q < 4; q++) {
+      double a = 0.0;
+      for (int k = 0; k < c->mdegr; k++) a = a + U_(unkno, c, k, q, ielem) * bq[k];
+      unknvq[iv][q] = a;
+    }
+  }
+}
+
+/* bilinear Jacobian at (r, s) (the 4-node shape derivatives of
+ * barthlimit_sympre_quadlb, Limiterlag.f90:8262-8282) */
+static void jac4(const double (*xpq)[2], double r, double s, double *dxdr, double *dxds,
+                 double *dydr, double *dyds) {
+  const double rp = 1.0 + r, rm = 1.0 - r, sp = 1.0 + s, sm = 1.0 - s;
+  const double dsprq[4] = {-0.25 * sm, 0.25 * sm, 0.25 * sp, -0.25 * sp};
+  const double dspsq[4] = {-0.25 * rm, -0.25 * rp, 0.25 * rp, 0.25 * rm};
+  double a = 0, b = 0, cc = 0, d = 0;
+  for (int k = 0; k < 4; k++) {
+    a = a + dsprq[k] * xpq[k][0];
+    b = b + dspsq[k] * xpq[k][0];
+    cc = cc + dsprq[k] * xpq[k][1];
+    d = d + dspsq[k] * xpq[k][1];
+  }
+  *dxdr = a; *dxds = b; *dydr = cc; *dyds = d;
+}
+
+void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
+            double *rhsel, const double *geoel, const double *coord,
+            double *aflim_out, double *afvec_out) {
+  const int nquad = m->nquad, npoin = m->npoin;
+  const double g = c->gamlg, epsd = 1.0e-6;
+  const double slpdu = (g + 1.0) / 2.0;
+  double *gelq = (double *)calloc((size_t)12 * nquad, sizeof(double));   /* (3,4,nquad) */
+  double *unmax = (double *)malloc(sizeof(double) * 5 * (size_t)npoin);
+  double *unmin = (double *)malloc(sizeof(double) * 5 * (size_t)npoin);
+  double *aflim = (double *)calloc((size_t)5 * nquad, sizeof(double));  /* (nq+1, ncell) */
+  double *afvec = (double *)calloc((size_t)4 * nquad, sizeof(double));  /* (2,2,ncell) col-major */
+  double *mapmt = (double *)calloc((size_t)4 * nquad, sizeof(double));
+  int *bnd = (int *)calloc((size_t)npoin, sizeof(int));
+  int *indbd = (int *)calloc((size_t)npoin, sizeof(int));
+  int *indnd = (int *)calloc((size_t)npoin, sizeof(int));
+  double *munacn = (double *)calloc((size_t)4 * npoin, sizeof(double));
+  double *munacu = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *snsigm = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *mcl = (double *)malloc(sizeof(double) * 4 * 8 * (size_t)nquad);  /* munaclq(2,2,2,4) */
+  double *mul = (double *)malloc(sizeof(double) * 2 * 8 * (size_t)nquad);  /* munaulq(2,2,4) */
+  double *snl = (double *)malloc(sizeof(double) * 2 * 8 * (size_t)nquad);  /* snsigmlq(2,2,4) */
+  double *fst = (double *)malloc(sizeof(double) * 2 * 8 * (size_t)nquad);  /* fstarq(2,2,4) */
+  double *vlave = (double *)malloc(sizeof(double) * 2 * (size_t)npoin);
+#define QN(ie, k) (m->ipqua[4 * (ie) + (k)] - 1)
+#define GL(f, ie) (gelq + 3 * ((f) + 4 * (ie)))
+#define AF(k, ie) aflim[(k) + 5 * (ie)]
+#define AV(i, j, ie) afvec[(i) + 2 * (j) + 4 * (ie)]
+#define MP(i, j, ie) mapmt[(i) + 2 * (j) + 4 * (ie)]
+
+  /* I.1.1 getfnds_lag_mc_hybrid, Getrhslagmc.f90:2117-2265 (quad faces) */
+  for (int ie = 0; ie < nquad; ie++) {
+    for (int f = 0; f < 4; f++) {
+      int a = QN(ie, f), b = QN(ie, (f + 1) % 4);
+      double anx = X_(coord, 1, b) - X_(coord, 1, a);
+      double any = -(X_(coord, 0, b) - X_(coord, 0, a));
+      GL(f, ie)[0] = anx / sqrt(anx * anx + any * any);
+      GL(f, ie)[1] = any / sqrt(anx * anx + any * any);
+      GL(f, ie)[2] = sqrt(anx * anx + any * any);
+    }
+  }
+
+  /* I.1.2a barthlimit_lag_vtxunknew, Getrhslagmctria.f90:2373-2643:
+   * node bounds of (tau, u, v, p, e) over the cells sharing the node */
+  for (int ip = 0; ip < npoin; ip++)
+    for (int q = 0; q < 5; q++) { unmax[q + 5 * ip] = -1.0e10; unmin[q + 5 * ip] = 1.0e10; }
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rhom = U_(unkno, c, 0, 0, ielem);
+    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+    double rhoct = 1.0 / rhom;
+    double pctr = fmax(EPS_S, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    double unctr[5] = {U_(unkno, c, 0, 0, ielem), uctr, vctr, pctr, ectr};
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      for (int q = 0; q < 5; q++) {
+        if (unctr[q] > unmax[q + 5 * ip]) unmax[q + 5 * ip] = unctr[q];
+        if (unctr[q] < unmin[q + 5 * ip]) unmin[q + 5 * ip] = unctr[q];
+      }
+    }
+  }
+
+  /* I.1.2b barthlimit_lagsym_quad, Limiterlag.f90:4-404 */
+  for (int ifa = 0; ifa < m->nbfac; ifa++)
+    for (int k = 0; k < 2; k++) bnd[m->bface[5 * ifa + k] - 1] = 1;
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double unknvq[4][5];
+    p1_vertex(c, unkno, ielem, rc, sc, unknvq);
+    for (int iv = 0; iv < 4; iv++) {
+      double rhov = 1.0 / unknvq[iv][0];
+      double uv = unknvq[iv][1], vv = unknvq[iv][2], ev = unknvq[iv][3];
+      double pvtx = fmax(EPS_S, (g - 1.0) * rhov * (ev - 0.5 * (uv * uv + vv * vv)));
+      unknvq[iv][0] = 1.0 / rhov;
+      unknvq[iv][3] = pvtx;
+    }
+    double rhom = U_(unkno, c, 0, 0, ielem);
+    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+    double rhoct = 1.0 / rhom;
+    double pctr = fmax(EPS_S, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    double unctr[4] = {1.0 / rhoct, uctr, vctr, pctr};
+    double alfa[4][4];
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      double dunk[4];
+      for (int q = 0; q < 4; q++) {
+        dunk[q] = unknvq[iv][q] - unctr[q];
+        alfa[iv][q] = barthfct(unmax[q + 5 * ip], unmin[q + 5 * ip], unctr[q], dunk[q]);
+      }
+      if (bnd[ip] && c->ncase == 1) {
+        if (X_(coord, 0, ip) < 1.0e-6 || fabs(X_(coord, 0, ip) - 1.0) < 1.0e-6)
+          alfa[iv][1] = fmin(fmax((-unctr[1]) / (dunk[1]), 0.0), 1.0);
+        if (X_(coord, 1, ip) < 1.0e-6 || fabs(X_(coord, 1, ip) - 1.0) < 1.0e-6)
+          alfa[iv][2] = fmin(fmax((-unctr[2]) / (dunk[2]), 0.0), 1.0);
+      }
+    }
+    for (int q = 0; q < 4; q++) {
+      double a = alfa[0][q];
+      for (int iv = 1; iv < 4; iv++) if (alfa[iv][q] < a) a = alfa[iv][q];
+      AF(q, ie) = a;
+    }
+  }
+
+  /* barthlimit_sympre_quadlb, Limiterlag.f90:8127-8692: the velocity
+   * limited in the principal frame of the strain rate, as a 2x2 tensor */
+  if (c->ncase != 1) {
+    for (int ifa = 0; ifa < m->nbfac; ifa++)
+      if (m->bface[5 * ifa + 2] == 22 && m->bface[5 * ifa + 3] == 221)
+        for (int k = 0; k < 2; k++) indbd[m->bface[5 * ifa + k] - 1] = 3;
+    for (int ifa = 0; ifa < m->nbfac; ifa++)
+      if (m->bface[5 * ifa + 2] == 22 && m->bface[5 * ifa + 3] == 222)
+        for (int k = 0; k < 2; k++) {
+          int ip = m->bface[5 * ifa + k] - 1;
+          indbd[ip] = (indbd[ip] == 3) ? 10 : 2;
+        }
+  } else {
+    for (int ifa = 0; ifa < m->nbfac; ifa++)
+      for (int k = 0; k < 2; k++) indbd[m->bface[5 * ifa + k] - 1] = 1;
+  }
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double xpq[4][2];
+    for (int k = 0; k < 4; k++) { xpq[k][0] = X_(coord, 0, QN(ie, k)); xpq[k][1] = X_(coord, 1, QN(ie, k)); }
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double dudr = U_(unkno, c, 1, 1, ielem) / 1.0, duds = U_(unkno, c, 2, 1, ielem) / 1.0;
+    double dvdr = U_(unkno, c, 1, 2, ielem) / 1.0, dvds = U_(unkno, c, 2, 2, ielem) / 1.0;
+    double dxdr, dxds, dydr, dyds;
+    jac4((const double(*)[2])xpq, rc, sc, &dxdr, &dxds, &dydr, &dyds);
+    double jacom = dxdr * dyds - dydr * dxds;
+    double drdx = dyds / jacom, drdy = -dxds / jacom, dsdx = -dydr / jacom, dsdy = dxdr / jacom;
+    double dudx = dudr * drdx + duds * dsdx, dudy = dudr * drdy + duds * dsdy;
+    double dvdx = dvdr * drdx + dvds * dsdx, dvdy = dvdr * drdy + dvds * dsdy;
+    /* the velocity-aligned frame set first (:8290-8301) is always overwritten below */
+    double matra = dudx, matrb = 0.5 * (dudy + dvdx), matrc = matrb, matrd = dvdy;
+    double mapt = matra + matrd, mapd = matra * matrd - matrb * matrc;
+    double lamda1 = 0.5 * mapt + sqrt(0.25 * (mapt * mapt) - mapd);
+    double lamda2 = 0.5 * mapt - sqrt(0.25 * (mapt * mapt) - mapd);
+    if (fabs(matrc) > 1.0e-8) {
+      double lmat1 = sqrt((lamda1 - matrd) * (lamda1 - matrd) + matrc * matrc);
+      double lmat2 = sqrt((lamda2 - matrd) * (lamda2 - matrd) + matrc * matrc);
+      int r1 = (matrc > 0.0) ? 0 : 1, r2 = 1 - r1;
+      MP(r1, 0, ie) = (lamda1 - matrd) / lmat1;
+      MP(r1, 1, ie) = matrc / lmat1;
+      MP(r2, 0, ie) = (lamda2 - matrd) / lmat2;
+      MP(r2, 1, ie) = matrc / lmat2;
+    } else {
+      MP(0, 0, ie) = 0.0; MP(0, 1, ie) = 0.0; MP(1, 0, ie) = 0.0; MP(1, 1, ie) = 0.0;
+    }
+  }
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    const double m11 = MP(0, 0, ie), m12 = MP(0, 1, ie), m21 = MP(1, 0, ie), m22 = MP(1, 1, ie);
+    double unknvq[4][5];
+    p1_vertex(c, unkno, ielem, rc, sc, unknvq);
+    for (int iv = 0; iv < 4; iv++) {
+      double uv = unknvq[iv][1], vv = unknvq[iv][2];
+      unknvq[iv][1] = uv * m11 + vv * m12;
+      unknvq[iv][2] = uv * m21 + vv * m22;
+    }
+    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem);
+    double unctr[3] = {0.0, uctr * m11 + vctr * m12, uctr * m21 + vctr * m22};
+    double alfa[4][3];
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      double mx[3] = {0, unctr[1], unctr[2]}, mn[3] = {0, unctr[1], unctr[2]};
+      for (int is = m->esuv2[ip]; is < m->esuv2[ip + 1]; is++) {
+        int je = m->esuv1[is] - 1;
+        double uj = U_(unkno, c, 0, 1, je), vj = U_(unkno, c, 0, 2, je);
+        /* the cell's own average, then the images across the walls */
+        double img[4][2];
+        int nimg = 0;
+        img[nimg][0] = uj; img[nimg][1] = vj; nimg++;
+        if (c->ncase != 1) {
+          if (indbd[ip] == 3) { img[nimg][0] = uj; img[nimg][1] = -vj; nimg++; }
+          else if (indbd[ip] == 2) { img[nimg][0] = -uj; img[nimg][1] = vj; nimg++; }
+          else if (indbd[ip] == 10) {
+            img[nimg][0] = uj; img[nimg][1] = -vj; nimg++;
+            img[nimg][0] = -uj; img[nimg][1] = vj; nimg++;
+            img[nimg][0] = -uj; img[nimg][1] = -vj; nimg++;
+          }
+        }
+        for (int k = 0; k < nimg; k++) {
+          double ul = img[k][0] * m11 + img[k][1] * m12;
+          double vl = img[k][0] * m21 + img[k][1] * m22;
+          mx[1] = fmax(mx[1], ul); mx[2] = fmax(mx[2], vl);
+          mn[1] = fmin(mn[1], ul); mn[2] = fmin(mn[2], vl);
+        }
+      }
+      for (int q = 1; q < 3; q++) {
+        double dunk = unknvq[iv][q] - unctr[q];
+        alfa[iv][q] = barthfct(mx[q], mn[q], unctr[q], dunk);
+      }
+      if (indbd[ip] == 1 && c->ncase == 1) {
+        if (X_(coord, 0, ip) < 1.0e-6 || fabs(X_(coord, 0, ip) - 1.0) < 1.0e-6) { alfa[iv][1] = 1.0; alfa[iv][2] = 1.0; }
+        if (X_(coord, 1, ip) < 1.0e-6 || fabs(X_(coord, 1, ip) - 1.0) < 1.0e-6) { alfa[iv][1] = 1.0; alfa[iv][2] = 1.0; }
+      }
+    }
+    double fl[3];
+    for (int q = 1; q < 3; q++) {
+      double a = alfa[0][q];
+      for (int iv = 1; iv < 4; iv++) if (alfa[iv][q] < a) a = alfa[iv][q];
+      fl[q] = a;
+    }
+    /* afvec = R^T diag(fixi, fiet) R, R = mapmt (:8679-8691) */
+    double fixi = fl[1], fiet = fl[2];
+    double fi11 = (m11 * m11) * fixi + (m21 * m21) * fiet;
+    double fi12 = m11 * m12 * fixi + m21 * m22 * fiet;
+    double fi22 = (m12 * m12) * fixi + (m22 * m22) * fiet;
+    AV(0, 0, ie) = fi11; AV(0, 1, ie) = fi12; AV(1, 0, ie) = fi12; AV(1, 1, ie) = fi22;
+  }
+  /* energy limiter on the reconstructed vertex energy (Limiterlag.f90:290-380) */
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double rhom = U_(unkno, c, 0, 0, ielem);
+    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+    double rhoct = 1.0 / rhom;
+    double pctr = fmax(EPS_S, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    double unknvq[4][5];
+    p1_vertex(c, unkno, ielem, rc, sc, unknvq);
+    double alfa5[4];
+    for (int iv = 0; iv < 4; iv++) {
+      double rhov = 1.0 / unknvq[iv][0];
+      double uv = unknvq[iv][1], vv = unknvq[iv][2], ev = unknvq[iv][3];
+      double pvtx = fmax(EPS_S, (g - 1.0) * rhov * (ev - 0.5 * (uv * uv + vv * vv)));
+      double t = rhom + AF(0, ie) * (1.0 / rhov - rhom);
+      double pv = pctr + AF(3, ie) * (pvtx - pctr);
+      double e5 = pv / (g - 1.0) * t + 0.5 * (uv * uv + vv * vv);
+      int ip = QN(ie, iv);
+      double dunk = e5 - ectr;
+      alfa5[iv] = barthfct(unmax[4 + 5 * ip], unmin[4 + 5 * ip], ectr, dunk);
+    }
+    double a = alfa5[0];
+    for (int iv = 1; iv < 4; iv++) if (alfa5[iv] < a) a = alfa5[iv];
+    AF(4, ie) = a;
+  }
+
+  /* I.1.3 getndvelo_lag_mc_matrixsym, Limiterlag.f90:408-704 */
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    if (c->ncase == 2) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
+    if (m->bface[5 * ifa + 2] == 25) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
+  }
+  memcpy(vlave, ustar, sizeof(double) * 2 * (size_t)npoin);
+  /* getriem_quad_matrixsym, Limiterlag.f90:708-1033, scattering in cell order */
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double bq[4][3];
+    for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
+    /* corner iv touches faces iv-1 and iv; the area weight (2 r_a + r_b)/3 * 0.5 * |f| with r = 1 */
+    double vn[4][2][3];
+    for (int iv = 0; iv < 4; iv++) {
+      int fa = (iv + 3) % 4, fb = iv;
+      for (int k = 0; k < 3; k++) { vn[iv][0][k] = GL(fa, ie)[k]; vn[iv][1][k] = GL(fb, ie)[k]; }
+      vn[iv][0][2] = (2.0 * 1.0 + 1.0) / 3.0 * 0.5 * vn[iv][0][2];
+      vn[iv][1][2] = (2.0 * 1.0 + 1.0) / 3.0 * 0.5 * vn[iv][1][2];
+    }
+    double rhomc = U_(unkno, c, 0, 0, ielem);
+    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+    double rhoct = 1.0 / rhomc;
+    double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    double unknvq[4][5], sig[4], aujmp[4][3];
+    p1_vertex(c, unkno, ielem, rc, sc, unknvq);
+    const double a11 = AV(0, 0, ie), a12 = AV(0, 1, ie), a21 = AV(1, 0, ie), a22 = AV(1, 1, ie);
+    for (int iv = 0; iv < 4; iv++) {
+      double rhovt = 1.0 / unknvq[iv][0];
+      double uv = unknvq[iv][1], vv = unknvq[iv][2], ev = unknvq[iv][3];
+      double pvtx = fmax(epsd, (g - 1.0) * rhovt * (ev - 0.5 * (uv * uv + vv * vv)));
+      double rhomv = rhomc + AF(0, ie) * (unknvq[iv][0] - rhomc);
+      rhovt = 1.0 / rhomv;
+      (void)rhovt;
+      double dudr = a11 * U_(unkno, c, 1, 1, ielem) + a12 * U_(unkno, c, 1, 2, ielem);
+      double duds = a11 * U_(unkno, c, 2, 1, ielem) + a12 * U_(unkno, c, 2, 2, ielem);
+      double dvdr = a21 * U_(unkno, c, 1, 1, ielem) + a22 * U_(unkno, c, 1, 2, ielem);
+      double dvds = a21 * U_(unkno, c, 2, 1, ielem) + a22 * U_(unkno, c, 2, 2, ielem);
+      uv = U_(unkno, c, 0, 1, ielem) + dudr * bq[iv][1] + duds * bq[iv][2];
+      vv = U_(unkno, c, 0, 2, ielem) + dvdr * bq[iv][1] + dvds * bq[iv][2];
+      pvtx = pctr + AF(3, ie) * (pvtx - pctr);
+      unknvq[iv][1] = uv;
+      unknvq[iv][2] = vv;
+      sig[iv] = -pvtx + 0.0;
+      int ip = QN(ie, iv);
+      double acnx = X_(vlave, 0, ip) - uv, acny = X_(vlave, 1, ip) - vv;
+      double nrm = sqrt(acnx * acnx + acny * acny);
+      if (nrm < TINY_S) { aujmp[iv][0] = TINY_S; aujmp[iv][1] = TINY_S; }
+      else { aujmp[iv][0] = acnx / nrm; aujmp[iv][1] = acny / nrm; }
+      aujmp[iv][2] = nrm;
+    }
+    double sdctr = sqrt(fmax(epsd, g * pctr / rhoct));
+    for (int iv = 0; iv < 4; iv++) aujmp[iv][2] = aujmp[iv][2] / sdctr;
+    double murie[4][2];
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      double dux = X_(vlave, 0, ip) - unknvq[iv][1], duy = X_(vlave, 1, ip) - unknvq[iv][2];
+      for (int f = 0; f < 2; f++) {
+        double deltu = fabs(dux * vn[iv][f][0] + duy * vn[iv][f][1]);
+        murie[iv][f] = rhoct * sdctr + c->cimpd * rhoct * slpdu * deltu;
+      }
+    }
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      for (int f = 0; f < 2; f++) {
+        /* getriecoef_matrixnew, Limiterlag.f90:1037-1076 */
+        double area = vn[iv][f][2], n1 = vn[iv][f][0], n2 = vn[iv][f][1];
+        double vnau = (aujmp[iv][2] < 1.0e12) ? 1.0 : n1 * aujmp[iv][0] + n2 * aujmp[iv][1];
+        double mc11 = murie[iv][f] * area * fabs(vnau), mc21 = 0.0, mc12 = 0.0, mc22 = murie[iv][f] * area * fabs(vnau);
+        double mu1 = mc11 * unknvq[iv][1] + mc21 * unknvq[iv][2];
+        double mu2 = mc21 * unknvq[iv][1] + mc22 * unknvq[iv][2];
+        double s1 = sig[iv] * area * n1 + (0.0 + 0.0) * area * n2;
+        double s2 = (0.0 + 0.0) * area * n1 + sig[iv] * area * n2;
+        munacn[0 + 4 * ip] = munacn[0 + 4 * ip] + mc11;
+        munacn[1 + 4 * ip] = munacn[1 + 4 * ip] + mc21;
+        munacn[2 + 4 * ip] = munacn[2 + 4 * ip] + mc12;
+        munacn[3 + 4 * ip] = munacn[3 + 4 * ip] + mc22;
+        munacu[0 + 2 * ip] = munacu[0 + 2 * ip] + mu1;
+        munacu[1 + 2 * ip] = munacu[1 + 2 * ip] + mu2;
+        snsigm[0 + 2 * ip] = snsigm[0 + 2 * ip] + s1;
+        snsigm[1 + 2 * ip] = snsigm[1 + 2 * ip] + s2;
+        const size_t o = (size_t)f + 2 * (iv + 4 * (size_t)ie);
+        mcl[4 * o + 0] = mc11; mcl[4 * o + 1] = mc21; mcl[4 * o + 2] = mc12; mcl[4 * o + 3] = mc22;
+        mul[2 * o + 0] = mu1; mul[2 * o + 1] = mu2;
+        snl[2 * o + 0] = s1; snl[2 * o + 1] = s2;
+      }
+    }
+  }
+  for (int ip = 0; ip < npoin; ip++) {
+    if (indnd[ip]) continue;
+    const double *mn = munacn + 4 * ip;  /* (1,1), (2,1), (1,2), (2,2) */
+    double detma = mn[0] * mn[3] - mn[1] * mn[2];
+    double i11 = mn[3] / detma, i12 = -mn[2] / detma, i21 = -mn[1] / detma, i22 = mn[0] / detma;
+    double r1 = munacu[2 * ip] - snsigm[2 * ip], r2 = munacu[2 * ip + 1] - snsigm[2 * ip + 1];
+    X_(ustar, 0, ip) = i11 * r1 + i12 * r2;
+    X_(ustar, 1, ip) = i21 * r1 + i22 * r2;
+  }
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    const int *bf = m->bface + 5 * ifa;
+    for (int k = 0; k < 2; k++) {
+      int ip = bf[k] - 1;
+      if (bf[2] == 22) {
+        if (bf[3] == 221) X_(ustar, 1, ip) = 0.0;
+        else if (bf[3] == 222) X_(ustar, 0, ip) = 0.0;
+      } else if (bf[2] == 25) {
+        X_(ustar, 0, ip) = 0.0;
+        X_(ustar, 1, ip) = 0.0;
+      }
+    }
+  }
+  for (int ie = 0; ie < nquad; ie++)
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      for (int f = 0; f < 2; f++) {
+        const size_t o = (size_t)f + 2 * (iv + 4 * (size_t)ie);
+        fst[2 * o + 0] = snl[2 * o + 0] + mcl[4 * o + 0] * X_(ustar, 0, ip) + mcl[4 * o + 1] * X_(ustar, 1, ip) - mul[2 * o + 0];
+        fst[2 * o + 1] = snl[2 * o + 1] + mcl[4 * o + 2] * X_(ustar, 0, ip) + mcl[4 * o + 3] * X_(ustar, 1, ip) - mul[2 * o + 1];
+      }
+    }
+
+  /* I.1.4 rhsifacedg_lag_mc_hybridquad2, Getrhslagmc.f90:14468-14618 */
+  const double c16 = 0.1666666666666666, c13 = 0.3333333333333333;
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double bq[4][3];
+    for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
+    double ul[3] = {0, 0, 0}, p1[3] = {0, 0, 0}, p2[3] = {0, 0, 0}, el[3] = {0, 0, 0};
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      int fa = (iv + 3) % 4, fb = iv;
+      double us = X_(ustar, 0, ip), vs = X_(ustar, 1, ip);
+      const size_t o0 = 2 * (iv + 4 * (size_t)ie), o1 = o0 + 1;
+      for (int k = 0; k < c->ndegr; k++) {
+        double b3 = 2.0 * bq[iv][k] + bq[iv][k];
+        double l1x = c16 * b3 * GL(fa, ie)[0] * GL(fa, ie)[2], l1y = c16 * b3 * GL(fa, ie)[1] * GL(fa, ie)[2];
+        double l2x = c16 * b3 * GL(fb, ie)[0] * GL(fb, ie)[2], l2y = c16 * b3 * GL(fb, ie)[1] * GL(fb, ie)[2];
+        ul[k] = ul[k] + us * l1x + vs * l1y + us * l2x + vs * l2y;
+        p1[k] = p1[k] + fst[2 * o0] * c13 * b3 + fst[2 * o1] * c13 * b3;
+        p2[k] = p2[k] + fst[2 * o0 + 1] * c13 * b3 + fst[2 * o1 + 1] * c13 * b3;
+        el[k] = el[k] + us * fst[2 * o0] * c13 * b3 + vs * fst[2 * o0 + 1] * c13 * b3 +
+                us * fst[2 * o1] * c13 * b3 + vs * fst[2 * o1 + 1] * c13 * b3;
+      }
+    }
+    for (int k = 0; k < c->ndegr; k++) {
+      U_(rhsel, c, k, 0, ielem) = ul[k];
+      U_(rhsel, c, k, 1, ielem) = p1[k];
+      U_(rhsel, c, k, 2, ielem) = p2[k];
+      U_(rhsel, c, k, 3, ielem) = el[k];
+    }
+  }
+
+  /* I.1.5 rhsdomndg_lag_mc_quadsym, Limiterlag.f90:1108-1490 (5x5 Gauss) */
+  double pos25[25][2], w25[25];
+  quad_rule(25, 0, pos25, w25);
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double xpq[4][2];
+    for (int k = 0; k < 4; k++) { xpq[k][0] = X_(coord, 0, QN(ie, k)); xpq[k][1] = X_(coord, 1, QN(ie, k)); }
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    const double dbdr[3] = {0.0, 1.0 / 1.0, 0.0}, dbds[3] = {0.0, 0.0, 1.0 / 1.0};
+    const double a11 = AV(0, 0, ie), a12 = AV(0, 1, ie), a21 = AV(1, 0, ie), a22 = AV(1, 1, ie);
+    for (int ig = 0; ig < 25; ig++) {
+      double r = pos25[ig][0], s = pos25[ig][1], wi = w25[ig];
+      double dxdr, dxds, dydr, dyds;
+      jac4((const double(*)[2])xpq, r, s, &dxdr, &dxds, &dydr, &dyds);
+      double djaco = wi;
+      double rcoef = 1.0;  /* 1 - alfrz + alfrz*ygaus with alfrz = 0 */
+      double gd[2][3];
+      for (int k = 0; k < 3; k++) {
+        gd[0][k] = dyds * dbdr[k] + (-dydr) * dbds[k];
+        gd[1][k] = (-dxds) * dbdr[k] + dxdr * dbds[k];
+      }
+      double b[3] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+      double un[4];
+      for (int q = 0; q < 4; q++) {
+        double a = 0.0;
+        for (int k = 0; k < c->mdegr; k++) a = a + U_(unkno, c, k, q, ielem) * b[k];
+        un[q] = a;
+      }
+      double rhoad = 1.0 / un[0];
+      double uadv = un[1], vadv = un[2], eadv = un[3];
+      double pres = (g - 1.0) * rhoad * (eadv - 0.5 * (uadv * uadv + vadv * vadv));
+      double rhomc = U_(unkno, c, 0, 0, ielem);
+      double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+      double rhoct = 1.0 / rhomc;
+      double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+      double dudr = a11 * U_(unkno, c, 1, 1, ielem) + a12 * U_(unkno, c, 1, 2, ielem);
+      double duds = a11 * U_(unkno, c, 2, 1, ielem) + a12 * U_(unkno, c, 2, 2, ielem);
+      double dvdr = a21 * U_(unkno, c, 1, 1, ielem) + a22 * U_(unkno, c, 1, 2, ielem);
+      double dvds = a21 * U_(unkno, c, 2, 1, ielem) + a22 * U_(unkno, c, 2, 2, ielem);
+      uadv = U_(unkno, c, 0, 1, ielem) + dudr * b[1] + duds * b[2];
+      vadv = U_(unkno, c, 0, 2, ielem) + dvdr * b[1] + dvds * b[2];
+      pres = pctr + AF(3, ie) * (pres - pctr);
+      double s11 = -pres + 0.0, s12 = 0.0 + 0.0, s21 = 0.0 + 0.0, s22 = -pres + 0.0;
+      for (int k = 0; k < c->ndegr; k++) {
+        double f1 = gd[0][k] * uadv + gd[1][k] * vadv;
+        double f2 = gd[0][k] * s11 + gd[1][k] * s12;
+        double f3 = gd[0][k] * s21 + gd[1][k] * s22;
+        double f4 = gd[0][k] * (s11 * uadv + s12 * vadv) + gd[1][k] * (s21 * uadv + s22 * vadv);
+        U_(rhsel, c, k, 0, ielem) = U_(rhsel, c, k, 0, ielem) - f1 * djaco * rcoef;
+        U_(rhsel, c, k, 1, ielem) = U_(rhsel, c, k, 1, ielem) - f2 * djaco * rcoef;
+        U_(rhsel, c, k, 2, ielem) = U_(rhsel, c, k, 2, ielem) - f3 * djaco * rcoef;
+        U_(rhsel, c, k, 3, ielem) = U_(rhsel, c, k, 3, ielem) - f4 * djaco * rcoef;
+      }
+    }
+  }
+
+  /* I.x.7 limited slopes into the stage state, Getrhslagmc.f90:7283-7298 */
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    for (int k = 1; k < 3; k++) U_(unkno, c, k, 0, ielem) = U_(unkno, c, k, 0, ielem) * AF(0, ie);
+    double u22 = U_(unkno, c, 1, 1, ielem), u32 = U_(unkno, c, 2, 1, ielem);
+    double u23 = U_(unkno, c, 1, 2, ielem), u33 = U_(unkno, c, 2, 2, ielem);
+    double dudr = AV(0, 0, ie) * u22 + AV(0, 1, ie) * u23;
+    double duds = AV(0, 0, ie) * u32 + AV(0, 1, ie) * u33;
+    double dvdr = AV(1, 0, ie) * u22 + AV(1, 1, ie) * u23;
+    double dvds = AV(1, 0, ie) * u32 + AV(1, 1, ie) * u33;
+    U_(unkno, c, 1, 1, ielem) = dudr; U_(unkno, c, 2, 1, ielem) = duds;
+    U_(unkno, c, 1, 2, ielem) = dvdr; U_(unkno, c, 2, 2, ielem) = dvds;
+    for (int k = 1; k < 3; k++) U_(unkno, c, k, 3, ielem) = U_(unkno, c, k, 3, ielem) * AF(4, ie);
+  }
+  if (aflim_out) memcpy(aflim_out, aflim, sizeof(double) * 5 * (size_t)nquad);
+  if (afvec_out) memcpy(afvec_out, afvec, sizeof(double) * 4 * (size_t)nquad);
+#undef QN
+#undef GL
+#undef AF
+#undef AV
+#undef MP
+  free(gelq); free(unmax); free(unmin); free(aflim); free(afvec); free(mapmt); free(bnd); free(indbd);
+  free(indnd); free(munacn); free(munacu); free(snsigm); free(mcl); free(mul); free(snl); free(fst);
+  free(vlave);
 }

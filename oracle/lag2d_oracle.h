@@ -22,6 +22,7 @@
  *   geoel(24, nsize)         -> G[k + 24*ie]
  *   amatr(nmatr, ncell)      -> A[k + nmatr*ie]
  *   ipqua(9, nquad)          -> 1-based node ids, node index fastest
+ *                               (ipqua(4, nquad) on the straight-quad P1 path)
  *   bface(5, nbfac)          -> (node1, node2, bc code, bc sub-code, mid node)
  *   esuv1 / esuv2            -> cells-surrounding-point CSR (1-based)
  *   esqua(4, nquad)          -> cell across quad face k (ghost = ncell+iface)
@@ -40,6 +41,7 @@ typedef struct {
   const int *esuv1;  /* (npoin1)    */
   const int *esuv2;  /* (npoin+1)   */
   const int *esqua;  /* (4, nquad)  */
+  int nvqua;         /* nodes per quad in ipqua: 9 (curved, ncurv=1) or 4 (straight, ncurv=0) */
 } o_mesh;
 
 typedef struct {
@@ -93,6 +95,19 @@ void o_step(const o_mesh *m, const o_cfg *c, const double *unkno, double *unold,
 int o_run(const o_mesh *m, const o_cfg *c, double *unkno, double *coord,
           const double *coold, double *geoel, const double *amatr,
           double *ustar, int itime0, int nsteps, double *dtfix, double *tacru);
+
+/* ---- Linear P1 path (ncurv=0, nfint=1, nlimi=6, nrz=0; 4-node quads, no
+ * triangles).  o_init, o_cellvol and o_run serve it too (o_mesh.nvqua = 4,
+ * o_cfg.npoly = 1); these are its inner seams. ---- */
+
+/* getrhsdg_lag_mcnew, ncurv=0 / nfint=1 branch (Getrhslagmc.f90:6810-6980,
+ * 7270-7300): Barth limiting, nodal solver, face and volume integrals, then
+ * the limited slopes applied to unkno in place.  ustar is overwritten with
+ * the new nodal velocity; aflim (5, ncell) and afvec (4, ncell), if not
+ * NULL, receive the limiter coefficients. */
+void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
+            double *rhsel, const double *geoel, const double *coord,
+            double *aflim, double *afvec);
 
 #ifdef __cplusplus
 }

@@ -23,7 +23,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 class _OMesh(ctypes.Structure):
     _fields_ = [("ntria", ctypes.c_int), ("nquad", ctypes.c_int), ("npoin", ctypes.c_int),
                 ("nbfac", ctypes.c_int), ("iptri", _ip), ("ipqua", _ip), ("bface", _ip),
-                ("esuv1", _ip), ("esuv2", _ip), ("esqua", _ip)]
+                ("esuv1", _ip), ("esuv2", _ip), ("esqua", _ip), ("nvqua", ctypes.c_int)]
 
 
 class _OCfg(ctypes.Structure):
@@ -69,7 +69,7 @@ class Oracle:
         k = self._keep
         self.om = _OMesh(mesh.ntria, mesh.nquad, mesh.npoin, mesh.nbfac,
                          _p(k[0], _ip), _p(k[1], _ip), _p(k[2], _ip), _p(k[3], _ip), _p(k[4], _ip),
-                         _p(k[5], _ip))
+                         _p(k[5], _ip), int(getattr(mesh, "nvqua", 9)))
         sc = (ctypes.c_int * 4)(*(list(cfg.sedov_cells) + [0, 0, 0, 0])[:4])
         self.oc = _OCfg(cfg.npoly, cfg.ndegr, cfg.mdegr, cfg.nq, cfg.nstag, cfg.ndt, cfg.ncase,
                         cfg.nlimi, 1, cfg.ngausd, cfg.ngausd_geo, len(cfg.sedov_cells), sc,
@@ -104,6 +104,17 @@ class Oracle:
         f = np.ascontiguousarray(flags, dtype=np.int32)
         lib().o_weno(ctypes.byref(self.om), ctypes.byref(self.oc), _p(unkno, _dp), _p(geoel, _dp),
                      _p(coord, _dp), _p(coold, _dp), _p(f, _ip))
+
+    def rhs_p1(self, ustar, unkno, geoel, coord):
+        """The linear P1 branch of getrhsdg_lag_mcnew; unkno is limited and
+        ustar updated in place.  Returns (rhsel, aflim (ncell, 5), afvec (ncell, 4))."""
+        m, c = self.mesh, self.cfg
+        rhsel = np.zeros((m.ncell, c.nq, c.ndegr))
+        aflim = np.zeros((m.ncell, 5))
+        afvec = np.zeros((m.ncell, 4))
+        lib().o1_rhs(ctypes.byref(self.om), ctypes.byref(self.oc), _p(ustar, _dp), _p(unkno, _dp),
+                     _p(rhsel, _dp), _p(geoel, _dp), _p(coord, _dp), _p(aflim, _dp), _p(afvec, _dp))
+        return rhsel, aflim, afvec
 
     @staticmethod
     def status() -> int:

@@ -5,7 +5,8 @@ golden outputs, so these fixtures pin the CPU oracle against regressions and
 give the GPU path fixed targets: small Taylor-Green and Sedov runs (8 x 8, a
 12 x 12 Sedov with troubled cells, a curved 6 x 6 quad mesh, a curved
 tri/quad mesh and the Noh implosion on a 4 x 4 quarter-disk mesh with
-triangles at the origin), 3 time steps each.
+triangles at the origin), 3 time steps each, and the radial Sod problem on a
+jittered 12 x 4 mesh of straight quads on the linear P1 path, 6 steps.
 
     python tests/golden/make_golden.py            # all fixtures
     python tests/golden/make_golden.py tgv6_hybrid # one fixture
@@ -20,7 +21,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from lag2d_b200 import quad_mesh, StepConfig  # noqa: E402
-from lag2d_b200.mesh import hybrid_mesh, polar_mesh  # noqa: E402
+from lag2d_b200.mesh import hybrid_mesh, linear_quad_mesh, polar_mesh  # noqa: E402
 from oracle.oracle import Oracle  # noqa: E402
 
 CASES = {
@@ -36,6 +37,9 @@ CASES = {
     # Noh on the curved quarter disk, fixed time step
     "noh4_polar": (lambda: polar_mesh(4, 4),
                    StepConfig(ncase=3, gamlg=5.0 / 3.0, nstag=3, ndt=0, dtfix=1.0e-4, tend=0.6), 3),
+    # radial Sod on jittered straight quads, linear P1 branch (ncurv=0, nfint=1)
+    "sod12_p1": (lambda: linear_quad_mesh(12, 4, 0.0, 1.0, 0.0, 0.4, jitter=0.15, seed=7),
+                 StepConfig(npoly=1, ndegr=3, mdegr=3, ncase=6, gamlg=1.4, nstag=2, cfl=0.3, tend=0.2), 6),
 }
 
 

@@ -52,9 +52,11 @@ def test_create_validates_arguments_without_device():
     cc.precision, cc.order_exact = 1, 1      # the reference-order kernels are FP64 only
     assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
     cc.precision, cc.order_exact = 0, 0
-    cc.npoly, cc.ndegr = 1, 3                # the linear P1 chain is not on this path
+    cc.npoly, cc.ndegr, cc.mdegr = 1, 3, 6   # the P1 path: mdegr must be <= 3
+    assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
+    cc.mdegr = 3                             # the P1 path has no Taylor-Green source
     assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 3
-    cc.npoly, cc.ndegr = c.npoly, c.ndegr
+    cc.npoly, cc.ndegr, cc.mdegr = c.npoly, c.ndegr, c.mdegr
     cc.nstag = 4
     assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 1
     del s

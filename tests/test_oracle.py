@@ -155,7 +155,7 @@ def test_tgv_symmetry():
     assert np.abs(tau - np.rot90(tau, -1)).max() < 1e-12
 
 
-@pytest.mark.parametrize("name", ["tgv8", "sedov12", "tgv6_curved", "tgv6_hybrid", "noh4_polar"])
+@pytest.mark.parametrize("name", ["tgv8", "sedov12", "tgv6_curved", "tgv6_hybrid", "noh4_polar", "sod12_p1"])
 def test_golden_fixtures(name):
     from tests.golden.make_golden import run_case
     ref = np.load(os.path.join(GOLDEN, f"{name}.npz"))
