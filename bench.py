@@ -45,6 +45,7 @@ def parse():
                     help="fixed time step (ndt = 0) instead of the CFL one, for the configurations whose "
                          "CFL steps break the scheme (Noh, hybrid Sedov)")
     ap.add_argument("--rho0", action="store_true", help="per-cell initial densities 1 + 0.01 N(0, 1)")
+    ap.add_argument("--no-p1", action="store_true", help="skip the linear P1 (Sod) block")
     ap.add_argument("--adjoint-steps", type=int, default=4)
     ap.add_argument("--adjoint-checkpoint", type=int, default=2)
     return ap.parse_args()
@@ -245,6 +246,41 @@ def adjoint_block(s, args, fwd_ms_per_step, state, grads=None):
                           if s._c.precision == 1 else "FP64")}
 
 
+def p1_block(args, timed, families):
+    """Throughput of the linear P1 path on the Sod workloads (DOF-updates/s
+    per RK stage, 12 DOFs per cell), its kernel split and stage roofline, and
+    the oracle timed on the reference's 200 x 10 case."""
+    from lag2d_b200.config import workload
+    from lag2d_b200.roofline import stage_bytes_p1
+    peak, peak_kind = peaks()
+    names = ("bounds", "cell", "node", "rhs", "dt", "update", "nodes", "geom", "copy")
+    out = {"path": "ncurv=0, nfint=1, nlimi=6 (linear P1, straight quads); parity: bit for bit with the "
+                   "oracle in the no-FMA build (tests/test_gpu_p1.py)"}
+    for name in ("sod200", "sod1024"):
+        m, c = workload(name)
+        s = new_solver(m, c, None)
+        ms, done, launches = timed(s)
+        dof_stage = m.ncell * c.ndegr * c.nq
+        ms_step = ms / max(done, 1)
+        fams = families(s, names)
+        sb = stage_bytes_p1(m.ncell, m.npoin)
+        gbs = sb / (ms_step / c.nstag / 1e3) / 1e9
+        out[name] = {"value": dof_stage * c.nstag * done / (ms / 1e3), "unit": UNIT, "ms_per_step": ms_step,
+                     "steps": done, "cells": m.ncell, "nodes": m.npoin, "rk_stages": c.nstag,
+                     "gpu_launches": launches,
+                     "kernels_ms_per_step": {f: v["ms_per_launch"] * v["launches"] / 2 for f, v in fams.items()},
+                     "stage_roofline": {"bytes_per_stage": sb, "achieved_gbs": gbs, "peak": peak,
+                                        "peak_kind": peak_kind, "frac": gbs / peak}}
+        s.close()
+    if not args.no_cpu_baseline:
+        nc, nstag, times = _cpu_worker(("sod200", 0, 60))
+        total = sum(times)
+        out["sod200"]["cpu_baseline"] = {
+            "value": nc * 12 * nstag * len(times) / total, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"sod200: the first {len(times)} steps, {total:.2f} s, oracle C restatement -O2 single thread"}
+    return out
+
+
 def run_ours(args):
     rank, local_rank, world = dist_env()
     import numpy as np
@@ -281,11 +317,11 @@ def run_ours(args):
         torch.cuda.synchronize()
         return max_over_ranks(e0.elapsed_time(e1)), n, solver.kernel_launches - l0
 
-    def families(solver):
+    def families(solver, names=("persson", "weno", "corner", "node", "rhs", "dt", "update", "nodes", "geom", "copy")):
         solver.timing(True)
         solver.run(2)
         out = {}
-        for f in ("persson", "weno", "corner", "node", "rhs", "dt", "update", "nodes", "geom", "copy"):
+        for f in names:
             k_ms, n = solver.kernel_ms(f)
             if k_ms is not None:
                 out[f] = {"ms_per_launch": k_ms, "launches": n}
@@ -377,6 +413,10 @@ def run_ours(args):
         adjoint["fp32_mixed"]["grad_rel_l2_vs_fp64_adjoint"] = rel
         adjoint["fp32_mixed"]["J_rel_vs_fp64"] = abs(g32["J"] - g64["J"]) / abs(g64["J"])
 
+    # ---- the linear P1 path (Sod on straight 4-node quads): the reference's
+    # 200 x 10 configuration and a 1024 x 512 one, FP64, graph-replayed steps
+    p1 = None if args.no_p1 else p1_block(args, timed, families)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -390,6 +430,8 @@ def run_ours(args):
                                    "frac": stage_gbs / peak, "roofline_dof_updates_per_s": dof_stage / (sb / (peak * 1e9))},
                 "kernels_ms_per_step": per_step, "fp32_mixed": mixed,
                 "adjoint_forward_ratio": adjoint.get("ratio"), "adjoint": adjoint}
+        if p1 is not None:
+            line["p1_sod"] = p1
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)

@@ -356,6 +356,7 @@ __global__ void k1_bounds(Dev1 d) {
 // ---------------------------------------------------------------------------
 // Limiter and corner coefficients of one quad
 // ---------------------------------------------------------------------------
+template <int MD>
 __device__ void cell_pass(const Dev1 &d, int iq) {
   const int e = iq;
   const double g = d.gamlg, epsd = 1.0e-6, slpdu = (g + 1.0) / 2.0;
@@ -380,7 +381,8 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       double a = 0.0;
-      for (int k = 0; k < d.mdegr; k++) a = a + u[q][k] * bq[iv][k];
+#pragma unroll
+      for (int k = 0; k < MD; k++) a = a + u[q][k] * bq[iv][k];
       uvq[iv][q] = a;
     }
   const double rhom = u[0][0], uctr = u[1][0], vctr = u[2][0], ectr = u[3][0];
@@ -436,33 +438,27 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
   double fl1 = 0.0, fl2 = 0.0;
   {
     const double uc = uctr * m11 + vctr * m12, vc = uctr * m21 + vctr * m22;
-#pragma unroll 1
+#pragma unroll
     for (int iv = 0; iv < 4; iv++) {
       const double ur = uvq[iv][1] * m11 + uvq[iv][2] * m12;
       const double vr = uvq[iv][1] * m21 + uvq[iv][2] * m22;
       double mx1 = uc, mx2 = vc, mn1 = uc, mn2 = vc;
       const int p = ip[iv];
       const int cls = (d.ncase != 1) ? d.wall[p] : 0;
+      auto take = [&](double a, double b) {
+        const double ul = a * m11 + b * m12;
+        const double vl = a * m21 + b * m22;
+        mx1 = fmax(mx1, ul); mx2 = fmax(mx2, vl);
+        mn1 = fmin(mn1, ul); mn2 = fmin(mn2, vl);
+      };
       for (int i = d.esuv_ptr[p]; i < d.esuv_ptr[p + 1]; i++) {
         const int je = d.esuv[i];
         const double uj = U(d, d.Us, 0, 1, je), vj = U(d, d.Us, 0, 2, je);
         // the cell's own average, then its images across the walls at the node
-        double iu[4], iv2[4];
-        int n = 0;
-        iu[n] = uj; iv2[n] = vj; n++;
-        if (cls == 3) { iu[n] = uj; iv2[n] = -vj; n++; }
-        else if (cls == 2) { iu[n] = -uj; iv2[n] = vj; n++; }
-        else if (cls == 10) {
-          iu[n] = uj; iv2[n] = -vj; n++;
-          iu[n] = -uj; iv2[n] = vj; n++;
-          iu[n] = -uj; iv2[n] = -vj; n++;
-        }
-        for (int k = 0; k < n; k++) {
-          const double ul = iu[k] * m11 + iv2[k] * m12;
-          const double vl = iu[k] * m21 + iv2[k] * m22;
-          mx1 = fmax(mx1, ul); mx2 = fmax(mx2, vl);
-          mn1 = fmin(mn1, ul); mn2 = fmin(mn2, vl);
-        }
+        take(uj, vj);
+        if (cls == 3 || cls == 10) take(uj, -vj);
+        if (cls == 2 || cls == 10) take(-uj, vj);
+        if (cls == 10) take(-uj, -vj);
       }
       const double a1 = barthfct(mx1, mn1, uc, ur - uc);
       const double a2 = barthfct(mx2, mn2, vc, vr - vc);
@@ -557,10 +553,11 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
     }
   }
 }
+template <int MD>
 __global__ void __launch_bounds__(128) k1_cell(Dev1 d) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
-  cell_pass(d, iq);
+  cell_pass<MD>(d, iq);
 }
 
 // ---------------------------------------------------------------------------
@@ -666,6 +663,7 @@ __global__ void k1_update(Dev1 d, double alfa) {
 // ---------------------------------------------------------------------------
 // Corner forces, face and volume integrals of one quad
 // ---------------------------------------------------------------------------
+template <int MD>
 __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
@@ -752,7 +750,8 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
     for (int q = 0; q < 4; q++) {
       const double bb[ND] = {1.0, b1, b2};
       double a = 0.0;
-      for (int k = 0; k < d.mdegr; k++) a = a + u[q][k] * bb[k];
+#pragma unroll
+      for (int k = 0; k < MD; k++) a = a + u[q][k] * bb[k];
       un[q] = a;
     }
     const double rhoad = 1.0 / un[0];
@@ -986,17 +985,30 @@ static void geom(Solver *s, const double *X, const double *Y) {
 static void enqueue_rhs(Solver *s, int fuse, double alfa) {
   const Dev1 &d = s->d;
   launch(s, "bounds", [&] { k1_bounds<<<nb(d.npoin, 256), 256, 0, s->st>>>(d); });
-  launch(s, "cell", [&] { k1_cell<<<nb(d.nquad, 128), 128, 0, s->st>>>(d); });
+  const dim3 gq(nb(d.nquad, 128)), bq(128);
+  launch(s, "cell", [&] {
+    if (d.mdegr == 3) k1_cell<3><<<gq, bq, 0, s->st>>>(d);
+    else if (d.mdegr == 2) k1_cell<2><<<gq, bq, 0, s->st>>>(d);
+    else k1_cell<1><<<gq, bq, 0, s->st>>>(d);
+  });
   launch(s, "node", [&] { k1_node<<<nb(d.npoin, 256), 256, 0, s->st>>>(d); });
-  launch(s, "rhs", [&] { k1_rhs<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, fuse, alfa); });
+  launch(s, "rhs", [&] {
+    if (d.mdegr == 3) k1_rhs<3><<<gq, bq, 0, s->st>>>(d, fuse, alfa);
+    else if (d.mdegr == 2) k1_rhs<2><<<gq, bq, 0, s->st>>>(d, fuse, alfa);
+    else k1_rhs<1><<<gq, bq, 0, s->st>>>(d, fuse, alfa);
+  });
 }
 
-// getsolvdg_lag (Getrhslag.f90:1553-2035) and the driver copy-back
+// getsolvdg_lag (Getrhslag.f90:1553-2035) and the driver copy-back.  On
+// this branch the cell volume is read only by getdelt_lag in the first stage,
+// so of the reference's getcellvol_lag calls (at the start of the step and
+// after every stage) only the one after the last stage is made: it is the
+// start-of-step volume of the next step (same coordinates, same arithmetic),
+// and set_state / init_fields compute it for the first step.
 static void enqueue_step(Solver *s, int itime) {
   const Dev1 &d = s->d;
   const int ns = s->cfg.nstag;
   launch(s, "copy", [&] { k1_step_begin<<<1, 1, 0, s->st>>>(d, itime); });
-  geom(s, d.xn, d.yn);
   for (int istag = 1; istag <= ns; istag++) {
     const double alfa = kRK[ns - 2][istag - 1];
     if (istag == 1) {
@@ -1011,7 +1023,7 @@ static void enqueue_step(Solver *s, int itime) {
       enqueue_rhs(s, 1, alfa);
     }
     launch(s, "nodes", [&] { k1_nodes<<<nb(d.npoin, 256), 256, 0, s->st>>>(d, alfa); });
-    geom(s, d.xs, d.ys);
+    if (istag == ns) geom(s, d.xs, d.ys);
   }
   launch(s, "copy", [&] {
     k1_copyback<<<nb(std::max(NU1 * d.ncell, d.npoin), 256), 256, 0, s->st>>>(d);

@@ -41,6 +41,13 @@ def stage_bytes(ncell: int, npoin: int, ndegr: int = 6, nq: int = 4) -> int:
     return ncell * (3 * ndegr * nq * W + 16 * W + 5 * W + 8 + 9 * 4) + npoin * (4 * 16 + 2 * 16 + 4) + 16 * ncell * 4
 
 
+def stage_bytes_p1(ncell: int, npoin: int) -> int:
+    """The same stage rule on the linear P1 path (straight 4-node quads):
+    12 DOFs per cell, M^-1 of 4 values, rc/sc, the volume, 4 node ids, the
+    same node traffic, 4 corners per quad in the node-to-corner list."""
+    return ncell * (3 * 3 * 4 * W + 4 * W + 2 * W + 8 + 4 * 4) + npoin * (4 * 16 + 2 * 16 + 4) + 4 * ncell * 4
+
+
 def kernel_bytes(family: str, ncell: int, npoin: int, nstag: int = 3) -> int:
     """Interface bytes of one launch of a kernel family on an all-quad mesh,
     averaged over the family's launches in one time step."""
