@@ -29,14 +29,20 @@
 // nodal solve leaves unused, getAS_llnl (Limiterlag.f90:15476) ends by
 // zeroing its stress, and the divergence limiter of
 // barthlimit_sympre_quadlb writes only geoel(10), which this branch never
-// reads.  Arithmetic keeps the reference's expression order, so the build
-// with --fmad=false reproduces the CPU restatement bit for bit.
+// reads.  With order_exact the kernels keep the reference's expression and
+// summation order, so the build with --fmad=false reproduces the CPU
+// restatement bit for bit; the optimised form (order_exact 0) sums the two
+// faces of each corner before the node gather and the face integral, takes
+// the volume of the straight quad in closed form and evaluates the limiter
+// function with one division.
 //
 // Layout in HBM (0-based, structure of arrays):
 //   U[(q*3 + k)*ncell + e]        P1 DOF k of field q (tau, u, v, e)
 //   ipq[k*nquad + iq]             vertex k (0..3, counter-clockwise) of quad iq
 //   cf[(v*8 + f + 2*iv)*nquad+iq] corner-face coefficient v (m, m u, m v,
 //                                 sigma.n A x, y) of corner iv, face f
+//                                 (optimised kernels: cf[(v*4 + iv)*nquad+iq],
+//                                 the two faces of corner iv summed)
 //   lim[k*ncell + e]              aflim(1), aflim(4), aflim(5), afvec(1,1),
 //                                 afvec(1,2), afvec(2,1), afvec(2,2)
 #include <cuda_runtime.h>
@@ -155,6 +161,20 @@ __device__ __forceinline__ double barthfct(double umax, double umin, double uctr
     return fmin((fiy * fiy + 2.0 * fiy) / (fiy * fiy + fiy + 2.0), 1.0);
   }
   return 1.0;
+}
+
+// The same limiter function with one division: with fiy = a / b,
+// (fiy^2 + 2 fiy) / (fiy^2 + fiy + 2) = (a^2 + 2 a b) / (a^2 + a b + 2 b^2)
+// (optimised kernels; equal up to rounding).
+__device__ __forceinline__ double barthfct1(double umax, double umin, double uctr, double dunk) {
+  if (!(dunk > 1.0e-8) && !(dunk < -1.0e-8)) return 1.0;
+  const double a = 0.7 * ((dunk > 1.0e-8 ? umax : umin) - uctr), b = dunk;
+  return fmin((a * a + 2.0 * a * b) / (a * a + a * b + 2.0 * b * b), 1.0);
+}
+
+template <bool FAST>
+__device__ __forceinline__ double limfct(double umax, double umin, double uctr, double dunk) {
+  return FAST ? barthfct1(umax, umin, uctr, dunk) : barthfct(umax, umin, uctr, dunk);
 }
 
 __device__ __forceinline__ double xv(int iv) { return (iv == 0 || iv == 3) ? -1.0 : 1.0; }
@@ -322,6 +342,28 @@ __global__ void k1_geom(Dev1 d, const double *X, const double *Y) {
   if (!(volel > 0.0)) atomicOr(&d.sc_dev->status, ST_NONPHYS);
 }
 
+// The same volume and volume centre in closed form: the 9-node image of a
+// straight quad is its bilinear map, whose Jacobian is J0 + J1 r + J2 s, so
+// V = 4 J0 and the centre in reference coordinates is (J1, J2) / (3 J0).
+__global__ void k1_geom_fast(Dev1 d, const double *X, const double *Y) {
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iq >= d.nquad || stopped(d)) return;
+  double x[4][2];
+  load4(d, X, Y, iq, x);
+  const double e1 = 0.25 * (-x[0][0] + x[1][0] + x[2][0] - x[3][0]);
+  const double e2 = 0.25 * (-x[0][0] - x[1][0] + x[2][0] + x[3][0]);
+  const double e3 = 0.25 * (x[0][0] - x[1][0] + x[2][0] - x[3][0]);
+  const double f1 = 0.25 * (-x[0][1] + x[1][1] + x[2][1] - x[3][1]);
+  const double f2 = 0.25 * (-x[0][1] - x[1][1] + x[2][1] + x[3][1]);
+  const double f3 = 0.25 * (x[0][1] - x[1][1] + x[2][1] - x[3][1]);
+  const double j0 = e1 * f2 - f1 * e2, j1 = e1 * f3 - f1 * e3, j2 = e3 * f2 - f3 * e2;
+  const double volel = 4.0 * j0;
+  d.vol[iq] = volel;
+  d.vcx[iq] = j1 / (3.0 * j0);
+  d.vcy[iq] = j2 / (3.0 * j0);
+  if (!(volel > 0.0)) atomicOr(&d.sc_dev->status, ST_NONPHYS);
+}
+
 // ---------------------------------------------------------------------------
 // Node bounds (barthlimit_lag_vtxunknew, Getrhslagmctria.f90:2548-2641):
 // max/min over the cells around the node, so the visiting order is free
@@ -356,7 +398,7 @@ __global__ void k1_bounds(Dev1 d) {
 // ---------------------------------------------------------------------------
 // Limiter and corner coefficients of one quad
 // ---------------------------------------------------------------------------
-template <int MD>
+template <int MD, bool FAST>
 __device__ void cell_pass(const Dev1 &d, int iq) {
   const int e = iq;
   const double g = d.gamlg, epsd = 1.0e-6, slpdu = (g + 1.0) / 2.0;
@@ -404,8 +446,8 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         const double dunk = w[q] - unctr[q];
-        const double a = barthfct(d.bmax[q * (size_t)d.npoin + ip[iv]], d.bmin[q * (size_t)d.npoin + ip[iv]],
-                                  unctr[q], dunk);
+        const double a = limfct<FAST>(d.bmax[q * (size_t)d.npoin + ip[iv]], d.bmin[q * (size_t)d.npoin + ip[iv]],
+                                      unctr[q], dunk);
         if (iv == 0 || a < af[q]) af[q] = a;
       }
     }
@@ -460,8 +502,8 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
         if (cls == 2 || cls == 10) take(-uj, vj);
         if (cls == 10) take(-uj, -vj);
       }
-      const double a1 = barthfct(mx1, mn1, uc, ur - uc);
-      const double a2 = barthfct(mx2, mn2, vc, vr - vc);
+      const double a1 = limfct<FAST>(mx1, mn1, uc, ur - uc);
+      const double a2 = limfct<FAST>(mx2, mn2, vc, vr - vc);
       if (iv == 0 || a1 < fl1) fl1 = a1;
       if (iv == 0 || a2 < fl2) fl2 = a2;
     }
@@ -481,8 +523,8 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
     const double t = rhom + af[0] * (1.0 / rhov - rhom);
     const double pv = pctr_s + af[3] * (pvtx - pctr_s);
     const double e5 = pv / (g - 1.0) * t + 0.5 * (uv * uv + vv * vv);
-    const double a = barthfct(d.bmax[4 * (size_t)d.npoin + ip[iv]], d.bmin[4 * (size_t)d.npoin + ip[iv]], ectr,
-                              e5 - ectr);
+    const double a = limfct<FAST>(d.bmax[4 * (size_t)d.npoin + ip[iv]], d.bmin[4 * (size_t)d.npoin + ip[iv]],
+                                  ectr, e5 - ectr);
     if (iv == 0 || a < af5) af5 = a;
   }
   const size_t nc = d.ncell;
@@ -509,6 +551,7 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
   }
   const double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
   const double sdctr = sqrt(fmax(epsd, g * pctr / rhoct));
+  double csum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   const double dudr = fi11 * u[1][1] + fi12 * u[2][1];
   const double duds = fi11 * u[1][2] + fi12 * u[2][2];
   const double dvdr = fi12 * u[1][1] + fi22 * u[2][1];
@@ -544,20 +587,30 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
       const double mu2 = 0.0 * uvl + m * vvl;
       const double s1 = sig * area * n1 + (0.0 + 0.0) * area * n2;
       const double s2 = (0.0 + 0.0) * area * n1 + sig * area * n2;
-      const int slot = f + 2 * iv;
-      d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq] = m;
-      d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq] = mu1;
-      d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq] = mu2;
-      d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq] = s1;
-      d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq] = s2;
+      if (FAST) {
+        const double v[5] = {m, mu1, mu2, s1, s2};
+#pragma unroll
+        for (int k = 0; k < 5; k++) csum[k] = (f == 0) ? v[k] : csum[k] + v[k];
+      } else {
+        const int slot = f + 2 * iv;
+        d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq] = m;
+        d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq] = mu1;
+        d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq] = mu2;
+        d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq] = s1;
+        d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq] = s2;
+      }
+    }
+    if (FAST) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) d.cf[(k * 4 + iv) * (size_t)d.nquad + iq] = csum[k];
     }
   }
 }
-template <int MD>
+template <int MD, bool FAST>
 __global__ void __launch_bounds__(128) k1_cell(Dev1 d) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
-  cell_pass<MD>(d, iq);
+  cell_pass<MD, FAST>(d, iq);
 }
 
 // ---------------------------------------------------------------------------
@@ -565,12 +618,23 @@ __global__ void __launch_bounds__(128) k1_cell(Dev1 d) {
 // corner sums in the order the reference scatters them (cells ascending,
 // corner faces 1, 2), the 2x2 solve and the wall conditions
 // ---------------------------------------------------------------------------
+template <bool FAST>
 __global__ void k1_node(Dev1 d) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= d.npoin || stopped(d)) return;
   double n11 = 0.0, n21 = 0.0, n12 = 0.0, n22 = 0.0, a1 = 0.0, a2 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int i = d.ncor_ptr[p]; i < d.ncor_ptr[p + 1]; i++) {
     const int c = d.ncor[i], iq = c >> 2, iv = c & 3;
+    if (FAST) {
+      const double m = d.cf[(0 * 4 + iv) * (size_t)d.nquad + iq];
+      n11 = n11 + m;
+      n22 = n22 + m;
+      a1 = a1 + d.cf[(1 * 4 + iv) * (size_t)d.nquad + iq];
+      a2 = a2 + d.cf[(2 * 4 + iv) * (size_t)d.nquad + iq];
+      s1 = s1 + d.cf[(3 * 4 + iv) * (size_t)d.nquad + iq];
+      s2 = s2 + d.cf[(4 * 4 + iv) * (size_t)d.nquad + iq];
+      continue;
+    }
 #pragma unroll
     for (int f = 0; f < 2; f++) {
       const int slot = f + 2 * iv;
@@ -663,7 +727,7 @@ __global__ void k1_update(Dev1 d, double alfa) {
 // ---------------------------------------------------------------------------
 // Corner forces, face and volume integrals of one quad
 // ---------------------------------------------------------------------------
-template <int MD>
+template <int MD, bool FAST>
 __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
@@ -701,8 +765,16 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
     const double us = d.us[p], vs = d.vs[p];
     // fstarq (Limiterlag.f90:686-698): sigma.n A + mu A (u* - u_v)
     double F[2][2];
+    if (FAST) {
+      // the corner's two faces summed: F = sum sigma.n A + (sum mu A) u* - sum mu A u_v
+      const double m = d.cf[(0 * 4 + iv) * (size_t)d.nquad + iq];
+      F[0][0] = d.cf[(3 * 4 + iv) * (size_t)d.nquad + iq] + m * us - d.cf[(1 * 4 + iv) * (size_t)d.nquad + iq];
+      F[0][1] = d.cf[(4 * 4 + iv) * (size_t)d.nquad + iq] + m * vs - d.cf[(2 * 4 + iv) * (size_t)d.nquad + iq];
+      F[1][0] = 0.0;
+      F[1][1] = 0.0;
+    }
 #pragma unroll
-    for (int f = 0; f < 2; f++) {
+    for (int f = 0; f < (FAST ? 0 : 2); f++) {
       const int slot = f + 2 * iv;
       const double m = d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq];
       const double mu1 = d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq];
@@ -719,6 +791,14 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
       const double b3 = 2.0 * bqv[k] + bqv[k];
       const double l1x = c16 * b3 * fn[fa][0] * fn[fa][2], l1y = c16 * b3 * fn[fa][1] * fn[fa][2];
       const double l2x = c16 * b3 * fn[fb][0] * fn[fb][2], l2y = c16 * b3 * fn[fb][1] * fn[fb][2];
+      if (FAST) {
+        const double w = c13 * b3;
+        R[k][0] = R[k][0] + us * (l1x + l2x) + vs * (l1y + l2y);
+        R[k][1] = R[k][1] + F[0][0] * w;
+        R[k][2] = R[k][2] + F[0][1] * w;
+        R[k][3] = R[k][3] + (us * F[0][0] + vs * F[0][1]) * w;
+        continue;
+      }
       R[k][0] = R[k][0] + us * l1x + vs * l1y + us * l2x + vs * l2y;
       R[k][1] = R[k][1] + F[0][0] * c13 * b3 + F[1][0] * c13 * b3;
       R[k][2] = R[k][2] + F[0][1] * c13 * b3 + F[1][1] * c13 * b3;
@@ -978,24 +1058,38 @@ static const double kRK[2][3] = {{0.0, 0.5, 0.0}, {0.0, 0.75, 0.3333333333333333
 
 static void geom(Solver *s, const double *X, const double *Y) {
   const Dev1 &d = s->d;
-  launch(s, "geom", [&] { k1_geom<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, X, Y); });
+  launch(s, "geom", [&] {
+    if (s->cfg.order_exact) k1_geom<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, X, Y);
+    else k1_geom_fast<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, X, Y);
+  });
+}
+
+template <bool FAST>
+static void launch_cell(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st) {
+  if (d.mdegr == 3) k1_cell<3, FAST><<<g, b, 0, st>>>(d);
+  else if (d.mdegr == 2) k1_cell<2, FAST><<<g, b, 0, st>>>(d);
+  else k1_cell<1, FAST><<<g, b, 0, st>>>(d);
+}
+template <bool FAST>
+static void launch_rhs(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st, int fuse, double alfa) {
+  if (d.mdegr == 3) k1_rhs<3, FAST><<<g, b, 0, st>>>(d, fuse, alfa);
+  else if (d.mdegr == 2) k1_rhs<2, FAST><<<g, b, 0, st>>>(d, fuse, alfa);
+  else k1_rhs<1, FAST><<<g, b, 0, st>>>(d, fuse, alfa);
 }
 
 // the stage sequence of getrhsdg_lag_mcnew's linear branch
 static void enqueue_rhs(Solver *s, int fuse, double alfa) {
   const Dev1 &d = s->d;
   launch(s, "bounds", [&] { k1_bounds<<<nb(d.npoin, 256), 256, 0, s->st>>>(d); });
-  const dim3 gq(nb(d.nquad, 128)), bq(128);
-  launch(s, "cell", [&] {
-    if (d.mdegr == 3) k1_cell<3><<<gq, bq, 0, s->st>>>(d);
-    else if (d.mdegr == 2) k1_cell<2><<<gq, bq, 0, s->st>>>(d);
-    else k1_cell<1><<<gq, bq, 0, s->st>>>(d);
+  const dim3 gq(nb(d.nquad, 128)), bq(128), gp(nb(d.npoin, 256)), bp(256);
+  const bool ex = s->cfg.order_exact != 0;
+  launch(s, "cell", [&] { ex ? launch_cell<false>(d, gq, bq, s->st) : launch_cell<true>(d, gq, bq, s->st); });
+  launch(s, "node", [&] {
+    if (ex) k1_node<false><<<gp, bp, 0, s->st>>>(d);
+    else k1_node<true><<<gp, bp, 0, s->st>>>(d);
   });
-  launch(s, "node", [&] { k1_node<<<nb(d.npoin, 256), 256, 0, s->st>>>(d); });
   launch(s, "rhs", [&] {
-    if (d.mdegr == 3) k1_rhs<3><<<gq, bq, 0, s->st>>>(d, fuse, alfa);
-    else if (d.mdegr == 2) k1_rhs<2><<<gq, bq, 0, s->st>>>(d, fuse, alfa);
-    else k1_rhs<1><<<gq, bq, 0, s->st>>>(d, fuse, alfa);
+    ex ? launch_rhs<false>(d, gq, bq, s->st, fuse, alfa) : launch_rhs<true>(d, gq, bq, s->st, fuse, alfa);
   });
 }
 

@@ -1,10 +1,12 @@
 """Parity of the CUDA linear P1 path (straight 4-node quads, the Sod
 configuration; lag2d_p1.cu behind the same C-ABI) against the CPU oracle.
 
-The P1 kernels keep the reference's summation order, so the no-FMA build
-(liblag2d_exact.so) must match the restatement bit for bit: initial fields,
-one getrhsdg_lag_mcnew call (RHS, limited state, nodal velocity) and whole
-steps.  The FMA build stays within 1e-12 of the field scale per step.  The
+With order_exact the P1 kernels keep the reference's summation order, so the
+no-FMA build (liblag2d_exact.so) must match the restatement bit for bit:
+initial fields, one getrhsdg_lag_mcnew call (RHS, limited state, nodal
+velocity) and whole steps.  The optimised kernels (corner faces summed per
+corner, closed-form volumes, one-division limiter function) in the FMA build
+stay within 1e-12 of the field scale per step.  The
 limiter branches on comparisons (barthfct, the strain-rate frame), so the FMA
 build is compared over a few steps only.
 """
@@ -43,7 +45,7 @@ def _oracle_state(name, nsteps):
 def test_p1_init_fields(name, exact):
     m, c = workload(name)
     geoel, amatr, unkno = Oracle(m, c).init()
-    s = Lag2DSolver(m, c, exact=exact)
+    s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
     g2, a2, u2 = s.init_fields()
     n = m.ncell
     if exact:
@@ -64,7 +66,7 @@ def test_p1_rhs_single(name, nsteps, exact):
     """One getrhsdg_lag_mcnew call on a state a few steps in: rhsel, the
     limited stage state and the new nodal velocity."""
     m, c, o, geoel, amatr, unkno, coord, ustar, _, _ = _oracle_state(name, nsteps)
-    s = Lag2DSolver(m, c, exact=exact)
+    s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
     s.set_state(unkno, coord, ustar, geoel, amatr)
     r2, f2 = s.rhs()
     u2, _, us2, _ = s.get_state()
@@ -92,7 +94,7 @@ def test_p1_steps(name, nsteps, exact):
     geoel, amatr, unkno = o.init()
     coord = m.coord.copy()
     ustar = np.zeros_like(coord)
-    s = Lag2DSolver(m, c, exact=exact)
+    s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
     s.init_fields()
     dt, ta = c.dtfix, 0.0
     n = m.ncell
@@ -117,11 +119,11 @@ def test_p1_steps(name, nsteps, exact):
 @pytest.mark.parametrize("exact", [True, False])
 def test_p1_graph_run_matches_steps(exact):
     m, c = workload("sod_jitter40")
-    a = Lag2DSolver(m, c, exact=exact)
+    a = Lag2DSolver(m, c, exact=exact, order_exact=exact)
     a.init_fields()
     for _ in range(8):
         a.step()
-    b = Lag2DSolver(m, c, exact=exact)
+    b = Lag2DSolver(m, c, exact=exact, order_exact=exact)
     b.init_fields()
     assert b.run(8) == 8
     ua, xa, usa, _ = a.get_state()
@@ -137,7 +139,7 @@ def test_p1_golden_fixture():
     ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "sod12_p1.npz"))
     m = linear_quad_mesh(12, 4, 0.0, 1.0, 0.0, 0.4, jitter=0.15, seed=7)
     c = StepConfig(npoly=1, ndegr=3, mdegr=3, ncase=6, gamlg=1.4, nstag=2, cfl=0.3, tend=0.2)
-    s = Lag2DSolver(m, c, exact=True)
+    s = Lag2DSolver(m, c, exact=True, order_exact=True)
     _, a2, u0 = s.init_fields()
     n = m.ncell
     assert np.array_equal(u0[:n], ref["unkno0"][:n]) and np.array_equal(a2, ref["amatr"])
