@@ -128,6 +128,15 @@ int lag2d_weno(lag2d_handle *h, const int *flags);
  * geoel(24,nsize) with fields 3, 5, 6 refreshed if geoel is not NULL. */
 int lag2d_cellvol(lag2d_handle *h, double *geoel);
 
+/* geterror_lag_curvhybrid (Postprocess.f90:3587-4143): the L2 errors of the
+ * handle's state against the exact solution, 25-point Gauss on the current
+ * coordinates, errl2[3] = sqrt of the integrals of the squared errors of
+ * (rho, |u|, p) for ncase 1 (Taylor-Green) or (rho, e_int, p) for ncase 2
+ * (shockless Noh).  The reference prints these at the end of a run.  P2
+ * all-quad meshes; other cases, triangles and the P1 path return
+ * LAG2D_EUNSUP.  The sum over cells is a fixed-order reduction. */
+int lag2d_error_norms(lag2d_handle *h, double *errl2);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that time or
  * order work against the library's launches. */
 void *lag2d_stream(const lag2d_handle *h);

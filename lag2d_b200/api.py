@@ -65,7 +65,8 @@ _libs = {}
 EXPORTS = ("lag2d_create", "lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run",
            "lag2d_get_state", "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_stream",
            "lag2d_kernel_launches", "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error",
-           "lag2d_delt_noalloc", "lag2d_adjoint_step", "lag2d_adjoint", "lag2d_set_rho0")
+           "lag2d_delt_noalloc", "lag2d_adjoint_step", "lag2d_adjoint", "lag2d_set_rho0",
+           "lag2d_error_norms")
 
 
 def library_path(exact: bool = False) -> str:
@@ -89,7 +90,7 @@ def load(exact: bool = False):
     lib.lag2d_create.argtypes = [ctypes.POINTER(_Mesh), ctypes.POINTER(_Cfg), ctypes.POINTER(ctypes.c_void_p)]
     for name in ("lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run", "lag2d_get_state",
                  "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_timing", "lag2d_adjoint_step",
-                 "lag2d_adjoint", "lag2d_set_rho0"):
+                 "lag2d_adjoint", "lag2d_set_rho0", "lag2d_error_norms"):
         getattr(lib, name).restype = ctypes.c_int
     lib.lag2d_destroy.argtypes = [ctypes.c_void_p]
     _libs[key] = lib
@@ -211,6 +212,14 @@ class Lag2DSolver:
     def weno(self, flags):
         f = np.ascontiguousarray(flags, dtype=np.int32)
         self._check(self.lib.lag2d_weno(self.h, _p(f, _ip)))
+
+    def error_norms(self) -> np.ndarray:
+        """geterror_lag_curvhybrid's L2 errors of the current state against the
+        exact solution: (rho, |u|, p) for Taylor-Green, (rho, e_int, p) for the
+        shockless Noh case."""
+        e = np.zeros(3)
+        self._check(self.lib.lag2d_error_norms(self.h, _p(e, _dp)))
+        return e
 
     def cellvol(self):
         geoel = np.zeros((self.mesh.nsize, 24))

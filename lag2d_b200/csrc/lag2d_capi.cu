@@ -58,6 +58,8 @@ void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const doub
 void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold,
                           int mixed);
 int adjoint_stage_launches(const Dev &d);
+int error_blocks(const Dev &d);
+void launch_error(const Dev &d, cudaStream_t st, const double *X, const double *Y, double *part);
 }  // namespace lag2d
 
 using namespace lag2d;
@@ -102,6 +104,7 @@ struct lag2d_handle {
   std::map<std::string, Family> fam;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   p1::Solver *p1 = nullptr;    // the linear P1 path (npoly = 1) when set; Dev d is then unused
+  double *errpart = nullptr;   // per-block partial sums of lag2d_error_norms
 };
 
 template <typename T>
@@ -909,6 +912,30 @@ int lag2d_cellvol(lag2d_handle *h, double *geoel) {
   int r = read_status(h);
   if (r) return r;
   if (geoel) return download_geoel(h, geoel);
+  return LAG2D_OK;
+}
+
+int lag2d_error_norms(lag2d_handle *h, double *errl2) {
+  if (!h || !errl2) return fail(LAG2D_EINVAL, "null argument");
+  if (h->p1) return fail(LAG2D_EUNSUP, "the error norms are built for the P2 path");
+  Dev &d = h->d;
+  if (d.ntria > 0) return fail(LAG2D_EUNSUP, "the error norms are built for all-quad meshes");
+  if (d.ncase != 1 && d.ncase != 2)
+    return fail(LAG2D_EUNSUP, "geterror_lag_curvhybrid has an exact solution for the cases 1 and 2 only");
+  const int nb = error_blocks(d);
+  if (!h->errpart) {
+    int r = dalloc(h, &h->errpart, 3 * (size_t)nb);
+    if (r) return r;
+  }
+  run(h, "error", [&] { launch_error(d, h->st, d.xs, d.ys, h->errpart); });
+  std::vector<double> part(3 * (size_t)nb);
+  CK(cudaMemcpyAsync(part.data(), h->errpart, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  double e[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < nb; b++)
+    for (int k = 0; k < 3; k++) e[k] += part[3 * (size_t)b + k];
+  for (int k = 0; k < 3; k++) errl2[k] = std::sqrt(e[k]);
   return LAG2D_OK;
 }
 

@@ -2930,6 +2930,71 @@ void launch_persson(const Dev &d, cudaStream_t st) { k_persson<<<nblk(d.nquad, 1
 void launch_flags_from_host(const Dev &d, cudaStream_t st, const int *flags) {
   k_flags_from_host<<<nblk(d.nquad, 256), 256, 0, st>>>(d, flags);
 }
+// geterror_lag_curvhybrid (Postprocess.f90:3587-4143, quad loop :3736-3944):
+// per-block partial sums of the squared L2 errors against the exact solution
+// of ncase 1 (rho, |u|, p) or 2 (rho, e_int, p), 25-point Gauss on the current
+// coordinates; the host adds the block partials in block order.
+__global__ void k_error_partial(Dev d, const double *X, const double *Y, double *part) {
+  __shared__ double sm[3][256];
+  const int iq = blockIdx.x * blockDim.x + threadIdx.x;
+  double err[3] = {0.0, 0.0, 0.0};
+  if (iq < d.nquad) {
+    const int e = iq + d.ntria;
+    const double g = d.gamlg;
+    double xp[9][2], shp[9], dr[9], ds[9];
+    load_quad(d, X, Y, iq, xp);
+    const double rc = d.rc[e], sc = d.sc[e];
+    for (int ig = 0; ig < 25; ig++) {
+      const double r = cQ.g25[ig][0], s = cQ.g25[ig][1], wi = cQ.w25[ig];
+      shp9v(r, s, shp);
+      shp9d(r, s, dr, ds);
+      Jac j = jac9(xp, dr, ds);
+      const double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+      double xg, yg;
+      map9(xp, shp, xg, yg);
+      double bq[6];
+      bq[0] = 1.0; bq[1] = (r - rc) / 1.0; bq[2] = (s - sc) / 1.0;
+      bq[3] = 0.5 * bq[1] * bq[1] - d.g19[e];
+      bq[4] = 0.5 * bq[2] * bq[2] - d.g20[e];
+      bq[5] = bq[1] * bq[2] - d.g21[e];
+      double un[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int k = 0; k < d.mdegr; k++)
+        for (int q = 0; q < 4; q++) un[q] = un[q] + Uget(d, d.Us, k, q, e) * bq[k];
+      const double rho = 1.0 / un[0], uadv = un[1], vadv = un[2], eadv = un[3];
+      const double pres = (g - 1.0) * rho * (eadv - 0.5 * (uadv * uadv + vadv * vadv));
+      double e0, e1, e2;
+      if (d.ncase == 1) {
+        const double pexa = 0.25 * (cos(2.0 * cPI * xg) + cos(2.0 * cPI * yg)) + 1.0;
+        const double uexa = sin(cPI * xg) * cos(cPI * yg), vexa = -cos(cPI * xg) * sin(cPI * yg);
+        e0 = rho - 1.0;
+        e1 = sqrt(uadv * uadv + vadv * vadv) - sqrt(uexa * uexa + vexa * vexa);
+        e2 = pres - pexa;
+      } else {
+        const double eiadv = eadv - 0.5 * (uadv * uadv + vadv * vadv);
+        const double eiexa = pow(1.0 - 0.6, -2.0 * (g - 1.0)), rhoexa = pow(1.0 - 0.6, -2.0);
+        e0 = rho - rhoexa;
+        e1 = eiadv - eiexa;
+        e2 = pres - (g - 1.0) * rhoexa * eiadv;
+      }
+      err[0] = err[0] + fabs(e0) * fabs(e0) * djaco;
+      err[1] = err[1] + fabs(e1) * fabs(e1) * djaco;
+      err[2] = err[2] + fabs(e2) * fabs(e2) * djaco;
+    }
+  }
+  for (int k = 0; k < 3; k++) sm[k][threadIdx.x] = err[k];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int k = 0; k < 3; k++) sm[k][threadIdx.x] += sm[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; k++) part[3 * blockIdx.x + k] = sm[k][0];
+}
+int error_blocks(const Dev &d) { return nblk(d.nquad, 256); }
+void launch_error(const Dev &d, cudaStream_t st, const double *X, const double *Y, double *part) {
+  k_error_partial<<<nblk(d.nquad, 256), 256, 0, st>>>(d, X, Y, part);
+}
 void launch_weno(const Dev &d, cudaStream_t st) { k_weno<<<nblk(d.nquad, 64), 64, 0, st>>>(d); }
 // one warp per troubled quad, a grid of at most 8 blocks per SM looping over the list
 void launch_weno_warp(const Dev &d, cudaStream_t st) {

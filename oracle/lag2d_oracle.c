@@ -3014,3 +3014,63 @@ void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
   free(indnd); free(munacn); free(munacu); free(snsigm); free(mcl); free(mul); free(snl); free(fst);
   free(vlave);
 }
+
+/* ---------------------------------------------------------------------- */
+/* geterror_lag_curvhybrid, Postprocess.f90:3587-4143 (quad loop          */
+/* :3736-3944): L2 errors against the exact solution, 25-point Gauss on    */
+/* the current coordinates, returned as sqrt(errlp(1:3)).  ncase 1         */
+/* (Taylor-Green: rho, |u|, p) and 2 (shockless Noh: rho, e_int, p).       */
+/* ---------------------------------------------------------------------- */
+void o_error(const o_mesh *m, const o_cfg *c, const double *unkno, const double *geoel,
+             const double *coord, double *errl2) {
+  double pos25[25][2], w25[25];
+  quad_rule(25, 0, pos25, w25);
+  const double g = c->gamlg;
+  double errlp[3] = {0.0, 0.0, 0.0};
+  for (int ie = 0; ie < m->nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double xp[9][2], shp[9], dr[9], ds[9];
+    load_quad(m, coord, ie, xp);
+    const double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    for (int ig = 0; ig < 25; ig++) {
+      double r = pos25[ig][0], s = pos25[ig][1], wi = w25[ig];
+      double a, b, cc, d, xg, yg;
+      shp9(r, s, shp, dr, ds);
+      jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+      double djaco = wi * (a * d - cc * b);
+      map9((const double(*)[2])xp, shp, &xg, &yg);
+      double bq[6];
+      bq[0] = 1.0;
+      bq[1] = (r - rc) / 1.0;
+      bq[2] = (s - sc) / 1.0;
+      if (c->npoly == 2) {
+        bq[3] = 0.5 * bq[1] * bq[1] - G_(geoel, 18, ielem);
+        bq[4] = 0.5 * bq[2] * bq[2] - G_(geoel, 19, ielem);
+        bq[5] = bq[1] * bq[2] - G_(geoel, 20, ielem);
+      }
+      double un[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int k = 0; k < c->mdegr; k++)
+        for (int q = 0; q < 4; q++) un[q] = un[q] + U_(unkno, c, k, q, ielem) * bq[k];
+      const double rho = 1.0 / un[0], uadv = un[1], vadv = un[2], eadv = un[3];
+      const double pres = (g - 1.0) * rho * (eadv - 0.5 * (uadv * uadv + vadv * vadv));
+      if (c->ncase == 1) {
+        const double pexa = 0.25 * (cos(2.0 * PI_ * xg) + cos(2.0 * PI_ * yg)) + 1.0;
+        const double uexa = sin(PI_ * xg) * cos(PI_ * yg);
+        const double vexa = -cos(PI_ * xg) * sin(PI_ * yg);
+        const double vemag = sqrt(uadv * uadv + vadv * vadv), veexa = sqrt(uexa * uexa + vexa * vexa);
+        errlp[0] = errlp[0] + fabs(rho - 1.0) * fabs(rho - 1.0) * djaco;
+        errlp[1] = errlp[1] + fabs(vemag - veexa) * fabs(vemag - veexa) * djaco;
+        errlp[2] = errlp[2] + fabs(pres - pexa) * fabs(pres - pexa) * djaco;
+      } else if (c->ncase == 2) {
+        const double eiadv = eadv - 0.5 * (uadv * uadv + vadv * vadv);
+        const double eiexa = pow(1.0 - 0.6, -2.0 * (g - 1.0));
+        const double rhoexa = pow(1.0 - 0.6, -2.0);
+        const double pexa = (g - 1.0) * rhoexa * eiadv;
+        errlp[0] = errlp[0] + fabs(rho - rhoexa) * fabs(rho - rhoexa) * djaco;
+        errlp[1] = errlp[1] + fabs(eiadv - eiexa) * fabs(eiadv - eiexa) * djaco;
+        errlp[2] = errlp[2] + fabs(pres - pexa) * fabs(pres - pexa) * djaco;
+      }
+    }
+  }
+  for (int k = 0; k < 3; k++) errl2[k] = sqrt(errlp[k]);
+}

@@ -96,6 +96,12 @@ int o_run(const o_mesh *m, const o_cfg *c, double *unkno, double *coord,
           const double *coold, double *geoel, const double *amatr,
           double *ustar, int itime0, int nsteps, double *dtfix, double *tacru);
 
+/* geterror_lag_curvhybrid (Postprocess.f90:3587-4143), quads: L2 errors
+ * against the exact solution of ncase 1 (rho, |u|, p) or 2 (rho, e_int, p)
+ * on the current coordinates; errl2[3] = sqrt(errlp(1:3)). */
+void o_error(const o_mesh *m, const o_cfg *c, const double *unkno, const double *geoel,
+             const double *coord, double *errl2);
+
 /* ---- Linear P1 path (ncurv=0, nfint=1, nlimi=6, nrz=0; 4-node quads, no
  * triangles).  o_init, o_cellvol and o_run serve it too (o_mesh.nvqua = 4,
  * o_cfg.npoly = 1); these are its inner seams. ---- */

@@ -105,6 +105,13 @@ class Oracle:
         lib().o_weno(ctypes.byref(self.om), ctypes.byref(self.oc), _p(unkno, _dp), _p(geoel, _dp),
                      _p(coord, _dp), _p(coold, _dp), _p(f, _ip))
 
+    def error_norms(self, unkno, geoel, coord):
+        """geterror_lag_curvhybrid's L2 errors (3,) on the quads."""
+        e = np.zeros(3)
+        lib().o_error(ctypes.byref(self.om), ctypes.byref(self.oc), _p(np.ascontiguousarray(unkno), _dp),
+                      _p(np.ascontiguousarray(geoel), _dp), _p(np.ascontiguousarray(coord), _dp), _p(e, _dp))
+        return e
+
     def rhs_p1(self, ustar, unkno, geoel, coord):
         """The linear P1 branch of getrhsdg_lag_mcnew; unkno is limited and
         ustar updated in place.  Returns (rhsel, aflim (ncell, 5), afvec (ncell, 4))."""

@@ -260,3 +260,21 @@ def test_initial_density_factors():
     p0 = (c.gamlg - 1.0) / u0[:n, 0, 0] * (u0[:n, 3, 0] - 0.5 * (u0[:n, 1, 0] ** 2 + u0[:n, 2, 0] ** 2))
     p1 = (c.gamlg - 1.0) / u1[:n, 0, 0] * (u1[:n, 3, 0] - 0.5 * (u1[:n, 1, 0] ** 2 + u1[:n, 2, 0] ** 2))
     assert np.allclose(p1, p0, rtol=1e-11, atol=1e-17)
+
+
+def test_error_norms_third_order_projection():
+    """geterror_lag_curvhybrid's L2 errors of the initial Taylor-Green P2
+    projection fall by ~8x per mesh halving (third order) for |u| and p, and
+    the density error is rounding (the projection of rho = 1)."""
+    from lag2d_b200.config import _tgv
+    errs = []
+    for n in (8, 16, 32):
+        m, c = _tgv(n)
+        o = Oracle(m, c)
+        geoel, _, unkno = o.init()
+        errs.append(o.error_norms(unkno, geoel, m.coord))
+    errs = np.array(errs)
+    assert (errs[:, 0] < 1e-13).all()
+    for k in (1, 2):
+        ratios = errs[:-1, k] / errs[1:, k]
+        assert (ratios > 7.5).all() and (ratios < 8.5).all(), ratios
