@@ -299,6 +299,12 @@ static void corner_pass(lag2d_handle *h, const Dev &d) {
   if (h->cfg.precision == 1) launch_mixed_corner(d, h->st);
   else launch_fast_corner(d, h->st);
 }
+// launches of rhs_pass: the triangles' kernel, then one (FP32-mixed) or two
+// (FP64: face integral, rest) quad kernels
+static int rhs_launches(const lag2d_handle *h, const Dev &d) {
+  return (d.ntria > 0) + (h->cfg.precision == 1 ? 1 : 2);
+}
+
 static void rhs_pass(lag2d_handle *h, const Dev &d, int fuse, double alfa) {
   launch_tri_rhs(d, h->st, d.us_new, d.vs_new, fuse, alfa);
   if (h->cfg.precision == 1) launch_mixed_rhs(d, h->st, fuse, alfa);
@@ -378,13 +384,13 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
     run(h, "corner", [&] { corner_pass(h, d); }, 1 + T);
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
-      run(h, "rhs", [&] { rhs_pass(h, d, 0, alfa); }, 1 + T);
+      run(h, "rhs", [&] { rhs_pass(h, d, 0, alfa); }, rhs_launches(h, d));
       run(h, "dt", [&] { launch_dt(d, h->st, h->cfg.ndt); }, 2);
       if (rec)
         cudaMemcpyAsync(rec->dt + rec->step, &d.sc_dev->dtfix, sizeof(double), cudaMemcpyDeviceToDevice, h->st);
       run(h, "update", [&] { launch_fast_update(d, h->st, alfa); });
     } else {
-      run(h, "rhs", [&] { rhs_pass(h, d, 1, alfa); }, 1 + T);
+      run(h, "rhs", [&] { rhs_pass(h, d, 1, alfa); }, rhs_launches(h, d));
     }
     run(h, "nodes", [&] { launch_fast_nodes(d, h->st, alfa); });
     run(h, "geom", [&] { launch_tri_geom(d, h->st, d.xs, d.ys); launch_fast_geom(d, h->st, 1); }, 1 + T);
@@ -862,7 +868,7 @@ int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
   } else {
     run(h, "corner", [&] { corner_pass(h, d); }, 1 + (d.ntria > 0));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
-    run(h, "rhs", [&] { rhs_pass(h, d, 0, 0.0); }, 1 + (d.ntria > 0));
+    run(h, "rhs", [&] { rhs_pass(h, d, 0, 0.0); }, rhs_launches(h, d));
     // the RHS keeps ustar of the previous stage for the impedances; expose the new one
     CK(cudaMemcpyAsync(d.us, d.us_new, d.npoin * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
     CK(cudaMemcpyAsync(d.vs, d.vs_new, d.npoin * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
