@@ -133,6 +133,7 @@ WORKLOADS = {
     "tgv16": lambda: _tgv(16),
     # Sedov blast: [0,1.2]^2, gamma 1.4, energy in the corner cell
     "sedov128": lambda: _sedov(128),
+    "sedov64": lambda: _sedov(64),
     "sedov32": lambda: _sedov(32),
     "sedov16": lambda: _sedov(16),
     # the same cases on tri/quad meshes (alternate rows of quads split into triangles)

@@ -408,9 +408,10 @@ static int read_status(lag2d_handle *h) {
   CK(cudaMemcpyAsync(&s, h->d.sc_dev, sizeof(Scalars), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
+  // a broken state outranks the stencil notice (which leaves the step complete)
+  if (s.status & ST_NONPHYS) return fail(LAG2D_ENONPHYS, "non-positive cell volume");
   if (s.status & ST_STENCIL)
     return fail(LAG2D_ESTENCIL, "WENO: a troubled quad has a vertex valence the reference rejects");
-  if (s.status & ST_NONPHYS) return fail(LAG2D_ENONPHYS, "non-positive cell volume");
   return LAG2D_OK;
 }
 
