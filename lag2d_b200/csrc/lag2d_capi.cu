@@ -294,6 +294,12 @@ static void enqueue_step_reference_order(lag2d_handle *h, int itime) {
 // Corner and RHS passes of the optimised step: FP64, or the FP32-mixed form
 // (config precision = 1) with the same node pass, update and geometry.
 // Triangles run their FP64 kernels in both forms.
+// launches of corner_pass: the triangles' kernel, then one (FP32-mixed) or
+// two (FP64: sub-cell corrections, corner faces) quad kernels
+static int corner_launches(const lag2d_handle *h, const Dev &d) {
+  return (d.ntria > 0) + (h->cfg.precision == 1 ? 1 : 2);
+}
+
 static void corner_pass(lag2d_handle *h, const Dev &d) {
   launch_tri_corner(d, h->st);
   if (h->cfg.precision == 1) launch_mixed_corner(d, h->st);
@@ -381,7 +387,7 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
       k_count_limited<<<1, 256, 0, h->st>>>(d, rec->troubled);
       h->launches += 1;
     }
-    run(h, "corner", [&] { corner_pass(h, d); }, 1 + T);
+    run(h, "corner", [&] { corner_pass(h, d); }, corner_launches(h, d));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
       run(h, "rhs", [&] { rhs_pass(h, d, 0, alfa); }, rhs_launches(h, d));
@@ -867,7 +873,7 @@ int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
     run(h, "node", [&] { launch_node(d, h->st); });
     run(h, "rhs", [&] { launch_tri_rhs(d, h->st, d.us, d.vs, 0, 0.0); launch_rhs(d, h->st); }, 1 + (d.ntria > 0));
   } else {
-    run(h, "corner", [&] { corner_pass(h, d); }, 1 + (d.ntria > 0));
+    run(h, "corner", [&] { corner_pass(h, d); }, corner_launches(h, d));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     run(h, "rhs", [&] { rhs_pass(h, d, 0, 0.0); }, rhs_launches(h, d));
     // the RHS keeps ustar of the previous stage for the impedances; expose the new one
