@@ -1741,10 +1741,16 @@ __global__ void k_nodes2(Dev d, double alfa) { f_nodes(d, blockIdx.x * blockDim.
 __global__ void k_geom2(Dev d, int fix) { f_geom(d, blockIdx.x * blockDim.x + threadIdx.x, fix); }
 __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + threadIdx.x); }
 
+// resident blocks of 128 per SM the reverse corner and RHS kernels are
+// compiled for: 3 (168 registers) in the FP32-mixed adjoint (reverse sweep
+// 15.65 -> 15.08 ms per step on the 1024x1024 Taylor-Green mesh), 1 (255)
+// in the FP64 one (3 would cost 12%)
 template <typename R>
-__global__ void __launch_bounds__(128) k_a_corner(Dev d, Adj a) { a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+constexpr int arev_minb() { return sizeof(R) == 4 ? 3 : 1; }
 template <typename R>
-__global__ void __launch_bounds__(128) k_a_rhs(Dev d, Adj a) { a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(128, arev_minb<R>()) k_a_corner(Dev d, Adj a) { a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+template <typename R>
+__global__ void __launch_bounds__(128, arev_minb<R>()) k_a_rhs(Dev d, Adj a) { a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_gather(Dev d, Adj a, int nv) { a_gather(d, a, blockIdx.x * blockDim.x + threadIdx.x, nv); }
 __global__ void k_a_gather_solve(Dev d, Adj a) { a_gather_solve(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_update(Dev d, Adj a, double alfa, const double *dtp, int fold) {
