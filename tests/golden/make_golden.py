@@ -6,7 +6,9 @@ give the GPU path fixed targets: small Taylor-Green and Sedov runs (8 x 8, a
 12 x 12 Sedov with troubled cells, a curved 6 x 6 quad mesh, a curved
 tri/quad mesh and the Noh implosion on a 4 x 4 quarter-disk mesh with
 triangles at the origin), 3 time steps each, and the radial Sod problem on a
-jittered 12 x 4 mesh of straight quads on the linear P1 path, 6 steps.
+jittered 12 x 4 mesh of straight quads on the linear P1 path, 6 steps; and the
+Sedov problem on 32 x 32 quads run to t_end = 1 (`sedov32_tend`: cell averages
+and coordinates only).
 
     python tests/golden/make_golden.py            # all fixtures
     python tests/golden/make_golden.py tgv6_hybrid # one fixture
@@ -56,7 +58,22 @@ def run_case(name):
                 dtfix=np.float64(dt), tacru=np.float64(ta), nsteps=np.int64(nsteps))
 
 
+def run_to_end(name="sedov32"):
+    """The full-box Sedov problem on 32 x 32 quads run to t_end = 1 (322
+    steps): cell averages, coordinates and the driver scalars only."""
+    from lag2d_b200.config import workload
+    m, c = workload(name)
+    o = Oracle(m, c)
+    geoel, amatr, unkno = o.init()
+    coord = m.coord.copy()
+    ustar = np.zeros_like(coord)
+    n, dt, ta = o.run(unkno, coord, m.coord, geoel, amatr, ustar, 1, 1000, c.dtfix, 0.0)
+    return dict(avg=unkno[:m.ncell, :, 0].copy(), coord=coord, dtfix=np.float64(dt), tacru=np.float64(ta),
+                nsteps=np.int64(n))
+
+
 if __name__ == "__main__":
-    for name in (sys.argv[1:] or CASES):
-        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **run_case(name))
+    for name in (sys.argv[1:] or list(CASES) + ["sedov32_tend"]):
+        data = run_to_end() if name == "sedov32_tend" else run_case(name)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
         print("wrote", name)
