@@ -178,3 +178,33 @@ def test_p1_unsupported_calls():
     with pytest.raises(Lag2DError) as e:
         Lag2DSolver(m, c, precision=1)
     assert e.value.code == 3
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_p1_sod_strip_to_end_time(exact):
+    """The Sod strip (200 x 1 straight quads, planar discontinuity at x = 0.5)
+    run to t_end = 0.2 through lag2d_run: bit for bit with the oracle in the
+    reference-order no-FMA build, within 1e-10 in the optimised FMA build, and
+    the star state of the exact Riemann solution (u* = 0.92745, p* = 0.30313)
+    on the plateau."""
+    from lag2d_b200.config import _sod
+    m, c = _sod(200, 1, 0.005)
+    o = Oracle(m, c)
+    geoel, amatr, unkno = o.init()
+    coord = m.coord.copy()
+    ustar = np.zeros_like(coord)
+    n1, dt1, ta1 = o.run(unkno, coord, m.coord.copy(), geoel, amatr, ustar, 1, 2000, c.dtfix, 0.0)
+    s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
+    s.init_fields()
+    assert s.run(2000) == n1 and abs(s.tacru - 0.2) < 1e-12
+    u2, x2, _, _ = s.get_state()
+    n = m.ncell
+    if exact:
+        assert np.array_equal(u2[:n], unkno[:n]) and np.array_equal(x2, coord)
+    else:
+        assert _field_err(u2[:n, :, :1], unkno[:n, :, :1]).max() < 1e-10
+    tau, u, e = u2[:n, 0, 0], u2[:n, 1, 0], u2[:n, 3, 0]
+    p = 0.4 / tau * (e - 0.5 * u * u)
+    xc = x2[m.ipqua - 1][:, :, 0].mean(axis=1)
+    star = (xc > 0.58) & (xc < 0.82)
+    assert np.abs(u[star] - 0.92745).max() < 0.03 and np.abs(p[star] - 0.30313).max() < 0.02
