@@ -208,9 +208,14 @@ int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every,
  * LAG2D_DELT_NOALLOC_MAX_QUADS quads (256 KiB); larger meshes are rejected
  * with LAG2D_EINVAL.  Nothing in that scratch has to start at zero.
  *
- * Arguments: ntria, nquad, npoin, ndegr, nq, ngeel are the reference's
- * dimensions; every array is a DEVICE pointer in the reference's layout:
- * ipqua(9,nquad) 1-based, unkno(ndegr,nq,nsize) (the stage-1 state after
+ * Arguments: ntria, nquad, npoin, nvqua, ndegr, nq, ngeel are the
+ * reference's dimensions and ncurv its geometry knob: ncurv = 0 takes the
+ * edge lengths between the 4 corner nodes (straight quads, nvqua >= 4, e.g.
+ * the linear P1 path's ipqua(4,nquad)); ncurv >= 1 takes corner - mid-edge
+ * node - corner over nodes 1..8 (curved quads, nvqua >= 8, e.g.
+ * ipqua(9,nquad)); other combinations are rejected with LAG2D_EINVAL.  Every
+ * array is a DEVICE pointer in the reference's layout: ipqua(nvqua,nquad)
+ * 1-based, unkno(ndegr,nq,nsize) (the stage-1 state after
  * limiting), geoel(ngeel,nsize) (geoel(3,:) = cell volume), coord(2,npoin)
  * (positions at the start of the step), dvdt(ncell) = rhsel(1,1,:) of stage
  * 1.  itime == 1 gives dtfix = min(cfl dtcfl, 0.1 dtvol); otherwise the
@@ -220,16 +225,17 @@ int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every,
  * queued on `stream` (a cudaStream_t; NULL = the default stream) and the call
  * returns without synchronising.
  *
- * Set-up: the first call on each device (with that device current) looks up
- * the scratch address and loads the kernels; make one call per device before
- * any stream capture begins.  Concurrency: the scratch is one array per
+ * Set-up: every call looks up the scratch address on the current device
+ * (so a device reset between calls is harmless); the first call on each
+ * device (with that device current) also loads the kernels, so make one call
+ * per device before any stream capture begins.  Concurrency: the scratch is one array per
  * device, so calls that may overlap on the same device (different streams or
  * host threads with no order between them) race and give wrong results:
  * serialise them.
  * ------------------------------------------------------------------------- */
 #define LAG2D_DELT_NOALLOC_MAX_QUADS 4194304
-int lag2d_delt_noalloc(int ntria, int nquad, int npoin, int ndegr, int nq, int ngeel,
-                       const int *ipqua, const double *unkno, const double *geoel,
+int lag2d_delt_noalloc(int ntria, int nquad, int npoin, int nvqua, int ncurv, int ndegr, int nq,
+                       int ngeel, const int *ipqua, const double *unkno, const double *geoel,
                        const double *coord, const double *dvdt, int itime, int ndens,
                        double gamlg, double cfl, double *dtfix, void *stream);
 

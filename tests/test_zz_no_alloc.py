@@ -7,7 +7,8 @@ limited stage state and dvdt = rhsel(1,1,:) exactly as the step computes
 them; lag2d_delt_noalloc on caller-owned device copies of those arrays must
 give the dtfix lag2d_step returns (bit for bit in the no-FMA build, within
 1e-14 relative in the FMA build, where the compiler may contract the two
-kernels' arithmetic differently).
+kernels' arithmetic differently).  Curved 9-node quads (ncurv = 1) and the
+straight 4-node quads of the linear P1 path (ncurv = 0) are both covered.
 """
 import ctypes
 
@@ -26,19 +27,28 @@ MAX_QUADS = 4194304   # LAG2D_DELT_NOALLOC_MAX_QUADS
 def _noalloc(lib):
     f = lib.lag2d_delt_noalloc
     f.restype = ctypes.c_int
-    f.argtypes = [ctypes.c_int] * 6 + [ctypes.c_void_p] * 5 + [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+    f.argtypes = [ctypes.c_int] * 8 + [ctypes.c_void_p] * 5 + [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                                 ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
     return f
 
 
+def _layout(m):
+    """(nvqua, ncurv) of the mesh: 9-node curved quads or 4-node straight ones."""
+    nvqua = m.ipqua.shape[1]
+    return nvqua, (0 if nvqua == 4 else 1)
+
+
 def _call(f, m, c, dev, itime, dtfix_d):
-    return f(m.ntria, m.nquad, m.npoin, c.ndegr, c.nq, 24, dev["ipqua"].data_ptr(), dev["unkno"].data_ptr(),
+    nvqua, ncurv = _layout(m)
+    ngeel = dev["geoel"].shape[1]
+    return f(m.ntria, m.nquad, m.npoin, nvqua, ncurv, c.ndegr, c.nq, ngeel, dev["ipqua"].data_ptr(),
+             dev["unkno"].data_ptr(),
              dev["geoel"].data_ptr(), dev["coord"].data_ptr(), dev["dvdt"].data_ptr(), itime, c.ndens,
              c.gamlg, c.cfl, dtfix_d.data_ptr(), None)
 
 
 @pytest.mark.parametrize("exact", [True, False])
-@pytest.mark.parametrize("name", ["tgv16", "sedov16"])
+@pytest.mark.parametrize("name", ["tgv16", "sedov16", "sod_jitter40"])
 def test_delt_noalloc_matches_step(name, exact):
     torch = pytest.importorskip("torch")
     m, c = workload(name)
@@ -82,7 +92,7 @@ def test_delt_noalloc_rejects_oversize():
     lib = _api.load(False)
     f = _noalloc(lib)
     d = torch.zeros(1, dtype=torch.float64, device="cuda")
-    rc = f(0, MAX_QUADS + 1, 9, 6, 4, 24, d.data_ptr(), d.data_ptr(), d.data_ptr(), d.data_ptr(), d.data_ptr(),
+    rc = f(0, MAX_QUADS + 1, 9, 9, 1, 6, 4, 24, d.data_ptr(), d.data_ptr(), d.data_ptr(), d.data_ptr(), d.data_ptr(),
            1, 1, 1.4, 0.1, d.data_ptr(), None)
     assert rc == 1
     assert b"LAG2D_DELT_NOALLOC_MAX_QUADS" in lib.lag2d_last_error()
@@ -94,7 +104,52 @@ def test_delt_noalloc_empty_mesh():
     lib = _api.load(False)
     f = _noalloc(lib)
     d = torch.full((1,), 5.0, dtype=torch.float64, device="cuda")
-    rc = f(0, 0, 0, 6, 4, 24, None, None, None, None, None, 2, 1, 1.4, 0.1, d.data_ptr(), None)
+    rc = f(0, 0, 0, 9, 1, 6, 4, 24, None, None, None, None, None, 2, 1, 1.4, 0.1, d.data_ptr(), None)
     assert rc == 0, lib.lag2d_last_error()
     torch.cuda.synchronize()
     assert float(d.cpu()[0]) == min(0.1 * 1e10, 0.1 * 1e10, 1.01 * 5.0)
+
+
+@pytest.mark.parametrize("nvqua,ncurv", [(4, 1), (8, -1), (3, 0)])
+def test_delt_noalloc_rejects_layout(nvqua, ncurv):
+    """ipqua with fewer entries per quad than the edge rule of ncurv reads
+    (4 for straight edges, 8 for curved ones), or a negative ncurv, is
+    rejected before any device work."""
+    torch = pytest.importorskip("torch")
+    lib = _api.load(False)
+    f = _noalloc(lib)
+    d = torch.full((64,), 1.0, dtype=torch.float64, device="cuda")
+    rc = f(0, 1, 9, nvqua, ncurv, 3, 4, 24, d.data_ptr(), d.data_ptr(), d.data_ptr(), d.data_ptr(), d.data_ptr(),
+           1, 1, 1.4, 0.1, d.data_ptr(), None)
+    assert rc == 1
+    assert b"ncurv" in lib.lag2d_last_error()
+
+
+@pytest.mark.parametrize("bad_id", [0, "npoin+1"])
+def test_delt_noalloc_bad_node_id_gives_nan(bad_id):
+    """A node id outside 1..npoin in ipqua is not dereferenced: the call
+    succeeds and dtfix comes back NaN (followed by a call on the intact mesh,
+    so the scratch left by the first call does not leak into the second)."""
+    torch = pytest.importorskip("torch")
+    m, c = workload("tgv16")
+    s = Lag2DSolver(m, c)
+    f = _noalloc(s.lib)
+    s.init_fields()
+    geoel = s.get_state()[3]
+    rhsel, _ = s.rhs(itime=1)
+    ulim, coord = s.get_state()[:2]
+    s.close()
+    ipq = np.ascontiguousarray(m.ipqua, dtype=np.int32).copy()
+    ipq[m.nquad // 2, 4] = 0 if bad_id == 0 else m.npoin + 1
+    good = {"ipqua": torch.from_numpy(np.ascontiguousarray(m.ipqua, dtype=np.int32)).cuda(),
+            "unkno": torch.from_numpy(ulim).cuda(), "geoel": torch.from_numpy(geoel).cuda(),
+            "coord": torch.from_numpy(coord).cuda(),
+            "dvdt": torch.from_numpy(np.ascontiguousarray(rhsel[:, 0, 0])).cuda()}
+    bad = dict(good, ipqua=torch.from_numpy(ipq).cuda())
+    for dev, expect_nan in ((bad, True), (good, False)):
+        dt_d = torch.tensor([c.dtfix], dtype=torch.float64, device="cuda")
+        rc = _call(f, m, c, dev, 1, dt_d)
+        assert rc == 0, s.lib.lag2d_last_error()
+        torch.cuda.synchronize()
+        got = float(dt_d.cpu()[0])
+        assert np.isnan(got) == expect_nan, got
