@@ -55,6 +55,25 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+def host_info():
+    """CPU model (as lscpu reports it, from /proc/cpuinfo) and the number of
+    host threads the process may use."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    return {"cpu_model": model, "nproc": n}
+
+
 def config_block(name, mesh, cfg, n):
     out = {"workload": name, "cells": mesh.ncell, "triangles": mesh.ntria, "nodes": mesh.npoin,
            "basis": "P2 Taylor (ndegr=6, nq=4)", "rk_stages": cfg.nstag, "limiter": "Persson + WENO",
@@ -63,6 +82,7 @@ def config_block(name, mesh, cfg, n):
                   else "working set within the 126 MB L2 (small configuration)")}
     if cfg.ndt == 0:
         out["dt"] = f"fixed {cfg.dtfix:g}"
+    out["host"] = host_info()
     return out
 
 
@@ -124,7 +144,8 @@ def cpu_baseline(seconds: float):
     value = ncell * 24 * nstag * nsteps / total
     return {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{CPU_SAMPLE}: Taylor-Green 64x64 P2 quads (same step: Persson+WENO, RK3), "
-                      f"{nsteps} steps, {total:.1f} s, oracle C restatement -O2 single thread"}
+                      f"{nsteps} steps, {total:.1f} s, oracle C restatement -O2 single thread",
+            "host": host_info()}
 
 
 def run_reference(args):
@@ -134,7 +155,7 @@ def run_reference(args):
     import multiprocessing as mp
     from lag2d_b200.config import workload
     m, c = workload(args.workload)
-    nproc = os.cpu_count() or 1
+    nproc = host_info()["nproc"]
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(nproc) as pool:
@@ -147,10 +168,15 @@ def run_reference(args):
     sample = (f"{CPU_SAMPLE}: Taylor-Green 64x64 P2 quads per process, {nproc} processes x {args.steps} timed "
               f"steps (after {args.warmup} warm-up), oracle C restatement of the reference step "
               f"(the Fortran reference cannot be compiled here), wall {wall:.1f} s")
+    cfgb = config_block(args.workload, m, c, args.gpus)
+    # the metric is per-cell work, so the 1024^2 rate is sampled on independent
+    # 64^2 problems, one per host thread (a whole 1024^2 step takes ~55 s on one thread)
+    cfgb["cpu_sample"] = (f"{CPU_SAMPLE} (64x64 P2 quads, same step) x {nproc} independent processes, "
+                          f"DOF-updates/s summed over processes")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference", "config": config_block(args.workload, m, c, args.gpus),
+            "impl": "reference", "config": cfgb,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -197,6 +223,34 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def fp64_peak():
+    """Measured FP64 FMA throughput of this GPU (TFLOP/s, best of 3 launches of
+    independent FMA chains on every SM, CUDA events); None if the measurement
+    library is missing."""
+    import ctypes
+    lib_path = os.path.join(ROOT, "lag2d_b200", "_lib", "liblag2d_bench.so")
+    if not os.path.exists(lib_path):
+        return None
+    lib = ctypes.CDLL(lib_path)
+    lib.lag2d_bench_dfma_tflops.restype = ctypes.c_double
+    lib.lag2d_bench_dfma_tflops.argtypes = [ctypes.c_int, ctypes.c_int]
+    tf = lib.lag2d_bench_dfma_tflops(200000, 3)
+    return tf if tf > 0 else None
+
+
+def measured_flops(family, ncell):
+    """FP64 FLOPs per launch of a kernel family (2 per DFMA, 1 per DMUL/DADD,
+    from ncu's executed-instruction counters of a capture, per cell in
+    profiles/flops.json), scaled to this workload's cells; None when no
+    capture is recorded."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "flops.json")) as f:
+            t = json.load(f)
+        return t[family]["fp64_flops_per_cell"] * ncell
+    except Exception:
+        return None
 
 
 def measured_traffic(family, ncell):
@@ -391,9 +445,31 @@ def run_ours(args):
         s.step()
         s.get_state_ptrs(u_h.data_ptr(), x_h.data_ptr(), us_h.data_ptr())
     te = max_over_ranks(time.perf_counter() - t0)
+    # the link these copies run on: one pinned copy of the same bytes each way,
+    # CUDA events (a bound for the end-to-end step: step time + both copies)
+    dev_buf = torch.empty(h2d // 8, dtype=torch.float64, device="cuda")
+    host_buf = torch.empty(h2d // 8, dtype=torch.float64, pin_memory=True)
+    link = {}
+    for name, (dst, src) in (("h2d", (dev_buf, host_buf)), ("d2h", (host_buf, dev_buf))):
+        best = None
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            dst.copy_(src, non_blocking=True)
+            b.record()
+            b.synchronize()
+            ms_c = a.elapsed_time(b)
+            best = ms_c if best is None else min(best, ms_c)
+        link[name] = {"ms": best, "gbs": h2d / (best / 1e3) / 1e9}
+    del dev_buf, host_buf
+    bound_ms = ms_per_step + link["h2d"]["ms"] + link["d2h"]["ms"]
     e2e = {"value": aggregate_rate(dof_stage * c.nstag * args.e2e_steps, te, world), "unit": UNIT,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "api": "lag2d_set_state + lag2d_step + lag2d_get_state (pinned host, Fortran layout)"}
+           "ms_per_step": 1e3 * te / args.e2e_steps,
+           "api": "lag2d_set_state + lag2d_step + lag2d_get_state (pinned host, Fortran layout)",
+           "link": link,
+           "bound": {"ms_per_step": bound_ms, "value": dof_stage * c.nstag / (bound_ms / 1e3),
+                     "note": "device step + one pinned copy of the step's state each way (measured above)"}}
 
     # ---- adjoint: reverse sweep per step against the forward step time, FP64
     # and FP32-mixed from the same state (the FP64 solver's current one)
@@ -417,7 +493,20 @@ def run_ours(args):
     # 200 x 10 configuration and a 1024 x 512 one, FP64, graph-replayed steps
     p1 = None if args.no_p1 else p1_block(args, timed, families)
 
+    # ---- FP64 pipe: measured DFMA peak and each pass's FP64 FLOP rate
+    tf_peak = fp64_peak() if rank == 0 else None
+    fp64 = {"peak_tflops": tf_peak, "peak_kind": "measured (DFMA chains on every SM, CUDA events)",
+            "per_kernel": {}}
+    for f, v in fams.items():
+        fl = measured_flops(f, m.ncell)
+        if fl is None:
+            continue
+        tf = fl / (v["ms_per_launch"] / 1e3) / 1e12
+        fp64["per_kernel"][f] = {"flops_per_launch": fl, "achieved_tflops": tf,
+                                 "frac": (tf / tf_peak) if tf_peak else None}
+
     if rank == 0:
+        # short summaries first: the line is long and readers may only see its head
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seedless structured mesh, analytic IC)",
@@ -426,14 +515,19 @@ def run_ours(args):
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                              "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                              "bytes_per_launch": kb},
-                "stage_roofline": {"bytes_per_stage": sb, "achieved_gbs": stage_gbs, "peak": peak,
-                                   "frac": stage_gbs / peak, "roofline_dof_updates_per_s": dof_stage / (sb / (peak * 1e9))},
-                "kernels_ms_per_step": per_step, "fp32_mixed": mixed,
-                "adjoint_forward_ratio": adjoint.get("ratio"), "adjoint": adjoint}
-        if p1 is not None:
-            line["p1_sod"] = p1
+                "fp32_mixed_summary": {"value": value_mx, "ms_per_step": mixed["ms_per_step"],
+                                       "speedup_vs_fp64": mixed["speedup_vs_fp64"],
+                                       "max_cell_avg_err_vs_fp64": max(mixed["cell_avg_err_vs_fp64"].values())},
+                "adjoint_forward_ratio": adjoint.get("ratio"),
+                "adjoint_forward_ratio_fp32_mixed": adjoint.get("fp32_mixed", {}).get("ratio")}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        line.update({
+            "stage_roofline": {"bytes_per_stage": sb, "achieved_gbs": stage_gbs, "peak": peak,
+                               "frac": stage_gbs / peak, "roofline_dof_updates_per_s": dof_stage / (sb / (peak * 1e9))},
+            "fp64_pipe": fp64, "kernels_ms_per_step": per_step, "fp32_mixed": mixed, "adjoint": adjoint})
+        if p1 is not None:
+            line["p1_sod"] = p1
         print(json.dumps(line), flush=True)
     s.close()
     if dist:

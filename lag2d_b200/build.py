@@ -31,6 +31,22 @@ def targets():
     return {"liblag2d.so": True, "liblag2d_exact.so": False}
 
 
+# measurement aid for bench.py (FP64 FMA peak), not part of the time-step API
+BENCH_SRC = os.path.join(HERE, "csrc", "lag2d_peak.cu")
+BENCH_LIB = os.path.join(OUT_DIR, "liblag2d_bench.so")
+
+
+def _build_bench(verbose: bool, force: bool) -> str:
+    if not force and os.path.exists(BENCH_LIB) and os.path.getmtime(BENCH_LIB) >= os.path.getmtime(BENCH_SRC):
+        return BENCH_LIB
+    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC", "-cudart", "static",
+           "-o", BENCH_LIB, BENCH_SRC]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return BENCH_LIB
+
+
 def build(verbose: bool = False, force: bool = False) -> list:
     os.makedirs(OUT_DIR, exist_ok=True)
     built = []
@@ -48,6 +64,7 @@ def build(verbose: bool = False, force: bool = False) -> list:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         built.append(out)
+    built.append(_build_bench(verbose, force))
     return built
 
 
