@@ -9,18 +9,24 @@ averages (the shock position), for Taylor-Green the L2 errors.
     python -m lag2d_b200.run_case sod1024 --steps 100
 
 The loop is lag2d_run in chunks (dgflo2d.f90:358-472 on the device, exit
-test at t_end included).
+test at t_end included).  Two modes for profilers (ncu) replace the chunked
+loop, so that every kernel launch of a step is visible in launch order:
+
+    python -m lag2d_b200.run_case tgv256 --steps 2 --per-step          # one lag2d_step per step, no graph
+    python -m lag2d_b200.run_case tgv256 --steps 2 --per-step --mixed  # the FP32-mixed step
+    python -m lag2d_b200.run_case tgv256 --steps 2 --adjoint 1         # lag2d_adjoint over 2 steps, K = 1
 """
 from __future__ import annotations
 
 import argparse
 import ctypes
+import dataclasses
 import time
 
 import numpy as np
 
 from .api import Lag2DError, Lag2DSolver
-from .config import workload
+from .config import initial_density_factors, workload
 
 LAG2D_ESTENCIL = 5
 
@@ -45,10 +51,32 @@ def main():
     ap.add_argument("--steps", type=int, default=0, help="stop after this many steps (0: run to t_end)")
     ap.add_argument("--chunk", type=int, default=500)
     ap.add_argument("--mixed", action="store_true", help="FP32-mixed form (precision = 1)")
+    ap.add_argument("--cfl", type=float, default=0.0, help="override the workload's CFL number")
+    ap.add_argument("--rho0", action="store_true",
+                    help="per-cell initial densities 1 + 0.01 N(0, 1) (seed 5678) before the initial fields")
+    ap.add_argument("--per-step", action="store_true",
+                    help="one lag2d_step call per step (no graph), for profilers; prints one line")
+    ap.add_argument("--adjoint", type=int, default=0, metavar="K",
+                    help="run lag2d_adjoint over --steps steps with checkpoints every K steps; prints one line")
     a = ap.parse_args()
     m, c = workload(a.workload)
+    if a.cfl > 0:
+        c = dataclasses.replace(c, cfl=a.cfl)
     s = Lag2DSolver(m, c, precision=1 if a.mixed else 0)
+    if a.rho0:
+        s.set_rho0(initial_density_factors(m))
     geoel, _, unkno = s.init_fields()
+    if a.per_step or a.adjoint > 0:
+        nsteps = max(a.steps, 1)
+        if a.adjoint > 0:
+            J, _, _, _, ms = s.adjoint(nsteps, a.adjoint)
+            print(f"adjoint J={J:.12e} forward/recompute/reverse ms = {ms[0]:.3f} {ms[1]:.3f} {ms[2]:.3f}")
+        else:
+            for _ in range(nsteps):
+                s.step()
+        print(f"ok {a.workload} steps={nsteps} mixed={a.mixed} dtfix={s.dtfix:.6e} tacru={s.tacru:.6e}")
+        s.close()
+        return
     n = m.ncell
     mass = geoel[:n, 3].copy()
     e0 = float((mass * unkno[:n, 3, 0]).sum())

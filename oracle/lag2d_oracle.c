@@ -34,6 +34,15 @@ static const double PI_ = 3.14159265358979311599796346854;  /* 4*atan(1) */
  * stencil search rejects with `stop` (WENO.f90:7699); the cell is skipped. */
 static int g_status = 0;
 int o_status(void) { int s = g_status; g_status = 0; return s; }
+/* test bookkeeping (not part of the reference): Persson marks and WENO
+ * replacements counted since the last o_counts call */
+static long long g_marked = 0, g_replaced = 0;
+void o_counts(long long *marked, long long *replaced) {
+  if (marked) *marked = g_marked;
+  if (replaced) *replaced = g_replaced;
+  g_marked = 0;
+  g_replaced = 0;
+}
 
 /* ---------------------------------------------------------------------- */
 /* Quadrature rules: dgflo2d.f90:2497-2783 (2-D tensor rules).            */
@@ -635,6 +644,7 @@ static void persson(const o_mesh *m, const o_cfg *c, const double *coord,
       }
     }
     G_(geoel, 9, ielem) = (log10(unvar2[0] / unvar1[0]) <= thr) ? 0.0 : 100.0;
+    if (G_(geoel, 9, ielem) >= 10) g_marked++;
   }
 }
 
@@ -1073,6 +1083,7 @@ static void weno_stencil(const weno_ctx *w, int ielem, const double *mapmt, doub
   for (int d = 1; d < 6; d++) vec_local_back(mapmt, &out[1][d], &out[2][d]);
   for (int q = 0; q < 4; q++)
     for (int d = 1; d < 6; d++) U_(unkno, c, d, q, ielem) = out[q][d];
+  g_replaced++;
 }
 
 /* weno_char_quad_orthgl, WENO.f90:5927-6123 */

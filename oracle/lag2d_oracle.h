@@ -69,6 +69,11 @@ void o_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
            double *rhsel, double *geoel, const double *coord,
            const double *coold, const double *amatr, int itime, int *flags);
 
+/* Test bookkeeping (no counterpart in the reference): the number of quads
+ * Persson marked troubled and of quads whose DOFs WENO replaced since the
+ * previous call; resets both. */
+void o_counts(long long *marked, long long *replaced);
+
 /* weno_char_quad_orthgl on the cells with flags[ie] != 0. */
 void o_weno(const o_mesh *m, const o_cfg *c, double *unkno, double *geoel,
             const double *coord, const double *coold, const int *flags);

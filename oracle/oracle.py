@@ -127,6 +127,14 @@ class Oracle:
     def status() -> int:
         return int(lib().o_status())
 
+    @staticmethod
+    def counts():
+        """(Persson-marked quads, WENO-replaced quads) summed over every stage
+        since the previous call; resets both."""
+        a, b = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        lib().o_counts(ctypes.byref(a), ctypes.byref(b))
+        return int(a.value), int(b.value)
+
     def delt(self, unkno, geoel, coord, dvdt, itime, dtfix):
         return lib().o_delt(ctypes.byref(self.om), ctypes.byref(self.oc), _p(unkno, _dp), _p(geoel, _dp),
                             _p(coord, _dp), _p(dvdt, _dp), ctypes.c_int(itime), ctypes.c_double(dtfix))

@@ -1,0 +1,124 @@
+"""Parity at the sizes of the benchmark configurations, through the C-ABI.
+
+The production path (optimised kernels, FMA contraction) and the FP32-mixed
+path are stepped from the oracle's own initial arrays and compared with the
+oracle after every step:
+
+  * tgv256      Taylor-Green 256x256 curved P2 quads, 10 steps (CFL dt)
+  * tgv1024     Taylor-Green 1024x1024 (the benchmark mesh), 1 step
+  * sedov128    Sedov 128x128, 50 steps, WENO replacing cells every stage
+  * noh100      Noh on the quarter disk 100x100 (triangles at the origin),
+                10 steps at the fixed dt of the parity configuration
+  * sedov_hybrid_jitter256   Sedov on the jittered 256x256 tri/quad mesh with
+                per-cell initial densities 1 + 0.01 N(0,1), 1 step
+
+Bounds: FP64 cell averages within 1e-12 relative of the oracle (relative to
+the field scale where a field crosses zero), dt within 1e-12, node positions
+within 1e-13 absolute; FP32-mixed cell averages within 1e-6, dt within 1e-6,
+node displacements within 1e-6 of the oracle's.  Where the configuration
+exercises them, the oracle's own counts show that Persson marked quads and
+WENO replaced them inside the compared window.
+"""
+import functools
+
+import numpy as np
+import pytest
+
+from lag2d_b200 import workload
+from lag2d_b200.api import Lag2DSolver
+from lag2d_b200.config import initial_density_factors, noh_parity_config
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-6
+
+# name: (steps, fixed-dt parity config, per-cell initial densities,
+#        least Persson marks, least WENO replacements over the window)
+CASES = {
+    "tgv256": (10, False, False, 0, 0),
+    "tgv1024": (1, False, False, 0, 0),
+    "sedov128": (50, False, False, 1000, 1000),
+    "noh100": (10, True, False, 1000, 500),
+    "sedov_hybrid_jitter256": (1, False, True, 1, 0),
+}
+
+
+def _avg_err(u, ref):
+    """Per field: |u - ref| relative to the value, or to the field scale where
+    that is smaller (fields that cross zero)."""
+    d = np.abs(u - ref)
+    rel = d / np.maximum(np.abs(ref), 1e-300)
+    scl = d / np.maximum(np.abs(ref).max(axis=0), 1e-300)
+    return np.minimum(rel, scl).max(axis=0)
+
+
+@functools.lru_cache(maxsize=None)
+def _oracle_run(name):
+    """The oracle's run of a case: its mesh, configuration, initial arrays and
+    per step (dtfix, cell averages (ncell, 4), node positions), with the
+    Persson marks and WENO replacements counted over the window."""
+    nsteps, fixed_dt, dens, _, _ = CASES[name]
+    m, c = workload(name)
+    if fixed_dt:
+        c = noh_parity_config(c)
+    rho0 = initial_density_factors(m) if dens else None
+    o = Oracle(m, c, rho0=rho0)
+    geoel, amatr, unkno = o.init()
+    init = (geoel.copy(), amatr.copy(), unkno.copy())
+    coord = m.coord.copy()
+    ustar = np.zeros_like(coord)
+    dt, ta = c.dtfix, 0.0
+    Oracle.counts()
+    traj = []
+    for it in range(1, nsteps + 1):
+        _, dt, ta = o.run(unkno, coord, m.coord, geoel, amatr, ustar, it, 1, dt, ta)
+        traj.append((dt, unkno[:m.ncell, :, 0].copy(), coord.copy()))
+    counts = Oracle.counts()
+    return m, c, rho0, init, tuple(traj), counts
+
+
+def _gpu_solver(name, precision):
+    m, c, rho0, (geoel, amatr, unkno), traj, counts = _oracle_run(name)
+    s = Lag2DSolver(m, c, precision=precision)
+    if rho0 is not None:
+        s.set_rho0(rho0)
+    s.init_fields()
+    s.set_state(unkno, m.coord, np.zeros_like(m.coord), geoel, amatr)
+    return m, c, s, traj, counts
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_production_parity_large(name):
+    m, c, s, traj, (marked, replaced) = _gpu_solver(name, 0)
+    _, _, _, need_marked, need_replaced = CASES[name]
+    assert marked >= need_marked and replaced >= need_replaced, (marked, replaced)
+    n = m.ncell
+    for it, (dt, avg, coord) in enumerate(traj, 1):
+        dt2, _ = s.step()
+        assert abs(dt2 - dt) <= FP64_TOL * dt, (it, dt2, dt)
+        u2, x2, _, _ = s.get_state()
+        err = _avg_err(u2[:n, :, 0], avg)
+        assert err.max() < FP64_TOL, (it, err)
+        assert np.abs(x2 - coord).max() < 1e-13, (it, np.abs(x2 - coord).max())
+    s.close()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_mixed_parity_large(name):
+    m, c, s, traj, _ = _gpu_solver(name, 1)
+    n = m.ncell
+    worst = np.zeros(4)
+    for it, (dt, avg, coord) in enumerate(traj, 1):
+        dt2, _ = s.step()
+        assert abs(dt2 - dt) <= MIXED_TOL * dt, (it, dt2, dt)
+        u2, x2, _, _ = s.get_state()
+        err = _avg_err(u2[:n, :, 0], avg)
+        worst = np.maximum(worst, err)
+        assert err.max() < MIXED_TOL, (it, err)
+        disp = np.abs(coord - m.coord).max()
+        assert np.abs(x2 - coord).max() <= MIXED_TOL * disp, (it, np.abs(x2 - coord).max(), disp)
+    # the mixed form is not the FP64 one: its error sits well above FP64 rounding
+    assert worst.max() > 1e-13
+    s.close()
