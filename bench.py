@@ -396,7 +396,7 @@ def run_ours(args):
     fams_mx = families(sm)
     per_step = {f: v["ms_per_launch"] * v["launches"] / 2 for f, v in fams.items()}
     per_step_mx = {f: v["ms_per_launch"] * v["launches"] / 2 for f, v in fams_mx.items()}
-    dom = max((f for f in per_step if f in ("corner", "node", "rhs", "update", "persson", "nodes", "geom")),
+    dom = max((f for f in per_step if f in ("corner", "node", "rhs", "dt", "persson", "nodes", "geom")),
               key=lambda f: per_step[f])
     peak, peak_kind = peaks()
     kb = kernel_bytes(dom, m.ncell, m.npoin, c.nstag)

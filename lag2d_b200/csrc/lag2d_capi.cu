@@ -45,7 +45,7 @@ void launch_fast_persson(const Dev &d, cudaStream_t st);
 void launch_fast_corner(const Dev &d, cudaStream_t st);
 void launch_fast_node(const Dev &d, cudaStream_t st);
 void launch_fast_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa);
-void launch_fast_update(const Dev &d, cudaStream_t st, double alfa);
+void launch_fast_dt(const Dev &d, cudaStream_t st, int ndt);
 void launch_mixed_corner(const Dev &d, cudaStream_t st);
 void launch_mixed_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa);
 void launch_fast_nodes(const Dev &d, cudaStream_t st, double alfa);
@@ -96,7 +96,8 @@ struct lag2d_handle {
   int *flags_dev = nullptr;
   double *rho0_dev = nullptr;  // per-cell initial-density factors (lag2d_set_rho0)
   double *stage_u = nullptr;   // staging for unkno(ndegr,nq,ncell) in the caller's layout
-  double *stage_x = nullptr;   // staging for coord / ustar (2,npoin)
+  double *stage_x = nullptr;   // staging for coord(2,npoin)
+  double *stage_v = nullptr;   // staging for ustar(2,npoin) (its own, so no copy waits for another)
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0;
   long long launches = 0;
@@ -305,10 +306,10 @@ static void corner_pass(lag2d_handle *h, const Dev &d) {
   if (h->cfg.precision == 1) launch_mixed_corner(d, h->st);
   else launch_fast_corner(d, h->st);
 }
-// launches of rhs_pass: the triangles' kernel, then one (FP32-mixed) or two
-// (FP64: face integral, rest) quad kernels
+// launches of rhs_pass: the triangles' kernel, then one quad kernel
 static int rhs_launches(const lag2d_handle *h, const Dev &d) {
-  return (d.ntria > 0) + (h->cfg.precision == 1 ? 1 : 2);
+  (void)h;
+  return (d.ntria > 0) + 1;
 }
 
 static void rhs_pass(lag2d_handle *h, const Dev &d, int fuse, double alfa) {
@@ -390,14 +391,14 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
     run(h, "corner", [&] { corner_pass(h, d); }, corner_launches(h, d));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
-      run(h, "rhs", [&] { rhs_pass(h, d, 0, alfa); }, rhs_launches(h, d));
-      run(h, "dt", [&] { launch_dt(d, h->st, h->cfg.ndt); }, 2);
+      // getdelt_lag needs only the cell-average mass flux of this stage's
+      // RHS, which the node velocities give: dt first, then every stage's
+      // RHS pass carries its own update
+      run(h, "dt", [&] { launch_fast_dt(d, h->st, h->cfg.ndt); }, 2);
       if (rec)
         cudaMemcpyAsync(rec->dt + rec->step, &d.sc_dev->dtfix, sizeof(double), cudaMemcpyDeviceToDevice, h->st);
-      run(h, "update", [&] { launch_fast_update(d, h->st, alfa); });
-    } else {
-      run(h, "rhs", [&] { rhs_pass(h, d, 1, alfa); }, rhs_launches(h, d));
     }
+    run(h, "rhs", [&] { rhs_pass(h, d, 1, alfa); }, rhs_launches(h, d));
     run(h, "nodes", [&] { launch_fast_nodes(d, h->st, alfa); });
     run(h, "geom", [&] { launch_tri_geom(d, h->st, d.xs, d.ys); launch_fast_geom(d, h->st, 1); }, 1 + T);
   }
@@ -601,7 +602,7 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   A(&d.flag, ncell); A(&d.geoph, 2 * (size_t)ncell); A(&d.mapmt, 4 * (size_t)ncell);
   A(&d.Uw, 20 * (size_t)nq); A(&d.wlist, nq); A(&d.wcount, 1);
   A(&d.dtpart, 2 * (size_t)dt_blocks(d) + 2); A(&d.sc_dev, 1); A(&h->flags_dev, ncell);
-  A(&h->stage_u, NU * (size_t)ncell); A(&h->stage_x, 2 * (size_t)np);
+  A(&h->stage_u, NU * (size_t)ncell); A(&h->stage_x, 2 * (size_t)np); A(&h->stage_v, 2 * (size_t)np);
   int *ptr2_d, *slot_d;
   A(&ptr2_d, cnt2.size()); A(&slot_d, slots.size());
   A(&d.npart, 45 * (size_t)nq); A(&d.corr, 4 * (size_t)nq); A(&d.us_new, np); A(&d.vs_new, np);
@@ -668,14 +669,6 @@ static int download_unkno(lag2d_handle *h, double *unkno) {
   return LAG2D_OK;
 }
 
-static int download_xy(lag2d_handle *h, const double *X, const double *Y, double *xy) {
-  const int np = h->d.npoin;
-  launch_xy_out(np, h->st, h->stage_x, X, Y);
-  h->launches += 1;
-  CK(cudaMemcpyAsync(xy, h->stage_x, 2 * (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
-  CK(cudaStreamSynchronize(h->st));
-  return LAG2D_OK;
-}
 
 int lag2d_set_rho0(lag2d_handle *h, const double *rho0) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
@@ -738,30 +731,32 @@ int lag2d_set_state(lag2d_handle *h, const double *unkno, const double *coord, c
   const int ncell = d.ncell, np = d.npoin;
   // straight copies of the caller's buffers (pinned buffers go at full link
   // speed), then layout conversion on the device
+  // the three copies go back to back (each into its own staging buffer), the
+  // layout conversions queue behind them on the same stream
   CK(cudaMemcpyAsync(h->stage_u, unkno, NU * (size_t)ncell * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  launch_unkno_in(d, h->st, h->stage_u, 1);
   CK(cudaMemcpyAsync(h->stage_x, coord, 2 * (size_t)np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->stage_v, ustar, 2 * (size_t)np * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  launch_unkno_in(d, h->st, h->stage_u, 1);
   launch_xy_in(np, h->st, h->stage_x, d.xn, d.yn, d.xs, d.ys);
-  CK(cudaStreamSynchronize(h->st));
-  CK(cudaMemcpyAsync(h->stage_x, ustar, 2 * (size_t)np * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  launch_xy_in(np, h->st, h->stage_x, d.us, d.vs, nullptr, nullptr);
+  launch_xy_in(np, h->st, h->stage_v, d.us, d.vs, nullptr, nullptr);
   h->launches += 3;
+  // host-side repacks of geoel / amatr live until the stream sync below
+  std::vector<double> gslab, aslab;
   if (geoel) {
-    std::vector<double> g(ncell);
     double *dst[7] = {d.rc, d.sc, d.vol, d.mass, d.g19, d.g20, d.g21};
     const int slot[7] = {0, 1, 2, 3, 18, 19, 20};
+    gslab.resize(7 * (size_t)ncell);
     for (int k = 0; k < 7; k++) {
+      double *g = gslab.data() + k * (size_t)ncell;
       for (int e = 0; e < ncell; e++) g[e] = geoel[24 * (size_t)e + slot[k]];
-      CK(cudaMemcpyAsync(dst[k], g.data(), ncell * sizeof(double), cudaMemcpyHostToDevice, h->st));
-      CK(cudaStreamSynchronize(h->st));
+      CK(cudaMemcpyAsync(dst[k], g, ncell * sizeof(double), cudaMemcpyHostToDevice, h->st));
     }
   }
   if (amatr) {
-    std::vector<double> g(16 * (size_t)ncell);
+    aslab.resize(16 * (size_t)ncell);
     for (int e = 0; e < ncell; e++)
-      for (int k = 0; k < 16; k++) g[k * (size_t)ncell + e] = amatr[16 * (size_t)e + k];
-    CK(cudaMemcpyAsync(d.amatr, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    CK(cudaStreamSynchronize(h->st));
+      for (int k = 0; k < 16; k++) aslab[k * (size_t)ncell + e] = amatr[16 * (size_t)e + k];
+    CK(cudaMemcpyAsync(d.amatr, aslab.data(), aslab.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
   }
   Scalars s0{};
   CK(cudaMemcpyAsync(d.sc_dev, &s0, sizeof(Scalars), cudaMemcpyHostToDevice, h->st));
@@ -841,10 +836,21 @@ int lag2d_run(lag2d_handle *h, int itime0, int nsteps, double *dtfix, double *ta
 int lag2d_get_state(lag2d_handle *h, double *unkno, double *coord, double *ustar, double *geoel) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
   if (h->p1) P1_CALL(p1::get_state(h->p1, unkno, coord, ustar, geoel, err_));
+  // layout conversions into the staging buffers first, then the copies back to
+  // back, then one synchronisation
+  const Dev &d = h->d;
+  const int np = d.npoin;
+  const size_t nu = NU * (size_t)d.ncell;
+  if (unkno) launch_unkno_out(d, h->st, h->stage_u);
+  if (coord) launch_xy_out(np, h->st, h->stage_x, d.xn, d.yn);
+  if (ustar) launch_xy_out(np, h->st, h->stage_v, d.us, d.vs);
+  h->launches += (unkno != nullptr) + (coord != nullptr) + (ustar != nullptr);
+  if (unkno) CK(cudaMemcpyAsync(unkno, h->stage_u, nu * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  if (coord) CK(cudaMemcpyAsync(coord, h->stage_x, 2 * (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  if (ustar) CK(cudaMemcpyAsync(ustar, h->stage_v, 2 * (size_t)np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (unkno) std::fill(unkno + nu, unkno + NU * (size_t)(d.ncell + d.nbfac), 0.0);
   int r;
-  if (unkno && (r = download_unkno(h, unkno))) return r;
-  if (coord && (r = download_xy(h, h->d.xn, h->d.yn, coord))) return r;
-  if (ustar && (r = download_xy(h, h->d.us, h->d.vs, ustar))) return r;
   if (geoel && (r = download_geoel(h, geoel))) return r;
   return LAG2D_OK;
 }

@@ -59,14 +59,26 @@ __host__ __device__ __forceinline__ void dlag3(double r, double *l) {
   l[2] = r + 0.5;
 }
 
-// cos(pi d) and sin(pi d) for |d| <= 0.15 from their Taylor series in
-// t = pi d, to degree 14 and 13 (the first omitted terms are below 1e-17)
-__host__ __device__ __forceinline__ void cossin_pi_small(double d, double &c, double &s) {
+// cos(pi d) and sin(pi d) for small |d| from their Taylor series in t = pi d
+// with N terms each: cos to degree 2N-2, sin to degree 2N-1.  N = 7 covers
+// |d| <= 0.15, N = 4 covers |d| <= 0.00625 and N = 3 covers |d| <= 0.0009375,
+// each with the first omitted term below 1e-17 relative.  Coefficients are
+// (-1)^k / (2k)! and (-1)^k / (2k+1)!, evaluated by Horner's rule in t^2.
+template <int N>
+__host__ __device__ __forceinline__ void cossin_pi_series(double d, double &c, double &s) {
+  constexpr double kc[7] = {1.0, -1.0 / 2.0, 1.0 / 24.0, -1.0 / 720.0, 1.0 / 40320.0, -1.0 / 3628800.0,
+                            1.0 / 479001600.0};
+  constexpr double ks[7] = {1.0, -1.0 / 6.0, 1.0 / 120.0, -1.0 / 5040.0, 1.0 / 362880.0, -1.0 / 39916800.0,
+                            1.0 / 6227020800.0};
   const double t = 3.14159265358979311599796346854 * d, t2 = t * t;
-  c = 1.0 + t2 * (-1.0 / 2.0 + t2 * (1.0 / 24.0 + t2 * (-1.0 / 720.0 + t2 * (1.0 / 40320.0 + t2 * (-1.0 / 3628800.0 +
-      t2 * (1.0 / 479001600.0 - t2 * (1.0 / 87178291200.0)))))));
-  s = t * (1.0 + t2 * (-1.0 / 6.0 + t2 * (1.0 / 120.0 + t2 * (-1.0 / 5040.0 + t2 * (1.0 / 362880.0 + t2 * (-1.0 /
-      39916800.0 + t2 * (1.0 / 6227020800.0)))))));
+  double pc = kc[N - 1], ps = ks[N - 1];
+#pragma unroll
+  for (int k = N - 2; k >= 0; k--) {
+    pc = kc[k] + t2 * pc;
+    ps = ks[k] + t2 * ps;
+  }
+  c = pc;
+  s = t * ps;
 }
 
 __host__ __device__ __forceinline__ double deteval(const double *D, double r, double s) {
@@ -385,12 +397,18 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
     for (int isg = 0; isg < 4; isg++) corr[isg] = d.corr[isg * (size_t)d.nquad + iq];
   }
   if (PART != 2) subareas(c, vsub4);
+  // The harmonic mean sum masel = sum_g w_g det_g / tau_g is kept as one
+  // fraction num / den (a/b + c/d = (a d + c b) / (b d)): three multiply-adds
+  // per point and one division per sub-cell instead of one division per point.
+  // tau is scaled by the cell-average tau first (rtc), so that the product of
+  // the 25 scaled values stays near 1; masel = rtc num / den.
+  const double rtc = 1.0 / u[0][0];
 #pragma unroll
   for (int isg = 0; isg < (PART == 2 ? 0 : 4); isg++) {
     const double unksgq = (1.0 / vsub4[isg]) * d.msub[isg * (size_t)d.nquad + iq];
     const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
     const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
-    double masel = 0.0;
+    double num = 0.0, den = 1.0;
 #pragma unroll 1
     for (int i = 0; i < 5; i++) {
       const double r = (g5p(i) + ofr) / 2.0;
@@ -399,8 +417,9 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
 #pragma unroll
       for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
       const double dr = r - G.rc;
-      const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
-      const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
+      const double t0 = rtc * (u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 -
+                               u[0][5] * G.g21);
+      const double t1 = rtc * (u[0][2] + u[0][5] * dr), t2 = rtc * (0.5 * u[0][4]);
       const double wi = 0.25 * g5w(i);
 #pragma unroll
       for (int j = 0; j < 5; j++) {
@@ -408,12 +427,13 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
         const double ds = s - G.sc;
         const double tau = t0 + ds * (t1 + t2 * ds);
         const double det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
-        masel += (wi * g5w(j)) * det / tau;
+        num = num * tau + ((wi * g5w(j)) * det) * den;
+        den = den * tau;
       }
     }
     const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
-    const double uqsgc = volel / masel;
-    corr[isg] = d.cdrho * (unksgq - 1.0 / uqsgc);
+    // 1 / uqsgc = masel / volel with masel = rtc num / den
+    corr[isg] = d.cdrho * (unksgq - (rtc * num) / (den * volel));
     d.corr[isg * (size_t)d.nquad + iq] = corr[isg];
   }
   if (PART == 1) return;
@@ -510,12 +530,13 @@ __host__ __device__ void f_node(const Dev &d, int p) {
 // Taylor-Green source moments el[k] += sum_g src(x_g) b_k(g) detJ_g w_g over
 // the 5x5 Gauss points.  cos(pi x) at the points by angle addition from the
 // centre node x_c: cos(pi x) = cos(pi x_c) cos(pi d) - sin(pi x_c) sin(pi d),
-// d = x - x_c, with the series of cossin_pi_small when every node of the cell
-// lies within 0.09 of the centre node in x and y (the quadratic map then keeps
-// |d| <= 1.5625 * 0.09 < 0.15 at the Gauss points), so the point loop has no
-// branch; otherwise cospi at each point.  The basis sums are taken per row:
+// d = x - x_c, with the NSER-term series of cossin_pi_series when every node
+// of the cell lies within delta of the centre node in x and y (the quadratic
+// map then keeps |d| <= 1.5625 delta at the Gauss points): delta <= 0.09 for
+// 7 terms, 0.004 for 4, 0.0006 for 3; otherwise (NSER = 0) cospi at each
+// point.  The point loop has no branch.  The basis sums are taken per row:
 // b_k along a row is a polynomial in ds of degree <= 2.
-template <bool SMALL>
+template <int NSER>
 __host__ __device__ __forceinline__ void tgv_source_rows(const Loaded &L, const CellGeo &G, const double D[16],
                                                          double g, double el[6]) {
   const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
@@ -546,10 +567,10 @@ __host__ __device__ __forceinline__ void tgv_source_rows(const Loaded &L, const 
       const double dy = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
       const double djaco = wi * g5w(j) * (e[0] + s * (e[1] + s * (e[2] + s * e[3])));
       double cx, cy;
-      if (SMALL) {
+      if (NSER > 0) {
         double cdx, sdx, cdy, sdy;
-        cossin_pi_small(dx, cdx, sdx);
-        cossin_pi_small(dy, cdy, sdy);
+        cossin_pi_series<NSER>(dx, cdx, sdx);
+        cossin_pi_series<NSER>(dy, cdy, sdy);
         cx = cxc * cdx - sxc * sdx;
         cy = cyc * cdy - syc * sdy;
       } else {
@@ -581,82 +602,96 @@ __host__ __device__ __forceinline__ void tgv_source(const Loaded &L, const CellG
       mx = fmax(mx, fabs(L.X[a][b] - L.X[1][1]));
       my = fmax(my, fabs(L.Y[a][b] - L.Y[1][1]));
     }
-  if (mx <= 0.09 && my <= 0.09) tgv_source_rows<true>(L, G, D, g, el);
-  else tgv_source_rows<false>(L, G, D, g, el);
+  const double delta = fmax(mx, my);
+  if (delta <= 0.0006) tgv_source_rows<3>(L, G, D, g, el);
+  else if (delta <= 0.004) tgv_source_rows<4>(L, G, D, g, el);
+  else if (delta <= 0.09) tgv_source_rows<7>(L, G, D, g, el);
+  else tgv_source_rows<0>(L, G, D, g, el);
 }
 
-// The RHS pass runs as two kernels: PART 1, the face integral, written to
-// d.rhs; PART 2, the rest (volume integral, source, store or fused update)
-// on top of the face integral read back from d.rhs.  Each half needs fewer
-// registers than the whole, so both are compiled for 3 resident blocks of 128
-// per SM (168 registers): on the 1024x1024 Taylor-Green step the pair takes
-// 2.62 ms against 2.88 ms for the single kernel at 255 registers (2 blocks),
-// the round trip through d.rhs (384 B per cell) included.
-template <int PART>
-__host__ __device__ void f_rhs_t(const Dev &d, int iq, int fuse_update, double alfa) {
+// The momentum and energy face weights of rhsifacedg_lagsubgq2 are 1 on every
+// corner entry of the 8 boundary nodes of the quad and 0 on the 4 entries of
+// the centre node (Getrhslaggauss.f90:8580-8603), and the mass weights vanish
+// on the centre node's corner faces; the face integral below relies on both.
+constexpr FastTables kFastTablesC = LAG2D_FAST_TABLES;
+constexpr int node_wmom(int k) {
+  int ones = 0, zeros = 0;
+  for (int i = kFastTablesC.nc_start[k]; i < kFastTablesC.nc_start[k + 1]; i++) {
+    const double w = kFastTablesC.wmom[kFastTablesC.nc_entry[i]];
+    ones += w == 1.0;
+    zeros += w == 0.0;
+  }
+  return zeros == 0 ? 1 : (ones == 0 ? 0 : -1);
+}
+static_assert(node_wmom(0) == 1 && node_wmom(1) == 1 && node_wmom(2) == 1 && node_wmom(3) == 1 &&
+              node_wmom(4) == 1 && node_wmom(5) == 1 && node_wmom(6) == 1 && node_wmom(7) == 1 &&
+              node_wmom(8) == 0, "momentum face weights: 1 on the boundary nodes, 0 at the centre");
+constexpr bool centre_wmas_zero() {
+  for (int i = kFastTablesC.nc_start[8]; i < kFastTablesC.nc_start[9]; i++)
+    for (int f = 0; f < 2; f++)
+      if (kFastTablesC.wmas[2 * kFastTablesC.nc_entry[i] + f] != 0.0) return false;
+  return true;
+}
+static_assert(centre_wmas_zero(), "mass face weights vanish at the centre node");
+
+// Mass-flux weights of node k (0..7): t = sum over the node's outer corner
+// faces of 2 w_mass,f an_f, so that the node's mass flux is u* . t.
+__host__ __device__ __forceinline__ void mass_flux_weights(const Loaded &L, int k, double &tx, double &ty) {
+  tx = 0.0;
+  ty = 0.0;
+#pragma unroll
+  for (int i = nc_start(k); i < nc_start(k + 1); i++) {
+    const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      if (wmas(isg, ivsg, f) != 0.0) {
+        double ax, ay;
+        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
+        tx += ax * (2.0 * wmas(isg, ivsg, f));
+        ty += ay * (2.0 * wmas(isg, ivsg, f));
+      }
+    }
+  }
+}
+
+// RHS pass, one kernel per quad: face integral, volume integral, Taylor-Green
+// source, and either the RHS store or the M^-1 solve and RK combine.
+//
+// Face integral (rhsifacedg_lagsubgq2, Getrhslaggauss.f90:8501-8748).  At node
+// k the corner force of corner face f is F_f = sigma.n A w_f + m_f (u* - u_k),
+// with u* the node's new velocity and m_f, sigma.n A w_f, u_k what the corner
+// pass used (Getrhslaggauss.f90:10409-10867).  The momentum sum is therefore
+// affine in u*: sum_f F_f = (P3, P4) + u* P0 - (P1, P2), where P0..P4 are the
+// node partial sums the corner pass wrote (sum m, sum m u_k, sum m v_k, sum
+// sigma.n A w); the energy term is u* . sum_f F_f; the mass term is
+// u* . sum_f 2 w_mass,f an_f over the 16 outer corner faces.  So the corner
+// data are not recomputed here: 40 partials and the 8 boundary nodes'
+// velocities replace the 32 corner faces' vertex states, impedances and
+// forces (same sums up to rounding and summation order).
+__host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa) {
   if (iq >= d.nquad || d.sc_dev->done) return;
   const int e = iq + d.ntria;
-  const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
+  const double eps = 1.0e-6, g = d.gamlg;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-  double u[4][6];
-  load_u(d, d.Us, e, u);
-  const double rhoct = 1.0 / u[0][0];
-  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
-  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
   double ul[6] = {0, 0, 0, 0, 0, 0}, p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
-  if (PART == 2) {
 #pragma unroll
-    for (int k = 0; k < 6; k++) {
-      ul[k] = d.rhs[(0 * 6 + k) * (size_t)d.ncell + e];
-      p0[k] = d.rhs[(1 * 6 + k) * (size_t)d.ncell + e];
-      p1[k] = d.rhs[(2 * 6 + k) * (size_t)d.ncell + e];
-      el[k] = d.rhs[(3 * 6 + k) * (size_t)d.ncell + e];
-    }
-  }
-  if (PART != 2) {
-  // face integral: corner forces F* = sigma.n A + m (u* - u_c), node by node
-#pragma unroll
-  for (int k = 0; k < 9; k++) {
+  for (int k = 0; k < 8; k++) {
     double b[6];
     node_basis2(G, k, b);
-    double st[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      double acc = 0.0;
-#pragma unroll
-      for (int kk = 0; kk < 6; kk++)
-        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
-      st[q] = acc;
-    }
-    const double rhovt = 1.0 / st[0];
-    const double ke = st[3] - 0.5 * (st[1] * st[1] + st[2] * st[2]);
     const int pn = d.ipq[k * d.nquad + iq];
-    const double dux = d.us[pn] - st[1], duy = d.vs[pn] - st[2];
     const double un = d.us_new[pn], vn = d.vs_new[pn];
-    const double du0 = un - st[1], du1 = vn - st[2];
-    double tw = 0.0, f0 = 0.0, f1 = 0.0, fe = 0.0;
-#pragma unroll
-    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
-      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
-      const double pv = fmax(eps, (g - 1.0) * (rhovt + d.corr[isg * (size_t)d.nquad + iq]) * ke);
-      const double wq = wmom(isg, ivsg);
-#pragma unroll
-      for (int f = 0; f < 2; f++) {
-        double ax, ay;
-        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
-        const double w = wrie(isg, ivsg, f);
-        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w);
-        const double pw = -2.0 * pv * w;
-        const double fs0 = pw * ax + m * du0;
-        const double fs1 = pw * ay + m * du1;
-        tw += (un * ax + vn * ay) * (2.0 * wmas(isg, ivsg, f));
-        f0 += fs0 * wq;
-        f1 += fs1 * wq;
-        fe += (un * fs0 + vn * fs1) * wq;
-      }
-    }
+    double tx, ty;
+    mass_flux_weights(L, k, tx, ty);
+    const double tw = un * tx + vn * ty;
+    const size_t nq = d.nquad;
+    const double P0 = d.npart[(0 * 9 + k) * nq + iq], P1 = d.npart[(1 * 9 + k) * nq + iq];
+    const double P2 = d.npart[(2 * 9 + k) * nq + iq], P3 = d.npart[(3 * 9 + k) * nq + iq];
+    const double P4 = d.npart[(4 * 9 + k) * nq + iq];
+    const double f0 = P3 + (un * P0 - P1);
+    const double f1 = P4 + (vn * P0 - P2);
+    const double fe = un * f0 + vn * f1;
 #pragma unroll
     for (int kk = 0; kk < 6; kk++) {
       ul[kk] += tw * b[kk];
@@ -665,17 +700,8 @@ __host__ __device__ void f_rhs_t(const Dev &d, int iq, int fuse_update, double a
       el[kk] += fe * b[kk];
     }
   }
-  }
-  if (PART == 1) {
-#pragma unroll
-    for (int k = 0; k < 6; k++) {
-      d.rhs[(0 * 6 + k) * (size_t)d.ncell + e] = ul[k];
-      d.rhs[(1 * 6 + k) * (size_t)d.ncell + e] = p0[k];
-      d.rhs[(2 * 6 + k) * (size_t)d.ncell + e] = p1[k];
-      d.rhs[(3 * 6 + k) * (size_t)d.ncell + e] = el[k];
-    }
-    return;
-  }
+  double u[4][6];
+  load_u(d, d.Us, e, u);
   // volume integral on the 5x5 Gauss-Lobatto grid (cofactor form), sum
   // factorised row by row: for fixed r_i, Q_b = sum_a L'_a(r_i) X[a][b] and
   // P_b = sum_a L_a(r_i) X[a][b] give dx/dr and dx/ds along the row
@@ -701,6 +727,25 @@ __host__ __device__ void f_rhs_t(const Dev &d, int iq, int fuse_update, double a
       rb[q] = u[q][2] + u[q][5] * dr;
     }
     const double wi = l5w(i);
+    // 1/tau at the row's 5 points with one division (batched reciprocals:
+    // prefix products, one reciprocal of the last, then back substitution)
+    double rtau[5];
+    {
+      double tq[5], pre[5];
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const double ds = l5p(j) - G.sc;
+        tq[j] = ra[0] + ds * (rb[0] + 0.5 * u[0][4] * ds);
+        pre[j] = j == 0 ? tq[0] : pre[j - 1] * tq[j];
+      }
+      double inv = 1.0 / pre[4];
+#pragma unroll
+      for (int j = 4; j > 0; j--) {
+        rtau[j] = inv * pre[j - 1];
+        inv = inv * tq[j];
+      }
+      rtau[0] = inv;
+    }
 #pragma unroll
     for (int j = 0; j < 5; j++) {
       const double s = l5p(j), ds = s - G.sc;
@@ -714,8 +759,8 @@ __host__ __device__ void f_rhs_t(const Dev &d, int iq, int fuse_update, double a
       const double ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
       double un[4];
 #pragma unroll
-      for (int q = 0; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * u[q][4] * ds);
-      const double rhoad = 1.0 / un[0];
+      for (int q = 1; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * u[q][4] * ds);
+      const double rhoad = rtau[j];
       const double pres = fmax(eps, (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2])));
       // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
       double gd0[5], gd1[5];
@@ -790,32 +835,49 @@ __host__ __device__ void f_rhs_t(const Dev &d, int iq, int fuse_update, double a
   }
 }
 
-// Stage update for stage 1 (the dt reduction sits between RHS and update)
-__host__ __device__ void f_update(const Dev &d, int e, double alfa) {
-  if (e >= d.ncell || d.sc_dev->done) return;
-  const double dt = d.sc_dev->dtfix;
-  double am[16];
+// getdelt_lag's per-quad limits (Getrhslag.f90:20641-20700) before the RHS
+// pass of stage 1: dvdt = rhsel(1,1,ielem) is the cell-average mass flux,
+// which only the face integral contributes to (the volume integral has no
+// moment-0 term and the source acts on the energy), i.e. sum_k u*_k . t_k
+// with the same per-node sums as f_rhs3.  With dt known before the RHS pass,
+// stage 1 fuses its M^-1 solve and update into the RHS kernel like the later
+// stages.  Edge lengths use the stage's nodes, which in stage 1 are x^n.
+__host__ __device__ void f_dt_quad(const Dev &d, int iq, double &dtcfl, double &dtvol) {
+  dtcfl = 1e10;
+  dtvol = 1e10;
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  const double eps = 1.0e-6, g = d.gamlg;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  double dvdt = 0.0;
 #pragma unroll
-  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * (size_t)d.ncell + e];
-  const double oma = 1.0 - alfa;
-  const int IDX[5][5] = {{0, 1, 2, 3, 4}, {1, 5, 6, 7, 8}, {2, 6, 9, 10, 11}, {3, 7, 10, 12, 13}, {4, 8, 11, 13, 14}};
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    double R[6];
-#pragma unroll
-    for (int k = 0; k < 6; k++) R[k] = dt * d.rhs[(q * 6 + k) * (size_t)d.ncell + e];
-    const size_t base = (size_t)(q * 6) * d.ncell + e;
-    const double d0 = am[15] * R[0];
-    d.Us[base] = alfa * d.Un[base] + oma * (d.Us[base] + d0);
-#pragma unroll
-    for (int i = 0; i < 5; i++) {
-      double acc = 0.0;
-#pragma unroll
-      for (int j = 0; j < 5; j++) acc += am[IDX[i][j]] * R[j + 1];
-      const size_t idx = base + (size_t)(i + 1) * d.ncell;
-      d.Us[idx] = alfa * d.Un[idx] + oma * (d.Us[idx] + acc);
-    }
+  for (int k = 0; k < 8; k++) {
+    const int pn = d.ipq[k * d.nquad + iq];
+    double tx, ty;
+    mass_flux_weights(L, k, tx, ty);
+    dvdt += d.us_new[pn] * tx + d.vs_new[pn] * ty;
   }
+  double xp[9][2];
+  node_xy(L, xp);
+  // curved edges: corner - mid-edge node - corner
+  const int ed[4][3] = {{0, 4, 1}, {1, 5, 2}, {2, 6, 3}, {3, 7, 0}};
+  double dlen = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const double *a = xp[ed[k][0]], *b = xp[ed[k][1]], *c = xp[ed[k][2]];
+    const double dl = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1])) +
+                      sqrt((b[0] - c[0]) * (b[0] - c[0]) + (b[1] - c[1]) * (b[1] - c[1]));
+    if (k == 0 || dl < dlen) dlen = dl;
+  }
+  const size_t nc = d.ncell;
+  const double rhomc = d.Us[0 * nc + e];
+  const double uctr = d.Us[6 * nc + e], vctr = d.Us[12 * nc + e], ectr = d.Us[18 * nc + e];
+  const double rhoct = 1.0 / rhomc;
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  dtcfl = dlen / sdctr;
+  dtvol = d.vol[e] / fabs(dvdt);
 }
 
 // Node motion with the new ustar, which becomes the previous ustar of the next stage
@@ -1506,8 +1568,8 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
         double cx, sx, cy, sy;
         if (fabs(dx) <= 0.15 && fabs(dy) <= 0.15) {
           double cdx, sdx, cdy, sdy;
-          cossin_pi_small(dx, cdx, sdx);
-          cossin_pi_small(dy, cdy, sdy);
+          cossin_pi_series<7>(dx, cdx, sdx);
+          cossin_pi_series<7>(dy, cdy, sdy);
           cx = cxc * cdx - sxc * sdx;
           sx = sxc * cdx + cxc * sdx;
           cy = cyc * cdy - syc * sdy;
@@ -1730,13 +1792,29 @@ __global__ void __launch_bounds__(128, 4) k_corner2_faces(Dev d) {
   f_corner_t<2>(d, blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void k_node2(Dev d) { f_node(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128, 3) k_rhs2_face(Dev d) {
-  f_rhs_t<1>(d, blockIdx.x * blockDim.x + threadIdx.x, 0, 0.0);
+__global__ void __launch_bounds__(128, 3) k_rhs3(Dev d, int fuse, double alfa) {
+  f_rhs3(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa);
 }
-__global__ void __launch_bounds__(128, 3) k_rhs2_rest(Dev d, int fuse, double alfa) {
-  f_rhs_t<2>(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa);
+// per-block minima of getdelt_lag's two limits (consumed by k_dt_final)
+__global__ void __launch_bounds__(256) k_dt2_partial(Dev d) {
+  __shared__ double sm_cfl[256], sm_vol[256];
+  double dtcfl, dtvol;
+  f_dt_quad(d, blockIdx.x * blockDim.x + threadIdx.x, dtcfl, dtvol);
+  sm_cfl[threadIdx.x] = dtcfl;
+  sm_vol[threadIdx.x] = dtvol;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sm_cfl[threadIdx.x] = fmin(sm_cfl[threadIdx.x], sm_cfl[threadIdx.x + s]);
+      sm_vol[threadIdx.x] = fmin(sm_vol[threadIdx.x], sm_vol[threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    d.dtpart[2 * blockIdx.x] = sm_cfl[0];
+    d.dtpart[2 * blockIdx.x + 1] = sm_vol[0];
+  }
 }
-__global__ void k_update2(Dev d, double alfa) { f_update(d, blockIdx.x * blockDim.x + threadIdx.x, alfa); }
 __global__ void k_nodes2(Dev d, double alfa) { f_nodes(d, blockIdx.x * blockDim.x + threadIdx.x, alfa); }
 __global__ void k_geom2(Dev d, int fix) { f_geom(d, blockIdx.x * blockDim.x + threadIdx.x, fix); }
 __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + threadIdx.x); }
@@ -1804,11 +1882,13 @@ void launch_fast_corner(const Dev &d, cudaStream_t st) {
 }
 void launch_fast_node(const Dev &d, cudaStream_t st) { fast::k_node2<<<fast::nb(d.npoin, 256), 256, 0, st>>>(d); }
 void launch_fast_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa) {
-  fast::k_rhs2_face<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d);
-  fast::k_rhs2_rest<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d, fuse, alfa);
+  fast::k_rhs3<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d, fuse, alfa);
 }
-void launch_fast_update(const Dev &d, cudaStream_t st, double alfa) {
-  fast::k_update2<<<fast::nb(d.ncell, 256), 256, 0, st>>>(d, alfa);
+void launch_dt_final(const Dev &d, cudaStream_t st, int nblk, int ndt);  // lag2d_kernels.cu
+void launch_fast_dt(const Dev &d, cudaStream_t st, int ndt) {
+  const int nb = fast::nb(d.nquad, 256);
+  fast::k_dt2_partial<<<nb, 256, 0, st>>>(d);
+  launch_dt_final(d, st, nb, ndt);
 }
 void launch_fast_nodes(const Dev &d, cudaStream_t st, double alfa) {
   fast::k_nodes2<<<fast::nb(d.npoin, 256), 256, 0, st>>>(d, alfa);

@@ -3010,6 +3010,7 @@ void launch_dt(const Dev &d, cudaStream_t st, int ndt) {
   k_dt_partial<<<nb, 256, 0, st>>>(d);
   k_dt_final<<<1, 256, 0, st>>>(d, nb, ndt);
 }
+void launch_dt_final(const Dev &d, cudaStream_t st, int nb, int ndt) { k_dt_final<<<1, 256, 0, st>>>(d, nb, ndt); }
 void launch_update(const Dev &d, cudaStream_t st, double alfa) {
   k_update<<<nblk(d.ncell, 128), 128, 0, st>>>(d, alfa);
 }

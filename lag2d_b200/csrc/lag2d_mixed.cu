@@ -386,66 +386,55 @@ __device__ void m_corner(const Dev &d, int iq) {
 }
 
 // ---------------------------------------------------------------------------
-// RHS pass: face integral with FP64 corner forces, the tau equation in FP64,
-// FP32 momentum/energy volume terms and source, FP64 moment 0; in stages 2
-// and 3 the FP64 M^-1 solve and RK combine
+// RHS pass: face integral from the corner pass's FP64 node partial sums, the
+// tau equation in FP64, FP32 momentum/energy volume terms and source, FP64
+// moment 0; the FP64 M^-1 solve and RK combine when fused
 // ---------------------------------------------------------------------------
+// Face integral (rhsifacedg_lagsubgq2, Getrhslaggauss.f90:8501-8748): at node
+// k the corner forces sum to (P3, P4) + u* P0 - (P1, P2) with P0..P4 the
+// FP64 partial sums of the FP32 corner coefficients that the corner pass
+// wrote (the momentum weights are 1 on the 8 boundary nodes and 0 at the
+// centre node), the energy term is u* . that sum and the mass term u* . sum_f
+// 2 w_mass,f an_f over the outer corner faces; see f_rhs3 in lag2d_fast.cu.
 __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
   if (iq >= d.nquad || d.sc_dev->done) return;
   const int e = iq + d.ntria;
-  const float eps = 1.0e-6f, g = (float)d.gamlg, slpdu = (g + 1.0f) / 2.0f, cimpd = (float)d.cimpd;
+  const float eps = 1.0e-6f, g = (float)d.gamlg;
   CellXY L;
   load_cell(d, iq, L, nullptr);
   const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
   const GeoF G{(float)rc, (float)sc, (float)g19, (float)g20, (float)g21};
-  double ud[3][6];  // tau, u, v in FP64 (tau equation)
-  float u[4][6];
-#pragma unroll
-  for (int q = 0; q < 4; q++)
-#pragma unroll
-    for (int k = 0; k < 6; k++) {
-      const double v = d.Us[(q * 6 + k) * (size_t)d.ncell + e];
-      if (q < 3) ud[q][k] = v;
-      u[q][k] = (float)v;
-    }
-  float rhoct, sdctr;
-  centre_state(u, g, rhoct, sdctr);
   double tr[6] = {0, 0, 0, 0, 0, 0};          // tau equation, all moments
   double pa0 = 0.0, pb0 = 0.0, el0 = 0.0;     // cell averages of momentum and energy
   float p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
-  for (int k = 0; k < 9; k++) {
-    float b[6], st[4];
+  for (int k = 0; k < 8; k++) {
+    float b[6];
     node_basis(G, k, b);
-    vertex_state(u, b, d.mdegr, st);
-    const float rhovt = __fdiv_rn(1.0f, st[0]);
-    const float ke = kinetic_f(st);
     const int pn = d.ipq[k * d.nquad + iq];
-    const float dux = (float)d.us[pn] - st[1];
-    const float duy = (float)d.vs[pn] - st[2];
     const double un = d.us_new[pn], vn = d.vs_new[pn];
-    const double du0 = un - (double)st[1], du1 = vn - (double)st[2];
-    double tw = 0.0, f0 = 0.0, f1 = 0.0, fe = 0.0;
+    double tx = 0.0, ty = 0.0;
 #pragma unroll
     for (int i = MT().nc_start[k]; i < MT().nc_start[k + 1]; i++) {
       const int isg = MT().nc_entry[i] >> 2, ivsg = MT().nc_entry[i] & 3;
-      const float ci = (float)d.corr[isg * (size_t)d.nquad + iq];
-      const float pv = fmaxf(eps, __fmul_rn(__fmul_rn(g - 1.0f, __fadd_rn(rhovt, ci)), ke));
-      const double wq = MD().wmom[4 * isg + ivsg];
 #pragma unroll
       for (int f = 0; f < 2; f++) {
-        double ax, ay;
-        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
-        float m, sx, sy;
-        corner_coeffs(ax, ay, MT().wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy);
-        const double fs0 = (double)sx + (double)m * du0;
-        const double fs1 = (double)sy + (double)m * du1;
-        tw += (un * ax + vn * ay) * (2.0 * MD().wmas[8 * isg + 2 * ivsg + f]);
-        f0 += fs0 * wq;
-        f1 += fs1 * wq;
-        fe += (un * fs0 + vn * fs1) * wq;
+        if (MD().wmas[8 * isg + 2 * ivsg + f] != 0.0) {
+          double ax, ay;
+          corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
+          tx += ax * (2.0 * MD().wmas[8 * isg + 2 * ivsg + f]);
+          ty += ay * (2.0 * MD().wmas[8 * isg + 2 * ivsg + f]);
+        }
       }
     }
+    const double tw = un * tx + vn * ty;
+    const size_t nq = d.nquad;
+    const double P0 = d.npart[(0 * 9 + k) * nq + iq], P1 = d.npart[(1 * 9 + k) * nq + iq];
+    const double P2 = d.npart[(2 * 9 + k) * nq + iq], P3 = d.npart[(3 * 9 + k) * nq + iq];
+    const double P4 = d.npart[(4 * 9 + k) * nq + iq];
+    const double f0 = P3 + (un * P0 - P1);
+    const double f1 = P4 + (vn * P0 - P2);
+    const double fe = un * f0 + vn * f1;
     // tau: all moments in FP64 with the FP64 node basis
     {
       const double b1 = MD().xv[k] - rc, b2 = MD().yv[k] - sc;
@@ -467,6 +456,16 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
       el[kk] += fef * b[kk];
     }
   }
+  double ud[3][6];  // tau, u, v in FP64 (tau equation)
+  float u[4][6];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      const double v = d.Us[(q * 6 + k) * (size_t)d.ncell + e];
+      if (q < 3) ud[q][k] = v;
+      u[q][k] = (float)v;
+    }
   // volume integral, 5x5 Gauss-Lobatto, cofactor form, sum-factorised rows:
   // Jacobian and velocity in FP64 (tau equation), pressure work in FP32
 #pragma unroll 1

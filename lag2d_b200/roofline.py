@@ -17,16 +17,18 @@ written once, intermediates excluded), FP64:
 
 Per kernel family the same rule is applied to that kernel's own interface
 (its inputs read once, its outputs written once), for the optimised kernels
-the step runs (corner data are recomputed in the RHS pass, not stored):
+the step runs (the RHS pass takes the face integral from the corner pass's
+node partial sums):
 
   corner   U^(s), rc/sc/g19..g21, sub-cell masses, connectivity, x^(s),
            ustar_prev -> 4 sub-cell corrections, 45 node partial sums
   node     45 partial sums and 9 gather ids per quad, CSR offset, mask,
            ustar_prev -> ustar
-  rhs      U^(s), geometry, corrections, connectivity, x^(s), ustar_prev,
-           ustar -> RHS (stage 1), or in stages 2..nstag also U^n and M^-1
-           -> U^(s+1) (the M^-1 solve and RK combine are fused there)
-  update   RHS, U^n, U^(s), M^-1 -> U^(s+1) (stage 1)
+  dt       (stage 1) connectivity, cell averages, volume, x^(s), ustar
+           -> two per-block minima
+  rhs      U^(s), U^n, M^-1, geometry, the 40 partial sums of the 8
+           boundary nodes, connectivity, x^(s), ustar -> U^(s+1) (the M^-1
+           solve and RK combine are fused into every stage)
   persson  tau DOFs, mean velocity, geometry, mass, shape moments,
            connectivity, x^(s) -> flag, physical centre, frame
   nodes    x^n, x^(s), ustar -> x^(s+1), ustar_prev
@@ -55,13 +57,11 @@ def kernel_bytes(family: str, ncell: int, npoin: int, nstag: int = 3) -> int:
     GEO = 5 * W           # rc, sc, g19..g21
     CONN = 9 * 4          # ipqua row
     XY = 2 * W            # one node pair (x, y) or (u, v)
-    rhs_plain = ncell * (U + GEO + 4 * W + CONN + U) + npoin * 3 * XY
-    rhs_fused = ncell * (U + U + 16 * W + GEO + 4 * W + CONN + U) + npoin * 3 * XY
     fam = {
         "corner": ncell * (U + GEO + 4 * W + CONN + 4 * W + 45 * W) + npoin * (XY + XY),
         "node": ncell * (45 * W + 9 * 4) + npoin * (4 + 1 + XY + XY),
-        "rhs": (rhs_plain + (nstag - 1) * rhs_fused) // nstag,
-        "update": ncell * (U + U + 2 * U + 16 * W),
+        "dt": ncell * (CONN + 4 * W + W) + npoin * 2 * XY,
+        "rhs": ncell * (U + U + 16 * W + GEO + 40 * W + CONN + U) + npoin * 2 * XY,
         "persson": ncell * (6 * W + 2 * W + GEO + W + 9 * W + CONN + 4 + 2 * W + 4 * W) + npoin * XY,
         "nodes": npoin * (3 * XY + 2 * XY),
         "geom": ncell * (CONN + W + XY) + npoin * XY,
