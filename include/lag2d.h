@@ -124,6 +124,17 @@ int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags);
  * applied to the device state.  For limiter parity checks. */
 int lag2d_weno(lag2d_handle *h, const int *flags);
 
+/* The WENO reconstruction of the handle's current state, linearised with its
+ * active set frozen (Persson marks, stencils, nonlinear weights, velocity
+ * frame and characteristic matrices held at their values for that state):
+ * the map M with M(v) = v except on the quads WENO replaces, whose moments
+ * 2..ndegr become the frozen reconstruction of v's stencil DOFs.  transpose =
+ * 0 writes out = M(in), 1 writes out = M^T(in); in and out have the layout
+ * of unkno(ndegr,nq,nsize) (ghost entries of out are zeroed).  M(unkno) is
+ * the reconstruction itself; M^T is what the adjoint applies per RK stage.
+ * No counterpart in the reference (it has no adjoint). */
+int lag2d_weno_linear(lag2d_handle *h, int transpose, const double *in, double *out);
+
 /* getcellvol_lag (Limiterlag.f90:1869) on the device coordinates; returns
  * geoel(24,nsize) with fields 3, 5, 6 refreshed if geoel is not NULL. */
 int lag2d_cellvol(lag2d_handle *h, double *geoel);
@@ -160,11 +171,14 @@ double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *lau
  * FP32-mixed adjoint); precision 0 is FP64 throughout.  Reverse mode per RK
  * stage with these held fixed: the time step size of each step (ndt == 1
  * picks it on the forward pass; the gradient treats it as a constant), the
- * Persson marks, and the reference-configuration quantities (geoel fields 1-4
- * and 19-21, amatr, the initial sub-cell masses).  A window in which WENO
- * replaces the DOFs of a cell returns LAG2D_EUNSUP (the adjoint of the WENO
- * reconstruction is not built); marked cells whose stencil is rejected keep
- * their DOFs and are differentiated as such.  Gradients use the
+ * Persson marks, the WENO reconstruction's active set (stencils, nonlinear
+ * weights, velocity frame and characteristic matrices taken at each stage's
+ * input: the reconstruction is differentiated as the linear map
+ * lag2d_weno_linear describes, with no sensitivity through the node
+ * positions), and the reference-configuration quantities (geoel fields 1-4
+ * and 19-21, amatr, the initial sub-cell masses).  Marked cells whose
+ * stencil is rejected keep their DOFs and are differentiated as such.  More
+ * than 16384 WENO-limited quads in one stage return LAG2D_EUNSUP.  Gradients use the
  * layouts of lag2d_set_state: unkno(ndegr,nq,ncell), coord(2,npoin),
  * ustar(2,npoin).
  * ------------------------------------------------------------------------- */

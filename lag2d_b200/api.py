@@ -66,7 +66,7 @@ EXPORTS = ("lag2d_create", "lag2d_init_fields", "lag2d_set_state", "lag2d_step",
            "lag2d_get_state", "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_stream",
            "lag2d_kernel_launches", "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error",
            "lag2d_delt_noalloc", "lag2d_adjoint_step", "lag2d_adjoint", "lag2d_set_rho0",
-           "lag2d_error_norms")
+           "lag2d_error_norms", "lag2d_weno_linear")
 
 
 def library_path(exact: bool = False) -> str:
@@ -90,7 +90,7 @@ def load(exact: bool = False):
     lib.lag2d_create.argtypes = [ctypes.POINTER(_Mesh), ctypes.POINTER(_Cfg), ctypes.POINTER(ctypes.c_void_p)]
     for name in ("lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run", "lag2d_get_state",
                  "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_timing", "lag2d_adjoint_step",
-                 "lag2d_adjoint", "lag2d_set_rho0", "lag2d_error_norms"):
+                 "lag2d_adjoint", "lag2d_set_rho0", "lag2d_error_norms", "lag2d_weno_linear"):
         getattr(lib, name).restype = ctypes.c_int
     lib.lag2d_destroy.argtypes = [ctypes.c_void_p]
     _libs[key] = lib
@@ -212,6 +212,17 @@ class Lag2DSolver:
     def weno(self, flags):
         f = np.ascontiguousarray(flags, dtype=np.int32)
         self._check(self.lib.lag2d_weno(self.h, _p(f, _ip)))
+
+    def weno_linear(self, v: np.ndarray, transpose: bool = False) -> np.ndarray:
+        """The WENO reconstruction at the current state with its active set
+        frozen, applied to v (nsize, nq, ndegr): M(v), or M^T(v)."""
+        m, c = self.mesh, self.cfg
+        vin = np.zeros((m.nsize, c.nq, c.ndegr))
+        vin[:v.shape[0]] = v
+        out = np.zeros((m.nsize, c.nq, c.ndegr))
+        self._check(self.lib.lag2d_weno_linear(self.h, ctypes.c_int(1 if transpose else 0), _p(vin, _dp),
+                                               _p(out, _dp)))
+        return out
 
     def error_norms(self) -> np.ndarray:
         """geterror_lag_curvhybrid's L2 errors of the current state against the

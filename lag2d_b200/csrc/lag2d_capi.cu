@@ -56,7 +56,12 @@ void launch_tri_geom(const Dev &d, cudaStream_t st, const double *X, const doubl
 void launch_tri_corner(const Dev &d, cudaStream_t st);
 void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa);
 void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold,
-                          int mixed);
+                          int fold_u, int mixed);
+void launch_adjoint_fold_u(const Dev &d, const void *adj, cudaStream_t st);
+void launch_weno_linear(const Dev &d, cudaStream_t st, int mode, const double *v, double *out, double *wbuf,
+                        int *wslot, int cap, int *overflow);
+void launch_weno_gather(const Dev &d, cudaStream_t st, double *lamU, const double *wbuf, const int *wslot, int cap,
+                        const int *inv_ptr, const int *inv_ent);
 int adjoint_stage_launches(const Dev &d);
 int error_blocks(const Dev &d);
 void launch_error(const Dev &d, cudaStream_t st, const double *X, const double *Y, double *part);
@@ -106,6 +111,10 @@ struct lag2d_handle {
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   p1::Solver *p1 = nullptr;    // the linear P1 path (npoly = 1) when set; Dev d is then unused
   double *errpart = nullptr;   // per-block partial sums of lag2d_error_norms
+  // inverse of the WENO stencil table: for quad j, the entries c*9 + s of the
+  // quads c whose stencil position s is j, c ascending (the WENO transpose's
+  // fixed summation order)
+  int *sinv_ptr = nullptr, *sinv_ent = nullptr;
 };
 
 template <typename T>
@@ -328,7 +337,6 @@ static void rhs_pass(lag2d_handle *h, const Dev &d, int fuse, double alfa) {
 struct StageRec {
   double *U, *x, *y, *us, *vs, *dt;
   double *npart, *corr, *usn, *vsn, *tcf, *tpart;
-  int *troubled;
   int step, nstag;
   size_t nu, np, nq, nt;
   // the handle's device view with the corner/node outputs of a slot
@@ -355,14 +363,6 @@ struct StageRec {
     return d;
   }
 };
-// cells the WENO pass actually replaced (flag 2): marked cells whose stencil
-// was rejected keep their DOFs, so the step stays differentiable there
-__global__ void k_count_limited(Dev d, int *acc) {
-  int n = 0;
-  for (int t = threadIdx.x; t < *d.wcount; t += blockDim.x) n += d.flag[d.wlist[t] + d.ntria] == 2;
-  if (n) atomicAdd(acc, n);
-}
-
 // The same step with the optimised kernels: node partial sums, recomputed
 // corner data, closed-form volumes and the stage update fused into the RHS
 // pass in stages 2 and 3.
@@ -384,10 +384,6 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
     }
     run(h, "persson", [&] { launch_reset_count(d, h->st); launch_fast_persson(d, h->st); }, 2);
     run(h, "weno", [&] { launch_weno_warp(d, h->st); launch_weno_commit(d, h->st); }, 2);
-    if (rec) {
-      k_count_limited<<<1, 256, 0, h->st>>>(d, rec->troubled);
-      h->launches += 1;
-    }
     run(h, "corner", [&] { corner_pass(h, d); }, corner_launches(h, d));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
@@ -618,6 +614,25 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   for (int p = 0; p < np; p++) { xx[p] = m->coold[2 * (size_t)p]; yy[p] = m->coold[2 * (size_t)p + 1]; }
 #define UP(dst, src, n) cudaMemcpyAsync((void *)(dst), (src), (n) * sizeof(*(src)), cudaMemcpyHostToDevice, h->st)
   UP(ipq_d, ipq.data(), ipq.size()); UP(esq_d, esq.data(), esq.size()); UP(sten_d, sten.data(), sten.size());
+  {
+    std::vector<int> iptr(nq + 1, 0), ient;
+    for (int c = 0; c < nq; c++)
+      if (sten[c] >= 0)
+        for (int k = 0; k < 9; k++) iptr[sten[k * (size_t)nq + c] - m->ntria + 1]++;
+    for (int j = 0; j < nq; j++) iptr[j + 1] += iptr[j];
+    ient.assign(std::max(iptr[nq], 1), 0);
+    std::vector<int> fill(iptr.begin(), iptr.end() - 1);
+    for (int c = 0; c < nq; c++)
+      if (sten[c] >= 0)
+        for (int k = 0; k < 9; k++) ient[fill[sten[k * (size_t)nq + c] - m->ntria]++] = c * 9 + k;
+    if (dalloc(h, &h->sinv_ptr, iptr.size()) || dalloc(h, &h->sinv_ent, ient.size())) {
+      lag2d_destroy(h);
+      return LAG2D_ECUDA;
+    }
+    CK(cudaMemcpyAsync(h->sinv_ptr, iptr.data(), iptr.size() * sizeof(int), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->sinv_ent, ient.data(), ient.size() * sizeof(int), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+  }
   UP(ptr_d, cnt.data(), cnt.size()); UP(ncf_d, nodecf.data(), nodecf.size()); UP(mask_d, mask.data(), mask.size());
   UP(x0, xx.data(), np); UP(y0, yy.data(), np);
   UP(ptr2_d, cnt2.data(), cnt2.size()); UP(slot_d, slots.data(), slots.size());
@@ -924,6 +939,57 @@ int lag2d_weno(lag2d_handle *h, const int *flags) {
   return r;
 }
 
+int lag2d_weno_linear(lag2d_handle *h, int transpose, const double *in, double *out) {
+  if (!h || !in || !out) return fail(LAG2D_EINVAL, "null argument");
+  if (h->p1) return fail(LAG2D_EUNSUP, "WENO is not on the P1 branch");
+  if (h->cfg.order_exact) return fail(LAG2D_EUNSUP, "the linearised WENO follows the optimised step (order_exact 0)");
+  Dev &d = h->d;
+  const size_t nu = (size_t)NU * d.ncell;
+  int r = put_scalars(h, 1, 0.0, 0.0);
+  if (r) return r;
+  // Persson marks and the reconstruction at the handle's state (not committed)
+  run(h, "persson", [&] { launch_reset_count(d, h->st); launch_fast_persson(d, h->st); }, 2);
+  run(h, "weno", [&] { launch_weno_warp(d, h->st); });
+  const int cap = std::max(1, std::min(d.nquad, 16384));
+  double *vbuf = nullptr, *obuf = nullptr, *wbuf = nullptr;
+  int *wslot = nullptr, *overflow = nullptr;
+  struct Free {
+    std::vector<void *> p;
+    ~Free() { for (void *q : p) cudaFree(q); }
+  } fr;
+  auto alloc = [&](void **q, size_t bytes) {
+    cudaError_t e = cudaMalloc(q, std::max<size_t>(bytes, 8));
+    if (e == cudaSuccess) { fr.p.push_back(*q); cudaMemsetAsync(*q, 0, std::max<size_t>(bytes, 8), h->st); }
+    return e;
+  };
+  if (alloc((void **)&vbuf, nu * 8) || alloc((void **)&obuf, nu * 8) || alloc((void **)&wbuf, 216 * (size_t)cap * 8) ||
+      alloc((void **)&wslot, (size_t)d.nquad * 4) || alloc((void **)&overflow, 4))
+    return fail(LAG2D_ECUDA, "cudaMalloc (lag2d_weno_linear)");
+  // the layout conversions read and write the view's U^n slab
+  Dev dv = d, dout = d;
+  dv.Un = vbuf;
+  dout.Un = obuf;
+  CK(cudaMemcpyAsync(h->stage_u, in, nu * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  launch_unkno_in(dv, h->st, h->stage_u, 0);
+  CK(cudaMemcpyAsync(obuf, vbuf, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  if (transpose) {
+    launch_weno_linear(d, h->st, 1, vbuf, nullptr, wbuf, wslot, cap, overflow);
+    launch_weno_gather(d, h->st, obuf, wbuf, wslot, cap, h->sinv_ptr, h->sinv_ent);
+  } else {
+    launch_weno_linear(d, h->st, 0, vbuf, obuf, nullptr, nullptr, cap, overflow);
+  }
+  launch_unkno_out(dout, h->st, h->stage_u);
+  h->launches += 4;
+  CK(cudaMemcpyAsync(out, h->stage_u, nu * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  int o = 0;
+  CK(cudaMemcpyAsync(&o, overflow, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  if (o) return fail(LAG2D_EUNSUP, "more WENO-limited quads than the buffer holds");
+  std::fill(out + nu, out + NU * (size_t)(d.ncell + d.nbfac), 0.0);
+  return read_status(h);
+}
+
 int lag2d_cellvol(lag2d_handle *h, double *geoel) {
   if (!h) return fail(LAG2D_EINVAL, "null handle");
   if (h->p1) P1_CALL(p1::cellvol(h->p1, geoel, err_));
@@ -1004,6 +1070,11 @@ struct AdjWork {
   Adj a{};
   StageRec rec{};
   int rc = LAG2D_OK;
+  // WENO transpose: the stage state after WENO, per-slot stencil adjoints,
+  // slot of each troubled quad, overflow flag; cap = slots per stage
+  double *post = nullptr, *wbuf = nullptr;
+  int *wslot = nullptr, *overflow = nullptr;
+  int cap = 0;
   explicit AdjWork(lag2d_handle *hh) : h(hh) {}
   ~AdjWork() {
     cudaStreamSynchronize(h->st);
@@ -1035,39 +1106,62 @@ struct AdjWork {
     alloc(&a.tbuf, 36 * (size_t)d.ntria); alloc(&a.ltcf, 120 * (size_t)d.ntria);
     const size_t ns = (size_t)K * nstag;
     alloc(&rec.U, ns * nu); alloc(&rec.x, ns * np); alloc(&rec.y, ns * np);
-    alloc(&rec.us, ns * np); alloc(&rec.vs, ns * np); alloc(&rec.dt, K); alloc(&rec.troubled, 1);
+    alloc(&rec.us, ns * np); alloc(&rec.vs, ns * np); alloc(&rec.dt, K);
     alloc(&rec.npart, ns * 45 * (size_t)d.nquad); alloc(&rec.corr, ns * 4 * (size_t)d.nquad);
     alloc(&rec.usn, ns * np); alloc(&rec.vsn, ns * np);
     alloc(&rec.tcf, ns * 120 * (size_t)d.ntria); alloc(&rec.tpart, ns * 30 * (size_t)d.ntria);
     rec.nstag = nstag; rec.nu = nu; rec.np = np; rec.nq = d.nquad; rec.nt = d.ntria;
+    cap = std::max(1, std::min(d.nquad, 16384));
+    alloc(&post, nu); alloc(&wbuf, 216 * (size_t)cap); alloc(&wslot, (size_t)d.nquad); alloc(&overflow, 1);
   }
   // forward of nk steps from the handle's state, recording every stage input
   int record(int itime, int nk) {
-    cudaMemsetAsync(rec.troubled, 0, sizeof(int), h->st);
     for (int k = 0; k < nk; k++) {
       rec.step = k;
       enqueue_step_fast(h, itime + k, &rec);
     }
     return LAG2D_OK;
   }
-  int check_troubled() {
-    int troubled = 0;
-    CK(cudaMemcpyAsync(&troubled, rec.troubled, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  int check_overflow() {
+    int o = 0;
+    CK(cudaMemcpyAsync(&o, overflow, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    if (troubled) return fail(LAG2D_EUNSUP, "WENO limits cells in the adjoint window: its adjoint is not built");
+    if (o)
+      return fail(LAG2D_EUNSUP, "more WENO-limited quads in one stage than the adjoint's WENO buffer holds (" +
+                                    std::to_string(cap) + ")");
     return LAG2D_OK;
   }
   // reverse of the nk recorded steps; a.lU / a.lx / a.lus hold the adjoints of
   // the last step's outputs on entry and of the first step's inputs on return
+  // Each stage's reverse linearises at the state after WENO: the recorded
+  // stage input (before WENO) is copied to `post`, and Persson and WENO are
+  // run again on it (same marks, same reconstruction); the reverse kernels
+  // run on `post`; then the WENO transpose, with its stencils, weights, frame
+  // and characteristic matrices taken at the recorded input (the limiter's
+  // active set frozen), maps the adjoint of `post` to that of the input.
   void reverse(int nk) {
     const int nstag = h->cfg.nstag;
+    const size_t nu = (size_t)NU * h->d.ncell;
+    // the recompute must not see the end-of-run flag a window ending at tend leaves
+    cudaMemsetAsync(&h->d.sc_dev->done, 0, sizeof(int), h->st);
     for (int k = nk - 1; k >= 0; k--) {
       for (int istag = nstag; istag >= 1; istag--) {
         const Dev ds = rec.inputs(h->d, (size_t)k * nstag + (istag - 1));
-        // stage 1 reads U^n and x^n directly: its reverse folds their adjoints in
-        launch_adjoint_stage(ds, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k, istag == 1,
+        Dev dp = ds;
+        dp.Us = post;
+        cudaMemcpyAsync(post, ds.Us, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
+        launch_reset_count(ds, h->st);
+        launch_fast_persson(ds, h->st);
+        launch_weno_warp(ds, h->st);
+        launch_weno_commit(dp, h->st);
+        // stage 1 reads x^n directly: its reverse folds the coordinate adjoints
+        // in; the U^n fold waits for the WENO transpose
+        launch_adjoint_stage(dp, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k, istag == 1, 0,
                              h->cfg.precision == 1);
-        h->launches += adjoint_stage_launches(h->d);
+        launch_weno_linear(ds, h->st, 1, a.lU, nullptr, wbuf, wslot, cap, overflow);
+        launch_weno_gather(ds, h->st, a.lU, wbuf, wslot, cap, h->sinv_ptr, h->sinv_ent);
+        if (istag == 1) launch_adjoint_fold_u(ds, &a, h->st);
+        h->launches += adjoint_stage_launches(h->d) + 6 + (istag == 1);
       }
     }
   }
@@ -1183,8 +1277,6 @@ int lag2d_adjoint_step(lag2d_handle *h, int itime, double *dtfix, double *tacru,
   r = get_scalars(h, &fin);
   if (r) return r;
   if (fin.status) return read_status(h);
-  r = w.check_troubled();
-  if (r) return r;
   r = put_adjoint(h, w.a, seed_unkno, seed_coord, seed_ustar);
   if (r) return r;
   // keep the step's outputs: the reverse pass overwrites the stage buffers
@@ -1196,6 +1288,7 @@ int lag2d_adjoint_step(lag2d_handle *h, int itime, double *dtfix, double *tacru,
   out.restore(h, 0);
   CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
+  if ((r = w.check_overflow())) return r;
   r = get_adjoint(h, w.a, grad_unkno, grad_coord, grad_ustar);
   if (r) return r;
   *dtfix = fin.dtfix;
@@ -1276,11 +1369,6 @@ int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every,
     w.record(itime0 + n0, nk);
     cudaEventRecord(ev[1], h->st);
     t_rec += elapsed();
-    r = w.check_troubled();
-    if (r) {
-      ck.restore(h, nseg);
-      return r;
-    }
     cudaEventRecord(ev[0], h->st);
     w.reverse(nk);
     cudaEventRecord(ev[1], h->st);
@@ -1290,6 +1378,7 @@ int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every,
   ck.restore(h, nseg);
   CK(cudaStreamSynchronize(h->st));
   CK(cudaGetLastError());
+  if ((r = w.check_overflow())) return r;
   r = get_adjoint(h, w.a, dJ_dunkno, dJ_dcoord, dJ_dustar);
   if (r) return r;
   *dtfix = fin.dtfix;

