@@ -1102,7 +1102,7 @@ struct AdjWork {
     alloc(&a.lU, nu); alloc(&a.lUn, nu); alloc(&a.lR, nu);
     alloc(&a.lx, np); alloc(&a.ly, np); alloc(&a.lxn, np); alloc(&a.lyn, np); alloc(&a.lus, np); alloc(&a.lvs, np);
     alloc(&a.luw, np); alloc(&a.lvw, np); alloc(&a.tx, np); alloc(&a.ty, np);
-    alloc(&a.lS, 5 * np); alloc(&a.lcorr, 4 * (size_t)d.nquad); alloc(&a.pbuf, 54 * (size_t)d.nquad);
+    alloc(&a.lS, 5 * np); alloc(&a.lP, 45 * (size_t)d.nquad); alloc(&a.pbuf, 54 * (size_t)d.nquad);
     alloc(&a.tbuf, 36 * (size_t)d.ntria); alloc(&a.ltcf, 120 * (size_t)d.ntria);
     const size_t ns = (size_t)K * nstag;
     alloc(&rec.U, ns * nu); alloc(&rec.x, ns * np); alloc(&rec.y, ns * np);

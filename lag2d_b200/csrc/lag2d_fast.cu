@@ -256,6 +256,22 @@ __host__ __device__ __forceinline__ void load_cell(const Dev &d, const double *X
   }
 }
 
+// node coordinates relative to the centre node, in the reference node order:
+// the cross products x_i y_j - x_j y_i of absolute coordinates cancel about
+// log10(|x|^2 / V) digits on a small cell far from the origin; every
+// quantity built from them here (areas, sub-areas, det J coefficients) is
+// invariant under translation, so they are taken relative to the cell
+__host__ __device__ __forceinline__ void node_xy_rel(const Loaded &L, double (*xp)[2]) {
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  const double ox = L.X[1][1], oy = L.Y[1][1];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    xp[k][0] = L.X[A[k]][B[k]] - ox;
+    xp[k][1] = L.Y[A[k]][B[k]] - oy;
+  }
+}
+
 // node coordinates back in the reference node order
 __host__ __device__ __forceinline__ void node_xy(const Loaded &L, double (*xp)[2]) {
   const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
@@ -285,7 +301,7 @@ __host__ __device__ void f_persson(const Dev &d, int iq) {
   double c[36], D[16];
   {
     double xp[9][2];
-    node_xy(L, xp);
+    node_xy_rel(L, xp);
     cross36(xp, c);
   }
   detpoly(c, D);
@@ -379,7 +395,7 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
   double c[36], D[16];
   {
     double xp[9][2];
-    node_xy(L, xp);
+    node_xy_rel(L, xp);
     cross36(xp, c);
   }
   detpoly(c, D);
@@ -787,7 +803,7 @@ __host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double al
     double c[36], D[16];
     {
       double xp[9][2];
-      node_xy(L, xp);
+      node_xy_rel(L, xp);
       cross36(xp, c);
     }
     detpoly(c, D);
@@ -909,7 +925,7 @@ __host__ __device__ void f_geom(const Dev &d, int iq, int fix_centre) {
   double c[36], D[16];
   {
     double xp[9][2];
-    node_xy(L, xp);
+    node_xy_rel(L, xp);
     cross36(xp, c);
   }
   detpoly(c, D);
@@ -933,7 +949,7 @@ __host__ __device__ void f_init_wmom(const Dev &d, int iq) {
   double c[36], D[16];
   {
     double xp[9][2];
-    node_xy(L, xp);
+    node_xy_rel(L, xp);
     cross36(xp, c);
   }
   detpoly(c, D);
@@ -1120,8 +1136,9 @@ __host__ __device__ __forceinline__ void vertex_T(const double *b, int mdegr, co
 }
 
 // Reverse of the corner pass of quad iq: reads the node-sum adjoints lS at
-// its nodes and lcorr; adds the cell DOF adjoint into lU and writes the node
-// contributions (x, y, u*_prev, v*_prev) into pbuf.
+// its nodes plus the RHS pass's adjoints of its partials (lP); adds the cell
+// DOF adjoint into lU and writes the node contributions (x, y, u*_prev,
+// v*_prev) into pbuf.
 template <typename R>
 __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   if (iq >= d.nquad) return;
@@ -1131,7 +1148,7 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
   double xp[9][2], c[36], D[16];
-  node_xy(L, xp);
+  node_xy_rel(L, xp);
   cross36(xp, c);
   detpoly(c, D);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
@@ -1171,9 +1188,13 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
     const double ke = st[3] - 0.5 * (st[1] * st[1] + st[2] * st[2]);
     const int pn = d.ipq[k * d.nquad + iq];
     const double dux = d.us[pn] - st[1], duy = d.vs[pn] - st[2];
-    const double lP0 = a.lS[0 * (size_t)d.npoin + pn], lP1 = a.lS[1 * (size_t)d.npoin + pn];
-    const double lP2 = a.lS[2 * (size_t)d.npoin + pn], lP3 = a.lS[3 * (size_t)d.npoin + pn];
-    const double lP4 = a.lS[4 * (size_t)d.npoin + pn];
+    // adjoint of this quad's partials at node k: through the node sums (node
+    // solve) and directly through the RHS pass's face integral
+    const double lP0 = a.lS[0 * (size_t)d.npoin + pn] + a.lP[(0 * 9 + k) * nq + iq];
+    const double lP1 = a.lS[1 * (size_t)d.npoin + pn] + a.lP[(1 * 9 + k) * nq + iq];
+    const double lP2 = a.lS[2 * (size_t)d.npoin + pn] + a.lP[(2 * 9 + k) * nq + iq];
+    const double lP3 = a.lS[3 * (size_t)d.npoin + pn] + a.lP[(3 * 9 + k) * nq + iq];
+    const double lP4 = a.lS[4 * (size_t)d.npoin + pn] + a.lP[(4 * 9 + k) * nq + iq];
     double lst1 = 0, lst2 = 0, lrhovt = 0, lke = 0, ldux = 0, lduy = 0;
     for (int i = nc_start(k); i < nc_start(k + 1); i++) {
       const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
@@ -1214,7 +1235,7 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   double lD[16], lv4[4] = {0, 0, 0, 0};
   for (int t = 0; t < 16; t++) lD[t] = 0.0;
   for (int isg = 0; isg < 4; isg++) {
-    const double lc = lcr[isg] + a.lcorr[isg * nq + iq];
+    const double lc = lcr[isg];
     const double msub = d.msub[isg * nq + iq];
     lv4[isg] += -d.cdrho * lc * msub / (vsub4[isg] * vsub4[isg]);
     const double lmasel = -d.cdrho * lc / volel4[isg];
@@ -1430,22 +1451,20 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
 }
 
 // Reverse of the RHS pass of quad iq (the RHS written, no fused update):
-// from lR adds into lU, writes pbuf (x, y, u*_prev, v*_prev, u*_new, v*_new)
-// and lcorr.
+// from lR adds into lU, writes pbuf (x, y, u*_prev = 0, v*_prev = 0, u*_new,
+// v*_new) and the adjoints of the node partial sums the face integral reads
+// (lP, consumed by a_corner).
 template <typename R>
 __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
   if (iq >= d.nquad) return;
   const int e = iq + d.ntria;
   const size_t nq = d.nquad, nc = d.ncell;
-  const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
+  const double eps = 1.0e-6, g = d.gamlg;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
   double u[4][6];
   load_u(d, d.Us, e, u);
-  const double rhoct = 1.0 / u[0][0];
-  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
-  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
   double lR[4][6];
   for (int q = 0; q < 4; q++)
     for (int k = 0; k < 6; k++) lR[q][k] = a.lR[(q * 6 + k) * nc + e];
@@ -1453,24 +1472,26 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
   for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
   double lX[3][3], lY[3][3];
   for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
-  double lrho = 0.0, lsd = 0.0, lcr[4] = {0, 0, 0, 0};
-  // ---- face integral
+  // ---- face integral (f_rhs3): transpose of f = (P3, P4) + u* P0 - (P1, P2),
+  // fe = u* . f, tw = u* . t per boundary node; the adjoints of the node
+  // partial sums P0..P4 go to a.lP for the corner pass's transpose, those of
+  // u* to pbuf, those of the mass-flux weights t to the face vectors
   for (int k = 0; k < 9; k++) {
+    if (k == 8) {
+      for (int v = 2; v < 6; v++) a.pbuf[(v * 9 + k) * nq + iq] = 0.0;
+      for (int v = 0; v < 5; v++) a.lP[(v * 9 + k) * nq + iq] = 0.0;
+      continue;
+    }
     double b[6];
     node_basis2(G, k, b);
-    double st[4];
-    for (int q = 0; q < 4; q++) {
-      double acc = 0.0;
-      for (int kk = 0; kk < 6; kk++)
-        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
-      st[q] = acc;
-    }
-    const double rhovt = 1.0 / st[0];
-    const double ke = st[3] - 0.5 * (st[1] * st[1] + st[2] * st[2]);
     const int pn = d.ipq[k * d.nquad + iq];
-    const double dux = d.us[pn] - st[1], duy = d.vs[pn] - st[2];
     const double un = d.us_new[pn], vn = d.vs_new[pn];
-    const double du0 = un - st[1], du1 = vn - st[2];
+    double tx, ty;
+    mass_flux_weights(L, k, tx, ty);
+    const double P0 = d.npart[(0 * 9 + k) * nq + iq], P1 = d.npart[(1 * 9 + k) * nq + iq];
+    const double P2 = d.npart[(2 * 9 + k) * nq + iq], P3 = d.npart[(3 * 9 + k) * nq + iq];
+    const double P4 = d.npart[(4 * 9 + k) * nq + iq];
+    const double f0 = P3 + (un * P0 - P1), f1 = P4 + (vn * P0 - P2);
     double ltw = 0, lf0 = 0, lf1 = 0, lfe = 0;
     for (int kk = 0; kk < 6; kk++) {
       ltw += lR[0][kk] * b[kk];
@@ -1478,48 +1499,27 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
       lf1 += lR[2][kk] * b[kk];
       lfe += lR[3][kk] * b[kk];
     }
-    double lun = 0, lvn = 0, ldu0 = 0, ldu1 = 0, ldux = 0, lduy = 0, lst1 = 0, lst2 = 0, lrhovt = 0, lke = 0;
-    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
-      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
-      const double ci = d.corr[isg * nq + iq];
-      const double pe = (g - 1.0) * (rhovt + ci) * ke;
-      const double pv = fmax(eps, pe);
-      const double wq = wmom(isg, ivsg);
-      double lpv = 0.0;
-      for (int f = 0; f < 2; f++) {
-        double ax, ay;
-        corner_an(L.X, L.Y, isg, ivsg, f, ax, ay);
-        const double w = wrie(isg, ivsg, f), wm2 = 2.0 * wmas(isg, ivsg, f);
-        const double m = corner_m(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w);
-        const double pw = -2.0 * pv * w;
-        const double fs0 = pw * ax + m * du0, fs1 = pw * ay + m * du1;
-        double lfs0 = lf0 * wq + lfe * wq * un, lfs1 = lf1 * wq + lfe * wq * vn;
-        lun += lfe * wq * fs0 + ltw * wm2 * ax;
-        lvn += lfe * wq * fs1 + ltw * wm2 * ay;
-        double lax = ltw * wm2 * un + lfs0 * pw, lay = ltw * wm2 * vn + lfs1 * pw;
-        const double lpw = lfs0 * ax + lfs1 * ay;
-        const double lm = lfs0 * du0 + lfs1 * du1;
-        ldu0 += lfs0 * m;
-        ldu1 += lfs1 * m;
-        lpv += -2.0 * w * lpw;
-        corner_m_T(rhoct, sdctr, d.cimpd, slpdu, dux, duy, ax, ay, w, lm, lrho, lsd, ldux, lduy, lax, lay);
-        corner_an_T(isg, ivsg, f, lax, lay, lX, lY);
-      }
-      if (pe > eps) {
-        lrhovt += lpv * (g - 1.0) * ke;
-        add4(lcr, isg, lpv * (g - 1.0) * ke);
-        lke += lpv * (g - 1.0) * (rhovt + ci);
-      }
-    }
-    lun += ldu0;
-    lvn += ldu1;
-    lst1 -= ldu0 + ldux;
-    lst2 -= ldu1 + lduy;
-    a.pbuf[(2 * 9 + k) * nq + iq] = ldux;
-    a.pbuf[(3 * 9 + k) * nq + iq] = lduy;
+    lf0 += lfe * un;
+    lf1 += lfe * vn;
+    const double lun = lfe * f0 + lf0 * P0 + ltw * tx;
+    const double lvn = lfe * f1 + lf1 * P0 + ltw * ty;
+    a.lP[(0 * 9 + k) * nq + iq] = lf0 * un + lf1 * vn;
+    a.lP[(1 * 9 + k) * nq + iq] = -lf0;
+    a.lP[(2 * 9 + k) * nq + iq] = -lf1;
+    a.lP[(3 * 9 + k) * nq + iq] = lf0;
+    a.lP[(4 * 9 + k) * nq + iq] = lf1;
+    a.pbuf[(2 * 9 + k) * nq + iq] = 0.0;
+    a.pbuf[(3 * 9 + k) * nq + iq] = 0.0;
     a.pbuf[(4 * 9 + k) * nq + iq] = lun;
     a.pbuf[(5 * 9 + k) * nq + iq] = lvn;
-    vertex_T(b, d.mdegr, st, lrhovt, lke, lst1, lst2, lu);
+    // t = sum over the node's outer corner faces of 2 w_mass,f an_f
+    const double ltx = ltw * un, lty = ltw * vn;
+    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
+      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
+      for (int f = 0; f < 2; f++)
+        if (wmas(isg, ivsg, f) != 0.0)
+          corner_an_T(isg, ivsg, f, ltx * (2.0 * wmas(isg, ivsg, f)), lty * (2.0 * wmas(isg, ivsg, f)), lX, lY);
+    }
   }
   vol_T<R>(L, G, u, lR, g, eps, lu, lX, lY);
   // ---- Taylor-Green source: cos and sin of pi x at the Gauss points by angle
@@ -1528,7 +1528,7 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
   for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
   if (d.ncase == 1) {
     double xp[9][2], c[36], D[16];
-    node_xy(L, xp);
+    node_xy_rel(L, xp);
     cross36(xp, c);
     detpoly(c, D);
     const double PI = 3.14159265358979311599796346854;
@@ -1616,14 +1616,12 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     detpoly_T(lD, lc36);
     cross36_T(xp, lc36, lxp);
   }
-  centre_T(u, g, lrho, lsd, lu);
   const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
   const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
   for (int k = 0; k < 9; k++) {
     a.pbuf[(0 * 9 + k) * nq + iq] = lxp[k][0] + lX[A[k]][B[k]];
     a.pbuf[(1 * 9 + k) * nq + iq] = lxp[k][1] + lY[A[k]][B[k]];
   }
-  for (int isg = 0; isg < 4; isg++) a.lcorr[isg * nq + iq] = lcr[isg];
   for (int q = 0; q < 4; q++)
     for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu[q][k];
 }
