@@ -601,7 +601,7 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   A(&h->stage_u, NU * (size_t)ncell); A(&h->stage_x, 2 * (size_t)np); A(&h->stage_v, 2 * (size_t)np);
   int *ptr2_d, *slot_d;
   A(&ptr2_d, cnt2.size()); A(&slot_d, slots.size());
-  A(&d.npart, 45 * (size_t)nq); A(&d.corr, 4 * (size_t)nq); A(&d.us_new, np); A(&d.vs_new, np);
+  A(&d.npart, 45 * (size_t)nq); A(&d.corr, 4 * (size_t)nq); A(&d.src, 6 * (size_t)nq); A(&d.us_new, np); A(&d.vs_new, np);
   A(&d.wmom, 9 * (size_t)nq);
   int *ipt_d;
   A(&ipt_d, ipt.size()); A(&d.tmsub, 4 * (size_t)nt); A(&d.tcf, 5 * 24 * (size_t)nt); A(&d.tpart, 5 * 6 * (size_t)nt);

@@ -66,6 +66,7 @@ struct Dev {
   const int *node_slot;    // iq*9 + k: quad iq touches the node as its node k, cells ascending
   double *npart;           // [5][9][nquad] per-cell node partial sums (m, m*u, m*v, s_x, s_y)
   double *corr;            // [4][nquad] sub-cell density corrections
+  double *src;             // [6][nquad] Taylor-Green source moments of the stage (corner pass -> RHS pass)
   double *us_new, *vs_new; // ustar of the current stage (us, vs hold the previous one)
   double *wmom;            // [9][nquad] time-invariant mass-weighted shape moments
   // triangles (cells 0..ntria-1)

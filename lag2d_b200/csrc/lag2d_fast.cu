@@ -15,6 +15,7 @@
 //    RHS pass recomputes the cheap corner data instead of reading it back;
 //  * in RK stages 2 and 3 the mass-matrix solve and RK combine are fused into
 //    the RHS pass.
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -272,6 +273,13 @@ __host__ __device__ __forceinline__ void node_xy_rel(const Loaded &L, double (*x
   }
 }
 
+// cross36 of centre-relative coordinates (xp[8] = 0): the 8 products with
+// the centre node vanish and are zero constants here, so the tables fold them
+__host__ __device__ __forceinline__ void cross36_rel(const double (*xp)[2], double *c) {
+  cross36(xp, c);
+  c[7] = 0.0; c[14] = 0.0; c[20] = 0.0; c[25] = 0.0; c[29] = 0.0; c[32] = 0.0; c[34] = 0.0; c[35] = 0.0;
+}
+
 // node coordinates back in the reference node order
 __host__ __device__ __forceinline__ void node_xy(const Loaded &L, double (*xp)[2]) {
   const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
@@ -302,7 +310,7 @@ __host__ __device__ void f_persson(const Dev &d, int iq) {
   {
     double xp[9][2];
     node_xy_rel(L, xp);
-    cross36(xp, c);
+    cross36_rel(xp, c);
   }
   detpoly(c, D);
   const CellGeo g{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
@@ -375,6 +383,88 @@ __host__ __device__ void f_persson(const Dev &d, int iq) {
   }
 }
 
+// Taylor-Green source moments el[k] += sum_g src(x_g) b_k(g) detJ_g w_g over
+// the 5x5 Gauss points.  cos(pi x) at the points by angle addition from the
+// centre node x_c: cos(pi x) = cos(pi x_c) cos(pi d) - sin(pi x_c) sin(pi d),
+// d = x - x_c, with the NSER-term series of cossin_pi_series when every node
+// of the cell lies within delta of the centre node in x and y (the quadratic
+// map then keeps |d| <= 1.5625 delta at the Gauss points): delta <= 0.09 for
+// 7 terms, 0.004 for 4, 0.0006 for 3; otherwise (NSER = 0) cospi at each
+// point.  The point loop has no branch.  The basis sums are taken per row:
+// b_k along a row is a polynomial in ds of degree <= 2.
+template <int NSER>
+__host__ __device__ __forceinline__ void tgv_source_rows(const Loaded &L, const CellGeo &G, const double D[16],
+                                                         double g, double el[6]) {
+  const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
+  const double xc = L.X[1][1], yc = L.Y[1][1];
+  const double cxc = cospi(xc), sxc = sinpi(xc), cyc = cospi(yc), syc = sinpi(yc);
+#pragma unroll 1
+  for (int i = 0; i < 5; i++) {
+    const double r = g5p(i), dr = r - G.rc;
+    double lr[3];
+    lag3(r, lr);
+    double Px[3], Py[3];
+#pragma unroll
+    for (int bb = 0; bb < 3; bb++) {
+      Px[bb] = lr[0] * (L.X[0][bb] - xc) + lr[1] * (L.X[1][bb] - xc) + lr[2] * (L.X[2][bb] - xc);
+      Py[bb] = lr[0] * (L.Y[0][bb] - yc) + lr[1] * (L.Y[1][bb] - yc) + lr[2] * (L.Y[2][bb] - yc);
+    }
+    double e[4];
+#pragma unroll
+    for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
+    const double wi = coef * g5w(i);
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const double s = g5p(j), ds = s - G.sc;
+      double ls[3];
+      lag3(s, ls);
+      const double dx = Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2];
+      const double dy = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
+      const double djaco = wi * g5w(j) * (e[0] + s * (e[1] + s * (e[2] + s * e[3])));
+      double cx, cy;
+      if (NSER > 0) {
+        double cdx, sdx, cdy, sdy;
+        cossin_pi_series<NSER>(dx, cdx, sdx);
+        cossin_pi_series<NSER>(dy, cdy, sdy);
+        cx = cxc * cdx - sxc * sdx;
+        cy = cyc * cdy - syc * sdy;
+      } else {
+        cx = cospi(xc + dx);
+        cy = cospi(yc + dy);
+      }
+      const double c3x = cx * (4.0 * cx * cx - 3.0), c3y = cy * (4.0 * cy * cy - 3.0);
+      const double src = (c3x * cy - c3y * cx) * djaco;
+      m0 += src;
+      m1 += src * ds;
+      m2 += src * ds * ds;
+    }
+    // b = (1, dr, ds, dr^2/2 - g19, ds^2/2 - g20, dr ds - g21) along the row
+    el[0] += m0;
+    el[1] += m0 * dr;
+    el[2] += m1;
+    el[3] += m0 * (0.5 * dr * dr - G.g19);
+    el[4] += 0.5 * m2 - G.g20 * m0;
+    el[5] += m1 * dr - G.g21 * m0;
+  }
+}
+__host__ __device__ __forceinline__ void tgv_source(const Loaded &L, const CellGeo &G, const double D[16], double g,
+                                                    double el[6]) {
+  double mx = 0.0, my = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      mx = fmax(mx, fabs(L.X[a][b] - L.X[1][1]));
+      my = fmax(my, fabs(L.Y[a][b] - L.Y[1][1]));
+    }
+  const double delta = fmax(mx, my);
+  if (delta <= 0.0006) tgv_source_rows<3>(L, G, D, g, el);
+  else if (delta <= 0.004) tgv_source_rows<4>(L, G, D, g, el);
+  else if (delta <= 0.09) tgv_source_rows<7>(L, G, D, g, el);
+  else tgv_source_rows<0>(L, G, D, g, el);
+}
+
 // ---------------------------------------------------------------------------
 // Corner pass: node partial sums of the Riemann coefficients + sub-cell
 // density corrections (getriem_quadsubg2 with getrhosubg_averg/_daverg)
@@ -396,7 +486,7 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
   {
     double xp[9][2];
     node_xy_rel(L, xp);
-    cross36(xp, c);
+    cross36_rel(xp, c);
   }
   detpoly(c, D);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
@@ -452,7 +542,19 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
     corr[isg] = d.cdrho * (unksgq - (rtc * num) / (den * volel));
     d.corr[isg * (size_t)d.nquad + iq] = corr[isg];
   }
-  if (PART == 1) return;
+  if (PART == 1) {
+    // Taylor-Green energy source of the stage (rhsdomnsrcdg_lag_curvquad,
+    // Getrhslag.f90:4070-4251): it depends on the stage's nodes and the
+    // reference geometry only, and this kernel has the det J coefficients;
+    // the RHS pass adds the 6 moments
+    if (d.ncase == 1) {
+      double el[6] = {0, 0, 0, 0, 0, 0};
+      tgv_source(L, G, D, g, el);
+#pragma unroll
+      for (int k = 0; k < 6; k++) d.src[k * (size_t)d.nquad + iq] = el[k];
+    }
+    return;
+  }
   // per node: vertex state, then its corner faces in the reference's order
 #pragma unroll
   for (int k = 0; k < 9; k++) {
@@ -543,87 +645,6 @@ __host__ __device__ void f_node(const Dev &d, int p) {
 // RHS pass: corner forces + face integral + volume integral (+ source), and
 // in stages 2 and 3 the M^-1 solve and RK combine
 // ---------------------------------------------------------------------------
-// Taylor-Green source moments el[k] += sum_g src(x_g) b_k(g) detJ_g w_g over
-// the 5x5 Gauss points.  cos(pi x) at the points by angle addition from the
-// centre node x_c: cos(pi x) = cos(pi x_c) cos(pi d) - sin(pi x_c) sin(pi d),
-// d = x - x_c, with the NSER-term series of cossin_pi_series when every node
-// of the cell lies within delta of the centre node in x and y (the quadratic
-// map then keeps |d| <= 1.5625 delta at the Gauss points): delta <= 0.09 for
-// 7 terms, 0.004 for 4, 0.0006 for 3; otherwise (NSER = 0) cospi at each
-// point.  The point loop has no branch.  The basis sums are taken per row:
-// b_k along a row is a polynomial in ds of degree <= 2.
-template <int NSER>
-__host__ __device__ __forceinline__ void tgv_source_rows(const Loaded &L, const CellGeo &G, const double D[16],
-                                                         double g, double el[6]) {
-  const double coef = 0.25 * 3.14159265358979311599796346854 / (g - 1.0);
-  const double xc = L.X[1][1], yc = L.Y[1][1];
-  const double cxc = cospi(xc), sxc = sinpi(xc), cyc = cospi(yc), syc = sinpi(yc);
-#pragma unroll 1
-  for (int i = 0; i < 5; i++) {
-    const double r = g5p(i), dr = r - G.rc;
-    double lr[3];
-    lag3(r, lr);
-    double Px[3], Py[3];
-#pragma unroll
-    for (int bb = 0; bb < 3; bb++) {
-      Px[bb] = lr[0] * (L.X[0][bb] - xc) + lr[1] * (L.X[1][bb] - xc) + lr[2] * (L.X[2][bb] - xc);
-      Py[bb] = lr[0] * (L.Y[0][bb] - yc) + lr[1] * (L.Y[1][bb] - yc) + lr[2] * (L.Y[2][bb] - yc);
-    }
-    double e[4];
-#pragma unroll
-    for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
-    const double wi = coef * g5w(i);
-    double m0 = 0.0, m1 = 0.0, m2 = 0.0;
-#pragma unroll
-    for (int j = 0; j < 5; j++) {
-      const double s = g5p(j), ds = s - G.sc;
-      double ls[3];
-      lag3(s, ls);
-      const double dx = Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2];
-      const double dy = Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2];
-      const double djaco = wi * g5w(j) * (e[0] + s * (e[1] + s * (e[2] + s * e[3])));
-      double cx, cy;
-      if (NSER > 0) {
-        double cdx, sdx, cdy, sdy;
-        cossin_pi_series<NSER>(dx, cdx, sdx);
-        cossin_pi_series<NSER>(dy, cdy, sdy);
-        cx = cxc * cdx - sxc * sdx;
-        cy = cyc * cdy - syc * sdy;
-      } else {
-        cx = cospi(xc + dx);
-        cy = cospi(yc + dy);
-      }
-      const double c3x = cx * (4.0 * cx * cx - 3.0), c3y = cy * (4.0 * cy * cy - 3.0);
-      const double src = (c3x * cy - c3y * cx) * djaco;
-      m0 += src;
-      m1 += src * ds;
-      m2 += src * ds * ds;
-    }
-    // b = (1, dr, ds, dr^2/2 - g19, ds^2/2 - g20, dr ds - g21) along the row
-    el[0] += m0;
-    el[1] += m0 * dr;
-    el[2] += m1;
-    el[3] += m0 * (0.5 * dr * dr - G.g19);
-    el[4] += 0.5 * m2 - G.g20 * m0;
-    el[5] += m1 * dr - G.g21 * m0;
-  }
-}
-__host__ __device__ __forceinline__ void tgv_source(const Loaded &L, const CellGeo &G, const double D[16], double g,
-                                                    double el[6]) {
-  double mx = 0.0, my = 0.0;
-#pragma unroll
-  for (int a = 0; a < 3; a++)
-#pragma unroll
-    for (int b = 0; b < 3; b++) {
-      mx = fmax(mx, fabs(L.X[a][b] - L.X[1][1]));
-      my = fmax(my, fabs(L.Y[a][b] - L.Y[1][1]));
-    }
-  const double delta = fmax(mx, my);
-  if (delta <= 0.0006) tgv_source_rows<3>(L, G, D, g, el);
-  else if (delta <= 0.004) tgv_source_rows<4>(L, G, D, g, el);
-  else if (delta <= 0.09) tgv_source_rows<7>(L, G, D, g, el);
-  else tgv_source_rows<0>(L, G, D, g, el);
-}
 
 // The momentum and energy face weights of rhsifacedg_lagsubgq2 are 1 on every
 // corner entry of the 8 boundary nodes of the quad and 0 on the 4 entries of
@@ -684,10 +705,30 @@ __host__ __device__ __forceinline__ void mass_flux_weights(const Loaded &L, int 
 // data are not recomputed here: 40 partials and the 8 boundary nodes'
 // velocities replace the 32 corner faces' vertex states, impedances and
 // forces (same sums up to rounding and summation order).
-__host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa) {
+//
+// Staging: the cell's DOFs U^(s) (24 values) and, for the fused update, M^-1
+// (16) and U^n (24) are copied asynchronously (cp.async) into this thread's
+// column of shared memory (stride kRhsBlock) when the thread starts, so their
+// load latency overlaps the face integral and they are read from shared
+// memory where used instead of being held in registers.
+constexpr int kRhsBlock = 128;
+constexpr int kRhsStage = 64;
+__device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, double *col) {
   if (iq >= d.nquad || d.sc_dev->done) return;
   const int e = iq + d.ntria;
   const double eps = 1.0e-6, g = d.gamlg;
+  {
+    const size_t nc = d.ncell;
+    for (int v = 0; v < 24; v++) __pipeline_memcpy_async(col + v * kRhsBlock, d.Us + v * nc + e, sizeof(double));
+    if (fuse_update) {
+      for (int i = 0; i < 16; i++)
+        __pipeline_memcpy_async(col + (24 + i) * kRhsBlock, d.amatr + i * nc + e, sizeof(double));
+      for (int v = 0; v < 24; v++)
+        __pipeline_memcpy_async(col + (40 + v) * kRhsBlock, d.Un + v * nc + e, sizeof(double));
+    }
+    __pipeline_commit();
+  }
+#define RHS_U(q, k) col[((q) * 6 + (k)) * kRhsBlock]
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
@@ -716,8 +757,7 @@ __host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double al
       el[kk] += fe * b[kk];
     }
   }
-  double u[4][6];
-  load_u(d, d.Us, e, u);
+  __pipeline_wait_prior(0);
   // volume integral on the 5x5 Gauss-Lobatto grid (cofactor form), sum
   // factorised row by row: for fixed r_i, Q_b = sum_a L'_a(r_i) X[a][b] and
   // P_b = sum_a L_a(r_i) X[a][b] give dx/dr and dx/ds along the row
@@ -739,8 +779,9 @@ __host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double al
     double ra[4], rb[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      ra[q] = u[q][0] + u[q][1] * dr + u[q][3] * (0.5 * dr * dr - G.g19) - u[q][4] * G.g20 - u[q][5] * G.g21;
-      rb[q] = u[q][2] + u[q][5] * dr;
+      ra[q] = RHS_U(q, 0) + RHS_U(q, 1) * dr + RHS_U(q, 3) * (0.5 * dr * dr - G.g19) - RHS_U(q, 4) * G.g20 -
+              RHS_U(q, 5) * G.g21;
+      rb[q] = RHS_U(q, 2) + RHS_U(q, 5) * dr;
     }
     const double wi = l5w(i);
     // 1/tau at the row's 5 points with one division (batched reciprocals:
@@ -751,7 +792,7 @@ __host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double al
 #pragma unroll
       for (int j = 0; j < 5; j++) {
         const double ds = l5p(j) - G.sc;
-        tq[j] = ra[0] + ds * (rb[0] + 0.5 * u[0][4] * ds);
+        tq[j] = ra[0] + ds * (rb[0] + 0.5 * RHS_U(0, 4) * ds);
         pre[j] = j == 0 ? tq[0] : pre[j - 1] * tq[j];
       }
       double inv = 1.0 / pre[4];
@@ -775,7 +816,7 @@ __host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double al
       const double ys = Py[0] * dls[0] + Py[1] * dls[1] + Py[2] * dls[2];
       double un[4];
 #pragma unroll
-      for (int q = 1; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * u[q][4] * ds);
+      for (int q = 1; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * RHS_U(q, 4) * ds);
       const double rhoad = rtau[j];
       const double pres = fmax(eps, (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2])));
       // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
@@ -798,16 +839,9 @@ __host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double al
     }
   }
   if (d.ncase == 1) {
-    // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:
-    // 4070-4251), 5x5 Gauss; cos(3t) = cos t (4 cos^2 t - 3).
-    double c[36], D[16];
-    {
-      double xp[9][2];
-      node_xy_rel(L, xp);
-      cross36(xp, c);
-    }
-    detpoly(c, D);
-    tgv_source(L, G, D, g, el);
+    // Taylor-Green energy source, computed by the corner pass (k_corner2_corr)
+#pragma unroll
+    for (int k = 0; k < 6; k++) el[k] += d.src[k * (size_t)d.nquad + iq];
   }
   if (!fuse_update) {
 #pragma unroll
@@ -821,9 +855,8 @@ __host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double al
   }
   // fused stage update (Getrhslag.f90:1789-1904)
   const double dt = d.sc_dev->dtfix;
-  double am[16];
-#pragma unroll
-  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * (size_t)d.ncell + e];
+#define RHS_AM(i) col[(24 + (i)) * kRhsBlock]
+#define RHS_UN(v) col[(40 + (v)) * kRhsBlock]
   double R[4][6];
 #pragma unroll
   for (int k = 0; k < 6; k++) {
@@ -838,17 +871,20 @@ __host__ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double al
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const size_t base = (size_t)(q * 6) * d.ncell + e;
-    const double d0 = am[15] * R[q][0];
-    d.Us[base] = alfa * d.Un[base] + oma * (u[q][0] + d0);
+    const double d0 = RHS_AM(15) * R[q][0];
+    d.Us[base] = alfa * RHS_UN(q * 6) + oma * (RHS_U(q, 0) + d0);
 #pragma unroll
     for (int i = 0; i < 5; i++) {
       double acc = 0.0;
 #pragma unroll
-      for (int j = 0; j < 5; j++) acc += am[IDX[i][j]] * R[q][j + 1];
+      for (int j = 0; j < 5; j++) acc += RHS_AM(IDX[i][j]) * R[q][j + 1];
       const size_t idx = base + (size_t)(i + 1) * d.ncell;
-      d.Us[idx] = alfa * d.Un[idx] + oma * (u[q][i + 1] + acc);
+      d.Us[idx] = alfa * RHS_UN(q * 6 + i + 1) + oma * (RHS_U(q, i + 1) + acc);
     }
   }
+#undef RHS_U
+#undef RHS_AM
+#undef RHS_UN
 }
 
 // getdelt_lag's per-quad limits (Getrhslag.f90:20641-20700) before the RHS
@@ -926,7 +962,7 @@ __host__ __device__ void f_geom(const Dev &d, int iq, int fix_centre) {
   {
     double xp[9][2];
     node_xy_rel(L, xp);
-    cross36(xp, c);
+    cross36_rel(xp, c);
   }
   detpoly(c, D);
   const double vol = cell_area(D);
@@ -950,7 +986,7 @@ __host__ __device__ void f_init_wmom(const Dev &d, int iq) {
   {
     double xp[9][2];
     node_xy_rel(L, xp);
-    cross36(xp, c);
+    cross36_rel(xp, c);
   }
   detpoly(c, D);
   // initial density of the reference cases is uniform per cell
@@ -1149,7 +1185,7 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   load_cell(d, d.xs, d.ys, iq, L);
   double xp[9][2], c[36], D[16];
   node_xy_rel(L, xp);
-  cross36(xp, c);
+  cross36_rel(xp, c);
   detpoly(c, D);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
   double u[4][6];
@@ -1529,7 +1565,7 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
   if (d.ncase == 1) {
     double xp[9][2], c[36], D[16];
     node_xy_rel(L, xp);
-    cross36(xp, c);
+    cross36_rel(xp, c);
     detpoly(c, D);
     const double PI = 3.14159265358979311599796346854;
     const double coef = 0.25 * PI / (g - 1.0);
@@ -1790,8 +1826,9 @@ __global__ void __launch_bounds__(128, 4) k_corner2_faces(Dev d) {
   f_corner_t<2>(d, blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void k_node2(Dev d) { f_node(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128, 3) k_rhs3(Dev d, int fuse, double alfa) {
-  f_rhs3(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa);
+__global__ void __launch_bounds__(kRhsBlock, 3) k_rhs3(Dev d, int fuse, double alfa) {
+  extern __shared__ double rhs_stage[];
+  f_rhs3(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa, rhs_stage + threadIdx.x);
 }
 // per-block minima of getdelt_lag's two limits (consumed by k_dt_final)
 __global__ void __launch_bounds__(256) k_dt2_partial(Dev d) {
@@ -1895,7 +1932,14 @@ void launch_fast_corner(const Dev &d, cudaStream_t st) {
 }
 void launch_fast_node(const Dev &d, cudaStream_t st) { fast::k_node2<<<fast::nb(d.npoin, 256), 256, 0, st>>>(d); }
 void launch_fast_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa) {
-  fast::k_rhs3<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d, fuse, alfa);
+  constexpr int smem = fast::kRhsStage * fast::kRhsBlock * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(fast::k_rhs3, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(fast::k_rhs3, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    attr = true;
+  }
+  fast::k_rhs3<<<fast::nb(d.nquad, fast::kRhsBlock), fast::kRhsBlock, smem, st>>>(d, fuse, alfa);
 }
 void launch_dt_final(const Dev &d, cudaStream_t st, int nblk, int ndt);  // lag2d_kernels.cu
 void launch_fast_dt(const Dev &d, cudaStream_t st, int ndt) {
