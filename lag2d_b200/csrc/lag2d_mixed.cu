@@ -24,6 +24,7 @@
 // corner forces of the surrounding cells cancel to FP64 rounding: momentum
 // and total energy are conserved to FP64 round-off, as in the FP64 step.
 // Storage (DOFs, M^-1, geometry, nodes) stays FP64.
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -348,6 +349,57 @@ __device__ void m_corner(const Dev &d, int iq) {
     d.corr[isg * (size_t)d.nquad + iq] = cr;
     corr[isg] = (float)cr;
   }
+  if (d.ncase == 1) {
+    // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:4070-4251)
+    // in FP32, for the RHS pass (it depends on the stage's nodes only)
+    double el0 = 0.0;
+    float el[6] = {0, 0, 0, 0, 0, 0};
+    // det J coefficients D, Df and the centre-relative nodes come from above
+    float Xf[3][3], Yf[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        Xf[a][bb] = (float)L.X[a][bb];
+        Yf[a][bb] = (float)L.Y[a][bb];
+      }
+    const float coef = (float)(0.25 * 3.14159265358979311599796346854 / (d.gamlg - 1.0));
+    const float oxf = (float)L.ox, oyf = (float)L.oy;
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) {
+      const float r = g5p(i), dr = r - G.rc;
+      float lr[3];
+      lag3f(r, lr);
+      float Px[3], Py[3];
+#pragma unroll
+      for (int bb = 0; bb < 3; bb++) {
+        Px[bb] = lr[0] * Xf[0][bb] + lr[1] * Xf[1][bb] + lr[2] * Xf[2][bb];
+        Py[bb] = lr[0] * Yf[0][bb] + lr[1] * Yf[1][bb] + lr[2] * Yf[2][bb];
+      }
+      const float wi = g5w(i);
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const float s = g5p(j), ds = s - G.sc;
+        float ls[3];
+        lag3f(s, ls);
+        const float xg = oxf + (Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2]);
+        const float yg = oyf + (Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2]);
+        const float djaco = wi * g5w(j) * detevalf(Df, r, s);
+        const float cx = cospif(xg), cy = cospif(yg);
+        const float c3x = cx * (4.0f * cx * cx - 3.0f), c3y = cy * (4.0f * cy * cy - 3.0f);
+        const float src = coef * (c3x * cy - c3y * cx) * djaco;
+        el0 += (double)src;
+        el[1] += src * dr;
+        el[2] += src * ds;
+        el[3] += src * (0.5f * dr * dr - G.g19);
+        el[4] += src * (0.5f * ds * ds - G.g20);
+        el[5] += src * (dr * ds - G.g21);
+      }
+    }
+    d.src[(size_t)iq] = el0;
+#pragma unroll
+    for (int k = 1; k < 6; k++) d.src[k * (size_t)d.nquad + iq] = (double)el[k];
+  }
 #pragma unroll
   for (int k = 0; k < 9; k++) {
     float b[6], st[4];
@@ -396,10 +448,26 @@ __device__ void m_corner(const Dev &d, int iq) {
 // wrote (the momentum weights are 1 on the 8 boundary nodes and 0 at the
 // centre node), the energy term is u* . that sum and the mass term u* . sum_f
 // 2 w_mass,f an_f over the outer corner faces; see f_rhs3 in lag2d_fast.cu.
-__device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
+// The cell's U^(s), M^-1 and U^n are staged in shared memory by cp.async at
+// entry, as in the FP64 RHS kernel (thread column, stride kMxBlock).
+constexpr int kMxBlock = 128;
+constexpr int kMxStage = 64;
+__device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa, double *col) {
   if (iq >= d.nquad || d.sc_dev->done) return;
   const int e = iq + d.ntria;
   const float eps = 1.0e-6f, g = (float)d.gamlg;
+  {
+    const size_t nc = d.ncell;
+    for (int v = 0; v < 24; v++) __pipeline_memcpy_async(col + v * kMxBlock, d.Us + v * nc + e, sizeof(double));
+    if (fuse_update) {
+      for (int i = 0; i < 16; i++)
+        __pipeline_memcpy_async(col + (24 + i) * kMxBlock, d.amatr + i * nc + e, sizeof(double));
+      for (int v = 0; v < 24; v++)
+        __pipeline_memcpy_async(col + (40 + v) * kMxBlock, d.Un + v * nc + e, sizeof(double));
+    }
+    __pipeline_commit();
+  }
+#define MX_U(q, k) col[((q) * 6 + (k)) * kMxBlock]
   CellXY L;
   load_cell(d, iq, L, nullptr);
   const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
@@ -456,16 +524,12 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
       el[kk] += fef * b[kk];
     }
   }
-  double ud[3][6];  // tau, u, v in FP64 (tau equation)
+  __pipeline_wait_prior(0);
   float u[4][6];
 #pragma unroll
   for (int q = 0; q < 4; q++)
 #pragma unroll
-    for (int k = 0; k < 6; k++) {
-      const double v = d.Us[(q * 6 + k) * (size_t)d.ncell + e];
-      if (q < 3) ud[q][k] = v;
-      u[q][k] = (float)v;
-    }
+    for (int k = 0; k < 6; k++) u[q][k] = (float)MX_U(q, k);
   // volume integral, 5x5 Gauss-Lobatto, cofactor form, sum-factorised rows:
   // Jacobian and velocity in FP64 (tau equation), pressure work in FP32
 #pragma unroll 1
@@ -483,6 +547,13 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
       Py[bb] = lr0 * L.Y[0][bb] + lr1 * L.Y[1][bb] + lr2 * L.Y[2][bb];
     }
     const float drf = (float)dr;
+    // FP64 velocities along the row: a + ds (b + c ds)
+    const double rau = MX_U(1, 0) + MX_U(1, 1) * dr + MX_U(1, 3) * (0.5 * dr * dr - g19) - MX_U(1, 4) * g20 -
+                       MX_U(1, 5) * g21;
+    const double rbu = MX_U(1, 2) + MX_U(1, 5) * dr, rcu = 0.5 * MX_U(1, 4);
+    const double rav = MX_U(2, 0) + MX_U(2, 1) * dr + MX_U(2, 3) * (0.5 * dr * dr - g19) - MX_U(2, 4) * g20 -
+                       MX_U(2, 5) * g21;
+    const double rbv = MX_U(2, 2) + MX_U(2, 5) * dr, rcv = 0.5 * MX_U(2, 4);
 #pragma unroll
     for (int j = 0; j < 5; j++) {
       const double s = l5pd(j);
@@ -495,8 +566,8 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
       const double xs = Px[0] * dls0 + Px[1] * dls1 + Px[2] * dls2;
       const double ys = Py[0] * dls0 + Py[1] * dls1 + Py[2] * dls2;
       const double b3 = 0.5 * dr * dr - g19, b4 = 0.5 * ds * ds - g20, b5 = dr * ds - g21;
-      const double uq = ud[1][0] + ud[1][1] * dr + ud[1][2] * ds + ud[1][3] * b3 + ud[1][4] * b4 + ud[1][5] * b5;
-      const double vq = ud[2][0] + ud[2][1] * dr + ud[2][2] * ds + ud[2][3] * b3 + ud[2][4] * b4 + ud[2][5] * b5;
+      const double uq = rau + ds * (rbu + rcu * ds);
+      const double vq = rav + ds * (rbv + rcv * ds);
       // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
       double gd0[5], gd1[5];
       gd0[0] = ys;       gd1[0] = -xs;
@@ -524,64 +595,10 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
     }
   }
   if (d.ncase == 1) {
-    // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:4070-4251)
-    double c[36], D[16];
-    {
-      const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
-      const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
-      double xp[9][2];
+    // Taylor-Green energy source (FP32), computed by the corner pass
+    el0 += d.src[(size_t)iq];
 #pragma unroll
-      for (int k = 0; k < 9; k++) {
-        xp[k][0] = L.X[A[k]][B[k]];
-        xp[k][1] = L.Y[A[k]][B[k]];
-      }
-      cross36(xp, c);
-    }
-    detpoly(c, D);
-    float Df[16];
-#pragma unroll
-    for (int t = 0; t < 16; t++) Df[t] = (float)D[t];
-    float Xf[3][3], Yf[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-      for (int bb = 0; bb < 3; bb++) {
-        Xf[a][bb] = (float)L.X[a][bb];
-        Yf[a][bb] = (float)L.Y[a][bb];
-      }
-    const float coef = (float)(0.25 * 3.14159265358979311599796346854 / (d.gamlg - 1.0));
-    const float oxf = (float)L.ox, oyf = (float)L.oy;
-#pragma unroll 1
-    for (int i = 0; i < 5; i++) {
-      const float r = g5p(i), dr = r - G.rc;
-      float lr[3];
-      lag3f(r, lr);
-      float Px[3], Py[3];
-#pragma unroll
-      for (int bb = 0; bb < 3; bb++) {
-        Px[bb] = lr[0] * Xf[0][bb] + lr[1] * Xf[1][bb] + lr[2] * Xf[2][bb];
-        Py[bb] = lr[0] * Yf[0][bb] + lr[1] * Yf[1][bb] + lr[2] * Yf[2][bb];
-      }
-      const float wi = g5w(i);
-#pragma unroll
-      for (int j = 0; j < 5; j++) {
-        const float s = g5p(j), ds = s - G.sc;
-        float ls[3];
-        lag3f(s, ls);
-        const float xg = oxf + (Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2]);
-        const float yg = oyf + (Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2]);
-        const float djaco = wi * g5w(j) * detevalf(Df, r, s);
-        const float cx = cospif(xg), cy = cospif(yg);
-        const float c3x = cx * (4.0f * cx * cx - 3.0f), c3y = cy * (4.0f * cy * cy - 3.0f);
-        const float src = coef * (c3x * cy - c3y * cx) * djaco;
-        el0 += (double)src;
-        el[1] += src * dr;
-        el[2] += src * ds;
-        el[3] += src * (0.5f * dr * dr - G.g19);
-        el[4] += src * (0.5f * ds * ds - G.g20);
-        el[5] += src * (dr * ds - G.g21);
-      }
-    }
+    for (int k = 1; k < 6; k++) el[k] += (float)d.src[k * (size_t)d.nquad + iq];
   }
   double R[4][6];
   R[1][0] = pa0;
@@ -604,29 +621,32 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa) {
   }
   // fused stage update in FP64 (Getrhslag.f90:1789-1904)
   const double dt = d.sc_dev->dtfix;
-  double am[16];
-#pragma unroll
-  for (int i = 0; i < 16; i++) am[i] = d.amatr[i * (size_t)d.ncell + e];
+#define MX_AM(i) col[(24 + (i)) * kMxBlock]
+#define MX_UN(v) col[(40 + (v)) * kMxBlock]
   const double oma = 1.0 - alfa;
   const int IDX[5][5] = {{0, 1, 2, 3, 4}, {1, 5, 6, 7, 8}, {2, 6, 9, 10, 11}, {3, 7, 10, 12, 13}, {4, 8, 11, 13, 14}};
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const size_t base = (size_t)(q * 6) * d.ncell + e;
-    d.Us[base] = alfa * d.Un[base] + oma * (d.Us[base] + am[15] * (dt * R[q][0]));
+    d.Us[base] = alfa * MX_UN(q * 6) + oma * (MX_U(q, 0) + MX_AM(15) * (dt * R[q][0]));
 #pragma unroll
     for (int i = 0; i < 5; i++) {
       double acc = 0.0;
 #pragma unroll
-      for (int j = 0; j < 5; j++) acc += am[IDX[i][j]] * (dt * R[q][j + 1]);
+      for (int j = 0; j < 5; j++) acc += MX_AM(IDX[i][j]) * (dt * R[q][j + 1]);
       const size_t idx = base + (size_t)(i + 1) * d.ncell;
-      d.Us[idx] = alfa * d.Un[idx] + oma * (d.Us[idx] + acc);
+      d.Us[idx] = alfa * MX_UN(q * 6 + i + 1) + oma * (MX_U(q, i + 1) + acc);
     }
   }
+#undef MX_U
+#undef MX_AM
+#undef MX_UN
 }
 
-__global__ void __launch_bounds__(128) k_corner_mx(Dev d) { m_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128) k_rhs_mx(Dev d, int fuse, double alfa) {
-  m_rhs(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa);
+__global__ void __launch_bounds__(128, 3) k_corner_mx(Dev d) { m_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(kMxBlock, 3) k_rhs_mx(Dev d, int fuse, double alfa) {
+  extern __shared__ double mx_stage[];
+  m_rhs(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa, mx_stage + threadIdx.x);
 }
 
 static inline int nb(int n, int b) { return (n + b - 1) / b; }
@@ -637,7 +657,14 @@ void launch_mixed_corner(const Dev &d, cudaStream_t st) {
   mixed::k_corner_mx<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d);
 }
 void launch_mixed_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa) {
-  mixed::k_rhs_mx<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d, fuse, alfa);
+  constexpr int smem = mixed::kMxStage * mixed::kMxBlock * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(mixed::k_rhs_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(mixed::k_rhs_mx, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    attr = true;
+  }
+  mixed::k_rhs_mx<<<mixed::nb(d.nquad, mixed::kMxBlock), mixed::kMxBlock, smem, st>>>(d, fuse, alfa);
 }
 
 }  // namespace lag2d
