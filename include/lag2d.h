@@ -177,8 +177,11 @@ double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *lau
  * lag2d_weno_linear describes, with no sensitivity through the node
  * positions), and the reference-configuration quantities (geoel fields 1-4
  * and 19-21, amatr, the initial sub-cell masses).  Marked cells whose
- * stencil is rejected keep their DOFs and are differentiated as such.  More
- * than 16384 WENO-limited quads in one stage return LAG2D_EUNSUP.  Gradients use the
+ * stencil is rejected keep their DOFs and are differentiated as such; a
+ * window in which the step reports LAG2D_ESTENCIL (a troubled quad left
+ * unlimited) is differentiated all the same and returns LAG2D_ESTENCIL with
+ * every output written.  More than 16384 WENO-limited quads in one stage
+ * return LAG2D_EUNSUP.  Gradients use the
  * layouts of lag2d_set_state: unkno(ndegr,nq,ncell), coord(2,npoin),
  * ustar(2,npoin).
  * ------------------------------------------------------------------------- */

@@ -273,10 +273,14 @@ class Lag2DSolver:
         J = ctypes.c_double(0.0)
         dt = ctypes.c_double(self.dtfix)
         ta = ctypes.c_double(self.tacru)
-        self._check(self.lib.lag2d_adjoint(self.h, ctypes.c_int(self.itime), ctypes.c_int(nsteps),
-                                           ctypes.c_int(checkpoint_every), ctypes.byref(dt), ctypes.byref(ta),
-                                           ctypes.byref(J), _p(gu, _dp), _p(gx, _dp), _p(gs, _dp),
-                                           _p(ms, _dp)))
+        rc = self.lib.lag2d_adjoint(self.h, ctypes.c_int(self.itime), ctypes.c_int(nsteps),
+                                    ctypes.c_int(checkpoint_every), ctypes.byref(dt), ctypes.byref(ta),
+                                    ctypes.byref(J), _p(gu, _dp), _p(gx, _dp), _p(gs, _dp), _p(ms, _dp))
+        # LAG2D_ESTENCIL (5) is a notice: a troubled quad was left unlimited, the
+        # window and its gradients are complete
+        self.stencil_notice = rc == 5
+        if rc != 5:
+            self._check(rc)
         self.dtfix, self.tacru = dt.value, ta.value
         self.itime += nsteps
         return J.value, gu, gx, gs, ms

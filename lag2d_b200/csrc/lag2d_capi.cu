@@ -1276,7 +1276,9 @@ int lag2d_adjoint_step(lag2d_handle *h, int itime, double *dtfix, double *tacru,
   Scalars fin;
   r = get_scalars(h, &fin);
   if (r) return r;
-  if (fin.status) return read_status(h);
+  // a broken state ends here; the stencil notice (a troubled quad left
+  // unlimited, the step complete) lets the reverse run and is returned last
+  if (fin.status & ST_NONPHYS) return read_status(h);
   r = put_adjoint(h, w.a, seed_unkno, seed_coord, seed_ustar);
   if (r) return r;
   // keep the step's outputs: the reverse pass overwrites the stage buffers
@@ -1293,6 +1295,8 @@ int lag2d_adjoint_step(lag2d_handle *h, int itime, double *dtfix, double *tacru,
   if (r) return r;
   *dtfix = fin.dtfix;
   *tacru = fin.tacru;
+  if (fin.status & ST_STENCIL)
+    return fail(LAG2D_ESTENCIL, "WENO left a troubled quad unlimited (vertex valence); step and gradients complete");
   return LAG2D_OK;
 }
 
@@ -1339,7 +1343,7 @@ int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every,
   Scalars fin;
   r = get_scalars(h, &fin);
   if (r) return r;
-  if (fin.status) return read_status(h);
+  if (fin.status & ST_NONPHYS) return read_status(h);
   if (fin.done && fin.itime != itime0 + nsteps - 1)
     return fail(LAG2D_EINVAL, "the window runs past tend (the steps after it are skipped)");
   // J and its seed dJ/dU = m (0, u, v, 0) in the cell-average modes
@@ -1388,6 +1392,8 @@ int lag2d_adjoint(lag2d_handle *h, int itime0, int nsteps, int checkpoint_every,
     ms[1] = t_rec;
     ms[2] = t_rev;
   }
+  if (fin.status & ST_STENCIL)
+    return fail(LAG2D_ESTENCIL, "WENO left a troubled quad unlimited (vertex valence); window and gradients complete");
   return LAG2D_OK;
 }
 

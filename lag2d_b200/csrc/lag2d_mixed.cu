@@ -311,6 +311,15 @@ __device__ void m_corner(const Dev &d, int iq) {
   for (int q = 0; q < 4; q++)
 #pragma unroll
     for (int k = 0; k < 6; k++) u[q][k] = (float)d.Us[(q * 6 + k) * (size_t)d.ncell + e];
+  // the velocity DOFs in FP64 as well: the node sums sum m u_vertex take the
+  // vertex velocities in FP64 (an FP32 vertex velocity's rounding, carried
+  // into u* tangentially, is amplified by the long faces of stretched cells)
+  double uvd[2][6];
+#pragma unroll
+  for (int q = 0; q < 2; q++)
+#pragma unroll
+    for (int k = 0; k < 6; k++) uvd[q][k] = d.Us[((q + 1) * 6 + k) * (size_t)d.ncell + e];
+  const double rcd = d.rc[e], scd = d.sc[e], g19d = d.g19[e], g20d = d.g20[e], g21d = d.g21[e];
   float rhoct, sdctr;
   centre_state(u, g, rhoct, sdctr);
   // sub-cell densities: initial mass / exact sub-cell area (FP64) against the
@@ -410,6 +419,19 @@ __device__ void m_corner(const Dev &d, int iq) {
     const int pn = d.ipq[k * d.nquad + iq];
     const float dux = (float)d.us[pn] - st[1];
     const float duy = (float)d.vs[pn] - st[2];
+    double st1d, st2d;
+    {
+      const double b1 = MD().xv[k] - rcd, b2 = MD().yv[k] - scd;
+      const double bd[6] = {1.0, b1, b2, 0.5 * b1 * b1 - g19d, 0.5 * b2 * b2 - g20d, b1 * b2 - g21d};
+      st1d = 0.0;
+      st2d = 0.0;
+#pragma unroll
+      for (int kk = 0; kk < 6; kk++)
+        if (kk < d.mdegr) {
+          st1d += uvd[0][kk] * bd[kk];
+          st2d += uvd[1][kk] * bd[kk];
+        }
+    }
     double P0 = 0.0, P1 = 0.0, P2 = 0.0, P3 = 0.0, P4 = 0.0;
 #pragma unroll
     for (int i = MT().nc_start[k]; i < MT().nc_start[k + 1]; i++) {
@@ -423,8 +445,8 @@ __device__ void m_corner(const Dev &d, int iq) {
         float m, sx, sy;
         corner_coeffs(ax, ay, MT().wrie[8 * isg + 2 * ivsg + f], pv, rhoct, sdctr, cimpd, slpdu, dux, duy, m, sx, sy);
         P0 += (double)m;
-        P1 += (double)m * (double)st[1];
-        P2 += (double)m * (double)st[2];
+        P1 += (double)m * st1d;
+        P2 += (double)m * st2d;
         P3 += (double)sx;
         P4 += (double)sy;
       }

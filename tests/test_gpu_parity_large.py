@@ -12,12 +12,17 @@ oracle after every step:
   * sedov_hybrid_jitter256   Sedov on the jittered 256x256 tri/quad mesh with
                 per-cell initial densities 1 + 0.01 N(0,1), 1 step
 
-Bounds: FP64 cell averages within 1e-12 relative of the oracle (relative to
-the field scale where a field crosses zero), dt within 1e-12, node positions
-within 1e-13 absolute; FP32-mixed cell averages within 1e-6, dt within 1e-6,
-node displacements within 1e-6 of the oracle's.  Where the configuration
-exercises them, the oracle's own counts show that Persson marked quads and
-WENO replaced them inside the compared window.
+FP64, one step on the same inputs (the GPU is set to the oracle's state
+before every step): cell averages within 1e-12 relative of the oracle
+(relative to the field scale where a field crosses zero), dt within 1e-12,
+node positions within 1e-13 absolute.  FP64 over the whole window (both
+runs free): the same bounds, except on noh100, where rounding differences
+are amplified by the converging flow at the singular origin (1e-14 after
+one step, 1.6e-12 after four): 1e-11 there.  FP32-mixed over the whole
+window: cell averages within 1e-6, dt within 1e-6, node displacements
+within 1e-6 of the oracle's.  Where the configuration exercises them, the
+oracle's own counts show that Persson marked quads and WENO replaced them
+inside the compared window.
 """
 import functools
 
@@ -32,6 +37,7 @@ from oracle.oracle import Oracle
 pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
+FP64_WINDOW_TOL = {"noh100": 1e-11}
 MIXED_TOL = 1e-6
 
 # name: (steps, fixed-dt parity config, per-cell initial densities,
@@ -73,8 +79,9 @@ def _oracle_run(name):
     Oracle.counts()
     traj = []
     for it in range(1, nsteps + 1):
+        inputs = (unkno.copy(), coord.copy(), ustar.copy(), geoel[:, 2].copy(), dt, ta)
         _, dt, ta = o.run(unkno, coord, m.coord, geoel, amatr, ustar, it, 1, dt, ta)
-        traj.append((dt, unkno[:m.ncell, :, 0].copy(), coord.copy()))
+        traj.append((dt, unkno[:m.ncell, :, 0].copy(), coord.copy(), inputs))
     counts = Oracle.counts()
     return m, c, rho0, init, tuple(traj), counts
 
@@ -90,13 +97,18 @@ def _gpu_solver(name, precision):
 
 
 @pytest.mark.parametrize("name", list(CASES))
-def test_production_parity_large(name):
+def test_production_step_parity_large(name):
+    """Every step of the window from the oracle's own input state."""
     m, c, s, traj, (marked, replaced) = _gpu_solver(name, 0)
     _, _, _, need_marked, need_replaced = CASES[name]
     assert marked >= need_marked and replaced >= need_replaced, (marked, replaced)
+    geoel0, amatr = _oracle_run(name)[3][0], _oracle_run(name)[3][1]
     n = m.ncell
-    for it, (dt, avg, coord) in enumerate(traj, 1):
-        dt2, _ = s.step()
+    for it, (dt, avg, coord, (u_in, x_in, us_in, vol_in, dt_in, ta_in)) in enumerate(traj, 1):
+        g_in = geoel0.copy()
+        g_in[:, 2] = vol_in
+        s.set_state(u_in, x_in, us_in, g_in, amatr)
+        dt2, _ = s.step(itime=it, dtfix=dt_in, tacru=ta_in)
         assert abs(dt2 - dt) <= FP64_TOL * dt, (it, dt2, dt)
         u2, x2, _, _ = s.get_state()
         err = _avg_err(u2[:n, :, 0], avg)
@@ -106,11 +118,27 @@ def test_production_parity_large(name):
 
 
 @pytest.mark.parametrize("name", list(CASES))
+def test_production_parity_large(name):
+    """The whole window, GPU and oracle each running freely."""
+    m, c, s, traj, _ = _gpu_solver(name, 0)
+    tol = FP64_WINDOW_TOL.get(name, FP64_TOL)
+    n = m.ncell
+    for it, (dt, avg, coord, _) in enumerate(traj, 1):
+        dt2, _ = s.step()
+        assert abs(dt2 - dt) <= tol * dt, (it, dt2, dt)
+        u2, x2, _, _ = s.get_state()
+        err = _avg_err(u2[:n, :, 0], avg)
+        assert err.max() < tol, (it, err)
+        assert np.abs(x2 - coord).max() < 1e-13, (it, np.abs(x2 - coord).max())
+    s.close()
+
+
+@pytest.mark.parametrize("name", list(CASES))
 def test_mixed_parity_large(name):
     m, c, s, traj, _ = _gpu_solver(name, 1)
     n = m.ncell
     worst = np.zeros(4)
-    for it, (dt, avg, coord) in enumerate(traj, 1):
+    for it, (dt, avg, coord, _) in enumerate(traj, 1):
         dt2, _ = s.step()
         assert abs(dt2 - dt) <= MIXED_TOL * dt, (it, dt2, dt)
         u2, x2, _, _ = s.get_state()
