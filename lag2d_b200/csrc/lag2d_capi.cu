@@ -57,11 +57,11 @@ void launch_tri_corner(const Dev &d, cudaStream_t st);
 void launch_tri_rhs(const Dev &d, cudaStream_t st, const double *usn, const double *vsn, int fuse, double alfa);
 void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold,
                           int fold_u, int mixed);
-void launch_adjoint_fold_u(const Dev &d, const void *adj, cudaStream_t st);
 void launch_weno_linear(const Dev &d, cudaStream_t st, int mode, const double *v, double *out, double *wbuf,
                         int *wslot, int cap, int *overflow);
-void launch_weno_gather(const Dev &d, cudaStream_t st, double *lamU, const double *wbuf, const int *wslot, int cap,
-                        const int *inv_ptr, const int *inv_ent);
+void launch_weno_gather(const Dev &d, cudaStream_t st, double *lamU, double *lamUn, int fold, const double *wbuf,
+                        const int *wslot, int cap, const int *inv_ptr, const int *inv_ent);
+void launch_weno_swap(const Dev &d, cudaStream_t st);
 int adjoint_stage_launches(const Dev &d);
 int error_blocks(const Dev &d);
 void launch_error(const Dev &d, cudaStream_t st, const double *X, const double *Y, double *part);
@@ -974,7 +974,7 @@ int lag2d_weno_linear(lag2d_handle *h, int transpose, const double *in, double *
   CK(cudaMemcpyAsync(obuf, vbuf, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
   if (transpose) {
     launch_weno_linear(d, h->st, 1, vbuf, nullptr, wbuf, wslot, cap, overflow);
-    launch_weno_gather(d, h->st, obuf, wbuf, wslot, cap, h->sinv_ptr, h->sinv_ent);
+    launch_weno_gather(d, h->st, obuf, nullptr, 0, wbuf, wslot, cap, h->sinv_ptr, h->sinv_ent);
   } else {
     launch_weno_linear(d, h->st, 0, vbuf, obuf, nullptr, nullptr, cap, overflow);
   }
@@ -1070,9 +1070,9 @@ struct AdjWork {
   Adj a{};
   StageRec rec{};
   int rc = LAG2D_OK;
-  // WENO transpose: the stage state after WENO, per-slot stencil adjoints,
-  // slot of each troubled quad, overflow flag; cap = slots per stage
-  double *post = nullptr, *wbuf = nullptr;
+  // WENO transpose: per-slot stencil adjoints, slot of each troubled quad,
+  // overflow flag; cap = slots per stage
+  double *wbuf = nullptr;
   int *wslot = nullptr, *overflow = nullptr;
   int cap = 0;
   explicit AdjWork(lag2d_handle *hh) : h(hh) {}
@@ -1112,7 +1112,7 @@ struct AdjWork {
     alloc(&rec.tcf, ns * 120 * (size_t)d.ntria); alloc(&rec.tpart, ns * 30 * (size_t)d.ntria);
     rec.nstag = nstag; rec.nu = nu; rec.np = np; rec.nq = d.nquad; rec.nt = d.ntria;
     cap = std::max(1, std::min(d.nquad, 16384));
-    alloc(&post, nu); alloc(&wbuf, 216 * (size_t)cap); alloc(&wslot, (size_t)d.nquad); alloc(&overflow, 1);
+    alloc(&wbuf, 216 * (size_t)cap); alloc(&wslot, (size_t)d.nquad); alloc(&overflow, 1);
   }
   // forward of nk steps from the handle's state, recording every stage input
   int record(int itime, int nk) {
@@ -1133,35 +1133,32 @@ struct AdjWork {
   }
   // reverse of the nk recorded steps; a.lU / a.lx / a.lus hold the adjoints of
   // the last step's outputs on entry and of the first step's inputs on return
-  // Each stage's reverse linearises at the state after WENO: the recorded
-  // stage input (before WENO) is copied to `post`, and Persson and WENO are
-  // run again on it (same marks, same reconstruction); the reverse kernels
-  // run on `post`; then the WENO transpose, with its stencils, weights, frame
-  // and characteristic matrices taken at the recorded input (the limiter's
-  // active set frozen), maps the adjoint of `post` to that of the input.
+  // Each stage's reverse linearises at the state after WENO: Persson and
+  // WENO run again on the recorded stage input (same marks, same
+  // reconstruction) and the replaced moments are swapped into the record in
+  // place; the reverse kernels run on it; the swap back restores the input;
+  // then the WENO transpose, with its stencils, weights, frame and
+  // characteristic matrices taken at the input (the limiter's active set
+  // frozen), maps the adjoint of the post-WENO state to that of the input.
   void reverse(int nk) {
     const int nstag = h->cfg.nstag;
-    const size_t nu = (size_t)NU * h->d.ncell;
     // the recompute must not see the end-of-run flag a window ending at tend leaves
     cudaMemsetAsync(&h->d.sc_dev->done, 0, sizeof(int), h->st);
     for (int k = nk - 1; k >= 0; k--) {
       for (int istag = nstag; istag >= 1; istag--) {
         const Dev ds = rec.inputs(h->d, (size_t)k * nstag + (istag - 1));
-        Dev dp = ds;
-        dp.Us = post;
-        cudaMemcpyAsync(post, ds.Us, nu * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
         launch_reset_count(ds, h->st);
         launch_fast_persson(ds, h->st);
         launch_weno_warp(ds, h->st);
-        launch_weno_commit(dp, h->st);
+        launch_weno_swap(ds, h->st);
         // stage 1 reads x^n directly: its reverse folds the coordinate adjoints
-        // in; the U^n fold waits for the WENO transpose
-        launch_adjoint_stage(dp, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k, istag == 1, 0,
+        // in; the U^n fold waits for the WENO transpose (in the gather)
+        launch_adjoint_stage(ds, &a, h->st, kRK[nstag - 2][istag - 1], rec.dt + k, istag == 1, 0,
                              h->cfg.precision == 1);
+        launch_weno_swap(ds, h->st);
         launch_weno_linear(ds, h->st, 1, a.lU, nullptr, wbuf, wslot, cap, overflow);
-        launch_weno_gather(ds, h->st, a.lU, wbuf, wslot, cap, h->sinv_ptr, h->sinv_ent);
-        if (istag == 1) launch_adjoint_fold_u(ds, &a, h->st);
-        h->launches += adjoint_stage_launches(h->d) + 6 + (istag == 1);
+        launch_weno_gather(ds, h->st, a.lU, a.lUn, istag == 1, wbuf, wslot, cap, h->sinv_ptr, h->sinv_ent);
+        h->launches += adjoint_stage_launches(h->d) + 7;
       }
     }
   }

@@ -1893,7 +1893,7 @@ void launch_tri_adjoint_corner(const Dev &d, const Adj &a, cudaStream_t st);
 // coefficients, the node solve, the update and node motion stay FP64.
 // fold_u = 0 keeps the adjoint of U^n apart from that of the stage state in
 // stage 1 too, so that the WENO transpose can act on the latter alone; the
-// caller then folds them with launch_adjoint_fold_u.
+// caller then folds them (the WENO gather does, with its fold flag).
 void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double alfa, const double *dtp, int fold,
                           int fold_u, int mixed) {
   const Adj &a = *static_cast<const Adj *>(adj);
@@ -1911,18 +1911,6 @@ void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double
   fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
 }
 int adjoint_stage_launches(const Dev &d) { return d.ntria > 0 ? 9 : 7; }
-// end of stage 1's reverse: the adjoint of U^(1) = U^n takes the U^n part in
-__global__ void k_a_fold_u(Dev d, Adj a) {
-  const size_t n = (size_t)24 * d.ncell;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    a.lU[i] += a.lUn[i];
-    a.lUn[i] = 0.0;
-  }
-}
-void launch_adjoint_fold_u(const Dev &d, const void *adj, cudaStream_t st) {
-  k_a_fold_u<<<fast::nb(24 * d.ncell, 256) < 4736 ? fast::nb(24 * d.ncell, 256) : 4736, 256, 0, st>>>(
-      d, *static_cast<const Adj *>(adj));
-}
 
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }

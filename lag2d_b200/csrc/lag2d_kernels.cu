@@ -624,6 +624,23 @@ __host__ __device__ void b_weno_commit(const Dev &d, int t) {
     for (int k = 1; k < 6; k++) d.Us[(q * NDEG + k) * d.ncell + e] = d.Uw[(q * 5 + (k - 1)) * d.nquad + iq];
 }
 __global__ void k_weno_commit(Dev d) { b_weno_commit(d, blockIdx.x * blockDim.x + threadIdx.x); }
+// Exchange the replaced moments between the state and the reconstruction
+// buffer (the adjoint's reverse stage switches the recorded stage input
+// between its values before and after WENO this way, in place).
+__global__ void k_weno_swap(Dev d) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= *d.wcount) return;
+  const int iq = d.wlist[t];
+  const int e = iq + d.ntria;
+  if (d.flag[e] != 2) return;
+  for (int q = 0; q < 4; q++)
+    for (int k = 1; k < 6; k++) {
+      double *a = d.Us + (q * NDEG + k) * (size_t)d.ncell + e, *b = d.Uw + (q * 5 + (k - 1)) * (size_t)d.nquad + iq;
+      const double v = *a;
+      *a = *b;
+      *b = v;
+    }
+}
 
 // ---------------------------------------------------------------------------
 // The same WENO reconstruction with one warp per troubled quad (the optimised
@@ -1281,25 +1298,37 @@ __global__ void __launch_bounds__(32) k_weno_linear(Dev d, int mode, const doubl
   }
 }
 
-// per quad j: the adjoint of the stage state before WENO from the one after it
-__global__ void k_weno_gather(Dev d, double *lamU, const double *wbuf, const int *wslot, int cap,
-                              const int *inv_ptr, const int *inv_ent) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= d.nquad) return;
+// per cell: the adjoint of the stage state before WENO from the one after it
+// (quads), and with fold the adjoint of U^n added in (the end of stage 1's
+// reverse, every cell); nothing to do, and no memory touched, when WENO
+// replaced no quad and fold is 0
+__global__ void k_weno_gather(Dev d, double *lamU, double *lamUn, int fold, const double *wbuf, const int *wslot,
+                              int cap, const int *inv_ptr, const int *inv_ent) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.ncell) return;
+  const int nw = *d.wcount;
+  if (nw == 0 && !fold) return;
   const size_t nc = d.ncell;
-  const int e = j + d.ntria;
   double l[24];
   for (int v = 0; v < 24; v++) l[v] = lamU[v * nc + e];
-  if (d.flag[e] == 2 && d.stencil[j] >= 0)
-    for (int q = 0; q < 4; q++)
-      for (int k = 1; k < 6; k++) l[q * 6 + k] = 0.0;
-  for (int i = inv_ptr[j]; i < inv_ptr[j + 1]; i++) {
-    const int c = inv_ent[i] / 9, s = inv_ent[i] - 9 * c;
-    if (d.flag[c + d.ntria] != 2 || d.stencil[c] < 0) continue;
-    const int t = wslot[c];
-    if (t < 0 || t >= cap) continue;
-    for (int v = 0; v < 24; v++) l[v] += wbuf[((size_t)(s * 24 + v)) * cap + t];
+  const int j = e - d.ntria;
+  if (nw > 0 && j >= 0) {
+    if (d.flag[e] == 2 && d.stencil[j] >= 0)
+      for (int q = 0; q < 4; q++)
+        for (int k = 1; k < 6; k++) l[q * 6 + k] = 0.0;
+    for (int i = inv_ptr[j]; i < inv_ptr[j + 1]; i++) {
+      const int c = inv_ent[i] / 9, s = inv_ent[i] - 9 * c;
+      if (d.flag[c + d.ntria] != 2 || d.stencil[c] < 0) continue;
+      const int t = wslot[c];
+      if (t < 0 || t >= cap) continue;
+      for (int v = 0; v < 24; v++) l[v] += wbuf[((size_t)(s * 24 + v)) * cap + t];
+    }
   }
+  if (fold)
+    for (int v = 0; v < 24; v++) {
+      l[v] += lamUn[v * nc + e];
+      lamUn[v * nc + e] = 0.0;
+    }
   for (int v = 0; v < 24; v++) lamU[v * nc + e] = l[v];
 }
 
@@ -3378,10 +3407,11 @@ void launch_weno_linear(const Dev &d, cudaStream_t st, int mode, const double *v
   const int g = d.nquad < 1184 ? (d.nquad > 0 ? d.nquad : 1) : 1184;
   k_weno_linear<<<g, 32, sizeof(WenoAdjBlock), st>>>(d, mode, v, out, wbuf, wslot, cap, overflow);
 }
-void launch_weno_gather(const Dev &d, cudaStream_t st, double *lamU, const double *wbuf, const int *wslot, int cap,
-                        const int *inv_ptr, const int *inv_ent) {
-  k_weno_gather<<<nblk(d.nquad, 128), 128, 0, st>>>(d, lamU, wbuf, wslot, cap, inv_ptr, inv_ent);
+void launch_weno_gather(const Dev &d, cudaStream_t st, double *lamU, double *lamUn, int fold, const double *wbuf,
+                        const int *wslot, int cap, const int *inv_ptr, const int *inv_ent) {
+  k_weno_gather<<<nblk(d.ncell, 128), 128, 0, st>>>(d, lamU, lamUn, fold, wbuf, wslot, cap, inv_ptr, inv_ent);
 }
+void launch_weno_swap(const Dev &d, cudaStream_t st) { k_weno_swap<<<nblk(d.nquad, 256), 256, 0, st>>>(d); }
 void launch_weno_commit(const Dev &d, cudaStream_t st) { k_weno_commit<<<nblk(d.nquad, 256), 256, 0, st>>>(d); }
 void launch_corner(const Dev &d, cudaStream_t st) { k_corner<<<nblk(d.nquad, 128), 128, 0, st>>>(d); }
 void launch_node(const Dev &d, cudaStream_t st) { k_node<<<nblk(d.npoin, 256), 256, 0, st>>>(d); }
