@@ -1055,12 +1055,14 @@ double lag2d_kernel_ms(const lag2d_handle *h, const char *family, long long *lau
 // the handle's precision is 1: the recompute runs the mixed forward passes and the
 // reverse the mixed transposes).
 //
-// Reverse mode per RK stage with the time step size and the Persson marks
-// frozen from the forward pass; WENO must replace no cell in the window (its
-// reconstruction's adjoint is not built, so a window that limits returns
-// LAG2D_EUNSUP; marked cells whose stencil is rejected keep their DOFs and are
-// differentiated as unlimited cells).  Reference-configuration
-// quantities (cell masses, mass matrices, initial-mesh moments) are constants.
+// Reverse mode per RK stage with the time step size, the Persson marks and
+// the WENO active set (chosen stencil, nonlinear weights, characteristic
+// frame) frozen from the forward pass: the reconstruction is differentiated
+// as the linear map it is for those choices.  Marked cells whose stencil is
+// rejected keep their DOFs and are differentiated as unlimited cells; more
+// than 16384 replaced quads in a stage return LAG2D_EUNSUP.
+// Reference-configuration quantities (cell masses, mass matrices,
+// initial-mesh moments) are constants.
 // The stage inputs are recorded by recomputing each checkpoint segment, so the
 // device memory of a window is (segments + 1) checkpoints plus K steps of
 // stage records.
@@ -1147,6 +1149,10 @@ struct AdjWork {
     for (int k = nk - 1; k >= 0; k--) {
       for (int istag = nstag; istag >= 1; istag--) {
         const Dev ds = rec.inputs(h->d, (size_t)k * nstag + (istag - 1));
+        // the stage's cell volumes (WENO scales its stencil bases by them) from
+        // the recorded nodes, as the forward pass had them
+        launch_tri_geom(ds, h->st, ds.xs, ds.ys);
+        launch_fast_geom(ds, h->st, 0);
         launch_reset_count(ds, h->st);
         launch_fast_persson(ds, h->st);
         launch_weno_warp(ds, h->st);
@@ -1158,7 +1164,7 @@ struct AdjWork {
         launch_weno_swap(ds, h->st);
         launch_weno_linear(ds, h->st, 1, a.lU, nullptr, wbuf, wslot, cap, overflow);
         launch_weno_gather(ds, h->st, a.lU, a.lUn, istag == 1, wbuf, wslot, cap, h->sinv_ptr, h->sinv_ent);
-        h->launches += adjoint_stage_launches(h->d) + 7;
+        h->launches += adjoint_stage_launches(h->d) + 8 + (h->d.ntria > 0);
       }
     }
   }
@@ -1195,6 +1201,11 @@ struct Snapshot {
     cudaMemcpyAsync(d.us, us + c * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
     cudaMemcpyAsync(d.vs, vs + c * np, np * sizeof(double), cudaMemcpyDeviceToDevice, h->st);
     cudaMemcpyAsync(d.sc_dev, sc + c, sizeof(Scalars), cudaMemcpyDeviceToDevice, h->st);
+    // cell volumes (and triangle centres) of the restored nodes: the next
+    // stage 1 reads them in WENO and the time step
+    launch_tri_geom(d, h->st, d.xs, d.ys);
+    launch_fast_geom(d, h->st, 0);
+    h->launches += 1 + (d.ntria > 0);
   }
 };
 
