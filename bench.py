@@ -371,7 +371,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         return max_over_ranks(e0.elapsed_time(e1)), n, solver.kernel_launches - l0
 
-    def families(solver, names=("persson", "weno", "corner", "node", "rhs", "dt", "update", "nodes", "geom", "copy")):
+    def families(solver, names=("persson", "weno", "src", "corner", "node", "rhs", "dt", "nodes", "geom", "copy")):
         solver.timing(True)
         solver.run(2)
         out = {}
@@ -396,10 +396,10 @@ def run_ours(args):
     fams_mx = families(sm)
     per_step = {f: v["ms_per_launch"] * v["launches"] / 2 for f, v in fams.items()}
     per_step_mx = {f: v["ms_per_launch"] * v["launches"] / 2 for f, v in fams_mx.items()}
-    dom = max((f for f in per_step if f in ("corner", "node", "rhs", "dt", "persson", "nodes", "geom")),
+    dom = max((f for f in per_step if f in ("src", "corner", "node", "rhs", "dt", "persson", "nodes", "geom")),
               key=lambda f: per_step[f])
     peak, peak_kind = peaks()
-    kb = kernel_bytes(dom, m.ncell, m.npoin, c.nstag)
+    kb = kernel_bytes(dom, m.ncell, m.npoin, c.nstag, source=c.ncase == 1)
     traffic = measured_traffic(dom, m.ncell)
     achieved = kb / (fams[dom]["ms_per_launch"] / 1e3) / 1e9
     sb = stage_bytes(m.ncell, m.npoin)

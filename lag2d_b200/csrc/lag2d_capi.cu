@@ -47,6 +47,8 @@ void launch_fast_node(const Dev &d, cudaStream_t st);
 void launch_fast_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa);
 void launch_fast_dt(const Dev &d, cudaStream_t st, int ndt);
 void launch_mixed_corner(const Dev &d, cudaStream_t st);
+void launch_fast_src(const Dev &d, cudaStream_t st);
+void launch_mixed_src(const Dev &d, cudaStream_t st);
 void launch_mixed_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa);
 void launch_fast_nodes(const Dev &d, cudaStream_t st, double alfa);
 void launch_fast_geom(const Dev &d, cudaStream_t st, int fix);
@@ -310,6 +312,15 @@ static int corner_launches(const lag2d_handle *h, const Dev &d) {
   return (d.ntria > 0) + (h->cfg.precision == 1 ? 1 : 2);
 }
 
+// Taylor-Green energy source of the stage (quads; ncase 1 only), read by the
+// RHS pass
+static int src_launches(const Dev &d) { return d.ncase == 1 && d.nquad > 0; }
+static void src_pass(lag2d_handle *h, const Dev &d) {
+  if (!src_launches(d)) return;
+  if (h->cfg.precision == 1) launch_mixed_src(d, h->st);
+  else launch_fast_src(d, h->st);
+}
+
 static void corner_pass(lag2d_handle *h, const Dev &d) {
   launch_tri_corner(d, h->st);
   if (h->cfg.precision == 1) launch_mixed_corner(d, h->st);
@@ -384,6 +395,7 @@ static void enqueue_step_fast(lag2d_handle *h, int itime, const StageRec *rec = 
     }
     run(h, "persson", [&] { launch_reset_count(d, h->st); launch_fast_persson(d, h->st); }, 2);
     run(h, "weno", [&] { launch_weno_warp(d, h->st); launch_weno_commit(d, h->st); }, 2);
+    if (src_launches(d)) run(h, "src", [&] { src_pass(h, d); });
     run(h, "corner", [&] { corner_pass(h, d); }, corner_launches(h, d));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     if (istag == 1) {
@@ -894,6 +906,7 @@ int lag2d_rhs(lag2d_handle *h, int itime, double *rhsel, int *flags) {
     run(h, "node", [&] { launch_node(d, h->st); });
     run(h, "rhs", [&] { launch_tri_rhs(d, h->st, d.us, d.vs, 0, 0.0); launch_rhs(d, h->st); }, 1 + (d.ntria > 0));
   } else {
+    if (src_launches(d)) run(h, "src", [&] { src_pass(h, d); });
     run(h, "corner", [&] { corner_pass(h, d); }, corner_launches(h, d));
     run(h, "node", [&] { launch_fast_node(d, h->st); });
     run(h, "rhs", [&] { rhs_pass(h, d, 0, 0.0); }, rhs_launches(h, d));

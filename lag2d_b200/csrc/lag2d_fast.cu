@@ -17,6 +17,9 @@
 //    the RHS pass.
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
+#ifndef LAG2D_FACES_MINB
+#define LAG2D_FACES_MINB 4
+#endif
 #include <math.h>
 
 #include "lag2d_device.cuh"
@@ -465,21 +468,14 @@ __host__ __device__ __forceinline__ void tgv_source(const Loaded &L, const CellG
   else tgv_source_rows<0>(L, G, D, g, el);
 }
 
-// ---------------------------------------------------------------------------
-// Corner pass: node partial sums of the Riemann coefficients + sub-cell
-// density corrections (getriem_quadsubg2 with getrhosubg_averg/_daverg)
-// ---------------------------------------------------------------------------
-// The corner pass runs as two kernels: PART 1, the sub-cell density
-// corrections (written to d.corr, which the RHS pass reads anyway); PART 2,
-// the corner faces with the corrections read back.  Each is compiled for 4
-// resident blocks of 128 per SM (128 registers): on the 1024x1024
-// Taylor-Green step the pair takes 1.68 ms against 1.83 ms for the single
-// kernel (PART 0) at 168 registers (3 blocks).
-template <int PART>
-__host__ __device__ void f_corner_t(const Dev &d, int iq) {
+// Taylor-Green energy source of the stage (rhsdomnsrcdg_lag_curvquad,
+// Getrhslag.f90:4070-4251), one thread per quad: it depends on the stage's
+// nodes and the reference geometry only; the RHS pass adds the 6 moments
+// (d.src, [6][nquad]).  A kernel of its own: inside the corner or RHS kernels
+// its registers and code cost those kernels more than its own launch.
+__host__ __device__ void f_tgv_src(const Dev &d, int iq) {
   if (iq >= d.nquad || d.sc_dev->done) return;
   const int e = iq + d.ntria;
-  const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
   double c[36], D[16];
@@ -490,27 +486,51 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
   }
   detpoly(c, D);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-  double u[4][6];
-  load_u(d, d.Us, e, u);
-  const double rhoct = 1.0 / u[0][0];
-  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
-  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
+  double el[6] = {0, 0, 0, 0, 0, 0};
+  tgv_source(L, G, D, d.gamlg, el);
+#pragma unroll
+  for (int k = 0; k < 6; k++) d.src[k * (size_t)d.nquad + iq] = el[k];
+}
+
+// ---------------------------------------------------------------------------
+// Corner pass: node partial sums of the Riemann coefficients + sub-cell
+// density corrections (getriem_quadsubg2 with getrhosubg_averg/_daverg)
+// ---------------------------------------------------------------------------
+// The corner pass runs as two kernels: f_corner_corr, the sub-cell density
+// corrections (written to d.corr, which the RHS pass reads anyway), and
+// f_corner_faces, the corner faces with the corrections read back.  Each is
+// compiled for 4 resident blocks of 128 per SM (128 registers): on the
+// 1024x1024 Taylor-Green step the pair takes 1.68 ms against 1.83 ms for a
+// single kernel at 168 registers (3 blocks).
+__host__ __device__ void f_corner_corr(const Dev &d, int iq) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  double c[36], D[16];
+  {
+    double xp[9][2];
+    node_xy_rel(L, xp);
+    cross36_rel(xp, c);
+  }
+  detpoly(c, D);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  // the tau DOFs
+  double u[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) u[k] = d.Us[k * (size_t)d.ncell + e];
   // sub-cell densities: initial mass / exact sub-cell area, and the DG-implied
   // harmonic mean of tau over each sub-cell (5x5 Gauss per sub-cell)
-  double corr[4], vsub4[4];
-  if (PART == 2) {
-#pragma unroll
-    for (int isg = 0; isg < 4; isg++) corr[isg] = d.corr[isg * (size_t)d.nquad + iq];
-  }
-  if (PART != 2) subareas(c, vsub4);
+  double vsub4[4];
+  subareas(c, vsub4);
   // The harmonic mean sum masel = sum_g w_g det_g / tau_g is kept as one
   // fraction num / den (a/b + c/d = (a d + c b) / (b d)): three multiply-adds
   // per point and one division per sub-cell instead of one division per point.
   // tau is scaled by the cell-average tau first (rtc), so that the product of
   // the 25 scaled values stays near 1; masel = rtc num / den.
-  const double rtc = 1.0 / u[0][0];
+  const double rtc = 1.0 / u[0];
 #pragma unroll
-  for (int isg = 0; isg < (PART == 2 ? 0 : 4); isg++) {
+  for (int isg = 0; isg < 4; isg++) {
     const double unksgq = (1.0 / vsub4[isg]) * d.msub[isg * (size_t)d.nquad + iq];
     const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
     const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
@@ -523,9 +543,8 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
 #pragma unroll
       for (int n = 0; n < 4; n++) e[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
       const double dr = r - G.rc;
-      const double t0 = rtc * (u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 -
-                               u[0][5] * G.g21);
-      const double t1 = rtc * (u[0][2] + u[0][5] * dr), t2 = rtc * (0.5 * u[0][4]);
+      const double t0 = rtc * (u[0] + u[1] * dr + u[3] * (0.5 * dr * dr - G.g19) - u[4] * G.g20 - u[5] * G.g21);
+      const double t1 = rtc * (u[2] + u[5] * dr), t2 = rtc * (0.5 * u[4]);
       const double wi = 0.25 * g5w(i);
 #pragma unroll
       for (int j = 0; j < 5; j++) {
@@ -539,23 +558,39 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
     }
     const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
     // 1 / uqsgc = masel / volel with masel = rtc num / den
-    corr[isg] = d.cdrho * (unksgq - (rtc * num) / (den * volel));
-    d.corr[isg * (size_t)d.nquad + iq] = corr[isg];
+    d.corr[isg * (size_t)d.nquad + iq] = d.cdrho * (unksgq - (rtc * num) / (den * volel));
   }
-  if (PART == 1) {
-    // Taylor-Green energy source of the stage (rhsdomnsrcdg_lag_curvquad,
-    // Getrhslag.f90:4070-4251): it depends on the stage's nodes and the
-    // reference geometry only, and this kernel has the det J coefficients;
-    // the RHS pass adds the 6 moments
-    if (d.ncase == 1) {
-      double el[6] = {0, 0, 0, 0, 0, 0};
-      tgv_source(L, G, D, g, el);
-#pragma unroll
-      for (int k = 0; k < 6; k++) d.src[k * (size_t)d.nquad + iq] = el[k];
-    }
-    return;
+}
+
+// Corner faces of one quad: per node the vertex state, then its corner faces
+// in the reference's order, summed into the node's 5 partials.  The cell's
+// 24 DOFs and 4 sub-cell corrections are copied asynchronously (cp.async)
+// into this thread's column of shared memory (stride kCornerBlock) at entry,
+// so their loads overlap the coordinate gathers and they take no registers
+// between the vertex states.
+constexpr int kCornerBlock = 128;
+constexpr int kCornerStage = 28;
+__device__ void f_corner_faces(const Dev &d, int iq, double *col) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  {
+    const size_t nc = d.ncell;
+    for (int v = 0; v < 24; v++) __pipeline_memcpy_async(col + v * kCornerBlock, d.Us + v * nc + e, sizeof(double));
+    for (int s = 0; s < 4; s++)
+      __pipeline_memcpy_async(col + (24 + s) * kCornerBlock, d.corr + s * (size_t)d.nquad + iq, sizeof(double));
+    __pipeline_commit();
   }
-  // per node: vertex state, then its corner faces in the reference's order
+#define CF_U(q, k) col[((q) * 6 + (k)) * kCornerBlock]
+#define CF_CORR(s) col[(24 + (s)) * kCornerBlock]
+  const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  __pipeline_wait_prior(0);
+  const double rhoct = 1.0 / CF_U(0, 0);
+  const double pctr =
+      fmax(eps, (g - 1.0) * rhoct * (CF_U(3, 0) - 0.5 * (CF_U(1, 0) * CF_U(1, 0) + CF_U(2, 0) * CF_U(2, 0))));
+  const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
 #pragma unroll
   for (int k = 0; k < 9; k++) {
     double b[6];
@@ -566,7 +601,7 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
       double acc = 0.0;
 #pragma unroll
       for (int kk = 0; kk < 6; kk++)
-        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
+        if (kk < d.mdegr) acc += CF_U(q, kk) * b[kk];
       st[q] = acc;
     }
     const double rhovt = 1.0 / st[0];
@@ -578,8 +613,7 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
 #pragma unroll
     for (int i = nc_start(k); i < nc_start(k + 1); i++) {
       const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
-      const double ci = isg == 0 ? corr[0] : isg == 1 ? corr[1] : isg == 2 ? corr[2] : corr[3];
-      const double pv = fmax(eps, (g - 1.0) * (rhovt + ci) * ke);
+      const double pv = fmax(eps, (g - 1.0) * (rhovt + CF_CORR(isg)) * ke);
 #pragma unroll
       for (int f = 0; f < 2; f++) {
         double ax, ay;
@@ -600,6 +634,8 @@ __host__ __device__ void f_corner_t(const Dev &d, int iq) {
     d.npart[(3 * 9 + k) * (size_t)d.nquad + iq] = P3;
     d.npart[(4 * 9 + k) * (size_t)d.nquad + iq] = P4;
   }
+#undef CF_U
+#undef CF_CORR
 }
 
 // ---------------------------------------------------------------------------
@@ -839,7 +875,7 @@ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, doubl
     }
   }
   if (d.ncase == 1) {
-    // Taylor-Green energy source, computed by the corner pass (k_corner2_corr)
+    // Taylor-Green energy source, computed by k_tgv_src2 before the corner pass
 #pragma unroll
     for (int k = 0; k < 6; k++) el[k] += d.src[k * (size_t)d.nquad + iq];
   }
@@ -1820,11 +1856,13 @@ __host__ __device__ void a_centre(const Dev &d, const Adj &a, int p) {
 
 __global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void __launch_bounds__(128, 4) k_corner2_corr(Dev d) {
-  f_corner_t<1>(d, blockIdx.x * blockDim.x + threadIdx.x);
+  f_corner_corr(d, blockIdx.x * blockDim.x + threadIdx.x);
 }
-__global__ void __launch_bounds__(128, 4) k_corner2_faces(Dev d) {
-  f_corner_t<2>(d, blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(kCornerBlock, LAG2D_FACES_MINB) k_corner2_faces(Dev d) {
+  extern __shared__ double faces_stage[];
+  f_corner_faces(d, blockIdx.x * blockDim.x + threadIdx.x, faces_stage + threadIdx.x);
 }
+__global__ void __launch_bounds__(128) k_tgv_src2(Dev d) { f_tgv_src(d, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_node2(Dev d) { f_node(d, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void __launch_bounds__(kRhsBlock, 3) k_rhs3(Dev d, int fuse, double alfa) {
   extern __shared__ double rhs_stage[];
@@ -1916,8 +1954,10 @@ int adjoint_stage_launches(const Dev &d) { return d.ntria > 0 ? 9 : 7; }
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
 void launch_fast_corner(const Dev &d, cudaStream_t st) {
   fast::k_corner2_corr<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d);
-  fast::k_corner2_faces<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d);
+  constexpr int smem = fast::kCornerStage * fast::kCornerBlock * sizeof(double);
+  fast::k_corner2_faces<<<fast::nb(d.nquad, fast::kCornerBlock), fast::kCornerBlock, smem, st>>>(d);
 }
+void launch_fast_src(const Dev &d, cudaStream_t st) { fast::k_tgv_src2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
 void launch_fast_node(const Dev &d, cudaStream_t st) { fast::k_node2<<<fast::nb(d.npoin, 256), 256, 0, st>>>(d); }
 void launch_fast_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa) {
   constexpr int smem = fast::kRhsStage * fast::kRhsBlock * sizeof(double);

@@ -292,6 +292,70 @@ __device__ __forceinline__ void corner_coeffs(double axd, double ayd, float w, f
 }
 
 // ---------------------------------------------------------------------------
+// Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:4070-4251)
+// in FP32, one thread per quad, for the RHS pass (it depends on the stage's
+// nodes only); the cell-average moment is accumulated in FP64
+// ---------------------------------------------------------------------------
+__device__ void m_tgv_src(const Dev &d, int iq) {
+  if (iq >= d.nquad || d.sc_dev->done) return;
+  const int e = iq + d.ntria;
+  CellXY L;
+  double c[36], D[16];
+  load_cell(d, iq, L, c);
+  detpoly(c, D);
+  float Df[16];
+#pragma unroll
+  for (int t = 0; t < 16; t++) Df[t] = (float)D[t];
+  const GeoF G{(float)d.rc[e], (float)d.sc[e], (float)d.g19[e], (float)d.g20[e], (float)d.g21[e]};
+  double el0 = 0.0;
+  float el[6] = {0, 0, 0, 0, 0, 0};
+  float Xf[3][3], Yf[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int bb = 0; bb < 3; bb++) {
+      Xf[a][bb] = (float)L.X[a][bb];
+      Yf[a][bb] = (float)L.Y[a][bb];
+    }
+  const float coef = (float)(0.25 * 3.14159265358979311599796346854 / (d.gamlg - 1.0));
+  const float oxf = (float)L.ox, oyf = (float)L.oy;
+#pragma unroll 1
+  for (int i = 0; i < 5; i++) {
+    const float r = g5p(i), dr = r - G.rc;
+    float lr[3];
+    lag3f(r, lr);
+    float Px[3], Py[3];
+#pragma unroll
+    for (int bb = 0; bb < 3; bb++) {
+      Px[bb] = lr[0] * Xf[0][bb] + lr[1] * Xf[1][bb] + lr[2] * Xf[2][bb];
+      Py[bb] = lr[0] * Yf[0][bb] + lr[1] * Yf[1][bb] + lr[2] * Yf[2][bb];
+    }
+    const float wi = g5w(i);
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const float s = g5p(j), ds = s - G.sc;
+      float ls[3];
+      lag3f(s, ls);
+      const float xg = oxf + (Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2]);
+      const float yg = oyf + (Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2]);
+      const float djaco = wi * g5w(j) * detevalf(Df, r, s);
+      const float cx = cospif(xg), cy = cospif(yg);
+      const float c3x = cx * (4.0f * cx * cx - 3.0f), c3y = cy * (4.0f * cy * cy - 3.0f);
+      const float src = coef * (c3x * cy - c3y * cx) * djaco;
+      el0 += (double)src;
+      el[1] += src * dr;
+      el[2] += src * ds;
+      el[3] += src * (0.5f * dr * dr - G.g19);
+      el[4] += src * (0.5f * ds * ds - G.g20);
+      el[5] += src * (dr * ds - G.g21);
+    }
+  }
+  d.src[(size_t)iq] = el0;
+#pragma unroll
+  for (int k = 1; k < 6; k++) d.src[k * (size_t)d.nquad + iq] = (double)el[k];
+}
+
+// ---------------------------------------------------------------------------
 // Corner pass (getriem_quadsubg2 with getrhosubg_averg/_daverg)
 // ---------------------------------------------------------------------------
 __device__ void m_corner(const Dev &d, int iq) {
@@ -357,57 +421,6 @@ __device__ void m_corner(const Dev &d, int iq) {
     const double cr = d.cdrho * (unksgq - (double)masel / volel);
     d.corr[isg * (size_t)d.nquad + iq] = cr;
     corr[isg] = (float)cr;
-  }
-  if (d.ncase == 1) {
-    // Taylor-Green energy source (rhsdomnsrcdg_lag_curvquad, Getrhslag.f90:4070-4251)
-    // in FP32, for the RHS pass (it depends on the stage's nodes only)
-    double el0 = 0.0;
-    float el[6] = {0, 0, 0, 0, 0, 0};
-    // det J coefficients D, Df and the centre-relative nodes come from above
-    float Xf[3][3], Yf[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-      for (int bb = 0; bb < 3; bb++) {
-        Xf[a][bb] = (float)L.X[a][bb];
-        Yf[a][bb] = (float)L.Y[a][bb];
-      }
-    const float coef = (float)(0.25 * 3.14159265358979311599796346854 / (d.gamlg - 1.0));
-    const float oxf = (float)L.ox, oyf = (float)L.oy;
-#pragma unroll 1
-    for (int i = 0; i < 5; i++) {
-      const float r = g5p(i), dr = r - G.rc;
-      float lr[3];
-      lag3f(r, lr);
-      float Px[3], Py[3];
-#pragma unroll
-      for (int bb = 0; bb < 3; bb++) {
-        Px[bb] = lr[0] * Xf[0][bb] + lr[1] * Xf[1][bb] + lr[2] * Xf[2][bb];
-        Py[bb] = lr[0] * Yf[0][bb] + lr[1] * Yf[1][bb] + lr[2] * Yf[2][bb];
-      }
-      const float wi = g5w(i);
-#pragma unroll
-      for (int j = 0; j < 5; j++) {
-        const float s = g5p(j), ds = s - G.sc;
-        float ls[3];
-        lag3f(s, ls);
-        const float xg = oxf + (Px[0] * ls[0] + Px[1] * ls[1] + Px[2] * ls[2]);
-        const float yg = oyf + (Py[0] * ls[0] + Py[1] * ls[1] + Py[2] * ls[2]);
-        const float djaco = wi * g5w(j) * detevalf(Df, r, s);
-        const float cx = cospif(xg), cy = cospif(yg);
-        const float c3x = cx * (4.0f * cx * cx - 3.0f), c3y = cy * (4.0f * cy * cy - 3.0f);
-        const float src = coef * (c3x * cy - c3y * cx) * djaco;
-        el0 += (double)src;
-        el[1] += src * dr;
-        el[2] += src * ds;
-        el[3] += src * (0.5f * dr * dr - G.g19);
-        el[4] += src * (0.5f * ds * ds - G.g20);
-        el[5] += src * (dr * ds - G.g21);
-      }
-    }
-    d.src[(size_t)iq] = el0;
-#pragma unroll
-    for (int k = 1; k < 6; k++) d.src[k * (size_t)d.nquad + iq] = (double)el[k];
   }
 #pragma unroll
   for (int k = 0; k < 9; k++) {
@@ -617,7 +630,7 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa, double
     }
   }
   if (d.ncase == 1) {
-    // Taylor-Green energy source (FP32), computed by the corner pass
+    // Taylor-Green energy source (FP32), computed by k_tgv_src_mx before the corner pass
     el0 += d.src[(size_t)iq];
 #pragma unroll
     for (int k = 1; k < 6; k++) el[k] += (float)d.src[k * (size_t)d.nquad + iq];
@@ -666,6 +679,7 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa, double
 }
 
 __global__ void __launch_bounds__(128, 3) k_corner_mx(Dev d) { m_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(128) k_tgv_src_mx(Dev d) { m_tgv_src(d, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void __launch_bounds__(kMxBlock, 3) k_rhs_mx(Dev d, int fuse, double alfa) {
   extern __shared__ double mx_stage[];
   m_rhs(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa, mx_stage + threadIdx.x);
@@ -677,6 +691,9 @@ static inline int nb(int n, int b) { return (n + b - 1) / b; }
 
 void launch_mixed_corner(const Dev &d, cudaStream_t st) {
   mixed::k_corner_mx<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d);
+}
+void launch_mixed_src(const Dev &d, cudaStream_t st) {
+  mixed::k_tgv_src_mx<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d);
 }
 void launch_mixed_rhs(const Dev &d, cudaStream_t st, int fuse, double alfa) {
   constexpr int smem = mixed::kMxStage * mixed::kMxBlock * sizeof(double);

@@ -27,8 +27,10 @@ node partial sums):
   dt       (stage 1) connectivity, cell averages, volume, x^(s), ustar
            -> two per-block minima
   rhs      U^(s), U^n, M^-1, geometry, the 40 partial sums of the 8
-           boundary nodes, connectivity, x^(s), ustar -> U^(s+1) (the M^-1
-           solve and RK combine are fused into every stage)
+           boundary nodes, connectivity, x^(s), ustar (+ the 6 source
+           moments on Taylor-Green) -> U^(s+1) (the M^-1 solve and RK
+           combine are fused into every stage)
+  src      (Taylor-Green) connectivity, geometry, x^(s) -> 6 source moments
   persson  tau DOFs, mean velocity, geometry, mass, shape moments,
            connectivity, x^(s) -> flag, physical centre, frame
   nodes    x^n, x^(s), ustar -> x^(s+1), ustar_prev
@@ -50,9 +52,10 @@ def stage_bytes_p1(ncell: int, npoin: int) -> int:
     return ncell * (3 * 3 * 4 * W + 4 * W + 2 * W + 8 + 4 * 4) + npoin * (4 * 16 + 2 * 16 + 4) + 4 * ncell * 4
 
 
-def kernel_bytes(family: str, ncell: int, npoin: int, nstag: int = 3) -> int:
+def kernel_bytes(family: str, ncell: int, npoin: int, nstag: int = 3, source: bool = False) -> int:
     """Interface bytes of one launch of a kernel family on an all-quad mesh,
-    averaged over the family's launches in one time step."""
+    averaged over the family's launches in one time step (``source``: the
+    Taylor-Green source moments are read by the RHS pass)."""
     U = 24 * W            # 24 DOFs of one cell
     GEO = 5 * W           # rc, sc, g19..g21
     CONN = 9 * 4          # ipqua row
@@ -61,7 +64,8 @@ def kernel_bytes(family: str, ncell: int, npoin: int, nstag: int = 3) -> int:
         "corner": ncell * (U + GEO + 4 * W + CONN + 4 * W + 45 * W) + npoin * (XY + XY),
         "node": ncell * (45 * W + 9 * 4) + npoin * (4 + 1 + XY + XY),
         "dt": ncell * (CONN + 4 * W + W) + npoin * 2 * XY,
-        "rhs": ncell * (U + U + 16 * W + GEO + 40 * W + CONN + U) + npoin * 2 * XY,
+        "rhs": ncell * (U + U + 16 * W + GEO + 40 * W + CONN + U + (6 * W if source else 0)) + npoin * 2 * XY,
+        "src": ncell * (CONN + GEO + 6 * W) + npoin * XY,
         "persson": ncell * (6 * W + 2 * W + GEO + W + 9 * W + CONN + 4 + 2 * W + 4 * W) + npoin * XY,
         "nodes": npoin * (3 * XY + 2 * XY),
         "geom": ncell * (CONN + W + XY) + npoin * XY,
