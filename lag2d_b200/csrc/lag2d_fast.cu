@@ -1169,11 +1169,23 @@ __host__ __device__ __forceinline__ void corner_m_T(double rhoct, double sdctr, 
 
 // transpose of the cell-centre state: rhoct = 1/tau, pctr = max(eps, ...),
 // sdctr = sqrt(max(eps, g pctr / rhoct)); adds into lu
-__host__ __device__ __forceinline__ void centre_T(const double u[4][6], double g, double lrho_in, double lsd,
-                                                  double lu[4][6]) {
+// 24 values of one cell in this thread's column of shared memory (stride
+// kAdjBlock), read as v(q, k)
+constexpr int kAdjBlock = 128;
+struct ColView {
+  const double *p;
+  __device__ __forceinline__ double operator()(int q, int k) const { return p[(q * 6 + k) * kAdjBlock]; }
+};
+struct ColRef {
+  double *p;
+  __device__ __forceinline__ double &operator()(int q, int k) const { return p[(q * 6 + k) * kAdjBlock]; }
+};
+
+template <typename UA, typename LU>
+__host__ __device__ __forceinline__ void centre_T(const UA &u, double g, double lrho_in, double lsd, const LU &lu) {
   const double eps = 1.0e-6;
-  const double rhoct = 1.0 / u[0][0];
-  const double kin = u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0]);
+  const double rhoct = 1.0 / u(0, 0);
+  const double kin = u(3, 0) - 0.5 * (u(1, 0) * u(1, 0) + u(2, 0) * u(2, 0));
   const double pe = (g - 1.0) * rhoct * kin;
   const double pctr = fmax(eps, pe);
   const double se = g * pctr / rhoct;
@@ -1186,17 +1198,18 @@ __host__ __device__ __forceinline__ void centre_T(const double u[4][6], double g
   }
   if (pe > eps) {
     lrho += lp * (g - 1.0) * kin;
-    lu[3][0] += lp * (g - 1.0) * rhoct;
-    lu[1][0] -= lp * (g - 1.0) * rhoct * u[1][0];
-    lu[2][0] -= lp * (g - 1.0) * rhoct * u[2][0];
+    lu(3, 0) += lp * (g - 1.0) * rhoct;
+    lu(1, 0) -= lp * (g - 1.0) * rhoct * u(1, 0);
+    lu(2, 0) -= lp * (g - 1.0) * rhoct * u(2, 0);
   }
-  lu[0][0] += -lrho * rhoct * rhoct;
+  lu(0, 0) += -lrho * rhoct * rhoct;
 }
 
 // vertex state transpose: st[q] = sum_{k<mdegr} u[q][k] b[k], rhovt = 1/st0,
 // ke = st3 - (st1^2 + st2^2)/2
+template <typename LU>
 __host__ __device__ __forceinline__ void vertex_T(const double *b, int mdegr, const double st[4], double lrhovt,
-                                                  double lke, double lst1, double lst2, double lu[4][6]) {
+                                                  double lke, double lst1, double lst2, const LU &lu) {
   double lst[4];
   lst[0] = -lrhovt / (st[0] * st[0]);
   lst[1] = lst1 - lke * st[1];
@@ -1204,30 +1217,40 @@ __host__ __device__ __forceinline__ void vertex_T(const double *b, int mdegr, co
   lst[3] = lke;
   for (int q = 0; q < 4; q++)
     for (int k = 0; k < 6; k++)
-      if (k < mdegr) lu[q][k] += lst[q] * b[k];
+      if (k < mdegr) lu(q, k) += lst[q] * b[k];
 }
 
 // Reverse of the corner pass of quad iq: reads the node-sum adjoints lS at
 // its nodes plus the RHS pass's adjoints of its partials (lP); adds the cell
 // DOF adjoint into lU and writes the node contributions (x, y, u*_prev,
-// v*_prev) into pbuf.
+// v*_prev) into pbuf.  The cell's DOFs are copied asynchronously into this
+// thread's shared-memory column at entry and their adjoints accumulated
+// there (stride kAdjBlock).
+constexpr int kAcorStage = 48;
 template <typename R>
-__host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
+__device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
   if (iq >= d.nquad) return;
   const int e = iq + d.ntria;
   const size_t nq = d.nquad;
+  for (int v = 0; v < 24; v++)
+    __pipeline_memcpy_async(col + v * kAdjBlock, d.Us + v * (size_t)d.ncell + e, sizeof(double));
+  __pipeline_commit();
   const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
-  double xp[9][2], c[36], D[16];
-  node_xy_rel(L, xp);
-  cross36_rel(xp, c);
+  double c[36], D[16];
+  {
+    double xp[9][2];
+    node_xy_rel(L, xp);
+    cross36_rel(xp, c);
+  }
   detpoly(c, D);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-  double u[4][6];
-  load_u(d, d.Us, e, u);
-  const double rhoct = 1.0 / u[0][0];
-  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
+  __pipeline_wait_prior(0);
+  const ColView u{col};
+  const ColRef lu{col + 24 * kAdjBlock};
+  const double rhoct = 1.0 / u(0, 0);
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u(3, 0) - 0.5 * (u(1, 0) * u(1, 0) + u(2, 0) * u(2, 0))));
   const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
   // the stage's sub-cell density corrections come from the forward pass;
   // corr = cdrho (msub / vsub - masel / volel) gives the sub-cell masses
@@ -1241,8 +1264,7 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
     const double rho_sub = d.cdrho != 0.0 ? d.msub[isg * nq + iq] / vsub4[isg] - corr[isg] / d.cdrho : 0.0;
     masel4[isg] = volel4[isg] * rho_sub;
   }
-  double lu[4][6];
-  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
+  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu(q, k) = 0.0;
   double lX[3][3], lY[3][3];
   for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
   double lrho = 0.0, lsd = 0.0, lcr[4] = {0, 0, 0, 0};
@@ -1253,7 +1275,7 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
     for (int q = 0; q < 4; q++) {
       double acc = 0.0;
       for (int kk = 0; kk < 6; kk++)
-        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
+        if (kk < d.mdegr) acc += u(q, kk) * b[kk];
       st[q] = acc;
     }
     const double rhovt = 1.0 / st[0];
@@ -1336,8 +1358,8 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
       double ee[4];
 #pragma unroll
       for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
-      const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
-      const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
+      const double t0 = u(0, 0) + u(0, 1) * dr + u(0, 3) * (0.5 * dr * dr - G.g19) - u(0, 4) * G.g20 - u(0, 5) * G.g21;
+      const double t1 = u(0, 2) + u(0, 5) * dr, t2 = 0.5 * u(0, 4);
       // point arithmetic in R (FP32 in the mixed adjoint), rows added in FP64
       const R t0r = R(t0), t1r = R(t1), t2r = R(t2), lm = R(lmasel), wi = R(0.25 * g5w(i));
       const R e0 = R(ee[0]), e1 = R(ee[1]), e2 = R(ee[2]), e3 = R(ee[3]);
@@ -1360,12 +1382,12 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
         Ls[3] += ldet * s * s * s;
       }
       const double a0 = m0, a1 = m1, a2 = m2;
-      lu[0][0] += a0;
-      lu[0][1] += dr * a0;
-      lu[0][2] += a1;
-      lu[0][3] += (0.5 * dr * dr - G.g19) * a0;
-      lu[0][4] += 0.5 * a2 - G.g20 * a0;
-      lu[0][5] += dr * a1 - G.g21 * a0;
+      lu(0, 0) += a0;
+      lu(0, 1) += dr * a0;
+      lu(0, 2) += a1;
+      lu(0, 3) += (0.5 * dr * dr - G.g19) * a0;
+      lu(0, 4) += 0.5 * a2 - G.g20 * a0;
+      lu(0, 5) += dr * a1 - G.g21 * a0;
       double rp = 1.0;
 #pragma unroll
       for (int mm = 0; mm < 4; mm++) {
@@ -1382,7 +1404,11 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   subareas_T(lv4, lc36);
   double lxp[9][2];
   for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
-  cross36_T(xp, lc36, lxp);
+  {
+    double xp[9][2];
+    node_xy_rel(L, xp);
+    cross36_T(xp, lc36, lxp);
+  }
   const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
   const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
   for (int k = 0; k < 9; k++) {
@@ -1392,7 +1418,7 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
     a.pbuf[(5 * 9 + k) * nq + iq] = 0.0;
   }
   for (int q = 0; q < 4; q++)
-    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * (size_t)d.ncell + e] += lu[q][k];
+    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * (size_t)d.ncell + e] += lu(q, k);
 }
 
 // Reverse of the volume integral of the RHS pass (5x5 Gauss-Lobatto,
@@ -1402,10 +1428,9 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
 // the node adjoints).  R = double for the FP64 adjoint; R = float for the
 // FP32-mixed one, where the point arithmetic and the per-row moments are FP32
 // and the rows are added into the FP64 adjoints.
-template <typename R>
-__host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G, const double u[4][6],
-                                               const double lR[4][6], double g, double eps, double lu[4][6],
-                                               double lX[3][3], double lY[3][3]) {
+template <typename R, typename UA, typename LA, typename LU>
+__host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G, const UA &u, const LA &lR, double g,
+                                               double eps, const LU &lu, double lX[3][3], double lY[3][3]) {
 #pragma unroll 1
   for (int i = 0; i < 5; i++) {
     const double r = l5p(i), dr = r - G.rc;
@@ -1423,15 +1448,12 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
     R ra[4], rb[4], rc2[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      ra[q] = R(u[q][0] + u[q][1] * dr + u[q][3] * (0.5 * dr * dr - G.g19) - u[q][4] * G.g20 - u[q][5] * G.g21);
-      rb[q] = R(u[q][2] + u[q][5] * dr);
-      rc2[q] = R(0.5 * u[q][4]);
+      ra[q] = R(u(q, 0) + u(q, 1) * dr + u(q, 3) * (0.5 * dr * dr - G.g19) - u(q, 4) * G.g20 - u(q, 5) * G.g21);
+      rb[q] = R(u(q, 2) + u(q, 5) * dr);
+      rc2[q] = R(0.5 * u(q, 4));
     }
-    R lR1[4][5];
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-#pragma unroll
-      for (int kk = 0; kk < 5; kk++) lR1[q][kk] = R(lR[q][kk + 1]);
+    // the RHS adjoints of modes 1..5, read where used (not held across the row)
+    auto lR1 = [&](int q, int kk) { return R(lR(q, kk + 1)); };
     R m0[4] = {0, 0, 0, 0}, m1[4] = {0, 0, 0, 0}, m2[4] = {0, 0, 0, 0};
     R Mxr[3] = {0, 0, 0}, Mxs[3] = {0, 0, 0}, Myr[3] = {0, 0, 0}, Mys[3] = {0, 0, 0};
     const R wi = R(l5w(i)), drr = R(dr), gm1 = R(g - 1.0), epsr = R(eps), half = R(0.5), one = R(1);
@@ -1466,10 +1488,10 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
 #pragma unroll
       for (int kk = 0; kk < 5; kk++) {
         const R fv = gd0[kk] * un[1] + gd1[kk] * un[2];
-        const R lfv = -lR1[0][kk] * w + lR1[3][kk] * wp;
-        lwp += lR1[3][kk] * fv + lR1[1][kk] * gd0[kk] + lR1[2][kk] * gd1[kk];
-        lgd0[kk] = lR1[1][kk] * wp + lfv * un[1];
-        lgd1[kk] = lR1[2][kk] * wp + lfv * un[2];
+        const R lfv = -lR1(0, kk) * w + lR1(3, kk) * wp;
+        lwp += lR1(3, kk) * fv + lR1(1, kk) * gd0[kk] + lR1(2, kk) * gd1[kk];
+        lgd0[kk] = lR1(1, kk) * wp + lfv * un[1];
+        lgd1[kk] = lR1(2, kk) * wp + lfv * un[2];
         lun1 += lfv * gd0[kk];
         lun2 += lfv * gd1[kk];
       }
@@ -1505,12 +1527,12 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const double a0 = m0[q], a1 = m1[q], a2 = m2[q];
-      lu[q][0] += a0;
-      lu[q][1] += dr * a0;
-      lu[q][2] += a1;
-      lu[q][3] += (0.5 * dr * dr - G.g19) * a0;
-      lu[q][4] += 0.5 * a2 - G.g20 * a0;
-      lu[q][5] += dr * a1 - G.g21 * a0;
+      lu(q, 0) += a0;
+      lu(q, 1) += dr * a0;
+      lu(q, 2) += a1;
+      lu(q, 3) += (0.5 * dr * dr - G.g19) * a0;
+      lu(q, 4) += 0.5 * a2 - G.g20 * a0;
+      lu(q, 5) += dr * a1 - G.g21 * a0;
     }
 #pragma unroll
     for (int aa = 0; aa < 3; aa++)
@@ -1522,26 +1544,33 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
   }
 }
 
+
 // Reverse of the RHS pass of quad iq (the RHS written, no fused update):
 // from lR adds into lU, writes pbuf (x, y, u*_prev = 0, v*_prev = 0, u*_new,
 // v*_new) and the adjoints of the node partial sums the face integral reads
-// (lP, consumed by a_corner).
+// (lP, consumed by a_corner).  The Taylor-Green source's transpose is a_src.
+// The cell's DOFs and RHS adjoints (48 values) are copied asynchronously into
+// this thread's shared-memory column at entry and read from there; the 24
+// DOF adjoints are accumulated in the same column.
+constexpr int kArhsStage = 72;
 template <typename R>
-__host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
+__device__ void a_rhs(const Dev &d, const Adj &a, int iq, double *col) {
   if (iq >= d.nquad) return;
   const int e = iq + d.ntria;
   const size_t nq = d.nquad, nc = d.ncell;
+  for (int v = 0; v < 24; v++) {
+    __pipeline_memcpy_async(col + v * kAdjBlock, d.Us + v * nc + e, sizeof(double));
+    __pipeline_memcpy_async(col + (24 + v) * kAdjBlock, a.lR + v * nc + e, sizeof(double));
+  }
+  __pipeline_commit();
   const double eps = 1.0e-6, g = d.gamlg;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-  double u[4][6];
-  load_u(d, d.Us, e, u);
-  double lR[4][6];
-  for (int q = 0; q < 4; q++)
-    for (int k = 0; k < 6; k++) lR[q][k] = a.lR[(q * 6 + k) * nc + e];
-  double lu[4][6];
-  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
+  __pipeline_wait_prior(0);
+  const ColView u{col}, lR{col + 24 * kAdjBlock};
+  const ColRef lu{col + 48 * kAdjBlock};
+  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu(q, k) = 0.0;
   double lX[3][3], lY[3][3];
   for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
   // ---- face integral (f_rhs3): transpose of f = (P3, P4) + u* P0 - (P1, P2),
@@ -1566,10 +1595,10 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     const double f0 = P3 + (un * P0 - P1), f1 = P4 + (vn * P0 - P2);
     double ltw = 0, lf0 = 0, lf1 = 0, lfe = 0;
     for (int kk = 0; kk < 6; kk++) {
-      ltw += lR[0][kk] * b[kk];
-      lf0 += lR[1][kk] * b[kk];
-      lf1 += lR[2][kk] * b[kk];
-      lfe += lR[3][kk] * b[kk];
+      ltw += lR(0, kk) * b[kk];
+      lf0 += lR(1, kk) * b[kk];
+      lf1 += lR(2, kk) * b[kk];
+      lfe += lR(3, kk) * b[kk];
     }
     lf0 += lfe * un;
     lf1 += lfe * vn;
@@ -1594,11 +1623,35 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     }
   }
   vol_T<R>(L, G, u, lR, g, eps, lu, lX, lY);
-  // ---- Taylor-Green source: cos and sin of pi x at the Gauss points by angle
-  // addition from the centre node, as in the forward pass
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  for (int k = 0; k < 9; k++) {
+    a.pbuf[(0 * 9 + k) * nq + iq] = lX[A[k]][B[k]];
+    a.pbuf[(1 * 9 + k) * nq + iq] = lY[A[k]][B[k]];
+  }
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu(q, k);
+}
+
+// Reverse of the Taylor-Green source (f_tgv_src) of quad iq: from the energy
+// rows of lR adds the node-coordinate adjoints into pbuf (after a_rhs).  cos
+// and sin of pi x at the Gauss points by angle addition from the centre node.
+__host__ __device__ void a_src(const Dev &d, const Adj &a, int iq) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  const size_t nq = d.nquad, nc = d.ncell;
+  const double g = d.gamlg;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double lR3[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) lR3[k] = a.lR[(18 + k) * nc + e];
+  double lX[3][3], lY[3][3];
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
   double lxp[9][2];
   for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
-  if (d.ncase == 1) {
+  {
     double xp[9][2], c[36], D[16];
     node_xy_rel(L, xp);
     cross36_rel(xp, c);
@@ -1623,9 +1676,9 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
       double ee[4];
 #pragma unroll
       for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
-      // lsrc = sum_k lR[3][k] b_k(s) = sa + ds (sb + sc ds) along the row
-      const double sa = lR[3][0] + lR[3][1] * dr + lR[3][3] * (0.5 * dr * dr - G.g19) - lR[3][4] * G.g20 - lR[3][5] * G.g21;
-      const double sb = lR[3][2] + lR[3][5] * dr, sc = 0.5 * lR[3][4];
+      // lsrc = sum_k lR3[k] b_k(s) = sa + ds (sb + sc ds) along the row
+      const double sa = lR3[0] + lR3[1] * dr + lR3[3] * (0.5 * dr * dr - G.g19) - lR3[4] * G.g20 - lR3[5] * G.g21;
+      const double sb = lR3[2] + lR3[5] * dr, sc = 0.5 * lR3[4];
       double Mx[3] = {0, 0, 0}, My[3] = {0, 0, 0}, Ls[4] = {0, 0, 0, 0};
       const double wi = g5w(i);
 #pragma unroll 1
@@ -1691,11 +1744,9 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
   const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
   const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
   for (int k = 0; k < 9; k++) {
-    a.pbuf[(0 * 9 + k) * nq + iq] = lxp[k][0] + lX[A[k]][B[k]];
-    a.pbuf[(1 * 9 + k) * nq + iq] = lxp[k][1] + lY[A[k]][B[k]];
+    a.pbuf[(0 * 9 + k) * nq + iq] += lxp[k][0] + lX[A[k]][B[k]];
+    a.pbuf[(1 * 9 + k) * nq + iq] += lxp[k][1] + lY[A[k]][B[k]];
   }
-  for (int q = 0; q < 4; q++)
-    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu[q][k];
 }
 
 // Gather of the per-(quad, node) contributions into the node adjoints:
@@ -1896,12 +1947,22 @@ __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + th
 // compiled for: 3 (168 registers) in the FP32-mixed adjoint (reverse sweep
 // 15.65 -> 15.08 ms per step on the 1024x1024 Taylor-Green mesh), 1 (255)
 // in the FP64 one (3 would cost 12%)
+#ifndef LAG2D_AREV_MINB_F32
+#define LAG2D_AREV_MINB_F32 3
+#endif
 template <typename R>
-constexpr int arev_minb() { return sizeof(R) == 4 ? 3 : 1; }
+constexpr int arev_minb() { return sizeof(R) == 4 ? LAG2D_AREV_MINB_F32 : 1; }
 template <typename R>
-__global__ void __launch_bounds__(128, arev_minb<R>()) k_a_corner(Dev d, Adj a) { a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(kAdjBlock, arev_minb<R>()) k_a_corner(Dev d, Adj a) {
+  extern __shared__ double acor_stage[];
+  a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x, acor_stage + threadIdx.x);
+}
 template <typename R>
-__global__ void __launch_bounds__(128, arev_minb<R>()) k_a_rhs(Dev d, Adj a) { a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(kAdjBlock, arev_minb<R>()) k_a_rhs(Dev d, Adj a) {
+  extern __shared__ double arhs_stage[];
+  a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x, arhs_stage + threadIdx.x);
+}
+__global__ void __launch_bounds__(128) k_a_src(Dev d, Adj a) { a_src(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_gather(Dev d, Adj a, int nv) { a_gather(d, a, blockIdx.x * blockDim.x + threadIdx.x, nv); }
 __global__ void k_a_gather_solve(Dev d, Adj a) { a_gather_solve(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_update(Dev d, Adj a, double alfa, const double *dtp, int fold) {
@@ -1939,16 +2000,25 @@ void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double
   fast::k_a_centre<<<bp, 256, 0, st>>>(d, a);
   fast::k_a_nodes<<<bp, 256, 0, st>>>(d, a, alfa, dtp, fold);
   fast::k_a_update<<<bc, 256, 0, st>>>(d, a, alfa, dtp, fold_u);
-  if (mixed) fast::k_a_rhs<float><<<bq, 128, 0, st>>>(d, a);
-  else fast::k_a_rhs<double><<<bq, 128, 0, st>>>(d, a);
+  constexpr int arhs_smem = fast::kArhsStage * fast::kAdjBlock * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(fast::k_a_rhs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, arhs_smem);
+    cudaFuncSetAttribute(fast::k_a_rhs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, arhs_smem);
+    attr = true;
+  }
+  if (mixed) fast::k_a_rhs<float><<<bq, fast::kAdjBlock, arhs_smem, st>>>(d, a);
+  else fast::k_a_rhs<double><<<bq, fast::kAdjBlock, arhs_smem, st>>>(d, a);
+  if (d.ncase == 1) fast::k_a_src<<<bq, 128, 0, st>>>(d, a);
   launch_tri_adjoint_rhs(d, a, st);
   fast::k_a_gather_solve<<<bp, 256, 0, st>>>(d, a);
-  if (mixed) fast::k_a_corner<float><<<bq, 128, 0, st>>>(d, a);
-  else fast::k_a_corner<double><<<bq, 128, 0, st>>>(d, a);
+  constexpr int acor_smem = fast::kAcorStage * fast::kAdjBlock * sizeof(double);
+  if (mixed) fast::k_a_corner<float><<<bq, fast::kAdjBlock, acor_smem, st>>>(d, a);
+  else fast::k_a_corner<double><<<bq, fast::kAdjBlock, acor_smem, st>>>(d, a);
   launch_tri_adjoint_corner(d, a, st);
   fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
 }
-int adjoint_stage_launches(const Dev &d) { return d.ntria > 0 ? 9 : 7; }
+int adjoint_stage_launches(const Dev &d) { return (d.ntria > 0 ? 9 : 7) + (d.ncase == 1 && d.nquad > 0); }
 
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }
