@@ -17,8 +17,17 @@
 //    the RHS pass.
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
+#ifndef LAG2D_CORR_MINB
+#define LAG2D_CORR_MINB 4
+#endif
 #ifndef LAG2D_FACES_MINB
 #define LAG2D_FACES_MINB 4
+#endif
+#ifndef LAG2D_ASRC_SPLIT
+#define LAG2D_ASRC_SPLIT 0
+#endif
+#ifndef LAG2D_FACES_SYNC
+#define LAG2D_FACES_SYNC 0
 #endif
 #include <math.h>
 
@@ -528,13 +537,15 @@ __host__ __device__ void f_corner_corr(const Dev &d, int iq) {
   // per point and one division per sub-cell instead of one division per point.
   // tau is scaled by the cell-average tau first (rtc), so that the product of
   // the 25 scaled values stays near 1; masel = rtc num / den.
+  // Sub-cells 0 and 3 (r in [-1, 0]) share their Gauss rows, and so do 1 and
+  // 2 (r in [0, 1]): each row's det J and tau coefficients serve both, whose
+  // two fraction chains (s in [-1, 0] and [0, 1]) run side by side.
   const double rtc = 1.0 / u[0];
 #pragma unroll
-  for (int isg = 0; isg < 4; isg++) {
-    const double unksgq = (1.0 / vsub4[isg]) * d.msub[isg * (size_t)d.nquad + iq];
-    const double ofr = (isg == 0 || isg == 3) ? -1.0 : 1.0;
-    const double ofs = (isg == 0 || isg == 1) ? -1.0 : 1.0;
-    double num = 0.0, den = 1.0;
+  for (int h = 0; h < 2; h++) {
+    const double ofr = h == 0 ? -1.0 : 1.0;
+    const int ilo = h == 0 ? 0 : 1, ihi = h == 0 ? 3 : 2;  // s in [-1, 0], [0, 1]
+    double nlo = 0.0, dlo = 1.0, nhi = 0.0, dhi = 1.0;
 #pragma unroll 1
     for (int i = 0; i < 5; i++) {
       const double r = (g5p(i) + ofr) / 2.0;
@@ -548,17 +559,34 @@ __host__ __device__ void f_corner_corr(const Dev &d, int iq) {
       const double wi = 0.25 * g5w(i);
 #pragma unroll
       for (int j = 0; j < 5; j++) {
-        const double s = (g5p(j) + ofs) / 2.0;
-        const double ds = s - G.sc;
-        const double tau = t0 + ds * (t1 + t2 * ds);
-        const double det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
-        num = num * tau + ((wi * g5w(j)) * det) * den;
-        den = den * tau;
+        const double w = wi * g5w(j);
+        {
+          const double s = (g5p(j) - 1.0) / 2.0;
+          const double ds = s - G.sc;
+          const double tau = t0 + ds * (t1 + t2 * ds);
+          const double det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
+          nlo = nlo * tau + (w * det) * dlo;
+          dlo = dlo * tau;
+        }
+        {
+          const double s = (g5p(j) + 1.0) / 2.0;
+          const double ds = s - G.sc;
+          const double tau = t0 + ds * (t1 + t2 * ds);
+          const double det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
+          nhi = nhi * tau + (w * det) * dhi;
+          dhi = dhi * tau;
+        }
       }
     }
-    const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
     // 1 / uqsgc = masel / volel with masel = rtc num / den
-    d.corr[isg * (size_t)d.nquad + iq] = d.cdrho * (unksgq - (rtc * num) / (den * volel));
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int isg = t == 0 ? ilo : ihi;
+      const double num = t == 0 ? nlo : nhi, den = t == 0 ? dlo : dhi;
+      const double unksgq = (1.0 / vsub4[isg]) * d.msub[isg * (size_t)d.nquad + iq];
+      const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
+      d.corr[isg * (size_t)d.nquad + iq] = d.cdrho * (unksgq - (rtc * num) / (den * volel));
+    }
   }
 }
 
@@ -570,8 +598,18 @@ __host__ __device__ void f_corner_corr(const Dev &d, int iq) {
 // between the vertex states.
 constexpr int kCornerBlock = 128;
 constexpr int kCornerStage = 28;
-__device__ void f_corner_faces(const Dev &d, int iq, double *col) {
-  if (iq >= d.nquad || d.sc_dev->done) return;
+__device__ void f_corner_faces(const Dev &d, int iq_in, double *col) {
+#if LAG2D_FACES_SYNC
+  // every thread of the block reaches the barriers below: a thread past the
+  // last quad works on the last quad and stores nothing
+  if (d.nquad <= 0 || d.sc_dev->done) return;
+  const bool live = iq_in < d.nquad;
+  const int iq = live ? iq_in : d.nquad - 1;
+#else
+  if (iq_in >= d.nquad || d.sc_dev->done) return;
+  const bool live = true;
+  const int iq = iq_in;
+#endif
   const int e = iq + d.ntria;
   {
     const size_t nc = d.ncell;
@@ -628,11 +666,17 @@ __device__ void f_corner_faces(const Dev &d, int iq, double *col) {
         P4 += pw * ay;
       }
     }
-    d.npart[(0 * 9 + k) * (size_t)d.nquad + iq] = P0;
-    d.npart[(1 * 9 + k) * (size_t)d.nquad + iq] = P1;
-    d.npart[(2 * 9 + k) * (size_t)d.nquad + iq] = P2;
-    d.npart[(3 * 9 + k) * (size_t)d.nquad + iq] = P3;
-    d.npart[(4 * 9 + k) * (size_t)d.nquad + iq] = P4;
+    if (live) {
+      d.npart[(0 * 9 + k) * (size_t)d.nquad + iq] = P0;
+      d.npart[(1 * 9 + k) * (size_t)d.nquad + iq] = P1;
+      d.npart[(2 * 9 + k) * (size_t)d.nquad + iq] = P2;
+      d.npart[(3 * 9 + k) * (size_t)d.nquad + iq] = P3;
+      d.npart[(4 * 9 + k) * (size_t)d.nquad + iq] = P4;
+    }
+#if LAG2D_FACES_SYNC
+    // keep the block's warps on the same stretch of this long unrolled code
+    __syncthreads();
+#endif
   }
 #undef CF_U
 #undef CF_CORR
@@ -839,13 +883,15 @@ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, doubl
       }
       rtau[0] = inv;
     }
+    double SA = 0, SB = 0, TA = 0, TB = 0, X1 = 0, X2 = 0, X3 = 0, X4 = 0;
+    double Y1 = 0, Y2 = 0, Y3 = 0, Y4 = 0, E1 = 0, E2 = 0, E3 = 0, E4 = 0;
 #pragma unroll
     for (int j = 0; j < 5; j++) {
       const double s = l5p(j), ds = s - G.sc;
       double ls[3], dls[3];
       lag3(s, ls);
       dlag3(s, dls);
-      const double w = wi * l5w(j);
+      const double wj = l5w(j);
       const double xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
       const double yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
       const double xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
@@ -855,24 +901,39 @@ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, doubl
       for (int q = 1; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * RHS_U(q, 4) * ds);
       const double rhoad = rtau[j];
       const double pres = fmax(eps, (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2])));
-      // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
-      double gd0[5], gd1[5];
-      gd0[0] = ys;       gd1[0] = -xs;
-      gd0[1] = -yr;      gd1[1] = xr;
-      gd0[2] = ys * dr;  gd1[2] = -xs * dr;
-      gd0[3] = -yr * ds; gd1[3] = xr * ds;
-      gd0[4] = ys * ds - yr * dr;
-      gd1[4] = -xs * ds + xr * dr;
-      const double wp = w * pres;
-#pragma unroll
-      for (int kk = 0; kk < 5; kk++) {
-        const double fv = gd0[kk] * un[1] + gd1[kk] * un[2];
-        ul[kk + 1] -= fv * w;
-        p0[kk + 1] += gd0[kk] * wp;
-        p1[kk + 1] += gd1[kk] * wp;
-        el[kk + 1] += fv * wp;
-      }
+      // G . grad_xi b for b = 2..6 with dbdr = (1, 0, dr, 0, ds), dbds = (0,
+      // 1, 0, ds, dr): G0 = (ys, -yr, ys dr, -yr ds, ys ds - yr dr), G1 =
+      // (-xs, xr, -xs dr, xr ds, -xs ds + xr dr), and the mass flux
+      // G0 u + G1 v = (A, B, dr A, ds B, ds A + dr B).  dr is fixed along the
+      // row, so each equation needs only 4 sums over the row: of A, B (or ys,
+      // yr, xs, xr) weighted by w_j and by w_j ds.
+      const double A = ys * un[1] - xs * un[2], B = xr * un[2] - yr * un[1];
+      const double wd = wj * ds, pw = wj * pres, pwd = wd * pres;
+      SA += wj * A; SB += wj * B; TA += wd * A; TB += wd * B;
+      X1 += pw * ys; X2 += pw * yr; X3 += pwd * yr; X4 += pwd * ys;
+      Y1 += pw * xs; Y2 += pw * xr; Y3 += pwd * xr; Y4 += pwd * xs;
+      E1 += pw * A; E2 += pw * B; E3 += pwd * B; E4 += pwd * A;
     }
+    ul[1] -= wi * SA;
+    ul[2] -= wi * SB;
+    ul[3] -= wi * (dr * SA);
+    ul[4] -= wi * TB;
+    ul[5] -= wi * (TA + dr * SB);
+    p0[1] += wi * X1;
+    p0[2] -= wi * X2;
+    p0[3] += wi * (dr * X1);
+    p0[4] -= wi * X3;
+    p0[5] += wi * (X4 - dr * X2);
+    p1[1] -= wi * Y1;
+    p1[2] += wi * Y2;
+    p1[3] -= wi * (dr * Y1);
+    p1[4] += wi * Y3;
+    p1[5] += wi * (dr * Y2 - Y4);
+    el[1] += wi * E1;
+    el[2] += wi * E2;
+    el[3] += wi * (dr * E1);
+    el[4] += wi * E3;
+    el[5] += wi * (E4 + dr * E2);
   }
   if (d.ncase == 1) {
     // Taylor-Green energy source, computed by k_tgv_src2 before the corner pass
@@ -1169,23 +1230,11 @@ __host__ __device__ __forceinline__ void corner_m_T(double rhoct, double sdctr, 
 
 // transpose of the cell-centre state: rhoct = 1/tau, pctr = max(eps, ...),
 // sdctr = sqrt(max(eps, g pctr / rhoct)); adds into lu
-// 24 values of one cell in this thread's column of shared memory (stride
-// kAdjBlock), read as v(q, k)
-constexpr int kAdjBlock = 128;
-struct ColView {
-  const double *p;
-  __device__ __forceinline__ double operator()(int q, int k) const { return p[(q * 6 + k) * kAdjBlock]; }
-};
-struct ColRef {
-  double *p;
-  __device__ __forceinline__ double &operator()(int q, int k) const { return p[(q * 6 + k) * kAdjBlock]; }
-};
-
-template <typename UA, typename LU>
-__host__ __device__ __forceinline__ void centre_T(const UA &u, double g, double lrho_in, double lsd, const LU &lu) {
+__host__ __device__ __forceinline__ void centre_T(const double u[4][6], double g, double lrho_in, double lsd,
+                                                  double lu[4][6]) {
   const double eps = 1.0e-6;
-  const double rhoct = 1.0 / u(0, 0);
-  const double kin = u(3, 0) - 0.5 * (u(1, 0) * u(1, 0) + u(2, 0) * u(2, 0));
+  const double rhoct = 1.0 / u[0][0];
+  const double kin = u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0]);
   const double pe = (g - 1.0) * rhoct * kin;
   const double pctr = fmax(eps, pe);
   const double se = g * pctr / rhoct;
@@ -1198,18 +1247,17 @@ __host__ __device__ __forceinline__ void centre_T(const UA &u, double g, double 
   }
   if (pe > eps) {
     lrho += lp * (g - 1.0) * kin;
-    lu(3, 0) += lp * (g - 1.0) * rhoct;
-    lu(1, 0) -= lp * (g - 1.0) * rhoct * u(1, 0);
-    lu(2, 0) -= lp * (g - 1.0) * rhoct * u(2, 0);
+    lu[3][0] += lp * (g - 1.0) * rhoct;
+    lu[1][0] -= lp * (g - 1.0) * rhoct * u[1][0];
+    lu[2][0] -= lp * (g - 1.0) * rhoct * u[2][0];
   }
-  lu(0, 0) += -lrho * rhoct * rhoct;
+  lu[0][0] += -lrho * rhoct * rhoct;
 }
 
 // vertex state transpose: st[q] = sum_{k<mdegr} u[q][k] b[k], rhovt = 1/st0,
 // ke = st3 - (st1^2 + st2^2)/2
-template <typename LU>
 __host__ __device__ __forceinline__ void vertex_T(const double *b, int mdegr, const double st[4], double lrhovt,
-                                                  double lke, double lst1, double lst2, const LU &lu) {
+                                                  double lke, double lst1, double lst2, double lu[4][6]) {
   double lst[4];
   lst[0] = -lrhovt / (st[0] * st[0]);
   lst[1] = lst1 - lke * st[1];
@@ -1217,40 +1265,30 @@ __host__ __device__ __forceinline__ void vertex_T(const double *b, int mdegr, co
   lst[3] = lke;
   for (int q = 0; q < 4; q++)
     for (int k = 0; k < 6; k++)
-      if (k < mdegr) lu(q, k) += lst[q] * b[k];
+      if (k < mdegr) lu[q][k] += lst[q] * b[k];
 }
 
 // Reverse of the corner pass of quad iq: reads the node-sum adjoints lS at
 // its nodes plus the RHS pass's adjoints of its partials (lP); adds the cell
 // DOF adjoint into lU and writes the node contributions (x, y, u*_prev,
-// v*_prev) into pbuf.  The cell's DOFs are copied asynchronously into this
-// thread's shared-memory column at entry and their adjoints accumulated
-// there (stride kAdjBlock).
-constexpr int kAcorStage = 48;
+// v*_prev) into pbuf.
 template <typename R>
-__device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
+__host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   if (iq >= d.nquad) return;
   const int e = iq + d.ntria;
   const size_t nq = d.nquad;
-  for (int v = 0; v < 24; v++)
-    __pipeline_memcpy_async(col + v * kAdjBlock, d.Us + v * (size_t)d.ncell + e, sizeof(double));
-  __pipeline_commit();
   const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
-  double c[36], D[16];
-  {
-    double xp[9][2];
-    node_xy_rel(L, xp);
-    cross36_rel(xp, c);
-  }
+  double xp[9][2], c[36], D[16];
+  node_xy_rel(L, xp);
+  cross36_rel(xp, c);
   detpoly(c, D);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-  __pipeline_wait_prior(0);
-  const ColView u{col};
-  const ColRef lu{col + 24 * kAdjBlock};
-  const double rhoct = 1.0 / u(0, 0);
-  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u(3, 0) - 0.5 * (u(1, 0) * u(1, 0) + u(2, 0) * u(2, 0))));
+  double u[4][6];
+  load_u(d, d.Us, e, u);
+  const double rhoct = 1.0 / u[0][0];
+  const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
   const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
   // the stage's sub-cell density corrections come from the forward pass;
   // corr = cdrho (msub / vsub - masel / volel) gives the sub-cell masses
@@ -1264,7 +1302,8 @@ __device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
     const double rho_sub = d.cdrho != 0.0 ? d.msub[isg * nq + iq] / vsub4[isg] - corr[isg] / d.cdrho : 0.0;
     masel4[isg] = volel4[isg] * rho_sub;
   }
-  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu(q, k) = 0.0;
+  double lu[4][6];
+  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
   double lX[3][3], lY[3][3];
   for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
   double lrho = 0.0, lsd = 0.0, lcr[4] = {0, 0, 0, 0};
@@ -1275,7 +1314,7 @@ __device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
     for (int q = 0; q < 4; q++) {
       double acc = 0.0;
       for (int kk = 0; kk < 6; kk++)
-        if (kk < d.mdegr) acc += u(q, kk) * b[kk];
+        if (kk < d.mdegr) acc += u[q][kk] * b[kk];
       st[q] = acc;
     }
     const double rhovt = 1.0 / st[0];
@@ -1358,8 +1397,8 @@ __device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
       double ee[4];
 #pragma unroll
       for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
-      const double t0 = u(0, 0) + u(0, 1) * dr + u(0, 3) * (0.5 * dr * dr - G.g19) - u(0, 4) * G.g20 - u(0, 5) * G.g21;
-      const double t1 = u(0, 2) + u(0, 5) * dr, t2 = 0.5 * u(0, 4);
+      const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
+      const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
       // point arithmetic in R (FP32 in the mixed adjoint), rows added in FP64
       const R t0r = R(t0), t1r = R(t1), t2r = R(t2), lm = R(lmasel), wi = R(0.25 * g5w(i));
       const R e0 = R(ee[0]), e1 = R(ee[1]), e2 = R(ee[2]), e3 = R(ee[3]);
@@ -1382,12 +1421,12 @@ __device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
         Ls[3] += ldet * s * s * s;
       }
       const double a0 = m0, a1 = m1, a2 = m2;
-      lu(0, 0) += a0;
-      lu(0, 1) += dr * a0;
-      lu(0, 2) += a1;
-      lu(0, 3) += (0.5 * dr * dr - G.g19) * a0;
-      lu(0, 4) += 0.5 * a2 - G.g20 * a0;
-      lu(0, 5) += dr * a1 - G.g21 * a0;
+      lu[0][0] += a0;
+      lu[0][1] += dr * a0;
+      lu[0][2] += a1;
+      lu[0][3] += (0.5 * dr * dr - G.g19) * a0;
+      lu[0][4] += 0.5 * a2 - G.g20 * a0;
+      lu[0][5] += dr * a1 - G.g21 * a0;
       double rp = 1.0;
 #pragma unroll
       for (int mm = 0; mm < 4; mm++) {
@@ -1404,11 +1443,7 @@ __device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
   subareas_T(lv4, lc36);
   double lxp[9][2];
   for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
-  {
-    double xp[9][2];
-    node_xy_rel(L, xp);
-    cross36_T(xp, lc36, lxp);
-  }
+  cross36_T(xp, lc36, lxp);
   const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
   const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
   for (int k = 0; k < 9; k++) {
@@ -1418,7 +1453,7 @@ __device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
     a.pbuf[(5 * 9 + k) * nq + iq] = 0.0;
   }
   for (int q = 0; q < 4; q++)
-    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * (size_t)d.ncell + e] += lu(q, k);
+    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * (size_t)d.ncell + e] += lu[q][k];
 }
 
 // Reverse of the volume integral of the RHS pass (5x5 Gauss-Lobatto,
@@ -1428,9 +1463,10 @@ __device__ void a_corner(const Dev &d, const Adj &a, int iq, double *col) {
 // the node adjoints).  R = double for the FP64 adjoint; R = float for the
 // FP32-mixed one, where the point arithmetic and the per-row moments are FP32
 // and the rows are added into the FP64 adjoints.
-template <typename R, typename UA, typename LA, typename LU>
-__host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G, const UA &u, const LA &lR, double g,
-                                               double eps, const LU &lu, double lX[3][3], double lY[3][3]) {
+template <typename R>
+__host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G, const double u[4][6],
+                                               const double lR[4][6], double g, double eps, double lu[4][6],
+                                               double lX[3][3], double lY[3][3]) {
 #pragma unroll 1
   for (int i = 0; i < 5; i++) {
     const double r = l5p(i), dr = r - G.rc;
@@ -1448,12 +1484,15 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
     R ra[4], rb[4], rc2[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      ra[q] = R(u(q, 0) + u(q, 1) * dr + u(q, 3) * (0.5 * dr * dr - G.g19) - u(q, 4) * G.g20 - u(q, 5) * G.g21);
-      rb[q] = R(u(q, 2) + u(q, 5) * dr);
-      rc2[q] = R(0.5 * u(q, 4));
+      ra[q] = R(u[q][0] + u[q][1] * dr + u[q][3] * (0.5 * dr * dr - G.g19) - u[q][4] * G.g20 - u[q][5] * G.g21);
+      rb[q] = R(u[q][2] + u[q][5] * dr);
+      rc2[q] = R(0.5 * u[q][4]);
     }
-    // the RHS adjoints of modes 1..5, read where used (not held across the row)
-    auto lR1 = [&](int q, int kk) { return R(lR(q, kk + 1)); };
+    R lR1[4][5];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int kk = 0; kk < 5; kk++) lR1[q][kk] = R(lR[q][kk + 1]);
     R m0[4] = {0, 0, 0, 0}, m1[4] = {0, 0, 0, 0}, m2[4] = {0, 0, 0, 0};
     R Mxr[3] = {0, 0, 0}, Mxs[3] = {0, 0, 0}, Myr[3] = {0, 0, 0}, Mys[3] = {0, 0, 0};
     const R wi = R(l5w(i)), drr = R(dr), gm1 = R(g - 1.0), epsr = R(eps), half = R(0.5), one = R(1);
@@ -1488,10 +1527,10 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
 #pragma unroll
       for (int kk = 0; kk < 5; kk++) {
         const R fv = gd0[kk] * un[1] + gd1[kk] * un[2];
-        const R lfv = -lR1(0, kk) * w + lR1(3, kk) * wp;
-        lwp += lR1(3, kk) * fv + lR1(1, kk) * gd0[kk] + lR1(2, kk) * gd1[kk];
-        lgd0[kk] = lR1(1, kk) * wp + lfv * un[1];
-        lgd1[kk] = lR1(2, kk) * wp + lfv * un[2];
+        const R lfv = -lR1[0][kk] * w + lR1[3][kk] * wp;
+        lwp += lR1[3][kk] * fv + lR1[1][kk] * gd0[kk] + lR1[2][kk] * gd1[kk];
+        lgd0[kk] = lR1[1][kk] * wp + lfv * un[1];
+        lgd1[kk] = lR1[2][kk] * wp + lfv * un[2];
         lun1 += lfv * gd0[kk];
         lun2 += lfv * gd1[kk];
       }
@@ -1527,12 +1566,12 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const double a0 = m0[q], a1 = m1[q], a2 = m2[q];
-      lu(q, 0) += a0;
-      lu(q, 1) += dr * a0;
-      lu(q, 2) += a1;
-      lu(q, 3) += (0.5 * dr * dr - G.g19) * a0;
-      lu(q, 4) += 0.5 * a2 - G.g20 * a0;
-      lu(q, 5) += dr * a1 - G.g21 * a0;
+      lu[q][0] += a0;
+      lu[q][1] += dr * a0;
+      lu[q][2] += a1;
+      lu[q][3] += (0.5 * dr * dr - G.g19) * a0;
+      lu[q][4] += 0.5 * a2 - G.g20 * a0;
+      lu[q][5] += dr * a1 - G.g21 * a0;
     }
 #pragma unroll
     for (int aa = 0; aa < 3; aa++)
@@ -1544,114 +1583,12 @@ __host__ __device__ __forceinline__ void vol_T(const Loaded &L, const CellGeo &G
   }
 }
 
-
-// Reverse of the RHS pass of quad iq (the RHS written, no fused update):
-// from lR adds into lU, writes pbuf (x, y, u*_prev = 0, v*_prev = 0, u*_new,
-// v*_new) and the adjoints of the node partial sums the face integral reads
-// (lP, consumed by a_corner).  The Taylor-Green source's transpose is a_src.
-// The cell's DOFs and RHS adjoints (48 values) are copied asynchronously into
-// this thread's shared-memory column at entry and read from there; the 24
-// DOF adjoints are accumulated in the same column.
-constexpr int kArhsStage = 72;
-template <typename R>
-__device__ void a_rhs(const Dev &d, const Adj &a, int iq, double *col) {
-  if (iq >= d.nquad) return;
-  const int e = iq + d.ntria;
-  const size_t nq = d.nquad, nc = d.ncell;
-  for (int v = 0; v < 24; v++) {
-    __pipeline_memcpy_async(col + v * kAdjBlock, d.Us + v * nc + e, sizeof(double));
-    __pipeline_memcpy_async(col + (24 + v) * kAdjBlock, a.lR + v * nc + e, sizeof(double));
-  }
-  __pipeline_commit();
-  const double eps = 1.0e-6, g = d.gamlg;
-  Loaded L;
-  load_cell(d, d.xs, d.ys, iq, L);
-  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-  __pipeline_wait_prior(0);
-  const ColView u{col}, lR{col + 24 * kAdjBlock};
-  const ColRef lu{col + 48 * kAdjBlock};
-  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu(q, k) = 0.0;
-  double lX[3][3], lY[3][3];
-  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
-  // ---- face integral (f_rhs3): transpose of f = (P3, P4) + u* P0 - (P1, P2),
-  // fe = u* . f, tw = u* . t per boundary node; the adjoints of the node
-  // partial sums P0..P4 go to a.lP for the corner pass's transpose, those of
-  // u* to pbuf, those of the mass-flux weights t to the face vectors
-  for (int k = 0; k < 9; k++) {
-    if (k == 8) {
-      for (int v = 2; v < 6; v++) a.pbuf[(v * 9 + k) * nq + iq] = 0.0;
-      for (int v = 0; v < 5; v++) a.lP[(v * 9 + k) * nq + iq] = 0.0;
-      continue;
-    }
-    double b[6];
-    node_basis2(G, k, b);
-    const int pn = d.ipq[k * d.nquad + iq];
-    const double un = d.us_new[pn], vn = d.vs_new[pn];
-    double tx, ty;
-    mass_flux_weights(L, k, tx, ty);
-    const double P0 = d.npart[(0 * 9 + k) * nq + iq], P1 = d.npart[(1 * 9 + k) * nq + iq];
-    const double P2 = d.npart[(2 * 9 + k) * nq + iq], P3 = d.npart[(3 * 9 + k) * nq + iq];
-    const double P4 = d.npart[(4 * 9 + k) * nq + iq];
-    const double f0 = P3 + (un * P0 - P1), f1 = P4 + (vn * P0 - P2);
-    double ltw = 0, lf0 = 0, lf1 = 0, lfe = 0;
-    for (int kk = 0; kk < 6; kk++) {
-      ltw += lR(0, kk) * b[kk];
-      lf0 += lR(1, kk) * b[kk];
-      lf1 += lR(2, kk) * b[kk];
-      lfe += lR(3, kk) * b[kk];
-    }
-    lf0 += lfe * un;
-    lf1 += lfe * vn;
-    const double lun = lfe * f0 + lf0 * P0 + ltw * tx;
-    const double lvn = lfe * f1 + lf1 * P0 + ltw * ty;
-    a.lP[(0 * 9 + k) * nq + iq] = lf0 * un + lf1 * vn;
-    a.lP[(1 * 9 + k) * nq + iq] = -lf0;
-    a.lP[(2 * 9 + k) * nq + iq] = -lf1;
-    a.lP[(3 * 9 + k) * nq + iq] = lf0;
-    a.lP[(4 * 9 + k) * nq + iq] = lf1;
-    a.pbuf[(2 * 9 + k) * nq + iq] = 0.0;
-    a.pbuf[(3 * 9 + k) * nq + iq] = 0.0;
-    a.pbuf[(4 * 9 + k) * nq + iq] = lun;
-    a.pbuf[(5 * 9 + k) * nq + iq] = lvn;
-    // t = sum over the node's outer corner faces of 2 w_mass,f an_f
-    const double ltx = ltw * un, lty = ltw * vn;
-    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
-      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
-      for (int f = 0; f < 2; f++)
-        if (wmas(isg, ivsg, f) != 0.0)
-          corner_an_T(isg, ivsg, f, ltx * (2.0 * wmas(isg, ivsg, f)), lty * (2.0 * wmas(isg, ivsg, f)), lX, lY);
-    }
-  }
-  vol_T<R>(L, G, u, lR, g, eps, lu, lX, lY);
-  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
-  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
-  for (int k = 0; k < 9; k++) {
-    a.pbuf[(0 * 9 + k) * nq + iq] = lX[A[k]][B[k]];
-    a.pbuf[(1 * 9 + k) * nq + iq] = lY[A[k]][B[k]];
-  }
-  for (int q = 0; q < 4; q++)
-    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu(q, k);
-}
-
-// Reverse of the Taylor-Green source (f_tgv_src) of quad iq: from the energy
-// rows of lR adds the node-coordinate adjoints into pbuf (after a_rhs).  cos
-// and sin of pi x at the Gauss points by angle addition from the centre node.
-__host__ __device__ void a_src(const Dev &d, const Adj &a, int iq) {
-  if (iq >= d.nquad) return;
-  const int e = iq + d.ntria;
-  const size_t nq = d.nquad, nc = d.ncell;
-  const double g = d.gamlg;
-  Loaded L;
-  load_cell(d, d.xs, d.ys, iq, L);
-  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-  double lR3[6];
-#pragma unroll
-  for (int k = 0; k < 6; k++) lR3[k] = a.lR[(18 + k) * nc + e];
-  double lX[3][3], lY[3][3];
-  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
-  double lxp[9][2];
-  for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
-  {
+// Transpose of the Taylor-Green source moments (f_tgv_src) of one quad: from
+// the energy rows lR3 of the RHS adjoint adds the node-coordinate adjoints
+// into lX, lY (tensor nodes) and lxp (through the det J polynomial).  cos and
+// sin of pi x at the Gauss points by angle addition from the centre node.
+__host__ __device__ __forceinline__ void src_T(const Loaded &L, const CellGeo &G, const double lR3[6], double g,
+                                               double lX[3][3], double lY[3][3], double lxp[9][2]) {
     double xp[9][2], c[36], D[16];
     node_xy_rel(L, xp);
     cross36_rel(xp, c);
@@ -1741,6 +1678,112 @@ __host__ __device__ void a_src(const Dev &d, const Adj &a, int iq) {
     detpoly_T(lD, lc36);
     cross36_T(xp, lc36, lxp);
   }
+
+// Reverse of the RHS pass of quad iq (the RHS written, no fused update):
+// from lR adds into lU, writes pbuf (x, y, u*_prev = 0, v*_prev = 0, u*_new,
+// v*_new) and the adjoints of the node partial sums the face integral reads
+// (lP, consumed by a_corner).
+template <typename R>
+__host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  const size_t nq = d.nquad, nc = d.ncell;
+  const double eps = 1.0e-6, g = d.gamlg;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double u[4][6];
+  load_u(d, d.Us, e, u);
+  double lR[4][6];
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) lR[q][k] = a.lR[(q * 6 + k) * nc + e];
+  double lu[4][6];
+  for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
+  double lX[3][3], lY[3][3];
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
+  // ---- face integral (f_rhs3): transpose of f = (P3, P4) + u* P0 - (P1, P2),
+  // fe = u* . f, tw = u* . t per boundary node; the adjoints of the node
+  // partial sums P0..P4 go to a.lP for the corner pass's transpose, those of
+  // u* to pbuf, those of the mass-flux weights t to the face vectors
+  for (int k = 0; k < 9; k++) {
+    if (k == 8) {
+      for (int v = 2; v < 6; v++) a.pbuf[(v * 9 + k) * nq + iq] = 0.0;
+      for (int v = 0; v < 5; v++) a.lP[(v * 9 + k) * nq + iq] = 0.0;
+      continue;
+    }
+    double b[6];
+    node_basis2(G, k, b);
+    const int pn = d.ipq[k * d.nquad + iq];
+    const double un = d.us_new[pn], vn = d.vs_new[pn];
+    double tx, ty;
+    mass_flux_weights(L, k, tx, ty);
+    const double P0 = d.npart[(0 * 9 + k) * nq + iq], P1 = d.npart[(1 * 9 + k) * nq + iq];
+    const double P2 = d.npart[(2 * 9 + k) * nq + iq], P3 = d.npart[(3 * 9 + k) * nq + iq];
+    const double P4 = d.npart[(4 * 9 + k) * nq + iq];
+    const double f0 = P3 + (un * P0 - P1), f1 = P4 + (vn * P0 - P2);
+    double ltw = 0, lf0 = 0, lf1 = 0, lfe = 0;
+    for (int kk = 0; kk < 6; kk++) {
+      ltw += lR[0][kk] * b[kk];
+      lf0 += lR[1][kk] * b[kk];
+      lf1 += lR[2][kk] * b[kk];
+      lfe += lR[3][kk] * b[kk];
+    }
+    lf0 += lfe * un;
+    lf1 += lfe * vn;
+    const double lun = lfe * f0 + lf0 * P0 + ltw * tx;
+    const double lvn = lfe * f1 + lf1 * P0 + ltw * ty;
+    a.lP[(0 * 9 + k) * nq + iq] = lf0 * un + lf1 * vn;
+    a.lP[(1 * 9 + k) * nq + iq] = -lf0;
+    a.lP[(2 * 9 + k) * nq + iq] = -lf1;
+    a.lP[(3 * 9 + k) * nq + iq] = lf0;
+    a.lP[(4 * 9 + k) * nq + iq] = lf1;
+    a.pbuf[(2 * 9 + k) * nq + iq] = 0.0;
+    a.pbuf[(3 * 9 + k) * nq + iq] = 0.0;
+    a.pbuf[(4 * 9 + k) * nq + iq] = lun;
+    a.pbuf[(5 * 9 + k) * nq + iq] = lvn;
+    // t = sum over the node's outer corner faces of 2 w_mass,f an_f
+    const double ltx = ltw * un, lty = ltw * vn;
+    for (int i = nc_start(k); i < nc_start(k + 1); i++) {
+      const int isg = nc_entry(i) >> 2, ivsg = nc_entry(i) & 3;
+      for (int f = 0; f < 2; f++)
+        if (wmas(isg, ivsg, f) != 0.0)
+          corner_an_T(isg, ivsg, f, ltx * (2.0 * wmas(isg, ivsg, f)), lty * (2.0 * wmas(isg, ivsg, f)), lX, lY);
+    }
+  }
+  vol_T<R>(L, G, u, lR, g, eps, lu, lX, lY);
+  // ---- Taylor-Green source (in a_src when LAG2D_ASRC_SPLIT)
+  double lxp[9][2];
+  for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
+  if (!LAG2D_ASRC_SPLIT && d.ncase == 1) {
+    double lR3[6];
+    for (int k = 0; k < 6; k++) lR3[k] = lR[3][k];
+    src_T(L, G, lR3, g, lX, lY, lxp);
+  }
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  for (int k = 0; k < 9; k++) {
+    a.pbuf[(0 * 9 + k) * nq + iq] = lxp[k][0] + lX[A[k]][B[k]];
+    a.pbuf[(1 * 9 + k) * nq + iq] = lxp[k][1] + lY[A[k]][B[k]];
+  }
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu[q][k];
+}
+
+// Reverse of the Taylor-Green source of quad iq on its own (after a_rhs):
+// adds the node-coordinate adjoints of the source moments into pbuf
+__host__ __device__ void a_src(const Dev &d, const Adj &a, int iq) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  const size_t nq = d.nquad, nc = d.ncell;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double lR3[6];
+  for (int k = 0; k < 6; k++) lR3[k] = a.lR[(18 + k) * nc + e];
+  double lX[3][3], lY[3][3], lxp[9][2];
+  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
+  for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
+  src_T(L, G, lR3, d.gamlg, lX, lY, lxp);
   const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
   const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
   for (int k = 0; k < 9; k++) {
@@ -1906,7 +1949,7 @@ __host__ __device__ void a_centre(const Dev &d, const Adj &a, int p) {
 }
 
 __global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128, 4) k_corner2_corr(Dev d) {
+__global__ void __launch_bounds__(128, LAG2D_CORR_MINB) k_corner2_corr(Dev d) {
   f_corner_corr(d, blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void __launch_bounds__(kCornerBlock, LAG2D_FACES_MINB) k_corner2_faces(Dev d) {
@@ -1947,21 +1990,12 @@ __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + th
 // compiled for: 3 (168 registers) in the FP32-mixed adjoint (reverse sweep
 // 15.65 -> 15.08 ms per step on the 1024x1024 Taylor-Green mesh), 1 (255)
 // in the FP64 one (3 would cost 12%)
-#ifndef LAG2D_AREV_MINB_F32
-#define LAG2D_AREV_MINB_F32 3
-#endif
 template <typename R>
-constexpr int arev_minb() { return sizeof(R) == 4 ? LAG2D_AREV_MINB_F32 : 1; }
+constexpr int arev_minb() { return sizeof(R) == 4 ? 3 : 1; }
 template <typename R>
-__global__ void __launch_bounds__(kAdjBlock, arev_minb<R>()) k_a_corner(Dev d, Adj a) {
-  extern __shared__ double acor_stage[];
-  a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x, acor_stage + threadIdx.x);
-}
+__global__ void __launch_bounds__(128, arev_minb<R>()) k_a_corner(Dev d, Adj a) { a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 template <typename R>
-__global__ void __launch_bounds__(kAdjBlock, arev_minb<R>()) k_a_rhs(Dev d, Adj a) {
-  extern __shared__ double arhs_stage[];
-  a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x, arhs_stage + threadIdx.x);
-}
+__global__ void __launch_bounds__(128, arev_minb<R>()) k_a_rhs(Dev d, Adj a) { a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void __launch_bounds__(128) k_a_src(Dev d, Adj a) { a_src(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_gather(Dev d, Adj a, int nv) { a_gather(d, a, blockIdx.x * blockDim.x + threadIdx.x, nv); }
 __global__ void k_a_gather_solve(Dev d, Adj a) { a_gather_solve(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
@@ -2000,25 +2034,17 @@ void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double
   fast::k_a_centre<<<bp, 256, 0, st>>>(d, a);
   fast::k_a_nodes<<<bp, 256, 0, st>>>(d, a, alfa, dtp, fold);
   fast::k_a_update<<<bc, 256, 0, st>>>(d, a, alfa, dtp, fold_u);
-  constexpr int arhs_smem = fast::kArhsStage * fast::kAdjBlock * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(fast::k_a_rhs<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, arhs_smem);
-    cudaFuncSetAttribute(fast::k_a_rhs<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, arhs_smem);
-    attr = true;
-  }
-  if (mixed) fast::k_a_rhs<float><<<bq, fast::kAdjBlock, arhs_smem, st>>>(d, a);
-  else fast::k_a_rhs<double><<<bq, fast::kAdjBlock, arhs_smem, st>>>(d, a);
-  if (d.ncase == 1) fast::k_a_src<<<bq, 128, 0, st>>>(d, a);
+  if (mixed) fast::k_a_rhs<float><<<bq, 128, 0, st>>>(d, a);
+  else fast::k_a_rhs<double><<<bq, 128, 0, st>>>(d, a);
+  if (LAG2D_ASRC_SPLIT && d.ncase == 1) fast::k_a_src<<<bq, 128, 0, st>>>(d, a);
   launch_tri_adjoint_rhs(d, a, st);
   fast::k_a_gather_solve<<<bp, 256, 0, st>>>(d, a);
-  constexpr int acor_smem = fast::kAcorStage * fast::kAdjBlock * sizeof(double);
-  if (mixed) fast::k_a_corner<float><<<bq, fast::kAdjBlock, acor_smem, st>>>(d, a);
-  else fast::k_a_corner<double><<<bq, fast::kAdjBlock, acor_smem, st>>>(d, a);
+  if (mixed) fast::k_a_corner<float><<<bq, 128, 0, st>>>(d, a);
+  else fast::k_a_corner<double><<<bq, 128, 0, st>>>(d, a);
   launch_tri_adjoint_corner(d, a, st);
   fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
 }
-int adjoint_stage_launches(const Dev &d) { return (d.ntria > 0 ? 9 : 7) + (d.ncase == 1 && d.nquad > 0); }
+int adjoint_stage_launches(const Dev &d) { return (d.ntria > 0 ? 9 : 7) + (LAG2D_ASRC_SPLIT && d.ncase == 1); }
 
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }

@@ -507,6 +507,7 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa, double
   load_cell(d, iq, L, nullptr);
   const double rc = d.rc[e], sc = d.sc[e], g19 = d.g19[e], g20 = d.g20[e], g21 = d.g21[e];
   const GeoF G{(float)rc, (float)sc, (float)g19, (float)g20, (float)g21};
+  const float g19f = G.g19, g20f = G.g20, g21f = G.g21;
   double tr[6] = {0, 0, 0, 0, 0, 0};          // tau equation, all moments
   double pa0 = 0.0, pb0 = 0.0, el0 = 0.0;     // cell averages of momentum and energy
   float p0[6] = {0, 0, 0, 0, 0, 0}, p1[6] = {0, 0, 0, 0, 0, 0}, el[6] = {0, 0, 0, 0, 0, 0};
@@ -589,45 +590,71 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa, double
     const double rav = MX_U(2, 0) + MX_U(2, 1) * dr + MX_U(2, 3) * (0.5 * dr * dr - g19) - MX_U(2, 4) * g20 -
                        MX_U(2, 5) * g21;
     const double rbv = MX_U(2, 2) + MX_U(2, 5) * dr, rcv = 0.5 * MX_U(2, 4);
+    // FP32 tau and total energy along the row: a + ds (b + c ds)
+    const float b3r = 0.5f * drf * drf - g19f;
+    const float rat = u[0][0] + u[0][1] * drf + u[0][3] * b3r - u[0][4] * g20f - u[0][5] * g21f;
+    const float rbt = u[0][2] + u[0][5] * drf, rct = 0.5f * u[0][4];
+    const float rae = u[3][0] + u[3][1] * drf + u[3][3] * b3r - u[3][4] * g20f - u[3][5] * g21f;
+    const float rbe = u[3][2] + u[3][5] * drf, rce = 0.5f * u[3][4];
+    // G . grad_xi b for b = 2..6 with dbdr = (1, 0, dr, 0, ds), dbds = (0,
+    // 1, 0, ds, dr): G0 = (ys, -yr, ys dr, -yr ds, ys ds - yr dr), G1 =
+    // (-xs, xr, -xs dr, xr ds, -xs ds + xr dr), and the mass flux
+    // G0 u + G1 v = (A, B, dr A, ds B, ds A + dr B).  dr is fixed along the
+    // row, so each equation needs only 4 sums over the row: of A, B (or ys,
+    // yr, xs, xr) weighted by w_j and by w_j ds; those of the tau equation
+    // in FP64, the pressure work in FP32.
+    double SA = 0, SB = 0, TA = 0, TB = 0;
+    float X1 = 0, X2 = 0, X3 = 0, X4 = 0, Y1 = 0, Y2 = 0, Y3 = 0, Y4 = 0, E1 = 0, E2 = 0, E3 = 0, E4 = 0;
 #pragma unroll
     for (int j = 0; j < 5; j++) {
       const double s = l5pd(j);
       const double ds = s - sc;
       const double ls0 = 0.5 * s * (s - 1.0), ls1 = 1.0 - s * s, ls2 = 0.5 * s * (s + 1.0);
       const double dls0 = s - 0.5, dls1 = -2.0 * s, dls2 = s + 0.5;
-      const double wd = l5wd(i) * l5wd(j);
+      const double wj = l5wd(j);
       const double xr = Qx[0] * ls0 + Qx[1] * ls1 + Qx[2] * ls2;
       const double yr = Qy[0] * ls0 + Qy[1] * ls1 + Qy[2] * ls2;
       const double xs = Px[0] * dls0 + Px[1] * dls1 + Px[2] * dls2;
       const double ys = Py[0] * dls0 + Py[1] * dls1 + Py[2] * dls2;
-      const double b3 = 0.5 * dr * dr - g19, b4 = 0.5 * ds * ds - g20, b5 = dr * ds - g21;
       const double uq = rau + ds * (rbu + rcu * ds);
       const double vq = rav + ds * (rbv + rcv * ds);
-      // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
-      double gd0[5], gd1[5];
-      gd0[0] = ys;       gd1[0] = -xs;
-      gd0[1] = -yr;      gd1[1] = xr;
-      gd0[2] = ys * dr;  gd1[2] = -xs * dr;
-      gd0[3] = -yr * ds; gd1[3] = xr * ds;
-      gd0[4] = ys * ds - yr * dr;
-      gd1[4] = -xs * ds + xr * dr;
+      const double A = ys * uq - xs * vq, B = xr * vq - yr * uq;
+      const double wd = wj * ds;
+      SA += wj * A; SB += wj * B; TA += wd * A; TB += wd * B;
       // FP32 pressure work
-      const float dsf = (float)ds, b3f = (float)b3, b4f = (float)b4, b5f = (float)b5;
-      const float tq = u[0][0] + u[0][1] * drf + u[0][2] * dsf + u[0][3] * b3f + u[0][4] * b4f + u[0][5] * b5f;
-      const float eq = u[3][0] + u[3][1] * drf + u[3][2] * dsf + u[3][3] * b3f + u[3][4] * b4f + u[3][5] * b5f;
+      const float dsf = (float)ds;
+      const float tq = rat + dsf * (rbt + rct * dsf);
+      const float eq = rae + dsf * (rbe + rce * dsf);
       const float uqf = (float)uq, vqf = (float)vq;
       const float pres = fmaxf(eps, (g - 1.0f) * (1.0f / tq) * (eq - 0.5f * (uqf * uqf + vqf * vqf)));
-      const float wp = (float)wd * pres;
-#pragma unroll
-      for (int kk = 0; kk < 5; kk++) {
-        const double fv = gd0[kk] * uq + gd1[kk] * vq;
-        tr[kk + 1] -= fv * wd;
-        const float g0 = (float)gd0[kk], g1 = (float)gd1[kk];
-        p0[kk + 1] += g0 * wp;
-        p1[kk + 1] += g1 * wp;
-        el[kk + 1] += (float)fv * wp;
-      }
+      const float pw = (float)wj * pres, pwd = (float)wd * pres;
+      const float ysf = (float)ys, yrf = (float)yr, xsf = (float)xs, xrf = (float)xr, Af = (float)A, Bf = (float)B;
+      X1 += pw * ysf; X2 += pw * yrf; X3 += pwd * yrf; X4 += pwd * ysf;
+      Y1 += pw * xsf; Y2 += pw * xrf; Y3 += pwd * xrf; Y4 += pwd * xsf;
+      E1 += pw * Af; E2 += pw * Bf; E3 += pwd * Bf; E4 += pwd * Af;
     }
+    const double wi = l5wd(i);
+    tr[1] -= wi * SA;
+    tr[2] -= wi * SB;
+    tr[3] -= wi * (dr * SA);
+    tr[4] -= wi * TB;
+    tr[5] -= wi * (TA + dr * SB);
+    const float wif = (float)wi;
+    p0[1] += wif * X1;
+    p0[2] -= wif * X2;
+    p0[3] += wif * (drf * X1);
+    p0[4] -= wif * X3;
+    p0[5] += wif * (X4 - drf * X2);
+    p1[1] -= wif * Y1;
+    p1[2] += wif * Y2;
+    p1[3] -= wif * (drf * Y1);
+    p1[4] += wif * Y3;
+    p1[5] += wif * (drf * Y2 - Y4);
+    el[1] += wif * E1;
+    el[2] += wif * E2;
+    el[3] += wif * (drf * E1);
+    el[4] += wif * E3;
+    el[5] += wif * (E4 + drf * E2);
   }
   if (d.ncase == 1) {
     // Taylor-Green energy source (FP32), computed by k_tgv_src_mx before the corner pass
