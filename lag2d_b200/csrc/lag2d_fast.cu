@@ -17,17 +17,14 @@
 //    the RHS pass.
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
-#ifndef LAG2D_CORR_MINB
-#define LAG2D_CORR_MINB 4
-#endif
 #ifndef LAG2D_FACES_MINB
 #define LAG2D_FACES_MINB 4
 #endif
-#ifndef LAG2D_ASRC_SPLIT
-#define LAG2D_ASRC_SPLIT 0
+#ifndef LAG2D_RHS_PREFETCH
+#define LAG2D_RHS_PREFETCH 0
 #endif
-#ifndef LAG2D_FACES_SYNC
-#define LAG2D_FACES_SYNC 0
+#ifndef LAG2D_FACES_STAGE
+#define LAG2D_FACES_STAGE 1
 #endif
 #include <math.h>
 
@@ -599,18 +596,13 @@ __host__ __device__ void f_corner_corr(const Dev &d, int iq) {
 constexpr int kCornerBlock = 128;
 constexpr int kCornerStage = 28;
 __device__ void f_corner_faces(const Dev &d, int iq_in, double *col) {
-#if LAG2D_FACES_SYNC
   // every thread of the block reaches the barriers below: a thread past the
   // last quad works on the last quad and stores nothing
   if (d.nquad <= 0 || d.sc_dev->done) return;
   const bool live = iq_in < d.nquad;
   const int iq = live ? iq_in : d.nquad - 1;
-#else
-  if (iq_in >= d.nquad || d.sc_dev->done) return;
-  const bool live = true;
-  const int iq = iq_in;
-#endif
   const int e = iq + d.ntria;
+#if LAG2D_FACES_STAGE
   {
     const size_t nc = d.ncell;
     for (int v = 0; v < 24; v++) __pipeline_memcpy_async(col + v * kCornerBlock, d.Us + v * nc + e, sizeof(double));
@@ -620,11 +612,21 @@ __device__ void f_corner_faces(const Dev &d, int iq_in, double *col) {
   }
 #define CF_U(q, k) col[((q) * 6 + (k)) * kCornerBlock]
 #define CF_CORR(s) col[(24 + (s)) * kCornerBlock]
+#else
+  double ureg[4][6], creg[4];
+  load_u(d, d.Us, e, ureg);
+#pragma unroll
+  for (int s = 0; s < 4; s++) creg[s] = d.corr[s * (size_t)d.nquad + iq];
+#define CF_U(q, k) ureg[q][k]
+#define CF_CORR(s) creg[s]
+#endif
   const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+#if LAG2D_FACES_STAGE
   __pipeline_wait_prior(0);
+#endif
   const double rhoct = 1.0 / CF_U(0, 0);
   const double pctr =
       fmax(eps, (g - 1.0) * rhoct * (CF_U(3, 0) - 0.5 * (CF_U(1, 0) * CF_U(1, 0) + CF_U(2, 0) * CF_U(2, 0))));
@@ -673,10 +675,10 @@ __device__ void f_corner_faces(const Dev &d, int iq_in, double *col) {
       d.npart[(3 * 9 + k) * (size_t)d.nquad + iq] = P3;
       d.npart[(4 * 9 + k) * (size_t)d.nquad + iq] = P4;
     }
-#if LAG2D_FACES_SYNC
     // keep the block's warps on the same stretch of this long unrolled code
+    // (fewer instruction-fetch stalls: 1.233 -> 1.188 ms per step for the
+    // corner pass on the 1024x1024 Taylor-Green mesh)
     __syncthreads();
-#endif
   }
 #undef CF_U
 #undef CF_CORR
@@ -807,6 +809,19 @@ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, doubl
         __pipeline_memcpy_async(col + (40 + v) * kRhsBlock, d.Un + v * nc + e, sizeof(double));
     }
     __pipeline_commit();
+#if LAG2D_RHS_PREFETCH
+    // the node partial sums of the 8 boundary nodes (and the source moments)
+    // towards L2 while the coordinates are gathered
+    const size_t nq = d.nquad;
+#pragma unroll
+    for (int v = 0; v < 5; v++)
+#pragma unroll
+      for (int k = 0; k < 8; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.npart + (v * 9 + k) * nq + iq));
+    if (d.ncase == 1) {
+#pragma unroll
+      for (int k = 0; k < 6; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.src + k * nq + iq));
+    }
+#endif
   }
 #define RHS_U(q, k) col[((q) * 6 + (k)) * kRhsBlock]
   Loaded L;
@@ -883,15 +898,13 @@ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, doubl
       }
       rtau[0] = inv;
     }
-    double SA = 0, SB = 0, TA = 0, TB = 0, X1 = 0, X2 = 0, X3 = 0, X4 = 0;
-    double Y1 = 0, Y2 = 0, Y3 = 0, Y4 = 0, E1 = 0, E2 = 0, E3 = 0, E4 = 0;
 #pragma unroll
     for (int j = 0; j < 5; j++) {
       const double s = l5p(j), ds = s - G.sc;
       double ls[3], dls[3];
       lag3(s, ls);
       dlag3(s, dls);
-      const double wj = l5w(j);
+      const double w = wi * l5w(j);
       const double xr = Qx[0] * ls[0] + Qx[1] * ls[1] + Qx[2] * ls[2];
       const double yr = Qy[0] * ls[0] + Qy[1] * ls[1] + Qy[2] * ls[2];
       const double xs = Px[0] * dls[0] + Px[1] * dls[1] + Px[2] * dls[2];
@@ -901,39 +914,27 @@ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, doubl
       for (int q = 1; q < 4; q++) un[q] = ra[q] + ds * (rb[q] + 0.5 * RHS_U(q, 4) * ds);
       const double rhoad = rtau[j];
       const double pres = fmax(eps, (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2])));
-      // G . grad_xi b for b = 2..6 with dbdr = (1, 0, dr, 0, ds), dbds = (0,
-      // 1, 0, ds, dr): G0 = (ys, -yr, ys dr, -yr ds, ys ds - yr dr), G1 =
-      // (-xs, xr, -xs dr, xr ds, -xs ds + xr dr), and the mass flux
-      // G0 u + G1 v = (A, B, dr A, ds B, ds A + dr B).  dr is fixed along the
-      // row, so each equation needs only 4 sums over the row: of A, B (or ys,
-      // yr, xs, xr) weighted by w_j and by w_j ds.
-      const double A = ys * un[1] - xs * un[2], B = xr * un[2] - yr * un[1];
-      const double wd = wj * ds, pw = wj * pres, pwd = wd * pres;
-      SA += wj * A; SB += wj * B; TA += wd * A; TB += wd * B;
-      X1 += pw * ys; X2 += pw * yr; X3 += pwd * yr; X4 += pwd * ys;
-      Y1 += pw * xs; Y2 += pw * xr; Y3 += pwd * xr; Y4 += pwd * xs;
-      E1 += pw * A; E2 += pw * B; E3 += pwd * B; E4 += pwd * A;
+      // G . grad_xi b for b = 2..6: dbdr = (1, 0, dr, 0, ds), dbds = (0, 1, 0, ds, dr)
+      // (the FP32-mixed kernel sums these per row instead; here the row sums'
+      // 16 extra accumulators cost more in spills than the 16 operations a
+      // point they save)
+      double gd0[5], gd1[5];
+      gd0[0] = ys;       gd1[0] = -xs;
+      gd0[1] = -yr;      gd1[1] = xr;
+      gd0[2] = ys * dr;  gd1[2] = -xs * dr;
+      gd0[3] = -yr * ds; gd1[3] = xr * ds;
+      gd0[4] = ys * ds - yr * dr;
+      gd1[4] = -xs * ds + xr * dr;
+      const double wp = w * pres;
+#pragma unroll
+      for (int kk = 0; kk < 5; kk++) {
+        const double fv = gd0[kk] * un[1] + gd1[kk] * un[2];
+        ul[kk + 1] -= fv * w;
+        p0[kk + 1] += gd0[kk] * wp;
+        p1[kk + 1] += gd1[kk] * wp;
+        el[kk + 1] += fv * wp;
+      }
     }
-    ul[1] -= wi * SA;
-    ul[2] -= wi * SB;
-    ul[3] -= wi * (dr * SA);
-    ul[4] -= wi * TB;
-    ul[5] -= wi * (TA + dr * SB);
-    p0[1] += wi * X1;
-    p0[2] -= wi * X2;
-    p0[3] += wi * (dr * X1);
-    p0[4] -= wi * X3;
-    p0[5] += wi * (X4 - dr * X2);
-    p1[1] -= wi * Y1;
-    p1[2] += wi * Y2;
-    p1[3] -= wi * (dr * Y1);
-    p1[4] += wi * Y3;
-    p1[5] += wi * (dr * Y2 - Y4);
-    el[1] += wi * E1;
-    el[2] += wi * E2;
-    el[3] += wi * (dr * E1);
-    el[4] += wi * E3;
-    el[5] += wi * (E4 + dr * E2);
   }
   if (d.ncase == 1) {
     // Taylor-Green energy source, computed by k_tgv_src2 before the corner pass
@@ -1751,10 +1752,10 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     }
   }
   vol_T<R>(L, G, u, lR, g, eps, lu, lX, lY);
-  // ---- Taylor-Green source (in a_src when LAG2D_ASRC_SPLIT)
+  // ---- Taylor-Green source
   double lxp[9][2];
   for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
-  if (!LAG2D_ASRC_SPLIT && d.ncase == 1) {
+  if (d.ncase == 1) {
     double lR3[6];
     for (int k = 0; k < 6; k++) lR3[k] = lR[3][k];
     src_T(L, G, lR3, g, lX, lY, lxp);
@@ -1767,29 +1768,6 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
   }
   for (int q = 0; q < 4; q++)
     for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu[q][k];
-}
-
-// Reverse of the Taylor-Green source of quad iq on its own (after a_rhs):
-// adds the node-coordinate adjoints of the source moments into pbuf
-__host__ __device__ void a_src(const Dev &d, const Adj &a, int iq) {
-  if (iq >= d.nquad) return;
-  const int e = iq + d.ntria;
-  const size_t nq = d.nquad, nc = d.ncell;
-  Loaded L;
-  load_cell(d, d.xs, d.ys, iq, L);
-  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-  double lR3[6];
-  for (int k = 0; k < 6; k++) lR3[k] = a.lR[(18 + k) * nc + e];
-  double lX[3][3], lY[3][3], lxp[9][2];
-  for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) { lX[i][j] = 0.0; lY[i][j] = 0.0; }
-  for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
-  src_T(L, G, lR3, d.gamlg, lX, lY, lxp);
-  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
-  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
-  for (int k = 0; k < 9; k++) {
-    a.pbuf[(0 * 9 + k) * nq + iq] += lxp[k][0] + lX[A[k]][B[k]];
-    a.pbuf[(1 * 9 + k) * nq + iq] += lxp[k][1] + lY[A[k]][B[k]];
-  }
 }
 
 // Gather of the per-(quad, node) contributions into the node adjoints:
@@ -1949,7 +1927,7 @@ __host__ __device__ void a_centre(const Dev &d, const Adj &a, int p) {
 }
 
 __global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128, LAG2D_CORR_MINB) k_corner2_corr(Dev d) {
+__global__ void __launch_bounds__(128, 4) k_corner2_corr(Dev d) {
   f_corner_corr(d, blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void __launch_bounds__(kCornerBlock, LAG2D_FACES_MINB) k_corner2_faces(Dev d) {
@@ -1996,7 +1974,6 @@ template <typename R>
 __global__ void __launch_bounds__(128, arev_minb<R>()) k_a_corner(Dev d, Adj a) { a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 template <typename R>
 __global__ void __launch_bounds__(128, arev_minb<R>()) k_a_rhs(Dev d, Adj a) { a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128) k_a_src(Dev d, Adj a) { a_src(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_gather(Dev d, Adj a, int nv) { a_gather(d, a, blockIdx.x * blockDim.x + threadIdx.x, nv); }
 __global__ void k_a_gather_solve(Dev d, Adj a) { a_gather_solve(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_update(Dev d, Adj a, double alfa, const double *dtp, int fold) {
@@ -2036,7 +2013,6 @@ void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double
   fast::k_a_update<<<bc, 256, 0, st>>>(d, a, alfa, dtp, fold_u);
   if (mixed) fast::k_a_rhs<float><<<bq, 128, 0, st>>>(d, a);
   else fast::k_a_rhs<double><<<bq, 128, 0, st>>>(d, a);
-  if (LAG2D_ASRC_SPLIT && d.ncase == 1) fast::k_a_src<<<bq, 128, 0, st>>>(d, a);
   launch_tri_adjoint_rhs(d, a, st);
   fast::k_a_gather_solve<<<bp, 256, 0, st>>>(d, a);
   if (mixed) fast::k_a_corner<float><<<bq, 128, 0, st>>>(d, a);
@@ -2044,7 +2020,7 @@ void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double
   launch_tri_adjoint_corner(d, a, st);
   fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
 }
-int adjoint_stage_launches(const Dev &d) { return (d.ntria > 0 ? 9 : 7) + (LAG2D_ASRC_SPLIT && d.ncase == 1); }
+int adjoint_stage_launches(const Dev &d) { return d.ntria > 0 ? 9 : 7; }
 
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }

@@ -10,10 +10,10 @@ WENO replaces cells:
   * M^T is the transpose of M: <M v, w> = <v, M^T w> to 1e-12 relative, for
     seeded random v, w;
   * lag2d_adjoint runs on windows in which WENO replaces cells (it used to
-    return LAG2D_EUNSUP there), with finite gradients that do not depend on
-    the checkpoint interval, and the frozen-limiter directional derivatives
-    agree with central differences of the full step in directions that leave
-    the troubled cells' stencils alone.
+    return LAG2D_EUNSUP there), with finite gradients that agree across
+    checkpoint intervals to 1e-12 of their scale, and the frozen-limiter
+    directional derivatives agree with central differences of the full step
+    in directions that leave the troubled cells' stencils alone.
 """
 import dataclasses
 
@@ -101,7 +101,11 @@ def test_adjoint_window_with_weno():
         assert np.isfinite(gU).all() and np.isfinite(gX).all() and np.isfinite(gS).all()
         out.append((J, gU, gX, gS))
     assert out[0][0] == out[1][0]
-    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+    # each schedule is bitwise repeatable; the two schedules recompute the same
+    # stages but agree to rounding only (measured 1.3e-15 of the gradient scale)
+    for i in (1, 2, 3):
+        scale = np.abs(out[0][i]).max()
+        assert np.abs(out[0][i] - out[1][i]).max() <= 1e-12 * scale, i
     # directions away from the limited region: the frozen limiter is exact there
     J0, gU = out[0][0], out[0][1]
     # the Persson marks of the window's first stage, from the oracle
