@@ -306,10 +306,11 @@ static void enqueue_step_reference_order(lag2d_handle *h, int itime) {
 // Corner and RHS passes of the optimised step: FP64, or the FP32-mixed form
 // (config precision = 1) with the same node pass, update and geometry.
 // Triangles run their FP64 kernels in both forms.
-// launches of corner_pass: the triangles' kernel, then one (FP32-mixed) or
-// two (FP64: sub-cell corrections, corner faces) quad kernels
+// launches of corner_pass: the triangles' kernel, then two quad kernels
+// (sub-cell corrections, corner faces)
 static int corner_launches(const lag2d_handle *h, const Dev &d) {
-  return (d.ntria > 0) + (h->cfg.precision == 1 ? 1 : 2);
+  (void)h;
+  return (d.ntria > 0) + 2;
 }
 
 // Taylor-Green energy source of the stage (quads; ncase 1 only), read by the
@@ -1118,6 +1119,7 @@ struct AdjWork {
     alloc(&a.lx, np); alloc(&a.ly, np); alloc(&a.lxn, np); alloc(&a.lyn, np); alloc(&a.lus, np); alloc(&a.lvs, np);
     alloc(&a.luw, np); alloc(&a.lvw, np); alloc(&a.tx, np); alloc(&a.ty, np);
     alloc(&a.lS, 5 * np); alloc(&a.lP, 45 * (size_t)d.nquad); alloc(&a.pbuf, 54 * (size_t)d.nquad);
+    alloc(&a.lcorr, 4 * (size_t)d.nquad);
     alloc(&a.tbuf, 36 * (size_t)d.ntria); alloc(&a.ltcf, 120 * (size_t)d.ntria);
     const size_t ns = (size_t)K * nstag;
     alloc(&rec.U, ns * nu); alloc(&rec.x, ns * np); alloc(&rec.y, ns * np);

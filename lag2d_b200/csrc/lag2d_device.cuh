@@ -95,6 +95,7 @@ struct Adj {
   double *lR;              // [24][ncell] adjoint of the stage RHS
   double *lS;              // [5][npoin] adjoint of the node sums (m, m u, m v, sigma.n A)
   double *lP;              // [5][9][nquad] RHS pass's adjoint of each quad's node partial sums
+  double *lcorr;           // [4][nquad] adjoint of the sub-cell density corrections (corner faces -> corrections)
   double *pbuf;            // [6][9][nquad] per (quad, node) adjoint contributions
   double *tx, *ty;         // scratch of the centre-node transpose
   double *tbuf;            // [6][6][ntria] per (triangle, node) adjoint contributions

@@ -17,14 +17,11 @@
 //    the RHS pass.
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
-#ifndef LAG2D_FACES_MINB
-#define LAG2D_FACES_MINB 4
+#ifndef LAG2D_ACC_MINB
+#define LAG2D_ACC_MINB 3
 #endif
-#ifndef LAG2D_RHS_PREFETCH
-#define LAG2D_RHS_PREFETCH 0
-#endif
-#ifndef LAG2D_FACES_STAGE
-#define LAG2D_FACES_STAGE 1
+#ifndef LAG2D_ACF_MINB
+#define LAG2D_ACF_MINB 2
 #endif
 #include <math.h>
 
@@ -592,7 +589,9 @@ __host__ __device__ void f_corner_corr(const Dev &d, int iq) {
 // 24 DOFs and 4 sub-cell corrections are copied asynchronously (cp.async)
 // into this thread's column of shared memory (stride kCornerBlock) at entry,
 // so their loads overlap the coordinate gathers and they take no registers
-// between the vertex states.
+// between the vertex states (corner pass 1.404 -> 1.189 ms per step on the
+// 1024x1024 Taylor-Green mesh against the same kernel with them in
+// registers).
 constexpr int kCornerBlock = 128;
 constexpr int kCornerStage = 28;
 __device__ void f_corner_faces(const Dev &d, int iq_in, double *col) {
@@ -602,7 +601,6 @@ __device__ void f_corner_faces(const Dev &d, int iq_in, double *col) {
   const bool live = iq_in < d.nquad;
   const int iq = live ? iq_in : d.nquad - 1;
   const int e = iq + d.ntria;
-#if LAG2D_FACES_STAGE
   {
     const size_t nc = d.ncell;
     for (int v = 0; v < 24; v++) __pipeline_memcpy_async(col + v * kCornerBlock, d.Us + v * nc + e, sizeof(double));
@@ -612,21 +610,11 @@ __device__ void f_corner_faces(const Dev &d, int iq_in, double *col) {
   }
 #define CF_U(q, k) col[((q) * 6 + (k)) * kCornerBlock]
 #define CF_CORR(s) col[(24 + (s)) * kCornerBlock]
-#else
-  double ureg[4][6], creg[4];
-  load_u(d, d.Us, e, ureg);
-#pragma unroll
-  for (int s = 0; s < 4; s++) creg[s] = d.corr[s * (size_t)d.nquad + iq];
-#define CF_U(q, k) ureg[q][k]
-#define CF_CORR(s) creg[s]
-#endif
   const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
-#if LAG2D_FACES_STAGE
   __pipeline_wait_prior(0);
-#endif
   const double rhoct = 1.0 / CF_U(0, 0);
   const double pctr =
       fmax(eps, (g - 1.0) * rhoct * (CF_U(3, 0) - 0.5 * (CF_U(1, 0) * CF_U(1, 0) + CF_U(2, 0) * CF_U(2, 0))));
@@ -809,9 +797,10 @@ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, doubl
         __pipeline_memcpy_async(col + (40 + v) * kRhsBlock, d.Un + v * nc + e, sizeof(double));
     }
     __pipeline_commit();
-#if LAG2D_RHS_PREFETCH
     // the node partial sums of the 8 boundary nodes (and the source moments)
-    // towards L2 while the coordinates are gathered
+    // towards L2 while the coordinates are gathered: their loads in the face
+    // loop then wait on L2, not HBM (RHS pass 1.635 -> 1.507 ms per step on
+    // the 1024x1024 Taylor-Green mesh)
     const size_t nq = d.nquad;
 #pragma unroll
     for (int v = 0; v < 5; v++)
@@ -821,7 +810,6 @@ __device__ void f_rhs3(const Dev &d, int iq, int fuse_update, double alfa, doubl
 #pragma unroll
       for (int k = 0; k < 6; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.src + k * nq + iq));
     }
-#endif
   }
 #define RHS_U(q, k) col[((q) * 6 + (k)) * kRhsBlock]
   Loaded L;
@@ -1269,40 +1257,31 @@ __host__ __device__ __forceinline__ void vertex_T(const double *b, int mdegr, co
       if (k < mdegr) lu[q][k] += lst[q] * b[k];
 }
 
-// Reverse of the corner pass of quad iq: reads the node-sum adjoints lS at
-// its nodes plus the RHS pass's adjoints of its partials (lP); adds the cell
-// DOF adjoint into lU and writes the node contributions (x, y, u*_prev,
-// v*_prev) into pbuf.
-template <typename R>
-__host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
+// Reverse of the corner pass of quad iq, in two kernels like the forward
+// pass.  First the corner faces: reads the node-sum adjoints lS at its nodes
+// plus the RHS pass's adjoints of its partials (lP); adds the cell DOF
+// adjoint into lU, writes the node contributions (x, y, u*_prev, v*_prev)
+// into pbuf and the adjoints of the 4 sub-cell density corrections into
+// lcorr.  Without the det J polynomial, sub-cell areas and masses the
+// corrections' transpose needs, it holds far fewer values across its 32
+// unrolled faces.
+__host__ __device__ void a_corner_faces(const Dev &d, const Adj &a, int iq) {
   if (iq >= d.nquad) return;
   const int e = iq + d.ntria;
   const size_t nq = d.nquad;
   const double eps = 1.0e-6, g = d.gamlg, slpdu = (g + 1.0) / 2.0;
   Loaded L;
   load_cell(d, d.xs, d.ys, iq, L);
-  double xp[9][2], c[36], D[16];
-  node_xy_rel(L, xp);
-  cross36_rel(xp, c);
-  detpoly(c, D);
   const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
   double u[4][6];
   load_u(d, d.Us, e, u);
   const double rhoct = 1.0 / u[0][0];
   const double pctr = fmax(eps, (g - 1.0) * rhoct * (u[3][0] - 0.5 * (u[1][0] * u[1][0] + u[2][0] * u[2][0])));
   const double sdctr = sqrt(fmax(eps, g * pctr / rhoct));
-  // the stage's sub-cell density corrections come from the forward pass;
-  // corr = cdrho (msub / vsub - masel / volel) gives the sub-cell masses
-  // masel back from the closed-form volumes volel
-  double vsub4[4], corr[4], masel4[4], volel4[4];
-  subareas(c, vsub4);
+  // the stage's sub-cell density corrections come from the forward pass
+  double corr[4];
 #pragma unroll
-  for (int isg = 0; isg < 4; isg++) {
-    corr[isg] = d.corr[isg * nq + iq];
-    volel4[isg] = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
-    const double rho_sub = d.cdrho != 0.0 ? d.msub[isg * nq + iq] / vsub4[isg] - corr[isg] / d.cdrho : 0.0;
-    masel4[isg] = volel4[isg] * rho_sub;
-  }
+  for (int isg = 0; isg < 4; isg++) corr[isg] = d.corr[isg * nq + iq];
   double lu[4][6];
   for (int q = 0; q < 4; q++) for (int k = 0; k < 6; k++) lu[q][k] = 0.0;
   double lX[3][3], lY[3][3];
@@ -1365,6 +1344,52 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
     lst2 -= lduy;
     vertex_T(b, d.mdegr, st, lrhovt, lke, lst1, lst2, lu);
   }
+  centre_T(u, g, lrho, lsd, lu);
+#pragma unroll
+  for (int isg = 0; isg < 4; isg++) a.lcorr[isg * nq + iq] = lcr[isg];
+  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  for (int k = 0; k < 9; k++) {
+    a.pbuf[(0 * 9 + k) * nq + iq] = lX[A[k]][B[k]];
+    a.pbuf[(1 * 9 + k) * nq + iq] = lY[A[k]][B[k]];
+    a.pbuf[(4 * 9 + k) * nq + iq] = 0.0;
+    a.pbuf[(5 * 9 + k) * nq + iq] = 0.0;
+  }
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * (size_t)d.ncell + e] += lu[q][k];
+}
+
+// Second part: the transpose of the sub-cell density corrections
+// corr = cdrho (msub / vsub - masel / volel) from their adjoints in lcorr;
+// adds into the tau DOF adjoints and the node-coordinate contributions.
+// The corrections come from the forward pass; the sub-cell masses masel
+// are recovered from them and the closed-form volumes volel.
+template <typename R>
+__host__ __device__ void a_corner_corr(const Dev &d, const Adj &a, int iq) {
+  if (iq >= d.nquad) return;
+  const int e = iq + d.ntria;
+  const size_t nq = d.nquad;
+  Loaded L;
+  load_cell(d, d.xs, d.ys, iq, L);
+  double xp[9][2], c[36], D[16];
+  node_xy_rel(L, xp);
+  cross36_rel(xp, c);
+  detpoly(c, D);
+  const CellGeo G{d.rc[e], d.sc[e], d.g19[e], d.g20[e], d.g21[e]};
+  double u0[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) u0[k] = d.Us[k * (size_t)d.ncell + e];
+  double vsub4[4], masel4[4], volel4[4], lcr[4];
+  subareas(c, vsub4);
+#pragma unroll
+  for (int isg = 0; isg < 4; isg++) {
+    const double corr = d.corr[isg * nq + iq];
+    volel4[isg] = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
+    const double rho_sub = d.cdrho != 0.0 ? d.msub[isg * nq + iq] / vsub4[isg] - corr / d.cdrho : 0.0;
+    masel4[isg] = volel4[isg] * rho_sub;
+    lcr[isg] = a.lcorr[isg * nq + iq];
+  }
+  double lu0[6] = {0, 0, 0, 0, 0, 0};
   // sub-cell density corrections: corr = cdrho (msub / vsub - masel / volel)
   double lD[16], lv4[4] = {0, 0, 0, 0};
   for (int t = 0; t < 16; t++) lD[t] = 0.0;
@@ -1398,8 +1423,8 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
       double ee[4];
 #pragma unroll
       for (int n = 0; n < 4; n++) ee[n] = D[n] + r * (D[4 + n] + r * (D[8 + n] + r * D[12 + n]));
-      const double t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5 * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
-      const double t1 = u[0][2] + u[0][5] * dr, t2 = 0.5 * u[0][4];
+      const double t0 = u0[0] + u0[1] * dr + u0[3] * (0.5 * dr * dr - G.g19) - u0[4] * G.g20 - u0[5] * G.g21;
+      const double t1 = u0[2] + u0[5] * dr, t2 = 0.5 * u0[4];
       // point arithmetic in R (FP32 in the mixed adjoint), rows added in FP64
       const R t0r = R(t0), t1r = R(t1), t2r = R(t2), lm = R(lmasel), wi = R(0.25 * g5w(i));
       const R e0 = R(ee[0]), e1 = R(ee[1]), e2 = R(ee[2]), e3 = R(ee[3]);
@@ -1422,12 +1447,12 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
         Ls[3] += ldet * s * s * s;
       }
       const double a0 = m0, a1 = m1, a2 = m2;
-      lu[0][0] += a0;
-      lu[0][1] += dr * a0;
-      lu[0][2] += a1;
-      lu[0][3] += (0.5 * dr * dr - G.g19) * a0;
-      lu[0][4] += 0.5 * a2 - G.g20 * a0;
-      lu[0][5] += dr * a1 - G.g21 * a0;
+      lu0[0] += a0;
+      lu0[1] += dr * a0;
+      lu0[2] += a1;
+      lu0[3] += (0.5 * dr * dr - G.g19) * a0;
+      lu0[4] += 0.5 * a2 - G.g20 * a0;
+      lu0[5] += dr * a1 - G.g21 * a0;
       double rp = 1.0;
 #pragma unroll
       for (int mm = 0; mm < 4; mm++) {
@@ -1437,7 +1462,6 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
       }
     }
   }
-  centre_T(u, g, lrho, lsd, lu);
   double lc36[36];
   for (int p = 0; p < 36; p++) lc36[p] = 0.0;
   detpoly_T(lD, lc36);
@@ -1445,16 +1469,12 @@ __host__ __device__ void a_corner(const Dev &d, const Adj &a, int iq) {
   double lxp[9][2];
   for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
   cross36_T(xp, lc36, lxp);
-  const int A[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
-  const int B[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
   for (int k = 0; k < 9; k++) {
-    a.pbuf[(0 * 9 + k) * nq + iq] = lxp[k][0] + lX[A[k]][B[k]];
-    a.pbuf[(1 * 9 + k) * nq + iq] = lxp[k][1] + lY[A[k]][B[k]];
-    a.pbuf[(4 * 9 + k) * nq + iq] = 0.0;
-    a.pbuf[(5 * 9 + k) * nq + iq] = 0.0;
+    a.pbuf[(0 * 9 + k) * nq + iq] += lxp[k][0];
+    a.pbuf[(1 * 9 + k) * nq + iq] += lxp[k][1];
   }
-  for (int q = 0; q < 4; q++)
-    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * (size_t)d.ncell + e] += lu[q][k];
+#pragma unroll
+  for (int k = 0; k < 6; k++) a.lU[k * (size_t)d.ncell + e] += lu0[k];
 }
 
 // Reverse of the volume integral of the RHS pass (5x5 Gauss-Lobatto,
@@ -1752,6 +1772,9 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     }
   }
   vol_T<R>(L, G, u, lR, g, eps, lu, lX, lY);
+  // the DOF adjoints are complete: out before the source's transpose
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu[q][k];
   // ---- Taylor-Green source
   double lxp[9][2];
   for (int k = 0; k < 9; k++) { lxp[k][0] = 0.0; lxp[k][1] = 0.0; }
@@ -1766,8 +1789,6 @@ __host__ __device__ void a_rhs(const Dev &d, const Adj &a, int iq) {
     a.pbuf[(0 * 9 + k) * nq + iq] = lxp[k][0] + lX[A[k]][B[k]];
     a.pbuf[(1 * 9 + k) * nq + iq] = lxp[k][1] + lY[A[k]][B[k]];
   }
-  for (int q = 0; q < 4; q++)
-    for (int k = 0; k < 6; k++) a.lU[(q * 6 + k) * nc + e] += lu[q][k];
 }
 
 // Gather of the per-(quad, node) contributions into the node adjoints:
@@ -1930,7 +1951,7 @@ __global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx
 __global__ void __launch_bounds__(128, 4) k_corner2_corr(Dev d) {
   f_corner_corr(d, blockIdx.x * blockDim.x + threadIdx.x);
 }
-__global__ void __launch_bounds__(kCornerBlock, LAG2D_FACES_MINB) k_corner2_faces(Dev d) {
+__global__ void __launch_bounds__(kCornerBlock, 4) k_corner2_faces(Dev d) {
   extern __shared__ double faces_stage[];
   f_corner_faces(d, blockIdx.x * blockDim.x + threadIdx.x, faces_stage + threadIdx.x);
 }
@@ -1970,8 +1991,13 @@ __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + th
 // in the FP64 one (3 would cost 12%)
 template <typename R>
 constexpr int arev_minb() { return sizeof(R) == 4 ? 3 : 1; }
+__global__ void __launch_bounds__(128, LAG2D_ACF_MINB) k_a_corner_faces(Dev d, Adj a) {
+  a_corner_faces(d, a, blockIdx.x * blockDim.x + threadIdx.x);
+}
 template <typename R>
-__global__ void __launch_bounds__(128, arev_minb<R>()) k_a_corner(Dev d, Adj a) { a_corner<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(128, LAG2D_ACC_MINB) k_a_corner_corr(Dev d, Adj a) {
+  a_corner_corr<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x);
+}
 template <typename R>
 __global__ void __launch_bounds__(128, arev_minb<R>()) k_a_rhs(Dev d, Adj a) { a_rhs<R>(d, a, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_a_gather(Dev d, Adj a, int nv) { a_gather(d, a, blockIdx.x * blockDim.x + threadIdx.x, nv); }
@@ -2015,12 +2041,13 @@ void launch_adjoint_stage(const Dev &d, const void *adj, cudaStream_t st, double
   else fast::k_a_rhs<double><<<bq, 128, 0, st>>>(d, a);
   launch_tri_adjoint_rhs(d, a, st);
   fast::k_a_gather_solve<<<bp, 256, 0, st>>>(d, a);
-  if (mixed) fast::k_a_corner<float><<<bq, 128, 0, st>>>(d, a);
-  else fast::k_a_corner<double><<<bq, 128, 0, st>>>(d, a);
+  fast::k_a_corner_faces<<<bq, 128, 0, st>>>(d, a);
+  if (mixed) fast::k_a_corner_corr<float><<<bq, 128, 0, st>>>(d, a);
+  else fast::k_a_corner_corr<double><<<bq, 128, 0, st>>>(d, a);
   launch_tri_adjoint_corner(d, a, st);
   fast::k_a_gather<<<bp, 256, 0, st>>>(d, a, 4);
 }
-int adjoint_stage_launches(const Dev &d) { return d.ntria > 0 ? 9 : 7; }
+int adjoint_stage_launches(const Dev &d) { return d.ntria > 0 ? 10 : 8; }
 
 
 void launch_fast_persson(const Dev &d, cudaStream_t st) { fast::k_persson2<<<fast::nb(d.nquad, 128), 128, 0, st>>>(d); }

@@ -31,6 +31,10 @@
 #include "lag2d_device.cuh"
 #include "lag2d_fast_tables.h"
 
+#ifndef LAG2D_MXF_MINB
+#define LAG2D_MXF_MINB 3
+#endif
+
 namespace lag2d {
 
 namespace mixed {
@@ -358,10 +362,12 @@ __device__ void m_tgv_src(const Dev &d, int iq) {
 // ---------------------------------------------------------------------------
 // Corner pass (getriem_quadsubg2 with getrhosubg_averg/_daverg)
 // ---------------------------------------------------------------------------
-__device__ void m_corner(const Dev &d, int iq) {
+// The corner pass runs as two kernels, as in the FP64 form: the sub-cell
+// density corrections (m_corner_corr, written to d.corr in FP64), then the
+// corner faces (m_corner_faces) with the corrections read back.
+__device__ void m_corner_corr(const Dev &d, int iq) {
   if (iq >= d.nquad || d.sc_dev->done) return;
   const int e = iq + d.ntria;
-  const float eps = 1.0e-6f, g = (float)d.gamlg, slpdu = (g + 1.0f) / 2.0f, cimpd = (float)d.cimpd;
   CellXY L;
   double c[36], D[16];
   load_cell(d, iq, L, c);
@@ -369,6 +375,72 @@ __device__ void m_corner(const Dev &d, int iq) {
   float Df[16];
 #pragma unroll
   for (int t = 0; t < 16; t++) Df[t] = (float)D[t];
+  const GeoF G{(float)d.rc[e], (float)d.sc[e], (float)d.g19[e], (float)d.g20[e], (float)d.g21[e]};
+  float u0[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) u0[k] = (float)d.Us[k * (size_t)d.ncell + e];
+  // sub-cell densities: initial mass / exact sub-cell area (FP64) against the
+  // DG-implied harmonic tau mean (FP32 5x5 Gauss per sub-cell).  Sub-cells 0
+  // and 3 (r in [-1, 0]) share their Gauss rows, and so do 1 and 2: each
+  // row's det J and tau coefficients serve both.
+  double vsub4[4];
+  subareas(c, vsub4);
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const float ofr = h == 0 ? -1.0f : 1.0f;
+    const int ilo = h == 0 ? 0 : 1, ihi = h == 0 ? 3 : 2;  // s in [-1, 0], [0, 1]
+    float mlo = 0.0f, mhi = 0.0f;
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) {
+      const float r = (g5p(i) + ofr) * 0.5f;
+      // along the row r, det J is a cubic and tau a quadratic in s
+      float e[4];
+#pragma unroll
+      for (int n = 0; n < 4; n++) e[n] = Df[n] + r * (Df[4 + n] + r * (Df[8 + n] + r * Df[12 + n]));
+      const float dr = r - G.rc;
+      const float t0 = u0[0] + u0[1] * dr + u0[3] * (0.5f * dr * dr - G.g19) - u0[4] * G.g20 - u0[5] * G.g21;
+      const float t1 = u0[2] + u0[5] * dr, t2 = 0.5f * u0[4];
+      const float wi = 0.25f * g5w(i);
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const float w = wi * g5w(j);
+        {
+          const float s = (g5p(j) - 1.0f) * 0.5f;
+          const float ds = s - G.sc;
+          const float tau = t0 + ds * (t1 + t2 * ds);
+          const float det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
+          mlo += w * __fdividef(det, tau);
+        }
+        {
+          const float s = (g5p(j) + 1.0f) * 0.5f;
+          const float ds = s - G.sc;
+          const float tau = t0 + ds * (t1 + t2 * ds);
+          const float det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
+          mhi += w * __fdividef(det, tau);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int isg = t == 0 ? ilo : ihi;
+      const float masel = t == 0 ? mlo : mhi;
+      const double unksgq = d.msub[isg * (size_t)d.nquad + iq] / vsub4[isg];
+      const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
+      d.corr[isg * (size_t)d.nquad + iq] = d.cdrho * (unksgq - (double)masel / volel);
+    }
+  }
+}
+
+__device__ void m_corner_faces(const Dev &d, int iq_in) {
+  // every thread of the block reaches the barriers below: a thread past the
+  // last quad works on the last quad and stores nothing
+  if (d.nquad <= 0 || d.sc_dev->done) return;
+  const bool live = iq_in < d.nquad;
+  const int iq = live ? iq_in : d.nquad - 1;
+  const int e = iq + d.ntria;
+  const float eps = 1.0e-6f, g = (float)d.gamlg, slpdu = (g + 1.0f) / 2.0f, cimpd = (float)d.cimpd;
+  CellXY L;
+  load_cell(d, iq, L, nullptr);
   const GeoF G{(float)d.rc[e], (float)d.sc[e], (float)d.g19[e], (float)d.g20[e], (float)d.g21[e]};
   float u[4][6];
 #pragma unroll
@@ -386,42 +458,9 @@ __device__ void m_corner(const Dev &d, int iq) {
   const double rcd = d.rc[e], scd = d.sc[e], g19d = d.g19[e], g20d = d.g20[e], g21d = d.g21[e];
   float rhoct, sdctr;
   centre_state(u, g, rhoct, sdctr);
-  // sub-cell densities: initial mass / exact sub-cell area (FP64) against the
-  // DG-implied harmonic tau mean (FP32 5x5 Gauss per sub-cell)
-  double vsub4[4];
-  subareas(c, vsub4);
   float corr[4];
 #pragma unroll
-  for (int isg = 0; isg < 4; isg++) {
-    const double unksgq = d.msub[isg * (size_t)d.nquad + iq] / vsub4[isg];
-    const float ofr = (isg == 0 || isg == 3) ? -1.0f : 1.0f;
-    const float ofs = (isg == 0 || isg == 1) ? -1.0f : 1.0f;
-    float masel = 0.0f;
-#pragma unroll 1
-    for (int i = 0; i < 5; i++) {
-      const float r = (g5p(i) + ofr) * 0.5f;
-      // along the row r, det J is a cubic and tau a quadratic in s
-      float e[4];
-#pragma unroll
-      for (int n = 0; n < 4; n++) e[n] = Df[n] + r * (Df[4 + n] + r * (Df[8 + n] + r * Df[12 + n]));
-      const float dr = r - G.rc;
-      const float t0 = u[0][0] + u[0][1] * dr + u[0][3] * (0.5f * dr * dr - G.g19) - u[0][4] * G.g20 - u[0][5] * G.g21;
-      const float t1 = u[0][2] + u[0][5] * dr, t2 = 0.5f * u[0][4];
-      const float wi = 0.25f * g5w(i);
-#pragma unroll
-      for (int j = 0; j < 5; j++) {
-        const float s = (g5p(j) + ofs) * 0.5f;
-        const float ds = s - G.sc;
-        const float tau = t0 + ds * (t1 + t2 * ds);
-        const float det = e[0] + s * (e[1] + s * (e[2] + s * e[3]));
-        masel += (wi * g5w(j)) * __fdividef(det, tau);
-      }
-    }
-    const double volel = det_integral(D, (isg == 0 || isg == 3) ? -1.0 : 0.0, (isg == 0 || isg == 1) ? -1.0 : 0.0);
-    const double cr = d.cdrho * (unksgq - (double)masel / volel);
-    d.corr[isg * (size_t)d.nquad + iq] = cr;
-    corr[isg] = (float)cr;
-  }
+  for (int isg = 0; isg < 4; isg++) corr[isg] = (float)d.corr[isg * (size_t)d.nquad + iq];
 #pragma unroll
   for (int k = 0; k < 9; k++) {
     float b[6], st[4];
@@ -464,11 +503,15 @@ __device__ void m_corner(const Dev &d, int iq) {
         P4 += (double)sy;
       }
     }
-    d.npart[(0 * 9 + k) * (size_t)d.nquad + iq] = P0;
-    d.npart[(1 * 9 + k) * (size_t)d.nquad + iq] = P1;
-    d.npart[(2 * 9 + k) * (size_t)d.nquad + iq] = P2;
-    d.npart[(3 * 9 + k) * (size_t)d.nquad + iq] = P3;
-    d.npart[(4 * 9 + k) * (size_t)d.nquad + iq] = P4;
+    if (live) {
+      d.npart[(0 * 9 + k) * (size_t)d.nquad + iq] = P0;
+      d.npart[(1 * 9 + k) * (size_t)d.nquad + iq] = P1;
+      d.npart[(2 * 9 + k) * (size_t)d.nquad + iq] = P2;
+      d.npart[(3 * 9 + k) * (size_t)d.nquad + iq] = P3;
+      d.npart[(4 * 9 + k) * (size_t)d.nquad + iq] = P4;
+    }
+    // keep the block's warps on the same stretch of the unrolled code
+    __syncthreads();
   }
 }
 
@@ -501,6 +544,17 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa, double
         __pipeline_memcpy_async(col + (40 + v) * kMxBlock, d.Un + v * nc + e, sizeof(double));
     }
     __pipeline_commit();
+    // the node partial sums of the 8 boundary nodes (and the source moments)
+    // towards L2 while the coordinates are gathered
+    const size_t nq = d.nquad;
+#pragma unroll
+    for (int v = 0; v < 5; v++)
+#pragma unroll
+      for (int k = 0; k < 8; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.npart + (v * 9 + k) * nq + iq));
+    if (d.ncase == 1) {
+#pragma unroll
+      for (int k = 0; k < 6; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(d.src + k * nq + iq));
+    }
   }
 #define MX_U(q, k) col[((q) * 6 + (k)) * kMxBlock]
   CellXY L;
@@ -705,7 +759,12 @@ __device__ void m_rhs(const Dev &d, int iq, int fuse_update, double alfa, double
 #undef MX_UN
 }
 
-__global__ void __launch_bounds__(128, 3) k_corner_mx(Dev d) { m_corner(d, blockIdx.x * blockDim.x + threadIdx.x); }
+__global__ void __launch_bounds__(128, 4) k_corner_mx_corr(Dev d) {
+  m_corner_corr(d, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void __launch_bounds__(128, LAG2D_MXF_MINB) k_corner_mx_faces(Dev d) {
+  m_corner_faces(d, blockIdx.x * blockDim.x + threadIdx.x);
+}
 __global__ void __launch_bounds__(128) k_tgv_src_mx(Dev d) { m_tgv_src(d, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void __launch_bounds__(kMxBlock, 3) k_rhs_mx(Dev d, int fuse, double alfa) {
   extern __shared__ double mx_stage[];
@@ -717,7 +776,8 @@ static inline int nb(int n, int b) { return (n + b - 1) / b; }
 }  // namespace mixed
 
 void launch_mixed_corner(const Dev &d, cudaStream_t st) {
-  mixed::k_corner_mx<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d);
+  mixed::k_corner_mx_corr<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d);
+  mixed::k_corner_mx_faces<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d);
 }
 void launch_mixed_src(const Dev &d, cudaStream_t st) {
   mixed::k_tgv_src_mx<<<mixed::nb(d.nquad, 128), 128, 0, st>>>(d);
