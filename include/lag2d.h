@@ -148,6 +148,19 @@ int lag2d_cellvol(lag2d_handle *h, double *geoel);
  * LAG2D_EUNSUP.  The sum over cells is a fixed-order reduction. */
 int lag2d_error_norms(lag2d_handle *h, double *errl2);
 
+/* End-of-run cell values of the reference's post-processing, from the
+ * handle's state (cell averages U^n and the current nodes): cellout(9, ncell)
+ * = (radius of the cell centre, rho, p, e_int, x_c, y_c, |u|, u, v) per
+ * cell, the values geterror_lag_curvhybrid (Postprocess.f90:3700-3717,
+ * :3944-3983) and geterror_lag_hybrid (:3515-3560) write to their radial
+ * profile files and getoutput_cellvtk (:1258-1398) writes as cell data; the
+ * centre is the map at (0, 0) for quads and at (rc, sc) for triangles.
+ * badcell(ncell), if not NULL, receives the troubled-cell marker of a
+ * Persson pass on the state (getSIHO_Persson, Limiterlag.f90:12042-12239;
+ * 100 or 0, as the driver computes it before the VTK file,
+ * dgflo2d.f90:525-528), 0 on triangles and on the P1 path. */
+int lag2d_cell_output(lag2d_handle *h, double *cellout, double *badcell);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that time or
  * order work against the library's launches. */
 void *lag2d_stream(const lag2d_handle *h);

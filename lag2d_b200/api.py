@@ -66,7 +66,7 @@ EXPORTS = ("lag2d_create", "lag2d_init_fields", "lag2d_set_state", "lag2d_step",
            "lag2d_get_state", "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_stream",
            "lag2d_kernel_launches", "lag2d_timing", "lag2d_kernel_ms", "lag2d_destroy", "lag2d_last_error",
            "lag2d_delt_noalloc", "lag2d_adjoint_step", "lag2d_adjoint", "lag2d_set_rho0",
-           "lag2d_error_norms", "lag2d_weno_linear")
+           "lag2d_error_norms", "lag2d_weno_linear", "lag2d_cell_output")
 
 
 def library_path(exact: bool = False) -> str:
@@ -90,7 +90,8 @@ def load(exact: bool = False):
     lib.lag2d_create.argtypes = [ctypes.POINTER(_Mesh), ctypes.POINTER(_Cfg), ctypes.POINTER(ctypes.c_void_p)]
     for name in ("lag2d_init_fields", "lag2d_set_state", "lag2d_step", "lag2d_run", "lag2d_get_state",
                  "lag2d_rhs", "lag2d_weno", "lag2d_cellvol", "lag2d_timing", "lag2d_adjoint_step",
-                 "lag2d_adjoint", "lag2d_set_rho0", "lag2d_error_norms", "lag2d_weno_linear"):
+                 "lag2d_adjoint", "lag2d_set_rho0", "lag2d_error_norms", "lag2d_weno_linear",
+                 "lag2d_cell_output"):
         getattr(lib, name).restype = ctypes.c_int
     lib.lag2d_destroy.argtypes = [ctypes.c_void_p]
     _libs[key] = lib
@@ -231,6 +232,16 @@ class Lag2DSolver:
         e = np.zeros(3)
         self._check(self.lib.lag2d_error_norms(self.h, _p(e, _dp)))
         return e
+
+    def cell_output(self, badcell: bool = True):
+        """End-of-run cell values from the device: (ncell, 9) array of
+        (radius of the centre, rho, p, e_int, x_c, y_c, |u|, u, v) and, with
+        ``badcell``, the Persson troubled-cell marker (100 or 0) per cell."""
+        n = self.mesh.ncell
+        out = np.zeros((n, 9))
+        bad = np.zeros(n) if badcell else None
+        self._check(self.lib.lag2d_cell_output(self.h, _p(out, _dp), _p(bad, _dp)))
+        return out, bad
 
     def cellvol(self):
         geoel = np.zeros((self.mesh.nsize, 24))

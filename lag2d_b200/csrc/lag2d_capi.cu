@@ -67,6 +67,8 @@ void launch_weno_swap(const Dev &d, cudaStream_t st);
 int adjoint_stage_launches(const Dev &d);
 int error_blocks(const Dev &d);
 void launch_error(const Dev &d, cudaStream_t st, const double *X, const double *Y, double *part);
+void launch_cell_output(const Dev &d, cudaStream_t st, const double *U, const double *X, const double *Y,
+                        double *out);
 }  // namespace lag2d
 
 using namespace lag2d;
@@ -113,6 +115,7 @@ struct lag2d_handle {
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   p1::Solver *p1 = nullptr;    // the linear P1 path (npoly = 1) when set; Dev d is then unused
   double *errpart = nullptr;   // per-block partial sums of lag2d_error_norms
+  double *cellout = nullptr;   // [9][ncell] values of lag2d_cell_output
   // inverse of the WENO stencil table: for quad j, the entries c*9 + s of the
   // quads c whose stencil position s is j, c ascending (the WENO transpose's
   // fixed summation order)
@@ -1035,6 +1038,39 @@ int lag2d_error_norms(lag2d_handle *h, double *errl2) {
   for (int b = 0; b < nb; b++)
     for (int k = 0; k < 3; k++) e[k] += part[3 * (size_t)b + k];
   for (int k = 0; k < 3; k++) errl2[k] = std::sqrt(e[k]);
+  return LAG2D_OK;
+}
+
+int lag2d_cell_output(lag2d_handle *h, double *cellout, double *badcell) {
+  if (!h || !cellout) return fail(LAG2D_EINVAL, "null argument");
+  if (h->p1) {
+    if (badcell) std::fill(badcell, badcell + h->d.ncell, 0.0);
+    P1_CALL(p1::cell_output(h->p1, cellout, err_));
+  }
+  Dev &d = h->d;
+  if (!h->cellout) {
+    int r = dalloc(h, &h->cellout, 9 * (size_t)d.ncell);
+    if (r) return r;
+  }
+  run(h, "post", [&] { launch_cell_output(d, h->st, d.Un, d.xn, d.yn, h->cellout); });
+  std::vector<double> v(9 * (size_t)d.ncell);
+  CK(cudaMemcpyAsync(v.data(), h->cellout, v.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  if (badcell) {
+    // getSIHO_Persson on the state, as the reference's driver runs it before
+    // writing the cell file: 100 on troubled quads, 0 elsewhere
+    run(h, "persson", [&] {
+      launch_reset_count(d, h->st);
+      if (h->cfg.order_exact) launch_persson(d, h->st); else launch_fast_persson(d, h->st);
+    }, 2);
+    std::vector<int> f(d.ncell);
+    CK(cudaMemcpyAsync(f.data(), d.flag, d.ncell * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int e = 0; e < d.ncell; e++) badcell[e] = (e >= d.ntria && f[e] != 0) ? 100.0 : 0.0;
+  }
+  CK(cudaStreamSynchronize(h->st));
+  CK(cudaGetLastError());
+  for (size_t e = 0; e < (size_t)d.ncell; e++)
+    for (int k = 0; k < 9; k++) cellout[9 * e + k] = v[k * (size_t)d.ncell + e];
   return LAG2D_OK;
 }
 

@@ -3393,6 +3393,53 @@ __global__ void k_error_partial(Dev d, const double *X, const double *Y, double 
     for (int k = 0; k < 3; k++) part[3 * blockIdx.x + k] = sm[k][0];
 }
 int error_blocks(const Dev &d) { return nblk(d.nquad, 256); }
+
+// Per-cell output values of the end-of-run post-processing: the quantities
+// geterror_lag_curvhybrid writes for each cell to its radial profile file
+// (Postprocess.f90:3700-3717 triangles, :3944-3983 quads) and
+// getoutput_cellvtk writes as cell data (:1324-1391), from the cell averages:
+// out[k*ncell + e] for k = 0..8 = (radius of the centre, rho, p, e_int, x_c,
+// y_c, |u|, u, v), with rho = 1/tau (ndens = 1), p = (gamma - 1) rho (e -
+// (u^2 + v^2)/2), e_int = p / rho / (gamma - 1).  The centre is the map at
+// (r, s) = (0, 0) for quads (the 9th node) and at the reference mass centre
+// (rc, sc) for triangles (6-node shape functions), from the state U and the
+// coordinates X, Y.
+__global__ void k_cell_output(Dev d, const double *U, const double *X, const double *Y, double *out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.ncell) return;
+  const double g = d.gamlg;
+  double xc = 0.0, yc = 0.0;
+  if (e < d.ntria) {
+    double shp[6];
+    shp6v(d.rc[e], d.sc[e], shp);
+    for (int k = 0; k < 6; k++) {
+      const int p = d.ipt[k * d.ntria + e];
+      xc = xc + shp[k] * X[p];
+      yc = yc + shp[k] * Y[p];
+    }
+  } else {
+    const int p = d.ipq[8 * d.nquad + (e - d.ntria)];
+    xc = X[p];
+    yc = Y[p];
+  }
+  const double rhoc = 1.0 / Uget(d, U, 0, 0, e);
+  const double uctr = Uget(d, U, 0, 1, e), vctr = Uget(d, U, 0, 2, e), ectr = Uget(d, U, 0, 3, e);
+  const double pctr = (g - 1.0) * rhoc * (ectr - 0.5 * (uctr * uctr + vctr * vctr));
+  const size_t n = d.ncell;
+  out[0 * n + e] = sqrt(xc * xc + yc * yc);
+  out[1 * n + e] = rhoc;
+  out[2 * n + e] = pctr;
+  out[3 * n + e] = pctr / rhoc / (g - 1.0);
+  out[4 * n + e] = xc;
+  out[5 * n + e] = yc;
+  out[6 * n + e] = sqrt(uctr * uctr + vctr * vctr);
+  out[7 * n + e] = uctr;
+  out[8 * n + e] = vctr;
+}
+void launch_cell_output(const Dev &d, cudaStream_t st, const double *U, const double *X, const double *Y,
+                        double *out) {
+  k_cell_output<<<nblk(d.ncell, 256), 256, 0, st>>>(d, U, X, Y, out);
+}
 void launch_error(const Dev &d, cudaStream_t st, const double *X, const double *Y, double *part) {
   k_error_partial<<<nblk(d.nquad, 256), 256, 0, st>>>(d, X, Y, part);
 }

@@ -992,12 +992,43 @@ __global__ void k1_unkno_out(Dev1 d, const double *src, double *aos) {
 // ---------------------------------------------------------------------------
 struct Family { double ms = 0.0; long long n = 0; };
 
+// Per-cell output values of the end-of-run post-processing of the linear
+// path (geterror_lag_hybrid, Postprocess.f90:3515-3560, written to its radial
+// profile file): out[k*ncell + e] for k = 0..8 = (radius of the centre, rho,
+// p, e_int, x_c, y_c, |u|, u, v) from the cell averages of U^n, the centre
+// being the bilinear map at (r, s) = (0, 0).
+__global__ void k1_cell_output(Dev1 d, double *out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.nquad) return;
+  double x4[4][2];
+  load4(d, d.xn, d.yn, e, x4);
+  double xc = 0.0, yc = 0.0;
+  for (int k = 0; k < 4; k++) {
+    xc = xc + 0.25 * x4[k][0];
+    yc = yc + 0.25 * x4[k][1];
+  }
+  const double g = d.gamlg;
+  const double rhoc = 1.0 / U(d, d.Un, 0, 0, e);
+  const double uctr = U(d, d.Un, 0, 1, e), vctr = U(d, d.Un, 0, 2, e), ectr = U(d, d.Un, 0, 3, e);
+  const double pctr = (g - 1.0) * rhoc * (ectr - 0.5 * (uctr * uctr + vctr * vctr));
+  const size_t n = d.ncell;
+  out[0 * n + e] = sqrt(xc * xc + yc * yc);
+  out[1 * n + e] = rhoc;
+  out[2 * n + e] = pctr;
+  out[3 * n + e] = pctr / rhoc / (g - 1.0);
+  out[4 * n + e] = xc;
+  out[5 * n + e] = yc;
+  out[6 * n + e] = sqrt(uctr * uctr + vctr * vctr);
+  out[7 * n + e] = uctr;
+  out[8 * n + e] = vctr;
+}
+
 struct Solver {
   Dev1 d{};
   lag2d_config cfg{};
   cudaStream_t st = nullptr;
   std::vector<void *> allocs;
-  double *stage_u = nullptr, *stage_x = nullptr;
+  double *stage_u = nullptr, *stage_x = nullptr, *cellout = nullptr;
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0, launches = 0;
   bool timing = false;
@@ -1426,6 +1457,19 @@ int cellvol(Solver *s, double *geoel, std::string &err) {
     std::fill(geoel, geoel + 24 * (size_t)s->d.ncell, 0.0);
     return download_geoel(s, geoel, err);
   }
+  return LAG2D_OK;
+}
+
+int cell_output(Solver *s, double *out, std::string &err) {
+  const Dev1 &d = s->d;
+  if (!s->cellout && !dalloc(s, &s->cellout, 9 * (size_t)d.ncell)) { err = "cudaMalloc failed"; return LAG2D_ECUDA; }
+  launch(s, "post", [&] { k1_cell_output<<<nb(d.ncell, 256), 256, 0, s->st>>>(d, s->cellout); });
+  std::vector<double> h(9 * (size_t)d.ncell);
+  CK1(cudaMemcpyAsync(h.data(), s->cellout, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  CK1(cudaStreamSynchronize(s->st));
+  CK1(cudaGetLastError());
+  for (size_t e = 0; e < (size_t)d.ncell; e++)
+    for (int k = 0; k < 9; k++) out[9 * e + k] = h[k * (size_t)d.ncell + e];
   return LAG2D_OK;
 }
 

@@ -21,6 +21,7 @@ int run(Solver *s, int itime0, int nsteps, double *dtfix, double *tacru, int *do
 int get_state(Solver *s, double *unkno, double *coord, double *ustar, double *geoel, std::string &err);
 int rhs(Solver *s, double *rhsel, std::string &err);
 int cellvol(Solver *s, double *geoel, std::string &err);
+int cell_output(Solver *s, double *out, std::string &err);
 long long launches(const Solver *s);
 void set_timing(Solver *s, bool on);
 double kernel_ms(const Solver *s, const char *family, long long *n);

@@ -223,6 +223,49 @@ def build_esuv(iptri: np.ndarray, ipqua: np.ndarray, npoin: int):
     return esuv1, esuv2
 
 
+def boundary_hosts(iptri: np.ndarray, ipqua: np.ndarray, bface: np.ndarray) -> np.ndarray:
+    """Host cell of each boundary face (1-based, triangles first), the
+    result of preprocess1's step 2 (Preprocess.f90:679-717).
+
+    The reference tests every cell's corner vertices against both end points
+    of every boundary face, O(nbfac x ncell), and keeps the last cell that
+    holds both (triangles, then quads).  Here every pair of corner vertices
+    of every cell is keyed once and the boundary faces are looked up in the
+    sorted keys: O((ncell + nbfac) log ncell), same answer (0 where no cell
+    holds both end points)."""
+    ntria, nquad = iptri.shape[0], ipqua.shape[0]
+    pairs, cells = [], []
+    for conn, nv, first in ((iptri, 3, 1), (ipqua, 4, ntria + 1)):
+        if conn.shape[0] == 0:
+            continue
+        corner = conn[:, :nv].astype(np.int64)
+        ids = np.arange(first, first + conn.shape[0], dtype=np.int64)
+        for a in range(nv):
+            for b in range(a + 1, nv):
+                lo = np.minimum(corner[:, a], corner[:, b])
+                hi = np.maximum(corner[:, a], corner[:, b])
+                pairs.append(lo * (1 << 32) + hi)
+                cells.append(ids)
+    hosts = np.zeros(bface.shape[0], dtype=np.int32)
+    if not pairs or bface.shape[0] == 0:
+        return hosts
+    keys = np.concatenate(pairs)
+    owner = np.concatenate(cells)
+    order = np.lexsort((owner, keys))       # by key, then cell id: the last of a run is the highest id
+    ks, os_ = keys[order], owner[order]
+    last = np.ones(ks.size, dtype=bool)
+    last[:-1] = ks[1:] != ks[:-1]
+    ks, os_ = ks[last], os_[last]
+    b0 = bface[:, 0].astype(np.int64)
+    b1 = bface[:, 1].astype(np.int64)
+    q = np.minimum(b0, b1) * (1 << 32) + np.maximum(b0, b1)
+    pos = np.searchsorted(ks, q)
+    pos = np.minimum(pos, ks.size - 1)
+    hit = ks[pos] == q
+    hosts[hit] = os_[pos[hit]].astype(np.int32)
+    return hosts
+
+
 def build_esqua(ipqua: np.ndarray, iptri: np.ndarray, bface: np.ndarray) -> np.ndarray:
     """Cell across each quad face (face k joins corner k and corner k+1).
 

@@ -79,6 +79,7 @@ def test_entry_points_reject_null_handles_without_device():
     assert lib.lag2d_step(None, 1, ctypes.byref(d), ctypes.byref(d)) == 1
     assert lib.lag2d_set_rho0(None, p) == 1
     assert lib.lag2d_error_norms(None, p) == 1
+    assert lib.lag2d_cell_output(None, p, p) == 1
     assert lib.lag2d_adjoint(None, 1, 2, 1, ctypes.byref(d), ctypes.byref(d), ctypes.byref(d),
                              None, None, None, None) == 1
     assert lib.lag2d_adjoint_step(None, 1, ctypes.byref(d), ctypes.byref(d), None, None, None,
