@@ -57,7 +57,8 @@ class _Cfg(ctypes.Structure):
                 ("order_exact", ctypes.c_int),
                 ("nsedov", ctypes.c_int), ("sedov_cell", ctypes.c_int * 4),
                 ("gamlg", ctypes.c_double), ("cfl", ctypes.c_double), ("cdrho", ctypes.c_double),
-                ("cimpd", ctypes.c_double), ("tend", ctypes.c_double), ("sedov_energy", ctypes.c_double)]
+                ("cimpd", ctypes.c_double), ("tend", ctypes.c_double), ("sedov_energy", ctypes.c_double),
+                ("nrz", ctypes.c_int)]
 
 
 _libs = {}
@@ -125,7 +126,7 @@ class Lag2DSolver:
                        cfg.ndens, cfg.ngausd, cfg.ngausd_geo, int(precision), 1 if order_exact else 0,
                        len(cfg.sedov_cells),
                        sc, cfg.gamlg, cfg.cfl,
-                       cfg.cdrho, cfg.cimpd, cfg.tend, cfg.sedov_energy)
+                       cfg.cdrho, cfg.cimpd, cfg.tend, cfg.sedov_energy, int(cfg.nrz))
         h = ctypes.c_void_p()
         self._check(self.lib.lag2d_create(ctypes.byref(self._m), ctypes.byref(self._c), ctypes.byref(h)))
         self.h = h

@@ -39,6 +39,7 @@ class StepConfig:
     dtfix: float = 1.0e-4   # initial / fixed time step
     sedov_cells: Tuple[int, ...] = ()      # 1-based cells receiving the Sedov energy
     sedov_energy: float = 0.244816
+    nrz: int = 0            # 0: Cartesian; 1: RZ with y the radius (true volume, linear P1 cells)
 
     @property
     def nmatr(self) -> int:
@@ -106,6 +107,31 @@ def _sod(nx: int, ny: int, y1: float, jitter: float = 0.0) -> Tuple[Mesh, StepCo
     return m, c
 
 
+def _noh_rz(n: int, cfl: float = 0.3, jitter: float = 0.0) -> Tuple[Mesh, StepConfig]:
+    """Noh implosion in RZ (nrz = 1: y is the radius, x the axial
+    coordinate; true-volume weights), i.e. the spherical implosion, on the
+    linear P1 path: n x n straight quads on [0,1]^2, rho = 1, u = -(x, y)/r,
+    p = 1e-6 (getunkin ncase 3), gamma 5/3, SSP-RK2.  x = 0 is a slip wall
+    (222), y = 0 the axis (221), the outer sides are pressure boundaries
+    (code 21, p = 1e-6, getbc_lagmaire2).  Node 1 is the origin, which the
+    RZ node solve holds (Getrhslagmc.f90:17475).  The exact solution has the
+    shock at r = t/3 with density ((gamma+1)/(gamma-1))^3 = 64 behind it.
+    ``jitter`` moves the interior vertices (seeded), for parity checks off
+    the axis-aligned geometry."""
+    m = linear_quad_mesh(n, n, 0.0, 1.0, 0.0, 1.0, jitter=jitter)
+    bf = m.bface.copy()
+    for i in range(bf.shape[0]):
+        if i < n:                       # y = 0: the axis
+            bf[i, 2], bf[i, 3] = 22, 221
+        elif i < 3 * n:                 # x = 1 and y = 1: free, p = 1e-6
+            bf[i, 2], bf[i, 3] = 21, 0
+        else:                           # x = 0: slip wall
+            bf[i, 2], bf[i, 3] = 22, 222
+    m = Mesh(coord=m.coord, ipqua=m.ipqua, iptri=m.iptri, bface=bf, nvqua=4)
+    c = StepConfig(npoly=1, ndegr=3, mdegr=3, ncase=3, gamlg=5.0 / 3.0, nstag=2, cfl=cfl, tend=0.6, nrz=1)
+    return m, c
+
+
 def initial_density_factors(mesh: Mesh, sigma: float = 0.01, seed: int = 5678) -> np.ndarray:
     """Per-cell initial-density factors 1 + sigma N(0, 1) (seeded), in cell
     order (triangles first), for lag2d_set_rho0 / Lag2DSolver.set_rho0: the
@@ -153,6 +179,12 @@ WORKLOADS = {
     "sod40": lambda: _sod(40, 4, 0.1),
     "sod_jitter40": lambda: _sod(40, 8, 0.2, jitter=0.15),
     "sod1024": lambda: _sod(1024, 512, 0.5),
+    "noh_rz8": lambda: _noh_rz(8),
+    "noh_rz_jitter16": lambda: _noh_rz(16, jitter=0.15),
+    "noh_rz32": lambda: _noh_rz(32),
+    "noh_rz50": lambda: _noh_rz(50),
+    "noh_rz100": lambda: _noh_rz(100),
+    "noh_rz1024": lambda: _noh_rz(1024),
 }
 
 

@@ -97,6 +97,13 @@ struct Dev1 {
   double *rhs;                        // [12][ncell]
   double *dtpart;
   Scalars *sc_dev;
+  // RZ (nrz = 1, y the radius): alfrz = 1, and per node its boundary faces
+  // in face order (bf_ptr/bf_list) with the faces' end nodes and codes
+  int nrz, nbfac;
+  double alfrz;
+  const int *bf_ptr, *bf_list;        // node -> boundary faces, ascending
+  const int *bfn;                     // [2][nbfac] end nodes (0-based)
+  const int *bfcode;                  // [nbfac] code * 1000 + sub-code
 };
 
 struct Rules {
@@ -217,7 +224,7 @@ __device__ void getunkin1(const Dev1 &d, double *unkin, double xg, double yg, in
 __global__ void k1_init_geo(Dev1 d) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad) return;
-  const double alfrz = 0.0;
+  const double alfrz = d.alfrz;
   double x4[4][2], xp[9][2], shp[9], dr[9], ds[9];
   load4(d, d.x0, d.y0, iq, x4);
   image9(x4, xp);
@@ -250,7 +257,7 @@ __global__ void k1_init_fields(Dev1 d) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad) return;
   const int e = iq;
-  const double alfrz = 0.0;
+  const double alfrz = d.alfrz;
   double x4[4][2], xp[9][2], shp[9], dr[9], ds[9];
   load4(d, d.x0, d.y0, iq, x4);
   image9(x4, xp);
@@ -318,7 +325,7 @@ __global__ void k1_init_fields(Dev1 d) {
 __global__ void k1_geom(Dev1 d, const double *X, const double *Y) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
-  const double alfrz = 0.0;
+  const double alfrz = d.alfrz;
   double x4[4][2], xp[9][2], shp[9], dr[9], ds[9];
   load4(d, X, Y, iq, x4);
   image9(x4, xp);
@@ -398,7 +405,76 @@ __global__ void k1_bounds(Dev1 d) {
 // ---------------------------------------------------------------------------
 // Limiter and corner coefficients of one quad
 // ---------------------------------------------------------------------------
-template <int MD, bool FAST>
+// RZ corner coefficients (getriem_quadrz, Getrhslagmc.f90:17963-18336):
+// 4 corner faces per vertex (its two edges, each twice: faces 1, 3 the edge
+// to the previous vertex, 2, 4 to the next) with the radius weights of the
+// edge halves, the acoustic impedance rho c only and the 1e-9 floors; stored
+// per face in cf[(k*16 + f + 4*iv)*nquad + iq] (k: m, m u, m v, sigma.n A).
+template <int MD>
+__device__ void rz_corners(const Dev1 &d, int iq, const double (*x4)[2], const int *ip, const double (*u)[ND],
+                           const double (*bq)[ND], const double (*uvq)[4], double af4, double fi11, double fi12,
+                           double fi22) {
+  const double g = d.gamlg, eps9 = 1.0e-09, alfrz = d.alfrz;
+  double fn[4][3], rco[4];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int b = (f + 1) & 3;
+    const double anx = x4[b][1] - x4[f][1];
+    const double any = -(x4[b][0] - x4[f][0]);
+    fn[f][0] = anx / sqrt(anx * anx + any * any);
+    fn[f][1] = any / sqrt(anx * anx + any * any);
+    fn[f][2] = sqrt(anx * anx + any * any);
+    rco[f] = 1.0 - alfrz + alfrz * fabs(x4[f][1]);
+  }
+  const double rhomc = u[0][0], uctr = u[1][0], vctr = u[2][0], ectr = u[3][0];
+  const double rhoct = 1.0 / rhomc;
+  const double pctr = fmax(eps9, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  const double sdctr = sqrt(fmax(eps9, g * pctr / rhoct));
+  const double murie = rhoct * sdctr;
+  const double dudr = fi11 * u[1][1] + fi12 * u[2][1];
+  const double duds = fi11 * u[1][2] + fi12 * u[2][2];
+  const double dvdr = fi12 * u[1][1] + fi22 * u[2][1];
+  const double dvds = fi12 * u[1][2] + fi22 * u[2][2];
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++) {
+    const int vp = (iv + 3) & 3, vx = (iv + 1) & 3;
+    const double rhovt = 1.0 / uvq[iv][0];
+    const double ev = uvq[iv][3];
+    double pvtx = fmax(eps9, (g - 1.0) * rhovt * (ev - 0.5 * (uvq[iv][1] * uvq[iv][1] + uvq[iv][2] * uvq[iv][2])));
+    const double uvl = u[1][0] + dudr * bq[iv][1] + duds * bq[iv][2];
+    const double vvl = u[2][0] + dvdr * bq[iv][1] + dvds * bq[iv][2];
+    pvtx = pctr + af4 * (pvtx - pctr);
+    const double sig = -pvtx;
+    const double acnx = d.us[ip[iv]] - uvl, acny = d.vs[ip[iv]] - vvl;
+    const double nrm = sqrt(acnx * acnx + acny * acny);
+    double aj0, aj1;
+    if (nrm < TINY_S) { aj0 = TINY_S; aj1 = TINY_S; }
+    else { aj0 = acnx / nrm; aj1 = acny / nrm; }
+    const double aj2 = nrm / sdctr;
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      const int edge = (f & 1) ? iv : vp;
+      const double rw = (f < 2) ? 3.0 * rco[iv] : 1.0 * rco[iv];
+      const double ro = (f & 1) ? rco[vx] : rco[vp];
+      const double n1 = fn[edge][0], n2 = fn[edge][1];
+      const double area = 0.5 * ((rw + ro) / 3.0 * 0.5 * fn[edge][2]);
+      const double vnau = (aj2 < 1.0e12) ? 1.0 : n1 * aj0 + n2 * aj1;
+      const double m = murie * area * fabs(vnau);
+      const double mu1 = m * uvl + 0.0 * vvl;
+      const double mu2 = 0.0 * uvl + m * vvl;
+      const double s1 = sig * area * n1 + (0.0 + 0.0) * area * n2;
+      const double s2 = (0.0 + 0.0) * area * n1 + sig * area * n2;
+      const int slot = f + 4 * iv;
+      d.cf[(0 * 16 + slot) * (size_t)d.nquad + iq] = m;
+      d.cf[(1 * 16 + slot) * (size_t)d.nquad + iq] = mu1;
+      d.cf[(2 * 16 + slot) * (size_t)d.nquad + iq] = mu2;
+      d.cf[(3 * 16 + slot) * (size_t)d.nquad + iq] = s1;
+      d.cf[(4 * 16 + slot) * (size_t)d.nquad + iq] = s2;
+    }
+  }
+}
+
+template <int MD, bool FAST, bool RZ>
 __device__ void cell_pass(const Dev1 &d, int iq) {
   const int e = iq;
   const double g = d.gamlg, epsd = 1.0e-6, slpdu = (g + 1.0) / 2.0;
@@ -536,6 +612,10 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
   d.lim[5 * nc + e] = fi12;
   d.lim[6 * nc + e] = fi22;
 
+  if (RZ) {
+    rz_corners<MD>(d, iq, x4, ip, u, bq, uvq, af[3], fi11, fi12, fi22);
+    return;
+  }
   // (4) corner Riemann coefficients (getriem_quad_matrixsym, Limiterlag.f90:
   // 708-1033): face f of quad iq joins vertices f and f+1, its normal is
   // (dy, -dx)/|.| (getfnds_lag_mc_hybrid, Getrhslagmc.f90:2210-2262)
@@ -608,11 +688,11 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
 }
 // compiled for 4 resident blocks of 128 per SM (128 registers): on the
 // 1024 x 512 Sod mesh 136 us per launch against 161 us at 138 registers
-template <int MD, bool FAST>
+template <int MD, bool FAST, bool RZ>
 __global__ void __launch_bounds__(128, 4) k1_cell(Dev1 d) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
-  cell_pass<MD, FAST>(d, iq);
+  cell_pass<MD, FAST, RZ>(d, iq);
 }
 
 // ---------------------------------------------------------------------------
@@ -620,10 +700,106 @@ __global__ void __launch_bounds__(128, 4) k1_cell(Dev1 d) {
 // corner sums in the order the reference scatters them (cells ascending,
 // corner faces 1, 2), the 2x2 solve and the wall conditions
 // ---------------------------------------------------------------------------
-template <bool FAST>
+// RZ nodal solve (getndvelo_lagmc_rz, Getrhslagmc.f90:17284-17597, with
+// getbc_lagmaire2, Getrhslag.f90:11269-11491): the node sums of the 4 corner
+// faces per corner in the reference's scatter order; at the node's boundary
+// faces (in face order) the radius-weighted area vectors of the velocity
+// walls (code 22) and the pressure forces of code 21 (ncase 3: p = 1e-6);
+// fpres removes the wall-normal velocity from the solve; node 1 is held, 222
+// holds u and code 25 both (the 221 zeroing is commented out in RZ).
+__device__ void rz_node(const Dev1 &d, int p) {
+  double n11 = 0.0, n21 = 0.0, n12 = 0.0, n22 = 0.0, a1 = 0.0, a2 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int i = d.ncor_ptr[p]; i < d.ncor_ptr[p + 1]; i++) {
+    const int c = d.ncor[i], iq = c >> 2, iv = c & 3;
+    for (int f = 0; f < 4; f++) {
+      const int slot = f + 4 * iv;
+      const double m = d.cf[(0 * 16 + slot) * (size_t)d.nquad + iq];
+      n11 = n11 + m;
+      n21 = n21 + 0.0;
+      n12 = n12 + 0.0;
+      n22 = n22 + m;
+      a1 = a1 + d.cf[(1 * 16 + slot) * (size_t)d.nquad + iq];
+      a2 = a2 + d.cf[(2 * 16 + slot) * (size_t)d.nquad + iq];
+      s1 = s1 + d.cf[(3 * 16 + slot) * (size_t)d.nquad + iq];
+      s2 = s2 + d.cf[(4 * 16 + slot) * (size_t)d.nquad + iq];
+    }
+  }
+  const double alfrz = d.alfrz;
+  double bvx = 0.0, bvy = 0.0, bpx = 0.0, bpy = 0.0;
+  bool wall22 = false;
+  for (int i = d.bf_ptr[p]; i < d.bf_ptr[p + 1]; i++) {
+    const int ifa = d.bf_list[i];
+    const int q0 = d.bfn[ifa], q1 = d.bfn[d.nbfac + ifa], code = d.bfcode[ifa];
+    const double anx = d.ys[q1] - d.ys[q0];
+    const double any = -(d.xs[q1] - d.xs[q0]);
+    const double gf3 = sqrt(anx * anx + any * any);
+    const double r0 = 1.0 - alfrz + alfrz * d.ys[q0], r1 = 1.0 - alfrz + alfrz * d.ys[q1];
+    // this node's weight (2 r_self + r_other) / 3, divided last as the reference does
+    const double wsum = (q0 == p) ? (2.0 * r0 + r1) : (2.0 * r1 + r0);
+    if (code / 1000 == 22) {
+      wall22 = true;
+      double bsnx = 0.0, bsny = 0.0;
+      const int sub = code % 1000;
+      if (sub == 221) {
+        bsnx = 0.0 * gf3 * 0.5;
+        bsny = -1.0 * gf3 * 0.5;
+        if (d.ncase == 1 || d.ncase == 2 || d.ncase == 12) {
+          if (d.ys[q0] < 1.0e-6 && d.ys[q1] < 1.0e-6) { bsnx = 0.0 * gf3 * 0.5; bsny = -1.0 * gf3 * 0.5; }
+          else if (fabs(d.ys[q0] - 1.0) < 1.0e-6 && fabs(d.ys[q1] - 1.0) < 1.0e-6) { bsnx = 0.0 * gf3 * 0.5; bsny = 1.0 * gf3 * 0.5; }
+        }
+      } else if (sub == 222) {
+        bsnx = -1.0 * gf3 * 0.5;
+        bsny = 0.0 * gf3 * 0.5;
+        if (d.ncase == 1) {
+          if (d.xs[q0] < 1.0e-6 && d.xs[q1] < 1.0e-6) { bsnx = -1.0 * gf3 * 0.5; bsny = 0.0 * gf3 * 0.5; }
+          else if (fabs(d.xs[q0] - 1.0) < 1.0e-6 && fabs(d.xs[q1] - 1.0) < 1.0e-6) { bsnx = 1.0 * gf3 * 0.5; bsny = 0.0 * gf3 * 0.5; }
+        }
+      }
+      bvx = bvx + bsnx * wsum / 3.0;
+      bvy = bvy + bsny * wsum / 3.0;
+    } else if (code / 1000 == 21 && d.ncase == 3) {
+      const double pres0 = 1.0e-6;
+      const double bsnx = anx / gf3 * gf3 * 0.5, bsny = any / gf3 * gf3 * 0.5;
+      bpx = bpx + pres0 * bsnx * wsum / 3.0;
+      bpy = bpy + pres0 * bsny * wsum / 3.0;
+    }
+  }
+  double fpx = 0.0, fpy = 0.0;
+  if (wall22) {
+    const double detma = n11 * n22 - n21 * n12;
+    const double i11 = n22 / detma, i12 = -n12 / detma, i21 = -n21 / detma, i22 = n11 / detma;
+    const double coefl = (i11 * bvx + i12 * bvy) * bvx + (i21 * bvx + i22 * bvy) * bvy;
+    const double rhsx = a1 - s1 - bpx, rhsy = a2 - s2 - bpy;
+    const double coefr = (i11 * rhsx + i12 * rhsy) * bvx + (i21 * rhsx + i22 * rhsy) * bvy;
+    fpx = coefr / fmax(1.0e-16, coefl) * bvx;
+    fpy = coefr / fmax(1.0e-16, coefl) * bvy;
+  }
+  fpx = fpx + bpx;
+  fpy = fpy + bpy;
+  const unsigned char bc = d.bc[p];
+  double us = d.us[p], vs = d.vs[p];
+  if (!(bc & BC_KEEP)) {
+    const double detma = n11 * n22 - n21 * n12;
+    const double i11 = n22 / detma, i12 = -n12 / detma, i21 = -n21 / detma, i22 = n11 / detma;
+    const double r1 = a1 - s1 - fpx, r2 = a2 - s2 - fpy;
+    us = i11 * r1 + i12 * r2;
+    vs = i21 * r1 + i22 * r2;
+  }
+  if (p == 0) { us = 0.0; vs = 0.0; }
+  if (bc & BC_UV0) vs = 0.0;
+  if (bc & (BC_U0 | BC_UV0)) us = 0.0;
+  d.us[p] = us;
+  d.vs[p] = vs;
+}
+
+template <bool FAST, bool RZ>
 __global__ void k1_node(Dev1 d) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= d.npoin || stopped(d)) return;
+  if (RZ) {
+    rz_node(d, p);
+    return;
+  }
   double n11 = 0.0, n21 = 0.0, n12 = 0.0, n22 = 0.0, a1 = 0.0, a2 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int i = d.ncor_ptr[p]; i < d.ncor_ptr[p + 1]; i++) {
     const int c = d.ncor[i], iq = c >> 2, iv = c & 3;
@@ -729,7 +905,62 @@ __global__ void k1_update(Dev1 d, double alfa) {
 // ---------------------------------------------------------------------------
 // Corner forces, face and volume integrals of one quad
 // ---------------------------------------------------------------------------
-template <int MD, bool FAST>
+// RZ face integral (rhsifacedg_lagmc_quadrz, Getrhslagmc.f90:18534-18734):
+// corner forces F = sigma.n A + m (u* - u_v) of the 16 corner faces; face f
+// of vertex iv weighs the basis of its own vertex (f = 1, 2) or of the edge's
+// other vertex (f = 3, 4), the mass flux with the radius weights rcapt
+__device__ void rz_faces(const Dev1 &d, int iq, const double (*x4)[2], double rc, double sc, double (*R)[4]) {
+  const double alfrz = d.alfrz, c05 = 0.5;
+  double fn[4][3], rco[4], bq[4][ND];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int b = (f + 1) & 3;
+    const double anx = x4[b][1] - x4[f][1];
+    const double any = -(x4[b][0] - x4[f][0]);
+    fn[f][0] = anx / sqrt(anx * anx + any * any);
+    fn[f][1] = any / sqrt(anx * anx + any * any);
+    fn[f][2] = sqrt(anx * anx + any * any);
+    rco[f] = 1.0 - alfrz + alfrz * fabs(x4[f][1]);
+    bq[f][0] = 1.0; bq[f][1] = (xv(f) - rc) / 1.0; bq[f][2] = (yv(f) - sc) / 1.0;
+  }
+#pragma unroll
+  for (int k = 0; k < ND; k++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) R[k][q] = 0.0;
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++) {
+    const int vp = (iv + 3) & 3, vx = (iv + 1) & 3;
+    const int p = d.ipq[iv * d.nquad + iq];
+    const double us = d.us[p], vs = d.vs[p];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      const int edge = (f & 1) ? iv : vp;
+      const int bv = (f < 2) ? iv : ((f == 2) ? vp : vx);
+      const double rw = (f < 2) ? 3.0 * rco[iv] : 1.0 * rco[iv];
+      const double rcapt = (rw + ((f & 1) ? rco[vx] : rco[vp])) / 6.0;
+      const int slot = f + 4 * iv;
+      const double m = d.cf[(0 * 16 + slot) * (size_t)d.nquad + iq];
+      const double mu1 = d.cf[(1 * 16 + slot) * (size_t)d.nquad + iq];
+      const double mu2 = d.cf[(2 * 16 + slot) * (size_t)d.nquad + iq];
+      const double s1 = d.cf[(3 * 16 + slot) * (size_t)d.nquad + iq];
+      const double s2 = d.cf[(4 * 16 + slot) * (size_t)d.nquad + iq];
+      const double F0 = s1 + m * us + 0.0 * vs - mu1;
+      const double F1 = s2 + 0.0 * us + m * vs - mu2;
+#pragma unroll
+      for (int k = 0; k < ND; k++) {
+        const double lx = c05 * fn[edge][0] * fn[edge][2] * bq[bv][k];
+        const double ly = c05 * fn[edge][1] * fn[edge][2] * bq[bv][k];
+        const double bc = bq[bv][k];
+        R[k][0] = R[k][0] + us * lx * rcapt + vs * ly * rcapt;
+        R[k][1] = R[k][1] + F0 * bc;
+        R[k][2] = R[k][2] + F1 * bc;
+        R[k][3] = R[k][3] + us * F0 * bc + vs * F1 * bc;
+      }
+    }
+  }
+}
+
+template <int MD, bool FAST, bool RZ>
 __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
@@ -761,51 +992,55 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
   for (int k = 0; k < ND; k++)
 #pragma unroll
     for (int q = 0; q < 4; q++) R[k][q] = 0.0;
+  if (RZ) {
+    rz_faces(d, iq, x4, rc, sc, R);
+  } else {
 #pragma unroll
-  for (int iv = 0; iv < 4; iv++) {
-    const int p = d.ipq[iv * d.nquad + iq];
-    const double us = d.us[p], vs = d.vs[p];
-    // fstarq (Limiterlag.f90:686-698): sigma.n A + mu A (u* - u_v)
-    double F[2][2];
-    if (FAST) {
-      // the corner's two faces summed: F = sum sigma.n A + (sum mu A) u* - sum mu A u_v
-      const double m = d.cf[(0 * 4 + iv) * (size_t)d.nquad + iq];
-      F[0][0] = d.cf[(3 * 4 + iv) * (size_t)d.nquad + iq] + m * us - d.cf[(1 * 4 + iv) * (size_t)d.nquad + iq];
-      F[0][1] = d.cf[(4 * 4 + iv) * (size_t)d.nquad + iq] + m * vs - d.cf[(2 * 4 + iv) * (size_t)d.nquad + iq];
-      F[1][0] = 0.0;
-      F[1][1] = 0.0;
-    }
-#pragma unroll
-    for (int f = 0; f < (FAST ? 0 : 2); f++) {
-      const int slot = f + 2 * iv;
-      const double m = d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq];
-      const double mu1 = d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq];
-      const double mu2 = d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq];
-      const double s1 = d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq];
-      const double s2 = d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq];
-      F[f][0] = s1 + m * us + 0.0 * vs - mu1;
-      F[f][1] = s2 + 0.0 * us + m * vs - mu2;
-    }
-    const int fa = (iv + 3) & 3, fb = iv;
-    const double bqv[ND] = {1.0, (xv(iv) - rc) / 1.0, (yv(iv) - sc) / 1.0};
-#pragma unroll
-    for (int k = 0; k < ND; k++) {
-      const double b3 = 2.0 * bqv[k] + bqv[k];
-      const double l1x = c16 * b3 * fn[fa][0] * fn[fa][2], l1y = c16 * b3 * fn[fa][1] * fn[fa][2];
-      const double l2x = c16 * b3 * fn[fb][0] * fn[fb][2], l2y = c16 * b3 * fn[fb][1] * fn[fb][2];
+    for (int iv = 0; iv < 4; iv++) {
+      const int p = d.ipq[iv * d.nquad + iq];
+      const double us = d.us[p], vs = d.vs[p];
+      // fstarq (Limiterlag.f90:686-698): sigma.n A + mu A (u* - u_v)
+      double F[2][2];
       if (FAST) {
-        const double w = c13 * b3;
-        R[k][0] = R[k][0] + us * (l1x + l2x) + vs * (l1y + l2y);
-        R[k][1] = R[k][1] + F[0][0] * w;
-        R[k][2] = R[k][2] + F[0][1] * w;
-        R[k][3] = R[k][3] + (us * F[0][0] + vs * F[0][1]) * w;
-        continue;
+        // the corner's two faces summed: F = sum sigma.n A + (sum mu A) u* - sum mu A u_v
+        const double m = d.cf[(0 * 4 + iv) * (size_t)d.nquad + iq];
+        F[0][0] = d.cf[(3 * 4 + iv) * (size_t)d.nquad + iq] + m * us - d.cf[(1 * 4 + iv) * (size_t)d.nquad + iq];
+        F[0][1] = d.cf[(4 * 4 + iv) * (size_t)d.nquad + iq] + m * vs - d.cf[(2 * 4 + iv) * (size_t)d.nquad + iq];
+        F[1][0] = 0.0;
+        F[1][1] = 0.0;
       }
-      R[k][0] = R[k][0] + us * l1x + vs * l1y + us * l2x + vs * l2y;
-      R[k][1] = R[k][1] + F[0][0] * c13 * b3 + F[1][0] * c13 * b3;
-      R[k][2] = R[k][2] + F[0][1] * c13 * b3 + F[1][1] * c13 * b3;
-      R[k][3] = R[k][3] + us * F[0][0] * c13 * b3 + vs * F[0][1] * c13 * b3 + us * F[1][0] * c13 * b3 +
-                vs * F[1][1] * c13 * b3;
+#pragma unroll
+      for (int f = 0; f < (FAST ? 0 : 2); f++) {
+        const int slot = f + 2 * iv;
+        const double m = d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq];
+        const double mu1 = d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq];
+        const double mu2 = d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq];
+        const double s1 = d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq];
+        const double s2 = d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq];
+        F[f][0] = s1 + m * us + 0.0 * vs - mu1;
+        F[f][1] = s2 + 0.0 * us + m * vs - mu2;
+      }
+      const int fa = (iv + 3) & 3, fb = iv;
+      const double bqv[ND] = {1.0, (xv(iv) - rc) / 1.0, (yv(iv) - sc) / 1.0};
+#pragma unroll
+      for (int k = 0; k < ND; k++) {
+        const double b3 = 2.0 * bqv[k] + bqv[k];
+        const double l1x = c16 * b3 * fn[fa][0] * fn[fa][2], l1y = c16 * b3 * fn[fa][1] * fn[fa][2];
+        const double l2x = c16 * b3 * fn[fb][0] * fn[fb][2], l2y = c16 * b3 * fn[fb][1] * fn[fb][2];
+        if (FAST) {
+          const double w = c13 * b3;
+          R[k][0] = R[k][0] + us * (l1x + l2x) + vs * (l1y + l2y);
+          R[k][1] = R[k][1] + F[0][0] * w;
+          R[k][2] = R[k][2] + F[0][1] * w;
+          R[k][3] = R[k][3] + (us * F[0][0] + vs * F[0][1]) * w;
+          continue;
+        }
+        R[k][0] = R[k][0] + us * l1x + vs * l1y + us * l2x + vs * l2y;
+        R[k][1] = R[k][1] + F[0][0] * c13 * b3 + F[1][0] * c13 * b3;
+        R[k][2] = R[k][2] + F[0][1] * c13 * b3 + F[1][1] * c13 * b3;
+        R[k][3] = R[k][3] + us * F[0][0] * c13 * b3 + vs * F[0][1] * c13 * b3 + us * F[1][0] * c13 * b3 +
+                  vs * F[1][1] * c13 * b3;
+      }
     }
   }
   // volume integral (rhsdomndg_lag_mc_quadsym, 5x5 Gauss)
@@ -822,7 +1057,17 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
     const double r = cR.g25[ig][0], s = cR.g25[ig][1], wi = cR.w25[ig];
     double dxdr, dxds, dydr, dyds;
     jac4(x4, r, s, dxdr, dxds, dydr, dyds);
-    const double djaco = wi, rcoef = 1.0;
+    const double djaco = wi;
+    // rcoef = 1 - alfrz + alfrz * ygaus (Limiterlag.f90:1268-1279): 1 in plane geometry
+    double rcoef = 1.0;
+    if (RZ) {
+      const double rp = 1.0 + r, rm = 1.0 - r, sp = 1.0 + s, sm = 1.0 - s;
+      const double shpq[4] = {0.25 * rm * sm, 0.25 * rp * sm, 0.25 * rp * sp, 0.25 * rm * sp};
+      double ygaus = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) ygaus = ygaus + shpq[k] * x4[k][1];
+      rcoef = 1.0 - d.alfrz + d.alfrz * ygaus;
+    }
     // gdshp = adj(J) grad_xi b, b = (1, r - rc, s - sc): the rows for b2, b3
     const double g1[ND] = {dyds * 0.0 + (-dydr) * 0.0, dyds * 1.0 + (-dydr) * 0.0, dyds * 0.0 + (-dydr) * 1.0};
     const double g2[ND] = {(-dxds) * 0.0 + dxdr * 0.0, (-dxds) * 1.0 + dxdr * 0.0, (-dxds) * 0.0 + dxdr * 1.0};
@@ -852,6 +1097,34 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
       R[k][1] = R[k][1] - f2 * djaco * rcoef;
       R[k][2] = R[k][2] - f3 * djaco * rcoef;
       R[k][3] = R[k][3] - f4 * djaco * rcoef;
+    }
+  }
+  if (RZ) {
+    // RZ hoop-stress source of the radial (y) momentum
+    // (rhsdomnsrcdg_lagmc_quadrz, Getrhslagmc.f90:15800-16048): 5x5 Gauss,
+    // the limited pressure of the point, no radius weight
+    for (int ig = 0; ig < 25; ig++) {
+      const double r = cR.g25[ig][0], s = cR.g25[ig][1], wi = cR.w25[ig];
+      double dxdr, dxds, dydr, dyds;
+      jac4(x4, r, s, dxdr, dxds, dydr, dyds);
+      const double djaco = wi * (dxdr * dyds - dydr * dxds);
+      const double bb[ND] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+      double un[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        double a = 0.0;
+#pragma unroll
+        for (int k = 0; k < MD; k++) a = a + u[q][k] * bb[k];
+        un[q] = a;
+      }
+      const double rhoad = 1.0 / un[0];
+      double pres = (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]));
+      pres = pctr + af4 * (pres - pctr);
+#pragma unroll
+      for (int k = 0; k < ND; k++) {
+        const double f3 = d.alfrz * (-pres) * bb[k];
+        R[k][2] = R[k][2] - f3 * djaco;
+      }
     }
   }
   if (!fuse) {
@@ -1092,22 +1365,37 @@ static const double kRK[2][3] = {{0.0, 0.5, 0.0}, {0.0, 0.75, 0.3333333333333333
 static void geom(Solver *s, const double *X, const double *Y) {
   const Dev1 &d = s->d;
   launch(s, "geom", [&] {
-    if (s->cfg.order_exact) k1_geom<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, X, Y);
+    // the closed form is the plane area; RZ volumes carry the radius weight
+    if (s->cfg.order_exact || d.nrz) k1_geom<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, X, Y);
     else k1_geom_fast<<<nb(d.nquad, 128), 128, 0, s->st>>>(d, X, Y);
   });
 }
 
+// RZ runs its own instantiations (in the reference's order: the RZ branch
+// has no optimised variant), so the plane kernels keep their registers
 template <bool FAST>
 static void launch_cell(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st) {
-  if (d.mdegr == 3) k1_cell<3, FAST><<<g, b, 0, st>>>(d);
-  else if (d.mdegr == 2) k1_cell<2, FAST><<<g, b, 0, st>>>(d);
-  else k1_cell<1, FAST><<<g, b, 0, st>>>(d);
+  if (d.nrz) {
+    if (d.mdegr == 3) k1_cell<3, false, true><<<g, b, 0, st>>>(d);
+    else if (d.mdegr == 2) k1_cell<2, false, true><<<g, b, 0, st>>>(d);
+    else k1_cell<1, false, true><<<g, b, 0, st>>>(d);
+    return;
+  }
+  if (d.mdegr == 3) k1_cell<3, FAST, false><<<g, b, 0, st>>>(d);
+  else if (d.mdegr == 2) k1_cell<2, FAST, false><<<g, b, 0, st>>>(d);
+  else k1_cell<1, FAST, false><<<g, b, 0, st>>>(d);
 }
 template <bool FAST>
 static void launch_rhs(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st, int fuse, double alfa) {
-  if (d.mdegr == 3) k1_rhs<3, FAST><<<g, b, 0, st>>>(d, fuse, alfa);
-  else if (d.mdegr == 2) k1_rhs<2, FAST><<<g, b, 0, st>>>(d, fuse, alfa);
-  else k1_rhs<1, FAST><<<g, b, 0, st>>>(d, fuse, alfa);
+  if (d.nrz) {
+    if (d.mdegr == 3) k1_rhs<3, false, true><<<g, b, 0, st>>>(d, fuse, alfa);
+    else if (d.mdegr == 2) k1_rhs<2, false, true><<<g, b, 0, st>>>(d, fuse, alfa);
+    else k1_rhs<1, false, true><<<g, b, 0, st>>>(d, fuse, alfa);
+    return;
+  }
+  if (d.mdegr == 3) k1_rhs<3, FAST, false><<<g, b, 0, st>>>(d, fuse, alfa);
+  else if (d.mdegr == 2) k1_rhs<2, FAST, false><<<g, b, 0, st>>>(d, fuse, alfa);
+  else k1_rhs<1, FAST, false><<<g, b, 0, st>>>(d, fuse, alfa);
 }
 
 // the stage sequence of getrhsdg_lag_mcnew's linear branch
@@ -1118,8 +1406,9 @@ static void enqueue_rhs(Solver *s, int fuse, double alfa) {
   const bool ex = s->cfg.order_exact != 0;
   launch(s, "cell", [&] { ex ? launch_cell<false>(d, gq, bq, s->st) : launch_cell<true>(d, gq, bq, s->st); });
   launch(s, "node", [&] {
-    if (ex) k1_node<false><<<gp, bp, 0, s->st>>>(d);
-    else k1_node<true><<<gp, bp, 0, s->st>>>(d);
+    if (d.nrz) k1_node<false, true><<<gp, bp, 0, s->st>>>(d);
+    else if (ex) k1_node<false, false><<<gp, bp, 0, s->st>>>(d);
+    else k1_node<true, false><<<gp, bp, 0, s->st>>>(d);
   });
   launch(s, "rhs", [&] {
     ex ? launch_rhs<false>(d, gq, bq, s->st, fuse, alfa) : launch_rhs<true>(d, gq, bq, s->st, fuse, alfa);
@@ -1187,6 +1476,11 @@ int create(const lag2d_mesh *m, const lag2d_config *c, cudaStream_t st, Solver *
   const int nsu = m->esuv2[np];
   for (int i = 0; i < nsu; i++)
     if (m->esuv1[i] < 1 || m->esuv1[i] > nq) { err = "esuv1 cell id out of range"; return LAG2D_EINVAL; }
+  if (c->nrz != 0 && c->nrz != 1) { err = "nrz = 2 (area-weighted RZ) is not built"; return LAG2D_EUNSUP; }
+  if (c->nrz == 1 && c->ncase == 7) {
+    err = "RZ Sedov runs a hard-coded dt schedule (Getrhslag.f90:1673-1693) that is not built";
+    return LAG2D_EUNSUP;
+  }
   Solver *s = new Solver();
   s->cfg = *c;
   s->st = st;
@@ -1195,6 +1489,7 @@ int create(const lag2d_mesh *m, const lag2d_config *c, cudaStream_t st, Solver *
   d.nsedov = c->nsedov;
   for (int i = 0; i < 4; i++) d.sedov_cell[i] = c->sedov_cell[i];
   d.gamlg = c->gamlg; d.cfl = c->cfl; d.cimpd = c->cimpd; d.tend = c->tend; d.sedov_energy = c->sedov_energy;
+  d.nrz = c->nrz; d.alfrz = c->nrz ? 1.0 : 0.0; d.nbfac = m->nbfac;
   // connectivity
   std::vector<int> ipq(4 * (size_t)nq), eptr(np + 1), esv(nsu), cptr(np + 1, 0), cor(4 * (size_t)nq);
   for (int iq = 0; iq < nq; iq++)
@@ -1233,19 +1528,43 @@ int create(const lag2d_mesh *m, const lag2d_config *c, cudaStream_t st, Solver *
     if (b[2] == 22 && b[3] == 222)
       for (int k = 0; k < 2; k++) wall[b[k] - 1] = (wall[b[k] - 1] == 3) ? 10 : 2;
   }
-  int *ipq_d, *eptr_d, *esv_d, *cptr_d, *cor_d;
+  // RZ: each node's boundary faces in face order, the faces' end nodes and
+  // codes (getbc_lagmaire2 loops over the boundary faces)
+  const int nbf = m->nbfac;
+  std::vector<int> bptr(np + 1, 0), blist, bfn(2 * (size_t)std::max(nbf, 1)), bfcode(std::max(nbf, 1));
+  for (int i = 0; i < nbf; i++) {
+    const int *b = m->bface + 5 * (size_t)i;
+    bfn[i] = b[0] - 1;
+    bfn[nbf + i] = b[1] - 1;
+    bfcode[i] = b[2] * 1000 + b[3];
+    bptr[b[0]]++;
+    if (b[1] != b[0]) bptr[b[1]]++;
+  }
+  for (int p = 0; p < np; p++) bptr[p + 1] += bptr[p];
+  blist.resize(std::max(bptr[np], 1));
+  {
+    std::vector<int> fill(bptr.begin(), bptr.end() - 1);
+    for (int i = 0; i < nbf; i++) {
+      const int *b = m->bface + 5 * (size_t)i;
+      blist[fill[b[0] - 1]++] = i;
+      if (b[1] != b[0]) blist[fill[b[1] - 1]++] = i;
+    }
+  }
+  int *ipq_d, *eptr_d, *esv_d, *cptr_d, *cor_d, *bptr_d, *blist_d, *bfn_d, *bfcode_d;
   unsigned char *bc_d, *wall_d;
   double *x0, *y0;
   bool ok = dalloc(s, &ipq_d, ipq.size()) && dalloc(s, &eptr_d, eptr.size()) && dalloc(s, &esv_d, esv.size()) &&
             dalloc(s, &cptr_d, cptr.size()) && dalloc(s, &cor_d, cor.size()) && dalloc(s, &bc_d, bc.size()) &&
-            dalloc(s, &wall_d, wall.size()) && dalloc(s, &x0, np) && dalloc(s, &y0, np);
+            dalloc(s, &wall_d, wall.size()) && dalloc(s, &x0, np) && dalloc(s, &y0, np) &&
+            dalloc(s, &bptr_d, bptr.size()) && dalloc(s, &blist_d, blist.size()) && dalloc(s, &bfn_d, bfn.size()) &&
+            dalloc(s, &bfcode_d, bfcode.size());
   const size_t ncl = nq;
   ok = ok && dalloc(s, &d.rc, ncl) && dalloc(s, &d.sc, ncl) && dalloc(s, &d.vol, ncl) && dalloc(s, &d.vcx, ncl) &&
        dalloc(s, &d.vcy, ncl) && dalloc(s, &d.mass, ncl) && dalloc(s, &d.amatr, 4 * ncl) &&
        dalloc(s, &d.Un, NU1 * ncl) && dalloc(s, &d.Us, NU1 * ncl) && dalloc(s, &d.xn, np) && dalloc(s, &d.yn, np) &&
        dalloc(s, &d.xs, np) && dalloc(s, &d.ys, np) && dalloc(s, &d.us, np) && dalloc(s, &d.vs, np) &&
        dalloc(s, &d.bmax, 5 * (size_t)np) && dalloc(s, &d.bmin, 5 * (size_t)np) && dalloc(s, &d.lim, 7 * ncl) &&
-       dalloc(s, &d.cf, 40 * ncl) && dalloc(s, &d.rhs, NU1 * ncl) &&
+       dalloc(s, &d.cf, (c->nrz ? 80 : 40) * ncl) && dalloc(s, &d.rhs, NU1 * ncl) &&
        dalloc(s, &d.dtpart, 2 * (size_t)nb(nq, 256)) && dalloc(s, &d.sc_dev, 1) &&
        dalloc(s, &s->stage_u, NU1 * ncl) && dalloc(s, &s->stage_x, 2 * (size_t)np);
   if (!ok) {
@@ -1255,12 +1574,15 @@ int create(const lag2d_mesh *m, const lag2d_config *c, cudaStream_t st, Solver *
   }
   d.ipq = ipq_d; d.esuv_ptr = eptr_d; d.esuv = esv_d; d.ncor_ptr = cptr_d; d.ncor = cor_d; d.bc = bc_d;
   d.wall = wall_d; d.x0 = x0; d.y0 = y0;
+  d.bf_ptr = bptr_d; d.bf_list = blist_d; d.bfn = bfn_d; d.bfcode = bfcode_d;
   std::vector<double> xx(np), yy(np);
   for (int p = 0; p < np; p++) { xx[p] = m->coold[2 * (size_t)p]; yy[p] = m->coold[2 * (size_t)p + 1]; }
 #define UP1(dst, src, n) cudaMemcpyAsync((void *)(dst), (src), (n) * sizeof(*(src)), cudaMemcpyHostToDevice, st)
   UP1(ipq_d, ipq.data(), ipq.size()); UP1(eptr_d, eptr.data(), eptr.size()); UP1(esv_d, esv.data(), esv.size());
   UP1(cptr_d, cptr.data(), cptr.size()); UP1(cor_d, cor.data(), cor.size()); UP1(bc_d, bc.data(), bc.size());
   UP1(wall_d, wall.data(), wall.size()); UP1(x0, xx.data(), np); UP1(y0, yy.data(), np);
+  UP1(bptr_d, bptr.data(), bptr.size()); UP1(blist_d, blist.data(), blist.size());
+  UP1(bfn_d, bfn.data(), bfn.size()); UP1(bfcode_d, bfcode.data(), bfcode.size());
   UP1(d.xn, xx.data(), np); UP1(d.yn, yy.data(), np); UP1(d.xs, xx.data(), np); UP1(d.ys, yy.data(), np);
 #undef UP1
   Rules rl;

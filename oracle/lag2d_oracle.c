@@ -339,7 +339,9 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
             double *geoel, double *amatr, double *unkno) {
   const int ntria = m->ntria, nquad = m->nquad;
   const int ncell = ntria + nquad, nsize = ncell + m->nbfac;
-  const double alfrz = 0.0;
+  /* alfrz (dgflo2d.f90:150-156): 1 in RZ, where the cell integrals carry the
+   * radius y as a weight; RZ is dispatched on linear cells only */
+  const double alfrz = (c->npoly == 1 && c->nrz == 1) ? 1.0 : 0.0;
   double pos36[36][2], w36[36], pos25[25][2], w25[25];
   quad_rule(36, 0, pos36, w36);
   quad_rule(25, 0, pos25, w25);
@@ -525,7 +527,7 @@ void o_cellvol(const o_mesh *m, const o_cfg *c, double *geoel, const double *coo
   if (m->ntria > 0) cellvol_tria(m, c, geoel, coord);
   double pos36[36][2], w36[36];
   quad_rule(36, 0, pos36, w36);
-  const double alfrz = 0.0;
+  const double alfrz = (c->npoly == 1 && c->nrz == 1) ? 1.0 : 0.0;
   for (int ie = 0; ie < m->nquad; ie++) {
     const int ielem = ie + m->ntria;
     double xp[9][2], shp[9], dr[9], ds[9];
@@ -2554,6 +2556,292 @@ static void jac4(const double (*xpq)[2], double r, double s, double *dxdr, doubl
   *dxdr = a; *dxds = b; *dydr = cc; *dyds = d;
 }
 
+/* ---------------------------------------------------------------------- */
+/* RZ (nrz = 1, alfrz = 1, the radius is y) nodal solve and face integral */
+/* of the linear P1 branch: getndvelo_lagmc_rz (Getrhslagmc.f90:          */
+/* 17284-17597) with getriem_quadrz (:17963-18336) and getbc_lagmaire2    */
+/* (Getrhslag.f90:11269-11491), then rhsifacedg_lagmc_quadrz              */
+/* (Getrhslagmc.f90:18534-18734).  Quads only.  Each vertex has 4 corner  */
+/* faces: its two edges, each twice, with the radius weights of the two   */
+/* halves of the edge's r-weighted length.  aflim (5, nquad), afvec       */
+/* (2,2,nquad) and gelq (3,4,nquad) are o1_rhs's arrays; ustar holds the  */
+/* previous nodal velocity on entry and the new one on return.            */
+/* ---------------------------------------------------------------------- */
+static void o1_rz_nodes_faces(const o_mesh *m, const o_cfg *c, double *ustar, const double *unkno,
+                              double *rhsel, const double *geoel, const double *coord, const double *aflim,
+                              const double *afvec, const double *gelq) {
+  const int nquad = m->nquad, npoin = m->npoin;
+  const double g = c->gamlg, alfrz = 1.0, eps9 = 1.0e-09;
+#define QN(ie, k) (m->ipqua[4 * (ie) + (k)] - 1)
+#define GL(f, ie) (gelq + 3 * ((f) + 4 * (ie)))
+#define AF(k, ie) aflim[(k) + 5 * (ie)]
+#define AV(i, j, ie) afvec[(i) + 2 * (j) + 4 * (ie)]
+  int *indnd = (int *)calloc((size_t)npoin, sizeof(int));
+  double *vlave = (double *)malloc(sizeof(double) * 2 * (size_t)npoin);
+  double *munacn = (double *)calloc((size_t)4 * npoin, sizeof(double));
+  double *munacu = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *snsigm = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *mcl = (double *)malloc(sizeof(double) * 4 * 16 * (size_t)nquad);  /* munaclq(2,2,4,4) */
+  double *mul = (double *)malloc(sizeof(double) * 2 * 16 * (size_t)nquad);  /* munaulq(2,4,4) */
+  double *snl = (double *)malloc(sizeof(double) * 2 * 16 * (size_t)nquad);  /* snsigmlq(2,4,4) */
+  double *fst = (double *)malloc(sizeof(double) * 2 * 16 * (size_t)nquad);  /* fsqrz(2,4,4) */
+  double *fpres = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *bsnv = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *bsnpf = (double *)calloc((size_t)2 * npoin, sizeof(double));
+
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    if (c->ncase == 2) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
+  }
+  for (int ifa = 0; ifa < m->nbfac; ifa++)
+    if (m->bface[5 * ifa + 2] == 25) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
+  /* getvlavenew's average is overwritten by the previous nodal velocity (:17404-17407) */
+  memcpy(vlave, ustar, sizeof(double) * 2 * (size_t)npoin);
+
+  /* getriem_quadrz, scattering in cell order */
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double bq[4][3];
+    for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
+    double rcoeq[4];
+    for (int iv = 0; iv < 4; iv++) rcoeq[iv] = 1.0 - alfrz + alfrz * fabs(X_(coord, 1, QN(ie, iv)));
+    /* faces 1, 3: the edge to the previous vertex; 2, 4: the edge to the next */
+    double vn[4][4][3];
+    for (int iv = 0; iv < 4; iv++) {
+      const int ep = (iv + 3) % 4, en = iv, vp = (iv + 3) % 4, vx = (iv + 1) % 4;
+      for (int k = 0; k < 3; k++) {
+        vn[iv][0][k] = GL(ep, ie)[k]; vn[iv][1][k] = GL(en, ie)[k];
+        vn[iv][2][k] = GL(ep, ie)[k]; vn[iv][3][k] = GL(en, ie)[k];
+      }
+      vn[iv][0][2] = (3.0 * rcoeq[iv] + rcoeq[vp]) / 3.0 * 0.5 * vn[iv][0][2];
+      vn[iv][1][2] = (3.0 * rcoeq[iv] + rcoeq[vx]) / 3.0 * 0.5 * vn[iv][1][2];
+      vn[iv][2][2] = (1.0 * rcoeq[iv] + rcoeq[vp]) / 3.0 * 0.5 * vn[iv][2][2];
+      vn[iv][3][2] = (1.0 * rcoeq[iv] + rcoeq[vx]) / 3.0 * 0.5 * vn[iv][3][2];
+    }
+    for (int iv = 0; iv < 4; iv++)
+      for (int f = 0; f < 4; f++) vn[iv][f][2] = 0.5 * vn[iv][f][2];
+    double rhomc = U_(unkno, c, 0, 0, ielem);
+    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+    double rhoct = 1.0 / rhomc;
+    double pctr = fmax(eps9, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    double unknvq[4][5], sig[4], aujmp[4][3];
+    p1_vertex(c, unkno, ielem, rc, sc, unknvq);
+    const double a11 = AV(0, 0, ie), a12 = AV(0, 1, ie), a21 = AV(1, 0, ie), a22 = AV(1, 1, ie);
+    for (int iv = 0; iv < 4; iv++) {
+      double rhovt = 1.0 / unknvq[iv][0];
+      double uv = unknvq[iv][1], vv = unknvq[iv][2], ev = unknvq[iv][3];
+      double pvtx = fmax(eps9, (g - 1.0) * rhovt * (ev - 0.5 * (uv * uv + vv * vv)));
+      double dudr = a11 * U_(unkno, c, 1, 1, ielem) + a12 * U_(unkno, c, 1, 2, ielem);
+      double duds = a11 * U_(unkno, c, 2, 1, ielem) + a12 * U_(unkno, c, 2, 2, ielem);
+      double dvdr = a21 * U_(unkno, c, 1, 1, ielem) + a22 * U_(unkno, c, 1, 2, ielem);
+      double dvds = a21 * U_(unkno, c, 2, 1, ielem) + a22 * U_(unkno, c, 2, 2, ielem);
+      uv = U_(unkno, c, 0, 1, ielem) + dudr * bq[iv][1] + duds * bq[iv][2];
+      vv = U_(unkno, c, 0, 2, ielem) + dvdr * bq[iv][1] + dvds * bq[iv][2];
+      pvtx = pctr + AF(3, ie) * (pvtx - pctr);
+      unknvq[iv][1] = uv;
+      unknvq[iv][2] = vv;
+      sig[iv] = -pvtx;
+      int ip = QN(ie, iv);
+      double acnx = X_(vlave, 0, ip) - uv, acny = X_(vlave, 1, ip) - vv;
+      double nrm = sqrt(acnx * acnx + acny * acny);
+      if (nrm < TINY_S) { aujmp[iv][0] = TINY_S; aujmp[iv][1] = TINY_S; }
+      else { aujmp[iv][0] = acnx / nrm; aujmp[iv][1] = acny / nrm; }
+      aujmp[iv][2] = nrm;
+    }
+    double sdctr = sqrt(fmax(eps9, g * pctr / rhoct));
+    for (int iv = 0; iv < 4; iv++) aujmp[iv][2] = aujmp[iv][2] / sdctr;
+    /* the impedance is the acoustic one: the shock term is commented out (:18273) */
+    const double murie = rhoct * sdctr;
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      for (int f = 0; f < 4; f++) {
+        /* getriecoef_matrixnew, Limiterlag.f90:1037-1076 */
+        double area = vn[iv][f][2], n1 = vn[iv][f][0], n2 = vn[iv][f][1];
+        double vnau = (aujmp[iv][2] < 1.0e12) ? 1.0 : n1 * aujmp[iv][0] + n2 * aujmp[iv][1];
+        double mc11 = murie * area * fabs(vnau), mc21 = 0.0, mc12 = 0.0, mc22 = murie * area * fabs(vnau);
+        double mu1 = mc11 * unknvq[iv][1] + mc21 * unknvq[iv][2];
+        double mu2 = mc21 * unknvq[iv][1] + mc22 * unknvq[iv][2];
+        double s1 = sig[iv] * area * n1 + (0.0 + 0.0) * area * n2;
+        double s2 = (0.0 + 0.0) * area * n1 + sig[iv] * area * n2;
+        munacn[0 + 4 * ip] = munacn[0 + 4 * ip] + mc11;
+        munacn[1 + 4 * ip] = munacn[1 + 4 * ip] + mc21;
+        munacn[2 + 4 * ip] = munacn[2 + 4 * ip] + mc12;
+        munacn[3 + 4 * ip] = munacn[3 + 4 * ip] + mc22;
+        munacu[0 + 2 * ip] = munacu[0 + 2 * ip] + mu1;
+        munacu[1 + 2 * ip] = munacu[1 + 2 * ip] + mu2;
+        snsigm[0 + 2 * ip] = snsigm[0 + 2 * ip] + s1;
+        snsigm[1 + 2 * ip] = snsigm[1 + 2 * ip] + s2;
+        const size_t o = (size_t)f + 4 * (iv + 4 * (size_t)ie);
+        mcl[4 * o + 0] = mc11; mcl[4 * o + 1] = mc21; mcl[4 * o + 2] = mc12; mcl[4 * o + 3] = mc22;
+        mul[2 * o + 0] = mu1; mul[2 * o + 1] = mu2;
+        snl[2 * o + 0] = s1; snl[2 * o + 1] = s2;
+      }
+    }
+  }
+  /* getbc_lagmaire2 (Getrhslag.f90:11269-11491): boundary area vectors of
+   * the velocity walls (code 22, with the radius weights of the face's two
+   * ends) and pressure forces of code 21 (ncase 3: p = 1e-6); then at the
+   * wall nodes the force fpres that removes the wall-normal velocity from
+   * the node solve.  gflag = unit normal and length of the boundary face
+   * (getfnds_lag_mc_hybrid, Getrhslagmc.f90:2147-2162). */
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    const int *bf = m->bface + 5 * ifa;
+    const int ipf[2] = {bf[0] - 1, bf[1] - 1};
+    double anx = X_(coord, 1, ipf[1]) - X_(coord, 1, ipf[0]);
+    double any = -(X_(coord, 0, ipf[1]) - X_(coord, 0, ipf[0]));
+    const double gf1 = anx / sqrt(anx * anx + any * any), gf2 = any / sqrt(anx * anx + any * any);
+    const double gf3 = sqrt(anx * anx + any * any);
+    double rcoef[2];
+    rcoef[0] = 1.0 - alfrz + alfrz * X_(coord, 1, ipf[0]);
+    rcoef[1] = 1.0 - alfrz + alfrz * X_(coord, 1, ipf[1]);
+    double bsnx = 0.0, bsny = 0.0;
+    if (bf[2] == 22) {
+      if (bf[3] == 221) {
+        bsnx = 0.0 * gf3 * 0.5;
+        bsny = -1.0 * gf3 * 0.5;
+        if (c->ncase == 1 || c->ncase == 2 || c->ncase == 12) {
+          if (X_(coord, 1, ipf[0]) < 1.0e-6 && X_(coord, 1, ipf[1]) < 1.0e-6) {
+            bsnx = 0.0 * gf3 * 0.5; bsny = -1.0 * gf3 * 0.5;
+          } else if (fabs(X_(coord, 1, ipf[0]) - 1.0) < 1.0e-6 && fabs(X_(coord, 1, ipf[1]) - 1.0) < 1.0e-6) {
+            bsnx = 0.0 * gf3 * 0.5; bsny = 1.0 * gf3 * 0.5;
+          }
+        }
+      } else if (bf[3] == 222) {
+        bsnx = -1.0 * gf3 * 0.5;
+        bsny = 0.0 * gf3 * 0.5;
+        if (c->ncase == 1) {
+          if (X_(coord, 0, ipf[0]) < 1.0e-6 && X_(coord, 0, ipf[1]) < 1.0e-6) {
+            bsnx = -1.0 * gf3 * 0.5; bsny = 0.0 * gf3 * 0.5;
+          } else if (fabs(X_(coord, 0, ipf[0]) - 1.0) < 1.0e-6 && fabs(X_(coord, 0, ipf[1]) - 1.0) < 1.0e-6) {
+            bsnx = 1.0 * gf3 * 0.5; bsny = 0.0 * gf3 * 0.5;
+          }
+        }
+      }
+      bsnv[0 + 2 * ipf[0]] = bsnv[0 + 2 * ipf[0]] + bsnx * (2.0 * rcoef[0] + rcoef[1]) / 3.0;
+      bsnv[1 + 2 * ipf[0]] = bsnv[1 + 2 * ipf[0]] + bsny * (2.0 * rcoef[0] + rcoef[1]) / 3.0;
+      bsnv[0 + 2 * ipf[1]] = bsnv[0 + 2 * ipf[1]] + bsnx * (2.0 * rcoef[1] + rcoef[0]) / 3.0;
+      bsnv[1 + 2 * ipf[1]] = bsnv[1 + 2 * ipf[1]] + bsny * (2.0 * rcoef[1] + rcoef[0]) / 3.0;
+    } else if (bf[2] == 21) {
+      bsnx = gf1 * gf3 * 0.5;
+      bsny = gf2 * gf3 * 0.5;
+      if (c->ncase == 3) {
+        const double pres0 = 1.0e-6;
+        bsnpf[0 + 2 * ipf[0]] = bsnpf[0 + 2 * ipf[0]] + pres0 * bsnx * (2.0 * rcoef[0] + rcoef[1]) / 3.0;
+        bsnpf[1 + 2 * ipf[0]] = bsnpf[1 + 2 * ipf[0]] + pres0 * bsny * (2.0 * rcoef[0] + rcoef[1]) / 3.0;
+        bsnpf[0 + 2 * ipf[1]] = bsnpf[0 + 2 * ipf[1]] + pres0 * bsnx * (2.0 * rcoef[1] + rcoef[0]) / 3.0;
+        bsnpf[1 + 2 * ipf[1]] = bsnpf[1 + 2 * ipf[1]] + pres0 * bsny * (2.0 * rcoef[1] + rcoef[0]) / 3.0;
+      }
+    }
+  }
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    const int *bf = m->bface + 5 * ifa;
+    if (bf[2] != 22) continue;
+    for (int k = 0; k < 2; k++) {
+      const int ip = bf[k] - 1;
+      const double *mn = munacn + 4 * ip;  /* (1,1), (2,1), (1,2), (2,2) */
+      double detma = mn[0] * mn[3] - mn[1] * mn[2];
+      double i11 = mn[3] / detma, i12 = -mn[2] / detma, i21 = -mn[1] / detma, i22 = mn[0] / detma;
+      double lnx = bsnv[0 + 2 * ip], lny = bsnv[1 + 2 * ip];
+      double coefl = (i11 * lnx + i12 * lny) * lnx + (i21 * lnx + i22 * lny) * lny;
+      double rhsx = munacu[0 + 2 * ip] - snsigm[0 + 2 * ip] - bsnpf[0 + 2 * ip];
+      double rhsy = munacu[1 + 2 * ip] - snsigm[1 + 2 * ip] - bsnpf[1 + 2 * ip];
+      double coefr = (i11 * rhsx + i12 * rhsy) * lnx + (i21 * rhsx + i22 * rhsy) * lny;
+      fpres[0 + 2 * ip] = coefr / fmax(1.0e-16, coefl) * lnx;
+      fpres[1 + 2 * ip] = coefr / fmax(1.0e-16, coefl) * lny;
+    }
+  }
+  for (int ip = 0; ip < npoin; ip++) {
+    fpres[0 + 2 * ip] = fpres[0 + 2 * ip] + bsnpf[0 + 2 * ip];
+    fpres[1 + 2 * ip] = fpres[1 + 2 * ip] + bsnpf[1 + 2 * ip];
+  }
+  /* the node solve with the boundary forces (:17446-17461) */
+  for (int ip = 0; ip < npoin; ip++) {
+    if (indnd[ip]) continue;
+    const double *mn = munacn + 4 * ip;
+    double detma = mn[0] * mn[3] - mn[1] * mn[2];
+    double i11 = mn[3] / detma, i12 = -mn[2] / detma, i21 = -mn[1] / detma, i22 = mn[0] / detma;
+    double r1 = munacu[2 * ip] - snsigm[2 * ip] - fpres[2 * ip];
+    double r2 = munacu[2 * ip + 1] - snsigm[2 * ip + 1] - fpres[2 * ip + 1];
+    X_(ustar, 0, ip) = i11 * r1 + i12 * r2;
+    X_(ustar, 1, ip) = i21 * r1 + i22 * r2;
+  }
+  /* node 1 held (:17475), then the walls: 222 holds u, code 25 both; the
+   * zeroing of v on 221 is commented out in RZ (:17482) */
+  X_(ustar, 0, 0) = 0.0;
+  X_(ustar, 1, 0) = 0.0;
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    const int *bf = m->bface + 5 * ifa;
+    for (int k = 0; k < 2; k++) {
+      int ip = bf[k] - 1;
+      if (bf[2] == 22) {
+        if (bf[3] == 222) X_(ustar, 0, ip) = 0.0;
+      } else if (bf[2] == 25) {
+        X_(ustar, 1, ip) = 0.0;
+        X_(ustar, 0, ip) = 0.0;
+      }
+    }
+  }
+  /* corner forces fsqrz (:17568-17590) */
+  for (int ie = 0; ie < nquad; ie++)
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      for (int f = 0; f < 4; f++) {
+        const size_t o = (size_t)f + 4 * (iv + 4 * (size_t)ie);
+        fst[2 * o + 0] = snl[2 * o + 0] + mcl[4 * o + 0] * X_(ustar, 0, ip) + mcl[4 * o + 1] * X_(ustar, 1, ip) - mul[2 * o + 0];
+        fst[2 * o + 1] = snl[2 * o + 1] + mcl[4 * o + 2] * X_(ustar, 0, ip) + mcl[4 * o + 3] * X_(ustar, 1, ip) - mul[2 * o + 1];
+      }
+    }
+  /* rhsifacedg_lagmc_quadrz: per corner face the basis of the face's own
+   * vertex (faces 1, 2) or of the edge's other vertex (3, 4), with the
+   * radius weights rcapt */
+  const double c05 = 0.5;
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double bq[4][3];
+    for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
+    double rcoeq[4];
+    for (int iv = 0; iv < 4; iv++) rcoeq[iv] = 1.0 - alfrz + alfrz * fabs(X_(coord, 1, QN(ie, iv)));
+    double ul[3] = {0, 0, 0}, p1[3] = {0, 0, 0}, p2[3] = {0, 0, 0}, el[3] = {0, 0, 0};
+    for (int iv = 0; iv < 4; iv++) {
+      const int ep = (iv + 3) % 4, en = iv, vp = (iv + 3) % 4, vx = (iv + 1) % 4;
+      const int edge[4] = {ep, en, ep, en}, bvert[4] = {iv, iv, vp, vx};
+      double rcapt[4];
+      rcapt[0] = (3.0 * rcoeq[iv] + rcoeq[vp]) / 6.0;
+      rcapt[1] = (3.0 * rcoeq[iv] + rcoeq[vx]) / 6.0;
+      rcapt[2] = (1.0 * rcoeq[iv] + rcoeq[vp]) / 6.0;
+      rcapt[3] = (1.0 * rcoeq[iv] + rcoeq[vx]) / 6.0;
+      int ip = QN(ie, iv);
+      double us = X_(ustar, 0, ip), vs = X_(ustar, 1, ip);
+      for (int f = 0; f < 4; f++) {
+        const size_t o = (size_t)f + 4 * (iv + 4 * (size_t)ie);
+        const double *gl = GL(edge[f], ie);
+        for (int k = 0; k < c->ndegr; k++) {
+          double lx = c05 * gl[0] * gl[2] * bq[bvert[f]][k];
+          double ly = c05 * gl[1] * gl[2] * bq[bvert[f]][k];
+          double bc = bq[bvert[f]][k];
+          ul[k] = ul[k] + us * lx * rcapt[f] + vs * ly * rcapt[f];
+          p1[k] = p1[k] + fst[2 * o] * bc;
+          p2[k] = p2[k] + fst[2 * o + 1] * bc;
+          el[k] = el[k] + us * fst[2 * o] * bc + vs * fst[2 * o + 1] * bc;
+        }
+      }
+    }
+    for (int k = 0; k < c->ndegr; k++) {
+      U_(rhsel, c, k, 0, ielem) = ul[k];
+      U_(rhsel, c, k, 1, ielem) = p1[k];
+      U_(rhsel, c, k, 2, ielem) = p2[k];
+      U_(rhsel, c, k, 3, ielem) = el[k];
+    }
+  }
+#undef QN
+#undef GL
+#undef AF
+#undef AV
+  free(indnd); free(vlave); free(munacn); free(munacu); free(snsigm); free(mcl); free(mul); free(snl);
+  free(fst); free(fpres); free(bsnv); free(bsnpf);
+}
+
 void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
             double *rhsel, const double *geoel, const double *coord,
             double *aflim_out, double *afvec_out) {
@@ -2792,155 +3080,160 @@ void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
     AF(4, ie) = a;
   }
 
-  /* I.1.3 getndvelo_lag_mc_matrixsym, Limiterlag.f90:408-704 */
-  for (int ifa = 0; ifa < m->nbfac; ifa++) {
-    if (c->ncase == 2) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
-    if (m->bface[5 * ifa + 2] == 25) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
-  }
-  memcpy(vlave, ustar, sizeof(double) * 2 * (size_t)npoin);
-  /* getriem_quad_matrixsym, Limiterlag.f90:708-1033, scattering in cell order */
-  for (int ie = 0; ie < nquad; ie++) {
-    const int ielem = ie + m->ntria;
-    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
-    double bq[4][3];
-    for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
-    /* corner iv touches faces iv-1 and iv; the area weight (2 r_a + r_b)/3 * 0.5 * |f| with r = 1 */
-    double vn[4][2][3];
-    for (int iv = 0; iv < 4; iv++) {
-      int fa = (iv + 3) % 4, fb = iv;
-      for (int k = 0; k < 3; k++) { vn[iv][0][k] = GL(fa, ie)[k]; vn[iv][1][k] = GL(fb, ie)[k]; }
-      vn[iv][0][2] = (2.0 * 1.0 + 1.0) / 3.0 * 0.5 * vn[iv][0][2];
-      vn[iv][1][2] = (2.0 * 1.0 + 1.0) / 3.0 * 0.5 * vn[iv][1][2];
+  if (c->nrz == 1) {
+    /* RZ: getndvelo_lagmc_rz and rhsifacedg_lagmc_quadrz (Getrhslagmc.f90:6884-6887, :6911-6917) */
+    o1_rz_nodes_faces(m, c, ustar, unkno, rhsel, geoel, coord, aflim, afvec, gelq);
+  } else {
+    /* I.1.3 getndvelo_lag_mc_matrixsym, Limiterlag.f90:408-704 */
+    for (int ifa = 0; ifa < m->nbfac; ifa++) {
+      if (c->ncase == 2) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
+      if (m->bface[5 * ifa + 2] == 25) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
     }
-    double rhomc = U_(unkno, c, 0, 0, ielem);
-    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
-    double rhoct = 1.0 / rhomc;
-    double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
-    double unknvq[4][5], sig[4], aujmp[4][3];
-    p1_vertex(c, unkno, ielem, rc, sc, unknvq);
-    const double a11 = AV(0, 0, ie), a12 = AV(0, 1, ie), a21 = AV(1, 0, ie), a22 = AV(1, 1, ie);
-    for (int iv = 0; iv < 4; iv++) {
-      double rhovt = 1.0 / unknvq[iv][0];
-      double uv = unknvq[iv][1], vv = unknvq[iv][2], ev = unknvq[iv][3];
-      double pvtx = fmax(epsd, (g - 1.0) * rhovt * (ev - 0.5 * (uv * uv + vv * vv)));
-      double rhomv = rhomc + AF(0, ie) * (unknvq[iv][0] - rhomc);
-      rhovt = 1.0 / rhomv;
-      (void)rhovt;
-      double dudr = a11 * U_(unkno, c, 1, 1, ielem) + a12 * U_(unkno, c, 1, 2, ielem);
-      double duds = a11 * U_(unkno, c, 2, 1, ielem) + a12 * U_(unkno, c, 2, 2, ielem);
-      double dvdr = a21 * U_(unkno, c, 1, 1, ielem) + a22 * U_(unkno, c, 1, 2, ielem);
-      double dvds = a21 * U_(unkno, c, 2, 1, ielem) + a22 * U_(unkno, c, 2, 2, ielem);
-      uv = U_(unkno, c, 0, 1, ielem) + dudr * bq[iv][1] + duds * bq[iv][2];
-      vv = U_(unkno, c, 0, 2, ielem) + dvdr * bq[iv][1] + dvds * bq[iv][2];
-      pvtx = pctr + AF(3, ie) * (pvtx - pctr);
-      unknvq[iv][1] = uv;
-      unknvq[iv][2] = vv;
-      sig[iv] = -pvtx + 0.0;
-      int ip = QN(ie, iv);
-      double acnx = X_(vlave, 0, ip) - uv, acny = X_(vlave, 1, ip) - vv;
-      double nrm = sqrt(acnx * acnx + acny * acny);
-      if (nrm < TINY_S) { aujmp[iv][0] = TINY_S; aujmp[iv][1] = TINY_S; }
-      else { aujmp[iv][0] = acnx / nrm; aujmp[iv][1] = acny / nrm; }
-      aujmp[iv][2] = nrm;
-    }
-    double sdctr = sqrt(fmax(epsd, g * pctr / rhoct));
-    for (int iv = 0; iv < 4; iv++) aujmp[iv][2] = aujmp[iv][2] / sdctr;
-    double murie[4][2];
-    for (int iv = 0; iv < 4; iv++) {
-      int ip = QN(ie, iv);
-      double dux = X_(vlave, 0, ip) - unknvq[iv][1], duy = X_(vlave, 1, ip) - unknvq[iv][2];
-      for (int f = 0; f < 2; f++) {
-        double deltu = fabs(dux * vn[iv][f][0] + duy * vn[iv][f][1]);
-        murie[iv][f] = rhoct * sdctr + c->cimpd * rhoct * slpdu * deltu;
+    memcpy(vlave, ustar, sizeof(double) * 2 * (size_t)npoin);
+    /* getriem_quad_matrixsym, Limiterlag.f90:708-1033, scattering in cell order */
+    for (int ie = 0; ie < nquad; ie++) {
+      const int ielem = ie + m->ntria;
+      double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+      double bq[4][3];
+      for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
+      /* corner iv touches faces iv-1 and iv; the area weight (2 r_a + r_b)/3 * 0.5 * |f| with r = 1 */
+      double vn[4][2][3];
+      for (int iv = 0; iv < 4; iv++) {
+        int fa = (iv + 3) % 4, fb = iv;
+        for (int k = 0; k < 3; k++) { vn[iv][0][k] = GL(fa, ie)[k]; vn[iv][1][k] = GL(fb, ie)[k]; }
+        vn[iv][0][2] = (2.0 * 1.0 + 1.0) / 3.0 * 0.5 * vn[iv][0][2];
+        vn[iv][1][2] = (2.0 * 1.0 + 1.0) / 3.0 * 0.5 * vn[iv][1][2];
+      }
+      double rhomc = U_(unkno, c, 0, 0, ielem);
+      double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+      double rhoct = 1.0 / rhomc;
+      double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+      double unknvq[4][5], sig[4], aujmp[4][3];
+      p1_vertex(c, unkno, ielem, rc, sc, unknvq);
+      const double a11 = AV(0, 0, ie), a12 = AV(0, 1, ie), a21 = AV(1, 0, ie), a22 = AV(1, 1, ie);
+      for (int iv = 0; iv < 4; iv++) {
+        double rhovt = 1.0 / unknvq[iv][0];
+        double uv = unknvq[iv][1], vv = unknvq[iv][2], ev = unknvq[iv][3];
+        double pvtx = fmax(epsd, (g - 1.0) * rhovt * (ev - 0.5 * (uv * uv + vv * vv)));
+        double rhomv = rhomc + AF(0, ie) * (unknvq[iv][0] - rhomc);
+        rhovt = 1.0 / rhomv;
+        (void)rhovt;
+        double dudr = a11 * U_(unkno, c, 1, 1, ielem) + a12 * U_(unkno, c, 1, 2, ielem);
+        double duds = a11 * U_(unkno, c, 2, 1, ielem) + a12 * U_(unkno, c, 2, 2, ielem);
+        double dvdr = a21 * U_(unkno, c, 1, 1, ielem) + a22 * U_(unkno, c, 1, 2, ielem);
+        double dvds = a21 * U_(unkno, c, 2, 1, ielem) + a22 * U_(unkno, c, 2, 2, ielem);
+        uv = U_(unkno, c, 0, 1, ielem) + dudr * bq[iv][1] + duds * bq[iv][2];
+        vv = U_(unkno, c, 0, 2, ielem) + dvdr * bq[iv][1] + dvds * bq[iv][2];
+        pvtx = pctr + AF(3, ie) * (pvtx - pctr);
+        unknvq[iv][1] = uv;
+        unknvq[iv][2] = vv;
+        sig[iv] = -pvtx + 0.0;
+        int ip = QN(ie, iv);
+        double acnx = X_(vlave, 0, ip) - uv, acny = X_(vlave, 1, ip) - vv;
+        double nrm = sqrt(acnx * acnx + acny * acny);
+        if (nrm < TINY_S) { aujmp[iv][0] = TINY_S; aujmp[iv][1] = TINY_S; }
+        else { aujmp[iv][0] = acnx / nrm; aujmp[iv][1] = acny / nrm; }
+        aujmp[iv][2] = nrm;
+      }
+      double sdctr = sqrt(fmax(epsd, g * pctr / rhoct));
+      for (int iv = 0; iv < 4; iv++) aujmp[iv][2] = aujmp[iv][2] / sdctr;
+      double murie[4][2];
+      for (int iv = 0; iv < 4; iv++) {
+        int ip = QN(ie, iv);
+        double dux = X_(vlave, 0, ip) - unknvq[iv][1], duy = X_(vlave, 1, ip) - unknvq[iv][2];
+        for (int f = 0; f < 2; f++) {
+          double deltu = fabs(dux * vn[iv][f][0] + duy * vn[iv][f][1]);
+          murie[iv][f] = rhoct * sdctr + c->cimpd * rhoct * slpdu * deltu;
+        }
+      }
+      for (int iv = 0; iv < 4; iv++) {
+        int ip = QN(ie, iv);
+        for (int f = 0; f < 2; f++) {
+          /* getriecoef_matrixnew, Limiterlag.f90:1037-1076 */
+          double area = vn[iv][f][2], n1 = vn[iv][f][0], n2 = vn[iv][f][1];
+          double vnau = (aujmp[iv][2] < 1.0e12) ? 1.0 : n1 * aujmp[iv][0] + n2 * aujmp[iv][1];
+          double mc11 = murie[iv][f] * area * fabs(vnau), mc21 = 0.0, mc12 = 0.0, mc22 = murie[iv][f] * area * fabs(vnau);
+          double mu1 = mc11 * unknvq[iv][1] + mc21 * unknvq[iv][2];
+          double mu2 = mc21 * unknvq[iv][1] + mc22 * unknvq[iv][2];
+          double s1 = sig[iv] * area * n1 + (0.0 + 0.0) * area * n2;
+          double s2 = (0.0 + 0.0) * area * n1 + sig[iv] * area * n2;
+          munacn[0 + 4 * ip] = munacn[0 + 4 * ip] + mc11;
+          munacn[1 + 4 * ip] = munacn[1 + 4 * ip] + mc21;
+          munacn[2 + 4 * ip] = munacn[2 + 4 * ip] + mc12;
+          munacn[3 + 4 * ip] = munacn[3 + 4 * ip] + mc22;
+          munacu[0 + 2 * ip] = munacu[0 + 2 * ip] + mu1;
+          munacu[1 + 2 * ip] = munacu[1 + 2 * ip] + mu2;
+          snsigm[0 + 2 * ip] = snsigm[0 + 2 * ip] + s1;
+          snsigm[1 + 2 * ip] = snsigm[1 + 2 * ip] + s2;
+          const size_t o = (size_t)f + 2 * (iv + 4 * (size_t)ie);
+          mcl[4 * o + 0] = mc11; mcl[4 * o + 1] = mc21; mcl[4 * o + 2] = mc12; mcl[4 * o + 3] = mc22;
+          mul[2 * o + 0] = mu1; mul[2 * o + 1] = mu2;
+          snl[2 * o + 0] = s1; snl[2 * o + 1] = s2;
+        }
       }
     }
-    for (int iv = 0; iv < 4; iv++) {
-      int ip = QN(ie, iv);
-      for (int f = 0; f < 2; f++) {
-        /* getriecoef_matrixnew, Limiterlag.f90:1037-1076 */
-        double area = vn[iv][f][2], n1 = vn[iv][f][0], n2 = vn[iv][f][1];
-        double vnau = (aujmp[iv][2] < 1.0e12) ? 1.0 : n1 * aujmp[iv][0] + n2 * aujmp[iv][1];
-        double mc11 = murie[iv][f] * area * fabs(vnau), mc21 = 0.0, mc12 = 0.0, mc22 = murie[iv][f] * area * fabs(vnau);
-        double mu1 = mc11 * unknvq[iv][1] + mc21 * unknvq[iv][2];
-        double mu2 = mc21 * unknvq[iv][1] + mc22 * unknvq[iv][2];
-        double s1 = sig[iv] * area * n1 + (0.0 + 0.0) * area * n2;
-        double s2 = (0.0 + 0.0) * area * n1 + sig[iv] * area * n2;
-        munacn[0 + 4 * ip] = munacn[0 + 4 * ip] + mc11;
-        munacn[1 + 4 * ip] = munacn[1 + 4 * ip] + mc21;
-        munacn[2 + 4 * ip] = munacn[2 + 4 * ip] + mc12;
-        munacn[3 + 4 * ip] = munacn[3 + 4 * ip] + mc22;
-        munacu[0 + 2 * ip] = munacu[0 + 2 * ip] + mu1;
-        munacu[1 + 2 * ip] = munacu[1 + 2 * ip] + mu2;
-        snsigm[0 + 2 * ip] = snsigm[0 + 2 * ip] + s1;
-        snsigm[1 + 2 * ip] = snsigm[1 + 2 * ip] + s2;
-        const size_t o = (size_t)f + 2 * (iv + 4 * (size_t)ie);
-        mcl[4 * o + 0] = mc11; mcl[4 * o + 1] = mc21; mcl[4 * o + 2] = mc12; mcl[4 * o + 3] = mc22;
-        mul[2 * o + 0] = mu1; mul[2 * o + 1] = mu2;
-        snl[2 * o + 0] = s1; snl[2 * o + 1] = s2;
+    for (int ip = 0; ip < npoin; ip++) {
+      if (indnd[ip]) continue;
+      const double *mn = munacn + 4 * ip;  /* (1,1), (2,1), (1,2), (2,2) */
+      double detma = mn[0] * mn[3] - mn[1] * mn[2];
+      double i11 = mn[3] / detma, i12 = -mn[2] / detma, i21 = -mn[1] / detma, i22 = mn[0] / detma;
+      double r1 = munacu[2 * ip] - snsigm[2 * ip], r2 = munacu[2 * ip + 1] - snsigm[2 * ip + 1];
+      X_(ustar, 0, ip) = i11 * r1 + i12 * r2;
+      X_(ustar, 1, ip) = i21 * r1 + i22 * r2;
+    }
+    for (int ifa = 0; ifa < m->nbfac; ifa++) {
+      const int *bf = m->bface + 5 * ifa;
+      for (int k = 0; k < 2; k++) {
+        int ip = bf[k] - 1;
+        if (bf[2] == 22) {
+          if (bf[3] == 221) X_(ustar, 1, ip) = 0.0;
+          else if (bf[3] == 222) X_(ustar, 0, ip) = 0.0;
+        } else if (bf[2] == 25) {
+          X_(ustar, 0, ip) = 0.0;
+          X_(ustar, 1, ip) = 0.0;
+        }
       }
     }
-  }
-  for (int ip = 0; ip < npoin; ip++) {
-    if (indnd[ip]) continue;
-    const double *mn = munacn + 4 * ip;  /* (1,1), (2,1), (1,2), (2,2) */
-    double detma = mn[0] * mn[3] - mn[1] * mn[2];
-    double i11 = mn[3] / detma, i12 = -mn[2] / detma, i21 = -mn[1] / detma, i22 = mn[0] / detma;
-    double r1 = munacu[2 * ip] - snsigm[2 * ip], r2 = munacu[2 * ip + 1] - snsigm[2 * ip + 1];
-    X_(ustar, 0, ip) = i11 * r1 + i12 * r2;
-    X_(ustar, 1, ip) = i21 * r1 + i22 * r2;
-  }
-  for (int ifa = 0; ifa < m->nbfac; ifa++) {
-    const int *bf = m->bface + 5 * ifa;
-    for (int k = 0; k < 2; k++) {
-      int ip = bf[k] - 1;
-      if (bf[2] == 22) {
-        if (bf[3] == 221) X_(ustar, 1, ip) = 0.0;
-        else if (bf[3] == 222) X_(ustar, 0, ip) = 0.0;
-      } else if (bf[2] == 25) {
-        X_(ustar, 0, ip) = 0.0;
-        X_(ustar, 1, ip) = 0.0;
+    for (int ie = 0; ie < nquad; ie++)
+      for (int iv = 0; iv < 4; iv++) {
+        int ip = QN(ie, iv);
+        for (int f = 0; f < 2; f++) {
+          const size_t o = (size_t)f + 2 * (iv + 4 * (size_t)ie);
+          fst[2 * o + 0] = snl[2 * o + 0] + mcl[4 * o + 0] * X_(ustar, 0, ip) + mcl[4 * o + 1] * X_(ustar, 1, ip) - mul[2 * o + 0];
+          fst[2 * o + 1] = snl[2 * o + 1] + mcl[4 * o + 2] * X_(ustar, 0, ip) + mcl[4 * o + 3] * X_(ustar, 1, ip) - mul[2 * o + 1];
+        }
       }
-    }
-  }
-  for (int ie = 0; ie < nquad; ie++)
-    for (int iv = 0; iv < 4; iv++) {
-      int ip = QN(ie, iv);
-      for (int f = 0; f < 2; f++) {
-        const size_t o = (size_t)f + 2 * (iv + 4 * (size_t)ie);
-        fst[2 * o + 0] = snl[2 * o + 0] + mcl[4 * o + 0] * X_(ustar, 0, ip) + mcl[4 * o + 1] * X_(ustar, 1, ip) - mul[2 * o + 0];
-        fst[2 * o + 1] = snl[2 * o + 1] + mcl[4 * o + 2] * X_(ustar, 0, ip) + mcl[4 * o + 3] * X_(ustar, 1, ip) - mul[2 * o + 1];
-      }
-    }
 
-  /* I.1.4 rhsifacedg_lag_mc_hybridquad2, Getrhslagmc.f90:14468-14618 */
-  const double c16 = 0.1666666666666666, c13 = 0.3333333333333333;
-  for (int ie = 0; ie < nquad; ie++) {
-    const int ielem = ie + m->ntria;
-    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
-    double bq[4][3];
-    for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
-    double ul[3] = {0, 0, 0}, p1[3] = {0, 0, 0}, p2[3] = {0, 0, 0}, el[3] = {0, 0, 0};
-    for (int iv = 0; iv < 4; iv++) {
-      int ip = QN(ie, iv);
-      int fa = (iv + 3) % 4, fb = iv;
-      double us = X_(ustar, 0, ip), vs = X_(ustar, 1, ip);
-      const size_t o0 = 2 * (iv + 4 * (size_t)ie), o1 = o0 + 1;
-      for (int k = 0; k < c->ndegr; k++) {
-        double b3 = 2.0 * bq[iv][k] + bq[iv][k];
-        double l1x = c16 * b3 * GL(fa, ie)[0] * GL(fa, ie)[2], l1y = c16 * b3 * GL(fa, ie)[1] * GL(fa, ie)[2];
-        double l2x = c16 * b3 * GL(fb, ie)[0] * GL(fb, ie)[2], l2y = c16 * b3 * GL(fb, ie)[1] * GL(fb, ie)[2];
-        ul[k] = ul[k] + us * l1x + vs * l1y + us * l2x + vs * l2y;
-        p1[k] = p1[k] + fst[2 * o0] * c13 * b3 + fst[2 * o1] * c13 * b3;
-        p2[k] = p2[k] + fst[2 * o0 + 1] * c13 * b3 + fst[2 * o1 + 1] * c13 * b3;
-        el[k] = el[k] + us * fst[2 * o0] * c13 * b3 + vs * fst[2 * o0 + 1] * c13 * b3 +
-                us * fst[2 * o1] * c13 * b3 + vs * fst[2 * o1 + 1] * c13 * b3;
+    /* I.1.4 rhsifacedg_lag_mc_hybridquad2, Getrhslagmc.f90:14468-14618 */
+    const double c16 = 0.1666666666666666, c13 = 0.3333333333333333;
+    for (int ie = 0; ie < nquad; ie++) {
+      const int ielem = ie + m->ntria;
+      double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+      double bq[4][3];
+      for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
+      double ul[3] = {0, 0, 0}, p1[3] = {0, 0, 0}, p2[3] = {0, 0, 0}, el[3] = {0, 0, 0};
+      for (int iv = 0; iv < 4; iv++) {
+        int ip = QN(ie, iv);
+        int fa = (iv + 3) % 4, fb = iv;
+        double us = X_(ustar, 0, ip), vs = X_(ustar, 1, ip);
+        const size_t o0 = 2 * (iv + 4 * (size_t)ie), o1 = o0 + 1;
+        for (int k = 0; k < c->ndegr; k++) {
+          double b3 = 2.0 * bq[iv][k] + bq[iv][k];
+          double l1x = c16 * b3 * GL(fa, ie)[0] * GL(fa, ie)[2], l1y = c16 * b3 * GL(fa, ie)[1] * GL(fa, ie)[2];
+          double l2x = c16 * b3 * GL(fb, ie)[0] * GL(fb, ie)[2], l2y = c16 * b3 * GL(fb, ie)[1] * GL(fb, ie)[2];
+          ul[k] = ul[k] + us * l1x + vs * l1y + us * l2x + vs * l2y;
+          p1[k] = p1[k] + fst[2 * o0] * c13 * b3 + fst[2 * o1] * c13 * b3;
+          p2[k] = p2[k] + fst[2 * o0 + 1] * c13 * b3 + fst[2 * o1 + 1] * c13 * b3;
+          el[k] = el[k] + us * fst[2 * o0] * c13 * b3 + vs * fst[2 * o0 + 1] * c13 * b3 +
+                  us * fst[2 * o1] * c13 * b3 + vs * fst[2 * o1 + 1] * c13 * b3;
+        }
       }
-    }
-    for (int k = 0; k < c->ndegr; k++) {
-      U_(rhsel, c, k, 0, ielem) = ul[k];
-      U_(rhsel, c, k, 1, ielem) = p1[k];
-      U_(rhsel, c, k, 2, ielem) = p2[k];
-      U_(rhsel, c, k, 3, ielem) = el[k];
+      for (int k = 0; k < c->ndegr; k++) {
+        U_(rhsel, c, k, 0, ielem) = ul[k];
+        U_(rhsel, c, k, 1, ielem) = p1[k];
+        U_(rhsel, c, k, 2, ielem) = p2[k];
+        U_(rhsel, c, k, 3, ielem) = el[k];
+      }
     }
   }
 
@@ -2959,7 +3252,15 @@ void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
       double dxdr, dxds, dydr, dyds;
       jac4((const double(*)[2])xpq, r, s, &dxdr, &dxds, &dydr, &dyds);
       double djaco = wi;
-      double rcoef = 1.0;  /* 1 - alfrz + alfrz*ygaus with alfrz = 0 */
+      /* rcoef = 1 - alfrz + alfrz*ygaus (Limiterlag.f90:1268-1279) */
+      double rcoef = 1.0;
+      if (c->nrz == 1) {
+        const double rp = 1.0 + r, rm = 1.0 - r, sp = 1.0 + s, sm = 1.0 - s;
+        const double shpq[4] = {0.25 * rm * sm, 0.25 * rp * sm, 0.25 * rp * sp, 0.25 * rm * sp};
+        double ygaus = 0.0;
+        for (int k = 0; k < 4; k++) ygaus = ygaus + shpq[k] * xpq[k][1];
+        rcoef = 1.0 - 1.0 + 1.0 * ygaus;
+      }
       double gd[2][3];
       for (int k = 0; k < 3; k++) {
         gd[0][k] = dyds * dbdr[k] + (-dydr) * dbds[k];
@@ -2996,6 +3297,42 @@ void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
         U_(rhsel, c, k, 1, ielem) = U_(rhsel, c, k, 1, ielem) - f2 * djaco * rcoef;
         U_(rhsel, c, k, 2, ielem) = U_(rhsel, c, k, 2, ielem) - f3 * djaco * rcoef;
         U_(rhsel, c, k, 3, ielem) = U_(rhsel, c, k, 3, ielem) - f4 * djaco * rcoef;
+      }
+    }
+  }
+
+  /* I.1.6 rhsdomnsrcdg_lagmc_quadrz (Getrhslagmc.f90:15800-16048): the
+   * RZ hoop-stress source of the radial (y) momentum, 5x5 Gauss, the
+   * limited pressure of the point, no radius weight */
+  if (c->nrz == 1) {
+    for (int ie = 0; ie < nquad; ie++) {
+      const int ielem = ie + m->ntria;
+      double xpq[4][2];
+      for (int k = 0; k < 4; k++) { xpq[k][0] = X_(coord, 0, QN(ie, k)); xpq[k][1] = X_(coord, 1, QN(ie, k)); }
+      double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+      for (int ig = 0; ig < 25; ig++) {
+        double r = pos25[ig][0], s = pos25[ig][1], wi = w25[ig];
+        double dxdr, dxds, dydr, dyds;
+        jac4((const double(*)[2])xpq, r, s, &dxdr, &dxds, &dydr, &dyds);
+        double djaco = wi * (dxdr * dyds - dydr * dxds);
+        double b[3] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+        double un[4];
+        for (int q = 0; q < 4; q++) {
+          double a = 0.0;
+          for (int k = 0; k < c->mdegr; k++) a = a + U_(unkno, c, k, q, ielem) * b[k];
+          un[q] = a;
+        }
+        double rhoad = 1.0 / un[0];
+        double pres = (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]));
+        double rhomc = U_(unkno, c, 0, 0, ielem);
+        double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+        double rhoct = 1.0 / rhomc;
+        double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+        pres = pctr + AF(3, ie) * (pres - pctr);
+        for (int k = 0; k < c->ndegr; k++) {
+          double f3 = 1.0 * (-pres) * b[k];
+          U_(rhsel, c, k, 2, ielem) = U_(rhsel, c, k, 2, ielem) - f3 * djaco;
+        }
       }
     }
   }

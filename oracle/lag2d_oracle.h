@@ -52,6 +52,7 @@ typedef struct {
   double gamlg, cfl, cdrho, cimpd, tend;
   double sedov_energy;         /* 0.244816 in the reference */
   const double *rho0;          /* (ncell) initial-density factor per cell, or NULL (1) */
+  int nrz;                     /* 0: Cartesian; 1: RZ, y the radius (P1 path only) */
 } o_cfg;
 
 /* Initial geometry, mass matrix and DOFs: getgeoel_initial_lag,

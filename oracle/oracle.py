@@ -34,7 +34,8 @@ class _OCfg(ctypes.Structure):
                 ("sedov_ncell", ctypes.c_int), ("sedov_cell", ctypes.c_int * 4),
                 ("gamlg", ctypes.c_double), ("cfl", ctypes.c_double), ("cdrho", ctypes.c_double),
                 ("cimpd", ctypes.c_double), ("tend", ctypes.c_double),
-                ("sedov_energy", ctypes.c_double), ("rho0", ctypes.POINTER(ctypes.c_double))]
+                ("sedov_energy", ctypes.c_double), ("rho0", ctypes.POINTER(ctypes.c_double)),
+                ("nrz", ctypes.c_int)]
 
 
 def build() -> str:
@@ -74,7 +75,7 @@ class Oracle:
         self.oc = _OCfg(cfg.npoly, cfg.ndegr, cfg.mdegr, cfg.nq, cfg.nstag, cfg.ndt, cfg.ncase,
                         cfg.nlimi, 1, cfg.ngausd, cfg.ngausd_geo, len(cfg.sedov_cells), sc,
                         cfg.gamlg, cfg.cfl, cfg.cdrho, cfg.cimpd, cfg.tend, cfg.sedov_energy,
-                        _p(self._rho0, _dp))
+                        _p(self._rho0, _dp), int(getattr(cfg, "nrz", 0)))
 
     # arrays are returned in C order with the Fortran memory layout:
     #   unkno (nsize, nq, ndegr), geoel (nsize, 24), amatr (ncell, nmatr), coord (npoin, 2)

@@ -62,6 +62,27 @@ def test_create_validates_arguments_without_device():
     del s
 
 
+def test_rz_configurations_rejected_without_device():
+    """RZ is built on the linear P1 path: P2 with nrz = 1, the area-weighted
+    nrz = 2 and the RZ Sedov case (a hard-coded dt schedule) return
+    LAG2D_EUNSUP before any device work."""
+    import dataclasses
+    lib = api.load()
+    for name, change in (("tgv16", {"nrz": 1}), ("noh_rz8", {"nrz": 2}), ("noh_rz8", {"ncase": 7})):
+        m, c = workload(name)
+        c = dataclasses.replace(c, **change)
+        k = [np.ascontiguousarray(a, dtype=np.int32) for a in (m.iptri, m.ipqua, m.bface, m.esuv1, m.esuv2, m.esqua)]
+        coold = np.ascontiguousarray(m.coord)
+        mm = api._Mesh(m.ntria, m.nquad, m.npoin, m.nbfac, *[api._p(a, api._ip) for a in k],
+                       api._p(coold, api._dp))
+        cc = api._Cfg(c.npoly, c.ndegr, c.mdegr, c.nq, c.nstag, c.ndt, c.ncase, c.nlimi, c.ndens, c.ngausd,
+                      c.ngausd_geo, 0, 0, 0, (ctypes.c_int * 4)(), c.gamlg, c.cfl, c.cdrho, c.cimpd, c.tend,
+                      c.sedov_energy, c.nrz)
+        h = ctypes.c_void_p()
+        assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 3, name
+        assert b"RZ" in lib.lag2d_last_error() or b"nrz" in lib.lag2d_last_error()
+
+
 def test_missing_library_fails_loudly(tmp_path, monkeypatch):
     monkeypatch.setattr(api, "_LIBDIR", str(tmp_path))
     monkeypatch.setattr(api, "_libs", {})

@@ -1,0 +1,129 @@
+"""The RZ branch (nrz = 1) of the linear P1 path on the device, through the
+C-ABI, against the CPU restatement (getndvelo_lagmc_rz with getriem_quadrz
+and getbc_lagmaire2, rhsifacedg_lagmc_quadrz, the radius-weighted volume
+integral and rhsdomnsrcdg_lagmc_quadrz; radius-weighted geometry and mass
+matrices).  The RZ kernels keep the reference's summation order, so the
+no-FMA build reproduces the restatement bit for bit; the FMA build stays
+within 1e-12 of the field scale per step.  A whole run of the spherical Noh
+implosion to t = 0.6 follows the restatement's and its exact solution."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from lag2d_b200 import workload
+from lag2d_b200.api import Lag2DError, Lag2DSolver
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _scales(u):
+    sc = [max(np.abs(u[:, q]).max(), 1e-300) for q in range(u.shape[1])]
+    sc[1] = sc[2] = max(sc[1], sc[2])
+    return np.array(sc)
+
+
+@pytest.mark.parametrize("name", ["noh_rz8", "noh_rz_jitter16"])
+@pytest.mark.parametrize("exact", [True, False])
+def test_rz_init_fields(name, exact):
+    m, c = workload(name)
+    geoel, amatr, unkno = Oracle(m, c).init()
+    s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
+    g2, a2, u2 = s.init_fields()
+    n = m.ncell
+    if exact:
+        for k in range(4):
+            assert np.array_equal(g2[:n, k], geoel[:n, k]), k
+        assert np.array_equal(a2, amatr)
+        assert np.array_equal(u2[:n], unkno[:n])
+    else:
+        for k in range(4):
+            scale = max(np.abs(geoel[:n, k]).max(), 1.0 if k < 2 else 0.0)
+            assert np.abs(g2[:n, k] - geoel[:n, k]).max() <= 1e-12 * scale, k
+        assert np.abs(a2 - amatr).max() <= 1e-11 * np.abs(amatr).max()
+        sc = _scales(unkno[:n, :, 0])
+        assert np.all(np.abs(u2[:n, :, 0] - unkno[:n, :, 0]).max(axis=0) <= 1e-12 * sc)
+    s.close()
+
+
+@pytest.mark.parametrize("name,nsteps", [("noh_rz8", 12), ("noh_rz_jitter16", 8)])
+@pytest.mark.parametrize("exact", [True, False])
+def test_rz_steps(name, nsteps, exact):
+    """Whole RK2 steps one at a time against the restatement: cell DOFs,
+    node coordinates and nodal velocities, and the CFL time step."""
+    m, c = workload(name)
+    o = Oracle(m, c)
+    g, a, u = o.init()
+    x = m.coord.copy()
+    us = np.zeros_like(x)
+    s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
+    s.init_fields()
+    n = m.ncell
+    dt, ta = c.dtfix, 0.0
+    Oracle.status()  # reads and clears what earlier calls left
+    for it in range(1, nsteps + 1):
+        _, dt, ta = o.run(u, x, m.coord, g, a, us, it, 1, dt, ta)
+        assert Oracle.status() == 0
+        s.step()
+        u2, x2, us2, _ = s.get_state()
+        if exact:
+            assert np.array_equal(u2[:n], u[:n]), it
+            assert np.array_equal(x2, x) and np.array_equal(us2, us), it
+            assert s.dtfix == dt and s.tacru == ta
+            continue
+        sc = _scales(u[:n, :, 0])
+        err = np.abs(u2[:n, :, 0] - u[:n, :, 0]).max(axis=0) / sc
+        assert err.max() <= 1e-12, (it, err)
+        assert np.abs(x2 - x).max() <= 1e-13, it
+        assert abs(s.dtfix - dt) <= 1e-12 * dt
+    s.close()
+
+
+def test_rz_noh_run_to_end_time():
+    """The spherical Noh implosion on 32 x 32 quads to t = 0.6 through
+    lag2d_run (graph-replayed steps) against the restatement's run: the same
+    number of steps, the same end time, and densities that agree where the
+    flow is smooth; post-shock density near 64, the pre-shock (1 + t/r)^2."""
+    m, c = workload("noh_rz32")
+    o = Oracle(m, c)
+    g, a, u = o.init()
+    x = m.coord.copy()
+    us = np.zeros_like(x)
+    it, dt, ta = 1, c.dtfix, 0.0
+    while ta < c.tend * (1.0 - 1e-12):
+        done, dt, ta = o.run(u, x, m.coord, g, a, us, it, 100, dt, ta)
+        it += done
+        if done < 100:
+            break
+    s = Lag2DSolver(m, c)
+    s.init_fields()
+    steps = 0
+    while s.tacru < c.tend * (1.0 - 1e-12) and steps < 5 * it:
+        steps += s.run(100)
+    assert steps == it - 1 and abs(s.tacru - ta) <= 1e-12
+    u2, x2, _, _ = s.get_state()
+    n = m.ncell
+    rho, rho2 = 1.0 / u[:n, 0, 0], 1.0 / u2[:n, 0, 0]
+    # 383 limited steps in the FMA build: 8.5e-12 measured (bit for bit in
+    # the no-FMA build with order_exact)
+    assert np.abs(rho2 / rho - 1.0).max() <= 1e-9
+    ctr = np.array([x2[m.ipqua[i] - 1].mean(axis=0) for i in range(n)])
+    r = np.hypot(ctr[:, 0], ctr[:, 1])
+    assert 50.0 < rho2[(r > 0.1) & (r < 0.15)].mean() < 68.0
+    ahead = (r > 0.4) & (r < 0.7) & (ctr.max(axis=1) < 0.75)
+    assert np.abs(rho2[ahead] / (1.0 + s.tacru / r[ahead]) ** 2 - 1.0).mean() < 0.05
+    s.close()
+
+
+def test_rz_cell_output_and_profile():
+    m, c = workload("noh_rz8")
+    s = Lag2DSolver(m, c)
+    s.init_fields()
+    s.run(5)
+    out, bad = s.cell_output()
+    u, x, _, _ = s.get_state()
+    n = m.ncell
+    assert np.allclose(out[:, 1], 1.0 / u[:n, 0, 0], rtol=1e-15)
+    assert np.all(bad == 0.0)
+    s.close()
