@@ -309,8 +309,9 @@ def p1_block(args, timed, families):
     peak, peak_kind = peaks()
     names = ("bounds", "cell", "node", "rhs", "dt", "update", "nodes", "geom", "copy")
     out = {"path": "ncurv=0, nfint=1, nlimi=6 (linear P1, straight quads); parity: bit for bit with the "
-                   "oracle in the no-FMA build (tests/test_gpu_p1.py)"}
-    for name in ("sod200", "sod1024"):
+                   "oracle in the no-FMA build (tests/test_gpu_p1.py, tests/test_gpu_rz.py)",
+           "noh_rz100_note": "Noh implosion in RZ (nrz=1, y the radius): the spherical implosion on 100x100 quads"}
+    for name in ("sod200", "sod1024", "noh_rz100"):
         m, c = workload(name)
         s = new_solver(m, c, None)
         ms, done, launches = timed(s)
