@@ -56,14 +56,14 @@ def _tgv(n: int) -> Tuple[Mesh, StepConfig]:
     return m, c
 
 
-def _sedov(n: int) -> Tuple[Mesh, StepConfig]:
+def _sedov(n: int, cfl: float = 0.1) -> Tuple[Mesh, StepConfig]:
     """Full-box Sedov as the reference's active setup runs it
     (Getrhslagmc.f90:5634: E = 0.244816 in each of the 4 central cells);
     ``n`` x ``n`` cells on [-1.2, 1.2]^2."""
     m = quad_mesh(n, n, -1.2, 1.2, -1.2, 1.2)
     h = n // 2
     cells = ((h - 1) * n + h, (h - 1) * n + h + 1, h * n + h, h * n + h + 1)
-    c = StepConfig(ncase=7, gamlg=1.4, nstag=3, cfl=0.1, tend=1.0, sedov_cells=cells)
+    c = StepConfig(ncase=7, gamlg=1.4, nstag=3, cfl=cfl, tend=1.0, sedov_cells=cells)
     return m, c
 
 
@@ -158,6 +158,12 @@ WORKLOADS = {
     "tgv64": lambda: _tgv(64),
     "tgv16": lambda: _tgv(16),
     # Sedov blast: [0,1.2]^2, gamma 1.4, energy in the corner cell
+    "sedov256": lambda: _sedov(256),
+    # at CFL 0.3 (the value of the reference's Sod configuration) the 32^2,
+    # 64^2 and 128^2 blasts reach t = 1; at 0.1 they break down first
+    "sedov32_cfl03": lambda: _sedov(32, 0.3),
+    "sedov64_cfl03": lambda: _sedov(64, 0.3),
+    "sedov128_cfl03": lambda: _sedov(128, 0.3),
     "sedov128": lambda: _sedov(128),
     "sedov64": lambda: _sedov(64),
     "sedov32": lambda: _sedov(32),

@@ -1308,6 +1308,20 @@ __global__ void k_weno_gather(Dev d, double *lamU, double *lamUn, int fold, cons
   if (e >= d.ncell) return;
   const int nw = *d.wcount;
   if (nw == 0 && !fold) return;
+  const int jq = e - d.ntria;
+  if (!fold) {
+    // a cell that is neither replaced nor in a replaced quad's stencil keeps
+    // its adjoint: leave it untouched (most cells, when few quads are troubled)
+    bool touched = false;
+    if (jq >= 0) {
+      touched = d.flag[e] == 2 && d.stencil[jq] >= 0;
+      for (int i = inv_ptr[jq]; i < inv_ptr[jq + 1] && !touched; i++) {
+        const int c = inv_ent[i] / 9;
+        touched = d.flag[c + d.ntria] == 2 && d.stencil[c] >= 0 && wslot[c] >= 0 && wslot[c] < cap;
+      }
+    }
+    if (!touched) return;
+  }
   const size_t nc = d.ncell;
   double l[24];
   for (int v = 0; v < 24; v++) l[v] = lamU[v * nc + e];

@@ -43,3 +43,68 @@ def test_sedov32_to_end_time(exact):
     ctr = x[m.ipqua[:, :4] - 1].mean(axis=1)
     r = np.hypot(ctr[:, 0], ctr[:, 1])
     assert 0.95 < r[int(np.argmax(rho))] < 1.02
+
+
+_SEDOV32_CFL03 = {}
+
+
+def _oracle_sedov32_cfl03():
+    """The CPU restatement's run of sedov32_cfl03 to t = 1 (about 20 s; once)."""
+    if not _SEDOV32_CFL03:
+        from oracle.oracle import Oracle
+        m, c = workload("sedov32_cfl03")
+        o = Oracle(m, c)
+        g, a, u = o.init()
+        x = m.coord.copy()
+        us = np.zeros_like(x)
+        it, dt, ta = 1, c.dtfix, 0.0
+        while ta < c.tend * (1.0 - 1e-12):
+            done, dt, ta = o.run(u, x, m.coord, g, a, us, it, 100, dt, ta)
+            it += done
+            if done < 100:
+                break
+        _SEDOV32_CFL03.update(u=u, x=x, it=it)
+    r = _SEDOV32_CFL03
+    return r["u"], r["x"], r["it"]
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_sedov32_cfl03_to_end_time(exact):
+    """The same blast at CFL 0.3 (219 steps) against a live run of the CPU
+    restatement: bit for bit in the no-FMA build, within 1e-10 with FMA."""
+    m, c = workload("sedov32_cfl03")
+    u, x, it = _oracle_sedov32_cfl03()
+    s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
+    s.init_fields()
+    done = s.run(1000)
+    u2, x2, _, _ = s.get_state()
+    n = m.ncell
+    assert done == it - 1 and abs(s.tacru - 1.0) < 1e-12
+    if exact:
+        assert np.array_equal(u2[:n], u[:n]) and np.array_equal(x2, x)
+    else:
+        scale = np.abs(u[:n, :, 0]).max(axis=0)
+        assert (np.abs(u2[:n, :, 0] - u[:n, :, 0]).max(axis=0) / scale).max() < 1e-10
+    s.close()
+
+
+def test_sedov128_cfl03_reaches_end_time():
+    """BASELINE's Sedov configuration (128 x 128 P2 quads, WENO, RK3) to
+    t_end = 1 at CFL 0.3: 879 steps, total energy conserved to round-off,
+    cell masses fixed, the density peak at the similarity solution's shock
+    radius r = 1.0 (the CFL 0.1 run breaks down near t = 0.19)."""
+    m, c = workload("sedov128_cfl03")
+    s = Lag2DSolver(m, c)
+    g0, _, u0 = s.init_fields()
+    n = m.ncell
+    e0 = float((g0[:n, 3] * u0[:n, 3, 0]).sum())
+    done = 0
+    while s.tacru < 1.0 - 1e-12 and done < 5000:
+        done += s.run(500)
+    u, x, _, g = s.get_state()
+    assert abs(s.tacru - 1.0) < 1e-12 and 800 < done < 1000
+    assert np.array_equal(g[:n, 3], g0[:n, 3])
+    assert abs(float((g[:n, 3] * u[:n, 3, 0]).sum()) - e0) <= 1e-12 * e0
+    out, _ = s.cell_output(badcell=False)
+    assert 0.97 < out[int(np.argmax(out[:, 1])), 0] < 1.03
+    s.close()
