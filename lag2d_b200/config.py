@@ -107,6 +107,21 @@ def _sod(nx: int, ny: int, y1: float, jitter: float = 0.0) -> Tuple[Mesh, StepCo
     return m, c
 
 
+def _noh_square(n: int, cfl: float = 0.3) -> Tuple[Mesh, StepConfig]:
+    """Cartesian Noh implosion (ncase 3, gamma 5/3, SSP-RK2) on n x n curved
+    P2 quads of [0,1]^2 without triangles: slip walls on x = 0 (222) and
+    y = 0 (221), free outer sides (code 22, sub-code 0).  The exact solution
+    has the shock at r = t/3 with density 16 behind it, (1 + t/r) ahead."""
+    m = quad_mesh(n, n, 0.0, 1.0, 0.0, 1.0)
+    bf = m.bface.copy()
+    for i in range(bf.shape[0]):
+        if n <= i < 3 * n:          # x = 1 and y = 1: free
+            bf[i, 3] = 0
+    m = Mesh(coord=m.coord, ipqua=m.ipqua, iptri=m.iptri, bface=bf)
+    c = StepConfig(ncase=3, gamlg=5.0 / 3.0, nstag=2, cfl=cfl, tend=0.6)
+    return m, c
+
+
 def _noh_rz(n: int, cfl: float = 0.3, jitter: float = 0.0) -> Tuple[Mesh, StepConfig]:
     """Noh implosion in RZ (nrz = 1: y is the radius, x the axial
     coordinate; true-volume weights), i.e. the spherical implosion, on the
@@ -185,6 +200,9 @@ WORKLOADS = {
     "sod40": lambda: _sod(40, 4, 0.1),
     "sod_jitter40": lambda: _sod(40, 8, 0.2, jitter=0.15),
     "sod1024": lambda: _sod(1024, 512, 0.5),
+    "noh_square32": lambda: _noh_square(32),
+    "noh_square64": lambda: _noh_square(64),
+    "noh_square100": lambda: _noh_square(100),
     "noh_rz8": lambda: _noh_rz(8),
     "noh_rz_jitter16": lambda: _noh_rz(16, jitter=0.15),
     "noh_rz32": lambda: _noh_rz(32),
