@@ -65,8 +65,9 @@ typedef struct {
   int nsedov;           /* number of Sedov energy cells (<= 4)           */
   int sedov_cell[4];    /* their 1-based ids                             */
   double gamlg, cfl, cdrho, cimpd, tend, sedov_energy;
-  int nrz;              /* 0: Cartesian; 1: RZ (true volume, axis y = 0),
-                           built on the P1 path (npoly = 1)                */
+  int nrz;              /* 0: Cartesian; 1: RZ (true volume, axis y = 0);
+                           2: area-weighted RZ; both built on the P1 path
+                           (npoly = 1)                                     */
 } lag2d_config;
 
 /* Create a handle: validates the mesh, builds the device connectivity

@@ -39,7 +39,7 @@ class StepConfig:
     dtfix: float = 1.0e-4   # initial / fixed time step
     sedov_cells: Tuple[int, ...] = ()      # 1-based cells receiving the Sedov energy
     sedov_energy: float = 0.244816
-    nrz: int = 0            # 0: Cartesian; 1: RZ with y the radius (true volume, linear P1 cells)
+    nrz: int = 0            # 0: Cartesian; RZ with y the radius on linear P1 cells: 1 true volume, 2 area-weighted
 
     @property
     def nmatr(self) -> int:
@@ -122,14 +122,17 @@ def _noh_square(n: int, cfl: float = 0.3) -> Tuple[Mesh, StepConfig]:
     return m, c
 
 
-def _noh_rz(n: int, cfl: float = 0.3, jitter: float = 0.0) -> Tuple[Mesh, StepConfig]:
-    """Noh implosion in RZ (nrz = 1: y is the radius, x the axial
-    coordinate; true-volume weights), i.e. the spherical implosion, on the
+def _noh_rz(n: int, cfl: float = 0.3, jitter: float = 0.0, nrz: int = 1) -> Tuple[Mesh, StepConfig]:
+    """Noh implosion in RZ (y is the radius, x the axial coordinate; nrz = 1
+    the true-volume form, nrz = 2 the area-weighted form of
+    Getrhslagrz.f90), i.e. the spherical implosion, on the
     linear P1 path: n x n straight quads on [0,1]^2, rho = 1, u = -(x, y)/r,
     p = 1e-6 (getunkin ncase 3), gamma 5/3, SSP-RK2.  x = 0 is a slip wall
     (222), y = 0 the axis (221), the outer sides are pressure boundaries
-    (code 21, p = 1e-6, getbc_lagmaire2).  Node 1 is the origin, which the
-    RZ node solve holds (Getrhslagmc.f90:17475).  The exact solution has the
+    (code 21, p = 1e-6, getbc_lagmaire2 / getbc_lagmaire_rzaw).  Node 1 is
+    the origin, which the nrz = 1 node solve holds (Getrhslagmc.f90:17475);
+    the area-weighted solve holds it through the two walls.  The exact
+    solution has the
     shock at r = t/3 with density ((gamma+1)/(gamma-1))^3 = 64 behind it.
     ``jitter`` moves the interior vertices (seeded), for parity checks off
     the axis-aligned geometry."""
@@ -143,7 +146,7 @@ def _noh_rz(n: int, cfl: float = 0.3, jitter: float = 0.0) -> Tuple[Mesh, StepCo
         else:                           # x = 0: slip wall
             bf[i, 2], bf[i, 3] = 22, 222
     m = Mesh(coord=m.coord, ipqua=m.ipqua, iptri=m.iptri, bface=bf, nvqua=4)
-    c = StepConfig(npoly=1, ndegr=3, mdegr=3, ncase=3, gamlg=5.0 / 3.0, nstag=2, cfl=cfl, tend=0.6, nrz=1)
+    c = StepConfig(npoly=1, ndegr=3, mdegr=3, ncase=3, gamlg=5.0 / 3.0, nstag=2, cfl=cfl, tend=0.6, nrz=nrz)
     return m, c
 
 
@@ -209,6 +212,11 @@ WORKLOADS = {
     "noh_rz50": lambda: _noh_rz(50),
     "noh_rz100": lambda: _noh_rz(100),
     "noh_rz1024": lambda: _noh_rz(1024),
+    "noh_rzaw8": lambda: _noh_rz(8, nrz=2),
+    "noh_rzaw_jitter16": lambda: _noh_rz(16, jitter=0.15, nrz=2),
+    "noh_rzaw32": lambda: _noh_rz(32, nrz=2),
+    "noh_rzaw100": lambda: _noh_rz(100, nrz=2),
+    "noh_rzaw1024": lambda: _noh_rz(1024, nrz=2),
 }
 
 

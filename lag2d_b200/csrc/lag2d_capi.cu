@@ -446,8 +446,8 @@ static int create_p1(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **
   if (c->nsedov < 0 || c->nsedov > 4) return fail(LAG2D_EINVAL, "nsedov must be 0..4");
   if (c->ncase != 3 && c->ncase != 6 && c->ncase != 7)
     return fail(LAG2D_EUNSUP, "the P1 path is built for the cases 3, 6 and 7");
-  if (c->nrz != 0 && c->nrz != 1) return fail(LAG2D_EUNSUP, "nrz = 2 (area-weighted RZ) is not built");
-  if (c->nrz == 1 && c->ncase == 7)
+  if (c->nrz < 0 || c->nrz > 2) return fail(LAG2D_EINVAL, "nrz must be 0, 1 or 2");
+  if (c->nrz != 0 && c->ncase == 7)
     return fail(LAG2D_EUNSUP, "RZ Sedov runs a hard-coded dt schedule (Getrhslag.f90:1673-1693) that is not built");
   if (m->esuv2[0] != 0) return fail(LAG2D_EINVAL, "esuv2(1) must be 0");
   for (int p = 0; p < m->npoin; p++)
@@ -496,7 +496,7 @@ int lag2d_create(const lag2d_mesh *m, const lag2d_config *c, lag2d_handle **out)
   if (m->ntria > 0 && !m->iptri) return fail(LAG2D_EINVAL, "missing iptri");
   if (c->npoly == 1) return create_p1(m, c, out);
   // the reference dispatches RZ on linear cells only (Getrhslagmc.f90:6876-6975)
-  if (c->nrz != 0) return fail(LAG2D_EUNSUP, "RZ (nrz = 1) is built for the linear P1 path only");
+  if (c->nrz != 0) return fail(LAG2D_EUNSUP, "RZ (nrz = 1, 2) is built for the linear P1 path only");
   if (m->ntria > 0 && (c->ngausd != 7 || c->ngausd_geo != 7))
     return fail(LAG2D_EUNSUP, "triangles need the 7-point rule (ngausd = ngausd_geo = 7)");
   if (c->npoly != 2 || c->ndegr != 6 || c->nq != 4 || c->ndens != 1)

@@ -97,10 +97,13 @@ struct Dev1 {
   double *rhs;                        // [12][ncell]
   double *dtpart;
   Scalars *sc_dev;
-  // RZ (nrz = 1, y the radius): alfrz = 1, and per node its boundary faces
-  // in face order (bf_ptr/bf_list) with the faces' end nodes and codes
+  // RZ (nrz = 1 true volume, 2 area-weighted; y the radius): alfrz = 1,
+  // per node its boundary faces in face order (bf_ptr/bf_list) with the
+  // faces' end nodes and codes, and (nrz = 2) the cell-averaged radius
+  // geoel(11) = volume / area
   int nrz, nbfac;
   double alfrz;
+  double *rbar;                       // [ncell] geoel(11), nrz = 2
   const int *bf_ptr, *bf_list;        // node -> boundary faces, ascending
   const int *bfn;                     // [2][nbfac] end nodes (0-based)
   const int *bfcode;                  // [nbfac] code * 1000 + sub-code
@@ -232,6 +235,7 @@ __global__ void k1_init_geo(Dev1 d) {
   shp9v(0.0, 0.0, shp);
   map9(xp, shp, xc, yc);
   double xcent = 0, ycent = 0, volel = 0, masel = 0;
+  double maselrz = 0, xcerz = 0, ycerz = 0, areel = 0;
   for (int ig = 0; ig < 36; ig++) {
     const double r = cR.g36[ig][0], s = cR.g36[ig][1], wi = cR.w36[ig];
     shp9v(r, s, shp);
@@ -246,11 +250,23 @@ __global__ void k1_init_geo(Dev1 d) {
     volel = volel + djaco * rcoef;
     xcent = xcent + rhog * r * djaco * rcoef;
     ycent = ycent + rhog * s * djaco * rcoef;
+    if (d.nrz == 2) {  // the area integrals of nrz = 2 (GetInitial.f90:1655-1666)
+      maselrz = maselrz + rhog * djaco;
+      xcerz = xcerz + rhog * r * djaco;
+      ycerz = ycerz + rhog * s * djaco;
+      areel = areel + djaco;
+    }
   }
   d.rc[iq] = xcent / masel;
   d.sc[iq] = ycent / masel;
   d.vol[iq] = volel;
   d.mass[iq] = masel;
+  if (d.nrz == 2) {  // GetInitial.f90:1682-1691
+    d.rc[iq] = xcerz / maselrz;
+    d.sc[iq] = ycerz / maselrz;
+    d.mass[iq] = maselrz;
+    d.rbar[iq] = volel / areel;
+  }
 }
 
 __global__ void k1_init_fields(Dev1 d) {
@@ -274,7 +290,9 @@ __global__ void k1_init_fields(Dev1 d) {
     map9(xp, shp, xg, yg);
     getunkin1(d, unkin, xg, yg, e + 1, volel, xcel, ycel);
     const double rcoef = 1.0 - alfrz + alfrz * yg;
-    for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
+    // nrz = 2 integrates over the area (Getrhslagmc.f90:3744-3754)
+    if (d.nrz == 2) for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco;
+    else for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
   }
   double xc, yc;
   shp9v(rc, sc, shp);
@@ -296,6 +314,13 @@ __global__ void k1_init_fields(Dev1 d) {
       for (int k = 0; k < ND; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bq[k] * djaco;
     const double rho0 = rho_initial1(d, xc, yc);
     const double rcoef = 1.0 - alfrz + alfrz * yg;
+    if (d.nrz == 2) {  // the area mass matrix (GetInitial.f90:604-610)
+      f0 = f0 + rho0 * djaco;
+      mm[0] = mm[0] + rho0 * bq[1] * bq[1] * djaco;
+      mm[2] = mm[2] + rho0 * bq[1] * bq[2] * djaco;
+      mm[3] = mm[3] + rho0 * bq[2] * bq[2] * djaco;
+      continue;
+    }
     f0 = f0 + rho0 * djaco * rcoef;
     // mmatr(1,1), (2,1), (1,2), (2,2) (GetInitial.f90:622-627); (2,1) is not used
     mm[0] = mm[0] + rho0 * bq[1] * bq[1] * djaco * rcoef;
@@ -304,10 +329,12 @@ __global__ void k1_init_fields(Dev1 d) {
   }
   const double det = mm[0] * mm[3] - mm[2] * mm[2];
   const double a1 = mm[3] / det, a2 = -mm[2] / det, a3 = mm[0] / det;
-  d.amatr[0 * (size_t)d.ncell + e] = a1;
-  d.amatr[1 * (size_t)d.ncell + e] = a2;
-  d.amatr[2 * (size_t)d.ncell + e] = a3;
-  d.amatr[3 * (size_t)d.ncell + e] = 1.0 / f0;
+  // nrz = 2 divides M^-1 by geoel(11) after the projection's copy was taken (GetInitial.f90:675)
+  const double rb = (d.nrz == 2) ? d.rbar[e] : 1.0;
+  d.amatr[0 * (size_t)d.ncell + e] = (d.nrz == 2) ? a1 / rb : a1;
+  d.amatr[1 * (size_t)d.ncell + e] = (d.nrz == 2) ? a2 / rb : a2;
+  d.amatr[2 * (size_t)d.ncell + e] = (d.nrz == 2) ? a3 / rb : a3;
+  d.amatr[3 * (size_t)d.ncell + e] = (d.nrz == 2) ? 1.0 / f0 / rb : 1.0 / f0;
   const double mi[2][2] = {{a1, a2}, {a2, a3}};
   for (int q = 0; q < 4; q++) {
     d.Un[(q * ND + 0) * (size_t)d.ncell + e] = rv[q] / masel;
@@ -329,7 +356,7 @@ __global__ void k1_geom(Dev1 d, const double *X, const double *Y) {
   double x4[4][2], xp[9][2], shp[9], dr[9], ds[9];
   load4(d, X, Y, iq, x4);
   image9(x4, xp);
-  double rcv = 0.0, scv = 0.0, volel = 0.0;
+  double rcv = 0.0, scv = 0.0, volel = 0.0, areel = 0.0, rcvrz = 0.0, scvrz = 0.0;
   for (int ig = 0; ig < 36; ig++) {
     const double r = cR.g36[ig][0], s = cR.g36[ig][1], wi = cR.w36[ig];
     shp9v(r, s, shp);
@@ -342,10 +369,20 @@ __global__ void k1_geom(Dev1 d, const double *X, const double *Y) {
     volel = volel + djaco * rcoef;
     rcv = rcv + r * djaco * rcoef;
     scv = scv + s * djaco * rcoef;
+    if (d.nrz == 2) {
+      areel = areel + djaco;
+      rcvrz = rcvrz + r * djaco;
+      scvrz = scvrz + s * djaco;
+    }
   }
   d.vol[iq] = volel;
   d.vcx[iq] = rcv / volel;
   d.vcy[iq] = scv / volel;
+  if (d.nrz == 2) {  // the area centroid and geoel(11) (Limiterlag.f90:2149-2156)
+    d.vcx[iq] = rcvrz / areel;
+    d.vcy[iq] = scvrz / areel;
+    d.rbar[iq] = volel / areel;
+  }
   if (!(volel > 0.0)) atomicOr(&d.sc_dev->status, ST_NONPHYS);
 }
 
@@ -474,8 +511,146 @@ __device__ void rz_corners(const Dev1 &d, int iq, const double (*x4)[2], const i
   }
 }
 
-template <int MD, bool FAST, bool RZ>
-__device__ void cell_pass(const Dev1 &d, int iq) {
+// Area-weighted RZ (nrz = 2), at the start of every stage but the very
+// first: the mass centre geoel(1:2) of the limited DG density over the
+// cell's area, 5 fixed-point passes from the area centroid
+// (getgeoel_lagmc_rzawrev, Getrhslagrz.f90:4790-4990), then M^-1 of the
+// area mass matrix about it divided by geoel(11) (getamatr_lagmc_rzawrev,
+// :3990-4219).  Writes rc, sc and amatr of quad iq.
+template <int MD>
+__device__ void aw_rev(const Dev1 &d, int iq, const double (*x4)[2], const double (*u)[ND], double af1, double &rc,
+                       double &sc) {
+  double xp[9][2], shp[9], dr[9], ds[9];
+  image9(x4, xp);
+  const double rhomc = u[0][0];
+  for (int iloop = 1; iloop <= 5; iloop++) {
+    double xcent = 0.0, ycent = 0.0, masel = 0.0;
+    for (int ig = 0; ig < 36; ig++) {
+      const double r = cR.g36[ig][0], s = cR.g36[ig][1], wi = cR.w36[ig];
+      shp9d(r, s, dr, ds);
+      Jac j = jac9(xp, dr, ds);
+      const double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+      const double bq[ND] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+      double rhomg = 0.0;
+#pragma unroll
+      for (int k = 0; k < MD; k++) rhomg = rhomg + u[0][k] * bq[k];
+      if (iloop == 1) rhomg = rhomc;
+      rhomg = rhomc + af1 * (rhomg - rhomc);
+      const double rhog = 1.0 / rhomg;
+      masel = masel + 1.0 / rhomc * djaco;
+      xcent = xcent + rhog * r * djaco;
+      ycent = ycent + rhog * s * djaco;
+    }
+    rc = xcent / masel;
+    sc = ycent / masel;
+  }
+  double f0 = 0.0, f1 = 0.0, f2 = 0.0, f3 = 0.0;
+  for (int ig = 0; ig < 25; ig++) {
+    const double r = cR.g25[ig][0], s = cR.g25[ig][1], wi = cR.w25[ig];
+    shp9d(r, s, dr, ds);
+    Jac j = jac9(xp, dr, ds);
+    const double djaco = wi * (j.xr * j.ys - j.yr * j.xs);
+    const double bq[ND] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+    double rhomg = 0.0;
+#pragma unroll
+    for (int k = 0; k < MD; k++) rhomg = rhomg + u[0][k] * bq[k];
+    rhomg = rhomc + af1 * (rhomg - rhomc);
+    const double rhog = 1.0 / rhomg;
+    f0 = f0 + rhog * djaco;
+    f1 = f1 + rhog * (r - rc) / 1.0 * (r - rc) / 1.0 * djaco;
+    f2 = f2 + rhog * (r - rc) / 1.0 * (s - sc) / 1.0 * djaco;
+    f3 = f3 + rhog * (s - sc) / 1.0 * (s - sc) / 1.0 * djaco;
+  }
+  (void)shp;
+  const double det = f1 * f3 - f2 * f2;
+  const double rb = d.rbar[iq];
+  const size_t nc = d.ncell;
+  d.amatr[0 * nc + iq] = f3 / det / rb;
+  d.amatr[1 * nc + iq] = -f2 / det / rb;
+  d.amatr[2 * nc + iq] = f1 / det / rb;
+  d.amatr[3 * nc + iq] = 1.0 / f0 / rb;
+  d.rc[iq] = rc;
+  d.sc[iq] = sc;
+}
+
+// Area-weighted RZ corner coefficients (getriem_quadrzaw, Getrhslagrz.f90:
+// 1389-1669): the two corner faces of the plane solver (half of each edge at
+// the vertex, no radius weight), the acoustic impedance rho c and the 1e-8
+// floors, on the vertex values of the stage's mass centre; stored per face
+// in cf[(k*8 + f + 2*iv)*nquad + iq] (k: m, m u, m v, sigma.n A).
+template <int MD>
+__device__ void aw_corners(const Dev1 &d, int iq, const double (*x4)[2], const int *ip, const double (*u)[ND],
+                           double rc, double sc, double af4, double fi11, double fi12, double fi22) {
+  const double g = d.gamlg, eps8 = 1.0e-08, slpdu = (g + 1.0) / 2.0;
+  double fn[4][3], bq[4][ND], uvq[4][4];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int b = (f + 1) & 3;
+    const double anx = x4[b][1] - x4[f][1];
+    const double any = -(x4[b][0] - x4[f][0]);
+    fn[f][0] = anx / sqrt(anx * anx + any * any);
+    fn[f][1] = any / sqrt(anx * anx + any * any);
+    fn[f][2] = sqrt(anx * anx + any * any);
+    bq[f][0] = 1.0; bq[f][1] = (xv(f) - rc) / 1.0; bq[f][2] = (yv(f) - sc) / 1.0;
+  }
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      double a = 0.0;
+#pragma unroll
+      for (int k = 0; k < MD; k++) a = a + u[q][k] * bq[iv][k];
+      uvq[iv][q] = a;
+    }
+  const double rhomc = u[0][0], uctr = u[1][0], vctr = u[2][0], ectr = u[3][0];
+  const double rhoct = 1.0 / rhomc;
+  const double pctr = fmax(eps8, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+  const double sdctr = sqrt(fmax(eps8, g * pctr / rhoct));
+  const double dudr = fi11 * u[1][1] + fi12 * u[2][1];
+  const double duds = fi11 * u[1][2] + fi12 * u[2][2];
+  const double dvdr = fi12 * u[1][1] + fi22 * u[2][1];
+  const double dvds = fi12 * u[1][2] + fi22 * u[2][2];
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++) {
+    const double rhovt = 1.0 / uvq[iv][0];
+    const double ev = uvq[iv][3];
+    double pvtx = fmax(eps8, (g - 1.0) * rhovt * (ev - 0.5 * (uvq[iv][1] * uvq[iv][1] + uvq[iv][2] * uvq[iv][2])));
+    const double uvl = u[1][0] + dudr * bq[iv][1] + duds * bq[iv][2];
+    const double vvl = u[2][0] + dvdr * bq[iv][1] + dvds * bq[iv][2];
+    pvtx = pctr + af4 * (pvtx - pctr);
+    const double sig = -pvtx;
+    const double acnx = d.us[ip[iv]] - uvl, acny = d.vs[ip[iv]] - vvl;
+    const double nrm = sqrt(acnx * acnx + acny * acny);
+    double aj0, aj1;
+    if (nrm < TINY_S) { aj0 = TINY_S; aj1 = TINY_S; }
+    else { aj0 = acnx / nrm; aj1 = acny / nrm; }
+    const double aj2 = nrm / sdctr;
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const int edge = (f == 0) ? ((iv + 3) & 3) : iv;
+      const double n1 = fn[edge][0], n2 = fn[edge][1];
+      const double area = 0.5 * fn[edge][2];
+      // the shock term is switched off in the reference: deltu = 0 |du.n|
+      const double deltu = 0.0 * fabs(acnx * n1 + acny * n2);
+      const double murie = rhoct * sdctr + rhoct * slpdu * deltu;
+      const double vnau = (aj2 < 1.0e12) ? 1.0 : n1 * aj0 + n2 * aj1;
+      const double m = murie * area * fabs(vnau);
+      const double mu1 = m * uvl + 0.0 * vvl;
+      const double mu2 = 0.0 * uvl + m * vvl;
+      const double s1 = sig * area * n1 + 0.0 * area * n2;
+      const double s2 = 0.0 * area * n1 + sig * area * n2;
+      const int slot = f + 2 * iv;
+      d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq] = m;
+      d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq] = mu1;
+      d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq] = mu2;
+      d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq] = s1;
+      d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq] = s2;
+    }
+  }
+}
+
+template <int MD, bool FAST, int GEO>
+__device__ void cell_pass(const Dev1 &d, int iq, int rev) {
   const int e = iq;
   const double g = d.gamlg, epsd = 1.0e-6, slpdu = (g + 1.0) / 2.0;
   double x4[4][2];
@@ -612,8 +787,16 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
   d.lim[5 * nc + e] = fi12;
   d.lim[6 * nc + e] = fi22;
 
-  if (RZ) {
+  if (GEO == 1) {
     rz_corners<MD>(d, iq, x4, ip, u, bq, uvq, af[3], fi11, fi12, fi22);
+    return;
+  }
+  if (GEO == 2) {
+    // the stage's mass centre and mass matrix (Getrhslagmc.f90:6882-6885),
+    // then the corners on the vertex values about that centre
+    double rcn = rc, scn = sc;
+    if (rev) aw_rev<MD>(d, iq, x4, u, af[0], rcn, scn);
+    aw_corners<MD>(d, iq, x4, ip, u, rcn, scn, af[3], fi11, fi12, fi22);
     return;
   }
   // (4) corner Riemann coefficients (getriem_quad_matrixsym, Limiterlag.f90:
@@ -688,11 +871,15 @@ __device__ void cell_pass(const Dev1 &d, int iq) {
 }
 // compiled for 4 resident blocks of 128 per SM (128 registers): on the
 // 1024 x 512 Sod mesh 136 us per launch against 161 us at 138 registers
-template <int MD, bool FAST, bool RZ>
-__global__ void __launch_bounds__(128, 4) k1_cell(Dev1 d) {
+// GEO: 0 plane, 1 RZ (nrz = 1), 2 area-weighted RZ (nrz = 2); `stage` is
+// the RK stage (1-based): nrz = 2 renews the mass centre and mass matrix at
+// every stage but the first of step 1
+template <int MD, bool FAST, int GEO>
+__global__ void __launch_bounds__(128, 4) k1_cell(Dev1 d, int stage) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
-  cell_pass<MD, FAST, RZ>(d, iq);
+  const int rev = (GEO == 2) && (stage > 1 || d.sc_dev->itime > 1);
+  cell_pass<MD, FAST, GEO>(d, iq, rev);
 }
 
 // ---------------------------------------------------------------------------
@@ -792,12 +979,103 @@ __device__ void rz_node(const Dev1 &d, int p) {
   d.vs[p] = vs;
 }
 
-template <bool FAST, bool RZ>
+// Area-weighted RZ nodal solve (getndvelo_lagmc_rzaw, Getrhslagrz.f90:
+// 822-1100, with getbc_lagmaire_rzaw, GetBClag.f90:57-250): the node sums of
+// the two corner faces per corner in the reference's scatter order; at the
+// node's boundary faces (in face order) the area vectors of the velocity
+// walls (code 22, half the face at each end) and the pressure forces of
+// code 21 (ncase 3: p = 1e-6); fpres removes the wall-normal velocity from
+// the solve; then 221 holds v, 222 holds u and code 25 both.
+__device__ void aw_node(const Dev1 &d, int p) {
+  double n11 = 0.0, n21 = 0.0, n12 = 0.0, n22 = 0.0, a1 = 0.0, a2 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int i = d.ncor_ptr[p]; i < d.ncor_ptr[p + 1]; i++) {
+    const int c = d.ncor[i], iq = c >> 2, iv = c & 3;
+    for (int f = 0; f < 2; f++) {
+      const int slot = f + 2 * iv;
+      const double m = d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq];
+      n11 = n11 + m;
+      n21 = n21 + 0.0;
+      n12 = n12 + 0.0;
+      n22 = n22 + m;
+      a1 = a1 + d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq];
+      a2 = a2 + d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq];
+      s1 = s1 + d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq];
+      s2 = s2 + d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq];
+    }
+  }
+  double bvx = 0.0, bvy = 0.0, bpx = 0.0, bpy = 0.0;
+  bool wall22 = false;
+  for (int i = d.bf_ptr[p]; i < d.bf_ptr[p + 1]; i++) {
+    const int ifa = d.bf_list[i];
+    const int q0 = d.bfn[ifa], q1 = d.bfn[d.nbfac + ifa], code = d.bfcode[ifa];
+    const double anx = d.ys[q1] - d.ys[q0];
+    const double any = -(d.xs[q1] - d.xs[q0]);
+    const double gf3 = sqrt(anx * anx + any * any);
+    if (code / 1000 == 22) {
+      wall22 = true;
+      double bsnx = 0.0, bsny = 0.0;
+      const int sub = code % 1000;
+      if (sub == 221) {
+        bsnx = 0.0 * gf3 * 0.5;
+        bsny = -1.0 * gf3 * 0.5;
+        if (d.ncase == 1 || d.ncase == 2 || d.ncase == 12) {
+          if (d.ys[q0] < 1.0e-6 && d.ys[q1] < 1.0e-6) { bsnx = 0.0 * gf3 * 0.5; bsny = -1.0 * gf3 * 0.5; }
+          else if (fabs(d.ys[q0] - 1.0) < 1.0e-6 && fabs(d.ys[q1] - 1.0) < 1.0e-6) { bsnx = 0.0 * gf3 * 0.5; bsny = 1.0 * gf3 * 0.5; }
+        }
+      } else if (sub == 222) {
+        bsnx = -1.0 * gf3 * 0.5;
+        bsny = 0.0 * gf3 * 0.5;
+        if (d.ncase == 1) {
+          if (d.xs[q0] < 1.0e-6 && d.xs[q1] < 1.0e-6) { bsnx = -1.0 * gf3 * 0.5; bsny = 0.0 * gf3 * 0.5; }
+          else if (fabs(d.xs[q0] - 1.0) < 1.0e-6 && fabs(d.xs[q1] - 1.0) < 1.0e-6) { bsnx = 1.0 * gf3 * 0.5; bsny = 0.0 * gf3 * 0.5; }
+        }
+      }
+      bvx = bvx + bsnx;
+      bvy = bvy + bsny;
+    } else if (code / 1000 == 21 && d.ncase == 3) {
+      const double pres0 = 1.0e-6;
+      const double bsnx = anx / gf3 * gf3 * 0.5, bsny = any / gf3 * gf3 * 0.5;
+      bpx = bpx + pres0 * bsnx;
+      bpy = bpy + pres0 * bsny;
+    }
+  }
+  double fpx = 0.0, fpy = 0.0;
+  if (wall22) {
+    const double detma = n11 * n22 - n21 * n12;
+    const double i11 = n22 / detma, i12 = -n12 / detma, i21 = -n21 / detma, i22 = n11 / detma;
+    const double coefl = (i11 * bvx + i12 * bvy) * bvx + (i21 * bvx + i22 * bvy) * bvy;
+    const double rhsx = a1 - s1 - bpx, rhsy = a2 - s2 - bpy;
+    const double coefr = (i11 * rhsx + i12 * rhsy) * bvx + (i21 * rhsx + i22 * rhsy) * bvy;
+    fpx = coefr / fmax(1.0e-16, coefl) * bvx;
+    fpy = coefr / fmax(1.0e-16, coefl) * bvy;
+  }
+  fpx = fpx + bpx;
+  fpy = fpy + bpy;
+  const unsigned char bc = d.bc[p];
+  double us = d.us[p], vs = d.vs[p];
+  if (!(bc & BC_KEEP)) {
+    const double detma = n11 * n22 - n21 * n12;
+    const double i11 = n22 / detma, i12 = -n12 / detma, i21 = -n21 / detma, i22 = n11 / detma;
+    const double r1 = a1 - s1 - fpx, r2 = a2 - s2 - fpy;
+    us = i11 * r1 + i12 * r2;
+    vs = i21 * r1 + i22 * r2;
+  }
+  if (bc & (BC_V0 | BC_UV0)) vs = 0.0;
+  if (bc & (BC_U0 | BC_UV0)) us = 0.0;
+  d.us[p] = us;
+  d.vs[p] = vs;
+}
+
+template <bool FAST, int GEO>
 __global__ void k1_node(Dev1 d) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= d.npoin || stopped(d)) return;
-  if (RZ) {
+  if (GEO == 1) {
     rz_node(d, p);
+    return;
+  }
+  if (GEO == 2) {
+    aw_node(d, p);
     return;
   }
   double n11 = 0.0, n21 = 0.0, n12 = 0.0, n22 = 0.0, a1 = 0.0, a2 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -960,7 +1238,59 @@ __device__ void rz_faces(const Dev1 &d, int iq, const double (*x4)[2], double rc
   }
 }
 
-template <int MD, bool FAST, bool RZ>
+// Area-weighted RZ face integral (rhsifacedg_lagmc_quadrzaw, Getrhslagrz.f90:
+// 1673-1812): corner forces F = sigma.n A + m (u* - u_v) of the two corner
+// faces; face 1 of vertex iv (the edge to the previous vertex w) weighs
+// (2 b_iv + b_w)/3, face 2 (to the next vertex) likewise
+__device__ void aw_faces(const Dev1 &d, int iq, const double (*x4)[2], double rc, double sc, double (*R)[4]) {
+  const double c16 = 0.1666666666666666, c13 = 0.3333333333333333;
+  double fn[4][3], bq[4][ND];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int b = (f + 1) & 3;
+    const double anx = x4[b][1] - x4[f][1];
+    const double any = -(x4[b][0] - x4[f][0]);
+    fn[f][0] = anx / sqrt(anx * anx + any * any);
+    fn[f][1] = any / sqrt(anx * anx + any * any);
+    fn[f][2] = sqrt(anx * anx + any * any);
+    bq[f][0] = 1.0; bq[f][1] = (xv(f) - rc) / 1.0; bq[f][2] = (yv(f) - sc) / 1.0;
+  }
+#pragma unroll
+  for (int k = 0; k < ND; k++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) R[k][q] = 0.0;
+#pragma unroll
+  for (int iv = 0; iv < 4; iv++) {
+    const int vp = (iv + 3) & 3, vx = (iv + 1) & 3;
+    const int p = d.ipq[iv * d.nquad + iq];
+    const double us = d.us[p], vs = d.vs[p];
+    double F[2][2];
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const int slot = f + 2 * iv;
+      const double m = d.cf[(0 * 8 + slot) * (size_t)d.nquad + iq];
+      const double mu1 = d.cf[(1 * 8 + slot) * (size_t)d.nquad + iq];
+      const double mu2 = d.cf[(2 * 8 + slot) * (size_t)d.nquad + iq];
+      const double s1 = d.cf[(3 * 8 + slot) * (size_t)d.nquad + iq];
+      const double s2 = d.cf[(4 * 8 + slot) * (size_t)d.nquad + iq];
+      F[f][0] = s1 + m * us + 0.0 * vs - mu1;
+      F[f][1] = s2 + 0.0 * us + m * vs - mu2;
+    }
+#pragma unroll
+    for (int k = 0; k < ND; k++) {
+      const double wa = 2.0 * bq[iv][k] + bq[vp][k], wb = 2.0 * bq[iv][k] + bq[vx][k];
+      const double l1x = c16 * wa * fn[vp][0] * fn[vp][2], l1y = c16 * wa * fn[vp][1] * fn[vp][2];
+      const double l2x = c16 * wb * fn[iv][0] * fn[iv][2], l2y = c16 * wb * fn[iv][1] * fn[iv][2];
+      R[k][0] = R[k][0] + us * l1x + vs * l1y + us * l2x + vs * l2y;
+      R[k][1] = R[k][1] + F[0][0] * c13 * wa + F[1][0] * c13 * wb;
+      R[k][2] = R[k][2] + F[0][1] * c13 * wa + F[1][1] * c13 * wb;
+      R[k][3] = R[k][3] + us * F[0][0] * c13 * wa + vs * F[0][1] * c13 * wa + us * F[1][0] * c13 * wb +
+                vs * F[1][1] * c13 * wb;
+    }
+  }
+}
+
+template <int MD, bool FAST, int GEO>
 __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
   const int iq = blockIdx.x * blockDim.x + threadIdx.x;
   if (iq >= d.nquad || stopped(d)) return;
@@ -992,8 +1322,10 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
   for (int k = 0; k < ND; k++)
 #pragma unroll
     for (int q = 0; q < 4; q++) R[k][q] = 0.0;
-  if (RZ) {
+  if (GEO == 1) {
     rz_faces(d, iq, x4, rc, sc, R);
+  } else if (GEO == 2) {
+    aw_faces(d, iq, x4, rc, sc, R);
   } else {
 #pragma unroll
     for (int iv = 0; iv < 4; iv++) {
@@ -1060,7 +1392,7 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
     const double djaco = wi;
     // rcoef = 1 - alfrz + alfrz * ygaus (Limiterlag.f90:1268-1279): 1 in plane geometry
     double rcoef = 1.0;
-    if (RZ) {
+    if (GEO == 1) {
       const double rp = 1.0 + r, rm = 1.0 - r, sp = 1.0 + s, sm = 1.0 - s;
       const double shpq[4] = {0.25 * rm * sm, 0.25 * rp * sm, 0.25 * rp * sp, 0.25 * rm * sp};
       double ygaus = 0.0;
@@ -1086,6 +1418,22 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
     const double uadv = uctr + dudr * b1 + duds * b2;
     const double vadv = vctr + dvdr * b1 + dvds * b2;
     pres = pctr + af4 * (pres - pctr);
+    if (GEO == 2) {
+      // rhsdomndg_lagmc_quadrzaw (Getrhslagrz.f90:2243-2555): the plane
+      // fluxes written without the stress tensor, no radius weight
+#pragma unroll
+      for (int k = 0; k < ND; k++) {
+        const double f1 = g1[k] * uadv + g2[k] * vadv;
+        const double f2 = g1[k] * (-pres);
+        const double f3 = g2[k] * (-pres);
+        const double f4 = (g1[k] * uadv + g2[k] * vadv) * (-pres);
+        R[k][0] = R[k][0] - f1 * djaco;
+        R[k][1] = R[k][1] - f2 * djaco;
+        R[k][2] = R[k][2] - f3 * djaco;
+        R[k][3] = R[k][3] - f4 * djaco;
+      }
+      continue;
+    }
     const double s11 = -pres + 0.0, s12 = 0.0 + 0.0, s21 = 0.0 + 0.0, s22 = -pres + 0.0;
 #pragma unroll
     for (int k = 0; k < ND; k++) {
@@ -1099,7 +1447,42 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
       R[k][3] = R[k][3] - f4 * djaco * rcoef;
     }
   }
-  if (RZ) {
+  if (GEO == 2) {
+    // nrz = 2 (Getrhslagmc.f90:6962-6974): the right-hand side times the
+    // cell-averaged radius geoel(11), then rhsdomnsrcdg_lagmc_quadrzaw
+    // (Getrhslagrz.f90:2818-3096): 5x5 Gauss over the area, v of the cell
+    // average times b into the specific volume, -p v b (the limited
+    // pressure of the point) into the energy
+    const double rb = d.rbar[e];
+#pragma unroll
+    for (int k = 0; k < ND; k++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) R[k][q] = rb * R[k][q];
+    for (int ig = 0; ig < 25; ig++) {
+      const double r = cR.g25[ig][0], s = cR.g25[ig][1], wi = cR.w25[ig];
+      double dxdr, dxds, dydr, dyds;
+      jac4(x4, r, s, dxdr, dxds, dydr, dyds);
+      const double djaco = wi * (dxdr * dyds - dxds * dydr);
+      const double bb[ND] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+      double un[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        double a = 0.0;
+#pragma unroll
+        for (int k = 0; k < MD; k++) a = a + u[q][k] * bb[k];
+        un[q] = a;
+      }
+      const double rhoad = 1.0 / un[0];
+      double pres = (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]));
+      pres = pctr + af4 * (pres - pctr);
+#pragma unroll
+      for (int k = 0; k < ND; k++) {
+        R[k][0] = R[k][0] + vctr * bb[k] * djaco;
+        R[k][3] = R[k][3] + vctr * (-pres) * bb[k] * djaco;
+      }
+    }
+  }
+  if (GEO == 1) {
     // RZ hoop-stress source of the radial (y) momentum
     // (rhsdomnsrcdg_lagmc_quadrz, Getrhslagmc.f90:15800-16048): 5x5 Gauss,
     // the limited pressure of the point, no radius weight
@@ -1373,42 +1756,45 @@ static void geom(Solver *s, const double *X, const double *Y) {
 
 // RZ runs its own instantiations (in the reference's order: the RZ branch
 // has no optimised variant), so the plane kernels keep their registers
+template <int GEO, bool FAST>
+static void launch_cell_g(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st, int stage) {
+  if (d.mdegr == 3) k1_cell<3, FAST, GEO><<<g, b, 0, st>>>(d, stage);
+  else if (d.mdegr == 2) k1_cell<2, FAST, GEO><<<g, b, 0, st>>>(d, stage);
+  else k1_cell<1, FAST, GEO><<<g, b, 0, st>>>(d, stage);
+}
 template <bool FAST>
-static void launch_cell(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st) {
-  if (d.nrz) {
-    if (d.mdegr == 3) k1_cell<3, false, true><<<g, b, 0, st>>>(d);
-    else if (d.mdegr == 2) k1_cell<2, false, true><<<g, b, 0, st>>>(d);
-    else k1_cell<1, false, true><<<g, b, 0, st>>>(d);
-    return;
-  }
-  if (d.mdegr == 3) k1_cell<3, FAST, false><<<g, b, 0, st>>>(d);
-  else if (d.mdegr == 2) k1_cell<2, FAST, false><<<g, b, 0, st>>>(d);
-  else k1_cell<1, FAST, false><<<g, b, 0, st>>>(d);
+static void launch_cell(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st, int stage) {
+  if (d.nrz == 1) launch_cell_g<1, false>(d, g, b, st, stage);
+  else if (d.nrz == 2) launch_cell_g<2, false>(d, g, b, st, stage);
+  else launch_cell_g<0, FAST>(d, g, b, st, stage);
+}
+template <int GEO, bool FAST>
+static void launch_rhs_g(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st, int fuse, double alfa) {
+  if (d.mdegr == 3) k1_rhs<3, FAST, GEO><<<g, b, 0, st>>>(d, fuse, alfa);
+  else if (d.mdegr == 2) k1_rhs<2, FAST, GEO><<<g, b, 0, st>>>(d, fuse, alfa);
+  else k1_rhs<1, FAST, GEO><<<g, b, 0, st>>>(d, fuse, alfa);
 }
 template <bool FAST>
 static void launch_rhs(const Dev1 &d, dim3 g, dim3 b, cudaStream_t st, int fuse, double alfa) {
-  if (d.nrz) {
-    if (d.mdegr == 3) k1_rhs<3, false, true><<<g, b, 0, st>>>(d, fuse, alfa);
-    else if (d.mdegr == 2) k1_rhs<2, false, true><<<g, b, 0, st>>>(d, fuse, alfa);
-    else k1_rhs<1, false, true><<<g, b, 0, st>>>(d, fuse, alfa);
-    return;
-  }
-  if (d.mdegr == 3) k1_rhs<3, FAST, false><<<g, b, 0, st>>>(d, fuse, alfa);
-  else if (d.mdegr == 2) k1_rhs<2, FAST, false><<<g, b, 0, st>>>(d, fuse, alfa);
-  else k1_rhs<1, FAST, false><<<g, b, 0, st>>>(d, fuse, alfa);
+  if (d.nrz == 1) launch_rhs_g<1, false>(d, g, b, st, fuse, alfa);
+  else if (d.nrz == 2) launch_rhs_g<2, false>(d, g, b, st, fuse, alfa);
+  else launch_rhs_g<0, FAST>(d, g, b, st, fuse, alfa);
 }
 
 // the stage sequence of getrhsdg_lag_mcnew's linear branch
-static void enqueue_rhs(Solver *s, int fuse, double alfa) {
+static void enqueue_rhs(Solver *s, int fuse, double alfa, int stage) {
   const Dev1 &d = s->d;
   launch(s, "bounds", [&] { k1_bounds<<<nb(d.npoin, 256), 256, 0, s->st>>>(d); });
   const dim3 gq(nb(d.nquad, 128)), bq(128), gp(nb(d.npoin, 256)), bp(256);
   const bool ex = s->cfg.order_exact != 0;
-  launch(s, "cell", [&] { ex ? launch_cell<false>(d, gq, bq, s->st) : launch_cell<true>(d, gq, bq, s->st); });
+  launch(s, "cell", [&] {
+    ex ? launch_cell<false>(d, gq, bq, s->st, stage) : launch_cell<true>(d, gq, bq, s->st, stage);
+  });
   launch(s, "node", [&] {
-    if (d.nrz) k1_node<false, true><<<gp, bp, 0, s->st>>>(d);
-    else if (ex) k1_node<false, false><<<gp, bp, 0, s->st>>>(d);
-    else k1_node<true, false><<<gp, bp, 0, s->st>>>(d);
+    if (d.nrz == 1) k1_node<false, 1><<<gp, bp, 0, s->st>>>(d);
+    else if (d.nrz == 2) k1_node<false, 2><<<gp, bp, 0, s->st>>>(d);
+    else if (ex) k1_node<false, 0><<<gp, bp, 0, s->st>>>(d);
+    else k1_node<true, 0><<<gp, bp, 0, s->st>>>(d);
   });
   launch(s, "rhs", [&] {
     ex ? launch_rhs<false>(d, gq, bq, s->st, fuse, alfa) : launch_rhs<true>(d, gq, bq, s->st, fuse, alfa);
@@ -1420,7 +1806,9 @@ static void enqueue_rhs(Solver *s, int fuse, double alfa) {
 // so of the reference's getcellvol_lag calls (at the start of the step and
 // after every stage) only the one after the last stage is made: it is the
 // start-of-step volume of the next step (same coordinates, same arithmetic),
-// and set_state / init_fields compute it for the first step.
+// and set_state / init_fields compute it for the first step.  Area-weighted
+// RZ (nrz = 2) reads geoel(11) in every stage, so there it follows each
+// stage.
 static void enqueue_step(Solver *s, int itime) {
   const Dev1 &d = s->d;
   const int ns = s->cfg.nstag;
@@ -1428,7 +1816,7 @@ static void enqueue_step(Solver *s, int itime) {
   for (int istag = 1; istag <= ns; istag++) {
     const double alfa = kRK[ns - 2][istag - 1];
     if (istag == 1) {
-      enqueue_rhs(s, 0, 0.0);
+      enqueue_rhs(s, 0, 0.0, 1);
       const int nblk = nb(d.nquad, 256);
       launch(s, "dt", [&] {
         k1_dt_partial<<<nblk, 256, 0, s->st>>>(d);
@@ -1436,10 +1824,10 @@ static void enqueue_step(Solver *s, int itime) {
       }, 2);
       launch(s, "update", [&] { k1_update<<<nb(d.ncell, 128), 128, 0, s->st>>>(d, alfa); });
     } else {
-      enqueue_rhs(s, 1, alfa);
+      enqueue_rhs(s, 1, alfa, istag);
     }
     launch(s, "nodes", [&] { k1_nodes<<<nb(d.npoin, 256), 256, 0, s->st>>>(d, alfa); });
-    if (istag == ns) geom(s, d.xs, d.ys);
+    if (istag == ns || d.nrz == 2) geom(s, d.xs, d.ys);
   }
   launch(s, "copy", [&] {
     k1_copyback<<<nb(std::max(NU1 * d.ncell, d.npoin), 256), 256, 0, s->st>>>(d);
@@ -1476,8 +1864,8 @@ int create(const lag2d_mesh *m, const lag2d_config *c, cudaStream_t st, Solver *
   const int nsu = m->esuv2[np];
   for (int i = 0; i < nsu; i++)
     if (m->esuv1[i] < 1 || m->esuv1[i] > nq) { err = "esuv1 cell id out of range"; return LAG2D_EINVAL; }
-  if (c->nrz != 0 && c->nrz != 1) { err = "nrz = 2 (area-weighted RZ) is not built"; return LAG2D_EUNSUP; }
-  if (c->nrz == 1 && c->ncase == 7) {
+  if (c->nrz < 0 || c->nrz > 2) { err = "nrz must be 0, 1 or 2"; return LAG2D_EINVAL; }
+  if (c->nrz != 0 && c->ncase == 7) {
     err = "RZ Sedov runs a hard-coded dt schedule (Getrhslag.f90:1673-1693) that is not built";
     return LAG2D_EUNSUP;
   }
@@ -1564,7 +1952,7 @@ int create(const lag2d_mesh *m, const lag2d_config *c, cudaStream_t st, Solver *
        dalloc(s, &d.Un, NU1 * ncl) && dalloc(s, &d.Us, NU1 * ncl) && dalloc(s, &d.xn, np) && dalloc(s, &d.yn, np) &&
        dalloc(s, &d.xs, np) && dalloc(s, &d.ys, np) && dalloc(s, &d.us, np) && dalloc(s, &d.vs, np) &&
        dalloc(s, &d.bmax, 5 * (size_t)np) && dalloc(s, &d.bmin, 5 * (size_t)np) && dalloc(s, &d.lim, 7 * ncl) &&
-       dalloc(s, &d.cf, (c->nrz ? 80 : 40) * ncl) && dalloc(s, &d.rhs, NU1 * ncl) &&
+       dalloc(s, &d.cf, (c->nrz == 1 ? 80 : 40) * ncl) && dalloc(s, &d.rhs, NU1 * ncl) && dalloc(s, &d.rbar, ncl) &&
        dalloc(s, &d.dtpart, 2 * (size_t)nb(nq, 256)) && dalloc(s, &d.sc_dev, 1) &&
        dalloc(s, &s->stage_u, NU1 * ncl) && dalloc(s, &s->stage_x, 2 * (size_t)np);
   if (!ok) {
@@ -1607,6 +1995,11 @@ static int download_geoel(Solver *s, double *geoel, std::string &err) {
     CK1(cudaMemcpyAsync(f.data(), src[k], ncell * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK1(cudaStreamSynchronize(s->st));
     for (int e = 0; e < ncell; e++) geoel[24 * (size_t)e + k] = f[e];
+  }
+  if (d.nrz == 2) {  // geoel(11), the cell-averaged radius
+    CK1(cudaMemcpyAsync(f.data(), d.rbar, ncell * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK1(cudaStreamSynchronize(s->st));
+    for (int e = 0; e < ncell; e++) geoel[24 * (size_t)e + 10] = f[e];
   }
   return LAG2D_OK;
 }
@@ -1761,7 +2154,7 @@ int rhs(Solver *s, double *rhsel, std::string &err) {
   const Dev1 &d = s->d;
   int r = put_scalars(s, 1, 0.0, 0.0, err);
   if (r) return r;
-  enqueue_rhs(s, 0, 0.0);
+  enqueue_rhs(s, 0, 0.0, 1);
   // the slope application of :7283-7298 alone: the update with alfa = 0 and dt = 0
   launch(s, "update", [&] { k1_update<<<nb(d.ncell, 128), 128, 0, s->st>>>(d, 0.0); });
   if ((r = read_status(s, err))) return r;

@@ -339,9 +339,11 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
             double *geoel, double *amatr, double *unkno) {
   const int ntria = m->ntria, nquad = m->nquad;
   const int ncell = ntria + nquad, nsize = ncell + m->nbfac;
-  /* alfrz (dgflo2d.f90:150-156): 1 in RZ, where the cell integrals carry the
-   * radius y as a weight; RZ is dispatched on linear cells only */
-  const double alfrz = (c->npoly == 1 && c->nrz == 1) ? 1.0 : 0.0;
+  /* alfrz (dgflo2d.f90:150-156): 1 in RZ (nrz = 1 or 2), where the cell
+   * integrals carry the radius y as a weight; RZ is dispatched on linear
+   * cells only */
+  const double alfrz = (c->npoly == 1 && c->nrz >= 1) ? 1.0 : 0.0;
+  const int aw = (c->npoly == 1 && c->nrz == 2);
   double pos36[36][2], w36[36], pos25[25][2], w25[25];
   quad_rule(36, 0, pos36, w36);
   quad_rule(25, 0, pos25, w25);
@@ -359,6 +361,7 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
     shp9(0.0, 0.0, shp, NULL, NULL);
     map9((const double(*)[2])xp, shp, &xc, &yc);
     double xcent = 0, ycent = 0, xcel = 0, ycel = 0, volel = 0, masel = 0;
+    double maselrz = 0, xcerz = 0, ycerz = 0, xceli = 0, yceli = 0, areel = 0;
     for (int ig = 0; ig < 36; ig++) {
       double r = pos36[ig][0], s = pos36[ig][1], wi = w36[ig];
       double a, b, cc, d, xg, yg;
@@ -374,6 +377,14 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
       ycent = ycent + rhog * s * djaco * rcoef;
       xcel = xcel + djaco * r * rcoef;
       ycel = ycel + djaco * s * rcoef;
+      if (aw) {  /* the area (plane) integrals of nrz = 2 (GetInitial.f90:1655-1666) */
+        maselrz = maselrz + rhog * djaco;
+        xcerz = xcerz + rhog * r * djaco;
+        ycerz = ycerz + rhog * s * djaco;
+        xceli = xceli + djaco * r;
+        yceli = yceli + djaco * s;
+        areel = areel + djaco;
+      }
     }
     G_(geoel, 0, ielem) = xcent / masel;
     G_(geoel, 1, ielem) = ycent / masel;
@@ -386,6 +397,16 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
     }
     G_(geoel, 6, ielem) = xcel / volel;
     G_(geoel, 7, ielem) = ycel / volel;
+    if (aw) {  /* GetInitial.f90:1682-1691: geoel(11) the cell-averaged radius */
+      G_(geoel, 0, ielem) = xcerz / maselrz;
+      G_(geoel, 1, ielem) = ycerz / maselrz;
+      G_(geoel, 2, ielem) = volel;
+      G_(geoel, 3, ielem) = maselrz;
+      G_(geoel, 6, ielem) = xceli / areel;
+      G_(geoel, 7, ielem) = yceli / areel;
+      G_(geoel, 10, ielem) = volel / areel;
+      G_(geoel, 11, ielem) = areel;
+    }
   }
 
   if (c->npoly == 2) {
@@ -449,7 +470,9 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
       map9((const double(*)[2])xp, shp, &xg, &yg);
       getunkin(c, unkin, xg, yg, ielem + 1, volel, xcel, ycel);
       double rcoef = 1.0 - alfrz + alfrz * yg;
-      for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
+      /* nrz = 2 integrates over the area (Getrhslagmc.f90:3744-3754) */
+      if (aw) for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco;
+      else for (int q = 0; q < 4; q++) rv[q] = rv[q] + unkin[q] * djaco * rcoef;
     }
     for (int q = 0; q < 4; q++) U_(unkno, c, 0, q, ielem) = rv[q] / masel;
   }
@@ -491,6 +514,13 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
         for (int k = 0; k < nd; k++) rhsini[k][q] = rhsini[k][q] + unkin[q] * bq[k] * djaco;
       double rho0 = rho_initial(c, ielem, xg, yg, xc, yc);
       double rcoef = 1.0 - alfrz + alfrz * yg;
+      if (aw) {  /* GetInitial.f90:604-610: the area mass matrix */
+        f0 = f0 + rho0 * djaco;
+        for (int ix = 0; ix < nb; ix++)
+          for (int iy = 0; iy < nb; iy++)
+            mmatr[ix + nb * iy] = mmatr[ix + nb * iy] + rho0 * bq[ix + 1] * bq[iy + 1] * djaco;
+        continue;
+      }
       f0 = f0 + rho0 * djaco * rcoef;
       for (int ix = 0; ix < nb; ix++)
         for (int iy = 0; iy < nb; iy++)
@@ -511,6 +541,9 @@ void o_init(const o_mesh *m, const o_cfg *c, const double *coord,
         for (int jm = im; jm < 5; jm++) am[k++] = matri[im + 5 * jm];
       am[15] = 1.0 / f0;
     }
+    /* GetInitial.f90:675: nrz = 2 divides M^-1 by the cell-averaged radius
+     * (after matri, which projects the initial state, was taken) */
+    if (aw) for (int k = 0; k < nmatr; k++) am[k] = am[k] / G_(geoel, 10, ielem);
     for (int q = 0; q < 4; q++)
       for (int k = 1; k < nd; k++) U_(unkno, c, k, q, ielem) = 0.0;
     for (int q = 0; q < 4; q++)
@@ -527,12 +560,13 @@ void o_cellvol(const o_mesh *m, const o_cfg *c, double *geoel, const double *coo
   if (m->ntria > 0) cellvol_tria(m, c, geoel, coord);
   double pos36[36][2], w36[36];
   quad_rule(36, 0, pos36, w36);
-  const double alfrz = (c->npoly == 1 && c->nrz == 1) ? 1.0 : 0.0;
+  const double alfrz = (c->npoly == 1 && c->nrz >= 1) ? 1.0 : 0.0;
+  const int aw = (c->npoly == 1 && c->nrz == 2);
   for (int ie = 0; ie < m->nquad; ie++) {
     const int ielem = ie + m->ntria;
     double xp[9][2], shp[9], dr[9], ds[9];
     load_quad(m, coord, ie, xp);
-    double rcv = 0, scv = 0, volel = 0;
+    double rcv = 0, scv = 0, volel = 0, areel = 0, rcvrz = 0, scvrz = 0;
     for (int ig = 0; ig < 36; ig++) {
       double r = pos36[ig][0], s = pos36[ig][1], wi = w36[ig];
       double a, b, cc, d, xg, yg;
@@ -544,10 +578,23 @@ void o_cellvol(const o_mesh *m, const o_cfg *c, double *geoel, const double *coo
       volel = volel + djaco * rcoef;
       rcv = rcv + r * djaco * rcoef;
       scv = scv + s * djaco * rcoef;
+      if (aw) {
+        areel = areel + djaco;
+        rcvrz = rcvrz + r * djaco;
+        scvrz = scvrz + s * djaco;
+      }
     }
     G_(geoel, 2, ielem) = volel;
     G_(geoel, 4, ielem) = rcv / volel;
     G_(geoel, 5, ielem) = scv / volel;
+    if (aw) {  /* Limiterlag.f90:2149-2156 */
+      G_(geoel, 4, ielem) = rcvrz / areel;
+      G_(geoel, 5, ielem) = scvrz / areel;
+      G_(geoel, 10, ielem) = volel / areel;
+      G_(geoel, 11, ielem) = areel;
+      G_(geoel, 14, ielem) = rcvrz / areel;
+      G_(geoel, 15, ielem) = scvrz / areel;
+    }
   }
 }
 
@@ -2390,6 +2437,10 @@ double o_delt(const o_mesh *m, const o_cfg *c, const double *unkno,
   return fmin(fmin(c->cfl * dtcfl, 0.1 * dtvol), 1.01 * dtfix);
 }
 
+static void o1_rhs_x(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
+                     double *rhsel, double *geoel, const double *coord, double *amatr, int rev,
+                     double *aflim_out, double *afvec_out);
+
 /* ---------------------------------------------------------------------- */
 /* getsolvdg_lag, Getrhslag.f90:1553-2035                                 */
 /* ---------------------------------------------------------------------- */
@@ -2406,7 +2457,9 @@ void o_step(const o_mesh *m, const o_cfg *c, const double *unkno, double *unold,
   o_cellvol(m, c, geoel, coord);
   for (int istag = 1; istag <= c->nstag; istag++) {
     double alfa = rklag[c->nstag - 2][istag - 1];
-    if (c->npoly == 1) o1_rhs(m, c, ustar, unold, rhsel, geoel, cooro, NULL, NULL);
+    /* nrz = 2 rewrites amatr each stage (getamatr_lagmc_rzawrev) */
+    if (c->npoly == 1)
+      o1_rhs_x(m, c, ustar, unold, rhsel, geoel, cooro, (double *)amatr, itime > 1 || istag > 1, NULL, NULL);
     else o_rhs(m, c, ustar, unold, rhsel, geoel, cooro, coold, amatr, itime, NULL);
     if (c->ndt == 1) {
       if (istag == 1) {
@@ -2842,9 +2895,352 @@ static void o1_rz_nodes_faces(const o_mesh *m, const o_cfg *c, double *ustar, co
   free(fst); free(fpres); free(bsnv); free(bsnpf);
 }
 
-void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
-            double *rhsel, const double *geoel, const double *coord,
-            double *aflim_out, double *afvec_out) {
+/* ---------------------------------------------------------------------- */
+/* Area-weighted RZ (nrz = 2) of the linear P1 branch.  The per-stage     */
+/* geometry of getgeoel_lagmc_rzawrev (Getrhslagrz.f90:4590-4998, quads   */
+/* :4790-4990): the mass centre (geoel(1:2)) of the limited DG density    */
+/* over the cell's area, 5 fixed-point passes from the area centroid;     */
+/* then getamatr_lagmc_rzawrev (:3633-4221, quads :3990-4219): M^-1 of    */
+/* the area mass matrix about that centre, divided by geoel(11).  Both    */
+/* run at the start of every stage but the very first (Getrhslagmc.f90:   */
+/* 6882-6885); aflim is this stage's limiter (5, nquad).                  */
+/* ---------------------------------------------------------------------- */
+static void o1_rzaw_rev(const o_mesh *m, const o_cfg *c, const double *unkno, double *geoel, double *amatr,
+                        const double *coord, const double *aflim) {
+  double pos36[36][2], w36[36], pos25[25][2], w25[25];
+  quad_rule(36, 0, pos36, w36);
+  quad_rule(25, 0, pos25, w25);
+  for (int ie = 0; ie < m->nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double xp[9][2], shp[9], dr[9], ds[9];
+    load_quad(m, coord, ie, xp);
+    const double af1 = aflim[0 + 5 * ie];
+    const double rhomc = U_(unkno, c, 0, 0, ielem);
+    for (int iloop = 1; iloop <= 5; iloop++) {
+      double xcent = 0.0, ycent = 0.0, masel = 0.0;
+      const double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+      for (int ig = 0; ig < 36; ig++) {
+        const double r = pos36[ig][0], s = pos36[ig][1], wi = w36[ig];
+        double a, b, cc, d;
+        shp9(r, s, shp, dr, ds);
+        jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+        const double djaco = wi * (a * d - cc * b);
+        const double bq[3] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+        double rhomg = 0.0;
+        for (int k = 0; k < c->mdegr; k++) rhomg = rhomg + U_(unkno, c, k, 0, ielem) * bq[k];
+        if (iloop == 1) rhomg = rhomc;
+        rhomg = rhomc + af1 * (rhomg - rhomc);
+        const double rhog = 1.0 / rhomg;
+        masel = masel + 1.0 / rhomc * djaco;
+        xcent = xcent + rhog * r * djaco;
+        ycent = ycent + rhog * s * djaco;
+      }
+      G_(geoel, 0, ielem) = xcent / masel;
+      G_(geoel, 1, ielem) = ycent / masel;
+    }
+    const double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0, f3 = 0.0;
+    for (int ig = 0; ig < 25; ig++) {
+      const double r = pos25[ig][0], s = pos25[ig][1], wi = w25[ig];
+      double a, b, cc, d;
+      shp9(r, s, shp, dr, ds);
+      jac9((const double(*)[2])xp, dr, ds, &a, &b, &cc, &d);
+      const double djaco = wi * (a * d - cc * b);
+      const double bq[3] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+      double rhomg = 0.0;
+      for (int k = 0; k < c->mdegr; k++) rhomg = rhomg + U_(unkno, c, k, 0, ielem) * bq[k];
+      rhomg = rhomc + af1 * (rhomg - rhomc);
+      const double rhog = 1.0 / rhomg;
+      f0 = f0 + rhog * djaco;
+      f1 = f1 + rhog * (r - rc) / 1.0 * (r - rc) / 1.0 * djaco;
+      f2 = f2 + rhog * (r - rc) / 1.0 * (s - sc) / 1.0 * djaco;
+      f3 = f3 + rhog * (s - sc) / 1.0 * (s - sc) / 1.0 * djaco;
+    }
+    const double det = f1 * f3 - f2 * f2;
+    double *am = amatr + 4 * (size_t)ielem;
+    am[0] = f3 / det;
+    am[1] = -f2 / det;
+    am[2] = f1 / det;
+    am[3] = 1.0 / f0;
+    for (int k = 0; k < 4; k++) am[k] = am[k] / G_(geoel, 10, ielem);
+  }
+}
+
+/* ---------------------------------------------------------------------- */
+/* Area-weighted RZ (nrz = 2) nodal solve and face integral of the linear */
+/* P1 branch: getndvelo_lagmc_rzaw (Getrhslagrz.f90:822-1100) with        */
+/* getriem_quadrzaw (:1389-1669) and getbc_lagmaire_rzaw (GetBClag.f90:   */
+/* 57-250), then rhsifacedg_lagmc_quadrzaw (Getrhslagrz.f90:1673-1812).   */
+/* Quads only.  Each vertex has the two corner faces of the plane solver  */
+/* (half of each edge at the vertex, no radius weight), the impedance is  */
+/* the acoustic one and the floors are 1e-8; the face integral weighs the */
+/* corner forces with the linear basis along the edge, (2 b_v + b_w)/3.   */
+/* ---------------------------------------------------------------------- */
+static void o1_rzaw_nodes_faces(const o_mesh *m, const o_cfg *c, double *ustar, const double *unkno,
+                                double *rhsel, const double *geoel, const double *coord, const double *aflim,
+                                const double *afvec, const double *gelq) {
+  const int nquad = m->nquad, npoin = m->npoin;
+  const double g = c->gamlg, eps8 = 1.0e-08, slpdu = (g + 1.0) / 2.0;
+#define QN(ie, k) (m->ipqua[4 * (ie) + (k)] - 1)
+#define GL(f, ie) (gelq + 3 * ((f) + 4 * (ie)))
+#define AF(k, ie) aflim[(k) + 5 * (ie)]
+#define AV(i, j, ie) afvec[(i) + 2 * (j) + 4 * (ie)]
+  int *indnd = (int *)calloc((size_t)npoin, sizeof(int));
+  double *vlave = (double *)malloc(sizeof(double) * 2 * (size_t)npoin);
+  double *munacn = (double *)calloc((size_t)4 * npoin, sizeof(double));
+  double *munacu = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *snsigm = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *mcl = (double *)malloc(sizeof(double) * 4 * 8 * (size_t)nquad);  /* munaclq(2,2,2,4) */
+  double *mul = (double *)malloc(sizeof(double) * 2 * 8 * (size_t)nquad);  /* munaulq(2,2,4) */
+  double *snl = (double *)malloc(sizeof(double) * 2 * 8 * (size_t)nquad);  /* snsigmlq(2,2,4) */
+  double *fst = (double *)malloc(sizeof(double) * 2 * 8 * (size_t)nquad);  /* fsqrzaw(2,2,4) */
+  double *fpres = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *bsnv = (double *)calloc((size_t)2 * npoin, sizeof(double));
+  double *bsnpf = (double *)calloc((size_t)2 * npoin, sizeof(double));
+
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    if (c->ncase == 2) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
+  }
+  for (int ifa = 0; ifa < m->nbfac; ifa++)
+    if (m->bface[5 * ifa + 2] == 25) for (int k = 0; k < 2; k++) indnd[m->bface[5 * ifa + k] - 1] = 1;
+  /* getvlavenew's average is overwritten by the previous nodal velocity (`vlave = ustar`) */
+  memcpy(vlave, ustar, sizeof(double) * 2 * (size_t)npoin);
+
+  /* getriem_quadrzaw, scattering in cell order */
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double bq[4][3];
+    for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
+    /* face 1 of vertex iv: the edge to the previous vertex; face 2: to the next */
+    double vn[4][2][3];
+    for (int iv = 0; iv < 4; iv++) {
+      const int fa = (iv + 3) % 4, fb = iv;
+      for (int k = 0; k < 3; k++) { vn[iv][0][k] = GL(fa, ie)[k]; vn[iv][1][k] = GL(fb, ie)[k]; }
+      vn[iv][0][2] = 0.5 * vn[iv][0][2];
+      vn[iv][1][2] = 0.5 * vn[iv][1][2];
+    }
+    double rhomc = U_(unkno, c, 0, 0, ielem);
+    double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+    double rhoct = 1.0 / rhomc;
+    double pctr = fmax(eps8, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+    double unknvq[4][5], sig[4], aujmp[4][3];
+    p1_vertex(c, unkno, ielem, rc, sc, unknvq);
+    const double a11 = AV(0, 0, ie), a12 = AV(0, 1, ie), a21 = AV(1, 0, ie), a22 = AV(1, 1, ie);
+    for (int iv = 0; iv < 4; iv++) {
+      double rhovt = 1.0 / unknvq[iv][0];
+      double uv = unknvq[iv][1], vv = unknvq[iv][2], ev = unknvq[iv][3];
+      double pvtx = fmax(eps8, (g - 1.0) * rhovt * (ev - 0.5 * (uv * uv + vv * vv)));
+      double dudr = a11 * U_(unkno, c, 1, 1, ielem) + a12 * U_(unkno, c, 1, 2, ielem);
+      double duds = a11 * U_(unkno, c, 2, 1, ielem) + a12 * U_(unkno, c, 2, 2, ielem);
+      double dvdr = a21 * U_(unkno, c, 1, 1, ielem) + a22 * U_(unkno, c, 1, 2, ielem);
+      double dvds = a21 * U_(unkno, c, 2, 1, ielem) + a22 * U_(unkno, c, 2, 2, ielem);
+      uv = U_(unkno, c, 0, 1, ielem) + dudr * bq[iv][1] + duds * bq[iv][2];
+      vv = U_(unkno, c, 0, 2, ielem) + dvdr * bq[iv][1] + dvds * bq[iv][2];
+      pvtx = pctr + AF(3, ie) * (pvtx - pctr);
+      unknvq[iv][1] = uv;
+      unknvq[iv][2] = vv;
+      sig[iv] = -pvtx;
+      int ip = QN(ie, iv);
+      double acnx = X_(vlave, 0, ip) - uv, acny = X_(vlave, 1, ip) - vv;
+      double nrm = sqrt(acnx * acnx + acny * acny);
+      if (nrm < TINY_S) { aujmp[iv][0] = TINY_S; aujmp[iv][1] = TINY_S; }
+      else { aujmp[iv][0] = acnx / nrm; aujmp[iv][1] = acny / nrm; }
+      aujmp[iv][2] = nrm;
+    }
+    double sdctr = sqrt(fmax(eps8, g * pctr / rhoct));
+    for (int iv = 0; iv < 4; iv++) aujmp[iv][2] = aujmp[iv][2] / sdctr;
+    double murie[4][2];
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      double dux = X_(vlave, 0, ip) - unknvq[iv][1], duy = X_(vlave, 1, ip) - unknvq[iv][2];
+      for (int f = 0; f < 2; f++) {
+        /* the shock term is switched off: deltu = 0 * |du.n| */
+        double deltu = 0.0 * fabs(dux * vn[iv][f][0] + duy * vn[iv][f][1]);
+        murie[iv][f] = rhoct * sdctr + rhoct * slpdu * deltu;
+      }
+    }
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      for (int f = 0; f < 2; f++) {
+        /* getriecoef_matrixnew, Limiterlag.f90:1037-1076 */
+        double area = vn[iv][f][2], n1 = vn[iv][f][0], n2 = vn[iv][f][1];
+        double vnau = (aujmp[iv][2] < 1.0e12) ? 1.0 : n1 * aujmp[iv][0] + n2 * aujmp[iv][1];
+        double mc11 = murie[iv][f] * area * fabs(vnau), mc21 = 0.0, mc12 = 0.0, mc22 = murie[iv][f] * area * fabs(vnau);
+        double mu1 = mc11 * unknvq[iv][1] + mc21 * unknvq[iv][2];
+        double mu2 = mc21 * unknvq[iv][1] + mc22 * unknvq[iv][2];
+        double s1 = sig[iv] * area * n1 + 0.0 * area * n2;
+        double s2 = 0.0 * area * n1 + sig[iv] * area * n2;
+        munacn[0 + 4 * ip] = munacn[0 + 4 * ip] + mc11;
+        munacn[1 + 4 * ip] = munacn[1 + 4 * ip] + mc21;
+        munacn[2 + 4 * ip] = munacn[2 + 4 * ip] + mc12;
+        munacn[3 + 4 * ip] = munacn[3 + 4 * ip] + mc22;
+        munacu[0 + 2 * ip] = munacu[0 + 2 * ip] + mu1;
+        munacu[1 + 2 * ip] = munacu[1 + 2 * ip] + mu2;
+        snsigm[0 + 2 * ip] = snsigm[0 + 2 * ip] + s1;
+        snsigm[1 + 2 * ip] = snsigm[1 + 2 * ip] + s2;
+        const size_t o = (size_t)f + 2 * (iv + 4 * (size_t)ie);
+        mcl[4 * o + 0] = mc11; mcl[4 * o + 1] = mc21; mcl[4 * o + 2] = mc12; mcl[4 * o + 3] = mc22;
+        mul[2 * o + 0] = mu1; mul[2 * o + 1] = mu2;
+        snl[2 * o + 0] = s1; snl[2 * o + 1] = s2;
+      }
+    }
+  }
+  /* getbc_lagmaire_rzaw (GetBClag.f90:57-250): the boundary area vectors of
+   * the velocity walls (code 22, half the face at each end, no radius
+   * weight) and the pressure forces of code 21 (ncase 3: p = 1e-6); then
+   * at the wall nodes the force fpres that removes the wall-normal
+   * velocity from the node solve. */
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    const int *bf = m->bface + 5 * ifa;
+    const int ipf[2] = {bf[0] - 1, bf[1] - 1};
+    double anx = X_(coord, 1, ipf[1]) - X_(coord, 1, ipf[0]);
+    double any = -(X_(coord, 0, ipf[1]) - X_(coord, 0, ipf[0]));
+    const double gf1 = anx / sqrt(anx * anx + any * any), gf2 = any / sqrt(anx * anx + any * any);
+    const double gf3 = sqrt(anx * anx + any * any);
+    double bsnx = 0.0, bsny = 0.0;
+    if (bf[2] == 22) {
+      if (bf[3] == 221) {
+        bsnx = 0.0 * gf3 * 0.5;
+        bsny = -1.0 * gf3 * 0.5;
+        if (c->ncase == 1 || c->ncase == 2 || c->ncase == 12) {
+          if (X_(coord, 1, ipf[0]) < 1.0e-6 && X_(coord, 1, ipf[1]) < 1.0e-6) {
+            bsnx = 0.0 * gf3 * 0.5; bsny = -1.0 * gf3 * 0.5;
+          } else if (fabs(X_(coord, 1, ipf[0]) - 1.0) < 1.0e-6 && fabs(X_(coord, 1, ipf[1]) - 1.0) < 1.0e-6) {
+            bsnx = 0.0 * gf3 * 0.5; bsny = 1.0 * gf3 * 0.5;
+          }
+        }
+      } else if (bf[3] == 222) {
+        bsnx = -1.0 * gf3 * 0.5;
+        bsny = 0.0 * gf3 * 0.5;
+        if (c->ncase == 1) {
+          if (X_(coord, 0, ipf[0]) < 1.0e-6 && X_(coord, 0, ipf[1]) < 1.0e-6) {
+            bsnx = -1.0 * gf3 * 0.5; bsny = 0.0 * gf3 * 0.5;
+          } else if (fabs(X_(coord, 0, ipf[0]) - 1.0) < 1.0e-6 && fabs(X_(coord, 0, ipf[1]) - 1.0) < 1.0e-6) {
+            bsnx = 1.0 * gf3 * 0.5; bsny = 0.0 * gf3 * 0.5;
+          }
+        }
+      }
+      for (int k = 0; k < 2; k++) {
+        bsnv[0 + 2 * ipf[k]] = bsnv[0 + 2 * ipf[k]] + bsnx;
+        bsnv[1 + 2 * ipf[k]] = bsnv[1 + 2 * ipf[k]] + bsny;
+      }
+    } else if (bf[2] == 21) {
+      bsnx = gf1 * gf3 * 0.5;
+      bsny = gf2 * gf3 * 0.5;
+      if (c->ncase == 3) {
+        const double pres0 = 1.0e-6;
+        for (int k = 0; k < 2; k++) {
+          bsnpf[0 + 2 * ipf[k]] = bsnpf[0 + 2 * ipf[k]] + pres0 * bsnx;
+          bsnpf[1 + 2 * ipf[k]] = bsnpf[1 + 2 * ipf[k]] + pres0 * bsny;
+        }
+      }
+    }
+  }
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    const int *bf = m->bface + 5 * ifa;
+    if (bf[2] != 22) continue;
+    for (int k = 0; k < 2; k++) {
+      const int ip = bf[k] - 1;
+      const double *mn = munacn + 4 * ip;  /* (1,1), (2,1), (1,2), (2,2) */
+      double detma = mn[0] * mn[3] - mn[1] * mn[2];
+      double i11 = mn[3] / detma, i12 = -mn[2] / detma, i21 = -mn[1] / detma, i22 = mn[0] / detma;
+      double lnx = bsnv[0 + 2 * ip], lny = bsnv[1 + 2 * ip];
+      double coefl = (i11 * lnx + i12 * lny) * lnx + (i21 * lnx + i22 * lny) * lny;
+      double rhsx = munacu[0 + 2 * ip] - snsigm[0 + 2 * ip] - bsnpf[0 + 2 * ip];
+      double rhsy = munacu[1 + 2 * ip] - snsigm[1 + 2 * ip] - bsnpf[1 + 2 * ip];
+      double coefr = (i11 * rhsx + i12 * rhsy) * lnx + (i21 * rhsx + i22 * rhsy) * lny;
+      fpres[0 + 2 * ip] = coefr / fmax(1.0e-16, coefl) * lnx;
+      fpres[1 + 2 * ip] = coefr / fmax(1.0e-16, coefl) * lny;
+    }
+  }
+  for (int ip = 0; ip < npoin; ip++) {
+    fpres[0 + 2 * ip] = fpres[0 + 2 * ip] + bsnpf[0 + 2 * ip];
+    fpres[1 + 2 * ip] = fpres[1 + 2 * ip] + bsnpf[1 + 2 * ip];
+  }
+  /* the node solve with the boundary forces */
+  for (int ip = 0; ip < npoin; ip++) {
+    if (indnd[ip]) continue;
+    const double *mn = munacn + 4 * ip;
+    double detma = mn[0] * mn[3] - mn[1] * mn[2];
+    double i11 = mn[3] / detma, i12 = -mn[2] / detma, i21 = -mn[1] / detma, i22 = mn[0] / detma;
+    double r1 = munacu[2 * ip] - snsigm[2 * ip] - fpres[2 * ip];
+    double r2 = munacu[2 * ip + 1] - snsigm[2 * ip + 1] - fpres[2 * ip + 1];
+    X_(ustar, 0, ip) = i11 * r1 + i12 * r2;
+    X_(ustar, 1, ip) = i21 * r1 + i22 * r2;
+  }
+  /* the walls: 221 holds v, 222 holds u, code 25 both */
+  for (int ifa = 0; ifa < m->nbfac; ifa++) {
+    const int *bf = m->bface + 5 * ifa;
+    for (int k = 0; k < 2; k++) {
+      int ip = bf[k] - 1;
+      if (bf[2] == 22) {
+        if (bf[3] == 221) X_(ustar, 1, ip) = 0.0;
+        else if (bf[3] == 222) X_(ustar, 0, ip) = 0.0;
+      } else if (bf[2] == 25) {
+        X_(ustar, 1, ip) = 0.0;
+        X_(ustar, 0, ip) = 0.0;
+      }
+    }
+  }
+  /* corner forces fsqrzaw */
+  for (int ie = 0; ie < nquad; ie++)
+    for (int iv = 0; iv < 4; iv++) {
+      int ip = QN(ie, iv);
+      for (int f = 0; f < 2; f++) {
+        const size_t o = (size_t)f + 2 * (iv + 4 * (size_t)ie);
+        fst[2 * o + 0] = snl[2 * o + 0] + mcl[4 * o + 0] * X_(ustar, 0, ip) + mcl[4 * o + 1] * X_(ustar, 1, ip) - mul[2 * o + 0];
+        fst[2 * o + 1] = snl[2 * o + 1] + mcl[4 * o + 2] * X_(ustar, 0, ip) + mcl[4 * o + 3] * X_(ustar, 1, ip) - mul[2 * o + 1];
+      }
+    }
+  /* rhsifacedg_lagmc_quadrzaw: face 1 of vertex iv is the edge to the
+   * previous vertex, face 2 to the next; each weighs (2 b_iv + b_w) */
+  const double c16 = 0.1666666666666666, c13 = 0.3333333333333333;
+  for (int ie = 0; ie < nquad; ie++) {
+    const int ielem = ie + m->ntria;
+    double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+    double bq[4][3];
+    for (int iv = 0; iv < 4; iv++) { bq[iv][0] = 1.0; bq[iv][1] = (XVQ[iv] - rc) / 1.0; bq[iv][2] = (YVQ[iv] - sc) / 1.0; }
+    double ul[3] = {0, 0, 0}, p1[3] = {0, 0, 0}, p2[3] = {0, 0, 0}, el[3] = {0, 0, 0};
+    for (int iv = 0; iv < 4; iv++) {
+      const int vp = (iv + 3) % 4, vx = (iv + 1) % 4;
+      const double *ga = GL(vp, ie), *gb = GL(iv, ie);
+      int ip = QN(ie, iv);
+      double us = X_(ustar, 0, ip), vs = X_(ustar, 1, ip);
+      const size_t o0 = 2 * (iv + 4 * (size_t)ie), o1 = o0 + 1;
+      for (int k = 0; k < c->ndegr; k++) {
+        const double wa = 2.0 * bq[iv][k] + bq[vp][k], wb = 2.0 * bq[iv][k] + bq[vx][k];
+        const double l1x = c16 * wa * ga[0] * ga[2], l1y = c16 * wa * ga[1] * ga[2];
+        const double l2x = c16 * wb * gb[0] * gb[2], l2y = c16 * wb * gb[1] * gb[2];
+        ul[k] = ul[k] + us * l1x + vs * l1y + us * l2x + vs * l2y;
+        p1[k] = p1[k] + fst[2 * o0] * c13 * wa + fst[2 * o1] * c13 * wb;
+        p2[k] = p2[k] + fst[2 * o0 + 1] * c13 * wa + fst[2 * o1 + 1] * c13 * wb;
+        el[k] = el[k] + us * fst[2 * o0] * c13 * wa + vs * fst[2 * o0 + 1] * c13 * wa +
+                us * fst[2 * o1] * c13 * wb + vs * fst[2 * o1 + 1] * c13 * wb;
+      }
+    }
+    for (int k = 0; k < c->ndegr; k++) {
+      U_(rhsel, c, k, 0, ielem) = ul[k];
+      U_(rhsel, c, k, 1, ielem) = p1[k];
+      U_(rhsel, c, k, 2, ielem) = p2[k];
+      U_(rhsel, c, k, 3, ielem) = el[k];
+    }
+  }
+#undef QN
+#undef GL
+#undef AF
+#undef AV
+  free(indnd); free(vlave); free(munacn); free(munacu); free(snsigm); free(mcl); free(mul); free(snl);
+  free(fst); free(fpres); free(bsnv); free(bsnpf);
+}
+
+/* One stage's right-hand side; with nrz = 2, `amatr` (4, ncell) and
+ * `rev` = (itime > 1 or the stage > 1) select the per-stage mass centre and
+ * mass matrix of getgeoel_lagmc_rzawrev / getamatr_lagmc_rzawrev, which
+ * rewrite geoel(1:2) and amatr. */
+static void o1_rhs_x(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
+                     double *rhsel, double *geoel, const double *coord, double *amatr, int rev,
+                     double *aflim_out, double *afvec_out) {
   const int nquad = m->nquad, npoin = m->npoin;
   const double g = c->gamlg, epsd = 1.0e-6;
   const double slpdu = (g + 1.0) / 2.0;
@@ -3080,9 +3476,14 @@ void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
     AF(4, ie) = a;
   }
 
+  if (c->nrz == 2 && rev && amatr) o1_rzaw_rev(m, c, unkno, geoel, amatr, coord, aflim);
   if (c->nrz == 1) {
     /* RZ: getndvelo_lagmc_rz and rhsifacedg_lagmc_quadrz (Getrhslagmc.f90:6884-6887, :6911-6917) */
     o1_rz_nodes_faces(m, c, ustar, unkno, rhsel, geoel, coord, aflim, afvec, gelq);
+  } else if (c->nrz == 2) {
+    /* area-weighted RZ: getndvelo_lagmc_rzaw and rhsifacedg_lagmc_quadrzaw
+     * (Getrhslagmc.f90:6889-6890, :6918-6922) */
+    o1_rzaw_nodes_faces(m, c, ustar, unkno, rhsel, geoel, coord, aflim, afvec, gelq);
   } else {
     /* I.1.3 getndvelo_lag_mc_matrixsym, Limiterlag.f90:408-704 */
     for (int ifa = 0; ifa < m->nbfac; ifa++) {
@@ -3287,6 +3688,21 @@ void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
       uadv = U_(unkno, c, 0, 1, ielem) + dudr * b[1] + duds * b[2];
       vadv = U_(unkno, c, 0, 2, ielem) + dvdr * b[1] + dvds * b[2];
       pres = pctr + AF(3, ie) * (pres - pctr);
+      if (c->nrz == 2) {
+        /* rhsdomndg_lagmc_quadrzaw (Getrhslagrz.f90:2243-2555): the plane
+         * fluxes written without the stress tensor, no radius weight */
+        for (int k = 0; k < c->ndegr; k++) {
+          double f1 = gd[0][k] * uadv + gd[1][k] * vadv;
+          double f2 = gd[0][k] * (-pres);
+          double f3 = gd[1][k] * (-pres);
+          double f4 = (gd[0][k] * uadv + gd[1][k] * vadv) * (-pres);
+          U_(rhsel, c, k, 0, ielem) = U_(rhsel, c, k, 0, ielem) - f1 * djaco;
+          U_(rhsel, c, k, 1, ielem) = U_(rhsel, c, k, 1, ielem) - f2 * djaco;
+          U_(rhsel, c, k, 2, ielem) = U_(rhsel, c, k, 2, ielem) - f3 * djaco;
+          U_(rhsel, c, k, 3, ielem) = U_(rhsel, c, k, 3, ielem) - f4 * djaco;
+        }
+        continue;
+      }
       double s11 = -pres + 0.0, s12 = 0.0 + 0.0, s21 = 0.0 + 0.0, s22 = -pres + 0.0;
       for (int k = 0; k < c->ndegr; k++) {
         double f1 = gd[0][k] * uadv + gd[1][k] * vadv;
@@ -3337,6 +3753,51 @@ void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
     }
   }
 
+  /* I.1.6 for nrz = 2 (Getrhslagmc.f90:6962-6974): the right-hand side
+   * times the cell-averaged radius geoel(11), then the source terms of
+   * rhsdomnsrcdg_lagmc_quadrzaw (Getrhslagrz.f90:2818-3096): 5x5 Gauss over
+   * the area, v of the cell average times b into the specific volume and
+   * -p v b (the limited pressure of the point) into the energy */
+  if (c->nrz == 2) {
+    for (int ie = 0; ie < nquad; ie++) {
+      const int ielem = ie + m->ntria;
+      const double rb = G_(geoel, 10, ielem);
+      for (int q = 0; q < 4; q++)
+        for (int k = 0; k < c->ndegr; k++) U_(rhsel, c, k, q, ielem) = rb * U_(rhsel, c, k, q, ielem);
+    }
+    for (int ie = 0; ie < nquad; ie++) {
+      const int ielem = ie + m->ntria;
+      double xpq[4][2];
+      for (int k = 0; k < 4; k++) { xpq[k][0] = X_(coord, 0, QN(ie, k)); xpq[k][1] = X_(coord, 1, QN(ie, k)); }
+      double rc = G_(geoel, 0, ielem), sc = G_(geoel, 1, ielem);
+      for (int ig = 0; ig < 25; ig++) {
+        double r = pos25[ig][0], s = pos25[ig][1], wi = w25[ig];
+        double dxdr, dxds, dydr, dyds;
+        jac4((const double(*)[2])xpq, r, s, &dxdr, &dxds, &dydr, &dyds);
+        double djaco = wi * (dxdr * dyds - dxds * dydr);
+        double b[3] = {1.0, (r - rc) / 1.0, (s - sc) / 1.0};
+        double un[4];
+        for (int q = 0; q < 4; q++) {
+          double a = 0.0;
+          for (int k = 0; k < c->mdegr; k++) a = a + U_(unkno, c, k, q, ielem) * b[k];
+          un[q] = a;
+        }
+        double rhoad = 1.0 / un[0];
+        double pres = (g - 1.0) * rhoad * (un[3] - 0.5 * (un[1] * un[1] + un[2] * un[2]));
+        double rhomc = U_(unkno, c, 0, 0, ielem);
+        double uctr = U_(unkno, c, 0, 1, ielem), vctr = U_(unkno, c, 0, 2, ielem), ectr = U_(unkno, c, 0, 3, ielem);
+        double rhoct = 1.0 / rhomc;
+        double pctr = fmax(epsd, (g - 1.0) * rhoct * (ectr - 0.5 * (uctr * uctr + vctr * vctr)));
+        double vadv = vctr;
+        pres = pctr + AF(3, ie) * (pres - pctr);
+        for (int k = 0; k < c->ndegr; k++) {
+          U_(rhsel, c, k, 0, ielem) = U_(rhsel, c, k, 0, ielem) + vadv * b[k] * djaco;
+          U_(rhsel, c, k, 3, ielem) = U_(rhsel, c, k, 3, ielem) + vadv * (-pres) * b[k] * djaco;
+        }
+      }
+    }
+  }
+
   /* I.x.7 limited slopes into the stage state, Getrhslagmc.f90:7283-7298 */
   for (int ie = 0; ie < nquad; ie++) {
     const int ielem = ie + m->ntria;
@@ -3361,6 +3822,12 @@ void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
   free(gelq); free(unmax); free(unmin); free(aflim); free(afvec); free(mapmt); free(bnd); free(indbd);
   free(indnd); free(munacn); free(munacu); free(snsigm); free(mcl); free(mul); free(snl); free(fst);
   free(vlave);
+}
+
+void o1_rhs(const o_mesh *m, const o_cfg *c, double *ustar, double *unkno,
+            double *rhsel, const double *geoel, const double *coord,
+            double *aflim_out, double *afvec_out) {
+  o1_rhs_x(m, c, ustar, unkno, rhsel, (double *)geoel, coord, NULL, 0, aflim_out, afvec_out);
 }
 
 /* ---------------------------------------------------------------------- */

@@ -63,12 +63,14 @@ def test_create_validates_arguments_without_device():
 
 
 def test_rz_configurations_rejected_without_device():
-    """RZ is built on the linear P1 path: P2 with nrz = 1, the area-weighted
-    nrz = 2 and the RZ Sedov case (a hard-coded dt schedule) return
-    LAG2D_EUNSUP before any device work."""
+    """RZ is built on the linear P1 path: P2 with nrz = 1 or 2 and the RZ
+    Sedov case (a hard-coded dt schedule) in either RZ form return
+    LAG2D_EUNSUP (3) before any device work; nrz = 3 is LAG2D_EINVAL (1)."""
     import dataclasses
     lib = api.load()
-    for name, change in (("tgv16", {"nrz": 1}), ("noh_rz8", {"nrz": 2}), ("noh_rz8", {"ncase": 7})):
+    cases = (("tgv16", {"nrz": 1}, 3), ("tgv16", {"nrz": 2}, 3), ("noh_rz8", {"ncase": 7}, 3),
+             ("noh_rz8", {"nrz": 2, "ncase": 7}, 3), ("noh_rz8", {"nrz": 3}, 1))
+    for name, change, rc in cases:
         m, c = workload(name)
         c = dataclasses.replace(c, **change)
         k = [np.ascontiguousarray(a, dtype=np.int32) for a in (m.iptri, m.ipqua, m.bface, m.esuv1, m.esuv2, m.esqua)]
@@ -79,7 +81,7 @@ def test_rz_configurations_rejected_without_device():
                       c.ngausd_geo, 0, 0, 0, (ctypes.c_int * 4)(), c.gamlg, c.cfl, c.cdrho, c.cimpd, c.tend,
                       c.sedov_energy, c.nrz)
         h = ctypes.c_void_p()
-        assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == 3, name
+        assert lib.lag2d_create(ctypes.byref(mm), ctypes.byref(cc), ctypes.byref(h)) == rc, (name, change)
         assert b"RZ" in lib.lag2d_last_error() or b"nrz" in lib.lag2d_last_error()
 
 

@@ -1,11 +1,16 @@
-"""The RZ branch (nrz = 1) of the linear P1 path on the device, through the
-C-ABI, against the CPU restatement (getndvelo_lagmc_rz with getriem_quadrz
-and getbc_lagmaire2, rhsifacedg_lagmc_quadrz, the radius-weighted volume
-integral and rhsdomnsrcdg_lagmc_quadrz; radius-weighted geometry and mass
-matrices).  The RZ kernels keep the reference's summation order, so the
-no-FMA build reproduces the restatement bit for bit; the FMA build stays
-within 1e-12 of the field scale per step.  A whole run of the spherical Noh
-implosion to t = 0.6 follows the restatement's and its exact solution."""
+"""The RZ branches of the linear P1 path on the device, through the C-ABI,
+against the CPU restatement.  nrz = 1 (true volume): getndvelo_lagmc_rz with
+getriem_quadrz and getbc_lagmaire2, rhsifacedg_lagmc_quadrz, the
+radius-weighted volume integral and rhsdomnsrcdg_lagmc_quadrz;
+radius-weighted geometry and mass matrices.  nrz = 2 (area-weighted):
+getndvelo_lagmc_rzaw with getriem_quadrzaw and getbc_lagmaire_rzaw,
+rhsifacedg_lagmc_quadrzaw, rhsdomndg_lagmc_quadrzaw, the geoel(11) scaling
+and rhsdomnsrcdg_lagmc_quadrzaw, with the per-stage mass centre and mass
+matrix of getgeoel_lagmc_rzawrev / getamatr_lagmc_rzawrev.  The RZ kernels
+keep the reference's summation order, so the no-FMA build reproduces the
+restatement bit for bit; the FMA build stays within 1e-12 of the field
+scale per step.  Whole runs of the spherical Noh implosion to t = 0.6 follow
+the restatement's and its exact solution."""
 import dataclasses
 
 import numpy as np
@@ -24,7 +29,7 @@ def _scales(u):
     return np.array(sc)
 
 
-@pytest.mark.parametrize("name", ["noh_rz8", "noh_rz_jitter16"])
+@pytest.mark.parametrize("name", ["noh_rz8", "noh_rz_jitter16", "noh_rzaw8", "noh_rzaw_jitter16"])
 @pytest.mark.parametrize("exact", [True, False])
 def test_rz_init_fields(name, exact):
     m, c = workload(name)
@@ -32,6 +37,8 @@ def test_rz_init_fields(name, exact):
     s = Lag2DSolver(m, c, exact=exact, order_exact=exact)
     g2, a2, u2 = s.init_fields()
     n = m.ncell
+    if c.nrz == 2:  # geoel(11), the cell-averaged radius
+        assert np.abs(g2[:n, 10] - geoel[:n, 10]).max() <= (0.0 if exact else 1e-13)
     if exact:
         for k in range(4):
             assert np.array_equal(g2[:n, k], geoel[:n, k]), k
@@ -47,7 +54,8 @@ def test_rz_init_fields(name, exact):
     s.close()
 
 
-@pytest.mark.parametrize("name,nsteps", [("noh_rz8", 12), ("noh_rz_jitter16", 8)])
+@pytest.mark.parametrize("name,nsteps", [("noh_rz8", 12), ("noh_rz_jitter16", 8), ("noh_rzaw8", 12),
+                                          ("noh_rzaw_jitter16", 8)])
 @pytest.mark.parametrize("exact", [True, False])
 def test_rz_steps(name, nsteps, exact):
     """Whole RK2 steps one at a time against the restatement: cell DOFs,
@@ -80,12 +88,13 @@ def test_rz_steps(name, nsteps, exact):
     s.close()
 
 
-def test_rz_noh_run_to_end_time():
+@pytest.mark.parametrize("name", ["noh_rz32", "noh_rzaw32"])
+def test_rz_noh_run_to_end_time(name):
     """The spherical Noh implosion on 32 x 32 quads to t = 0.6 through
     lag2d_run (graph-replayed steps) against the restatement's run: the same
     number of steps, the same end time, and densities that agree where the
     flow is smooth; post-shock density near 64, the pre-shock (1 + t/r)^2."""
-    m, c = workload("noh_rz32")
+    m, c = workload(name)
     o = Oracle(m, c)
     g, a, u = o.init()
     x = m.coord.copy()
@@ -105,8 +114,8 @@ def test_rz_noh_run_to_end_time():
     u2, x2, _, _ = s.get_state()
     n = m.ncell
     rho, rho2 = 1.0 / u[:n, 0, 0], 1.0 / u2[:n, 0, 0]
-    # 383 limited steps in the FMA build: 8.5e-12 measured (bit for bit in
-    # the no-FMA build with order_exact)
+    # nrz = 1: 383 limited steps, 8.5e-12 measured in the FMA build (bit for
+    # bit in the no-FMA build with order_exact); nrz = 2: 291 steps
     assert np.abs(rho2 / rho - 1.0).max() <= 1e-9
     ctr = np.array([x2[m.ipqua[i] - 1].mean(axis=0) for i in range(n)])
     r = np.hypot(ctr[:, 0], ctr[:, 1])
