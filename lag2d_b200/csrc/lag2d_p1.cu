@@ -514,13 +514,13 @@ __device__ void rz_corners(const Dev1 &d, int iq, const double (*x4)[2], const i
 // Area-weighted RZ (nrz = 2), at the start of every stage but the very
 // first: the mass centre geoel(1:2) of the limited DG density over the
 // cell's area, 5 fixed-point passes from the area centroid
-// (getgeoel_lagmc_rzawrev, Getrhslagrz.f90:4790-4990), then M^-1 of the
+// (getgeoel_lagmc_rzawrev, Getrhslagrz.f90:4812-4994), then M^-1 of the
 // area mass matrix about it divided by geoel(11) (getamatr_lagmc_rzawrev,
-// :3990-4219).  Writes rc, sc and amatr of quad iq.
+// :3949-4219).  Writes rc, sc and amatr of quad iq.
 template <int MD>
 __device__ void aw_rev(const Dev1 &d, int iq, const double (*x4)[2], const double (*u)[ND], double af1, double &rc,
                        double &sc) {
-  double xp[9][2], shp[9], dr[9], ds[9];
+  double xp[9][2], dr[9], ds[9];
   image9(x4, xp);
   const double rhomc = u[0][0];
   for (int iloop = 1; iloop <= 5; iloop++) {
@@ -561,7 +561,6 @@ __device__ void aw_rev(const Dev1 &d, int iq, const double (*x4)[2], const doubl
     f2 = f2 + rhog * (r - rc) / 1.0 * (s - sc) / 1.0 * djaco;
     f3 = f3 + rhog * (s - sc) / 1.0 * (s - sc) / 1.0 * djaco;
   }
-  (void)shp;
   const double det = f1 * f3 - f2 * f2;
   const double rb = d.rbar[iq];
   const size_t nc = d.ncell;
@@ -792,7 +791,7 @@ __device__ void cell_pass(const Dev1 &d, int iq, int rev) {
     return;
   }
   if (GEO == 2) {
-    // the stage's mass centre and mass matrix (Getrhslagmc.f90:6882-6885),
+    // the stage's mass centre and mass matrix (Getrhslagmc.f90:6883-6886),
     // then the corners on the vertex values about that centre
     double rcn = rc, scn = sc;
     if (rev) aw_rev<MD>(d, iq, x4, u, af[0], rcn, scn);
@@ -1448,7 +1447,7 @@ __global__ void __launch_bounds__(128) k1_rhs(Dev1 d, int fuse, double alfa) {
     }
   }
   if (GEO == 2) {
-    // nrz = 2 (Getrhslagmc.f90:6962-6974): the right-hand side times the
+    // nrz = 2 (Getrhslagmc.f90:6961-6973): the right-hand side times the
     // cell-averaged radius geoel(11), then rhsdomnsrcdg_lagmc_quadrzaw
     // (Getrhslagrz.f90:2818-3096): 5x5 Gauss over the area, v of the cell
     // average times b into the specific volume, -p v b (the limited

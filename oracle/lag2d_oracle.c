@@ -2898,12 +2898,12 @@ static void o1_rz_nodes_faces(const o_mesh *m, const o_cfg *c, double *ustar, co
 /* ---------------------------------------------------------------------- */
 /* Area-weighted RZ (nrz = 2) of the linear P1 branch.  The per-stage     */
 /* geometry of getgeoel_lagmc_rzawrev (Getrhslagrz.f90:4590-4998, quads   */
-/* :4790-4990): the mass centre (geoel(1:2)) of the limited DG density    */
+/* :4812-4994): the mass centre (geoel(1:2)) of the limited DG density    */
 /* over the cell's area, 5 fixed-point passes from the area centroid;     */
-/* then getamatr_lagmc_rzawrev (:3633-4221, quads :3990-4219): M^-1 of    */
+/* then getamatr_lagmc_rzawrev (:3633-4221, quads :3949-4219): M^-1 of    */
 /* the area mass matrix about that centre, divided by geoel(11).  Both    */
 /* run at the start of every stage but the very first (Getrhslagmc.f90:   */
-/* 6882-6885); aflim is this stage's limiter (5, nquad).                  */
+/* 6883-6886); aflim is this stage's limiter (5, nquad).                  */
 /* ---------------------------------------------------------------------- */
 static void o1_rzaw_rev(const o_mesh *m, const o_cfg *c, const double *unkno, double *geoel, double *amatr,
                         const double *coord, const double *aflim) {
@@ -3482,7 +3482,7 @@ static void o1_rhs_x(const o_mesh *m, const o_cfg *c, double *ustar, double *unk
     o1_rz_nodes_faces(m, c, ustar, unkno, rhsel, geoel, coord, aflim, afvec, gelq);
   } else if (c->nrz == 2) {
     /* area-weighted RZ: getndvelo_lagmc_rzaw and rhsifacedg_lagmc_quadrzaw
-     * (Getrhslagmc.f90:6889-6890, :6918-6922) */
+     * (Getrhslagmc.f90:6888-6889, :6919-6922) */
     o1_rzaw_nodes_faces(m, c, ustar, unkno, rhsel, geoel, coord, aflim, afvec, gelq);
   } else {
     /* I.1.3 getndvelo_lag_mc_matrixsym, Limiterlag.f90:408-704 */
@@ -3753,7 +3753,7 @@ static void o1_rhs_x(const o_mesh *m, const o_cfg *c, double *ustar, double *unk
     }
   }
 
-  /* I.1.6 for nrz = 2 (Getrhslagmc.f90:6962-6974): the right-hand side
+  /* I.1.6 for nrz = 2 (Getrhslagmc.f90:6961-6973): the right-hand side
    * times the cell-averaged radius geoel(11), then the source terms of
    * rhsdomnsrcdg_lagmc_quadrzaw (Getrhslagrz.f90:2818-3096): 5x5 Gauss over
    * the area, v of the cell average times b into the specific volume and
