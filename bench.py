@@ -310,8 +310,10 @@ def p1_block(args, timed, families):
     names = ("bounds", "cell", "node", "rhs", "dt", "update", "nodes", "geom", "copy")
     out = {"path": "ncurv=0, nfint=1, nlimi=6 (linear P1, straight quads); parity: bit for bit with the "
                    "oracle in the no-FMA build (tests/test_gpu_p1.py, tests/test_gpu_rz.py)",
-           "noh_rz100_note": "Noh implosion in RZ (nrz=1, y the radius): the spherical implosion on 100x100 quads"}
-    for name in ("sod200", "sod1024", "noh_rz100"):
+           "noh_rz100_note": "Noh implosion in RZ (nrz=1, y the radius): the spherical implosion on 100x100 quads",
+           "noh_rzaw100_note": "the same in the area-weighted RZ form (nrz=2): per-stage mass centre and mass "
+                               "matrix, geometry after every stage"}
+    for name in ("sod200", "sod1024", "noh_rz100", "noh_rzaw100"):
         m, c = workload(name)
         s = new_solver(m, c, None)
         ms, done, launches = timed(s)
