@@ -59,10 +59,14 @@ def _fortran_lines(values, per_line: int, w: int, d: int):
 # restart
 # ---------------------------------------------------------------------------
 def write_restart(directory: str, unkno: np.ndarray, coord: np.ndarray, ustar: np.ndarray,
-                  itime: int, tacru: float, dtfix: float, ncell: Optional[int] = None) -> Tuple[str, str]:
+                  itime: int, tacru: float, dtfix: float, ncell: Optional[int] = None,
+                  centre: Optional[np.ndarray] = None) -> Tuple[str, str]:
     """Write restartdg.dat (reference format) and restartlag.dat (coordinates,
     nodal velocities and time state) into ``directory``; ``unkno`` is
-    (nsize or ncell, nq, ndegr) as Lag2DSolver.get_state returns it."""
+    (nsize or ncell, nq, ndegr) as Lag2DSolver.get_state returns it.
+    ``centre`` (ncell, 2), geoel(1:2) of get_state, is appended to
+    restartlag.dat when given: the area-weighted RZ form (nrz = 2) moves the
+    mass centre every stage and its limiter reads it before renewing it."""
     import os
     u = np.asarray(unkno, dtype=np.float64)
     n = u.shape[0] if ncell is None else ncell
@@ -78,14 +82,20 @@ def write_restart(directory: str, unkno: np.ndarray, coord: np.ndarray, ustar: n
         f.write(f"{int(itime)} {float(tacru)!r} {float(dtfix)!r} {x.shape[0]}\n")
         for i in range(x.shape[0]):
             f.write(f"{float(x[i, 0])!r} {float(x[i, 1])!r} {float(s[i, 0])!r} {float(s[i, 1])!r}\n")
+        if centre is not None:
+            cen = np.asarray(centre, dtype=np.float64)
+            f.write(f"{cen.shape[0]}\n")
+            for e in range(cen.shape[0]):
+                f.write(f"{float(cen[e, 0])!r} {float(cen[e, 1])!r}\n")
     return p1, p2
 
 
-def read_restart(directory: str, ncell: int, nq: int = 4, ndegr: int = 6):
+def read_restart(directory: str, ncell: int, nq: int = 4, ndegr: int = 6, with_centre: bool = False):
     """Read the pair write_restart wrote: (unkno (ncell, nq, ndegr), coord
-    (npoin, 2), ustar (npoin, 2), itime, tacru, dtfix).  restartdg.dat keeps
-    16 significant digits, as the reference writes it; restartlag.dat is
-    exact."""
+    (npoin, 2), ustar (npoin, 2), itime, tacru, dtfix), and with
+    ``with_centre`` the mass centres (ncell, 2) or None if the file has
+    none.  restartdg.dat keeps 16 significant digits, as the reference
+    writes it; restartlag.dat is exact."""
     import os
     with open(os.path.join(directory, "restartdg.dat")) as f:
         vals = np.array([float(t.replace("D", "E")) for t in f.read().split()])
@@ -96,7 +106,12 @@ def read_restart(directory: str, ncell: int, nq: int = 4, ndegr: int = 6):
         head = f.readline().split()
         itime, tacru, dtfix, npoin = int(head[0]), float(head[1]), float(head[2]), int(head[3])
         rows = np.array([[float(t) for t in f.readline().split()] for _ in range(npoin)])
-    return unkno, rows[:, :2].copy(), rows[:, 2:4].copy(), itime, tacru, dtfix
+        head = f.readline().split()
+        centre = None
+        if head:
+            centre = np.array([[float(t) for t in f.readline().split()] for _ in range(int(head[0]))])
+    out = (unkno, rows[:, :2].copy(), rows[:, 2:4].copy(), itime, tacru, dtfix)
+    return out + (centre,) if with_centre else out
 
 
 # ---------------------------------------------------------------------------

@@ -84,8 +84,11 @@ def test_badcell_is_the_persson_mark():
     s.close()
 
 
-@pytest.mark.parametrize("name", ["tgv16", "sod40"])
+@pytest.mark.parametrize("name", ["tgv16", "sod40", "noh_rzaw8"])
 def test_restart_continues_the_run(tmp_path, name):
+    """A run resumed from the restart pair equals the uninterrupted run; the
+    area-weighted RZ form (nrz = 2) also restores its per-stage mass
+    centre geoel(1:2), which its limiter reads first."""
     m, c = workload(name)
     a = Lag2DSolver(m, c)
     a.init_fields()
@@ -94,15 +97,21 @@ def test_restart_continues_the_run(tmp_path, name):
     b = Lag2DSolver(m, c)
     b.init_fields()
     b.run(4)
-    u, x, us, _ = b.get_state()
-    post.write_restart(str(tmp_path), u[:m.ncell], x, us, b.itime, b.tacru, b.dtfix)
+    u, x, us, g = b.get_state()
+    cen = g[:m.ncell, :2] if c.nrz == 2 else None
+    post.write_restart(str(tmp_path), u[:m.ncell], x, us, b.itime, b.tacru, b.dtfix, centre=cen)
     b.close()
-    u2, x2, us2, it, ta, dt = post.read_restart(str(tmp_path), m.ncell, c.nq, c.ndegr)
+    u2, x2, us2, it, ta, dt, cen2 = post.read_restart(str(tmp_path), m.ncell, c.nq, c.ndegr, with_centre=True)
+    assert (cen2 is None) == (cen is None)
     r = Lag2DSolver(m, c)
-    r.init_fields()
+    g0, _, _ = r.init_fields()
     full = np.zeros((m.nsize, c.nq, c.ndegr))
     full[:m.ncell] = u2
-    r.set_state(full, x2, us2)
+    if cen2 is not None:
+        g0[:m.ncell, :2] = cen2
+        r.set_state(full, x2, us2, geoel=g0)
+    else:
+        r.set_state(full, x2, us2)
     r.itime, r.tacru, r.dtfix = it, ta, dt
     r.run(4)
     ur, xr, _, _ = r.get_state()

@@ -136,3 +136,27 @@ def test_rz_cell_output_and_profile():
     assert np.allclose(out[:, 1], 1.0 / u[:n, 0, 0], rtol=1e-15)
     assert np.all(bad == 0.0)
     s.close()
+
+
+@pytest.mark.parametrize("name", ["noh_rz100", "noh_rzaw100"])
+def test_rz_noh100_steps(name):
+    """The RZ Noh case at 100 x 100 quads in both forms: 3 graph-replayed
+    steps of the production (FMA) build against the restatement."""
+    m, c = workload(name)
+    o = Oracle(m, c)
+    g, a, u = o.init()
+    x = m.coord.copy()
+    us = np.zeros_like(x)
+    Oracle.status()  # reads and clears what earlier calls left
+    _, dt, ta = o.run(u, x, m.coord, g, a, us, 1, 3, c.dtfix, 0.0)
+    assert Oracle.status() == 0
+    s = Lag2DSolver(m, c)
+    s.init_fields()
+    assert s.run(3) == 3
+    u2, x2, _, _ = s.get_state()
+    n = m.ncell
+    err = np.abs(u2[:n, :, 0] - u[:n, :, 0]).max(axis=0) / _scales(u[:n, :, 0])
+    assert err.max() <= 1e-11, err
+    assert np.abs(x2 - x).max() <= 1e-13
+    assert abs(s.tacru - ta) <= 1e-12 * ta
+    s.close()

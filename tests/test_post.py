@@ -65,6 +65,12 @@ def test_restart_round_trip(tmp_path):
     assert (it, ta, dt) == (17, 0.123, 4.5e-4)
     lines = open(tmp_path / "restartdg.dat").read().splitlines()
     assert len(lines) == ncell * 4 * 2 and all(len(l) == 96 for l in lines)
+    assert post.read_restart(str(tmp_path), ncell, with_centre=True)[6] is None
+    # with the mass centres (nrz = 2): exact
+    cen = rng.standard_normal((ncell, 2))
+    post.write_restart(str(tmp_path), u, x, us, 17, 0.123, 4.5e-4, centre=cen)
+    r = post.read_restart(str(tmp_path), ncell, with_centre=True)
+    assert np.array_equal(r[6], cen) and np.array_equal(r[1], x)
 
 
 def test_restart_rejects_wrong_size(tmp_path):
