@@ -23,6 +23,16 @@
 #ifndef LAG2D_ACF_MINB
 #define LAG2D_ACF_MINB 2
 #endif
+// the RHS kernel: 2 resident blocks of kRhsBlock per SM leave it up to 255
+// registers and no spills (on the 1024 x 1024 Taylor-Green step 1.11 ms per
+// step against 1.49 ms at 3 blocks and 168 registers with 584 bytes of
+// spill loads per thread)
+#ifndef LAG2D_RHS_MINB
+#define LAG2D_RHS_MINB 2
+#endif
+#ifndef LAG2D_AREVF_MINB
+#define LAG2D_AREVF_MINB 3
+#endif
 #include <math.h>
 
 #include "lag2d_device.cuh"
@@ -1957,7 +1967,7 @@ __global__ void __launch_bounds__(kCornerBlock, 4) k_corner2_faces(Dev d) {
 }
 __global__ void __launch_bounds__(128) k_tgv_src2(Dev d) { f_tgv_src(d, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_node2(Dev d) { f_node(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(kRhsBlock, 3) k_rhs3(Dev d, int fuse, double alfa) {
+__global__ void __launch_bounds__(kRhsBlock, LAG2D_RHS_MINB) k_rhs3(Dev d, int fuse, double alfa) {
   extern __shared__ double rhs_stage[];
   f_rhs3(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa, rhs_stage + threadIdx.x);
 }
@@ -1990,7 +2000,7 @@ __global__ void k_init_wmom(Dev d) { f_init_wmom(d, blockIdx.x * blockDim.x + th
 // 15.65 -> 15.08 ms per step on the 1024x1024 Taylor-Green mesh), 1 (255)
 // in the FP64 one (3 would cost 12%)
 template <typename R>
-constexpr int arev_minb() { return sizeof(R) == 4 ? 3 : 1; }
+constexpr int arev_minb() { return sizeof(R) == 4 ? LAG2D_AREVF_MINB : 1; }
 __global__ void __launch_bounds__(128, LAG2D_ACF_MINB) k_a_corner_faces(Dev d, Adj a) {
   a_corner_faces(d, a, blockIdx.x * blockDim.x + threadIdx.x);
 }

@@ -34,6 +34,11 @@
 #ifndef LAG2D_MXF_MINB
 #define LAG2D_MXF_MINB 3
 #endif
+// the mixed RHS kernel at 2 resident blocks per SM: 255 registers, 60 bytes
+// of spill loads (500 at 3 blocks); 1.22 against 1.38 ms per 1024 x 1024 step
+#ifndef LAG2D_RHSMX_MINB
+#define LAG2D_RHSMX_MINB 2
+#endif
 
 namespace lag2d {
 
@@ -766,7 +771,7 @@ __global__ void __launch_bounds__(128, LAG2D_MXF_MINB) k_corner_mx_faces(Dev d) 
   m_corner_faces(d, blockIdx.x * blockDim.x + threadIdx.x);
 }
 __global__ void __launch_bounds__(128) k_tgv_src_mx(Dev d) { m_tgv_src(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(kMxBlock, 3) k_rhs_mx(Dev d, int fuse, double alfa) {
+__global__ void __launch_bounds__(kMxBlock, LAG2D_RHSMX_MINB) k_rhs_mx(Dev d, int fuse, double alfa) {
   extern __shared__ double mx_stage[];
   m_rhs(d, blockIdx.x * blockDim.x + threadIdx.x, fuse, alfa, mx_stage + threadIdx.x);
 }
