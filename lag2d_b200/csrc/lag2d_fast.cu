@@ -33,6 +33,12 @@
 #ifndef LAG2D_AREVF_MINB
 #define LAG2D_AREVF_MINB 3
 #endif
+#ifndef LAG2D_CCORR_MINB
+#define LAG2D_CCORR_MINB 4
+#endif
+#ifndef LAG2D_CFACES_MINB
+#define LAG2D_CFACES_MINB 4
+#endif
 #include <math.h>
 
 #include "lag2d_device.cuh"
@@ -1958,10 +1964,10 @@ __host__ __device__ void a_centre(const Dev &d, const Adj &a, int p) {
 }
 
 __global__ void __launch_bounds__(128) k_persson2(Dev d) { f_persson(d, blockIdx.x * blockDim.x + threadIdx.x); }
-__global__ void __launch_bounds__(128, 4) k_corner2_corr(Dev d) {
+__global__ void __launch_bounds__(128, LAG2D_CCORR_MINB) k_corner2_corr(Dev d) {
   f_corner_corr(d, blockIdx.x * blockDim.x + threadIdx.x);
 }
-__global__ void __launch_bounds__(kCornerBlock, 4) k_corner2_faces(Dev d) {
+__global__ void __launch_bounds__(kCornerBlock, LAG2D_CFACES_MINB) k_corner2_faces(Dev d) {
   extern __shared__ double faces_stage[];
   f_corner_faces(d, blockIdx.x * blockDim.x + threadIdx.x, faces_stage + threadIdx.x);
 }
